@@ -1,0 +1,405 @@
+"""Benchmark: LBVH build + closest-hit throughput on B200 (one JSON line).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload tet|tri|particles]
+
+Default workload (``tet``): the tetrahedral-mesh configuration -- 64^3 cells in
+the unit cube, five tetrahedra per cell (1,310,720 tets), interior vertices
+jittered by +-0.2 cell, per-vertex scalar; 1024x1024 orthographic rays.  One
+step = LBVH build from the resident mesh + closest hit (FP64 Pluecker test)
+with barycentric scalar interpolation for every ray.  ``value`` = rays per
+second of the whole step (build included), in Mrays/s.  ``tri`` is the
+131,072-triangle / 512^2 pinhole configuration; ``particles`` one frame of the
+16,777,216-sphere configuration (rebuild + 2048^2 primaries).
+
+Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
+on the launching stream; the L2 is flushed (256 MiB write) between steps,
+outside the events.  Multi-GPU (torchrun): every rank runs the same workload
+(independent replicas, weak scaling); the step time is the max over ranks.
+``e2e`` repeats the step through the C ABI with pinned host buffers (mesh and
+rays copied in, hits and scalars copied out every step).
+
+``--impl reference`` times the reference's own CPU code (Build32 + OpenMP
+Traverse, compiled from its sources into oracle/_ref) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+MEASURED = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM = 6650.0
+
+
+def peaks():
+    try:
+        with open(MEASURED) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:  # noqa: BLE001
+        return FALLBACK_HBM, "fallback"
+
+
+# ---------------------------------------------------------------- workloads
+def make_workload(name):
+    from surface_b200 import scenes as S
+    if name == "tet":
+        v, f, sc = S.tet_grid(64)
+        rays = S.ortho_rays(1024, 1024)
+        return dict(kind="tet", verts=v, prims=f, scalar=sc, rays=rays,
+                    config={"workload": "tet64: 1,310,720 tetrahedra (64^3 cells x 5), "
+                                        "1024x1024 orthographic rays, closest hit + "
+                                        "barycentric scalar",
+                            "prims": int(f.shape[0]), "rays": int(rays.size)})
+    if name == "tri":
+        v, f = S.displaced_octasphere(7)
+        rays = S.pinhole_rays(512, 512, (0, 0, 3), (0, 0, 0))
+        return dict(kind="tri", verts=v, prims=f, rays=rays,
+                    config={"workload": "tri131k: displaced octasphere, 131,072 triangles, "
+                                        "512x512 pinhole rays",
+                            "prims": int(f.shape[0]), "rays": int(rays.size)})
+    if name == "particles":
+        pos, rad = S.particles()
+        rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+        return dict(kind="sphere", verts=pos, radius=rad, rays=rays,
+                    config={"workload": "particles16M: 16,777,216 spheres, one frame "
+                                        "(rebuild + 2048x2048 primaries)",
+                            "prims": int(pos.shape[0]), "rays": int(rays.size)})
+    raise SystemExit(f"unknown workload {name}")
+
+
+def algorithmic_bytes_per_ray(kind, stats, nrays):
+    """Per-ray bytes the traversal must move: ray (32) + hit (16) + nodes
+    visited x node size + primitives tested x primitive record."""
+    branch, leaf, prim = (float(x) / nrays for x in stats)
+    if kind == "tet":
+        return 32 + 16 + 4 + 4 + branch * 32 + prim * (48 + 4)
+    if kind == "tri":
+        return 32 + 16 + branch * 64 + prim * 48
+    return 32 + 16 + branch * 64 + prim * (16 + 4)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    def __init__(self, device):
+        self.proc = None
+        self.device = device
+        self.path = os.path.join("/tmp", f"srt_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device),
+                 "--query-gpu=clocks.sm,clocks.max.sm,power.draw,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:  # noqa: BLE001
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:  # noqa: BLE001
+                self.proc.kill()
+        try:
+            self.f.close()
+        except Exception:  # noqa: BLE001
+            pass
+
+    def summary(self):
+        try:
+            rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+            sm = [float(r[0]) for r in rows if r[0].strip().isdigit()]
+            mx = max(float(r[1]) for r in rows)
+            names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+            reasons = sorted({names[k] for r in rows for k in range(4)
+                              if r[3 + k].strip() == "Active"})
+            return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                    "reasons": reasons, "samples": len(rows)}
+        except Exception:  # noqa: BLE001
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+
+
+# ---------------------------------------------------------------- CPU side
+def cpu_reference_step(W, nthreads=0, stride=4):
+    """Reference Build32 + OpenMP Traverse on a strided ray sample.
+    Returns (Mrays/s scaled to the full ray set, build s, trace s, sample rays)."""
+    from oracle import oracle as O
+    kind = {"tet": O.TET, "tri": O.TRI, "sphere": O.SPHERE}[W["kind"]]
+    use_ref = O.have_ref() and O.ref() is not None
+    t0 = time.perf_counter()
+    if use_ref:
+        acc = O.RefAccel(kind, W["verts"], W.get("prims"), W.get("radius"))
+    else:
+        acc = O.OracleAccel(kind, W["verts"], W.get("prims"), W.get("radius"))
+    tb = time.perf_counter() - t0
+    sample = W["rays"][::stride]
+    t0 = time.perf_counter()
+    if use_ref:
+        acc.trace(sample, nthreads=nthreads, chunk=64)
+    else:
+        acc.trace(sample, nthreads=nthreads)
+    tt = time.perf_counter() - t0
+    nr = W["rays"].size
+    value = nr / (tb + tt * (nr / sample.size)) / 1e6
+    return value, tb, tt, sample.size, ("reference" if use_ref else "port")
+
+
+def run_reference_arm(args, W):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        cpu_reference_step(W)
+    vals, tbs, tts = [], [], []
+    for _ in range(args.steps):
+        v, tb, tt, ns, kind = cpu_reference_step(W)
+        vals.append(v)
+        tbs.append(tb)
+        tts.append(tt)
+    value = statistics.median(vals)
+    nr = W["rays"].size
+    ms = 1e3 * nr / (value * 1e6)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": DTYPE[W["kind"]], "data": "synthetic",
+        "config": W["config"],
+        "build_ms": round(1e3 * statistics.median(tbs), 3),
+        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores,
+                         "kind": kind,
+                         "sample": f"full Build32 + every 4th ray ({ns} of {nr}) per step, "
+                                   f"trace time scaled to all rays; median of {args.steps}"},
+        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+METRIC = "Mrays/s (LBVH build + closest hit per step)"
+DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)"}
+
+
+# ---------------------------------------------------------------- GPU arm
+def run_ours(args, W):
+    import torch
+    import torch.distributed as dist
+
+    import surface_b200 as sb
+    from surface_b200 import _lib
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+
+    kind = W["kind"]
+    ctx = sb.Context(local)
+    Acc = {"tet": sb.TetraAccel, "tri": sb.TriangleAccel, "sphere": sb.ParticleAccel}[kind]
+    acc = Acc(ctx)
+    nr = W["rays"].size
+    verts = torch.as_tensor(W["verts"], device=dev)
+    prims = torch.as_tensor(W["prims"].astype(np.int32), device=dev) if "prims" in W else None
+    radius = torch.as_tensor(W["radius"], device=dev) if "radius" in W else None
+    scalar = torch.as_tensor(W["scalar"], device=dev) if "scalar" in W else None
+    rays = torch.as_tensor(W["rays"].view(np.float32).reshape(-1, 8), device=dev)
+    hits = torch.empty((nr, 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    def build():
+        if kind == "tri":
+            acc.Build32(sb.Mesh(verts, prims))
+        elif kind == "tet":
+            acc.Build32(sb.Tetrahedron(verts, prims))
+        else:
+            acc.Build32(sb.Particles(verts, radius))
+
+    def trace():
+        if kind == "tet":
+            return acc.Traverse(rays, hits=hits, vertex_scalar=scalar, want_scalar=True)
+        return acc.Traverse(rays, hits=hits)
+
+    def step():
+        build()
+        trace()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+
+    # traversal work counters for the roofline (one extra untimed pass)
+    st = torch.zeros(3, dtype=torch.int64, device=dev)
+    L = _lib.load()
+    opts = _lib.TraceOpts(None, None, scalar.data_ptr() if scalar is not None else None,
+                          None, None, st.data_ptr())
+    ctx.use_torch_stream()
+    _lib.check(L.srt_trace_closest(acc.h, rays.data_ptr(), nr, hits.data_ptr(),
+                                   __import__("ctypes").byref(opts)))
+    torch.cuda.synchronize()
+    stats = st.cpu().numpy().astype(np.float64)
+
+    launches0 = L.srt_ctx_launch_count(ctx.h)
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+           torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            e0, e1, e2 = ev[k]
+            e0.record()
+            build()
+            e1.record()
+            trace()
+            e2.record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = L.srt_ctx_launch_count(ctx.h) - launches0
+    build_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    trace_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    total_ms = sum(b + t for b, t in zip(build_ms, trace_ms))
+    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * nr / (ms_per_step * 1e-3) / 1e6
+
+    # ---- e2e through the C ABI with pinned host buffers
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_verts = pin(W["verts"])
+    h_prims = pin(W["prims"]) if "prims" in W else None
+    h_rad = pin(W["radius"]) if "radius" in W else None
+    h_rays = pin(W["rays"].view(np.float32).reshape(-1, 8))
+    h_hits = torch.empty((nr, 4), dtype=torch.float32).pin_memory()
+    h_scal = torch.empty((nr,), dtype=torch.float32).pin_memory()
+    import ctypes as C
+    e2e_acc = C.c_void_p()
+    _lib.check(L.srt_accel_create(ctx.h, acc.KIND, C.byref(e2e_acc)))
+    ctx.use_own_stream()
+    d_scalar = scalar
+
+    def e2e_step():
+        if kind == "tri":
+            _lib.check(L.srt_accel_build_triangles(e2e_acc, h_verts.data_ptr(),
+                                                   h_verts.shape[0], h_prims.data_ptr(),
+                                                   h_prims.shape[0]))
+        elif kind == "tet":
+            _lib.check(L.srt_accel_build_tetrahedra(e2e_acc, h_verts.data_ptr(),
+                                                    h_verts.shape[0], h_prims.data_ptr(),
+                                                    h_prims.shape[0]))
+        else:
+            _lib.check(L.srt_accel_build_spheres(e2e_acc, h_verts.data_ptr(),
+                                                 h_rad.data_ptr(), C.c_float(0.0),
+                                                 h_verts.shape[0]))
+        o = _lib.TraceOpts(None, None, d_scalar.data_ptr() if d_scalar is not None else None,
+                           h_scal.data_ptr() if kind == "tet" else None, None, None)
+        _lib.check(L.srt_trace_closest(e2e_acc, h_rays.data_ptr(), nr, h_hits.data_ptr(),
+                                       C.byref(o)))
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    L.srt_accel_destroy(e2e_acc)
+    e2e_ms = 1e3 * sum(e2e_s) / len(e2e_s)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * nr / (float(te.item()) * 1e-3) / 1e6
+    h2d = (h_verts.numel() * 4 + (h_prims.numel() * 4 if h_prims is not None else 0)
+           + (h_rad.numel() * 4 if h_rad is not None else 0) + h_rays.numel() * 4)
+    d2h = h_hits.numel() * 4 + (h_scal.numel() * 4 if kind == "tet" else 0)
+
+    # ---- roofline of the dominant kernel (traversal)
+    hbm, src = peaks()
+    bpr = algorithmic_bytes_per_ray(kind, stats, nr)
+    tr_ms = statistics.mean(trace_ms)
+    achieved = bpr * nr / (tr_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "trace", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_ray": round(bpr, 1),
+                "visits_per_ray": [round(float(x) / nr, 3) for x in stats]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, tb, tt, ns, ck = cpu_reference_step(W)
+        cpu = {"value": round(v, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
+               "kind": ck, "build_s": round(tb, 4), "trace_s": round(tt, 4),
+               "sample": f"full Build32 + every 4th ray ({ns} of {nr}), trace time "
+                         f"scaled to all rays"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(value, 3), "unit": "Mrays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_per_step, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": DTYPE[kind], "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)",
+                           parallelism=f"replicas x{world}"),
+            "build_ms": round(statistics.mean(build_ms), 4),
+            "trace_ms": round(tr_ms, 4),
+            "trace_mrays": round(nr / (tr_ms * 1e-3) / 1e6, 2),
+            "clocks": clk.summary(),
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="tet", choices=["tet", "tri", "particles"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    W = make_workload(args.workload)
+    if args.impl == "reference":
+        run_reference_arm(args, W)
+    else:
+        run_ours(args, W)
+
+
+if __name__ == "__main__":
+    main()

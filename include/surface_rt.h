@@ -1,0 +1,273 @@
+/*
+ * surface_rt.h -- C ABI of the B200 ray-tracing core (libsurface_rt.so).
+ *
+ * A drop-in for SURFACE's render/ accel classes and the ray-dispatch calls the
+ * GLES layer makes into them.  Plain pointers and sizes only.  Every entry
+ * point returns srt_status (SRT_OK = 0).
+ *
+ * Pointers passed as primitive data, rays or hits may be host or device
+ * memory; the library inspects each one (cudaPointerGetAttributes) and copies
+ * host data through its own device buffers.  Device pointers are used in
+ * place and must stay valid until the call's work has completed on the
+ * context's stream (srt_ctx_synchronize).
+ *
+ * Reference interface each group replaces (paths relative to the SURFACE tree):
+ *   srt_build_*            XxxAccel::Build32          render/render_accel_triangle.h:79,
+ *                                                     render/render_accel_tetra.h:88,
+ *                                                     render/render_accel_particle.h:86
+ *                          called from AccelBuilder   gles/gles_accel_builder.cc:572,673,867
+ *   srt_trace_closest      XxxAccel::Traverse         render/render_accel_triangle.h:88,
+ *                                                     render/render_accel_tetra.h:97,
+ *                                                     render/render_accel_particle.h:95
+ *                          called per ray from        gles/gles_render_graph.cc:224-264
+ *   srt_accel_bbox         XxxAccel::BoundingBox      render/render_accel_triangle.h:91
+ *                          called from                gles/gles_primitive.cc:174,215,271
+ *   srt_accel_dump         XxxAccel::Dump             render/render_accel_triangle.cc:1692-1719
+ *   srt_volume_march_*     the shader ray march       examples/nonuniform_volume_render/input.frag:99-141
+ *                          + Texture::Fetch           gles/gles_common.h:344-403
+ *                          -> FilterTexture3DFloat    render/render_texture.cc:946
+ *   srt_stage_*            the build's inner steps    render/render_prefix_tree_util.h:143,296,
+ *                                                     render/render_prefix_tree_util.cc:230,267,562
+ */
+#ifndef SURFACE_RT_H_
+#define SURFACE_RT_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define SRT_API __attribute__((visibility("default")))
+#else
+#define SRT_API
+#endif
+
+typedef enum {
+  SRT_OK = 0,
+  SRT_ERR_INVALID = 1,     /* bad argument (NULL, size out of range, kind) */
+  SRT_ERR_CUDA = 2,        /* CUDA runtime error (see srt_last_error) */
+  SRT_ERR_NO_MEMORY = 3,   /* device allocation failed */
+  SRT_ERR_LIMIT = 4,       /* a kernel hit a hard limit (stack depth,
+                              iteration cap) and stopped that ray */
+  SRT_ERR_UNSUPPORTED = 5  /* valid request this build does not handle */
+} srt_status;
+
+typedef enum {
+  SRT_TRIANGLES = 0,  /* TriangleAccel */
+  SRT_TETRAHEDRA = 1, /* TetraAccel */
+  SRT_SPHERES = 2     /* ParticleAccel */
+} srt_kind;
+
+#define SRT_MISS 0xFFFFFFFFu
+
+/* One ray (32 bytes, 16-byte aligned arrays give vector loads).  prev_prim /
+ * prev_t mirror Ray::prev_prim_id / prev_hit_t (render/render_ray.h:121-125):
+ * a primary ray has prev_prim = SRT_MISS.  prev_t is the previous hit's
+ * distance; the reference stores it as double but fills it from a float
+ * (gles/gles_raytrace_engine.cc:482), so float loses nothing. */
+typedef struct srt_ray {
+  float org[3];
+  uint32_t prev_prim;
+  float dir[3];
+  float prev_t;
+} srt_ray;
+
+/* Closest hit (16 bytes): Intersection::t/u/v/prim_id
+ * (render/render_intersection.h:18-24).  prim = SRT_MISS on a miss (t then
+ * holds FLT_MAX, u = v = 0). */
+typedef struct srt_hit {
+  float t;
+  float u;
+  float v;
+  uint32_t prim;
+} srt_hit;
+
+/* Optional per-call inputs/outputs of srt_trace_closest.  Any field may be
+ * NULL / 0. */
+typedef struct srt_trace_opts {
+  /* spheres: Ray::prev_hit_normal, 3 floats per ray, for the self-hit rule
+   * of SphereIsect (render/render_accel_particle.cc:2470-2489) */
+  const float *prev_normals;
+  /* tetrahedra: Intersection::subface_id per ray (entering face 0..3) */
+  uint32_t *subface;
+  /* tetrahedra: per-vertex scalar; with scalar_out, the scalar interpolated
+   * at the entering point with the entering face's barycentrics */
+  const float *vertex_scalar;
+  float *scalar_out;
+  /* triangles and spheres: geometric normal at the hit (3 floats per ray,
+   * as BuildIntersection computes it) */
+  float *normal_out;
+  /* work counters (device memory, 3 x uint64, accumulated): branch nodes
+   * visited, leaves visited, primitive tests -- the reference's
+   * TetraTraversalStatistics (render/render_accel_tetra.h:70-78) */
+  unsigned long long *stats;
+} srt_trace_opts;
+
+typedef struct srt_ctx srt_ctx;
+typedef struct srt_accel srt_accel;
+
+typedef struct srt_accel_info {
+  int32_t kind;          /* srt_kind */
+  int32_t node_bytes;    /* bytes per record in srt_accel_export's node dump */
+  uint64_t num_prims;
+  uint64_t num_nodes;    /* records in the device node array */
+  uint64_t num_branches; /* branch nodes of the reference tree */
+  uint64_t num_leaves;   /* leaf nodes of the reference tree */
+  float scene_min[3];    /* scene box used for the Morton quantisation */
+  float scene_max[3];
+  double eps_scale;      /* triangles: max scene extent; others 16 */
+} srt_accel_info;
+
+/* ---- context ---------------------------------------------------------- */
+SRT_API srt_status srt_ctx_create(int device, srt_ctx **out);
+SRT_API srt_status srt_ctx_destroy(srt_ctx *ctx);
+/* Use `stream` (a cudaStream_t) for all work of this context; NULL = the
+ * context's own stream. */
+SRT_API srt_status srt_ctx_set_stream(srt_ctx *ctx, void *stream);
+SRT_API void *srt_ctx_get_stream(srt_ctx *ctx);
+/* Wait for all queued work; reports kernel-side limit hits (SRT_ERR_LIMIT)
+ * and asynchronous CUDA errors since the last call. */
+SRT_API srt_status srt_ctx_synchronize(srt_ctx *ctx);
+/* Human-readable text of the last error on this thread. */
+SRT_API const char *srt_last_error(void);
+/* Number of kernels this context has launched so far. */
+SRT_API uint64_t srt_ctx_launch_count(srt_ctx *ctx);
+
+/* ---- acceleration structures ------------------------------------------ */
+SRT_API srt_status srt_accel_create(srt_ctx *ctx, srt_kind kind, srt_accel **out);
+SRT_API srt_status srt_accel_destroy(srt_accel *accel);
+
+/* (Re)build from nfaces triangles (3 uint32 vertex ids each) over float
+ * xyz vertices.  Reuses the accel's device buffers when they are large
+ * enough.  Asynchronous on the context stream.  nfaces >= 2, < 2^30. */
+SRT_API srt_status srt_accel_build_triangles(srt_accel *accel,
+                                             const float *vertices,
+                                             size_t nvertices,
+                                             const uint32_t *faces,
+                                             size_t nfaces);
+/* ntets tetrahedra (4 uint32 vertex ids each). */
+SRT_API srt_status srt_accel_build_tetrahedra(srt_accel *accel,
+                                              const float *vertices,
+                                              size_t nvertices,
+                                              const uint32_t *tets,
+                                              size_t ntets);
+/* n spheres: xyz centres; radius per sphere, or NULL for constant_radius
+ * (Particles::radius / constantRadius, render/render_prim_particle.h:19-27). */
+SRT_API srt_status srt_accel_build_spheres(srt_accel *accel,
+                                           const float *centers,
+                                           const float *radius,
+                                           float constant_radius, size_t n);
+
+/* Convenience: create + build. */
+SRT_API srt_status srt_build_triangles(srt_ctx *ctx, const float *vertices,
+                                       size_t nvertices, const uint32_t *faces,
+                                       size_t nfaces, srt_accel **out);
+SRT_API srt_status srt_build_tetrahedra(srt_ctx *ctx, const float *vertices,
+                                        size_t nvertices, const uint32_t *tets,
+                                        size_t ntets, srt_accel **out);
+SRT_API srt_status srt_build_spheres(srt_ctx *ctx, const float *centers,
+                                     const float *radius, float constant_radius,
+                                     size_t n, srt_accel **out);
+
+/* Root box of the built tree (synchronises the context stream). */
+SRT_API srt_status srt_accel_bbox(srt_accel *accel, double bmin[3],
+                                  double bmax[3]);
+SRT_API srt_status srt_accel_info_get(srt_accel *accel, srt_accel_info *info);
+
+/* Copy the device tree to host memory (synchronises).  Any pointer may be
+ * NULL.  nodes: info.num_nodes records of info.node_bytes (layout in
+ * DESIGN.md of this repository: two-child 64-byte nodes for triangles and
+ * spheres, own-box 32-byte nodes for tetrahedra); indices: sorted primitive
+ * ids (TriangleAccel::indices_); codes: sorted Morton codes. */
+SRT_API srt_status srt_accel_export(srt_accel *accel, void *nodes,
+                                    uint32_t *indices, uint32_t *codes);
+/* Write the reference's Dump() file (u64 node count, reference node records,
+ * u64 index count, u32 indices). */
+SRT_API srt_status srt_accel_dump(srt_accel *accel, const char *path);
+
+/* Closest hit for n rays.  opts may be NULL.  Asynchronous when rays and
+ * hits are device pointers; synchronous (results copied back) otherwise.
+ * Ray and hit arrays must be 16-byte aligned. */
+SRT_API srt_status srt_trace_closest(srt_accel *accel, const srt_ray *rays,
+                                     size_t n, srt_hit *hits,
+                                     const srt_trace_opts *opts);
+
+/* ---- build stages (bit-exact against the reference's own stages) ------ */
+/* Scene box and 30-bit Morton code per primitive, in input order. */
+SRT_API srt_status srt_stage_morton(srt_ctx *ctx, srt_kind kind,
+                                    const float *vertices, size_t nvertices,
+                                    const uint32_t *prims, const float *radius,
+                                    float constant_radius, size_t n,
+                                    uint32_t *codes, float scene_box[6]);
+/* Stable sort of (code, index) pairs by code, in place. */
+SRT_API srt_status srt_stage_sort_pairs(srt_ctx *ctx, uint32_t *codes,
+                                        uint32_t *indices, size_t n);
+/* Karras radix tree over n sorted codes: per internal node i in [0,n-2] the
+ * split child[i] and whether the left/right child is a single key. */
+SRT_API srt_status srt_stage_karras(srt_ctx *ctx, const uint32_t *codes,
+                                    size_t n, uint32_t *child, uint8_t *left_leaf,
+                                    uint8_t *right_leaf);
+
+/* ---- volume ray march --------------------------------------------------- */
+/* Emission-absorption march over a scalar FP32 grid (x fastest) through the
+ * cube [-1,1]^3 with the shader's camera and texel-corner trilinear fetch. */
+typedef struct srt_volume_params {
+  int32_t width, height;
+  int32_t max_steps;     /* hard cap on samples per ray */
+  int32_t reserved;
+  float eye[3];
+  float corner[3];       /* image-plane corner (srt_volume_camera) */
+  float du[3], dv[3];    /* image-plane step per pixel */
+  float step;            /* world distance between samples */
+  float sigma_scale;     /* extinction = sigma_scale * tf.a */
+  float alpha_max;       /* per-sample opacity clamp, < 1 */
+} srt_volume_params;
+
+/* build_cameraframe (input.frag:16-29, FP32, pi as 3.14). */
+SRT_API srt_status srt_volume_camera(int32_t width, int32_t height,
+                                     const float eye[3], const float lookat[3],
+                                     const float up[3], float fov_deg,
+                                     srt_volume_params *params);
+/* image: width*height*4 floats (premultiplied RGB, A = 1 - transmittance).
+ * transmittance (optional): per-pixel final transmittance, kept for the
+ * backward pass.  All pointers device or host. */
+SRT_API srt_status srt_volume_march_fwd(srt_ctx *ctx,
+                                        const srt_volume_params *params,
+                                        const float *density, const int32_t dims[3],
+                                        const float *tf, int32_t tf_entries,
+                                        float *image, float *transmittance);
+/* Adjoint: given d(loss)/d(image), accumulate d(loss)/d(density) and
+ * d(loss)/d(tf) (both zeroed by the caller).  Recomputes transmittance in
+ * reverse order from the forward image and final transmittance. */
+SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx,
+                                        const srt_volume_params *params,
+                                        const float *density, const int32_t dims[3],
+                                        const float *tf, int32_t tf_entries,
+                                        const float *image,
+                                        const float *transmittance,
+                                        const float *grad_image,
+                                        float *grad_density, float *grad_tf);
+
+/* ---- batched build + trace ---------------------------------------------- */
+/* Many triangle scenes of uneven size, built and traced in one pass.
+ * Scene s owns faces [face_offsets[s], face_offsets[s+1]) of `faces` (vertex
+ * ids into `vertices`) and rays [ray_offsets[s], ray_offsets[s+1]).  Hits
+ * are written per ray.  All arrays are device pointers. */
+typedef struct srt_batch srt_batch;
+SRT_API srt_status srt_batch_create(srt_ctx *ctx, srt_batch **out);
+SRT_API srt_status srt_batch_destroy(srt_batch *b);
+SRT_API srt_status srt_batch_build_trace(srt_batch *b, int32_t nscenes,
+                                         const float *vertices,
+                                         const uint32_t *faces,
+                                         const uint64_t *face_offsets,
+                                         const srt_ray *rays,
+                                         const uint64_t *ray_offsets,
+                                         srt_hit *hits);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SURFACE_RT_H_ */

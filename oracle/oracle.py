@@ -1,0 +1,514 @@
+"""ctypes bindings to the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+Two libraries live here:
+
+* ``liboracle.so`` -- the plain-C restatement of SURFACE's LBVH build, closest-hit
+  traversal, trilinear fetch and volume march (``surface_oracle.c``), built from
+  this directory by ``make -C oracle oracle``.
+* ``_ref/libsurface_ref.so`` -- the reference's own ``render/`` sources linked
+  with ``ref_harness.cc`` (``make -C oracle ref``; needs the reference tree at
+  build time, the built library travels with the working tree).
+
+Only the tests, ``__graft_entry__.smoke()`` and the CPU-baseline leg of
+``bench.py`` import this module.  The product package never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "liboracle.so")
+REF_SO = os.path.join(HERE, "_ref", "libsurface_ref.so")
+
+TRI, TET, SPHERE = 0, 1, 2
+MISS = 0xFFFFFFFF
+
+# ray / hit records shared by the oracle, the reference harness and the C ABI
+RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
+                      ("prev_t", "<f4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4")])
+# generic node (own box, leaf flag, axis, d0, d1): so_node in surface_oracle.c
+NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("leaf", "<i4"),
+                       ("axis", "<i4"), ("d0", "<u4"), ("d1", "<u4")])
+
+# test/cctest/test-prefix-tree.cc:10-23 fixture RNG parameters
+TMT_MAT1, TMT_MAT2, TMT_TMAT = 0xFA051F40, 0xFFD0FFF4, 0x58D02FFEFFBFFFBC
+
+_P = C.c_void_p
+_SZ = C.c_size_t
+
+
+def _ptr(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _build(target):
+    subprocess.run(["make", "-s", "-C", HERE, target], check=True,
+                   stdout=subprocess.DEVNULL)
+
+
+_ORACLE = None
+_REF = None
+
+
+def lib():
+    """The restatement library (built on first use if missing)."""
+    global _ORACLE
+    if _ORACLE is None:
+        if not os.path.exists(ORACLE_SO):
+            _build("oracle")
+        L = C.CDLL(ORACLE_SO)
+        L.so_build.restype = _P
+        L.so_build.argtypes = [C.c_int, _P, _P, _P, C.c_float, _SZ]
+        L.so_free.argtypes = [_P]
+        L.so_num_nodes.restype = _SZ
+        L.so_num_nodes.argtypes = [_P]
+        L.so_export.argtypes = [_P, _P, _P, _P, _P, _P]
+        L.so_export_karras.argtypes = [_P, _P, _P, _P]
+        L.so_canonicalize.restype = C.c_long
+        L.so_canonicalize.argtypes = [_P, _SZ, _SZ, _P, _SZ]
+        L.so_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, _P, _P, C.c_int]
+        L.so_morton_bits.restype = C.c_uint32
+        L.so_morton_bits.argtypes = [C.c_uint32] * 3
+        for n in ("so_morton_tris", "so_morton_tets"):
+            getattr(L, n).argtypes = [_P, _P, _SZ, _P, _P, _P]
+        L.so_morton_points.argtypes = [_P, _SZ, _P, _P, _P]
+        L.so_bbox_tris.argtypes = [_P, _P, _SZ, _P, _P]
+        L.so_bbox_tets.argtypes = [_P, _P, _SZ, _P, _P]
+        L.so_bbox_spheres.argtypes = [_P, _P, C.c_float, _SZ, _P, _P]
+        L.so_sort_pairs.argtypes = [_P, _P, _SZ]
+        L.so_karras.argtypes = [_P, _SZ, _P, _P, _P]
+        L.so_tinymt64_doubles.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32,
+                                          C.c_uint64, _SZ, _P]
+        L.so_tex3d.argtypes = [_P, _P, _P, _SZ, C.c_int, C.c_int, C.c_int, _P]
+        L.so_volume_camera.argtypes = [C.c_int, C.c_int, _P, _P, _P, C.c_float,
+                                       _P, _P, _P]
+        L.so_volume_fwd_f32.argtypes = [_P, _P, _P, _P, _P, C.c_int]
+        L.so_volume_f64.restype = C.c_double
+        L.so_volume_f64.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
+        _ORACLE = L
+    return _ORACLE
+
+
+def have_ref():
+    return os.path.exists(REF_SO)
+
+
+def ref():
+    """The reference's own code (None when it was never built here)."""
+    global _REF
+    if _REF is None:
+        if not os.path.exists(REF_SO):
+            try:
+                _build("ref")
+            except Exception:
+                pass
+        if not os.path.exists(REF_SO):
+            return None
+        L = C.CDLL(REF_SO)
+        for k in ("tri", "tet", "sphere"):
+            getattr(L, f"ref_{k}_free").argtypes = [_P]
+            getattr(L, f"ref_{k}_dump").argtypes = [_P, C.c_char_p]
+            getattr(L, f"ref_{k}_bbox").argtypes = [_P, _P, _P]
+        L.ref_tri_build.restype = _P
+        L.ref_tri_build.argtypes = [_P, _SZ, _P, _SZ]
+        L.ref_tet_build.restype = _P
+        L.ref_tet_build.argtypes = [_P, _P, _SZ]
+        L.ref_sphere_build.restype = _P
+        L.ref_sphere_build.argtypes = [_P, _P, C.c_float, _SZ]
+        L.ref_tri_trace.argtypes = [_P, _P, _SZ, _P, C.c_int, C.c_int]
+        L.ref_tet_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
+        L.ref_sphere_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
+        L.ref_node_sizes.argtypes = [_P]
+        L.ref_morton_points.argtypes = [_P, _SZ, _P, _P, _P, C.c_int]
+        L.ref_morton_tris.argtypes = [_P, _P, _SZ, _P, _P, _P]
+        L.ref_morton_tets.argtypes = [_P, _P, _SZ, _P, _P, _P]
+        L.ref_morton_code.restype = C.c_uint32
+        L.ref_morton_code.argtypes = [_P, _P, C.c_float]
+        L.ref_radix_sort.argtypes = [_P, _P, _SZ]
+        L.ref_karras.argtypes = [_P, _SZ, _P, _P, _P]
+        L.ref_tex3d.argtypes = [_P, C.c_int, C.c_int, C.c_int, C.c_int, _P, _SZ,
+                                C.c_int, C.c_int, C.c_int, _P]
+        L.ref_tinymt64_doubles.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32,
+                                           C.c_uint64, _SZ, _P]
+        _REF = L
+    return _REF
+
+
+# --------------------------------------------------------------------------
+# oracle accel
+# --------------------------------------------------------------------------
+class OracleAccel:
+    """LBVH built by the C restatement; nodes in the reference's sequential
+    emission order (depth-first, left first)."""
+
+    def __init__(self, kind, verts, faces=None, radius=None, const_radius=0.0):
+        self.kind = kind
+        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.faces = None if faces is None else np.ascontiguousarray(faces, np.uint32).reshape(-1)
+        self.radius = None if radius is None else np.ascontiguousarray(radius, np.float32)
+        n = {TRI: None, TET: None, SPHERE: None}[kind]
+        if kind == TRI:
+            n = self.faces.size // 3
+        elif kind == TET:
+            n = self.faces.size // 4
+        else:
+            n = self.verts.size // 3
+        self.n = n
+        self.h = lib().so_build(kind, _ptr(self.verts), _ptr(self.faces),
+                                _ptr(self.radius), C.c_float(const_radius), n)
+        if not self.h:
+            raise ValueError("oracle build needs at least 2 primitives")
+        nn = lib().so_num_nodes(self.h)
+        self.nodes = np.zeros(nn, NODE_DTYPE)
+        self.indices = np.zeros(n, np.uint32)
+        self.codes = np.zeros(n, np.uint32)
+        scene = np.zeros(6, np.float32)
+        eps = C.c_double()
+        lib().so_export(self.h, _ptr(self.nodes), _ptr(self.indices), _ptr(self.codes),
+                        _ptr(scene), C.byref(eps))
+        self.scene_bmin, self.scene_bmax = scene[:3].copy(), scene[3:].copy()
+        self.eps_scale = eps.value
+
+    def karras(self):
+        m = self.n - 1
+        child = np.zeros(m, np.uint32)
+        lt = np.zeros(m, np.uint8)
+        rt = np.zeros(m, np.uint8)
+        lib().so_export_karras(self.h, _ptr(child), _ptr(lt), _ptr(rt))
+        return child, lt, rt
+
+    def canonical(self):
+        return canonicalize(self.nodes, 0)
+
+    def trace(self, rays, prev_normals=None, want_subface=False, want_stats=False,
+              nthreads=0, vertex_scalar=None):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        sub = np.zeros(rays.size, np.uint32) if want_subface else None
+        st = np.zeros(3, np.uint64)
+        pn = None if prev_normals is None else np.ascontiguousarray(prev_normals, np.float32)
+        vs = None if vertex_scalar is None else np.ascontiguousarray(vertex_scalar, np.float32)
+        so = np.zeros(rays.size, np.float32) if vs is not None else None
+        lib().so_trace(self.h, _ptr(rays), rays.size, _ptr(pn), _ptr(hits), _ptr(sub),
+                       _ptr(vs), _ptr(so), _ptr(st), nthreads)
+        out = [hits]
+        if want_subface:
+            out.append(sub)
+        if vs is not None:
+            out.append(so)
+        if want_stats:
+            out.append(st)
+        return out[0] if len(out) == 1 else tuple(out)
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().so_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+def canonicalize(generic_nodes, root=0):
+    """Depth-first (left first) listing: (n, 10) uint32 records of leaf flag,
+    axis, count, offset, bmin[3], bmax[3] bits, 0, 0."""
+    g = np.ascontiguousarray(generic_nodes, NODE_DTYPE)
+    out = np.zeros((g.size, 10), np.uint32)
+    cnt = lib().so_canonicalize(_ptr(g), g.size, root, _ptr(out), g.size)
+    if cnt < 0:
+        raise ValueError("malformed tree")
+    return out[:cnt]
+
+
+# --------------------------------------------------------------------------
+# reference accel (the real thing)
+# --------------------------------------------------------------------------
+def _read_dump(path, node_size):
+    raw = open(path, "rb").read()
+    nn = int(np.frombuffer(raw, np.uint64, 1, 0)[0])
+    nodes = np.frombuffer(raw, np.uint8, nn * node_size, 8).reshape(nn, node_size)
+    off = 8 + nn * node_size
+    ni = int(np.frombuffer(raw, np.uint64, 1, off)[0])
+    idx = np.frombuffer(raw, np.uint32, ni, off + 8).copy()
+    return nodes.copy(), idx
+
+
+def _min_ref(a, b):
+    """std::min(a, b) elementwise: the first operand on ties."""
+    return np.where(b < a, b, a)
+
+
+def _max_ref(a, b):
+    return np.where(a < b, b, a)
+
+
+def generic_from_device(kind, raw):
+    """Device node records of libsurface_rt (srt_accel_export) -> generic
+    nodes.  Two-child 64-byte nodes for triangles/spheres (leaves folded into
+    the parent's child slots), own-box 32-byte nodes for tetrahedra."""
+    raw = np.ascontiguousarray(raw, np.uint8)
+    if kind == TET:
+        f = raw.view(np.float32).reshape(-1, 8)
+        u = raw.view(np.uint32).reshape(-1, 8)
+        meta, ref_ = u[:, 3], u[:, 7]
+        leaf = (meta & 0x80000000) != 0
+        g = np.zeros(f.shape[0], NODE_DTYPE)
+        g["bmin"] = f[:, 0:3]
+        g["bmax"] = f[:, 4:7]
+        g["leaf"] = leaf
+        g["axis"] = np.where(leaf, 0, meta & 3)
+        g["d0"] = np.where(leaf, meta & 0x3FFFFFFF, ref_)
+        g["d1"] = np.where(leaf, ref_, ref_ + 1)
+        return g
+    f = raw.view(np.float32).reshape(-1, 16)
+    u = raw.view(np.uint32).reshape(-1, 16)
+    nb = f.shape[0]
+    lo = [f[:, 0:3], f[:, 6:9]]
+    hi = [f[:, 3:6], f[:, 9:12]]
+    ref_ = [u[:, 12], u[:, 13]]
+    cnt = [u[:, 14] & 0x3FFFFFFF, u[:, 15] & 0x3FFFFFFF]
+    axis = u[:, 14] >> 30
+    is_leaf = np.stack([cnt[0] > 0, cnt[1] > 0], 1)  # (nb, 2), row-major order
+    nl = int(is_leaf.sum())
+    leaf_id = np.full(is_leaf.shape, -1, np.int64)
+    leaf_id[is_leaf] = nb + np.arange(nl)
+    g = np.zeros(nb + nl, NODE_DTYPE)
+    g["leaf"][:nb] = 0
+    g["axis"][:nb] = axis
+    child = [np.where(is_leaf[:, k], leaf_id[:, k], ref_[k]).astype(np.int64) for k in (0, 1)]
+    g["d0"][:nb] = child[0]
+    g["d1"][:nb] = child[1]
+    for k in (0, 1):
+        g["bmin"][child[k]] = lo[k]
+        g["bmax"][child[k]] = hi[k]
+        lk = is_leaf[:, k]
+        ids = leaf_id[lk, k]
+        g["leaf"][ids] = 1
+        g["d0"][ids] = cnt[k][lk]
+        g["d1"][ids] = ref_[k][lk]
+    g["bmin"][0] = _min_ref(lo[0][0], lo[1][0])
+    g["bmax"][0] = _max_ref(hi[0][0], hi[1][0])
+    return g
+
+
+def generic_from_two_box(slot_bmin, slot_bmax, leaf, axis, d0, d1):
+    """Reference TriangleNode / ParticleNode arrays -> generic (own box) nodes.
+    A branch keeps its children's boxes in slots 0/1; a leaf its own in slot 0."""
+    nn = leaf.size
+    g = np.zeros(nn, NODE_DTYPE)
+    g["leaf"] = leaf
+    g["axis"] = np.where(leaf == 1, 0, axis)
+    g["d0"] = d0
+    g["d1"] = d1
+    br = np.nonzero(leaf == 0)[0]
+    g["bmin"][d0[br]] = slot_bmin[br, 0]
+    g["bmax"][d0[br]] = slot_bmax[br, 0]
+    g["bmin"][d1[br]] = slot_bmin[br, 1]
+    g["bmax"][d1[br]] = slot_bmax[br, 1]
+    g["bmin"][0] = _min_ref(slot_bmin[0, 0], slot_bmin[0, 1])
+    g["bmax"][0] = _max_ref(slot_bmax[0, 0], slot_bmax[0, 1])
+    lf = np.nonzero(leaf == 1)[0]
+    # a leaf's own copy must agree with its parent's slot
+    if not (np.array_equal(g["bmin"][lf].view(np.uint32), slot_bmin[lf, 0].view(np.uint32))
+            and np.array_equal(g["bmax"][lf].view(np.uint32), slot_bmax[lf, 0].view(np.uint32))):
+        raise ValueError("leaf box differs from its parent's slot")
+    return g
+
+
+class RefAccel:
+    """The reference's own Build32 / Traverse / Dump."""
+
+    def __init__(self, kind, verts, faces=None, radius=None, const_radius=0.0):
+        L = ref()
+        if L is None:
+            raise RuntimeError("reference harness not built")
+        self.L = L
+        self.kind = kind
+        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.faces = None if faces is None else np.ascontiguousarray(faces, np.uint32).reshape(-1)
+        self.radius = None if radius is None else np.ascontiguousarray(radius, np.float32)
+        if kind == TRI:
+            self.n = self.faces.size // 3
+            self.h = L.ref_tri_build(_ptr(self.verts), self.verts.size // 3,
+                                     _ptr(self.faces), self.n)
+            self.tag = "tri"
+        elif kind == TET:
+            self.n = self.faces.size // 4
+            self.h = L.ref_tet_build(_ptr(self.verts), _ptr(self.faces), self.n)
+            self.tag = "tet"
+        else:
+            self.n = self.verts.size // 3
+            self.h = L.ref_sphere_build(_ptr(self.verts), _ptr(self.radius),
+                                        C.c_float(const_radius), self.n)
+            self.tag = "sphere"
+
+    def bbox(self):
+        mn = np.zeros(3)
+        mx = np.zeros(3)
+        getattr(self.L, f"ref_{self.tag}_bbox")(self.h, _ptr(mn), _ptr(mx))
+        return mn, mx
+
+    def dump(self):
+        """(generic nodes, sorted indices) from the reference's Dump()."""
+        sizes = np.zeros(3, np.uint64)
+        self.L.ref_node_sizes(_ptr(sizes))
+        ns = int(sizes[self.kind])
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "accel.bin")
+            getattr(self.L, f"ref_{self.tag}_dump")(self.h, path.encode())
+            raw, idx = _read_dump(path, ns)
+        if self.kind == TET:
+            f = raw[:, :24].copy().view(np.float32).reshape(-1, 6)
+            ints = raw[:, 24:40].copy().view(np.int32).reshape(-1, 4)
+            g = np.zeros(raw.shape[0], NODE_DTYPE)
+            g["bmin"] = f[:, :3]
+            g["bmax"] = f[:, 3:]
+            g["leaf"] = ints[:, 0]
+            g["axis"] = np.where(ints[:, 0] == 1, 0, ints[:, 1])
+            g["d0"] = ints[:, 2].view(np.uint32)
+            g["d1"] = ints[:, 3].view(np.uint32)
+            return g, idx
+        f = raw[:, :48].copy().view(np.float32).reshape(-1, 2, 2, 3)
+        slot_bmin, slot_bmax = f[:, 0], f[:, 1]
+        if self.kind == TRI:
+            ints = raw[:, 48:64].copy().view(np.int32).reshape(-1, 4)
+            leaf, axis = ints[:, 0], ints[:, 1]
+            d0, d1 = ints[:, 2].view(np.uint32), ints[:, 3].view(np.uint32)
+        else:
+            d = raw[:, 48:56].copy().view(np.uint32).reshape(-1, 2)
+            sh = raw[:, 56:60].copy().view(np.int16).reshape(-1, 2)
+            leaf, axis = sh[:, 0].astype(np.int32), sh[:, 1].astype(np.int32)
+            d0, d1 = d[:, 0], d[:, 1]
+        return generic_from_two_box(slot_bmin, slot_bmax, leaf, axis, d0, d1), idx
+
+    def canonical(self):
+        g, idx = self.dump()
+        return canonicalize(g, 0), idx
+
+    def trace(self, rays, prev_normals=None, nthreads=0, chunk=64):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        if self.kind == TRI:
+            self.L.ref_tri_trace(self.h, _ptr(rays), rays.size, _ptr(hits), nthreads, chunk)
+            return hits
+        if self.kind == TET:
+            sub = np.zeros(rays.size, np.uint32)
+            self.L.ref_tet_trace(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(sub),
+                                 nthreads, chunk)
+            return hits, sub
+        pn = None if prev_normals is None else np.ascontiguousarray(prev_normals, np.float32)
+        self.L.ref_sphere_trace(self.h, _ptr(rays), rays.size, _ptr(pn), _ptr(hits),
+                                nthreads, chunk)
+        return hits
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                getattr(self.L, f"ref_{self.tag}_free")(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+# --------------------------------------------------------------------------
+# stage-level helpers
+# --------------------------------------------------------------------------
+def tinymt64_doubles(n, seed=123456, use_ref=False):
+    out = np.zeros(n, np.float64)
+    if use_ref:
+        ref().ref_tinymt64_doubles(seed, TMT_MAT1, TMT_MAT2, TMT_TMAT, n, _ptr(out))
+    else:
+        lib().so_tinymt64_doubles(seed, TMT_MAT1, TMT_MAT2, TMT_TMAT, n, _ptr(out))
+    return out
+
+
+def fixture_points(n, rng_state=None, seed=123456):
+    """The reference tests' point draws: (float)genrand_double() x 3 per point."""
+    d = tinymt64_doubles(3 * n, seed)
+    return d.astype(np.float32).reshape(n, 3)
+
+
+def morton_points(pts, bmin, bmax):
+    pts = np.ascontiguousarray(pts, np.float32)
+    out = np.zeros(pts.size // 3, np.uint32)
+    lib().so_morton_points(_ptr(pts), out.size, _ptr(np.asarray(bmin, np.float32)),
+                           _ptr(np.asarray(bmax, np.float32)), _ptr(out))
+    return out
+
+
+def sort_pairs(codes, index=None):
+    c = np.ascontiguousarray(codes, np.uint32).copy()
+    i = (np.arange(c.size, dtype=np.uint32) if index is None
+         else np.ascontiguousarray(index, np.uint32).copy())
+    lib().so_sort_pairs(_ptr(c), _ptr(i), c.size)
+    return c, i
+
+
+def karras(sorted_codes):
+    c = np.ascontiguousarray(sorted_codes, np.uint32)
+    m = c.size - 1
+    child = np.zeros(m, np.uint32)
+    lt = np.zeros(m, np.uint8)
+    rt = np.zeros(m, np.uint8)
+    lib().so_karras(_ptr(c), c.size, _ptr(child), _ptr(lt), _ptr(rt))
+    return child, lt, rt
+
+
+def tex3d(img, dims, uvw, clamp=(1, 1, 1)):
+    img = np.ascontiguousarray(img, np.float32)
+    uvw = np.ascontiguousarray(uvw, np.float32)
+    out = np.zeros(uvw.size // 3, np.float32)
+    d = np.asarray(dims, np.int32)
+    lib().so_tex3d(_ptr(img), _ptr(d), _ptr(uvw), out.size, *clamp, _ptr(out))
+    return out
+
+
+# volume parameters (so_vol_params)
+VOL_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("max_steps", "<i4"),
+                      ("reserved", "<i4"), ("eye", "<f4", 3), ("corner", "<f4", 3),
+                      ("du", "<f4", 3), ("dv", "<f4", 3), ("step", "<f4"),
+                      ("sigma_scale", "<f4"), ("alpha_max", "<f4")])
+
+
+def volume_params(width, height, eye, lookat, up, fov_deg, step, sigma_scale,
+                  alpha_max, max_steps):
+    p = np.zeros(1, VOL_DTYPE)
+    p["width"], p["height"], p["max_steps"] = width, height, max_steps
+    corner = np.zeros(3, np.float32)
+    du = np.zeros(3, np.float32)
+    dv = np.zeros(3, np.float32)
+    e = np.asarray(eye, np.float32)
+    lib().so_volume_camera(width, height, _ptr(e), _ptr(np.asarray(lookat, np.float32)),
+                           _ptr(np.asarray(up, np.float32)), C.c_float(fov_deg),
+                           _ptr(corner), _ptr(du), _ptr(dv))
+    p["eye"], p["corner"], p["du"], p["dv"] = e, corner, du, dv
+    p["step"], p["sigma_scale"], p["alpha_max"] = step, sigma_scale, alpha_max
+    return p
+
+
+def volume_fwd_f32(params, dens, dims, tf, nthreads=0):
+    W, H = int(params["width"][0]), int(params["height"][0])
+    img = np.zeros((H, W, 4), np.float32)
+    lib().so_volume_fwd_f32(_ptr(params), _ptr(np.ascontiguousarray(dens, np.float32)),
+                            _ptr(np.asarray(dims, np.int32)),
+                            _ptr(np.ascontiguousarray(tf, np.float32)), _ptr(img), nthreads)
+    return img
+
+
+def volume_f64(params, dens, dims, tf, target=None, want_grad=False, want_img=False):
+    W, H = int(params["width"][0]), int(params["height"][0])
+    dens = np.ascontiguousarray(dens, np.float64)
+    tf = np.ascontiguousarray(tf, np.float64)
+    img = np.zeros((H, W, 4)) if want_img else None
+    gd = np.zeros(dens.shape) if want_grad else None
+    gt = np.zeros(tf.shape) if want_grad else None
+    tg = None if target is None else np.ascontiguousarray(target, np.float32)
+    loss = lib().so_volume_f64(_ptr(params), _ptr(dens), _ptr(np.asarray(dims, np.int32)),
+                               _ptr(tf), _ptr(tg), _ptr(img), _ptr(gd), _ptr(gt))
+    return loss, img, gd, gt

@@ -1,0 +1,345 @@
+// ref_harness.cc -- C entry points over the reference's own render/ classes.
+//
+// TEST INFRASTRUCTURE ONLY.  Compiled together with the unmodified reference
+// sources (render/render_prefix_tree_util.cc, render_accel_triangle.cc,
+// render_accel_tetra.cc, render_accel_particle.cc, render_texture.cc,
+// tinymt64.cpp) by oracle/Makefile into oracle/_ref/libsurface_ref.so.  It pins
+// the C restatement (surface_oracle.c) and serves as the timed CPU baseline
+// ("cpu_baseline.kind = reference").  Nothing here re-implements an
+// algorithm: each function only marshals plain arrays into the reference's
+// own types and calls its public API:
+//   TriangleAccel/TetraAccel/ParticleAccel::Build32, ::Traverse, ::Dump,
+//   ::BoundingBox          (render/render_accel_*.h)
+//   CalculateMortonCodes*, RadixSort30OMP, ConstructBinaryRadixTree30
+//                          (render/render_prefix_tree_util.h)
+//   FilterTexture3DFloat   (render/render_texture.h)
+//   tinymt64_*             (render/tinymt64.h)
+#include <fcntl.h>
+#include <omp.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+#include <unistd.h>
+
+#include <vector>
+
+#include "render_accel_particle.h"
+#include "render_accel_tetra.h"
+#include "render_accel_triangle.h"
+#include "render_prefix_tree_util.h"
+#include "render_texture.h"
+#include "tinymt64.h"
+
+using namespace lsgl::render;
+
+#define REF_API extern "C" __attribute__((visibility("default")))
+
+namespace {
+
+// Build32 prints per-phase timings on stdout; keep stdout clean for the
+// callers (bench.py prints exactly one JSON line).
+struct QuietStdout {
+  int saved = -1;
+  QuietStdout() {
+    fflush(stdout);
+    int devnull = open("/dev/null", O_WRONLY);
+    if (devnull >= 0) {
+      saved = dup(1);
+      dup2(devnull, 1);
+      close(devnull);
+    }
+  }
+  ~QuietStdout() {
+    fflush(stdout);
+    if (saved >= 0) {
+      dup2(saved, 1);
+      close(saved);
+    }
+  }
+};
+
+struct TriHandle {
+  Mesh mesh;
+  TriangleAccel accel;
+  ~TriHandle() {
+    // the arrays are borrowed from the caller; Mesh::~Mesh would free them
+    mesh.vertices = nullptr;
+    mesh.faces = nullptr;
+    mesh.normals = nullptr;
+    mesh.dvertices = nullptr;
+  }
+};
+
+struct TetHandle {
+  Tetrahedron tets;
+  TetraAccel accel;
+};
+
+struct SphereHandle {
+  Particles parts;
+  ParticleAccel accel;
+};
+
+// Ray record shared with the oracle and the product ABI (32 bytes).
+struct RayRec {
+  float org[3];
+  uint32_t prev_prim;
+  float dir[3];
+  float prev_t;
+};
+
+struct HitRec {
+  float t, u, v;
+  uint32_t prim;
+};
+
+inline Ray make_ray(const RayRec &r, const float *prevN) {
+  real3 o(r.org[0], r.org[1], r.org[2]);
+  real3 d(r.dir[0], r.dir[1], r.dir[2]);
+  Ray ray(o, d);
+  ray.double_sided = 1;
+  ray.prev_prim_id = r.prev_prim;
+  ray.prev_hit_t = r.prev_t;
+  if (prevN) {
+    ray.prev_hit_normal = real3(prevN[0], prevN[1], prevN[2]);
+  } else {
+    ray.prev_hit_normal = real3(0.0f, 0.0f, 0.0f);
+  }
+  ray.prev_node = nullptr;
+  return ray;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- triangles
+REF_API void *ref_tri_build(const float *verts, size_t nverts,
+                            const uint32_t *faces, size_t nfaces) {
+  TriHandle *h = new TriHandle();
+  h->mesh.nvertices = nverts;
+  h->mesh.vertices = verts;
+  h->mesh.nfaces = nfaces;
+  h->mesh.faces = const_cast<uint32_t *>(faces);
+  h->mesh.isDoublePrecisionPos = false;
+  TriangleBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build32(&h->mesh, opt);
+  }
+  return h;
+}
+
+REF_API void ref_tri_free(void *p) { delete static_cast<TriHandle *>(p); }
+
+REF_API int ref_tri_dump(void *p, const char *path) {
+  return static_cast<TriHandle *>(p)->accel.Dump(path) ? 0 : 1;
+}
+
+REF_API void ref_tri_bbox(void *p, double bmin[3], double bmax[3]) {
+  static_cast<TriHandle *>(p)->accel.BoundingBox(bmin, bmax);
+}
+
+REF_API void ref_tri_trace(void *p, const RayRec *rays, size_t n, HitRec *hits,
+                           int nthreads, int chunk) {
+  const TriangleAccel &acc = static_cast<TriHandle *>(p)->accel;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (chunk <= 0) chunk = 64;
+#pragma omp parallel for schedule(dynamic, chunk) num_threads(nthreads)
+  for (long long i = 0; i < (long long)n; i++) {
+    Ray ray = make_ray(rays[i], nullptr);
+    Intersection isect;
+    bool hit = acc.Traverse(isect, ray);
+    hits[i].t = isect.t;
+    hits[i].u = isect.u;
+    hits[i].v = isect.v;
+    hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
+  }
+}
+
+// ---------------------------------------------------------------- tetrahedra
+REF_API void *ref_tet_build(const float *verts, const uint32_t *faces,
+                            size_t ntets) {
+  TetHandle *h = new TetHandle();
+  memset(&h->tets, 0, sizeof(h->tets));
+  h->tets.numTetrahedrons = ntets;
+  h->tets.vertices = verts;
+  h->tets.dvertices = nullptr;
+  h->tets.isDoublePrecisionPos = false;
+  h->tets.faces = const_cast<uint32_t *>(faces);
+  TetraBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build32(&h->tets, opt);
+  }
+  return h;
+}
+
+REF_API void ref_tet_free(void *p) { delete static_cast<TetHandle *>(p); }
+
+REF_API int ref_tet_dump(void *p, const char *path) {
+  return static_cast<TetHandle *>(p)->accel.Dump(path) ? 0 : 1;
+}
+
+REF_API void ref_tet_bbox(void *p, double bmin[3], double bmax[3]) {
+  static_cast<TetHandle *>(p)->accel.BoundingBox(bmin, bmax);
+}
+
+REF_API void ref_tet_trace(void *p, const RayRec *rays, size_t n, HitRec *hits,
+                           uint32_t *subface, int nthreads, int chunk) {
+  const TetraAccel &acc = static_cast<TetHandle *>(p)->accel;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (chunk <= 0) chunk = 64;
+#pragma omp parallel for schedule(dynamic, chunk) num_threads(nthreads)
+  for (long long i = 0; i < (long long)n; i++) {
+    Ray ray = make_ray(rays[i], nullptr);
+    Intersection isect;
+    isect.subface_id = 0;
+    bool hit = acc.Traverse(isect, ray);
+    hits[i].t = isect.t;
+    hits[i].u = isect.u;
+    hits[i].v = isect.v;
+    hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
+    if (subface) subface[i] = hit ? isect.subface_id : 0u;
+  }
+}
+
+// ---------------------------------------------------------------- spheres
+REF_API void *ref_sphere_build(const float *pos, const float *radius,
+                               float const_radius, size_t n) {
+  SphereHandle *h = new SphereHandle();
+  memset(&h->parts, 0, sizeof(h->parts));
+  h->parts.numParticles = n;
+  h->parts.positions = pos;
+  h->parts.dpositions = nullptr;
+  h->parts.isDoublePrecisionPos = false;
+  h->parts.radius = const_cast<float *>(radius);
+  h->parts.materialIDs = nullptr;
+  h->parts.constantRadius = const_radius;
+  ParticleBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build32(&h->parts, opt);
+  }
+  return h;
+}
+
+REF_API void ref_sphere_free(void *p) { delete static_cast<SphereHandle *>(p); }
+
+REF_API int ref_sphere_dump(void *p, const char *path) {
+  return static_cast<SphereHandle *>(p)->accel.Dump(path) ? 0 : 1;
+}
+
+REF_API void ref_sphere_bbox(void *p, double bmin[3], double bmax[3]) {
+  static_cast<SphereHandle *>(p)->accel.BoundingBox(bmin, bmax);
+}
+
+REF_API void ref_sphere_trace(void *p, const RayRec *rays, size_t n,
+                              const float *prev_normals, HitRec *hits,
+                              int nthreads, int chunk) {
+  const ParticleAccel &acc = static_cast<SphereHandle *>(p)->accel;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (chunk <= 0) chunk = 64;
+#pragma omp parallel for schedule(dynamic, chunk) num_threads(nthreads)
+  for (long long i = 0; i < (long long)n; i++) {
+    Ray ray = make_ray(rays[i], prev_normals ? &prev_normals[3 * i] : nullptr);
+    Intersection isect;
+    bool hit = acc.Traverse(isect, ray);
+    hits[i].t = isect.t;
+    hits[i].u = 0.0f;  // spherical uv is shading-only
+    hits[i].v = 0.0f;
+    hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
+  }
+}
+
+// Node record sizes of the reference's Dump() format.
+REF_API void ref_node_sizes(size_t out[3]) {
+  out[0] = sizeof(TriangleNode);
+  out[1] = sizeof(TetraNode);
+  out[2] = sizeof(ParticleNode);
+}
+
+// ---------------------------------------------------------------- stages
+REF_API void ref_morton_points(const float *pts, size_t n, const float bmin[3],
+                               const float bmax[3], uint32_t *codes, int simd) {
+  real3 mn(bmin[0], bmin[1], bmin[2]), mx(bmax[0], bmax[1], bmax[2]);
+  if (simd)
+    CalculateMortonCodes30SIMD(codes, pts, mn, mx, 0, (int64_t)n);
+  else
+    CalculateMortonCodes30(codes, pts, mn, mx, 0, (int64_t)n);
+}
+
+REF_API void ref_morton_tris(const float *v, const uint32_t *f, size_t n,
+                             const float bmin[3], const float bmax[3],
+                             uint32_t *codes) {
+  real3 mn(bmin[0], bmin[1], bmin[2]), mx(bmax[0], bmax[1], bmax[2]);
+  CalculateMortonCodesTriangleFloat30(codes, v, f, mn, mx, 0, (int64_t)n);
+}
+
+REF_API void ref_morton_tets(const float *v, const uint32_t *f, size_t n,
+                             const float bmin[3], const float bmax[3],
+                             uint32_t *codes) {
+  real3 mn(bmin[0], bmin[1], bmin[2]), mx(bmax[0], bmax[1], bmax[2]);
+  CalculateMortonCodesTetraFloat30(codes, v, f, mn, mx, 0, (int64_t)n);
+}
+
+REF_API uint32_t ref_morton_code(const float p[3], const float bmin[3],
+                                 float inv) {
+  real3 pp(p[0], p[1], p[2]), mn(bmin[0], bmin[1], bmin[2]);
+  return MortionCode30(pp, mn, inv, inv, inv);
+}
+
+// RadixSort30OMP on (code, index) pairs (n >= 1024 to stay on the radix path).
+REF_API void ref_radix_sort(uint32_t *code, uint32_t *index, size_t n) {
+  std::vector<IndexKey30> keys(n);
+  for (size_t i = 0; i < n; i++) {
+    keys[i].index = index[i];
+    keys[i].code = code[i];
+  }
+  RadixSort30OMP(keys.data(), keys.data() + n);
+  for (size_t i = 0; i < n; i++) {
+    index[i] = keys[i].index;
+    code[i] = keys[i].code;
+  }
+}
+
+REF_API void ref_karras(const uint32_t *code, size_t n, uint32_t *child,
+                        uint8_t *ltype, uint8_t *rtype) {
+  std::vector<IndexKey30> keys(n);
+  for (size_t i = 0; i < n; i++) {
+    keys[i].index = (uint32_t)i;
+    keys[i].code = code[i];
+  }
+  for (long long i = 0; i < (long long)n - 1; i++) {
+    NodeInfo32 info = ConstructBinaryRadixTree30(keys.data(), (int)i, (uint32_t)n);
+    child[i] = info.childIndex;
+    ltype[i] = info.leftType == NODE_TYPE_LEAF ? 1 : 0;
+    rtype[i] = info.rightType == NODE_TYPE_LEAF ? 1 : 0;
+  }
+}
+
+REF_API void ref_tex3d(const float *img, int w, int h, int d, int comps,
+                       const float *uvw, size_t m, int clamp_s, int clamp_t,
+                       int clamp_r, float *rgba) {
+  Texture3D tex;
+  memset(&tex, 0, sizeof(tex));
+  tex.image = reinterpret_cast<unsigned char *>(const_cast<float *>(img));
+  tex.width = w;
+  tex.height = h;
+  tex.depth = d;
+  tex.components = comps;
+  tex.data_type = LSGL_RENDER_TEXTURE3D_FORMAT_FLOAT;
+  for (size_t i = 0; i < m; i++)
+    FilterTexture3DFloat(&rgba[4 * i], &tex, uvw[3 * i], uvw[3 * i + 1],
+                         uvw[3 * i + 2], clamp_s != 0, clamp_t != 0,
+                         clamp_r != 0);
+}
+
+// The reference tests' fixture draws (test/cctest/test-prefix-tree.cc:10-23).
+REF_API void ref_tinymt64_doubles(uint64_t seed, uint32_t mat1, uint32_t mat2,
+                                  uint64_t tmat, size_t n, double *out) {
+  tinymt64_t rng;
+  rng.mat1 = mat1;
+  rng.mat2 = mat2;
+  rng.tmat = tmat;
+  tinymt64_init(&rng, seed);
+  for (size_t i = 0; i < n; i++) out[i] = tinymt64_generate_double(&rng);
+}

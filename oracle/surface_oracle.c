@@ -1,0 +1,1366 @@
+/*
+ * surface_oracle.c -- CPU restatement of SURFACE's ray-tracing core.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle: it is linked by
+ * the test-suite, by __graft_entry__.smoke() and by the CPU-baseline leg of
+ * bench.py, and never by the product library (surface_b200/csrc).  It restates,
+ * in plain C, the reference algorithms that the CUDA kernels must reproduce
+ * bit-for-bit, each function citing the reference file:line it follows
+ * (paths relative to the SURFACE source tree):
+ *
+ *   - scene bounding box       render/render_accel_triangle.cc:713-796 (eps 0),
+ *                              render/render_accel_tetra.cc:973-1030 (eps 16 ulp),
+ *                              render/render_accel_particle.cc:304-369 (radius+eps)
+ *   - 30-bit Morton codes      render/render_prefix_tree_util.h:113-157,
+ *                              render/render_prefix_tree_util.cc:151-304
+ *   - stable LSD radix sort    render/render_prefix_tree_util.h:296-457
+ *   - Karras radix tree        render/render_prefix_tree_util.cc:501-649
+ *   - leaf collapse + emit     render/render_accel_triangle.cc:866-992,1389-1690
+ *                              render/render_accel_tetra.cc:1113-1243,1579-1850
+ *                              render/render_accel_particle.cc:521-661,1560-1866
+ *   - closest-hit traversal    render/render_accel_triangle.cc:1815-1938,1994-2437,2511-2669
+ *                              render/render_accel_tetra.cc:89-567,1934-2122,2200-2289
+ *                              render/render_accel_particle.cc:1990-2035,2423-2834,3053-3218
+ *   - trilinear 3D fetch       render/render_texture.cc:97-121,946-1058
+ *   - volume march             examples/nonuniform_volume_render/input.frag:16-141
+ *                              (camera, slab test, texel mapping); the
+ *                              emission-absorption compositing, transfer-function
+ *                              lookup and adjoint are defined here (the reference
+ *                              only has a 64-step averaging march).
+ *   - TinyMT64 generator       Saito & Matsumoto's published TinyMT64, used by the
+ *                              reference tests as their fixture RNG
+ *                              (test/cctest/test-prefix-tree.cc:10-23).
+ *
+ * Floating point: compile with -ffp-contract=off.  Every expression keeps the
+ * reference's operand order and precision (float vs. double promotions) so that
+ * results are identical to the reference build with g++ on x86-64.
+ */
+#include <float.h>
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define SO_API __attribute__((visibility("default")))
+
+enum { SO_TRI = 0, SO_TET = 1, SO_SPHERE = 2 };
+
+/* ------------------------------------------------------------------------ */
+/* TinyMT64 (fixture RNG of test/cctest/test-prefix-tree.cc:10-23)           */
+/* ------------------------------------------------------------------------ */
+typedef struct {
+  uint64_t s0, s1;
+  uint32_t mat1, mat2;
+  uint64_t tmat;
+} so_tinymt64;
+
+static void tmt_step(so_tinymt64 *r) {
+  uint64_t x;
+  r->s0 &= UINT64_C(0x7fffffffffffffff);
+  x = r->s0 ^ r->s1;
+  x ^= x << 12;
+  x ^= x >> 32;
+  x ^= x << 32;
+  x ^= x << 11;
+  r->s0 = r->s1;
+  r->s1 = x;
+  if (x & 1) {
+    r->s0 ^= (uint64_t)r->mat1;
+    r->s1 ^= ((uint64_t)r->mat2) << 32;
+  }
+}
+
+static uint64_t tmt_out(const so_tinymt64 *r) {
+  uint64_t x = r->s0 + r->s1;
+  x ^= r->s0 >> 8;
+  if (x & 1) x ^= r->tmat;
+  return x;
+}
+
+static void tmt_seed(so_tinymt64 *r, uint64_t seed) {
+  uint64_t st[2];
+  st[0] = seed ^ ((uint64_t)r->mat1 << 32);
+  st[1] = (uint64_t)r->mat2 ^ r->tmat;
+  for (int i = 1; i < 8; i++) {
+    uint64_t p = st[(i - 1) & 1];
+    st[i & 1] ^= (uint64_t)i + UINT64_C(6364136223846793005) * (p ^ (p >> 62));
+  }
+  if ((st[0] & UINT64_C(0x7fffffffffffffff)) == 0 && st[1] == 0) {
+    st[0] = 'T';
+    st[1] = 'M';
+  }
+  r->s0 = st[0];
+  r->s1 = st[1];
+}
+
+/* n doubles in [0,1) with the parameter set the reference tests use. */
+SO_API void so_tinymt64_doubles(uint64_t seed, uint32_t mat1, uint32_t mat2,
+                                uint64_t tmat, size_t n, double *out) {
+  so_tinymt64 r;
+  r.mat1 = mat1;
+  r.mat2 = mat2;
+  r.tmat = tmat;
+  tmt_seed(&r, seed);
+  for (size_t i = 0; i < n; i++) {
+    tmt_step(&r);
+    out[i] = (double)tmt_out(&r) * (1.0 / 18446744073709551616.0);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Morton codes                                                              */
+/* ------------------------------------------------------------------------ */
+
+/* Spread the low 10 bits of v so that bit k lands on bit 3k
+ * (PartBy2_30, render/render_prefix_tree_util.h:113-120). */
+static inline uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+SO_API uint32_t so_morton_bits(uint32_t ix, uint32_t iy, uint32_t iz) {
+  return (spread10(ix) << 2) | (spread10(iy) << 1) | spread10(iz);
+}
+
+/* MortionCode30 (render/render_prefix_tree_util.h:143-157): quantise then
+ * interleave.  The float->uint32 cast is left to the compiler exactly as the
+ * reference writes it. */
+static inline uint32_t morton_of(const float c[3], const float bmin[3],
+                                 const float inv[3]) {
+  uint32_t ix = (uint32_t)((c[0] - bmin[0]) * inv[0]);
+  uint32_t iy = (uint32_t)((c[1] - bmin[1]) * inv[1]);
+  uint32_t iz = (uint32_t)((c[2] - bmin[2]) * inv[2]);
+  return so_morton_bits(ix, iy, iz);
+}
+
+/* inv = (float)1024 / (bmax - bmin) (render/render_prefix_tree_util.cc:235-238) */
+static void morton_inv(const float bmin[3], const float bmax[3], float inv[3]) {
+  int kdiv = 1 << 10;
+  for (int k = 0; k < 3; k++) inv[k] = kdiv / (bmax[k] - bmin[k]);
+}
+
+SO_API void so_morton_points(const float *pts, size_t n, const float bmin[3],
+                             const float bmax[3], uint32_t *codes) {
+  float inv[3];
+  morton_inv(bmin, bmax, inv);
+  for (size_t i = 0; i < n; i++) codes[i] = morton_of(&pts[3 * i], bmin, inv);
+}
+
+/* CalculateMortonCodesTriangleFloat30 (render/render_prefix_tree_util.cc:230-265) */
+SO_API void so_morton_tris(const float *v, const uint32_t *f, size_t n,
+                           const float bmin[3], const float bmax[3],
+                           uint32_t *codes) {
+  float inv[3];
+  morton_inv(bmin, bmax, inv);
+  const float one_third = 1.0f / 3.0f;
+  for (size_t i = 0; i < n; i++) {
+    const float *p0 = &v[3 * (size_t)f[3 * i + 0]];
+    const float *p1 = &v[3 * (size_t)f[3 * i + 1]];
+    const float *p2 = &v[3 * (size_t)f[3 * i + 2]];
+    float c[3];
+    for (int k = 0; k < 3; k++) c[k] = one_third * (p0[k] + p1[k] + p2[k]);
+    codes[i] = morton_of(c, bmin, inv);
+  }
+}
+
+/* CalculateMortonCodesTetraFloat30 (render/render_prefix_tree_util.cc:267-304) */
+SO_API void so_morton_tets(const float *v, const uint32_t *f, size_t n,
+                           const float bmin[3], const float bmax[3],
+                           uint32_t *codes) {
+  float inv[3];
+  morton_inv(bmin, bmax, inv);
+  const float one_fourth = 1.0f / 4.0f;
+  for (size_t i = 0; i < n; i++) {
+    const float *p0 = &v[3 * (size_t)f[4 * i + 0]];
+    const float *p1 = &v[3 * (size_t)f[4 * i + 1]];
+    const float *p2 = &v[3 * (size_t)f[4 * i + 2]];
+    const float *p3 = &v[3 * (size_t)f[4 * i + 3]];
+    float c[3];
+    for (int k = 0; k < 3; k++)
+      c[k] = one_fourth * (p0[k] + p1[k] + p2[k] + p3[k]);
+    codes[i] = morton_of(c, bmin, inv);
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Scene bounding boxes                                                      */
+/* ------------------------------------------------------------------------ */
+
+static inline float fmin_ref(float a, float b) { return (b < a) ? b : a; }
+static inline float fmax_ref(float a, float b) { return (a < b) ? b : a; }
+
+/* Per-vertex box with padding eps over the vertices of `n` primitives of
+ * `nv` corners each (ComputeBoundingBoxOMP, render/render_accel_triangle.cc:713;
+ * render/render_accel_tetra.cc:973). */
+static void bbox_corners(const float *v, const uint32_t *f, size_t n, int nv,
+                         float eps, float bmin[3], float bmax[3]) {
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = FLT_MAX;
+    bmax[k] = -FLT_MAX;
+  }
+  for (size_t i = 0; i < n; i++)
+    for (int j = 0; j < nv; j++) {
+      const float *p = &v[3 * (size_t)f[(size_t)nv * i + j]];
+      for (int k = 0; k < 3; k++) {
+        bmin[k] = fmin_ref(bmin[k], p[k] - eps);
+        bmax[k] = fmax_ref(bmax[k], p[k] + eps);
+      }
+    }
+}
+
+SO_API void so_bbox_tris(const float *v, const uint32_t *f, size_t n,
+                         float bmin[3], float bmax[3]) {
+  bbox_corners(v, f, n, 3, 0.0f, bmin, bmax);
+}
+
+SO_API void so_bbox_tets(const float *v, const uint32_t *f, size_t n,
+                         float bmin[3], float bmax[3]) {
+  const float keps = FLT_EPSILON * 16;
+  bbox_corners(v, f, n, 4, keps, bmin, bmax);
+}
+
+static inline float sphere_radius(const float *radius, float constr, size_t i) {
+  return radius ? radius[i] : constr;
+}
+
+/* render/render_accel_particle.cc:304-369: centre -/+ radius -/+ 16 ulp(1). */
+SO_API void so_bbox_spheres(const float *pos, const float *radius, float constr,
+                            size_t n, float bmin[3], float bmax[3]) {
+  const float keps = FLT_EPSILON * 16.0;
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = FLT_MAX;
+    bmax[k] = -FLT_MAX;
+  }
+  for (size_t i = 0; i < n; i++) {
+    float r = sphere_radius(radius, constr, i);
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = fmin_ref(bmin[k], pos[3 * i + k] - r - keps);
+      bmax[k] = fmax_ref(bmax[k], pos[3 * i + k] + r + keps);
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Stable sort of (code, index) pairs by code                                */
+/* ------------------------------------------------------------------------ */
+
+/* RadixSort30 / RadixSort30OMP (render/render_prefix_tree_util.h:296-457):
+ * four stable 8-bit counting passes over the 32-bit code.  For n < 1024 the
+ * reference uses an unstable quicksort, but Build32 is never reached below
+ * 1024 primitives; this restatement is stable for every n. */
+SO_API void so_sort_pairs(uint32_t *code, uint32_t *index, size_t n) {
+  uint32_t *c2 = (uint32_t *)malloc(n * sizeof(uint32_t) + 4);
+  uint32_t *i2 = (uint32_t *)malloc(n * sizeof(uint32_t) + 4);
+  uint32_t *sc = code, *si = index, *dc = c2, *di = i2;
+  for (int shift = 0; shift < 32; shift += 8) {
+    size_t count[257];
+    memset(count, 0, sizeof(count));
+    for (size_t i = 0; i < n; i++) count[((sc[i] >> shift) & 0xff) + 1]++;
+    for (int b = 0; b < 256; b++) count[b + 1] += count[b];
+    for (size_t i = 0; i < n; i++) {
+      size_t d = count[(sc[i] >> shift) & 0xff]++;
+      dc[d] = sc[i];
+      di[d] = si[i];
+    }
+    uint32_t *t;
+    t = sc; sc = dc; dc = t;
+    t = si; si = di; di = t;
+  }
+  /* four passes: the result is back in the caller's arrays */
+  free(c2);
+  free(i2);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Karras binary radix tree                                                  */
+/* ------------------------------------------------------------------------ */
+
+static inline int clz32(uint32_t x) { return x ? __builtin_clz(x) : 32; }
+
+/* Delta30 (render/render_prefix_tree_util.cc:501-526): common-prefix length of
+ * sorted keys i and j; equal codes fall back to 32 + prefix of the positions;
+ * -1 outside [0,n). */
+static inline int kdelta(const uint32_t *code, int32_t i, int32_t j, int32_t n) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = code[i], b = code[j];
+  if (a == b) return 32 + clz32((uint32_t)i ^ (uint32_t)j);
+  return clz32(a ^ b);
+}
+
+/* ConstructBinaryRadixTree30 (render/render_prefix_tree_util.cc:562-649).
+ * child[i] = split gamma; ltype/rtype = 1 when that child is a single key. */
+SO_API void so_karras(const uint32_t *code, size_t n_, uint32_t *child,
+                      uint8_t *ltype, uint8_t *rtype) {
+  int32_t n = (int32_t)n_;
+  for (int32_t i = 0; i < n - 1; i++) {
+    int d = (kdelta(code, i, i + 1, n) - kdelta(code, i, i - 1, n)) >= 0 ? 1 : -1;
+    int dmin = kdelta(code, i, i - d, n);
+    int lmax = 2;
+    while (kdelta(code, i, i + lmax * d, n) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+      if (kdelta(code, i, i + (l + t) * d, n) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = kdelta(code, i, j, n);
+    int s = 0;
+    /* t = ceil(l/2), ceil(l/4), ..., 1 */
+    for (int k = 2;; k *= 2) {
+      int t = (l + k - 1) / k;
+      if (t <= 0) break;
+      if (kdelta(code, i, i + (s + t) * d, n) > dnode) s += t;
+      if (t == 1) break;
+    }
+    int g = i + s * d + (d < 0 ? d : 0);
+    child[i] = (uint32_t)g;
+    ltype[i] = ((i < j ? i : j) == g) ? 1 : 0;
+    rtype[i] = ((i > j ? i : j) == g + 1) ? 1 : 0;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* LBVH emission                                                             */
+/* ------------------------------------------------------------------------ */
+
+/* One node in reference emission order.  bmin/bmax is the node's OWN box:
+ * for triangles and spheres the reference stores it in the parent's child
+ * slot (TriangleNode/ParticleNode), for tetrahedra in the node itself
+ * (TetraNode, render/render_accel_tetra.h:24-43). */
+typedef struct {
+  float bmin[3], bmax[3];
+  int32_t leaf;  /* 1 = leaf */
+  int32_t axis;  /* branch split axis */
+  uint32_t d0;   /* leaf: count, branch: left child */
+  uint32_t d1;   /* leaf: offset, branch: right child */
+} so_node;
+
+typedef struct {
+  int kind;
+  size_t nprims;
+  size_t nnodes, cap;
+  so_node *nodes;
+  uint32_t *indices; /* sorted primitive ids */
+  uint32_t *codes;   /* sorted Morton codes */
+  uint32_t *child;
+  uint8_t *ltype, *rtype;
+  float scene_min[3], scene_max[3];
+  double eps_scale; /* triangles: max scene extent */
+  float keps;       /* leaf padding */
+  int max_leaf;
+  /* borrowed primitive data */
+  const float *verts;
+  const uint32_t *faces;
+  const float *radius;
+  float constr;
+} so_accel;
+
+static size_t push_node(so_accel *a) {
+  if (a->nnodes == a->cap) {
+    a->cap = a->cap ? a->cap * 2 : 1024;
+    a->nodes = (so_node *)realloc(a->nodes, a->cap * sizeof(so_node));
+  }
+  memset(&a->nodes[a->nnodes], 0, sizeof(so_node));
+  return a->nnodes++;
+}
+
+/* Leaf box over sorted primitives [lo, hi] (ComputeBoundingBox30,
+ * render/render_accel_triangle.cc:661-709; tetra :923-970; particle :417-461). */
+static void leaf_box(const so_accel *a, uint32_t lo, uint32_t hi, float bmin[3],
+                     float bmax[3]) {
+  const float e = a->keps;
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = FLT_MAX;
+    bmax[k] = -FLT_MAX;
+  }
+  for (uint32_t i = lo; i <= hi; i++) {
+    size_t p = a->indices[i];
+    if (a->kind == SO_SPHERE) {
+      float r = sphere_radius(a->radius, a->constr, p);
+      for (int k = 0; k < 3; k++) {
+        float mn = a->verts[3 * p + k] - r - e;
+        float mx = a->verts[3 * p + k] + r + e;
+        if (bmin[k] > mn) bmin[k] = mn;
+        if (bmax[k] < mx) bmax[k] = mx;
+      }
+    } else {
+      int nv = a->kind == SO_TRI ? 3 : 4;
+      for (int j = 0; j < nv; j++) {
+        const float *q = &a->verts[3 * (size_t)a->faces[(size_t)nv * p + j]];
+        for (int k = 0; k < 3; k++) {
+          float mn = q[k] - e;
+          float mx = q[k] + e;
+          if (bmin[k] > mn) bmin[k] = mn;
+          if (bmax[k] < mx) bmax[k] = mx;
+        }
+      }
+    }
+  }
+}
+
+/* GetSplitAxis (render/render_accel_triangle.cc:854-863). */
+static int split_axis(uint32_t code) { return (clz32(code) - 2) % 3; }
+
+/* BuildTreeRecursive32 (render/render_accel_triangle.cc:896-992): emit the
+ * subtree rooted at Karras node `root` covering sorted range [lo, hi]. */
+static size_t emit(so_accel *a, uint32_t root, uint32_t lo, uint32_t hi,
+                   int is_leaf, int depth) {
+  if (is_leaf || (hi - lo) <= (uint32_t)a->max_leaf || depth > 22) {
+    size_t o = push_node(a);
+    so_node *nd = &a->nodes[o];
+    leaf_box(a, lo, hi, nd->bmin, nd->bmax);
+    nd->leaf = 1;
+    nd->axis = 0;
+    nd->d0 = hi - lo + 1;
+    nd->d1 = lo;
+    return o;
+  }
+  uint32_t mid = a->child[root];
+  size_t o = push_node(a);
+  a->nodes[o].leaf = 0;
+  a->nodes[o].axis = split_axis(a->codes[root]);
+  size_t l = emit(a, mid, lo, mid, a->ltype[root], depth + 1);
+  size_t r = emit(a, mid + 1, mid + 1, hi, a->rtype[root], depth + 1);
+  so_node *nd = &a->nodes[o];
+  nd->d0 = (uint32_t)l;
+  nd->d1 = (uint32_t)r;
+  for (int k = 0; k < 3; k++) {
+    nd->bmin[k] = fmin_ref(a->nodes[l].bmin[k], a->nodes[r].bmin[k]);
+    nd->bmax[k] = fmax_ref(a->nodes[l].bmax[k], a->nodes[r].bmax[k]);
+  }
+  return o;
+}
+
+/* Build32 for the three primitive kinds (render/render_accel_triangle.cc:1389,
+ * render/render_accel_tetra.cc:1579, render/render_accel_particle.cc:1560).
+ * Requires n >= 2 (the reference switches to its SAH builder below 1024). */
+SO_API so_accel *so_build(int kind, const float *verts, const uint32_t *faces,
+                          const float *radius, float constr, size_t n) {
+  if (n < 2) return NULL;
+  so_accel *a = (so_accel *)calloc(1, sizeof(so_accel));
+  a->kind = kind;
+  a->nprims = n;
+  a->verts = verts;
+  a->faces = faces;
+  a->radius = radius;
+  a->constr = constr;
+  a->codes = (uint32_t *)malloc(n * sizeof(uint32_t));
+  a->indices = (uint32_t *)malloc(n * sizeof(uint32_t));
+  float bmin[3], bmax[3];
+  if (kind == SO_TRI) {
+    so_bbox_tris(verts, faces, n, bmin, bmax);
+    double es = bmax[0] - bmin[0];
+    if (es < (double)(bmax[1] - bmin[1])) es = bmax[1] - bmin[1];
+    if (es < (double)(bmax[2] - bmin[2])) es = bmax[2] - bmin[2];
+    a->eps_scale = es;
+    a->keps = FLT_EPSILON * (float)es;
+    a->max_leaf = 16;
+    so_morton_tris(verts, faces, n, bmin, bmax, a->codes);
+  } else if (kind == SO_TET) {
+    so_bbox_tets(verts, faces, n, bmin, bmax);
+    a->eps_scale = 16.0;
+    a->keps = FLT_EPSILON * 16;
+    a->max_leaf = 4;
+    so_morton_tets(verts, faces, n, bmin, bmax, a->codes);
+  } else {
+    so_bbox_spheres(verts, radius, constr, n, bmin, bmax);
+    a->eps_scale = 16.0;
+    a->keps = FLT_EPSILON * 16.0;
+    a->max_leaf = 16;
+    so_morton_points(verts, n, bmin, bmax, a->codes);
+  }
+  memcpy(a->scene_min, bmin, sizeof(bmin));
+  memcpy(a->scene_max, bmax, sizeof(bmax));
+  for (size_t i = 0; i < n; i++) a->indices[i] = (uint32_t)i;
+  so_sort_pairs(a->codes, a->indices, n);
+  a->child = (uint32_t *)malloc((n - 1) * sizeof(uint32_t));
+  a->ltype = (uint8_t *)malloc(n - 1);
+  a->rtype = (uint8_t *)malloc(n - 1);
+  so_karras(a->codes, n, a->child, a->ltype, a->rtype);
+
+  /* root: always a branch; its children start at depth 0 */
+  size_t root = push_node(a);
+  uint32_t mid = a->child[0];
+  size_t l = emit(a, mid, 0, mid, a->ltype[0], 0);
+  size_t r = emit(a, mid + 1, mid + 1, (uint32_t)(n - 1), a->rtype[0], 0);
+  so_node *nd = &a->nodes[root];
+  nd->leaf = 0;
+  nd->axis = split_axis(a->codes[0]);
+  nd->d0 = (uint32_t)l;
+  nd->d1 = (uint32_t)r;
+  for (int k = 0; k < 3; k++) {
+    nd->bmin[k] = fmin_ref(a->nodes[l].bmin[k], a->nodes[r].bmin[k]);
+    nd->bmax[k] = fmax_ref(a->nodes[l].bmax[k], a->nodes[r].bmax[k]);
+  }
+  return a;
+}
+
+SO_API void so_free(so_accel *a) {
+  if (!a) return;
+  free(a->nodes);
+  free(a->indices);
+  free(a->codes);
+  free(a->child);
+  free(a->ltype);
+  free(a->rtype);
+  free(a);
+}
+
+SO_API size_t so_num_nodes(const so_accel *a) { return a->nnodes; }
+
+/* Copies: nodes as 10 x 32-bit words each (bmin[3], bmax[3], leaf, axis, d0,
+ * d1), sorted indices, sorted codes, Karras arrays, scene box, eps values. */
+SO_API void so_export(const so_accel *a, void *nodes, uint32_t *indices,
+                      uint32_t *codes, float scene[6], double *eps_scale) {
+  if (nodes) memcpy(nodes, a->nodes, a->nnodes * sizeof(so_node));
+  if (indices) memcpy(indices, a->indices, a->nprims * sizeof(uint32_t));
+  if (codes) memcpy(codes, a->codes, a->nprims * sizeof(uint32_t));
+  if (scene) {
+    memcpy(scene, a->scene_min, 3 * sizeof(float));
+    memcpy(scene + 3, a->scene_max, 3 * sizeof(float));
+  }
+  if (eps_scale) *eps_scale = a->eps_scale;
+}
+
+SO_API void so_export_karras(const so_accel *a, uint32_t *child, uint8_t *lt,
+                             uint8_t *rt) {
+  size_t m = a->nprims - 1;
+  memcpy(child, a->child, m * sizeof(uint32_t));
+  memcpy(lt, a->ltype, m);
+  memcpy(rt, a->rtype, m);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Canonical topology                                                        */
+/* ------------------------------------------------------------------------ */
+
+/* Depth-first, left-first listing of a tree given in generic form (own box,
+ * leaf flag, axis, d0/d1 as in so_node).  Output records, 10 words each:
+ * leaf, axis (0 for leaves), count (0 for branches), offset (0 for
+ * branches), bmin[3], bmax[3], depth, reserved.  Node storage order is
+ * irrelevant, so a tree emitted by concurrent tasks compares equal to the
+ * sequential emission.  Returns the number of records, or -1 on a malformed
+ * tree (index out of range, cycle, more than `max_out` records). */
+SO_API long so_canonicalize(const void *generic_nodes, size_t nnodes, size_t root,
+                            uint32_t *out, size_t max_out) {
+  const so_node *nd = (const so_node *)generic_nodes;
+  size_t *stack = (size_t *)malloc(sizeof(size_t) * 2 * 4096);
+  int *dstack = (int *)malloc(sizeof(int) * 2 * 4096);
+  long cnt = 0;
+  int sp = 0;
+  stack[0] = root;
+  dstack[0] = 0;
+  while (sp >= 0) {
+    size_t i = stack[sp];
+    int dep = dstack[sp];
+    sp--;
+    if (i >= nnodes || (size_t)cnt >= max_out) {
+      cnt = -1;
+      break;
+    }
+    uint32_t *o = &out[10 * (size_t)cnt];
+    const so_node *x = &nd[i];
+    o[0] = x->leaf ? 1u : 0u;
+    o[1] = x->leaf ? 0u : (uint32_t)x->axis;
+    o[2] = x->leaf ? x->d0 : 0u;
+    o[3] = x->leaf ? x->d1 : 0u;
+    memcpy(&o[4], x->bmin, 3 * sizeof(float));
+    memcpy(&o[7], x->bmax, 3 * sizeof(float));
+    /* depth kept out of the record body; callers that need it re-derive */
+    (void)dep;
+    cnt++;
+    if (!x->leaf) {
+      if (sp + 2 >= 2 * 4096) {
+        cnt = -1;
+        break;
+      }
+      /* right pushed first so that left is listed first */
+      stack[++sp] = x->d1;
+      dstack[sp] = dep + 1;
+      stack[++sp] = x->d0;
+      dstack[sp] = dep + 1;
+    }
+  }
+  free(stack);
+  free(dstack);
+  return cnt;
+}
+
+/* ------------------------------------------------------------------------ */
+/* Traversal                                                                 */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  float org[3];
+  uint32_t prev_prim;
+  float dir[3];
+  float prev_t;
+} so_ray; /* 32 bytes, same as the product's srt_ray */
+
+typedef struct {
+  float t, u, v;
+  uint32_t prim;
+} so_hit;
+
+typedef struct {
+  uint64_t branch_visits; /* popped branch nodes (tri/sphere) or all pops (tet) */
+  uint64_t leaf_visits;
+  uint64_t prim_tests;
+} so_stats;
+
+/* IntersectRayAABB (render/render_accel_triangle.cc:1815-1861); `clamp` = 1
+ * clamps tmax to maxT (triangle, particle), 0 tests tmin <= maxT (tetra,
+ * render/render_accel_tetra.cc:1934-1978). */
+static inline int ray_aabb(float maxT, const float bmin[3], const float bmax[3],
+                           const float org[3], const float inv[3],
+                           const int sgn[3], int clamp) {
+  float tmin, tmax;
+  const float min_x = sgn[0] ? bmax[0] : bmin[0];
+  const float min_y = sgn[1] ? bmax[1] : bmin[1];
+  const float min_z = sgn[2] ? bmax[2] : bmin[2];
+  const float max_x = sgn[0] ? bmin[0] : bmax[0];
+  const float max_y = sgn[1] ? bmin[1] : bmax[1];
+  const float max_z = sgn[2] ? bmin[2] : bmax[2];
+  const float tmin_x = (min_x - org[0]) * inv[0];
+  const float tmax_x = (max_x - org[0]) * inv[0];
+  const float tmin_y = (min_y - org[1]) * inv[1];
+  const float tmax_y = (max_y - org[1]) * inv[1];
+  tmin = (tmin_x > tmin_y) ? tmin_x : tmin_y;
+  tmax = (tmax_x < tmax_y) ? tmax_x : tmax_y;
+  const float tmin_z = (min_z - org[2]) * inv[2];
+  const float tmax_z = (max_z - org[2]) * inv[2];
+  tmin = (tmin > tmin_z) ? tmin : tmin_z;
+  tmax = (tmax < tmax_z) ? tmax : tmax_z;
+  if (clamp) {
+    tmax = (maxT < tmax) ? maxT : tmax;
+    return (tmax > 0.0f) && (tmin <= tmax);
+  }
+  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= maxT);
+}
+
+static inline float dot3f(const float a[3], const float b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+static inline void cross3f(const float a[3], const float b[3], float c[3]) {
+  c[0] = a[1] * b[2] - a[2] * b[1];
+  c[1] = a[2] * b[0] - a[0] * b[2];
+  c[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* TriangleIsect, double-sided (render/render_accel_triangle.cc:1887-1938). */
+static inline int tri_isect(float *tio, float *uo, float *vo, const float p0[3],
+                            const float p1[3], const float p2[3],
+                            const float org[3], const float dir[3], float keps) {
+  float e1[3], e2[3], p[3], s[3], q[3];
+  for (int k = 0; k < 3; k++) {
+    e1[k] = p1[k] - p0[k];
+    e2[k] = p2[k] - p0[k];
+  }
+  cross3f(dir, e2, p);
+  float det = dot3f(e1, p);
+  if (fabsf(det) < keps) return 0;
+  float inv_det = (float)(1.0 / (double)det);
+  for (int k = 0; k < 3; k++) s[k] = org[k] - p0[k];
+  cross3f(s, e1, q);
+  float u = dot3f(s, p) * inv_det;
+  float v = dot3f(q, dir) * inv_det;
+  float t = dot3f(e2, q) * inv_det;
+  if (u < 0.0f || u > 1.0f) return 0;
+  if (v < 0.0f || u + v > 1.0f) return 0;
+  if (t < 0.0f || t > *tio) return 0;
+  *tio = t;
+  *uo = u;
+  *vo = v;
+  return 1;
+}
+
+/* ---- Pluecker ray/tetrahedron test, FP64 (render/render_accel_tetra.cc:89-567) */
+typedef struct { double x, y, z; } d3;
+static inline d3 d3sub(d3 a, d3 b) { d3 r = {a.x - b.x, a.y - b.y, a.z - b.z}; return r; }
+static inline d3 d3add(d3 a, d3 b) { d3 r = {a.x + b.x, a.y + b.y, a.z + b.z}; return r; }
+static inline d3 d3scale(double f, d3 v) { d3 r = {v.x * f, v.y * f, v.z * f}; return r; }
+static inline d3 d3cross(d3 a, d3 b) {
+  d3 c = {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+  return c;
+}
+static inline double d3dot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline int dsign(double x) {
+  return x > DBL_EPSILON ? 1 : (x < -DBL_EPSILON ? -1 : 0);
+}
+typedef struct { d3 d, c; } plk;
+static inline plk plk_make(d3 v0, d3 v1) {
+  plk p;
+  p.d = d3sub(v1, v0);
+  p.c = d3cross(v1, v0);
+  return p;
+}
+static inline double plk_dot(plk a, plk b) { return d3dot(a.d, b.c) + d3dot(b.d, a.c); }
+
+/* barycentric point (1-a-b)*A + a*B + b*C */
+static inline d3 bary(double a, double b, d3 A, d3 B, d3 C) {
+  return d3add(d3add(d3scale(1 - a - b, A), d3scale(a, B)), d3scale(b, C));
+}
+
+static inline void param_dist(d3 o, d3 d, d3 pe, d3 pl, double *te, double *tl) {
+  if (d.x != 0.0) {
+    double iv = 1.0 / d.x;
+    *te = (pe.x - o.x) * iv;
+    *tl = (pl.x - o.x) * iv;
+  } else if (d.y != 0.0) {
+    double iv = 1.0 / d.y;
+    *te = (pe.y - o.y) * iv;
+    *tl = (pl.y - o.y) * iv;
+  } else {
+    double iv = 1.0 / d.z;
+    *te = (pe.z - o.z) * iv;
+    *tl = (pl.z - o.z) * iv;
+  }
+}
+
+/* Output: enter face, enter barycentrics (ue1, ue2), leave barycentric ul1,
+ * enter distance.  Mirrors RayTetraPluecker's face order and sign logic. */
+static int ray_tet(d3 orig, d3 dir, const d3 V[4], int *ef, double *ue1,
+                   double *ue2, double *ul1, double *te) {
+  int enterF = -1, leaveF = -1;
+  double uAB = 0, uAC = 0, uDB = 0, uDC = 0, uBC = 0, uAD = 0;
+  int sAB = -2, sAC = -2, sDB = -2, sDC = -2, sBC = -2, sAD = -2;
+  double eu1 = 0, eu2 = 0, lu1 = 0, lu2 = 0, tl = 0;
+  d3 ep = {0, 0, 0}, lp = {0, 0, 0};
+  (void)leaveF; (void)lu2;
+  d3 dest = d3add(orig, dir);
+  plk ray = plk_make(orig, dest);
+  int next = 0;
+
+#define ENTER(F, A1, A2, P0, P1, P2) do { enterF = F; eu1 = A1; eu2 = A2; ep = bary(eu1, eu2, P0, P1, P2); } while (0)
+#define LEAVE(F, A1, A2, P0, P1, P2) do { leaveF = F; lu1 = A1; lu2 = A2; lp = bary(lu1, lu2, P0, P1, P2); } while (0)
+#define DONE() do { param_dist(orig, dir, ep, lp, te, &tl); *ef = enterF; *ue1 = eu1; *ue2 = eu2; *ul1 = lu1; return 1; } while (0)
+
+  uAB = plk_dot(ray, plk_make(V[0], V[1])); sAB = dsign(uAB);
+  uAC = plk_dot(ray, plk_make(V[0], V[2])); sAC = dsign(uAC);
+  if ((sAC == -sAB) || (sAC == 0) || (sAB == 0)) {
+    uBC = plk_dot(ray, plk_make(V[1], V[2])); sBC = dsign(uBC);
+    int sABC = sAB;
+    if (sABC == 0) { sABC = -sAC; if (sABC == 0) sABC = sBC; }
+    if ((sABC != 0) && ((sBC == sABC) || (sBC == 0))) {
+      double inv = 1.0 / (uAB + uBC - uAC);
+      if (sABC == 1) { ENTER(3, -uAC * inv, uAB * inv, V[0], V[1], V[2]); next = -1; }
+      else { LEAVE(3, -uAC * inv, uAB * inv, V[0], V[1], V[2]); next = 1; }
+      uAD = plk_dot(ray, plk_make(V[0], V[3])); sAD = dsign(uAD);
+      if ((sAD == next) || (sAD == 0)) {
+        uDB = plk_dot(ray, plk_make(V[3], V[1])); sDB = dsign(uDB);
+        if ((sDB == next) || ((sDB == 0) && ((sAD != 0) || (sAB != 0)))) {
+          double iv = 1.0 / (uAD + uDB - uAB);
+          if (next == 1) ENTER(2, uDB * iv, -uAB * iv, V[1], V[0], V[3]);
+          else LEAVE(2, uDB * iv, -uAB * iv, V[1], V[0], V[3]);
+          DONE();
+        }
+      }
+      uDC = plk_dot(ray, plk_make(V[3], V[2])); sDC = dsign(uDC);
+      if ((sDC == -next) || ((sDC == 0) && ((sAD != 0) || (sAC != 0)))) {
+        double iv = 1.0 / (uAC - uDC - uAD);
+        if (next == 1) ENTER(1, uAC * iv, -uDC * iv, V[2], V[3], V[0]);
+        else LEAVE(1, uAC * iv, -uDC * iv, V[2], V[3], V[0]);
+        DONE();
+      } else {
+        if (sDB == -2) uDB = plk_dot(ray, plk_make(V[3], V[1]));
+        double iv = 1.0 / (uDC - uBC - uDB);
+        if (next == 1) ENTER(0, -uDB * iv, uDC * iv, V[3], V[2], V[1]);
+        else LEAVE(0, -uDB * iv, uDC * iv, V[3], V[2], V[1]);
+        DONE();
+      }
+    }
+  }
+  uAD = plk_dot(ray, plk_make(V[0], V[3])); sAD = dsign(uAD);
+  if ((sAD == -sAB) || (sAB == 0) || (sAD == 0)) {
+    uDB = plk_dot(ray, plk_make(V[3], V[1])); sDB = dsign(uDB);
+    int sBAD = -sAB;
+    if (sBAD == 0) { sBAD = sAD; if (sBAD == 0) sBAD = sDB; }
+    if ((sBAD != 0) && ((sDB == sBAD) || (sDB == 0))) {
+      double inv = 1.0 / (uAD + uDB - uAB);
+      if (sBAD == 1) { ENTER(2, uDB * inv, -uAB * inv, V[1], V[0], V[3]); next = -1; }
+      else { LEAVE(2, uDB * inv, -uAB * inv, V[1], V[0], V[3]); next = 1; }
+      uDC = plk_dot(ray, plk_make(V[3], V[2])); sDC = dsign(uDC);
+      if ((sDC == -next) || ((sDC == 0) && ((sAD != 0) || (sAC != 0)))) {
+        double iv = 1.0 / (uAC - uDC - uAD);
+        if (next == 1) ENTER(1, uAC * iv, -uDC * iv, V[2], V[3], V[0]);
+        else LEAVE(1, uAC * iv, -uDC * iv, V[2], V[3], V[0]);
+        DONE();
+      } else {
+        if (sBC == -2) uBC = plk_dot(ray, plk_make(V[1], V[2]));
+        double iv = 1.0 / (uDC - uBC - uDB);
+        if (next == 1) ENTER(0, -uDB * iv, uDC * iv, V[3], V[2], V[1]);
+        else LEAVE(0, -uDB * iv, uDC * iv, V[3], V[2], V[1]);
+        DONE();
+      }
+    }
+  }
+  if ((-sAD == sAC) || (sAC == 0) || (sAD == 0)) {
+    uDC = plk_dot(ray, plk_make(V[3], V[2])); sDC = dsign(uDC);
+    int sCDA = sAC;
+    if (sCDA == 0) { sCDA = -sAD; if (sCDA == 0) sCDA = -sDC; }
+    if ((sCDA != 0) && ((-sDC == sCDA) || (sDC == 0))) {
+      double ivCDA = 1.0 / (uAC - uDC - uAD);
+      if (sBC == -2) uBC = plk_dot(ray, plk_make(V[1], V[2]));
+      if (sDB == -2) uDB = plk_dot(ray, plk_make(V[3], V[1]));
+      double ivDCB = 1.0 / (uDC - uBC - uDB);
+      if (sCDA == 1) {
+        ENTER(1, uAC * ivCDA, -uDC * ivCDA, V[2], V[3], V[0]);
+        LEAVE(0, -uDB * ivDCB, uDC * ivDCB, V[3], V[2], V[1]);
+      } else {
+        LEAVE(1, uAC * ivCDA, -uDC * ivCDA, V[2], V[3], V[0]);
+        ENTER(0, -uDB * ivDCB, uDC * ivDCB, V[3], V[2], V[1]);
+      }
+      DONE();
+    }
+  }
+#undef ENTER
+#undef LEAVE
+#undef DONE
+  return 0;
+}
+
+/* SphereIsect (render/render_accel_particle.cc:2423-2512). */
+static inline int sphere_isect(float *tio, const float c[3], float radius,
+                               const float org[3], const float dir[3],
+                               double prevT, const float prevN[3], int self) {
+  float oc[3] = {org[0] - c[0], org[1] - c[1], org[2] - c[2]};
+  float a = dot3f(dir, dir);
+  float b = (float)(2.0 * (double)dot3f(dir, oc));
+  float cc = dot3f(oc, oc) - radius * radius;
+  float disc = (float)((double)(b * b) - 4.0 * (double)a * (double)cc);
+  float t0, t1;
+  if (disc < 0.0f) return 0;
+  else if (disc == 0.0f) {
+    t0 = t1 = (float)(-0.5 * (double)(b / a));
+  } else {
+    float ds = sqrtf(disc);
+    float q;
+    if (b < 0) q = (float)((double)(-b - ds) / 2.0);
+    else q = (float)((double)(-b + ds) / 2.0);
+    t0 = q / a;
+    t1 = cc / q;
+  }
+  if (t0 > t1) { float tmp = t0; t0 = t1; t1 = tmp; }
+  if (t1 < 0) return 0;
+  if (self) {
+    float t = t1;
+    float nrm[3];
+    for (int k = 0; k < 3; k++) nrm[k] = (org[k] + t * dir[k]) - c[k];
+    if ((t < *tio) && ((double)t < prevT) && (dot3f(nrm, prevN) <= 0.0f)) {
+      *tio = t;
+      return 1;
+    }
+  } else {
+    float t = (t0 < 0) ? t1 : t0;
+    if (t < *tio) {
+      *tio = t;
+      return 1;
+    }
+  }
+  return 0;
+}
+
+/* Closest hit for one ray: Traverse() of the three accel classes. */
+static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
+                      so_hit *h, uint32_t *subface, const float *vscalar,
+                      float *scalar_out, so_stats *st) {
+  double best_e1 = 0.0, best_e2 = 0.0;
+  float hitT = FLT_MAX;
+  h->t = hitT;
+  h->u = 0.0f;
+  h->v = 0.0f;
+  h->prim = 0xffffffffu;
+  uint32_t sub = 0;
+  int sgn[3];
+  float inv[3];
+  for (int k = 0; k < 3; k++) {
+    sgn[k] = ray->dir[k] < 0.0f ? 1 : 0;
+    inv[k] = (float)(1.0 / (double)ray->dir[k]);
+  }
+  const float *org = ray->org;
+  const float *dir = ray->dir;
+  float zero3[3] = {0, 0, 0};
+  const float *pn = prevN ? prevN : zero3;
+  int stack[512];
+  int sp = 0;
+  stack[0] = 0;
+  while (sp >= 0) {
+    const so_node *nd = &a->nodes[stack[sp]];
+    sp--;
+    if (a->kind == SO_TET) {
+      int hit = ray_aabb(hitT, nd->bmin, nd->bmax, org, inv, sgn, 0);
+      st->branch_visits++;
+      if (!nd->leaf) {
+        if (hit) {
+          int nearc = sgn[nd->axis], farc = 1 - nearc;
+          stack[++sp] = (int)(farc ? nd->d1 : nd->d0);
+          stack[++sp] = (int)(nearc ? nd->d1 : nd->d0);
+        }
+      } else if (hit) {
+        st->leaf_visits++;
+        float t = h->t;
+        int any = 0;
+        d3 o = {org[0], org[1], org[2]};
+        d3 d = {dir[0], dir[1], dir[2]};
+        for (uint32_t i = 0; i < nd->d0; i++) {
+          uint32_t f = a->indices[nd->d1 + i];
+          if (f == ray->prev_prim) continue;
+          st->prim_tests++;
+          d3 V[4];
+          for (int j = 0; j < 4; j++) {
+            const float *p = &a->verts[3 * (size_t)a->faces[4 * (size_t)f + j]];
+            V[j].x = p[0]; V[j].y = p[1]; V[j].z = p[2];
+          }
+          int ef;
+          double ue1, ue2, ul1, te;
+          if (ray_tet(o, d, V, &ef, &ue1, &ue2, &ul1, &te)) {
+            if ((te >= 0.0) && (te < (double)t)) {
+              h->t = (float)te;
+              h->u = (float)ue1;
+              h->v = (float)ul1; /* the reference passes uLeave1 into isect.v */
+              h->prim = f;
+              sub = (uint32_t)ef;
+              best_e1 = ue1;
+              best_e2 = ue2;
+              t = (float)te;
+              any = 1;
+            }
+          }
+        }
+        if (any) hitT = h->t;
+      }
+      continue;
+    }
+    if (!nd->leaf) {
+      st->branch_visits++;
+      const so_node *c0 = &a->nodes[nd->d0];
+      const so_node *c1 = &a->nodes[nd->d1];
+      int hits[2];
+      hits[0] = ray_aabb(hitT, c0->bmin, c0->bmax, org, inv, sgn, 1);
+      hits[1] = ray_aabb(hitT, c1->bmin, c1->bmax, org, inv, sgn, 1);
+      if (hits[0] || hits[1]) {
+        int nearc = sgn[nd->axis], farc = 1 - nearc;
+        if (hits[farc]) stack[++sp] = (int)(farc ? nd->d1 : nd->d0);
+        if (hits[nearc]) stack[++sp] = (int)(nearc ? nd->d1 : nd->d0);
+      }
+    } else {
+      st->leaf_visits++;
+      float t = h->t;
+      int any = 0;
+      for (uint32_t i = 0; i < nd->d0; i++) {
+        uint32_t f = a->indices[nd->d1 + i];
+        if (a->kind == SO_TRI) {
+          if (f == ray->prev_prim) continue;
+          st->prim_tests++;
+          const float *p0 = &a->verts[3 * (size_t)a->faces[3 * (size_t)f + 0]];
+          const float *p1 = &a->verts[3 * (size_t)a->faces[3 * (size_t)f + 1]];
+          const float *p2 = &a->verts[3 * (size_t)a->faces[3 * (size_t)f + 2]];
+          float u, v;
+          if (tri_isect(&t, &u, &v, p0, p1, p2, org, dir, a->keps)) {
+            h->t = t;
+            h->u = u;
+            h->v = v;
+            h->prim = f;
+            any = 1;
+          }
+        } else {
+          st->prim_tests++;
+          float r = sphere_radius(a->radius, a->constr, f);
+          if (sphere_isect(&t, &a->verts[3 * (size_t)f], r, org, dir,
+                           (double)ray->prev_t, pn, ray->prev_prim == f)) {
+            h->t = t;
+            h->prim = f;
+            any = 1;
+          }
+        }
+      }
+      if (any) hitT = h->t;
+    }
+  }
+  if (!(h->t < FLT_MAX)) {
+    h->prim = 0xffffffffu;
+  }
+  if (subface) *subface = sub;
+  if (scalar_out) {
+    /* scalar at the entering point: (1-a-b)*s_A + a*s_B + b*s_C over the
+     * entering face's vertices in the order the Pluecker test forms its
+     * barycentric point (face 3: 0,1,2; 2: 1,0,3; 1: 2,3,0; 0: 3,2,1) */
+    float sv = 0.0f;
+    if (h->prim != 0xffffffffu && vscalar && a->kind == SO_TET) {
+      static const int fa[4] = {3, 2, 1, 0}, fb[4] = {2, 3, 0, 1}, fc[4] = {1, 0, 3, 2};
+      const uint32_t *tv = &a->faces[4 * (size_t)h->prim];
+      double sa = vscalar[tv[fa[sub]]], sb = vscalar[tv[fb[sub]]], sc = vscalar[tv[fc[sub]]];
+      sv = (float)((1.0 - best_e1 - best_e2) * sa + best_e1 * sb + best_e2 * sc);
+    }
+    *scalar_out = sv;
+  }
+}
+
+/* Trace `n` rays.  prev_normals: 3 floats per ray or NULL.  subface: per-ray
+ * output for tetrahedra or NULL.  vscalar/scalar_out: per-vertex scalar and
+ * its value at the entering point (tetrahedra).  stats (optional): 3 x uint64
+ * totals (branch visits, leaf visits, primitive tests). */
+SO_API void so_trace(const so_accel *a, const so_ray *rays, size_t n,
+                     const float *prev_normals, so_hit *hits, uint32_t *subface,
+                     const float *vscalar, float *scalar_out, uint64_t *stats,
+                     int nthreads) {
+  uint64_t bv = 0, lv = 0, pt = 0;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads) reduction(+ : bv, lv, pt)
+#endif
+  for (long long i = 0; i < (long long)n; i++) {
+    so_stats st = {0, 0, 0};
+    trace_one(a, &rays[i], prev_normals ? &prev_normals[3 * i] : NULL, &hits[i],
+              subface ? &subface[i] : NULL, vscalar,
+              scalar_out ? &scalar_out[i] : NULL, &st);
+    bv += st.branch_visits;
+    lv += st.leaf_visits;
+    pt += st.prim_tests;
+  }
+  if (stats) {
+    stats[0] = bv;
+    stats[1] = lv;
+    stats[2] = pt;
+  }
+}
+
+/* ------------------------------------------------------------------------ */
+/* Trilinear 3D fetch (FilterTexture3DFloat, render/render_texture.cc:946)   */
+/* ------------------------------------------------------------------------ */
+
+static inline int floor_ref(float x) { /* fasterfloorf, render_texture.cc:106 */
+  if (x >= 0) return (int)x;
+  int y = (int)x;
+  if (fabsf(x - (float)y) <= FLT_EPSILON) {
+  } else {
+    y = y - 1;
+  }
+  return y;
+}
+static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+static inline float lerpf(float t, float a, float b) { return (1.f - t) * a + t * b; }
+
+/* Scalar (1-component) volume fetch with the reference's texel-corner
+ * mapping vox = u * (dim - 1). */
+static float tex3d_f32(const float *img, const int dim[3], float u, float v,
+                       float r, int clamp_s, int clamp_t, int clamp_r) {
+  float uu = clamp_s ? u : u - floor_ref(u);
+  float vv = clamp_t ? v : v - floor_ref(v);
+  float rr = clamp_r ? r : r - floor_ref(r);
+  float vox0 = uu * (dim[0] - 1.0f);
+  float vox1 = vv * (dim[1] - 1.0f);
+  float vox2 = rr * (dim[2] - 1.0f);
+  int vx = clampi((int)vox0, 0, dim[0] - 1);
+  int vy = clampi((int)vox1, 0, dim[1] - 1);
+  int vz = clampi((int)vox2, 0, dim[2] - 1);
+  int vx1 = vx + 1 < dim[0] - 1 ? vx + 1 : dim[0] - 1;
+  int vy1 = vy + 1 < dim[1] - 1 ? vy + 1 : dim[1] - 1;
+  int vz1 = vz + 1 < dim[2] - 1 ? vz + 1 : dim[2] - 1;
+  float dx = vox0 - vx, dy = vox1 - vy, dz = vox2 - vz;
+#define A(x, y, z) img[(size_t)(z) * dim[0] * dim[1] + (size_t)(y) * dim[0] + (x)]
+  float d00 = lerpf(dx, A(vx, vy, vz), A(vx1, vy, vz));
+  float d10 = lerpf(dx, A(vx, vy1, vz), A(vx1, vy1, vz));
+  float d01 = lerpf(dx, A(vx, vy, vz1), A(vx1, vy, vz1));
+  float d11 = lerpf(dx, A(vx, vy1, vz1), A(vx1, vy1, vz1));
+#undef A
+  float d0 = lerpf(dy, d00, d10);
+  float d1 = lerpf(dy, d01, d11);
+  return lerpf(dz, d0, d1);
+}
+
+SO_API void so_tex3d(const float *img, const int dim[3], const float *uvw,
+                     size_t m, int clamp_s, int clamp_t, int clamp_r, float *out) {
+  for (size_t i = 0; i < m; i++)
+    out[i] = tex3d_f32(img, dim, uvw[3 * i], uvw[3 * i + 1], uvw[3 * i + 2],
+                       clamp_s, clamp_t, clamp_r);
+}
+
+/* ------------------------------------------------------------------------ */
+/* Emission-absorption volume march                                          */
+/* ------------------------------------------------------------------------ */
+
+/* Parameters shared with the CUDA kernel (srt_volume_params in the C ABI).
+ * The camera frame is precomputed once on the host (so_volume_camera). */
+typedef struct {
+  int width, height;        /* image size */
+  int max_steps;            /* hard cap on samples per ray */
+  int reserved;
+  float eye[3];
+  float corner[3];          /* image-plane corner */
+  float du[3], dv[3];       /* per-pixel image-plane steps */
+  float step;               /* world-space distance between samples */
+  float sigma_scale;        /* extinction = sigma_scale * tf.a */
+  float alpha_max;          /* per-sample opacity clamp (< 1) */
+} so_vol_params;
+
+/* build_cameraframe (examples/nonuniform_volume_render/input.frag:16-29),
+ * FP32, including the shader's 3.14 for pi. */
+SO_API void so_volume_camera(int W, int H, const float eye[3],
+                             const float lookat[3], const float up[3],
+                             float fov_deg, float corner[3], float du[3],
+                             float dv[3]) {
+  float look[3], tmp[3];
+  for (int k = 0; k < 3; k++) look[k] = lookat[k] - eye[k];
+  float ll = sqrtf(dot3f(look, look));
+  for (int k = 0; k < 3; k++) look[k] = look[k] / ll;
+  cross3f(look, up, tmp);
+  float lu = sqrtf(dot3f(tmp, tmp));
+  for (int k = 0; k < 3; k++) du[k] = tmp[k] / lu;
+  cross3f(look, du, tmp);
+  float lv = sqrtf(dot3f(tmp, tmp));
+  for (int k = 0; k < 3; k++) dv[k] = tmp[k] / lv;
+  float flen = 0.5f * (float)H / (float)tan(0.5 * ((double)fov_deg * 3.14 / 180.0));
+  for (int k = 0; k < 3; k++) {
+    float lk = flen * look[k] + eye[k];
+    corner[k] = lk - 0.5f * ((float)W * du[k] + (float)H * dv[k]);
+  }
+}
+
+/* Ray through fragment centre (px+0.5, py+0.5) (input.frag:101-108). */
+static void vol_ray_f32(const so_vol_params *P, int px, int py, float org[3],
+                        float dir[3]) {
+  float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
+  float d[3];
+  for (int k = 0; k < 3; k++)
+    d[k] = (P->corner[k] + fx * P->du[k] + fy * P->dv[k]) - P->eye[k];
+  float dl = sqrtf(dot3f(d, d));
+  for (int k = 0; k < 3; k++) {
+    dir[k] = d[k] / dl;
+    org[k] = P->eye[k];
+  }
+}
+
+/* IntersectP against [-1,1]^3 (input.frag:59-97). */
+static int vol_slab_f32(const float o[3], const float d[3], float *t0o, float *t1o) {
+  float t0 = -10000.0f, t1 = 10000.0f;
+  for (int k = 0; k < 3; k++) {
+    float tn = (-1.0f - o[k]) / d[k];
+    float tf = (1.0f - o[k]) / d[k];
+    if (tn > tf) { float x = tn; tn = tf; tf = x; }
+    t0 = tn > t0 ? tn : t0;
+    t1 = tf < t1 ? tf : t1;
+  }
+  *t0o = t0;
+  *t1o = t1;
+  return t0 <= t1;
+}
+
+static inline int vol_inside_f(const float p[3]) {
+  return p[0] >= -1.0f && p[0] < 1.0f && p[1] >= -1.0f && p[1] < 1.0f &&
+         p[2] >= -1.0f && p[2] < 1.0f;
+}
+
+/* Forward march, FP32.  img: width*height*4 (RGB premultiplied, A = 1 - T). */
+SO_API void so_volume_fwd_f32(const so_vol_params *P, const float *dens,
+                              const int dim[3], const float *tf, float *img,
+                              int nthreads) {
+  int W = P->width, H = P->height;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 4) num_threads(nthreads)
+#endif
+  for (int py = 0; py < H; py++) {
+    for (int px = 0; px < W; px++) {
+      float o[3], d[3], t0, t1;
+      vol_ray_f32(P, px, py, o, d);
+      float C[3] = {0, 0, 0}, T = 1.0f;
+      if (vol_slab_f32(o, d, &t0, &t1)) {
+        int ns = (int)((t1 - t0) / P->step);
+        if (ns > P->max_steps) ns = P->max_steps;
+        for (int s = 0; s < ns; s++) {
+          float t = t0 + ((float)s + 0.5f) * P->step;
+          float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+          if (!vol_inside_f(p)) continue;
+          float rho = tex3d_f32(dens, dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
+                                0.5f * p[2] + 0.5f, 1, 1, 1);
+          float x = rho * 255.0f;
+          x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
+          int i0 = (int)x;
+          int i1 = i0 + 1 < 255 ? i0 + 1 : 255;
+          float f = x - (float)i0;
+          float c[4];
+          for (int k = 0; k < 4; k++) c[k] = lerpf(f, tf[4 * i0 + k], tf[4 * i1 + k]);
+          float sig = P->sigma_scale * c[3];
+          float al = 1.0f - expf(-sig * P->step);
+          if (al > P->alpha_max) al = P->alpha_max;
+          float w = T * al;
+          for (int k = 0; k < 3; k++) C[k] += w * c[k];
+          T = T * (1.0f - al);
+        }
+      }
+      float *out = &img[4 * ((size_t)py * W + px)];
+      out[0] = C[0];
+      out[1] = C[1];
+      out[2] = C[2];
+      out[3] = 1.0f - T;
+    }
+  }
+}
+
+/* ---- FP64 forward + analytic adjoint (reference gradient) --------------- */
+
+
+static void vol_ray_f64(const so_vol_params *P, int px, int py, double o[3], double dir[3]) {
+  /* same construction as the FP32 path, in double, so that the ray set is
+   * the FP32 one to within rounding */
+  float of[3], df[3];
+  vol_ray_f32(P, px, py, of, df);
+  for (int k = 0; k < 3; k++) {
+    o[k] = of[k];
+    dir[k] = df[k];
+  }
+}
+
+static double tex3d_f64(const double *img, const int dim[3], const double q[3],
+                        int cx[8], double w[8]) {
+  double vox[3];
+  int v0[3], v1[3];
+  double fr[3];
+  for (int k = 0; k < 3; k++) {
+    vox[k] = q[k] * (dim[k] - 1.0);
+    int vi = (int)vox[k];
+    vi = clampi(vi, 0, dim[k] - 1);
+    v0[k] = vi;
+    v1[k] = vi + 1 < dim[k] - 1 ? vi + 1 : dim[k] - 1;
+    fr[k] = vox[k] - vi;
+  }
+  double val = 0.0;
+  for (int c = 0; c < 8; c++) {
+    int ix = (c & 1) ? v1[0] : v0[0];
+    int iy = (c & 2) ? v1[1] : v0[1];
+    int iz = (c & 4) ? v1[2] : v0[2];
+    double wx = (c & 1) ? fr[0] : 1.0 - fr[0];
+    double wy = (c & 2) ? fr[1] : 1.0 - fr[1];
+    double wz = (c & 4) ? fr[2] : 1.0 - fr[2];
+    cx[c] = (iz * dim[1] + iy) * dim[0] + ix;
+    w[c] = wx * wy * wz;
+    val += w[c] * img[cx[c]];
+  }
+  return val;
+}
+
+/* FP64 march.  If target != NULL returns loss = sum((img - target)^2) and,
+ * when grad_dens/grad_tf are non-NULL, accumulates the analytic gradients
+ * (reverse-order transmittance recomputation, the same scheme as the CUDA
+ * adjoint).  img (optional): width*height*4 output. */
+SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
+                            const int dim[3], const double *tf,
+                            const float *target, double *img, double *grad_dens,
+                            double *grad_tf) {
+  int W = P->width, H = P->height;
+  double loss = 0.0;
+  const double step = P->step;
+  const int maxs = P->max_steps;
+  for (int py = 0; py < H; py++) {
+    for (int px = 0; px < W; px++) {
+      double o[3], d[3];
+      vol_ray_f64(P, px, py, o, d);
+      /* slab test in double mirroring the FP32 one */
+      double t0 = -10000.0, t1 = 10000.0;
+      for (int k = 0; k < 3; k++) {
+        double tn = (-1.0 - o[k]) / d[k], tf_ = (1.0 - o[k]) / d[k];
+        if (tn > tf_) { double x = tn; tn = tf_; tf_ = x; }
+        t0 = tn > t0 ? tn : t0;
+        t1 = tf_ < t1 ? tf_ : t1;
+      }
+      double C[3] = {0, 0, 0}, T = 1.0;
+      int ns = 0;
+      if (t0 <= t1) {
+        /* the sample count is taken from the FP32 path so both march the
+         * same samples */
+        float of[3], df[3], f0, f1;
+        vol_ray_f32(P, px, py, of, df);
+        vol_slab_f32(of, df, &f0, &f1);
+        ns = (int)((f1 - f0) / P->step);
+        if (ns > maxs) ns = maxs;
+      }
+      for (int s = 0; s < ns; s++) {
+        double t = t0 + (s + 0.5) * step;
+        double p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+        if (!(p[0] >= -1 && p[0] < 1 && p[1] >= -1 && p[1] < 1 && p[2] >= -1 && p[2] < 1))
+          continue;
+        double q[3] = {0.5 * p[0] + 0.5, 0.5 * p[1] + 0.5, 0.5 * p[2] + 0.5};
+        int cx[8];
+        double w[8];
+        double rho = tex3d_f64(dens, dim, q, cx, w);
+        double x = rho * 255.0;
+        x = x < 0 ? 0 : (x > 255 ? 255 : x);
+        int i0 = (int)x, i1 = i0 + 1 < 255 ? i0 + 1 : 255;
+        double f = x - i0;
+        double c[4];
+        for (int k = 0; k < 4; k++) c[k] = (1 - f) * tf[4 * i0 + k] + f * tf[4 * i1 + k];
+        double al = 1.0 - exp(-P->sigma_scale * c[3] * step);
+        if (al > P->alpha_max) al = P->alpha_max;
+        for (int k = 0; k < 3; k++) C[k] += T * al * c[k];
+        T *= (1.0 - al);
+      }
+      double out[4] = {C[0], C[1], C[2], 1.0 - T};
+      if (img)
+        for (int k = 0; k < 4; k++) img[4 * ((size_t)py * W + px) + k] = out[k];
+      if (!target) continue;
+      const float *tg = &target[4 * ((size_t)py * W + px)];
+      double dC[4];
+      for (int k = 0; k < 4; k++) {
+        double e = out[k] - tg[k];
+        loss += e * e;
+        dC[k] = 2.0 * e;
+      }
+      if (!grad_dens && !grad_tf) continue;
+      /* reverse pass: T_k = T_{k+1} / (1 - a_k); Cb = colour of the samples behind k */
+      double Tn = T;         /* transmittance after the current sample */
+      double Cb[3] = {0, 0, 0}; /* accumulated color of samples behind */
+      for (int s = ns - 1; s >= 0; s--) {
+        double t = t0 + (s + 0.5) * step;
+        double p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+        if (!(p[0] >= -1 && p[0] < 1 && p[1] >= -1 && p[1] < 1 && p[2] >= -1 && p[2] < 1))
+          continue;
+        double q[3] = {0.5 * p[0] + 0.5, 0.5 * p[1] + 0.5, 0.5 * p[2] + 0.5};
+        int cx[8];
+        double w[8];
+        double rho = tex3d_f64(dens, dim, q, cx, w);
+        double xr = rho * 255.0;
+        int inr = (xr > 0.0 && xr < 255.0);
+        double x = xr < 0 ? 0 : (xr > 255 ? 255 : xr);
+        int i0 = (int)x, i1 = i0 + 1 < 255 ? i0 + 1 : 255;
+        double f = x - i0;
+        double c[4];
+        for (int k = 0; k < 4; k++) c[k] = (1 - f) * tf[4 * i0 + k] + f * tf[4 * i1 + k];
+        double e = exp(-P->sigma_scale * c[3] * step);
+        double al = 1.0 - e;
+        int clamped = al > P->alpha_max;
+        if (clamped) al = P->alpha_max;
+        double Tk = Tn / (1.0 - al);
+        /* dL/dc_rgb = dC * T_k * a_k */
+        double gc[4];
+        for (int k = 0; k < 3; k++) gc[k] = dC[k] * Tk * al;
+        /* dL/da_k */
+        double ga = 0.0;
+        for (int k = 0; k < 3; k++) ga += dC[k] * (Tk * c[k] - Cb[k] / (1.0 - al));
+        ga += dC[3] * (T / (1.0 - al)); /* dA/da_k = T_final / (1 - a_k) */
+        /* a = 1 - exp(-s*c_a*step) -> da/dc_a = s*step*exp(...) */
+        gc[3] = clamped ? 0.0 : ga * P->sigma_scale * step * e;
+        if (grad_tf) {
+          for (int k = 0; k < 4; k++) {
+            grad_tf[4 * i0 + k] += (1 - f) * gc[k];
+            grad_tf[4 * i1 + k] += f * gc[k];
+          }
+        }
+        if (grad_dens && inr) {
+          double drho = 0.0;
+          for (int k = 0; k < 4; k++) drho += gc[k] * (tf[4 * i1 + k] - tf[4 * i0 + k]);
+          drho *= 255.0;
+          for (int cc = 0; cc < 8; cc++) grad_dens[cx[cc]] += w[cc] * drho;
+        }
+        for (int k = 0; k < 3; k++) Cb[k] += Tk * al * c[k];
+        Tn = Tk;
+      }
+    }
+  }
+  return loss;
+}

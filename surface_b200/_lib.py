@@ -1,0 +1,123 @@
+"""ctypes declarations for libsurface_rt.so (include/surface_rt.h).
+
+The library is the product: there is no CPU fallback.  ``load()`` raises if
+the shared object is missing and cannot be built, and ``Context`` raises if no
+CUDA device is present.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+import numpy as np
+
+from . import build as _build
+
+SRT_OK, SRT_ERR_INVALID, SRT_ERR_CUDA, SRT_ERR_NO_MEMORY, SRT_ERR_LIMIT, SRT_ERR_UNSUPPORTED = range(6)
+SRT_TRIANGLES, SRT_TETRAHEDRA, SRT_SPHERES = 0, 1, 2
+MISS = 0xFFFFFFFF
+
+RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
+                      ("prev_t", "<f4")])
+HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4")])
+VOL_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("max_steps", "<i4"),
+                      ("reserved", "<i4"), ("eye", "<f4", 3), ("corner", "<f4", 3),
+                      ("du", "<f4", 3), ("dv", "<f4", 3), ("step", "<f4"),
+                      ("sigma_scale", "<f4"), ("alpha_max", "<f4")])
+
+
+class SurfaceError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"surface_rt error {status}: {msg}")
+        self.status = status
+
+
+class TraceOpts(C.Structure):
+    _fields_ = [("prev_normals", C.c_void_p), ("subface", C.c_void_p),
+                ("vertex_scalar", C.c_void_p), ("scalar_out", C.c_void_p),
+                ("normal_out", C.c_void_p), ("stats", C.c_void_p)]
+
+
+class AccelInfo(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("node_bytes", C.c_int32), ("num_prims", C.c_uint64),
+                ("num_nodes", C.c_uint64), ("num_branches", C.c_uint64),
+                ("num_leaves", C.c_uint64), ("scene_min", C.c_float * 3),
+                ("scene_max", C.c_float * 3), ("eps_scale", C.c_double)]
+
+
+_P = C.c_void_p
+_SZ = C.c_size_t
+_S = C.c_int
+
+# name -> argtypes (all return srt_status unless listed in _RESTYPES)
+_SIGS = {
+    "srt_ctx_create": [C.c_int, C.POINTER(_P)],
+    "srt_ctx_destroy": [_P],
+    "srt_ctx_set_stream": [_P, _P],
+    "srt_ctx_get_stream": [_P],
+    "srt_ctx_synchronize": [_P],
+    "srt_last_error": [],
+    "srt_ctx_launch_count": [_P],
+    "srt_accel_create": [_P, C.c_int, C.POINTER(_P)],
+    "srt_accel_destroy": [_P],
+    "srt_accel_build_triangles": [_P, _P, _SZ, _P, _SZ],
+    "srt_accel_build_tetrahedra": [_P, _P, _SZ, _P, _SZ],
+    "srt_accel_build_spheres": [_P, _P, _P, C.c_float, _SZ],
+    "srt_build_triangles": [_P, _P, _SZ, _P, _SZ, C.POINTER(_P)],
+    "srt_build_tetrahedra": [_P, _P, _SZ, _P, _SZ, C.POINTER(_P)],
+    "srt_build_spheres": [_P, _P, _P, C.c_float, _SZ, C.POINTER(_P)],
+    "srt_accel_bbox": [_P, _P, _P],
+    "srt_accel_info_get": [_P, C.POINTER(AccelInfo)],
+    "srt_accel_export": [_P, _P, _P, _P],
+    "srt_accel_dump": [_P, C.c_char_p],
+    "srt_trace_closest": [_P, _P, _SZ, _P, C.POINTER(TraceOpts)],
+    "srt_stage_morton": [_P, C.c_int, _P, _SZ, _P, _P, C.c_float, _SZ, _P, _P],
+    "srt_stage_sort_pairs": [_P, _P, _P, _SZ],
+    "srt_stage_karras": [_P, _P, _SZ, _P, _P, _P],
+    "srt_volume_camera": [C.c_int32, C.c_int32, _P, _P, _P, C.c_float, _P],
+    "srt_volume_march_fwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P],
+    "srt_volume_march_bwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P],
+    "srt_batch_create": [_P, C.POINTER(_P)],
+    "srt_batch_destroy": [_P],
+    "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],
+}
+_RESTYPES = {"srt_last_error": C.c_char_p, "srt_ctx_get_stream": _P,
+             "srt_ctx_launch_count": C.c_uint64}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def library_path():
+    return _build.LIB
+
+
+def load():
+    """Load libsurface_rt.so, building it first if it is absent or stale."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(_build.LIB):
+            try:
+                _build.build()
+            except Exception as e:  # noqa: BLE001
+                raise ImportError(f"libsurface_rt.so is missing and could not be built: {e}")
+        L = C.CDLL(_build.LIB)
+        for name, args in _SIGS.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = _RESTYPES.get(name, _S)
+        _lib = L
+        return L
+
+
+def check(status):
+    if status != SRT_OK:
+        raise SurfaceError(status, load().srt_last_error().decode(errors="replace"))
+    return status
+
+
+def exported_symbols():
+    return list(_SIGS)

@@ -1,0 +1,903 @@
+// srt_build.cu -- LBVH build on the GPU, bit-exact with the reference's Build32.
+//
+// Pipeline (one CUDA stream, no host round trip):
+//   1. scene box          bbox_partial + bbox_final
+//        render/render_accel_triangle.cc:713-796 (eps 0),
+//        render/render_accel_tetra.cc:973-1030, render/render_accel_particle.cc:304-369
+//   2. Morton codes       morton_kernel
+//        render/render_prefix_tree_util.cc:151-304, render/render_prefix_tree_util.h:113-157
+//   3. stable sort        rs_hist / scan / rs_scatter, 4 x 8-bit LSD passes
+//        render/render_prefix_tree_util.h:296-457 (stable; ties keep input order)
+//   4. Karras tree        karras_kernel
+//        render/render_prefix_tree_util.cc:501-649
+//   5. bottom-up boxes    refit_kernel (also writes the leaf-ordered primitive
+//        cache used by traversal); union order = the reference's MergeBoundingBox
+//        render/render_accel_triangle.cc:804, ComputeBoundingBox30 :661-709
+//   6. leaf collapse      level_kernel: a Karras node is emitted as a branch iff
+//        its range holds more than max_leaf+1 keys and its level is <= 23;
+//        both tests are monotone along root paths, so the emitted branches
+//        are exactly the top-down recursion's (BuildTreeRecursive32,
+//        render/render_accel_triangle.cc:896-992; tetra :1113-1243;
+//        particle :521-661)
+//   7. compaction         exclusive scan of the branch flags -> node slots
+//   8. emission           emit_node2_kernel / emit_tet_kernel
+#include <algorithm>
+#include <cstdio>
+
+#include "srt_internal.cuh"
+
+namespace srt {
+namespace {
+
+constexpr int kBlock = 256;
+
+inline int grid_for(size_t n, int block, int max_blocks) {
+  size_t g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if ((size_t)max_blocks < g) g = max_blocks;
+  return (int)g;
+}
+
+// ------------------------------------------------------------------ primitives
+// Leaf-ordered primitive cache (written by refit_kernel, read by traversal):
+//   triangles: 3 float4 per prim: (p0, id bits), (p1, 0), (p2, 0)
+//   tetrahedra: 3 float4 per prim: 12 vertex coordinates v0..v3
+//   spheres:   1 float4 per prim: (centre, radius)
+template <int KIND>
+struct PrimTraits;
+
+template <>
+struct PrimTraits<SRT_TRIANGLES> {
+  static constexpr int kCacheF4 = 3;
+  static constexpr int kMaxLeaf = 16;
+};
+template <>
+struct PrimTraits<SRT_TETRAHEDRA> {
+  static constexpr int kCacheF4 = 3;
+  static constexpr int kMaxLeaf = 4;
+};
+template <>
+struct PrimTraits<SRT_SPHERES> {
+  static constexpr int kCacheF4 = 1;
+  static constexpr int kMaxLeaf = 16;
+};
+
+__device__ __forceinline__ void box_init(Box &b) {
+  b.lo[0] = b.lo[1] = b.lo[2] = FLT_MAX;
+  b.hi[0] = b.hi[1] = b.hi[2] = -FLT_MAX;
+}
+
+// Fold point p padded by e into b, first-value-kept on ties (the
+// `if (bmin[k] > minval) bmin[k] = minval` loop of ComputeBoundingBox30).
+__device__ __forceinline__ void box_add(Box &b, float x, float y, float z, float e) {
+  float m;
+  m = x - e; if (b.lo[0] > m) b.lo[0] = m;
+  m = y - e; if (b.lo[1] > m) b.lo[1] = m;
+  m = z - e; if (b.lo[2] > m) b.lo[2] = m;
+  m = x + e; if (b.hi[0] < m) b.hi[0] = m;
+  m = y + e; if (b.hi[1] < m) b.hi[1] = m;
+  m = z + e; if (b.hi[2] < m) b.hi[2] = m;
+}
+
+// MergeBoundingBox (render/render_accel_triangle.cc:804): left first.
+__device__ __forceinline__ Box box_merge(const Box &l, const Box &r) {
+  Box o;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    o.lo[k] = fmin_ref(l.lo[k], r.lo[k]);
+    o.hi[k] = fmax_ref(l.hi[k], r.hi[k]);
+  }
+  return o;
+}
+
+// Box of sorted primitive j from the primitive cache.
+template <int KIND>
+__device__ __forceinline__ Box cache_box(const float4 *__restrict__ prims, uint32_t j,
+                                         float keps) {
+  Box b;
+  box_init(b);
+  if (KIND == SRT_TRIANGLES) {
+    float4 p0 = __ldcg(&prims[3 * (size_t)j + 0]);
+    float4 p1 = __ldcg(&prims[3 * (size_t)j + 1]);
+    float4 p2 = __ldcg(&prims[3 * (size_t)j + 2]);
+    box_add(b, p0.x, p0.y, p0.z, keps);
+    box_add(b, p1.x, p1.y, p1.z, keps);
+    box_add(b, p2.x, p2.y, p2.z, keps);
+  } else if (KIND == SRT_TETRAHEDRA) {
+    float4 a = __ldcg(&prims[3 * (size_t)j + 0]);
+    float4 c = __ldcg(&prims[3 * (size_t)j + 1]);
+    float4 d = __ldcg(&prims[3 * (size_t)j + 2]);
+    box_add(b, a.x, a.y, a.z, keps);
+    box_add(b, a.w, c.x, c.y, keps);
+    box_add(b, c.z, c.w, d.x, keps);
+    box_add(b, d.y, d.z, d.w, keps);
+  } else {
+    float4 s = __ldcg(&prims[j]);
+    // (centre - radius) - eps, (centre + radius) + eps
+    float lx = s.x - s.w, ly = s.y - s.w, lz = s.z - s.w;
+    float hx = s.x + s.w, hy = s.y + s.w, hz = s.z + s.w;
+    b.lo[0] = lx - keps; b.lo[1] = ly - keps; b.lo[2] = lz - keps;
+    b.hi[0] = hx + keps; b.hi[1] = hy + keps; b.hi[2] = hz + keps;
+  }
+  return b;
+}
+
+// ------------------------------------------------------------------ 1. scene box
+template <int KIND>
+__global__ void bbox_partial_kernel(const float *__restrict__ v,
+                                    const uint32_t *__restrict__ f,
+                                    const float *__restrict__ radius, float constr,
+                                    size_t n, Box *__restrict__ partial) {
+  Box b;
+  box_init(b);
+  const float e = (KIND == SRT_TRIANGLES) ? 0.0f : FLT_EPSILON * 16;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    if (KIND == SRT_SPHERES) {
+      float r = radius ? radius[i] : constr;
+      float x = v[3 * i], y = v[3 * i + 1], z = v[3 * i + 2];
+      float m;
+      m = x - r - e; if (b.lo[0] > m) b.lo[0] = m;
+      m = y - r - e; if (b.lo[1] > m) b.lo[1] = m;
+      m = z - r - e; if (b.lo[2] > m) b.lo[2] = m;
+      m = x + r + e; if (b.hi[0] < m) b.hi[0] = m;
+      m = y + r + e; if (b.hi[1] < m) b.hi[1] = m;
+      m = z + r + e; if (b.hi[2] < m) b.hi[2] = m;
+    } else {
+      const int nv = (KIND == SRT_TRIANGLES) ? 3 : 4;
+#pragma unroll
+      for (int c = 0; c < nv; c++) {
+        size_t vi = f[(size_t)nv * i + c];
+        box_add(b, v[3 * vi], v[3 * vi + 1], v[3 * vi + 2], e);
+      }
+    }
+  }
+  // block reduction (min/max are exact; order only matters for the sign of
+  // zero, which the reference's own OpenMP merge leaves unspecified)
+  __shared__ Box sh[kBlock / 32];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      b.lo[k] = fmin_ref(b.lo[k], __shfl_down_sync(0xffffffffu, b.lo[k], o));
+      b.hi[k] = fmax_ref(b.hi[k], __shfl_down_sync(0xffffffffu, b.hi[k], o));
+    }
+  }
+  int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Box r = sh[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) r = box_merge(r, sh[i]);
+    partial[blockIdx.x] = r;
+  }
+}
+
+template <int KIND>
+__global__ void bbox_final_kernel(const Box *__restrict__ partial, int np,
+                                  SceneInfo *__restrict__ scene) {
+  if (threadIdx.x != 0) return;
+  Box r = partial[0];
+  for (int i = 1; i < np; i++) r = box_merge(r, partial[i]);
+  SceneInfo s;
+  for (int k = 0; k < 3; k++) {
+    s.lo[k] = r.lo[k];
+    s.hi[k] = r.hi[k];
+    s.inv[k] = 1024.0f / (r.hi[k] - r.lo[k]);
+  }
+  if (KIND == SRT_TRIANGLES) {
+    // epsScale = max extent (render/render_accel_triangle.cc:1452-1463)
+    double es = (double)(r.hi[0] - r.lo[0]);
+    if (es < (double)(r.hi[1] - r.lo[1])) es = (double)(r.hi[1] - r.lo[1]);
+    if (es < (double)(r.hi[2] - r.lo[2])) es = (double)(r.hi[2] - r.lo[2]);
+    s.eps_scale = es;
+    s.keps = FLT_EPSILON * (float)es;
+  } else {
+    s.eps_scale = 16.0;
+    s.keps = FLT_EPSILON * 16;
+  }
+  s.nbranches = 0;
+  s.pad = 0;
+  *scene = s;
+}
+
+// ------------------------------------------------------------------ 2. Morton
+template <int KIND>
+__global__ void morton_kernel(const float *__restrict__ v,
+                              const uint32_t *__restrict__ f, size_t n,
+                              const SceneInfo *__restrict__ scene,
+                              uint32_t *__restrict__ codes,
+                              uint32_t *__restrict__ index) {
+  const float lx = scene->lo[0], ly = scene->lo[1], lz = scene->lo[2];
+  const float ix = scene->inv[0], iy = scene->inv[1], iz = scene->inv[2];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float cx, cy, cz;
+    if (KIND == SRT_SPHERES) {
+      cx = v[3 * i];
+      cy = v[3 * i + 1];
+      cz = v[3 * i + 2];
+    } else if (KIND == SRT_TRIANGLES) {
+      const float third = 1.0f / 3.0f;
+      size_t a = f[3 * i], b = f[3 * i + 1], c = f[3 * i + 2];
+      cx = third * ((v[3 * a] + v[3 * b]) + v[3 * c]);
+      cy = third * ((v[3 * a + 1] + v[3 * b + 1]) + v[3 * c + 1]);
+      cz = third * ((v[3 * a + 2] + v[3 * b + 2]) + v[3 * c + 2]);
+    } else {
+      const float fourth = 1.0f / 4.0f;
+      size_t a = f[4 * i], b = f[4 * i + 1], c = f[4 * i + 2], d = f[4 * i + 3];
+      cx = fourth * (((v[3 * a] + v[3 * b]) + v[3 * c]) + v[3 * d]);
+      cy = fourth * (((v[3 * a + 1] + v[3 * b + 1]) + v[3 * c + 1]) + v[3 * d + 1]);
+      cz = fourth * (((v[3 * a + 2] + v[3 * b + 2]) + v[3 * c + 2]) + v[3 * d + 2]);
+    }
+    uint32_t qx = f2u32_x86((cx - lx) * ix);
+    uint32_t qy = f2u32_x86((cy - ly) * iy);
+    uint32_t qz = f2u32_x86((cz - lz) * iz);
+    codes[i] = (spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz);
+    if (index) index[i] = (uint32_t)i;
+  }
+}
+
+// ------------------------------------------------------------------ scan
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+// Block-wide exclusive scan of a tile; returns the tile total.
+__device__ uint32_t block_exclusive_scan(uint32_t (&x)[kScanItems]) {
+  __shared__ uint32_t warp_tot[32];
+  __shared__ uint32_t total;
+  const int nwarps = (int)(blockDim.x >> 5);
+  uint32_t s = 0;
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) {
+    uint32_t t = x[i];
+    x[i] = s;
+    s += t;
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t inc = s;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) warp_tot[w] = inc;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t t = (lane < nwarps) ? warp_tot[lane] : 0u;
+    uint32_t ti = t;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, ti, o);
+      if (lane >= o) ti += y;
+    }
+    if (lane < nwarps) warp_tot[lane] = ti - t;
+    if (lane == nwarps - 1) total = ti;
+  }
+  __syncthreads();
+  const uint32_t base = warp_tot[w] + (inc - s);
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) x[i] += base;
+  const uint32_t r = total;
+  __syncthreads();
+  return r;
+}
+
+__global__ void scan_tiles_kernel(const uint32_t *__restrict__ in,
+                                  uint32_t *__restrict__ out, size_t n,
+                                  uint32_t *__restrict__ tile_sums) {
+  size_t base = (size_t)blockIdx.x * kScanTile + (size_t)threadIdx.x * kScanItems;
+  uint32_t x[kScanItems];
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++) x[i] = (base + i < n) ? in[base + i] : 0u;
+  uint32_t tot = block_exclusive_scan(x);
+#pragma unroll
+  for (int i = 0; i < kScanItems; i++)
+    if (base + i < n) out[base + i] = x[i];
+  if (threadIdx.x == 0 && tile_sums) tile_sums[blockIdx.x] = tot;
+}
+
+__global__ void scan_add_kernel(uint32_t *__restrict__ out, size_t n,
+                                const uint32_t *__restrict__ tile_off) {
+  uint32_t add = tile_off[blockIdx.x];
+  size_t base = (size_t)blockIdx.x * kScanTile;
+  for (int i = threadIdx.x; i < kScanTile; i += blockDim.x)
+    if (base + i < n) out[base + i] += add;
+}
+
+}  // namespace
+
+// Exclusive scan of n uint32 (out may alias in); tile sums of each level go
+// to `scratch` (needs about n / 4095 + 4 words).
+static srt_status scan_levels(cudaStream_t st, const uint32_t *in, uint32_t *out,
+                              size_t n, uint32_t *scratch, uint64_t &launches) {
+  size_t tiles = (n + kScanTile - 1) / kScanTile;
+  if (tiles <= 1) {
+    scan_tiles_kernel<<<1, kScanThreads, 0, st>>>(in, out, n, nullptr);
+    launches++;
+    return cuda_status(cudaGetLastError(), "scan");
+  }
+  uint32_t *sums = scratch;
+  scan_tiles_kernel<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, sums);
+  launches++;
+  srt_status s = cuda_status(cudaGetLastError(), "scan tiles");
+  if (s != SRT_OK) return s;
+  s = scan_levels(st, sums, sums, tiles, scratch + tiles, launches);
+  if (s != SRT_OK) return s;
+  scan_add_kernel<<<(unsigned)tiles, 256, 0, st>>>(out, n, sums);
+  launches++;
+  return cuda_status(cudaGetLastError(), "scan add");
+}
+
+static srt_status exclusive_scan(srt_ctx *ctx, const uint32_t *in, uint32_t *out,
+                                 size_t n) {
+  size_t need = 64;
+  for (size_t t = (n + kScanTile - 1) / kScanTile; t > 1;
+       t = (t + kScanTile - 1) / kScanTile)
+    need += t + 1;
+  cudaError_t e = ctx->s_scan.ensure(need * sizeof(uint32_t));
+  if (e != cudaSuccess) return cuda_status(e, "scan scratch");
+  return scan_levels(ctx->stream, in, out, n, ctx->s_scan.as<uint32_t>(), ctx->launches);
+}
+
+namespace {
+// ------------------------------------------------------------------ 3. radix sort
+constexpr int kRsBits = 8;
+constexpr int kRsBins = 1 << kRsBits;
+constexpr int kRsWarps = 8;
+constexpr int kRsThreads = kRsWarps * 32;
+constexpr int kRsRounds = 16;
+constexpr int kRsWChunk = 32 * kRsRounds;
+constexpr int kRsTile = kRsWarps * kRsWChunk;
+
+// Per-tile digit histogram, digit-major: hist[d * ntiles + tile].
+__global__ void __launch_bounds__(kRsThreads)
+rs_hist_kernel(const uint32_t *__restrict__ keys, size_t n, int shift,
+               uint32_t *__restrict__ hist, uint32_t ntiles) {
+  __shared__ uint32_t wh[kRsWarps][kRsBins];
+  for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads)
+    (&wh[0][0])[i] = 0;
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  size_t base = (size_t)blockIdx.x * kRsTile + (size_t)w * kRsWChunk;
+#pragma unroll 4
+  for (int r = 0; r < kRsRounds; r++) {
+    size_t idx = base + (size_t)r * 32 + lane;
+    bool ok = idx < n;
+    unsigned valid = __ballot_sync(0xffffffffu, ok);
+    if (ok) {
+      uint32_t d = (keys[idx] >> shift) & (kRsBins - 1);
+      unsigned peers = __match_any_sync(valid, d);
+      if (lane == __ffs(peers) - 1) wh[w][d] += __popc(peers);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < kRsBins; d += kRsThreads) {
+    uint32_t s = 0;
+#pragma unroll
+    for (int k = 0; k < kRsWarps; k++) s += wh[k][d];
+    hist[(size_t)d * ntiles + blockIdx.x] = s;
+  }
+}
+
+// Stable scatter of one tile: warps own consecutive chunks, rounds go in key
+// order, lanes within a round are ranked by lane order among equal digits.
+__global__ void __launch_bounds__(kRsThreads)
+rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
+                  uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, size_t n,
+                  int shift, const uint32_t *__restrict__ offs, uint32_t ntiles) {
+  __shared__ uint32_t wc[kRsWarps][kRsBins];
+  for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads)
+    (&wc[0][0])[i] = 0;
+  __syncthreads();
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const unsigned lt = (1u << lane) - 1u;
+  size_t base = (size_t)blockIdx.x * kRsTile + (size_t)w * kRsWChunk;
+  uint32_t k[kRsRounds], v[kRsRounds];
+#pragma unroll
+  for (int r = 0; r < kRsRounds; r++) {
+    size_t idx = base + (size_t)r * 32 + lane;
+    if (idx < n) {
+      k[r] = kin[idx];
+      v[r] = vin ? vin[idx] : (uint32_t)idx;
+    } else {
+      k[r] = 0;
+      v[r] = 0;
+    }
+  }
+  // warp histograms
+#pragma unroll
+  for (int r = 0; r < kRsRounds; r++) {
+    size_t idx = base + (size_t)r * 32 + lane;
+    bool ok = idx < n;
+    unsigned valid = __ballot_sync(0xffffffffu, ok);
+    if (ok) {
+      uint32_t d = (k[r] >> shift) & (kRsBins - 1);
+      unsigned peers = __match_any_sync(valid, d);
+      if (lane == __ffs(peers) - 1) wc[w][d] += __popc(peers);
+    }
+    __syncwarp();
+  }
+  __syncthreads();
+  // warp start offsets: global tile offset + counts of earlier warps
+  for (int d = threadIdx.x; d < kRsBins; d += kRsThreads) {
+    uint32_t run = offs[(size_t)d * ntiles + blockIdx.x];
+#pragma unroll
+    for (int q = 0; q < kRsWarps; q++) {
+      uint32_t c = wc[q][d];
+      wc[q][d] = run;
+      run += c;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < kRsRounds; r++) {
+    size_t idx = base + (size_t)r * 32 + lane;
+    bool ok = idx < n;
+    unsigned valid = __ballot_sync(0xffffffffu, ok);
+    uint32_t d = (k[r] >> shift) & (kRsBins - 1);
+    unsigned peers = ok ? __match_any_sync(valid, d) : 0u;
+    uint32_t pos = 0;
+    if (ok) pos = wc[w][d] + __popc(peers & lt);
+    __syncwarp();
+    if (ok) {
+      kout[pos] = k[r];
+      vout[pos] = v[r];
+      if (lane == __ffs(peers) - 1) wc[w][d] += __popc(peers);
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+// Stable LSD sort of (keys, vals) by key; result lands back in keys/vals.
+srt_status sort_pairs(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
+                      bool identity_vals) {
+  if (n == 0) return SRT_OK;
+  cudaStream_t st = ctx->stream;
+  uint32_t ntiles = (uint32_t)((n + kRsTile - 1) / kRsTile);
+  cudaError_t e;
+  if ((e = ctx->s_keys2.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "sort");
+  if ((e = ctx->s_vals2.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "sort");
+  if ((e = ctx->s_hist.ensure((size_t)kRsBins * ntiles * 4)) != cudaSuccess)
+    return cuda_status(e, "sort");
+  uint32_t *k0 = keys, *v0 = vals, *k1 = ctx->s_keys2.as<uint32_t>(),
+           *v1 = ctx->s_vals2.as<uint32_t>();
+  uint32_t *hist = ctx->s_hist.as<uint32_t>();
+  for (int pass = 0; pass < 4; pass++) {
+    int shift = pass * kRsBits;
+    rs_hist_kernel<<<ntiles, kRsThreads, 0, st>>>(k0, n, shift, hist, ntiles);
+    ctx->launches++;
+    srt_status s = cuda_status(cudaGetLastError(), "rs_hist");
+    if (s != SRT_OK) return s;
+    s = exclusive_scan(ctx, hist, hist, (size_t)kRsBins * ntiles);
+    if (s != SRT_OK) return s;
+    const uint32_t *vin = (pass == 0 && identity_vals) ? nullptr : v0;
+    rs_scatter_kernel<<<ntiles, kRsThreads, 0, st>>>(k0, vin, k1, v1, n, shift, hist,
+                                                    ntiles);
+    ctx->launches++;
+    s = cuda_status(cudaGetLastError(), "rs_scatter");
+    if (s != SRT_OK) return s;
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  return SRT_OK;  // even number of passes: data is back in keys/vals
+}
+
+namespace {
+// ------------------------------------------------------------------ 4. Karras
+// Delta30 (render/render_prefix_tree_util.cc:501-526).
+__device__ __forceinline__ int kdelta(const uint32_t *__restrict__ c, int i, int j,
+                                      int n) {
+  if (j < 0 || j >= n) return -1;
+  uint32_t a = __ldg(&c[i]), b = __ldg(&c[j]);
+  if (a == b) return 32 + __clz((uint32_t)i ^ (uint32_t)j);
+  return __clz(a ^ b);
+}
+
+// ConstructBinaryRadixTree30 for every internal node; also records ranges
+// and parent links for the bottom-up pass.
+__global__ void karras_kernel(const uint32_t *__restrict__ codes, int n,
+                              uint32_t *__restrict__ kchild, uint8_t *__restrict__ kflags,
+                              uint2 *__restrict__ krange, uint32_t *__restrict__ kparent,
+                              uint32_t *__restrict__ lparent) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+       i += gridDim.x * blockDim.x) {
+    int d = (kdelta(codes, i, i + 1, n) - kdelta(codes, i, i - 1, n)) >= 0 ? 1 : -1;
+    int dmin = kdelta(codes, i, i - d, n);
+    int lmax = 2;
+    while (kdelta(codes, i, i + lmax * d, n) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+      if (kdelta(codes, i, i + (l + t) * d, n) > dmin) l += t;
+    int j = i + l * d;
+    int dnode = kdelta(codes, i, j, n);
+    int s = 0;
+    for (int k = 2;; k *= 2) {  // t = ceil(l/2), ceil(l/4), ..., 1
+      int t = (l + k - 1) / k;
+      if (t <= 0) break;
+      if (kdelta(codes, i, i + (s + t) * d, n) > dnode) s += t;
+      if (t == 1) break;
+    }
+    int g = i + s * d + (d < 0 ? d : 0);
+    int lo = i < j ? i : j, hi = i < j ? j : i;
+    bool lleaf = (lo == g), rleaf = (hi == g + 1);
+    if (kchild) kchild[i] = (uint32_t)g;
+    kflags[i] = (uint8_t)((lleaf ? 1 : 0) | (rleaf ? 2 : 0));
+    if (krange) krange[i] = make_uint2((uint32_t)lo, (uint32_t)hi);
+    if (kparent) {
+      if (lleaf) lparent[g] = (uint32_t)i; else kparent[g] = (uint32_t)i;
+      if (rleaf) lparent[g + 1] = (uint32_t)i; else kparent[g + 1] = (uint32_t)i;
+      if (i == 0) kparent[0] = kNone;
+    }
+  }
+}
+
+// ------------------------------------------------------------------ 5. refit
+// Thread per sorted position j: write the primitive cache entry, then climb
+// while this thread is the second child to finish (atomic counter per node).
+template <int KIND>
+__global__ void refit_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f,
+                             const float *__restrict__ radius, float constr,
+                             const uint32_t *__restrict__ sidx, int n,
+                             const SceneInfo *__restrict__ scene,
+                             const uint32_t *__restrict__ lparent,
+                             const uint32_t *__restrict__ kparent,
+                             const uint32_t *__restrict__ kchild,
+                             const uint8_t *__restrict__ kflags,
+                             uint32_t *__restrict__ counter, Box *__restrict__ ibox,
+                             float4 *__restrict__ prims, uint32_t *__restrict__ err) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const float keps = scene->keps;
+  uint32_t p = sidx[j];
+  Box mine;
+  box_init(mine);
+  if (KIND == SRT_TRIANGLES) {
+    size_t a = f[3 * (size_t)p], b = f[3 * (size_t)p + 1], c = f[3 * (size_t)p + 2];
+    float4 p0 = make_float4(v[3 * a], v[3 * a + 1], v[3 * a + 2], __uint_as_float(p));
+    float4 p1 = make_float4(v[3 * b], v[3 * b + 1], v[3 * b + 2], 0.0f);
+    float4 p2 = make_float4(v[3 * c], v[3 * c + 1], v[3 * c + 2], 0.0f);
+    prims[3 * (size_t)j + 0] = p0;
+    prims[3 * (size_t)j + 1] = p1;
+    prims[3 * (size_t)j + 2] = p2;
+    box_add(mine, p0.x, p0.y, p0.z, keps);
+    box_add(mine, p1.x, p1.y, p1.z, keps);
+    box_add(mine, p2.x, p2.y, p2.z, keps);
+  } else if (KIND == SRT_TETRAHEDRA) {
+    size_t q[4];
+#pragma unroll
+    for (int c = 0; c < 4; c++) q[c] = f[4 * (size_t)p + c];
+    float x[12];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      x[3 * c] = v[3 * q[c]];
+      x[3 * c + 1] = v[3 * q[c] + 1];
+      x[3 * c + 2] = v[3 * q[c] + 2];
+      box_add(mine, x[3 * c], x[3 * c + 1], x[3 * c + 2], keps);
+    }
+    prims[3 * (size_t)j + 0] = make_float4(x[0], x[1], x[2], x[3]);
+    prims[3 * (size_t)j + 1] = make_float4(x[4], x[5], x[6], x[7]);
+    prims[3 * (size_t)j + 2] = make_float4(x[8], x[9], x[10], x[11]);
+  } else {
+    float r = radius ? radius[p] : constr;
+    float4 s = make_float4(v[3 * (size_t)p], v[3 * (size_t)p + 1], v[3 * (size_t)p + 2], r);
+    prims[j] = s;
+    mine.lo[0] = (s.x - r) - keps; mine.lo[1] = (s.y - r) - keps; mine.lo[2] = (s.z - r) - keps;
+    mine.hi[0] = (s.x + r) + keps; mine.hi[1] = (s.y + r) + keps; mine.hi[2] = (s.z + r) + keps;
+  }
+  uint32_t cur = (uint32_t)j;
+  bool cur_leaf = true;
+  uint32_t node = lparent[j];
+  for (int guard = 0; guard < 2 * n + 64; guard++) {
+    __threadfence();
+    uint32_t old = atomicAdd(&counter[node], 1u);
+    if (old == 0) return;  // sibling still pending; it will continue
+    __threadfence();
+    uint32_t g = __ldcg(&kchild[node]);
+    uint8_t fl = __ldcg(&kflags[node]);
+    bool lleaf = fl & 1, rleaf = fl & 2;
+    bool i_am_left = (cur == g) && (cur_leaf == lleaf);
+    uint32_t sib = i_am_left ? g + 1 : g;
+    bool sib_leaf = i_am_left ? rleaf : lleaf;
+    Box sb;
+    if (sib_leaf) {
+      sb = cache_box<KIND>(prims, sib, keps);
+    } else {
+      const float *src = reinterpret_cast<const float *>(&ibox[sib]);
+      sb.lo[0] = __ldcg(src + 0); sb.lo[1] = __ldcg(src + 1); sb.lo[2] = __ldcg(src + 2);
+      sb.hi[0] = __ldcg(src + 3); sb.hi[1] = __ldcg(src + 4); sb.hi[2] = __ldcg(src + 5);
+    }
+    mine = i_am_left ? box_merge(mine, sb) : box_merge(sb, mine);
+    ibox[node] = mine;
+    if (node == 0) return;
+    cur = node;
+    cur_leaf = false;
+    node = __ldcg(&kparent[node]);
+    if (node == kNone) return;
+  }
+  atomicOr(err, kErrTree);
+}
+
+// ------------------------------------------------------------------ 6. levels
+// flag[i] = 1 iff Karras internal node i is emitted as a branch.
+__global__ void level_kernel(const uint2 *__restrict__ krange,
+                             const uint32_t *__restrict__ kparent, int n, int max_leaf,
+                             uint32_t *__restrict__ flag) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+       i += gridDim.x * blockDim.x) {
+    uint2 r = krange[i];
+    uint32_t f = 0;
+    if (i == 0) {
+      f = 1;  // Build32 always splits the root
+    } else if (r.y - r.x > (uint32_t)max_leaf) {
+      int lvl = 0;
+      uint32_t x = (uint32_t)i;
+      while (x != 0 && lvl <= kMaxLevel) {
+        x = kparent[x];
+        lvl++;
+      }
+      f = (lvl <= kMaxLevel) ? 1u : 0u;
+    }
+    flag[i] = f;
+  }
+}
+
+// ------------------------------------------------------------------ 7. emission
+template <int KIND>
+__device__ __forceinline__ void child_info(uint32_t c, bool kleaf,
+                                           const uint2 *__restrict__ krange,
+                                           const uint32_t *__restrict__ flag,
+                                           const uint32_t *__restrict__ slot,
+                                           const Box *__restrict__ ibox,
+                                           const float4 *__restrict__ prims, float keps,
+                                           Box &box, bool &is_branch, uint32_t &ref,
+                                           uint32_t &count) {
+  if (kleaf) {
+    box = cache_box<KIND>(prims, c, keps);
+    is_branch = false;
+    ref = c;
+    count = 1;
+    return;
+  }
+  box = ibox[c];
+  if (flag[c]) {
+    is_branch = true;
+    ref = slot[c];
+    count = 0;
+  } else {
+    uint2 r = krange[c];
+    is_branch = false;
+    ref = r.x;
+    count = r.y - r.x + 1;
+  }
+}
+
+template <int KIND>
+__global__ void emit_node2_kernel(const uint32_t *__restrict__ codes,
+                                  const uint32_t *__restrict__ kchild,
+                                  const uint8_t *__restrict__ kflags,
+                                  const uint2 *__restrict__ krange,
+                                  const uint32_t *__restrict__ flag,
+                                  const uint32_t *__restrict__ slot,
+                                  const Box *__restrict__ ibox,
+                                  const float4 *__restrict__ prims,
+                                  const SceneInfo *__restrict__ scene, int n,
+                                  Node2 *__restrict__ nodes, uint32_t *__restrict__ err) {
+  const float keps = scene->keps;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+       i += gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    uint32_t g = kchild[i];
+    uint8_t fl = kflags[i];
+    Box b0, b1;
+    bool br0, br1;
+    uint32_t r0, r1, c0, c1;
+    child_info<KIND>(g, fl & 1, krange, flag, slot, ibox, prims, keps, b0, br0, r0, c0);
+    child_info<KIND>(g + 1, fl & 2, krange, flag, slot, ibox, prims, keps, b1, br1, r1, c1);
+    if (c0 > kCountMask || c1 > kCountMask) atomicOr(err, kErrTree);
+    uint32_t axis = (uint32_t)split_axis(codes[i]);
+    Node2 nd;
+    nd.a = make_float4(b0.lo[0], b0.lo[1], b0.lo[2], b0.hi[0]);
+    nd.b = make_float4(b0.hi[1], b0.hi[2], b1.lo[0], b1.lo[1]);
+    nd.c = make_float4(b1.lo[2], b1.hi[0], b1.hi[1], b1.hi[2]);
+    nd.d = make_uint4(r0, r1, (c0 & kCountMask) | (axis << 30), c1 & kCountMask);
+    nodes[slot[i]] = nd;
+  }
+}
+
+__device__ __forceinline__ NodeT make_tet_node(const Box &b, uint32_t meta, uint32_t ref) {
+  NodeT t;
+  t.a = make_float4(b.lo[0], b.lo[1], b.lo[2], __uint_as_float(meta));
+  t.b = make_float4(b.hi[0], b.hi[1], b.hi[2], __uint_as_float(ref));
+  return t;
+}
+
+__global__ void emit_tet_kernel(const uint32_t *__restrict__ codes,
+                                const uint32_t *__restrict__ kchild,
+                                const uint8_t *__restrict__ kflags,
+                                const uint2 *__restrict__ krange,
+                                const uint32_t *__restrict__ flag,
+                                const uint32_t *__restrict__ slot,
+                                const Box *__restrict__ ibox,
+                                const float4 *__restrict__ prims,
+                                const SceneInfo *__restrict__ scene, int n,
+                                NodeT *__restrict__ nodes, uint32_t *__restrict__ err) {
+  const float keps = scene->keps;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
+       i += gridDim.x * blockDim.x) {
+    if (!flag[i]) continue;
+    uint32_t s = slot[i];
+    if (i == 0) nodes[0] = make_tet_node(ibox[0], (uint32_t)split_axis(codes[0]), 1u);
+    uint32_t g = kchild[i];
+    uint8_t fl = kflags[i];
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+      uint32_t c = g + side;
+      Box b;
+      bool br;
+      uint32_t ref, cnt;
+      child_info<SRT_TETRAHEDRA>(c, fl & (1 << side), krange, flag, slot, ibox, prims,
+                                 keps, b, br, ref, cnt);
+      uint32_t meta, r;
+      if (br) {
+        meta = (uint32_t)split_axis(codes[c]);
+        r = 1u + 2u * ref;
+      } else {
+        if (cnt > kCountMask) atomicOr(err, kErrTree);
+        meta = kLeafBit | cnt;
+        r = ref;
+      }
+      nodes[1 + 2 * (size_t)s + side] = make_tet_node(b, meta, r);
+    }
+  }
+}
+
+__global__ void finish_kernel(const uint32_t *__restrict__ flag,
+                              const uint32_t *__restrict__ slot, int n,
+                              SceneInfo *__restrict__ scene) {
+  scene->nbranches = slot[n - 2] + flag[n - 2];
+}
+
+template <int KIND>
+srt_status launch_bbox_morton(srt_ctx *ctx, const float *v, const uint32_t *f,
+                              const float *radius, float constr, size_t n,
+                              SceneInfo *scene, uint32_t *codes, uint32_t *index) {
+  cudaStream_t st = ctx->stream;
+  int gb = grid_for(n, kBlock, ctx->num_sms * 4);
+  cudaError_t e = ctx->s_partial.ensure((size_t)gb * sizeof(Box));
+  if (e != cudaSuccess) return cuda_status(e, "bbox scratch");
+  Box *partial = ctx->s_partial.as<Box>();
+  bbox_partial_kernel<KIND><<<gb, kBlock, 0, st>>>(v, f, radius, constr, n, partial);
+  ctx->launches++;
+  bbox_final_kernel<KIND><<<1, 32, 0, st>>>(partial, gb, scene);
+  ctx->launches++;
+  int gm = grid_for(n, kBlock, ctx->num_sms * 16);
+  morton_kernel<KIND><<<gm, kBlock, 0, st>>>(v, f, n, scene, codes, index);
+  ctx->launches++;
+  return cuda_status(cudaGetLastError(), "bbox/morton");
+}
+
+template <int KIND>
+srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
+                      const float *radius, float constr, size_t n) {
+  srt_ctx *ctx = a->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const int in = (int)n;
+  const size_t m = n - 1;  // internal nodes
+#define ENSURE(buf, bytes)                                   \
+  do {                                                       \
+    if ((e = (buf).ensure(bytes)) != cudaSuccess)            \
+      return cuda_status(e, "build allocation " #buf);       \
+  } while (0)
+  ENSURE(a->codes, n * 4);
+  ENSURE(a->indices, n * 4);
+  ENSURE(a->prims, n * sizeof(float4) * PrimTraits<KIND>::kCacheF4);
+  ENSURE(a->scene, sizeof(SceneInfo));
+  size_t max_nodes = (KIND == SRT_TETRAHEDRA) ? (2 * m + 1) : m;
+  ENSURE(a->nodes, max_nodes * (KIND == SRT_TETRAHEDRA ? sizeof(NodeT) : sizeof(Node2)));
+  ENSURE(ctx->s_kchild, m * 4);
+  ENSURE(ctx->s_kflags, m);
+  ENSURE(ctx->s_krange, m * sizeof(uint2));
+  ENSURE(ctx->s_kparent, m * 4);
+  ENSURE(ctx->s_lparent, n * 4);
+  ENSURE(ctx->s_counter, m * 4);
+  ENSURE(ctx->s_ibox, m * sizeof(Box));
+  ENSURE(ctx->s_flag, m * 4);
+  ENSURE(ctx->s_slot, m * 4);
+#undef ENSURE
+  SceneInfo *scene = a->scene.as<SceneInfo>();
+  uint32_t *codes = a->codes.as<uint32_t>();
+  uint32_t *idx = a->indices.as<uint32_t>();
+  srt_status s = launch_bbox_morton<KIND>(ctx, v, f, radius, constr, n, scene, codes, nullptr);
+  if (s != SRT_OK) return s;
+  s = sort_pairs(ctx, codes, idx, n, true);
+  if (s != SRT_OK) return s;
+  uint32_t *kchild = ctx->s_kchild.as<uint32_t>();
+  uint8_t *kflags = ctx->s_kflags.as<uint8_t>();
+  uint2 *krange = ctx->s_krange.as<uint2>();
+  uint32_t *kparent = ctx->s_kparent.as<uint32_t>();
+  uint32_t *lparent = ctx->s_lparent.as<uint32_t>();
+  uint32_t *counter = ctx->s_counter.as<uint32_t>();
+  Box *ibox = ctx->s_ibox.as<Box>();
+  uint32_t *flag = ctx->s_flag.as<uint32_t>();
+  uint32_t *slot = ctx->s_slot.as<uint32_t>();
+  int gk = grid_for(m, kBlock, ctx->num_sms * 16);
+  karras_kernel<<<gk, kBlock, 0, st>>>(codes, in, kchild, kflags, krange, kparent, lparent);
+  ctx->launches++;
+  if ((e = cudaMemsetAsync(counter, 0, m * 4, st)) != cudaSuccess)
+    return cuda_status(e, "refit counters");
+  refit_kernel<KIND><<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+      v, f, radius, constr, idx, in, scene, lparent, kparent, kchild, kflags, counter,
+      ibox, a->prims.as<float4>(), ctx->d_err);
+  ctx->launches++;
+  level_kernel<<<gk, kBlock, 0, st>>>(krange, kparent, in, PrimTraits<KIND>::kMaxLeaf,
+                                      flag);
+  ctx->launches++;
+  s = cuda_status(cudaGetLastError(), "karras/refit/level");
+  if (s != SRT_OK) return s;
+  s = exclusive_scan(ctx, flag, slot, m);
+  if (s != SRT_OK) return s;
+  if (KIND == SRT_TETRAHEDRA) {
+    emit_tet_kernel<<<gk, kBlock, 0, st>>>(codes, kchild, kflags, krange, flag, slot, ibox,
+                                           a->prims.as<float4>(), scene, in,
+                                           a->nodes.as<NodeT>(), ctx->d_err);
+    ctx->launches++;
+  } else {
+    emit_node2_kernel<KIND><<<gk, kBlock, 0, st>>>(codes, kchild, kflags, krange, flag,
+                                                   slot, ibox, a->prims.as<float4>(),
+                                                   scene, in, a->nodes.as<Node2>(),
+                                                   ctx->d_err);
+    ctx->launches++;
+  }
+  finish_kernel<<<1, 1, 0, st>>>(flag, slot, in, scene);
+  ctx->launches++;
+  return cuda_status(cudaGetLastError(), "emit");
+}
+
+}  // namespace
+
+srt_status build_accel(srt_accel *a, const float *v, const uint32_t *f,
+                       const float *radius, float constr, size_t n) {
+  a->host_scene_valid = false;
+  switch (a->kind) {
+    case SRT_TRIANGLES:
+      return build_kind<SRT_TRIANGLES>(a, v, f, radius, constr, n);
+    case SRT_TETRAHEDRA:
+      return build_kind<SRT_TETRAHEDRA>(a, v, f, radius, constr, n);
+    case SRT_SPHERES:
+      return build_kind<SRT_SPHERES>(a, v, f, radius, constr, n);
+  }
+  return SRT_ERR_INVALID;
+}
+
+srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *v, const uint32_t *f,
+                        const float *radius, float constr, size_t n, uint32_t *codes,
+                        SceneInfo *scene) {
+  switch (kind) {
+    case SRT_TRIANGLES:
+      return launch_bbox_morton<SRT_TRIANGLES>(ctx, v, f, radius, constr, n, scene, codes,
+                                               nullptr);
+    case SRT_TETRAHEDRA:
+      return launch_bbox_morton<SRT_TETRAHEDRA>(ctx, v, f, radius, constr, n, scene, codes,
+                                                nullptr);
+    case SRT_SPHERES:
+      return launch_bbox_morton<SRT_SPHERES>(ctx, v, f, radius, constr, n, scene, codes,
+                                             nullptr);
+  }
+  return SRT_ERR_INVALID;
+}
+
+srt_status stage_karras(srt_ctx *ctx, const uint32_t *codes, size_t n, uint32_t *child,
+                        uint8_t *flags) {
+  int gk = grid_for(n - 1, kBlock, ctx->num_sms * 16);
+  karras_kernel<<<gk, kBlock, 0, ctx->stream>>>(codes, (int)n, child, flags, nullptr,
+                                                nullptr, nullptr);
+  ctx->launches++;
+  return cuda_status(cudaGetLastError(), "karras");
+}
+
+}  // namespace srt

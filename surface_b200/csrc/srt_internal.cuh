@@ -1,0 +1,167 @@
+// srt_internal.cuh -- shared device/host internals of libsurface_rt.
+//
+// Floating point: the whole library is compiled with --fmad=false and without
+// fast-math, so every float/double expression rounds exactly like the
+// reference's x86-64 g++ build (SSE2, no contraction).  Division and sqrt are
+// IEEE round-to-nearest.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <float.h>
+#include <stdint.h>
+
+#include <string>
+
+#include "surface_rt.h"
+
+namespace srt {
+
+// ---------------------------------------------------------------- limits
+constexpr int kMaxLevel = 23;        // reference depth > 22 forces a leaf;
+                                     // root = level 0, its children level 1
+constexpr int kStack = 64;           // traversal stack (tree depth <= 24)
+constexpr uint32_t kCountMask = 0x3fffffffu;
+constexpr uint32_t kLeafBit = 0x80000000u;
+constexpr uint32_t kNone = 0xffffffffu;
+
+// device error word bits (set by kernels, reported by srt_ctx_synchronize)
+constexpr uint32_t kErrStack = 1u;
+constexpr uint32_t kErrIter = 2u;
+constexpr uint32_t kErrTree = 4u;
+
+// ---------------------------------------------------------------- layouts
+// Two-child node (triangles, spheres): 64 bytes, the reference's
+// TriangleNode/ParticleNode information with leaves folded into the parent:
+//   a = (c0.lo.x, c0.lo.y, c0.lo.z, c0.hi.x)
+//   b = (c0.hi.y, c0.hi.z, c1.lo.x, c1.lo.y)
+//   c = (c1.lo.z, c1.hi.x, c1.hi.y, c1.hi.z)
+//   d = (ref0, ref1, meta0, meta1)
+// meta_k & kCountMask = leaf primitive count of child k (0: child k is a
+// branch and ref_k its node index; else ref_k = first sorted primitive);
+// meta0 >> 30 = this node's split axis.
+struct __align__(16) Node2 {
+  float4 a, b, c;
+  uint4 d;
+};
+
+// Own-box node (tetrahedra): 32 bytes, the reference's TetraNode.
+//   a = (lo.x, lo.y, lo.z, meta)  meta: leaf -> kLeafBit | count, branch -> axis
+//   b = (hi.x, hi.y, hi.z, ref)   ref:  leaf -> first sorted primitive,
+//                                       branch -> left child (right = ref + 1)
+struct __align__(16) NodeT {
+  float4 a, b;
+};
+
+// Scene box and derived build constants (one per build, device resident).
+struct SceneInfo {
+  float lo[3], hi[3];
+  float inv[3];      // 1024 / (hi - lo)
+  float keps;        // leaf box padding
+  double eps_scale;  // triangles: max scene extent
+  uint32_t nbranches;
+  uint32_t pad;
+};
+
+struct Box {
+  float lo[3], hi[3];
+};
+
+// ---------------------------------------------------------------- device math
+// std::min / std::max with the reference's tie behaviour (first operand kept).
+__device__ __forceinline__ float fmin_ref(float a, float b) { return (b < a) ? b : a; }
+__device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b : a; }
+
+// (uint32_t)x as g++ emits it on x86-64: a 64-bit truncating convert whose low
+// 32 bits are kept; NaN and |x| >= 2^63 give 0.
+__device__ __forceinline__ uint32_t f2u32_x86(float x) {
+  if (!(fabsf(x) < 9.2233720368547758e18f)) return 0u;
+  return (uint32_t)(long long)x;
+}
+
+__device__ __forceinline__ uint32_t spread10(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+
+__device__ __forceinline__ int split_axis(uint32_t code) {
+  return (__clz(code) - 2) % 3;  // __clz(0) = 32
+}
+
+// ---------------------------------------------------------------- host side
+struct DevBuf {
+  void *p = nullptr;
+  size_t cap = 0;
+  DevBuf() = default;
+  DevBuf(const DevBuf &) = delete;
+  DevBuf &operator=(const DevBuf &) = delete;
+  ~DevBuf() { release(); }
+  cudaError_t ensure(size_t bytes);
+  void release();
+  template <typename T>
+  T *as() const {
+    return static_cast<T *>(p);
+  }
+};
+
+}  // namespace srt
+
+struct srt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaStream_t own_stream = nullptr;
+  uint32_t *d_err = nullptr;  // device error word
+  uint32_t *h_err = nullptr;  // pinned mirror
+  int num_sms = 148;
+  uint64_t launches = 0;  // kernels launched by this context
+  // scratch shared by the builds of this context (stream ordered)
+  srt::DevBuf s_keys2, s_vals2, s_hist, s_scan, s_kchild, s_kflags, s_krange,
+      s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
+      s_stage_in, s_stage_out, s_stage_aux;
+};
+
+struct srt_accel {
+  srt_ctx *ctx = nullptr;
+  srt_kind kind = SRT_TRIANGLES;
+  size_t n = 0;
+  size_t nnodes_cap = 0;
+  bool built = false;
+  srt::DevBuf nodes, indices, codes, prims, scene;
+  srt::DevBuf in_verts, in_faces, in_radius;  // device copies of host inputs
+  // primitive arrays the tree was built from (owned copies of host inputs,
+  // or the caller's device arrays, borrowed like the reference's mesh_)
+  const float *src_verts = nullptr;
+  const uint32_t *src_faces = nullptr;
+  // host-side cache of the device SceneInfo (valid after a sync)
+  srt::SceneInfo host_scene;
+  bool host_scene_valid = false;
+};
+
+namespace srt {
+void set_error(const std::string &msg);
+srt_status cuda_status(cudaError_t e, const char *what);
+// pointer classification
+bool is_device_ptr(const void *p);
+
+// build pipeline pieces (srt_build.cu)
+srt_status build_accel(srt_accel *a, const float *d_verts, const uint32_t *d_faces,
+                       const float *d_radius, float const_radius, size_t n);
+srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *d_verts,
+                        const uint32_t *d_faces, const float *d_radius,
+                        float const_radius, size_t n, uint32_t *d_codes,
+                        SceneInfo *d_scene);
+srt_status sort_pairs(srt_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals,
+                      size_t n, bool identity_vals);
+srt_status stage_karras(srt_ctx *ctx, const uint32_t *d_codes, size_t n,
+                        uint32_t *d_child, uint8_t *d_flags);
+
+// traversal (srt_trace.cu)
+srt_status launch_trace(srt_accel *a, const srt_ray *d_rays, size_t n,
+                        srt_hit *d_hits, const float *d_prev_normals,
+                        uint32_t *d_subface, const float *d_vertex_scalar,
+                        float *d_scalar_out, float *d_normal_out,
+                        unsigned long long *d_stats);
+}  // namespace srt

@@ -1,0 +1,412 @@
+// srt_volume.cu -- emission-absorption volume march and its adjoint.
+//
+// Geometry follows the reference shader (examples/nonuniform_volume_render/
+// input.frag): build_cameraframe with pi written as 3.14 (:16-29), a ray
+// through each fragment centre (:101-108), the IntersectP slab test against
+// [-1,1]^3 with +-10000 initial bounds (:59-97), the half-open inside() test
+// (:50-57) and texture3D(tex0, 0.5*p + 0.5) fetched with FilterTexture3DFloat's
+// texel-corner trilinear weights (render/render_texture.cc:946-1058, vox =
+// u*(dim-1)).  Compositing is front-to-back emission-absorption, samples at
+// t0 + (s + 1/2) * step for s < floor((t1 - t0) / step):
+//   rgba = lerp of the transfer function at rho*(entries-1)
+//   alpha = min(1 - exp(-sigma_scale * rgba.a * step), alpha_max)
+//   C += T * alpha * rgba.rgb;  T *= 1 - alpha;  output (C, 1 - T)
+// The adjoint walks the samples in reverse and rebuilds transmittance as
+// T_k = T_{k+1} / (1 - alpha_k) from the stored final T (no per-sample
+// state); alpha_max < 1 keeps the division bounded.
+#include <cmath>
+#include <cstring>
+
+#include "srt_internal.cuh"
+
+namespace srt {
+namespace {
+
+struct VolConst {
+  srt_volume_params p;
+  int dim[3];
+  int tfn;
+};
+
+struct Sample {
+  int cx[8];
+  float w[8];
+  float rho;
+};
+
+__device__ __forceinline__ float lerpf(float t, float a, float b) {
+  return (1.f - t) * a + t * b;
+}
+
+__device__ __forceinline__ void pixel_ray(const srt_volume_params &P, int px, int py,
+                                          float o[3], float d[3]) {
+  const float fx = (float)px + 0.5f, fy = (float)py + 0.5f;
+  float v[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) v[k] = (P.corner[k] + fx * P.du[k] + fy * P.dv[k]) - P.eye[k];
+  const float l = sqrtf(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    d[k] = v[k] / l;
+    o[k] = P.eye[k];
+  }
+}
+
+__device__ __forceinline__ bool slab(const float o[3], const float d[3], float &t0,
+                                     float &t1) {
+  t0 = -10000.0f;
+  t1 = 10000.0f;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    float tn = (-1.0f - o[k]) / d[k];
+    float tf = (1.0f - o[k]) / d[k];
+    if (tn > tf) {
+      float x = tn;
+      tn = tf;
+      tf = x;
+    }
+    t0 = tn > t0 ? tn : t0;
+    t1 = tf < t1 ? tf : t1;
+  }
+  return t0 <= t1;
+}
+
+__device__ __forceinline__ bool inside(const float p[3]) {
+  return p[0] >= -1.0f && p[0] < 1.0f && p[1] >= -1.0f && p[1] < 1.0f && p[2] >= -1.0f &&
+         p[2] < 1.0f;
+}
+
+// FilterTexture3DFloat, clamp-to-edge, one component.
+__device__ __forceinline__ float fetch(const float *__restrict__ img, const int dim[3],
+                                       float u, float v, float r, Sample *smp) {
+  const float vox0 = u * (dim[0] - 1.0f);
+  const float vox1 = v * (dim[1] - 1.0f);
+  const float vox2 = r * (dim[2] - 1.0f);
+  int vx = min(max((int)vox0, 0), dim[0] - 1);
+  int vy = min(max((int)vox1, 0), dim[1] - 1);
+  int vz = min(max((int)vox2, 0), dim[2] - 1);
+  const int vx1 = min(vx + 1, dim[0] - 1), vy1 = min(vy + 1, dim[1] - 1),
+            vz1 = min(vz + 1, dim[2] - 1);
+  const float dx = vox0 - vx, dy = vox1 - vy, dz = vox2 - vz;
+  const size_t sx = 1, sy = (size_t)dim[0], sz = (size_t)dim[0] * dim[1];
+  const size_t i000 = vz * sz + vy * sy + vx * sx;
+  const float D000 = __ldg(&img[i000]);
+  const float D100 = __ldg(&img[vz * sz + vy * sy + vx1]);
+  const float D010 = __ldg(&img[vz * sz + vy1 * sy + vx]);
+  const float D110 = __ldg(&img[vz * sz + vy1 * sy + vx1]);
+  const float D001 = __ldg(&img[vz1 * sz + vy * sy + vx]);
+  const float D101 = __ldg(&img[vz1 * sz + vy * sy + vx1]);
+  const float D011 = __ldg(&img[vz1 * sz + vy1 * sy + vx]);
+  const float D111 = __ldg(&img[vz1 * sz + vy1 * sy + vx1]);
+  const float d00 = lerpf(dx, D000, D100);
+  const float d10 = lerpf(dx, D010, D110);
+  const float d01 = lerpf(dx, D001, D101);
+  const float d11 = lerpf(dx, D011, D111);
+  const float d0 = lerpf(dy, d00, d10);
+  const float d1 = lerpf(dy, d01, d11);
+  const float val = lerpf(dz, d0, d1);
+  if (smp) {
+    const int xs[2] = {vx, vx1}, ys[2] = {vy, vy1}, zs[2] = {vz, vz1};
+#pragma unroll
+    for (int c = 0; c < 8; c++) {
+      smp->cx[c] = (int)(zs[c >> 2] * sz + ys[(c >> 1) & 1] * sy + xs[c & 1]);
+      smp->w[c] = ((c & 1) ? dx : 1.0f - dx) * (((c >> 1) & 1) ? dy : 1.0f - dy) *
+                  ((c >> 2) ? dz : 1.0f - dz);
+    }
+    smp->rho = val;
+  }
+  return val;
+}
+
+// Transfer-function lookup: returns rgba, sets i0/i1/f and whether rho was
+// inside the table's range (clamped samples have no density gradient).
+__device__ __forceinline__ void tf_lookup(const float4 *__restrict__ tf, int tfn,
+                                          float rho, float4 &c, int &i0, int &i1,
+                                          float &f, bool &inrange) {
+  const float top = (float)(tfn - 1);
+  float x = rho * top;
+  inrange = (x > 0.0f) && (x < top);
+  x = x < 0.0f ? 0.0f : (x > top ? top : x);
+  i0 = (int)x;
+  i1 = min(i0 + 1, tfn - 1);
+  f = x - (float)i0;
+  const float4 a = __ldg(&tf[i0]), b = __ldg(&tf[i1]);
+  c = make_float4(lerpf(f, a.x, b.x), lerpf(f, a.y, b.y), lerpf(f, a.z, b.z),
+                  lerpf(f, a.w, b.w));
+}
+
+__global__ void __launch_bounds__(128)
+vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
+               const float4 *__restrict__ tf, float4 *__restrict__ image,
+               float *__restrict__ trans) {
+  const int W = K.p.width, H = K.p.height;
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix >= W * H) return;
+  const int px = pix % W, py = pix / W;
+  float o[3], d[3], t0, t1;
+  pixel_ray(K.p, px, py, o, d);
+  float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.0f;
+  if (slab(o, d, t0, t1)) {
+    int ns = (int)((t1 - t0) / K.p.step);
+    if (ns > K.p.max_steps) ns = K.p.max_steps;
+    for (int s = 0; s < ns; s++) {
+      const float t = t0 + ((float)s + 0.5f) * K.p.step;
+      const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+      if (!inside(p)) continue;
+      const float rho = fetch(dens, K.dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
+                              0.5f * p[2] + 0.5f, nullptr);
+      float4 c;
+      int i0, i1;
+      float f;
+      bool inr;
+      tf_lookup(tf, K.tfn, rho, c, i0, i1, f, inr);
+      const float sig = K.p.sigma_scale * c.w;
+      float al = 1.0f - expf(-sig * K.p.step);
+      if (al > K.p.alpha_max) al = K.p.alpha_max;
+      const float w = T * al;
+      C0 += w * c.x;
+      C1 += w * c.y;
+      C2 += w * c.z;
+      T = T * (1.0f - al);
+    }
+  }
+  image[pix] = make_float4(C0, C1, C2, 1.0f - T);
+  if (trans) trans[pix] = T;
+}
+
+constexpr int kTfMax = 4096;
+
+__global__ void __launch_bounds__(128)
+vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
+               const float4 *__restrict__ tf, const float *__restrict__ trans,
+               const float4 *__restrict__ gimg, float *__restrict__ gdens,
+               float *__restrict__ gtf) {
+  extern __shared__ float s_gtf[];  // 4 * tfn block-local TF gradient
+  for (int i = threadIdx.x; i < 4 * K.tfn; i += blockDim.x) s_gtf[i] = 0.0f;
+  __syncthreads();
+  const int W = K.p.width, H = K.p.height;
+  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
+  if (pix < W * H) {
+    const int px = pix % W, py = pix / W;
+    float o[3], d[3], t0, t1;
+    pixel_ray(K.p, px, py, o, d);
+    if (slab(o, d, t0, t1)) {
+      int ns = (int)((t1 - t0) / K.p.step);
+      if (ns > K.p.max_steps) ns = K.p.max_steps;
+      const float4 g = gimg[pix];
+      const float Tfin = trans[pix];
+      float Tn = Tfin;
+      float Cb0 = 0.f, Cb1 = 0.f, Cb2 = 0.f;
+      const float top = (float)(K.tfn - 1);
+      for (int s = ns - 1; s >= 0; s--) {
+        const float t = t0 + ((float)s + 0.5f) * K.p.step;
+        const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+        if (!inside(p)) continue;
+        Sample smp;
+        const float rho = fetch(dens, K.dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
+                                0.5f * p[2] + 0.5f, &smp);
+        float4 c;
+        int i0, i1;
+        float f;
+        bool inr;
+        tf_lookup(tf, K.tfn, rho, c, i0, i1, f, inr);
+        const float sig = K.p.sigma_scale * c.w;
+        const float e = expf(-sig * K.p.step);
+        float al = 1.0f - e;
+        const bool clamped = al > K.p.alpha_max;
+        if (clamped) al = K.p.alpha_max;
+        const float om = 1.0f - al;
+        const float Tk = Tn / om;
+        const float gc0 = g.x * Tk * al, gc1 = g.y * Tk * al, gc2 = g.z * Tk * al;
+        float ga = g.x * (Tk * c.x - Cb0 / om) + g.y * (Tk * c.y - Cb1 / om) +
+                   g.z * (Tk * c.z - Cb2 / om) + g.w * (Tfin / om);
+        const float gc3 = clamped ? 0.0f : ga * K.p.sigma_scale * K.p.step * e;
+        // transfer-function gradient (block-local)
+        const float wf0 = 1.0f - f, wf1 = f;
+        atomicAdd(&s_gtf[4 * i0 + 0], wf0 * gc0);
+        atomicAdd(&s_gtf[4 * i0 + 1], wf0 * gc1);
+        atomicAdd(&s_gtf[4 * i0 + 2], wf0 * gc2);
+        atomicAdd(&s_gtf[4 * i0 + 3], wf0 * gc3);
+        atomicAdd(&s_gtf[4 * i1 + 0], wf1 * gc0);
+        atomicAdd(&s_gtf[4 * i1 + 1], wf1 * gc1);
+        atomicAdd(&s_gtf[4 * i1 + 2], wf1 * gc2);
+        atomicAdd(&s_gtf[4 * i1 + 3], wf1 * gc3);
+        if (inr) {
+          const float4 a = __ldg(&tf[i0]), b = __ldg(&tf[i1]);
+          const float drho = (gc0 * (b.x - a.x) + gc1 * (b.y - a.y) + gc2 * (b.z - a.z) +
+                              gc3 * (b.w - a.w)) * top;
+#pragma unroll
+          for (int cc = 0; cc < 8; cc++) atomicAdd(&gdens[smp.cx[cc]], smp.w[cc] * drho);
+        }
+        Cb0 += Tk * al * c.x;
+        Cb1 += Tk * al * c.y;
+        Cb2 += Tk * al * c.z;
+        Tn = Tk;
+      }
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 4 * K.tfn; i += blockDim.x) {
+    const float v = s_gtf[i];
+    if (v != 0.0f) atomicAdd(&gtf[i], v);
+  }
+}
+
+srt_status make_const(const srt_volume_params *params, const int32_t dims[3],
+                      int32_t tfn, VolConst &K) {
+  if (!params || !dims || params->width <= 0 || params->height <= 0 || tfn < 2 ||
+      tfn > kTfMax || dims[0] < 1 || dims[1] < 1 || dims[2] < 1 ||
+      !(params->alpha_max < 1.0f) || params->step <= 0.0f || params->max_steps < 0) {
+    set_error("invalid volume parameters");
+    return SRT_ERR_INVALID;
+  }
+  if ((double)dims[0] * dims[1] * dims[2] >= 2147483647.0) {
+    set_error("volume larger than 2^31 voxels");
+    return SRT_ERR_INVALID;
+  }
+  K.p = *params;
+  for (int k = 0; k < 3; k++) K.dim[k] = dims[k];
+  K.tfn = tfn;
+  return SRT_OK;
+}
+
+}  // namespace
+
+// device view helper shared with the C API (declared here to keep the
+// volume entry points self-contained)
+static srt_status vol_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
+                           const void **out, cudaStream_t st) {
+  if (!p) {
+    *out = nullptr;
+    return SRT_OK;
+  }
+  if (is_device_ptr(p)) {
+    *out = p;
+    return SRT_OK;
+  }
+  cudaError_t e = stage.ensure(bytes);
+  if (e != cudaSuccess) return cuda_status(e, "volume staging");
+  e = cudaMemcpyAsync(stage.p, p, bytes, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_status(e, "volume copy");
+  *out = stage.p;
+  return SRT_OK;
+}
+
+}  // namespace srt
+
+using namespace srt;
+
+extern "C" {
+
+SRT_API srt_status srt_volume_camera(int32_t W, int32_t H, const float eye[3],
+                                     const float lookat[3], const float up[3],
+                                     float fov_deg, srt_volume_params *P) {
+  if (!eye || !lookat || !up || !P || W <= 0 || H <= 0) return SRT_ERR_INVALID;
+  // build_cameraframe, FP32 (same expression order as the oracle)
+  float look[3], tmp[3], du[3], dv[3];
+  for (int k = 0; k < 3; k++) look[k] = lookat[k] - eye[k];
+  float ll = sqrtf(look[0] * look[0] + look[1] * look[1] + look[2] * look[2]);
+  for (int k = 0; k < 3; k++) look[k] = look[k] / ll;
+  tmp[0] = look[1] * up[2] - look[2] * up[1];
+  tmp[1] = look[2] * up[0] - look[0] * up[2];
+  tmp[2] = look[0] * up[1] - look[1] * up[0];
+  float lu = sqrtf(tmp[0] * tmp[0] + tmp[1] * tmp[1] + tmp[2] * tmp[2]);
+  for (int k = 0; k < 3; k++) du[k] = tmp[k] / lu;
+  tmp[0] = look[1] * du[2] - look[2] * du[1];
+  tmp[1] = look[2] * du[0] - look[0] * du[2];
+  tmp[2] = look[0] * du[1] - look[1] * du[0];
+  float lv = sqrtf(tmp[0] * tmp[0] + tmp[1] * tmp[1] + tmp[2] * tmp[2]);
+  for (int k = 0; k < 3; k++) dv[k] = tmp[k] / lv;
+  float flen = 0.5f * (float)H / (float)tan(0.5 * ((double)fov_deg * 3.14 / 180.0));
+  P->width = W;
+  P->height = H;
+  for (int k = 0; k < 3; k++) {
+    float lk = flen * look[k] + eye[k];
+    P->corner[k] = lk - 0.5f * ((float)W * du[k] + (float)H * dv[k]);
+    P->eye[k] = eye[k];
+    P->du[k] = du[k];
+    P->dv[k] = dv[k];
+  }
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_volume_march_fwd(srt_ctx *ctx, const srt_volume_params *params,
+                                        const float *density, const int32_t dims[3],
+                                        const float *tf, int32_t tf_entries, float *image,
+                                        float *transmittance) {
+  if (!ctx || !density || !tf || !image) return SRT_ERR_INVALID;
+  VolConst K;
+  srt_status s = make_const(params, dims, tf_entries, K);
+  if (s != SRT_OK) return s;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const size_t nvox = (size_t)dims[0] * dims[1] * dims[2];
+  const size_t npix = (size_t)params->width * params->height;
+  const void *dd, *dt;
+  if ((s = vol_view(ctx, density, nvox * 4, ctx->s_stage_in, &dd, st)) != SRT_OK) return s;
+  if ((s = vol_view(ctx, tf, (size_t)tf_entries * 16, ctx->s_stage_aux, &dt, st)) != SRT_OK)
+    return s;
+  const bool img_dev = is_device_ptr(image);
+  const bool tr_dev = transmittance ? is_device_ptr(transmittance) : true;
+  float *di = image, *dtr = transmittance;
+  DevBuf tmp_tr;
+  cudaError_t e;
+  if (!img_dev) {
+    if ((e = ctx->s_stage_out.ensure(npix * 16)) != cudaSuccess) return cuda_status(e, "img");
+    di = ctx->s_stage_out.as<float>();
+  }
+  if (!tr_dev) {
+    if ((e = tmp_tr.ensure(npix * 4)) != cudaSuccess) return cuda_status(e, "trans");
+    dtr = tmp_tr.as<float>();
+  }
+  vol_fwd_kernel<<<(unsigned)((npix + 127) / 128), 128, 0, st>>>(
+      K, static_cast<const float *>(dd), static_cast<const float4 *>(dt),
+      reinterpret_cast<float4 *>(di), dtr);
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "volume fwd");
+  if (!img_dev) cudaMemcpyAsync(image, di, npix * 16, cudaMemcpyDeviceToHost, st);
+  if (!tr_dev) cudaMemcpyAsync(transmittance, dtr, npix * 4, cudaMemcpyDeviceToHost, st);
+  if (!img_dev || !tr_dev) return cuda_status(cudaStreamSynchronize(st), "volume fwd");
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx, const srt_volume_params *params,
+                                        const float *density, const int32_t dims[3],
+                                        const float *tf, int32_t tf_entries,
+                                        const float *image, const float *transmittance,
+                                        const float *grad_image, float *grad_density,
+                                        float *grad_tf) {
+  (void)image;  // the colour behind each sample is accumulated during the walk
+  if (!ctx || !density || !tf || !transmittance || !grad_image || !grad_density || !grad_tf)
+    return SRT_ERR_INVALID;
+  VolConst K;
+  srt_status s = make_const(params, dims, tf_entries, K);
+  if (s != SRT_OK) return s;
+  cudaSetDevice(ctx->device);
+  cudaStream_t st = ctx->stream;
+  const size_t nvox = (size_t)dims[0] * dims[1] * dims[2];
+  const size_t npix = (size_t)params->width * params->height;
+  if (!is_device_ptr(grad_density) || !is_device_ptr(grad_tf)) {
+    set_error("gradient outputs must be device memory");
+    return SRT_ERR_INVALID;
+  }
+  DevBuf s_tr, s_g;
+  const void *dd, *dt, *dtr, *dg;
+  if ((s = vol_view(ctx, density, nvox * 4, ctx->s_stage_in, &dd, st)) != SRT_OK) return s;
+  if ((s = vol_view(ctx, tf, (size_t)tf_entries * 16, ctx->s_stage_aux, &dt, st)) != SRT_OK)
+    return s;
+  if ((s = vol_view(ctx, transmittance, npix * 4, s_tr, &dtr, st)) != SRT_OK) return s;
+  if ((s = vol_view(ctx, grad_image, npix * 16, s_g, &dg, st)) != SRT_OK) return s;
+  size_t shmem = (size_t)tf_entries * 4 * sizeof(float);
+  vol_bwd_kernel<<<(unsigned)((npix + 127) / 128), 128, shmem, st>>>(
+      K, static_cast<const float *>(dd), static_cast<const float4 *>(dt),
+      static_cast<const float *>(dtr), static_cast<const float4 *>(dg), grad_density,
+      grad_tf);
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess) return cuda_status(e, "volume bwd");
+  if (s_tr.p || s_g.p) return cuda_status(cudaStreamSynchronize(st), "volume bwd");
+  return SRT_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,243 @@
+"""Seeded synthetic scenes and ray sets for the five workloads.
+
+Every generator is a pure function of its seed (numpy PCG64), so the CUDA path,
+the CPU oracle and the reference build see byte-identical inputs.  No dataset
+is named by the reference; these stand in for its scenes with the shapes and
+value distributions of the workloads:
+
+* ``displaced_octasphere`` -- triangle sphere: an octahedron subdivided k times
+  (8 * 4**k faces; k = 7 gives 131,072), projected to the unit sphere and
+  displaced radially by seeded value noise (amplitude 0.1).  ``nfaces``
+  truncates the face list (used by the batched workload).
+* ``tet_grid`` -- 64^3 cells in [0,1]^3, interior vertices jittered by
+  U(+-0.2 cell), five tetrahedra per cell in alternating orientation
+  (1,310,720 tets), plus a per-vertex scalar (sum of four Gaussians).
+* ``particles`` -- centres U[0,1)^3, radii log-normal (median 1e-3,
+  sigma 0.5), advected by a seeded smooth velocity field.
+* ``volume_blobs`` -- a density grid as a sum of anisotropic Gaussian blobs,
+  clamped to [0,1], plus an RGBA transfer-function table.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
+                      ("prev_t", "<f4")])
+MISS = 0xFFFFFFFF
+
+
+# ---------------------------------------------------------------- triangles
+def _value_noise(p, rng, lattice=8):
+    """Trilinear value noise on a random lattice over [-1.5,1.5]^3, in [-1,1]."""
+    g = rng.uniform(-1.0, 1.0, size=(lattice + 1,) * 3)
+    q = (np.clip(p, -1.5, 1.5) + 1.5) / 3.0 * lattice
+    i = np.minimum(np.floor(q).astype(np.int64), lattice - 1)
+    f = q - i
+    out = np.zeros(p.shape[0])
+    for dz in (0, 1):
+        for dy in (0, 1):
+            for dx in (0, 1):
+                w = ((f[:, 0] if dx else 1 - f[:, 0]) * (f[:, 1] if dy else 1 - f[:, 1])
+                     * (f[:, 2] if dz else 1 - f[:, 2]))
+                out += w * g[i[:, 0] + dx, i[:, 1] + dy, i[:, 2] + dz]
+    return out
+
+
+def octasphere(levels):
+    """Unit octasphere: (vertices float64 (V,3), faces uint32 (F,3)); the
+    children of face f are faces 4f..4f+3."""
+    v = np.array([[1, 0, 0], [-1, 0, 0], [0, 1, 0], [0, -1, 0], [0, 0, 1], [0, 0, -1]],
+                 np.float64)
+    f = np.array([[0, 2, 4], [2, 1, 4], [1, 3, 4], [3, 0, 4],
+                  [2, 0, 5], [1, 2, 5], [3, 1, 5], [0, 3, 5]], np.int64)
+    for _ in range(levels):
+        e = np.stack([f[:, [0, 1]], f[:, [1, 2]], f[:, [2, 0]]], 1).reshape(-1, 2)
+        key = np.minimum(e[:, 0], e[:, 1]) * (v.shape[0] + 1) + np.maximum(e[:, 0], e[:, 1])
+        uk, inv = np.unique(key, return_inverse=True)
+        a = uk // (v.shape[0] + 1)
+        b = uk % (v.shape[0] + 1)
+        mid = 0.5 * (v[a] + v[b])
+        mid /= np.linalg.norm(mid, axis=1, keepdims=True)
+        m = (inv.reshape(-1, 3) + v.shape[0])
+        v = np.concatenate([v, mid])
+        a0, a1, a2 = f[:, 0], f[:, 1], f[:, 2]
+        m01, m12, m20 = m[:, 0], m[:, 1], m[:, 2]
+        f = np.stack([np.stack([a0, m01, m20], 1), np.stack([m01, a1, m12], 1),
+                      np.stack([m20, m12, a2], 1), np.stack([m01, m12, m20], 1)],
+                     1).reshape(-1, 3)
+    return v, f.astype(np.uint32)
+
+
+def displaced_octasphere(levels=7, seed=123456, amplitude=0.1, nfaces=None):
+    """(vertices float32 (V,3), faces uint32 (F,3))."""
+    rng = np.random.default_rng(seed)
+    v, f = octasphere(levels)
+    r = 1.0 + amplitude * _value_noise(v, rng)
+    verts = (v * r[:, None]).astype(np.float32)
+    if nfaces is not None:
+        f = f[:nfaces]
+    return verts, np.ascontiguousarray(f)
+
+
+def octasphere_for_count(n, seed):
+    """Truncated displaced octasphere with exactly n faces."""
+    levels = 0
+    while 8 * 4 ** levels < n:
+        levels += 1
+    return displaced_octasphere(levels, seed=seed, nfaces=n)
+
+
+# ---------------------------------------------------------------- tetrahedra
+# corner c = x + 2y + 4z of a cube cell; five tets per cell in two parities
+_TETS_EVEN = [(0, 1, 2, 4), (3, 2, 1, 7), (5, 4, 7, 1), (6, 7, 4, 2), (1, 2, 4, 7)]
+_TETS_ODD = [(1, 0, 5, 3), (2, 3, 6, 0), (4, 5, 0, 6), (7, 6, 3, 5), (0, 3, 5, 6)]
+
+
+def tet_grid(cells=64, seed=123456, jitter=0.2, orient=-1):
+    """(vertices float32 (V,3), tets uint32 (N,4), scalar float32 (V,)).
+
+    Every tetrahedron is ordered so that det(v1-v0, v2-v0, v3-v0) has the sign
+    ``orient``; -1 is the orientation for which the reference's Pluecker test
+    (render/render_accel_tetra.cc:243-567) reports the entering face first."""
+    rng = np.random.default_rng(seed)
+    n1 = cells + 1
+    g = np.stack(np.meshgrid(np.arange(n1), np.arange(n1), np.arange(n1),
+                             indexing="ij"), -1).reshape(-1, 3)  # (x,y,z), x slowest
+    h = 1.0 / cells
+    p = g * h
+    interior = np.all((g > 0) & (g < cells), axis=1)
+    p[interior] += rng.uniform(-jitter * h, jitter * h, size=(interior.sum(), 3))
+    verts = p.astype(np.float32)
+
+    def vid(x, y, z):
+        return (x * n1 + y) * n1 + z
+
+    cx, cy, cz = np.meshgrid(np.arange(cells), np.arange(cells), np.arange(cells),
+                             indexing="ij")
+    cx, cy, cz = cx.ravel(), cy.ravel(), cz.ravel()
+    corner = np.stack([vid(cx + (c & 1), cy + ((c >> 1) & 1), cz + ((c >> 2) & 1))
+                       for c in range(8)], 1)
+    par = (cx + cy + cz) & 1
+    te = corner[:, np.array(_TETS_EVEN)]  # (cells^3, 5, 4)
+    to = corner[:, np.array(_TETS_ODD)]
+    tets = np.where(par[:, None, None] == 0, te, to).reshape(-1, 4).astype(np.int64)
+    v = verts.astype(np.float64)
+    d = np.linalg.det(np.stack([v[tets[:, 1]] - v[tets[:, 0]], v[tets[:, 2]] - v[tets[:, 0]],
+                                v[tets[:, 3]] - v[tets[:, 0]]], 1))
+    flip = np.sign(d) != orient
+    tets[flip, 1], tets[flip, 2] = tets[flip, 2].copy(), tets[flip, 1].copy()
+    # scalar field: sum of four seeded isotropic Gaussians
+    cen = rng.uniform(0.2, 0.8, size=(4, 3))
+    wid = rng.uniform(0.1, 0.3, size=4)
+    amp = rng.uniform(0.5, 1.0, size=4)
+    s = np.zeros(v.shape[0])
+    for k in range(4):
+        s += amp[k] * np.exp(-np.sum((v - cen[k]) ** 2, 1) / (2 * wid[k] ** 2))
+    return verts, tets.astype(np.uint32), s.astype(np.float32)
+
+
+# ---------------------------------------------------------------- particles
+def particles(n=16_777_216, seed=123456, median_radius=1e-3, sigma=0.5):
+    """(centres float32 (n,3), radii float32 (n,))."""
+    rng = np.random.default_rng(seed)
+    pos = rng.random((n, 3), dtype=np.float32)
+    rad = (median_radius * np.exp(sigma * rng.standard_normal(n))).astype(np.float32)
+    return pos, rad
+
+
+class VelocityField:
+    """Seeded smooth velocity field: a few random Fourier modes."""
+
+    def __init__(self, seed=7, modes=4, speed=2e-3):
+        rng = np.random.default_rng(seed)
+        self.k = rng.normal(0, 2.0 * np.pi, size=(modes, 3)).astype(np.float32)
+        self.ph = rng.uniform(0, 2 * np.pi, size=(modes, 3)).astype(np.float32)
+        self.a = (speed * rng.normal(size=(modes, 3)) / np.sqrt(modes)).astype(np.float32)
+
+    def advect(self, pos, dt=1.0):
+        v = np.zeros_like(pos)
+        for m in range(self.k.shape[0]):
+            arg = pos @ self.k[m]
+            for c in range(3):
+                v[:, c] += self.a[m, c] * np.sin(arg + self.ph[m, c])
+        return (pos + dt * v).astype(np.float32)
+
+
+# ---------------------------------------------------------------- rays
+def _normalize(d):
+    return d / np.linalg.norm(d, axis=-1, keepdims=True)
+
+
+def pinhole_rays(width, height, eye, lookat, up=(0, 1, 0), fov_deg=45.0):
+    """One ray per pixel centre, row-major from the top row; pinhole camera
+    with vertical field of view fov_deg (the frame of render/render_camera.cc:17-63)."""
+    eye = np.asarray(eye, np.float64)
+    look = np.asarray(lookat, np.float64) - eye
+    u = _normalize(np.cross(look, up))
+    v = _normalize(np.cross(look, u))
+    look = _normalize(look)
+    flen = 0.5 * height / np.tan(0.5 * np.radians(fov_deg))
+    corner = flen * look + eye - 0.5 * (width * u + height * v)
+    px = np.arange(width) + 0.5
+    py = np.arange(height) + 0.5
+    P = corner[None, None] + px[None, :, None] * u + py[:, None, None] * v
+    d = _normalize(P - eye).astype(np.float32).reshape(-1, 3)
+    rays = np.zeros(width * height, RAY_DTYPE)
+    rays["org"] = eye.astype(np.float32)
+    rays["dir"] = d
+    rays["prev_prim"] = MISS
+    return rays
+
+
+def ortho_rays(width, height, lo=(0.0, 0.0), hi=(1.0, 1.0), z=2.0):
+    """Orthographic rays along -z through pixel centres of [lo,hi]^2."""
+    xs = lo[0] + (np.arange(width) + 0.5) * (hi[0] - lo[0]) / width
+    ys = lo[1] + (np.arange(height) + 0.5) * (hi[1] - lo[1]) / height
+    X, Y = np.meshgrid(xs, ys)
+    rays = np.zeros(width * height, RAY_DTYPE)
+    rays["org"][:, 0] = X.ravel()
+    rays["org"][:, 1] = Y.ravel()
+    rays["org"][:, 2] = z
+    rays["dir"][:, 2] = -1.0
+    rays["prev_prim"] = MISS
+    return rays
+
+
+def hemisphere_dirs(normals, seed):
+    """Uniform directions on the hemisphere about each normal."""
+    rng = np.random.default_rng(seed)
+    n = normals.shape[0]
+    d = rng.normal(size=(n, 3))
+    d = _normalize(d)
+    s = np.sign(np.sum(d * normals, 1))
+    s[s == 0] = 1.0
+    return (d * s[:, None]).astype(np.float32)
+
+
+# ---------------------------------------------------------------- volume
+def volume_blobs(res=256, nblobs=32, seed=123456, shift_voxels=0.0):
+    """Density grid (res,res,res) float32 (z slowest, x fastest) in [0,1]."""
+    rng = np.random.default_rng(seed)
+    cen = rng.uniform(0.2, 0.8, size=(nblobs, 3))
+    cen = cen + shift_voxels / (res - 1)
+    sig = rng.uniform(0.03, 0.12, size=(nblobs, 3))
+    amp = rng.uniform(0.3, 0.9, size=nblobs)
+    x = np.linspace(0.0, 1.0, res)
+    out = np.zeros((res, res, res), np.float32)
+    for b in range(nblobs):
+        gx = np.exp(-0.5 * ((x - cen[b, 0]) / sig[b, 0]) ** 2)
+        gy = np.exp(-0.5 * ((x - cen[b, 1]) / sig[b, 1]) ** 2)
+        gz = np.exp(-0.5 * ((x - cen[b, 2]) / sig[b, 2]) ** 2)
+        out += (amp[b] * gz[:, None, None] * gy[None, :, None] * gx[None, None, :]).astype(np.float32)
+    return np.clip(out, 0.0, 1.0).astype(np.float32)
+
+
+def transfer_function(entries=256, seed=123456):
+    """RGBA table (entries, 4) float32: smooth colour ramp, opacity rising
+    with density."""
+    rng = np.random.default_rng(seed)
+    x = np.linspace(0.0, 1.0, entries)
+    ph = rng.uniform(0, 2 * np.pi, size=3)
+    rgb = 0.5 + 0.5 * np.sin(2 * np.pi * x[:, None] * np.array([1.0, 1.3, 1.7]) + ph)
+    a = np.clip((x - 0.05) * 1.2, 0.0, 1.0) ** 1.5
+    return np.concatenate([rgb, a[:, None]], 1).astype(np.float32)

@@ -1,0 +1,289 @@
+"""CUDA path vs the CPU oracle (and the reference's golden fixtures).
+
+Bit-exact bar for integer/index work (Morton codes, sorted order, Karras tree,
+canonical topology, leaf ranges) and for the boxes and hits, which the kernels
+compute with the reference's own float/double operation order."""
+import os
+import tempfile
+
+import numpy as np
+import pytest
+
+import surface_b200 as sb
+from oracle import oracle as O
+from surface_b200 import scenes as S
+
+from conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+KIND = {O.TRI: sb.TriangleAccel, O.TET: sb.TetraAccel, O.SPHERE: sb.ParticleAccel}
+
+
+def gpu_build(kind, verts, faces=None, radius=None):
+    acc = KIND[kind]()
+    if kind == O.TRI:
+        acc.Build32(sb.Mesh(verts, faces))
+    elif kind == O.TET:
+        acc.Build32(sb.Tetrahedron(verts, faces))
+    else:
+        acc.Build32(sb.Particles(verts, radius))
+    return acc
+
+
+def gpu_canonical(acc, kind):
+    raw, idx, codes = acc.export()
+    g = O.generic_from_device(kind, raw)
+    return O.canonicalize(g, 0), idx, codes
+
+
+def assert_hits_equal(h, ref, fields=("t", "u", "v", "prim")):
+    for f in fields:
+        a, b = bits(h[f]), bits(ref[f])
+        bad = np.nonzero(a != b)[0]
+        assert bad.size == 0, f"{f}: {bad.size} mismatches, first at {bad[:5]}"
+
+
+# ---------------------------------------------------------------- stages
+def test_morton_stage_matches_oracle():
+    v, f = S.displaced_octasphere(6, seed=11)
+    codes, box = sb.stage_morton(sb.accel.SRT_TRIANGLES, v, f)
+    lo = np.zeros(3, np.float32)
+    hi = np.zeros(3, np.float32)
+    O.lib().so_bbox_tris(O._ptr(v), O._ptr(f), f.shape[0], O._ptr(lo), O._ptr(hi))
+    assert np.array_equal(bits(box), bits(np.concatenate([lo, hi])))
+    ref = np.zeros(f.shape[0], np.uint32)
+    O.lib().so_morton_tris(O._ptr(v), O._ptr(f), f.shape[0], O._ptr(lo), O._ptr(hi),
+                           O._ptr(ref))
+    assert np.array_equal(codes, ref)
+    # tetrahedra and points
+    vt, ft, _ = S.tet_grid(10, seed=2)
+    codes, box = sb.stage_morton(sb.accel.SRT_TETRAHEDRA, vt, ft)
+    O.lib().so_bbox_tets(O._ptr(vt), O._ptr(ft), ft.shape[0], O._ptr(lo), O._ptr(hi))
+    ref = np.zeros(ft.shape[0], np.uint32)
+    O.lib().so_morton_tets(O._ptr(vt), O._ptr(ft), ft.shape[0], O._ptr(lo), O._ptr(hi),
+                           O._ptr(ref))
+    assert np.array_equal(codes, ref)
+    pos, rad = S.particles(50000, seed=3)
+    codes, box = sb.stage_morton(sb.accel.SRT_SPHERES, pos, None, rad)
+    O.lib().so_bbox_spheres(O._ptr(pos), O._ptr(rad), 0.0, pos.shape[0], O._ptr(lo),
+                            O._ptr(hi))
+    assert np.array_equal(bits(box), bits(np.concatenate([lo, hi])))
+    assert np.array_equal(codes, O.morton_points(pos, lo, hi))
+
+
+@pytest.mark.parametrize("n", [2, 8, 1023, 1024, 4097, 100_000, 3_456_663])
+def test_sort_stage_is_stable_and_exact(n):
+    rng = np.random.default_rng(n)
+    codes = rng.integers(0, 1 << 30, size=n, dtype=np.uint32)
+    codes[::3] = codes[0]  # many ties
+    c, i = sb.stage_sort_pairs(codes)
+    rc, ri = O.sort_pairs(codes)
+    assert np.array_equal(c, rc)
+    assert np.array_equal(i, ri)
+
+
+def test_karras_stage_matches_reference_fixture(golden):
+    g = golden("prefix_tree.npz")
+    for n in [8, 15, 31, 1023, 1000, 3211]:
+        for pre in ("", "same_"):
+            sc = np.sort(g[f"{pre}codes_{n}"])
+            child, lt, rt = sb.stage_karras(sc)
+            assert np.array_equal(child, g[f"{pre}child_{n}"])
+            assert np.array_equal(lt, g[f"{pre}ltype_{n}"])
+            assert np.array_equal(rt, g[f"{pre}rtype_{n}"])
+
+
+def test_karras_stage_large():
+    rng = np.random.default_rng(1)
+    codes = np.sort(rng.integers(0, 1 << 30, size=2_000_000, dtype=np.uint32))
+    codes[1000:5000] = codes[1000]
+    codes = np.sort(codes)
+    child, lt, rt = sb.stage_karras(codes)
+    oc, olt, ort = O.karras(codes)
+    assert np.array_equal(child, oc) and np.array_equal(lt, olt) and np.array_equal(rt, ort)
+
+
+# ---------------------------------------------------------------- golden scenes
+@pytest.mark.parametrize("tag,kind", [("tri", O.TRI), ("tet", O.TET), ("sph", O.SPHERE)])
+def test_build_and_trace_match_reference_fixture(golden, tag, kind):
+    g = golden("scenes_small.npz")
+    if kind == O.TRI:
+        acc = gpu_build(kind, g["tri_verts"], g["tri_faces"])
+    elif kind == O.TET:
+        acc = gpu_build(kind, g["tet_verts"], g["tet_faces"])
+    else:
+        acc = gpu_build(kind, g["sph_pos"], None, g["sph_rad"])
+    can, idx, _ = gpu_canonical(acc, kind)
+    assert np.array_equal(can, g[f"{tag}_canon"])
+    assert np.array_equal(idx, g[f"{tag}_index"])
+    lo, hi = acc.BoundingBox()
+    assert np.array_equal(np.concatenate([lo, hi]), g[f"{tag}_bbox"])
+    if kind == O.TET:
+        res = acc.Traverse(g["tet_rays"], want_subface=True)
+        assert_hits_equal(res.hits, g["tet_hits"])
+        assert np.array_equal(res.subface, g["tet_subface"])
+    elif kind == O.TRI:
+        assert_hits_equal(acc.Traverse(g["tri_rays"]), g["tri_hits"])
+    else:
+        assert_hits_equal(acc.Traverse(g["sph_rays"]), g["sph_hits"], ("t", "prim"))
+        h2 = acc.Traverse(g["sph_sec_rays"], prev_normals=g["sph_sec_normals"])
+        assert_hits_equal(h2, g["sph_sec_hits"], ("t", "prim"))
+
+
+# ---------------------------------------------------------------- vs oracle
+def _compare_build(kind, verts, faces=None, radius=None):
+    o = O.OracleAccel(kind, verts, faces, radius)
+    acc = gpu_build(kind, verts, faces, radius)
+    can, idx, codes = gpu_canonical(acc, kind)
+    oc = o.canonical()
+    assert can.shape == oc.shape, (can.shape, oc.shape)
+    assert np.array_equal(can, oc)
+    assert np.array_equal(idx, o.indices)
+    assert np.array_equal(codes, o.codes)
+    inf = acc.info()
+    assert inf.num_prims == o.n
+    return o, acc
+
+
+@pytest.mark.parametrize("levels", [0, 1, 3, 5, 7])
+def test_triangles_build_and_trace(levels):
+    v, f = S.displaced_octasphere(levels, seed=100 + levels)
+    o, acc = _compare_build(O.TRI, v, f)
+    rays = S.pinhole_rays(128, 128, (0, 0, 3), (0, 0, 0))
+    assert_hits_equal(acc.Traverse(rays), o.trace(rays))
+
+
+@pytest.mark.parametrize("n", [2, 3, 17, 18, 1023, 1024, 1025, 5000])
+def test_triangle_counts_at_boundaries(n):
+    v, f = S.octasphere_for_count(max(n, 8), seed=n)
+    f = f[:n]
+    o, acc = _compare_build(O.TRI, v, f)
+    rays = S.pinhole_rays(48, 48, (0, 0, 3), (0, 0, 0))
+    assert_hits_equal(acc.Traverse(rays), o.trace(rays))
+
+
+@pytest.mark.parametrize("cells", [2, 8, 20])
+def test_tetra_build_and_trace(cells):
+    v, f, sc = S.tet_grid(cells, seed=cells)
+    o, acc = _compare_build(O.TET, v, f)
+    for rays in (S.ortho_rays(96, 96),
+                 S.pinhole_rays(64, 64, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)):
+        import torch
+        res = acc.Traverse(rays, want_subface=True)
+        oh, osub, osc = o.trace(rays, want_subface=True, vertex_scalar=sc)
+        assert_hits_equal(res.hits, oh)
+        assert np.array_equal(res.subface, osub)
+        # barycentric scalar at the entering point (needs the scalar on device)
+        acc_t = torch.as_tensor(rays.view(np.float32).reshape(-1, 8)).cuda()
+        r2 = acc.Traverse(acc_t, vertex_scalar=torch.as_tensor(sc).cuda(), want_scalar=True)
+        torch.cuda.synchronize()
+        assert np.array_equal(bits(r2.scalar.cpu().numpy()), bits(osc))
+
+
+def test_spheres_build_trace_and_self_hit_rule():
+    pos, rad = S.particles(200_000, seed=5)
+    pos[1000:1300] = pos[1000]  # coincident centres
+    o, acc = _compare_build(O.SPHERE, pos, None, rad)
+    rays = S.pinhole_rays(128, 128, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    res = acc.Traverse(rays, want_normal=True)
+    oh = o.trace(rays)
+    assert_hits_equal(res.hits, oh, ("t", "prim"))
+    hit = oh["prim"] != O.MISS
+    sec = np.zeros(int(hit.sum()), O.RAY_DTYPE)
+    p = rays["org"][hit] + res.hits["t"][hit, None] * rays["dir"][hit]
+    nrm = res.normal[hit]
+    sec["org"] = p.astype(np.float32)
+    sec["dir"] = S.hemisphere_dirs(nrm, seed=7)
+    sec["prev_prim"] = oh["prim"][hit]
+    sec["prev_t"] = oh["t"][hit]
+    assert_hits_equal(acc.Traverse(sec, prev_normals=nrm), o.trace(sec, prev_normals=nrm),
+                      ("t", "prim"))
+
+
+def test_constant_radius_spheres():
+    pos, _ = S.particles(30_000, seed=8)
+    o = O.OracleAccel(O.SPHERE, pos, None, None, const_radius=0.004)
+    acc = sb.ParticleAccel()
+    acc.Build32(sb.Particles(pos, None, 0.004))
+    can, idx, _ = gpu_canonical(acc, O.SPHERE)
+    assert np.array_equal(can, o.canonical())
+    rays = S.pinhole_rays(64, 64, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    assert_hits_equal(acc.Traverse(rays), o.trace(rays), ("t", "prim"))
+
+
+def test_dump_is_reference_format():
+    v, f = S.displaced_octasphere(5, seed=3)
+    o = O.OracleAccel(O.TRI, v, f)
+    acc = gpu_build(O.TRI, v, f)
+    with tempfile.TemporaryDirectory() as td:
+        path = os.path.join(td, "a.bin")
+        acc.Dump(path)
+        raw, idx = O._read_dump(path, 64)
+    fl = raw[:, :48].copy().view(np.float32).reshape(-1, 2, 2, 3)
+    ints = raw[:, 48:64].copy().view(np.int32).reshape(-1, 4)
+    g = O.generic_from_two_box(fl[:, 0], fl[:, 1], ints[:, 0], ints[:, 1],
+                               ints[:, 2].view(np.uint32), ints[:, 3].view(np.uint32))
+    assert np.array_equal(O.canonicalize(g, 0), o.canonical())
+    assert np.array_equal(idx, o.indices)
+    # sequential depth-first emission: the node array equals the oracle's
+    assert np.array_equal(g["d0"], o.nodes["d0"]) and np.array_equal(g["d1"], o.nodes["d1"])
+
+
+def test_rebuild_reuses_accel():
+    acc = sb.TriangleAccel()
+    for lv in (6, 4, 6):
+        v, f = S.displaced_octasphere(lv, seed=lv)
+        acc.Build32(sb.Mesh(v, f))
+        o = O.OracleAccel(O.TRI, v, f)
+        can, idx, _ = gpu_canonical(acc, O.TRI)
+        assert np.array_equal(can, o.canonical())
+
+
+def test_torch_device_inputs_and_async_trace():
+    import torch
+    v, f = S.displaced_octasphere(6, seed=21)
+    rays = S.pinhole_rays(128, 96, (0, 0, 3), (0, 0, 0))
+    o = O.OracleAccel(O.TRI, v, f)
+    acc = sb.TriangleAccel()
+    vt = torch.as_tensor(v).cuda()
+    ft = torch.as_tensor(f.astype(np.int32)).cuda()
+    acc.Build32(sb.Mesh(vt, ft))
+    rt = torch.as_tensor(rays.view(np.float32).reshape(-1, 8)).cuda()
+    h = acc.Traverse(rt)
+    torch.cuda.synchronize()
+    hn = h.cpu().numpy().view(O.HIT_DTYPE).reshape(-1)
+    assert_hits_equal(hn, o.trace(rays))
+
+
+# ---------------------------------------------------------------- full size
+def test_full_size_triangle_workload():
+    """131,072-triangle displaced octasphere, 512^2 pinhole rays."""
+    v, f = S.displaced_octasphere(7)
+    o, acc = _compare_build(O.TRI, v, f)
+    rays = S.pinhole_rays(512, 512, (0, 0, 3), (0, 0, 0))
+    h = acc.Traverse(rays)
+    oh = o.trace(rays)
+    assert_hits_equal(h, oh)
+    assert acc.info().num_branches == len([1 for x in o.nodes if not x["leaf"]])
+
+
+def test_full_size_tetra_workload():
+    """1,310,720 tetrahedra (64^3 cells), 1024^2 orthographic rays."""
+    v, f, sc = S.tet_grid(64)
+    o, acc = _compare_build(O.TET, v, f)
+    rays = S.ortho_rays(1024, 1024)
+    res = acc.Traverse(rays, want_subface=True)
+    oh, osub = o.trace(rays, want_subface=True)
+    ids = np.mean(res.hits["prim"] == oh["prim"])
+    assert ids >= 0.9999
+    assert_hits_equal(res.hits, oh)
+    assert np.array_equal(res.subface, osub)
+
+
+def test_full_size_particle_frame():
+    """16,777,216 spheres: build and a strided subset of 2048^2 primaries."""
+    pos, rad = S.particles()
+    o, acc = _compare_build(O.SPHERE, pos, None, rad)
+    rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)[::37]
+    assert_hits_equal(acc.Traverse(rays), o.trace(rays), ("t", "prim"))

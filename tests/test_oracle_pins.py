@@ -1,0 +1,201 @@
+"""The CPU oracle pinned against the reference: its own known answers and
+invariants (test/cctest/test-prefix-tree.cc), golden fixtures generated from the
+reference's code (tests/golden/make_golden.py), and -- when the reference build
+is present -- direct differential runs against it."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from surface_b200 import scenes as S
+
+from conftest import bits
+
+NS = [8, 15, 31, 1023, 1000, 3211]
+
+
+def test_tinymt64_restatement_matches_fixture(golden):
+    g = golden("prefix_tree.npz")
+    d = O.tinymt64_doubles(3 * sum(NS))
+    off = 0
+    for n in NS:
+        pts = d[off:off + 3 * n].astype(np.float32).reshape(n, 3)
+        off += 3 * n
+        assert np.array_equal(bits(pts), bits(g[f"pts_{n}"]))
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+def test_tinymt64_restatement_matches_reference():
+    assert np.array_equal(O.tinymt64_doubles(5000), O.tinymt64_doubles(5000, use_ref=True))
+
+
+def test_morton_known_answer():
+    # test/cctest/test-prefix-tree.cc:27-41: (0.5,0.5,0.5) in the unit box, inv 1024
+    c = O.morton_points(np.array([[0.5, 0.5, 0.5]], np.float32), [0, 0, 0], [1, 1, 1])
+    assert int(c[0]) == (1 << 29) | (1 << 28) | (1 << 27)
+    assert O.lib().so_morton_bits(512, 512, 512) == (1 << 29) | (1 << 28) | (1 << 27)
+
+
+def test_morton_codes_match_reference_fixture(golden):
+    g = golden("prefix_tree.npz")
+    for n in NS:
+        c = O.morton_points(g[f"pts_{n}"], [0, 0, 0], [1, 1, 1])
+        assert np.array_equal(c, g[f"codes_{n}"])
+        # the reference's SSE path agrees with its scalar path (:44-82)
+        assert np.array_equal(c, g[f"codes_simd_{n}"])
+
+
+def test_sort_is_stable_and_matches_reference(golden):
+    g = golden("prefix_tree.npz")
+    for n in NS:
+        c, i = O.sort_pairs(g[f"codes_{n}"])
+        assert np.all(c[:-1] <= c[1:])
+        tie = c[:-1] == c[1:]
+        assert np.all(i[:-1][tie] < i[1:][tie])
+        assert np.array_equal(c, np.sort(g[f"codes_{n}"]))
+    c, i = O.sort_pairs(g["codes_3211"])
+    assert np.array_equal(c, g["sorted_codes_3211"])
+    assert np.array_equal(i, g["sorted_index_3211"])
+
+
+def _karras_invariants(child, lt, rt, n):
+    # every leaf referenced exactly once, flat count (test-prefix-tree.cc:470-488)
+    cnt = np.zeros(n, np.int64)
+    np.add.at(cnt, child[lt == 1], 1)
+    np.add.at(cnt, child[rt == 1] + 1, 1)
+    assert np.all(cnt == 1)
+    # ... and by a walk from the root, depth < 30 for distinct keys
+    seen = np.zeros(n, np.int64)
+    stack = [(0, 0)]
+    maxd = 0
+    while stack:
+        i, d = stack.pop()
+        maxd = max(maxd, d)
+        g = int(child[i])
+        for side, leaf in ((0, lt[i]), (1, rt[i])):
+            c = g + side
+            if leaf:
+                seen[c] += 1
+            else:
+                stack.append((c, d + 1))
+    assert np.all(seen == 1)
+    return maxd
+
+
+def test_karras_matches_reference_fixture(golden):
+    g = golden("prefix_tree.npz")
+    for n in NS:
+        sc = np.sort(g[f"codes_{n}"])
+        child, lt, rt = O.karras(sc)
+        assert np.array_equal(child, g[f"child_{n}"])
+        assert np.array_equal(lt, g[f"ltype_{n}"])
+        assert np.array_equal(rt, g[f"rtype_{n}"])
+        assert _karras_invariants(child, lt, rt, n) < 30
+        # all keys equal (test-prefix-tree.cc:700-918)
+        cs = g[f"same_codes_{n}"]
+        assert np.all(cs == cs[0])
+        child, lt, rt = O.karras(cs)
+        assert np.array_equal(child, g[f"same_child_{n}"])
+        assert np.array_equal(lt, g[f"same_ltype_{n}"])
+        assert np.array_equal(rt, g[f"same_rtype_{n}"])
+        _karras_invariants(child, lt, rt, n)
+
+
+@pytest.mark.parametrize("tag,kind", [("tri", O.TRI), ("tet", O.TET), ("sph", O.SPHERE)])
+def test_oracle_build_and_trace_match_reference_fixture(golden, tag, kind):
+    g = golden("scenes_small.npz")
+    if kind == O.TRI:
+        acc = O.OracleAccel(kind, g["tri_verts"], g["tri_faces"])
+    elif kind == O.TET:
+        acc = O.OracleAccel(kind, g["tet_verts"], g["tet_faces"])
+    else:
+        acc = O.OracleAccel(kind, g["sph_pos"], None, g["sph_rad"])
+    assert np.array_equal(acc.canonical(), g[f"{tag}_canon"])
+    assert np.array_equal(acc.indices, g[f"{tag}_index"])
+    if kind == O.TET:
+        h, sub = acc.trace(g["tet_rays"], want_subface=True)
+        assert np.array_equal(sub, g["tet_subface"])
+    else:
+        h = acc.trace(g[f"{tag}_rays"])
+    ref = g[f"{tag}_hits"]
+    for f in ("t", "u", "v", "prim"):
+        if kind == O.SPHERE and f in ("u", "v"):
+            continue
+        assert np.array_equal(bits(h[f]), bits(ref[f])), f
+    if kind == O.SPHERE:
+        h2 = acc.trace(g["sph_sec_rays"], prev_normals=g["sph_sec_normals"])
+        assert np.array_equal(h2["prim"], g["sph_sec_hits"]["prim"])
+        assert np.array_equal(bits(h2["t"]), bits(g["sph_sec_hits"]["t"]))
+
+
+def test_tex3d_matches_reference_fixture(golden):
+    g = golden("texture3d.npz")
+    img = g["tex_img"]
+    d, h, w = img.shape
+    for mode in (0, 1):
+        out = O.tex3d(img, (w, h, d), g["tex_uvw"], clamp=(mode, mode, mode))
+        assert np.array_equal(bits(out), bits(g[f"tex_out_clamp{mode}"]))
+
+
+# ---------------------------------------------------------------- direct runs
+need_ref = pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+
+
+@need_ref
+@pytest.mark.parametrize("levels", [5, 6])
+def test_oracle_vs_reference_triangles(levels):
+    v, f = S.displaced_octasphere(levels, seed=levels)
+    o = O.OracleAccel(O.TRI, v, f)
+    r = O.RefAccel(O.TRI, v, f)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc)
+    assert np.array_equal(o.indices, ridx)
+    rays = S.pinhole_rays(96, 96, (0, 0, 3), (0, 0, 0))
+    ho, hr = o.trace(rays), r.trace(rays)
+    for k in ("t", "u", "v", "prim"):
+        assert np.array_equal(bits(ho[k]), bits(hr[k]))
+
+
+@need_ref
+def test_oracle_vs_reference_tetra():
+    v, f, _ = S.tet_grid(12, seed=3)
+    o = O.OracleAccel(O.TET, v, f)
+    r = O.RefAccel(O.TET, v, f)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc)
+    rays = S.ortho_rays(96, 96)
+    (ho, so), (hr, sr) = o.trace(rays, want_subface=True), r.trace(rays)
+    assert np.array_equal(so, sr)
+    for k in ("t", "u", "v", "prim"):
+        assert np.array_equal(bits(ho[k]), bits(hr[k]))
+    # oblique rays exercise all Pluecker branches
+    obl = S.pinhole_rays(64, 64, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)
+    ho, hr = o.trace(obl), r.trace(obl)[0]
+    for k in ("t", "u", "v", "prim"):
+        assert np.array_equal(bits(ho[k]), bits(hr[k]))
+
+
+@need_ref
+def test_oracle_vs_reference_spheres_with_coincident_points():
+    pos, rad = S.particles(20000, seed=4)
+    pos[100:400] = pos[100]  # coincident centres (same Morton key)
+    o = O.OracleAccel(O.SPHERE, pos, None, rad)
+    r = O.RefAccel(O.SPHERE, pos, None, rad)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc)
+    assert np.array_equal(o.indices, ridx)
+    rays = S.pinhole_rays(96, 96, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    ho, hr = o.trace(rays), r.trace(rays)
+    assert np.array_equal(ho["prim"], hr["prim"])
+    assert np.array_equal(bits(ho["t"]), bits(hr["t"]))
+
+
+@need_ref
+def test_oracle_vs_reference_flat_mesh():
+    # a z-flat sheet: zero extent on one axis -> inf scale in the quantiser
+    v, f = S.displaced_octasphere(5, seed=9)
+    v[:, 2] = 0.25
+    o = O.OracleAccel(O.TRI, v, f)
+    r = O.RefAccel(O.TRI, v, f)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc)
+    assert np.array_equal(o.indices, ridx)
