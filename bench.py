@@ -211,6 +211,9 @@ def run_ours(args, W):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
+    # all work (ours and the timing events) on one dedicated stream
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
     if world > 1:
         import datetime
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
@@ -251,15 +254,16 @@ def run_ours(args, W):
     torch.cuda.synchronize()
 
     # traversal work counters for the roofline (one extra untimed pass)
-    st = torch.zeros(3, dtype=torch.int64, device=dev)
+    st = torch.zeros(4, dtype=torch.int64, device=dev)
     L = _lib.load()
     opts = _lib.TraceOpts(None, None, scalar.data_ptr() if scalar is not None else None,
-                          None, None, st.data_ptr())
+                          None, None, st.data_ptr(), 0, 0)
     ctx.use_torch_stream()
     _lib.check(L.srt_trace_closest(acc.h, rays.data_ptr(), nr, hits.data_ptr(),
                                    __import__("ctypes").byref(opts)))
     torch.cuda.synchronize()
-    stats = st.cpu().numpy().astype(np.float64)
+    stats_all = st.cpu().numpy().astype(np.float64)
+    stats = stats_all[:3]
 
     launches0 = L.srt_ctx_launch_count(ctx.h)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
@@ -318,7 +322,7 @@ def run_ours(args, W):
                                                  h_rad.data_ptr(), C.c_float(0.0),
                                                  h_verts.shape[0]))
         o = _lib.TraceOpts(None, None, d_scalar.data_ptr() if d_scalar is not None else None,
-                           h_scal.data_ptr() if kind == "tet" else None, None, None)
+                           h_scal.data_ptr() if kind == "tet" else None, None, None, 0, 0)
         _lib.check(L.srt_trace_closest(e2e_acc, h_rays.data_ptr(), nr, h_hits.data_ptr(),
                                        C.byref(o)))
 
@@ -350,7 +354,8 @@ def run_ours(args, W):
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": src, "traffic": None,
                 "algorithmic_bytes_per_ray": round(bpr, 1),
-                "visits_per_ray": [round(float(x) / nr, 3) for x in stats]}
+                "visits_per_ray": [round(float(x) / nr, 3) for x in stats],
+                "reference_walk_rays": int(stats_all[3])}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:

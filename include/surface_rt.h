@@ -100,11 +100,21 @@ typedef struct srt_trace_opts {
   /* triangles and spheres: geometric normal at the hit (3 floats per ray,
    * as BuildIntersection computes it) */
   float *normal_out;
-  /* work counters (device memory, 3 x uint64, accumulated): branch nodes
+  /* work counters (device memory, 4 x uint64, accumulated): branch nodes
    * visited, leaves visited, primitive tests -- the reference's
-   * TetraTraversalStatistics (render/render_accel_tetra.h:70-78) */
+   * TetraTraversalStatistics (render/render_accel_tetra.h:70-78) -- and
+   * rays that took the reference's walk */
   unsigned long long *stats;
+  /* SRT_TRACE_* bits */
+  uint32_t flags;
+  uint32_t reserved;
 } srt_trace_opts;
+
+/* srt_trace_opts.flags: walk the tree once in the reference's own order
+ * (its Traverse loop step for step) instead of the default walk, which goes
+ * front to back and replays the reference's order only to break exact
+ * ties.  Both give identical hits; the default does far less work. */
+#define SRT_TRACE_SINGLE_PASS 1u
 
 typedef struct srt_ctx srt_ctx;
 typedef struct srt_accel srt_accel;
@@ -125,7 +135,8 @@ typedef struct srt_accel_info {
 SRT_API srt_status srt_ctx_create(int device, srt_ctx **out);
 SRT_API srt_status srt_ctx_destroy(srt_ctx *ctx);
 /* Use `stream` (a cudaStream_t) for all work of this context; NULL = the
- * context's own stream. */
+ * context's own stream; (void*)1 = cudaStreamLegacy, the legacy default
+ * stream (handle 0 in most frameworks). */
 SRT_API srt_status srt_ctx_set_stream(srt_ctx *ctx, void *stream);
 SRT_API void *srt_ctx_get_stream(srt_ctx *ctx);
 /* Wait for all queued work; reports kernel-side limit hits (SRT_ERR_LIMIT)

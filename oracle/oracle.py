@@ -73,6 +73,7 @@ def lib():
         L.so_canonicalize.restype = C.c_long
         L.so_canonicalize.argtypes = [_P, _SZ, _SZ, _P, _SZ]
         L.so_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, _P, _P, C.c_int]
+        L.so_trace2.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, C.c_int]
         L.so_morton_bits.restype = C.c_uint32
         L.so_morton_bits.argtypes = [C.c_uint32] * 3
         for n in ("so_morton_tris", "so_morton_tets"):
@@ -202,6 +203,23 @@ class OracleAccel:
             out.append(sub)
         if vs is not None:
             out.append(so)
+        if want_stats:
+            out.append(st)
+        return out[0] if len(out) == 1 else tuple(out)
+
+    def trace2(self, rays, prev_normals=None, want_subface=False, want_stats=False,
+               nthreads=0):
+        """The product's two-pass walk, restated (for checking it on the CPU)."""
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        sub = np.zeros(rays.size, np.uint32) if want_subface else None
+        st = np.zeros(4, np.uint64)
+        pn = None if prev_normals is None else np.ascontiguousarray(prev_normals, np.float32)
+        lib().so_trace2(self.h, _ptr(rays), rays.size, _ptr(pn), _ptr(hits), _ptr(sub),
+                        _ptr(st), nthreads)
+        out = [hits]
+        if want_subface:
+            out.append(sub)
         if want_stats:
             out.append(st)
         return out[0] if len(out) == 1 else tuple(out)

@@ -1001,6 +1001,324 @@ static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
   }
 }
 
+/* ---- two-pass walk (restatement of the product's default traversal) ----
+ * Pass 1: front-to-back (nearer child box first), pruning boxes entered
+ * after bound(m), m = running smallest hit distance.  Pass 2: the
+ * reference's depth-first order through boxes entered before bound(m),
+ * applying the reference's acceptance rule to the candidates at m
+ * (tetrahedra: within 8 float steps of m).  This equals the reference's
+ * result whenever no intersected primitive reports a distance below the
+ * entry distance of its own leaf box; the walk checks that for every
+ * primitive it tests and otherwise falls back to the reference's walk. */
+static inline float bound_rel(float m, float rel) {
+  return (m < FLT_MAX) ? m + fabsf(m) * rel + 1e-30f : FLT_MAX;
+}
+#define SO_REL_TRI 3.90625e-3f      /* 2^-8 */
+#define SO_REL_TET 1.52587890625e-5f /* 2^-16 */
+#define SO_VIOL_TOL 4.76837158203125e-7f /* 2^-21 */
+
+/* candidate t below (or within rounding of) its leaf box entry */
+static inline int below_entry(double t, float entry) {
+  return t < (double)entry + fabs((double)entry) * (double)SO_VIOL_TOL;
+}
+
+static inline int ray_aabb_t(float maxT, const float bmin[3], const float bmax[3],
+                             const float org[3], const float inv[3], const int sgn[3],
+                             int clamp, float *tmin_out) {
+  float tmin, tmax;
+  const float min_x = sgn[0] ? bmax[0] : bmin[0];
+  const float min_y = sgn[1] ? bmax[1] : bmin[1];
+  const float min_z = sgn[2] ? bmax[2] : bmin[2];
+  const float max_x = sgn[0] ? bmin[0] : bmax[0];
+  const float max_y = sgn[1] ? bmin[1] : bmax[1];
+  const float max_z = sgn[2] ? bmin[2] : bmax[2];
+  const float tmin_x = (min_x - org[0]) * inv[0];
+  const float tmax_x = (max_x - org[0]) * inv[0];
+  const float tmin_y = (min_y - org[1]) * inv[1];
+  const float tmax_y = (max_y - org[1]) * inv[1];
+  tmin = (tmin_x > tmin_y) ? tmin_x : tmin_y;
+  tmax = (tmax_x < tmax_y) ? tmax_x : tmax_y;
+  const float tmin_z = (min_z - org[2]) * inv[2];
+  const float tmax_z = (max_z - org[2]) * inv[2];
+  tmin = (tmin > tmin_z) ? tmin : tmin_z;
+  tmax = (tmax < tmax_z) ? tmax : tmax_z;
+  *tmin_out = tmin;
+  if (clamp) {
+    tmax = (maxT < tmax) ? maxT : tmax;
+    return (tmax > 0.0f) && (tmin <= tmax);
+  }
+  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= maxT);
+}
+
+/* One primitive's hit distance for the two-pass walk; returns 1 on a hit
+ * whose distance is stored in *tc (double for tetrahedra).  The per-kind
+ * acceptance state is handled by the caller. */
+static inline int prim_candidate(const so_accel *a, uint32_t f, const so_ray *ray,
+                                 const float *org, const float *dir, const float *pn,
+                                 d3 o, d3 d, float tio, double *tc, float *u, float *v,
+                                 int *ef, double *e1, double *e2, double *ul1) {
+  if (a->kind == SO_TRI) {
+    if (f == ray->prev_prim) return 0;
+    const float *p0 = &a->verts[3 * (size_t)a->faces[3 * (size_t)f + 0]];
+    const float *p1 = &a->verts[3 * (size_t)a->faces[3 * (size_t)f + 1]];
+    const float *p2 = &a->verts[3 * (size_t)a->faces[3 * (size_t)f + 2]];
+    float t = tio;
+    if (!tri_isect(&t, u, v, p0, p1, p2, org, dir, a->keps)) return 0;
+    *tc = t;
+    return 1;
+  }
+  if (a->kind == SO_SPHERE) {
+    float r = sphere_radius(a->radius, a->constr, f);
+    float t = tio;
+    if (!sphere_isect(&t, &a->verts[3 * (size_t)f], r, org, dir, (double)ray->prev_t, pn,
+                      ray->prev_prim == f))
+      return 0;
+    *tc = t;
+    return 1;
+  }
+  if (f == ray->prev_prim) return 0;
+  d3 V[4];
+  for (int j = 0; j < 4; j++) {
+    const float *p = &a->verts[3 * (size_t)a->faces[4 * (size_t)f + j]];
+    V[j].x = p[0]; V[j].y = p[1]; V[j].z = p[2];
+  }
+  double te;
+  if (!ray_tet(o, d, V, ef, e1, e2, ul1, &te) || !(te >= 0.0)) return 0;
+  *tc = te;
+  return 1;
+}
+
+/* window membership: triangles and spheres t == m (float); tetrahedra
+ * within 8 float steps above m */
+static inline double window_hi(double m, int tet) {
+  if (!tet) return m;
+  float wf = (float)m;
+  for (int k = 0; k < 8; k++) wf = nextafterf(wf, FLT_MAX);
+  return (double)wf;
+}
+
+typedef struct {
+  double t, e1, e2, ul1;
+  float u, v;
+  uint32_t prim;
+  int ef;
+} so_cand;
+
+static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
+                       so_hit *h, uint32_t *subface, float *scal, const float *vscalar,
+                       so_stats *st, int *fallback) {
+  int sgn[3];
+  float inv[3];
+  for (int k = 0; k < 3; k++) {
+    sgn[k] = ray->dir[k] < 0.0f ? 1 : 0;
+    inv[k] = (float)(1.0 / (double)ray->dir[k]);
+  }
+  const float *org = ray->org, *dir = ray->dir;
+  float zero3[3] = {0, 0, 0};
+  const float *pn = prevN ? prevN : zero3;
+  const int tet = a->kind == SO_TET;
+  const int clamp = !tet;
+  const float rel = tet ? SO_REL_TET : SO_REL_TRI;
+  d3 o = {org[0], org[1], org[2]}, d = {dir[0], dir[1], dir[2]};
+  int stk[512];
+  float stt[512];
+  int sp, viol = 0;
+  /* ---- pass 1: front to back, collecting the candidates in the window */
+  double m = DBL_MAX;
+  so_cand win[4];
+  int nwin = 0, overflow = 0;
+  sp = -1;
+  {
+    float t0;
+    if (!tet || ray_aabb_t(FLT_MAX, a->nodes[0].bmin, a->nodes[0].bmax, org, inv, sgn, 0, &t0)) {
+      stk[0] = 0;
+      stt[0] = tet ? t0 : -FLT_MAX;
+      sp = 0;
+    }
+  }
+  while (sp >= 0) {
+    const int ni = stk[sp];
+    const float et = stt[sp];
+    sp--;
+    const float bnd = (m < DBL_MAX) ? bound_rel((float)m, rel) : FLT_MAX;
+    if (et > bnd) continue;
+    const so_node *nd = &a->nodes[ni];
+    if (!nd->leaf) {
+      st->branch_visits++;
+      float t0, t1;
+      const so_node *c0 = &a->nodes[nd->d0], *c1 = &a->nodes[nd->d1];
+      int h0 = ray_aabb_t(bnd, c0->bmin, c0->bmax, org, inv, sgn, clamp, &t0);
+      int h1 = ray_aabb_t(bnd, c1->bmin, c1->bmax, org, inv, sgn, clamp, &t1);
+      if (h0 && h1) {
+        int first1 = t1 < t0;
+        stk[++sp] = first1 ? (int)nd->d0 : (int)nd->d1; stt[sp] = first1 ? t0 : t1;
+        stk[++sp] = first1 ? (int)nd->d1 : (int)nd->d0; stt[sp] = first1 ? t1 : t0;
+      } else if (h0) {
+        stk[++sp] = (int)nd->d0; stt[sp] = t0;
+      } else if (h1) {
+        stk[++sp] = (int)nd->d1; stt[sp] = t1;
+      }
+      continue;
+    }
+    st->leaf_visits++;
+    for (uint32_t i = 0; i < nd->d0; i++) {
+      uint32_t f = a->indices[nd->d1 + i];
+      st->prim_tests++;
+      so_cand c;
+      if (!prim_candidate(a, f, ray, org, dir, pn, o, d, FLT_MAX, &c.t, &c.u, &c.v, &c.ef,
+                          &c.e1, &c.e2, &c.ul1))
+        continue;
+      c.prim = f;
+      if (below_entry(c.t, et)) viol = 1;
+      if (c.t < m) {
+        m = c.t;
+        /* drop the candidates that fell out of the window */
+        double whi = window_hi(m, tet);
+        int k2 = 0;
+        for (int k = 0; k < nwin; k++)
+          if (win[k].t <= whi) win[k2++] = win[k];
+        nwin = k2;
+      }
+      if (c.t <= window_hi(m, tet)) {
+        if (nwin < 4) win[nwin++] = c;
+        else overflow = 1;
+      }
+    }
+  }
+  h->t = FLT_MAX;
+  h->u = 0.0f;
+  h->v = 0.0f;
+  h->prim = 0xffffffffu;
+  uint32_t sub = 0;
+  double be1 = 0.0, be2 = 0.0;
+  if (!viol && m < DBL_MAX && nwin == 1 && !overflow) {
+    /* one candidate in the window: it is the reference's answer */
+    h->t = (float)win[0].t;
+    h->prim = win[0].prim;
+    if (tet) {
+      h->u = (float)win[0].e1;
+      h->v = (float)win[0].ul1;
+      sub = (uint32_t)win[0].ef;
+      be1 = win[0].e1;
+      be2 = win[0].e2;
+    } else if (a->kind == SO_TRI) {
+      h->u = win[0].u;
+      h->v = win[0].v;
+    }
+  } else if (!viol && m < DBL_MAX) {
+    /* ---- pass 2: several candidates at m; the reference's order decides */
+    float bnd, t;
+    double whi = window_hi(m, tet);
+    if (tet) {
+      bnd = bound_rel((float)whi, rel);
+      t = FLT_MAX;
+    } else {
+      bnd = bound_rel((float)m, rel);
+      t = (a->kind == SO_TRI) ? (float)m : nextafterf((float)m, FLT_MAX);
+    }
+    sp = 0;
+    stk[0] = 0;
+    while (sp >= 0) {
+      const so_node *nd = &a->nodes[stk[sp]];
+      sp--;
+      if (tet) {
+        float tm;
+        int hit = ray_aabb_t(bnd, nd->bmin, nd->bmax, org, inv, sgn, 0, &tm);
+        st->branch_visits++;
+        if (!hit) continue;
+        if (!nd->leaf) {
+          int nearc = sgn[nd->axis], farc = 1 - nearc;
+          stk[++sp] = (int)(farc ? nd->d1 : nd->d0);
+          stk[++sp] = (int)(nearc ? nd->d1 : nd->d0);
+          continue;
+        }
+      } else if (!nd->leaf) {
+        st->branch_visits++;
+        const so_node *c0 = &a->nodes[nd->d0], *c1 = &a->nodes[nd->d1];
+        int hits[2];
+        hits[0] = ray_aabb(bnd, c0->bmin, c0->bmax, org, inv, sgn, 1);
+        hits[1] = ray_aabb(bnd, c1->bmin, c1->bmax, org, inv, sgn, 1);
+        if (hits[0] || hits[1]) {
+          int nearc = sgn[nd->axis], farc = 1 - nearc;
+          if (hits[farc]) stk[++sp] = (int)(farc ? nd->d1 : nd->d0);
+          if (hits[nearc]) stk[++sp] = (int)(nearc ? nd->d1 : nd->d0);
+        }
+        continue;
+      }
+      st->leaf_visits++;
+      for (uint32_t i = 0; i < nd->d0; i++) {
+        uint32_t f = a->indices[nd->d1 + i];
+        st->prim_tests++;
+        so_cand c;
+        if (!prim_candidate(a, f, ray, org, dir, pn, o, d, FLT_MAX, &c.t, &c.u, &c.v, &c.ef,
+                            &c.e1, &c.e2, &c.ul1))
+          continue;
+        if (tet) {
+          if (c.t <= whi && c.t < (double)t) {
+            h->t = (float)c.t; h->u = (float)c.e1; h->v = (float)c.ul1; h->prim = f;
+            sub = (uint32_t)c.ef;
+            be1 = c.e1;
+            be2 = c.e2;
+            t = (float)c.t;
+          }
+        } else if (a->kind == SO_TRI) {
+          if ((float)c.t <= t) {
+            t = (float)c.t; h->t = t; h->u = c.u; h->v = c.v; h->prim = f;
+          }
+        } else if ((float)c.t < t) {
+          t = (float)c.t; h->t = t; h->prim = f;
+        }
+      }
+    }
+  }
+  if (viol) {
+    /* a primitive reported a distance below its leaf box's entry: the
+     * reference's pruning may matter, so take its walk */
+    trace_one(a, ray, prevN, h, subface, vscalar, scal, st);
+    if (fallback) *fallback = 1;
+    return;
+  }
+  if (subface) *subface = sub;
+  if (scal) {
+    float sv = 0.0f;
+    if (h->prim != 0xffffffffu && vscalar && tet) {
+      static const int fa[4] = {3, 2, 1, 0}, fb[4] = {2, 3, 0, 1}, fc[4] = {1, 0, 3, 2};
+      const uint32_t *tv = &a->faces[4 * (size_t)h->prim];
+      double sa = vscalar[tv[fa[sub]]], sb = vscalar[tv[fb[sub]]], sc = vscalar[tv[fc[sub]]];
+      sv = (float)((1.0 - be1 - be2) * sa + be1 * sb + be2 * sc);
+    }
+    *scal = sv;
+  }
+}
+
+/* stats (optional): 4 x uint64 (branch visits, leaf visits, primitive
+ * tests, rays that fell back to the reference's walk). */
+SO_API void so_trace2(const so_accel *a, const so_ray *rays, size_t n,
+                      const float *prev_normals, so_hit *hits, uint32_t *subface,
+                      uint64_t *stats, int nthreads) {
+  uint64_t bv = 0, lv = 0, pt = 0, fb = 0;
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads) reduction(+ : bv, lv, pt, fb)
+#endif
+  for (long long i = 0; i < (long long)n; i++) {
+    so_stats st = {0, 0, 0};
+    int fall = 0;
+    trace2_one(a, &rays[i], prev_normals ? &prev_normals[3 * i] : NULL, &hits[i],
+               subface ? &subface[i] : NULL, NULL, NULL, &st, &fall);
+    bv += st.branch_visits;
+    lv += st.leaf_visits;
+    pt += st.prim_tests;
+    fb += (uint64_t)fall;
+  }
+  if (stats) {
+    stats[0] = bv;
+    stats[1] = lv;
+    stats[2] = pt;
+    stats[3] = fb;
+  }
+}
+
 /* Trace `n` rays.  prev_normals: 3 floats per ray or NULL.  subface: per-ray
  * output for tetrahedra or NULL.  vscalar/scalar_out: per-vertex scalar and
  * its value at the entering point (tetrahedra).  stats (optional): 3 x uint64

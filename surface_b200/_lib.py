@@ -17,6 +17,7 @@ from . import build as _build
 SRT_OK, SRT_ERR_INVALID, SRT_ERR_CUDA, SRT_ERR_NO_MEMORY, SRT_ERR_LIMIT, SRT_ERR_UNSUPPORTED = range(6)
 SRT_TRIANGLES, SRT_TETRAHEDRA, SRT_SPHERES = 0, 1, 2
 MISS = 0xFFFFFFFF
+SRT_TRACE_SINGLE_PASS = 1
 
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
                       ("prev_t", "<f4")])
@@ -36,7 +37,8 @@ class SurfaceError(RuntimeError):
 class TraceOpts(C.Structure):
     _fields_ = [("prev_normals", C.c_void_p), ("subface", C.c_void_p),
                 ("vertex_scalar", C.c_void_p), ("scalar_out", C.c_void_p),
-                ("normal_out", C.c_void_p), ("stats", C.c_void_p)]
+                ("normal_out", C.c_void_p), ("stats", C.c_void_p),
+                ("flags", C.c_uint32), ("reserved", C.c_uint32)]
 
 
 class AccelInfo(C.Structure):

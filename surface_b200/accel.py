@@ -91,7 +91,9 @@ class Context:
         """Order this context's work on torch's current stream."""
         if torch is not None and torch.cuda.is_available():
             s = torch.cuda.current_stream(self.device).cuda_stream
-            check(self.L.srt_ctx_set_stream(self.h, C.c_void_p(s)))
+            # handle 0 is the legacy default stream; NULL would select the
+            # context's own stream, so pass cudaStreamLegacy (1) instead
+            check(self.L.srt_ctx_set_stream(self.h, C.c_void_p(s if s else 1)))
 
     def use_own_stream(self):
         check(self.L.srt_ctx_set_stream(self.h, None))
@@ -217,8 +219,12 @@ class _Accel:
 
     # -- traversal --------------------------------------------------------
     def Traverse(self, rays, hits=None, prev_normals=None, want_subface=False,
-                 vertex_scalar=None, want_scalar=False, want_normal=False):
-        """Closest hit for every ray (batched XxxAccel::Traverse)."""
+                 vertex_scalar=None, want_scalar=False, want_normal=False,
+                 single_pass=False):
+        """Closest hit for every ray (batched XxxAccel::Traverse).
+
+        single_pass=True walks the tree once in the reference's own order;
+        the default two-pass walk returns the same hits with less work."""
         if not self.built:
             raise SurfaceError(_lib.SRT_ERR_INVALID, "accel not built")
         cuda = _is_cuda(rays)
@@ -255,7 +261,8 @@ class _Accel:
             raise SurfaceError(_lib.SRT_ERR_INVALID, "vertex_scalar must be a CUDA tensor")
         o = TraceOpts(pn.ptr, _View(sub, np.uint32).ptr if sub is not None else None,
                       vs.ptr, _View(sca, np.float32).ptr if sca is not None else None,
-                      _View(nrm, np.float32).ptr if nrm is not None else None)
+                      _View(nrm, np.float32).ptr if nrm is not None else None, None,
+                      _lib.SRT_TRACE_SINGLE_PASS if single_pass else 0, 0)
         check(self.L.srt_trace_closest(self.h, rv.ptr, n, hv.ptr, C.byref(o)))
         if not (want_subface or want_scalar or want_normal):
             return hits

@@ -199,7 +199,8 @@ SRT_API srt_status srt_ctx_destroy(srt_ctx *c) {
   DevBuf *bufs[] = {&c->s_keys2, &c->s_vals2, &c->s_hist, &c->s_scan, &c->s_kchild,
                     &c->s_kflags, &c->s_krange, &c->s_kparent, &c->s_lparent,
                     &c->s_counter, &c->s_ibox, &c->s_flag, &c->s_slot, &c->s_partial,
-                    &c->s_stage_in, &c->s_stage_out, &c->s_stage_aux};
+                    &c->s_stage_in, &c->s_stage_out, &c->s_stage_aux, &c->s_stage_sub,
+                    &c->s_stage_scal, &c->s_stage_norm};
   for (DevBuf *b : bufs) b->release();
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -566,7 +567,6 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
   // outputs: device pointers are written in place, host ones via staging
   const bool hits_dev = is_device_ptr(hits);
   srt_hit *dh = hits;
-  DevBuf tmp_hits, tmp_sub, tmp_scal, tmp_norm;
   cudaError_t e;
   if (!hits_dev) {
     if ((e = ctx->s_stage_out.ensure(n * sizeof(srt_hit))) != cudaSuccess)
@@ -576,16 +576,16 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
   uint32_t *dsub = o.subface;
   float *dscal = o.scalar_out, *dnorm = o.normal_out;
   if (dsub && !is_device_ptr(dsub)) {
-    if ((e = tmp_sub.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
-    dsub = tmp_sub.as<uint32_t>();
+    if ((e = ctx->s_stage_sub.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
+    dsub = ctx->s_stage_sub.as<uint32_t>();
   }
   if (dscal && !is_device_ptr(dscal)) {
-    if ((e = tmp_scal.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
-    dscal = tmp_scal.as<float>();
+    if ((e = ctx->s_stage_scal.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
+    dscal = ctx->s_stage_scal.as<float>();
   }
   if (dnorm && !is_device_ptr(dnorm)) {
-    if ((e = tmp_norm.ensure(n * 12)) != cudaSuccess) return cuda_status(e, "staging");
-    dnorm = tmp_norm.as<float>();
+    if ((e = ctx->s_stage_norm.ensure(n * 12)) != cudaSuccess) return cuda_status(e, "staging");
+    dnorm = ctx->s_stage_norm.as<float>();
   }
   if ((reinterpret_cast<uintptr_t>(drays) | reinterpret_cast<uintptr_t>(dh)) & 15u) {
     set_error("ray and hit arrays must be 16-byte aligned");
@@ -597,7 +597,7 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
   }
   s = launch_trace(a, static_cast<const srt_ray *>(drays), n, dh,
                    static_cast<const float *>(dpn), dsub, static_cast<const float *>(dvs),
-                   dscal, dnorm, o.stats);
+                   dscal, dnorm, o.stats, o.flags);
   if (s != SRT_OK) return s;
   cudaStream_t st = ctx->stream;
   bool any_host = !hits_dev || (dsub != o.subface) || (dscal != o.scalar_out) ||

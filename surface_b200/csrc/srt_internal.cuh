@@ -120,7 +120,7 @@ struct srt_ctx {
   // scratch shared by the builds of this context (stream ordered)
   srt::DevBuf s_keys2, s_vals2, s_hist, s_scan, s_kchild, s_kflags, s_krange,
       s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
-      s_stage_in, s_stage_out, s_stage_aux;
+      s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm;
 };
 
 struct srt_accel {
@@ -163,5 +163,5 @@ srt_status launch_trace(srt_accel *a, const srt_ray *d_rays, size_t n,
                         srt_hit *d_hits, const float *d_prev_normals,
                         uint32_t *d_subface, const float *d_vertex_scalar,
                         float *d_scalar_out, float *d_normal_out,
-                        unsigned long long *d_stats);
+                        unsigned long long *d_stats, uint32_t flags);
 }  // namespace srt

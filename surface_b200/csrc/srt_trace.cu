@@ -1,7 +1,7 @@
 // srt_trace.cu -- closest-hit traversal, one ray per thread.
 //
-// Each kernel reproduces the reference's Traverse() step for step, so hits
-// (including which of several equal-t primitives wins) match bit for bit:
+// The hits are exactly the reference's Traverse() results, tie-breaking
+// included:
 //   triangles  TriangleAccel::Traverse  render/render_accel_triangle.cc:2511-2669
 //              IntersectRayAABB :1815-1861, TriangleIsect :1887-1938,
 //              TestLeafNode :1994-2437, BuildIntersection :2439-2507
@@ -10,8 +10,21 @@
 //              RayTetraPluecker :243-567 (FP64), ComputeParametricDist :123-139
 //   spheres    ParticleAccel::Traverse  render/render_accel_particle.cc:3053-3218
 //              SphereIsect :2423-2512, BuildIntersection :2968-3049
-// The stack discipline (far child pushed first, near child popped next,
-// near = dirSign[axis]) and the per-node hitT culling are the reference's.
+//
+// The reference walks depth first, near child = dirSign[axis] with its
+// axis taken from (clz(code) - 2) % 3, and prunes boxes entered after its
+// current hit.  Its answer is the sequential scan, in that order, of every
+// primitive the ray hits, provided no primitive reports a distance before
+// its own leaf box's entry (then no pruning ever hides an acceptable
+// primitive).  The default walk therefore goes front to back (pass 1),
+// finds m, the smallest hit distance, and counts the primitives at m
+// (tetrahedra: within 8 float steps, since the reference compares a double
+// distance with its float-rounded current one).  One such primitive is the
+// answer; several -- an exact tie -- are ordered by the reference-order walk
+// restricted to boxes entered before m.  A primitive hit before its leaf
+// box's entry sends the ray through the reference's own walk.  The
+// single-pass kernels (SRT_TRACE_SINGLE_PASS) run that walk for every ray.
+//
 // Leaves are folded into their parent's child slot for triangles/spheres;
 // a hit leaf is pushed as a (first primitive, count) entry, which visits
 // leaves in exactly the reference's order.
@@ -303,8 +316,209 @@ __device__ __forceinline__ void normalize_ref(float n[3]) {
   for (int k = 0; k < 3; k++) n[k] = (float)((double)n[k] * len);
 }
 
+
+// IntersectRayAABB that also reports the box entry distance.
+template <bool CLAMP>
+__device__ __forceinline__ bool ray_aabb_t(float maxT, float lx, float ly, float lz,
+                                           float hx, float hy, float hz, const RayF &r,
+                                           float &tmin_out) {
+  const float min_x = r.sgn[0] ? hx : lx;
+  const float min_y = r.sgn[1] ? hy : ly;
+  const float min_z = r.sgn[2] ? hz : lz;
+  const float max_x = r.sgn[0] ? lx : hx;
+  const float max_y = r.sgn[1] ? ly : hy;
+  const float max_z = r.sgn[2] ? lz : hz;
+  const float tmin_x = (min_x - r.o[0]) * r.inv[0];
+  const float tmax_x = (max_x - r.o[0]) * r.inv[0];
+  const float tmin_y = (min_y - r.o[1]) * r.inv[1];
+  const float tmax_y = (max_y - r.o[1]) * r.inv[1];
+  float tmin = (tmin_x > tmin_y) ? tmin_x : tmin_y;
+  float tmax = (tmax_x < tmax_y) ? tmax_x : tmax_y;
+  const float tmin_z = (min_z - r.o[2]) * r.inv[2];
+  const float tmax_z = (max_z - r.o[2]) * r.inv[2];
+  tmin = (tmin > tmin_z) ? tmin : tmin_z;
+  tmax = (tmax < tmax_z) ? tmax : tmax_z;
+  tmin_out = tmin;
+  if (CLAMP) {
+    tmax = (maxT < tmax) ? maxT : tmax;
+    return (tmax > 0.0f) && (tmin <= tmax);
+  }
+  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= maxT);
+}
+
+// --------------------------------------------------------------- walks
+// Tree walks shared by the kernels.  Every walk is "while-while": a lane
+// stops at its next leaf and the leaf's primitives are tested when all
+// lanes of the warp hold one, so the primitive tests run on full warps.
+
+// Relative pruning margins above the smallest hit distance m: boxes entered
+// before m * (1 + rel) are walked.  Float triangle and sphere distances can
+// err by ~1e-4 relative (ill-conditioned quadratic, grazing hits), so they
+// get 2^-8; the FP64 tetrahedron distance is exact to ~1e-15 and the leaf
+// padding is 16 ulp(1), so 2^-16 suffices.
+constexpr float kRelTri = 3.90625e-3f;          // 2^-8
+constexpr float kRelTet = 1.52587890625e-5f;    // 2^-16
+constexpr float kViolTol = 4.76837158203125e-7f; // 2^-21
+
+__device__ __forceinline__ float bound_rel(float m, float rel) {
+  return (m < FLT_MAX) ? m + fabsf(m) * rel + 1e-30f : FLT_MAX;
+}
+
+// A hit distance below (or within rounding of) the entry distance of its
+// own leaf box: the reference's pruning may then hide a primitive, so the
+// ray takes the reference's walk.
+__device__ __forceinline__ bool below_entry(double t, float entry) {
+  return t < (double)entry + fabs((double)entry) * (double)kViolTol;
+}
+
+struct Work {
+  uint32_t branch = 0, leaf = 0, prim = 0, it = 0;
+  bool fail = false;
+};
+
+struct Best {
+  float t = FLT_MAX, u = 0.0f, v = 0.0f;
+  uint32_t prim = kNone, j = kNone;
+  uint32_t sub = 0;
+  double e1 = 0.0, e2 = 0.0;
+};
+
+// Per-ray context of the two-child walks.
+struct Ctx2 {
+  RayF r;
+  uint32_t prev_prim;
+  float prev_t;
+  float pn[3];
+  float keps;
+};
+
+// Hit distance of sorted primitive j (two-child kinds), FLT_MAX on a miss.
+template <int KIND>
+__device__ __forceinline__ bool cand2(const float4 *__restrict__ prims,
+                                      const uint32_t *__restrict__ sidx, uint32_t j,
+                                      const Ctx2 &c, float tio, float &t, float &u, float &v,
+                                      uint32_t &f) {
+  if (KIND == SRT_TRIANGLES) {
+    const float4 q0 = __ldg(&prims[3 * (size_t)j]);
+    f = __float_as_uint(q0.w);
+    if (f == c.prev_prim) return false;
+    const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
+    const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
+    const float p0[3] = {q0.x, q0.y, q0.z}, p1[3] = {q1.x, q1.y, q1.z},
+                p2[3] = {q2.x, q2.y, q2.z};
+    t = tio;
+    return tri_isect(t, u, v, p0, p1, p2, c.r, c.keps);
+  } else {
+    const float4 s = __ldg(&prims[j]);
+    f = __ldg(&sidx[j]);
+    const float c3[3] = {s.x, s.y, s.z};
+    t = tio;
+    u = v = 0.0f;
+    return sphere_isect(t, c3, s.w, c.r, c.prev_t, c.pn, c.prev_prim == f);
+  }
+}
+
+// The reference's Traverse, step for step (render/render_accel_triangle.cc:2511,
+// render/render_accel_particle.cc:3053).
+template <int KIND>
+__device__ void ref_walk2(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
+                          const uint32_t *__restrict__ sidx, const Ctx2 &c, Best &b,
+                          Work &w, uint32_t max_iter) {
+  b = Best();
+  uint2 stk[kStack];
+  int sp = 0;
+  stk[0] = make_uint2(0u, 0u);
+  while (true) {
+    uint2 leaf = make_uint2(0u, 0u);
+    while (sp >= 0) {
+      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+      const uint2 e = stk[sp--];
+      if (e.y != 0) { leaf = e; break; }
+      w.branch++;
+      const float4 *np = reinterpret_cast<const float4 *>(nodes + e.x);
+      const float4 a = __ldg(np), bb = __ldg(np + 1), cc = __ldg(np + 2);
+      const uint4 d = __ldg(reinterpret_cast<const uint4 *>(np + 3));
+      bool h[2];
+      h[0] = ray_aabb<true>(b.t, a.x, a.y, a.z, a.w, bb.x, bb.y, c.r);
+      h[1] = ray_aabb<true>(b.t, bb.z, bb.w, cc.x, cc.y, cc.z, cc.w, c.r);
+      if (h[0] || h[1]) {
+        const int nearc = c.r.sgn[d.z >> 30], farc = 1 - nearc;
+        const uint2 ce[2] = {make_uint2(d.x, d.z & kCountMask),
+                             make_uint2(d.y, d.w & kCountMask)};
+        if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+        if (h[farc]) stk[++sp] = ce[farc];
+        if (h[nearc]) stk[++sp] = ce[nearc];
+      }
+    }
+    if (leaf.y == 0) break;
+    w.leaf++;
+    w.prim += leaf.y;
+    float t = b.t;
+    for (uint32_t j = leaf.x; j < leaf.x + leaf.y; j++) {
+      float u, v;
+      uint32_t f;
+      if (cand2<KIND>(prims, sidx, j, c, t, t, u, v, f)) {
+        b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
+      }
+    }
+  }
+}
+
+// Reference order through boxes entered before `bnd`, accepting from `t0`
+// on (the candidates at m).
+template <int KIND>
+__device__ void window_walk2(const Node2 *__restrict__ nodes,
+                             const float4 *__restrict__ prims,
+                             const uint32_t *__restrict__ sidx, const Ctx2 &c, float bnd,
+                             float t0, Best &b, Work &w, uint32_t max_iter) {
+  b = Best();
+  float t = t0;
+  uint2 stk[kStack];
+  int sp = 0;
+  stk[0] = make_uint2(0u, 0u);
+  while (true) {
+    uint2 leaf = make_uint2(0u, 0u);
+    while (sp >= 0) {
+      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+      const uint2 e = stk[sp--];
+      if (e.y != 0) { leaf = e; break; }
+      w.branch++;
+      const float4 *np = reinterpret_cast<const float4 *>(nodes + e.x);
+      const float4 a = __ldg(np), bb = __ldg(np + 1), cc = __ldg(np + 2);
+      const uint4 d = __ldg(reinterpret_cast<const uint4 *>(np + 3));
+      bool h[2];
+      h[0] = ray_aabb<true>(bnd, a.x, a.y, a.z, a.w, bb.x, bb.y, c.r);
+      h[1] = ray_aabb<true>(bnd, bb.z, bb.w, cc.x, cc.y, cc.z, cc.w, c.r);
+      if (h[0] || h[1]) {
+        const int nearc = c.r.sgn[d.z >> 30], farc = 1 - nearc;
+        const uint2 ce[2] = {make_uint2(d.x, d.z & kCountMask),
+                             make_uint2(d.y, d.w & kCountMask)};
+        if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+        if (h[farc]) stk[++sp] = ce[farc];
+        if (h[nearc]) stk[++sp] = ce[nearc];
+      }
+    }
+    if (leaf.y == 0) break;
+    w.leaf++;
+    w.prim += leaf.y;
+    for (uint32_t j = leaf.x; j < leaf.x + leaf.y; j++) {
+      float u, v;
+      uint32_t f;
+      if (cand2<KIND>(prims, sidx, j, c, t, t, u, v, f)) {
+        b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
+      }
+    }
+  }
+}
+
 // --------------------------------------------------------------- kernels
-template <int KIND>  // SRT_TRIANGLES or SRT_SPHERES
+// Two-child kinds (triangles, spheres).  Default: pass 1 walks front to
+// back and finds m, the smallest hit distance, counting the primitives that
+// hit exactly at m; one such primitive is the reference's answer, several
+// (an exact tie) are ordered by a reference-order walk restricted to boxes
+// entered before m.  A primitive hit before its own leaf box's entry sends
+// the ray through the reference's walk.  SINGLE: the reference's walk only.
+template <int KIND, bool SINGLE>
 __global__ void __launch_bounds__(128)
 trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
                    const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
@@ -313,123 +527,117 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
                    const float *__restrict__ prev_normals, float *__restrict__ normal_out,
                    unsigned long long *__restrict__ stats, uint32_t max_iter,
                    uint32_t *__restrict__ err) {
-  uint32_t n_branch = 0, n_leaf = 0, n_prim = 0;
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  uint32_t prev_prim;
-  float prev_t;
-  const RayF r = load_ray(rays, i, prev_prim, prev_t);
-  const float keps = scene->keps;
-  float pn[3] = {0.0f, 0.0f, 0.0f};
-  if (KIND == SRT_SPHERES && prev_normals && prev_prim != kNone) {
-    pn[0] = prev_normals[3 * i];
-    pn[1] = prev_normals[3 * i + 1];
-    pn[2] = prev_normals[3 * i + 2];
+  Ctx2 c;
+  c.r = load_ray(rays, i, c.prev_prim, c.prev_t);
+  c.keps = scene->keps;
+  c.pn[0] = c.pn[1] = c.pn[2] = 0.0f;
+  if (KIND == SRT_SPHERES && prev_normals && c.prev_prim != kNone) {
+    c.pn[0] = prev_normals[3 * i];
+    c.pn[1] = prev_normals[3 * i + 1];
+    c.pn[2] = prev_normals[3 * i + 2];
   }
-  float best_t = FLT_MAX, best_u = 0.0f, best_v = 0.0f;
-  uint32_t best_prim = kNone, best_j = kNone;
-  uint2 stk[kStack];
-  int sp = 0;
-  stk[0] = make_uint2(0u, 0u);
-  uint32_t it = 0;
-  while (sp >= 0) {
-    if (++it > max_iter) {
-      atomicOr(err, kErrIter);
-      break;
-    }
-    const uint2 e = stk[sp--];
-    if (e.y == 0) {
-      n_branch++;
-      const float4 *np = reinterpret_cast<const float4 *>(nodes + e.x);
-      const float4 a = __ldg(np), b = __ldg(np + 1), c = __ldg(np + 2);
-      const uint4 d = __ldg(reinterpret_cast<const uint4 *>(np + 3));
-      const float hitT = best_t;
-      bool h[2];
-      h[0] = ray_aabb<true>(hitT, a.x, a.y, a.z, a.w, b.x, b.y, r);
-      h[1] = ray_aabb<true>(hitT, b.z, b.w, c.x, c.y, c.z, c.w, r);
-      if (h[0] || h[1]) {
-        const int axis = (int)(d.z >> 30);
-        const int nearc = r.sgn[axis], farc = 1 - nearc;
-        const uint2 ce[2] = {make_uint2(d.x, d.z & kCountMask),
-                             make_uint2(d.y, d.w & kCountMask)};
-        if (sp + 2 >= kStack) {
-          atomicOr(err, kErrStack);
-          break;
-        }
-        if (h[farc]) stk[++sp] = ce[farc];
-        if (h[nearc]) stk[++sp] = ce[nearc];
-      }
-    } else {
-      n_leaf++;
-      n_prim += e.y;
-      float t = best_t;
-      for (uint32_t j = e.x; j < e.x + e.y; j++) {
-        if (KIND == SRT_TRIANGLES) {
-          const float4 q0 = __ldg(&prims[3 * (size_t)j]);
-          const uint32_t f = __float_as_uint(q0.w);
-          if (f == prev_prim) continue;
-          const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
-          const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
-          const float p0[3] = {q0.x, q0.y, q0.z};
-          const float p1[3] = {q1.x, q1.y, q1.z};
-          const float p2[3] = {q2.x, q2.y, q2.z};
-          float u, v;
-          if (tri_isect(t, u, v, p0, p1, p2, r, keps)) {
-            best_t = t;
-            best_u = u;
-            best_v = v;
-            best_prim = f;
-            best_j = j;
-          }
-        } else {
-          const float4 s = __ldg(&prims[j]);
-          const uint32_t f = __ldg(&sidx[j]);
-          const float c[3] = {s.x, s.y, s.z};
-          if (sphere_isect(t, c, s.w, r, prev_t, pn, prev_prim == f)) {
-            best_t = t;
-            best_prim = f;
-            best_j = j;
-          }
-        }
-      }
-    }
-  }
-  if (stats) {
-    atomicAdd(&stats[0], (unsigned long long)n_branch);
-    atomicAdd(&stats[1], (unsigned long long)n_leaf);
-    atomicAdd(&stats[2], (unsigned long long)n_prim);
-  }
-  srt_hit h;
-  if (best_t < FLT_MAX) {
-    h.t = best_t;
-    h.u = best_u;
-    h.v = best_v;
-    h.prim = best_prim;
+  Work w;
+  Best b;
+  uint32_t fallback = 0;
+  if (SINGLE) {
+    ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
   } else {
-    h.t = FLT_MAX;
-    h.u = 0.0f;
-    h.v = 0.0f;
-    h.prim = kNone;
+    // ---- pass 1
+    float m = FLT_MAX;
+    uint32_t at_m = 0;
+    bool viol = false;
+    uint2 stk[kStack];
+    float stt[kStack];
+    int sp = 0;
+    stk[0] = make_uint2(0u, 0u);
+    stt[0] = -FLT_MAX;
+    while (true) {
+      uint2 leaf = make_uint2(0u, 0u);
+      float lt = 0.0f;
+      while (sp >= 0) {
+        if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+        const uint2 e = stk[sp];
+        const float et = stt[sp];
+        sp--;
+        const float bnd = bound_rel(m, kRelTri);
+        if (et > bnd) continue;
+        if (e.y != 0) { leaf = e; lt = et; break; }
+        w.branch++;
+        const float4 *np = reinterpret_cast<const float4 *>(nodes + e.x);
+        const float4 a = __ldg(np), bb = __ldg(np + 1), cc = __ldg(np + 2);
+        const uint4 d = __ldg(reinterpret_cast<const uint4 *>(np + 3));
+        float t0, t1;
+        const bool h0 = ray_aabb_t<true>(bnd, a.x, a.y, a.z, a.w, bb.x, bb.y, c.r, t0);
+        const bool h1 = ray_aabb_t<true>(bnd, bb.z, bb.w, cc.x, cc.y, cc.z, cc.w, c.r, t1);
+        const uint2 e0 = make_uint2(d.x, d.z & kCountMask),
+                    e1 = make_uint2(d.y, d.w & kCountMask);
+        if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+        if (h0 && h1) {
+          const bool first1 = t1 < t0;
+          stk[++sp] = first1 ? e0 : e1; stt[sp] = first1 ? t0 : t1;
+          stk[++sp] = first1 ? e1 : e0; stt[sp] = first1 ? t1 : t0;
+        } else if (h0) {
+          stk[++sp] = e0; stt[sp] = t0;
+        } else if (h1) {
+          stk[++sp] = e1; stt[sp] = t1;
+        }
+      }
+      if (leaf.y == 0) break;
+      w.leaf++;
+      w.prim += leaf.y;
+      for (uint32_t j = leaf.x; j < leaf.x + leaf.y; j++) {
+        float t, u, v;
+        uint32_t f;
+        if (!cand2<KIND>(prims, sidx, j, c, FLT_MAX, t, u, v, f)) continue;
+        if (below_entry(t, lt)) viol = true;
+        if (t < m) {
+          m = t;
+          at_m = 1;
+          b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
+        } else if (t == m) {
+          at_m++;
+        }
+      }
+    }
+    if (viol && !w.fail) {
+      ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
+      fallback = 1;
+    } else if (at_m > 1 && !w.fail) {
+      // triangles keep the last candidate at m (t <= current), spheres the
+      // first (t < current)
+      const float t0 = (KIND == SRT_TRIANGLES) ? m : nextafterf(m, FLT_MAX);
+      window_walk2<KIND>(nodes, prims, sidx, c, bound_rel(m, kRelTri), t0, b, w, max_iter);
+    }
   }
+  if (w.fail) atomicOr(err, kErrIter);
+  if (stats) {
+    atomicAdd(&stats[0], (unsigned long long)w.branch);
+    atomicAdd(&stats[1], (unsigned long long)w.leaf);
+    atomicAdd(&stats[2], (unsigned long long)w.prim);
+    if (fallback) atomicAdd(&stats[3], 1ull);
+  }
+  const bool any = b.t < FLT_MAX && b.prim != kNone;
   reinterpret_cast<float4 *>(hits)[i] =
-      make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
+                  __uint_as_float(any ? b.prim : kNone));
   if (normal_out) {
     float nn[3] = {0.0f, 0.0f, 0.0f};
-    if (best_j != kNone) {
+    if (any) {
       if (KIND == SRT_TRIANGLES) {
-        const float4 q0 = prims[3 * (size_t)best_j];
-        const float4 q1 = prims[3 * (size_t)best_j + 1];
-        const float4 q2 = prims[3 * (size_t)best_j + 2];
+        const float4 q0 = prims[3 * (size_t)b.j];
+        const float4 q1 = prims[3 * (size_t)b.j + 1];
+        const float4 q2 = prims[3 * (size_t)b.j + 2];
         const float e1[3] = {q1.x - q0.x, q1.y - q0.y, q1.z - q0.z};
         const float e2[3] = {q2.x - q0.x, q2.y - q0.y, q2.z - q0.z};
         cross3(e1, e2, nn);
         normalize_ref(nn);
       } else {
-        const float4 s = prims[best_j];
-        const float c[3] = {s.x, s.y, s.z};
-        // position = org + t * dir; vnormalize(position - centre)
+        const float4 s = prims[b.j];
+        const float c3[3] = {s.x, s.y, s.z};
 #pragma unroll
-        for (int k = 0; k < 3; k++) nn[k] = (r.o[k] + best_t * r.d[k]) - c[k];
+        for (int k = 0; k < 3; k++) nn[k] = (c.r.o[k] + b.t * c.r.d[k]) - c3[k];
         const float len = sqrtf(dot3(nn, nn));
         if (len > FLT_EPSILON * 16) {
           const float il = __frcp_rn(len);
@@ -444,6 +652,91 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
   }
 }
 
+// ---- tetrahedra (own-box nodes, FP64 entry distance)
+struct CtxT {
+  RayF r;
+  D3 o, d;
+  uint32_t prev_prim;
+};
+
+__device__ __forceinline__ bool candT(const float4 *__restrict__ prims,
+                                      const uint32_t *__restrict__ sidx, uint32_t j,
+                                      const CtxT &c, uint32_t &f, int &ef, double &e1,
+                                      double &e2, double &ul1, double &te) {
+  f = __ldg(&sidx[j]);
+  if (f == c.prev_prim) return false;
+  const float4 q0 = __ldg(&prims[3 * (size_t)j]);
+  const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
+  const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
+  const D3 V[4] = {{q0.x, q0.y, q0.z}, {q0.w, q1.x, q1.y}, {q1.z, q1.w, q2.x},
+                   {q2.y, q2.z, q2.w}};
+  return ray_tet(c.o, c.d, V, ef, e1, e2, ul1, te) && te >= 0.0;
+}
+
+__device__ __forceinline__ void take_tet(Best &b, double te, double e1, double e2,
+                                         double ul1, uint32_t f, int ef) {
+  b.t = (float)te;
+  b.u = (float)e1;
+  b.v = (float)ul1;  // the reference's isect.v receives uLeave1
+  b.prim = f;
+  b.sub = (uint32_t)ef;
+  b.e1 = e1;
+  b.e2 = e2;
+}
+
+// The reference's walk (render/render_accel_tetra.cc:2200) or, with
+// WINDOW, the reference order through boxes entered before `bnd` keeping
+// only candidates at most `whi` away.
+template <bool WINDOW>
+__device__ void walkT(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
+                      const uint32_t *__restrict__ sidx, const CtxT &c, float bnd,
+                      double whi, Best &b, Work &w, uint32_t max_iter) {
+  b = Best();
+  float t = FLT_MAX;
+  uint32_t stk[kStack];
+  int sp = 0;
+  stk[0] = 0u;
+  while (true) {
+    uint32_t lref = 0, lcnt = 0;
+    while (sp >= 0) {
+      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+      const uint32_t ni = stk[sp--];
+      const float4 *np = reinterpret_cast<const float4 *>(nodes + ni);
+      const float4 a = __ldg(np), bb = __ldg(np + 1);
+      const uint32_t meta = __float_as_uint(a.w), ref = __float_as_uint(bb.w);
+      w.branch++;
+      if (!ray_aabb<false>(WINDOW ? bnd : t, a.x, a.y, a.z, bb.x, bb.y, bb.z, c.r)) continue;
+      if (meta & kLeafBit) { lref = ref; lcnt = meta & kCountMask; break; }
+      const int nearc = c.r.sgn[meta & 3u], farc = 1 - nearc;
+      if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+      stk[++sp] = ref + (uint32_t)farc;
+      stk[++sp] = ref + (uint32_t)nearc;
+    }
+    if (lcnt == 0) break;
+    w.leaf++;
+    w.prim += lcnt;
+    for (uint32_t j = lref; j < lref + lcnt; j++) {
+      uint32_t f;
+      int ef;
+      double e1, e2, ul1, te;
+      if (!candT(prims, sidx, j, c, f, ef, e1, e2, ul1, te)) continue;
+      if (WINDOW && !(te <= whi)) continue;
+      if (te < (double)t) {
+        take_tet(b, te, e1, e2, ul1, f, ef);
+        t = (float)te;
+      }
+    }
+  }
+}
+
+__device__ __forceinline__ double window_hi(double m) {
+  float wf = __double2float_rn(m);
+#pragma unroll
+  for (int k = 0; k < 8; k++) wf = nextafterf(wf, FLT_MAX);
+  return (double)wf;
+}
+
+template <bool SINGLE>
 __global__ void __launch_bounds__(128)
 trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
                  const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
@@ -451,93 +744,124 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
                  const uint32_t *__restrict__ faces, const float *__restrict__ vscalar,
                  float *__restrict__ scalar_out, unsigned long long *__restrict__ stats,
                  uint32_t max_iter, uint32_t *__restrict__ err) {
-  uint32_t n_branch = 0, n_leaf = 0, n_prim = 0;
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  uint32_t prev_prim;
+  CtxT c;
   float prev_t;
-  const RayF r = load_ray(rays, i, prev_prim, prev_t);
-  const D3 o = {r.o[0], r.o[1], r.o[2]};
-  const D3 dd = {r.d[0], r.d[1], r.d[2]};
-  float best_t = FLT_MAX, best_u = 0.0f, best_v = 0.0f;
-  uint32_t best_prim = kNone, best_sub = 0;
-  double best_e1 = 0.0, best_e2 = 0.0;
-  uint32_t stk[kStack];
-  int sp = 0;
-  stk[0] = 0u;
-  uint32_t it = 0;
-  while (sp >= 0) {
-    if (++it > max_iter) {
-      atomicOr(err, kErrIter);
-      break;
-    }
-    const uint32_t ni = stk[sp--];
-    const float4 *np = reinterpret_cast<const float4 *>(nodes + ni);
-    const float4 a = __ldg(np), b = __ldg(np + 1);
-    const uint32_t meta = __float_as_uint(a.w), ref = __float_as_uint(b.w);
-    const bool hit = ray_aabb<false>(best_t, a.x, a.y, a.z, b.x, b.y, b.z, r);
-    n_branch++;  // every popped node is box-tested (the reference's numNodeTraversals
-                 // counts the hit branches only)
-    if (!(meta & kLeafBit)) {
-      if (hit) {
-        const int nearc = r.sgn[meta & 3u], farc = 1 - nearc;
-        if (sp + 2 >= kStack) {
-          atomicOr(err, kErrStack);
-          break;
-        }
-        stk[++sp] = ref + (uint32_t)farc;
-        stk[++sp] = ref + (uint32_t)nearc;
+  c.r = load_ray(rays, i, c.prev_prim, prev_t);
+  c.o = {c.r.o[0], c.r.o[1], c.r.o[2]};
+  c.d = {c.r.d[0], c.r.d[1], c.r.d[2]};
+  Work w;
+  Best b;
+  uint32_t fallback = 0;
+  if (SINGLE) {
+    walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+  } else {
+    // ---- pass 1: front to back; window list = entry distances within 8
+    // float steps of the running minimum m (kept for the tie count)
+    double m = DBL_MAX;
+    double wl[4];
+    int nwin = 0;
+    bool overflow = false, viol = false;
+    uint32_t stk[kStack];
+    float stt[kStack];
+    int sp = -1;
+    {
+      const float4 *np = reinterpret_cast<const float4 *>(nodes);
+      const float4 a = __ldg(np), bb = __ldg(np + 1);
+      float t0;
+      if (ray_aabb_t<false>(FLT_MAX, a.x, a.y, a.z, bb.x, bb.y, bb.z, c.r, t0)) {
+        stk[0] = 0u;
+        stt[0] = t0;
+        sp = 0;
       }
-    } else if (hit) {
-      const uint32_t cnt = meta & kCountMask;
-      n_leaf++;
-      n_prim += cnt;
-      float t = best_t;
-      for (uint32_t j = ref; j < ref + cnt; j++) {
-        const uint32_t f = __ldg(&sidx[j]);
-        if (f == prev_prim) continue;
-        const float4 q0 = __ldg(&prims[3 * (size_t)j]);
-        const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
-        const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
-        const D3 V[4] = {{q0.x, q0.y, q0.z}, {q0.w, q1.x, q1.y},
-                         {q1.z, q1.w, q2.x}, {q2.y, q2.z, q2.w}};
+    }
+    while (true) {
+      uint32_t lref = 0, lcnt = 0;
+      float lt = 0.0f;
+      while (sp >= 0) {
+        if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+        const uint32_t ni = stk[sp];
+        const float et = stt[sp];
+        sp--;
+        const float bnd = (m < DBL_MAX) ? bound_rel((float)m, kRelTet) : FLT_MAX;
+        if (et > bnd) continue;
+        const float4 *np = reinterpret_cast<const float4 *>(nodes + ni);
+        const uint32_t meta = __float_as_uint(__ldg(&np[0].w));
+        const uint32_t ref = __float_as_uint(__ldg(&np[1].w));
+        if (meta & kLeafBit) { lref = ref; lcnt = meta & kCountMask; lt = et; break; }
+        w.branch++;
+        // the two children are adjacent: test their own boxes here
+        const float4 *cp = reinterpret_cast<const float4 *>(nodes + ref);
+        const float4 a0 = __ldg(cp), b0 = __ldg(cp + 1), a1 = __ldg(cp + 2), b1 = __ldg(cp + 3);
+        float t0, t1;
+        const bool h0 = ray_aabb_t<false>(bnd, a0.x, a0.y, a0.z, b0.x, b0.y, b0.z, c.r, t0);
+        const bool h1 = ray_aabb_t<false>(bnd, a1.x, a1.y, a1.z, b1.x, b1.y, b1.z, c.r, t1);
+        if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+        if (h0 && h1) {
+          const bool first1 = t1 < t0;
+          stk[++sp] = first1 ? ref : ref + 1; stt[sp] = first1 ? t0 : t1;
+          stk[++sp] = first1 ? ref + 1 : ref; stt[sp] = first1 ? t1 : t0;
+        } else if (h0) {
+          stk[++sp] = ref; stt[sp] = t0;
+        } else if (h1) {
+          stk[++sp] = ref + 1; stt[sp] = t1;
+        }
+      }
+      if (lcnt == 0) break;
+      w.leaf++;
+      w.prim += lcnt;
+      for (uint32_t j = lref; j < lref + lcnt; j++) {
+        uint32_t f;
         int ef;
-        double ue1, ue2, ul1, te;
-        if (ray_tet(o, dd, V, ef, ue1, ue2, ul1, te)) {
-          if ((te >= 0.0) && (te < (double)t)) {
-            best_t = (float)te;
-            best_u = (float)ue1;
-            best_v = (float)ul1;  // the reference's isect.v receives uLeave1
-            best_prim = f;
-            best_sub = (uint32_t)ef;
-            best_e1 = ue1;
-            best_e2 = ue2;
-            t = (float)te;
-          }
+        double e1, e2, ul1, te;
+        if (!candT(prims, sidx, j, c, f, ef, e1, e2, ul1, te)) continue;
+        if (below_entry(te, lt)) viol = true;
+        if (te < m) {
+          m = te;
+          take_tet(b, te, e1, e2, ul1, f, ef);
+          const double whi = window_hi(m);
+          int k2 = 0;
+          for (int k = 0; k < nwin; k++)
+            if (wl[k] <= whi) wl[k2++] = wl[k];
+          nwin = k2;
+        }
+        if (te <= window_hi(m)) {
+          if (nwin < 4) wl[nwin++] = te;
+          else overflow = true;
         }
       }
     }
+    if (viol && !w.fail) {
+      walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+      fallback = 1;
+    } else if ((nwin > 1 || overflow) && !w.fail) {
+      const double whi = window_hi(m);
+      walkT<true>(nodes, prims, sidx, c, bound_rel((float)whi, kRelTet), whi, b, w, max_iter);
+    }
   }
+  if (w.fail) atomicOr(err, kErrIter);
   if (stats) {
-    atomicAdd(&stats[0], (unsigned long long)n_branch);
-    atomicAdd(&stats[1], (unsigned long long)n_leaf);
-    atomicAdd(&stats[2], (unsigned long long)n_prim);
+    atomicAdd(&stats[0], (unsigned long long)w.branch);
+    atomicAdd(&stats[1], (unsigned long long)w.leaf);
+    atomicAdd(&stats[2], (unsigned long long)w.prim);
+    if (fallback) atomicAdd(&stats[3], 1ull);
   }
-  const bool any = best_t < FLT_MAX;
+  const bool any = b.t < FLT_MAX && b.prim != kNone;
   reinterpret_cast<float4 *>(hits)[i] =
-      make_float4(any ? best_t : FLT_MAX, any ? best_u : 0.0f, any ? best_v : 0.0f,
-                  __uint_as_float(any ? best_prim : kNone));
-  if (subface) subface[i] = any ? best_sub : 0u;
+      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
+                  __uint_as_float(any ? b.prim : kNone));
+  if (subface) subface[i] = any ? b.sub : 0u;
   if (scalar_out) {
     float s = 0.0f;
     if (any && faces && vscalar) {
       // entering face vertex order (A, B, C) per face id, as the Pluecker
-      // test's barycentric points are formed
+      // test forms its barycentric point
       const int fA[4] = {3, 2, 1, 0}, fB[4] = {2, 3, 0, 1}, fC[4] = {1, 0, 3, 2};
-      const uint32_t *tv = faces + 4 * (size_t)best_prim;
-      const double sa = vscalar[tv[fA[best_sub]]], sb = vscalar[tv[fB[best_sub]]],
-                   sc = vscalar[tv[fC[best_sub]]];
-      s = (float)((1.0 - best_e1 - best_e2) * sa + best_e1 * sb + best_e2 * sc);
+      const uint32_t *tv = faces + 4 * (size_t)b.prim;
+      const double sa = vscalar[tv[fA[b.sub]]], sb = vscalar[tv[fB[b.sub]]],
+                   sc = vscalar[tv[fC[b.sub]]];
+      s = (float)((1.0 - b.e1 - b.e2) * sa + b.e1 * sb + b.e2 * sc);
     }
     scalar_out[i] = s;
   }
@@ -548,31 +872,38 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
 srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hits,
                         const float *prev_normals, uint32_t *subface,
                         const float *vscalar, float *scalar_out, float *normal_out,
-                        unsigned long long *stats) {
+                        unsigned long long *stats, uint32_t flags) {
   if (n == 0) return SRT_OK;
   srt_ctx *ctx = a->ctx;
   const int block = 128;
   const unsigned grid = (unsigned)((n + block - 1) / block);
-  // each node and leaf is visited at most once per ray
-  const uint32_t max_iter = (uint32_t)std::min<size_t>(4 * a->n + 64, 0xfffffff0u);
+  // every node and leaf is visited at most once per walk; at most three walks
+  const uint32_t max_iter = (uint32_t)std::min<size_t>(12 * a->n + 64, 0xfffffff0u);
   const SceneInfo *scene = a->scene.as<SceneInfo>();
+  const bool single = (flags & SRT_TRACE_SINGLE_PASS) != 0;
+  cudaStream_t st = ctx->stream;
+#define SRT_NODE2(KIND, S)                                                             \
+  trace_node2_kernel<KIND, S><<<grid, block, 0, st>>>(                                 \
+      a->nodes.as<Node2>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n, \
+      hits, scene, KIND == SRT_SPHERES ? prev_normals : nullptr, normal_out, stats,    \
+      max_iter, ctx->d_err)
+#define SRT_TET(S)                                                                     \
+  trace_tet_kernel<S><<<grid, block, 0, st>>>(                                         \
+      a->nodes.as<NodeT>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n, \
+      hits, subface, a->src_faces, vscalar, scalar_out, stats, max_iter, ctx->d_err)
   switch (a->kind) {
     case SRT_TRIANGLES:
-      trace_node2_kernel<SRT_TRIANGLES><<<grid, block, 0, ctx->stream>>>(
-          a->nodes.as<Node2>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n,
-          hits, scene, nullptr, normal_out, stats, max_iter, ctx->d_err);
+      if (single) SRT_NODE2(SRT_TRIANGLES, true); else SRT_NODE2(SRT_TRIANGLES, false);
       break;
     case SRT_SPHERES:
-      trace_node2_kernel<SRT_SPHERES><<<grid, block, 0, ctx->stream>>>(
-          a->nodes.as<Node2>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n,
-          hits, scene, prev_normals, normal_out, stats, max_iter, ctx->d_err);
+      if (single) SRT_NODE2(SRT_SPHERES, true); else SRT_NODE2(SRT_SPHERES, false);
       break;
     case SRT_TETRAHEDRA:
-      trace_tet_kernel<<<grid, block, 0, ctx->stream>>>(
-          a->nodes.as<NodeT>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n,
-          hits, subface, a->src_faces, vscalar, scalar_out, stats, max_iter, ctx->d_err);
+      if (single) SRT_TET(true); else SRT_TET(false);
       break;
   }
+#undef SRT_NODE2
+#undef SRT_TET
   ctx->launches++;
   return cuda_status(cudaGetLastError(), "trace");
 }

@@ -174,7 +174,7 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
   if (trans) trans[pix] = T;
 }
 
-constexpr int kTfMax = 4096;
+constexpr int kTfMax = 2048;  // 4 * kTfMax floats of shared memory in the adjoint
 
 __global__ void __launch_bounds__(128)
 vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,

@@ -42,7 +42,7 @@ def test_library_exports_every_declared_symbol():
 def test_record_layouts_match_header():
     assert _lib.RAY_DTYPE.itemsize == 32
     assert _lib.HIT_DTYPE.itemsize == 16
-    assert C.sizeof(_lib.TraceOpts) == 6 * 8
+    assert C.sizeof(_lib.TraceOpts) == 6 * 8 + 8
     assert _lib.VOL_DTYPE.itemsize == 4 * 4 + 12 * 4 + 3 * 4
     from oracle import oracle as O
     assert O.RAY_DTYPE == _lib.RAY_DTYPE and O.HIT_DTYPE == _lib.HIT_DTYPE

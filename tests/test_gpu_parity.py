@@ -44,6 +44,19 @@ def assert_hits_equal(h, ref, fields=("t", "u", "v", "prim")):
         assert bad.size == 0, f"{f}: {bad.size} mismatches, first at {bad[:5]}"
 
 
+def trace_both(acc, rays, **kw):
+    """Trace with the default two-pass walk and the single-pass walk in the
+    reference's order; both must agree bit for bit.  Returns the first."""
+    a = acc.Traverse(rays, **kw)
+    b = acc.Traverse(rays, single_pass=True, **kw)
+    ha = a.hits if hasattr(a, "hits") else a
+    hb = b.hits if hasattr(b, "hits") else b
+    assert_hits_equal(ha, hb)
+    if hasattr(a, "subface") and a.subface is not None:
+        assert np.array_equal(a.subface, b.subface)
+    return a
+
+
 # ---------------------------------------------------------------- stages
 def test_morton_stage_matches_oracle():
     v, f = S.displaced_octasphere(6, seed=11)
@@ -120,14 +133,14 @@ def test_build_and_trace_match_reference_fixture(golden, tag, kind):
     lo, hi = acc.BoundingBox()
     assert np.array_equal(np.concatenate([lo, hi]), g[f"{tag}_bbox"])
     if kind == O.TET:
-        res = acc.Traverse(g["tet_rays"], want_subface=True)
+        res = trace_both(acc, g["tet_rays"], want_subface=True)
         assert_hits_equal(res.hits, g["tet_hits"])
         assert np.array_equal(res.subface, g["tet_subface"])
     elif kind == O.TRI:
-        assert_hits_equal(acc.Traverse(g["tri_rays"]), g["tri_hits"])
+        assert_hits_equal(trace_both(acc, g["tri_rays"]), g["tri_hits"])
     else:
-        assert_hits_equal(acc.Traverse(g["sph_rays"]), g["sph_hits"], ("t", "prim"))
-        h2 = acc.Traverse(g["sph_sec_rays"], prev_normals=g["sph_sec_normals"])
+        assert_hits_equal(trace_both(acc, g["sph_rays"]), g["sph_hits"], ("t", "prim"))
+        h2 = trace_both(acc, g["sph_sec_rays"], prev_normals=g["sph_sec_normals"])
         assert_hits_equal(h2, g["sph_sec_hits"], ("t", "prim"))
 
 
@@ -151,7 +164,7 @@ def test_triangles_build_and_trace(levels):
     v, f = S.displaced_octasphere(levels, seed=100 + levels)
     o, acc = _compare_build(O.TRI, v, f)
     rays = S.pinhole_rays(128, 128, (0, 0, 3), (0, 0, 0))
-    assert_hits_equal(acc.Traverse(rays), o.trace(rays))
+    assert_hits_equal(trace_both(acc, rays), o.trace(rays))
 
 
 @pytest.mark.parametrize("n", [2, 3, 17, 18, 1023, 1024, 1025, 5000])
@@ -160,7 +173,7 @@ def test_triangle_counts_at_boundaries(n):
     f = f[:n]
     o, acc = _compare_build(O.TRI, v, f)
     rays = S.pinhole_rays(48, 48, (0, 0, 3), (0, 0, 0))
-    assert_hits_equal(acc.Traverse(rays), o.trace(rays))
+    assert_hits_equal(trace_both(acc, rays), o.trace(rays))
 
 
 @pytest.mark.parametrize("cells", [2, 8, 20])
@@ -170,7 +183,7 @@ def test_tetra_build_and_trace(cells):
     for rays in (S.ortho_rays(96, 96),
                  S.pinhole_rays(64, 64, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)):
         import torch
-        res = acc.Traverse(rays, want_subface=True)
+        res = trace_both(acc, rays, want_subface=True)
         oh, osub, osc = o.trace(rays, want_subface=True, vertex_scalar=sc)
         assert_hits_equal(res.hits, oh)
         assert np.array_equal(res.subface, osub)
@@ -186,7 +199,7 @@ def test_spheres_build_trace_and_self_hit_rule():
     pos[1000:1300] = pos[1000]  # coincident centres
     o, acc = _compare_build(O.SPHERE, pos, None, rad)
     rays = S.pinhole_rays(128, 128, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
-    res = acc.Traverse(rays, want_normal=True)
+    res = trace_both(acc, rays, want_normal=True)
     oh = o.trace(rays)
     assert_hits_equal(res.hits, oh, ("t", "prim"))
     hit = oh["prim"] != O.MISS
@@ -197,8 +210,8 @@ def test_spheres_build_trace_and_self_hit_rule():
     sec["dir"] = S.hemisphere_dirs(nrm, seed=7)
     sec["prev_prim"] = oh["prim"][hit]
     sec["prev_t"] = oh["t"][hit]
-    assert_hits_equal(acc.Traverse(sec, prev_normals=nrm), o.trace(sec, prev_normals=nrm),
-                      ("t", "prim"))
+    assert_hits_equal(trace_both(acc, sec, prev_normals=nrm),
+                      o.trace(sec, prev_normals=nrm), ("t", "prim"))
 
 
 def test_constant_radius_spheres():
@@ -262,7 +275,7 @@ def test_full_size_triangle_workload():
     v, f = S.displaced_octasphere(7)
     o, acc = _compare_build(O.TRI, v, f)
     rays = S.pinhole_rays(512, 512, (0, 0, 3), (0, 0, 0))
-    h = acc.Traverse(rays)
+    h = trace_both(acc, rays)
     oh = o.trace(rays)
     assert_hits_equal(h, oh)
     assert acc.info().num_branches == len([1 for x in o.nodes if not x["leaf"]])
@@ -273,7 +286,7 @@ def test_full_size_tetra_workload():
     v, f, sc = S.tet_grid(64)
     o, acc = _compare_build(O.TET, v, f)
     rays = S.ortho_rays(1024, 1024)
-    res = acc.Traverse(rays, want_subface=True)
+    res = trace_both(acc, rays, want_subface=True)
     oh, osub = o.trace(rays, want_subface=True)
     ids = np.mean(res.hits["prim"] == oh["prim"])
     assert ids >= 0.9999
@@ -286,4 +299,56 @@ def test_full_size_particle_frame():
     pos, rad = S.particles()
     o, acc = _compare_build(O.SPHERE, pos, None, rad)
     rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)[::37]
-    assert_hits_equal(acc.Traverse(rays), o.trace(rays), ("t", "prim"))
+    assert_hits_equal(trace_both(acc, rays), o.trace(rays), ("t", "prim"))
+
+
+# ---------------------------------------------------------------- exact ties
+def test_duplicate_triangles_tie_break():
+    """Every face twice: each hit is an exact tie; the reference keeps the
+    last one of its depth-first order (t <= current)."""
+    v, f = S.displaced_octasphere(5, seed=31)
+    f2 = np.concatenate([f, f[::-1]])
+    o, acc = _compare_build(O.TRI, v, f2)
+    rays = S.pinhole_rays(96, 96, (0, 0, 3), (0, 0, 0))
+    h = trace_both(acc, rays)
+    oh = o.trace(rays)
+    assert_hits_equal(h, oh)
+    assert np.any(oh["prim"] >= f.shape[0]) and np.any(oh["prim"] < f.shape[0])
+
+
+def test_duplicate_spheres_tie_break():
+    pos, rad = S.particles(20_000, seed=32)
+    pos2 = np.concatenate([pos, pos[::-1]])
+    rad2 = np.concatenate([rad, rad[::-1]])
+    o, acc = _compare_build(O.SPHERE, pos2, None, rad2)
+    rays = S.pinhole_rays(96, 96, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    assert_hits_equal(trace_both(acc, rays), o.trace(rays), ("t", "prim"))
+
+
+def test_duplicate_tetrahedra_tie_break():
+    v, f, _ = S.tet_grid(10, seed=33)
+    f2 = np.concatenate([f, f[::-1]])
+    o, acc = _compare_build(O.TET, v, f2)
+    for rays in (S.ortho_rays(80, 80),
+                 S.pinhole_rays(64, 64, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)):
+        res = trace_both(acc, rays, want_subface=True)
+        oh, osub = o.trace(rays, want_subface=True)
+        assert_hits_equal(res.hits, oh)
+        assert np.array_equal(res.subface, osub)
+
+
+def test_rays_from_inside_the_mesh():
+    """Origins inside the tetrahedral mesh and the sphere cloud: entering
+    distances near zero and negative."""
+    v, f, _ = S.tet_grid(12, seed=34)
+    o, acc = _compare_build(O.TET, v, f)
+    rng = np.random.default_rng(3)
+    rays = np.zeros(4096, O.RAY_DTYPE)
+    rays["org"] = rng.uniform(0.05, 0.95, size=(4096, 3)).astype(np.float32)
+    d = rng.normal(size=(4096, 3))
+    rays["dir"] = (d / np.linalg.norm(d, axis=1, keepdims=True)).astype(np.float32)
+    rays["prev_prim"] = O.MISS
+    res = trace_both(acc, rays, want_subface=True)
+    oh, osub = o.trace(rays, want_subface=True)
+    assert_hits_equal(res.hits, oh)
+    assert np.array_equal(res.subface, osub)

@@ -1,0 +1,67 @@
+"""The product's default traversal (front-to-back pass, reference-order
+replay only for exact ties, reference walk when a primitive reports a
+distance before its leaf box's entry), restated in the oracle
+(so_trace2), against the reference's Traverse (so_trace, itself pinned to the
+reference build): identical hits on every ray."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from surface_b200 import scenes as S
+
+from conftest import bits
+
+
+def same(h1, h2, fields=("t", "u", "v", "prim")):
+    for f in fields:
+        assert np.array_equal(bits(h1[f]), bits(h2[f])), f
+
+
+def test_triangles_and_exact_ties():
+    v, f = S.displaced_octasphere(6, seed=41)
+    o = O.OracleAccel(O.TRI, v, f)
+    rays = S.pinhole_rays(192, 192, (0, 0, 3), (0, 0, 0))
+    same(o.trace2(rays), o.trace(rays))
+    dup = O.OracleAccel(O.TRI, v, np.concatenate([f, f[::-1]]))
+    rays = S.pinhole_rays(96, 96, (0, 0, 3), (0, 0, 0))
+    same(dup.trace2(rays), dup.trace(rays))
+
+
+def test_tetrahedra_ortho_ties_and_oblique():
+    v, f, _ = S.tet_grid(24, seed=42)
+    o = O.OracleAccel(O.TET, v, f)
+    for rays in (S.ortho_rays(192, 192),
+                 S.pinhole_rays(96, 96, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)):
+        (h2, s2), (h1, s1) = o.trace2(rays, want_subface=True), o.trace(rays, want_subface=True)
+        same(h2, h1)
+        assert np.array_equal(s2, s1)
+
+
+def test_spheres_fallback_path():
+    pos, rad = S.particles(300_000, seed=43)
+    o = O.OracleAccel(O.SPHERE, pos, None, rad)
+    rays = S.pinhole_rays(160, 160, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    h2, st = o.trace2(rays, want_stats=True)
+    same(h2, o.trace(rays), ("t", "prim"))
+    assert st[3] > 0  # some rays needed the reference walk (ill-conditioned hits)
+    # secondary rays with the self-hit rule
+    hit = h2["prim"] != O.MISS
+    p = rays["org"][hit] + h2["t"][hit, None] * rays["dir"][hit]
+    n = p - pos[h2["prim"][hit]]
+    n = (n / np.linalg.norm(n, axis=1, keepdims=True)).astype(np.float32)
+    sec = np.zeros(int(hit.sum()), O.RAY_DTYPE)
+    sec["org"] = p.astype(np.float32)
+    sec["dir"] = S.hemisphere_dirs(n, seed=5)
+    sec["prev_prim"] = h2["prim"][hit]
+    sec["prev_t"] = h2["t"][hit]
+    same(o.trace2(sec, prev_normals=n), o.trace(sec, prev_normals=n), ("t", "prim"))
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+def test_restated_walk_vs_reference_build():
+    v, f, _ = S.tet_grid(16, seed=44)
+    rays = S.ortho_rays(128, 128)
+    h2, s2 = O.OracleAccel(O.TET, v, f).trace2(rays, want_subface=True)
+    hr, sr = O.RefAccel(O.TET, v, f).trace(rays)
+    same(h2, hr)
+    assert np.array_equal(s2, sr)
