@@ -19,7 +19,7 @@ namespace srt {
 // ---------------------------------------------------------------- limits
 constexpr int kMaxLevel = 23;        // reference depth > 22 forces a leaf;
                                      // root = level 0, its children level 1
-constexpr int kStack = 64;           // traversal stack (tree depth <= 24)
+constexpr int kStack = 32;           // traversal stack (tree depth <= 24)
 constexpr uint32_t kCountMask = 0x3fffffffu;
 constexpr uint32_t kLeafBit = 0x80000000u;
 constexpr uint32_t kNone = 0xffffffffu;
@@ -120,7 +120,8 @@ struct srt_ctx {
   // scratch shared by the builds of this context (stream ordered)
   srt::DevBuf s_keys2, s_vals2, s_hist, s_scan, s_kchild, s_kflags, s_krange,
       s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
-      s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm;
+      s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm,
+      s_defer;
 };
 
 struct srt_accel {

@@ -512,23 +512,72 @@ __device__ void window_walk2(const Node2 *__restrict__ nodes,
 }
 
 // --------------------------------------------------------------- kernels
-// Two-child kinds (triangles, spheres).  Default: pass 1 walks front to
-// back and finds m, the smallest hit distance, counting the primitives that
-// hit exactly at m; one such primitive is the reference's answer, several
-// (an exact tie) are ordered by a reference-order walk restricted to boxes
-// entered before m.  A primitive hit before its own leaf box's entry sends
-// the ray through the reference's walk.  SINGLE: the reference's walk only.
-template <int KIND, bool SINGLE>
-__global__ void __launch_bounds__(128)
-trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
-                   const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
-                   size_t n, srt_hit *__restrict__ hits,
-                   const SceneInfo *__restrict__ scene,
-                   const float *__restrict__ prev_normals, float *__restrict__ normal_out,
-                   unsigned long long *__restrict__ stats, uint32_t max_iter,
-                   uint32_t *__restrict__ err) {
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+// Pass 1 (front to back) runs in the main kernels and settles the common
+// case: no hit, or exactly one primitive at the smallest distance m.  Rays
+// with an exact tie at m, or with a primitive reported before its own leaf
+// box's entry, are appended to a deferred list; a second kernel resolves
+// them with the reference-order walk restricted to boxes entered before m
+// (ties) or with the reference's full walk.  Keeping those walks out of the
+// main kernels keeps their register and stack footprint small.
+
+struct Deferred {
+  uint32_t ray;
+  uint32_t full;  // 1: the reference's full walk; 0: replay the tie at m
+  double m;
+};
+
+template <int KIND>
+__device__ __forceinline__ void store_node2(size_t i, const Best &b, const Ctx2 &c,
+                                            const float4 *__restrict__ prims,
+                                            srt_hit *__restrict__ hits,
+                                            float *__restrict__ normal_out) {
+  const bool any = b.t < FLT_MAX && b.prim != kNone;
+  reinterpret_cast<float4 *>(hits)[i] =
+      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
+                  __uint_as_float(any ? b.prim : kNone));
+  if (!normal_out) return;
+  float nn[3] = {0.0f, 0.0f, 0.0f};
+  if (any) {
+    if (KIND == SRT_TRIANGLES) {
+      const float4 q0 = prims[3 * (size_t)b.j];
+      const float4 q1 = prims[3 * (size_t)b.j + 1];
+      const float4 q2 = prims[3 * (size_t)b.j + 2];
+      const float e1[3] = {q1.x - q0.x, q1.y - q0.y, q1.z - q0.z};
+      const float e2[3] = {q2.x - q0.x, q2.y - q0.y, q2.z - q0.z};
+      cross3(e1, e2, nn);
+      normalize_ref(nn);
+    } else {
+      // position = org + t * dir; vnormalize(position - centre)
+      const float4 s = prims[b.j];
+      const float c3[3] = {s.x, s.y, s.z};
+#pragma unroll
+      for (int k = 0; k < 3; k++) nn[k] = (c.r.o[k] + b.t * c.r.d[k]) - c3[k];
+      const float len = sqrtf(dot3(nn, nn));
+      if (len > FLT_EPSILON * 16) {
+        const float il = __frcp_rn(len);
+#pragma unroll
+        for (int k = 0; k < 3; k++) nn[k] *= il;
+      }
+    }
+  }
+  normal_out[3 * i] = nn[0];
+  normal_out[3 * i + 1] = nn[1];
+  normal_out[3 * i + 2] = nn[2];
+}
+
+__device__ __forceinline__ void add_stats(unsigned long long *stats, const Work &w,
+                                          uint32_t full) {
+  if (!stats) return;
+  atomicAdd(&stats[0], (unsigned long long)w.branch);
+  atomicAdd(&stats[1], (unsigned long long)w.leaf);
+  atomicAdd(&stats[2], (unsigned long long)w.prim);
+  if (full) atomicAdd(&stats[3], 1ull);
+}
+
+template <int KIND>
+__device__ __forceinline__ Ctx2 make_ctx2(const srt_ray *__restrict__ rays, size_t i,
+                                          const SceneInfo *__restrict__ scene,
+                                          const float *__restrict__ prev_normals) {
   Ctx2 c;
   c.r = load_ray(rays, i, c.prev_prim, c.prev_t);
   c.keps = scene->keps;
@@ -538,13 +587,29 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
     c.pn[1] = prev_normals[3 * i + 1];
     c.pn[2] = prev_normals[3 * i + 2];
   }
+  return c;
+}
+
+// Two-child kinds (triangles, spheres).  SINGLE: the reference's walk for
+// every ray.
+template <int KIND, bool SINGLE>
+__global__ void __launch_bounds__(128)
+trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
+                   const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
+                   size_t n, srt_hit *__restrict__ hits,
+                   const SceneInfo *__restrict__ scene,
+                   const float *__restrict__ prev_normals, float *__restrict__ normal_out,
+                   unsigned long long *__restrict__ stats, Deferred *__restrict__ dlist,
+                   uint32_t *__restrict__ dcount, uint32_t max_iter,
+                   uint32_t *__restrict__ err) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const Ctx2 c = make_ctx2<KIND>(rays, i, scene, prev_normals);
   Work w;
   Best b;
-  uint32_t fallback = 0;
   if (SINGLE) {
     ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
   } else {
-    // ---- pass 1
     float m = FLT_MAX;
     uint32_t at_m = 0;
     bool viol = false;
@@ -601,54 +666,46 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
         }
       }
     }
-    if (viol && !w.fail) {
-      ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
-      fallback = 1;
-    } else if (at_m > 1 && !w.fail) {
-      // triangles keep the last candidate at m (t <= current), spheres the
-      // first (t < current)
-      const float t0 = (KIND == SRT_TRIANGLES) ? m : nextafterf(m, FLT_MAX);
-      window_walk2<KIND>(nodes, prims, sidx, c, bound_rel(m, kRelTri), t0, b, w, max_iter);
+    if (!w.fail && (viol || at_m > 1)) {
+      const uint32_t k = atomicAdd(dcount, 1u);
+      dlist[k] = Deferred{(uint32_t)i, viol ? 1u : 0u, (double)m};
+      add_stats(stats, w, 0);
+      return;
     }
   }
   if (w.fail) atomicOr(err, kErrIter);
-  if (stats) {
-    atomicAdd(&stats[0], (unsigned long long)w.branch);
-    atomicAdd(&stats[1], (unsigned long long)w.leaf);
-    atomicAdd(&stats[2], (unsigned long long)w.prim);
-    if (fallback) atomicAdd(&stats[3], 1ull);
-  }
-  const bool any = b.t < FLT_MAX && b.prim != kNone;
-  reinterpret_cast<float4 *>(hits)[i] =
-      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
-                  __uint_as_float(any ? b.prim : kNone));
-  if (normal_out) {
-    float nn[3] = {0.0f, 0.0f, 0.0f};
-    if (any) {
-      if (KIND == SRT_TRIANGLES) {
-        const float4 q0 = prims[3 * (size_t)b.j];
-        const float4 q1 = prims[3 * (size_t)b.j + 1];
-        const float4 q2 = prims[3 * (size_t)b.j + 2];
-        const float e1[3] = {q1.x - q0.x, q1.y - q0.y, q1.z - q0.z};
-        const float e2[3] = {q2.x - q0.x, q2.y - q0.y, q2.z - q0.z};
-        cross3(e1, e2, nn);
-        normalize_ref(nn);
-      } else {
-        const float4 s = prims[b.j];
-        const float c3[3] = {s.x, s.y, s.z};
-#pragma unroll
-        for (int k = 0; k < 3; k++) nn[k] = (c.r.o[k] + b.t * c.r.d[k]) - c3[k];
-        const float len = sqrtf(dot3(nn, nn));
-        if (len > FLT_EPSILON * 16) {
-          const float il = __frcp_rn(len);
-#pragma unroll
-          for (int k = 0; k < 3; k++) nn[k] *= il;
-        }
-      }
+  add_stats(stats, w, 0);
+  store_node2<KIND>(i, b, c, prims, hits, normal_out);
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(128)
+resolve_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
+                     const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
+                     srt_hit *__restrict__ hits, const SceneInfo *__restrict__ scene,
+                     const float *__restrict__ prev_normals,
+                     float *__restrict__ normal_out, unsigned long long *__restrict__ stats,
+                     const Deferred *__restrict__ dlist, const uint32_t *__restrict__ dcount,
+                     uint32_t max_iter, uint32_t *__restrict__ err) {
+  const uint32_t cnt = *dcount;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+       k += gridDim.x * blockDim.x) {
+    const Deferred dfr = dlist[k];
+    const Ctx2 c = make_ctx2<KIND>(rays, dfr.ray, scene, prev_normals);
+    Work w;
+    Best b;
+    if (dfr.full) {
+      ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
+    } else {
+      // triangles keep the last candidate at m (t <= current), spheres the
+      // first (t < current)
+      const float m = (float)dfr.m;
+      const float t0 = (KIND == SRT_TRIANGLES) ? m : nextafterf(m, FLT_MAX);
+      window_walk2<KIND>(nodes, prims, sidx, c, bound_rel(m, kRelTri), t0, b, w, max_iter);
     }
-    normal_out[3 * i] = nn[0];
-    normal_out[3 * i + 1] = nn[1];
-    normal_out[3 * i + 2] = nn[2];
+    if (w.fail) atomicOr(err, kErrIter);
+    add_stats(stats, w, dfr.full);
+    store_node2<KIND>(dfr.ray, b, c, prims, hits, normal_out);
   }
 }
 
@@ -736,6 +793,41 @@ __device__ __forceinline__ double window_hi(double m) {
   return (double)wf;
 }
 
+__device__ __forceinline__ void store_tet(size_t i, const Best &b,
+                                          srt_hit *__restrict__ hits,
+                                          uint32_t *__restrict__ subface,
+                                          const uint32_t *__restrict__ faces,
+                                          const float *__restrict__ vscalar,
+                                          float *__restrict__ scalar_out) {
+  const bool any = b.t < FLT_MAX && b.prim != kNone;
+  reinterpret_cast<float4 *>(hits)[i] =
+      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
+                  __uint_as_float(any ? b.prim : kNone));
+  if (subface) subface[i] = any ? b.sub : 0u;
+  if (scalar_out) {
+    float s = 0.0f;
+    if (any && faces && vscalar) {
+      // entering face vertex order (A, B, C) per face id, as the Pluecker
+      // test forms its barycentric point
+      const int fA[4] = {3, 2, 1, 0}, fB[4] = {2, 3, 0, 1}, fC[4] = {1, 0, 3, 2};
+      const uint32_t *tv = faces + 4 * (size_t)b.prim;
+      const double sa = vscalar[tv[fA[b.sub]]], sb = vscalar[tv[fB[b.sub]]],
+                   sc = vscalar[tv[fC[b.sub]]];
+      s = (float)((1.0 - b.e1 - b.e2) * sa + b.e1 * sb + b.e2 * sc);
+    }
+    scalar_out[i] = s;
+  }
+}
+
+__device__ __forceinline__ CtxT make_ctxT(const srt_ray *__restrict__ rays, size_t i) {
+  CtxT c;
+  float prev_t;
+  c.r = load_ray(rays, i, c.prev_prim, prev_t);
+  c.o = {c.r.o[0], c.r.o[1], c.r.o[2]};
+  c.d = {c.r.d[0], c.r.d[1], c.r.d[2]};
+  return c;
+}
+
 template <bool SINGLE>
 __global__ void __launch_bounds__(128)
 trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
@@ -743,22 +835,19 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
                  size_t n, srt_hit *__restrict__ hits, uint32_t *__restrict__ subface,
                  const uint32_t *__restrict__ faces, const float *__restrict__ vscalar,
                  float *__restrict__ scalar_out, unsigned long long *__restrict__ stats,
+                 Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
                  uint32_t max_iter, uint32_t *__restrict__ err) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  CtxT c;
-  float prev_t;
-  c.r = load_ray(rays, i, c.prev_prim, prev_t);
-  c.o = {c.r.o[0], c.r.o[1], c.r.o[2]};
-  c.d = {c.r.d[0], c.r.d[1], c.r.d[2]};
+  const CtxT c = make_ctxT(rays, i);
   Work w;
   Best b;
-  uint32_t fallback = 0;
   if (SINGLE) {
     walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
   } else {
-    // ---- pass 1: front to back; window list = entry distances within 8
-    // float steps of the running minimum m (kept for the tie count)
+    // pass 1: front to back; nwin counts entry distances within 8 float
+    // steps of the running minimum m (the list is kept to recount when m
+    // drops)
     double m = DBL_MAX;
     double wl[4];
     int nwin = 0;
@@ -832,38 +921,43 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
         }
       }
     }
-    if (viol && !w.fail) {
-      walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
-      fallback = 1;
-    } else if ((nwin > 1 || overflow) && !w.fail) {
-      const double whi = window_hi(m);
-      walkT<true>(nodes, prims, sidx, c, bound_rel((float)whi, kRelTet), whi, b, w, max_iter);
+    if (!w.fail && (viol || nwin > 1 || overflow)) {
+      const uint32_t k = atomicAdd(dcount, 1u);
+      dlist[k] = Deferred{(uint32_t)i, viol ? 1u : 0u, m};
+      add_stats(stats, w, 0);
+      return;
     }
   }
   if (w.fail) atomicOr(err, kErrIter);
-  if (stats) {
-    atomicAdd(&stats[0], (unsigned long long)w.branch);
-    atomicAdd(&stats[1], (unsigned long long)w.leaf);
-    atomicAdd(&stats[2], (unsigned long long)w.prim);
-    if (fallback) atomicAdd(&stats[3], 1ull);
-  }
-  const bool any = b.t < FLT_MAX && b.prim != kNone;
-  reinterpret_cast<float4 *>(hits)[i] =
-      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
-                  __uint_as_float(any ? b.prim : kNone));
-  if (subface) subface[i] = any ? b.sub : 0u;
-  if (scalar_out) {
-    float s = 0.0f;
-    if (any && faces && vscalar) {
-      // entering face vertex order (A, B, C) per face id, as the Pluecker
-      // test forms its barycentric point
-      const int fA[4] = {3, 2, 1, 0}, fB[4] = {2, 3, 0, 1}, fC[4] = {1, 0, 3, 2};
-      const uint32_t *tv = faces + 4 * (size_t)b.prim;
-      const double sa = vscalar[tv[fA[b.sub]]], sb = vscalar[tv[fB[b.sub]]],
-                   sc = vscalar[tv[fC[b.sub]]];
-      s = (float)((1.0 - b.e1 - b.e2) * sa + b.e1 * sb + b.e2 * sc);
+  add_stats(stats, w, 0);
+  store_tet(i, b, hits, subface, faces, vscalar, scalar_out);
+}
+
+__global__ void __launch_bounds__(128)
+resolve_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
+                   const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
+                   srt_hit *__restrict__ hits, uint32_t *__restrict__ subface,
+                   const uint32_t *__restrict__ faces, const float *__restrict__ vscalar,
+                   float *__restrict__ scalar_out, unsigned long long *__restrict__ stats,
+                   const Deferred *__restrict__ dlist, const uint32_t *__restrict__ dcount,
+                   uint32_t max_iter, uint32_t *__restrict__ err) {
+  const uint32_t cnt = *dcount;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+       k += gridDim.x * blockDim.x) {
+    const Deferred dfr = dlist[k];
+    const CtxT c = make_ctxT(rays, dfr.ray);
+    Work w;
+    Best b;
+    if (dfr.full) {
+      walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+    } else {
+      const double whi = window_hi(dfr.m);
+      walkT<true>(nodes, prims, sidx, c, bound_rel((float)whi, kRelTet), whi, b, w,
+                  max_iter);
     }
-    scalar_out[i] = s;
+    if (w.fail) atomicOr(err, kErrIter);
+    add_stats(stats, w, dfr.full);
+    store_tet(dfr.ray, b, hits, subface, faces, vscalar, scalar_out);
   }
 }
 
@@ -874,36 +968,90 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
                         const float *vscalar, float *scalar_out, float *normal_out,
                         unsigned long long *stats, uint32_t flags) {
   if (n == 0) return SRT_OK;
+  if (n > 0xffffffffull) {
+    set_error("at most 2^32-1 rays per call");
+    return SRT_ERR_INVALID;
+  }
   srt_ctx *ctx = a->ctx;
   const int block = 128;
   const unsigned grid = (unsigned)((n + block - 1) / block);
-  // every node and leaf is visited at most once per walk; at most three walks
-  const uint32_t max_iter = (uint32_t)std::min<size_t>(12 * a->n + 64, 0xfffffff0u);
+  const unsigned rgrid = (unsigned)ctx->num_sms * 8;
+  // every node and leaf is visited at most once per walk
+  const uint32_t max_iter = (uint32_t)std::min<size_t>(8 * a->n + 64, 0xfffffff0u);
   const SceneInfo *scene = a->scene.as<SceneInfo>();
   const bool single = (flags & SRT_TRACE_SINGLE_PASS) != 0;
   cudaStream_t st = ctx->stream;
-#define SRT_NODE2(KIND, S)                                                             \
-  trace_node2_kernel<KIND, S><<<grid, block, 0, st>>>(                                 \
-      a->nodes.as<Node2>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n, \
-      hits, scene, KIND == SRT_SPHERES ? prev_normals : nullptr, normal_out, stats,    \
-      max_iter, ctx->d_err)
-#define SRT_TET(S)                                                                     \
-  trace_tet_kernel<S><<<grid, block, 0, st>>>(                                         \
-      a->nodes.as<NodeT>(), a->prims.as<float4>(), a->indices.as<uint32_t>(), rays, n, \
-      hits, subface, a->src_faces, vscalar, scalar_out, stats, max_iter, ctx->d_err)
+  Deferred *dlist = nullptr;
+  uint32_t *dcount = nullptr;
+  if (!single) {
+    cudaError_t e = ctx->s_defer.ensure(n * sizeof(Deferred) + 256);
+    if (e != cudaSuccess) return cuda_status(e, "deferred list");
+    dcount = ctx->s_defer.as<uint32_t>();
+    dlist = reinterpret_cast<Deferred *>(ctx->s_defer.as<char>() + 256);
+    if ((e = cudaMemsetAsync(dcount, 0, 4, st)) != cudaSuccess)
+      return cuda_status(e, "deferred count");
+  }
+  const float *pn = a->kind == SRT_SPHERES ? prev_normals : nullptr;
   switch (a->kind) {
     case SRT_TRIANGLES:
-      if (single) SRT_NODE2(SRT_TRIANGLES, true); else SRT_NODE2(SRT_TRIANGLES, false);
+    case SRT_SPHERES: {
+      const Node2 *nd = a->nodes.as<Node2>();
+      const float4 *pr = a->prims.as<float4>();
+      const uint32_t *ix = a->indices.as<uint32_t>();
+      if (a->kind == SRT_TRIANGLES) {
+        if (single)
+          trace_node2_kernel<SRT_TRIANGLES, true><<<grid, block, 0, st>>>(
+              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, nullptr, nullptr,
+              max_iter, ctx->d_err);
+        else {
+          trace_node2_kernel<SRT_TRIANGLES, false><<<grid, block, 0, st>>>(
+              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount,
+              max_iter, ctx->d_err);
+          resolve_node2_kernel<SRT_TRIANGLES><<<rgrid, block, 0, st>>>(
+              nd, pr, ix, rays, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
+              ctx->d_err);
+          ctx->launches++;
+        }
+      } else {
+        if (single)
+          trace_node2_kernel<SRT_SPHERES, true><<<grid, block, 0, st>>>(
+              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, nullptr, nullptr,
+              max_iter, ctx->d_err);
+        else {
+          trace_node2_kernel<SRT_SPHERES, false><<<grid, block, 0, st>>>(
+              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount,
+              max_iter, ctx->d_err);
+          resolve_node2_kernel<SRT_SPHERES><<<rgrid, block, 0, st>>>(
+              nd, pr, ix, rays, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
+              ctx->d_err);
+          ctx->launches++;
+        }
+      }
       break;
-    case SRT_SPHERES:
-      if (single) SRT_NODE2(SRT_SPHERES, true); else SRT_NODE2(SRT_SPHERES, false);
+    }
+    case SRT_TETRAHEDRA: {
+      const NodeT *nd = a->nodes.as<NodeT>();
+      const float4 *pr = a->prims.as<float4>();
+      const uint32_t *ix = a->indices.as<uint32_t>();
+      if (single)
+        trace_tet_kernel<true><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
+                                                       a->src_faces, vscalar, scalar_out,
+                                                       stats, nullptr, nullptr, max_iter,
+                                                       ctx->d_err);
+      else {
+        trace_tet_kernel<false><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
+                                                        a->src_faces, vscalar, scalar_out,
+                                                        stats, dlist, dcount, max_iter,
+                                                        ctx->d_err);
+        resolve_tet_kernel<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, subface,
+                                                    a->src_faces, vscalar, scalar_out,
+                                                    stats, dlist, dcount, max_iter,
+                                                    ctx->d_err);
+        ctx->launches++;
+      }
       break;
-    case SRT_TETRAHEDRA:
-      if (single) SRT_TET(true); else SRT_TET(false);
-      break;
+    }
   }
-#undef SRT_NODE2
-#undef SRT_TET
   ctx->launches++;
   return cuda_status(cudaGetLastError(), "trace");
 }
