@@ -75,6 +75,17 @@ def make_workload(name):
                     config={"workload": "particles16M: 16,777,216 spheres, one frame "
                                         "(rebuild + 2048x2048 primaries)",
                             "prims": int(pos.shape[0]), "rays": int(rays.size)})
+    if name == "volume":
+        dens = S.volume_blobs(256, nblobs=32)
+        tgt = S.volume_blobs(256, nblobs=32, shift_voxels=2.0)
+        tf = S.transfer_function(256)
+        return dict(kind="volume", dens=dens, target_dens=tgt, tf=tf,
+                    rays=np.zeros(512 * 512, np.uint8),
+                    config={"workload": "volume256: 256^3 FP32 density (32 Gaussian blobs), "
+                                        "256-entry RGBA transfer function, 512x512 rays, "
+                                        "step 0.5 voxel, emission-absorption forward + "
+                                        "adjoint of an L2 loss",
+                            "rays": 512 * 512})
     raise SystemExit(f"unknown workload {name}")
 
 
@@ -195,7 +206,77 @@ def run_reference_arm(args, W):
 
 
 METRIC = "Mrays/s (LBVH build + closest hit per step)"
-DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)"}
+METRIC_VOL = "Mrays/s (volume march forward + adjoint per step)"
+DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
+         "volume": "f32"}
+
+
+def run_volume(args, W):
+    """Forward + adjoint of the L2 loss per step (device resident); forward
+    alone is timed too.  CPU baseline: the FP32 oracle forward (OpenMP)."""
+    import torch
+
+    from surface_b200 import volume as V
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    p = V.camera(512, 512, res=256)
+    dens = torch.as_tensor(W["dens"], device=dev)
+    tf = torch.as_tensor(W["tf"], device=dev)
+    target = V.march(torch.as_tensor(W["target_dens"], device=dev), tf, p)[0]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def fwd():
+        return V.march(dens, tf, p)
+
+    def fwd_bwd():
+        img, tr = V.march(dens, tf, p)
+        return V.march_backward(dens, tf, p, tr, 2 * (img - target))
+
+    for _ in range(max(args.warmup, 3)):
+        fwd_bwd()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    fe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            fe[k][0].record()
+            fwd()
+            fe[k][1].record()
+            flush.zero_()
+            ev[k][0].record()
+            fwd_bwd()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+    fb_ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
+    f_ms = statistics.mean(a.elapsed_time(b) for a, b in fe)
+    nr = 512 * 512
+    cpu = None
+    if not args.no_cpu:
+        from oracle import oracle as O
+        q = np.zeros(1, O.VOL_DTYPE)
+        q[...] = p.view(O.VOL_DTYPE)
+        t0 = time.perf_counter()
+        O.volume_fwd_f32(q, W["dens"], (256, 256, 256), W["tf"])
+        tc = time.perf_counter() - t0
+        cpu = {"value": round(nr / tc / 1e6, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
+               "kind": "port", "sample": "FP32 forward march restatement over all 512^2 "
+                                         "rays (the reference has no C++ march; its shader "
+                                         "march needs the closed GLSL compiler)",
+               "forward_ms": round(1e3 * tc, 2)}
+    line = {"metric": METRIC_VOL, "value": round(nr / (fb_ms * 1e-3) / 1e6, 3),
+            "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(fb_ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)"),
+            "forward_ms": round(f_ms, 4), "forward_backward_ms": round(fb_ms, 4),
+            "fwd_bwd_over_fwd": round(fb_ms / f_ms, 3), "clocks": clk.summary(),
+            "cpu_baseline": cpu}
+    print(json.dumps(line), flush=True)
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -396,10 +477,16 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tet", choices=["tet", "tri", "particles"])
+    ap.add_argument("--workload", default="tet",
+                    choices=["tet", "tri", "particles", "volume"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     W = make_workload(args.workload)
+    if args.workload == "volume":
+        if args.impl == "reference":
+            raise SystemExit("the volume workload has no reference CPU march")
+        run_volume(args, W)
+        return
     if args.impl == "reference":
         run_reference_arm(args, W)
     else:

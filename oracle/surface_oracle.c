@@ -1573,8 +1573,12 @@ SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
                             double *grad_tf) {
   int W = P->width, H = P->height;
   double loss = 0.0;
+  const int par = !grad_dens && !grad_tf; /* loss/image only: pixels in parallel */
   const double step = P->step;
   const int maxs = P->max_steps;
+#ifdef _OPENMP
+#pragma omp parallel for schedule(dynamic, 4) reduction(+ : loss) if (par)
+#endif
   for (int py = 0; py < H; py++) {
     for (int px = 0; px < W; px++) {
       double o[3], d[3];

@@ -22,6 +22,7 @@
 //   7. compaction         exclusive scan of the branch flags -> node slots
 //   8. emission           emit_node2_kernel / emit_tet_kernel
 #include <algorithm>
+#include <climits>
 #include <cstdio>
 
 #include "srt_internal.cuh"
@@ -350,10 +351,31 @@ constexpr int kRsRounds = 16;
 constexpr int kRsWChunk = 32 * kRsRounds;
 constexpr int kRsTile = kRsWarps * kRsWChunk;
 
+// Segment (scene) of global index x: the largest s with off[s] <= x.
+__device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int nseg, uint32_t x) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&off[mid]) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
+// Sort digit: a byte of the key, or (SEGDIG) the segment of the value --
+// the extra pass that groups a multi-scene sort by scene.
+template <bool SEGDIG>
+__device__ __forceinline__ uint32_t rs_digit(uint32_t k, uint32_t v, int shift,
+                                             const uint32_t *__restrict__ seg, int nseg) {
+  if (SEGDIG) return (uint32_t)seg_of(seg, nseg, v);
+  return (k >> shift) & (kRsBins - 1);
+}
+
 // Per-tile digit histogram, digit-major: hist[d * ntiles + tile].
+template <bool SEGDIG>
 __global__ void __launch_bounds__(kRsThreads)
-rs_hist_kernel(const uint32_t *__restrict__ keys, size_t n, int shift,
-               uint32_t *__restrict__ hist, uint32_t ntiles) {
+rs_hist_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
+               size_t n, int shift, uint32_t *__restrict__ hist, uint32_t ntiles,
+               const uint32_t *__restrict__ seg, int nseg) {
   __shared__ uint32_t wh[kRsWarps][kRsBins];
   for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads)
     (&wh[0][0])[i] = 0;
@@ -366,7 +388,7 @@ rs_hist_kernel(const uint32_t *__restrict__ keys, size_t n, int shift,
     bool ok = idx < n;
     unsigned valid = __ballot_sync(0xffffffffu, ok);
     if (ok) {
-      uint32_t d = (keys[idx] >> shift) & (kRsBins - 1);
+      uint32_t d = rs_digit<SEGDIG>(keys[idx], SEGDIG ? vals[idx] : 0u, shift, seg, nseg);
       unsigned peers = __match_any_sync(valid, d);
       if (lane == __ffs(peers) - 1) wh[w][d] += __popc(peers);
     }
@@ -383,10 +405,12 @@ rs_hist_kernel(const uint32_t *__restrict__ keys, size_t n, int shift,
 
 // Stable scatter of one tile: warps own consecutive chunks, rounds go in key
 // order, lanes within a round are ranked by lane order among equal digits.
+template <bool SEGDIG>
 __global__ void __launch_bounds__(kRsThreads)
 rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                   uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, size_t n,
-                  int shift, const uint32_t *__restrict__ offs, uint32_t ntiles) {
+                  int shift, const uint32_t *__restrict__ offs, uint32_t ntiles,
+                  const uint32_t *__restrict__ seg, int nseg) {
   __shared__ uint32_t wc[kRsWarps][kRsBins];
   for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads)
     (&wc[0][0])[i] = 0;
@@ -413,7 +437,7 @@ rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__
     bool ok = idx < n;
     unsigned valid = __ballot_sync(0xffffffffu, ok);
     if (ok) {
-      uint32_t d = (k[r] >> shift) & (kRsBins - 1);
+      uint32_t d = rs_digit<SEGDIG>(k[r], v[r], shift, seg, nseg);
       unsigned peers = __match_any_sync(valid, d);
       if (lane == __ffs(peers) - 1) wc[w][d] += __popc(peers);
     }
@@ -436,7 +460,7 @@ rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__
     size_t idx = base + (size_t)r * 32 + lane;
     bool ok = idx < n;
     unsigned valid = __ballot_sync(0xffffffffu, ok);
-    uint32_t d = (k[r] >> shift) & (kRsBins - 1);
+    uint32_t d = ok ? rs_digit<SEGDIG>(k[r], v[r], shift, seg, nseg) : 0u;
     unsigned peers = ok ? __match_any_sync(valid, d) : 0u;
     uint32_t pos = 0;
     if (ok) pos = wc[w][d] + __popc(peers & lt);
@@ -452,38 +476,72 @@ rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__
 
 }  // namespace
 
-// Stable LSD sort of (keys, vals) by key; result lands back in keys/vals.
-srt_status sort_pairs(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
-                      bool identity_vals) {
-  if (n == 0) return SRT_OK;
+// One stable counting pass (8-bit key digit, or SEGDIG: segment of the value)
+// from (k0, v0) into (k1, v1).
+template <bool SEGDIG>
+static srt_status sort_pass(srt_ctx *ctx, const uint32_t *k0, const uint32_t *v0,
+                            uint32_t *k1, uint32_t *v1, size_t n, int shift,
+                            const uint32_t *seg, int nseg) {
   cudaStream_t st = ctx->stream;
-  uint32_t ntiles = (uint32_t)((n + kRsTile - 1) / kRsTile);
+  const uint32_t ntiles = (uint32_t)((n + kRsTile - 1) / kRsTile);
+  uint32_t *hist = ctx->s_hist.as<uint32_t>();
+  rs_hist_kernel<SEGDIG><<<ntiles, kRsThreads, 0, st>>>(k0, v0, n, shift, hist, ntiles, seg,
+                                                        nseg);
+  ctx->launches++;
+  srt_status s = cuda_status(cudaGetLastError(), "rs_hist");
+  if (s != SRT_OK) return s;
+  s = exclusive_scan(ctx, hist, hist, (size_t)kRsBins * ntiles);
+  if (s != SRT_OK) return s;
+  rs_scatter_kernel<SEGDIG><<<ntiles, kRsThreads, 0, st>>>(k0, v0, k1, v1, n, shift, hist,
+                                                           ntiles, seg, nseg);
+  ctx->launches++;
+  return cuda_status(cudaGetLastError(), "rs_scatter");
+}
+
+static srt_status sort_scratch(srt_ctx *ctx, size_t n) {
+  const uint32_t ntiles = (uint32_t)((n + kRsTile - 1) / kRsTile);
   cudaError_t e;
   if ((e = ctx->s_keys2.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "sort");
   if ((e = ctx->s_vals2.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "sort");
   if ((e = ctx->s_hist.ensure((size_t)kRsBins * ntiles * 4)) != cudaSuccess)
     return cuda_status(e, "sort");
+  return SRT_OK;
+}
+
+// Stable LSD sort of (keys, vals) by key; result lands back in keys/vals.
+// identity_vals: vals are 0..n-1 on entry (not read).  With nseg > 1 a
+// fifth pass groups the result by the segment of each value (the segment
+// offsets `seg` are global indices), i.e. the order is (segment, key,
+// value).
+srt_status sort_pairs_seg(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
+                          bool identity_vals, const uint32_t *seg, int nseg) {
+  if (n == 0) return SRT_OK;
+  srt_status s = sort_scratch(ctx, n);
+  if (s != SRT_OK) return s;
   uint32_t *k0 = keys, *v0 = vals, *k1 = ctx->s_keys2.as<uint32_t>(),
            *v1 = ctx->s_vals2.as<uint32_t>();
-  uint32_t *hist = ctx->s_hist.as<uint32_t>();
   for (int pass = 0; pass < 4; pass++) {
-    int shift = pass * kRsBits;
-    rs_hist_kernel<<<ntiles, kRsThreads, 0, st>>>(k0, n, shift, hist, ntiles);
-    ctx->launches++;
-    srt_status s = cuda_status(cudaGetLastError(), "rs_hist");
-    if (s != SRT_OK) return s;
-    s = exclusive_scan(ctx, hist, hist, (size_t)kRsBins * ntiles);
-    if (s != SRT_OK) return s;
     const uint32_t *vin = (pass == 0 && identity_vals) ? nullptr : v0;
-    rs_scatter_kernel<<<ntiles, kRsThreads, 0, st>>>(k0, vin, k1, v1, n, shift, hist,
-                                                    ntiles);
-    ctx->launches++;
-    s = cuda_status(cudaGetLastError(), "rs_scatter");
+    s = sort_pass<false>(ctx, k0, vin, k1, v1, n, pass * kRsBits, nullptr, 0);
     if (s != SRT_OK) return s;
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
-  return SRT_OK;  // even number of passes: data is back in keys/vals
+  if (nseg > 1) {
+    // fifth pass into the scratch, then copy back (keys/vals stay the output)
+    s = sort_pass<true>(ctx, k0, v0, k1, v1, n, 0, seg, nseg);
+    if (s != SRT_OK) return s;
+    cudaError_t e = cudaMemcpyAsync(keys, k1, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(vals, v1, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e, "sort copy");
+  }
+  return SRT_OK;  // four passes: data is back in keys/vals
+}
+
+srt_status sort_pairs(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
+                      bool identity_vals) {
+  return sort_pairs_seg(ctx, keys, vals, n, identity_vals, nullptr, 1);
 }
 
 namespace {
@@ -859,6 +917,419 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
 }
 
 }  // namespace
+
+namespace {
+// =================================================================== batches
+// Many scenes in one build: primitives of scene s are the global range
+// [foff[s], foff[s+1]); its Karras internal nodes the global range
+// [ioff[s], ioff[s+1]) with ioff[s] = foff[s] - s.  Every stage runs once
+// over all scenes and computes exactly the per-scene build: boxes, Morton
+// codes and trees use each scene's own box and local key positions.
+
+__device__ __forceinline__ int f2o(float f) {  // order-preserving float -> int
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float o2f(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+// Block-wide box reduction; the result is valid in thread 0.
+__device__ Box block_reduce_box(Box b) {
+  __shared__ Box sh[32];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      b.lo[k] = fmin_ref(b.lo[k], __shfl_down_sync(0xffffffffu, b.lo[k], o));
+      b.hi[k] = fmax_ref(b.hi[k], __shfl_down_sync(0xffffffffu, b.hi[k], o));
+    }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) b = box_merge(b, sh[i]);
+  }
+  __syncthreads();
+  return b;
+}
+
+__global__ void seg_bbox_init_kernel(int *__restrict__ acc, int nseg) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < 6 * nseg; i += gridDim.x * blockDim.x)
+    acc[i] = (i % 6) < 3 ? INT_MAX : INT_MIN;
+}
+
+constexpr int kSegTile = 2048;
+
+template <int KIND>
+__global__ void seg_bbox_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f,
+                                const uint32_t *__restrict__ foff, int nseg, uint32_t N,
+                                int *__restrict__ acc) {
+  const uint32_t t0 = blockIdx.x * kSegTile;
+  if (t0 >= N) return;
+  const uint32_t t1 = min(N, t0 + kSegTile);
+  const int s0 = seg_of(foff, nseg, t0), s1 = seg_of(foff, nseg, t1 - 1);
+  const float e = (KIND == SRT_TRIANGLES) ? 0.0f : FLT_EPSILON * 16;
+  const int nv = (KIND == SRT_TRIANGLES) ? 3 : 4;
+  for (int sg = s0; sg <= s1; sg++) {
+    const uint32_t lo = max(t0, __ldg(&foff[sg])), hi = min(t1, __ldg(&foff[sg + 1]));
+    Box b;
+    box_init(b);
+    for (uint32_t i = lo + threadIdx.x; i < hi; i += blockDim.x) {
+      for (int c = 0; c < nv; c++) {
+        const size_t vi = f[(size_t)nv * i + c];
+        box_add(b, v[3 * vi], v[3 * vi + 1], v[3 * vi + 2], e);
+      }
+    }
+    b = block_reduce_box(b);
+    if (threadIdx.x == 0 && lo < hi) {
+      for (int k = 0; k < 3; k++) {
+        atomicMin(&acc[6 * sg + k], f2o(b.lo[k]));
+        atomicMax(&acc[6 * sg + 3 + k], f2o(b.hi[k]));
+      }
+    }
+  }
+}
+
+template <int KIND>
+__global__ void seg_finalize_kernel(const int *__restrict__ acc, int nseg,
+                                    SceneInfo *__restrict__ scenes) {
+  const int sg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg >= nseg) return;
+  SceneInfo si;
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; k++) {
+    lo[k] = o2f(acc[6 * sg + k]);
+    hi[k] = o2f(acc[6 * sg + 3 + k]);
+    si.lo[k] = lo[k];
+    si.hi[k] = hi[k];
+    si.inv[k] = 1024.0f / (hi[k] - lo[k]);
+  }
+  if (KIND == SRT_TRIANGLES) {
+    double es = (double)(hi[0] - lo[0]);
+    if (es < (double)(hi[1] - lo[1])) es = (double)(hi[1] - lo[1]);
+    if (es < (double)(hi[2] - lo[2])) es = (double)(hi[2] - lo[2]);
+    si.eps_scale = es;
+    si.keps = FLT_EPSILON * (float)es;
+  } else {
+    si.eps_scale = 16.0;
+    si.keps = FLT_EPSILON * 16;
+  }
+  si.nbranches = 0;
+  si.pad = 0;
+  scenes[sg] = si;
+}
+
+template <int KIND>
+__global__ void seg_morton_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f,
+                                  const uint32_t *__restrict__ foff, int nseg, uint32_t N,
+                                  const SceneInfo *__restrict__ scenes,
+                                  uint32_t *__restrict__ codes) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const SceneInfo &sc = scenes[seg_of(foff, nseg, i)];
+    float cx, cy, cz;
+    if (KIND == SRT_TRIANGLES) {
+      const float third = 1.0f / 3.0f;
+      const size_t a = f[3 * (size_t)i], b = f[3 * (size_t)i + 1], c = f[3 * (size_t)i + 2];
+      cx = third * ((v[3 * a] + v[3 * b]) + v[3 * c]);
+      cy = third * ((v[3 * a + 1] + v[3 * b + 1]) + v[3 * c + 1]);
+      cz = third * ((v[3 * a + 2] + v[3 * b + 2]) + v[3 * c + 2]);
+    } else {
+      const float fourth = 1.0f / 4.0f;
+      const size_t a = f[4 * (size_t)i], b = f[4 * (size_t)i + 1], c = f[4 * (size_t)i + 2],
+                   d = f[4 * (size_t)i + 3];
+      cx = fourth * (((v[3 * a] + v[3 * b]) + v[3 * c]) + v[3 * d]);
+      cy = fourth * (((v[3 * a + 1] + v[3 * b + 1]) + v[3 * c + 1]) + v[3 * d + 1]);
+      cz = fourth * (((v[3 * a + 2] + v[3 * b + 2]) + v[3 * c + 2]) + v[3 * d + 2]);
+    }
+    const uint32_t qx = f2u32_x86((cx - sc.lo[0]) * sc.inv[0]);
+    const uint32_t qy = f2u32_x86((cy - sc.lo[1]) * sc.inv[1]);
+    const uint32_t qz = f2u32_x86((cz - sc.lo[2]) * sc.inv[2]);
+    codes[i] = (spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz);
+  }
+}
+
+__global__ void seg_karras_kernel(const uint32_t *__restrict__ codes,
+                                  const uint32_t *__restrict__ foff,
+                                  const uint32_t *__restrict__ ioff, int nseg, uint32_t M,
+                                  uint32_t *__restrict__ kchild, uint8_t *__restrict__ kflags,
+                                  uint2 *__restrict__ krange, uint32_t *__restrict__ kparent,
+                                  uint32_t *__restrict__ lparent) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < M; g += gridDim.x * blockDim.x) {
+    const int sg = seg_of(ioff, nseg, g);
+    const uint32_t fb = __ldg(&foff[sg]), ib = __ldg(&ioff[sg]);
+    const int n = (int)(__ldg(&foff[sg + 1]) - fb);
+    const int i = (int)(g - ib);
+    const uint32_t *c = codes + fb;
+    int d = (kdelta(c, i, i + 1, n) - kdelta(c, i, i - 1, n)) >= 0 ? 1 : -1;
+    int dmin = kdelta(c, i, i - d, n);
+    int lmax = 2;
+    while (kdelta(c, i, i + lmax * d, n) > dmin) lmax *= 2;
+    int l = 0;
+    for (int t = lmax / 2; t >= 1; t /= 2)
+      if (kdelta(c, i, i + (l + t) * d, n) > dmin) l += t;
+    const int j = i + l * d;
+    const int dnode = kdelta(c, i, j, n);
+    int s = 0;
+    for (int k = 2;; k *= 2) {
+      const int t = (l + k - 1) / k;
+      if (t <= 0) break;
+      if (kdelta(c, i, i + (s + t) * d, n) > dnode) s += t;
+      if (t == 1) break;
+    }
+    const int gm = i + s * d + (d < 0 ? d : 0);
+    const int lo = i < j ? i : j, hi = i < j ? j : i;
+    const bool lleaf = (lo == gm), rleaf = (hi == gm + 1);
+    kchild[g] = (uint32_t)gm;
+    kflags[g] = (uint8_t)((lleaf ? 1 : 0) | (rleaf ? 2 : 0));
+    krange[g] = make_uint2((uint32_t)lo, (uint32_t)hi);
+    if (lleaf) lparent[fb + gm] = g; else kparent[ib + gm] = g;
+    if (rleaf) lparent[fb + gm + 1] = g; else kparent[ib + gm + 1] = g;
+    if (i == 0) kparent[g] = kNone;
+  }
+}
+
+template <int KIND>
+__global__ void seg_refit_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f,
+                                 const uint32_t *__restrict__ sidx,
+                                 const uint32_t *__restrict__ foff,
+                                 const uint32_t *__restrict__ ioff, int nseg, uint32_t N,
+                                 const SceneInfo *__restrict__ scenes,
+                                 const uint32_t *__restrict__ lparent,
+                                 const uint32_t *__restrict__ kparent,
+                                 const uint32_t *__restrict__ kchild,
+                                 const uint8_t *__restrict__ kflags,
+                                 uint32_t *__restrict__ counter, Box *__restrict__ ibox,
+                                 float4 *__restrict__ prims, uint32_t *__restrict__ err) {
+  const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= N) return;
+  const int sg = seg_of(foff, nseg, j);
+  const uint32_t fb = __ldg(&foff[sg]), ib = __ldg(&ioff[sg]);
+  const float keps = scenes[sg].keps;
+  const uint32_t p = sidx[j];
+  Box mine;
+  box_init(mine);
+  if (KIND == SRT_TRIANGLES) {
+    const size_t a = f[3 * (size_t)p], b = f[3 * (size_t)p + 1], c = f[3 * (size_t)p + 2];
+    const float4 p0 = make_float4(v[3 * a], v[3 * a + 1], v[3 * a + 2], __uint_as_float(p - fb));
+    const float4 p1 = make_float4(v[3 * b], v[3 * b + 1], v[3 * b + 2], 0.0f);
+    const float4 p2 = make_float4(v[3 * c], v[3 * c + 1], v[3 * c + 2], 0.0f);
+    prims[3 * (size_t)j + 0] = p0;
+    prims[3 * (size_t)j + 1] = p1;
+    prims[3 * (size_t)j + 2] = p2;
+    box_add(mine, p0.x, p0.y, p0.z, keps);
+    box_add(mine, p1.x, p1.y, p1.z, keps);
+    box_add(mine, p2.x, p2.y, p2.z, keps);
+  }
+  uint32_t cur = j;
+  bool cur_leaf = true;
+  uint32_t node = lparent[j];
+  for (uint32_t guard = 0; guard < 2 * N + 64; guard++) {
+    __threadfence();
+    if (atomicAdd(&counter[node], 1u) == 0) return;
+    __threadfence();
+    const uint32_t gl = __ldcg(&kchild[node]);
+    const uint8_t fl = __ldcg(&kflags[node]);
+    const bool lleaf = fl & 1, rleaf = fl & 2;
+    const uint32_t left = lleaf ? fb + gl : ib + gl;
+    const uint32_t right = rleaf ? fb + gl + 1 : ib + gl + 1;
+    const bool i_am_left = (cur == left) && (cur_leaf == lleaf);
+    const uint32_t sib = i_am_left ? right : left;
+    const bool sib_leaf = i_am_left ? rleaf : lleaf;
+    Box sb;
+    if (sib_leaf) {
+      sb = cache_box<KIND>(prims, sib, keps);
+    } else {
+      const float *src = reinterpret_cast<const float *>(&ibox[sib]);
+      sb.lo[0] = __ldcg(src + 0); sb.lo[1] = __ldcg(src + 1); sb.lo[2] = __ldcg(src + 2);
+      sb.hi[0] = __ldcg(src + 3); sb.hi[1] = __ldcg(src + 4); sb.hi[2] = __ldcg(src + 5);
+    }
+    mine = i_am_left ? box_merge(mine, sb) : box_merge(sb, mine);
+    ibox[node] = mine;
+    if (node == ib) return;  // scene root
+    cur = node;
+    cur_leaf = false;
+    node = __ldcg(&kparent[node]);
+    if (node == kNone) return;
+  }
+  atomicOr(err, kErrTree);
+}
+
+__global__ void seg_level_kernel(const uint2 *__restrict__ krange,
+                                 const uint32_t *__restrict__ kparent,
+                                 const uint32_t *__restrict__ ioff, int nseg, uint32_t M,
+                                 int max_leaf, uint32_t *__restrict__ flag) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < M; g += gridDim.x * blockDim.x) {
+    const uint32_t root = __ldg(&ioff[seg_of(ioff, nseg, g)]);
+    const uint2 r = krange[g];
+    uint32_t fl = 0;
+    if (g == root) {
+      fl = 1;
+    } else if (r.y - r.x > (uint32_t)max_leaf) {
+      int lvl = 0;
+      uint32_t x = g;
+      while (x != root && lvl <= kMaxLevel) {
+        x = kparent[x];
+        lvl++;
+      }
+      fl = (lvl <= kMaxLevel) ? 1u : 0u;
+    }
+    flag[g] = fl;
+  }
+}
+
+template <int KIND>
+__global__ void seg_emit_node2_kernel(const uint32_t *__restrict__ codes,
+                                      const uint32_t *__restrict__ kchild,
+                                      const uint8_t *__restrict__ kflags,
+                                      const uint2 *__restrict__ krange,
+                                      const uint32_t *__restrict__ flag,
+                                      const uint32_t *__restrict__ slot,
+                                      const Box *__restrict__ ibox,
+                                      const float4 *__restrict__ prims,
+                                      const SceneInfo *__restrict__ scenes,
+                                      const uint32_t *__restrict__ foff,
+                                      const uint32_t *__restrict__ ioff, int nseg, uint32_t M,
+                                      Node2 *__restrict__ nodes, uint32_t *__restrict__ err) {
+  for (uint32_t g = blockIdx.x * blockDim.x + threadIdx.x; g < M; g += gridDim.x * blockDim.x) {
+    if (!flag[g]) continue;
+    const int sg = seg_of(ioff, nseg, g);
+    const uint32_t fb = __ldg(&foff[sg]), ib = __ldg(&ioff[sg]);
+    const float keps = scenes[sg].keps;
+    const uint32_t gl = kchild[g];
+    const uint8_t fl = kflags[g];
+    Box bx[2];
+    uint32_t ref[2], cnt[2];
+    for (int side = 0; side < 2; side++) {
+      const uint32_t cl = gl + side;
+      if (fl & (1 << side)) {
+        bx[side] = cache_box<KIND>(prims, fb + cl, keps);
+        ref[side] = fb + cl;
+        cnt[side] = 1;
+      } else {
+        const uint32_t cg = ib + cl;
+        bx[side] = ibox[cg];
+        if (flag[cg]) {
+          ref[side] = slot[cg];
+          cnt[side] = 0;
+        } else {
+          const uint2 r = krange[cg];
+          ref[side] = fb + r.x;
+          cnt[side] = r.y - r.x + 1;
+        }
+      }
+      if (cnt[side] > kCountMask) atomicOr(err, kErrTree);
+    }
+    const uint32_t axis = (uint32_t)split_axis(codes[fb + (g - ib)]);
+    Node2 nd;
+    nd.a = make_float4(bx[0].lo[0], bx[0].lo[1], bx[0].lo[2], bx[0].hi[0]);
+    nd.b = make_float4(bx[0].hi[1], bx[0].hi[2], bx[1].lo[0], bx[1].lo[1]);
+    nd.c = make_float4(bx[1].lo[2], bx[1].hi[0], bx[1].hi[1], bx[1].hi[2]);
+    nd.d = make_uint4(ref[0], ref[1], (cnt[0] & kCountMask) | (axis << 30), cnt[1] & kCountMask);
+    nodes[slot[g]] = nd;
+  }
+}
+
+__global__ void seg_roots_kernel(const uint32_t *__restrict__ slot,
+                                 const uint32_t *__restrict__ flag,
+                                 const uint32_t *__restrict__ ioff, int nseg, uint32_t M,
+                                 uint32_t *__restrict__ roots) {
+  const int sg = blockIdx.x * blockDim.x + threadIdx.x;
+  if (sg < nseg) roots[sg] = slot[ioff[sg]];
+  if (sg == 0) roots[nseg] = slot[M - 1] + flag[M - 1];  // total branch nodes
+}
+
+}  // namespace
+
+// Batched triangle build: see the block comment above seg_bbox_kernel.
+// h_foff: host copy of the nseg+1 primitive offsets (each scene >= 2 faces).
+srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32_t *f,
+                       const uint32_t *h_foff, int nseg) {
+  constexpr int KIND = SRT_TRIANGLES;
+  cudaStream_t st = ctx->stream;
+  const uint32_t N = h_foff[nseg];
+  const uint32_t M = N - (uint32_t)nseg;
+  cudaError_t e;
+#define ENSURE(buf, bytes)                                   \
+  do {                                                       \
+    if ((e = (buf).ensure(bytes)) != cudaSuccess)            \
+      return cuda_status(e, "batch allocation " #buf);       \
+  } while (0)
+  ENSURE(bt.codes, (size_t)N * 4);
+  ENSURE(bt.indices, (size_t)N * 4);
+  ENSURE(bt.prims, (size_t)N * 3 * sizeof(float4));
+  ENSURE(bt.nodes, (size_t)M * sizeof(Node2));
+  ENSURE(bt.scenes, (size_t)nseg * sizeof(SceneInfo));
+  ENSURE(bt.roots, (size_t)(nseg + 1) * 4);
+  ENSURE(bt.acc, (size_t)nseg * 6 * 4);
+  ENSURE(ctx->s_kchild, (size_t)M * 4);
+  ENSURE(ctx->s_kflags, M);
+  ENSURE(ctx->s_krange, (size_t)M * sizeof(uint2));
+  ENSURE(ctx->s_kparent, (size_t)M * 4);
+  ENSURE(ctx->s_lparent, (size_t)N * 4);
+  ENSURE(ctx->s_counter, (size_t)M * 4);
+  ENSURE(ctx->s_ibox, (size_t)M * sizeof(Box));
+  ENSURE(ctx->s_flag, (size_t)M * 4);
+  ENSURE(ctx->s_slot, (size_t)M * 4);
+#undef ENSURE
+  srt_status s = sort_scratch(ctx, N);
+  if (s != SRT_OK) return s;
+  {
+    size_t need = 64;
+    for (size_t t = ((size_t)kRsBins * ((N + kRsTile - 1) / kRsTile) + kScanTile - 1) / kScanTile;
+         t > 1; t = (t + kScanTile - 1) / kScanTile)
+      need += t + 1;
+    for (size_t t = (M + kScanTile - 1) / kScanTile; t > 1; t = (t + kScanTile - 1) / kScanTile)
+      need += t + 1;
+    if ((e = ctx->s_scan.ensure(need * 4)) != cudaSuccess) return cuda_status(e, "scan scratch");
+  }
+  const uint32_t *foff = bt.foff.as<uint32_t>();
+  const uint32_t *ioff = bt.ioff.as<uint32_t>();
+  SceneInfo *scenes = bt.scenes.as<SceneInfo>();
+  uint32_t *codes = bt.codes.as<uint32_t>();
+  uint32_t *idx = bt.indices.as<uint32_t>();
+  int *acc = bt.acc.as<int>();
+  const int gsm = ctx->num_sms * 16;
+  seg_bbox_init_kernel<<<1, 256, 0, st>>>(acc, nseg);
+  seg_bbox_kernel<KIND><<<(N + kSegTile - 1) / kSegTile, 256, 0, st>>>(v, f, foff, nseg, N, acc);
+  seg_finalize_kernel<KIND><<<(nseg + 63) / 64, 64, 0, st>>>(acc, nseg, scenes);
+  seg_morton_kernel<KIND><<<grid_for(N, kBlock, gsm), kBlock, 0, st>>>(v, f, foff, nseg, N,
+                                                                       scenes, codes);
+  ctx->launches += 4;
+  s = cuda_status(cudaGetLastError(), "batch bbox/morton");
+  if (s != SRT_OK) return s;
+  s = sort_pairs_seg(ctx, codes, idx, N, true, foff, nseg);
+  if (s != SRT_OK) return s;
+  uint32_t *kchild = ctx->s_kchild.as<uint32_t>();
+  uint8_t *kflags = ctx->s_kflags.as<uint8_t>();
+  uint2 *krange = ctx->s_krange.as<uint2>();
+  uint32_t *kparent = ctx->s_kparent.as<uint32_t>();
+  uint32_t *lparent = ctx->s_lparent.as<uint32_t>();
+  uint32_t *counter = ctx->s_counter.as<uint32_t>();
+  Box *ibox = ctx->s_ibox.as<Box>();
+  uint32_t *flag = ctx->s_flag.as<uint32_t>();
+  uint32_t *slot = ctx->s_slot.as<uint32_t>();
+  seg_karras_kernel<<<grid_for(M, kBlock, gsm), kBlock, 0, st>>>(codes, foff, ioff, nseg, M,
+                                                               kchild, kflags, krange, kparent,
+                                                               lparent);
+  if ((e = cudaMemsetAsync(counter, 0, (size_t)M * 4, st)) != cudaSuccess)
+    return cuda_status(e, "refit counters");
+  seg_refit_kernel<KIND><<<(N + kBlock - 1) / kBlock, kBlock, 0, st>>>(
+      v, f, idx, foff, ioff, nseg, N, scenes, lparent, kparent, kchild, kflags, counter, ibox,
+      bt.prims.as<float4>(), ctx->d_err);
+  seg_level_kernel<<<grid_for(M, kBlock, gsm), kBlock, 0, st>>>(krange, kparent, ioff, nseg, M,
+                                                              PrimTraits<KIND>::kMaxLeaf, flag);
+  ctx->launches += 3;
+  s = cuda_status(cudaGetLastError(), "batch karras/refit/level");
+  if (s != SRT_OK) return s;
+  s = exclusive_scan(ctx, flag, slot, M);
+  if (s != SRT_OK) return s;
+  seg_emit_node2_kernel<KIND><<<grid_for(M, kBlock, gsm), kBlock, 0, st>>>(
+      codes, kchild, kflags, krange, flag, slot, ibox, bt.prims.as<float4>(), scenes, foff, ioff,
+      nseg, M, bt.nodes.as<Node2>(), ctx->d_err);
+  seg_roots_kernel<<<(nseg + 63) / 64, 64, 0, st>>>(slot, flag, ioff, nseg, M,
+                                                   bt.roots.as<uint32_t>());
+  ctx->launches += 2;
+  return cuda_status(cudaGetLastError(), "batch emit");
+}
 
 srt_status build_accel(srt_accel *a, const float *v, const uint32_t *f,
                        const float *radius, float constr, size_t n) {

@@ -142,6 +142,13 @@ struct srt_accel {
 };
 
 namespace srt {
+// Many triangle scenes built as one forest (srt_batch).
+struct BatchTree {
+  DevBuf nodes, indices, codes, prims, scenes, roots, acc, foff, ioff, roff;
+  int nseg = 0;
+  size_t nprims = 0, nrays = 0;
+};
+
 void set_error(const std::string &msg);
 srt_status cuda_status(cudaError_t e, const char *what);
 // pointer classification
@@ -158,6 +165,11 @@ srt_status sort_pairs(srt_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals,
                       size_t n, bool identity_vals);
 srt_status stage_karras(srt_ctx *ctx, const uint32_t *d_codes, size_t n,
                         uint32_t *d_child, uint8_t *d_flags);
+srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32_t *f,
+                       const uint32_t *h_foff, int nseg);
+srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
+                              srt_hit *hits, int block, int rays_per_thread,
+                              unsigned long long *stats);
 
 // traversal (srt_trace.cu)
 srt_status launch_trace(srt_accel *a, const srt_ray *d_rays, size_t n,

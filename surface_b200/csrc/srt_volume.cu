@@ -34,6 +34,17 @@ struct Sample {
   float rho;
 };
 
+// Pixel of thread index `idx`: each warp covers an 8x4 tile (blocks of 128
+// threads a 16x8 tile) so the rays of a warp sample neighbouring voxels.
+__device__ __forceinline__ bool tile_pixel(int idx, int W, int H, int &px, int &py) {
+  const int lane = idx & 31, warp = idx >> 5;
+  const int tiles_x = (W + 7) >> 3;
+  const int tx = warp % tiles_x, ty = warp / tiles_x;
+  px = tx * 8 + (lane & 7);
+  py = ty * 4 + (lane >> 3);
+  return px < W && py < H;
+}
+
 __device__ __forceinline__ float lerpf(float t, float a, float b) {
   return (1.f - t) * a + t * b;
 }
@@ -140,9 +151,9 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
                const float4 *__restrict__ tf, float4 *__restrict__ image,
                float *__restrict__ trans) {
   const int W = K.p.width, H = K.p.height;
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix >= W * H) return;
-  const int px = pix % W, py = pix / W;
+  int px, py;
+  if (!tile_pixel(blockIdx.x * blockDim.x + threadIdx.x, W, H, px, py)) return;
+  const int pix = py * W + px;
   float o[3], d[3], t0, t1;
   pixel_ray(K.p, px, py, o, d);
   float C0 = 0.f, C1 = 0.f, C2 = 0.f, T = 1.0f;
@@ -174,20 +185,46 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
   if (trans) trans[pix] = T;
 }
 
-constexpr int kTfMax = 2048;  // 4 * kTfMax floats of shared memory in the adjoint
+constexpr int kTfCopies = 8;  // copies of the block-local TF gradient
+
+__device__ __forceinline__ void flush_tf(float *g, int i0, int i1, float (&a0)[4],
+                                         float (&a1)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (a0[k] != 0.0f) atomicAdd(&g[4 * i0 + k], a0[k]);
+    if (a1[k] != 0.0f) atomicAdd(&g[4 * i1 + k], a1[k]);
+    a0[k] = 0.0f;
+    a1[k] = 0.0f;
+  }
+}
+
+__device__ __forceinline__ void flush_dens(float *__restrict__ g, const int (&cx)[8],
+                                           float (&a)[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; k++) {
+    if (a[k] != 0.0f) atomicAdd(&g[cx[k]], a[k]);
+    a[k] = 0.0f;
+  }
+}
+constexpr int kTfMax = 1024;  // kTfCopies * (4 * kTfMax + 1) floats of shared memory
 
 __global__ void __launch_bounds__(128)
 vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
                const float4 *__restrict__ tf, const float *__restrict__ trans,
                const float4 *__restrict__ gimg, float *__restrict__ gdens,
                float *__restrict__ gtf) {
-  extern __shared__ float s_gtf[];  // 4 * tfn block-local TF gradient
-  for (int i = threadIdx.x; i < 4 * K.tfn; i += blockDim.x) s_gtf[i] = 0.0f;
+  // Block-local transfer-function gradient in kTfCopies copies, lane-hashed
+  // so that lanes accumulating into the same entry hit different copies;
+  // copies are padded by one word to fall on different banks.
+  extern __shared__ float s_gtf[];
+  const int tstride = 4 * K.tfn + 1;
+  for (int i = threadIdx.x; i < kTfCopies * tstride; i += blockDim.x) s_gtf[i] = 0.0f;
   __syncthreads();
+  float *my_gtf = s_gtf + (threadIdx.x & (kTfCopies - 1)) * tstride;
   const int W = K.p.width, H = K.p.height;
-  const int pix = blockIdx.x * blockDim.x + threadIdx.x;
-  if (pix < W * H) {
-    const int px = pix % W, py = pix / W;
+  int px, py;
+  if (tile_pixel(blockIdx.x * blockDim.x + threadIdx.x, W, H, px, py)) {
+    const int pix = py * W + px;
     float o[3], d[3], t0, t1;
     pixel_ray(K.p, px, py, o, d);
     if (slab(o, d, t0, t1)) {
@@ -198,6 +235,17 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
       float Tn = Tfin;
       float Cb0 = 0.f, Cb1 = 0.f, Cb2 = 0.f;
       const float top = (float)(K.tfn - 1);
+      // Run-length accumulators: consecutive samples often share the
+      // transfer-function bin (always in empty space) and the voxel cell
+      // (the step is half a voxel); contributions are summed in registers
+      // and flushed when the bin / cell changes.
+      int run_i0 = -1;
+      float ta0[4] = {0.f, 0.f, 0.f, 0.f}, ta1[4] = {0.f, 0.f, 0.f, 0.f};
+      int run_cell = -1;
+      int run_cx[8];
+      float da[8];
+#pragma unroll
+      for (int cc = 0; cc < 8; cc++) { run_cx[cc] = 0; da[cc] = 0.0f; }
       for (int s = ns - 1; s >= 0; s--) {
         const float t = t0 + ((float)s + 0.5f) * K.p.step;
         const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
@@ -215,39 +263,47 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         float al = 1.0f - e;
         const bool clamped = al > K.p.alpha_max;
         if (clamped) al = K.p.alpha_max;
-        const float om = 1.0f - al;
-        const float Tk = Tn / om;
+        const float iom = 1.0f / (1.0f - al);
+        const float Tk = Tn * iom;  // transmittance in front of sample s
         const float gc0 = g.x * Tk * al, gc1 = g.y * Tk * al, gc2 = g.z * Tk * al;
-        float ga = g.x * (Tk * c.x - Cb0 / om) + g.y * (Tk * c.y - Cb1 / om) +
-                   g.z * (Tk * c.z - Cb2 / om) + g.w * (Tfin / om);
+        float ga = g.x * (Tk * c.x - Cb0 * iom) + g.y * (Tk * c.y - Cb1 * iom) +
+                   g.z * (Tk * c.z - Cb2 * iom) + g.w * (Tfin * iom);
         const float gc3 = clamped ? 0.0f : ga * K.p.sigma_scale * K.p.step * e;
-        // transfer-function gradient (block-local)
+        // transfer-function gradient: i1 = i0 + 1 except at the top entry
+        if (i0 != run_i0) {
+          if (run_i0 >= 0) flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
+          run_i0 = i0;
+        }
         const float wf0 = 1.0f - f, wf1 = f;
-        atomicAdd(&s_gtf[4 * i0 + 0], wf0 * gc0);
-        atomicAdd(&s_gtf[4 * i0 + 1], wf0 * gc1);
-        atomicAdd(&s_gtf[4 * i0 + 2], wf0 * gc2);
-        atomicAdd(&s_gtf[4 * i0 + 3], wf0 * gc3);
-        atomicAdd(&s_gtf[4 * i1 + 0], wf1 * gc0);
-        atomicAdd(&s_gtf[4 * i1 + 1], wf1 * gc1);
-        atomicAdd(&s_gtf[4 * i1 + 2], wf1 * gc2);
-        atomicAdd(&s_gtf[4 * i1 + 3], wf1 * gc3);
+        ta0[0] += wf0 * gc0; ta0[1] += wf0 * gc1; ta0[2] += wf0 * gc2; ta0[3] += wf0 * gc3;
+        ta1[0] += wf1 * gc0; ta1[1] += wf1 * gc1; ta1[2] += wf1 * gc2; ta1[3] += wf1 * gc3;
         if (inr) {
           const float4 a = __ldg(&tf[i0]), b = __ldg(&tf[i1]);
           const float drho = (gc0 * (b.x - a.x) + gc1 * (b.y - a.y) + gc2 * (b.z - a.z) +
                               gc3 * (b.w - a.w)) * top;
+          if (smp.cx[0] != run_cell) {
+            if (run_cell >= 0) flush_dens(gdens, run_cx, da);
+            run_cell = smp.cx[0];
 #pragma unroll
-          for (int cc = 0; cc < 8; cc++) atomicAdd(&gdens[smp.cx[cc]], smp.w[cc] * drho);
+            for (int cc = 0; cc < 8; cc++) run_cx[cc] = smp.cx[cc];
+          }
+#pragma unroll
+          for (int cc = 0; cc < 8; cc++) da[cc] += smp.w[cc] * drho;
         }
         Cb0 += Tk * al * c.x;
         Cb1 += Tk * al * c.y;
         Cb2 += Tk * al * c.z;
         Tn = Tk;
       }
+      if (run_i0 >= 0) flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
+      if (run_cell >= 0) flush_dens(gdens, run_cx, da);
     }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 4 * K.tfn; i += blockDim.x) {
-    const float v = s_gtf[i];
+    float v = 0.0f;
+#pragma unroll
+    for (int c = 0; c < kTfCopies; c++) v += s_gtf[c * tstride + i];
     if (v != 0.0f) atomicAdd(&gtf[i], v);
   }
 }
@@ -359,7 +415,8 @@ SRT_API srt_status srt_volume_march_fwd(srt_ctx *ctx, const srt_volume_params *p
     if ((e = tmp_tr.ensure(npix * 4)) != cudaSuccess) return cuda_status(e, "trans");
     dtr = tmp_tr.as<float>();
   }
-  vol_fwd_kernel<<<(unsigned)((npix + 127) / 128), 128, 0, st>>>(
+  const size_t nthreads = (size_t)((params->width + 7) / 8) * ((params->height + 3) / 4) * 32;
+  vol_fwd_kernel<<<(unsigned)((nthreads + 127) / 128), 128, 0, st>>>(
       K, static_cast<const float *>(dd), static_cast<const float4 *>(dt),
       reinterpret_cast<float4 *>(di), dtr);
   ctx->launches++;
@@ -397,8 +454,15 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx, const srt_volume_params *p
     return s;
   if ((s = vol_view(ctx, transmittance, npix * 4, s_tr, &dtr, st)) != SRT_OK) return s;
   if ((s = vol_view(ctx, grad_image, npix * 16, s_g, &dg, st)) != SRT_OK) return s;
-  size_t shmem = (size_t)tf_entries * 4 * sizeof(float);
-  vol_bwd_kernel<<<(unsigned)((npix + 127) / 128), 128, shmem, st>>>(
+  size_t shmem = (size_t)kTfCopies * (4 * tf_entries + 1) * sizeof(float);
+  if (shmem > 48 * 1024) {
+    cudaError_t ea = cudaFuncSetAttribute(vol_bwd_kernel,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)shmem);
+    if (ea != cudaSuccess) return cuda_status(ea, "volume bwd shared memory");
+  }
+  const size_t nthreads = (size_t)((params->width + 7) / 8) * ((params->height + 3) / 4) * 32;
+  vol_bwd_kernel<<<(unsigned)((nthreads + 127) / 128), 128, shmem, st>>>(
       K, static_cast<const float *>(dd), static_cast<const float4 *>(dt),
       static_cast<const float *>(dtr), static_cast<const float4 *>(dg), grad_density,
       grad_tf);
