@@ -86,7 +86,22 @@ def make_workload(name):
                                         "step 0.5 voxel, emission-absorption forward + "
                                         "adjoint of an L2 loss",
                             "rays": 512 * 512})
+    if name == "batched":
+        B = S.batched_scenes()
+        return dict(kind="batched", B=B, rays=B["rays"],
+                    config={"workload": "batched64: 64 displaced-octasphere triangle scenes, "
+                                        "faces log-uniform in [1e3,1e6] (>= 1024), square "
+                                        "pinhole images of side 128/256/512/1024",
+                            "scenes": 64, "prims": int(B["face_offsets"][-1]),
+                            "rays": int(B["ray_offsets"][-1])})
     raise SystemExit(f"unknown workload {name}")
+
+
+# build: vertices of each triangle (3 x 12) read twice (bbox, Morton) and once
+# more in the refit, code + index written and read per radix pass (5 passes
+# x 16), leaf record (48) written, internal node (64) written, Karras tree
+# arrays (~40 per node) written and read
+BUILD_BYTES_PER_TRI = 3 * 36 + 5 * 16 + 48 + 64 + 40
 
 
 def algorithmic_bytes_per_ray(kind, stats, nrays):
@@ -172,24 +187,56 @@ def cpu_reference_step(W, nthreads=0, stride=4):
     return value, tb, tt, sample.size, ("reference" if use_ref else "port")
 
 
+def cpu_reference_batched(W, nthreads=0, stride=16):
+    """Reference loop over the scenes: Build32 of every scene + OpenMP
+    Traverse of every 16th ray of each.  Returns (Mrays/s scaled to all rays,
+    build s, trace s, sample rays, kind)."""
+    from oracle import oracle as O
+    B = W["B"]
+    use_ref = O.have_ref() and O.ref() is not None
+    fo, ro = B["face_offsets"], B["ray_offsets"]
+    tb = tt = 0.0
+    ns = 0
+    for s in range(fo.size - 1):
+        faces = B["faces"][int(fo[s]):int(fo[s + 1])]
+        t0 = time.perf_counter()
+        acc = (O.RefAccel if use_ref else O.OracleAccel)(O.TRI, B["vertices"], faces)
+        tb += time.perf_counter() - t0
+        sample = B["rays"][int(ro[s]):int(ro[s + 1])][::stride]
+        t0 = time.perf_counter()
+        if use_ref:
+            acc.trace(sample, nthreads=nthreads, chunk=64)
+        else:
+            acc.trace(sample, nthreads=nthreads)
+        tt += time.perf_counter() - t0
+        ns += sample.size
+        del acc
+    nr = int(ro[-1])
+    value = nr / (tb + tt * (nr / ns)) / 1e6
+    return value, tb, tt, ns, ("reference" if use_ref else "port")
+
+
 def run_reference_arm(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cores = os.cpu_count() or 1
+    step = cpu_reference_batched if W["kind"] == "batched" else cpu_reference_step
     for _ in range(args.warmup):
-        cpu_reference_step(W)
+        step(W)
     vals, tbs, tts = [], [], []
     for _ in range(args.steps):
-        v, tb, tt, ns, kind = cpu_reference_step(W)
+        v, tb, tt, ns, kind = step(W)
         vals.append(v)
         tbs.append(tb)
         tts.append(tt)
     value = statistics.median(vals)
     nr = W["rays"].size
     ms = 1e3 * nr / (value * 1e6)
+    stride = 16 if W["kind"] == "batched" else 4
     line = {
-        "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": "Mrays/s",
+        "impl": "reference", "metric": METRIC_BATCH if W["kind"] == "batched" else METRIC,
+        "value": round(value, 4), "unit": "Mrays/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPE[W["kind"]], "data": "synthetic",
@@ -197,8 +244,9 @@ def run_reference_arm(args, W):
         "build_ms": round(1e3 * statistics.median(tbs), 3),
         "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores,
                          "kind": kind,
-                         "sample": f"full Build32 + every 4th ray ({ns} of {nr}) per step, "
-                                   f"trace time scaled to all rays; median of {args.steps}"},
+                         "sample": f"full Build32 + every {stride}th ray ({ns} of {nr}) per "
+                                   f"step, trace time scaled to all rays; median of "
+                                   f"{args.steps}"},
         "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -207,8 +255,9 @@ def run_reference_arm(args, W):
 
 METRIC = "Mrays/s (LBVH build + closest hit per step)"
 METRIC_VOL = "Mrays/s (volume march forward + adjoint per step)"
+METRIC_BATCH = "Mrays/s (64-scene batched LBVH build + closest hit per step)"
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
-         "volume": "f32"}
+         "volume": "f32", "batched": "f32"}
 
 
 def run_volume(args, W):
@@ -277,6 +326,202 @@ def run_volume(args, W):
             "fwd_bwd_over_fwd": round(fb_ms / f_ms, 3), "clocks": clk.summary(),
             "cpu_baseline": cpu}
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- batched
+def run_batched(args, W):
+    """One step = every scene built and traced.  Timed twice per step, each
+    bracketed by CUDA events on the launching stream with an L2 flush before:
+    (a) the batch (srt_batch_build_trace: one launch sequence over all scenes,
+    autotuned, replayed from a CUDA graph), (b) the per-scene plain loop
+    (srt_accel_build_triangles + srt_trace_closest per scene, one accel per
+    scene, same stream).  value = rays / batch step time."""
+    import ctypes as C
+
+    import torch
+    import torch.distributed as dist
+
+    import surface_b200 as sb
+    from surface_b200 import _lib
+    from surface_b200.batch import TriangleBatch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+    B = W["B"]
+    fo, ro = B["face_offsets"], B["ray_offsets"]
+    ns = fo.size - 1
+    nr = int(ro[-1])
+    v = torch.as_tensor(B["vertices"], device=dev)
+    f = torch.as_tensor(B["faces"].view(np.int32), device=dev)
+    r = torch.as_tensor(B["rays"].view(np.float32).reshape(-1, 8), device=dev)
+    hits = torch.empty((nr, 4), dtype=torch.float32, device=dev)
+    hits_loop = torch.empty((nr, 4), dtype=torch.float32, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+
+    tb = TriangleBatch(local)
+
+    def batch_step():
+        tb.build_trace(v, f, fo, r, ro, hits=hits)
+
+    # the per-scene loop straight through the C ABI (no Python wrapper cost)
+    L = _lib.load()
+    ctx = sb.Context(local)
+    ctx.use_torch_stream()
+    accs = []
+    for _ in range(ns):
+        h = C.c_void_p()
+        _lib.check(L.srt_accel_create(ctx.h, _lib.SRT_TRIANGLES, C.byref(h)))
+        accs.append(h)
+    nv = v.shape[0]
+    vp, fp, rp, hp = v.data_ptr(), f.data_ptr(), r.data_ptr(), hits_loop.data_ptr()
+    build = L.srt_accel_build_triangles
+    trace = L.srt_trace_closest
+    chk = _lib.check
+
+    def loop_step():
+        for s in range(ns):
+            a, b = int(fo[s]), int(fo[s + 1])
+            chk(build(accs[s], vp, nv, fp + 12 * a, b - a))
+            x, y = int(ro[s]), int(ro[s + 1])
+            chk(trace(accs[s], rp + 32 * x, y - x, hp + 16 * x, None))
+
+    for _ in range(max(args.warmup, 3)):
+        batch_step()
+        loop_step()
+    torch.cuda.synchronize()
+    _lib.check(L.srt_ctx_synchronize(ctx.h))
+    same = torch.equal(hits.view(torch.int32), hits_loop.view(torch.int32))
+    block, rpt, captured, kpc = tb.config()
+
+    # traversal work counters of every scene (one untimed pass) for the roofline
+    st = torch.zeros(4, dtype=torch.int64, device=dev)
+    opts = _lib.TraceOpts(None, None, None, None, None, st.data_ptr(), 0, 0)
+    for s in range(ns):
+        x, y = int(ro[s]), int(ro[s + 1])
+        _lib.check(trace(accs[s], rp + 32 * x, y - x, hp + 16 * x, C.byref(opts)))
+    torch.cuda.synchronize()
+    stats = st.cpu().numpy().astype(np.float64)[:3]
+
+    l_b0 = tb.launches()
+    l_l0 = L.srt_ctx_launch_count(ctx.h)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            batch_step()
+            ev[k][1].record()
+            flush.zero_()
+            ev[k][2].record()
+            loop_step()
+            ev[k][3].record()
+        torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    launches = tb.launches() - l_b0
+    loop_launches = L.srt_ctx_launch_count(ctx.h) - l_l0
+    b_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    l_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    t = torch.tensor([sum(b_ms), sum(l_ms)], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_per_step = float(t[0]) / args.steps
+    loop_ms = float(t[1]) / args.steps
+    value = world * nr / (ms_per_step * 1e-3) / 1e6
+
+    # ---- e2e: scenes and rays copied in from pinned host memory, hits out
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_v = pin(B["vertices"])
+    h_f = pin(B["faces"].view(np.int32))
+    h_r = pin(B["rays"].view(np.float32).reshape(-1, 8))
+    h_h = torch.empty((nr, 4), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        v.copy_(h_v, non_blocking=True)
+        f.copy_(h_f, non_blocking=True)
+        r.copy_(h_r, non_blocking=True)
+        batch_step()
+        h_h.copy_(hits, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = 1e3 * sum(e2e_s) / len(e2e_s)
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = world * nr / (float(te.item()) * 1e-3) / 1e6
+    h2d = (h_v.numel() + h_f.numel() + h_r.numel()) * 4
+    d2h = h_h.numel() * 4
+
+    # ---- roofline of the whole batched step (build + trace in one graph):
+    # traversal bytes from the work counters + build bytes per primitive
+    hbm, src = peaks()
+    nprim = int(fo[-1])
+    trace_bytes = algorithmic_bytes_per_ray("tri", stats, nr) * nr
+    build_bytes = nprim * BUILD_BYTES_PER_TRI
+    achieved = (trace_bytes + build_bytes) / (ms_per_step * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "whole batched step (graph)",
+                "achieved": round(achieved, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(achieved / hbm, 4), "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_step": int(trace_bytes + build_bytes),
+                "visits_per_ray": [round(float(x) / nr, 3) for x in stats]}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cv, ctb, ctt, cns, ck = cpu_reference_batched(W)
+        cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
+               "kind": ck, "build_s": round(ctb, 3), "trace_s": round(ctt, 3),
+               "sample": f"Build32 of all 64 scenes + every 16th ray of each ({cns} of "
+                         f"{nr}), trace time scaled to all rays"}
+    for a in accs:
+        L.srt_accel_destroy(a)
+    if rank == 0:
+        line = {
+            "metric": METRIC_BATCH, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)",
+                           parallelism=f"replicas x{world}"),
+            "per_scene_loop_ms": round(loop_ms, 4),
+            "speedup_vs_per_scene_loop": round(loop_ms / ms_per_step, 3),
+            "batch_launch_shape": {"block": block, "rays_per_grab": rpt,
+                                   "graph_captured": captured, "kernels_per_call": kpc},
+            "loop_kernels_per_step": int(loop_launches // args.steps),
+            "hits_identical_to_loop": bool(same),
+            "clocks": clk.summary(),
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    tb.close()
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 # ---------------------------------------------------------------- GPU arm
@@ -478,7 +723,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
-                    choices=["tet", "tri", "particles", "volume"])
+                    choices=["tet", "tri", "particles", "volume", "batched"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     W = make_workload(args.workload)
@@ -489,6 +734,8 @@ def main():
         return
     if args.impl == "reference":
         run_reference_arm(args, W)
+    elif args.workload == "batched":
+        run_batched(args, W)
     else:
         run_ours(args, W)
 

@@ -263,10 +263,16 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx,
                                         float *grad_density, float *grad_tf);
 
 /* ---- batched build + trace ---------------------------------------------- */
-/* Many triangle scenes of uneven size, built and traced in one pass.
- * Scene s owns faces [face_offsets[s], face_offsets[s+1]) of `faces` (vertex
- * ids into `vertices`) and rays [ray_offsets[s], ray_offsets[s+1]).  Hits
- * are written per ray.  All arrays are device pointers. */
+/* Many triangle scenes of uneven size, built and traced in one pass (the
+ * per-scene Build32 + Traverse of every scene, with identical results).
+ * Scene s owns faces [face_offsets[s], face_offsets[s+1]) of `faces`
+ * (vertex ids into `vertices`) and rays [ray_offsets[s], ray_offsets[s+1]);
+ * hits are written per ray, prim = face index within the scene.  vertices,
+ * faces, rays and hits are device pointers; the nscenes+1 offsets are host
+ * arrays.  1 <= nscenes <= 256, each scene >= 2 faces.
+ * The first call autotunes the traversal launch shape; the second call with
+ * the same arguments captures build + trace in a CUDA graph (on the
+ * context's own stream) and later identical calls replay it. */
 typedef struct srt_batch srt_batch;
 SRT_API srt_status srt_batch_create(srt_ctx *ctx, srt_batch **out);
 SRT_API srt_status srt_batch_destroy(srt_batch *b);
@@ -277,6 +283,12 @@ SRT_API srt_status srt_batch_build_trace(srt_batch *b, int32_t nscenes,
                                          const srt_ray *rays,
                                          const uint64_t *ray_offsets,
                                          srt_hit *hits);
+/* Launch shape picked by the autotuner, whether a graph is captured, and
+ * the kernels one call runs. */
+SRT_API srt_status srt_batch_config(srt_batch *b, int32_t *block,
+                                    int32_t *rays_per_thread,
+                                    int32_t *graph_captured,
+                                    uint64_t *kernels_per_call);
 
 #ifdef __cplusplus
 }

@@ -83,6 +83,7 @@ _SIGS = {
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],
+    "srt_batch_config": [_P, _P, _P, _P, _P],
 }
 _RESTYPES = {"srt_last_error": C.c_char_p, "srt_ctx_get_stream": _P,
              "srt_ctx_launch_count": C.c_uint64}

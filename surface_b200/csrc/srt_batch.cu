@@ -1,18 +1,122 @@
-// srt_batch.cu -- many triangle scenes built and traced in one call.
+// srt_batch.cu -- many triangle scenes built and traced as one forest.
 //
-// This first version runs the plain build + trace per scene on the
-// context stream (the per-scene loop the batched workload is measured
-// against); the scene table is read once from device memory.
+// Every build stage runs once over all scenes (srt_build.cu, build_batch)
+// and all rays are traced by one persistent kernel (srt_trace.cu,
+// launch_trace_batch).  The first call runs eagerly and autotunes the
+// traversal launch shape (block size x rays per grab, timed with CUDA
+// events); the second identical call captures the whole sequence in a CUDA
+// graph, later identical calls replay it with one graph launch.
+#include <cstring>
 #include <vector>
 
 #include "srt_internal.cuh"
 
+using namespace srt;
+
 struct srt_batch {
   srt_ctx *ctx = nullptr;
-  std::vector<srt_accel *> accels;
+  BatchTree bt;
+  std::vector<uint64_t> fo, ro;
+  const float *verts = nullptr;
+  const uint32_t *faces = nullptr;
+  const srt_ray *rays = nullptr;
+  srt_hit *hits = nullptr;
+  int block = 128, R = 1;
+  bool tuned = false;
+  int same_calls = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  uint64_t kernels_per_call = 0;
+  uint64_t epoch = 0;  // g_buffer_epoch when the graph was captured
+
+  void drop_graph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    exec = nullptr;
+    graph = nullptr;
+  }
 };
 
-using namespace srt;
+namespace {
+
+// Upload the per-scene offsets as uint32 (global primitive, internal node
+// and ray offsets).
+srt_status upload_offsets(srt_batch *b) {
+  const int ns = (int)b->fo.size() - 1;
+  std::vector<uint32_t> f(ns + 1), in(ns + 1), r(ns + 1);
+  for (int s = 0; s <= ns; s++) {
+    f[s] = (uint32_t)b->fo[s];
+    in[s] = (uint32_t)(b->fo[s] - (uint64_t)s);
+    r[s] = (uint32_t)b->ro[s];
+  }
+  cudaError_t e;
+  if ((e = b->bt.foff.ensure((ns + 1) * 4)) != cudaSuccess ||
+      (e = b->bt.ioff.ensure((ns + 1) * 4)) != cudaSuccess ||
+      (e = b->bt.roff.ensure((ns + 1) * 4)) != cudaSuccess)
+    return cuda_status(e, "batch offsets");
+  cudaStream_t st = b->ctx->stream;
+  e = cudaMemcpyAsync(b->bt.foff.p, f.data(), (ns + 1) * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->bt.ioff.p, in.data(), (ns + 1) * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(b->bt.roff.p, r.data(), (ns + 1) * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_status(e, "batch offsets");
+  b->bt.nseg = ns;
+  b->bt.nprims = b->fo[ns];
+  b->bt.nrays = b->ro[ns];
+  return SRT_OK;
+}
+
+srt_status build_and_trace(srt_batch *b, const uint32_t *h_foff) {
+  srt_status s = build_batch(b->ctx, b->bt, b->verts, b->faces, h_foff, b->bt.nseg);
+  if (s != SRT_OK) return s;
+  return launch_trace_batch(b->ctx, b->bt, b->rays, b->hits, b->block, b->R, nullptr);
+}
+
+// Time the traversal for a few launch shapes and keep the fastest.
+srt_status autotune(srt_batch *b) {
+  static const int blocks[] = {64, 128, 256};
+  static const int Rs[] = {1, 2, 4};
+  cudaStream_t st = b->ctx->stream;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int bb = 128, br = 1;
+  for (int blk : blocks)
+    for (int r : Rs) {
+      float tot = 0.0f;
+      for (int rep = 0; rep < 2; rep++) {
+        cudaEventRecord(e0, st);
+        srt_status s = launch_trace_batch(b->ctx, b->bt, b->rays, b->hits, blk, r, nullptr);
+        cudaEventRecord(e1, st);
+        if (s != SRT_OK) {
+          cudaEventDestroy(e0);
+          cudaEventDestroy(e1);
+          return s;
+        }
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) return cuda_status(e, "autotune");
+        float ms = 0.0f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0) tot += ms;  // first repetition warms caches
+      }
+      if (tot < best) {
+        best = tot;
+        bb = blk;
+        br = r;
+      }
+    }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  b->block = bb;
+  b->R = br;
+  b->tuned = true;
+  return SRT_OK;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -26,42 +130,128 @@ SRT_API srt_status srt_batch_create(srt_ctx *ctx, srt_batch **out) {
 
 SRT_API srt_status srt_batch_destroy(srt_batch *b) {
   if (!b) return SRT_OK;
-  for (srt_accel *a : b->accels) srt_accel_destroy(a);
+  cudaSetDevice(b->ctx->device);
+  cudaStreamSynchronize(b->ctx->stream);
+  b->drop_graph();
   delete b;
   return SRT_OK;
 }
 
-SRT_API srt_status srt_batch_build_trace(srt_batch *b, int32_t nscenes,
-                                         const float *vertices, const uint32_t *faces,
-                                         const uint64_t *face_offsets,
+SRT_API srt_status srt_batch_config(srt_batch *b, int32_t *block, int32_t *rays_per_thread,
+                                    int32_t *graph_captured, uint64_t *kernels_per_call) {
+  if (!b) return SRT_ERR_INVALID;
+  if (block) *block = b->block;
+  if (rays_per_thread) *rays_per_thread = b->R;
+  if (graph_captured) *graph_captured = b->exec ? 1 : 0;
+  if (kernels_per_call) *kernels_per_call = b->kernels_per_call;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_batch_build_trace(srt_batch *b, int32_t nscenes, const float *vertices,
+                                         const uint32_t *faces, const uint64_t *face_offsets,
                                          const srt_ray *rays, const uint64_t *ray_offsets,
                                          srt_hit *hits) {
-  if (!b || nscenes <= 0 || !vertices || !faces || !face_offsets || !rays ||
-      !ray_offsets || !hits)
+  if (!b || nscenes <= 0 || nscenes > 256 || !vertices || !faces || !face_offsets || !rays ||
+      !ray_offsets || !hits) {
+    set_error("invalid batch arguments");
     return SRT_ERR_INVALID;
+  }
   srt_ctx *ctx = b->ctx;
   cudaSetDevice(ctx->device);
-  std::vector<uint64_t> fo(nscenes + 1), ro(nscenes + 1);
-  cudaMemcpyAsync(fo.data(), face_offsets, fo.size() * 8, cudaMemcpyDefault, ctx->stream);
-  cudaMemcpyAsync(ro.data(), ray_offsets, ro.size() * 8, cudaMemcpyDefault, ctx->stream);
-  cudaError_t e = cudaStreamSynchronize(ctx->stream);
-  if (e != cudaSuccess) return cuda_status(e, "batch offsets");
-  while ((int)b->accels.size() < nscenes) {
-    srt_accel *a = nullptr;
-    srt_status s = srt_accel_create(ctx, SRT_TRIANGLES, &a);
-    if (s != SRT_OK) return s;
-    b->accels.push_back(a);
+  if (face_offsets[0] != 0 || ray_offsets[0] != 0) {
+    set_error("offsets must start at 0");
+    return SRT_ERR_INVALID;
   }
-  for (int i = 0; i < nscenes; i++) {
-    srt_accel *a = b->accels[i];
-    // the vertex array is shared; each scene indexes into it
-    srt_status s = srt_accel_build_triangles(a, vertices, 1, faces + 3 * fo[i],
-                                             (size_t)(fo[i + 1] - fo[i]));
-    if (s != SRT_OK) return s;
-    s = srt_trace_closest(a, rays + ro[i], (size_t)(ro[i + 1] - ro[i]), hits + ro[i], nullptr);
-    if (s != SRT_OK) return s;
+  for (int s = 0; s < nscenes; s++) {
+    if (face_offsets[s + 1] < face_offsets[s] + 2 || ray_offsets[s + 1] < ray_offsets[s]) {
+      set_error("every scene needs at least 2 faces; offsets must not decrease");
+      return SRT_ERR_INVALID;
+    }
   }
-  return SRT_OK;
+  if (face_offsets[nscenes] >= (1ull << 30) || ray_offsets[nscenes] >= (1ull << 31)) {
+    set_error("batch too large");
+    return SRT_ERR_INVALID;
+  }
+  if (!is_device_ptr(vertices) || !is_device_ptr(faces) || !is_device_ptr(rays) ||
+      !is_device_ptr(hits)) {
+    set_error("batch arrays must be device memory");
+    return SRT_ERR_INVALID;
+  }
+  if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15u) {
+    set_error("ray and hit arrays must be 16-byte aligned");
+    return SRT_ERR_INVALID;
+  }
+  std::vector<uint64_t> fo(face_offsets, face_offsets + nscenes + 1);
+  std::vector<uint64_t> ro(ray_offsets, ray_offsets + nscenes + 1);
+  const bool same = fo == b->fo && ro == b->ro && vertices == b->verts && faces == b->faces &&
+                    rays == b->rays && hits == b->hits;
+  std::vector<uint32_t> h_foff(nscenes + 1);
+  for (int s = 0; s <= nscenes; s++) h_foff[s] = (uint32_t)fo[s];
+  srt_status s;
+  if (!same) {
+    const bool reshaped = fo != b->fo || ro != b->ro;
+    b->drop_graph();
+    b->fo = fo;
+    b->ro = ro;
+    b->verts = vertices;
+    b->faces = faces;
+    b->rays = rays;
+    b->hits = hits;
+    b->same_calls = 0;
+    if (reshaped) {  // new scene sizes: new offsets, tune again
+      b->tuned = false;
+      if ((s = upload_offsets(b)) != SRT_OK) return s;
+    }
+  }
+  // graph replay, unless a scratch buffer it points into has been freed since
+  if (b->exec && b->epoch != g_buffer_epoch.load(std::memory_order_relaxed)) {
+    b->drop_graph();
+    b->same_calls = 1;
+  }
+  if (b->exec) {
+    cudaError_t e = cudaGraphLaunch(b->exec, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e, "batch graph launch");
+    ctx->launches += b->kernels_per_call;
+    return SRT_OK;
+  }
+  // eager run (allocates, autotunes on the first call)
+  const uint64_t l0 = ctx->launches;
+  if ((s = build_batch(ctx, b->bt, vertices, faces, h_foff.data(), nscenes)) != SRT_OK) return s;
+  const uint64_t lb = ctx->launches;
+  if (!b->tuned && (s = autotune(b)) != SRT_OK) return s;
+  const uint64_t lt = ctx->launches;
+  if ((s = launch_trace_batch(ctx, b->bt, rays, hits, b->block, b->R, nullptr)) != SRT_OK)
+    return s;
+  b->kernels_per_call = (lb - l0) + (ctx->launches - lt);
+  b->same_calls++;
+  // capture on the second identical call (the legacy and per-thread default
+  // streams cannot be captured; those stay eager)
+  if (b->same_calls >= 2 && ctx->stream != nullptr && ctx->stream != cudaStreamLegacy &&
+      ctx->stream != cudaStreamPerThread) {
+    cudaError_t e = cudaStreamSynchronize(ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e, "batch sync");
+    const uint64_t c0 = ctx->launches;
+    e = cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal);
+    if (e != cudaSuccess) return cuda_status(e, "batch capture");
+    srt_status cs = build_and_trace(b, h_foff.data());
+    cudaGraph_t g = nullptr;
+    e = cudaStreamEndCapture(ctx->stream, &g);
+    if (cs != SRT_OK || e != cudaSuccess || !g) {
+      if (g) cudaGraphDestroy(g);
+      cudaGetLastError();
+      ctx->launches = c0;
+      return SRT_OK;  // stay eager; results of this call are complete
+    }
+    b->kernels_per_call = ctx->launches - c0;
+    ctx->launches = c0;
+    b->graph = g;
+    b->epoch = g_buffer_epoch.load(std::memory_order_relaxed);
+    if (cudaGraphInstantiate(&b->exec, g, 0) != cudaSuccess) {
+      cudaGetLastError();
+      b->drop_graph();
+    }
+  }
+  return cuda_status(cudaGetLastError(), "batch");
 }
 
 }  // extern "C"

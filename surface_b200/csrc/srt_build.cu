@@ -351,16 +351,6 @@ constexpr int kRsRounds = 16;
 constexpr int kRsWChunk = 32 * kRsRounds;
 constexpr int kRsTile = kRsWarps * kRsWChunk;
 
-// Segment (scene) of global index x: the largest s with off[s] <= x.
-__device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int nseg, uint32_t x) {
-  int lo = 0, hi = nseg - 1;
-  while (lo < hi) {
-    const int mid = (lo + hi + 1) >> 1;
-    if (__ldg(&off[mid]) <= x) lo = mid; else hi = mid - 1;
-  }
-  return lo;
-}
-
 // Sort digit: a byte of the key, or (SEGDIG) the segment of the value --
 // the extra pass that groups a multi-scene sort by scene.
 template <bool SEGDIG>

@@ -19,6 +19,8 @@ srt_status cuda_status(cudaError_t e, const char *what) {
   return e == cudaErrorMemoryAllocation ? SRT_ERR_NO_MEMORY : SRT_ERR_CUDA;
 }
 
+std::atomic<uint64_t> g_buffer_epoch{0};
+
 cudaError_t DevBuf::ensure(size_t bytes) {
   if (bytes <= cap && p) return cudaSuccess;
   release();
@@ -35,7 +37,10 @@ cudaError_t DevBuf::ensure(size_t bytes) {
 }
 
 void DevBuf::release() {
-  if (p) cudaFree(p);
+  if (p) {
+    cudaFree(p);
+    g_buffer_epoch.fetch_add(1, std::memory_order_relaxed);
+  }
   p = nullptr;
   cap = 0;
 }

@@ -10,6 +10,7 @@
 #include <float.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <string>
 
 #include "surface_rt.h"
@@ -87,11 +88,25 @@ __device__ __forceinline__ uint32_t spread10(uint32_t v) {
   return v;
 }
 
+// Segment (scene) of global index x: the largest s with off[s] <= x.
+__device__ __forceinline__ int seg_of(const uint32_t *__restrict__ off, int nseg, uint32_t x) {
+  int lo = 0, hi = nseg - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (__ldg(&off[mid]) <= x) lo = mid; else hi = mid - 1;
+  }
+  return lo;
+}
+
 __device__ __forceinline__ int split_axis(uint32_t code) {
   return (__clz(code) - 2) % 3;  // __clz(0) = 32
 }
 
 // ---------------------------------------------------------------- host side
+// Bumped whenever any DevBuf frees memory; a captured CUDA graph that holds
+// scratch pointers is valid only while the epoch it was captured at holds.
+extern std::atomic<uint64_t> g_buffer_epoch;
+
 struct DevBuf {
   void *p = nullptr;
   size_t cap = 0;

@@ -423,11 +423,11 @@ __device__ __forceinline__ bool cand2(const float4 *__restrict__ prims,
 template <int KIND>
 __device__ void ref_walk2(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
                           const uint32_t *__restrict__ sidx, const Ctx2 &c, Best &b,
-                          Work &w, uint32_t max_iter) {
+                          Work &w, uint32_t max_iter, uint32_t root = 0) {
   b = Best();
   uint2 stk[kStack];
   int sp = 0;
-  stk[0] = make_uint2(0u, 0u);
+  stk[0] = make_uint2(root, 0u);
   while (true) {
     uint2 leaf = make_uint2(0u, 0u);
     while (sp >= 0) {
@@ -470,12 +470,13 @@ template <int KIND>
 __device__ void window_walk2(const Node2 *__restrict__ nodes,
                              const float4 *__restrict__ prims,
                              const uint32_t *__restrict__ sidx, const Ctx2 &c, float bnd,
-                             float t0, Best &b, Work &w, uint32_t max_iter) {
+                             float t0, Best &b, Work &w, uint32_t max_iter,
+                             uint32_t root = 0) {
   b = Best();
   float t = t0;
   uint2 stk[kStack];
   int sp = 0;
-  stk[0] = make_uint2(0u, 0u);
+  stk[0] = make_uint2(root, 0u);
   while (true) {
     uint2 leaf = make_uint2(0u, 0u);
     while (sp >= 0) {
@@ -590,6 +591,78 @@ __device__ __forceinline__ Ctx2 make_ctx2(const srt_ray *__restrict__ rays, size
   return c;
 }
 
+// Pass 1 of the default walk for the two-child kinds: front to back from
+// `root`; returns m (smallest hit distance), how many primitives hit at m,
+// the one found first (in b), and whether any primitive was reported before
+// its own leaf box's entry.
+template <int KIND>
+__device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
+                                            const float4 *__restrict__ prims,
+                                            const uint32_t *__restrict__ sidx,
+                                            const Ctx2 &c, uint32_t root, Best &b, Work &w,
+                                            uint32_t max_iter, float &m_out,
+                                            uint32_t &at_m_out, bool &viol_out) {
+  float m = FLT_MAX;
+  uint32_t at_m = 0;
+  bool viol = false;
+  uint2 stk[kStack];
+  float stt[kStack];
+  int sp = 0;
+  stk[0] = make_uint2(root, 0u);
+  stt[0] = -FLT_MAX;
+  while (true) {
+    uint2 leaf = make_uint2(0u, 0u);
+    float lt = 0.0f;
+    while (sp >= 0) {
+      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+      const uint2 e = stk[sp];
+      const float et = stt[sp];
+      sp--;
+      const float bnd = bound_rel(m, kRelTri);
+      if (et > bnd) continue;
+      if (e.y != 0) { leaf = e; lt = et; break; }
+      w.branch++;
+      const float4 *np = reinterpret_cast<const float4 *>(nodes + e.x);
+      const float4 a = __ldg(np), bb = __ldg(np + 1), cc = __ldg(np + 2);
+      const uint4 d = __ldg(reinterpret_cast<const uint4 *>(np + 3));
+      float t0, t1;
+      const bool h0 = ray_aabb_t<true>(bnd, a.x, a.y, a.z, a.w, bb.x, bb.y, c.r, t0);
+      const bool h1 = ray_aabb_t<true>(bnd, bb.z, bb.w, cc.x, cc.y, cc.z, cc.w, c.r, t1);
+      const uint2 e0 = make_uint2(d.x, d.z & kCountMask),
+                  e1 = make_uint2(d.y, d.w & kCountMask);
+      if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+      if (h0 && h1) {
+        const bool first1 = t1 < t0;
+        stk[++sp] = first1 ? e0 : e1; stt[sp] = first1 ? t0 : t1;
+        stk[++sp] = first1 ? e1 : e0; stt[sp] = first1 ? t1 : t0;
+      } else if (h0) {
+        stk[++sp] = e0; stt[sp] = t0;
+      } else if (h1) {
+        stk[++sp] = e1; stt[sp] = t1;
+      }
+    }
+    if (leaf.y == 0) break;
+    w.leaf++;
+    w.prim += leaf.y;
+    for (uint32_t j = leaf.x; j < leaf.x + leaf.y; j++) {
+      float t, u, v;
+      uint32_t f;
+      if (!cand2<KIND>(prims, sidx, j, c, FLT_MAX, t, u, v, f)) continue;
+      if (below_entry(t, lt)) viol = true;
+      if (t < m) {
+        m = t;
+        at_m = 1;
+        b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
+      } else if (t == m) {
+        at_m++;
+      }
+    }
+  }
+  m_out = m;
+  at_m_out = at_m;
+  viol_out = viol;
+}
+
 // Two-child kinds (triangles, spheres).  SINGLE: the reference's walk for
 // every ray.
 template <int KIND, bool SINGLE>
@@ -610,62 +683,10 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
   if (SINGLE) {
     ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
   } else {
-    float m = FLT_MAX;
-    uint32_t at_m = 0;
-    bool viol = false;
-    uint2 stk[kStack];
-    float stt[kStack];
-    int sp = 0;
-    stk[0] = make_uint2(0u, 0u);
-    stt[0] = -FLT_MAX;
-    while (true) {
-      uint2 leaf = make_uint2(0u, 0u);
-      float lt = 0.0f;
-      while (sp >= 0) {
-        if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
-        const uint2 e = stk[sp];
-        const float et = stt[sp];
-        sp--;
-        const float bnd = bound_rel(m, kRelTri);
-        if (et > bnd) continue;
-        if (e.y != 0) { leaf = e; lt = et; break; }
-        w.branch++;
-        const float4 *np = reinterpret_cast<const float4 *>(nodes + e.x);
-        const float4 a = __ldg(np), bb = __ldg(np + 1), cc = __ldg(np + 2);
-        const uint4 d = __ldg(reinterpret_cast<const uint4 *>(np + 3));
-        float t0, t1;
-        const bool h0 = ray_aabb_t<true>(bnd, a.x, a.y, a.z, a.w, bb.x, bb.y, c.r, t0);
-        const bool h1 = ray_aabb_t<true>(bnd, bb.z, bb.w, cc.x, cc.y, cc.z, cc.w, c.r, t1);
-        const uint2 e0 = make_uint2(d.x, d.z & kCountMask),
-                    e1 = make_uint2(d.y, d.w & kCountMask);
-        if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
-        if (h0 && h1) {
-          const bool first1 = t1 < t0;
-          stk[++sp] = first1 ? e0 : e1; stt[sp] = first1 ? t0 : t1;
-          stk[++sp] = first1 ? e1 : e0; stt[sp] = first1 ? t1 : t0;
-        } else if (h0) {
-          stk[++sp] = e0; stt[sp] = t0;
-        } else if (h1) {
-          stk[++sp] = e1; stt[sp] = t1;
-        }
-      }
-      if (leaf.y == 0) break;
-      w.leaf++;
-      w.prim += leaf.y;
-      for (uint32_t j = leaf.x; j < leaf.x + leaf.y; j++) {
-        float t, u, v;
-        uint32_t f;
-        if (!cand2<KIND>(prims, sidx, j, c, FLT_MAX, t, u, v, f)) continue;
-        if (below_entry(t, lt)) viol = true;
-        if (t < m) {
-          m = t;
-          at_m = 1;
-          b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
-        } else if (t == m) {
-          at_m++;
-        }
-      }
-    }
+    float m;
+    uint32_t at_m;
+    bool viol;
+    pass1_node2<KIND>(nodes, prims, sidx, c, 0u, b, w, max_iter, m, at_m, viol);
     if (!w.fail && (viol || at_m > 1)) {
       const uint32_t k = atomicAdd(dcount, 1u);
       dlist[k] = Deferred{(uint32_t)i, viol ? 1u : 0u, (double)m};
@@ -961,6 +982,86 @@ resolve_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ p
   }
 }
 
+// --------------------------------------------------------------- batches
+// All rays of many triangle scenes in one persistent launch: each block
+// takes the next blockDim.x * R rays from a global counter (scenes of very
+// different cost balance across the GPU), finds the ray's scene from the
+// ray offsets and walks that scene's tree from its root.
+__global__ void __launch_bounds__(256)
+trace_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
+                   const srt_ray *__restrict__ rays, srt_hit *__restrict__ hits,
+                   const SceneInfo *__restrict__ scenes, const uint32_t *__restrict__ roots,
+                   const uint32_t *__restrict__ roff, int nseg, uint32_t total,
+                   uint32_t *__restrict__ work, int R, unsigned long long *__restrict__ stats,
+                   Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
+                   uint32_t max_iter, uint32_t *__restrict__ err) {
+  __shared__ uint32_t s_base;
+  while (true) {
+    if (threadIdx.x == 0) s_base = atomicAdd(work, blockDim.x * (uint32_t)R);
+    __syncthreads();
+    const uint32_t base = s_base;
+    __syncthreads();
+    if (base >= total) break;
+    for (int r = 0; r < R; r++) {
+      const uint32_t i = base + (uint32_t)r * blockDim.x + threadIdx.x;
+      if (i >= total) break;
+      const int sg = seg_of(roff, nseg, i);
+      Ctx2 c;
+      c.r = load_ray(rays, i, c.prev_prim, c.prev_t);
+      c.keps = scenes[sg].keps;
+      c.pn[0] = c.pn[1] = c.pn[2] = 0.0f;
+      Work w;
+      Best b;
+      float m;
+      uint32_t at_m;
+      bool viol;
+      pass1_node2<SRT_TRIANGLES>(nodes, prims, nullptr, c, __ldg(&roots[sg]), b, w, max_iter,
+                                 m, at_m, viol);
+      if (!w.fail && (viol || at_m > 1)) {
+        const uint32_t k = atomicAdd(dcount, 1u);
+        dlist[k] = Deferred{i, viol ? 1u : 0u, (double)m};
+      } else {
+        if (w.fail) atomicOr(err, kErrIter);
+        store_node2<SRT_TRIANGLES>(i, b, c, prims, hits, nullptr);
+      }
+      add_stats(stats, w, 0);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128)
+resolve_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
+                     const srt_ray *__restrict__ rays, srt_hit *__restrict__ hits,
+                     const SceneInfo *__restrict__ scenes, const uint32_t *__restrict__ roots,
+                     const uint32_t *__restrict__ roff, int nseg,
+                     unsigned long long *__restrict__ stats,
+                     const Deferred *__restrict__ dlist, const uint32_t *__restrict__ dcount,
+                     uint32_t max_iter, uint32_t *__restrict__ err) {
+  const uint32_t cnt = *dcount;
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+       k += gridDim.x * blockDim.x) {
+    const Deferred dfr = dlist[k];
+    const int sg = seg_of(roff, nseg, dfr.ray);
+    Ctx2 c;
+    c.r = load_ray(rays, dfr.ray, c.prev_prim, c.prev_t);
+    c.keps = scenes[sg].keps;
+    c.pn[0] = c.pn[1] = c.pn[2] = 0.0f;
+    const uint32_t root = __ldg(&roots[sg]);
+    Work w;
+    Best b;
+    if (dfr.full) {
+      ref_walk2<SRT_TRIANGLES>(nodes, prims, nullptr, c, b, w, max_iter, root);
+    } else {
+      const float m = (float)dfr.m;
+      window_walk2<SRT_TRIANGLES>(nodes, prims, nullptr, c, bound_rel(m, kRelTri), m, b, w,
+                                  max_iter, root);
+    }
+    if (w.fail) atomicOr(err, kErrIter);
+    add_stats(stats, w, dfr.full);
+    store_node2<SRT_TRIANGLES>(dfr.ray, b, c, prims, hits, nullptr);
+  }
+}
+
 }  // namespace
 
 srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hits,
@@ -1054,6 +1155,34 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
   }
   ctx->launches++;
   return cuda_status(cudaGetLastError(), "trace");
+}
+
+srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
+                              srt_hit *hits, int block, int R,
+                              unsigned long long *stats) {
+  const uint32_t total = (uint32_t)bt.nrays;
+  if (total == 0) return SRT_OK;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = ctx->s_defer.ensure((size_t)total * sizeof(Deferred) + 256);
+  if (e != cudaSuccess) return cuda_status(e, "deferred list");
+  uint32_t *dcount = ctx->s_defer.as<uint32_t>();  // [0] deferred count, [1] work counter
+  Deferred *dlist = reinterpret_cast<Deferred *>(ctx->s_defer.as<char>() + 256);
+  if ((e = cudaMemsetAsync(dcount, 0, 8, st)) != cudaSuccess)
+    return cuda_status(e, "batch counters");
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_batch_kernel, block, 0);
+  if (per_sm < 1) per_sm = 1;
+  const uint32_t max_iter = (uint32_t)std::min<size_t>(8 * bt.nprims + 64, 0xfffffff0u);
+  trace_batch_kernel<<<ctx->num_sms * per_sm, block, 0, st>>>(
+      bt.nodes.as<Node2>(), bt.prims.as<float4>(), rays, hits, bt.scenes.as<SceneInfo>(),
+      bt.roots.as<uint32_t>(), bt.roff.as<uint32_t>(), bt.nseg, total, dcount + 1, R, stats,
+      dlist, dcount, max_iter, ctx->d_err);
+  resolve_batch_kernel<<<ctx->num_sms * 8, 128, 0, st>>>(
+      bt.nodes.as<Node2>(), bt.prims.as<float4>(), rays, hits, bt.scenes.as<SceneInfo>(),
+      bt.roots.as<uint32_t>(), bt.roff.as<uint32_t>(), bt.nseg, stats, dlist, dcount,
+      max_iter, ctx->d_err);
+  ctx->launches += 2;
+  return cuda_status(cudaGetLastError(), "batch trace");
 }
 
 }  // namespace srt

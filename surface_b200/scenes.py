@@ -241,3 +241,55 @@ def transfer_function(entries=256, seed=123456):
     rgb = 0.5 + 0.5 * np.sin(2 * np.pi * x[:, None] * np.array([1.0, 1.3, 1.7]) + ph)
     a = np.clip((x - 0.05) * 1.2, 0.0, 1.0) ** 1.5
     return np.concatenate([rgb, a[:, None]], 1).astype(np.float32)
+
+
+# ---------------------------------------------------------------- batched
+_OCTA_CACHE: dict = {}
+
+
+def _octa(levels):
+    if levels not in _OCTA_CACHE:
+        _OCTA_CACHE[levels] = octasphere(levels)
+    return _OCTA_CACHE[levels]
+
+
+def batched_scenes(nscenes=64, seed=2024, lo=1e3, hi=1e6, sizes=(128, 256, 512, 1024),
+                   min_faces=1024):
+    """Uneven triangle scenes for the batched build+trace.
+
+    Scene s: a displaced octasphere truncated to n_s faces, n_s log-uniform in
+    [lo, hi] (at least ``min_faces``, the size from which Build32 applies),
+    seen by a square pinhole image of a side drawn uniformly from ``sizes``
+    (camera at distance 3 on +z, 45 degree field of view).  Returns a dict with
+    the concatenated ``vertices``, ``faces`` (vertex ids into the concatenated
+    vertices), ``rays``, the nscenes+1 ``face_offsets`` / ``ray_offsets``, and
+    per-scene ``counts`` and ``sides``."""
+    rng = np.random.default_rng(seed)
+    counts = np.exp(rng.uniform(np.log(lo), np.log(hi), nscenes)).astype(np.int64)
+    counts = np.maximum(counts, min_faces)
+    sides = rng.choice(np.asarray(sizes), nscenes)
+    verts, faces, rays = [], [], []
+    fo, ro = [0], [0]
+    vbase = 0
+    for s in range(nscenes):
+        n = int(counts[s])
+        levels = 0
+        while 8 * 4 ** levels < n:
+            levels += 1
+        v, f = _octa(levels)
+        srng = np.random.default_rng([seed, s])
+        r = 1.0 + 0.1 * _value_noise(v, srng)
+        vs = (v * r[:, None]).astype(np.float32)
+        fs = f[:n]
+        verts.append(vs)
+        faces.append(fs.astype(np.uint64) + vbase)
+        vbase += vs.shape[0]
+        fo.append(fo[-1] + n)
+        side = int(sides[s])
+        rays.append(pinhole_rays(side, side, (0, 0, 3), (0, 0, 0)))
+        ro.append(ro[-1] + side * side)
+    faces = np.concatenate(faces)
+    assert faces.max() < 2 ** 32
+    return dict(vertices=np.concatenate(verts), faces=faces.astype(np.uint32),
+                rays=np.concatenate(rays), face_offsets=np.asarray(fo, np.uint64),
+                ray_offsets=np.asarray(ro, np.uint64), counts=counts, sides=sides)
