@@ -189,10 +189,15 @@ SRT_API srt_status srt_accel_bbox(srt_accel *accel, double bmin[3],
 SRT_API srt_status srt_accel_info_get(srt_accel *accel, srt_accel_info *info);
 
 /* Copy the device tree to host memory (synchronises).  Any pointer may be
- * NULL.  nodes: info.num_nodes records of info.node_bytes (layout in
- * DESIGN.md of this repository: two-child 64-byte nodes for triangles and
- * spheres, own-box 32-byte nodes for tetrahedra); indices: sorted primitive
- * ids (TriangleAccel::indices_); codes: sorted Morton codes. */
+ * NULL.  nodes: info.num_nodes records of info.node_bytes -- triangles and
+ * spheres: 64-byte two-child nodes {float lo0[3], hi0[3], lo1[3], hi1[3];
+ * uint32 ref0, ref1, count0 | axis << 30, count1} where count 0 marks a
+ * branch child (ref = node index) and count > 0 a leaf (ref = first sorted
+ * primitive); tetrahedra: 32-byte own-box nodes {float lo[3]; uint32 meta;
+ * float hi[3]; uint32 ref} with meta = 0x80000000 | count for a leaf (ref =
+ * first sorted primitive) or the split axis for a branch (children at ref,
+ * ref+1).  indices: sorted primitive ids
+ * (TriangleAccel::indices_); codes: sorted Morton codes. */
 SRT_API srt_status srt_accel_export(srt_accel *accel, void *nodes,
                                     uint32_t *indices, uint32_t *codes);
 /* Write the reference's Dump() file (u64 node count, reference node records,
