@@ -211,6 +211,29 @@ SRT_API srt_status srt_trace_closest(srt_accel *accel, const srt_ray *rays,
                                      size_t n, srt_hit *hits,
                                      const srt_trace_opts *opts);
 
+/* Closest hit for n rays without allocating memory (no counterpart in the
+ * reference, whose Traverse works one ray at a time on the stack).  Same
+ * hits as srt_trace_closest with opts == NULL, for callers that must not
+ * allocate once running: cudaFree synchronises the whole device, and a
+ * cudaMalloc can fail mid-frame in a process that fixed its device-memory
+ * budget at start-up.  srt_trace_closest grows the context's deferred-ray
+ * scratch on demand; this call keeps that list in a fixed 4 MiB device array
+ * compiled into the library instead.
+ *   - n <= 262144 rays per call (SRT_ERR_LIMIT above that; split the array).
+ *   - rays and hits: device memory, 16-byte aligned.  Asynchronous on the
+ *     context's stream; errors of the kernels surface at srt_ctx_synchronize.
+ *   - The first call on each device does a one-time set-up (it looks up the
+ *     array's device address, which may load the library's device code on
+ *     that device); make it once at start-up, before any stream capture.
+ *   - The array is shared by all contexts on a device: calls whose kernels
+ *     overlap in time (different streams, unordered threads) race on it.
+ *     Order them on one stream or synchronise between them.
+ *   - Nothing needs to be zeroed by the caller: each call clears the array's
+ *     deferred-ray count on the stream before its first kernel. */
+SRT_API srt_status srt_trace_closest_noalloc(srt_accel *accel,
+                                             const srt_ray *rays, size_t n,
+                                             srt_hit *hits);
+
 /* ---- build stages (bit-exact against the reference's own stages) ------ */
 /* Scene box and 30-bit Morton code per primitive, in input order. */
 SRT_API srt_status srt_stage_morton(srt_ctx *ctx, srt_kind kind,

@@ -74,6 +74,7 @@ _SIGS = {
     "srt_accel_export": [_P, _P, _P, _P],
     "srt_accel_dump": [_P, C.c_char_p],
     "srt_trace_closest": [_P, _P, _SZ, _P, C.POINTER(TraceOpts)],
+    "srt_trace_closest_noalloc": [_P, _P, _SZ, _P],
     "srt_stage_morton": [_P, C.c_int, _P, _SZ, _P, _P, C.c_float, _SZ, _P, _P],
     "srt_stage_sort_pairs": [_P, _P, _P, _SZ],
     "srt_stage_karras": [_P, _P, _SZ, _P, _P, _P],

@@ -28,6 +28,8 @@
 // Leaves are folded into their parent's child slot for triangles/spheres;
 // a hit leaf is pushed as a (first primitive, count) entry, which visits
 // leaves in exactly the reference's order.
+#include <mutex>
+
 #include "srt_internal.cuh"
 
 namespace srt {
@@ -1186,3 +1188,133 @@ srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
 }
 
 }  // namespace srt
+
+// ======================================================= no-allocation trace
+// srt_trace_closest_noalloc runs the same two kernels as srt_trace_closest
+// (first pass + deferred-ray resolve) but keeps its deferred-ray list in the
+// fixed device array below instead of the context's growable scratch, so a
+// call allocates no device or host memory.
+//
+// Layout of g_noalloc_scratch: bytes [0, 256) are the header, whose first
+// uint32 is the deferred-ray count.  That count must be zero when the first
+// kernel starts; every call clears it itself (cudaMemsetAsync on the
+// context's stream) before its first launch.  Records of 16 bytes follow at
+// byte 256, one per deferred ray, at most kNoAllocMaxRays of them (4 MiB).
+// The rest of the array needs no initial value.
+//
+// The array is one per device and shared by every context and stream on that
+// device: two calls whose kernels overlap in time (different streams, or
+// different host threads without ordering) race on it and may return wrong
+// hits.  Order such calls on one stream or synchronise between them.
+namespace srt {
+namespace {
+
+constexpr size_t kNoAllocMaxRays = 262144;
+constexpr size_t kNoAllocHeader = 256;
+constexpr int kNoAllocMaxDevices = 64;
+
+__device__ __align__(256) unsigned char
+    g_noalloc_scratch[kNoAllocHeader + kNoAllocMaxRays * sizeof(Deferred)];
+
+std::mutex g_noalloc_mu;
+void *g_noalloc_base[kNoAllocMaxDevices];
+
+// Device address of g_noalloc_scratch on the current device, looked up once
+// per device (the lookup is the set-up: it may load this module's device
+// code on that device).
+srt_status noalloc_scratch(int device, unsigned char **out) {
+  if (device < 0 || device >= kNoAllocMaxDevices) {
+    set_error("device ordinal out of range for the no-allocation scratch");
+    return SRT_ERR_INVALID;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_base[device]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) return cuda_status(e, "no-allocation scratch set-up");
+    g_noalloc_base[device] = p;
+  }
+  *out = static_cast<unsigned char *>(g_noalloc_base[device]);
+  return SRT_OK;
+}
+
+}  // namespace
+}  // namespace srt
+
+extern "C" SRT_API srt_status srt_trace_closest_noalloc(srt_accel *a, const srt_ray *rays,
+                                                        size_t n, srt_hit *hits) {
+  using namespace srt;
+  if (!a || (!rays && n) || (!hits && n)) {
+    set_error("NULL argument");
+    return SRT_ERR_INVALID;
+  }
+  if (!a->built) {
+    set_error("accel not built");
+    return SRT_ERR_INVALID;
+  }
+  if (n > kNoAllocMaxRays) {
+    set_error("srt_trace_closest_noalloc: at most 262144 rays per call; split the ray array");
+    return SRT_ERR_LIMIT;
+  }
+  if (n == 0) return SRT_OK;
+  srt_ctx *ctx = a->ctx;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  if (e != cudaSuccess) return cuda_status(e, "set device");
+  if (!is_device_ptr(rays) || !is_device_ptr(hits)) {
+    set_error("srt_trace_closest_noalloc: rays and hits must be device memory");
+    return SRT_ERR_INVALID;
+  }
+  if ((reinterpret_cast<uintptr_t>(rays) | reinterpret_cast<uintptr_t>(hits)) & 15u) {
+    set_error("ray and hit arrays must be 16-byte aligned");
+    return SRT_ERR_INVALID;
+  }
+  unsigned char *base = nullptr;
+  srt_status s = noalloc_scratch(ctx->device, &base);
+  if (s != SRT_OK) return s;
+  uint32_t *dcount = reinterpret_cast<uint32_t *>(base);
+  Deferred *dlist = reinterpret_cast<Deferred *>(base + kNoAllocHeader);
+  cudaStream_t st = ctx->stream;
+  if ((e = cudaMemsetAsync(dcount, 0, 4, st)) != cudaSuccess)
+    return cuda_status(e, "deferred count");
+  const int block = 128;
+  const unsigned grid = (unsigned)((n + block - 1) / block);
+  const unsigned rgrid = (unsigned)ctx->num_sms * 8;
+  const uint32_t max_iter = (uint32_t)std::min<size_t>(8 * a->n + 64, 0xfffffff0u);
+  const SceneInfo *scene = a->scene.as<SceneInfo>();
+  const float4 *pr = a->prims.as<float4>();
+  const uint32_t *ix = a->indices.as<uint32_t>();
+  switch (a->kind) {
+    case SRT_TRIANGLES: {
+      const Node2 *nd = a->nodes.as<Node2>();
+      trace_node2_kernel<SRT_TRIANGLES, false><<<grid, block, 0, st>>>(
+          nd, pr, ix, rays, n, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
+          ctx->d_err);
+      resolve_node2_kernel<SRT_TRIANGLES><<<rgrid, block, 0, st>>>(
+          nd, pr, ix, rays, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
+          ctx->d_err);
+      break;
+    }
+    case SRT_SPHERES: {
+      const Node2 *nd = a->nodes.as<Node2>();
+      trace_node2_kernel<SRT_SPHERES, false><<<grid, block, 0, st>>>(
+          nd, pr, ix, rays, n, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
+          ctx->d_err);
+      resolve_node2_kernel<SRT_SPHERES><<<rgrid, block, 0, st>>>(
+          nd, pr, ix, rays, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
+          ctx->d_err);
+      break;
+    }
+    case SRT_TETRAHEDRA: {
+      const NodeT *nd = a->nodes.as<NodeT>();
+      trace_tet_kernel<false><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, nullptr,
+                                                      a->src_faces, nullptr, nullptr, nullptr,
+                                                      dlist, dcount, max_iter, ctx->d_err);
+      resolve_tet_kernel<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, nullptr, a->src_faces,
+                                                  nullptr, nullptr, nullptr, dlist, dcount,
+                                                  max_iter, ctx->d_err);
+      break;
+    }
+  }
+  ctx->launches += 2;
+  return cuda_status(cudaGetLastError(), "trace (no allocation)");
+}
