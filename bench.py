@@ -104,6 +104,22 @@ def make_workload(name):
 BUILD_BYTES_PER_TRI = 3 * 36 + 5 * 16 + 48 + 64 + 40
 
 
+PROFILES = os.path.join(ROOT, "profiles")
+# DRAM bytes per launch of the dominant kernel, from the committed ncu capture
+TRAFFIC_PROFILE = {"tet": "trace_tet_kernel.tet64.md"}
+
+
+def profiled_traffic(kind):
+    try:
+        with open(os.path.join(PROFILES, TRAFFIC_PROFILE[kind])) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(line.split(":")[1])
+    except Exception:  # noqa: BLE001
+        pass
+    return None
+
+
 def algorithmic_bytes_per_ray(kind, stats, nrays):
     """Per-ray bytes the traversal must move: ray (32) + hit (16) + nodes
     visited x node size + primitives tested x primitive record."""
@@ -120,6 +136,7 @@ class ClockSampler:
     def __init__(self, device):
         self.proc = None
         self.device = device
+        self.first = None
         self.path = os.path.join("/tmp", f"srt_clocks_{os.getpid()}.csv")
 
     def __enter__(self):
@@ -148,9 +165,31 @@ class ClockSampler:
         except Exception:  # noqa: BLE001
             pass
 
+    def count(self):
+        try:
+            self.f.flush()
+            with open(self.path) as f:
+                return sum(1 for line in f if line.strip())
+        except Exception:  # noqa: BLE001
+            return 0
+
+    def keep_busy(self, step, sync, extra=2, limit_s=3.0):
+        """Run `step` until `extra` more clock samples have landed (the
+        sampler starts slower than a short timed region), bounded in time."""
+        if self.proc is None:
+            return
+        n0 = self.count()
+        if self.first is None:
+            self.first = n0  # samples before the first busy period are idle
+        t_end = time.time() + limit_s
+        while self.count() < n0 + extra and time.time() < t_end:
+            step()
+            sync()
+
     def summary(self):
         try:
             rows = [r.split(",") for r in open(self.path).read().strip().splitlines()]
+            rows = rows[self.first or 0:] or rows
             sm = [float(r[0]) for r in rows if r[0].strip().isdigit()]
             mx = max(float(r[1]) for r in rows)
             names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
@@ -291,6 +330,7 @@ def run_volume(args, W):
     fe = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
           for _ in range(args.steps)]
     with ClockSampler(dev.index) as clk:
+        clk.keep_busy(fwd_bwd, torch.cuda.synchronize)
         for k in range(args.steps):
             flush.zero_()
             fe[k][0].record()
@@ -301,6 +341,7 @@ def run_volume(args, W):
             fwd_bwd()
             ev[k][1].record()
         torch.cuda.synchronize()
+        clk.keep_busy(fwd_bwd, torch.cuda.synchronize, extra=1)
     fb_ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
     f_ms = statistics.mean(a.elapsed_time(b) for a, b in fe)
     nr = 512 * 512
@@ -418,6 +459,7 @@ def run_batched(args, W):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        clk.keep_busy(batch_step, torch.cuda.synchronize)
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record()
@@ -428,6 +470,7 @@ def run_batched(args, W):
             loop_step()
             ev[k][3].record()
         torch.cuda.synchronize()
+        clk.keep_busy(batch_step, torch.cuda.synchronize, extra=1)
     if world > 1:
         dist.barrier()
     launches = tb.launches() - l_b0
@@ -598,6 +641,7 @@ def run_ours(args, W):
         dist.barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
         for k in range(args.steps):
             flush.zero_()
             e0, e1, e2 = ev[k]
@@ -607,6 +651,7 @@ def run_ours(args, W):
             trace()
             e2.record()
         torch.cuda.synchronize()
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
     if world > 1:
         dist.barrier()
     launches = L.srt_ctx_launch_count(ctx.h) - launches0
@@ -678,7 +723,9 @@ def run_ours(args, W):
     achieved = bpr * nr / (tr_ms * 1e-3) / 1e9
     roofline = {"bound": "hbm", "kernel": "trace", "achieved": round(achieved, 1),
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
-                "peak_source": src, "traffic": None,
+                "peak_source": src, "traffic": profiled_traffic(kind),
+                "traffic_source": (f"profiles/{TRAFFIC_PROFILE[kind]} (first-pass kernel)"
+                                   if kind in TRAFFIC_PROFILE else None),
                 "algorithmic_bytes_per_ray": round(bpr, 1),
                 "visits_per_ray": [round(float(x) / nr, 3) for x in stats],
                 "reference_walk_rays": int(stats_all[3])}
