@@ -201,6 +201,56 @@ class ClockSampler:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
 
 
+# ---------------------------------------------------------------- ranks
+def dist_setup(dev):
+    """One process per GPU (torchrun): NCCL on CUDA, gloo on CPU; returns
+    (world, rank).  The group only carries the barrier and the max-over-ranks
+    step time: replicas exchange no data."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        kw = {"device_id": dev} if dev.type == "cuda" else {}
+        dist.init_process_group("nccl" if dev.type == "cuda" else "gloo",
+                                timeout=datetime.timedelta(seconds=120), **kw)
+    return world, rank
+
+
+def _dist_on():
+    import torch.distributed as dist
+    return dist.is_available() and dist.is_initialized() and dist.get_world_size() > 1
+
+
+def barrier():
+    if _dist_on():
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(vals, dev):
+    """Element-wise maximum of per-rank values (step times) over all ranks."""
+    import torch
+    t = torch.tensor([float(v) for v in vals], dtype=torch.float64, device=dev)
+    if _dist_on():
+        import torch.distributed as dist
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(x) for x in t.cpu().tolist()]
+
+
+def whole_job_mrays(units_per_rank, world, ms_per_step):
+    """Rays of all ranks per second of the slowest rank, in Mrays/s."""
+    return world * units_per_rank / (ms_per_step * 1e-3) / 1e6
+
+
+def dist_teardown():
+    if _dist_on():
+        import torch.distributed as dist
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 # ---------------------------------------------------------------- CPU side
 def cpu_reference_step(W, nthreads=0, stride=4):
     """Reference Build32 + OpenMP Traverse on a strided ray sample.
@@ -309,6 +359,7 @@ def run_volume(args, W):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
     p = V.camera(512, 512, res=256)
     dens = torch.as_tensor(W["dens"], device=dev)
     tf = torch.as_tensor(W["tf"], device=dev)
@@ -342,11 +393,11 @@ def run_volume(args, W):
             ev[k][1].record()
         torch.cuda.synchronize()
         clk.keep_busy(fwd_bwd, torch.cuda.synchronize, extra=1)
-    fb_ms = statistics.mean(a.elapsed_time(b) for a, b in ev)
-    f_ms = statistics.mean(a.elapsed_time(b) for a, b in fe)
+    fb_ms, f_ms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in ev),
+                                  statistics.mean(a.elapsed_time(b) for a, b in fe)], dev)
     nr = 512 * 512
     cpu = None
-    if not args.no_cpu:
+    if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle as O
         q = np.zeros(1, O.VOL_DTYPE)
         q[...] = p.view(O.VOL_DTYPE)
@@ -358,15 +409,17 @@ def run_volume(args, W):
                                          "rays (the reference has no C++ march; its shader "
                                          "march needs the closed GLSL compiler)",
                "forward_ms": round(1e3 * tc, 2)}
-    line = {"metric": METRIC_VOL, "value": round(nr / (fb_ms * 1e-3) / 1e6, 3),
-            "unit": "Mrays/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+    line = {"metric": METRIC_VOL, "value": round(whole_job_mrays(nr, world, fb_ms), 3),
+            "unit": "Mrays/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": round(fb_ms, 4), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": dict(W["config"], l2="flushed between steps (256 MiB write)"),
             "forward_ms": round(f_ms, 4), "forward_backward_ms": round(fb_ms, 4),
             "fwd_bwd_over_fwd": round(fb_ms / f_ms, 3), "clocks": clk.summary(),
             "cpu_baseline": cpu}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    dist_teardown()
 
 
 # ---------------------------------------------------------------- batched
@@ -380,23 +433,17 @@ def run_batched(args, W):
     import ctypes as C
 
     import torch
-    import torch.distributed as dist
 
     import surface_b200 as sb
     from surface_b200 import _lib
     from surface_b200.batch import TriangleBatch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    world, rank = dist_setup(dev)
     B = W["B"]
     fo, ro = B["face_offsets"], B["ray_offsets"]
     ns = fo.size - 1
@@ -455,8 +502,7 @@ def run_batched(args, W):
     l_b0 = tb.launches()
     l_l0 = L.srt_ctx_launch_count(ctx.h)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
+    barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         clk.keep_busy(batch_step, torch.cuda.synchronize)
@@ -471,18 +517,15 @@ def run_batched(args, W):
             ev[k][3].record()
         torch.cuda.synchronize()
         clk.keep_busy(batch_step, torch.cuda.synchronize, extra=1)
-    if world > 1:
-        dist.barrier()
+    barrier()
     launches = tb.launches() - l_b0
     loop_launches = L.srt_ctx_launch_count(ctx.h) - l_l0
     b_ms = [e[0].elapsed_time(e[1]) for e in ev]
     l_ms = [e[2].elapsed_time(e[3]) for e in ev]
-    t = torch.tensor([sum(b_ms), sum(l_ms)], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_per_step = float(t[0]) / args.steps
-    loop_ms = float(t[1]) / args.steps
-    value = world * nr / (ms_per_step * 1e-3) / 1e6
+    tb_tot, tl_tot = max_over_ranks([sum(b_ms), sum(l_ms)], dev)
+    ms_per_step = tb_tot / args.steps
+    loop_ms = tl_tot / args.steps
+    value = whole_job_mrays(nr, world, ms_per_step)
 
     # ---- e2e: scenes and rays copied in from pinned host memory, hits out
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
@@ -508,11 +551,8 @@ def run_batched(args, W):
         t0 = time.perf_counter()
         e2e_step()
         e2e_s.append(time.perf_counter() - t0)
-    e2e_ms = 1e3 * sum(e2e_s) / len(e2e_s)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * nr / (float(te.item()) * 1e-3) / 1e6
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e_value = whole_job_mrays(nr, world, e2e_ms)
     h2d = (h_v.numel() + h_f.numel() + h_r.numel()) * 4
     d2h = h_h.numel() * 4
 
@@ -562,31 +602,23 @@ def run_batched(args, W):
         }
         print(json.dumps(line), flush=True)
     tb.close()
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    dist_teardown()
 
 
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args, W):
     import torch
-    import torch.distributed as dist
 
     import surface_b200 as sb
     from surface_b200 import _lib
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     # all work (ours and the timing events) on one dedicated stream
     stream = torch.cuda.Stream(dev)
     torch.cuda.set_stream(stream)
-    if world > 1:
-        import datetime
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=dev)
+    world, rank = dist_setup(dev)
 
     kind = W["kind"]
     ctx = sb.Context(local)
@@ -637,8 +669,7 @@ def run_ours(args, W):
     launches0 = L.srt_ctx_launch_count(ctx.h)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    if world > 1:
-        dist.barrier()
+    barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         clk.keep_busy(step, torch.cuda.synchronize)
@@ -652,18 +683,13 @@ def run_ours(args, W):
             e2.record()
         torch.cuda.synchronize()
         clk.keep_busy(step, torch.cuda.synchronize, extra=1)
-    if world > 1:
-        dist.barrier()
+    barrier()
     launches = L.srt_ctx_launch_count(ctx.h) - launches0
     build_ms = [e[0].elapsed_time(e[1]) for e in ev]
     trace_ms = [e[1].elapsed_time(e[2]) for e in ev]
-    total_ms = sum(b + t for b, t in zip(build_ms, trace_ms))
-    t = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks([sum(b + t for b, t in zip(build_ms, trace_ms))], dev)[0]
     ms_per_step = total_ms / args.steps
-    value = world * nr / (ms_per_step * 1e-3) / 1e6
+    value = whole_job_mrays(nr, world, ms_per_step)
 
     # ---- e2e through the C ABI with pinned host buffers
     pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
@@ -707,11 +733,8 @@ def run_ours(args, W):
         e2e_step()
         e2e_s.append(time.perf_counter() - t0)
     L.srt_accel_destroy(e2e_acc)
-    e2e_ms = 1e3 * sum(e2e_s) / len(e2e_s)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * nr / (float(te.item()) * 1e-3) / 1e6
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e_value = whole_job_mrays(nr, world, e2e_ms)
     h2d = (h_verts.numel() * 4 + (h_prims.numel() * 4 if h_prims is not None else 0)
            + (h_rad.numel() * 4 if h_rad is not None else 0) + h_rays.numel() * 4)
     d2h = h_hits.numel() * 4 + (h_scal.numel() * 4 if kind == "tet" else 0)
@@ -758,9 +781,7 @@ def run_ours(args, W):
             "cpu_baseline": cpu,
         }
         print(json.dumps(line), flush=True)
-    if world > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    dist_teardown()
 
 
 def main():
@@ -773,10 +794,15 @@ def main():
                     choices=["tet", "tri", "particles", "volume", "batched"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
+    if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
+        return  # the CPU reference runs on rank 0 alone; other ranks exit 0
+    if args.impl == "reference" and args.workload == "volume":
+        print(json.dumps({"impl": "reference", "unavailable":
+                          "the reference's march is GLSL shader code that needs its closed "
+                          "prebuilt compiler; no reference CPU march exists"}), flush=True)
+        return
     W = make_workload(args.workload)
     if args.workload == "volume":
-        if args.impl == "reference":
-            raise SystemExit("the volume workload has no reference CPU march")
         run_volume(args, W)
         return
     if args.impl == "reference":
