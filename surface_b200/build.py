@@ -2,8 +2,10 @@
 
     python -m surface_b200.build [--force]
 
-Flags: -O3, -lineinfo, --fmad=false (no contraction, so float/double
-arithmetic rounds exactly like the reference's x86-64 build), static cudart,
+Flags: -O3, -lineinfo, --fmad=false for the build and traversal sources (no
+contraction, so float/double arithmetic rounds exactly like the reference's
+x86-64 build), --fmad=true for the volume march (its parity bar is a
+tolerance, and contraction shortens its arithmetic chains), static cudart,
 hidden visibility except the extern "C" entry points of include/surface_rt.h.
 """
 from __future__ import annotations
@@ -22,8 +24,9 @@ LIB = os.path.join(PKG, "libsurface_rt.so")
 
 SOURCES = ["srt_build.cu", "srt_trace.cu", "srt_volume.cu", "srt_batch.cu", "srt_capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "--fmad=false", "-Xcompiler", "-fPIC",
+NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "-I" + INCLUDE]
+FMAD = {"srt_volume.cu": "--fmad=true"}  # every other source: --fmad=false
 
 
 def _nvcc():
@@ -52,7 +55,7 @@ def build(force=False, verbose=False):
         o = os.path.join(OBJDIR, src.replace(".cu", ".o"))
         objs.append(o)
         if force or _stale(o, [s] + headers):
-            cmd = [nvcc, *NVCC_FLAGS, *ARCH, "-c", s, "-o", o]
+            cmd = [nvcc, *NVCC_FLAGS, FMAD.get(src, "--fmad=false"), *ARCH, "-c", s, "-o", o]
             if verbose:
                 print(" ".join(cmd))
             subprocess.run(cmd, check=True)

@@ -28,10 +28,10 @@ struct VolConst {
   int tfn;
 };
 
-struct Sample {
-  int cx[8];
-  float w[8];
-  float rho;
+// Lower texel corner (clamped) and trilinear fractions of a fetch.
+struct Cell {
+  int vx, vy, vz;
+  float dx, dy, dz;
 };
 
 // Pixel of thread index `idx`: each warp covers an 8x4 tile (blocks of 128
@@ -89,7 +89,7 @@ __device__ __forceinline__ bool inside(const float p[3]) {
 
 // FilterTexture3DFloat, clamp-to-edge, one component.
 __device__ __forceinline__ float fetch(const float *__restrict__ img, const int dim[3],
-                                       float u, float v, float r, Sample *smp) {
+                                       float u, float v, float r, Cell *cell) {
   const float vox0 = u * (dim[0] - 1.0f);
   const float vox1 = v * (dim[1] - 1.0f);
   const float vox2 = r * (dim[2] - 1.0f);
@@ -116,24 +116,22 @@ __device__ __forceinline__ float fetch(const float *__restrict__ img, const int 
   const float d0 = lerpf(dy, d00, d10);
   const float d1 = lerpf(dy, d01, d11);
   const float val = lerpf(dz, d0, d1);
-  if (smp) {
-    const int xs[2] = {vx, vx1}, ys[2] = {vy, vy1}, zs[2] = {vz, vz1};
-#pragma unroll
-    for (int c = 0; c < 8; c++) {
-      smp->cx[c] = (int)(zs[c >> 2] * sz + ys[(c >> 1) & 1] * sy + xs[c & 1]);
-      smp->w[c] = ((c & 1) ? dx : 1.0f - dx) * (((c >> 1) & 1) ? dy : 1.0f - dy) *
-                  ((c >> 2) ? dz : 1.0f - dz);
-    }
-    smp->rho = val;
+  if (cell) {
+    cell->vx = vx;
+    cell->vy = vy;
+    cell->vz = vz;
+    cell->dx = dx;
+    cell->dy = dy;
+    cell->dz = dz;
   }
   return val;
 }
 
 // Transfer-function lookup: returns rgba, sets i0/i1/f and whether rho was
 // inside the table's range (clamped samples have no density gradient).
-__device__ __forceinline__ void tf_lookup(const float4 *__restrict__ tf, int tfn,
-                                          float rho, float4 &c, int &i0, int &i1,
-                                          float &f, bool &inrange) {
+__device__ __forceinline__ void tf_lookup_ab(const float4 *__restrict__ tf, int tfn,
+                                             float rho, float4 &c, int &i0, int &i1,
+                                             float &f, bool &inrange, float4 &a, float4 &b) {
   const float top = (float)(tfn - 1);
   float x = rho * top;
   inrange = (x > 0.0f) && (x < top);
@@ -141,9 +139,17 @@ __device__ __forceinline__ void tf_lookup(const float4 *__restrict__ tf, int tfn
   i0 = (int)x;
   i1 = min(i0 + 1, tfn - 1);
   f = x - (float)i0;
-  const float4 a = __ldg(&tf[i0]), b = __ldg(&tf[i1]);
+  a = __ldg(&tf[i0]);
+  b = __ldg(&tf[i1]);
   c = make_float4(lerpf(f, a.x, b.x), lerpf(f, a.y, b.y), lerpf(f, a.z, b.z),
                   lerpf(f, a.w, b.w));
+}
+
+__device__ __forceinline__ void tf_lookup(const float4 *__restrict__ tf, int tfn,
+                                          float rho, float4 &c, int &i0, int &i1,
+                                          float &f, bool &inrange) {
+  float4 a, b;
+  tf_lookup_ab(tf, tfn, rho, c, i0, i1, f, inrange, a, b);
 }
 
 __global__ void __launch_bounds__(128)
@@ -187,6 +193,14 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
 
 constexpr int kTfCopies = 8;  // copies of the block-local TF gradient
 
+__device__ __forceinline__ void flush_entry(float *g, int i, float (&a)[4]) {
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    if (a[k] != 0.0f) atomicAdd(&g[4 * i + k], a[k]);
+    a[k] = 0.0f;
+  }
+}
+
 __device__ __forceinline__ void flush_tf(float *g, int i0, int i1, float (&a0)[4],
                                          float (&a1)[4]) {
 #pragma unroll
@@ -198,11 +212,17 @@ __device__ __forceinline__ void flush_tf(float *g, int i0, int i1, float (&a0)[4
   }
 }
 
-__device__ __forceinline__ void flush_dens(float *__restrict__ g, const int (&cx)[8],
-                                           float (&a)[8]) {
+// Add the eight corner sums of one texel cell (lower corner vx, vy, vz;
+// upper corners clamped like the fetch) to the density gradient.
+__device__ __forceinline__ void flush_dens(float *__restrict__ g, const int dim[3], int vx,
+                                           int vy, int vz, float (&a)[8]) {
+  const size_t sy = (size_t)dim[0], sz = (size_t)dim[0] * dim[1];
+  const int xs[2] = {vx, min(vx + 1, dim[0] - 1)};
+  const int ys[2] = {vy, min(vy + 1, dim[1] - 1)};
+  const int zs[2] = {vz, min(vz + 1, dim[2] - 1)};
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    if (a[k] != 0.0f) atomicAdd(&g[cx[k]], a[k]);
+    if (a[k] != 0.0f) atomicAdd(&g[zs[k >> 2] * sz + ys[(k >> 1) & 1] * sy + xs[k & 1]], a[k]);
     a[k] = 0.0f;
   }
 }
@@ -241,23 +261,22 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
       // and flushed when the bin / cell changes.
       int run_i0 = -1;
       float ta0[4] = {0.f, 0.f, 0.f, 0.f}, ta1[4] = {0.f, 0.f, 0.f, 0.f};
-      int run_cell = -1;
-      int run_cx[8];
+      int run_cell = -1, rvx = 0, rvy = 0, rvz = 0;
       float da[8];
 #pragma unroll
-      for (int cc = 0; cc < 8; cc++) { run_cx[cc] = 0; da[cc] = 0.0f; }
+      for (int cc = 0; cc < 8; cc++) da[cc] = 0.0f;
       for (int s = ns - 1; s >= 0; s--) {
         const float t = t0 + ((float)s + 0.5f) * K.p.step;
         const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
         if (!inside(p)) continue;
-        Sample smp;
+        Cell cl;
         const float rho = fetch(dens, K.dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
-                                0.5f * p[2] + 0.5f, &smp);
-        float4 c;
+                                0.5f * p[2] + 0.5f, &cl);
+        float4 c, ta, tb;
         int i0, i1;
         float f;
         bool inr;
-        tf_lookup(tf, K.tfn, rho, c, i0, i1, f, inr);
+        tf_lookup_ab(tf, K.tfn, rho, c, i0, i1, f, inr, ta, tb);
         const float sig = K.p.sigma_scale * c.w;
         const float e = expf(-sig * K.p.step);
         float al = 1.0f - e;
@@ -271,24 +290,50 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         const float gc3 = clamped ? 0.0f : ga * K.p.sigma_scale * K.p.step * e;
         // transfer-function gradient: i1 = i0 + 1 except at the top entry
         if (i0 != run_i0) {
-          if (run_i0 >= 0) flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
+          // The run's two table entries are run_i0 (ta0) and run_i0 + 1 (ta1).
+          // A step of one bin keeps the shared entry in registers and
+          // flushes only the entry that leaves.
+          if (run_i0 >= 0) {
+            if (i0 == run_i0 + 1) {
+              flush_entry(my_gtf, run_i0, ta0);
+#pragma unroll
+              for (int k = 0; k < 4; k++) { ta0[k] = ta1[k]; ta1[k] = 0.0f; }
+            } else if (i0 == run_i0 - 1) {
+              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1);
+#pragma unroll
+              for (int k = 0; k < 4; k++) { ta1[k] = ta0[k]; ta0[k] = 0.0f; }
+            } else {
+              flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
+            }
+          }
           run_i0 = i0;
         }
         const float wf0 = 1.0f - f, wf1 = f;
         ta0[0] += wf0 * gc0; ta0[1] += wf0 * gc1; ta0[2] += wf0 * gc2; ta0[3] += wf0 * gc3;
         ta1[0] += wf1 * gc0; ta1[1] += wf1 * gc1; ta1[2] += wf1 * gc2; ta1[3] += wf1 * gc3;
         if (inr) {
-          const float4 a = __ldg(&tf[i0]), b = __ldg(&tf[i1]);
-          const float drho = (gc0 * (b.x - a.x) + gc1 * (b.y - a.y) + gc2 * (b.z - a.z) +
-                              gc3 * (b.w - a.w)) * top;
-          if (smp.cx[0] != run_cell) {
-            if (run_cell >= 0) flush_dens(gdens, run_cx, da);
-            run_cell = smp.cx[0];
-#pragma unroll
-            for (int cc = 0; cc < 8; cc++) run_cx[cc] = smp.cx[cc];
+          const float drho = (gc0 * (tb.x - ta.x) + gc1 * (tb.y - ta.y) +
+                              gc2 * (tb.z - ta.z) + gc3 * (tb.w - ta.w)) * top;
+          const int key = (cl.vz * K.dim[1] + cl.vy) * K.dim[0] + cl.vx;
+          if (key != run_cell) {
+            if (run_cell >= 0) flush_dens(gdens, K.dim, rvx, rvy, rvz, da);
+            run_cell = key;
+            rvx = cl.vx;
+            rvy = cl.vy;
+            rvz = cl.vz;
           }
-#pragma unroll
-          for (int cc = 0; cc < 8; cc++) da[cc] += smp.w[cc] * drho;
+          // corner c = x + 2y + 4z gets drho * wx * wy * wz
+          const float x0 = drho * (1.0f - cl.dx), x1 = drho * cl.dx;
+          const float y0z0 = (1.0f - cl.dy) * (1.0f - cl.dz), y1z0 = cl.dy * (1.0f - cl.dz);
+          const float y0z1 = (1.0f - cl.dy) * cl.dz, y1z1 = cl.dy * cl.dz;
+          da[0] += x0 * y0z0;
+          da[1] += x1 * y0z0;
+          da[2] += x0 * y1z0;
+          da[3] += x1 * y1z0;
+          da[4] += x0 * y0z1;
+          da[5] += x1 * y0z1;
+          da[6] += x0 * y1z1;
+          da[7] += x1 * y1z1;
         }
         Cb0 += Tk * al * c.x;
         Cb1 += Tk * al * c.y;
@@ -296,7 +341,7 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         Tn = Tk;
       }
       if (run_i0 >= 0) flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
-      if (run_cell >= 0) flush_dens(gdens, run_cx, da);
+      if (run_cell >= 0) flush_dens(gdens, K.dim, rvx, rvy, rvz, da);
     }
   }
   __syncthreads();
