@@ -537,6 +537,31 @@ SRT_API srt_status srt_accel_dump(srt_accel *a, const char *path) {
   return SRT_OK;
 }
 
+// ---------------------------------------------------------------- zero copy
+// Device-visible address of page-locked host memory (cudaMallocHost /
+// cudaHostAlloc memory is mapped into the device's address space under
+// unified addressing), or nullptr for device or pageable memory.
+static void *mapped_host(const void *p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  if (at.type != cudaMemoryTypeHost || !at.devicePointer) return nullptr;
+  return at.devicePointer;
+}
+
+// An optional array that the kernels can address directly: NULL, device
+// memory, or page-locked host memory.  Sets ok = false for pageable memory.
+static void *direct_view(const void *p, bool &ok) {
+  if (!p) return nullptr;
+  if (is_device_ptr(p)) return const_cast<void *>(p);
+  void *m = mapped_host(p);
+  if (!m) ok = false;
+  return m;
+}
+
 SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n,
                                      srt_hit *hits, const srt_trace_opts *opts) {
   if (!a || (!rays && n) || (!hits && n)) {
@@ -553,6 +578,40 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
   srt_trace_opts o;
   memset(&o, 0, sizeof(o));
   if (opts) o = *opts;
+  if (o.vertex_scalar && a->kind == SRT_TETRAHEDRA && !is_device_ptr(o.vertex_scalar)) {
+    // vertex count is not stored; the scalar array is read only at hit
+    // vertices, so a host array would have to be staged whole
+    set_error("vertex_scalar must be device memory");
+    return SRT_ERR_INVALID;
+  }
+  if (o.stats && !is_device_ptr(o.stats)) {
+    set_error("stats must be device memory");
+    return SRT_ERR_INVALID;
+  }
+  {
+    // Page-locked host rays and hits: the kernels read the rays and write the
+    // hits over the host link while they traverse, so the transfers overlap
+    // the traversal instead of preceding and following it.
+    void *mr = mapped_host(rays), *mh = mapped_host(hits);
+    if (mr && mh) {
+      bool ok = true;
+      void *pn = direct_view(o.prev_normals, ok), *sub = direct_view(o.subface, ok);
+      void *scal = direct_view(o.scalar_out, ok), *norm = direct_view(o.normal_out, ok);
+      if (ok) {
+        if ((reinterpret_cast<uintptr_t>(mr) | reinterpret_cast<uintptr_t>(mh)) & 15u) {
+          set_error("ray and hit arrays must be 16-byte aligned");
+          return SRT_ERR_INVALID;
+        }
+        srt_status s = launch_trace(
+            a, static_cast<const srt_ray *>(mr), n, static_cast<srt_hit *>(mh),
+            static_cast<const float *>(pn), static_cast<uint32_t *>(sub),
+            a->kind == SRT_TETRAHEDRA ? o.vertex_scalar : nullptr, static_cast<float *>(scal),
+            static_cast<float *>(norm), o.stats, o.flags);
+        if (s != SRT_OK) return s;
+        return check_device_errors(ctx);
+      }
+    }
+  }
   const void *drays = nullptr, *dpn = nullptr, *dvs = nullptr;
   srt_status s = device_view(ctx, rays, n * sizeof(srt_ray), ctx->s_stage_in, &drays);
   if (s != SRT_OK) return s;

@@ -269,6 +269,72 @@ def test_torch_device_inputs_and_async_trace():
     assert_hits_equal(hn, o.trace(rays))
 
 
+def _pinned(a, dt=np.float32):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a).view(dt).copy()).pin_memory()
+
+
+def test_host_arrays_match_device_path():
+    """Pageable host arrays (staged copies) and page-locked host arrays (read
+    and written by the kernels in place) give the device path's results bit
+    for bit, with every optional input and output."""
+    import ctypes as C
+
+    import torch
+    from surface_b200 import _lib
+
+    def dev(a, dt=np.float32):
+        return torch.as_tensor(np.ascontiguousarray(a).view(dt)).cuda()
+
+    v, f, sc = S.tet_grid(24, seed=41)
+    acc = sb.TetraAccel()
+    acc.Build32(sb.Tetrahedron(v, f))
+    rays = S.ortho_rays(560, 560)  # 313,600 rays
+    n = rays.size
+    vs = torch.as_tensor(sc).cuda()
+    d = acc.Traverse(dev(rays).reshape(-1, 8), want_subface=True, vertex_scalar=vs,
+                     want_scalar=True)
+    dh = d.hits.cpu().numpy().reshape(-1).view(O.HIT_DTYPE)
+    h = acc.Traverse(rays, want_subface=True, vertex_scalar=vs, want_scalar=True)
+    assert_hits_equal(h.hits, dh)
+    assert np.array_equal(h.subface.view(np.int32), d.subface.cpu().numpy())
+    assert np.array_equal(bits(h.scalar), bits(d.scalar.cpu().numpy()))
+    assert (h.hits["prim"] != O.MISS).mean() > 0.5
+    pr, ph = _pinned(rays), torch.zeros((n, 4)).pin_memory()
+    psub, psc = torch.zeros(n, dtype=torch.int32).pin_memory(), torch.zeros(n).pin_memory()
+    o = _lib.TraceOpts(None, psub.data_ptr(), vs.data_ptr(), psc.data_ptr(), None, None, 0, 0)
+    _lib.check(acc.L.srt_trace_closest(acc.h, pr.data_ptr(), n, ph.data_ptr(), C.byref(o)))
+    assert_hits_equal(ph.numpy().reshape(-1).view(O.HIT_DTYPE), dh)
+    assert np.array_equal(psub.numpy(), d.subface.cpu().numpy())
+    assert np.array_equal(bits(psc.numpy()), bits(d.scalar.cpu().numpy()))
+
+    pos, rad = S.particles(100_000, seed=42)
+    sp = sb.ParticleAccel()
+    sp.Build32(sb.Particles(pos, rad))
+    prim = S.pinhole_rays(600, 500, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    r1 = sp.Traverse(prim, want_normal=True)
+    sec = prim.copy()
+    hit = r1.hits["prim"] != O.MISS
+    sec["org"][hit] = (prim["org"][hit] + r1.hits["t"][hit, None] * prim["dir"][hit])
+    sec["dir"][hit] = S.hemisphere_dirs(r1.normal[hit], seed=43)
+    sec["prev_prim"] = r1.hits["prim"]
+    sec["prev_t"] = r1.hits["t"]
+    nrm = np.ascontiguousarray(r1.normal, np.float32)
+    d = sp.Traverse(dev(sec).reshape(-1, 8), prev_normals=torch.as_tensor(nrm).cuda(),
+                    want_normal=True)
+    dh = d.hits.cpu().numpy().reshape(-1).view(O.HIT_DTYPE)
+    h = sp.Traverse(sec, prev_normals=nrm, want_normal=True)
+    assert_hits_equal(h.hits, dh)
+    assert np.array_equal(bits(h.normal), bits(d.normal.cpu().numpy()))
+    n = sec.size
+    pr, ph, pn = _pinned(sec), torch.zeros((n, 4)).pin_memory(), _pinned(nrm)
+    pno = torch.zeros((n, 3)).pin_memory()
+    o = _lib.TraceOpts(pn.data_ptr(), None, None, None, pno.data_ptr(), None, 0, 0)
+    _lib.check(sp.L.srt_trace_closest(sp.h, pr.data_ptr(), n, ph.data_ptr(), C.byref(o)))
+    assert_hits_equal(ph.numpy().reshape(-1).view(O.HIT_DTYPE), dh)
+    assert np.array_equal(bits(pno.numpy()), bits(d.normal.cpu().numpy()))
+
+
 # ---------------------------------------------------------------- full size
 def test_full_size_triangle_workload():
     """131,072-triangle displaced octasphere, 512^2 pinhole rays."""
