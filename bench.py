@@ -71,10 +71,13 @@ def make_workload(name):
     if name == "particles":
         pos, rad = S.particles()
         rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
-        return dict(kind="sphere", verts=pos, radius=rad, rays=rays,
-                    config={"workload": "particles16M: 16,777,216 spheres, one frame "
-                                        "(rebuild + 2048x2048 primaries)",
-                            "prims": int(pos.shape[0]), "rays": int(rays.size)})
+        return dict(kind="sphere", verts=pos, radius=rad, rays=rays, frames=10,
+                    config={"workload": "particles16M: 16,777,216 spheres advected over 10 "
+                                        "frames (step k = frame k mod 10): LBVH rebuild, "
+                                        "2048x2048 pinhole primaries, one uniform-hemisphere "
+                                        "secondary per hit with the self-hit rule",
+                            "prims": int(pos.shape[0]), "primary_rays": int(rays.size),
+                            "frames": 10})
     if name == "volume":
         dens = S.volume_blobs(256, nblobs=32)
         tgt = S.volume_blobs(256, nblobs=32, shift_voxels=2.0)
@@ -305,12 +308,42 @@ def cpu_reference_batched(W, nthreads=0, stride=16):
     return value, tb, tt, ns, ("reference" if use_ref else "port")
 
 
+def cpu_reference_particles(W, nthreads=0, stride=4):
+    """Reference Build32 of the frame-0 cloud + OpenMP Traverse of every 4th
+    primary and every 4th secondary (the secondaries spawned from the
+    reference's own primary hits by the workload's bounce rule, outside the
+    timed calls).  Returns (Mrays/s scaled to all rays, build s, trace s,
+    sample rays, kind)."""
+    from oracle import oracle as O
+    from surface_b200 import scenes as S
+    use_ref = O.have_ref() and O.ref() is not None
+    Acc = O.RefAccel if use_ref else O.OracleAccel
+    t0 = time.perf_counter()
+    acc = Acc(O.SPHERE, W["verts"], None, W["radius"])
+    tb = time.perf_counter() - t0
+    kw = {"nthreads": nthreads, "chunk": 64} if use_ref else {"nthreads": nthreads}
+    prim = W["rays"]
+    t0 = time.perf_counter()
+    h1 = acc.trace(prim[::stride], **kw)
+    tt = time.perf_counter() - t0
+    nrm = S.sphere_normals_np(prim[::stride], h1, W["verts"])
+    sec, sn = S.spawn_secondary_np(prim[::stride], h1, nrm, 0)
+    t0 = time.perf_counter()
+    acc.trace(sec, prev_normals=sn, **kw)
+    tt += time.perf_counter() - t0
+    ns = prim[::stride].size + sec.size
+    total = stride * ns  # primaries + secondaries of the whole frame (scaled)
+    value = total / (tb + tt * stride) / 1e6
+    return value, tb, tt, ns, ("reference" if use_ref else "port")
+
+
 def run_reference_arm(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    step = cpu_reference_batched if W["kind"] == "batched" else cpu_reference_step
+    step = {"batched": cpu_reference_batched,
+            "sphere": cpu_reference_particles}.get(W["kind"], cpu_reference_step)
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
@@ -321,10 +354,13 @@ def run_reference_arm(args, W):
         tts.append(tt)
     value = statistics.median(vals)
     nr = W["rays"].size
+    if W["kind"] == "sphere":
+        nr = int(ns * 4)  # primaries + secondaries of one frame
     ms = 1e3 * nr / (value * 1e6)
     stride = 16 if W["kind"] == "batched" else 4
     line = {
-        "impl": "reference", "metric": METRIC_BATCH if W["kind"] == "batched" else METRIC,
+        "impl": "reference",
+        "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART}.get(W["kind"], METRIC),
         "value": round(value, 4), "unit": "Mrays/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
@@ -345,6 +381,7 @@ def run_reference_arm(args, W):
 METRIC = "Mrays/s (LBVH build + closest hit per step)"
 METRIC_VOL = "Mrays/s (volume march forward + adjoint per step)"
 METRIC_BATCH = "Mrays/s (64-scene batched LBVH build + closest hit per step)"
+METRIC_PART = "Mrays/s (particle frame: LBVH rebuild + primaries + secondaries per step)"
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
          "volume": "f32", "batched": "f32"}
 
@@ -605,6 +642,185 @@ def run_batched(args, W):
     dist_teardown()
 
 
+# ---------------------------------------------------------------- particles
+def run_particles(args, W):
+    """One step = one frame f = k mod 10 of the advected cloud (frames made on
+    the device before timing): LBVH rebuild from the frame's centres, 2048^2
+    primaries with hit normals, srt_spawn_secondary (one hemisphere ray per
+    hit, ray order), secondaries traced with prev_normals (self-hit rule).
+    value = (primaries + secondaries) / step time."""
+    import ctypes as C
+
+    import torch
+
+    import surface_b200 as sb
+    from surface_b200 import _lib
+    from surface_b200 import scenes as S
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
+    nf = W["frames"]
+    frames = S.particle_frames(W["verts"], nf, device=dev)
+    rad = torch.as_tensor(W["radius"], device=dev)
+    npart = int(rad.numel())
+    nr = W["rays"].size
+    rays = torch.as_tensor(W["rays"].view(np.float32).reshape(-1, 8), device=dev)
+    h1 = torch.empty((nr, 4), device=dev)
+    n1 = torch.empty((nr, 3), device=dev)
+    sec = torch.empty((nr, 8), device=dev)
+    sn = torch.empty((nr, 3), device=dev)
+    h2 = torch.empty((nr, 4), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    L = _lib.load()
+    chk = _lib.check
+    ctx = sb.Context(local)
+    ctx.use_torch_stream()
+    acc = C.c_void_p()
+    chk(L.srt_accel_create(ctx.h, _lib.SRT_SPHERES, C.byref(acc)))
+    cnt = C.c_uint32()
+
+    def build(k):
+        chk(L.srt_accel_build_spheres(acc, frames[k % nf].data_ptr(), rad.data_ptr(),
+                                      C.c_float(0.0), npart))
+
+    def primaries(stats=None):
+        o = _lib.TraceOpts(None, None, None, None, n1.data_ptr(), stats, 0, 0)
+        chk(L.srt_trace_closest(acc, rays.data_ptr(), nr, h1.data_ptr(), C.byref(o)))
+
+    def secondaries(k):
+        chk(L.srt_spawn_secondary(ctx.h, rays.data_ptr(), h1.data_ptr(), n1.data_ptr(), nr,
+                                  C.c_uint64(k), sec.data_ptr(), sn.data_ptr(), C.byref(cnt)))
+        o = _lib.TraceOpts(sn.data_ptr(), None, None, None, None, None, 0, 0)
+        chk(L.srt_trace_closest(acc, sec.data_ptr(), cnt.value, h2.data_ptr(), C.byref(o)))
+        return cnt.value
+
+    def step(k=0):
+        build(k)
+        primaries()
+        return secondaries(k)
+
+    for k in range(max(args.warmup, 3)):
+        step(k)
+    torch.cuda.synchronize()
+    # primary traversal work counters for the roofline (untimed)
+    build(0)
+    st = torch.zeros(4, dtype=torch.int64, device=dev)
+    primaries(st.data_ptr())
+    torch.cuda.synchronize()
+    stats_all = st.cpu().numpy().astype(np.float64)
+    stats = stats_all[:3]
+    sec0 = secondaries(0)
+
+    launches0 = L.srt_ctx_launch_count(ctx.h)
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+    nsec = []
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            build(k)
+            ev[k][1].record()
+            primaries()
+            ev[k][2].record()
+            nsec.append(secondaries(k))
+            ev[k][3].record()
+        torch.cuda.synchronize()
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
+    barrier()
+    launches = L.srt_ctx_launch_count(ctx.h) - launches0
+    b_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    p_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    s_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    total_ms = max_over_ranks([sum(b_ms) + sum(p_ms) + sum(s_ms)], dev)[0]
+    ms_per_step = total_ms / args.steps
+    rays_per_step = nr + statistics.mean(nsec)
+    value = whole_job_mrays(rays_per_step, world, ms_per_step)
+
+    # ---- e2e: centres, radii and primaries from pinned host memory, both
+    # hit arrays back to pinned host memory, every step
+    pin = lambda a: torch.from_numpy(np.ascontiguousarray(a)).pin_memory()  # noqa: E731
+    h_pos = pin(W["verts"])
+    h_rad = pin(W["radius"])
+    h_rays = pin(W["rays"].view(np.float32).reshape(-1, 8))
+    h_h1 = torch.empty((nr, 4)).pin_memory()
+    h_h2 = torch.empty((nr, 4)).pin_memory()
+
+    def e2e_step(k=0):
+        chk(L.srt_accel_build_spheres(acc, h_pos.data_ptr(), h_rad.data_ptr(), C.c_float(0.0),
+                                      npart))
+        o = _lib.TraceOpts(None, None, None, None, n1.data_ptr(), None, 0, 0)
+        chk(L.srt_trace_closest(acc, h_rays.data_ptr(), nr, h1.data_ptr(), C.byref(o)))
+        c = secondaries(k)
+        h_h1.copy_(h1, non_blocking=True)
+        h_h2[:c].copy_(h2[:c], non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        return c
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s, e2e_c = [], []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_c.append(e2e_step())
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e_value = whole_job_mrays(nr + statistics.mean(e2e_c), world, e2e_ms)
+    h2d = (h_pos.numel() + h_rad.numel() + h_rays.numel()) * 4
+    d2h = int(16 * (nr + statistics.mean(e2e_c)))
+
+    hbm, src = peaks()
+    bpr = algorithmic_bytes_per_ray("sphere", stats, nr)
+    pr_ms = statistics.mean(p_ms)
+    achieved = bpr * nr / (pr_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "primary trace", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_ray": round(bpr, 1),
+                "visits_per_ray": [round(float(x) / nr, 3) for x in stats],
+                "reference_walk_rays": int(stats_all[3])}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cv, ctb, ctt, cns, ck = cpu_reference_particles(W)
+        cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
+               "kind": ck, "build_s": round(ctb, 3), "trace_s": round(ctt, 3),
+               "sample": f"Build32 of frame 0 + every 4th primary and the secondaries of "
+                         f"those hits ({cns} rays), trace time scaled to the frame"}
+    L.srt_accel_destroy(acc)
+    if rank == 0:
+        line = {
+            "metric": METRIC_PART, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE["sphere"],
+            "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)",
+                           parallelism=f"replicas x{world}"),
+            "build_ms": round(statistics.mean(b_ms), 4),
+            "primary_trace_ms": round(pr_ms, 4),
+            "secondary_ms": round(statistics.mean(s_ms), 4),
+            "secondary_rays_per_step": round(statistics.mean(nsec), 1),
+            "secondary_rays_frame0": int(sec0),
+            "clocks": clk.summary(),
+            "e2e": {"value": round(e2e_value, 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    dist_teardown()
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args, W):
     import torch
@@ -809,6 +1025,8 @@ def main():
         run_reference_arm(args, W)
     elif args.workload == "batched":
         run_batched(args, W)
+    elif args.workload == "particles":
+        run_particles(args, W)
     else:
         run_ours(args, W)
 

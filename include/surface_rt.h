@@ -290,6 +290,22 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx,
                                         const float *grad_image,
                                         float *grad_density, float *grad_tf);
 
+/* ---- secondary rays ----------------------------------------------------- */
+/* One secondary ray per hit ray (the particle workload's bounce; in the
+ * reference a fragment shader builds it and calls back trace() with
+ * prev_prim_id / prev_hit_t / prev_hit_normal set, gles/gles_glsl_runtime.cc:
+ * 119-136; no render/ counterpart).  For every i with hits[i].prim != miss,
+ * in order of i: origin = rays[i].org + t * rays[i].dir (float), direction
+ * uniform on the hemisphere about normals[i] (unit), drawn from a
+ * counter-based stream of `seed` and i; prev_prim = hit prim, prev_t = t;
+ * out_normals gets the unit normal (pass it as srt_trace_opts.prev_normals).
+ * All arrays are device memory (out / out_normals sized for n rays); *count
+ * receives the number of rays written; synchronises the context stream. */
+SRT_API srt_status srt_spawn_secondary(srt_ctx *ctx, const srt_ray *rays,
+                                       const srt_hit *hits, const float *normals,
+                                       size_t n, uint64_t seed, srt_ray *out,
+                                       float *out_normals, uint32_t *count);
+
 /* ---- batched build + trace ---------------------------------------------- */
 /* Many triangle scenes of uneven size, built and traced in one pass (the
  * per-scene Build32 + Traverse of every scene, with identical results).

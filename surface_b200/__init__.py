@@ -7,4 +7,4 @@ ABI of include/surface_rt.h); this package is its host-side mirror.
 from .accel import (HIT_DTYPE, MISS, RAY_DTYPE, Context, Mesh, ParticleAccel,  # noqa: F401
                     ParticleBuildOptions, Particles, SurfaceError, Tetrahedron,
                     TetraAccel, TetraBuildOptions, TriangleAccel, TriangleBuildOptions,
-                    stage_karras, stage_morton, stage_sort_pairs)
+                    spawn_secondary, stage_karras, stage_morton, stage_sort_pairs)

@@ -81,6 +81,7 @@ _SIGS = {
     "srt_volume_camera": [C.c_int32, C.c_int32, _P, _P, _P, C.c_float, _P],
     "srt_volume_march_fwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P],
     "srt_volume_march_bwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P],
+    "srt_spawn_secondary": [_P, _P, _P, _P, _SZ, C.c_uint64, _P, _P, _P],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],

@@ -369,7 +369,31 @@ def stage_karras(sorted_codes, ctx=None):
     return child, lt, rt
 
 
+# ---------------------------------------------------------------- rays
+def spawn_secondary(rays, hits, normals, seed, ctx=None):
+    """One hemisphere ray per hit (srt_spawn_secondary).  rays (n, 8), hits
+    (n, 4) and normals (n, 3) are CUDA float32 tensors (the outputs of a
+    Traverse with want_normal=True); returns (secondary rays (k, 8), their
+    unit normals (k, 3)) for the k hit rays, in ray order, to be traced with
+    prev_normals=normals."""
+    if not (_is_cuda(rays) and _is_cuda(hits) and _is_cuda(normals)):
+        raise SurfaceError(_lib.SRT_ERR_INVALID, "spawn_secondary takes CUDA tensors")
+    ctx = ctx or Context.default(rays.device.index or 0)
+    r, h, nrm = rays.contiguous(), hits.contiguous(), normals.contiguous().float()
+    n = r.shape[0]
+    out = torch.empty((n, 8), dtype=torch.float32, device=r.device)
+    out_n = torch.empty((n, 3), dtype=torch.float32, device=r.device)
+    cnt = C.c_uint32()
+    ctx.use_torch_stream()
+    check(ctx.L.srt_spawn_secondary(ctx.h, r.data_ptr(), h.data_ptr(), nrm.data_ptr(), n,
+                                    C.c_uint64(seed), out.data_ptr(), out_n.data_ptr(),
+                                    C.byref(cnt)))
+    k = cnt.value
+    return out[:k], out_n[:k]
+
+
 __all__ = ["Context", "Mesh", "Tetrahedron", "Particles", "TriangleAccel", "TetraAccel",
            "ParticleAccel", "TriangleBuildOptions", "TetraBuildOptions",
            "ParticleBuildOptions", "stage_morton", "stage_sort_pairs", "stage_karras",
+           "spawn_secondary",
            "RAY_DTYPE", "HIT_DTYPE", "MISS", "SurfaceError"]

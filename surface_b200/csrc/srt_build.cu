@@ -341,6 +341,10 @@ static srt_status exclusive_scan(srt_ctx *ctx, const uint32_t *in, uint32_t *out
   return scan_levels(ctx->stream, in, out, n, ctx->s_scan.as<uint32_t>(), ctx->launches);
 }
 
+srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n) {
+  return exclusive_scan(ctx, in, out, n);
+}
+
 namespace {
 // ------------------------------------------------------------------ 3. radix sort
 constexpr int kRsBits = 8;

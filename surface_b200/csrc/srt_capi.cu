@@ -205,7 +205,7 @@ SRT_API srt_status srt_ctx_destroy(srt_ctx *c) {
                     &c->s_kflags, &c->s_krange, &c->s_kparent, &c->s_lparent,
                     &c->s_counter, &c->s_ibox, &c->s_flag, &c->s_slot, &c->s_partial,
                     &c->s_stage_in, &c->s_stage_out, &c->s_stage_aux, &c->s_stage_sub,
-                    &c->s_stage_scal, &c->s_stage_norm, &c->s_defer};
+                    &c->s_stage_scal, &c->s_stage_norm, &c->s_defer, &c->s_spawn};
   for (DevBuf *b : bufs) b->release();
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);

@@ -162,6 +162,28 @@ class VelocityField:
                 v[:, c] += self.a[m, c] * np.sin(arg + self.ph[m, c])
         return (pos + dt * v).astype(np.float32)
 
+    def advect_torch(self, pos, dt=1.0):
+        """The same step on a torch tensor (device-side frame generation)."""
+        import torch
+        k = torch.as_tensor(self.k, device=pos.device)
+        v = torch.zeros_like(pos)
+        for m in range(self.k.shape[0]):
+            arg = pos @ k[m]
+            for c in range(3):
+                v[:, c] += float(self.a[m, c]) * torch.sin(arg + float(self.ph[m, c]))
+        return pos + dt * v
+
+
+def particle_frames(pos, nframes=10, seed=7, device=None):
+    """Centres of `nframes` frames: frame 0 = pos, frame f+1 = frame f advected
+    by VelocityField(seed); torch tensors on `device`."""
+    import torch
+    vf = VelocityField(seed)
+    frames = [torch.as_tensor(pos, device=device)]
+    for _ in range(nframes - 1):
+        frames.append(vf.advect_torch(frames[-1]).contiguous())
+    return frames
+
 
 # ---------------------------------------------------------------- rays
 def _normalize(d):
@@ -293,3 +315,53 @@ def batched_scenes(nscenes=64, seed=2024, lo=1e3, hi=1e6, sizes=(128, 256, 512, 
     return dict(vertices=np.concatenate(verts), faces=faces.astype(np.uint32),
                 rays=np.concatenate(rays), face_offsets=np.asarray(fo, np.uint64),
                 ray_offsets=np.asarray(ro, np.uint64), counts=counts, sides=sides)
+
+
+# ---------------------------------------------------------------- secondaries
+def _mix64(z):
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(0xbf58476d1ce4e5b9)
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(0x94d049bb133111eb)
+    return z ^ (z >> np.uint64(31))
+
+
+def spawn_secondary_np(rays, hits, normals, seed):
+    """NumPy statement of srt_spawn_secondary (the particle workload's bounce):
+    for every hit ray, in order, a ray from the hit point (float32
+    org + t * dir) in a uniform hemisphere direction about the unit normal,
+    with prev_prim / prev_t of the hit.  Directions are computed in float64
+    here (the device computes in float32), so they agree to ~1e-6.
+    Returns (rays RAY_DTYPE (k,), unit normals float32 (k, 3))."""
+    hit = np.nonzero(hits["prim"] != MISS)[0]
+    n = np.asarray(normals, np.float64)[hit]
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    with np.errstate(over="ignore"):
+        z = _mix64(np.uint64(seed) + np.uint64(0x9e3779b97f4a7c15) * (hit.astype(np.uint64)
+                                                                     + np.uint64(1)))
+    u1 = (z >> np.uint64(40)).astype(np.float64) / 16777216.0
+    u2 = ((z >> np.uint64(16)) & np.uint64(0xffffff)).astype(np.float64) / 16777216.0
+    ct = u1
+    st = np.sqrt(np.maximum(0.0, 1.0 - ct * ct))
+    lx, ly = st * np.cos(2 * np.pi * u2), st * np.sin(2 * np.pi * u2)
+    sg = np.where(np.signbit(n[:, 2]), -1.0, 1.0)
+    a = -1.0 / (sg + n[:, 2])
+    b = n[:, 0] * n[:, 1] * a
+    b1 = np.stack([1.0 + sg * n[:, 0] ** 2 * a, sg * b, -sg * n[:, 0]], 1)
+    b2 = np.stack([b, sg + n[:, 1] ** 2 * a, -n[:, 1]], 1)
+    d = lx[:, None] * b1 + ly[:, None] * b2 + ct[:, None] * n
+    out = np.zeros(hit.size, RAY_DTYPE)
+    out["org"] = rays["org"][hit] + hits["t"][hit, None] * rays["dir"][hit]
+    out["dir"] = d.astype(np.float32)
+    out["prev_prim"] = hits["prim"][hit]
+    out["prev_t"] = hits["t"][hit]
+    return out, n.astype(np.float32)
+
+
+def sphere_normals_np(rays, hits, centers):
+    """Unit normals at sphere hits (zero for misses): normalize(p - centre)
+    with p = org + t * dir in float32."""
+    nrm = np.zeros((rays.size, 3), np.float32)
+    hit = np.nonzero(hits["prim"] != MISS)[0]
+    p = rays["org"][hit] + hits["t"][hit, None] * rays["dir"][hit]
+    v = (p - centers[hits["prim"][hit]]).astype(np.float64)
+    nrm[hit] = (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
+    return nrm
