@@ -6,21 +6,23 @@
 //        render/render_accel_tetra.cc:973-1030, render/render_accel_particle.cc:304-369
 //   2. Morton codes       morton_kernel
 //        render/render_prefix_tree_util.cc:151-304, render/render_prefix_tree_util.h:113-157
-//   3. stable sort        rs_hist / scan / rs_scatter, 4 x 8-bit LSD passes
+//   3. stable sort        rs_hist / scan / rs_scatter: 3 x 10-bit LSD passes over
+//        the 30-bit codes (4 x 8-bit for full 32-bit keys)
 //        render/render_prefix_tree_util.h:296-457 (stable; ties keep input order)
 //   4. Karras tree        karras_kernel
 //        render/render_prefix_tree_util.cc:501-649
-//   5. bottom-up boxes    refit_kernel (also writes the leaf-ordered primitive
-//        cache used by traversal); union order = the reference's MergeBoundingBox
-//        render/render_accel_triangle.cc:804, ComputeBoundingBox30 :661-709
-//   6. leaf collapse      level_kernel: a Karras node is emitted as a branch iff
+//   5. leaf collapse      level_kernel: a Karras node is emitted as a branch iff
 //        its range holds more than max_leaf+1 keys and its level is <= 23;
 //        both tests are monotone along root paths, so the emitted branches
 //        are exactly the top-down recursion's (BuildTreeRecursive32,
 //        render/render_accel_triangle.cc:896-992; tetra :1113-1243;
 //        particle :521-661)
-//   7. compaction         exclusive scan of the branch flags -> node slots
-//   8. emission           emit_node2_kernel / emit_tet_kernel
+//   6. primitive cache    cache_kernel: leaf-ordered primitives for traversal
+//   7. boxes              refit_kernel over the emitted tree only: leaves by
+//        ComputeBoundingBox30 order (render/render_accel_triangle.cc:661-709),
+//        branches bottom up by MergeBoundingBox, left first (:804)
+//   8. compaction         exclusive scan of the branch flags -> node slots
+//   9. emission           emit_node2_kernel / emit_tet_kernel
 #include <algorithm>
 #include <climits>
 #include <cstdio>
@@ -40,7 +42,7 @@ inline int grid_for(size_t n, int block, int max_blocks) {
 }
 
 // ------------------------------------------------------------------ primitives
-// Leaf-ordered primitive cache (written by refit_kernel, read by traversal):
+// Leaf-ordered primitive cache (written by cache_kernel, read by traversal):
 //   triangles: 3 float4 per prim: (p0, id bits), (p1, 0), (p2, 0)
 //   tetrahedra: 3 float4 per prim: 12 vertex coordinates v0..v3
 //   spheres:   1 float4 per prim: (centre, radius)
@@ -176,9 +178,34 @@ __global__ void bbox_partial_kernel(const float *__restrict__ v,
 template <int KIND>
 __global__ void bbox_final_kernel(const Box *__restrict__ partial, int np,
                                   SceneInfo *__restrict__ scene) {
-  if (threadIdx.x != 0) return;
-  Box r = partial[0];
-  for (int i = 1; i < np; i++) r = box_merge(r, partial[i]);
+  // one warp: lane l merges the l-th contiguous chunk in order, then lanes
+  // merge pairwise with the earlier chunk on the left (first value seen
+  // wins, as in a sequential merge)
+  const int lane = threadIdx.x;
+  const int chunk = (np + 31) / 32;
+  const int b0 = min(np, lane * chunk), b1 = min(np, b0 + chunk);
+  Box r;
+  box_init(r);
+  bool any = b0 < b1;
+  if (any) {
+    r = partial[b0];
+    for (int i = b0 + 1; i < b1; i++) r = box_merge(r, partial[i]);
+  }
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    Box q;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      q.lo[k] = __shfl_down_sync(0xffffffffu, r.lo[k], o);
+      q.hi[k] = __shfl_down_sync(0xffffffffu, r.hi[k], o);
+    }
+    const bool qany = __shfl_down_sync(0xffffffffu, any ? 1 : 0, o) != 0;
+    if ((lane & (2 * o - 1)) == 0 && lane + o < 32 && qany) {
+      r = any ? box_merge(r, q) : q;
+      any = true;
+    }
+  }
+  if (lane != 0) return;
   SceneInfo s;
   for (int k = 0; k < 3; k++) {
     s.lo[k] = r.lo[k];
@@ -347,31 +374,34 @@ srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_
 
 namespace {
 // ------------------------------------------------------------------ 3. radix sort
-constexpr int kRsBits = 8;
-constexpr int kRsBins = 1 << kRsBits;
+// Digits of BITS bits: 10-bit digits sort 30-bit Morton codes in three
+// passes, 8-bit digits cover full 32-bit keys in four (and the scene-id
+// pass of a batched build).
+constexpr int kRsMaxBins = 1 << 10;
 constexpr int kRsWarps = 8;
 constexpr int kRsThreads = kRsWarps * 32;
 constexpr int kRsRounds = 16;
 constexpr int kRsWChunk = 32 * kRsRounds;
 constexpr int kRsTile = kRsWarps * kRsWChunk;
 
-// Sort digit: a byte of the key, or (SEGDIG) the segment of the value --
-// the extra pass that groups a multi-scene sort by scene.
-template <bool SEGDIG>
+// Sort digit: BITS bits of the key from `shift`, or (SEGDIG) the segment of
+// the value -- the extra pass that groups a multi-scene sort by scene.
+template <bool SEGDIG, int BITS>
 __device__ __forceinline__ uint32_t rs_digit(uint32_t k, uint32_t v, int shift,
                                              const uint32_t *__restrict__ seg, int nseg) {
   if (SEGDIG) return (uint32_t)seg_of(seg, nseg, v);
-  return (k >> shift) & (kRsBins - 1);
+  return (k >> shift) & ((1u << BITS) - 1u);
 }
 
 // Per-tile digit histogram, digit-major: hist[d * ntiles + tile].
-template <bool SEGDIG>
+template <bool SEGDIG, int BITS>
 __global__ void __launch_bounds__(kRsThreads)
 rs_hist_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ vals,
                size_t n, int shift, uint32_t *__restrict__ hist, uint32_t ntiles,
                const uint32_t *__restrict__ seg, int nseg) {
-  __shared__ uint32_t wh[kRsWarps][kRsBins];
-  for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads)
+  constexpr int kBins = 1 << BITS;
+  __shared__ uint32_t wh[kRsWarps][kBins];
+  for (int i = threadIdx.x; i < kRsWarps * kBins; i += kRsThreads)
     (&wh[0][0])[i] = 0;
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -381,15 +411,15 @@ rs_hist_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ v
     size_t idx = base + (size_t)r * 32 + lane;
     bool ok = idx < n;
     unsigned valid = __ballot_sync(0xffffffffu, ok);
+    (void)valid;
     if (ok) {
-      uint32_t d = rs_digit<SEGDIG>(keys[idx], SEGDIG ? vals[idx] : 0u, shift, seg, nseg);
-      unsigned peers = __match_any_sync(valid, d);
-      if (lane == __ffs(peers) - 1) wh[w][d] += __popc(peers);
+      const uint32_t d =
+          rs_digit<SEGDIG, BITS>(keys[idx], SEGDIG ? vals[idx] : 0u, shift, seg, nseg);
+      atomicAdd(&wh[w][d], 1u);
     }
-    __syncwarp();
   }
   __syncthreads();
-  for (int d = threadIdx.x; d < kRsBins; d += kRsThreads) {
+  for (int d = threadIdx.x; d < kBins; d += kRsThreads) {
     uint32_t s = 0;
 #pragma unroll
     for (int k = 0; k < kRsWarps; k++) s += wh[k][d];
@@ -399,14 +429,15 @@ rs_hist_kernel(const uint32_t *__restrict__ keys, const uint32_t *__restrict__ v
 
 // Stable scatter of one tile: warps own consecutive chunks, rounds go in key
 // order, lanes within a round are ranked by lane order among equal digits.
-template <bool SEGDIG>
+template <bool SEGDIG, int BITS>
 __global__ void __launch_bounds__(kRsThreads)
 rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__ vin,
                   uint32_t *__restrict__ kout, uint32_t *__restrict__ vout, size_t n,
                   int shift, const uint32_t *__restrict__ offs, uint32_t ntiles,
                   const uint32_t *__restrict__ seg, int nseg) {
-  __shared__ uint32_t wc[kRsWarps][kRsBins];
-  for (int i = threadIdx.x; i < kRsWarps * kRsBins; i += kRsThreads)
+  constexpr int kBins = 1 << BITS;
+  __shared__ uint32_t wc[kRsWarps][kBins];
+  for (int i = threadIdx.x; i < kRsWarps * kBins; i += kRsThreads)
     (&wc[0][0])[i] = 0;
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -424,22 +455,30 @@ rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__
       v[r] = 0;
     }
   }
-  // warp histograms
+  // warp histograms; peers[r] = lanes of round r with this lane's digit
+  // (one ballot per digit bit)
+  uint32_t dg[kRsRounds];
+  unsigned peers[kRsRounds];
 #pragma unroll
   for (int r = 0; r < kRsRounds; r++) {
-    size_t idx = base + (size_t)r * 32 + lane;
-    bool ok = idx < n;
-    unsigned valid = __ballot_sync(0xffffffffu, ok);
-    if (ok) {
-      uint32_t d = rs_digit<SEGDIG>(k[r], v[r], shift, seg, nseg);
-      unsigned peers = __match_any_sync(valid, d);
-      if (lane == __ffs(peers) - 1) wc[w][d] += __popc(peers);
+    const size_t idx = base + (size_t)r * 32 + lane;
+    const bool ok = idx < n;
+    unsigned pm = __ballot_sync(0xffffffffu, ok);
+    const uint32_t d = ok ? rs_digit<SEGDIG, BITS>(k[r], v[r], shift, seg, nseg) : 0u;
+#pragma unroll
+    for (int b = 0; b < BITS; b++) {
+      const bool bit = (d >> b) & 1u;
+      const unsigned m = __ballot_sync(0xffffffffu, bit);
+      pm &= bit ? m : ~m;
     }
+    dg[r] = d;
+    peers[r] = ok ? pm : 0u;
+    if (ok && lane == __ffs(pm) - 1) wc[w][d] += __popc(pm);
     __syncwarp();
   }
   __syncthreads();
   // warp start offsets: global tile offset + counts of earlier warps
-  for (int d = threadIdx.x; d < kRsBins; d += kRsThreads) {
+  for (int d = threadIdx.x; d < kBins; d += kRsThreads) {
     uint32_t run = offs[(size_t)d * ntiles + blockIdx.x];
 #pragma unroll
     for (int q = 0; q < kRsWarps; q++) {
@@ -451,18 +490,15 @@ rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__
   __syncthreads();
 #pragma unroll
   for (int r = 0; r < kRsRounds; r++) {
-    size_t idx = base + (size_t)r * 32 + lane;
-    bool ok = idx < n;
-    unsigned valid = __ballot_sync(0xffffffffu, ok);
-    uint32_t d = ok ? rs_digit<SEGDIG>(k[r], v[r], shift, seg, nseg) : 0u;
-    unsigned peers = ok ? __match_any_sync(valid, d) : 0u;
+    const bool ok = peers[r] != 0u;
+    const uint32_t d = dg[r];
     uint32_t pos = 0;
-    if (ok) pos = wc[w][d] + __popc(peers & lt);
+    if (ok) pos = wc[w][d] + __popc(peers[r] & lt);
     __syncwarp();
     if (ok) {
       kout[pos] = k[r];
       vout[pos] = v[r];
-      if (lane == __ffs(peers) - 1) wc[w][d] += __popc(peers);
+      if (lane == __ffs(peers[r]) - 1) wc[w][d] += __popc(peers[r]);
     }
     __syncwarp();
   }
@@ -470,24 +506,24 @@ rs_scatter_kernel(const uint32_t *__restrict__ kin, const uint32_t *__restrict__
 
 }  // namespace
 
-// One stable counting pass (8-bit key digit, or SEGDIG: segment of the value)
-// from (k0, v0) into (k1, v1).
-template <bool SEGDIG>
+// One stable counting pass (BITS-bit key digit at `shift`, or SEGDIG: segment
+// of the value) from (k0, v0) into (k1, v1).
+template <bool SEGDIG, int BITS>
 static srt_status sort_pass(srt_ctx *ctx, const uint32_t *k0, const uint32_t *v0,
                             uint32_t *k1, uint32_t *v1, size_t n, int shift,
                             const uint32_t *seg, int nseg) {
   cudaStream_t st = ctx->stream;
   const uint32_t ntiles = (uint32_t)((n + kRsTile - 1) / kRsTile);
   uint32_t *hist = ctx->s_hist.as<uint32_t>();
-  rs_hist_kernel<SEGDIG><<<ntiles, kRsThreads, 0, st>>>(k0, v0, n, shift, hist, ntiles, seg,
-                                                        nseg);
+  rs_hist_kernel<SEGDIG, BITS><<<ntiles, kRsThreads, 0, st>>>(k0, v0, n, shift, hist, ntiles,
+                                                              seg, nseg);
   ctx->launches++;
   srt_status s = cuda_status(cudaGetLastError(), "rs_hist");
   if (s != SRT_OK) return s;
-  s = exclusive_scan(ctx, hist, hist, (size_t)kRsBins * ntiles);
+  s = exclusive_scan(ctx, hist, hist, (size_t)(1u << BITS) * ntiles);
   if (s != SRT_OK) return s;
-  rs_scatter_kernel<SEGDIG><<<ntiles, kRsThreads, 0, st>>>(k0, v0, k1, v1, n, shift, hist,
-                                                           ntiles, seg, nseg);
+  rs_scatter_kernel<SEGDIG, BITS><<<ntiles, kRsThreads, 0, st>>>(k0, v0, k1, v1, n, shift,
+                                                                 hist, ntiles, seg, nseg);
   ctx->launches++;
   return cuda_status(cudaGetLastError(), "rs_scatter");
 }
@@ -497,45 +533,52 @@ static srt_status sort_scratch(srt_ctx *ctx, size_t n) {
   cudaError_t e;
   if ((e = ctx->s_keys2.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "sort");
   if ((e = ctx->s_vals2.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "sort");
-  if ((e = ctx->s_hist.ensure((size_t)kRsBins * ntiles * 4)) != cudaSuccess)
+  if ((e = ctx->s_hist.ensure((size_t)kRsMaxBins * ntiles * 4)) != cudaSuccess)
     return cuda_status(e, "sort");
   return SRT_OK;
 }
 
 // Stable LSD sort of (keys, vals) by key; result lands back in keys/vals.
-// identity_vals: vals are 0..n-1 on entry (not read).  With nseg > 1 a
-// fifth pass groups the result by the segment of each value (the segment
-// offsets `seg` are global indices), i.e. the order is (segment, key,
-// value).
+// identity_vals: vals are 0..n-1 on entry (not read).  key_bits <= 30 (Morton
+// codes): three 10-bit passes, otherwise four 8-bit passes; either way the
+// order is the stable order by key.  With nseg > 1 a last pass groups the
+// result by the segment of each value (the segment offsets `seg` are global
+// indices), i.e. the order is (segment, key, value).
 srt_status sort_pairs_seg(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
-                          bool identity_vals, const uint32_t *seg, int nseg) {
+                          bool identity_vals, const uint32_t *seg, int nseg, int key_bits) {
   if (n == 0) return SRT_OK;
   srt_status s = sort_scratch(ctx, n);
   if (s != SRT_OK) return s;
   uint32_t *k0 = keys, *v0 = vals, *k1 = ctx->s_keys2.as<uint32_t>(),
            *v1 = ctx->s_vals2.as<uint32_t>();
-  for (int pass = 0; pass < 4; pass++) {
+  const bool narrow = key_bits <= 30;
+  const int passes = narrow ? 3 : 4;
+  for (int pass = 0; pass < passes; pass++) {
     const uint32_t *vin = (pass == 0 && identity_vals) ? nullptr : v0;
-    s = sort_pass<false>(ctx, k0, vin, k1, v1, n, pass * kRsBits, nullptr, 0);
+    s = narrow ? sort_pass<false, 10>(ctx, k0, vin, k1, v1, n, pass * 10, nullptr, 0)
+               : sort_pass<false, 8>(ctx, k0, vin, k1, v1, n, pass * 8, nullptr, 0);
     if (s != SRT_OK) return s;
     std::swap(k0, k1);
     std::swap(v0, v1);
   }
   if (nseg > 1) {
-    // fifth pass into the scratch, then copy back (keys/vals stay the output)
-    s = sort_pass<true>(ctx, k0, v0, k1, v1, n, 0, seg, nseg);
+    s = sort_pass<true, 8>(ctx, k0, v0, k1, v1, n, 0, seg, nseg);
     if (s != SRT_OK) return s;
-    cudaError_t e = cudaMemcpyAsync(keys, k1, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+    std::swap(k0, k1);
+    std::swap(v0, v1);
+  }
+  if (k0 != keys) {  // an odd number of passes ends in the scratch
+    cudaError_t e = cudaMemcpyAsync(keys, k0, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
     if (e == cudaSuccess)
-      e = cudaMemcpyAsync(vals, v1, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
+      e = cudaMemcpyAsync(vals, v0, n * 4, cudaMemcpyDeviceToDevice, ctx->stream);
     if (e != cudaSuccess) return cuda_status(e, "sort copy");
   }
-  return SRT_OK;  // four passes: data is back in keys/vals
+  return SRT_OK;
 }
 
 srt_status sort_pairs(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
-                      bool identity_vals) {
-  return sort_pairs_seg(ctx, keys, vals, n, identity_vals, nullptr, 1);
+                      bool identity_vals, int key_bits) {
+  return sort_pairs_seg(ctx, keys, vals, n, identity_vals, nullptr, 1, key_bits);
 }
 
 namespace {
@@ -580,95 +623,127 @@ __global__ void karras_kernel(const uint32_t *__restrict__ codes, int n,
     kflags[i] = (uint8_t)((lleaf ? 1 : 0) | (rleaf ? 2 : 0));
     if (krange) krange[i] = make_uint2((uint32_t)lo, (uint32_t)hi);
     if (kparent) {
-      if (lleaf) lparent[g] = (uint32_t)i; else kparent[g] = (uint32_t)i;
-      if (rleaf) lparent[g + 1] = (uint32_t)i; else kparent[g + 1] = (uint32_t)i;
+      if (!lleaf) kparent[g] = (uint32_t)i;
+      else if (lparent) lparent[g] = (uint32_t)i;
+      if (!rleaf) kparent[g + 1] = (uint32_t)i;
+      else if (lparent) lparent[g + 1] = (uint32_t)i;
       if (i == 0) kparent[0] = kNone;
     }
   }
 }
 
 // ------------------------------------------------------------------ 5. refit
-// Thread per sorted position j: write the primitive cache entry, then climb
-// while this thread is the second child to finish (atomic counter per node).
+// Leaf-ordered primitive cache: thread per sorted position j gathers the
+// primitive's vertices (or centre and radius) once.
 template <int KIND>
-__global__ void refit_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f,
+__global__ void cache_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f,
                              const float *__restrict__ radius, float constr,
                              const uint32_t *__restrict__ sidx, int n,
-                             const SceneInfo *__restrict__ scene,
-                             const uint32_t *__restrict__ lparent,
-                             const uint32_t *__restrict__ kparent,
-                             const uint32_t *__restrict__ kchild,
-                             const uint8_t *__restrict__ kflags,
-                             uint32_t *__restrict__ counter, Box *__restrict__ ibox,
-                             float4 *__restrict__ prims, uint32_t *__restrict__ err) {
-  int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n) return;
-  const float keps = scene->keps;
-  uint32_t p = sidx[j];
-  Box mine;
-  box_init(mine);
-  if (KIND == SRT_TRIANGLES) {
-    size_t a = f[3 * (size_t)p], b = f[3 * (size_t)p + 1], c = f[3 * (size_t)p + 2];
-    float4 p0 = make_float4(v[3 * a], v[3 * a + 1], v[3 * a + 2], __uint_as_float(p));
-    float4 p1 = make_float4(v[3 * b], v[3 * b + 1], v[3 * b + 2], 0.0f);
-    float4 p2 = make_float4(v[3 * c], v[3 * c + 1], v[3 * c + 2], 0.0f);
-    prims[3 * (size_t)j + 0] = p0;
-    prims[3 * (size_t)j + 1] = p1;
-    prims[3 * (size_t)j + 2] = p2;
-    box_add(mine, p0.x, p0.y, p0.z, keps);
-    box_add(mine, p1.x, p1.y, p1.z, keps);
-    box_add(mine, p2.x, p2.y, p2.z, keps);
-  } else if (KIND == SRT_TETRAHEDRA) {
-    size_t q[4];
+                             float4 *__restrict__ prims) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t p = sidx[j];
+    if (KIND == SRT_TRIANGLES) {
+      const size_t a = f[3 * (size_t)p], b = f[3 * (size_t)p + 1], c = f[3 * (size_t)p + 2];
+      prims[3 * (size_t)j + 0] = make_float4(v[3 * a], v[3 * a + 1], v[3 * a + 2],
+                                             __uint_as_float(p));
+      prims[3 * (size_t)j + 1] = make_float4(v[3 * b], v[3 * b + 1], v[3 * b + 2], 0.0f);
+      prims[3 * (size_t)j + 2] = make_float4(v[3 * c], v[3 * c + 1], v[3 * c + 2], 0.0f);
+    } else if (KIND == SRT_TETRAHEDRA) {
+      float x[12];
 #pragma unroll
-    for (int c = 0; c < 4; c++) q[c] = f[4 * (size_t)p + c];
-    float x[12];
-#pragma unroll
-    for (int c = 0; c < 4; c++) {
-      x[3 * c] = v[3 * q[c]];
-      x[3 * c + 1] = v[3 * q[c] + 1];
-      x[3 * c + 2] = v[3 * q[c] + 2];
-      box_add(mine, x[3 * c], x[3 * c + 1], x[3 * c + 2], keps);
-    }
-    prims[3 * (size_t)j + 0] = make_float4(x[0], x[1], x[2], x[3]);
-    prims[3 * (size_t)j + 1] = make_float4(x[4], x[5], x[6], x[7]);
-    prims[3 * (size_t)j + 2] = make_float4(x[8], x[9], x[10], x[11]);
-  } else {
-    float r = radius ? radius[p] : constr;
-    float4 s = make_float4(v[3 * (size_t)p], v[3 * (size_t)p + 1], v[3 * (size_t)p + 2], r);
-    prims[j] = s;
-    mine.lo[0] = (s.x - r) - keps; mine.lo[1] = (s.y - r) - keps; mine.lo[2] = (s.z - r) - keps;
-    mine.hi[0] = (s.x + r) + keps; mine.hi[1] = (s.y + r) + keps; mine.hi[2] = (s.z + r) + keps;
-  }
-  uint32_t cur = (uint32_t)j;
-  bool cur_leaf = true;
-  uint32_t node = lparent[j];
-  for (int guard = 0; guard < 2 * n + 64; guard++) {
-    __threadfence();
-    uint32_t old = atomicAdd(&counter[node], 1u);
-    if (old == 0) return;  // sibling still pending; it will continue
-    __threadfence();
-    uint32_t g = __ldcg(&kchild[node]);
-    uint8_t fl = __ldcg(&kflags[node]);
-    bool lleaf = fl & 1, rleaf = fl & 2;
-    bool i_am_left = (cur == g) && (cur_leaf == lleaf);
-    uint32_t sib = i_am_left ? g + 1 : g;
-    bool sib_leaf = i_am_left ? rleaf : lleaf;
-    Box sb;
-    if (sib_leaf) {
-      sb = cache_box<KIND>(prims, sib, keps);
+      for (int c = 0; c < 4; c++) {
+        const size_t q = f[4 * (size_t)p + c];
+        x[3 * c] = v[3 * q];
+        x[3 * c + 1] = v[3 * q + 1];
+        x[3 * c + 2] = v[3 * q + 2];
+      }
+      prims[3 * (size_t)j + 0] = make_float4(x[0], x[1], x[2], x[3]);
+      prims[3 * (size_t)j + 1] = make_float4(x[4], x[5], x[6], x[7]);
+      prims[3 * (size_t)j + 2] = make_float4(x[8], x[9], x[10], x[11]);
     } else {
-      const float *src = reinterpret_cast<const float *>(&ibox[sib]);
-      sb.lo[0] = __ldcg(src + 0); sb.lo[1] = __ldcg(src + 1); sb.lo[2] = __ldcg(src + 2);
-      sb.hi[0] = __ldcg(src + 3); sb.hi[1] = __ldcg(src + 4); sb.hi[2] = __ldcg(src + 5);
+      const float r = radius ? radius[p] : constr;
+      prims[j] = make_float4(v[3 * (size_t)p], v[3 * (size_t)p + 1], v[3 * (size_t)p + 2], r);
     }
-    mine = i_am_left ? box_merge(mine, sb) : box_merge(sb, mine);
-    ibox[node] = mine;
+  }
+}
+
+// Box of the sorted primitive range [lo, hi] in order -- ComputeBoundingBox30
+// (render/render_accel_triangle.cc:661-709): the first value seen wins ties,
+// as the left-first merges of MergeBoundingBox do.
+template <int KIND>
+__device__ __forceinline__ Box range_box(const float4 *__restrict__ prims, uint32_t lo,
+                                         uint32_t hi, float keps) {
+  Box b = cache_box<KIND>(prims, lo, keps);
+  for (uint32_t j = lo + 1; j <= hi; j++) b = box_merge(b, cache_box<KIND>(prims, j, keps));
+  return b;
+}
+
+// Box of child `c` (kleaf: Karras leaf = one sorted primitive; else Karras
+// internal node whose box is in ibox).
+template <int KIND>
+__device__ __forceinline__ Box child_box(const float4 *__restrict__ prims,
+                                         const Box *__restrict__ ibox, uint32_t c, bool kleaf,
+                                         float keps) {
+  if (kleaf) return cache_box<KIND>(prims, c, keps);
+  Box b;
+  const float *src = reinterpret_cast<const float *>(&ibox[c]);
+  b.lo[0] = __ldcg(src + 0); b.lo[1] = __ldcg(src + 1); b.lo[2] = __ldcg(src + 2);
+  b.hi[0] = __ldcg(src + 3); b.hi[1] = __ldcg(src + 4); b.hi[2] = __ldcg(src + 5);
+  return b;
+}
+
+// Boxes of the emitted tree only.  Thread per Karras internal node i that is
+// emitted as a branch (flag[i]): children that become leaves of the emitted
+// tree get their box here -- a Karras leaf from the cache, a collapsed
+// subtree c by range_box into ibox[c] -- and branch boxes are merged bottom
+// up, left first, by the second of the two children to finish (atomic
+// counter per node).  Ancestors of an emitted branch are emitted branches.
+template <int KIND>
+__global__ void refit_kernel(const uint32_t *__restrict__ kchild,
+                             const uint8_t *__restrict__ kflags,
+                             const uint2 *__restrict__ krange,
+                             const uint32_t *__restrict__ kparent,
+                             const uint32_t *__restrict__ flag, int n,
+                             const SceneInfo *__restrict__ scene,
+                             const float4 *__restrict__ prims, uint32_t *__restrict__ counter,
+                             Box *__restrict__ ibox, uint32_t *__restrict__ err) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n - 1 || !flag[i]) return;
+  const float keps = scene->keps;
+  const uint32_t g = kchild[i];
+  const uint8_t fl = kflags[i];
+  bool leafside[2];
+#pragma unroll
+  for (int side = 0; side < 2; side++) {
+    const uint32_t c = g + side;
+    const bool kleaf = fl & (1 << side);
+    leafside[side] = kleaf || !flag[c];
+    if (!kleaf && !flag[c]) {  // collapsed subtree: one emitted leaf
+      const uint2 r = krange[c];
+      ibox[c] = range_box<KIND>(prims, r.x, r.y, keps);
+    }
+  }
+  uint32_t node = (uint32_t)i;
+  if (!(leafside[0] && leafside[1])) {
+    if (!leafside[0] && !leafside[1]) return;  // two branch children climb here
+    __threadfence();
+    if (atomicAdd(&counter[node], 1u) == 0) return;  // the branch child merges
+    __threadfence();
+  }
+  // this thread completes `node` (both children's boxes are written) and
+  // climbs while it is the second arrival
+  for (int guard = 0; guard < 64; guard++) {
+    const uint32_t gl = __ldcg(&kchild[node]);
+    const uint8_t f2 = __ldcg(&kflags[node]);
+    const Box bl = child_box<KIND>(prims, ibox, gl, f2 & 1, keps);
+    const Box br = child_box<KIND>(prims, ibox, gl + 1, f2 & 2, keps);
+    ibox[node] = box_merge(bl, br);
     if (node == 0) return;
-    cur = node;
-    cur_leaf = false;
     node = __ldcg(&kparent[node]);
     if (node == kNone) return;
+    __threadfence();
+    if (atomicAdd(&counter[node], 1u) == 0) return;
+    __threadfence();
   }
   atomicOr(err, kErrTree);
 }
@@ -855,7 +930,6 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
   ENSURE(ctx->s_kflags, m);
   ENSURE(ctx->s_krange, m * sizeof(uint2));
   ENSURE(ctx->s_kparent, m * 4);
-  ENSURE(ctx->s_lparent, n * 4);
   ENSURE(ctx->s_counter, m * 4);
   ENSURE(ctx->s_ibox, m * sizeof(Box));
   ENSURE(ctx->s_flag, m * 4);
@@ -866,30 +940,30 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
   uint32_t *idx = a->indices.as<uint32_t>();
   srt_status s = launch_bbox_morton<KIND>(ctx, v, f, radius, constr, n, scene, codes, nullptr);
   if (s != SRT_OK) return s;
-  s = sort_pairs(ctx, codes, idx, n, true);
+  s = sort_pairs(ctx, codes, idx, n, true, 30);  // 30-bit Morton codes
   if (s != SRT_OK) return s;
   uint32_t *kchild = ctx->s_kchild.as<uint32_t>();
   uint8_t *kflags = ctx->s_kflags.as<uint8_t>();
   uint2 *krange = ctx->s_krange.as<uint2>();
   uint32_t *kparent = ctx->s_kparent.as<uint32_t>();
-  uint32_t *lparent = ctx->s_lparent.as<uint32_t>();
   uint32_t *counter = ctx->s_counter.as<uint32_t>();
   Box *ibox = ctx->s_ibox.as<Box>();
   uint32_t *flag = ctx->s_flag.as<uint32_t>();
   uint32_t *slot = ctx->s_slot.as<uint32_t>();
   int gk = grid_for(m, kBlock, ctx->num_sms * 16);
-  karras_kernel<<<gk, kBlock, 0, st>>>(codes, in, kchild, kflags, krange, kparent, lparent);
+  karras_kernel<<<gk, kBlock, 0, st>>>(codes, in, kchild, kflags, krange, kparent, nullptr);
   ctx->launches++;
   if ((e = cudaMemsetAsync(counter, 0, m * 4, st)) != cudaSuccess)
     return cuda_status(e, "refit counters");
-  refit_kernel<KIND><<<(unsigned)((n + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-      v, f, radius, constr, idx, in, scene, lparent, kparent, kchild, kflags, counter,
-      ibox, a->prims.as<float4>(), ctx->d_err);
-  ctx->launches++;
   level_kernel<<<gk, kBlock, 0, st>>>(krange, kparent, in, PrimTraits<KIND>::kMaxLeaf,
                                       flag);
-  ctx->launches++;
-  s = cuda_status(cudaGetLastError(), "karras/refit/level");
+  cache_kernel<KIND><<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, st>>>(
+      v, f, radius, constr, idx, in, a->prims.as<float4>());
+  refit_kernel<KIND><<<(unsigned)((m + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+      kchild, kflags, krange, kparent, flag, in, scene, a->prims.as<float4>(), counter, ibox,
+      ctx->d_err);
+  ctx->launches += 3;
+  s = cuda_status(cudaGetLastError(), "karras/level/cache/refit");
   if (s != SRT_OK) return s;
   s = exclusive_scan(ctx, flag, slot, m);
   if (s != SRT_OK) return s;
@@ -1268,7 +1342,7 @@ srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32
   if (s != SRT_OK) return s;
   {
     size_t need = 64;
-    for (size_t t = ((size_t)kRsBins * ((N + kRsTile - 1) / kRsTile) + kScanTile - 1) / kScanTile;
+    for (size_t t = ((size_t)kRsMaxBins * ((N + kRsTile - 1) / kRsTile) + kScanTile - 1) / kScanTile;
          t > 1; t = (t + kScanTile - 1) / kScanTile)
       need += t + 1;
     for (size_t t = (M + kScanTile - 1) / kScanTile; t > 1; t = (t + kScanTile - 1) / kScanTile)
@@ -1290,7 +1364,7 @@ srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32
   ctx->launches += 4;
   s = cuda_status(cudaGetLastError(), "batch bbox/morton");
   if (s != SRT_OK) return s;
-  s = sort_pairs_seg(ctx, codes, idx, N, true, foff, nseg);
+  s = sort_pairs_seg(ctx, codes, idx, N, true, foff, nseg, 30);
   if (s != SRT_OK) return s;
   uint32_t *kchild = ctx->s_kchild.as<uint32_t>();
   uint8_t *kflags = ctx->s_kflags.as<uint8_t>();

@@ -178,8 +178,10 @@ srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *d_verts,
                         SceneInfo *d_scene);
 // Exclusive prefix sum of n uint32 on the context's stream (out may alias in).
 srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n);
+// Stable sort of (key, value) pairs by key; key_bits: how many low bits of
+// the keys can be non-zero (30 for Morton codes).
 srt_status sort_pairs(srt_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals,
-                      size_t n, bool identity_vals);
+                      size_t n, bool identity_vals, int key_bits = 32);
 srt_status stage_karras(srt_ctx *ctx, const uint32_t *d_codes, size_t n,
                         uint32_t *d_child, uint8_t *d_flags);
 srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32_t *f,
