@@ -115,6 +115,11 @@ typedef struct srt_trace_opts {
  * front to back and replays the reference's order only to break exact
  * ties.  Both give identical hits; the default does far less work. */
 #define SRT_TRACE_SINGLE_PASS 1u
+/* Trace the rays in a coherent order (a Morton curve over origin and
+ * direction, sorted on the GPU) instead of array order: fewer divergent warps
+ * on large ray sets at the cost of the sort.  Hits are identical and are
+ * written at each ray's own index. */
+#define SRT_TRACE_SORT_RAYS 2u
 
 typedef struct srt_ctx srt_ctx;
 typedef struct srt_accel srt_accel;

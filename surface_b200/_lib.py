@@ -18,6 +18,7 @@ SRT_OK, SRT_ERR_INVALID, SRT_ERR_CUDA, SRT_ERR_NO_MEMORY, SRT_ERR_LIMIT, SRT_ERR
 SRT_TRIANGLES, SRT_TETRAHEDRA, SRT_SPHERES = 0, 1, 2
 MISS = 0xFFFFFFFF
 SRT_TRACE_SINGLE_PASS = 1
+SRT_TRACE_SORT_RAYS = 2
 
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
                       ("prev_t", "<f4")])

@@ -220,11 +220,12 @@ class _Accel:
     # -- traversal --------------------------------------------------------
     def Traverse(self, rays, hits=None, prev_normals=None, want_subface=False,
                  vertex_scalar=None, want_scalar=False, want_normal=False,
-                 single_pass=False):
+                 single_pass=False, sort_rays=False):
         """Closest hit for every ray (batched XxxAccel::Traverse).
 
         single_pass=True walks the tree once in the reference's own order;
-        the default two-pass walk returns the same hits with less work."""
+        the default two-pass walk returns the same hits with less work.
+        sort_rays=True traverses in a coherent ray order (same hits)."""
         if not self.built:
             raise SurfaceError(_lib.SRT_ERR_INVALID, "accel not built")
         cuda = _is_cuda(rays)
@@ -262,7 +263,8 @@ class _Accel:
         o = TraceOpts(pn.ptr, _View(sub, np.uint32).ptr if sub is not None else None,
                       vs.ptr, _View(sca, np.float32).ptr if sca is not None else None,
                       _View(nrm, np.float32).ptr if nrm is not None else None, None,
-                      _lib.SRT_TRACE_SINGLE_PASS if single_pass else 0, 0)
+                      (_lib.SRT_TRACE_SINGLE_PASS if single_pass else 0)
+                      | (_lib.SRT_TRACE_SORT_RAYS if sort_rays else 0), 0)
         check(self.L.srt_trace_closest(self.h, rv.ptr, n, hv.ptr, C.byref(o)))
         if not (want_subface or want_scalar or want_normal):
             return hits

@@ -205,7 +205,8 @@ SRT_API srt_status srt_ctx_destroy(srt_ctx *c) {
                     &c->s_kflags, &c->s_krange, &c->s_kparent, &c->s_lparent,
                     &c->s_counter, &c->s_ibox, &c->s_flag, &c->s_slot, &c->s_partial,
                     &c->s_stage_in, &c->s_stage_out, &c->s_stage_aux, &c->s_stage_sub,
-                    &c->s_stage_scal, &c->s_stage_norm, &c->s_defer, &c->s_spawn};
+                    &c->s_stage_scal, &c->s_stage_norm, &c->s_defer, &c->s_spawn, &c->s_rkey,
+                    &c->s_rorder};
   for (DevBuf *b : bufs) b->release();
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);
@@ -592,8 +593,9 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
     // Page-locked host rays and hits: the kernels read the rays and write the
     // hits over the host link while they traverse, so the transfers overlap
     // the traversal instead of preceding and following it.
+    // (a sorted trace reads the rays three times: those are staged instead)
     void *mr = mapped_host(rays), *mh = mapped_host(hits);
-    if (mr && mh) {
+    if (mr && mh && !(o.flags & SRT_TRACE_SORT_RAYS)) {
       bool ok = true;
       void *pn = direct_view(o.prev_normals, ok), *sub = direct_view(o.subface, ok);
       void *scal = direct_view(o.scalar_out, ok), *norm = direct_view(o.normal_out, ok);

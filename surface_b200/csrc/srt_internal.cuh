@@ -136,7 +136,7 @@ struct srt_ctx {
   srt::DevBuf s_keys2, s_vals2, s_hist, s_scan, s_kchild, s_kflags, s_krange,
       s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
       s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm,
-      s_defer, s_spawn;
+      s_defer, s_spawn, s_rkey, s_rorder;
 };
 
 struct srt_accel {
@@ -176,6 +176,9 @@ srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *d_verts,
                         const uint32_t *d_faces, const float *d_radius,
                         float const_radius, size_t n, uint32_t *d_codes,
                         SceneInfo *d_scene);
+// Coherent traversal order of n rays (srt_raysort.cu): *order is a device
+// array in context scratch, valid until the context's next sort.
+srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);
 // Exclusive prefix sum of n uint32 on the context's stream (out may alias in).
 srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n);
 // Stable sort of (key, value) pairs by key; key_bits: how many low bits of

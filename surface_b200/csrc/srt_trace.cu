@@ -676,9 +676,10 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
                    const float *__restrict__ prev_normals, float *__restrict__ normal_out,
                    unsigned long long *__restrict__ stats, Deferred *__restrict__ dlist,
                    uint32_t *__restrict__ dcount, uint32_t max_iter,
-                   uint32_t *__restrict__ err) {
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                   uint32_t *__restrict__ err, const uint32_t *__restrict__ order) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
   const Ctx2 c = make_ctx2<KIND>(rays, i, scene, prev_normals);
   Work w;
   Best b;
@@ -859,9 +860,11 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
                  const uint32_t *__restrict__ faces, const float *__restrict__ vscalar,
                  float *__restrict__ scalar_out, unsigned long long *__restrict__ stats,
                  Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
-                 uint32_t max_iter, uint32_t *__restrict__ err) {
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                 uint32_t max_iter, uint32_t *__restrict__ err,
+                 const uint32_t *__restrict__ order) {
+  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
   const CtxT c = make_ctxT(rays, i);
   Work w;
   Best b;
@@ -1095,6 +1098,11 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
       return cuda_status(e, "deferred count");
   }
   const float *pn = a->kind == SRT_SPHERES ? prev_normals : nullptr;
+  const uint32_t *order = nullptr;
+  if (flags & SRT_TRACE_SORT_RAYS) {
+    srt_status s = ray_order(ctx, rays, n, &order);
+    if (s != SRT_OK) return s;
+  }
   switch (a->kind) {
     case SRT_TRIANGLES:
     case SRT_SPHERES: {
@@ -1105,11 +1113,11 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
         if (single)
           trace_node2_kernel<SRT_TRIANGLES, true><<<grid, block, 0, st>>>(
               nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, nullptr, nullptr,
-              max_iter, ctx->d_err);
+              max_iter, ctx->d_err, order);
         else {
           trace_node2_kernel<SRT_TRIANGLES, false><<<grid, block, 0, st>>>(
               nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount,
-              max_iter, ctx->d_err);
+              max_iter, ctx->d_err, order);
           resolve_node2_kernel<SRT_TRIANGLES><<<rgrid, block, 0, st>>>(
               nd, pr, ix, rays, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
               ctx->d_err);
@@ -1119,11 +1127,11 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
         if (single)
           trace_node2_kernel<SRT_SPHERES, true><<<grid, block, 0, st>>>(
               nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, nullptr, nullptr,
-              max_iter, ctx->d_err);
+              max_iter, ctx->d_err, order);
         else {
           trace_node2_kernel<SRT_SPHERES, false><<<grid, block, 0, st>>>(
               nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount,
-              max_iter, ctx->d_err);
+              max_iter, ctx->d_err, order);
           resolve_node2_kernel<SRT_SPHERES><<<rgrid, block, 0, st>>>(
               nd, pr, ix, rays, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
               ctx->d_err);
@@ -1140,12 +1148,12 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
         trace_tet_kernel<true><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
                                                        a->src_faces, vscalar, scalar_out,
                                                        stats, nullptr, nullptr, max_iter,
-                                                       ctx->d_err);
+                                                       ctx->d_err, order);
       else {
         trace_tet_kernel<false><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
                                                         a->src_faces, vscalar, scalar_out,
                                                         stats, dlist, dcount, max_iter,
-                                                        ctx->d_err);
+                                                        ctx->d_err, order);
         resolve_tet_kernel<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, subface,
                                                     a->src_faces, vscalar, scalar_out,
                                                     stats, dlist, dcount, max_iter,
@@ -1288,7 +1296,7 @@ extern "C" SRT_API srt_status srt_trace_closest_noalloc(srt_accel *a, const srt_
       const Node2 *nd = a->nodes.as<Node2>();
       trace_node2_kernel<SRT_TRIANGLES, false><<<grid, block, 0, st>>>(
           nd, pr, ix, rays, n, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
-          ctx->d_err);
+          ctx->d_err, nullptr);
       resolve_node2_kernel<SRT_TRIANGLES><<<rgrid, block, 0, st>>>(
           nd, pr, ix, rays, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
           ctx->d_err);
@@ -1298,7 +1306,7 @@ extern "C" SRT_API srt_status srt_trace_closest_noalloc(srt_accel *a, const srt_
       const Node2 *nd = a->nodes.as<Node2>();
       trace_node2_kernel<SRT_SPHERES, false><<<grid, block, 0, st>>>(
           nd, pr, ix, rays, n, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
-          ctx->d_err);
+          ctx->d_err, nullptr);
       resolve_node2_kernel<SRT_SPHERES><<<rgrid, block, 0, st>>>(
           nd, pr, ix, rays, hits, scene, nullptr, nullptr, nullptr, dlist, dcount, max_iter,
           ctx->d_err);
@@ -1308,7 +1316,7 @@ extern "C" SRT_API srt_status srt_trace_closest_noalloc(srt_accel *a, const srt_
       const NodeT *nd = a->nodes.as<NodeT>();
       trace_tet_kernel<false><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, nullptr,
                                                       a->src_faces, nullptr, nullptr, nullptr,
-                                                      dlist, dcount, max_iter, ctx->d_err);
+                                                      dlist, dcount, max_iter, ctx->d_err, nullptr);
       resolve_tet_kernel<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, nullptr, a->src_faces,
                                                   nullptr, nullptr, nullptr, dlist, dcount,
                                                   max_iter, ctx->d_err);

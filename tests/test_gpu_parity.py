@@ -45,15 +45,21 @@ def assert_hits_equal(h, ref, fields=("t", "u", "v", "prim")):
 
 
 def trace_both(acc, rays, **kw):
-    """Trace with the default two-pass walk and the single-pass walk in the
-    reference's order; both must agree bit for bit.  Returns the first."""
+    """Trace with the default two-pass walk, the single-pass walk in the
+    reference's order and the default walk in sorted ray order; all must
+    agree bit for bit.  Returns the first."""
     a = acc.Traverse(rays, **kw)
-    b = acc.Traverse(rays, single_pass=True, **kw)
-    ha = a.hits if hasattr(a, "hits") else a
-    hb = b.hits if hasattr(b, "hits") else b
-    assert_hits_equal(ha, hb)
-    if hasattr(a, "subface") and a.subface is not None:
-        assert np.array_equal(a.subface, b.subface)
+    for other in (acc.Traverse(rays, single_pass=True, **kw),
+                  acc.Traverse(rays, sort_rays=True, **kw)):
+        ha = a.hits if hasattr(a, "hits") else a
+        hb = other.hits if hasattr(other, "hits") else other
+        assert_hits_equal(ha, hb)
+        if hasattr(a, "subface") and a.subface is not None:
+            assert np.array_equal(a.subface, other.subface)
+        if hasattr(a, "scalar") and a.scalar is not None:
+            assert np.array_equal(bits(a.scalar), bits(other.scalar))
+        if hasattr(a, "normal") and a.normal is not None:
+            assert np.array_equal(bits(a.normal), bits(other.normal))
     return a
 
 
