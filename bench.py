@@ -386,6 +386,24 @@ DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 di
          "volume": "f32", "batched": "f32"}
 
 
+def volume_sample_count(p):
+    """Samples the march takes: floor((t1 - t0) / step) per pixel ray through
+    the [-1, 1]^3 slab (the kernel's camera and slab test, in float64)."""
+    W, H = int(p["width"][0]), int(p["height"][0])
+    px, py = np.meshgrid(np.arange(W) + 0.5, np.arange(H) + 0.5)
+    v = (p["corner"][0][None, None, :] + px[..., None] * p["du"][0] + py[..., None] * p["dv"][0]
+         - p["eye"][0])
+    d = v / np.linalg.norm(v, axis=-1, keepdims=True)
+    o = p["eye"][0].astype(np.float64)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        tn = (-1.0 - o) / d
+        tf = (1.0 - o) / d
+    t0 = np.maximum(np.minimum(tn, tf).max(-1), -10000.0)
+    t1 = np.minimum(np.maximum(tn, tf).min(-1), 10000.0)
+    ns = np.where(t0 <= t1, np.floor((t1 - t0) / float(p["step"][0])), 0)
+    return float(np.minimum(ns, int(p["max_steps"][0])).sum())
+
+
 def run_volume(args, W):
     """Forward + adjoint of the L2 loss per step (device resident); forward
     alone is timed too.  CPU baseline: the FP32 oracle forward (OpenMP)."""
@@ -410,6 +428,10 @@ def run_volume(args, W):
         img, tr = V.march(dens, tf, p)
         return V.march_backward(dens, tf, p, tr, 2 * (img - target))
 
+    from surface_b200 import _lib
+    from surface_b200.accel import Context
+    L = _lib.load()
+    vctx = Context.default(dev.index)
     for _ in range(max(args.warmup, 3)):
         fwd_bwd()
     torch.cuda.synchronize()
@@ -419,6 +441,7 @@ def run_volume(args, W):
           for _ in range(args.steps)]
     with ClockSampler(dev.index) as clk:
         clk.keep_busy(fwd_bwd, torch.cuda.synchronize)
+        launches0 = L.srt_ctx_launch_count(vctx.h)
         for k in range(args.steps):
             flush.zero_()
             fe[k][0].record()
@@ -429,10 +452,56 @@ def run_volume(args, W):
             fwd_bwd()
             ev[k][1].record()
         torch.cuda.synchronize()
+        launches = L.srt_ctx_launch_count(vctx.h) - launches0
         clk.keep_busy(fwd_bwd, torch.cuda.synchronize, extra=1)
     fb_ms, f_ms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in ev),
                                   statistics.mean(a.elapsed_time(b) for a, b in fe)], dev)
     nr = 512 * 512
+
+    # ---- e2e: density and table copied in from pinned host memory, both
+    # gradients copied back, every step
+    h_dens = torch.from_numpy(np.ascontiguousarray(W["dens"])).pin_memory()
+    h_tf = torch.from_numpy(np.ascontiguousarray(W["tf"])).pin_memory()
+    h_gd = torch.empty_like(h_dens).pin_memory()
+    h_gt = torch.empty_like(h_tf).pin_memory()
+
+    def e2e_step():
+        dens.copy_(h_dens, non_blocking=True)
+        tf.copy_(h_tf, non_blocking=True)
+        gd, gt = fwd_bwd()
+        h_gd.copy_(gd, non_blocking=True)
+        h_gt.copy_(gt, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e = {"value": round(whole_job_mrays(nr, world, e2e_ms), 3), "unit": "Mrays/s",
+           "h2d_bytes_per_step": int((h_dens.numel() + h_tf.numel()) * 4),
+           "d2h_bytes_per_step": int((h_gd.numel() + h_gt.numel()) * 4),
+           "ms_per_step": round(e2e_ms, 3)}
+
+    # ---- roofline of the adjoint kernel (the larger of the two): unique
+    # bytes it must move -- density read, density gradient written, image-
+    # sized inputs -- against HBM; the samples' trilinear gathers (32 B each)
+    # are served by L1/L2 and reported beside it
+    hbm, src = peaks()
+    nsamp = volume_sample_count(p)
+    bwd_ms = fb_ms - f_ms
+    uniq = 2 * W["dens"].nbytes + nr * (16 + 4 + 16) + 2 * W["tf"].nbytes
+    roofline = {"bound": "hbm", "kernel": "vol_bwd_kernel (fwd+bwd minus fwd)",
+                "achieved": round(uniq / (bwd_ms * 1e-3) / 1e9, 1), "peak": hbm,
+                "unit": "GB/s", "frac": round(uniq / (bwd_ms * 1e-3) / 1e9 / hbm, 4),
+                "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_launch": int(uniq), "samples": int(nsamp),
+                "sample_gather_gbs": round(32 * nsamp / (bwd_ms * 1e-3) / 1e9, 1)}
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         from oracle import oracle as O
@@ -453,6 +522,7 @@ def run_volume(args, W):
             "config": dict(W["config"], l2="flushed between steps (256 MiB write)"),
             "forward_ms": round(f_ms, 4), "forward_backward_ms": round(fb_ms, 4),
             "fwd_bwd_over_fwd": round(fb_ms / f_ms, 3), "clocks": clk.summary(),
+            "e2e": e2e, "gpu_launches": int(launches), "roofline": roofline,
             "cpu_baseline": cpu}
     if rank == 0:
         print(json.dumps(line), flush=True)
@@ -536,13 +606,13 @@ def run_batched(args, W):
     torch.cuda.synchronize()
     stats = st.cpu().numpy().astype(np.float64)[:3]
 
-    l_b0 = tb.launches()
-    l_l0 = L.srt_ctx_launch_count(ctx.h)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         clk.keep_busy(batch_step, torch.cuda.synchronize)
+        l_b0 = tb.launches()
+        l_l0 = L.srt_ctx_launch_count(ctx.h)
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record()
@@ -553,10 +623,10 @@ def run_batched(args, W):
             loop_step()
             ev[k][3].record()
         torch.cuda.synchronize()
+        launches = tb.launches() - l_b0
+        loop_launches = L.srt_ctx_launch_count(ctx.h) - l_l0
         clk.keep_busy(batch_step, torch.cuda.synchronize, extra=1)
     barrier()
-    launches = tb.launches() - l_b0
-    loop_launches = L.srt_ctx_launch_count(ctx.h) - l_l0
     b_ms = [e[0].elapsed_time(e[1]) for e in ev]
     l_ms = [e[2].elapsed_time(e[3]) for e in ev]
     tb_tot, tl_tot = max_over_ranks([sum(b_ms), sum(l_ms)], dev)
@@ -715,13 +785,13 @@ def run_particles(args, W):
     stats = stats_all[:3]
     sec0 = secondaries(0)
 
-    launches0 = L.srt_ctx_launch_count(ctx.h)
     ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
     nsec = []
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         clk.keep_busy(step, torch.cuda.synchronize)
+        launches0 = L.srt_ctx_launch_count(ctx.h)
         for k in range(args.steps):
             flush.zero_()
             ev[k][0].record()
@@ -732,9 +802,9 @@ def run_particles(args, W):
             nsec.append(secondaries(k))
             ev[k][3].record()
         torch.cuda.synchronize()
+        launches = L.srt_ctx_launch_count(ctx.h) - launches0
         clk.keep_busy(step, torch.cuda.synchronize, extra=1)
     barrier()
-    launches = L.srt_ctx_launch_count(ctx.h) - launches0
     b_ms = [e[0].elapsed_time(e[1]) for e in ev]
     p_ms = [e[1].elapsed_time(e[2]) for e in ev]
     s_ms = [e[2].elapsed_time(e[3]) for e in ev]
@@ -882,13 +952,13 @@ def run_ours(args, W):
     stats_all = st.cpu().numpy().astype(np.float64)
     stats = stats_all[:3]
 
-    launches0 = L.srt_ctx_launch_count(ctx.h)
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
            torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
     barrier()
     torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         clk.keep_busy(step, torch.cuda.synchronize)
+        launches0 = L.srt_ctx_launch_count(ctx.h)
         for k in range(args.steps):
             flush.zero_()
             e0, e1, e2 = ev[k]
@@ -898,9 +968,9 @@ def run_ours(args, W):
             trace()
             e2.record()
         torch.cuda.synchronize()
+        launches = L.srt_ctx_launch_count(ctx.h) - launches0
         clk.keep_busy(step, torch.cuda.synchronize, extra=1)
     barrier()
-    launches = L.srt_ctx_launch_count(ctx.h) - launches0
     build_ms = [e[0].elapsed_time(e[1]) for e in ev]
     trace_ms = [e[1].elapsed_time(e[2]) for e in ev]
     total_ms = max_over_ranks([sum(b + t for b, t in zip(build_ms, trace_ms))], dev)[0]

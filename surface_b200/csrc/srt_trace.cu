@@ -988,8 +988,8 @@ resolve_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ p
 }
 
 // --------------------------------------------------------------- batches
-// All rays of many triangle scenes in one persistent launch: each block
-// takes the next blockDim.x * R rays from a global counter (scenes of very
+// All rays of many triangle scenes in one persistent launch: each warp
+// takes the next 32 * R rays from a global counter (scenes of very
 // different cost balance across the GPU), finds the ray's scene from the
 // ray offsets and walks that scene's tree from its root.
 __global__ void __launch_bounds__(256)
@@ -1000,15 +1000,16 @@ trace_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
                    uint32_t *__restrict__ work, int R, unsigned long long *__restrict__ stats,
                    Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
                    uint32_t max_iter, uint32_t *__restrict__ err) {
-  __shared__ uint32_t s_base;
+  // each warp takes 32 * R rays at a time (no block-wide barrier: a warp
+  // whose rays finish early takes more work at once)
+  const uint32_t lane = threadIdx.x & 31u;
   while (true) {
-    if (threadIdx.x == 0) s_base = atomicAdd(work, blockDim.x * (uint32_t)R);
-    __syncthreads();
-    const uint32_t base = s_base;
-    __syncthreads();
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(work, 32u * (uint32_t)R);
+    base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
     for (int r = 0; r < R; r++) {
-      const uint32_t i = base + (uint32_t)r * blockDim.x + threadIdx.x;
+      const uint32_t i = base + (uint32_t)r * 32u + lane;
       if (i >= total) break;
       const int sg = seg_of(roff, nseg, i);
       Ctx2 c;
