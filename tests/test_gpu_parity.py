@@ -220,6 +220,29 @@ def test_spheres_build_trace_and_self_hit_rule():
                       o.trace(sec, prev_normals=nrm), ("t", "prim"))
 
 
+def test_sphere_pole_hits_take_the_reference_walk():
+    """Closest hits within rounding of their leaf box's entry with a second
+    hit inside the same rounding window: the reference's pruning decides,
+    and the GPU's second pass reproduces its walk."""
+    import ctypes as C
+
+    import torch
+    from surface_b200 import _lib
+    from test_walk_restatement import pole_pairs
+    pos, rad, rays = pole_pairs()
+    o, acc = _compare_build(O.SPHERE, pos, None, rad)
+    assert_hits_equal(trace_both(acc, rays), o.trace(rays), ("t", "prim"))
+    st = torch.zeros(4, dtype=torch.int64, device="cuda")
+    rt = torch.as_tensor(rays.view(np.float32).reshape(-1, 8)).cuda()
+    h = torch.empty((rays.size, 4), device="cuda")
+    opts = _lib.TraceOpts(None, None, None, None, None, st.data_ptr(), 0, 0)
+    acc.ctx.use_torch_stream()
+    _lib.check(acc.L.srt_trace_closest(acc.h, rt.data_ptr(), rays.size, h.data_ptr(),
+                                       C.byref(opts)))
+    torch.cuda.synchronize()
+    assert int(st[3]) > 0  # rays retraced by the reference's walk
+
+
 def test_constant_radius_spheres():
     pos, _ = S.particles(30_000, seed=8)
     o = O.OracleAccel(O.SPHERE, pos, None, None, const_radius=0.004)

@@ -37,13 +37,44 @@ def test_tetrahedra_ortho_ties_and_oblique():
         assert np.array_equal(s2, s1)
 
 
+def pole_pairs(n=48, z=0.5, dist=4.0, gap=5e-7, seed=45):
+    """Sphere pairs hit at their poles: centres on an n x n grid at height z,
+    each with a twin `gap` further down, and one orthographic ray down -z from
+    z + dist through every centre.  A pole hit lies one leaf padding (16
+    ulp(1)) behind its box face, within the rounding tolerance of a distance
+    of ~4, and the twin's hit is within it too -- the case where the
+    reference's pruning decides which of the two it reports."""
+    rng = np.random.default_rng(seed)
+    g = (np.arange(n) + 0.5) / n
+    X, Y = np.meshgrid(g, g)
+    c = np.stack([X.ravel(), Y.ravel(), np.full(n * n, z)], 1).astype(np.float32)
+    twin = c.copy()
+    twin[:, 2] -= np.float32(gap)
+    order = rng.permutation(2 * n * n)
+    pos = np.concatenate([c, twin])[order]
+    rad = np.full(2 * n * n, 0.004, np.float32)
+    rays = np.zeros(n * n, O.RAY_DTYPE)
+    rays["org"][:, :2] = c[:, :2]
+    rays["org"][:, 2] = z + dist
+    rays["dir"][:, 2] = -1.0
+    rays["prev_prim"] = O.MISS
+    return pos, rad, rays
+
+
 def test_spheres_fallback_path():
     pos, rad = S.particles(300_000, seed=43)
     o = O.OracleAccel(O.SPHERE, pos, None, rad)
     rays = S.pinhole_rays(160, 160, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
     h2, st = o.trace2(rays, want_stats=True)
     same(h2, o.trace(rays), ("t", "prim"))
-    assert st[3] > 0  # some rays needed the reference walk (ill-conditioned hits)
+    # pole hits with a twin inside the rounding window take the reference walk
+    pp, pr, prays = pole_pairs()
+    op = O.OracleAccel(O.SPHERE, pp, None, pr)
+    hp, sp = op.trace2(prays, want_stats=True)
+    same(hp, op.trace(prays), ("t", "prim"))
+    assert sp[3] > 0
+    if O.have_ref():
+        same(hp, O.RefAccel(O.SPHERE, pp, None, pr).trace(prays), ("t", "prim"))
     # secondary rays with the self-hit rule
     hit = h2["prim"] != O.MISS
     p = rays["org"][hit] + h2["t"][hit, None] * rays["dir"][hit]
