@@ -295,6 +295,42 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx,
                                         const float *grad_image,
                                         float *grad_density, float *grad_tf);
 
+/* ---- eye rays and framebuffer ------------------------------------------- */
+/* RaytraceEngine::OnData's per-pixel ray generation and framebuffer write
+ * (gles/gles_raytrace_engine.cc:547-879) for one sample per pixel, with the
+ * camera frame of Camera::buildFrame (render/render_camera.cc:17-63). */
+typedef struct srt_camera {
+  float eye[3], lookat[3], up[3];
+  float fov;            /* vertical field of view, degrees (perspective) */
+  int32_t ortho;        /* Camera's orthographic mode */
+  int32_t width, height;   /* framebuffer, 1..65535 */
+  int32_t viewport[4];     /* glViewport x, y, width, height */
+  int32_t region[4];       /* render region x0, y0, x1, y1 (scissor, screen tile) */
+  int32_t step;            /* pixel step (lsglSetPixelStep), >= 1 */
+} srt_camera;
+
+/* Eye rays of the loop pixels (x, y) = region start + multiples of step
+ * whose viewport-converted pixel lies on the framebuffer, row by row.
+ * rays (16-byte aligned) and pixel (optional; per ray (y << 16) | x of its
+ * loop pixel) are device arrays with room for every loop pixel of the
+ * region; *count receives the number written.  Asynchronous. */
+SRT_API srt_status srt_camera_rays(srt_ctx *ctx, const srt_camera *cam,
+                                   srt_ray *rays, uint32_t *pixel,
+                                   uint32_t *count);
+/* Write the hits of n rays made by srt_camera_rays: each hit fills the
+ * step x step block of its loop pixel (rows counted from the top, as the
+ * reference's Y-down framebuffer) with its colour -- rgba (n x float4, or
+ * NULL for the reference's hit colour (1,1,1,1)) -- as RGBA8 (format 0,
+ * clamp((int)(c * 255.0))) or RGBA32F (format 1), and its depth t into
+ * depth (optional, width x height floats).  Misses leave pixels as they
+ * are.  Device arrays, 16-byte aligned; asynchronous. */
+SRT_API srt_status srt_framebuffer_write(srt_ctx *ctx, const srt_camera *cam,
+                                         const srt_hit *hits,
+                                         const uint32_t *pixel,
+                                         const float *rgba, uint32_t n,
+                                         int32_t format, void *color,
+                                         float *depth);
+
 /* ---- secondary rays ----------------------------------------------------- */
 /* One secondary ray per hit ray (the particle workload's bounce; in the
  * reference a fragment shader builds it and calls back trace() with

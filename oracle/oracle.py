@@ -92,6 +92,11 @@ def lib():
         L.so_volume_fwd_f32.argtypes = [_P, _P, _P, _P, _P, C.c_int]
         L.so_volume_f64.restype = C.c_double
         L.so_volume_f64.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
+        L.so_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int, _P]
+        L.so_camera_rays.restype = _SZ
+        L.so_camera_rays.argtypes = [_P, _P, _P, _P]
+        L.so_framebuffer_write.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, _SZ,
+                                           C.c_int, _P, _P]
         _ORACLE = L
     return _ORACLE
 
@@ -137,6 +142,8 @@ def ref():
                                 C.c_int, C.c_int, C.c_int, _P]
         L.ref_tinymt64_doubles.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32,
                                            C.c_uint64, _SZ, _P]
+        L.ref_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int,
+                                       _P]
         _REF = L
     return _REF
 
@@ -530,3 +537,49 @@ def volume_f64(params, dens, dims, tf, target=None, want_grad=False, want_img=Fa
     loss = lib().so_volume_f64(_ptr(params), _ptr(dens), _ptr(np.asarray(dims, np.int32)),
                                _ptr(tf), _ptr(tg), _ptr(img), _ptr(gd), _ptr(gt))
     return loss, img, gd, gt
+
+
+# ---------------------------------------------------------------- eye rays
+def camera_frame(eye, lookat, up, fov, ortho, width, height, use_ref=False):
+    """(corner, u, v) of Camera::buildFrame -- the restatement, or with
+    use_ref the reference's own (render/render_camera.cc:17-63)."""
+    e, la, u = (np.ascontiguousarray(x, np.float32) for x in (eye, lookat, up))
+    out = np.zeros(9, np.float32)
+    L = ref() if use_ref else lib()
+    fn = L.ref_camera_frame if use_ref else L.so_camera_frame
+    fn(_ptr(e), _ptr(la), _ptr(u), C.c_float(fov), int(ortho), int(width), int(height),
+       _ptr(out))
+    return out[:3], out[3:6], out[6:]
+
+
+def camera_rays(cam):
+    """OnData's eye rays for one sample per pixel (see so_camera_rays).
+    cam: dict with eye, lookat, up, fov, ortho, width, height, viewport
+    (x, y, w, h), region (x0, y0, x1, y1), step.  Returns (rays, pixel)."""
+    f = np.zeros(10, np.float32)
+    f[0:3], f[3:6], f[6:9], f[9] = cam["eye"], cam["lookat"], cam["up"], cam["fov"]
+    ints = np.array([cam["ortho"], cam["width"], cam["height"], *cam["viewport"],
+                     *cam["region"], cam["step"]], np.int32)
+    x0, y0, x1, y1 = cam["region"]
+    cap = max(1, len(range(x0, x1, cam["step"])) * len(range(y0, y1, cam["step"])))
+    rays = np.zeros(cap, RAY_DTYPE)
+    pix = np.zeros(cap, np.uint32)
+    n = lib().so_camera_rays(_ptr(f), _ptr(ints), _ptr(rays), _ptr(pix))
+    return rays[:n], pix[:n]
+
+
+def framebuffer_write(cam, hits, pixel, rgba=None, fmt=0, color=None, depth=None):
+    """OnData's write of the hit rays into (color, depth); color RGBA8
+    (fmt 0, uint8 (H, W, 4)) or RGBA32F (fmt 1, float32 (H, W, 4))."""
+    W, H = cam["width"], cam["height"]
+    if color is None:
+        color = np.zeros((H, W, 4), np.uint8 if fmt == 0 else np.float32)
+    if depth is None:
+        depth = np.zeros((H, W), np.float32)
+    hits = np.ascontiguousarray(hits, HIT_DTYPE)
+    pixel = np.ascontiguousarray(pixel, np.uint32)
+    rg = None if rgba is None else np.ascontiguousarray(rgba, np.float32)
+    lib().so_framebuffer_write(W, H, cam["step"], _ptr(hits), _ptr(pixel),
+                               None if rg is None else _ptr(rg), hits.size, fmt,
+                               _ptr(color), _ptr(depth))
+    return color, depth

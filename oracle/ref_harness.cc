@@ -13,6 +13,7 @@
 //   CalculateMortonCodes*, RadixSort30OMP, ConstructBinaryRadixTree30
 //                          (render/render_prefix_tree_util.h)
 //   FilterTexture3DFloat   (render/render_texture.h)
+//   Camera::buildFrame     (render/render_camera.h)
 //   tinymt64_*             (render/tinymt64.h)
 #include <fcntl.h>
 #include <omp.h>
@@ -26,6 +27,7 @@
 #include "render_accel_particle.h"
 #include "render_accel_tetra.h"
 #include "render_accel_triangle.h"
+#include "render_camera.h"
 #include "render_prefix_tree_util.h"
 #include "render_texture.h"
 #include "tinymt64.h"
@@ -342,4 +344,18 @@ REF_API void ref_tinymt64_doubles(uint64_t seed, uint32_t mat1, uint32_t mat2,
   rng.tmat = tmat;
   tinymt64_init(&rng, seed);
   for (size_t i = 0; i < n; i++) out[i] = tinymt64_generate_double(&rng);
+}
+
+// Camera::buildFrame (render/render_camera.cc:17-63): out = corner, u, v.
+REF_API void ref_camera_frame(const float eye[3], const float lookat[3], const float up[3],
+                              float fov, int ortho, int width, int height, float out[9]) {
+  Camera cam(real3(eye[0], eye[1], eye[2]), real3(lookat[0], lookat[1], lookat[2]),
+             real3(up[0], up[1], up[2]), fov, ortho != 0);
+  real3 corner, u, v;
+  cam.buildFrame(corner, u, v, width, height);
+  for (int k = 0; k < 3; k++) {
+    out[k] = corner[k];
+    out[3 + k] = u[k];
+    out[6 + k] = v[k];
+  }
 }

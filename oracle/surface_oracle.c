@@ -1686,3 +1686,164 @@ SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
   }
   return loss;
 }
+
+/* ======================================================== eye rays, frames
+ * RaytraceEngine::OnData's eye rays and framebuffer write for one sample per
+ * pixel (gles/gles_raytrace_engine.cc:547-879), restated:
+ *   - Camera::buildFrame (render/render_camera.cc:17-63), float arithmetic
+ *     with real3::normalize's double reciprocal length
+ *     (render/render_common.h:69-83);
+ *   - ViewportConversion (gles/gles_raytrace_engine.cc:530-544);
+ *   - per pixel (x, y) of the render region in steps of `step`: the
+ *     viewport-converted pixel (px, py), and the ray through
+ *     corner + (px + step/2) u + (py - step/2 + 1) v (:770-795);
+ *   - the write of a hit: the step x step block at (x + u, height - y - 1 + v)
+ *     gets the colour (RGBA8 via clamp() (:50-58) or RGBA32F) and the depth t
+ *     (:840-877).  Rows above the framebuffer are skipped (the reference
+ *     would write outside it). */
+
+static void cam_norm(float v[3]) {
+  double l2 = (double)(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]);
+  double l = 0.0;
+  if (fabs(l2) > 1.0e-30) l = 1.0 / sqrt(l2);
+  for (int k = 0; k < 3; k++) v[k] = (float)((double)v[k] * l);
+}
+
+static void cam_cross(const float a[3], const float b[3], float o[3]) {
+  o[0] = a[1] * b[2] - a[2] * b[1];
+  o[1] = a[2] * b[0] - a[0] * b[2];
+  o[2] = a[0] * b[1] - a[1] * b[0];
+}
+
+/* out = corner[3], u[3], v[3] */
+SO_API void so_camera_frame(const float eye[3], const float lookat[3], const float up[3],
+                            float fov, int ortho, int width, int height, float out[9]) {
+  float look[3], u[3], v[3], corner[3];
+  for (int k = 0; k < 3; k++) look[k] = lookat[k] - eye[k];
+  cam_cross(look, up, u);
+  cam_norm(u);
+  cam_cross(look, u, v);
+  cam_norm(v);
+  cam_norm(look);
+  if (ortho) {
+    for (int k = 0; k < 3; k++) {
+      u[k] = u[k] / (float)width;
+      v[k] = v[k] / (float)height;
+    }
+    for (int k = 0; k < 3; k++) corner[k] = -(u[k] * (float)width + v[k] * (float)height);
+    for (int k = 0; k < 3; k++) {
+      u[k] = 2.0f * u[k];
+      v[k] = 2.0f * v[k];
+    }
+  } else {
+    const float flen =
+        (float)(0.5f * (float)height / tan(0.5 * ((double)fov * 3.14159265358979323846 / 180.0)));
+    for (int k = 0; k < 3; k++) look[k] = look[k] * flen + eye[k];
+    for (int k = 0; k < 3; k++) {
+      const float s = u[k] * (float)width + v[k] * (float)height;
+      corner[k] = look[k] - s * 0.5f;
+    }
+  }
+  for (int k = 0; k < 3; k++) {
+    out[k] = corner[k];
+    out[3 + k] = u[k];
+    out[6 + k] = v[k];
+  }
+}
+
+/* Viewport conversion of loop pixel x (axis 0) or y (axis 1). */
+static int cam_viewport(int x, int axis, int size, int vp_off, int vp_size) {
+  const float inv = 1.0f / (float)size;
+  const float x01 = ((float)x + 0.5f) * inv;
+  const float nd = 2.0f * (x01 - 0.5f);
+  const float w = (nd + 1.0f) * (0.5f * (float)vp_size);
+  return axis == 0 ? (int)(w - (float)vp_off) : (int)(w + (float)vp_off);
+}
+
+/* cam: eye[3], lookat[3], up[3], fov; ints: ortho, width, height, vx, vy,
+ * vw, vh, x0, y0, x1, y1, step.  Writes the rays (row-major over the loop
+ * pixels whose converted pixel is on screen) and each ray's loop pixel
+ * (y << 16 | x); returns the count. */
+SO_API size_t so_camera_rays(const float cam[10], const int ints[12], so_ray *rays,
+                             uint32_t *pixel) {
+  const int ortho = ints[0], W = ints[1], H = ints[2], vx = ints[3], vy = ints[4],
+            vw = ints[5], vh = ints[6], x0 = ints[7], y0 = ints[8], x1 = ints[9],
+            y1 = ints[10], step = ints[11];
+  float fr[9];
+  so_camera_frame(cam, cam + 3, cam + 6, cam[9], ortho, W, H, fr);
+  const float *corner = fr, *ud = fr + 3, *vd = fr + 6;
+  float look[3];
+  cam_cross(ud, vd, look);
+  cam_norm(look);
+  size_t n = 0;
+  for (int y = y0; y < y1; y += step) {
+    const int py = cam_viewport(y, 1, H, vy, vh);
+    if (py < 0 || py >= H) continue;
+    for (int x = x0; x < x1; x += step) {
+      const int px = cam_viewport(x, 0, W, vx, vw);
+      if (px < 0 || px >= W) continue;
+      const float a = ((float)px + 0.0f) + (float)step / 2.0f;
+      const float b = (((float)py + 0.0f) - (float)step / 2.0f) + 1.0f;
+      float o[3], d[3];
+      for (int k = 0; k < 3; k++) {
+        const float p = (corner[k] + ud[k] * a) + vd[k] * b;
+        if (ortho) {
+          o[k] = p;
+          d[k] = look[k];
+        } else {
+          o[k] = cam[k];
+          d[k] = p - cam[k];
+        }
+      }
+      cam_norm(d);
+      so_ray *r = &rays[n];
+      for (int k = 0; k < 3; k++) {
+        r->org[k] = o[k];
+        r->dir[k] = d[k];
+      }
+      r->prev_prim = 0xffffffffu;
+      r->prev_t = 0.0f;
+      pixel[n] = ((uint32_t)y << 16) | (uint32_t)x;
+      n++;
+    }
+  }
+  return n;
+}
+
+static unsigned char fb_clamp(float f) {
+  const double d = (double)f * 255.0;
+  int i = (d >= -2147483648.0 && d < 2147483648.0) ? (int)d : INT32_MIN; /* x86 cvttsd2si */
+  if (i < 0) i = 0;
+  if (i > 255) i = 255;
+  return (unsigned char)i;
+}
+
+/* format 0: RGBA8, 1: RGBA32F.  rgba: per-ray colour or NULL (1,1,1,1). */
+SO_API void so_framebuffer_write(int width, int height, int step, const so_hit *hits,
+                                 const uint32_t *pixel, const float *rgba, size_t n,
+                                 int format, void *color, float *depth) {
+  for (size_t i = 0; i < n; i++) {
+    if (hits[i].prim == 0xffffffffu) continue;
+    const int x = (int)(pixel[i] & 0xffffu), y = (int)(pixel[i] >> 16);
+    float c[4] = {1.0f, 1.0f, 1.0f, 1.0f};
+    if (rgba)
+      for (int k = 0; k < 4; k++) c[k] = rgba[4 * i + k];
+    for (int vv = 0; vv < step; vv++) {
+      const int row = height - y - 1 + vv;
+      if (row > height - 1 || row < 0) continue;
+      for (int uu = 0; uu < step; uu++) {
+        const int col = x + uu;
+        if (col > width - 1) continue;
+        const size_t p = (size_t)row * width + col;
+        if (color && format == 0) {
+          unsigned char *o = (unsigned char *)color + 4 * p;
+          for (int k = 0; k < 4; k++) o[k] = fb_clamp(c[k] * 1.0f);
+        } else if (color) {
+          float *o = (float *)color + 4 * p;
+          for (int k = 0; k < 4; k++) o[k] = c[k] * 1.0f;
+        }
+        if (depth) depth[p] = hits[i].t * 1.0f;
+      }
+    }
+  }
+}

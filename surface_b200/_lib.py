@@ -20,6 +20,14 @@ MISS = 0xFFFFFFFF
 SRT_TRACE_SINGLE_PASS = 1
 SRT_TRACE_SORT_RAYS = 2
 
+
+class Camera(C.Structure):
+    """srt_camera (include/surface_rt.h)."""
+    _fields_ = [("eye", C.c_float * 3), ("lookat", C.c_float * 3), ("up", C.c_float * 3),
+                ("fov", C.c_float), ("ortho", C.c_int32), ("width", C.c_int32),
+                ("height", C.c_int32), ("viewport", C.c_int32 * 4),
+                ("region", C.c_int32 * 4), ("step", C.c_int32)]
+
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
                       ("prev_t", "<f4")])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4")])
@@ -83,6 +91,8 @@ _SIGS = {
     "srt_volume_march_fwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P],
     "srt_volume_march_bwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P],
     "srt_spawn_secondary": [_P, _P, _P, _P, _SZ, C.c_uint64, _P, _P, _P],
+    "srt_camera_rays": [_P, _P, _P, _P, _P],
+    "srt_framebuffer_write": [_P, _P, _P, _P, _P, C.c_uint32, C.c_int32, _P, _P],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],

@@ -199,3 +199,37 @@ def test_oracle_vs_reference_flat_mesh():
     rc, ridx = r.canonical()
     assert np.array_equal(o.canonical(), rc)
     assert np.array_equal(o.indices, ridx)
+
+
+CAMERAS = [((0, 0, 3), (0, 0, 0), (0, 1, 0), 45.0, 0, 512, 512),
+           ((0.3, 0.2, 3), (0, 0.1, 0), (0, 1, 0), 30.0, 0, 640, 480),
+           ((1, 2, 3), (0, 0, 0), (0, 0, 1), 60.0, 1, 300, 200),
+           ((0.5, 0.5, 2.2), (0.5, 0.5, 0.5), (0, 1, 0), 30.0, 0, 2048, 2048),
+           ((-4, 1, -2), (0.2, -0.3, 0.9), (0.1, 1, 0), 75.0, 0, 333, 97)]
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+@pytest.mark.parametrize("cam", CAMERAS)
+def test_camera_frame_matches_reference(cam):
+    """The restated Camera::buildFrame equals the reference's, bit for bit."""
+    a = O.camera_frame(*cam)
+    b = O.camera_frame(*cam, use_ref=True)
+    for x, y in zip(a, b):
+        assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+def test_camera_rays_restatement_properties():
+    """Eye rays of the restated OnData loop: unit directions, the pinhole
+    rays pass through the eye, the viewport offset shifts pixels."""
+    cam = {"eye": (0, 0, 3), "lookat": (0, 0, 0), "up": (0, 1, 0), "fov": 45.0,
+           "ortho": 0, "width": 64, "height": 48, "viewport": (0, 0, 64, 48),
+           "region": (0, 0, 64, 48), "step": 1}
+    rays, pix = O.camera_rays(cam)
+    assert rays.size == 64 * 48
+    assert np.allclose(np.linalg.norm(rays["dir"], axis=1), 1, atol=1e-6)
+    assert np.all(rays["org"] == np.float32([0, 0, 3]))
+    sh, pix = O.camera_rays(dict(cam, viewport=(8, 0, 64, 48)))
+    # pixels converted off screen are skipped; x = 7 converts to -0.5, which
+    # the int conversion truncates to 0, so it stays
+    assert sh.size == (64 - 7) * 48
+    assert (pix & 0xFFFF).min() == 7
