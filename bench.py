@@ -89,6 +89,15 @@ def make_workload(name):
                                         "step 0.5 voxel, emission-absorption forward + "
                                         "adjoint of an L2 loss",
                             "rays": 512 * 512})
+    if name == "frame":
+        v, f = S.displaced_octasphere(7)
+        return dict(kind="frame", verts=v, prims=f, rays=np.zeros(512 * 512, np.uint8),
+                    cam=dict(width=512, height=512, eye=(0.0, 0.0, 3.0),
+                             lookat=(0.0, 0.0, 0.0), fov=45.0),
+                    config={"workload": "frame512: tri131k scene (built once, resident), "
+                                        "512x512 pinhole camera at distance 3, 45 deg: eye "
+                                        "rays + closest hit + RGBA8 and depth write per step",
+                            "prims": int(f.shape[0]), "rays": 512 * 512})
     if name == "batched":
         B = S.batched_scenes()
         return dict(kind="batched", B=B, rays=B["rays"],
@@ -337,13 +346,39 @@ def cpu_reference_particles(W, nthreads=0, stride=4):
     return value, tb, tt, ns, ("reference" if use_ref else "port")
 
 
+def cpu_reference_frame(W, nthreads=0):
+    """OnData on the host: the eye rays and framebuffer write of the CPU
+    restatement around the reference's own OpenMP Traverse over every pixel
+    (the accel is built once, outside the timing, as AccelBuilder caches it).
+    Returns (Mrays/s, rays s, trace s, rays, kind)."""
+    from oracle import oracle as O
+    from surface_b200 import camera as K
+    use_ref = O.have_ref() and O.ref() is not None
+    if "_cpu_acc" not in W:
+        W["_cpu_acc"] = (O.RefAccel if use_ref else O.OracleAccel)(O.TRI, W["verts"],
+                                                                   W["prims"])
+    acc = W["_cpu_acc"]
+    d = K.camera_dict(K.make_camera(**W["cam"]))
+    t0 = time.perf_counter()
+    rays, pix = O.camera_rays(d)
+    tr = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    hits = acc.trace(rays, nthreads=nthreads, chunk=64) if use_ref else acc.trace(
+        rays, nthreads=nthreads)
+    tt = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    O.framebuffer_write(d, hits, pix, None, 0)
+    tr += time.perf_counter() - t0
+    return rays.size / (tr + tt) / 1e6, tr, tt, rays.size, ("reference" if use_ref else "port")
+
+
 def run_reference_arm(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cores = os.cpu_count() or 1
-    step = {"batched": cpu_reference_batched,
-            "sphere": cpu_reference_particles}.get(W["kind"], cpu_reference_step)
+    step = {"batched": cpu_reference_batched, "sphere": cpu_reference_particles,
+            "frame": cpu_reference_frame}.get(W["kind"], cpu_reference_step)
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
@@ -358,20 +393,25 @@ def run_reference_arm(args, W):
         nr = int(ns * 4)  # primaries + secondaries of one frame
     ms = 1e3 * nr / (value * 1e6)
     stride = 16 if W["kind"] == "batched" else 4
+    sample = (f"full Build32 + every {stride}th ray ({ns} of {nr}) per step, trace time "
+              f"scaled to all rays; median of {args.steps}")
+    if W["kind"] == "frame":
+        sample = (f"every pixel ({ns} rays): eye rays and framebuffer write of the CPU "
+                  f"restatement, Traverse of the reference (accel built once); median of "
+                  f"{args.steps}")
     line = {
         "impl": "reference",
-        "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART}.get(W["kind"], METRIC),
+        "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART,
+                   "frame": METRIC_FRAME}.get(W["kind"], METRIC),
         "value": round(value, 4), "unit": "Mrays/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPE[W["kind"]], "data": "synthetic",
         "config": W["config"],
-        "build_ms": round(1e3 * statistics.median(tbs), 3),
+        ("rays_write_ms" if W["kind"] == "frame" else "build_ms"):
+            round(1e3 * statistics.median(tbs), 3),
         "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores,
-                         "kind": kind,
-                         "sample": f"full Build32 + every {stride}th ray ({ns} of {nr}) per "
-                                   f"step, trace time scaled to all rays; median of "
-                                   f"{args.steps}"},
+                         "kind": kind, "sample": sample},
         "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -382,8 +422,9 @@ METRIC = "Mrays/s (LBVH build + closest hit per step)"
 METRIC_VOL = "Mrays/s (volume march forward + adjoint per step)"
 METRIC_BATCH = "Mrays/s (64-scene batched LBVH build + closest hit per step)"
 METRIC_PART = "Mrays/s (particle frame: LBVH rebuild + primaries + secondaries per step)"
+METRIC_FRAME = "Mrays/s (frame: eye rays + closest hit + framebuffer write per step)"
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
-         "volume": "f32", "batched": "f32"}
+         "volume": "f32", "batched": "f32", "frame": "f32"}
 
 
 def volume_sample_count(p):
@@ -891,6 +932,147 @@ def run_particles(args, W):
     dist_teardown()
 
 
+# ---------------------------------------------------------------- frame
+def run_frame(args, W):
+    """One step = one frame of a resident scene: srt_camera_rays,
+    srt_trace_closest, srt_framebuffer_write (RGBA8 + depth).  e2e: the same
+    calls with the camera struct as the host input and the colour and depth
+    buffers copied back every frame."""
+    import ctypes as C
+
+    import torch
+
+    import surface_b200 as sb
+    from surface_b200 import _lib
+    from surface_b200 import camera as K
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
+    L = _lib.load()
+    chk = _lib.check
+    ctx = sb.Context(local)
+    ctx.use_torch_stream()
+    acc = C.c_void_p()
+    chk(L.srt_accel_create(ctx.h, _lib.SRT_TRIANGLES, C.byref(acc)))
+    v = torch.as_tensor(W["verts"], device=dev)
+    f = torch.as_tensor(W["prims"].view(np.int32), device=dev)
+    chk(L.srt_accel_build_triangles(acc, v.data_ptr(), v.shape[0], f.data_ptr(), f.shape[0]))
+    cam = K.make_camera(**W["cam"])
+    nr = W["cam"]["width"] * W["cam"]["height"]
+    rays = torch.empty((nr, 8), device=dev)
+    pix = torch.empty((nr,), dtype=torch.int32, device=dev)
+    hits = torch.empty((nr, 4), device=dev)
+    color = torch.zeros((cam.height, cam.width, 4), dtype=torch.uint8, device=dev)
+    depth = torch.zeros((cam.height, cam.width), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cnt = C.c_uint32()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(4)] for _ in range(args.steps)]
+
+    def step(e=None):
+        if e: e[0].record()
+        chk(L.srt_camera_rays(ctx.h, C.byref(cam), rays.data_ptr(), pix.data_ptr(),
+                              C.byref(cnt)))
+        if e: e[1].record()
+        chk(L.srt_trace_closest(acc, rays.data_ptr(), cnt.value, hits.data_ptr(), None))
+        if e: e[2].record()
+        chk(L.srt_framebuffer_write(ctx.h, C.byref(cam), hits.data_ptr(), pix.data_ptr(),
+                                    None, cnt.value, 0, color.data_ptr(), depth.data_ptr()))
+        if e: e[3].record()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    st = torch.zeros(4, dtype=torch.int64, device=dev)
+    opts = _lib.TraceOpts(None, None, None, None, None, st.data_ptr(), 0, 0)
+    chk(L.srt_trace_closest(acc, rays.data_ptr(), cnt.value, hits.data_ptr(), C.byref(opts)))
+    torch.cuda.synchronize()
+    stats = st.cpu().numpy().astype(np.float64)[:3]
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
+        launches0 = L.srt_ctx_launch_count(ctx.h)
+        for k in range(args.steps):
+            flush.zero_()
+            step(ev[k])
+        torch.cuda.synchronize()
+        launches = L.srt_ctx_launch_count(ctx.h) - launches0
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
+    barrier()
+    r_ms = [e[0].elapsed_time(e[1]) for e in ev]
+    t_ms = [e[1].elapsed_time(e[2]) for e in ev]
+    w_ms = [e[2].elapsed_time(e[3]) for e in ev]
+    total = max_over_ranks([sum(r_ms) + sum(t_ms) + sum(w_ms)], dev)[0]
+    ms_per_step = total / args.steps
+    value = whole_job_mrays(nr, world, ms_per_step)
+
+    # ---- e2e: camera in, colour and depth out, every frame
+    h_color = torch.empty_like(color, device="cpu").pin_memory()
+    h_depth = torch.empty_like(depth, device="cpu").pin_memory()
+
+    def e2e_step():
+        step()
+        h_color.copy_(color, non_blocking=True)
+        h_depth.copy_(depth, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+
+    hbm, src = peaks()
+    bpr = algorithmic_bytes_per_ray("tri", stats, nr)
+    tr_ms = statistics.mean(t_ms)
+    achieved = bpr * nr / (tr_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "trace", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_ray": round(bpr, 1),
+                "visits_per_ray": [round(float(x) / nr, 3) for x in stats]}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        vals = [cpu_reference_frame(W) for _ in range(3)]
+        cv, ctr, ctt, cns, ck = sorted(vals)[1]
+        cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(), "kind": ck,
+               "rays_write_s": round(ctr, 4), "trace_s": round(ctt, 4),
+               "sample": f"every pixel ({cns} rays), median of 3: eye rays and write of "
+                         f"the CPU restatement, Traverse of the reference"}
+    L.srt_accel_destroy(acc)
+    if rank == 0:
+        line = {
+            "metric": METRIC_FRAME, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)",
+                           parallelism=f"replicas x{world}"),
+            "camera_rays_ms": round(statistics.mean(r_ms), 4),
+            "trace_ms": round(tr_ms, 4),
+            "framebuffer_write_ms": round(statistics.mean(w_ms), 4),
+            "clocks": clk.summary(),
+            "e2e": {"value": round(whole_job_mrays(nr, world, e2e_ms), 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": C.sizeof(cam),
+                    "d2h_bytes_per_step": int(h_color.numel() + 4 * h_depth.numel()),
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    dist_teardown()
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args, W):
     import torch
@@ -1077,7 +1259,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
-                    choices=["tet", "tri", "particles", "volume", "batched"])
+                    choices=["tet", "tri", "particles", "volume", "batched", "frame"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -1097,6 +1279,8 @@ def main():
         run_batched(args, W)
     elif args.workload == "particles":
         run_particles(args, W)
+    elif args.workload == "frame":
+        run_frame(args, W)
     else:
         run_ours(args, W)
 

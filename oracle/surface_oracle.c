@@ -1775,13 +1775,35 @@ SO_API size_t so_camera_rays(const float cam[10], const int ints[12], so_ray *ra
   float look[3];
   cam_cross(ud, vd, look);
   cam_norm(look);
-  size_t n = 0;
+  /* kept loop pixels per axis (the conversion is separable), then one ray
+   * per kept (y, x) in row-major order, rows in parallel */
+  int nx = 0, ny = 0;
+  for (int x = x0; x < x1; x += step) {
+    const int px = cam_viewport(x, 0, W, vx, vw);
+    if (px >= 0 && px < W) nx++;
+  }
   for (int y = y0; y < y1; y += step) {
     const int py = cam_viewport(y, 1, H, vy, vh);
-    if (py < 0 || py >= H) continue;
-    for (int x = x0; x < x1; x += step) {
+    if (py >= 0 && py < H) ny++;
+  }
+  int *xs = (int *)malloc(sizeof(int) * (size_t)(nx > 0 ? nx : 1));
+  int *ys = (int *)malloc(sizeof(int) * (size_t)(ny > 0 ? ny : 1));
+  nx = ny = 0;
+  for (int x = x0; x < x1; x += step) {
+    const int px = cam_viewport(x, 0, W, vx, vw);
+    if (px >= 0 && px < W) xs[nx++] = x;
+  }
+  for (int y = y0; y < y1; y += step) {
+    const int py = cam_viewport(y, 1, H, vy, vh);
+    if (py >= 0 && py < H) ys[ny++] = y;
+  }
+#pragma omp parallel for schedule(static)
+  for (int j = 0; j < ny; j++) {
+    const int y = ys[j];
+    const int py = cam_viewport(y, 1, H, vy, vh);
+    for (int i = 0; i < nx; i++) {
+      const int x = xs[i];
       const int px = cam_viewport(x, 0, W, vx, vw);
-      if (px < 0 || px >= W) continue;
       const float a = ((float)px + 0.0f) + (float)step / 2.0f;
       const float b = (((float)py + 0.0f) - (float)step / 2.0f) + 1.0f;
       float o[3], d[3];
@@ -1796,6 +1818,7 @@ SO_API size_t so_camera_rays(const float cam[10], const int ints[12], so_ray *ra
         }
       }
       cam_norm(d);
+      const size_t n = (size_t)j * nx + i;
       so_ray *r = &rays[n];
       for (int k = 0; k < 3; k++) {
         r->org[k] = o[k];
@@ -1804,10 +1827,11 @@ SO_API size_t so_camera_rays(const float cam[10], const int ints[12], so_ray *ra
       r->prev_prim = 0xffffffffu;
       r->prev_t = 0.0f;
       pixel[n] = ((uint32_t)y << 16) | (uint32_t)x;
-      n++;
     }
   }
-  return n;
+  free(xs);
+  free(ys);
+  return (size_t)nx * ny;
 }
 
 static unsigned char fb_clamp(float f) {
@@ -1822,7 +1846,9 @@ static unsigned char fb_clamp(float f) {
 SO_API void so_framebuffer_write(int width, int height, int step, const so_hit *hits,
                                  const uint32_t *pixel, const float *rgba, size_t n,
                                  int format, void *color, float *depth) {
-  for (size_t i = 0; i < n; i++) {
+#pragma omp parallel for schedule(static)
+  for (long ii = 0; ii < (long)n; ii++) {
+    const size_t i = (size_t)ii;
     if (hits[i].prim == 0xffffffffu) continue;
     const int x = (int)(pixel[i] & 0xffffu), y = (int)(pixel[i] >> 16);
     float c[4] = {1.0f, 1.0f, 1.0f, 1.0f};
