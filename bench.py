@@ -1,7 +1,7 @@
 """Benchmark: LBVH build + closest-hit throughput on B200 (one JSON line).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tet|tri|particles]
+                    [--workload tet|tri|particles|volume|batched|frame|scene]
 
 Default workload (``tet``): the tetrahedral-mesh configuration -- 64^3 cells in
 the unit cube, five tetrahedra per cell (1,310,720 tets), interior vertices
@@ -98,6 +98,19 @@ def make_workload(name):
                                         "512x512 pinhole camera at distance 3, 45 deg: eye "
                                         "rays + closest hit + RGBA8 and depth write per step",
                             "prims": int(f.shape[0]), "rays": 512 * 512})
+    if name == "scene":
+        E = S.instanced_scene()
+        return dict(kind="scene", E=E, rays=np.zeros(1024 * 1024, np.uint8),
+                    cam=dict(width=1024, height=1024, eye=(-14.0, 10.0, 18.0),
+                             lookat=(0.0, 0.0, 0.0), fov=40.0),
+                    config={"workload": "scene64: 64 transformed elements on a 4x4x4 grid "
+                                        "(instances of a 131,072-triangle octasphere, a "
+                                        "1,000,000-sphere cloud and a 163,840-tet grid; "
+                                        "accels resident), 1024x1024 pinhole camera: "
+                                        "top-level tree build + eye rays + scene closest "
+                                        "hit + RGBA8 and depth write per step",
+                            "elements": len(E["elements"]),
+                            "prims": int(sum(E["prims"])), "rays": 1024 * 1024})
     if name == "batched":
         B = S.batched_scenes()
         return dict(kind="batched", B=B, rays=B["rays"],
@@ -372,13 +385,58 @@ def cpu_reference_frame(W, nthreads=0):
     return rays.size / (tr + tt) / 1e6, tr, tt, rays.size, ("reference" if use_ref else "port")
 
 
+def _oracle_scene(W):
+    from oracle import oracle as O
+    if "_cpu_scene" not in W:
+        E = W["E"]
+        accs = []
+        for a in E["accels"]:
+            if a["kind"] == 2:
+                accs.append(O.OracleAccel(O.SPHERE, a["verts"], None, a["radius"]))
+            else:
+                accs.append(O.OracleAccel(O.TRI if a["kind"] == 0 else O.TET, a["verts"],
+                                          a["faces"]))
+        W["_cpu_accs"] = accs
+        W["_cpu_scene"] = None
+    return W["_cpu_accs"]
+
+
+def cpu_reference_scene(W, nthreads=0, stride=4):
+    """The CPU restatement of one scene frame (RenderGraph::Build, the eye
+    rays, RenderGraph::Trace with OpenMP over every stride-th pixel, the
+    framebuffer write); element accels built once outside the timing.
+    Returns (Mrays/s, build+rays+write s, trace s scaled, rays traced, kind)."""
+    from oracle import oracle as O
+    from surface_b200 import camera as K
+    accs = _oracle_scene(W)
+    E = W["E"]
+    d = K.camera_dict(K.make_camera(**W["cam"]))
+    t0 = time.perf_counter()
+    mats = [O.element_update(el["T"], *accs[el["accel"]].bbox64())
+            for el in E["elements"]]
+    sc = O.OracleScene([accs[el["accel"]] for el in E["elements"]],
+                       [el["T"] for el in E["elements"]], [m[0] for m in mats],
+                       [m[1] for m in mats], [m[2] for m in mats], [m[3] for m in mats])
+    rays, pix = O.camera_rays(d)
+    tr = time.perf_counter() - t0
+    sample = rays[::stride]
+    t0 = time.perf_counter()
+    hits, _ = sc.trace(sample, nthreads=nthreads)
+    tt = (time.perf_counter() - t0) * stride
+    t0 = time.perf_counter()
+    O.framebuffer_write(d, hits, pix[::stride], None, 0)
+    tr += (time.perf_counter() - t0)
+    return rays.size / (tr + tt) / 1e6, tr, tt, sample.size, "port"
+
+
 def run_reference_arm(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cores = os.cpu_count() or 1
     step = {"batched": cpu_reference_batched, "sphere": cpu_reference_particles,
-            "frame": cpu_reference_frame}.get(W["kind"], cpu_reference_step)
+            "frame": cpu_reference_frame, "scene": cpu_reference_scene}.get(
+                W["kind"], cpu_reference_step)
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
@@ -399,16 +457,21 @@ def run_reference_arm(args, W):
         sample = (f"every pixel ({ns} rays): eye rays and framebuffer write of the CPU "
                   f"restatement, Traverse of the reference (accel built once); median of "
                   f"{args.steps}")
+    if W["kind"] == "scene":
+        sample = (f"top-level build, eye rays and write of every pixel, scene trace of every "
+                  f"4th pixel ({ns} of {nr}) scaled to all, by the CPU restatement "
+                  f"(OpenMP; the reference's RenderGraph needs its GL front end); median "
+                  f"of {args.steps}")
     line = {
         "impl": "reference",
         "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART,
-                   "frame": METRIC_FRAME}.get(W["kind"], METRIC),
+                   "frame": METRIC_FRAME, "scene": METRIC_SCENE}.get(W["kind"], METRIC),
         "value": round(value, 4), "unit": "Mrays/s",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPE[W["kind"]], "data": "synthetic",
         "config": W["config"],
-        ("rays_write_ms" if W["kind"] == "frame" else "build_ms"):
+        ("rays_write_ms" if W["kind"] in ("frame", "scene") else "build_ms"):
             round(1e3 * statistics.median(tbs), 3),
         "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores,
                          "kind": kind, "sample": sample},
@@ -423,8 +486,11 @@ METRIC_VOL = "Mrays/s (volume march forward + adjoint per step)"
 METRIC_BATCH = "Mrays/s (64-scene batched LBVH build + closest hit per step)"
 METRIC_PART = "Mrays/s (particle frame: LBVH rebuild + primaries + secondaries per step)"
 METRIC_FRAME = "Mrays/s (frame: eye rays + closest hit + framebuffer write per step)"
+METRIC_SCENE = ("Mrays/s (scene frame: top-level build + eye rays + closest hit over "
+                "transformed elements + framebuffer write per step)")
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
-         "volume": "f32", "batched": "f32", "frame": "f32"}
+         "volume": "f32", "batched": "f32", "frame": "f32",
+         "scene": "f64 transforms and top-level boxes / f32 + f64 element tests"}
 
 
 def volume_sample_count(p):
@@ -1073,6 +1139,179 @@ def run_frame(args, W):
     dist_teardown()
 
 
+def run_scene(args, W):
+    """One step = one frame of a resident multi-element scene, as glFinish
+    runs it: srt_scene_build (RenderGraph::Build), srt_camera_rays,
+    srt_scene_trace, srt_framebuffer_write (RGBA8 + depth).  e2e: the same
+    calls with the camera struct as the host input and the colour and depth
+    buffers copied back every frame."""
+    import ctypes as C
+
+    import torch
+
+    import surface_b200 as sb
+    from surface_b200 import _lib
+    from surface_b200 import camera as K
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
+    L = _lib.load()
+    chk = _lib.check
+    ctx = sb.Context(local)
+    ctx.use_torch_stream()
+    E = W["E"]
+    accs, keep = [], []
+    for a in E["accels"]:
+        h = C.c_void_p()
+        kind = {0: _lib.SRT_TRIANGLES, 1: _lib.SRT_TETRAHEDRA, 2: _lib.SRT_SPHERES}[a["kind"]]
+        chk(L.srt_accel_create(ctx.h, kind, C.byref(h)))
+        v = torch.as_tensor(a["verts"], device=dev)
+        if a["kind"] == 2:
+            r = torch.as_tensor(a["radius"], device=dev)
+            chk(L.srt_accel_build_spheres(h, v.data_ptr(), r.data_ptr(), C.c_float(0.0),
+                                          v.shape[0]))
+            keep += [v, r]
+        else:
+            f = torch.as_tensor(a["faces"].view(np.int32), device=dev)
+            build = (L.srt_accel_build_triangles if a["kind"] == 0
+                     else L.srt_accel_build_tetrahedra)
+            chk(build(h, v.data_ptr(), v.shape[0], f.data_ptr(), f.shape[0]))
+            keep += [v, f]
+        accs.append(h)
+    sc = C.c_void_p()
+    chk(L.srt_scene_create(ctx.h, C.byref(sc)))
+    for el in E["elements"]:
+        T = np.ascontiguousarray(el["T"], np.float64).reshape(16)
+        chk(L.srt_scene_add_element(sc, accs[el["accel"]], T.ctypes.data, None))
+    cam = K.make_camera(**W["cam"])
+    nr = W["cam"]["width"] * W["cam"]["height"]
+    rays = torch.empty((nr, 8), device=dev)
+    pix = torch.empty((nr,), dtype=torch.int32, device=dev)
+    hits = torch.empty((nr, 4), device=dev)
+    elem = torch.empty((nr,), dtype=torch.int32, device=dev)
+    color = torch.zeros((cam.height, cam.width, 4), dtype=torch.uint8, device=dev)
+    depth = torch.zeros((cam.height, cam.width), device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    cnt = C.c_uint32()
+    ev = [[torch.cuda.Event(enable_timing=True) for _ in range(5)] for _ in range(args.steps)]
+
+    def step(e=None, stats=None):
+        if e: e[0].record()
+        chk(L.srt_scene_build(sc))
+        if e: e[1].record()
+        chk(L.srt_camera_rays(ctx.h, C.byref(cam), rays.data_ptr(), pix.data_ptr(),
+                              C.byref(cnt)))
+        if e: e[2].record()
+        chk(L.srt_scene_trace(sc, rays.data_ptr(), cnt.value, None, None, hits.data_ptr(),
+                              elem.data_ptr(), stats))
+        if e: e[3].record()
+        chk(L.srt_framebuffer_write(ctx.h, C.byref(cam), hits.data_ptr(), pix.data_ptr(),
+                                    None, cnt.value, 0, color.data_ptr(), depth.data_ptr()))
+        if e: e[4].record()
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    chk(L.srt_ctx_synchronize(ctx.h))  # surfaces any kernel limit flag
+    st = torch.zeros(5, dtype=torch.int64, device=dev)
+    step(None, st.data_ptr())
+    torch.cuda.synchronize()
+    stats = st.cpu().numpy().astype(np.float64)
+    barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
+        launches0 = L.srt_ctx_launch_count(ctx.h)
+        for k in range(args.steps):
+            flush.zero_()
+            step(ev[k])
+        torch.cuda.synchronize()
+        launches = L.srt_ctx_launch_count(ctx.h) - launches0
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
+    barrier()
+    chk(L.srt_ctx_synchronize(ctx.h))
+    parts = [[e[j].elapsed_time(e[j + 1]) for e in ev] for j in range(4)]
+    total = max_over_ranks([sum(sum(p) for p in parts)], dev)[0]
+    ms_per_step = total / args.steps
+    value = whole_job_mrays(nr, world, ms_per_step)
+
+    h_color = torch.empty_like(color, device="cpu").pin_memory()
+    h_depth = torch.empty_like(depth, device="cpu").pin_memory()
+
+    def e2e_step():
+        step()
+        h_color.copy_(color, non_blocking=True)
+        h_depth.copy_(depth, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+
+    hbm, src = peaks()
+    ntop, nwalk, br, lf, pr = (float(x) / nr for x in stats)
+    # ray (32) + hit (16) + element (4) + top-level nodes (72) + per element
+    # walk its record (3 matrices, 400) + branch nodes (64) + primitive
+    # records (48: the triangle size; tets 52, spheres 20)
+    bpr = 32 + 16 + 4 + 72 * ntop + 400 * nwalk + 64 * br + 48 * pr
+    tr_ms = statistics.mean(parts[2])
+    achieved = bpr * nr / (tr_ms * 1e-3) / 1e9
+    roofline = {"bound": "hbm", "kernel": "scene_trace_kernel", "achieved": round(achieved, 1),
+                "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
+                "peak_source": src, "traffic": None,
+                "algorithmic_bytes_per_ray": round(bpr, 1),
+                "visits_per_ray": {"top_nodes": round(ntop, 3), "element_walks": round(nwalk, 3),
+                                   "branch": round(br, 3), "leaf": round(lf, 3),
+                                   "prims": round(pr, 3)}}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        vals = [cpu_reference_scene(W) for _ in range(3)]
+        cv, ctr, ctt, cns, ck = sorted(vals)[1]
+        cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(), "kind": ck,
+               "build_rays_write_s": round(ctr, 4), "trace_s": round(ctt, 4),
+               "sample": f"top-level build, eye rays and write of every pixel; scene trace "
+                         f"of every 4th pixel ({cns} rays, OpenMP) scaled to all; median "
+                         f"of 3, CPU restatement"}
+    L.srt_scene_destroy(sc)
+    for h in accs:
+        L.srt_accel_destroy(h)
+    if rank == 0:
+        line = {
+            "metric": METRIC_SCENE, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": DTYPE["scene"],
+            "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)",
+                           parallelism=f"replicas x{world}"),
+            "top_build_ms": round(statistics.mean(parts[0]), 4),
+            "camera_rays_ms": round(statistics.mean(parts[1]), 4),
+            "trace_ms": round(tr_ms, 4),
+            "framebuffer_write_ms": round(statistics.mean(parts[3]), 4),
+            "clocks": clk.summary(),
+            "e2e": {"value": round(whole_job_mrays(nr, world, e2e_ms), 3), "unit": "Mrays/s",
+                    "h2d_bytes_per_step": C.sizeof(cam),
+                    "d2h_bytes_per_step": int(h_color.numel() + 4 * h_depth.numel()),
+                    "ms_per_step": round(e2e_ms, 3)},
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    dist_teardown()
+
+
 # ---------------------------------------------------------------- GPU arm
 def run_ours(args, W):
     import torch
@@ -1259,7 +1498,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
-                    choices=["tet", "tri", "particles", "volume", "batched", "frame"])
+                    choices=["tet", "tri", "particles", "volume", "batched", "frame",
+                             "scene"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -1281,6 +1521,8 @@ def main():
         run_particles(args, W)
     elif args.workload == "frame":
         run_frame(args, W)
+    elif args.workload == "scene":
+        run_scene(args, W)
     else:
         run_ours(args, W)
 

@@ -331,6 +331,53 @@ SRT_API srt_status srt_framebuffer_write(srt_ctx *ctx, const srt_camera *cam,
                                          int32_t format, void *color,
                                          float *depth);
 
+/* ---- scenes: several accels with transforms ----------------------------- */
+/* RenderGraph (gles/gles_render_graph.cc:104-314) on the GPU: built accels
+ * placed in the world by 4x4 transforms, a top-level tree over their world
+ * boxes (BVHTree, render/render_bvh_tree.cc), and the nearest hit over all
+ * of them per ray.  Matrices are doubles in Matrixd's layout (m[row][col],
+ * p' = p m + m[3]); the caller passes T, its inverse, the inverse of its
+ * upper 3x3 and the world box, as RenderElement::Update computes them. */
+typedef struct srt_scene srt_scene;
+SRT_API srt_status srt_scene_create(srt_ctx *ctx, srt_scene **out);
+SRT_API srt_status srt_scene_destroy(srt_scene *scene);
+/* Add a built accel of the scene's context; *id (optional) = its element id
+ * (0, 1, ... in call order).  Accels must stay built and unchanged while the
+ * scene is used; rebuild the scene after rebuilding one of them. */
+SRT_API srt_status srt_scene_add(srt_scene *scene, srt_accel *accel,
+                                 const double T[16], const double invT[16],
+                                 const double invT33[16],
+                                 const double world_bmin[3],
+                                 const double world_bmax[3], uint32_t *id);
+/* The same, as RenderElement's constructor does it (gles/gles_primitive.cc:
+ * 346, gles/gles_render_graph.cc:77-101): local box = srt_accel_bbox, world
+ * box of its eight corners under T, invT and invT33 by Matrixd::Inverse's
+ * cofactor rule -- bit for bit the reference's values. */
+SRT_API srt_status srt_scene_add_element(srt_scene *scene, srt_accel *accel,
+                                         const double T[16], uint32_t *id);
+/* Matrixd::Inverse (render/render_matrix.h:40-134) of a row-major 4x4, in
+ * place (host only). */
+SRT_API void srt_matrix_inverse(double m[16]);
+/* RenderGraph::Build: the top-level tree (BVHTree::BuildTree). */
+SRT_API srt_status srt_scene_build(srt_scene *scene);
+/* RenderGraph::Trace for n rays (device arrays): hits in world distance t
+ * (u, v, prim of the element's own hit), element[i] (optional) = the hit
+ * element or 0xFFFFFFFF.  prev_element (optional): the element each ray's
+ * prev_prim belongs to (the self-hit rule applies only there), with
+ * prev_normals (optional, 3 floats per ray) for spheres.  stats (optional,
+ * device, 5 counters added to): top-level nodes visited, element walks,
+ * branch nodes, leaves and primitives visited inside the elements.
+ * Up to 64 candidate elements per ray (SRT_ERR_LIMIT beyond).  Asynchronous. */
+SRT_API srt_status srt_scene_trace(srt_scene *scene, const srt_ray *rays,
+                                   size_t n, const uint32_t *prev_element,
+                                   const float *prev_normals, srt_hit *hits,
+                                   uint32_t *element, uint64_t *stats);
+/* The top-level tree: per node bmin[3], bmax[3] (boxes, 6 doubles) and
+ * child0, child1, axis, leaf, element (ints, 5 int32); returns the node
+ * count (arrays may be NULL or shorter: cap entries are filled). */
+SRT_API size_t srt_scene_top_nodes(srt_scene *scene, double *boxes,
+                                   int32_t *ints, size_t cap);
+
 /* ---- secondary rays ----------------------------------------------------- */
 /* One secondary ray per hit ray (the particle workload's bounce; in the
  * reference a fragment shader builds it and calls back trace() with

@@ -97,6 +97,16 @@ def lib():
         L.so_camera_rays.argtypes = [_P, _P, _P, _P]
         L.so_framebuffer_write.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, _SZ,
                                            C.c_int, _P, _P]
+        L.so_matrix_inverse.argtypes = [_P]
+        L.so_element_update.argtypes = [_P, _P, _P, _P, _P, _P, _P]
+        L.so_scene_build.restype = _P
+        L.so_scene_build.argtypes = [_P, _P, _P, _P, _P, _P, _SZ]
+        L.so_scene_free.argtypes = [_P]
+        L.so_scene_top_nodes.restype = _SZ
+        L.so_scene_top_nodes.argtypes = [_P, _P, _P, _SZ]
+        L.so_scene_candidates.restype = _SZ
+        L.so_scene_candidates.argtypes = [_P, _P, _P, _P, _P, _SZ]
+        L.so_scene_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, C.c_int]
         _ORACLE = L
     return _ORACLE
 
@@ -144,6 +154,14 @@ def ref():
                                            C.c_uint64, _SZ, _P]
         L.ref_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int,
                                        _P]
+        L.ref_matrix_inverse.argtypes = [_P]
+        L.ref_bvh_build.restype = _P
+        L.ref_bvh_build.argtypes = [_P, _P, _P, _SZ]
+        L.ref_bvh_free.argtypes = [_P]
+        L.ref_bvh_nodes.restype = _SZ
+        L.ref_bvh_nodes.argtypes = [_P, _P, _P, _SZ]
+        L.ref_bvh_trace.restype = _SZ
+        L.ref_bvh_trace.argtypes = [_P, _P, _P, _P, _P, _SZ]
         _REF = L
     return _REF
 
@@ -182,6 +200,11 @@ class OracleAccel:
                         _ptr(scene), C.byref(eps))
         self.scene_bmin, self.scene_bmax = scene[:3].copy(), scene[3:].copy()
         self.eps_scale = eps.value
+
+    def bbox64(self):
+        """XxxAccel::BoundingBox: the root node's box, as doubles."""
+        return (self.nodes["bmin"][0].astype(np.float64),
+                self.nodes["bmax"][0].astype(np.float64))
 
     def karras(self):
         m = self.n - 1
@@ -583,3 +606,118 @@ def framebuffer_write(cam, hits, pixel, rgba=None, fmt=0, color=None, depth=None
                                None if rg is None else _ptr(rg), hits.size, fmt,
                                _ptr(color), _ptr(depth))
     return color, depth
+
+
+# ------------------------------------------------------------------- scenes
+def _top_arrays(fn, h, cap):
+    boxes = np.zeros((cap, 6), np.float64)
+    ints = np.zeros((cap, 5), np.int32)
+    n = fn(h, _ptr(boxes), _ptr(ints), cap)
+    return boxes[:n].copy(), ints[:n].copy()
+
+
+def matrix_inverse(m, use_ref=False):
+    """Matrixd::Inverse of a row-major 4x4: the restatement, or with use_ref
+    the reference's own."""
+    a = np.array(m, np.float64).reshape(16).copy()
+    (ref().ref_matrix_inverse if use_ref else lib().so_matrix_inverse)(_ptr(a))
+    return a.reshape(4, 4)
+
+
+def element_update(T, lbmin, lbmax):
+    """RenderElement::Update: (invT, invT33, world bmin, world bmax)."""
+    T = np.ascontiguousarray(T, np.float64).reshape(16)
+    lo = np.ascontiguousarray(lbmin, np.float64)
+    hi = np.ascontiguousarray(lbmax, np.float64)
+    iT, iT33 = np.zeros(16), np.zeros(16)
+    wlo, whi = np.zeros(3), np.zeros(3)
+    lib().so_element_update(_ptr(T), _ptr(lo), _ptr(hi), _ptr(iT), _ptr(iT33), _ptr(wlo),
+                            _ptr(whi))
+    return iT.reshape(4, 4), iT33.reshape(4, 4), wlo, whi
+
+
+class RefTopTree:
+    """The reference's own BVHTree (render/render_bvh_tree.cc) over world
+    boxes: node arrays and per-ray candidate lists."""
+
+    def __init__(self, bmin, bmax, ids=None):
+        self.bmin = np.ascontiguousarray(bmin, np.float64).reshape(-1, 3)
+        self.bmax = np.ascontiguousarray(bmax, np.float64).reshape(-1, 3)
+        n = self.bmin.shape[0]
+        self.ids = (np.arange(n, dtype=np.uint32) if ids is None
+                    else np.ascontiguousarray(ids, np.uint32))
+        self.h = ref().ref_bvh_build(_ptr(self.bmin), _ptr(self.bmax), _ptr(self.ids), n)
+        self.cap = 2 * n + 2
+
+    def nodes(self):
+        return _top_arrays(ref().ref_bvh_nodes, self.h, self.cap)
+
+    def candidates(self, org, dir_):
+        o = np.ascontiguousarray(org, np.float64)
+        d = np.ascontiguousarray(dir_, np.float64)
+        cap = self.bmin.shape[0] + 1
+        tt = np.zeros((cap, 2), np.float64)
+        ids = np.zeros(cap, np.uint32)
+        n = ref().ref_bvh_trace(self.h, _ptr(o), _ptr(d), _ptr(tt), _ptr(ids), cap)
+        return tt[:n, 0].copy(), ids[:n].copy()
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                ref().ref_bvh_free(self.h)
+                self.h = None
+        except Exception:
+            pass
+
+
+class OracleScene:
+    """RenderGraph::Build / Trace restated (so_scene_*): elements are
+    OracleAccel objects with their transforms (4x4 row-major doubles as
+    Matrixd's m[row][col]) and world boxes."""
+
+    def __init__(self, accels, T, invT, invT33, bmin, bmax):
+        self.accels = list(accels)  # None entries: top-level tree only
+        n = len(self.accels)
+        self._T = np.ascontiguousarray(T, np.float64).reshape(n, 16)
+        self._iT = np.ascontiguousarray(invT, np.float64).reshape(n, 16)
+        self._iT33 = np.ascontiguousarray(invT33, np.float64).reshape(n, 16)
+        self._bmin = np.ascontiguousarray(bmin, np.float64).reshape(n, 3)
+        self._bmax = np.ascontiguousarray(bmax, np.float64).reshape(n, 3)
+        hs = (C.c_void_p * n)(*[None if a is None else a.h for a in self.accels])
+        self.h = lib().so_scene_build(hs, _ptr(self._T), _ptr(self._iT), _ptr(self._iT33),
+                                      _ptr(self._bmin), _ptr(self._bmax), n)
+        self.cap = 2 * n + 2
+
+    def nodes(self):
+        return _top_arrays(lib().so_scene_top_nodes, self.h, self.cap)
+
+    def candidates(self, org, dir_):
+        o = np.ascontiguousarray(org, np.float64)
+        d = np.ascontiguousarray(dir_, np.float64)
+        cap = len(self.accels) + 1
+        tt = np.zeros(cap, np.float64)
+        ids = np.zeros(cap, np.uint32)
+        n = lib().so_scene_candidates(self.h, _ptr(o), _ptr(d), _ptr(tt), _ptr(ids), cap)
+        return tt[:n].copy(), ids[:n].copy()
+
+    def trace(self, rays, prev_element=None, prev_normals=None, nthreads=0):
+        """(hits, element): hit t is the world distance, prim / u / v the
+        element's own; element MISS where nothing was hit."""
+        if any(a is None for a in self.accels):
+            raise ValueError("scene built without accels")
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        el = np.zeros(rays.size, np.uint32)
+        pe = None if prev_element is None else np.ascontiguousarray(prev_element, np.uint32)
+        pn = None if prev_normals is None else np.ascontiguousarray(prev_normals, np.float32)
+        lib().so_scene_trace(self.h, _ptr(rays), rays.size, _ptr(pe), _ptr(pn), _ptr(hits),
+                             _ptr(el), nthreads)
+        return hits, el
+
+    def __del__(self):
+        try:
+            if getattr(self, "h", None):
+                lib().so_scene_free(self.h)
+                self.h = None
+        except Exception:
+            pass

@@ -14,6 +14,7 @@
 //                          (render/render_prefix_tree_util.h)
 //   FilterTexture3DFloat   (render/render_texture.h)
 //   Camera::buildFrame     (render/render_camera.h)
+//   BVHTree                (render/render_bvh_tree.h, RenderGraph's top level)
 //   tinymt64_*             (render/tinymt64.h)
 #include <fcntl.h>
 #include <omp.h>
@@ -22,12 +23,15 @@
 #include <string.h>
 #include <unistd.h>
 
+#include <limits>
 #include <vector>
 
 #include "render_accel_particle.h"
 #include "render_accel_tetra.h"
 #include "render_accel_triangle.h"
+#include "render_bvh_tree.h"
 #include "render_camera.h"
+#include "render_matrix.h"
 #include "render_prefix_tree_util.h"
 #include "render_texture.h"
 #include "tinymt64.h"
@@ -358,4 +362,66 @@ REF_API void ref_camera_frame(const float eye[3], const float lookat[3], const f
     out[3 + k] = u[k];
     out[6 + k] = v[k];
   }
+}
+
+// BVHTree (render/render_bvh_tree.cc), the top-level tree of RenderGraph.
+REF_API void *ref_bvh_build(const double *bmin, const double *bmax, const uint32_t *ids,
+                            size_t n) {
+  BVHTree *t = new BVHTree();
+  for (size_t i = 0; i < n; i++) {
+    BVHData d;
+    for (int k = 0; k < 3; k++) {
+      d.bmin[k] = bmin[3 * i + k];
+      d.bmax[k] = bmax[3 * i + k];
+    }
+    d.nodeID = ids[i];
+    t->AddNode(d);
+  }
+  t->BuildTree();
+  return t;
+}
+
+REF_API void ref_bvh_free(void *p) { delete static_cast<BVHTree *>(p); }
+
+// Node array: per node bmin[3], bmax[3] (doubles) and child0, child1, axis,
+// isLeaf, nodeID (ints).  Returns the node count (arrays sized by the caller).
+REF_API size_t ref_bvh_nodes(void *p, double *boxes, int32_t *ints, size_t cap) {
+  const std::vector<BVHNode> &nt = static_cast<BVHTree *>(p)->GetNodesTree();
+  for (size_t i = 0; i < nt.size() && i < cap; i++) {
+    for (int k = 0; k < 3; k++) {
+      boxes[6 * i + k] = nt[i].bmin[k];
+      boxes[6 * i + 3 + k] = nt[i].bmax[k];
+    }
+    ints[5 * i + 0] = nt[i].child[0];
+    ints[5 * i + 1] = nt[i].child[1];
+    ints[5 * i + 2] = nt[i].axis;
+    ints[5 * i + 3] = nt[i].isLeaf ? 1 : 0;
+    ints[5 * i + 4] = (int32_t)nt[i].nodeID;
+  }
+  return nt.size();
+}
+
+// Sorted candidate list of one ray: (tMin, tMax) pairs and node ids.
+REF_API size_t ref_bvh_trace(void *p, const double org[3], const double dir[3],
+                             double *tminmax, uint32_t *ids, size_t cap) {
+  StackVector<BVHNodeIntersection, 32> isects;
+  double o[3] = {org[0], org[1], org[2]}, d[3] = {dir[0], dir[1], dir[2]};
+  static_cast<BVHTree *>(p)->Trace(isects, o, d, (std::numeric_limits<double>::max)());
+  size_t n = isects->size();
+  for (size_t i = 0; i < n && i < cap; i++) {
+    tminmax[2 * i] = isects[i].tMin;
+    tminmax[2 * i + 1] = isects[i].tMax;
+    ids[i] = isects[i].nodeID;
+  }
+  return n;
+}
+
+// Matrixd::Inverse of a row-major 4x4 (render/render_matrix.h), in place.
+REF_API void ref_matrix_inverse(double *m16) {
+  double m[4][4];
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) m[r][c] = m16[4 * r + c];
+  Matrixd::Inverse(m);
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) m16[4 * r + c] = m[r][c];
 }

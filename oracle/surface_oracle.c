@@ -1873,3 +1873,407 @@ SO_API void so_framebuffer_write(int width, int height, int step, const so_hit *
     }
   }
 }
+
+/* ======================================================== scenes
+ * RenderGraph::Build / Trace (gles/gles_render_graph.cc:104-314) over
+ * elements = (accel, T, invT, invT33, world box), restated:
+ *   - BVHTree::BuildTree / ConstructTree (render/render_bvh_tree.cc:319-500):
+ *     spatial median on the longest axis (axis retries in the order
+ *     {0,1,2},{1,2,0},{2,0,1}), PartitionNodes' in-place swap order
+ *     (:83-130), object median fallback, child boxes widened by 1e-6 of their
+ *     extent, root = the unwidened scene box;
+ *   - BVHTree::Trace (:504-585): SetupRay's reciprocals (|d| <= 2e-15 gives
+ *     +-FLT_MAX), TestRayAABB in double, leaves tested with their own box,
+ *     near child by ray sign first, candidates sorted by entry distance
+ *     (std::sort: insertion sort, stable, for up to 16 candidates);
+ *   - per candidate: skipped when beyond the nearest world hit so far;
+ *     local ray by Matrixd::MultV with invT / invT33 (double) stored as
+ *     float; the element's reference walk; world point by MultV with T of
+ *     the float local point; world distance = float length; strictly nearer
+ *     wins.  prev_prim / prev_t / prev_normal apply only in prev_element. */
+typedef struct {
+  double bmin[3], bmax[3];
+  int child[2], axis, leaf;
+  uint32_t id;
+} so_top;
+
+typedef struct {
+  double bmin[3], bmax[3];
+  uint32_t id;
+} so_topdata;
+
+typedef struct {
+  size_t n, nn, cap;
+  const so_accel **acc;
+  double *T, *invT, *invT33;
+  so_top *nodes;
+} so_scene;
+
+static size_t top_partition(so_topdata *d, size_t l, size_t r, double pos, int axis) {
+  so_topdata leftmost = d[l];
+  size_t pivot = l;
+  for (size_t i = l + 1; i < r; i++) {
+    if (d[i].bmax[axis] < pos) {
+      pivot++;
+      so_topdata t = d[pivot];
+      d[pivot] = d[i];
+      d[i] = t;
+    }
+  }
+  d[l] = d[pivot];
+  d[pivot] = leftmost;
+  size_t split = l;
+  for (size_t i = l; i < r; i++)
+    if (d[i].bmax[axis] < pos) split++;
+  return split;
+}
+
+static void top_box(const so_topdata *d, size_t s, size_t e, double bmin[3], double bmax[3]) {
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = d[s].bmin[k];
+    bmax[k] = d[s].bmax[k];
+  }
+  for (size_t i = s + 1; i < e; i++)
+    for (int k = 0; k < 3; k++) {
+      if (d[i].bmin[k] < bmin[k]) bmin[k] = d[i].bmin[k];
+      if (bmax[k] < d[i].bmax[k]) bmax[k] = d[i].bmax[k];
+    }
+}
+
+static size_t top_push(so_scene *s, const double bmin[3], const double bmax[3]) {
+  if (s->nn == s->cap) {
+    s->cap = s->cap ? 2 * s->cap : 16;
+    s->nodes = (so_top *)realloc(s->nodes, s->cap * sizeof(so_top));
+  }
+  so_top *t = &s->nodes[s->nn];
+  memset(t, 0, sizeof(*t));
+  for (int k = 0; k < 3; k++) {
+    t->bmin[k] = bmin[k];
+    t->bmax[k] = bmax[k];
+  }
+  return s->nn++;
+}
+
+static void top_construct(so_scene *s, so_topdata *d, size_t root, size_t l, size_t r) {
+  static const int axl[3][3] = {{0, 1, 2}, {1, 2, 0}, {2, 0, 1}};
+  const size_t n = r - l;
+  if (n == 1) {
+    s->nodes[root].leaf = 1;
+    s->nodes[root].child[0] = s->nodes[root].child[1] = 0;
+    s->nodes[root].id = d[l].id;
+    return;
+  }
+  double bsize[3], bmin[3];
+  for (int k = 0; k < 3; k++) {
+    bsize[k] = s->nodes[root].bmax[k] - s->nodes[root].bmin[k];
+    bmin[k] = s->nodes[root].bmin[k];
+  }
+  double maxlen = bsize[0];
+  int at = 0;
+  if (maxlen < bsize[1]) {
+    maxlen = bsize[1];
+    at = 1;
+  }
+  if (maxlen < bsize[2]) {
+    maxlen = bsize[2];
+    at = 2;
+  }
+  size_t split = l, nl = 0, nr = n;
+  int axis = 0;
+  for (int i = 0; i < 3; i++) {
+    axis = axl[at][i];
+    split = top_partition(d, l, r, bmin[axis] + bsize[axis] * 0.5, axis);
+    if (split != l && split != r) {
+      nl = split - l;
+      nr = n - nl;
+      break;
+    }
+  }
+  if (split == l || split == r) {
+    nl = n / 2;
+    nr = n - nl;
+    split = l + (r - l) / 2;
+  }
+  s->nodes[root].axis = axis;
+  s->nodes[root].leaf = 0;
+  for (int side = 0; side < 2; side++) {
+    const size_t cnt = side ? nr : nl;
+    if (!cnt) {
+      s->nodes[root].child[side] = 0;
+      continue;
+    }
+    const size_t a = side ? split : l, b = side ? r : split;
+    double cb[3], ce[3];
+    top_box(d, a, b, cb, ce);
+    for (int k = 0; k < 3; k++) {
+      double ext = ce[k] - cb[k];
+      cb[k] = cb[k] - ext * 1.0e-6;
+      ce[k] = ce[k] + ext * 1.0e-6;
+    }
+    size_t child = top_push(s, cb, ce);
+    s->nodes[root].child[side] = (int)child;
+    top_construct(s, d, child, a, b);
+  }
+}
+
+SO_API so_scene *so_scene_build(const so_accel *const *acc, const double *T,
+                                const double *invT, const double *invT33, const double *bmin,
+                                const double *bmax, size_t n) {
+  so_scene *s = (so_scene *)calloc(1, sizeof(so_scene));
+  s->n = n;
+  s->acc = (const so_accel **)malloc(n * sizeof(*s->acc));
+  s->T = (double *)malloc(n * 16 * sizeof(double));
+  s->invT = (double *)malloc(n * 16 * sizeof(double));
+  s->invT33 = (double *)malloc(n * 16 * sizeof(double));
+  memcpy(s->acc, acc, n * sizeof(*s->acc));
+  memcpy(s->T, T, n * 16 * sizeof(double));
+  memcpy(s->invT, invT, n * 16 * sizeof(double));
+  memcpy(s->invT33, invT33, n * 16 * sizeof(double));
+  so_topdata *d = (so_topdata *)malloc(n * sizeof(so_topdata));
+  for (size_t i = 0; i < n; i++) {
+    for (int k = 0; k < 3; k++) {
+      d[i].bmin[k] = bmin[3 * i + k];
+      d[i].bmax[k] = bmax[3 * i + k];
+    }
+    d[i].id = (uint32_t)i;
+  }
+  double sb[3], se[3];
+  top_box(d, 0, n, sb, se);
+  top_push(s, sb, se);
+  top_construct(s, d, 0, 0, n);
+  free(d);
+  return s;
+}
+
+SO_API void so_scene_free(so_scene *s) {
+  if (!s) return;
+  free(s->acc);
+  free(s->T);
+  free(s->invT);
+  free(s->invT33);
+  free(s->nodes);
+  free(s);
+}
+
+SO_API size_t so_scene_top_nodes(const so_scene *s, double *boxes, int32_t *ints, size_t cap) {
+  for (size_t i = 0; i < s->nn && i < cap; i++) {
+    for (int k = 0; k < 3; k++) {
+      boxes[6 * i + k] = s->nodes[i].bmin[k];
+      boxes[6 * i + 3 + k] = s->nodes[i].bmax[k];
+    }
+    ints[5 * i + 0] = s->nodes[i].child[0];
+    ints[5 * i + 1] = s->nodes[i].child[1];
+    ints[5 * i + 2] = s->nodes[i].axis;
+    ints[5 * i + 3] = s->nodes[i].leaf;
+    ints[5 * i + 4] = (int32_t)s->nodes[i].id;
+  }
+  return s->nn;
+}
+
+static int top_aabb(const so_top *t, const double o[3], const double inv[3], const int sgn[3],
+                    double *tmin, double *tmax) {
+  double mn[3], mx[3];
+  for (int k = 0; k < 3; k++) {
+    mn[k] = sgn[k] ? t->bmax[k] : t->bmin[k];
+    mx[k] = sgn[k] ? t->bmin[k] : t->bmax[k];
+  }
+  const double tminx = (mn[0] - o[0]) * inv[0], tmaxx = (mx[0] - o[0]) * inv[0];
+  const double tminy = (mn[1] - o[1]) * inv[1], tmaxy = (mx[1] - o[1]) * inv[1];
+  double a = (tminx > tminy) ? tminx : tminy;
+  double b = (tmaxx < tmaxy) ? tmaxx : tmaxy;
+  const double tminz = (mn[2] - o[2]) * inv[2], tmaxz = (mx[2] - o[2]) * inv[2];
+  a = (a > tminz) ? a : tminz;
+  b = (b < tmaxz) ? b : tmaxz;
+  if ((b > 0.0) && (a <= b)) {
+    *tmin = a;
+    *tmax = b;
+    return 1;
+  }
+  return 0;
+}
+
+/* candidates of one ray in sorted order; returns their number */
+SO_API size_t so_scene_candidates(const so_scene *s, const double o[3], const double dir[3],
+                                  double *ct, uint32_t *cid, size_t cap) {
+  int sgn[3];
+  double inv[3];
+  for (int k = 0; k < 3; k++) {
+    sgn[k] = dir[k] < 0.0 ? 1 : 0;
+    inv[k] = fabs(dir[k]) > 2.0e-15 ? 1.0 / dir[k] : (dir[k] < 0.0 ? -FLT_MAX : FLT_MAX);
+  }
+  size_t nc = 0;
+  int stk[256], sp = 0, node = 0;
+  for (;;) {
+    const so_top *t = &s->nodes[node];
+    if (t->leaf) {
+      double a, b;
+      if (top_aabb(t, o, inv, sgn, &a, &b) && nc < cap) {
+        ct[nc] = a;
+        cid[nc] = t->id;
+        nc++;
+      }
+      if (sp < 1) break;
+      node = stk[--sp];
+    } else {
+      double a0 = 0, b0 = 0, a1 = 0, b1 = 0;
+      int h0 = t->child[0] > 0 && top_aabb(&s->nodes[t->child[0]], o, inv, sgn, &a0, &b0);
+      int h1 = t->child[1] > 0 && top_aabb(&s->nodes[t->child[1]], o, inv, sgn, &a1, &b1);
+      if (!h0 && !h1) {
+        if (sp < 1) break;
+        node = stk[--sp];
+      } else if (h0 && !h1) {
+        node = t->child[0];
+      } else if (h1 && !h0) {
+        node = t->child[1];
+      } else {
+        int order = sgn[t->axis];
+        stk[sp++] = t->child[1 - order];
+        node = t->child[order];
+      }
+    }
+  }
+  for (size_t a = 1; a < nc; a++) { /* stable insertion sort */
+    double kt = ct[a];
+    uint32_t kid = cid[a];
+    size_t b = a;
+    while (b > 0 && kt < ct[b - 1]) {
+      ct[b] = ct[b - 1];
+      cid[b] = cid[b - 1];
+      b--;
+    }
+    ct[b] = kt;
+    cid[b] = kid;
+  }
+  return nc;
+}
+
+static void scene_multv(const double *m, const double v[3], double o[3]) {
+  for (int k = 0; k < 3; k++) o[k] = ((m[k] * v[0] + m[4 + k] * v[1]) + m[8 + k] * v[2]) + m[12 + k];
+}
+
+SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
+                           const uint32_t *prev_element, const float *prev_normals,
+                           so_hit *hits, uint32_t *element, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel for schedule(dynamic, 64)
+#endif
+  for (long ii = 0; ii < (long)n; ii++) {
+    const size_t i = (size_t)ii;
+    const so_ray *r = &rays[i];
+    const double ro[3] = {r->org[0], r->org[1], r->org[2]};
+    const double rd[3] = {r->dir[0], r->dir[1], r->dir[2]};
+    double ct[64];
+    uint32_t cid[64];
+    size_t nc = so_scene_candidates(s, ro, rd, ct, cid, 64);
+    double tnear = DBL_MAX;
+    so_hit best = {FLT_MAX, 0.0f, 0.0f, 0xffffffffu};
+    uint32_t be = 0xffffffffu;
+    for (size_t c = 0; c < nc; c++) {
+      if (tnear < ct[c]) continue;
+      const uint32_t e = cid[c];
+      double lo[3], ld[3];
+      scene_multv(&s->invT[16 * e], ro, lo);
+      scene_multv(&s->invT33[16 * e], rd, ld);
+      const int same = prev_element && prev_element[i] == e;
+      so_ray lr;
+      for (int k = 0; k < 3; k++) {
+        lr.org[k] = (float)lo[k];
+        lr.dir[k] = (float)ld[k];
+      }
+      lr.prev_prim = same ? r->prev_prim : 0xffffffffu;
+      lr.prev_t = same ? r->prev_t : 0.0f;
+      float zero3[3] = {0, 0, 0};
+      const float *pn = (same && prev_normals) ? &prev_normals[3 * i] : zero3;
+      so_hit h;
+      so_stats st = {0, 0, 0};
+      trace_one(s->acc[e], &lr, pn, &h, NULL, NULL, NULL, &st);
+      if (h.prim == 0xffffffffu || !(h.t < FLT_MAX)) continue;
+      double lp[3], wp[3];
+      for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)h.t * ld[k]);
+      scene_multv(&s->T[16 * e], lp, wp);
+      float po[3];
+      for (int k = 0; k < 3; k++) po[k] = (float)wp[k] - r->org[k];
+      const float tw = sqrtf(po[0] * po[0] + po[1] * po[1] + po[2] * po[2]);
+      if ((double)tw < tnear) {
+        tnear = tw;
+        best = h;
+        best.t = tw;
+        be = e;
+      }
+    }
+    hits[i] = best;
+    if (element) element[i] = be;
+  }
+}
+
+/* Matrixd::Inverse (render/render_matrix.h:40-134), written out entry by
+ * entry in the routine's operation order (s = m transposed; the m[3][3]
+ * entry keeps the reference's s[0] factor). */
+SO_API void so_matrix_inverse(double m[16]) {
+  double s[16], p[12];
+  for (int r = 0; r < 4; r++)
+    for (int c = 0; c < 4; c++) s[4 * c + r] = m[4 * r + c];
+#define PAIRS(o)                                                               \
+  p[0] = s[10 - o] * s[15 - o]; p[1] = s[11 - o] * s[14 - o];                  \
+  p[2] = s[9 - o] * s[15 - o];  p[3] = s[11 - o] * s[13 - o];                  \
+  p[4] = s[9 - o] * s[14 - o];  p[5] = s[10 - o] * s[13 - o];                  \
+  p[6] = s[8 - o] * s[15 - o];  p[7] = s[11 - o] * s[12 - o];                  \
+  p[8] = s[8 - o] * s[14 - o];  p[9] = s[10 - o] * s[12 - o];                  \
+  p[10] = s[8 - o] * s[13 - o]; p[11] = s[9 - o] * s[12 - o];
+#define E(e, a0, b0, a1, b1, a2, b2, c0, d0, c1, d1, c2, d2)                   \
+  m[e] = p[a0] * s[b0] + p[a1] * s[b1] + p[a2] * s[b2];                        \
+  m[e] -= p[c0] * s[d0] + p[c1] * s[d1] + p[c2] * s[d2];
+  PAIRS(0)
+  E(0, 0, 5, 3, 6, 4, 7, 1, 5, 2, 6, 5, 7)
+  E(1, 1, 4, 6, 6, 9, 7, 0, 4, 7, 6, 8, 7)
+  E(2, 2, 4, 7, 5, 10, 7, 3, 4, 6, 5, 11, 7)
+  E(3, 5, 4, 8, 5, 11, 6, 4, 4, 9, 5, 10, 6)
+  E(4, 1, 1, 2, 2, 5, 3, 0, 1, 3, 2, 4, 3)
+  E(5, 0, 0, 7, 2, 8, 3, 1, 0, 6, 2, 9, 3)
+  E(6, 3, 0, 6, 1, 11, 3, 2, 0, 7, 1, 10, 3)
+  E(7, 4, 0, 9, 1, 10, 2, 5, 0, 8, 1, 11, 2)
+  PAIRS(8)
+  E(8, 0, 13, 3, 14, 4, 15, 1, 13, 2, 14, 5, 15)
+  E(9, 1, 12, 6, 14, 9, 15, 0, 12, 7, 14, 8, 15)
+  E(10, 2, 12, 7, 13, 10, 15, 3, 12, 6, 13, 11, 15)
+  E(11, 5, 12, 8, 13, 11, 14, 4, 12, 9, 13, 10, 14)
+  E(12, 2, 10, 5, 11, 1, 9, 4, 11, 0, 9, 3, 10)
+  E(13, 8, 11, 0, 8, 7, 10, 6, 10, 9, 11, 1, 8)
+  E(14, 6, 9, 11, 11, 3, 8, 10, 11, 2, 8, 7, 9)
+  E(15, 10, 10, 4, 8, 9, 9, 8, 9, 11, 0, 5, 8)
+#undef E
+#undef PAIRS
+  double det = s[0] * m[0] + s[1] * m[1] + s[2] * m[2] + s[3] * m[3];
+  det = 1.0 / det;
+  for (int e = 0; e < 16; e++) m[e] *= det;
+}
+
+/* RenderElement::Update (gles/gles_render_graph.cc:17-101): world box of
+ * the local box's corners (corner order of TransformBoundingBox), invT,
+ * invT33 (T without translation, inverted). */
+SO_API void so_element_update(const double T[16], const double lbmin[3], const double lbmax[3],
+                              double invT[16], double invT33[16], double wbmin[3],
+                              double wbmax[3]) {
+  for (int c = 0; c < 8; c++) {
+    double v[3], x[3];
+    v[0] = (c & 1) ? lbmax[0] : lbmin[0];
+    v[1] = (c & 2) ? lbmax[1] : lbmin[1];
+    v[2] = (c & 4) ? lbmax[2] : lbmin[2];
+    for (int k = 0; k < 3; k++) x[k] = T[k] * v[0] + T[4 + k] * v[1] + T[8 + k] * v[2] + T[12 + k];
+    for (int k = 0; k < 3; k++) {
+      if (c == 0) {
+        wbmin[k] = x[k];
+        wbmax[k] = x[k];
+      } else {
+        if (!(wbmin[k] < x[k])) wbmin[k] = x[k];
+        if (!(x[k] < wbmax[k])) wbmax[k] = x[k];
+      }
+    }
+  }
+  memcpy(invT, T, 16 * sizeof(double));
+  memcpy(invT33, T, 16 * sizeof(double));
+  so_matrix_inverse(invT);
+  invT33[12] = invT33[13] = invT33[14] = 0.0;
+  so_matrix_inverse(invT33);
+}

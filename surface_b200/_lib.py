@@ -92,6 +92,14 @@ _SIGS = {
     "srt_volume_march_bwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P],
     "srt_spawn_secondary": [_P, _P, _P, _P, _SZ, C.c_uint64, _P, _P, _P],
     "srt_camera_rays": [_P, _P, _P, _P, _P],
+    "srt_scene_create": [_P, C.POINTER(_P)],
+    "srt_scene_destroy": [_P],
+    "srt_scene_add": [_P, _P, _P, _P, _P, _P, _P, _P],
+    "srt_scene_add_element": [_P, _P, _P, _P],
+    "srt_matrix_inverse": [_P],
+    "srt_scene_build": [_P],
+    "srt_scene_trace": [_P, _P, _SZ, _P, _P, _P, _P, _P],
+    "srt_scene_top_nodes": [_P, _P, _P, _SZ],
     "srt_framebuffer_write": [_P, _P, _P, _P, _P, C.c_uint32, C.c_int32, _P, _P],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
@@ -99,6 +107,7 @@ _SIGS = {
     "srt_batch_config": [_P, _P, _P, _P, _P],
 }
 _RESTYPES = {"srt_last_error": C.c_char_p, "srt_ctx_get_stream": _P,
+             "srt_scene_top_nodes": _SZ, "srt_matrix_inverse": None,
              "srt_ctx_launch_count": C.c_uint64}
 
 _lib = None

@@ -176,6 +176,30 @@ srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *d_verts,
                         const uint32_t *d_faces, const float *d_radius,
                         float const_radius, size_t n, uint32_t *d_codes,
                         SceneInfo *d_scene);
+// Top level of a scene (RenderGraph): a node of the reference's BVHTree
+// (render/render_bvh_tree.h:28-43) over the elements' world boxes.
+struct TopNode {
+  double bmin[3], bmax[3];
+  int32_t child[2];  // 0: none
+  int32_t axis, leaf;
+  uint32_t id;       // element of a leaf
+  uint32_t pad;
+};
+// One element of a scene: a built accel and its transforms, 4x4 doubles in
+// the reference's Matrixd layout (m[row][col], p' = p m + m[3]).
+struct SceneElem {
+  int32_t kind;
+  uint32_t nprims;
+  const void *nodes;
+  const float4 *prims;
+  const uint32_t *sidx;
+  const SceneInfo *scene;
+  double T[16], invT[16], invT33[16];
+};
+srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, const SceneElem *elems,
+                              const srt_ray *rays, size_t n, const uint32_t *prev_element,
+                              const float *prev_normals, srt_hit *hits, uint32_t *element,
+                              uint32_t max_iter, unsigned long long *stats);
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
 // array in context scratch, valid until the context's next sort.
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);

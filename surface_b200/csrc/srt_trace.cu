@@ -1198,6 +1198,226 @@ srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
 
 }  // namespace srt
 
+// ================================================================ scenes
+// RenderGraph::Trace (gles/gles_render_graph.cc:143-314) for a whole ray
+// array.  Per ray: the top-level BVHTree walk collects the elements whose
+// world box the ray enters (render/render_bvh_tree.cc:504-585, double slab
+// test with SetupRay's guarded reciprocals), sorted by entry distance (a
+// stable insertion sort: std::sort's order for up to 16 candidates); each
+// element in that order unless its entry lies beyond the nearest world hit
+// so far: the ray is taken into the element's local space with the inverse
+// transforms (Matrixd::MultV, double), traversed with the reference's walk,
+// and the hit point taken back to world space; the world distance (float
+// length) decides, strictly smaller wins.  The previous hit's primitive,
+// distance and normal apply only inside the element the ray left.
+namespace srt {
+namespace {
+
+constexpr int kTopCand = 64;
+constexpr int kTopStack = 64;
+
+__device__ __forceinline__ bool top_aabb(const TopNode &t, const double o[3],
+                                         const double inv[3], const int sgn[3], double &tmin,
+                                         double &tmax) {
+  const double mnx = sgn[0] ? t.bmax[0] : t.bmin[0], mny = sgn[1] ? t.bmax[1] : t.bmin[1],
+               mnz = sgn[2] ? t.bmax[2] : t.bmin[2];
+  const double mxx = sgn[0] ? t.bmin[0] : t.bmax[0], mxy = sgn[1] ? t.bmin[1] : t.bmax[1],
+               mxz = sgn[2] ? t.bmin[2] : t.bmax[2];
+  const double tminx = (mnx - o[0]) * inv[0], tmaxx = (mxx - o[0]) * inv[0];
+  const double tminy = (mny - o[1]) * inv[1], tmaxy = (mxy - o[1]) * inv[1];
+  double a = (tminx > tminy) ? tminx : tminy;
+  double b = (tmaxx < tmaxy) ? tmaxx : tmaxy;
+  const double tminz = (mnz - o[2]) * inv[2], tmaxz = (mxz - o[2]) * inv[2];
+  a = (a > tminz) ? a : tminz;
+  b = (b < tmaxz) ? b : tmaxz;
+  if ((b > 0.0) && (a <= b)) {
+    tmin = a;
+    tmax = b;
+    return true;
+  }
+  return false;
+}
+
+// Matrixd::MultV: dst[k] = m[0][k] v0 + m[1][k] v1 + m[2][k] v2 + m[3][k].
+__device__ __forceinline__ void multv(const double m[16], const double v[3], double o[3]) {
+#pragma unroll
+  for (int k = 0; k < 3; k++) o[k] = ((m[k] * v[0] + m[4 + k] * v[1]) + m[8 + k] * v[2]) + m[12 + k];
+}
+
+__global__ void __launch_bounds__(128)
+scene_trace_kernel(const TopNode *__restrict__ top, const SceneElem *__restrict__ elems,
+                   const srt_ray *__restrict__ rays, size_t n,
+                   const uint32_t *__restrict__ prev_element,
+                   const float *__restrict__ prev_normals, srt_hit *__restrict__ hits,
+                   uint32_t *__restrict__ element, uint32_t max_iter,
+                   unsigned long long *__restrict__ stats, uint32_t *__restrict__ err) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t ntop = 0, nwalk = 0, nbranch = 0, nleaf = 0, nprim = 0;
+  uint32_t prev_prim;
+  float prev_t;
+  const RayF r0 = load_ray(rays, i, prev_prim, prev_t);
+  const double ro[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd[3] = {r0.d[0], r0.d[1], r0.d[2]};
+  int sgn[3];
+  double inv[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    sgn[k] = rd[k] < 0.0 ? 1 : 0;
+    inv[k] = fabs(rd[k]) > 2.0e-15 ? 1.0 / rd[k] : (rd[k] < 0.0 ? -(double)FLT_MAX : (double)FLT_MAX);
+  }
+  // ---- top level: candidates in walk order
+  double ct[kTopCand];
+  uint32_t cid[kTopCand];
+  int nc = 0;
+  int stk[kTopStack];
+  int sp = 0, node = 0;
+  for (uint32_t guard = 0; guard < max_iter; guard++) {
+    const TopNode &t = top[node];
+    ntop++;
+    if (t.leaf) {
+      double a, b;
+      if (top_aabb(t, ro, inv, sgn, a, b)) {
+        if (nc < kTopCand) {
+          ct[nc] = a;
+          cid[nc] = t.id;
+          nc++;
+        } else {
+          atomicOr(err, kErrStack);
+        }
+      }
+      if (sp < 1) break;
+      node = stk[--sp];
+    } else {
+      double a0, b0, a1, b1;
+      const bool h0 = t.child[0] > 0 && top_aabb(top[t.child[0]], ro, inv, sgn, a0, b0);
+      const bool h1 = t.child[1] > 0 && top_aabb(top[t.child[1]], ro, inv, sgn, a1, b1);
+      if (!h0 && !h1) {
+        if (sp < 1) break;
+        node = stk[--sp];
+      } else if (h0 && !h1) {
+        node = t.child[0];
+      } else if (h1 && !h0) {
+        node = t.child[1];
+      } else {
+        const int order = sgn[t.axis];
+        if (sp >= kTopStack) {
+          atomicOr(err, kErrStack);
+          break;
+        }
+        stk[sp++] = t.child[1 - order];
+        node = t.child[order];
+      }
+    }
+  }
+  // stable insertion sort by entry distance
+  for (int a = 1; a < nc; a++) {
+    const double kt = ct[a];
+    const uint32_t kid = cid[a];
+    int b = a - 1;
+    while (b >= 0 && kt < ct[b]) {
+      ct[b + 1] = ct[b];
+      cid[b + 1] = cid[b];
+      b--;
+    }
+    ct[b + 1] = kt;
+    cid[b + 1] = kid;
+  }
+  // ---- elements, nearest world distance
+  double tnear = DBL_MAX;
+  float bt = FLT_MAX, bu = 0.0f, bv = 0.0f;
+  uint32_t bp = kNone, be = kNone;
+  for (int c = 0; c < nc; c++) {
+    if (tnear < ct[c]) continue;
+    const SceneElem &e = elems[cid[c]];
+    double lo[3], ld[3];
+    multv(e.invT, ro, lo);
+    multv(e.invT33, rd, ld);
+    const bool same = prev_element && prev_element[i] == cid[c];
+    RayF lr;
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      lr.o[k] = (float)lo[k];
+      lr.d[k] = (float)ld[k];
+      lr.sgn[k] = lr.d[k] < 0.0f ? 1 : 0;
+      lr.inv[k] = __frcp_rn(lr.d[k]);
+    }
+    Work w;
+    Best b;
+    if (e.kind == SRT_TETRAHEDRA) {
+      CtxT ct2;
+      ct2.r = lr;
+      ct2.o = {lr.o[0], lr.o[1], lr.o[2]};
+      ct2.d = {lr.d[0], lr.d[1], lr.d[2]};
+      ct2.prev_prim = same ? prev_prim : kNone;
+      walkT<false>(static_cast<const NodeT *>(e.nodes), e.prims, e.sidx, ct2, 0.0f, 0.0, b, w,
+                   max_iter);
+    } else {
+      Ctx2 c2;
+      c2.r = lr;
+      c2.prev_prim = same ? prev_prim : kNone;
+      c2.prev_t = same ? prev_t : 0.0f;
+      c2.keps = e.scene->keps;
+#pragma unroll
+      for (int k = 0; k < 3; k++) c2.pn[k] = (same && prev_normals) ? prev_normals[3 * i + k] : 0.0f;
+      if (e.kind == SRT_TRIANGLES)
+        ref_walk2<SRT_TRIANGLES>(static_cast<const Node2 *>(e.nodes), e.prims, e.sidx, c2, b, w,
+                                 max_iter);
+      else
+        ref_walk2<SRT_SPHERES>(static_cast<const Node2 *>(e.nodes), e.prims, e.sidx, c2, b, w,
+                               max_iter);
+    }
+    if (w.fail) atomicOr(err, kErrIter);
+    nwalk++;
+    nbranch += w.branch;
+    nleaf += w.leaf;
+    nprim += w.prim;
+    if (!(b.t < FLT_MAX && b.prim != kNone)) continue;
+    double lp[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)b.t * ld[k]);
+    double wp[3];
+    multv(e.T, lp, wp);
+    float po[3];
+#pragma unroll
+    for (int k = 0; k < 3; k++) po[k] = (float)wp[k] - r0.o[k];
+    const float tw = sqrtf(po[0] * po[0] + po[1] * po[1] + po[2] * po[2]);
+    if ((double)tw < tnear) {
+      tnear = tw;
+      bt = tw;
+      bu = b.u;
+      bv = b.v;
+      bp = b.prim;
+      be = cid[c];
+    }
+  }
+  reinterpret_cast<float4 *>(hits)[i] = make_float4(bt, bu, bv, __uint_as_float(bp));
+  if (element) element[i] = be;
+  if (stats) {  // warp sums of the visit counters, one atomic per warp each
+    const unsigned m = __activemask();
+    const uint32_t c[5] = {__reduce_add_sync(m, ntop), __reduce_add_sync(m, nwalk),
+                           __reduce_add_sync(m, nbranch), __reduce_add_sync(m, nleaf),
+                           __reduce_add_sync(m, nprim)};
+    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(m) - 1))
+      for (int k = 0; k < 5; k++) atomicAdd(&stats[k], (unsigned long long)c[k]);
+  }
+}
+
+}  // namespace
+
+srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, const SceneElem *elems,
+                              const srt_ray *rays, size_t n, const uint32_t *prev_element,
+                              const float *prev_normals, srt_hit *hits, uint32_t *element,
+                              uint32_t max_iter, unsigned long long *stats) {
+  if (n == 0) return SRT_OK;
+  scene_trace_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
+      top, elems, rays, n, prev_element, prev_normals, hits, element, max_iter, stats,
+      ctx->d_err);
+  ctx->launches++;
+  return cuda_status(cudaGetLastError(), "scene trace");
+}
+
+}  // namespace srt
+
 // ======================================================= no-allocation trace
 // srt_trace_closest_noalloc runs the same two kernels as srt_trace_closest
 // (first pass + deferred-ray resolve) but keeps its deferred-ray list in the

@@ -365,3 +365,103 @@ def sphere_normals_np(rays, hits, centers):
     v = (p - centers[hits["prim"][hit]]).astype(np.float64)
     nrm[hit] = (v / np.linalg.norm(v, axis=1, keepdims=True)).astype(np.float32)
     return nrm
+
+
+# ---------------------------------------------------------------- scenes
+def affine(rotation_axis=(0.0, 0.0, 1.0), angle_deg=0.0, scale=(1.0, 1.0, 1.0),
+           translate=(0.0, 0.0, 0.0)):
+    """4x4 in Matrixd's layout (p' = (p, 1) m; translation in the last row)
+    for p' = R diag(scale) p + translate, R the rotation about the axis."""
+    a = np.asarray(rotation_axis, np.float64)
+    a = a / np.linalg.norm(a)
+    th = np.radians(angle_deg)
+    K = np.array([[0, -a[2], a[1]], [a[2], 0, -a[0]], [-a[1], a[0], 0]])
+    R = np.eye(3) + np.sin(th) * K + (1 - np.cos(th)) * (K @ K)
+    A = R @ np.diag(np.asarray(scale, np.float64))
+    m = np.eye(4)
+    m[:3, :3] = A.T
+    m[3, :3] = translate
+    return m
+
+
+def scene_elements(seed=31, ntri=3, nsph=2, ntet=1, spread=4.0):
+    """A mixed scene: ntri displaced octaspheres, nsph particle clouds and
+    ntet tetrahedral grids, each under a seeded rotation, (non-uniform)
+    scale and translation inside [-spread, spread]^3.  Returns a list of
+    dicts with kind (0 tri, 1 tet, 2 sphere), verts, faces or radius, T."""
+    rng = np.random.default_rng(seed)
+    out = []
+    kinds = [0] * ntri + [2] * nsph + [1] * ntet
+    for j, k in enumerate(kinds):
+        T = affine(rng.normal(size=3), rng.uniform(0, 360),
+                   rng.uniform(0.5, 1.5, size=3), rng.uniform(-spread, spread, size=3))
+        if k == 0:
+            v, f = displaced_octasphere(3 + j % 2, seed=seed + j)
+            out.append(dict(kind=0, verts=v, faces=f, T=T))
+        elif k == 2:
+            p, r = particles(2000 + 500 * j, seed=seed + j, median_radius=0.02)
+            out.append(dict(kind=2, verts=p, radius=r, T=T))
+        else:
+            v, f, _ = tet_grid(4 + j % 3, seed=seed + j)
+            out.append(dict(kind=1, verts=v, faces=f, T=T))
+    return out
+
+
+def scene_rays(n, bmin, bmax, seed=5, boxes=None):
+    """Rays from a sphere around the box to seeded points inside it, or
+    inside one of ``boxes`` ((lo, hi) arrays of shape (m, 3)) picked per ray,
+    with a share of axis-aligned directions."""
+    rng = np.random.default_rng(seed)
+    bmin = np.asarray(bmin, np.float64)
+    bmax = np.asarray(bmax, np.float64)
+    c = 0.5 * (bmin + bmax)
+    rad = 0.75 * np.linalg.norm(bmax - bmin)
+    o = c + rad * _normalize(rng.normal(size=(n, 3)))
+    if boxes is None:
+        tgt = bmin + rng.uniform(size=(n, 3)) * (bmax - bmin)
+    else:
+        lo, hi = (np.asarray(b, np.float64) for b in boxes)
+        k = rng.integers(0, lo.shape[0], size=n)
+        tgt = lo[k] + (0.25 + 0.5 * rng.uniform(size=(n, 3))) * (hi[k] - lo[k])
+    d = _normalize(tgt - o)
+    ax = rng.uniform(size=n) < 0.1  # axis-aligned: zero direction components
+    if ax.any():
+        k = rng.integers(0, 3, size=ax.sum())
+        dd = np.zeros((ax.sum(), 3))
+        dd[np.arange(ax.sum()), k] = np.where(rng.uniform(size=ax.sum()) < 0.5, -1.0, 1.0)
+        d[ax] = dd
+        o[ax] = tgt[ax] - rad * dd
+    rays = np.zeros(n, RAY_DTYPE)
+    rays["org"] = o.astype(np.float32)
+    rays["dir"] = d.astype(np.float32)
+    rays["prev_prim"] = MISS
+    return rays
+
+
+def instanced_scene(seed=77, grid=4, spacing=3.0):
+    """grid^3 elements on a lattice of the given spacing, each an instance of
+    one of three accels (131,072-triangle octasphere, 1,000,000-sphere cloud,
+    32^3-cell tetrahedral grid), centred, scaled to about 2 units, rotated
+    and jittered.  Returns dict(accels=[{kind, verts, faces|radius}],
+    elements=[{accel, T}], prims=[per-element primitive count])."""
+    rng = np.random.default_rng(seed)
+    v, f = displaced_octasphere(7)
+    p, r = particles(1_000_000, seed=seed, median_radius=0.004)
+    tv, tf, _ = tet_grid(32, seed=seed)
+    accels = [dict(kind=0, verts=v, faces=f, centre=(0.0, 0.0, 0.0), size=2.2),
+              dict(kind=2, verts=p, radius=r, centre=(0.5, 0.5, 0.5), size=1.0),
+              dict(kind=1, verts=tv, faces=tf, centre=(0.5, 0.5, 0.5), size=1.0)]
+    nprim = [f.shape[0], p.shape[0], tf.shape[0]]
+    elements, prims = [], []
+    off = 0.5 * (grid - 1) * spacing
+    for j in range(grid ** 3):
+        a = j % 3
+        cell = np.array(np.unravel_index(j, (grid,) * 3), np.float64) * spacing - off
+        s = 2.0 / accels[a]["size"] * rng.uniform(0.8, 1.2)
+        C = np.eye(4)
+        C[3, :3] = -np.asarray(accels[a]["centre"])
+        M = affine(rng.normal(size=3), rng.uniform(0, 360), (s, s, s),
+                   cell + rng.uniform(-0.3, 0.3, size=3))
+        elements.append(dict(accel=a, T=C @ M))
+        prims.append(nprim[a])
+    return dict(accels=accels, elements=elements, prims=prims)

@@ -1,0 +1,158 @@
+"""Scenes of transformed accels (srt_scene_*, RenderGraph) on the GPU against
+the oracle, bit for bit: the top-level tree, primary rays and secondary
+rays that leave a hit element (self-hit rule inside prev_element only)."""
+import numpy as np
+import pytest
+import torch
+
+import surface_b200 as sb
+from oracle import oracle as O
+from surface_b200 import scenes as S
+from surface_b200.scene import RenderGraph
+
+from conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+KIND = {0: (O.TRI, sb.TriangleAccel), 1: (O.TET, sb.TetraAccel), 2: (O.SPHERE, sb.ParticleAccel)}
+
+
+def gpu_accel(e):
+    cls = KIND[e["kind"]][1]
+    acc = cls()
+    if e["kind"] == 0:
+        acc.Build32(sb.Mesh(e["verts"], e["faces"]))
+    elif e["kind"] == 1:
+        acc.Build32(sb.Tetrahedron(e["verts"], e["faces"]))
+    else:
+        acc.Build32(sb.Particles(e["verts"], e["radius"]))
+    return acc
+
+
+def oracle_accel(e):
+    k = KIND[e["kind"]][0]
+    if e["kind"] == 2:
+        return O.OracleAccel(k, e["verts"], None, e["radius"])
+    return O.OracleAccel(k, e["verts"], e["faces"])
+
+
+def make_pair(elems):
+    gacc = [gpu_accel(e) for e in elems]
+    oacc = [oracle_accel(e) for e in elems]
+    g = RenderGraph()
+    T, iT, iT33, wlo, whi = [], [], [], [], []
+    for e, a in zip(elems, gacc):
+        assert g.AddRenderElement(a, e["T"]) == len(T)
+        lo, hi = a.BoundingBox()
+        i1, i2, b0, b1 = O.element_update(e["T"], lo, hi)
+        T.append(np.asarray(e["T"]).reshape(16))
+        iT.append(i1.reshape(16))
+        iT33.append(i2.reshape(16))
+        wlo.append(b0)
+        whi.append(b1)
+    g.Build()
+    o = O.OracleScene(oacc, T, iT, iT33, wlo, whi)
+    return g, o, gacc, np.array(wlo), np.array(whi)
+
+
+def assert_same(got, gel, want, wel):
+    h = got.cpu().numpy() if isinstance(got, torch.Tensor) else got.view(np.float32)
+    e = gel.cpu().numpy().view(np.uint32) if isinstance(gel, torch.Tensor) else gel
+    assert np.array_equal(e, wel)
+    assert np.array_equal(bits(np.ascontiguousarray(h).reshape(-1)),
+                          bits(want.view(np.float32).reshape(-1)))
+
+
+@pytest.fixture(scope="module")
+def mixed():
+    elems = S.scene_elements(seed=31)
+    return (elems,) + make_pair(elems)
+
+
+def test_top_tree_matches_oracle(mixed):
+    _, g, o, _, _, _ = mixed
+    gb, gi = g.top_nodes()
+    ob, oi = o.nodes()
+    assert np.array_equal(gi, oi)
+    assert np.array_equal(bits(gb), bits(ob))
+
+
+def test_primary_rays_match_oracle(mixed):
+    _, g, o, _, wlo, whi = mixed
+    rays = S.scene_rays(200_000, wlo.min(0), whi.max(0), seed=9, boxes=(wlo, whi))
+    want, wel = o.trace(rays)
+    assert (wel != S.MISS).mean() > 0.2
+    rt = torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda()
+    hits, el = g.Trace(rt)
+    torch.cuda.synchronize()
+    assert_same(hits, el, want, wel)
+    # host arrays through the same entry point
+    h2, e2 = g.Trace(rays[:5000])
+    assert np.array_equal(e2, wel[:5000])
+    assert np.array_equal(h2.view(np.uint32), want[:5000].view(np.uint32))
+
+
+def test_secondary_rays_match_oracle(mixed):
+    _, g, o, _, wlo, whi = mixed
+    rays = S.scene_rays(100_000, wlo.min(0), whi.max(0), seed=12, boxes=(wlo, whi))
+    want, wel = o.trace(rays)
+    hit = np.nonzero(wel != S.MISS)[0]
+    rng = np.random.default_rng(2)
+    sec = np.zeros(hit.size, O.RAY_DTYPE)
+    sec["org"] = rays["org"][hit] + want["t"][hit, None] * rays["dir"][hit]
+    sec["dir"] = S._normalize(rng.normal(size=(hit.size, 3))).astype(np.float32)
+    sec["prev_prim"] = want["prim"][hit]
+    sec["prev_t"] = want["t"][hit]
+    pe = wel[hit]
+    pn = S._normalize(rng.normal(size=(hit.size, 3))).astype(np.float32)
+    w2, we2 = o.trace(sec, pe, pn)
+    st = torch.from_numpy(sec.view(np.float32).reshape(-1, 8)).cuda()
+    hits, el = g.Trace(st, torch.from_numpy(pe.view(np.int32)).cuda(), torch.from_numpy(pn).cuda())
+    torch.cuda.synchronize()
+    assert_same(hits, el, w2, we2)
+
+
+def test_many_instances_of_one_accel():
+    """One accel under 40 transforms (instancing), touching and overlapping
+    world boxes."""
+    v, f = S.displaced_octasphere(4, seed=3)
+    p, r = S.particles(3000, seed=4, median_radius=0.02)
+    rng = np.random.default_rng(8)
+    elems = []
+    for j in range(40):
+        T = S.affine(rng.normal(size=3), rng.uniform(0, 360), rng.uniform(0.3, 1.2, size=3),
+                     rng.uniform(-6, 6, size=3))
+        if j % 4 == 3:
+            elems.append(dict(kind=2, verts=p, radius=r, T=T))
+        else:
+            elems.append(dict(kind=0, verts=v, faces=f, T=T))
+    g, o, _, wlo, whi = make_pair(elems)
+    gb, gi = g.top_nodes()
+    ob, oi = o.nodes()
+    assert np.array_equal(gi, oi) and np.array_equal(bits(gb), bits(ob))
+    rays = S.scene_rays(100_000, wlo.min(0), whi.max(0), seed=3, boxes=(wlo, whi))
+    want, wel = o.trace(rays)
+    hits, el = g.Trace(torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda())
+    torch.cuda.synchronize()
+    assert_same(hits, el, want, wel)
+
+
+def test_explicit_matrices_and_errors(mixed):
+    elems, g, o, gacc, wlo, whi = mixed
+    g2 = RenderGraph()
+    for e, a in zip(elems, gacc):
+        lo, hi = a.BoundingBox()
+        i1, i2, b0, b1 = O.element_update(e["T"], lo, hi)
+        g2.add_element_matrices(a, e["T"], i1, i2, b0, b1)
+    with pytest.raises(sb.SurfaceError):
+        g2.Trace(np.zeros(4, O.RAY_DTYPE))  # not built
+    g2.Build()
+    assert np.array_equal(bits(g2.top_nodes()[0]), bits(g.top_nodes()[0]))
+    rays = S.scene_rays(20_000, wlo.min(0), whi.max(0), seed=1, boxes=(wlo, whi))
+    h1, e1 = g.Trace(rays)
+    h2, e2 = g2.Trace(rays)
+    assert np.array_equal(e1, e2) and np.array_equal(h1.view(np.uint32), h2.view(np.uint32))
+    with pytest.raises(sb.SurfaceError):
+        RenderGraph().Build()  # empty scene
+    with pytest.raises(sb.SurfaceError):
+        RenderGraph().AddRenderElement(sb.TriangleAccel(), np.eye(4))  # not built
