@@ -106,7 +106,7 @@ def lib():
         L.so_scene_top_nodes.argtypes = [_P, _P, _P, _SZ]
         L.so_scene_candidates.restype = _SZ
         L.so_scene_candidates.argtypes = [_P, _P, _P, _P, _P, _SZ]
-        L.so_scene_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, C.c_int]
+        L.so_scene_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, _P, C.c_int, C.c_int]
         _ORACLE = L
     return _ORACLE
 
@@ -700,9 +700,12 @@ class OracleScene:
         n = lib().so_scene_candidates(self.h, _ptr(o), _ptr(d), _ptr(tt), _ptr(ids), cap)
         return tt[:n].copy(), ids[:n].copy()
 
-    def trace(self, rays, prev_element=None, prev_normals=None, nthreads=0):
+    def trace(self, rays, prev_element=None, prev_normals=None, nthreads=0,
+              want_visits=False, walk2=False):
         """(hits, element): hit t is the world distance, prim / u / v the
-        element's own; element MISS where nothing was hit."""
+        element's own; element MISS where nothing was hit.  want_visits adds
+        per-ray node + primitive visits of the element walks; walk2 walks the
+        elements with the two-pass walk restated instead of the reference's."""
         if any(a is None for a in self.accels):
             raise ValueError("scene built without accels")
         rays = np.ascontiguousarray(rays, RAY_DTYPE)
@@ -710,9 +713,10 @@ class OracleScene:
         el = np.zeros(rays.size, np.uint32)
         pe = None if prev_element is None else np.ascontiguousarray(prev_element, np.uint32)
         pn = None if prev_normals is None else np.ascontiguousarray(prev_normals, np.float32)
+        vis = np.zeros(rays.size, np.uint32) if want_visits else None
         lib().so_scene_trace(self.h, _ptr(rays), rays.size, _ptr(pe), _ptr(pn), _ptr(hits),
-                             _ptr(el), nthreads)
-        return hits, el
+                             _ptr(el), _ptr(vis), 1 if walk2 else 0, nthreads)
+        return (hits, el, vis) if want_visits else (hits, el)
 
     def __del__(self):
         try:

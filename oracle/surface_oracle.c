@@ -865,12 +865,14 @@ static inline int sphere_isect(float *tio, const float c[3], float radius,
   return 0;
 }
 
-/* Closest hit for one ray: Traverse() of the three accel classes. */
-static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
+/* Closest hit for one ray: Traverse() of the three accel classes, with the
+ * running distance starting at t0 (FLT_MAX: the reference's own walk).
+ * Returns whether a primitive was accepted. */
+static int trace_from(const so_accel *a, const so_ray *ray, const float *prevN,
                       so_hit *h, uint32_t *subface, const float *vscalar,
-                      float *scalar_out, so_stats *st) {
+                      float *scalar_out, so_stats *st, float t0) {
   double best_e1 = 0.0, best_e2 = 0.0;
-  float hitT = FLT_MAX;
+  float hitT = t0;
   h->t = hitT;
   h->u = 0.0f;
   h->v = 0.0f;
@@ -982,7 +984,10 @@ static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
       if (any) hitT = h->t;
     }
   }
-  if (!(h->t < FLT_MAX)) {
+  if (h->prim == 0xffffffffu || !(h->t < FLT_MAX)) {
+    h->t = FLT_MAX;
+    h->u = 0.0f;
+    h->v = 0.0f;
     h->prim = 0xffffffffu;
   }
   if (subface) *subface = sub;
@@ -999,6 +1004,13 @@ static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
     }
     *scalar_out = sv;
   }
+  return h->prim != 0xffffffffu;
+}
+
+static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
+                      so_hit *h, uint32_t *subface, const float *vscalar,
+                      float *scalar_out, so_stats *st) {
+  trace_from(a, ray, prevN, h, subface, vscalar, scalar_out, st, FLT_MAX);
 }
 
 /* ---- two-pass walk (restatement of the product's default traversal) ----
@@ -1007,19 +1019,20 @@ static void trace_one(const so_accel *a, const so_ray *ray, const float *prevN,
  * reference's depth-first order through boxes entered before bound(m),
  * applying the reference's acceptance rule to the candidates at m
  * (tetrahedra: within 8 float steps of m).  This equals the reference's
- * result whenever no intersected primitive reports a distance below the
- * entry distance of its own leaf box; the walk checks that for every
- * primitive it tests and otherwise falls back to the reference's walk. */
+ * result unless one of those candidates reports a distance below the entry
+ * distance of its own leaf box (the same float the reference's box test
+ * computes): a box around a primitive at or beyond its entry is entered
+ * no later than that primitive's distance, so it is pruned only for a
+ * running distance below it, i.e. by a nearer candidate.  The walk then
+ * falls back to the reference's walk. */
 static inline float bound_rel(float m, float rel) {
   return (m < FLT_MAX) ? m + fabsf(m) * rel + 1e-30f : FLT_MAX;
 }
 #define SO_REL_TRI 3.90625e-3f      /* 2^-8 */
 #define SO_REL_TET 1.52587890625e-5f /* 2^-16 */
-#define SO_VIOL_TOL 4.76837158203125e-7f /* 2^-21 */
-
-/* candidate t below (or within rounding of) its leaf box entry */
+/* candidate t below its leaf box entry (NaN counts as below) */
 static inline int below_entry(double t, float entry) {
-  return t < (double)entry + fabs((double)entry) * (double)SO_VIOL_TOL;
+  return !(t >= (double)entry);
 }
 
 static inline int ray_aabb_t(float maxT, const float bmin[3], const float bmax[3],
@@ -1102,6 +1115,8 @@ typedef struct {
   float u, v;
   uint32_t prim;
   int ef;
+  int viol;    /* distance below its own leaf box's entry */
+  float entry; /* that entry */
 } so_cand;
 
 static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
@@ -1126,7 +1141,8 @@ static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
   /* ---- pass 1: front to back, collecting the candidates in the window */
   double m = DBL_MAX;
   so_cand win[4];
-  int nwin = 0, overflow = 0;
+  int nwin = 0, overflow = 0, viol_lost = 0;
+  double m2 = DBL_MAX; /* second smallest distance */
   sp = -1;
   {
     float t0;
@@ -1169,8 +1185,10 @@ static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
                           &c.e1, &c.e2, &c.ul1))
         continue;
       c.prim = f;
-      if (below_entry(c.t, et)) viol = 1;
+      c.viol = below_entry(c.t, et);
+      c.entry = et;
       if (c.t < m) {
+        m2 = m;
         m = c.t;
         /* drop the candidates that fell out of the window */
         double whi = window_hi(m, tet);
@@ -1179,12 +1197,29 @@ static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
           if (win[k].t <= whi) win[k2++] = win[k];
         nwin = k2;
       }
+      else if (c.t < m2) {
+        m2 = c.t;
+      }
       if (c.t <= window_hi(m, tet)) {
-        if (nwin < 4) win[nwin++] = c;
-        else overflow = 1;
+        if (nwin < 4) {
+          win[nwin++] = c;
+        } else {
+          overflow = 1;
+          viol_lost |= c.viol;
+        }
       }
     }
   }
+  /* only the candidates left in the window at m can be hidden by the
+   * reference's pruning; a dropped candidate's violation is kept.  A single
+   * candidate below its box's entry e can only be pruned for a running
+   * distance below e, i.e. by another primitive nearer than e: none when the
+   * second smallest distance m2 >= e (every such primitive was tested, e
+   * lying below pass 1's pruning bound). */
+  viol = viol_lost;
+  for (int k = 0; k < nwin; k++) viol |= win[k].viol;
+  if (viol && nwin == 1 && !overflow)
+    viol = !(m2 >= (double)win[0].entry) || !(win[0].entry < bound_rel((float)m, rel));
   h->t = FLT_MAX;
   h->u = 0.0f;
   h->v = 0.0f;
@@ -1272,9 +1307,15 @@ static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
     }
   }
   if (viol) {
-    /* a primitive reported a distance below its leaf box's entry: the
-     * reference's pruning may matter, so take its walk */
-    trace_one(a, ray, prevN, h, subface, vscalar, scal, st);
+    /* a candidate reported a distance below its leaf box's entry: the
+     * reference's pruning may matter, so take its walk.  Started from the
+     * pruning bound T of pass 1 it returns the same primitive: the answer
+     * and every primitive that can prune its boxes lie below T by more than
+     * the float error of a distance, so a running distance at or above T
+     * (which the full walk may hold on the way) prunes none of them.  If
+     * nothing is accepted below T, the full walk decides. */
+    if (!trace_from(a, ray, prevN, h, subface, vscalar, scal, st, bound_rel((float)m, rel)))
+      trace_one(a, ray, prevN, h, subface, vscalar, scal, st);
     if (fallback) *fallback = 1;
     return;
   }
@@ -1890,7 +1931,10 @@ SO_API void so_framebuffer_write(int width, int height, int step, const so_hit *
  *     local ray by Matrixd::MultV with invT / invT33 (double) stored as
  *     float; the element's reference walk; world point by MultV with T of
  *     the float local point; world distance = float length; strictly nearer
- *     wins.  prev_prim / prev_t / prev_normal apply only in prev_element. */
+ *     wins.  prev_prim / prev_t / prev_normal apply only in prev_element.
+ * so_scene_trace walks each element with the reference's walk, or with
+ * walk2 with the two-pass walk restated (the same hits); visits (optional)
+ * receives per ray the node and primitive visits of its element walks. */
 typedef struct {
   double bmin[3], bmax[3];
   int child[2], axis, leaf;
@@ -2153,7 +2197,8 @@ static void scene_multv(const double *m, const double v[3], double o[3]) {
 
 SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
                            const uint32_t *prev_element, const float *prev_normals,
-                           so_hit *hits, uint32_t *element, int nthreads) {
+                           so_hit *hits, uint32_t *element, uint32_t *visits, int walk2,
+                           int nthreads) {
 #ifdef _OPENMP
   if (nthreads > 0) omp_set_num_threads(nthreads);
 #pragma omp parallel for schedule(dynamic, 64)
@@ -2167,6 +2212,7 @@ SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
     uint32_t cid[64];
     size_t nc = so_scene_candidates(s, ro, rd, ct, cid, 64);
     double tnear = DBL_MAX;
+    uint64_t nvis = 0;
     so_hit best = {FLT_MAX, 0.0f, 0.0f, 0xffffffffu};
     uint32_t be = 0xffffffffu;
     for (size_t c = 0; c < nc; c++) {
@@ -2187,7 +2233,13 @@ SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
       const float *pn = (same && prev_normals) ? &prev_normals[3 * i] : zero3;
       so_hit h;
       so_stats st = {0, 0, 0};
-      trace_one(s->acc[e], &lr, pn, &h, NULL, NULL, NULL, &st);
+      if (walk2) {
+        int fall = 0;
+        trace2_one(s->acc[e], &lr, pn, &h, NULL, NULL, NULL, &st, &fall);
+      } else {
+        trace_one(s->acc[e], &lr, pn, &h, NULL, NULL, NULL, &st);
+      }
+      nvis += st.branch_visits + st.prim_tests;
       if (h.prim == 0xffffffffu || !(h.t < FLT_MAX)) continue;
       double lp[3], wp[3];
       for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)h.t * ld[k]);
@@ -2204,6 +2256,7 @@ SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
     }
     hits[i] = best;
     if (element) element[i] = be;
+    if (visits) visits[i] = (uint32_t)(nvis < 0xffffffffu ? nvis : 0xffffffffu);
   }
 }
 

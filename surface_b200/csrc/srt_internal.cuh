@@ -196,10 +196,39 @@ struct SceneElem {
   const SceneInfo *scene;
   double T[16], invT[16], invT33[16];
 };
-srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, const SceneElem *elems,
-                              const srt_ray *rays, size_t n, const uint32_t *prev_element,
-                              const float *prev_normals, srt_hit *hits, uint32_t *element,
-                              uint32_t max_iter, unsigned long long *stats);
+// Device arrays of one scene trace (srt_trace.cu): per ray its candidates
+// (kRoundCand slots of entry distance and element) and running nearest
+// world distance; the item lists of the two phases (unsorted, then in
+// element order) with per-element counts and cursors, each kind's range of
+// the sorted list, per-(ray, slot) results of the second phase, and the
+// list of rays with more candidates than slots.  counters: [0] phase-0
+// items, [1] phase-1 items, [2] overflow rays, [3] unused; ecount [2][nelem]
+// follows counters directly (one memset clears both).
+constexpr int kRoundCand = 8;
+struct SceneWork {
+  const SceneElem *elems;
+  const uint32_t *elem_order;  // element ids by kind
+  uint32_t nelem;
+  const srt_ray *rays;
+  const uint32_t *prev_element;
+  const float *prev_normals;
+  srt_hit *hits;
+  uint32_t *element;
+  double *cand_t;
+  uint32_t *cand_e;
+  uint8_t *ncand;
+  float *tnear;
+  uint32_t *items, *sorted;
+  float4 *res;
+  uint32_t *counters, *ecount, *ecursor, *krange;
+  uint32_t *ovf;
+  size_t n;
+  uint32_t max_iter;
+  unsigned long long *stats;
+  uint32_t *err;
+};
+// kinds: bit k set when the scene holds elements of kind k.
+srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds);
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
 // array in context scratch, valid until the context's next sort.
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);

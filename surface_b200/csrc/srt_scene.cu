@@ -25,9 +25,10 @@ struct srt_scene {
   };
   std::vector<Elem> elems;
   std::vector<TopNode> top;
-  DevBuf d_top, d_elems;
+  DevBuf d_top, d_elems, d_order, scratch;
   bool built = false;
   uint32_t max_iter = 64;
+  uint32_t kinds = 0;  // bit k: the scene holds elements of kind k
 };
 
 namespace {
@@ -311,6 +312,7 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
   construct(s->top, d, 0, 0, d.size());
   std::vector<SceneElem> el(s->elems.size());
   size_t total = 0;
+  uint32_t kinds = 0;
   for (size_t i = 0; i < el.size(); i++) {
     const srt_accel *a = s->elems[i].acc;
     if (!a->built) {
@@ -329,11 +331,23 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
       el[i].invT33[k] = s->elems[i].invT33[k];
     }
     total += a->n;
+    kinds |= 1u << a->kind;
   }
   cudaSetDevice(s->ctx->device);
   cudaError_t e;
+  // element ids grouped by kind (triangles, tetrahedra, spheres), each
+  // group in id order: the layout of the trace's element-sorted item lists
+  std::vector<uint32_t> order;
+  for (int k = 0; k < 3; k++)
+    for (size_t i = 0; i < el.size(); i++)
+      if (el[i].kind == k) order.push_back((uint32_t)i);
+  if (order.size() != el.size()) {
+    set_error("scene element of unknown kind");
+    return SRT_ERR_INVALID;
+  }
   if ((e = s->d_top.ensure(s->top.size() * sizeof(TopNode))) != cudaSuccess ||
-      (e = s->d_elems.ensure(el.size() * sizeof(SceneElem))) != cudaSuccess)
+      (e = s->d_elems.ensure(el.size() * sizeof(SceneElem))) != cudaSuccess ||
+      (e = s->d_order.ensure(order.size() * sizeof(uint32_t))) != cudaSuccess)
     return cuda_status(e, "scene tables");
   cudaStream_t st = s->ctx->stream;
   e = cudaMemcpyAsync(s->d_top.p, s->top.data(), s->top.size() * sizeof(TopNode),
@@ -341,9 +355,13 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(s->d_elems.p, el.data(), el.size() * sizeof(SceneElem),
                         cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(s->d_order.p, order.data(), order.size() * sizeof(uint32_t),
+                        cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host tables go out of scope
   if (e != cudaSuccess) return cuda_status(e, "scene upload");
   s->max_iter = (uint32_t)std::min<size_t>(8 * total + 64 + 8 * s->top.size(), 0xfffffff0u);
+  s->kinds = kinds;
   s->built = true;
   return SRT_OK;
 }
@@ -394,9 +412,55 @@ SRT_API srt_status srt_scene_trace(srt_scene *s, const srt_ray *rays, size_t n,
     set_error("ray and hit arrays must be 16-byte aligned");
     return SRT_ERR_INVALID;
   }
-  return launch_scene_trace(ctx, s->d_top.as<TopNode>(), s->d_elems.as<SceneElem>(), rays, n,
-                            prev_element, prev_normals, hits, element, s->max_iter,
-                            reinterpret_cast<unsigned long long *>(stats));
+  if (n >= (1ull << 29)) {
+    set_error("srt_scene_trace: at most 2^29 - 1 rays per call");
+    return SRT_ERR_LIMIT;
+  }
+  // scratch sections (each 256-byte aligned): candidates, nearest distance,
+  // candidate counts, item lists, second-phase results, overflow list,
+  // counters + per-element counts, cursors, kind ranges
+  auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
+  const size_t ne = s->elems.size();
+  const size_t nk = n * kRoundCand;
+  const size_t b_ct = al(nk * sizeof(double)), b_ce = al(nk * 4), b_tn = al(n * 4),
+               b_nc = al(n), b_items = al(nk * 4), b_sorted = al(nk * 4),
+               b_res = al(nk * sizeof(float4)), b_ovf = al(n * 4),
+               b_cnt = al((4 + 2 * ne) * 4), b_cur = al(ne * 4), b_kr = al(6 * 4);
+  e = s->scratch.ensure(b_ct + b_ce + b_tn + b_nc + b_items + b_sorted + b_res + b_ovf + b_cnt +
+                        b_cur + b_kr);
+  if (e != cudaSuccess) return cuda_status(e, "scene trace scratch");
+  char *p = s->scratch.as<char>();
+  auto take = [&p](size_t bytes) {
+    char *q = p;
+    p += bytes;
+    return q;
+  };
+  SceneWork W;
+  W.elems = s->d_elems.as<SceneElem>();
+  W.elem_order = s->d_order.as<uint32_t>();
+  W.nelem = (uint32_t)ne;
+  W.rays = rays;
+  W.prev_element = prev_element;
+  W.prev_normals = prev_normals;
+  W.hits = hits;
+  W.element = element;
+  W.cand_t = reinterpret_cast<double *>(take(b_ct));
+  W.cand_e = reinterpret_cast<uint32_t *>(take(b_ce));
+  W.tnear = reinterpret_cast<float *>(take(b_tn));
+  W.ncand = reinterpret_cast<uint8_t *>(take(b_nc));
+  W.items = reinterpret_cast<uint32_t *>(take(b_items));
+  W.sorted = reinterpret_cast<uint32_t *>(take(b_sorted));
+  W.res = reinterpret_cast<float4 *>(take(b_res));
+  W.ovf = reinterpret_cast<uint32_t *>(take(b_ovf));
+  W.counters = reinterpret_cast<uint32_t *>(take(b_cnt));
+  W.ecount = W.counters + 4;
+  W.ecursor = reinterpret_cast<uint32_t *>(take(b_cur));
+  W.krange = reinterpret_cast<uint32_t *>(take(b_kr));
+  W.n = n;
+  W.max_iter = s->max_iter;
+  W.stats = reinterpret_cast<unsigned long long *>(stats);
+  W.err = ctx->d_err;
+  return launch_scene_trace(ctx, s->d_top.as<TopNode>(), W, s->kinds);
 }
 
 }  // extern "C"

@@ -360,17 +360,20 @@ __device__ __forceinline__ bool ray_aabb_t(float maxT, float lx, float ly, float
 // padding is 16 ulp(1), so 2^-16 suffices.
 constexpr float kRelTri = 3.90625e-3f;          // 2^-8
 constexpr float kRelTet = 1.52587890625e-5f;    // 2^-16
-constexpr float kViolTol = 4.76837158203125e-7f; // 2^-21
 
 __device__ __forceinline__ float bound_rel(float m, float rel) {
   return (m < FLT_MAX) ? m + fabsf(m) * rel + 1e-30f : FLT_MAX;
 }
 
-// A hit distance below (or within rounding of) the entry distance of its
-// own leaf box: the reference's pruning may then hide a primitive, so the
-// ray takes the reference's walk.
+// A hit distance below the entry distance of its own leaf box (the same
+// float the reference's box test computes; NaN counts as below).  Only a
+// primitive still among the candidates at the smallest distance m can then
+// be hidden by the reference's pruning: any box around a primitive with
+// t >= entry is entered at or before t, so a box can only be pruned for a
+// running distance below that primitive's own.  Such rays take the
+// reference's walk.
 __device__ __forceinline__ bool below_entry(double t, float entry) {
-  return t < (double)entry + fabs((double)entry) * (double)kViolTol;
+  return !(t >= (double)entry);
 }
 
 struct Work {
@@ -421,12 +424,16 @@ __device__ __forceinline__ bool cand2(const float4 *__restrict__ prims,
 }
 
 // The reference's Traverse, step for step (render/render_accel_triangle.cc:2511,
-// render/render_accel_particle.cc:3053).
+// render/render_accel_particle.cc:3053), with the running distance starting
+// at t0 (FLT_MAX: the reference's own walk; b.prim stays kNone when nothing
+// is accepted below t0).
 template <int KIND>
 __device__ void ref_walk2(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
                           const uint32_t *__restrict__ sidx, const Ctx2 &c, Best &b,
-                          Work &w, uint32_t max_iter, uint32_t root = 0) {
+                          Work &w, uint32_t max_iter, uint32_t root = 0,
+                          float t0 = FLT_MAX) {
   b = Best();
+  b.t = t0;
   uint2 stk[kStack];
   int sp = 0;
   stk[0] = make_uint2(root, 0u);
@@ -464,6 +471,26 @@ __device__ void ref_walk2(const Node2 *__restrict__ nodes, const float4 *__restr
       }
     }
   }
+  if (b.prim == kNone) b.t = FLT_MAX;
+}
+
+// The fallback for a ray whose candidate at m lies below its leaf box's
+// entry: the reference's walk started from pass 1's pruning bound T.  It
+// returns the reference's primitive: that primitive and every primitive
+// that can prune its boxes lie below T by more than the float error of a
+// distance, so a running distance at or above T (which the full walk may
+// hold on the way) prunes none of them.  Nothing accepted below T: the full
+// walk decides.
+template <int KIND>
+__device__ __forceinline__ void ref_walk2_from(const Node2 *__restrict__ nodes,
+                                               const float4 *__restrict__ prims,
+                                               const uint32_t *__restrict__ sidx,
+                                               const Ctx2 &c, Best &b, Work &w,
+                                               uint32_t max_iter, float m, uint32_t root = 0) {
+  ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter, root, bound_rel(m, kRelTri));
+  if (b.prim != kNone || w.fail) return;
+  w.it = 0;
+  ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter, root);
 }
 
 // Reference order through boxes entered before `bnd`, accepting from `t0`
@@ -595,8 +622,8 @@ __device__ __forceinline__ Ctx2 make_ctx2(const srt_ray *__restrict__ rays, size
 
 // Pass 1 of the default walk for the two-child kinds: front to back from
 // `root`; returns m (smallest hit distance), how many primitives hit at m,
-// the one found first (in b), and whether any primitive was reported before
-// its own leaf box's entry.
+// the one found first (in b), and whether one of those at m was reported
+// before its own leaf box's entry.
 template <int KIND>
 __device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
                                             const float4 *__restrict__ prims,
@@ -604,7 +631,8 @@ __device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
                                             const Ctx2 &c, uint32_t root, Best &b, Work &w,
                                             uint32_t max_iter, float &m_out,
                                             uint32_t &at_m_out, bool &viol_out) {
-  float m = FLT_MAX;
+  float m = FLT_MAX, m2 = FLT_MAX;  // smallest and second smallest distance
+  float e_best = 0.0f;              // leaf box entry of the candidate at m
   uint32_t at_m = 0;
   bool viol = false;
   uint2 stk[kStack];
@@ -650,16 +678,25 @@ __device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
       float t, u, v;
       uint32_t f;
       if (!cand2<KIND>(prims, sidx, j, c, FLT_MAX, t, u, v, f)) continue;
-      if (below_entry(t, lt)) viol = true;
       if (t < m) {
+        m2 = m;
         m = t;
         at_m = 1;
+        viol = below_entry(t, lt);
+        e_best = lt;
         b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
-      } else if (t == m) {
-        at_m++;
+      } else {
+        if (t < m2) m2 = t;
+        if (t == m) {
+          at_m++;
+          viol = viol || below_entry(t, lt);
+        }
       }
     }
   }
+  // a single candidate below its box's entry e is hidden only by another
+  // primitive nearer than e (all tested: e lies below the pruning bound)
+  if (viol && at_m == 1) viol = !(m2 >= e_best) || !(e_best < bound_rel(m, kRelTri));
   m_out = m;
   at_m_out = at_m;
   viol_out = viol;
@@ -719,7 +756,7 @@ resolve_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__
     Work w;
     Best b;
     if (dfr.full) {
-      ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
+      ref_walk2_from<KIND>(nodes, prims, sidx, c, b, w, max_iter, (float)dfr.m);
     } else {
       // triangles keep the last candidate at m (t <= current), spheres the
       // first (t < current)
@@ -765,15 +802,16 @@ __device__ __forceinline__ void take_tet(Best &b, double te, double e1, double e
   b.e2 = e2;
 }
 
-// The reference's walk (render/render_accel_tetra.cc:2200) or, with
-// WINDOW, the reference order through boxes entered before `bnd` keeping
-// only candidates at most `whi` away.
+// The reference's walk (render/render_accel_tetra.cc:2200) with the
+// running distance starting at t0 or, with WINDOW, the reference order
+// through boxes entered before `bnd` keeping only candidates at most `whi`
+// away.
 template <bool WINDOW>
 __device__ void walkT(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
                       const uint32_t *__restrict__ sidx, const CtxT &c, float bnd,
-                      double whi, Best &b, Work &w, uint32_t max_iter) {
+                      double whi, Best &b, Work &w, uint32_t max_iter, float t0 = FLT_MAX) {
   b = Best();
-  float t = FLT_MAX;
+  float t = t0;
   uint32_t stk[kStack];
   int sp = 0;
   stk[0] = 0u;
@@ -817,6 +855,18 @@ __device__ __forceinline__ double window_hi(double m) {
   return (double)wf;
 }
 
+// The tetrahedron fallback: the reference's walk from pass 1's pruning
+// bound, the full walk if nothing is accepted below it (see ref_walk2_from).
+__device__ __forceinline__ void walkT_from(const NodeT *__restrict__ nodes,
+                                           const float4 *__restrict__ prims,
+                                           const uint32_t *__restrict__ sidx, const CtxT &c,
+                                           Best &b, Work &w, uint32_t max_iter, double m) {
+  walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter, bound_rel((float)m, kRelTet));
+  if (b.prim != kNone || w.fail) return;
+  w.it = 0;
+  walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+}
+
 __device__ __forceinline__ void store_tet(size_t i, const Best &b,
                                           srt_hit *__restrict__ hits,
                                           uint32_t *__restrict__ subface,
@@ -852,6 +902,116 @@ __device__ __forceinline__ CtxT make_ctxT(const srt_ray *__restrict__ rays, size
   return c;
 }
 
+// Pass 1 of the default tetrahedron walk: front to back; nwin counts entry
+// distances within 8 float steps of the running minimum m (the list is kept
+// to recount when m drops).  defer: the ray needs the reference-order walk,
+// over the whole tree (full: a candidate in that window reported before its
+// own leaf box's entry) or through the window at m (several candidates near
+// m).
+__device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
+                                          const float4 *__restrict__ prims,
+                                          const uint32_t *__restrict__ sidx, const CtxT &c,
+                                          Best &b, Work &w, uint32_t max_iter, double &m_out,
+                                          bool &defer_out, bool &full_out) {
+  double m = DBL_MAX, m2 = DBL_MAX;  // smallest and second smallest distance
+  float e_best = 0.0f;               // leaf box entry of the candidate at m
+  double wl[4];
+  uint32_t wviol = 0;  // bit k: wl[k] lies below its own leaf box's entry
+  int nwin = 0;
+  bool overflow = false, viol_lost = false;
+  uint32_t stk[kStack];
+  float stt[kStack];
+  int sp = -1;
+  {
+    const float4 *np = reinterpret_cast<const float4 *>(nodes);
+    const float4 a = __ldg(np), bb = __ldg(np + 1);
+    float t0;
+    if (ray_aabb_t<false>(FLT_MAX, a.x, a.y, a.z, bb.x, bb.y, bb.z, c.r, t0)) {
+      stk[0] = 0u;
+      stt[0] = t0;
+      sp = 0;
+    }
+  }
+  while (true) {
+    uint32_t lref = 0, lcnt = 0;
+    float lt = 0.0f;
+    while (sp >= 0) {
+      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+      const uint32_t ni = stk[sp];
+      const float et = stt[sp];
+      sp--;
+      const float bnd = (m < DBL_MAX) ? bound_rel((float)m, kRelTet) : FLT_MAX;
+      if (et > bnd) continue;
+      const float4 *np = reinterpret_cast<const float4 *>(nodes + ni);
+      const uint32_t meta = __float_as_uint(__ldg(&np[0].w));
+      const uint32_t ref = __float_as_uint(__ldg(&np[1].w));
+      if (meta & kLeafBit) { lref = ref; lcnt = meta & kCountMask; lt = et; break; }
+      w.branch++;
+      // the two children are adjacent: test their own boxes here
+      const float4 *cp = reinterpret_cast<const float4 *>(nodes + ref);
+      const float4 a0 = __ldg(cp), b0 = __ldg(cp + 1), a1 = __ldg(cp + 2), b1 = __ldg(cp + 3);
+      float t0, t1;
+      const bool h0 = ray_aabb_t<false>(bnd, a0.x, a0.y, a0.z, b0.x, b0.y, b0.z, c.r, t0);
+      const bool h1 = ray_aabb_t<false>(bnd, a1.x, a1.y, a1.z, b1.x, b1.y, b1.z, c.r, t1);
+      if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+      if (h0 && h1) {
+        const bool first1 = t1 < t0;
+        stk[++sp] = first1 ? ref : ref + 1; stt[sp] = first1 ? t0 : t1;
+        stk[++sp] = first1 ? ref + 1 : ref; stt[sp] = first1 ? t1 : t0;
+      } else if (h0) {
+        stk[++sp] = ref; stt[sp] = t0;
+      } else if (h1) {
+        stk[++sp] = ref + 1; stt[sp] = t1;
+      }
+    }
+    if (lcnt == 0) break;
+    w.leaf++;
+    w.prim += lcnt;
+    for (uint32_t j = lref; j < lref + lcnt; j++) {
+      uint32_t f;
+      int ef;
+      double e1, e2, ul1, te;
+      if (!candT(prims, sidx, j, c, f, ef, e1, e2, ul1, te)) continue;
+      const bool below = below_entry(te, lt);
+      if (te < m) {
+        m2 = m;
+        m = te;
+        e_best = lt;
+        take_tet(b, te, e1, e2, ul1, f, ef);
+        const double whi = window_hi(m);
+        int k2 = 0;
+        uint32_t v2 = 0;
+        for (int k = 0; k < nwin; k++)
+          if (wl[k] <= whi) {
+            v2 |= ((wviol >> k) & 1u) << k2;
+            wl[k2++] = wl[k];
+          }
+        nwin = k2;
+        wviol = v2;
+      } else if (te < m2) {
+        m2 = te;
+      }
+      if (te <= window_hi(m)) {
+        if (nwin < 4) {
+          wviol |= (below ? 1u : 0u) << nwin;
+          wl[nwin++] = te;
+        } else {
+          overflow = true;
+          viol_lost = viol_lost || below;
+        }
+      }
+    }
+  }
+  bool viol = viol_lost || wviol != 0;
+  // a single candidate below its box's entry e is hidden only by another
+  // primitive nearer than e (all tested: e lies below the pruning bound)
+  if (viol && nwin == 1 && !overflow)
+    viol = !(m2 >= (double)e_best) || !(e_best < bound_rel((float)m, kRelTet));
+  m_out = m;
+  defer_out = viol || nwin > 1 || overflow;
+  full_out = viol;
+}
+
 template <bool SINGLE>
 __global__ void __launch_bounds__(128)
 trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
@@ -871,85 +1031,12 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
   if (SINGLE) {
     walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
   } else {
-    // pass 1: front to back; nwin counts entry distances within 8 float
-    // steps of the running minimum m (the list is kept to recount when m
-    // drops)
-    double m = DBL_MAX;
-    double wl[4];
-    int nwin = 0;
-    bool overflow = false, viol = false;
-    uint32_t stk[kStack];
-    float stt[kStack];
-    int sp = -1;
-    {
-      const float4 *np = reinterpret_cast<const float4 *>(nodes);
-      const float4 a = __ldg(np), bb = __ldg(np + 1);
-      float t0;
-      if (ray_aabb_t<false>(FLT_MAX, a.x, a.y, a.z, bb.x, bb.y, bb.z, c.r, t0)) {
-        stk[0] = 0u;
-        stt[0] = t0;
-        sp = 0;
-      }
-    }
-    while (true) {
-      uint32_t lref = 0, lcnt = 0;
-      float lt = 0.0f;
-      while (sp >= 0) {
-        if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
-        const uint32_t ni = stk[sp];
-        const float et = stt[sp];
-        sp--;
-        const float bnd = (m < DBL_MAX) ? bound_rel((float)m, kRelTet) : FLT_MAX;
-        if (et > bnd) continue;
-        const float4 *np = reinterpret_cast<const float4 *>(nodes + ni);
-        const uint32_t meta = __float_as_uint(__ldg(&np[0].w));
-        const uint32_t ref = __float_as_uint(__ldg(&np[1].w));
-        if (meta & kLeafBit) { lref = ref; lcnt = meta & kCountMask; lt = et; break; }
-        w.branch++;
-        // the two children are adjacent: test their own boxes here
-        const float4 *cp = reinterpret_cast<const float4 *>(nodes + ref);
-        const float4 a0 = __ldg(cp), b0 = __ldg(cp + 1), a1 = __ldg(cp + 2), b1 = __ldg(cp + 3);
-        float t0, t1;
-        const bool h0 = ray_aabb_t<false>(bnd, a0.x, a0.y, a0.z, b0.x, b0.y, b0.z, c.r, t0);
-        const bool h1 = ray_aabb_t<false>(bnd, a1.x, a1.y, a1.z, b1.x, b1.y, b1.z, c.r, t1);
-        if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
-        if (h0 && h1) {
-          const bool first1 = t1 < t0;
-          stk[++sp] = first1 ? ref : ref + 1; stt[sp] = first1 ? t0 : t1;
-          stk[++sp] = first1 ? ref + 1 : ref; stt[sp] = first1 ? t1 : t0;
-        } else if (h0) {
-          stk[++sp] = ref; stt[sp] = t0;
-        } else if (h1) {
-          stk[++sp] = ref + 1; stt[sp] = t1;
-        }
-      }
-      if (lcnt == 0) break;
-      w.leaf++;
-      w.prim += lcnt;
-      for (uint32_t j = lref; j < lref + lcnt; j++) {
-        uint32_t f;
-        int ef;
-        double e1, e2, ul1, te;
-        if (!candT(prims, sidx, j, c, f, ef, e1, e2, ul1, te)) continue;
-        if (below_entry(te, lt)) viol = true;
-        if (te < m) {
-          m = te;
-          take_tet(b, te, e1, e2, ul1, f, ef);
-          const double whi = window_hi(m);
-          int k2 = 0;
-          for (int k = 0; k < nwin; k++)
-            if (wl[k] <= whi) wl[k2++] = wl[k];
-          nwin = k2;
-        }
-        if (te <= window_hi(m)) {
-          if (nwin < 4) wl[nwin++] = te;
-          else overflow = true;
-        }
-      }
-    }
-    if (!w.fail && (viol || nwin > 1 || overflow)) {
+    double m;
+    bool defer, full;
+    pass1_tet(nodes, prims, sidx, c, b, w, max_iter, m, defer, full);
+    if (!w.fail && defer) {
       const uint32_t k = atomicAdd(dcount, 1u);
-      dlist[k] = Deferred{(uint32_t)i, viol ? 1u : 0u, m};
+      dlist[k] = Deferred{(uint32_t)i, full ? 1u : 0u, m};
       add_stats(stats, w, 0);
       return;
     }
@@ -975,7 +1062,7 @@ resolve_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ p
     Work w;
     Best b;
     if (dfr.full) {
-      walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+      walkT_from(nodes, prims, sidx, c, b, w, max_iter, dfr.m);
     } else {
       const double whi = window_hi(dfr.m);
       walkT<true>(nodes, prims, sidx, c, bound_rel((float)whi, kRelTet), whi, b, w,
@@ -1056,7 +1143,8 @@ resolve_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__
     Work w;
     Best b;
     if (dfr.full) {
-      ref_walk2<SRT_TRIANGLES>(nodes, prims, nullptr, c, b, w, max_iter, root);
+      ref_walk2_from<SRT_TRIANGLES>(nodes, prims, nullptr, c, b, w, max_iter, (float)dfr.m,
+                                    root);
     } else {
       const float m = (float)dfr.m;
       window_walk2<SRT_TRIANGLES>(nodes, prims, nullptr, c, bound_rel(m, kRelTri), m, b, w,
@@ -1206,10 +1294,21 @@ srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
 // stable insertion sort: std::sort's order for up to 16 candidates); each
 // element in that order unless its entry lies beyond the nearest world hit
 // so far: the ray is taken into the element's local space with the inverse
-// transforms (Matrixd::MultV, double), traversed with the reference's walk,
-// and the hit point taken back to world space; the world distance (float
-// length) decides, strictly smaller wins.  The previous hit's primitive,
-// distance and normal apply only inside the element the ray left.
+// transforms (Matrixd::MultV, double), traversed, and the hit point taken
+// back to world space; the world distance (float length) decides, strictly
+// smaller wins.  The previous hit's primitive, distance and normal apply
+// only inside the element the ray left.
+//
+// On the GPU this runs in rounds.  scene_top_kernel walks the top-level
+// tree of every ray and stores its sorted candidates; round r takes every
+// live ray's r-th candidate, one kernel per element kind (so a warp runs one
+// kind's walk), walks the element with the same exact walks as the single
+// accel trace, applies the world-distance rule to the ray's running best and
+// queues the ray's next candidate unless that one's entry lies beyond the
+// nearest hit (then so do all later ones: they are sorted).  An element's
+// hit depends on the ray and that element alone, so the rounds return the
+// sequential loop's result exactly.  Rays with more candidates than the
+// rounds hold run the loop in one thread (scene_loop_kernel).
 namespace srt {
 namespace {
 
@@ -1244,20 +1343,13 @@ __device__ __forceinline__ void multv(const double m[16], const double v[3], dou
   for (int k = 0; k < 3; k++) o[k] = ((m[k] * v[0] + m[4 + k] * v[1]) + m[8 + k] * v[2]) + m[12 + k];
 }
 
-__global__ void __launch_bounds__(128)
-scene_trace_kernel(const TopNode *__restrict__ top, const SceneElem *__restrict__ elems,
-                   const srt_ray *__restrict__ rays, size_t n,
-                   const uint32_t *__restrict__ prev_element,
-                   const float *__restrict__ prev_normals, srt_hit *__restrict__ hits,
-                   uint32_t *__restrict__ element, uint32_t max_iter,
-                   unsigned long long *__restrict__ stats, uint32_t *__restrict__ err) {
-  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  uint32_t ntop = 0, nwalk = 0, nbranch = 0, nleaf = 0, nprim = 0;
-  uint32_t prev_prim;
-  float prev_t;
-  const RayF r0 = load_ray(rays, i, prev_prim, prev_t);
-  const double ro[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd[3] = {r0.d[0], r0.d[1], r0.d[2]};
+// The top-level walk of one ray: candidates (entry distance, element) in
+// walk order, then stably sorted by entry distance.  Returns their number.
+__device__ __forceinline__ int top_candidates(const TopNode *__restrict__ top,
+                                              const double ro[3], const double rd[3],
+                                              double ct[kTopCand], uint32_t cid[kTopCand],
+                                              uint32_t max_iter, uint32_t &ntop,
+                                              uint32_t *__restrict__ err) {
   int sgn[3];
   double inv[3];
 #pragma unroll
@@ -1265,9 +1357,6 @@ scene_trace_kernel(const TopNode *__restrict__ top, const SceneElem *__restrict_
     sgn[k] = rd[k] < 0.0 ? 1 : 0;
     inv[k] = fabs(rd[k]) > 2.0e-15 ? 1.0 / rd[k] : (rd[k] < 0.0 ? -(double)FLT_MAX : (double)FLT_MAX);
   }
-  // ---- top level: candidates in walk order
-  double ct[kTopCand];
-  uint32_t cid[kTopCand];
   int nc = 0;
   int stk[kTopStack];
   int sp = 0, node = 0;
@@ -1309,8 +1398,7 @@ scene_trace_kernel(const TopNode *__restrict__ top, const SceneElem *__restrict_
       }
     }
   }
-  // stable insertion sort by entry distance
-  for (int a = 1; a < nc; a++) {
+  for (int a = 1; a < nc; a++) {  // stable insertion sort by entry distance
     const double kt = ct[a];
     const uint32_t kid = cid[a];
     int b = a - 1;
@@ -1322,97 +1410,441 @@ scene_trace_kernel(const TopNode *__restrict__ top, const SceneElem *__restrict_
     ct[b + 1] = kt;
     cid[b + 1] = kid;
   }
-  // ---- elements, nearest world distance
-  double tnear = DBL_MAX;
-  float bt = FLT_MAX, bu = 0.0f, bv = 0.0f;
-  uint32_t bp = kNone, be = kNone;
-  for (int c = 0; c < nc; c++) {
-    if (tnear < ct[c]) continue;
-    const SceneElem &e = elems[cid[c]];
+  return nc;
+}
+
+// The ray in the element's local space: double origin and direction by the
+// inverse transforms, stored as float as the reference's Ray does.
+__device__ __forceinline__ RayF local_ray(const SceneElem &e, const double ro[3],
+                                          const double rd[3], double lo[3], double ld[3]) {
+  multv(e.invT, ro, lo);
+  multv(e.invT33, rd, ld);
+  RayF lr;
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    lr.o[k] = (float)lo[k];
+    lr.d[k] = (float)ld[k];
+    lr.sgn[k] = lr.d[k] < 0.0f ? 1 : 0;
+    lr.inv[k] = __frcp_rn(lr.d[k]);
+  }
+  return lr;
+}
+
+// World distance of a local hit: the float hit point lo + t ld, taken to
+// world space by T, minus the world origin, float length.
+__device__ __forceinline__ float world_dist(const SceneElem &e, const double lo[3],
+                                            const double ld[3], float t, const float org[3]) {
+  double lp[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)t * ld[k]);
+  double wp[3];
+  multv(e.T, lp, wp);
+  float po[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) po[k] = (float)wp[k] - org[k];
+  return sqrtf(po[0] * po[0] + po[1] * po[1] + po[2] * po[2]);
+}
+
+// Closest hit in one two-child element: the front-to-back pass, replayed in
+// the reference's order when it is not conclusive (as the resolve kernels do).
+template <int KIND>
+__device__ __forceinline__ void elem_walk2(const SceneElem &e, const Ctx2 &c, Best &b,
+                                           Work &w, uint32_t max_iter) {
+  const Node2 *nodes = static_cast<const Node2 *>(e.nodes);
+  float m;
+  uint32_t at_m;
+  bool viol;
+  pass1_node2<KIND>(nodes, e.prims, e.sidx, c, 0u, b, w, max_iter, m, at_m, viol);
+  if (w.fail || !(viol || at_m > 1)) return;
+  w.it = 0;
+  if (viol) {
+    ref_walk2_from<KIND>(nodes, e.prims, e.sidx, c, b, w, max_iter, m);
+  } else {
+    const float t0 = (KIND == SRT_TRIANGLES) ? m : nextafterf(m, FLT_MAX);
+    window_walk2<KIND>(nodes, e.prims, e.sidx, c, bound_rel(m, kRelTri), t0, b, w, max_iter);
+  }
+}
+
+__device__ __forceinline__ void elem_walkT(const SceneElem &e, const CtxT &c, Best &b, Work &w,
+                                           uint32_t max_iter) {
+  const NodeT *nodes = static_cast<const NodeT *>(e.nodes);
+  double m;
+  bool defer, full;
+  pass1_tet(nodes, e.prims, e.sidx, c, b, w, max_iter, m, defer, full);
+  if (w.fail || !defer) return;
+  w.it = 0;
+  if (full) {
+    walkT_from(nodes, e.prims, e.sidx, c, b, w, max_iter, m);
+  } else {
+    const double whi = window_hi(m);
+    walkT<true>(nodes, e.prims, e.sidx, c, bound_rel((float)whi, kRelTet), whi, b, w, max_iter);
+  }
+}
+
+// Closest hit of ray i inside element e_id (local ray, self-hit data only
+// when e_id is the ray's previous element).  Returns whether it hit, with
+// the local hit in b and the local ray in lo / ld.
+template <int KIND>
+__device__ __forceinline__ bool elem_hit(const SceneWork &W, uint32_t i, uint32_t e_id,
+                                         const SceneElem &e, const RayF &r0, uint32_t prev_prim,
+                                         float prev_t, double lo[3], double ld[3], Best &b,
+                                         Work &w) {
+  const double ro[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd[3] = {r0.d[0], r0.d[1], r0.d[2]};
+  const RayF lr = local_ray(e, ro, rd, lo, ld);
+  const bool same = W.prev_element && __ldg(&W.prev_element[i]) == e_id;
+  if (KIND == SRT_TETRAHEDRA) {
+    CtxT c;
+    c.r = lr;
+    c.o = {lr.o[0], lr.o[1], lr.o[2]};
+    c.d = {lr.d[0], lr.d[1], lr.d[2]};
+    c.prev_prim = same ? prev_prim : kNone;
+    elem_walkT(e, c, b, w, W.max_iter);
+  } else {
+    Ctx2 c;
+    c.r = lr;
+    c.prev_prim = same ? prev_prim : kNone;
+    c.prev_t = same ? prev_t : 0.0f;
+    c.keps = e.scene->keps;
+#pragma unroll
+    for (int k = 0; k < 3; k++)
+      c.pn[k] = (same && W.prev_normals) ? __ldg(&W.prev_normals[3 * (size_t)i + k]) : 0.0f;
+    elem_walk2<KIND>(e, c, b, w, W.max_iter);
+  }
+  if (w.fail) atomicOr(W.err, kErrIter);
+  return b.t < FLT_MAX && b.prim != kNone;
+}
+
+__device__ __forceinline__ uint32_t lanemask_lt() {
+  return (1u << (threadIdx.x & 31u)) - 1u;
+}
+
+// Append item to the list and count it for element e (one atomic per warp
+// for the list, one per warp and element for the counts).
+__device__ __forceinline__ void push_item(uint32_t *__restrict__ list,
+                                          uint32_t *__restrict__ list_count,
+                                          uint32_t *__restrict__ ecount, uint32_t e,
+                                          uint32_t item) {
+  const unsigned act = __activemask();
+  const int lane = (int)(threadIdx.x & 31u);
+  const int leader = __ffs(act) - 1;
+  uint32_t base = 0;
+  if (lane == leader) base = atomicAdd(list_count, (uint32_t)__popc(act));
+  base = __shfl_sync(act, base, leader);
+  list[base + __popc(act & lanemask_lt())] = item;
+  const unsigned grp = __match_any_sync(act, e);
+  if (lane == __ffs(grp) - 1) atomicAdd(&ecount[e], (uint32_t)__popc(grp));
+}
+
+__device__ __forceinline__ void add_counts(unsigned long long *__restrict__ stats, int first,
+                                           const uint32_t *c, int nc) {
+  const unsigned m = __activemask();
+  const int leader = __ffs(m) - 1;
+  for (int k = 0; k < nc; k++) {
+    const uint32_t s = __reduce_add_sync(m, c[k]);
+    if ((int)(threadIdx.x & 31u) == leader) atomicAdd(&stats[first + k], (unsigned long long)s);
+  }
+}
+
+__device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
+
+// Items: phase 0 holds ray ids (the first candidate), phase 1 holds
+// ray * kRoundCand + slot.
+__device__ __forceinline__ void item_ray_slot(int phase, uint32_t item, uint32_t &ray,
+                                              uint32_t &slot) {
+  ray = phase ? item / kRoundCand : item;
+  slot = phase ? item % kRoundCand : 0u;
+}
+
+__global__ void __launch_bounds__(128)
+scene_top_kernel(const TopNode *__restrict__ top, SceneWork W) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= W.n) return;
+  const float4 *r4 = reinterpret_cast<const float4 *>(W.rays + i);
+  const float4 a = __ldg(&r4[0]), b = __ldg(&r4[1]);
+  const double ro[3] = {a.x, a.y, a.z}, rd[3] = {b.x, b.y, b.z};
+  double ct[kTopCand];
+  uint32_t cid[kTopCand];
+  uint32_t ntop = 0;
+  const int nc = top_candidates(top, ro, rd, ct, cid, W.max_iter, ntop, W.err);
+  reinterpret_cast<float4 *>(W.hits)[i] = make_float4(FLT_MAX, 0.0f, 0.0f, __uint_as_float(kNone));
+  if (W.element) W.element[i] = kNone;
+  W.tnear[i] = inf_f();
+  if (nc > kRoundCand) {
+    W.ncand[i] = 0;
+    W.ovf[atomicAdd(&W.counters[2], 1u)] = (uint32_t)i;
+  } else {
+    W.ncand[i] = (uint8_t)nc;
+    for (int c = 0; c < nc; c++) {
+      W.cand_t[i * kRoundCand + c] = ct[c];
+      W.cand_e[i * kRoundCand + c] = cid[c];
+    }
+    if (nc > 0) push_item(W.items, &W.counters[0], W.ecount, cid[0], (uint32_t)i);
+  }
+  if (W.stats) add_counts(W.stats, 0, &ntop, 1);
+}
+
+// Offsets of each element's items in the sorted list (elements taken in
+// kind order, so each kind's items are one range); one block.
+__global__ void __launch_bounds__(256)
+scene_scan_kernel(SceneWork W, int phase) {
+  const uint32_t *cnt = W.ecount + (size_t)phase * W.nelem;
+  __shared__ uint32_t warp_sum[8];
+  __shared__ uint32_t carry;
+  __shared__ uint32_t kstart[3], kend[3];
+  if (threadIdx.x == 0) carry = 0;
+  if (threadIdx.x < 3) {
+    kstart[threadIdx.x] = 0xffffffffu;
+    kend[threadIdx.x] = 0u;
+  }
+  __syncthreads();
+  for (uint32_t base = 0; base < W.nelem; base += blockDim.x) {
+    const uint32_t j = base + threadIdx.x;
+    const uint32_t e = j < W.nelem ? W.elem_order[j] : 0u;
+    const uint32_t v = j < W.nelem ? cnt[e] : 0u;
+    uint32_t x = v;  // inclusive warp scan
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
+      if ((int)(threadIdx.x & 31u) >= o) x += y;
+    }
+    if ((threadIdx.x & 31u) == 31u) warp_sum[threadIdx.x >> 5] = x;
+    __syncthreads();
+    uint32_t woff = 0;
+    for (uint32_t w = 0; w < (threadIdx.x >> 5); w++) woff += warp_sum[w];
+    const uint32_t excl = carry + woff + x - v;
+    if (j < W.nelem) {
+      W.ecursor[e] = excl;
+      const int k = __ldg(&W.elems[e].kind);
+      atomicMin(&kstart[k], excl);
+      atomicMax(&kend[k], excl + v);
+    }
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
+    __syncthreads();
+  }
+  if (threadIdx.x < 3) {
+    const bool any = kstart[threadIdx.x] != 0xffffffffu;
+    W.krange[2 * threadIdx.x] = any ? kstart[threadIdx.x] : 0u;
+    W.krange[2 * threadIdx.x + 1] = any ? kend[threadIdx.x] : 0u;
+  }
+}
+
+// Items into element order (contiguous per element; the warp's own rays
+// stay together).
+__global__ void __launch_bounds__(128)
+scene_scatter_kernel(SceneWork W, int phase) {
+  const uint32_t cnt = *(volatile uint32_t *)&W.counters[phase];
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t item = W.items[k];
+    uint32_t ray, slot;
+    item_ray_slot(phase, item, ray, slot);
+    const uint32_t e = W.cand_e[(size_t)ray * kRoundCand + slot];
+    const unsigned act = __activemask();
+    const unsigned grp = __match_any_sync(act, e);
+    const int leader = __ffs(grp) - 1;
+    uint32_t base = 0;
+    if ((int)(threadIdx.x & 31u) == leader) base = atomicAdd(&W.ecursor[e], (uint32_t)__popc(grp));
+    base = __shfl_sync(grp, base, leader);
+    W.sorted[base + __popc(grp & lanemask_lt())] = item;
+  }
+}
+
+// The element walks of one kind.  Phase 0 (each ray's first candidate):
+// the result becomes the ray's running best.  Phase 1 (later candidates
+// that the early cull keeps after phase 0): results per (ray, slot) for the
+// selection.
+template <int KIND>
+__global__ void __launch_bounds__(128)
+scene_walk_kernel(SceneWork W, int phase) {
+  const uint32_t lo_k = *(volatile uint32_t *)&W.krange[2 * KIND];
+  const uint32_t hi_k = *(volatile uint32_t *)&W.krange[2 * KIND + 1];
+  uint32_t c[4] = {0, 0, 0, 0};  // element walks, branch nodes, leaves, primitives
+  for (uint32_t k = lo_k + blockIdx.x * blockDim.x + threadIdx.x; k < hi_k;
+       k += gridDim.x * blockDim.x) {
+    uint32_t ray, slot;
+    item_ray_slot(phase, W.sorted[k], ray, slot);
+    const size_t cs = (size_t)ray * kRoundCand + slot;
+    const uint32_t e_id = W.cand_e[cs];
+    const SceneElem &e = W.elems[e_id];
+    uint32_t prev_prim;
+    float prev_t;
+    const RayF r0 = load_ray(W.rays, ray, prev_prim, prev_t);
     double lo[3], ld[3];
-    multv(e.invT, ro, lo);
-    multv(e.invT33, rd, ld);
-    const bool same = prev_element && prev_element[i] == cid[c];
-    RayF lr;
-#pragma unroll
-    for (int k = 0; k < 3; k++) {
-      lr.o[k] = (float)lo[k];
-      lr.d[k] = (float)ld[k];
-      lr.sgn[k] = lr.d[k] < 0.0f ? 1 : 0;
-      lr.inv[k] = __frcp_rn(lr.d[k]);
-    }
-    Work w;
     Best b;
-    if (e.kind == SRT_TETRAHEDRA) {
-      CtxT ct2;
-      ct2.r = lr;
-      ct2.o = {lr.o[0], lr.o[1], lr.o[2]};
-      ct2.d = {lr.d[0], lr.d[1], lr.d[2]};
-      ct2.prev_prim = same ? prev_prim : kNone;
-      walkT<false>(static_cast<const NodeT *>(e.nodes), e.prims, e.sidx, ct2, 0.0f, 0.0, b, w,
-                   max_iter);
+    Work w;
+    const bool hit = elem_hit<KIND>(W, ray, e_id, e, r0, prev_prim, prev_t, lo, ld, b, w);
+    c[0]++;
+    c[1] += w.branch;
+    c[2] += w.leaf;
+    c[3] += w.prim;
+    const float tw = hit ? world_dist(e, lo, ld, b.t, r0.o) : inf_f();
+    if (phase == 0) {
+      if (hit && tw < inf_f()) {
+        W.tnear[ray] = tw;
+        reinterpret_cast<float4 *>(W.hits)[ray] =
+            make_float4(tw, b.u, b.v, __uint_as_float(b.prim));
+        if (W.element) W.element[ray] = e_id;
+      }
     } else {
-      Ctx2 c2;
-      c2.r = lr;
-      c2.prev_prim = same ? prev_prim : kNone;
-      c2.prev_t = same ? prev_t : 0.0f;
-      c2.keps = e.scene->keps;
-#pragma unroll
-      for (int k = 0; k < 3; k++) c2.pn[k] = (same && prev_normals) ? prev_normals[3 * i + k] : 0.0f;
-      if (e.kind == SRT_TRIANGLES)
-        ref_walk2<SRT_TRIANGLES>(static_cast<const Node2 *>(e.nodes), e.prims, e.sidx, c2, b, w,
-                                 max_iter);
-      else
-        ref_walk2<SRT_SPHERES>(static_cast<const Node2 *>(e.nodes), e.prims, e.sidx, c2, b, w,
-                               max_iter);
-    }
-    if (w.fail) atomicOr(err, kErrIter);
-    nwalk++;
-    nbranch += w.branch;
-    nleaf += w.leaf;
-    nprim += w.prim;
-    if (!(b.t < FLT_MAX && b.prim != kNone)) continue;
-    double lp[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)b.t * ld[k]);
-    double wp[3];
-    multv(e.T, lp, wp);
-    float po[3];
-#pragma unroll
-    for (int k = 0; k < 3; k++) po[k] = (float)wp[k] - r0.o[k];
-    const float tw = sqrtf(po[0] * po[0] + po[1] * po[1] + po[2] * po[2]);
-    if ((double)tw < tnear) {
-      tnear = tw;
-      bt = tw;
-      bu = b.u;
-      bv = b.v;
-      bp = b.prim;
-      be = cid[c];
+      W.res[cs] = make_float4(tw, b.u, b.v, __uint_as_float(hit ? b.prim : kNone));
     }
   }
-  reinterpret_cast<float4 *>(hits)[i] = make_float4(bt, bu, bv, __uint_as_float(bp));
-  if (element) element[i] = be;
-  if (stats) {  // warp sums of the visit counters, one atomic per warp each
-    const unsigned m = __activemask();
-    const uint32_t c[5] = {__reduce_add_sync(m, ntop), __reduce_add_sync(m, nwalk),
-                           __reduce_add_sync(m, nbranch), __reduce_add_sync(m, nleaf),
-                           __reduce_add_sync(m, nprim)};
-    if ((threadIdx.x & 31u) == (uint32_t)(__ffs(m) - 1))
-      for (int k = 0; k < 5; k++) atomicAdd(&stats[k], (unsigned long long)c[k]);
+  if (W.stats) add_counts(W.stats, 1, c, 4);
+}
+
+// Phase 1 items: every later candidate whose entry does not lie beyond the
+// nearest hit of phase 0 (the candidates are sorted, so the first culled
+// one ends the list).  The sequential loop walks a subset of these: its
+// nearest distance only shrinks.
+__global__ void __launch_bounds__(128)
+scene_gather_kernel(SceneWork W) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= W.n) return;
+  const uint32_t nc = W.ncand[i];
+  if (nc < 2) return;
+  const double tn = (double)W.tnear[i];
+  for (uint32_t c = 1; c < nc; c++) {
+    const size_t cs = i * kRoundCand + c;
+    if (tn < W.cand_t[cs]) break;
+    push_item(W.items, &W.counters[1], W.ecount + W.nelem, W.cand_e[cs], (uint32_t)cs);
+  }
+}
+
+// The sequential rule over candidates 1.. of each ray, from the phase-0
+// best: skip a candidate entered beyond the nearest hit, take a strictly
+// nearer hit.
+__global__ void __launch_bounds__(128)
+scene_select_kernel(SceneWork W) {
+  const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  if (i >= W.n) return;
+  const uint32_t nc = W.ncand[i];
+  if (nc < 2) return;
+  float tn = W.tnear[i];
+  int best = -1;
+  float4 bh = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  for (uint32_t c = 1; c < nc; c++) {
+    const size_t cs = i * kRoundCand + c;
+    if ((double)tn < W.cand_t[cs]) break;
+    const float4 r = W.res[cs];
+    if (__float_as_uint(r.w) != kNone && r.x < tn) {
+      tn = r.x;
+      bh = r;
+      best = (int)c;
+    }
+  }
+  if (best >= 0) {
+    reinterpret_cast<float4 *>(W.hits)[i] = bh;
+    if (W.element) W.element[i] = W.cand_e[i * kRoundCand + best];
+  }
+}
+
+// The whole loop in one thread, for the rays with more candidates than
+// the per-ray slots hold.
+__global__ void __launch_bounds__(128)
+scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
+  const uint32_t cnt = *(volatile uint32_t *)&W.counters[2];
+  uint32_t c[4] = {0, 0, 0, 0};
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
+       k += gridDim.x * blockDim.x) {
+    const uint32_t i = W.ovf[k];
+    uint32_t prev_prim;
+    float prev_t;
+    const RayF r0 = load_ray(W.rays, i, prev_prim, prev_t);
+    const double ro[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd[3] = {r0.d[0], r0.d[1], r0.d[2]};
+    double ct[kTopCand];
+    uint32_t cid[kTopCand];
+    uint32_t ntop = 0;
+    const int nc = top_candidates(top, ro, rd, ct, cid, W.max_iter, ntop, W.err);
+    double tnear = DBL_MAX;
+    float bt = FLT_MAX, bu = 0.0f, bv = 0.0f;
+    uint32_t bp = kNone, be = kNone;
+    for (int q = 0; q < nc; q++) {
+      if (tnear < ct[q]) continue;
+      const SceneElem &e = W.elems[cid[q]];
+      double lo[3], ld[3];
+      Best b;
+      Work w;
+      bool hit;
+      if (e.kind == SRT_TETRAHEDRA)
+        hit = elem_hit<SRT_TETRAHEDRA>(W, i, cid[q], e, r0, prev_prim, prev_t, lo, ld, b, w);
+      else if (e.kind == SRT_TRIANGLES)
+        hit = elem_hit<SRT_TRIANGLES>(W, i, cid[q], e, r0, prev_prim, prev_t, lo, ld, b, w);
+      else
+        hit = elem_hit<SRT_SPHERES>(W, i, cid[q], e, r0, prev_prim, prev_t, lo, ld, b, w);
+      c[0]++;
+      c[1] += w.branch;
+      c[2] += w.leaf;
+      c[3] += w.prim;
+      if (!hit) continue;
+      const float tw = world_dist(e, lo, ld, b.t, r0.o);
+      if ((double)tw < tnear) {
+        tnear = tw;
+        bt = tw;
+        bu = b.u;
+        bv = b.v;
+        bp = b.prim;
+        be = cid[q];
+      }
+    }
+    reinterpret_cast<float4 *>(W.hits)[i] = make_float4(bt, bu, bv, __uint_as_float(bp));
+    if (W.element) W.element[i] = be;
+  }
+  if (W.stats) add_counts(W.stats, 1, c, 4);
+}
+
+// Resident blocks per SM of the persistent kernels (the same on every device
+// of one architecture): walks of the three kinds, scatter, loop.
+int g_per_sm[5] = {1, 1, 1, 1, 1};
+std::once_flag g_per_sm_once;
+
+void scene_occupancy() {
+  const void *fn[5] = {(const void *)scene_walk_kernel<SRT_TRIANGLES>,
+                       (const void *)scene_walk_kernel<SRT_TETRAHEDRA>,
+                       (const void *)scene_walk_kernel<SRT_SPHERES>,
+                       (const void *)scene_scatter_kernel, (const void *)scene_loop_kernel};
+  for (int k = 0; k < 5; k++) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn[k], 128, 0);
+    g_per_sm[k] = per_sm > 0 ? per_sm : 1;
   }
 }
 
 }  // namespace
 
-srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, const SceneElem *elems,
-                              const srt_ray *rays, size_t n, const uint32_t *prev_element,
-                              const float *prev_normals, srt_hit *hits, uint32_t *element,
-                              uint32_t max_iter, unsigned long long *stats) {
-  if (n == 0) return SRT_OK;
-  scene_trace_kernel<<<(unsigned)((n + 127) / 128), 128, 0, ctx->stream>>>(
-      top, elems, rays, n, prev_element, prev_normals, hits, element, max_iter, stats,
-      ctx->d_err);
+srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds) {
+  if (W.n == 0) return SRT_OK;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e = cudaMemsetAsync(W.counters, 0, (4 + 2 * (size_t)W.nelem) * sizeof(uint32_t), st);
+  if (e != cudaSuccess) return cuda_status(e, "scene counters");
+  std::call_once(g_per_sm_once, scene_occupancy);
+  const unsigned rgrid = (unsigned)((W.n + 127) / 128);
+  scene_top_kernel<<<rgrid, 128, 0, st>>>(top, W);
   ctx->launches++;
+  for (int phase = 0; phase < 2; phase++) {
+    if (phase == 1) {
+      scene_gather_kernel<<<rgrid, 128, 0, st>>>(W);
+      ctx->launches++;
+    }
+    scene_scan_kernel<<<1, 256, 0, st>>>(W, phase);
+    scene_scatter_kernel<<<(unsigned)(ctx->num_sms * g_per_sm[3]), 128, 0, st>>>(W, phase);
+    ctx->launches += 2;
+    static const int order[3] = {SRT_TRIANGLES, SRT_SPHERES, SRT_TETRAHEDRA};
+    for (int q = 0; q < 3; q++) {
+      const int k = order[q];
+      if (!(kinds & (1u << k))) continue;
+      const unsigned grid = (unsigned)(ctx->num_sms * g_per_sm[k]);
+      if (k == SRT_TRIANGLES)
+        scene_walk_kernel<SRT_TRIANGLES><<<grid, 128, 0, st>>>(W, phase);
+      else if (k == SRT_SPHERES)
+        scene_walk_kernel<SRT_SPHERES><<<grid, 128, 0, st>>>(W, phase);
+      else
+        scene_walk_kernel<SRT_TETRAHEDRA><<<grid, 128, 0, st>>>(W, phase);
+      ctx->launches++;
+    }
+  }
+  scene_select_kernel<<<rgrid, 128, 0, st>>>(W);
+  scene_loop_kernel<<<(unsigned)(ctx->num_sms * g_per_sm[4]), 128, 0, st>>>(top, W);
+  ctx->launches += 2;
   return cuda_status(cudaGetLastError(), "scene trace");
 }
 

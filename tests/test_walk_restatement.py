@@ -1,6 +1,6 @@
 """The product's default traversal (front-to-back pass, reference-order
-replay only for exact ties, reference walk when a primitive reports a
-distance before its leaf box's entry), restated in the oracle
+replay only for exact ties, reference walk when a candidate at the smallest
+distance reports a distance before its leaf box's entry), restated in the oracle
 (so_trace2), against the reference's Traverse (so_trace, itself pinned to the
 reference build): identical hits on every ray."""
 import numpy as np
@@ -41,9 +41,10 @@ def pole_pairs(n=48, z=0.5, dist=4.0, gap=5e-7, seed=45):
     """Sphere pairs hit at their poles: centres on an n x n grid at height z,
     each with a twin `gap` further down, and one orthographic ray down -z from
     z + dist through every centre.  A pole hit lies one leaf padding (16
-    ulp(1)) behind its box face, within the rounding tolerance of a distance
-    of ~4, and the twin's hit is within it too -- the case where the
-    reference's pruning decides which of the two it reports."""
+    ulp(1)) behind its box face, less than the float error of a hit distance
+    of ~4, so some hits report a distance below their box's entry, and the
+    twin's hit lies within that error too -- the case where the reference's
+    pruning decides which of the two it reports."""
     rng = np.random.default_rng(seed)
     g = (np.arange(n) + 0.5) / n
     X, Y = np.meshgrid(g, g)
@@ -96,3 +97,42 @@ def test_restated_walk_vs_reference_build():
     hr, sr = O.RefAccel(O.TET, v, f).trace(rays)
     same(h2, hr)
     assert np.array_equal(s2, sr)
+
+
+def _far_rays(rng, n, lo, hi, dist, scale):
+    c = 0.5 * (lo + hi)
+    rad = 0.5 * np.linalg.norm(hi - lo)
+    o = c + (rad + dist) * S._normalize(rng.normal(size=(n, 3)))
+    tgt = lo + rng.uniform(size=(n, 3)) * (hi - lo)
+    rays = np.zeros(n, O.RAY_DTYPE)
+    rays["org"] = o
+    rays["dir"] = S._normalize(tgt - o) * scale
+    rays["prev_prim"] = O.MISS
+    return rays
+
+
+@pytest.mark.parametrize("kind", ["tri", "tet", "sphere"])
+def test_far_origins_and_scaled_directions(kind):
+    """Rays from 10 and 100 units away with non-unit directions (the local
+    rays of transformed scene elements): hit distances far above the leaf
+    padding, where float distances round below their box's entry."""
+    rng = np.random.default_rng({"tri": 1, "tet": 2, "sphere": 3}[kind])
+    if kind == "tri":
+        v, f = S.displaced_octasphere(5, seed=46)
+        o, lo, hi = O.OracleAccel(O.TRI, v, f), -1.1 * np.ones(3), 1.1 * np.ones(3)
+    elif kind == "tet":
+        v, f, _ = S.tet_grid(20, seed=47)
+        o, lo, hi = O.OracleAccel(O.TET, v, f), np.zeros(3), np.ones(3)
+    else:
+        p, r = S.particles(100_000, seed=48, median_radius=0.01)
+        o, lo, hi = O.OracleAccel(O.SPHERE, p, None, r), np.zeros(3), np.ones(3)
+    fell = 0
+    for dist in (10.0, 100.0):
+        for scale in (0.37, 2.9):
+            rays = _far_rays(rng, 20_000, lo, hi, dist, scale)
+            h2, st = o.trace2(rays, want_stats=True)
+            h1 = o.trace(rays)
+            same(h2, h1[0] if isinstance(h1, tuple) else h1)
+            fell += int(st[3])
+    if kind == "sphere":
+        assert fell > 0  # the reference-walk fallback is exercised
