@@ -539,9 +539,9 @@ static srt_status sort_scratch(srt_ctx *ctx, size_t n) {
 }
 
 // Stable LSD sort of (keys, vals) by key; result lands back in keys/vals.
-// identity_vals: vals are 0..n-1 on entry (not read).  key_bits <= 30 (Morton
-// codes): three 10-bit passes, otherwise four 8-bit passes; either way the
-// order is the stable order by key.  With nseg > 1 a last pass groups the
+// identity_vals: vals are 0..n-1 on entry (not read).  key_bits <= 30: one
+// 10-bit pass per 10 bits (three for Morton codes), otherwise four 8-bit
+// passes; either way the order is the stable order by key.  With nseg > 1 a last pass groups the
 // result by the segment of each value (the segment offsets `seg` are global
 // indices), i.e. the order is (segment, key, value).
 srt_status sort_pairs_seg(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n,
@@ -552,7 +552,7 @@ srt_status sort_pairs_seg(srt_ctx *ctx, uint32_t *keys, uint32_t *vals, size_t n
   uint32_t *k0 = keys, *v0 = vals, *k1 = ctx->s_keys2.as<uint32_t>(),
            *v1 = ctx->s_vals2.as<uint32_t>();
   const bool narrow = key_bits <= 30;
-  const int passes = narrow ? 3 : 4;
+  const int passes = narrow ? (key_bits < 1 ? 1 : (key_bits + 9) / 10) : 4;
   for (int pass = 0; pass < passes; pass++) {
     const uint32_t *vin = (pass == 0 && identity_vals) ? nullptr : v0;
     s = narrow ? sort_pass<false, 10>(ctx, k0, vin, k1, v1, n, pass * 10, nullptr, 0)

@@ -198,17 +198,27 @@ struct SceneElem {
 };
 // Device arrays of one scene trace (srt_trace.cu): per ray its candidates
 // (kRoundCand slots of entry distance and element) and running nearest
-// world distance; the item lists of the two phases (unsorted, then in
-// element order) with per-element counts and cursors, each kind's range of
-// the sorted list, per-(ray, slot) results of the second phase, and the
-// list of rays with more candidates than slots.  counters: [0] phase-0
-// items, [1] phase-1 items, [2] overflow rays, [3] unused; ecount [2][nelem]
-// follows counters directly (one memset clears both).
+// world distance; the dense sort keys (element rank in kind order, nelem
+// for none) and values of the two phases -- phase 0: one per ray (its first
+// candidate), phase 1: kRoundCand - 1 per ray (its later candidates) --;
+// the per-(ray, slot) results of phase 1 and the list of rays with more
+// candidates than slots.  counters: [2] overflow rays, [4 + 3p + k] warp
+// fetch and [10 + 3p + k] deferred items of phase p, kind k; bounds [2][4]:
+// each kind's range of a phase's sorted keys (kinds are rank ranges
+// rank_start[k] .. rank_start[k + 1]).
 constexpr int kRoundCand = 8;
+constexpr int kSceneCounters = 16;
+// A ray (or scene item) whose front-to-back pass was not conclusive.
+struct Deferred {
+  uint32_t ray;
+  uint32_t full;  // 1: the reference's walk from the pass's bound; 0: replay the tie at m
+  double m;
+};
 struct SceneWork {
   const SceneElem *elems;
-  const uint32_t *elem_order;  // element ids by kind
+  const uint32_t *elem_rank;  // element id -> rank in kind order
   uint32_t nelem;
+  uint32_t rank_start[4];     // first rank of triangles, tetrahedra, spheres; nelem
   const srt_ray *rays;
   const uint32_t *prev_element;
   const float *prev_normals;
@@ -218,17 +228,27 @@ struct SceneWork {
   uint32_t *cand_e;
   uint8_t *ncand;
   float *tnear;
-  uint32_t *items, *sorted;
+  uint32_t *keys0, *vals0, *keys1, *vals1;
   float4 *res;
-  uint32_t *counters, *ecount, *ecursor, *krange;
+  Deferred *dlist;  // per phase, kind k's deferred items from bounds[k] on
+  uint32_t *counters, *bounds;
   uint32_t *ovf;
   size_t n;
   uint32_t max_iter;
   unsigned long long *stats;
   uint32_t *err;
 };
+// Side streams of a scene's trace: one per element kind and one for the
+// rays with more candidates than slots, forked from and joined to the
+// context stream with events (also inside a graph capture).
+struct SceneStreams {
+  cudaStream_t side[4] = {};
+  cudaEvent_t fork[3] = {};  // top level done, phase 0 items ready, phase 1 items ready
+  cudaEvent_t join[4] = {};  // each side stream's latest work
+};
 // kinds: bit k set when the scene holds elements of kind k.
-srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds);
+srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds,
+                              const SceneStreams &ss);
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
 // array in context scratch, valid until the context's next sort.
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);

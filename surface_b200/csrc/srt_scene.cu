@@ -25,10 +25,20 @@ struct srt_scene {
   };
   std::vector<Elem> elems;
   std::vector<TopNode> top;
-  DevBuf d_top, d_elems, d_order, scratch;
+  DevBuf d_top, d_elems, d_rank, scratch;
   bool built = false;
   uint32_t max_iter = 64;
-  uint32_t kinds = 0;  // bit k: the scene holds elements of kind k
+  uint32_t kinds = 0;          // bit k: the scene holds elements of kind k
+  uint32_t rank_start[4] = {};  // first rank of each kind (kind order), count
+  SceneStreams ss;
+  ~srt_scene() {
+    for (cudaStream_t &q : ss.side)
+      if (q) cudaStreamDestroy(q);
+    for (cudaEvent_t &v : ss.fork)
+      if (v) cudaEventDestroy(v);
+    for (cudaEvent_t &v : ss.join)
+      if (v) cudaEventDestroy(v);
+  }
 };
 
 namespace {
@@ -235,6 +245,17 @@ SRT_API srt_status srt_scene_create(srt_ctx *ctx, srt_scene **out) {
   srt_scene *s = new (std::nothrow) srt_scene();
   if (!s) return SRT_ERR_NO_MEMORY;
   s->ctx = ctx;
+  cudaError_t e = cudaSetDevice(ctx->device);
+  for (int k = 0; k < 4 && e == cudaSuccess; k++)
+    e = cudaStreamCreateWithFlags(&s->ss.side[k], cudaStreamNonBlocking);
+  for (int k = 0; k < 3 && e == cudaSuccess; k++)
+    e = cudaEventCreateWithFlags(&s->ss.fork[k], cudaEventDisableTiming);
+  for (int k = 0; k < 4 && e == cudaSuccess; k++)
+    e = cudaEventCreateWithFlags(&s->ss.join[k], cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    delete s;
+    return cuda_status(e, "scene streams");
+  }
   *out = s;
   return SRT_OK;
 }
@@ -243,6 +264,8 @@ SRT_API srt_status srt_scene_destroy(srt_scene *s) {
   if (!s) return SRT_OK;
   cudaSetDevice(s->ctx->device);
   cudaStreamSynchronize(s->ctx->stream);
+  for (cudaStream_t q : s->ss.side)
+    if (q) cudaStreamSynchronize(q);
   delete s;
   return SRT_OK;
 }
@@ -335,19 +358,24 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
   }
   cudaSetDevice(s->ctx->device);
   cudaError_t e;
-  // element ids grouped by kind (triangles, tetrahedra, spheres), each
-  // group in id order: the layout of the trace's element-sorted item lists
-  std::vector<uint32_t> order;
-  for (int k = 0; k < 3; k++)
+  // element ranks: ids grouped by kind (triangles, tetrahedra, spheres),
+  // each group in id order -- the trace sorts its items by rank, so each
+  // kind's items form one range
+  std::vector<uint32_t> rank(el.size());
+  uint32_t r = 0;
+  for (int k = 0; k < 3; k++) {
+    s->rank_start[k] = r;
     for (size_t i = 0; i < el.size(); i++)
-      if (el[i].kind == k) order.push_back((uint32_t)i);
-  if (order.size() != el.size()) {
+      if (el[i].kind == k) rank[i] = r++;
+  }
+  s->rank_start[3] = r;
+  if (r != el.size()) {
     set_error("scene element of unknown kind");
     return SRT_ERR_INVALID;
   }
   if ((e = s->d_top.ensure(s->top.size() * sizeof(TopNode))) != cudaSuccess ||
       (e = s->d_elems.ensure(el.size() * sizeof(SceneElem))) != cudaSuccess ||
-      (e = s->d_order.ensure(order.size() * sizeof(uint32_t))) != cudaSuccess)
+      (e = s->d_rank.ensure(rank.size() * sizeof(uint32_t))) != cudaSuccess)
     return cuda_status(e, "scene tables");
   cudaStream_t st = s->ctx->stream;
   e = cudaMemcpyAsync(s->d_top.p, s->top.data(), s->top.size() * sizeof(TopNode),
@@ -356,7 +384,7 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
     e = cudaMemcpyAsync(s->d_elems.p, el.data(), el.size() * sizeof(SceneElem),
                         cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(s->d_order.p, order.data(), order.size() * sizeof(uint32_t),
+    e = cudaMemcpyAsync(s->d_rank.p, rank.data(), rank.size() * sizeof(uint32_t),
                         cudaMemcpyHostToDevice, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // host tables go out of scope
   if (e != cudaSuccess) return cuda_status(e, "scene upload");
@@ -412,22 +440,22 @@ SRT_API srt_status srt_scene_trace(srt_scene *s, const srt_ray *rays, size_t n,
     set_error("ray and hit arrays must be 16-byte aligned");
     return SRT_ERR_INVALID;
   }
-  if (n >= (1ull << 29)) {
+  if (n >= (1ull << 29)) {  // the phase-1 items n * 7 are 32-bit indices
     set_error("srt_scene_trace: at most 2^29 - 1 rays per call");
     return SRT_ERR_LIMIT;
   }
   // scratch sections (each 256-byte aligned): candidates, nearest distance,
-  // candidate counts, item lists, second-phase results, overflow list,
-  // counters + per-element counts, cursors, kind ranges
+  // candidate counts, sort keys and values of both phases, phase-1 results,
+  // overflow list, counters, kind bounds
   auto al = [](size_t b) { return (b + 255) & ~(size_t)255; };
   const size_t ne = s->elems.size();
-  const size_t nk = n * kRoundCand;
+  const size_t nk = n * kRoundCand, n1 = n * (kRoundCand - 1);
   const size_t b_ct = al(nk * sizeof(double)), b_ce = al(nk * 4), b_tn = al(n * 4),
-               b_nc = al(n), b_items = al(nk * 4), b_sorted = al(nk * 4),
-               b_res = al(nk * sizeof(float4)), b_ovf = al(n * 4),
-               b_cnt = al((4 + 2 * ne) * 4), b_cur = al(ne * 4), b_kr = al(6 * 4);
-  e = s->scratch.ensure(b_ct + b_ce + b_tn + b_nc + b_items + b_sorted + b_res + b_ovf + b_cnt +
-                        b_cur + b_kr);
+               b_nc = al(n), b_k0 = al(n * 4), b_k1 = al(n1 * 4),
+               b_res = al(nk * sizeof(float4)), b_dl = al(n1 * sizeof(Deferred)),
+               b_ovf = al(n * 4), b_cnt = al(kSceneCounters * 4), b_bd = al(8 * 4);
+  e = s->scratch.ensure(b_ct + b_ce + b_tn + b_nc + 2 * b_k0 + 2 * b_k1 + b_res + b_dl + b_ovf +
+                        b_cnt + b_bd);
   if (e != cudaSuccess) return cuda_status(e, "scene trace scratch");
   char *p = s->scratch.as<char>();
   auto take = [&p](size_t bytes) {
@@ -437,8 +465,9 @@ SRT_API srt_status srt_scene_trace(srt_scene *s, const srt_ray *rays, size_t n,
   };
   SceneWork W;
   W.elems = s->d_elems.as<SceneElem>();
-  W.elem_order = s->d_order.as<uint32_t>();
+  W.elem_rank = s->d_rank.as<uint32_t>();
   W.nelem = (uint32_t)ne;
+  for (int k = 0; k < 4; k++) W.rank_start[k] = s->rank_start[k];
   W.rays = rays;
   W.prev_element = prev_element;
   W.prev_normals = prev_normals;
@@ -448,19 +477,20 @@ SRT_API srt_status srt_scene_trace(srt_scene *s, const srt_ray *rays, size_t n,
   W.cand_e = reinterpret_cast<uint32_t *>(take(b_ce));
   W.tnear = reinterpret_cast<float *>(take(b_tn));
   W.ncand = reinterpret_cast<uint8_t *>(take(b_nc));
-  W.items = reinterpret_cast<uint32_t *>(take(b_items));
-  W.sorted = reinterpret_cast<uint32_t *>(take(b_sorted));
+  W.keys0 = reinterpret_cast<uint32_t *>(take(b_k0));
+  W.vals0 = reinterpret_cast<uint32_t *>(take(b_k0));
+  W.keys1 = reinterpret_cast<uint32_t *>(take(b_k1));
+  W.vals1 = reinterpret_cast<uint32_t *>(take(b_k1));
   W.res = reinterpret_cast<float4 *>(take(b_res));
+  W.dlist = reinterpret_cast<Deferred *>(take(b_dl));
   W.ovf = reinterpret_cast<uint32_t *>(take(b_ovf));
   W.counters = reinterpret_cast<uint32_t *>(take(b_cnt));
-  W.ecount = W.counters + 4;
-  W.ecursor = reinterpret_cast<uint32_t *>(take(b_cur));
-  W.krange = reinterpret_cast<uint32_t *>(take(b_kr));
+  W.bounds = reinterpret_cast<uint32_t *>(take(b_bd));
   W.n = n;
   W.max_iter = s->max_iter;
   W.stats = reinterpret_cast<unsigned long long *>(stats);
   W.err = ctx->d_err;
-  return launch_scene_trace(ctx, s->d_top.as<TopNode>(), W, s->kinds);
+  return launch_scene_trace(ctx, s->d_top.as<TopNode>(), W, s->kinds, s->ss);
 }
 
 }  // extern "C"

@@ -550,11 +550,6 @@ __device__ void window_walk2(const Node2 *__restrict__ nodes,
 // (ties) or with the reference's full walk.  Keeping those walks out of the
 // main kernels keeps their register and stack footprint small.
 
-struct Deferred {
-  uint32_t ray;
-  uint32_t full;  // 1: the reference's full walk; 0: replay the tie at m
-  double m;
-};
 
 template <int KIND>
 __device__ __forceinline__ void store_node2(size_t i, const Best &b, const Ctx2 &c,
@@ -1445,60 +1440,33 @@ __device__ __forceinline__ float world_dist(const SceneElem &e, const double lo[
   return sqrtf(po[0] * po[0] + po[1] * po[1] + po[2] * po[2]);
 }
 
-// Closest hit in one two-child element: the front-to-back pass, replayed in
-// the reference's order when it is not conclusive (as the resolve kernels do).
+// Per-kind walk context of a ray inside one element.
 template <int KIND>
-__device__ __forceinline__ void elem_walk2(const SceneElem &e, const Ctx2 &c, Best &b,
-                                           Work &w, uint32_t max_iter) {
-  const Node2 *nodes = static_cast<const Node2 *>(e.nodes);
-  float m;
-  uint32_t at_m;
-  bool viol;
-  pass1_node2<KIND>(nodes, e.prims, e.sidx, c, 0u, b, w, max_iter, m, at_m, viol);
-  if (w.fail || !(viol || at_m > 1)) return;
-  w.it = 0;
-  if (viol) {
-    ref_walk2_from<KIND>(nodes, e.prims, e.sidx, c, b, w, max_iter, m);
-  } else {
-    const float t0 = (KIND == SRT_TRIANGLES) ? m : nextafterf(m, FLT_MAX);
-    window_walk2<KIND>(nodes, e.prims, e.sidx, c, bound_rel(m, kRelTri), t0, b, w, max_iter);
-  }
-}
+struct KindCtx {
+  using T = Ctx2;
+};
+template <>
+struct KindCtx<SRT_TETRAHEDRA> {
+  using T = CtxT;
+};
 
-__device__ __forceinline__ void elem_walkT(const SceneElem &e, const CtxT &c, Best &b, Work &w,
-                                           uint32_t max_iter) {
-  const NodeT *nodes = static_cast<const NodeT *>(e.nodes);
-  double m;
-  bool defer, full;
-  pass1_tet(nodes, e.prims, e.sidx, c, b, w, max_iter, m, defer, full);
-  if (w.fail || !defer) return;
-  w.it = 0;
-  if (full) {
-    walkT_from(nodes, e.prims, e.sidx, c, b, w, max_iter, m);
-  } else {
-    const double whi = window_hi(m);
-    walkT<true>(nodes, e.prims, e.sidx, c, bound_rel((float)whi, kRelTet), whi, b, w, max_iter);
-  }
-}
-
-// Closest hit of ray i inside element e_id (local ray, self-hit data only
-// when e_id is the ray's previous element).  Returns whether it hit, with
-// the local hit in b and the local ray in lo / ld.
+// Ray i in element e_id's local space (self-hit data only when e_id is the
+// ray's previous element); the local ray's double origin and direction in
+// lo / ld.
 template <int KIND>
-__device__ __forceinline__ bool elem_hit(const SceneWork &W, uint32_t i, uint32_t e_id,
-                                         const SceneElem &e, const RayF &r0, uint32_t prev_prim,
-                                         float prev_t, double lo[3], double ld[3], Best &b,
-                                         Work &w) {
+__device__ __forceinline__ typename KindCtx<KIND>::T
+elem_ctx(const SceneWork &W, uint32_t i, uint32_t e_id, const SceneElem &e, const RayF &r0,
+         uint32_t prev_prim, float prev_t, double lo[3], double ld[3]) {
   const double ro[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd[3] = {r0.d[0], r0.d[1], r0.d[2]};
   const RayF lr = local_ray(e, ro, rd, lo, ld);
   const bool same = W.prev_element && __ldg(&W.prev_element[i]) == e_id;
-  if (KIND == SRT_TETRAHEDRA) {
+  if constexpr (KIND == SRT_TETRAHEDRA) {
     CtxT c;
     c.r = lr;
     c.o = {lr.o[0], lr.o[1], lr.o[2]};
     c.d = {lr.d[0], lr.d[1], lr.d[2]};
     c.prev_prim = same ? prev_prim : kNone;
-    elem_walkT(e, c, b, w, W.max_iter);
+    return c;
   } else {
     Ctx2 c;
     c.r = lr;
@@ -1508,31 +1476,60 @@ __device__ __forceinline__ bool elem_hit(const SceneWork &W, uint32_t i, uint32_
 #pragma unroll
     for (int k = 0; k < 3; k++)
       c.pn[k] = (same && W.prev_normals) ? __ldg(&W.prev_normals[3 * (size_t)i + k]) : 0.0f;
-    elem_walk2<KIND>(e, c, b, w, W.max_iter);
+    return c;
   }
-  if (w.fail) atomicOr(W.err, kErrIter);
-  return b.t < FLT_MAX && b.prim != kNone;
 }
 
-__device__ __forceinline__ uint32_t lanemask_lt() {
-  return (1u << (threadIdx.x & 31u)) - 1u;
+// The front-to-back pass in one element.  Returns whether its result is
+// final; otherwise m and full tell the replay (as for the resolve kernels).
+template <int KIND>
+__device__ __forceinline__ bool elem_pass1(const SceneElem &e, const typename KindCtx<KIND>::T &c,
+                                           Best &b, Work &w, uint32_t max_iter, double &m,
+                                           bool &full) {
+  if constexpr (KIND == SRT_TETRAHEDRA) {
+    bool defer;
+    pass1_tet(static_cast<const NodeT *>(e.nodes), e.prims, e.sidx, c, b, w, max_iter, m, defer,
+              full);
+    return w.fail || !defer;
+  } else {
+    float mf;
+    uint32_t at_m;
+    bool viol;
+    pass1_node2<KIND>(static_cast<const Node2 *>(e.nodes), e.prims, e.sidx, c, 0u, b, w,
+                      max_iter, mf, at_m, viol);
+    m = mf;
+    full = viol;
+    return w.fail || !(viol || at_m > 1);
+  }
 }
 
-// Append item to the list and count it for element e (one atomic per warp
-// for the list, one per warp and element for the counts).
-__device__ __forceinline__ void push_item(uint32_t *__restrict__ list,
-                                          uint32_t *__restrict__ list_count,
-                                          uint32_t *__restrict__ ecount, uint32_t e,
-                                          uint32_t item) {
-  const unsigned act = __activemask();
-  const int lane = (int)(threadIdx.x & 31u);
-  const int leader = __ffs(act) - 1;
-  uint32_t base = 0;
-  if (lane == leader) base = atomicAdd(list_count, (uint32_t)__popc(act));
-  base = __shfl_sync(act, base, leader);
-  list[base + __popc(act & lanemask_lt())] = item;
-  const unsigned grp = __match_any_sync(act, e);
-  if (lane == __ffs(grp) - 1) atomicAdd(&ecount[e], (uint32_t)__popc(grp));
+// The replay of an inconclusive pass: the reference's walk from the pass's
+// bound (full) or the reference order through the window at m.
+template <int KIND>
+__device__ __forceinline__ void elem_replay(const SceneElem &e,
+                                            const typename KindCtx<KIND>::T &c, Best &b,
+                                            Work &w, uint32_t max_iter, double m, bool full) {
+  w.it = 0;
+  if constexpr (KIND == SRT_TETRAHEDRA) {
+    const NodeT *nodes = static_cast<const NodeT *>(e.nodes);
+    if (full) {
+      walkT_from(nodes, e.prims, e.sidx, c, b, w, max_iter, m);
+    } else {
+      const double whi = window_hi(m);
+      walkT<true>(nodes, e.prims, e.sidx, c, bound_rel((float)whi, kRelTet), whi, b, w,
+                  max_iter);
+    }
+  } else {
+    const Node2 *nodes = static_cast<const Node2 *>(e.nodes);
+    const float mf = (float)m;
+    if (full) {
+      ref_walk2_from<KIND>(nodes, e.prims, e.sidx, c, b, w, max_iter, mf);
+    } else {
+      const float t0 = (KIND == SRT_TRIANGLES) ? mf : nextafterf(mf, FLT_MAX);
+      window_walk2<KIND>(nodes, e.prims, e.sidx, c, bound_rel(mf, kRelTri), t0, b, w,
+                         max_iter);
+    }
+  }
 }
 
 __device__ __forceinline__ void add_counts(unsigned long long *__restrict__ stats, int first,
@@ -1547,12 +1544,12 @@ __device__ __forceinline__ void add_counts(unsigned long long *__restrict__ stat
 
 __device__ __forceinline__ float inf_f() { return __int_as_float(0x7f800000); }
 
-// Items: phase 0 holds ray ids (the first candidate), phase 1 holds
-// ray * kRoundCand + slot.
+// Sorted item -> (ray, candidate slot).  Phase 0 items are ray ids (slot
+// 0); phase 1 items index the dense [ray][slot - 1] key array.
 __device__ __forceinline__ void item_ray_slot(int phase, uint32_t item, uint32_t &ray,
                                               uint32_t &slot) {
-  ray = phase ? item / kRoundCand : item;
-  slot = phase ? item % kRoundCand : 0u;
+  ray = phase ? item / (kRoundCand - 1) : item;
+  slot = phase ? item % (kRoundCand - 1) + 1 : 0u;
 }
 
 __global__ void __launch_bounds__(128)
@@ -1569,6 +1566,7 @@ scene_top_kernel(const TopNode *__restrict__ top, SceneWork W) {
   reinterpret_cast<float4 *>(W.hits)[i] = make_float4(FLT_MAX, 0.0f, 0.0f, __uint_as_float(kNone));
   if (W.element) W.element[i] = kNone;
   W.tnear[i] = inf_f();
+  uint32_t key = W.nelem;  // no first candidate for the rounds
   if (nc > kRoundCand) {
     W.ncand[i] = 0;
     W.ovf[atomicAdd(&W.counters[2], 1u)] = (uint32_t)i;
@@ -1578,135 +1576,170 @@ scene_top_kernel(const TopNode *__restrict__ top, SceneWork W) {
       W.cand_t[i * kRoundCand + c] = ct[c];
       W.cand_e[i * kRoundCand + c] = cid[c];
     }
-    if (nc > 0) push_item(W.items, &W.counters[0], W.ecount, cid[0], (uint32_t)i);
+    if (nc > 0) key = __ldg(&W.elem_rank[cid[0]]);
   }
+  W.keys0[i] = key;
   if (W.stats) add_counts(W.stats, 0, &ntop, 1);
 }
 
-// Offsets of each element's items in the sorted list (elements taken in
-// kind order, so each kind's items are one range); one block.
-__global__ void __launch_bounds__(256)
-scene_scan_kernel(SceneWork W, int phase) {
-  const uint32_t *cnt = W.ecount + (size_t)phase * W.nelem;
-  __shared__ uint32_t warp_sum[8];
-  __shared__ uint32_t carry;
-  __shared__ uint32_t kstart[3], kend[3];
-  if (threadIdx.x == 0) carry = 0;
-  if (threadIdx.x < 3) {
-    kstart[threadIdx.x] = 0xffffffffu;
-    kend[threadIdx.x] = 0u;
+// Each kind's range of a sorted key array (element ranks, kinds in rank
+// order, nelem for none): lower bounds of the kinds' first ranks.
+__global__ void scene_range_kernel(SceneWork W, int phase) {
+  const int t = threadIdx.x;
+  if (t >= 4) return;
+  const uint32_t *keys = phase ? W.keys1 : W.keys0;
+  const size_t n = phase ? W.n * (kRoundCand - 1) : W.n;
+  const uint32_t want = W.rank_start[t];
+  size_t lo = 0, hi = n;
+  while (lo < hi) {
+    const size_t mid = lo + (hi - lo) / 2;
+    if (keys[mid] < want) lo = mid + 1;
+    else hi = mid;
   }
-  __syncthreads();
-  for (uint32_t base = 0; base < W.nelem; base += blockDim.x) {
-    const uint32_t j = base + threadIdx.x;
-    const uint32_t e = j < W.nelem ? W.elem_order[j] : 0u;
-    const uint32_t v = j < W.nelem ? cnt[e] : 0u;
-    uint32_t x = v;  // inclusive warp scan
-    for (int o = 1; o < 32; o <<= 1) {
-      const uint32_t y = __shfl_up_sync(0xffffffffu, x, o);
-      if ((int)(threadIdx.x & 31u) >= o) x += y;
+  W.bounds[4 * phase + t] = (uint32_t)lo;
+}
+
+// An element walk's result: phase 0 (each ray's first candidate) makes it
+// the ray's running best; phase 1 (later candidates that the early cull
+// keeps after phase 0) stores it per (ray, slot) for the selection.
+__device__ __forceinline__ void finish_item(const SceneWork &W, int phase, uint32_t ray,
+                                            size_t cs, uint32_t e_id, const SceneElem &e,
+                                            const double lo[3], const double ld[3],
+                                            const float org[3], const Best &b) {
+  const bool hit = b.t < FLT_MAX && b.prim != kNone;
+  const float tw = hit ? world_dist(e, lo, ld, b.t, org) : inf_f();
+  if (phase == 0) {
+    if (hit && tw < inf_f()) {
+      W.tnear[ray] = tw;
+      reinterpret_cast<float4 *>(W.hits)[ray] = make_float4(tw, b.u, b.v, __uint_as_float(b.prim));
+      if (W.element) W.element[ray] = e_id;
     }
-    if ((threadIdx.x & 31u) == 31u) warp_sum[threadIdx.x >> 5] = x;
-    __syncthreads();
-    uint32_t woff = 0;
-    for (uint32_t w = 0; w < (threadIdx.x >> 5); w++) woff += warp_sum[w];
-    const uint32_t excl = carry + woff + x - v;
-    if (j < W.nelem) {
-      W.ecursor[e] = excl;
-      const int k = __ldg(&W.elems[e].kind);
-      atomicMin(&kstart[k], excl);
-      atomicMax(&kend[k], excl + v);
-    }
-    __syncthreads();
-    if (threadIdx.x == blockDim.x - 1) carry = excl + v;
-    __syncthreads();
-  }
-  if (threadIdx.x < 3) {
-    const bool any = kstart[threadIdx.x] != 0xffffffffu;
-    W.krange[2 * threadIdx.x] = any ? kstart[threadIdx.x] : 0u;
-    W.krange[2 * threadIdx.x + 1] = any ? kend[threadIdx.x] : 0u;
+  } else {
+    W.res[cs] = make_float4(tw, b.u, b.v, __uint_as_float(hit ? b.prim : kNone));
   }
 }
 
-// Items into element order (contiguous per element; the warp's own rays
-// stay together).
-__global__ void __launch_bounds__(128)
-scene_scatter_kernel(SceneWork W, int phase) {
-  const uint32_t cnt = *(volatile uint32_t *)&W.counters[phase];
-  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
-       k += gridDim.x * blockDim.x) {
-    const uint32_t item = W.items[k];
-    uint32_t ray, slot;
-    item_ray_slot(phase, item, ray, slot);
-    const uint32_t e = W.cand_e[(size_t)ray * kRoundCand + slot];
-    const unsigned act = __activemask();
-    const unsigned grp = __match_any_sync(act, e);
-    const int leader = __ffs(grp) - 1;
-    uint32_t base = 0;
-    if ((int)(threadIdx.x & 31u) == leader) base = atomicAdd(&W.ecursor[e], (uint32_t)__popc(grp));
-    base = __shfl_sync(grp, base, leader);
-    W.sorted[base + __popc(grp & lanemask_lt())] = item;
-  }
-}
-
-// The element walks of one kind.  Phase 0 (each ray's first candidate):
-// the result becomes the ray's running best.  Phase 1 (later candidates
-// that the early cull keeps after phase 0): results per (ray, slot) for the
-// selection.
+// The element walks of one kind over its range of the sorted items, 32
+// items per warp fetch: the front-to-back pass; items it leaves
+// inconclusive go to the kind's deferred list (slots lo.. of dlist) for
+// scene_resolve_kernel, so the pass runs with the registers and branch
+// structure of the single-accel trace.
 template <int KIND>
 __global__ void __launch_bounds__(128)
 scene_walk_kernel(SceneWork W, int phase) {
-  const uint32_t lo_k = *(volatile uint32_t *)&W.krange[2 * KIND];
-  const uint32_t hi_k = *(volatile uint32_t *)&W.krange[2 * KIND + 1];
+  const uint32_t *vals = phase ? W.vals1 : W.vals0;
+  const uint32_t lo = *(volatile uint32_t *)&W.bounds[4 * phase + KIND];
+  const uint32_t hi = *(volatile uint32_t *)&W.bounds[4 * phase + KIND + 1];
+  uint32_t *fetch = &W.counters[4 + 3 * phase + KIND];
+  uint32_t *dcount = &W.counters[10 + 3 * phase + KIND];
+  const int lane = (int)(threadIdx.x & 31u);
   uint32_t c[4] = {0, 0, 0, 0};  // element walks, branch nodes, leaves, primitives
-  for (uint32_t k = lo_k + blockIdx.x * blockDim.x + threadIdx.x; k < hi_k;
+  while (true) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(fetch, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= hi - lo) break;
+    const uint32_t k = lo + base + (uint32_t)lane;
+    if (k < hi) {
+      const uint32_t item = vals[k];
+      uint32_t ray, slot;
+      item_ray_slot(phase, item, ray, slot);
+      const size_t cs = (size_t)ray * kRoundCand + slot;
+      const uint32_t e_id = W.cand_e[cs];
+      const SceneElem &e = W.elems[e_id];
+      uint32_t prev_prim;
+      float prev_t;
+      const RayF r0 = load_ray(W.rays, ray, prev_prim, prev_t);
+      double lo3[3], ld3[3];
+      const auto ctx = elem_ctx<KIND>(W, ray, e_id, e, r0, prev_prim, prev_t, lo3, ld3);
+      Best b;
+      Work w;
+      double m;
+      bool full;
+      const bool done = elem_pass1<KIND>(e, ctx, b, w, W.max_iter, m, full);
+      c[0]++;
+      c[1] += w.branch;
+      c[2] += w.leaf;
+      c[3] += w.prim;
+      if (w.fail) atomicOr(W.err, kErrIter);
+      if (done) {
+        finish_item(W, phase, ray, cs, e_id, e, lo3, ld3, r0.o, b);
+      } else {
+        W.dlist[lo + atomicAdd(dcount, 1u)] = Deferred{item, full ? 1u : 0u, m};
+      }
+    }
+  }
+  if (W.stats) add_counts(W.stats, 1, c, 4);
+}
+
+// The deferred items of one kind: the replay, then the same result.
+template <int KIND>
+__global__ void __launch_bounds__(128)
+scene_resolve_kernel(SceneWork W, int phase) {
+  const uint32_t lo = *(volatile uint32_t *)&W.bounds[4 * phase + KIND];
+  const uint32_t cnt = *(volatile uint32_t *)&W.counters[10 + 3 * phase + KIND];
+  uint32_t c[4] = {0, 0, 0, 0};
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < cnt;
        k += gridDim.x * blockDim.x) {
+    const Deferred d = W.dlist[lo + k];
     uint32_t ray, slot;
-    item_ray_slot(phase, W.sorted[k], ray, slot);
+    item_ray_slot(phase, d.ray, ray, slot);
     const size_t cs = (size_t)ray * kRoundCand + slot;
     const uint32_t e_id = W.cand_e[cs];
     const SceneElem &e = W.elems[e_id];
     uint32_t prev_prim;
     float prev_t;
     const RayF r0 = load_ray(W.rays, ray, prev_prim, prev_t);
-    double lo[3], ld[3];
+    double lo3[3], ld3[3];
+    const auto ctx = elem_ctx<KIND>(W, ray, e_id, e, r0, prev_prim, prev_t, lo3, ld3);
     Best b;
     Work w;
-    const bool hit = elem_hit<KIND>(W, ray, e_id, e, r0, prev_prim, prev_t, lo, ld, b, w);
-    c[0]++;
+    elem_replay<KIND>(e, ctx, b, w, W.max_iter, d.m, d.full != 0);
     c[1] += w.branch;
     c[2] += w.leaf;
     c[3] += w.prim;
-    const float tw = hit ? world_dist(e, lo, ld, b.t, r0.o) : inf_f();
-    if (phase == 0) {
-      if (hit && tw < inf_f()) {
-        W.tnear[ray] = tw;
-        reinterpret_cast<float4 *>(W.hits)[ray] =
-            make_float4(tw, b.u, b.v, __uint_as_float(b.prim));
-        if (W.element) W.element[ray] = e_id;
-      }
-    } else {
-      W.res[cs] = make_float4(tw, b.u, b.v, __uint_as_float(hit ? b.prim : kNone));
-    }
+    if (w.fail) atomicOr(W.err, kErrIter);
+    finish_item(W, phase, ray, cs, e_id, e, lo3, ld3, r0.o, b);
   }
   if (W.stats) add_counts(W.stats, 1, c, 4);
 }
 
-// Phase 1 items: every later candidate whose entry does not lie beyond the
-// nearest hit of phase 0 (the candidates are sorted, so the first culled
-// one ends the list).  The sequential loop walks a subset of these: its
-// nearest distance only shrinks.
+// Closest hit of ray i in element e_id: pass and, if needed, replay (the
+// loop kernel's per-candidate walk).  Local ray in lo / ld.
+template <int KIND>
+__device__ __forceinline__ bool elem_hit(const SceneWork &W, uint32_t i, uint32_t e_id,
+                                         const SceneElem &e, const RayF &r0, uint32_t prev_prim,
+                                         float prev_t, double lo[3], double ld[3], Best &b,
+                                         Work &w) {
+  const auto ctx = elem_ctx<KIND>(W, i, e_id, e, r0, prev_prim, prev_t, lo, ld);
+  double m;
+  bool full;
+  if (!elem_pass1<KIND>(e, ctx, b, w, W.max_iter, m, full)) elem_replay<KIND>(e, ctx, b, w, W.max_iter, m, full);
+  if (w.fail) atomicOr(W.err, kErrIter);
+  return b.t < FLT_MAX && b.prim != kNone;
+}
+
+// Phase 1 keys, dense per ray: the element rank of every later candidate
+// whose entry does not lie beyond the nearest hit of phase 0 (the
+// candidates are sorted, so the first culled one ends them), none (nelem)
+// for the rest.  The sequential loop walks a subset of these: its nearest
+// distance only shrinks.
 __global__ void __launch_bounds__(128)
 scene_gather_kernel(SceneWork W) {
   const size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
   if (i >= W.n) return;
   const uint32_t nc = W.ncand[i];
-  if (nc < 2) return;
   const double tn = (double)W.tnear[i];
-  for (uint32_t c = 1; c < nc; c++) {
+  bool live = true;
+#pragma unroll
+  for (uint32_t c = 1; c < (uint32_t)kRoundCand; c++) {
     const size_t cs = i * kRoundCand + c;
-    if (tn < W.cand_t[cs]) break;
-    push_item(W.items, &W.counters[1], W.ecount + W.nelem, W.cand_e[cs], (uint32_t)cs);
+    uint32_t key = W.nelem;
+    if (live && c < nc) {
+      if (tn < W.cand_t[cs]) live = false;
+      else key = __ldg(&W.elem_rank[W.cand_e[cs]]);
+    }
+    W.keys1[i * (kRoundCand - 1) + (c - 1)] = key;
   }
 }
 
@@ -1793,16 +1826,16 @@ scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
 }
 
 // Resident blocks per SM of the persistent kernels (the same on every device
-// of one architecture): walks of the three kinds, scatter, loop.
-int g_per_sm[5] = {1, 1, 1, 1, 1};
+// of one architecture): walks of the three kinds, loop.
+int g_per_sm[4] = {1, 1, 1, 1};
 std::once_flag g_per_sm_once;
 
 void scene_occupancy() {
-  const void *fn[5] = {(const void *)scene_walk_kernel<SRT_TRIANGLES>,
+  const void *fn[4] = {(const void *)scene_walk_kernel<SRT_TRIANGLES>,
                        (const void *)scene_walk_kernel<SRT_TETRAHEDRA>,
                        (const void *)scene_walk_kernel<SRT_SPHERES>,
-                       (const void *)scene_scatter_kernel, (const void *)scene_loop_kernel};
-  for (int k = 0; k < 5; k++) {
+                       (const void *)scene_loop_kernel};
+  for (int k = 0; k < 4; k++) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn[k], 128, 0);
     g_per_sm[k] = per_sm > 0 ? per_sm : 1;
@@ -1811,40 +1844,60 @@ void scene_occupancy() {
 
 }  // namespace
 
-srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds) {
+template <int KIND>
+static void launch_kind(srt_ctx *ctx, const SceneWork &W, int phase, cudaStream_t st) {
+  scene_walk_kernel<KIND><<<(unsigned)(ctx->num_sms * g_per_sm[KIND]), 128, 0, st>>>(W, phase);
+  scene_resolve_kernel<KIND><<<(unsigned)(ctx->num_sms * 4), 128, 0, st>>>(W, phase);
+  ctx->launches += 2;
+}
+
+srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds,
+                              const SceneStreams &ss) {
   if (W.n == 0) return SRT_OK;
   cudaStream_t st = ctx->stream;
-  cudaError_t e = cudaMemsetAsync(W.counters, 0, (4 + 2 * (size_t)W.nelem) * sizeof(uint32_t), st);
+  cudaError_t e = cudaMemsetAsync(W.counters, 0, kSceneCounters * sizeof(uint32_t), st);
   if (e != cudaSuccess) return cuda_status(e, "scene counters");
   std::call_once(g_per_sm_once, scene_occupancy);
   const unsigned rgrid = (unsigned)((W.n + 127) / 128);
+  int kb = 1;  // key bits: ranks 0..nelem-1 and none = nelem
+  while ((1u << kb) <= W.nelem) kb++;
   scene_top_kernel<<<rgrid, 128, 0, st>>>(top, W);
   ctx->launches++;
+  // the rays with more candidates than slots run their loop alongside
+  cudaEventRecord(ss.fork[0], st);
+  cudaStreamWaitEvent(ss.side[3], ss.fork[0], 0);
+  scene_loop_kernel<<<(unsigned)(ctx->num_sms * g_per_sm[3]), 128, 0, ss.side[3]>>>(top, W);
+  ctx->launches++;
+  cudaEventRecord(ss.join[3], ss.side[3]);
   for (int phase = 0; phase < 2; phase++) {
     if (phase == 1) {
       scene_gather_kernel<<<rgrid, 128, 0, st>>>(W);
       ctx->launches++;
     }
-    scene_scan_kernel<<<1, 256, 0, st>>>(W, phase);
-    scene_scatter_kernel<<<(unsigned)(ctx->num_sms * g_per_sm[3]), 128, 0, st>>>(W, phase);
-    ctx->launches += 2;
-    static const int order[3] = {SRT_TRIANGLES, SRT_SPHERES, SRT_TETRAHEDRA};
-    for (int q = 0; q < 3; q++) {
-      const int k = order[q];
+    // items in (element rank, ray) order: a stable sort of the dense keys
+    srt_status s = phase ? sort_pairs(ctx, W.keys1, W.vals1, W.n * (kRoundCand - 1), true, kb)
+                         : sort_pairs(ctx, W.keys0, W.vals0, W.n, true, kb);
+    if (s != SRT_OK) return s;
+    scene_range_kernel<<<1, 32, 0, st>>>(W, phase);
+    ctx->launches++;
+    // each kind's walks and replays on its own stream
+    cudaEventRecord(ss.fork[1 + phase], st);
+    for (int k = 0; k < 3; k++) {
       if (!(kinds & (1u << k))) continue;
-      const unsigned grid = (unsigned)(ctx->num_sms * g_per_sm[k]);
+      cudaStreamWaitEvent(ss.side[k], ss.fork[1 + phase], 0);
       if (k == SRT_TRIANGLES)
-        scene_walk_kernel<SRT_TRIANGLES><<<grid, 128, 0, st>>>(W, phase);
+        launch_kind<SRT_TRIANGLES>(ctx, W, phase, ss.side[k]);
       else if (k == SRT_SPHERES)
-        scene_walk_kernel<SRT_SPHERES><<<grid, 128, 0, st>>>(W, phase);
+        launch_kind<SRT_SPHERES>(ctx, W, phase, ss.side[k]);
       else
-        scene_walk_kernel<SRT_TETRAHEDRA><<<grid, 128, 0, st>>>(W, phase);
-      ctx->launches++;
+        launch_kind<SRT_TETRAHEDRA>(ctx, W, phase, ss.side[k]);
+      cudaEventRecord(ss.join[k], ss.side[k]);
+      cudaStreamWaitEvent(st, ss.join[k], 0);
     }
   }
   scene_select_kernel<<<rgrid, 128, 0, st>>>(W);
-  scene_loop_kernel<<<(unsigned)(ctx->num_sms * g_per_sm[4]), 128, 0, st>>>(top, W);
-  ctx->launches += 2;
+  ctx->launches++;
+  cudaStreamWaitEvent(st, ss.join[3], 0);
   return cuda_status(cudaGetLastError(), "scene trace");
 }
 
