@@ -1262,12 +1262,13 @@ def run_scene(args, W):
     hbm, src = peaks()
     ntop, nwalk, br, lf, pr = (float(x) / nr for x in stats)
     # ray (32) + hit (16) + element (4) + top-level nodes (72) + per element
-    # walk its record (3 matrices, 400) + branch nodes (64) + primitive
-    # records (48: the triangle size; tets 52, spheres 20)
-    bpr = 32 + 16 + 4 + 72 * ntop + 400 * nwalk + 64 * br + 48 * pr
+    # walk its record (424) + branch nodes (64) + primitive records (48: the
+    # triangle size; tets 52, spheres 20)
+    bpr = 32 + 16 + 4 + 72 * ntop + 424 * nwalk + 64 * br + 48 * pr
     tr_ms = statistics.mean(parts[2])
     achieved = bpr * nr / (tr_ms * 1e-3) / 1e9
-    roofline = {"bound": "hbm", "kernel": "scene_trace_kernel", "achieved": round(achieved, 1),
+    roofline = {"bound": "hbm", "kernel": "srt_scene_trace (top, walk and resolve kernels)",
+                "achieved": round(achieved, 1),
                 "peak": hbm, "unit": "GB/s", "frac": round(achieved / hbm, 4),
                 "peak_source": src, "traffic": None,
                 "algorithmic_bytes_per_ray": round(bpr, 1),
