@@ -378,6 +378,66 @@ SRT_API srt_status srt_scene_trace(srt_scene *scene, const srt_ray *rays,
 SRT_API size_t srt_scene_top_nodes(srt_scene *scene, double *boxes,
                                    int32_t *ints, size_t cap);
 
+/* ---- accels across frames and runs ------------------------------------
+ * srt_accel_load_*: the accel of the given primitives from a file in the
+ * reference's Dump() format (XxxAccel::Dump, render/render_accel_triangle.cc:
+ * 1692-1719, render/render_accel_tetra.cc:1900, render/render_accel_particle.cc:
+ * 1868; srt_accel_dump writes the same), without a rebuild.  The reference
+ * writes these files but reads none back.  The primitives must be the ones
+ * the tree was built from; the file is checked completely first (counts and
+ * size, node indices, leaf ranges covering every primitive once, split
+ * axes, depth <= 28, the sorted order a permutation) and a damaged file is
+ * SRT_ERR_INVALID (SRT_ERR_UNSUPPORTED for a leaf root or a deeper tree).
+ * Synchronises the context stream. */
+SRT_API srt_status srt_accel_load_triangles(srt_accel *accel, const char *path,
+                                            const float *vertices, size_t nvertices,
+                                            const uint32_t *faces, size_t nfaces);
+SRT_API srt_status srt_accel_load_tetrahedra(srt_accel *accel, const char *path,
+                                             const float *vertices, size_t nvertices,
+                                             const uint32_t *tets, size_t ntets);
+SRT_API srt_status srt_accel_load_spheres(srt_accel *accel, const char *path,
+                                          const float *centers, const float *radius,
+                                          float constant_radius, size_t n);
+
+/* AccelBuilder's cache (gles/gles_accel_builder.cc:34-117, 400-456,
+ * 1017-1037).  The key is what Locate compares: the element and array
+ * buffers (any caller ids), the position attribute's offset, count and
+ * offset; the kind is compared too.  srt_cache_build_* return the cached
+ * accel of a static entry (a hit) or build one and keep it: in the static
+ * list when is_static (both buffers static), else in the dynamic list,
+ * which srt_cache_end_frame frees (AccelBuilder::EndFrame); dynamic entries
+ * are never found again, as in Locate.  srt_cache_invalidate frees every
+ * entry built from a buffer (AccelBuilder::Invalidate).  The cache owns its
+ * accels: do not destroy them; they stay valid until invalidated, freed at
+ * the end of the frame (dynamic) or the cache is destroyed.  bytes_used
+ * counts the accels' device memory; like the reference, nothing is evicted
+ * when it exceeds bytes_max. */
+typedef struct srt_cache srt_cache;
+typedef struct srt_cache_key {
+  uint64_t elem_buffer, array_buffer, position_offset;
+  uint32_t count, offset;
+} srt_cache_key;
+typedef struct srt_cache_info {
+  uint64_t bytes_used, bytes_max, static_entries, dynamic_entries, hits, builds;
+} srt_cache_info;
+SRT_API srt_status srt_cache_create(srt_ctx *ctx, uint64_t max_bytes, srt_cache **out);
+SRT_API srt_status srt_cache_destroy(srt_cache *cache);
+SRT_API srt_status srt_cache_build_triangles(srt_cache *cache, const srt_cache_key *key,
+                                             int is_static, const float *vertices,
+                                             size_t nvertices, const uint32_t *faces,
+                                             size_t nfaces, srt_accel **out);
+SRT_API srt_status srt_cache_build_tetrahedra(srt_cache *cache, const srt_cache_key *key,
+                                              int is_static, const float *vertices,
+                                              size_t nvertices, const uint32_t *tets,
+                                              size_t ntets, srt_accel **out);
+SRT_API srt_status srt_cache_build_spheres(srt_cache *cache, const srt_cache_key *key,
+                                           int is_static, const float *centers,
+                                           const float *radius, float constant_radius,
+                                           size_t n, srt_accel **out);
+SRT_API srt_status srt_cache_invalidate(srt_cache *cache, uint64_t buffer);
+SRT_API srt_status srt_cache_end_frame(srt_cache *cache);
+SRT_API srt_status srt_cache_info_get(srt_cache *cache, srt_cache_info *info);
+
 /* ---- secondary rays ----------------------------------------------------- */
 /* One secondary ray per hit ray (the particle workload's bounce; in the
  * reference a fragment shader builds it and calls back trace() with

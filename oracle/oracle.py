@@ -277,8 +277,40 @@ def canonicalize(generic_nodes, root=0):
 # --------------------------------------------------------------------------
 # reference accel (the real thing)
 # --------------------------------------------------------------------------
-def _read_dump(path, node_size):
-    raw = open(path, "rb").read()
+DUMP_NODE_BYTES = {TRI: 64, TET: 40, SPHERE: 60}
+
+
+def parse_dump(kind, data):
+    """(generic nodes, sorted indices) of a file in the reference's Dump()
+    format (bytes): TriangleNode 64 B, TetraNode 40 B, ParticleNode 60 B
+    records, then the sorted primitive indices."""
+    raw, idx = _split_dump(bytes(data), DUMP_NODE_BYTES[kind])
+    if kind == TET:
+        f = raw[:, :24].copy().view(np.float32).reshape(-1, 6)
+        ints = raw[:, 24:40].copy().view(np.int32).reshape(-1, 4)
+        g = np.zeros(raw.shape[0], NODE_DTYPE)
+        g["bmin"] = f[:, :3]
+        g["bmax"] = f[:, 3:]
+        g["leaf"] = ints[:, 0]
+        g["axis"] = np.where(ints[:, 0] == 1, 0, ints[:, 1])
+        g["d0"] = ints[:, 2].view(np.uint32)
+        g["d1"] = ints[:, 3].view(np.uint32)
+        return g, idx
+    f = raw[:, :48].copy().view(np.float32).reshape(-1, 2, 2, 3)
+    slot_bmin, slot_bmax = f[:, 0], f[:, 1]
+    if kind == TRI:
+        ints = raw[:, 48:64].copy().view(np.int32).reshape(-1, 4)
+        leaf, axis = ints[:, 0], ints[:, 1]
+        d0, d1 = ints[:, 2].view(np.uint32), ints[:, 3].view(np.uint32)
+    else:
+        d = raw[:, 48:56].copy().view(np.uint32).reshape(-1, 2)
+        sh = raw[:, 56:60].copy().view(np.int16).reshape(-1, 2)
+        leaf, axis = sh[:, 0].astype(np.int32), sh[:, 1].astype(np.int32)
+        d0, d1 = d[:, 0], d[:, 1]
+    return generic_from_two_box(slot_bmin, slot_bmax, leaf, axis, d0, d1), idx
+
+
+def _split_dump(raw, node_size):
     nn = int(np.frombuffer(raw, np.uint64, 1, 0)[0])
     nodes = np.frombuffer(raw, np.uint8, nn * node_size, 8).reshape(nn, node_size)
     off = 8 + nn * node_size
@@ -404,36 +436,11 @@ class RefAccel:
 
     def dump(self):
         """(generic nodes, sorted indices) from the reference's Dump()."""
-        sizes = np.zeros(3, np.uint64)
-        self.L.ref_node_sizes(_ptr(sizes))
-        ns = int(sizes[self.kind])
         with tempfile.TemporaryDirectory() as td:
             path = os.path.join(td, "accel.bin")
             getattr(self.L, f"ref_{self.tag}_dump")(self.h, path.encode())
-            raw, idx = _read_dump(path, ns)
-        if self.kind == TET:
-            f = raw[:, :24].copy().view(np.float32).reshape(-1, 6)
-            ints = raw[:, 24:40].copy().view(np.int32).reshape(-1, 4)
-            g = np.zeros(raw.shape[0], NODE_DTYPE)
-            g["bmin"] = f[:, :3]
-            g["bmax"] = f[:, 3:]
-            g["leaf"] = ints[:, 0]
-            g["axis"] = np.where(ints[:, 0] == 1, 0, ints[:, 1])
-            g["d0"] = ints[:, 2].view(np.uint32)
-            g["d1"] = ints[:, 3].view(np.uint32)
-            return g, idx
-        f = raw[:, :48].copy().view(np.float32).reshape(-1, 2, 2, 3)
-        slot_bmin, slot_bmax = f[:, 0], f[:, 1]
-        if self.kind == TRI:
-            ints = raw[:, 48:64].copy().view(np.int32).reshape(-1, 4)
-            leaf, axis = ints[:, 0], ints[:, 1]
-            d0, d1 = ints[:, 2].view(np.uint32), ints[:, 3].view(np.uint32)
-        else:
-            d = raw[:, 48:56].copy().view(np.uint32).reshape(-1, 2)
-            sh = raw[:, 56:60].copy().view(np.int16).reshape(-1, 2)
-            leaf, axis = sh[:, 0].astype(np.int32), sh[:, 1].astype(np.int32)
-            d0, d1 = d[:, 0], d[:, 1]
-        return generic_from_two_box(slot_bmin, slot_bmax, leaf, axis, d0, d1), idx
+            with open(path, "rb") as fp:
+                return parse_dump(self.kind, fp.read())
 
     def canonical(self):
         g, idx = self.dump()

@@ -28,6 +28,19 @@ class Camera(C.Structure):
                 ("height", C.c_int32), ("viewport", C.c_int32 * 4),
                 ("region", C.c_int32 * 4), ("step", C.c_int32)]
 
+class CacheKey(C.Structure):
+    """srt_cache_key (include/surface_rt.h)."""
+    _fields_ = [("elem_buffer", C.c_uint64), ("array_buffer", C.c_uint64),
+                ("position_offset", C.c_uint64), ("count", C.c_uint32), ("offset", C.c_uint32)]
+
+
+class CacheInfo(C.Structure):
+    """srt_cache_info (include/surface_rt.h)."""
+    _fields_ = [("bytes_used", C.c_uint64), ("bytes_max", C.c_uint64),
+                ("static_entries", C.c_uint64), ("dynamic_entries", C.c_uint64),
+                ("hits", C.c_uint64), ("builds", C.c_uint64)]
+
+
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
                       ("prev_t", "<f4")])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4")])
@@ -101,6 +114,17 @@ _SIGS = {
     "srt_scene_trace": [_P, _P, _SZ, _P, _P, _P, _P, _P],
     "srt_scene_top_nodes": [_P, _P, _P, _SZ],
     "srt_framebuffer_write": [_P, _P, _P, _P, _P, C.c_uint32, C.c_int32, _P, _P],
+    "srt_accel_load_triangles": [_P, C.c_char_p, _P, _SZ, _P, _SZ],
+    "srt_accel_load_tetrahedra": [_P, C.c_char_p, _P, _SZ, _P, _SZ],
+    "srt_accel_load_spheres": [_P, C.c_char_p, _P, _P, C.c_float, _SZ],
+    "srt_cache_create": [_P, C.c_uint64, C.POINTER(_P)],
+    "srt_cache_destroy": [_P],
+    "srt_cache_build_triangles": [_P, _P, C.c_int, _P, _SZ, _P, _SZ, C.POINTER(_P)],
+    "srt_cache_build_tetrahedra": [_P, _P, C.c_int, _P, _SZ, _P, _SZ, C.POINTER(_P)],
+    "srt_cache_build_spheres": [_P, _P, C.c_int, _P, _P, C.c_float, _SZ, C.POINTER(_P)],
+    "srt_cache_invalidate": [_P, C.c_uint64],
+    "srt_cache_end_frame": [_P],
+    "srt_cache_info_get": [_P, _P],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],

@@ -297,6 +297,18 @@ class TriangleAccel(_Accel):
         self.built = True
         return True
 
+    def Load(self, filename, mesh: Mesh) -> bool:
+        """The accel of `mesh` from a Dump() file (no rebuild; no counterpart
+        in the reference, which writes these files only)."""
+        v = _View(mesh.vertices, np.float32, torch.float32 if torch is not None else None)
+        f = _View(mesh.faces, np.uint32, torch.int32 if torch is not None else None)
+        self._sync_stream(mesh.vertices, mesh.faces)
+        check(self.L.srt_accel_load_triangles(self.h, str(filename).encode(), v.ptr,
+                                              v.nbytes // 12, f.ptr, f.nbytes // 12))
+        self._keep = (v, f)
+        self.built = True
+        return True
+
 
 class TetraAccel(_Accel):
     KIND = SRT_TETRAHEDRA
@@ -308,6 +320,17 @@ class TetraAccel(_Accel):
         self._sync_stream(tetras.vertices, tetras.faces)
         check(self.L.srt_accel_build_tetrahedra(self.h, v.ptr, v.nbytes // 12, f.ptr,
                                                 f.nbytes // 16))
+        self._keep = (v, f)
+        self.built = True
+        return True
+
+    def Load(self, filename, tetras: Tetrahedron) -> bool:
+        """The accel of `tetras` from a Dump() file (no rebuild)."""
+        v = _View(tetras.vertices, np.float32, torch.float32 if torch is not None else None)
+        f = _View(tetras.faces, np.uint32, torch.int32 if torch is not None else None)
+        self._sync_stream(tetras.vertices, tetras.faces)
+        check(self.L.srt_accel_load_tetrahedra(self.h, str(filename).encode(), v.ptr,
+                                               v.nbytes // 12, f.ptr, f.nbytes // 16))
         self._keep = (v, f)
         self.built = True
         return True
@@ -324,6 +347,18 @@ class ParticleAccel(_Accel):
         check(self.L.srt_accel_build_spheres(self.h, p.ptr, r.ptr,
                                              C.c_float(particles.constantRadius),
                                              p.nbytes // 12))
+        self._keep = (p, r)
+        self.built = True
+        return True
+
+    def Load(self, filename, particles: Particles) -> bool:
+        """The accel of `particles` from a Dump() file (no rebuild)."""
+        p = _View(particles.positions, np.float32, torch.float32 if torch is not None else None)
+        r = _View(particles.radius, np.float32, torch.float32 if torch is not None else None)
+        self._sync_stream(particles.positions, particles.radius)
+        check(self.L.srt_accel_load_spheres(self.h, str(filename).encode(), p.ptr, r.ptr,
+                                            C.c_float(particles.constantRadius),
+                                            p.nbytes // 12))
         self._keep = (p, r)
         self.built = True
         return True

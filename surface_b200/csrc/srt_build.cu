@@ -1399,6 +1399,76 @@ srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32
   return cuda_status(cudaGetLastError(), "batch emit");
 }
 
+namespace {
+// Sorted Morton codes of a loaded tree: the code of each sorted primitive.
+__global__ void gather_codes_kernel(const uint32_t *__restrict__ codes,
+                                    const uint32_t *__restrict__ sidx, size_t n,
+                                    uint32_t *__restrict__ out) {
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
+       j += (size_t)gridDim.x * blockDim.x)
+    out[j] = codes[sidx[j]];
+}
+
+__global__ void set_branches_kernel(SceneInfo *__restrict__ scene, uint32_t nb) {
+  scene->nbranches = nb;
+}
+
+// An accel from a tree read from a file: the scene box and codes as the build
+// computes them, the given sorted order and nodes, the primitive cache.
+template <int KIND>
+srt_status load_kind(srt_accel *a, const float *v, const uint32_t *f, const float *radius,
+                     float constr, size_t n, const void *h_nodes, size_t nnodes,
+                     uint32_t nbranches, const uint32_t *h_idx) {
+  srt_ctx *ctx = a->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const size_t node_bytes = (KIND == SRT_TETRAHEDRA) ? sizeof(NodeT) : sizeof(Node2);
+  if ((e = a->codes.ensure(n * 4)) != cudaSuccess ||
+      (e = a->indices.ensure(n * 4)) != cudaSuccess ||
+      (e = a->prims.ensure(n * sizeof(float4) * PrimTraits<KIND>::kCacheF4)) != cudaSuccess ||
+      (e = a->scene.ensure(sizeof(SceneInfo))) != cudaSuccess ||
+      (e = a->nodes.ensure(nnodes * node_bytes)) != cudaSuccess ||
+      (e = ctx->s_keys2.ensure(n * 4)) != cudaSuccess)
+    return cuda_status(e, "load allocation");
+  SceneInfo *scene = a->scene.as<SceneInfo>();
+  uint32_t *tmp = ctx->s_keys2.as<uint32_t>();
+  srt_status s = launch_bbox_morton<KIND>(ctx, v, f, radius, constr, n, scene, tmp, nullptr);
+  if (s != SRT_OK) return s;
+  uint32_t *idx = a->indices.as<uint32_t>();
+  e = cudaMemcpyAsync(idx, h_idx, n * 4, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->nodes.p, h_nodes, nnodes * node_bytes, cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_status(e, "load upload");
+  const int g = grid_for(n, kBlock, ctx->num_sms * 16);
+  gather_codes_kernel<<<g, kBlock, 0, st>>>(tmp, idx, n, a->codes.as<uint32_t>());
+  cache_kernel<KIND><<<g, kBlock, 0, st>>>(v, f, radius, constr, idx, (int)n,
+                                           a->prims.as<float4>());
+  set_branches_kernel<<<1, 1, 0, st>>>(scene, nbranches);
+  ctx->launches += 3;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "load");
+  // the host arrays are the caller's until the copies are done
+  return cuda_status(cudaStreamSynchronize(st), "load");
+}
+}  // namespace
+
+srt_status load_accel(srt_accel *a, const float *v, const uint32_t *f, const float *radius,
+                      float constr, size_t n, const void *h_nodes, size_t nnodes,
+                      uint32_t nbranches, const uint32_t *h_idx) {
+  a->host_scene_valid = false;
+  switch (a->kind) {
+    case SRT_TRIANGLES:
+      return load_kind<SRT_TRIANGLES>(a, v, f, radius, constr, n, h_nodes, nnodes, nbranches,
+                                      h_idx);
+    case SRT_TETRAHEDRA:
+      return load_kind<SRT_TETRAHEDRA>(a, v, f, radius, constr, n, h_nodes, nnodes, nbranches,
+                                       h_idx);
+    case SRT_SPHERES:
+      return load_kind<SRT_SPHERES>(a, v, f, radius, constr, n, h_nodes, nnodes, nbranches,
+                                    h_idx);
+  }
+  return SRT_ERR_INVALID;
+}
+
 srt_status build_accel(srt_accel *a, const float *v, const uint32_t *f,
                        const float *radius, float constr, size_t n) {
   a->host_scene_valid = false;

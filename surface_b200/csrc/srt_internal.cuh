@@ -172,6 +172,12 @@ bool is_device_ptr(const void *p);
 // build pipeline pieces (srt_build.cu)
 srt_status build_accel(srt_accel *a, const float *d_verts, const uint32_t *d_faces,
                        const float *d_radius, float const_radius, size_t n);
+// An accel from a tree read from a file (srt_cache.cu): host nodes in the
+// device layout (nnodes records, nbranches branches) and host sorted order.
+srt_status load_accel(srt_accel *a, const float *d_verts, const uint32_t *d_faces,
+                      const float *d_radius, float const_radius, size_t n,
+                      const void *h_nodes, size_t nnodes, uint32_t nbranches,
+                      const uint32_t *h_idx);
 srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *d_verts,
                         const uint32_t *d_faces, const float *d_radius,
                         float const_radius, size_t n, uint32_t *d_codes,

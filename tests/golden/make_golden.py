@@ -131,13 +131,36 @@ def tex_fixture(L):
     return out
 
 
+def dump_fixtures():
+    """Files written by the reference's own XxxAccel::Dump() for small
+    scenes of each kind, with the scenes: the accel loader must read them and
+    the product's Dump() must write the same bytes."""
+    import tempfile
+    v, f = S.displaced_octasphere(4, seed=71)
+    tv, tf, _ = S.tet_grid(6, seed=72)  # >= 1024 primitives: the LBVH path of Build32
+    p, r = S.particles(3000, seed=73, median_radius=0.02)
+    out = {"tri_verts": v, "tri_faces": f, "tet_verts": tv, "tet_faces": tf,
+           "sph_pos": p, "sph_rad": r}
+    for tag, acc in (("tri", O.RefAccel(O.TRI, v, f)), ("tet", O.RefAccel(O.TET, tv, tf)),
+                     ("sph", O.RefAccel(O.SPHERE, p, None, r))):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "accel.bin")
+            getattr(acc.L, f"ref_{acc.tag}_dump")(acc.h, path.encode())
+            with open(path, "rb") as fp:
+                out[f"{tag}_dump"] = np.frombuffer(fp.read(), np.uint8).copy()
+    return out
+
+
 def main():
     L = O.ref()
     if L is None:
         raise SystemExit("reference harness missing: run `make -C oracle` with the reference tree")
-    np.savez_compressed(os.path.join(HERE, "prefix_tree.npz"), **prefix_tree(L))
-    np.savez_compressed(os.path.join(HERE, "scenes_small.npz"), **scene_fixtures())
-    np.savez_compressed(os.path.join(HERE, "texture3d.npz"), **tex_fixture(L))
+    only = sys.argv[1:]  # names of fixtures to write (default: all)
+    jobs = {"prefix_tree": lambda: prefix_tree(L), "scenes_small": scene_fixtures,
+            "texture3d": lambda: tex_fixture(L), "dumps_small": dump_fixtures}
+    for name, make in jobs.items():
+        if not only or name in only:
+            np.savez_compressed(os.path.join(HERE, name + ".npz"), **make())
     for f in sorted(os.listdir(HERE)):
         if f.endswith(".npz"):
             print(f, os.path.getsize(os.path.join(HERE, f)))

@@ -261,11 +261,8 @@ def test_dump_is_reference_format():
     with tempfile.TemporaryDirectory() as td:
         path = os.path.join(td, "a.bin")
         acc.Dump(path)
-        raw, idx = O._read_dump(path, 64)
-    fl = raw[:, :48].copy().view(np.float32).reshape(-1, 2, 2, 3)
-    ints = raw[:, 48:64].copy().view(np.int32).reshape(-1, 4)
-    g = O.generic_from_two_box(fl[:, 0], fl[:, 1], ints[:, 0], ints[:, 1],
-                               ints[:, 2].view(np.uint32), ints[:, 3].view(np.uint32))
+        with open(path, "rb") as fp:
+            g, idx = O.parse_dump(O.TRI, fp.read())
     assert np.array_equal(O.canonicalize(g, 0), o.canonical())
     assert np.array_equal(idx, o.indices)
     # sequential depth-first emission: the node array equals the oracle's

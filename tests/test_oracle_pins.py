@@ -233,3 +233,19 @@ def test_camera_rays_restatement_properties():
     # the int conversion truncates to 0, so it stays
     assert sh.size == (64 - 7) * 48
     assert (pix & 0xFFFF).min() == 7
+
+
+def test_reference_dump_fixtures_match_oracle(golden):
+    """The Dump() files written by the reference (tests/golden/dumps_small.npz)
+    hold the oracle's tree and sorted order for the same scenes."""
+    g = golden("dumps_small.npz")
+    for tag, kind, acc in (("tri", O.TRI, lambda: O.OracleAccel(O.TRI, g["tri_verts"],
+                                                                g["tri_faces"])),
+                           ("tet", O.TET, lambda: O.OracleAccel(O.TET, g["tet_verts"],
+                                                                g["tet_faces"])),
+                           ("sph", O.SPHERE, lambda: O.OracleAccel(O.SPHERE, g["sph_pos"],
+                                                                   None, g["sph_rad"]))):
+        nodes, idx = O.parse_dump(kind, g[f"{tag}_dump"].tobytes())
+        o = acc()
+        assert np.array_equal(idx, o.indices)
+        assert np.array_equal(O.canonicalize(nodes, 0), o.canonical())
