@@ -378,6 +378,43 @@ SRT_API srt_status srt_scene_trace(srt_scene *scene, const srt_ray *rays,
 SRT_API size_t srt_scene_top_nodes(srt_scene *scene, double *boxes,
                                    int32_t *ints, size_t cap);
 
+/* ---- 3D texture fetch ----------------------------------------------------
+ * Texture::Fetch for 3D textures (gles/gles_common.h:344-399) over an array
+ * of coordinates, bit for bit the reference's values.
+ *   dense: FilterTexture3D{Byte,Float,Double} (render/render_texture.cc:
+ *   832-1175) after the optional per-axis remap of non-uniform volumes
+ *   (local::remap, gles/gles_common.h:264-269, set by lsglTexCoordRemap);
+ *   repeat wrap unless clamp-to-edge (Texture::SetWrap*).
+ *   sparse: SparseVolumeAccel::Build / Sample (render/render_accel_volume.cc:
+ *   37-139) at u * globalDim, the nearest texel of the first block
+ *   BVHTree::Locate reaches; (0, 0, 0, 0) outside every block.
+ * format: 0 = bytes, 1 = float, 2 = double (LSGL_RENDER_TEXTURE3D_FORMAT_BYTE /
+ * FLOAT / DOUBLE); texels x fastest, components interleaved (1..4 dense).
+ * Data are copied to the device (the call synchronises the context stream).
+ * srt_texture3d_fetch: uvw (3 floats per sample) and rgba (4 floats per
+ * sample, 16-byte aligned) are device arrays; asynchronous. */
+typedef struct srt_texture3d srt_texture3d;
+typedef struct srt_volume_block {      /* VolumeBlock, render/render_prim_volume.h:18-26 */
+  int32_t offset[3], extent[3], size[3], level;
+  uint64_t data_offset;                /* byte offset of its voxels in the pool */
+} srt_volume_block;
+SRT_API srt_status srt_texture3d_create(srt_ctx *ctx, srt_texture3d **out);
+SRT_API srt_status srt_texture3d_destroy(srt_texture3d *tex);
+SRT_API srt_status srt_texture3d_set_dense(srt_texture3d *tex, int format, int width,
+                                           int height, int depth, int components,
+                                           const void *data);
+SRT_API srt_status srt_texture3d_set_wrap(srt_texture3d *tex, int clamp_s, int clamp_t,
+                                          int clamp_r);
+/* axis 0..2; n = 0 removes the remap of that axis */
+SRT_API srt_status srt_texture3d_set_remap(srt_texture3d *tex, int axis, const float *table,
+                                           size_t n);
+SRT_API srt_status srt_texture3d_set_sparse(srt_texture3d *tex, int format, int components,
+                                            const int global_dim[3],
+                                            const srt_volume_block *blocks, size_t nblocks,
+                                            const void *pool, size_t pool_bytes);
+SRT_API srt_status srt_texture3d_fetch(srt_texture3d *tex, const float *uvw, size_t n,
+                                       float *rgba);
+
 /* ---- accels across frames and runs ------------------------------------
  * srt_accel_load_*: the accel of the given primitives from a file in the
  * reference's Dump() format (XxxAccel::Dump, render/render_accel_triangle.cc:

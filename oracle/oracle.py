@@ -97,6 +97,10 @@ def lib():
         L.so_camera_rays.argtypes = [_P, _P, _P, _P]
         L.so_framebuffer_write.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, _SZ,
                                            C.c_int, _P, _P]
+        L.so_tex_fetch.argtypes = [C.c_int, _P, _P, C.c_int, _P, _P, _P, _P, _SZ, _P]
+        L.so_sparse_tree.restype = _P
+        L.so_sparse_tree.argtypes = [_P, _SZ]
+        L.so_sparse_fetch.argtypes = [_P, _P, _P, C.c_int, C.c_int, _P, _P, _SZ, _P]
         L.so_matrix_inverse.argtypes = [_P]
         L.so_element_update.argtypes = [_P, _P, _P, _P, _P, _P, _P]
         L.so_scene_build.restype = _P
@@ -154,6 +158,9 @@ def ref():
                                            C.c_uint64, _SZ, _P]
         L.ref_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int,
                                        _P]
+        L.ref_tex_fetch.argtypes = [C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P,
+                                    _P, C.c_int, _P, C.c_int, _P, C.c_int, _P, _SZ, _P]
+        L.ref_sparse_fetch.argtypes = [_P, _SZ, _P, C.c_int, C.c_int, _P, _P, _SZ, _P]
         L.ref_matrix_inverse.argtypes = [_P]
         L.ref_bvh_build.restype = _P
         L.ref_bvh_build.argtypes = [_P, _P, _P, _SZ]
@@ -732,3 +739,53 @@ class OracleScene:
                 self.h = None
         except Exception:
             pass
+
+
+# ---------------------------------------------------------- texture fetch
+TEX_FORMATS = {0: np.uint8, 1: np.float32, 2: np.float64}
+BLOCK_DTYPE = np.dtype([("offset", "<i4", 3), ("extent", "<i4", 3), ("size", "<i4", 3),
+                        ("level", "<i4"), ("data_offset", "<u8")])
+
+
+def tex_fetch(fmt, img, comps, uvw, clamp=(1, 1, 1), remap=(None, None, None), use_ref=False):
+    """Texture::Fetch of a dense 3D texture img (D, H, W[, comps]) of format
+    fmt (0 byte, 1 float, 2 double): (n, 4) float32."""
+    img = np.ascontiguousarray(img, TEX_FORMATS[fmt])
+    d, h, w = img.shape[:3]
+    uvw = np.ascontiguousarray(uvw, np.float32).reshape(-1, 3)
+    out = np.zeros((uvw.shape[0], 4), np.float32)
+    cl = np.ascontiguousarray(clamp, np.int32)
+    tabs = [None if t is None else np.ascontiguousarray(t, np.float32) for t in remap]
+    ns = [0 if t is None else t.size for t in tabs]
+    if use_ref:
+        ref().ref_tex_fetch(fmt, _ptr(img), w, h, d, comps, _ptr(cl), _ptr(tabs[0]), ns[0],
+                            _ptr(tabs[1]), ns[1], _ptr(tabs[2]), ns[2], _ptr(uvw),
+                            uvw.shape[0], _ptr(out))
+    else:
+        dim = np.array([w, h, d], np.int32)
+        tp = (C.c_void_p * 3)(*[None if t is None else t.ctypes.data for t in tabs])
+        npa = np.array(ns, np.int32)
+        lib().so_tex_fetch(fmt, _ptr(img), _ptr(dim), comps, _ptr(cl), tp, _ptr(npa),
+                           _ptr(uvw), uvw.shape[0], _ptr(out))
+    return out
+
+
+def sparse_fetch(blocks, pool, fmt, comps, gdim, uvw, use_ref=False):
+    """Texture::Fetch of a sparse volume: blocks (BLOCK_DTYPE), pool (bytes
+    of every block's voxels at data_offset): (n, 4) float32."""
+    blocks = np.ascontiguousarray(blocks, BLOCK_DTYPE)
+    pool = np.ascontiguousarray(np.frombuffer(bytes(pool), np.uint8))
+    g = np.ascontiguousarray(gdim, np.int32)
+    uvw = np.ascontiguousarray(uvw, np.float32).reshape(-1, 3)
+    out = np.zeros((uvw.shape[0], 4), np.float32)
+    if use_ref:
+        ref().ref_sparse_fetch(_ptr(blocks), blocks.size, _ptr(pool), fmt, comps, _ptr(g),
+                               _ptr(uvw), uvw.shape[0], _ptr(out))
+    else:
+        tree = lib().so_sparse_tree(_ptr(blocks), blocks.size)
+        try:
+            lib().so_sparse_fetch(tree, _ptr(blocks), _ptr(pool), fmt, comps, _ptr(g),
+                                  _ptr(uvw), uvw.shape[0], _ptr(out))
+        finally:
+            lib().so_scene_free(tree)
+    return out

@@ -29,6 +29,7 @@
 #include "render_accel_particle.h"
 #include "render_accel_tetra.h"
 #include "render_accel_triangle.h"
+#include "render_accel_volume.h"
 #include "render_bvh_tree.h"
 #include "render_camera.h"
 #include "render_matrix.h"
@@ -424,4 +425,82 @@ REF_API void ref_matrix_inverse(double *m16) {
   Matrixd::Inverse(m);
   for (int r = 0; r < 4; r++)
     for (int c = 0; c < 4; c++) m16[4 * r + c] = m[r][c];
+}
+
+// Texture::Fetch of a dense 3D texture (gles/gles_common.h:371-399): the
+// per-axis remap of local::remap (gles/gles_common.h:264-269, written out
+// here because that header needs the GL front end) and the reference's own
+// FilterTexture3D{Byte,Float,Double}.  fmt: 0 byte, 1 float, 2 double.
+REF_API void ref_tex_fetch(int fmt, const void *img, int w, int h, int d, int comps,
+                           const int *clamp, const float *remap0, int n0, const float *remap1,
+                           int n1, const float *remap2, int n2, const float *uvw, size_t m,
+                           float *rgba) {
+  Texture3D tex;
+  memset(&tex, 0, sizeof(tex));
+  tex.image = reinterpret_cast<unsigned char *>(const_cast<void *>(img));
+  tex.width = w;
+  tex.height = h;
+  tex.depth = d;
+  tex.components = comps;
+  const float *tab[3] = {remap0, remap1, remap2};
+  const int nt[3] = {n0, n1, n2};
+  for (size_t i = 0; i < m; i++) {
+    float c[3];
+    for (int k = 0; k < 3; k++) {
+      c[k] = uvw[3 * i + k];
+      if (tab[k] && nt[k] > 0) {
+        int idx = c[k] * nt[k];
+        idx = (std::max)((std::min)(nt[k] - 1, idx), 0);
+        c[k] = tab[k][idx];
+      }
+    }
+    if (fmt == 0)
+      FilterTexture3DByte(&rgba[4 * i], &tex, c[0], c[1], c[2], clamp[0] != 0, clamp[1] != 0,
+                          clamp[2] != 0);
+    else if (fmt == 1)
+      FilterTexture3DFloat(&rgba[4 * i], &tex, c[0], c[1], c[2], clamp[0] != 0, clamp[1] != 0,
+                           clamp[2] != 0);
+    else
+      FilterTexture3DDouble(&rgba[4 * i], &tex, c[0], c[1], c[2], clamp[0] != 0, clamp[1] != 0,
+                            clamp[2] != 0);
+  }
+}
+
+// Texture::Fetch of a sparse volume (gles/gles_common.h:344-369) through the
+// reference's SparseVolumeAccel.  Blocks: offset[3], extent[3], size[3],
+// level, then a 64-bit byte offset into the data pool (8 ints + 8 bytes).
+REF_API void ref_sparse_fetch(const int32_t *blocks, size_t nblocks, const unsigned char *pool,
+                              int fmt, int comps, const int *gdim, const float *uvw, size_t m,
+                              float *rgba) {
+  SparseVolume sv;
+  for (size_t i = 0; i < nblocks; i++) {
+    const int32_t *b = blocks + 12 * i;
+    VolumeBlock vb;
+    memset(&vb, 0, sizeof(vb));
+    for (int k = 0; k < 3; k++) {
+      vb.offset[k] = b[k];
+      vb.extent[k] = b[3 + k];
+      vb.size[k] = b[6 + k];
+    }
+    vb.level = b[9];
+    vb.id = (int)i;
+    uint64_t off;
+    memcpy(&off, b + 10, 8);
+    vb.data = pool + off;
+    sv.blocks.push_back(vb);
+  }
+  for (int k = 0; k < 3; k++) sv.globalDim[k] = gdim[k];
+  sv.components = comps;
+  sv.format = fmt == 0 ? LSGL_RENDER_TEXTURE3D_FORMAT_BYTE
+                       : fmt == 1 ? LSGL_RENDER_TEXTURE3D_FORMAT_FLOAT
+                                  : LSGL_RENDER_TEXTURE3D_FORMAT_DOUBLE;
+  sv.maxLevel = 0;
+  SparseVolumeAccel acc;
+  acc.Build(&sv);
+  for (size_t i = 0; i < m; i++) {
+    double value[4], position[3];
+    for (int k = 0; k < 3; k++) position[k] = uvw[3 * i + k] * sv.globalDim[k];
+    acc.Sample(value, position);
+    for (int k = 0; k < 4; k++) rgba[4 * i + k] = value[k];
+  }
 }

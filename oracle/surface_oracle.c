@@ -2330,3 +2330,177 @@ SO_API void so_element_update(const double T[16], const double lbmin[3], const d
   invT33[12] = invT33[13] = invT33[14] = 0.0;
   so_matrix_inverse(invT33);
 }
+
+/* ======================================================= texture fetch
+ * Texture::Fetch for 3D textures (gles/gles_common.h:344-399), restated:
+ *   dense: per-axis remap (local::remap, gles/gles_common.h:264-269: idx =
+ *   (int)(x * n) clamped to [0, n-1], table[idx]) then FilterTexture3D{Byte,
+ *   Float,Double} (render/render_texture.cc:832-1175): wrap by fasterfloorf
+ *   unless clamp-to-edge, vox = u * (dim - 1), texel-corner trilinear with
+ *   Lerp (float; dlerp for doubles), bytes read as v / 255.5f, one component
+ *   replicated to rgba;
+ *   sparse: position = u * globalDim, the first block the BVHTree's Locate
+ *   (render/render_bvh_tree.cc:587-655) reaches, then
+ *   SparseVolumeAccel::Sample (render/render_accel_volume.cc:61-139): the
+ *   nearest texel (local offset times size/extent of x for all three axes),
+ *   bytes as v / 255.0f, doubles through float, alpha 1 when fewer than four
+ *   components, (0,0,0,0) outside every block.
+ * Formats: 0 byte, 1 float, 2 double (LSGL_RENDER_TEXTURE3D_FORMAT_*). */
+static inline float remap_ref(float x, const float *table, int n) {
+  int idx = (int)(x * n);
+  idx = idx > n - 1 ? n - 1 : idx;
+  idx = idx < 0 ? 0 : idx;
+  return table[idx];
+}
+
+static double texel_d(int fmt, const void *img, size_t k) {
+  if (fmt == 0) return (double)(((const unsigned char *)img)[k] / 255.5f);
+  if (fmt == 1) return (double)((const float *)img)[k];
+  return ((const double *)img)[k];
+}
+
+SO_API void so_tex_fetch(int fmt, const void *img, const int dim[3], int comps,
+                         const int clamp[3], const float *const remap[3], const int nremap[3],
+                         const float *uvw, size_t n, float *rgba) {
+  for (size_t i = 0; i < n; i++) {
+    float c[3];
+    for (int k = 0; k < 3; k++) {
+      c[k] = uvw[3 * i + k];
+      if (remap[k] && nremap[k] > 0) c[k] = remap_ref(c[k], remap[k], nremap[k]);
+      if (!clamp[k]) c[k] = c[k] - floor_ref(c[k]);
+    }
+    float vox[3];
+    int v0[3], v1[3];
+    for (int k = 0; k < 3; k++) {
+      vox[k] = c[k] * (dim[k] - 1.0f);
+      v0[k] = clampi((int)vox[k], 0, dim[k] - 1);
+      v1[k] = v0[k] + 1 < dim[k] - 1 ? v0[k] + 1 : dim[k] - 1;
+    }
+    float vals[4] = {0, 0, 0, 0};
+    for (int ch = 0; ch < comps && ch < 4; ch++) {
+#define T(x, y, z)                                                                          \
+  texel_d(fmt, img,                                                                         \
+          (size_t)comps * ((size_t)(z) * dim[0] * dim[1] + (size_t)(y) * dim[0] + (x)) + ch)
+      if (fmt == 2) {
+        const double dx = vox[0] - v0[0], dy = vox[1] - v0[1], dz = vox[2] - v0[2];
+#define DL(t, a, b) ((1.0 - (t)) * (a) + (t) * (b))
+        double d00 = DL(dx, T(v0[0], v0[1], v0[2]), T(v1[0], v0[1], v0[2]));
+        double d10 = DL(dx, T(v0[0], v1[1], v0[2]), T(v1[0], v1[1], v0[2]));
+        double d01 = DL(dx, T(v0[0], v0[1], v1[2]), T(v1[0], v0[1], v1[2]));
+        double d11 = DL(dx, T(v0[0], v1[1], v1[2]), T(v1[0], v1[1], v1[2]));
+        double d0 = DL(dy, d00, d10), d1 = DL(dy, d01, d11);
+        vals[ch] = (float)DL(dz, d0, d1);
+#undef DL
+      } else {
+        const float dx = vox[0] - v0[0], dy = vox[1] - v0[1], dz = vox[2] - v0[2];
+        float d00 = lerpf(dx, (float)T(v0[0], v0[1], v0[2]), (float)T(v1[0], v0[1], v0[2]));
+        float d10 = lerpf(dx, (float)T(v0[0], v1[1], v0[2]), (float)T(v1[0], v1[1], v0[2]));
+        float d01 = lerpf(dx, (float)T(v0[0], v0[1], v1[2]), (float)T(v1[0], v0[1], v1[2]));
+        float d11 = lerpf(dx, (float)T(v0[0], v1[1], v1[2]), (float)T(v1[0], v1[1], v1[2]));
+        float d0 = lerpf(dy, d00, d10), d1 = lerpf(dy, d01, d11);
+        vals[ch] = lerpf(dz, d0, d1);
+      }
+#undef T
+    }
+    float *o = &rgba[4 * i];
+    if (comps == 1) {
+      o[0] = o[1] = o[2] = o[3] = vals[0];
+    } else {
+      o[0] = vals[0]; o[1] = vals[1]; o[2] = vals[2]; o[3] = vals[3];
+    }
+  }
+}
+
+typedef struct {
+  int offset[3], extent[3], size[3], level;
+  uint64_t data_offset; /* bytes into the data pool */
+} so_block;
+
+/* BVHTree::Locate: the first leaf (depth first, left child first) whose box
+ * holds p (inclusive); -1 if none. */
+static int top_locate(const so_scene *s, const double p[3]) {
+  int stk[256], sp = 0, node = 0;
+  for (;;) {
+    const so_top *t = &s->nodes[node];
+    if (t->leaf) {
+      if (p[0] >= t->bmin[0] && p[0] <= t->bmax[0] && p[1] >= t->bmin[1] &&
+          p[1] <= t->bmax[1] && p[2] >= t->bmin[2] && p[2] <= t->bmax[2])
+        return (int)t->id;
+      if (sp < 1) return -1;
+      node = stk[--sp];
+    } else {
+      int h[2];
+      for (int c = 0; c < 2; c++) {
+        const so_top *u = t->child[c] > 0 ? &s->nodes[t->child[c]] : NULL;
+        h[c] = u && p[0] >= u->bmin[0] && p[0] <= u->bmax[0] && p[1] >= u->bmin[1] &&
+               p[1] <= u->bmax[1] && p[2] >= u->bmin[2] && p[2] <= u->bmax[2];
+      }
+      if (!h[0] && !h[1]) {
+        if (sp < 1) return -1;
+        node = stk[--sp];
+      } else if (h[0] && !h[1]) {
+        node = t->child[0];
+      } else if (h[1] && !h[0]) {
+        node = t->child[1];
+      } else {
+        stk[sp++] = t->child[1];
+        node = t->child[0];
+      }
+    }
+  }
+}
+
+SO_API so_scene *so_sparse_tree(const so_block *b, size_t n) {
+  double *lo = (double *)malloc(n * 3 * sizeof(double));
+  double *hi = (double *)malloc(n * 3 * sizeof(double));
+  const so_accel **acc = (const so_accel **)calloc(n, sizeof(*acc));
+  double *z = (double *)calloc(n * 16, sizeof(double));
+  for (size_t i = 0; i < n; i++)
+    for (int k = 0; k < 3; k++) {
+      lo[3 * i + k] = (double)b[i].offset[k];
+      hi[3 * i + k] = (double)(b[i].offset[k] + b[i].extent[k]);
+    }
+  so_scene *s = so_scene_build(acc, z, z, z, lo, hi, n);
+  free(lo);
+  free(hi);
+  free((void *)acc);
+  free(z);
+  return s;
+}
+
+SO_API void so_sparse_fetch(const so_scene *tree, const so_block *b, const void *pool, int fmt,
+                            int comps, const int gdim[3], const float *uvw, size_t n,
+                            float *rgba) {
+  for (size_t i = 0; i < n; i++) {
+    double p[3];
+    for (int k = 0; k < 3; k++) p[k] = (double)(uvw[3 * i + k] * gdim[k]);
+    double v[4] = {0.0, 0.0, 0.0, 0.0};
+    const int id = top_locate(tree, p);
+    if (id >= 0) {
+      const so_block *bl = &b[id];
+      const int nc = comps >= 4 ? 4 : comps;
+      v[3] = 1.0;
+      double x = p[0] - bl->offset[0], y = p[1] - bl->offset[1], z = p[2] - bl->offset[2];
+      const double sx = bl->size[0] / (double)bl->extent[0];
+      x = x * sx;
+      y = y * sx; /* the reference scales all three axes by x's ratio */
+      z = z * sx;
+      int ix = (int)x, iy = (int)y, iz = (int)z;
+      ix = ix > bl->size[0] - 1 ? bl->size[0] - 1 : ix;
+      iy = iy > bl->size[1] - 1 ? bl->size[1] - 1 : iy;
+      iz = iz > bl->size[2] - 1 ? bl->size[2] - 1 : iz;
+      ix = ix < 0 ? 0 : ix;
+      iy = iy < 0 ? 0 : iy;
+      iz = iz < 0 ? 0 : iz;
+      const size_t idx = (size_t)iz * bl->size[0] * bl->size[1] + (size_t)iy * bl->size[0] + ix;
+      const unsigned char *base = (const unsigned char *)pool + bl->data_offset;
+      for (int c = 0; c < nc; c++) {
+        const size_t k = (size_t)nc * idx + c; /* the stride is the clamped count */
+        if (fmt == 0) v[c] = base[k] / 255.0f;
+        else if (fmt == 1) v[c] = ((const float *)base)[k];
+        else v[c] = (float)((const double *)base)[k];
+      }
+    }
+    for (int k = 0; k < 4; k++) rgba[4 * i + k] = (float)v[k];
+  }
+}

@@ -125,6 +125,13 @@ _SIGS = {
     "srt_cache_invalidate": [_P, C.c_uint64],
     "srt_cache_end_frame": [_P],
     "srt_cache_info_get": [_P, _P],
+    "srt_texture3d_create": [_P, C.POINTER(_P)],
+    "srt_texture3d_destroy": [_P],
+    "srt_texture3d_set_dense": [_P, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _P],
+    "srt_texture3d_set_wrap": [_P, C.c_int, C.c_int, C.c_int],
+    "srt_texture3d_set_remap": [_P, C.c_int, _P, _SZ],
+    "srt_texture3d_set_sparse": [_P, C.c_int, C.c_int, _P, _P, _SZ, _P, _SZ],
+    "srt_texture3d_fetch": [_P, _P, _SZ, _P],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],

@@ -12,6 +12,7 @@
 
 #include <atomic>
 #include <string>
+#include <vector>
 
 #include "surface_rt.h"
 
@@ -252,6 +253,10 @@ struct SceneStreams {
   cudaEvent_t fork[3] = {};  // top level done, phase 0 items ready, phase 1 items ready
   cudaEvent_t join[4] = {};  // each side stream's latest work
 };
+// BVHTree::BuildTree on the host over n boxes (srt_scene.cu): node 0 is
+// the root, TopNode.id of a leaf is its box's index.
+void build_top_tree(const double *bmin, const double *bmax, size_t n,
+                    std::vector<TopNode> &out);
 // kinds: bit k set when the scene holds elements of kind k.
 srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds,
                               const SceneStreams &ss);

@@ -236,6 +236,26 @@ void element_update(const double T[16], const double lbmin[3], const double lbma
 
 }  // namespace
 
+namespace srt {
+// BVHTree::BuildTree over n boxes (element or block ids 0..n-1).
+void build_top_tree(const double *bmin, const double *bmax, size_t n,
+                    std::vector<TopNode> &out) {
+  std::vector<TopData> d(n);
+  for (size_t i = 0; i < n; i++) {
+    for (int k = 0; k < 3; k++) {
+      d[i].bmin[k] = bmin[3 * i + k];
+      d[i].bmax[k] = bmax[3 * i + k];
+    }
+    d[i].id = (uint32_t)i;
+  }
+  double lo[3], hi[3];
+  range_box(d, 0, n, lo, hi);  // CalcSceneBBox (render/render_bvh_tree.cc:155-170)
+  out.clear();
+  out.push_back(make_node(lo, hi));
+  construct(out, d, 0, 0, n);
+}
+}  // namespace srt
+
 extern "C" {
 
 SRT_API void srt_matrix_inverse(double m[16]) { inverse4(m); }
@@ -319,20 +339,13 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
     set_error("empty scene");
     return SRT_ERR_INVALID;
   }
-  std::vector<TopData> d(s->elems.size());
-  for (size_t i = 0; i < d.size(); i++) {
+  std::vector<double> lo(3 * s->elems.size()), hi(3 * s->elems.size());
+  for (size_t i = 0; i < s->elems.size(); i++)
     for (int k = 0; k < 3; k++) {
-      d[i].bmin[k] = s->elems[i].bmin[k];
-      d[i].bmax[k] = s->elems[i].bmax[k];
+      lo[3 * i + k] = s->elems[i].bmin[k];
+      hi[3 * i + k] = s->elems[i].bmax[k];
     }
-    d[i].id = (uint32_t)i;
-  }
-  // CalcSceneBBox (render/render_bvh_tree.cc:155-170): the root's box
-  double bmin[3], bmax[3];
-  range_box(d, 0, d.size(), bmin, bmax);
-  s->top.clear();
-  s->top.push_back(make_node(bmin, bmax));
-  construct(s->top, d, 0, 0, d.size());
+  build_top_tree(lo.data(), hi.data(), s->elems.size(), s->top);
   std::vector<SceneElem> el(s->elems.size());
   size_t total = 0;
   uint32_t kinds = 0;

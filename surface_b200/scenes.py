@@ -465,3 +465,59 @@ def instanced_scene(seed=77, grid=4, spacing=3.0):
         elements.append(dict(accel=a, T=C @ M))
         prims.append(nprim[a])
     return dict(accels=accels, elements=elements, prims=prims)
+
+
+# ---------------------------------------------------------------- textures
+def dense_texture(fmt, dims=(9, 7, 5), comps=1, seed=1):
+    """A seeded 3D texture (D, H, W, comps) of format 0 byte, 1 float, 2 double."""
+    rng = np.random.default_rng(seed)
+    w, h, d = dims
+    shape = (d, h, w, comps) if comps > 1 else (d, h, w)
+    if fmt == 0:
+        return rng.integers(0, 256, size=shape, dtype=np.uint8)
+    x = rng.random(shape)
+    return x.astype(np.float32 if fmt == 1 else np.float64)
+
+
+def remap_table(n, seed=2, power=1.7):
+    """A monotone coordinate remap of n entries in [0, 1] (stretched toward
+    one end, as non-uniform grids are)."""
+    rng = np.random.default_rng(seed)
+    t = np.sort(rng.random(n)) ** power
+    t[0], t[-1] = 0.0, 1.0
+    return t.astype(np.float32)
+
+
+def sparse_blocks(fmt, comps, nblocks=12, seed=3, gdim=(64, 48, 40), overlap=False):
+    """Seeded sparse volume: blocks at random integer offsets (non-overlapping
+    on a lattice, or overlapping), extents 4-16 and voxel sizes that differ
+    from the extents.  Returns (blocks BLOCK-layout structured array, pool bytes,
+    gdim)."""
+    rng = np.random.default_rng(seed)
+    dt = np.dtype([("offset", "<i4", 3), ("extent", "<i4", 3), ("size", "<i4", 3),
+                   ("level", "<i4"), ("data_offset", "<u8")])
+    b = np.zeros(nblocks, dt)
+    itemsize = {0: 1, 1: 4, 2: 8}[fmt]
+    chunks, off = [], 0
+    cells = [(i, j, k) for i in range(4) for j in range(3) for k in range(2)]
+    rng.shuffle(cells)
+    for n in range(nblocks):
+        ext = rng.integers(4, 17, size=3)
+        if overlap:
+            o = rng.integers(0, np.array(gdim) - ext)
+        else:
+            c = np.array(cells[n % len(cells)])
+            o = c * np.array([16, 16, 20])
+        size = rng.integers(2, 9, size=3)
+        b[n]["offset"], b[n]["extent"], b[n]["size"] = o, ext, size
+        b[n]["data_offset"] = off
+        nvox = int(np.prod(size)) * min(comps, 4)
+        if fmt == 0:
+            data = rng.integers(0, 256, size=nvox, dtype=np.uint8)
+        else:
+            data = rng.random(nvox).astype(np.float32 if fmt == 1 else np.float64)
+        raw = data.tobytes()
+        raw += b"\0" * ((-len(raw)) % 16)
+        chunks.append(raw)
+        off += len(raw)
+    return b, b"".join(chunks), tuple(int(x) for x in gdim)
