@@ -295,6 +295,33 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx,
                                         const float *grad_image,
                                         float *grad_density, float *grad_tf);
 
+/* The density texture's sampling state for the march (the texture3D fetch
+ * of Texture::Fetch, gles/gles_common.h:371-399): remap[k] (remap_n[k]
+ * entries, NULL or 0 for none) is the coordinate remap of a non-uniform
+ * volume (lsglTexCoordRemap; the reference's nonuniform_volume_render example
+ * remaps y), applied as local::remap (gles/gles_common.h:264-269); clamp[k]
+ * selects clamp-to-edge, 0 the repeat wrap of FilterTexture3DFloat (GL's
+ * default, under which a coordinate remapped to 1.0 wraps to 0).  Tables
+ * may be device or host memory.  The entry points without _ex march with
+ * clamp-to-edge on every axis and no remap. */
+typedef struct srt_volume_sampling {
+  const float *remap[3];
+  uint32_t remap_n[3];
+  int32_t clamp[3];
+} srt_volume_sampling;
+SRT_API srt_status srt_volume_march_fwd_ex(srt_ctx *ctx, const srt_volume_params *params,
+                                           const srt_volume_sampling *sampling,
+                                           const float *density, const int32_t dims[3],
+                                           const float *tf, int32_t tf_entries,
+                                           float *image, float *transmittance);
+SRT_API srt_status srt_volume_march_bwd_ex(srt_ctx *ctx, const srt_volume_params *params,
+                                           const srt_volume_sampling *sampling,
+                                           const float *density, const int32_t dims[3],
+                                           const float *tf, int32_t tf_entries,
+                                           const float *image, const float *transmittance,
+                                           const float *grad_image, float *grad_density,
+                                           float *grad_tf);
+
 /* ---- eye rays and framebuffer ------------------------------------------- */
 /* RaytraceEngine::OnData's per-pixel ray generation and framebuffer write
  * (gles/gles_raytrace_engine.cc:547-879) for one sample per pixel, with the

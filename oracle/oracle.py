@@ -92,6 +92,9 @@ def lib():
         L.so_volume_fwd_f32.argtypes = [_P, _P, _P, _P, _P, C.c_int]
         L.so_volume_f64.restype = C.c_double
         L.so_volume_f64.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P]
+        L.so_volume_fwd_f32_ex.argtypes = [_P, _P, _P, _P, _P, _P, C.c_int]
+        L.so_volume_f64_ex.restype = C.c_double
+        L.so_volume_f64_ex.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P]
         L.so_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int, _P]
         L.so_camera_rays.restype = _SZ
         L.so_camera_rays.argtypes = [_P, _P, _P, _P]
@@ -554,16 +557,43 @@ def volume_params(width, height, eye, lookat, up, fov_deg, step, sigma_scale,
     return p
 
 
-def volume_fwd_f32(params, dens, dims, tf, nthreads=0):
+class _Sampling(C.Structure):
+    _fields_ = [("remap", C.c_void_p * 3), ("remap_n", C.c_uint32 * 3),
+                ("clamp", C.c_int32 * 3)]
+
+
+def _sampling(remap, clamp):
+    """so_sampling for remap tables (None each) and clamp flags, or None for
+    the default (clamp-to-edge, no remap); the tables are kept alive on it."""
+    if remap is None and clamp is None:
+        return None
+    sm = _Sampling()
+    remap = remap or (None, None, None)
+    clamp = (1, 1, 1) if clamp is None else clamp
+    sm.keep = [None if t is None else np.ascontiguousarray(t, np.float32) for t in remap]
+    for k in range(3):
+        t = sm.keep[k]
+        sm.remap[k] = None if t is None else t.ctypes.data
+        sm.remap_n[k] = 0 if t is None else t.size
+        sm.clamp[k] = int(clamp[k])
+    return sm
+
+
+def volume_fwd_f32(params, dens, dims, tf, nthreads=0, remap=None, clamp=None):
+    """FP32 march; remap (3 tables or None) and clamp (3 flags) give the
+    density texture's sampling state (default: clamp-to-edge, no remap)."""
     W, H = int(params["width"][0]), int(params["height"][0])
     img = np.zeros((H, W, 4), np.float32)
-    lib().so_volume_fwd_f32(_ptr(params), _ptr(np.ascontiguousarray(dens, np.float32)),
-                            _ptr(np.asarray(dims, np.int32)),
-                            _ptr(np.ascontiguousarray(tf, np.float32)), _ptr(img), nthreads)
+    sm = _sampling(remap, clamp)
+    lib().so_volume_fwd_f32_ex(_ptr(params), None if sm is None else C.byref(sm),
+                               _ptr(np.ascontiguousarray(dens, np.float32)),
+                               _ptr(np.asarray(dims, np.int32)),
+                               _ptr(np.ascontiguousarray(tf, np.float32)), _ptr(img), nthreads)
     return img
 
 
-def volume_f64(params, dens, dims, tf, target=None, want_grad=False, want_img=False):
+def volume_f64(params, dens, dims, tf, target=None, want_grad=False, want_img=False,
+               remap=None, clamp=None):
     W, H = int(params["width"][0]), int(params["height"][0])
     dens = np.ascontiguousarray(dens, np.float64)
     tf = np.ascontiguousarray(tf, np.float64)
@@ -571,8 +601,10 @@ def volume_f64(params, dens, dims, tf, target=None, want_grad=False, want_img=Fa
     gd = np.zeros(dens.shape) if want_grad else None
     gt = np.zeros(tf.shape) if want_grad else None
     tg = None if target is None else np.ascontiguousarray(target, np.float32)
-    loss = lib().so_volume_f64(_ptr(params), _ptr(dens), _ptr(np.asarray(dims, np.int32)),
-                               _ptr(tf), _ptr(tg), _ptr(img), _ptr(gd), _ptr(gt))
+    sm = _sampling(remap, clamp)
+    loss = lib().so_volume_f64_ex(_ptr(params), None if sm is None else C.byref(sm),
+                                  _ptr(dens), _ptr(np.asarray(dims, np.int32)), _ptr(tf),
+                                  _ptr(tg), _ptr(img), _ptr(gd), _ptr(gt))
     return loss, img, gd, gt
 
 

@@ -1403,6 +1403,13 @@ static inline int floor_ref(float x) { /* fasterfloorf, render_texture.cc:106 */
   return y;
 }
 static inline int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+/* local::remap (gles/gles_common.h:264-269) */
+static inline float remap_ref(float x, const float *table, int n) {
+  int idx = (int)(x * n);
+  idx = idx > n - 1 ? n - 1 : idx;
+  idx = idx < 0 ? 0 : idx;
+  return table[idx];
+}
 static inline float lerpf(float t, float a, float b) { return (1.f - t) * a + t * b; }
 
 /* Scalar (1-component) volume fetch with the reference's texel-corner
@@ -1516,9 +1523,51 @@ static inline int vol_inside_f(const float p[3]) {
 }
 
 /* Forward march, FP32.  img: width*height*4 (RGB premultiplied, A = 1 - T). */
+/* The density texture's sampling state (srt_volume_sampling): per-axis
+ * remap tables (local::remap) and clamp-to-edge flags (0: repeat wrap).
+ * NULL: clamp-to-edge, no remap. */
+typedef struct {
+  const float *remap[3];
+  uint32_t remap_n[3];
+  int32_t clamp[3];
+} so_sampling;
+
+static inline float samp_f32(const so_sampling *S, int k, float u) {
+  if (!S) return u;
+  if (S->remap[k] && S->remap_n[k]) u = remap_ref(u, S->remap[k], (int)S->remap_n[k]);
+  if (!S->clamp[k]) u = u - floor_ref(u);
+  return u;
+}
+
+static inline double samp_f64(const so_sampling *S, int k, double q) {
+  if (!S) return q;
+  if (S->remap[k] && S->remap_n[k]) {
+    const int n = (int)S->remap_n[k];
+    int idx = (int)(q * n);
+    idx = idx > n - 1 ? n - 1 : (idx < 0 ? 0 : idx);
+    q = S->remap[k][idx];
+  }
+  if (!S->clamp[k]) q = q - floor(q);
+  return q;
+}
+
+static void vol_fwd_f32(const so_vol_params *P, const so_sampling *S, const float *dens,
+                        const int dim[3], const float *tf, float *img, int nthreads);
+
 SO_API void so_volume_fwd_f32(const so_vol_params *P, const float *dens,
                               const int dim[3], const float *tf, float *img,
                               int nthreads) {
+  vol_fwd_f32(P, NULL, dens, dim, tf, img, nthreads);
+}
+
+SO_API void so_volume_fwd_f32_ex(const so_vol_params *P, const so_sampling *S,
+                                 const float *dens, const int dim[3], const float *tf,
+                                 float *img, int nthreads) {
+  vol_fwd_f32(P, S, dens, dim, tf, img, nthreads);
+}
+
+static void vol_fwd_f32(const so_vol_params *P, const so_sampling *S, const float *dens,
+                        const int dim[3], const float *tf, float *img, int nthreads) {
   int W = P->width, H = P->height;
 #ifdef _OPENMP
   if (nthreads <= 0) nthreads = omp_get_max_threads();
@@ -1536,8 +1585,9 @@ SO_API void so_volume_fwd_f32(const so_vol_params *P, const float *dens,
           float t = t0 + ((float)s + 0.5f) * P->step;
           float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
           if (!vol_inside_f(p)) continue;
-          float rho = tex3d_f32(dens, dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
-                                0.5f * p[2] + 0.5f, 1, 1, 1);
+          float rho = tex3d_f32(dens, dim, samp_f32(S, 0, 0.5f * p[0] + 0.5f),
+                                samp_f32(S, 1, 0.5f * p[1] + 0.5f),
+                                samp_f32(S, 2, 0.5f * p[2] + 0.5f), 1, 1, 1);
           float x = rho * 255.0f;
           x = x < 0.0f ? 0.0f : (x > 255.0f ? 255.0f : x);
           int i0 = (int)x;
@@ -1608,10 +1658,27 @@ static double tex3d_f64(const double *img, const int dim[3], const double q[3],
  * when grad_dens/grad_tf are non-NULL, accumulates the analytic gradients
  * (reverse-order transmittance recomputation, the same scheme as the CUDA
  * adjoint).  img (optional): width*height*4 output. */
+static double vol_f64(const so_vol_params *P, const so_sampling *S, const double *dens,
+                      const int dim[3], const double *tf, const float *target, double *img,
+                      double *grad_dens, double *grad_tf);
+
 SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
                             const int dim[3], const double *tf,
                             const float *target, double *img, double *grad_dens,
                             double *grad_tf) {
+  return vol_f64(P, NULL, dens, dim, tf, target, img, grad_dens, grad_tf);
+}
+
+SO_API double so_volume_f64_ex(const so_vol_params *P, const so_sampling *S,
+                               const double *dens, const int dim[3], const double *tf,
+                               const float *target, double *img, double *grad_dens,
+                               double *grad_tf) {
+  return vol_f64(P, S, dens, dim, tf, target, img, grad_dens, grad_tf);
+}
+
+static double vol_f64(const so_vol_params *P, const so_sampling *S, const double *dens,
+                      const int dim[3], const double *tf, const float *target, double *img,
+                      double *grad_dens, double *grad_tf) {
   int W = P->width, H = P->height;
   double loss = 0.0;
   const int par = !grad_dens && !grad_tf; /* loss/image only: pixels in parallel */
@@ -1648,7 +1715,8 @@ SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
         double p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
         if (!(p[0] >= -1 && p[0] < 1 && p[1] >= -1 && p[1] < 1 && p[2] >= -1 && p[2] < 1))
           continue;
-        double q[3] = {0.5 * p[0] + 0.5, 0.5 * p[1] + 0.5, 0.5 * p[2] + 0.5};
+        double q[3] = {samp_f64(S, 0, 0.5 * p[0] + 0.5), samp_f64(S, 1, 0.5 * p[1] + 0.5),
+                       samp_f64(S, 2, 0.5 * p[2] + 0.5)};
         int cx[8];
         double w[8];
         double rho = tex3d_f64(dens, dim, q, cx, w);
@@ -1683,7 +1751,8 @@ SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
         double p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
         if (!(p[0] >= -1 && p[0] < 1 && p[1] >= -1 && p[1] < 1 && p[2] >= -1 && p[2] < 1))
           continue;
-        double q[3] = {0.5 * p[0] + 0.5, 0.5 * p[1] + 0.5, 0.5 * p[2] + 0.5};
+        double q[3] = {samp_f64(S, 0, 0.5 * p[0] + 0.5), samp_f64(S, 1, 0.5 * p[1] + 0.5),
+                       samp_f64(S, 2, 0.5 * p[2] + 0.5)};
         int cx[8];
         double w[8];
         double rho = tex3d_f64(dens, dim, q, cx, w);
@@ -2346,12 +2415,6 @@ SO_API void so_element_update(const double T[16], const double lbmin[3], const d
  *   bytes as v / 255.0f, doubles through float, alpha 1 when fewer than four
  *   components, (0,0,0,0) outside every block.
  * Formats: 0 byte, 1 float, 2 double (LSGL_RENDER_TEXTURE3D_FORMAT_*). */
-static inline float remap_ref(float x, const float *table, int n) {
-  int idx = (int)(x * n);
-  idx = idx > n - 1 ? n - 1 : idx;
-  idx = idx < 0 ? 0 : idx;
-  return table[idx];
-}
 
 static double texel_d(int fmt, const void *img, size_t k) {
   if (fmt == 0) return (double)(((const unsigned char *)img)[k] / 255.5f);

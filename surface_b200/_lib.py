@@ -28,6 +28,12 @@ class Camera(C.Structure):
                 ("height", C.c_int32), ("viewport", C.c_int32 * 4),
                 ("region", C.c_int32 * 4), ("step", C.c_int32)]
 
+class VolumeSampling(C.Structure):
+    """srt_volume_sampling (include/surface_rt.h)."""
+    _fields_ = [("remap", C.c_void_p * 3), ("remap_n", C.c_uint32 * 3),
+                ("clamp", C.c_int32 * 3)]
+
+
 class CacheKey(C.Structure):
     """srt_cache_key (include/surface_rt.h)."""
     _fields_ = [("elem_buffer", C.c_uint64), ("array_buffer", C.c_uint64),
@@ -103,6 +109,8 @@ _SIGS = {
     "srt_volume_camera": [C.c_int32, C.c_int32, _P, _P, _P, C.c_float, _P],
     "srt_volume_march_fwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P],
     "srt_volume_march_bwd": [_P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P],
+    "srt_volume_march_fwd_ex": [_P, _P, _P, _P, _P, _P, C.c_int32, _P, _P],
+    "srt_volume_march_bwd_ex": [_P, _P, _P, _P, _P, _P, C.c_int32, _P, _P, _P, _P, _P],
     "srt_spawn_secondary": [_P, _P, _P, _P, _SZ, C.c_uint64, _P, _P, _P],
     "srt_camera_rays": [_P, _P, _P, _P, _P],
     "srt_scene_create": [_P, C.POINTER(_P)],

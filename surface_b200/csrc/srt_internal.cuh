@@ -8,6 +8,7 @@
 
 #include <cuda_runtime.h>
 #include <float.h>
+#include <limits.h>
 #include <stdint.h>
 
 #include <atomic>
@@ -75,6 +76,26 @@ __device__ __forceinline__ float fmax_ref(float a, float b) { return (a < b) ? b
 
 // (uint32_t)x as g++ emits it on x86-64: a 64-bit truncating convert whose low
 // 32 bits are kept; NaN and |x| >= 2^63 give 0.
+// (int)x as x86-64 converts it: truncation, INT_MIN for NaN and for values
+// outside the int range.
+__device__ __forceinline__ int f2i_x86(float x) {
+  return (x >= -2147483648.0f && x < 2147483648.0f) ? (int)x : INT_MIN;
+}
+__device__ __forceinline__ int d2i_x86(double x) {
+  return (x > -2147483649.0 && x < 2147483648.0) ? (int)x : INT_MIN;
+}
+
+// fasterfloorf (render/render_texture.cc:108-121), the repeat wrap's floor.
+__device__ __forceinline__ int floor_ref(float x) {
+  if (x >= 0) return f2i_x86(x);
+  int y = f2i_x86(x);
+  if (fabsf(x - (float)y) <= FLT_EPSILON) {
+  } else {
+    y = y - 1;
+  }
+  return y;
+}
+
 __device__ __forceinline__ uint32_t f2u32_x86(float x) {
   if (!(fabsf(x) < 9.2233720368547758e18f)) return 0u;
   return (uint32_t)(long long)x;

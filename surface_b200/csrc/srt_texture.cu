@@ -45,26 +45,6 @@ struct srt_texture3d {
 namespace srt {
 namespace {
 
-// (int)x as x86-64 converts it: truncation, INT_MIN for NaN and for values
-// outside the int range.
-__device__ __forceinline__ int f2i_x86(float x) {
-  return (x >= -2147483648.0f && x < 2147483648.0f) ? (int)x : INT_MIN;
-}
-__device__ __forceinline__ int d2i_x86(double x) {
-  return (x > -2147483649.0 && x < 2147483648.0) ? (int)x : INT_MIN;
-}
-
-// fasterfloorf (render/render_texture.cc:108-121).
-__device__ __forceinline__ int floor_ref(float x) {
-  if (x >= 0) return f2i_x86(x);
-  int y = f2i_x86(x);
-  if (fabsf(x - (float)y) <= FLT_EPSILON) {
-  } else {
-    y = y - 1;
-  }
-  return y;
-}
-
 __device__ __forceinline__ int clampi(int v, int lo, int hi) {
   return min(max(v, lo), hi);
 }

@@ -26,7 +26,25 @@ struct VolConst {
   srt_volume_params p;
   int dim[3];
   int tfn;
+  // sampling state of the density texture: per-axis coordinate remap of a
+  // non-uniform volume and clamp-to-edge (else repeat) per axis
+  const float *remap[3];
+  int nremap[3];
+  int clamp[3];
 };
+
+// The fetch coordinate of axis k: local::remap (gles/gles_common.h:264-269)
+// then the repeat wrap of FilterTexture3DFloat unless clamp-to-edge.
+__device__ __forceinline__ float tex_coord(const VolConst &K, int k, float u) {
+  if (K.nremap[k]) {
+    const int nk = K.nremap[k];
+    int idx = f2i_x86(u * (float)nk);
+    idx = max(min(nk - 1, idx), 0);
+    u = __ldg(&K.remap[k][idx]);
+  }
+  if (!K.clamp[k]) u = u - (float)floor_ref(u);
+  return u;
+}
 
 // Lower texel corner (clamped) and trilinear fractions of a fetch.
 struct Cell {
@@ -170,8 +188,9 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
       const float t = t0 + ((float)s + 0.5f) * K.p.step;
       const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
       if (!inside(p)) continue;
-      const float rho = fetch(dens, K.dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
-                              0.5f * p[2] + 0.5f, nullptr);
+      const float rho = fetch(dens, K.dim, tex_coord(K, 0, 0.5f * p[0] + 0.5f),
+                              tex_coord(K, 1, 0.5f * p[1] + 0.5f),
+                              tex_coord(K, 2, 0.5f * p[2] + 0.5f), nullptr);
       float4 c;
       int i0, i1;
       float f;
@@ -270,8 +289,9 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
         if (!inside(p)) continue;
         Cell cl;
-        const float rho = fetch(dens, K.dim, 0.5f * p[0] + 0.5f, 0.5f * p[1] + 0.5f,
-                                0.5f * p[2] + 0.5f, &cl);
+        const float rho = fetch(dens, K.dim, tex_coord(K, 0, 0.5f * p[0] + 0.5f),
+                                tex_coord(K, 1, 0.5f * p[1] + 0.5f),
+                                tex_coord(K, 2, 0.5f * p[2] + 0.5f), &cl);
         float4 c, ta, tb;
         int i0, i1;
         float f;
@@ -366,7 +386,12 @@ srt_status make_const(const srt_volume_params *params, const int32_t dims[3],
     return SRT_ERR_INVALID;
   }
   K.p = *params;
-  for (int k = 0; k < 3; k++) K.dim[k] = dims[k];
+  for (int k = 0; k < 3; k++) {
+    K.dim[k] = dims[k];
+    K.remap[k] = nullptr;
+    K.nremap[k] = 0;
+    K.clamp[k] = 1;  // without a sampling state: clamp-to-edge, no remap
+  }
   K.tfn = tfn;
   return SRT_OK;
 }
@@ -390,6 +415,27 @@ static srt_status vol_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &st
   e = cudaMemcpyAsync(stage.p, p, bytes, cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_status(e, "volume copy");
   *out = stage.p;
+  return SRT_OK;
+}
+
+// The texture's sampling state into K; host remap tables are staged in tmp.
+static srt_status apply_sampling(srt_ctx *ctx, const srt_volume_sampling *sm, VolConst &K,
+                                 DevBuf (&tmp)[3], cudaStream_t st) {
+  if (!sm) return SRT_OK;
+  for (int k = 0; k < 3; k++) {
+    K.clamp[k] = sm->clamp[k] != 0;
+    if (sm->remap[k] && sm->remap_n[k]) {
+      if (sm->remap_n[k] > 0x7fffffffu) {
+        set_error("remap table longer than 2^31 - 1 entries");
+        return SRT_ERR_INVALID;
+      }
+      const void *dv;
+      srt_status s = vol_view(ctx, sm->remap[k], (size_t)sm->remap_n[k] * 4, tmp[k], &dv, st);
+      if (s != SRT_OK) return s;
+      K.remap[k] = static_cast<const float *>(dv);
+      K.nremap[k] = (int)sm->remap_n[k];
+    }
+  }
   return SRT_OK;
 }
 
@@ -431,16 +477,19 @@ SRT_API srt_status srt_volume_camera(int32_t W, int32_t H, const float eye[3],
   return SRT_OK;
 }
 
-SRT_API srt_status srt_volume_march_fwd(srt_ctx *ctx, const srt_volume_params *params,
-                                        const float *density, const int32_t dims[3],
-                                        const float *tf, int32_t tf_entries, float *image,
-                                        float *transmittance) {
+SRT_API srt_status srt_volume_march_fwd_ex(srt_ctx *ctx, const srt_volume_params *params,
+                                           const srt_volume_sampling *sampling,
+                                           const float *density, const int32_t dims[3],
+                                           const float *tf, int32_t tf_entries, float *image,
+                                           float *transmittance) {
   if (!ctx || !density || !tf || !image) return SRT_ERR_INVALID;
   VolConst K;
   srt_status s = make_const(params, dims, tf_entries, K);
   if (s != SRT_OK) return s;
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
+  DevBuf remap_tmp[3];
+  if ((s = apply_sampling(ctx, sampling, K, remap_tmp, st)) != SRT_OK) return s;
   const size_t nvox = (size_t)dims[0] * dims[1] * dims[2];
   const size_t npix = (size_t)params->width * params->height;
   const void *dd, *dt;
@@ -468,16 +517,19 @@ SRT_API srt_status srt_volume_march_fwd(srt_ctx *ctx, const srt_volume_params *p
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "volume fwd");
   if (!img_dev) cudaMemcpyAsync(image, di, npix * 16, cudaMemcpyDeviceToHost, st);
   if (!tr_dev) cudaMemcpyAsync(transmittance, dtr, npix * 4, cudaMemcpyDeviceToHost, st);
-  if (!img_dev || !tr_dev) return cuda_status(cudaStreamSynchronize(st), "volume fwd");
+  const bool staged = remap_tmp[0].p || remap_tmp[1].p || remap_tmp[2].p;
+  if (!img_dev || !tr_dev || staged)
+    return cuda_status(cudaStreamSynchronize(st), "volume fwd");
   return SRT_OK;
 }
 
-SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx, const srt_volume_params *params,
-                                        const float *density, const int32_t dims[3],
-                                        const float *tf, int32_t tf_entries,
-                                        const float *image, const float *transmittance,
-                                        const float *grad_image, float *grad_density,
-                                        float *grad_tf) {
+SRT_API srt_status srt_volume_march_bwd_ex(srt_ctx *ctx, const srt_volume_params *params,
+                                           const srt_volume_sampling *sampling,
+                                           const float *density, const int32_t dims[3],
+                                           const float *tf, int32_t tf_entries,
+                                           const float *image, const float *transmittance,
+                                           const float *grad_image, float *grad_density,
+                                           float *grad_tf) {
   (void)image;  // the colour behind each sample is accumulated during the walk
   if (!ctx || !density || !tf || !transmittance || !grad_image || !grad_density || !grad_tf)
     return SRT_ERR_INVALID;
@@ -486,6 +538,8 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx, const srt_volume_params *p
   if (s != SRT_OK) return s;
   cudaSetDevice(ctx->device);
   cudaStream_t st = ctx->stream;
+  DevBuf remap_tmp[3];
+  if ((s = apply_sampling(ctx, sampling, K, remap_tmp, st)) != SRT_OK) return s;
   const size_t nvox = (size_t)dims[0] * dims[1] * dims[2];
   const size_t npix = (size_t)params->width * params->height;
   if (!is_device_ptr(grad_density) || !is_device_ptr(grad_tf)) {
@@ -514,8 +568,28 @@ SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx, const srt_volume_params *p
   ctx->launches++;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return cuda_status(e, "volume bwd");
-  if (s_tr.p || s_g.p) return cuda_status(cudaStreamSynchronize(st), "volume bwd");
+  if (s_tr.p || s_g.p || remap_tmp[0].p || remap_tmp[1].p || remap_tmp[2].p)
+    return cuda_status(cudaStreamSynchronize(st), "volume bwd");
   return SRT_OK;
+}
+
+
+SRT_API srt_status srt_volume_march_fwd(srt_ctx *ctx, const srt_volume_params *params,
+                                        const float *density, const int32_t dims[3],
+                                        const float *tf, int32_t tf_entries, float *image,
+                                        float *transmittance) {
+  return srt_volume_march_fwd_ex(ctx, params, nullptr, density, dims, tf, tf_entries, image,
+                                 transmittance);
+}
+
+SRT_API srt_status srt_volume_march_bwd(srt_ctx *ctx, const srt_volume_params *params,
+                                        const float *density, const int32_t dims[3],
+                                        const float *tf, int32_t tf_entries,
+                                        const float *image, const float *transmittance,
+                                        const float *grad_image, float *grad_density,
+                                        float *grad_tf) {
+  return srt_volume_march_bwd_ex(ctx, params, nullptr, density, dims, tf, tf_entries, image,
+                                 transmittance, grad_image, grad_density, grad_tf);
 }
 
 }  // extern "C"

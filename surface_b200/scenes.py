@@ -521,3 +521,10 @@ def sparse_blocks(fmt, comps, nblocks=12, seed=3, gdim=(64, 48, 40), overlap=Fal
         chunks.append(raw)
         off += len(raw)
     return b, b"".join(chunks), tuple(int(x) for x in gdim)
+
+
+def exp_coord_map(n):
+    """A non-uniform coordinate map of n entries: exp(4 i / n) normalised to
+    [0, 1] (the stretched axis of the reference's non-uniform volume example)."""
+    m = np.exp(4.0 * (np.arange(n, dtype=np.float32) / np.float32(n))).astype(np.float32)
+    return ((m - m[0]) / (m[-1] - m[0])).astype(np.float32)

@@ -51,7 +51,29 @@ def _dims(density):
     return np.array([w, h, d], np.int32)
 
 
-def march(density, tf, params, ctx: Context | None = None):
+class Sampling:
+    """The density texture's sampling state: per-axis remap tables of a
+    non-uniform volume (lsglTexCoordRemap; None for none) and clamp-to-edge
+    flags (False: GL's default repeat wrap).  Sampling() = clamp-to-edge, no
+    remap, which is what march() uses without one."""
+
+    def __init__(self, remap=(None, None, None), clamp=(True, True, True), device=0):
+        self.tables = [None if t is None else
+                       torch.as_tensor(np.ascontiguousarray(t, np.float32)).to(
+                           torch.device("cuda", device)) for t in remap]
+        self.clamp = tuple(bool(c) for c in clamp)
+
+    def struct(self):
+        sm = _lib.VolumeSampling()
+        for k in range(3):
+            t = self.tables[k]
+            sm.remap[k] = None if t is None else t.data_ptr()
+            sm.remap_n[k] = 0 if t is None else t.numel()
+            sm.clamp[k] = int(self.clamp[k])
+        return sm
+
+
+def march(density, tf, params, ctx: Context | None = None, sampling: Sampling | None = None):
     """Forward march: (image (H, W, 4), final transmittance (H, W))."""
     ctx = ctx or Context.default(density.device.index or 0)
     density = density.contiguous().float()
@@ -61,13 +83,16 @@ def march(density, tf, params, ctx: Context | None = None):
     trans = torch.empty((H, W), dtype=torch.float32, device=density.device)
     ctx.use_torch_stream()
     dims = _dims(density)
-    check(ctx.L.srt_volume_march_fwd(ctx.h, params.ctypes.data, density.data_ptr(),
-                                     dims.ctypes.data, tf.data_ptr(), tf.shape[0],
-                                     img.data_ptr(), trans.data_ptr()))
+    sm = None if sampling is None else sampling.struct()
+    check(ctx.L.srt_volume_march_fwd_ex(ctx.h, params.ctypes.data,
+                                        None if sm is None else C.byref(sm),
+                                        density.data_ptr(), dims.ctypes.data, tf.data_ptr(),
+                                        tf.shape[0], img.data_ptr(), trans.data_ptr()))
     return img, trans
 
 
-def march_backward(density, tf, params, trans, grad_image, ctx: Context | None = None):
+def march_backward(density, tf, params, trans, grad_image, ctx: Context | None = None,
+                   sampling: Sampling | None = None):
     """Adjoint: (d loss / d density, d loss / d tf)."""
     ctx = ctx or Context.default(density.device.index or 0)
     density = density.contiguous().float()
@@ -77,29 +102,34 @@ def march_backward(density, tf, params, trans, grad_image, ctx: Context | None =
     ctx.use_torch_stream()
     dims = _dims(density)
     g = grad_image.contiguous().float()
-    check(ctx.L.srt_volume_march_bwd(ctx.h, params.ctypes.data, density.data_ptr(),
-                                     dims.ctypes.data, tf.data_ptr(), tf.shape[0], None,
-                                     trans.contiguous().data_ptr(), g.data_ptr(),
-                                     gd.data_ptr(), gt.data_ptr()))
+    sm = None if sampling is None else sampling.struct()
+    check(ctx.L.srt_volume_march_bwd_ex(ctx.h, params.ctypes.data,
+                                        None if sm is None else C.byref(sm),
+                                        density.data_ptr(), dims.ctypes.data, tf.data_ptr(),
+                                        tf.shape[0], None, trans.contiguous().data_ptr(),
+                                        g.data_ptr(), gd.data_ptr(), gt.data_ptr()))
     return gd, gt
 
 
 class VolumeMarch(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, density, tf, params):
-        img, trans = march(density, tf, params)
+    def forward(ctx, density, tf, params, sampling=None):
+        img, trans = march(density, tf, params, sampling=sampling)
         ctx.save_for_backward(density, tf, trans)
         ctx.params = params
+        ctx.sampling = sampling
         return img
 
     @staticmethod
     def backward(ctx, grad_image):
         density, tf, trans = ctx.saved_tensors
-        gd, gt = march_backward(density, tf, ctx.params, trans, grad_image)
+        gd, gt = march_backward(density, tf, ctx.params, trans, grad_image,
+                                sampling=ctx.sampling)
         return (gd if ctx.needs_input_grad[0] else None,
-                gt if ctx.needs_input_grad[1] else None, None)
+                gt if ctx.needs_input_grad[1] else None, None, None)
 
 
-def render(density, tf, params):
-    """Differentiable image of `density` (D, H, W) through `tf` (entries, 4)."""
-    return VolumeMarch.apply(density, tf, params)
+def render(density, tf, params, sampling: Sampling | None = None):
+    """Differentiable image of `density` (D, H, W) through `tf` (entries, 4);
+    `sampling` adds non-uniform remap tables and wrap modes."""
+    return VolumeMarch.apply(density, tf, params, sampling)
