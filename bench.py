@@ -1,7 +1,7 @@
 """Benchmark: LBVH build + closest-hit throughput on B200 (one JSON line).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tet|tri|particles|volume|batched|frame|scene]
+                    [--workload tet|tri|particles|volume|batched|frame|scene|texture]
 
 Default workload (``tet``): the tetrahedral-mesh configuration -- 64^3 cells in
 the unit cube, five tetrahedra per cell (1,310,720 tets), interior vertices
@@ -10,7 +10,8 @@ step = LBVH build from the resident mesh + closest hit (FP64 Pluecker test)
 with barycentric scalar interpolation for every ray.  ``value`` = rays per
 second of the whole step (build included), in Mrays/s.  ``tri`` is the
 131,072-triangle / 512^2 pinhole configuration; ``particles`` one frame of the
-16,777,216-sphere configuration (rebuild + 2048^2 primaries).
+16,777,216-sphere configuration (rebuild + 2048^2 primaries); ``texture``
+16,777,216 texture3D fetches of a 512^3 sparse byte volume, in Mfetches/s.
 
 Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
 on the launching stream; the L2 is flushed (256 MiB write) between steps,
@@ -27,6 +28,7 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import re
 import statistics
 import subprocess
 import sys
@@ -111,6 +113,16 @@ def make_workload(name):
                                         "hit + RGBA8 and depth write per step",
                             "elements": len(E["elements"]),
                             "prims": int(sum(E["prims"])), "rays": 1024 * 1024})
+    if name == "texture":
+        blocks, pool, gdim = S.sparse_pages()
+        uvw = S.march_coords()
+        return dict(kind="texture", blocks=blocks, pool=pool, gdim=gdim, uvw=uvw,
+                    rays=np.zeros(uvw.shape[0], np.uint8),
+                    config={"workload": "sparse512: 512^3 sparse volume of 32^3 byte pages "
+                                        "in a 3D checkerboard (2048 of 4096 committed), "
+                                        "16,777,216 texture3D fetches per step (512x512 "
+                                        "march rays x 64 samples, ray-major)",
+                            "blocks": int(blocks.size), "fetches": int(uvw.shape[0])})
     if name == "batched":
         B = S.batched_scenes()
         return dict(kind="batched", B=B, rays=B["rays"],
@@ -429,14 +441,36 @@ def cpu_reference_scene(W, nthreads=0, stride=4):
     return rays.size / (tr + tt) / 1e6, tr, tt, sample.size, "port"
 
 
+def cpu_reference_texture(W, nthreads=0):
+    """Texture::Fetch of every coordinate on the host: the reference's own
+    SparseVolumeAccel (oracle/_ref) or else the CPU restatement, over
+    nthreads threads (each builds its block tree, as every texture unit of
+    the reference would).  Returns (Mfetches/s, 0, s, fetches, kind)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle import oracle as O
+    use_ref = O.have_ref() and O.ref() is not None
+    nt = nthreads or os.cpu_count() or 1
+    uvw = W["uvw"]
+    parts = np.array_split(np.arange(uvw.shape[0]), nt)
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(nt) as ex:
+        list(ex.map(lambda ix: O.sparse_fetch(W["blocks"], W["pool"], 0, 1, W["gdim"],
+                                              uvw[ix[0]:ix[-1] + 1], use_ref=use_ref),
+                    [q for q in parts if q.size]))
+    tt = time.perf_counter() - t0
+    return (uvw.shape[0] / tt / 1e6, 0.0, tt, uvw.shape[0],
+            "reference" if use_ref else "port")
+
+
 def run_reference_arm(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     cores = os.cpu_count() or 1
     step = {"batched": cpu_reference_batched, "sphere": cpu_reference_particles,
-            "frame": cpu_reference_frame, "scene": cpu_reference_scene}.get(
-                W["kind"], cpu_reference_step)
+            "frame": cpu_reference_frame, "scene": cpu_reference_scene,
+            "texture": cpu_reference_texture}.get(W["kind"], cpu_reference_step)
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
@@ -450,6 +484,7 @@ def run_reference_arm(args, W):
     if W["kind"] == "sphere":
         nr = int(ns * 4)  # primaries + secondaries of one frame
     ms = 1e3 * nr / (value * 1e6)
+    unit = "Mfetches/s" if W["kind"] == "texture" else "Mrays/s"
     stride = 16 if W["kind"] == "batched" else 4
     sample = (f"full Build32 + every {stride}th ray ({ns} of {nr}) per step, trace time "
               f"scaled to all rays; median of {args.steps}")
@@ -462,22 +497,29 @@ def run_reference_arm(args, W):
                   f"4th pixel ({ns} of {nr}) scaled to all, by the CPU restatement "
                   f"(OpenMP; the reference's RenderGraph needs its GL front end); median "
                   f"of {args.steps}")
+    if W["kind"] == "texture":
+        sample = (f"every fetch ({ns}) per step through the reference's own "
+                  f"SparseVolumeAccel (Build + Sample) over {cores} threads; median of "
+                  f"{args.steps}")
     line = {
         "impl": "reference",
         "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART,
-                   "frame": METRIC_FRAME, "scene": METRIC_SCENE}.get(W["kind"], METRIC),
-        "value": round(value, 4), "unit": "Mrays/s",
+                   "frame": METRIC_FRAME, "scene": METRIC_SCENE,
+                   "texture": METRIC_TEX}.get(W["kind"], METRIC),
+        "value": round(value, 4), "unit": unit,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPE[W["kind"]], "data": "synthetic",
         "config": W["config"],
         ("rays_write_ms" if W["kind"] in ("frame", "scene") else "build_ms"):
             round(1e3 * statistics.median(tbs), 3),
-        "cpu_baseline": {"value": round(value, 4), "unit": "Mrays/s", "cores": cores,
+        "cpu_baseline": {"value": round(value, 4), "unit": unit, "cores": cores,
                          "kind": kind, "sample": sample},
-        "e2e": {"value": round(value, 4), "unit": "Mrays/s", "h2d_bytes_per_step": 0,
+        "e2e": {"value": round(value, 4), "unit": unit, "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if W["kind"] == "texture":
+        line.pop("build_ms", None)
     print(json.dumps(line), flush=True)
 
 
@@ -488,7 +530,9 @@ METRIC_PART = "Mrays/s (particle frame: LBVH rebuild + primaries + secondaries p
 METRIC_FRAME = "Mrays/s (frame: eye rays + closest hit + framebuffer write per step)"
 METRIC_SCENE = ("Mrays/s (scene frame: top-level build + eye rays + closest hit over "
                 "transformed elements + framebuffer write per step)")
+METRIC_TEX = "Mfetches/s (sparse volume texture3D fetch per step)"
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
+         "texture": "u8 texels / f64 block tree",
          "volume": "f32", "batched": "f32", "frame": "f32",
          "scene": "f64 transforms and top-level boxes / f32 + f64 element tests"}
 
@@ -633,6 +677,115 @@ def run_volume(args, W):
             "cpu_baseline": cpu}
     if rank == 0:
         print(json.dumps(line), flush=True)
+    dist_teardown()
+
+
+# ---------------------------------------------------------------- texture
+# algorithmic bytes of one sparse fetch: its coordinate (12) read, its RGBA
+# (16) written, one byte texel read (the block tree, 4095 nodes, stays cached)
+TEX_BYTES_PER_FETCH = 12 + 16 + 1
+
+
+def run_texture(args, W):
+    """Texture::Fetch of a sparse volume: every step fetches all coordinates
+    (device resident, larger than L2).  e2e: coordinates from pinned host
+    memory in, RGBA back, every step."""
+    import torch
+
+    from surface_b200 import _lib
+    from surface_b200.texture import Texture3D
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
+    tex = Texture3D(device=dev.index)
+    tex.set_sparse(W["blocks"], W["pool"], 0, 1, W["gdim"])
+    L = _lib.load()
+    n = W["uvw"].shape[0]
+    uvw = torch.as_tensor(W["uvw"], device=dev)
+    out = torch.empty((n, 4), dtype=torch.float32, device=dev)
+
+    def step():
+        tex.Fetch(uvw, out)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = L.srt_ctx_launch_count(tex.ctx.h)
+        for k in range(args.steps):
+            ev[k][0].record()
+            step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        barrier()
+        launches = L.srt_ctx_launch_count(tex.ctx.h) - launches0
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
+    ms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in ev)], dev)[0]
+    value = world * n / (ms * 1e-3) / 1e6
+
+    # e2e through the public call with host buffers
+    h_uvw = torch.from_numpy(W["uvw"]).pin_memory()
+    h_out = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        uvw.copy_(h_uvw, non_blocking=True)
+        tex.Fetch(uvw, out)
+        h_out.copy_(out, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e = {"value": round(world * n / (e2e_ms * 1e-3) / 1e6, 3), "unit": "Mfetches/s",
+           "h2d_bytes_per_step": int(h_uvw.numel() * 4),
+           "d2h_bytes_per_step": int(h_out.numel() * 4), "ms_per_step": round(e2e_ms, 3)}
+    # parity of this run's output with the restatement on a slice
+    got = out[:65536].cpu().numpy()
+    hbm, src = peaks()
+    alg = TEX_BYTES_PER_FETCH * n
+    traffic = None
+    prof = os.path.join(PROFILES, "sparse_fetch_kernel.sparse512.md")
+    if os.path.exists(prof):
+        m = re.search(r"traffic_per_launch_bytes:\s*(\d+)", open(prof).read())
+        traffic = int(m.group(1)) if m else None
+    roofline = {"bound": "hbm", "kernel": "sparse_fetch_kernel",
+                "achieved": round(alg / (ms * 1e-3) / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(alg / (ms * 1e-3) / 1e9 / hbm, 4), "peak_source": src,
+                "traffic": traffic, "algorithmic_bytes_per_launch": int(alg)}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        want = O.sparse_fetch(W["blocks"], W["pool"], 0, 1, W["gdim"], W["uvw"][:65536])
+        if not np.array_equal(got.view(np.uint32), want.view(np.uint32)):
+            raise SystemExit("sparse fetch differs from the oracle")
+        v, _, tt, ns, kind = cpu_reference_texture(W)
+        cpu = {"value": round(v, 3), "unit": "Mfetches/s", "cores": os.cpu_count(),
+               "kind": kind, "sample": f"all {ns} fetches, {os.cpu_count()} threads",
+               "seconds": round(tt, 3)}
+    line = {"metric": METRIC_TEX, "value": round(value, 3), "unit": "Mfetches/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": DTYPE["texture"], "data": "synthetic",
+            "config": dict(W["config"], l2="inputs larger than L2 (201 MB coordinates, "
+                                           "268 MB RGBA)"),
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roofline, "cpu_baseline": cpu}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    tex.close()
     dist_teardown()
 
 
@@ -1500,7 +1653,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
                     choices=["tet", "tri", "particles", "volume", "batched", "frame",
-                             "scene"])
+                             "scene", "texture"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -1524,6 +1677,8 @@ def main():
         run_frame(args, W)
     elif args.workload == "scene":
         run_scene(args, W)
+    elif args.workload == "texture":
+        run_texture(args, W)
     else:
         run_ours(args, W)
 

@@ -528,3 +528,46 @@ def exp_coord_map(n):
     [0, 1] (the stretched axis of the reference's non-uniform volume example)."""
     m = np.exp(4.0 * (np.arange(n, dtype=np.float32) / np.float32(n))).astype(np.float32)
     return ((m - m[0]) / (m[-1] - m[0])).astype(np.float32)
+
+
+def sparse_pages(ndiv=16, page=32, seed=123456):
+    """A sparse volume of committed pages in a 3D checkerboard (the layout of
+    the reference's sparse_volume_render example, which commits the pages
+    with (x + y + z) even out of 2x2x2): ndiv^3 page slots of page^3 byte
+    texels, half of them committed, each with its own seeded smooth-ish
+    content.  Returns (blocks, pool bytes, global dims)."""
+    rng = np.random.default_rng(seed)
+    dt = np.dtype([("offset", "<i4", 3), ("extent", "<i4", 3), ("size", "<i4", 3),
+                   ("level", "<i4"), ("data_offset", "<u8")])
+    slots = [(x, y, z) for z in range(ndiv) for y in range(ndiv) for x in range(ndiv)
+             if (x + y + z) % 2 == 0]
+    b = np.zeros(len(slots), dt)
+    nv = page ** 3
+    g = np.arange(page, dtype=np.float32) / page
+    base = (np.sin(6.0 * g)[None, None, :] + np.cos(5.0 * g)[None, :, None]
+            + np.sin(4.0 * g + 1.0)[:, None, None])
+    pool = np.empty(len(slots) * nv, np.uint8)
+    for n, (x, y, z) in enumerate(slots):
+        b[n]["offset"] = (x * page, y * page, z * page)
+        b[n]["extent"] = (page, page, page)
+        b[n]["size"] = (page, page, page)
+        b[n]["data_offset"] = n * nv
+        a, c = rng.random(2).astype(np.float32)
+        pool[n * nv:(n + 1) * nv] = np.clip(40.0 * (base * (0.5 + a) + 3.0 * c), 0,
+                                            255).astype(np.uint8).reshape(-1)
+    return b, pool.tobytes(), (ndiv * page,) * 3
+
+
+def march_coords(w=512, h=512, steps=64):
+    """Texture coordinates of a shader march: w x h parallel rays tilted by
+    (0.2, 0.1) per unit depth, `steps` samples each from r = 1 down to 0,
+    ray-major ((ray, step) -> ray * steps + step), all inside [0, 1)^3.
+    Returns (w * h * steps, 3) float32."""
+    x = (0.8 * (np.arange(w, dtype=np.float32) + 0.5) / w).astype(np.float32)
+    y = (0.9 * (np.arange(h, dtype=np.float32) + 0.5) / h).astype(np.float32)
+    s = ((np.arange(steps, dtype=np.float32) + 0.5) / steps).astype(np.float32)
+    out = np.empty((h, w, steps, 3), np.float32)
+    out[..., 0] = x[None, :, None] + np.float32(0.2) * s[None, None, :]
+    out[..., 1] = y[:, None, None] + np.float32(0.1) * s[None, None, :]
+    out[..., 2] = np.float32(1.0) - s[None, None, :]
+    return out.reshape(-1, 3)
