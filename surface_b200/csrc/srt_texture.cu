@@ -17,10 +17,21 @@
 // all three axes as the reference does, bytes as v / 255.0f, doubles through
 // float, alpha 1 below four components, (0, 0, 0, 0) outside every block.
 //
+// Locate is answered through a cell grid built with the tree: Locate's
+// answer is the first leaf in depth-first (left first) order whose box holds
+// the point, because every node's box holds its children's (the 1e-6
+// widening grows with the extent).  Each cell of an integer lattice over the
+// blocks keeps the first leaf whose box holds the whole cell (its owner), the
+// earlier leaves that reach into the cell (tested in order) and a core box
+// clear of them; a point inside the core takes the owner (or no block, in a
+// cell without one) with no box test.
+// Cells with more than kCellList candidates walk the tree.
+//
 // Float-to-int conversions follow x86 (NaN and out-of-range values give
 // INT_MIN), so every coordinate gives the reference's texel.  Compiled without
 // FMA contraction: each expression rounds as in the reference.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -40,6 +51,9 @@ struct srt_texture3d {
   uint32_t nremap[3] = {0, 0, 0};
   DevBuf tree, blocks;       // sparse: BVHTree over the blocks, block table
   uint32_t nblocks = 0, ntree = 0;
+  DevBuf cells, leaves, list;  // sparse: the tree's cell grid (cells.p null: none)
+  float ulo[3], uhi[3];
+  int org[3], shift[3], g[3];
 };
 
 namespace srt {
@@ -131,12 +145,51 @@ dense_fetch_kernel(DenseTex t, const float *__restrict__ uvw, size_t n,
   }
 }
 
+// A leaf of the block tree in depth-first order: its (widened) box and block.
+struct SparseLeaf {
+  double bmin[3], bmax[3];
+  int32_t block, pad;
+};
+// One lattice cell: `owner` (the block of the first leaf holding the whole
+// cell, -1 if none), list[off .. off + n) the leaves to test in order before
+// the owner (with no owner: every leaf reaching into the cell), and the
+// cell's open core clear of those leaves, where the answer is `owner`.
+// walk != 0: walk the tree.
+struct alignas(16) SparseCell {
+  float core_lo[3];
+  int32_t owner;
+  float core_hi[3];
+  uint32_t off;
+  uint32_t n, walk, pad[2];
+};
+static_assert(sizeof(SparseCell) == 48, "three 16-byte loads");
+// A block as the sample reads it: size[0] / extent[0] (the reference scales
+// all three axes by x's ratio), offset, size and the texels' byte offset.
+struct alignas(16) BlockRec {
+  double sx;
+  uint64_t data_off;
+  int32_t off[3], size0;
+  int32_t size1, size2, pad[2];
+};
+static_assert(sizeof(BlockRec) == 48, "three 16-byte loads");
+#ifndef SRT_FETCH_ILP
+#define SRT_FETCH_ILP 1
+#endif
+constexpr int kFetchILP = SRT_FETCH_ILP;  // fetches in flight per thread
+constexpr uint32_t kCellList = 16;
+
 struct SparseTex {
   const TopNode *tree;
-  const srt_volume_block *blocks;
+  const BlockRec *blocks;
   const unsigned char *pool;
   int gdim[3], comps, format;
   uint32_t max_iter;
+  // cell grid (cells == nullptr: walk the tree for every point)
+  const SparseCell *cells;
+  const SparseLeaf *leaves;
+  const uint32_t *list;
+  float ulo[3], uhi[3];  // the union of the leaf boxes, rounded out to floats
+  int org[3], shift[3], g[3];  // lattice origin, log2 cell size, cells
 };
 
 __device__ __forceinline__ bool in_box(const TopNode &t, const double p[3]) {
@@ -177,41 +230,140 @@ __device__ int locate(const TopNode *__restrict__ tree, const double p[3], uint3
   return -1;
 }
 
+struct CellView {
+  float lo[3], hi[3];
+  int owner;
+  uint32_t off, n, walk;
+};
+
+__device__ __forceinline__ CellView load_cell(const SparseCell *c) {
+  const int4 *q = reinterpret_cast<const int4 *>(c);
+  const int4 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+  CellView v;
+  v.lo[0] = __int_as_float(a.x);
+  v.lo[1] = __int_as_float(a.y);
+  v.lo[2] = __int_as_float(a.z);
+  v.owner = a.w;
+  v.hi[0] = __int_as_float(b.x);
+  v.hi[1] = __int_as_float(b.y);
+  v.hi[2] = __int_as_float(b.z);
+  v.off = (uint32_t)b.w;
+  v.n = (uint32_t)d.x;
+  v.walk = (uint32_t)d.y;
+  return v;
+}
+
+// The cell of p, clamped to the grid: floor((p - org) / 2^shift) is
+// (floor(p) - org) >> shift for an integer origin (NaN maps to cell 0 and
+// then fails the union test).
+__device__ __forceinline__ size_t cell_of(const SparseTex &t, const float pf[3]) {
+  int c[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    const long long d = ((long long)__float2int_rd(pf[k]) - t.org[k]) >> t.shift[k];
+    c[k] = (int)(d < 0 ? 0 : (d >= t.g[k] ? t.g[k] - 1 : d));
+  }
+  return ((size_t)c[2] * t.g[1] + c[1]) * t.g[0] + c[0];
+}
+
+// Locate from p's cell; the same block as locate() for every point.
+__device__ __forceinline__ int locate_cell(const SparseTex &t, const CellView &cell,
+                                           const float pf[3], const double p[3],
+                                           uint32_t *err) {
+  // outside the union of the leaf boxes: in no leaf (NaN included).  p is a
+  // float, so p >= lo exactly when p >= lo rounded up to a float.
+  if (!(pf[0] >= t.ulo[0] && pf[0] <= t.uhi[0] && pf[1] >= t.ulo[1] && pf[1] <= t.uhi[1] &&
+        pf[2] >= t.ulo[2] && pf[2] <= t.uhi[2]))
+    return -1;
+  if (cell.walk) return locate(t.tree, p, t.max_iter, err);
+  if (pf[0] > cell.lo[0] && pf[0] < cell.hi[0] && pf[1] > cell.lo[1] && pf[1] < cell.hi[1] &&
+      pf[2] > cell.lo[2] && pf[2] < cell.hi[2])
+    return cell.owner;
+  for (uint32_t j = 0; j < cell.n; j++) {
+    const SparseLeaf &L = t.leaves[__ldg(&t.list[cell.off + j])];
+    if (p[0] >= L.bmin[0] && p[0] <= L.bmax[0] && p[1] >= L.bmin[1] && p[1] <= L.bmax[1] &&
+        p[2] >= L.bmin[2] && p[2] <= L.bmax[2])
+      return L.block;
+  }
+  return cell.owner;
+}
+
+// SparseVolumeAccel::Sample of block `id` (>= 0) at p: the nearest texel.
+// The reference stores each component as a double and the caller reads it as
+// a float, so bytes give (float)b / 255.0f (lut), floats themselves and
+// doubles (float)d.
+__device__ __forceinline__ float4 sample_block(const SparseTex &t, int id, const double p[3],
+                                               const float *lut) {
+  const int4 *q = reinterpret_cast<const int4 *>(t.blocks + id);
+  const int4 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
+  const double sx = __hiloint2double(a.y, a.x);
+  const uint64_t data_off = ((uint64_t)(uint32_t)a.w << 32) | (uint32_t)a.z;
+  const int size[3] = {b.w, d.x, d.y};
+  const double x = (p[0] - (double)b.x) * sx;
+  const double y = (p[1] - (double)b.y) * sx;  // x's ratio on every axis
+  const double z = (p[2] - (double)b.z) * sx;
+  const int ix = max(min(size[0] - 1, d2i_x86(x)), 0);
+  const int iy = max(min(size[1] - 1, d2i_x86(y)), 0);
+  const int iz = max(min(size[2] - 1, d2i_x86(z)), 0);
+  const size_t idx = ((size_t)iz * size[1] + (size_t)iy) * (size_t)size[0] + (size_t)ix;
+  const unsigned char *base = t.pool + data_off;
+  const int nc = t.comps >= 4 ? 4 : t.comps;
+  float v[4] = {0.f, 0.f, 0.f, 1.f};
+  for (int c = 0; c < nc; c++) {
+    const size_t k = (size_t)nc * idx + c;  // the stride is the clamped count
+    if (t.format == 0)
+      v[c] = lut[__ldg(base + k)];
+    else if (t.format == 1)
+      v[c] = __ldg(reinterpret_cast<const float *>(base) + k);
+    else
+      v[c] = (float)__ldg(reinterpret_cast<const double *>(base) + k);
+  }
+  return make_float4(v[0], v[1], v[2], v[3]);
+}
+
+// kFetchILP fetches per thread per round, block-strided so that every load
+// and store stays coalesced; the stages (coordinates, cells, locate, texels)
+// run for all of them before the next, keeping their loads in flight together.
 __global__ void __launch_bounds__(256)
 sparse_fetch_kernel(SparseTex t, const float *__restrict__ uvw, size_t n,
                     float4 *__restrict__ rgba, uint32_t *__restrict__ err) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    double p[3];
+  __shared__ float lut[256];  // byte texel b -> (float)b / 255.0f
+  for (int k = threadIdx.x; k < 256; k += blockDim.x) lut[k] = (float)k / 255.0f;
+  __syncthreads();
+  const size_t step = (size_t)blockDim.x * kFetchILP;
+  for (size_t base = (size_t)blockIdx.x * step + threadIdx.x; base < n;
+       base += (size_t)gridDim.x * step) {
+    float pf[kFetchILP][3];
+    double p[kFetchILP][3];
 #pragma unroll
-    for (int k = 0; k < 3; k++) p[k] = (double)(__ldg(&uvw[3 * i + k]) * (float)t.gdim[k]);
-    double v[4] = {0.0, 0.0, 0.0, 0.0};
-    const int id = locate(t.tree, p, t.max_iter, err);
-    if (id >= 0) {
-      const srt_volume_block &bl = t.blocks[id];
-      const int nc = t.comps >= 4 ? 4 : t.comps;
-      v[3] = 1.0;
-      const double sx = (double)bl.size[0] / (double)bl.extent[0];
-      const double x = (p[0] - (double)bl.offset[0]) * sx;
-      const double y = (p[1] - (double)bl.offset[1]) * sx;  // x's ratio on every axis
-      const double z = (p[2] - (double)bl.offset[2]) * sx;
-      const int ix = max(min(bl.size[0] - 1, d2i_x86(x)), 0);
-      const int iy = max(min(bl.size[1] - 1, d2i_x86(y)), 0);
-      const int iz = max(min(bl.size[2] - 1, d2i_x86(z)), 0);
-      const size_t idx =
-          ((size_t)iz * bl.size[1] + (size_t)iy) * (size_t)bl.size[0] + (size_t)ix;
-      const unsigned char *base = t.pool + bl.data_offset;
-      for (int c = 0; c < nc; c++) {
-        const size_t k = (size_t)nc * idx + c;  // the stride is the clamped count
-        if (t.format == 0)
-          v[c] = (double)((float)base[k] / 255.0f);
-        else if (t.format == 1)
-          v[c] = (double)reinterpret_cast<const float *>(base)[k];
-        else
-          v[c] = (double)(float)reinterpret_cast<const double *>(base)[k];
+    for (int j = 0; j < kFetchILP; j++) {
+      const size_t i = base + (size_t)j * blockDim.x;
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        pf[j][k] = (i < n ? __ldg(&uvw[3 * i + k]) : 0.0f) * (float)t.gdim[k];
+        p[j][k] = (double)pf[j][k];
       }
     }
-    rgba[i] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)v[3]);
+    int id[kFetchILP];
+    if (t.cells) {
+      CellView cv[kFetchILP];
+#pragma unroll
+      for (int j = 0; j < kFetchILP; j++) cv[j] = load_cell(t.cells + cell_of(t, pf[j]));
+#pragma unroll
+      for (int j = 0; j < kFetchILP; j++) id[j] = locate_cell(t, cv[j], pf[j], p[j], err);
+    } else {
+#pragma unroll
+      for (int j = 0; j < kFetchILP; j++) id[j] = locate(t.tree, p[j], t.max_iter, err);
+    }
+    float4 out[kFetchILP];
+#pragma unroll
+    for (int j = 0; j < kFetchILP; j++)
+      out[j] = id[j] >= 0 ? sample_block(t, id[j], p[j], lut) : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+    for (int j = 0; j < kFetchILP; j++) {
+      const size_t i = base + (size_t)j * blockDim.x;
+      if (i < n) rgba[i] = out[j];
+    }
   }
 }
 
@@ -225,6 +377,213 @@ srt_status upload(srt_ctx *ctx, DevBuf &dst, const void *src, size_t bytes) {
                         ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // src may be freed next
   return cuda_status(e, "texture upload");
+}
+
+// The cell grid of a block tree (host).  Lattice: origin at the smallest
+// block offset, per-axis cell size the power of two nearest the median block
+// extent, at most 2^20 cells; built = false when the blocks would need more
+// than 2^26 (leaf, cell) pairs, and every point then walks the tree.
+struct CellGrid {
+  bool built = false;
+  std::vector<SparseCell> cells;
+  std::vector<SparseLeaf> leaves;
+  std::vector<uint32_t> list;
+  double org[3], inv[3], ulo[3], uhi[3];
+  int g[3], shift[3];
+};
+
+float round_up_f(double x) {
+  float f = (float)x;
+  if ((double)f < x) f = nextafterf(f, INFINITY);
+  return f;
+}
+float round_down_f(double x) {
+  float f = (float)x;
+  if ((double)f > x) f = nextafterf(f, -INFINITY);
+  return f;
+}
+
+void build_cell_grid(const std::vector<TopNode> &tree, const srt_volume_block *blocks,
+                     size_t nblocks, CellGrid &G) {
+  G = CellGrid();
+  // leaves in depth-first order, left child first (Locate's visiting order)
+  std::vector<int32_t> stk{0};
+  while (!stk.empty()) {
+    const TopNode &t = tree[stk.back()];
+    stk.pop_back();
+    if (t.leaf) {
+      SparseLeaf L{};
+      for (int k = 0; k < 3; k++) {
+        L.bmin[k] = t.bmin[k];
+        L.bmax[k] = t.bmax[k];
+      }
+      L.block = (int32_t)t.id;
+      G.leaves.push_back(L);
+      continue;
+    }
+    if (t.child[1] > 0) stk.push_back(t.child[1]);
+    if (t.child[0] > 0) stk.push_back(t.child[0]);
+  }
+  if (G.leaves.empty()) return;
+  double c[3];
+  for (int k = 0; k < 3; k++) {
+    int64_t lo = blocks[0].offset[k], hi = (int64_t)blocks[0].offset[k] + blocks[0].extent[k];
+    std::vector<int32_t> ext(nblocks);
+    for (size_t i = 0; i < nblocks; i++) {
+      lo = std::min<int64_t>(lo, blocks[i].offset[k]);
+      hi = std::max<int64_t>(hi, (int64_t)blocks[i].offset[k] + blocks[i].extent[k]);
+      ext[i] = blocks[i].extent[k];
+    }
+    std::nth_element(ext.begin(), ext.begin() + nblocks / 2, ext.end());
+    const int e2 = std::max(0, (int)lrint(log2((double)ext[nblocks / 2])));
+    c[k] = ldexp(1.0, std::min(e2, 24));
+    G.org[k] = (double)lo;
+    const double span = (double)(hi - lo);
+    while (ceil(span / c[k]) > 1024.0) c[k] *= 2.0;
+    G.g[k] = std::max(1, (int)ceil(span / c[k]));
+    G.ulo[k] = G.leaves[0].bmin[k];
+    G.uhi[k] = G.leaves[0].bmax[k];
+    for (const SparseLeaf &L : G.leaves) {
+      G.ulo[k] = std::min(G.ulo[k], L.bmin[k]);
+      G.uhi[k] = std::max(G.uhi[k], L.bmax[k]);
+    }
+  }
+  while ((int64_t)G.g[0] * G.g[1] * G.g[2] > (1 << 20)) {
+    const int k = (G.g[0] >= G.g[1] && G.g[0] >= G.g[2]) ? 0 : (G.g[1] >= G.g[2] ? 1 : 2);
+    c[k] *= 2.0;
+    G.g[k] = (G.g[k] + 1) / 2;
+  }
+  for (int k = 0; k < 3; k++) {
+    G.inv[k] = 1.0 / c[k];
+    G.shift[k] = ilogb(c[k]);
+  }
+  // the region of points mapped to cell i on axis k: the lattice interval
+  // with a margin far above the rounding of the index, the outer cells out
+  // to the union box
+  auto cell_lo = [&](int k, int i) {
+    double v = G.org[k] + i * c[k];
+    v -= c[k] * 0x1p-30;
+    return i == 0 ? std::min(v, G.ulo[k]) : v;
+  };
+  auto cell_hi = [&](int k, int i) {
+    double v = G.org[k] + (i + 1) * c[k];
+    v += c[k] * 0x1p-30;
+    return i == G.g[k] - 1 ? std::max(v, G.uhi[k]) : v;
+  };
+  auto range = [&](int k, double a, double b, int &i0, int &i1) {
+    i0 = (int)std::max(0.0, std::min((double)G.g[k] - 1, floor((a - G.org[k]) * G.inv[k]) - 1));
+    i1 = (int)std::max(0.0, std::min((double)G.g[k] - 1, floor((b - G.org[k]) * G.inv[k]) + 1));
+  };
+  uint64_t pairs = 0;
+  for (const SparseLeaf &L : G.leaves) {
+    int r[3][2];
+    for (int k = 0; k < 3; k++) range(k, L.bmin[k], L.bmax[k], r[k][0], r[k][1]);
+    pairs += (uint64_t)(r[0][1] - r[0][0] + 1) * (r[1][1] - r[1][0] + 1) * (r[2][1] - r[2][0] + 1);
+    if (pairs > (1ull << 26)) return;
+  }
+  const size_t ncell = (size_t)G.g[0] * G.g[1] * G.g[2];
+  // the first kCellList + 1 leaves reaching into each cell, in order
+  const uint32_t cap = kCellList + 1;
+  std::vector<uint32_t> cnt(ncell, 0), cand(ncell * (size_t)cap);
+  std::vector<uint8_t> more(ncell, 0);
+  for (uint32_t li = 0; li < (uint32_t)G.leaves.size(); li++) {
+    const SparseLeaf &L = G.leaves[li];
+    int r[3][2];
+    for (int k = 0; k < 3; k++) range(k, L.bmin[k], L.bmax[k], r[k][0], r[k][1]);
+    for (int z = r[2][0]; z <= r[2][1]; z++)
+      for (int y = r[1][0]; y <= r[1][1]; y++)
+        for (int x = r[0][0]; x <= r[0][1]; x++) {
+          const int ix[3] = {x, y, z};
+          bool hit = true;
+          for (int k = 0; k < 3 && hit; k++)
+            hit = L.bmin[k] <= cell_hi(k, ix[k]) && L.bmax[k] >= cell_lo(k, ix[k]);
+          if (!hit) continue;
+          const size_t ci = ((size_t)z * G.g[1] + y) * G.g[0] + x;
+          if (cnt[ci] < cap)
+            cand[ci * cap + cnt[ci]++] = li;
+          else
+            more[ci] = 1;
+        }
+  }
+  G.cells.resize(ncell);
+  for (int z = 0; z < G.g[2]; z++)
+    for (int y = 0; y < G.g[1]; y++)
+      for (int x = 0; x < G.g[0]; x++) {
+        const size_t ci = ((size_t)z * G.g[1] + y) * G.g[0] + x;
+        const int ix[3] = {x, y, z};
+        double lo[3], hi[3];
+        for (int k = 0; k < 3; k++) {
+          lo[k] = cell_lo(k, ix[k]);
+          hi[k] = cell_hi(k, ix[k]);
+        }
+        SparseCell &C = G.cells[ci];
+        C = SparseCell{};
+        C.owner = -1;
+        C.off = (uint32_t)G.list.size();
+        uint32_t own = cnt[ci];
+        for (uint32_t j = 0; j < cnt[ci]; j++) {
+          const SparseLeaf &L = G.leaves[cand[ci * cap + j]];
+          if (L.bmin[0] <= lo[0] && L.bmax[0] >= hi[0] && L.bmin[1] <= lo[1] &&
+              L.bmax[1] >= hi[1] && L.bmin[2] <= lo[2] && L.bmax[2] >= hi[2]) {
+            own = j;
+            break;
+          }
+        }
+        const bool has_owner = own < cnt[ci];
+        if ((has_owner ? own : cnt[ci]) > kCellList || (!has_owner && more[ci])) {
+          C.walk = 1;
+          continue;
+        }
+        const uint32_t n = has_owner ? own : cnt[ci];
+        for (uint32_t j = 0; j < n; j++) G.list.push_back(cand[ci * cap + j]);
+        C.n = n;
+        for (int k = 0; k < 3; k++) {
+          C.core_lo[k] = INFINITY;
+          C.core_hi[k] = -INFINITY;
+        }
+        if (has_owner) C.owner = G.leaves[cand[ci * cap + own]].block;
+        // the open core: the cell cut clear of each listed leaf (those before
+        // the owner; with no owner, all that reach in), on the side that keeps
+        // the most of it.  A point in the core is in the owner (or in none).
+        double a[3] = {lo[0], lo[1], lo[2]}, b[3] = {hi[0], hi[1], hi[2]};
+        bool empty = false;
+        for (uint32_t j = 0; j < n && !empty; j++) {
+          const SparseLeaf &L = G.leaves[cand[ci * cap + j]];
+          bool meets = true;
+          for (int k = 0; k < 3; k++) meets = meets && L.bmin[k] < b[k] && L.bmax[k] > a[k];
+          if (!meets) continue;
+          int bk = -1, bside = 0;
+          double best = -1.0;
+          for (int k = 0; k < 3; k++) {
+            const double w = b[k] - a[k];
+            const double keep_hi = (b[k] - L.bmax[k]) / w;  // core above the leaf
+            const double keep_lo = (L.bmin[k] - a[k]) / w;  // core below the leaf
+            if (keep_hi > best) {
+              best = keep_hi;
+              bk = k;
+              bside = 0;
+            }
+            if (keep_lo > best) {
+              best = keep_lo;
+              bk = k;
+              bside = 1;
+            }
+          }
+          if (best <= 0.0) {
+            empty = true;
+          } else if (bside == 0) {
+            a[bk] = L.bmax[bk];
+          } else {
+            b[bk] = L.bmin[bk];
+          }
+        }
+        if (empty) continue;
+        for (int k = 0; k < 3; k++) {
+          C.core_lo[k] = round_up_f(a[k]);
+          C.core_hi[k] = round_down_f(b[k]);
+        }
+      }
+  G.built = true;
 }
 
 }  // namespace
@@ -327,11 +686,42 @@ SRT_API srt_status srt_texture3d_set_sparse(srt_texture3d *t, int format, int co
   }
   std::vector<TopNode> tree;
   build_top_tree(lo.data(), hi.data(), nblocks, tree);
+  CellGrid G;
+  build_cell_grid(tree, blocks, nblocks, G);
   cudaSetDevice(t->ctx->device);
   srt_status s = upload(t->ctx, t->data, pool, pool_bytes);
   if (s == SRT_OK) s = upload(t->ctx, t->tree, tree.data(), tree.size() * sizeof(TopNode));
-  if (s == SRT_OK) s = upload(t->ctx, t->blocks, blocks, nblocks * sizeof(srt_volume_block));
-  if (s != SRT_OK) return s;
+  std::vector<BlockRec> recs(nblocks);
+  for (size_t i = 0; i < nblocks; i++) {
+    BlockRec &r = recs[i];
+    r = BlockRec{};
+    r.sx = (double)blocks[i].size[0] / (double)blocks[i].extent[0];
+    r.data_off = blocks[i].data_offset;
+    for (int k = 0; k < 3; k++) r.off[k] = blocks[i].offset[k];
+    r.size0 = blocks[i].size[0];
+    r.size1 = blocks[i].size[1];
+    r.size2 = blocks[i].size[2];
+  }
+  if (s == SRT_OK) s = upload(t->ctx, t->blocks, recs.data(), nblocks * sizeof(BlockRec));
+  t->cells.release();
+  if (s == SRT_OK && G.built) {
+    s = upload(t->ctx, t->leaves, G.leaves.data(), G.leaves.size() * sizeof(SparseLeaf));
+    if (s == SRT_OK)
+      s = upload(t->ctx, t->list, G.list.data(), G.list.size() * sizeof(uint32_t));
+    if (s == SRT_OK)
+      s = upload(t->ctx, t->cells, G.cells.data(), G.cells.size() * sizeof(SparseCell));
+    for (int k = 0; k < 3; k++) {
+      t->org[k] = (int)G.org[k];
+      t->shift[k] = G.shift[k];
+      t->ulo[k] = round_up_f(G.ulo[k]);
+      t->uhi[k] = round_down_f(G.uhi[k]);
+      t->g[k] = G.g[k];
+    }
+  }
+  if (s != SRT_OK) {
+    t->cells.release();
+    return s;
+  }
   t->sparse = true;
   t->format = format;
   t->comps = components;
@@ -362,12 +752,22 @@ SRT_API srt_status srt_texture3d_fetch(srt_texture3d *t, const float *uvw, size_
   if (t->sparse) {
     SparseTex st;
     st.tree = t->tree.as<TopNode>();
-    st.blocks = t->blocks.as<srt_volume_block>();
+    st.blocks = t->blocks.as<BlockRec>();
     st.pool = t->data.as<unsigned char>();
     for (int k = 0; k < 3; k++) st.gdim[k] = t->dim[k];
     st.comps = t->comps;
     st.format = t->format;
     st.max_iter = 4 * t->ntree + 8;
+    st.cells = t->cells.as<SparseCell>();
+    st.leaves = t->leaves.as<SparseLeaf>();
+    st.list = t->list.as<uint32_t>();
+    for (int k = 0; k < 3; k++) {
+      st.org[k] = t->org[k];
+      st.shift[k] = t->shift[k];
+      st.ulo[k] = t->ulo[k];
+      st.uhi[k] = t->uhi[k];
+      st.g[k] = t->g[k];
+    }
     sparse_fetch_kernel<<<grid, 256, 0, ctx->stream>>>(st, uvw, n, out, ctx->d_err);
   } else {
     DenseTex dt;

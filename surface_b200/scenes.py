@@ -571,3 +571,90 @@ def march_coords(w=512, h=512, steps=64):
     out[..., 1] = y[:, None, None] + np.float32(0.1) * s[None, None, :]
     out[..., 2] = np.float32(1.0) - s[None, None, :]
     return out.reshape(-1, 3)
+
+
+def sparse_table(offsets, extents, sizes, fmt, comps, seed):
+    """A block table (BLOCK layout) and data pool from per-block offsets,
+    extents and voxel sizes, with seeded texels."""
+    rng = np.random.default_rng(seed)
+    dt = np.dtype([("offset", "<i4", 3), ("extent", "<i4", 3), ("size", "<i4", 3),
+                   ("level", "<i4"), ("data_offset", "<u8")])
+    b = np.zeros(len(offsets), dt)
+    chunks, off = [], 0
+    for i, (o, e, z) in enumerate(zip(offsets, extents, sizes)):
+        b[i]["offset"], b[i]["extent"], b[i]["size"] = o, e, z
+        b[i]["data_offset"] = off
+        nv = int(np.prod(z)) * min(comps, 4)
+        data = (rng.integers(0, 256, size=nv, dtype=np.uint8) if fmt == 0 else
+                rng.random(nv).astype(np.float32 if fmt == 1 else np.float64))
+        raw = data.tobytes()
+        raw += b"\0" * ((-len(raw)) % 16)
+        chunks.append(raw)
+        off += len(raw)
+    return b, b"".join(chunks)
+
+
+LOCATE_CASES = ("crowded", "negative", "single", "nested", "slabs")
+
+
+def sparse_locate_case(case, fmt, comps):
+    """Block layouts that stress BVHTree::Locate: crowded (80 overlapping
+    blocks in 40^3, more than 16 reaching into many cells), negative offsets,
+    a single block, nested blocks (one around all), long thin slabs.
+    Returns (blocks, pool, global dims)."""
+    rng = np.random.default_rng({"crowded": 1, "negative": 2, "single": 3, "nested": 4,
+                                 "slabs": 5}[case])
+    if case == "crowded":
+        n = 80
+        ext = rng.integers(3, 17, size=(n, 3))
+        off = rng.integers(0, 40 - ext)
+        gdim = (40, 40, 40)
+    elif case == "negative":
+        n = 30
+        ext = rng.integers(4, 12, size=(n, 3))
+        off = rng.integers(-37, 20, size=(n, 3))
+        gdim = (33, 29, 41)
+    elif case == "single":
+        n = 1
+        ext = np.array([[7, 5, 9]])
+        off = np.array([[3, -2, 1]])
+        gdim = (16, 16, 16)
+    elif case == "nested":
+        n = 25
+        ext = rng.integers(2, 10, size=(n, 3))
+        off = rng.integers(1, 30, size=(n, 3))
+        ext[0], off[0] = (40, 40, 40), (0, 0, 0)
+        ext[5], off[5] = (20, 20, 20), (10, 10, 10)
+        gdim = (40, 40, 40)
+    else:
+        n = 24
+        ext = np.where(rng.random((n, 3)) < 0.3, rng.integers(50, 200, size=(n, 3)),
+                       rng.integers(1, 4, size=(n, 3)))
+        off = rng.integers(0, 60, size=(n, 3))
+        gdim = (128, 128, 128)
+    sizes = rng.integers(1, 9, size=(n, 3))
+    blocks, pool = sparse_table(off, ext, sizes, fmt, comps, seed=n + fmt)
+    return blocks, pool, gdim
+
+
+def sparse_edge_coords(blocks, gdim, n, seed, spread=(0.0, 1.0)):
+    """Coordinates on block faces, edges and corners, a few float ulps and
+    the block tree's 1e-6 widening off them, inside blocks, and (n / 4 more)
+    uniform in `spread`.  (n + n // 4, 3) float32."""
+    rng = np.random.default_rng(seed)
+    g = np.array(gdim, np.float64)
+    b = blocks[rng.integers(0, blocks.size, size=n)]
+    corner = b["offset"] + b["extent"] * rng.integers(0, 2, size=(n, 3))
+    inner = b["offset"] + rng.random((n, 3)) * b["extent"]
+    pos = np.where(rng.integers(0, 2, size=(n, 3)).astype(bool), corner, inner)
+    nudge = np.array([0, 0, 1e-6, -1e-6, 2e-6, -2e-6, 1e-7])[rng.integers(0, 7, size=(n, 3))]
+    u = ((pos + nudge * b["extent"]) / g).astype(np.float32)
+    ulps = rng.integers(-2, 3, size=(n, 3))
+    for k in (-2, -1, 1, 2):
+        to = np.float32(np.inf if k > 0 else -np.inf)
+        step = np.nextafter(u, to).astype(np.float32)
+        if abs(k) == 2:
+            step = np.nextafter(step, to).astype(np.float32)
+        u = np.where(ulps == k, step, u)
+    anywhere = rng.uniform(*spread, size=(n // 4, 3)).astype(np.float32)
+    return np.concatenate([u, anywhere]).astype(np.float32)

@@ -87,3 +87,30 @@ def test_large_texture_and_errors():
     blocks["data_offset"][0] = len(pool)  # voxels outside the pool
     with pytest.raises(sb.SurfaceError):
         t.set_sparse(blocks, pool, 1, 1, gdim)
+
+
+
+def _check_sparse(blocks, pool, fmt, comps, gdim, uvw):
+    t = Texture3D()
+    t.set_sparse(blocks, pool, fmt, comps, gdim)
+    got = t.Fetch(torch.from_numpy(uvw).cuda()).cpu().numpy()
+    want = O.sparse_fetch(blocks, pool, fmt, comps, gdim, uvw)
+    assert same(got, want)
+    return want
+
+
+def test_sparse_pages_faces_and_widening():
+    """A page checkerboard: neighbours meet at edges, so points on an edge
+    or within the widening of one belong to the first page in tree order."""
+    blocks, pool, gdim = S.sparse_pages(ndiv=4, page=8, seed=5)
+    want = _check_sparse(blocks, pool, 0, 1, gdim, S.sparse_edge_coords(blocks, gdim, 60000, 1))
+    assert (want[:, 3] != 0).mean() > 0.3
+
+
+@pytest.mark.parametrize("case", S.LOCATE_CASES)
+def test_sparse_locate_edge_cases(case):
+    for fmt, comps in ((0, 1), (1, 3)):
+        blocks, pool, gdim = S.sparse_locate_case(case, fmt, comps)
+        uvw = S.sparse_edge_coords(blocks, gdim, 30000, fmt, spread=(-1.5, 1.5))
+        want = _check_sparse(blocks, pool, fmt, comps, gdim, uvw)
+        assert (want[:, 3] != 0).mean() > 0.2

@@ -55,3 +55,21 @@ def test_sparse_fetch_matches_reference(fmt, comps, overlap):
     want = O.sparse_fetch(blocks, pool, fmt, comps, gdim, uvw, use_ref=True)
     assert np.array_equal(bits(got), bits(want))
     assert (want[:, 3] != 0).mean() > 0.05  # a share of the samples lands in blocks
+
+
+@needs_ref
+@pytest.mark.parametrize("case", ("pages",) + S.LOCATE_CASES)
+def test_sparse_locate_edge_cases_match_reference(case):
+    """Points on block faces, edges and corners, ulps and the tree's 1e-6
+    widening off them, for layouts that stress BVHTree::Locate."""
+    for fmt, comps in ((0, 1), (1, 3)):
+        if case == "pages":
+            blocks, pool, gdim = S.sparse_pages(ndiv=4, page=8, seed=5)
+            fmt, comps = 0, 1
+        else:
+            blocks, pool, gdim = S.sparse_locate_case(case, fmt, comps)
+        uvw = S.sparse_edge_coords(blocks, gdim, 8000, fmt, spread=(-1.5, 1.5))
+        got = O.sparse_fetch(blocks, pool, fmt, comps, gdim, uvw)
+        want = O.sparse_fetch(blocks, pool, fmt, comps, gdim, uvw, use_ref=True)
+        assert np.array_equal(bits(got), bits(want))
+        assert (want[:, 3] != 0).mean() > 0.2
