@@ -150,33 +150,34 @@ struct SparseLeaf {
   double bmin[3], bmax[3];
   int32_t block, pad;
 };
-// One lattice cell: `owner` (the block of the first leaf holding the whole
-// cell, -1 if none), list[off .. off + n) the leaves to test in order before
-// the owner (with no owner: every leaf reaching into the cell), and the
-// cell's open core clear of those leaves, where the answer is `owner`.
-// walk != 0: walk the tree.
-struct alignas(16) SparseCell {
-  float core_lo[3];
-  int32_t owner;
-  float core_hi[3];
-  uint32_t off;
-  uint32_t n, walk, pad[2];
-};
-static_assert(sizeof(SparseCell) == 48, "three 16-byte loads");
 // A block as the sample reads it: size[0] / extent[0] (the reference scales
-// all three axes by x's ratio), offset, size and the texels' byte offset.
+// all three axes by x's ratio), the texels' byte offset, offset and size.
+// fast != 0: size[0] == extent[0], offsets >= 0 and offset + extent <= 2^22,
+// where trunc((p - offset) * 1.0) in double is floor(p) - offset for every p
+// in the block (a float p below an integer k >= 1 is at least 2^-24 k away
+// from it, more than the double rounding of p - offset < 2^22 can bridge).
 struct alignas(16) BlockRec {
   double sx;
   uint64_t data_off;
   int32_t off[3], size0;
-  int32_t size1, size2, pad[2];
+  int32_t size1, size2, fast, pad;
 };
 static_assert(sizeof(BlockRec) == 48, "three 16-byte loads");
-#ifndef SRT_FETCH_ILP
-#define SRT_FETCH_ILP 1
-#endif
-constexpr int kFetchILP = SRT_FETCH_ILP;  // fetches in flight per thread
+// One lattice cell: `owner` (the block of the first leaf holding the whole
+// cell, -1 if none) with its sample record, the leaves to test in order
+// before the owner (with no owner: every leaf reaching into the cell), and
+// the cell's open core clear of those leaves, where the answer is `owner`.
+// list = first << 5 | count; count kWalk: walk the tree.
+struct alignas(16) SparseCell {
+  float core_lo[3];
+  int32_t owner;
+  float core_hi[3];
+  uint32_t list;
+  BlockRec rec;
+};
+static_assert(sizeof(SparseCell) == 80, "five 16-byte loads");
 constexpr uint32_t kCellList = 16;
+constexpr uint32_t kWalk = 31;
 
 struct SparseTex {
   const TopNode *tree;
@@ -230,83 +231,60 @@ __device__ int locate(const TopNode *__restrict__ tree, const double p[3], uint3
   return -1;
 }
 
-struct CellView {
-  float lo[3], hi[3];
-  int owner;
-  uint32_t off, n, walk;
-};
+__device__ __forceinline__ BlockRec unpack_rec(int4 a, int4 b, int4 d) {
+  BlockRec r;
+  r.sx = __hiloint2double(a.y, a.x);
+  r.data_off = ((uint64_t)(uint32_t)a.w << 32) | (uint32_t)a.z;
+  r.off[0] = b.x;
+  r.off[1] = b.y;
+  r.off[2] = b.z;
+  r.size0 = b.w;
+  r.size1 = d.x;
+  r.size2 = d.y;
+  r.fast = d.z;
+  return r;
+}
 
-__device__ __forceinline__ CellView load_cell(const SparseCell *c) {
-  const int4 *q = reinterpret_cast<const int4 *>(c);
-  const int4 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
-  CellView v;
-  v.lo[0] = __int_as_float(a.x);
-  v.lo[1] = __int_as_float(a.y);
-  v.lo[2] = __int_as_float(a.z);
-  v.owner = a.w;
-  v.hi[0] = __int_as_float(b.x);
-  v.hi[1] = __int_as_float(b.y);
-  v.hi[2] = __int_as_float(b.z);
-  v.off = (uint32_t)b.w;
-  v.n = (uint32_t)d.x;
-  v.walk = (uint32_t)d.y;
-  return v;
+__device__ __forceinline__ BlockRec load_rec(const BlockRec *r) {
+  const int4 *q = reinterpret_cast<const int4 *>(r);
+  return unpack_rec(__ldg(q), __ldg(q + 1), __ldg(q + 2));
 }
 
 // The cell of p, clamped to the grid: floor((p - org) / 2^shift) is
 // (floor(p) - org) >> shift for an integer origin (NaN maps to cell 0 and
 // then fails the union test).
-__device__ __forceinline__ size_t cell_of(const SparseTex &t, const float pf[3]) {
+__device__ __forceinline__ size_t cell_of(const SparseTex &t, const int fl[3]) {
   int c[3];
 #pragma unroll
   for (int k = 0; k < 3; k++) {
-    const long long d = ((long long)__float2int_rd(pf[k]) - t.org[k]) >> t.shift[k];
+    const long long d = ((long long)fl[k] - t.org[k]) >> t.shift[k];
     c[k] = (int)(d < 0 ? 0 : (d >= t.g[k] ? t.g[k] - 1 : d));
   }
   return ((size_t)c[2] * t.g[1] + c[1]) * t.g[0] + c[0];
 }
 
-// Locate from p's cell; the same block as locate() for every point.
-__device__ __forceinline__ int locate_cell(const SparseTex &t, const CellView &cell,
-                                           const float pf[3], const double p[3],
-                                           uint32_t *err) {
-  // outside the union of the leaf boxes: in no leaf (NaN included).  p is a
-  // float, so p >= lo exactly when p >= lo rounded up to a float.
-  if (!(pf[0] >= t.ulo[0] && pf[0] <= t.uhi[0] && pf[1] >= t.ulo[1] && pf[1] <= t.uhi[1] &&
-        pf[2] >= t.ulo[2] && pf[2] <= t.uhi[2]))
-    return -1;
-  if (cell.walk) return locate(t.tree, p, t.max_iter, err);
-  if (pf[0] > cell.lo[0] && pf[0] < cell.hi[0] && pf[1] > cell.lo[1] && pf[1] < cell.hi[1] &&
-      pf[2] > cell.lo[2] && pf[2] < cell.hi[2])
-    return cell.owner;
-  for (uint32_t j = 0; j < cell.n; j++) {
-    const SparseLeaf &L = t.leaves[__ldg(&t.list[cell.off + j])];
-    if (p[0] >= L.bmin[0] && p[0] <= L.bmax[0] && p[1] >= L.bmin[1] && p[1] <= L.bmax[1] &&
-        p[2] >= L.bmin[2] && p[2] <= L.bmax[2])
-      return L.block;
-  }
-  return cell.owner;
-}
-
-// SparseVolumeAccel::Sample of block `id` (>= 0) at p: the nearest texel.
-// The reference stores each component as a double and the caller reads it as
-// a float, so bytes give (float)b / 255.0f (lut), floats themselves and
+// SparseVolumeAccel::Sample of block record r at p: the nearest texel.  The
+// reference stores each component as a double and the caller reads it as a
+// float, so bytes give (float)b / 255.0f (lut), floats themselves and
 // doubles (float)d.
-__device__ __forceinline__ float4 sample_block(const SparseTex &t, int id, const double p[3],
-                                               const float *lut) {
-  const int4 *q = reinterpret_cast<const int4 *>(t.blocks + id);
-  const int4 a = __ldg(q), b = __ldg(q + 1), d = __ldg(q + 2);
-  const double sx = __hiloint2double(a.y, a.x);
-  const uint64_t data_off = ((uint64_t)(uint32_t)a.w << 32) | (uint32_t)a.z;
-  const int size[3] = {b.w, d.x, d.y};
-  const double x = (p[0] - (double)b.x) * sx;
-  const double y = (p[1] - (double)b.y) * sx;  // x's ratio on every axis
-  const double z = (p[2] - (double)b.z) * sx;
-  const int ix = max(min(size[0] - 1, d2i_x86(x)), 0);
-  const int iy = max(min(size[1] - 1, d2i_x86(y)), 0);
-  const int iz = max(min(size[2] - 1, d2i_x86(z)), 0);
-  const size_t idx = ((size_t)iz * size[1] + (size_t)iy) * (size_t)size[0] + (size_t)ix;
-  const unsigned char *base = t.pool + data_off;
+__device__ __forceinline__ float4 sample_rec(const SparseTex &t, const BlockRec &r,
+                                             const float pf[3], const int fl[3],
+                                             const float *lut) {
+  const int size[3] = {r.size0, r.size1, r.size2};
+  int ix[3];
+  if (r.fast) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) ix[k] = max(min(size[k] - 1, fl[k] - r.off[k]), 0);
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+      const double x = ((double)pf[k] - (double)r.off[k]) * r.sx;  // x's ratio on every axis
+      ix[k] = max(min(size[k] - 1, d2i_x86(x)), 0);
+    }
+  }
+  const size_t idx =
+      ((size_t)ix[2] * size[1] + (size_t)ix[1]) * (size_t)size[0] + (size_t)ix[0];
+  const unsigned char *base = t.pool + r.data_off;
   const int nc = t.comps >= 4 ? 4 : t.comps;
   float v[4] = {0.f, 0.f, 0.f, 1.f};
   for (int c = 0; c < nc; c++) {
@@ -321,49 +299,76 @@ __device__ __forceinline__ float4 sample_block(const SparseTex &t, int id, const
   return make_float4(v[0], v[1], v[2], v[3]);
 }
 
-// kFetchILP fetches per thread per round, block-strided so that every load
-// and store stays coalesced; the stages (coordinates, cells, locate, texels)
-// run for all of them before the next, keeping their loads in flight together.
+// One fetch through the cell grid; the block is the one locate() finds for
+// every point.  The cell's first 32 bytes decide; its owner's record (the
+// last 48) is read only when the point is in the owner.
+__device__ __forceinline__ float4 fetch_cells(const SparseTex &t, const float pf[3],
+                                              const float *lut, uint32_t *err) {
+  int fl[3];
+#pragma unroll
+  for (int k = 0; k < 3; k++) fl[k] = __float2int_rd(pf[k]);
+  const int4 *q = reinterpret_cast<const int4 *>(t.cells + cell_of(t, fl));
+  const int4 c0 = __ldg(q), c1 = __ldg(q + 1);
+  // outside the union of the leaf boxes: in no leaf (NaN included).  p is a
+  // float, so p >= lo exactly when p >= lo rounded up to a float.
+  int id = -1;
+  bool own = false;
+  if (pf[0] >= t.ulo[0] && pf[0] <= t.uhi[0] && pf[1] >= t.ulo[1] && pf[1] <= t.uhi[1] &&
+      pf[2] >= t.ulo[2] && pf[2] <= t.uhi[2]) {
+    id = c0.w;
+    const bool core = pf[0] > __int_as_float(c0.x) && pf[0] < __int_as_float(c1.x) &&
+                      pf[1] > __int_as_float(c0.y) && pf[1] < __int_as_float(c1.y) &&
+                      pf[2] > __int_as_float(c0.z) && pf[2] < __int_as_float(c1.z);
+    if (!core) {
+      const uint32_t first = (uint32_t)c1.w >> 5, n = (uint32_t)c1.w & 31u;
+      const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
+      if (n == kWalk) {
+        id = locate(t.tree, p, t.max_iter, err);
+      } else {
+        for (uint32_t j = 0; j < n; j++) {
+          const SparseLeaf &L = t.leaves[__ldg(&t.list[first + j])];
+          if (p[0] >= L.bmin[0] && p[0] <= L.bmax[0] && p[1] >= L.bmin[1] &&
+              p[1] <= L.bmax[1] && p[2] >= L.bmin[2] && p[2] <= L.bmax[2]) {
+            id = L.block;
+            break;
+          }
+        }
+      }
+    }
+    own = id >= 0 && id == c0.w;  // a walking cell has no owner
+  }
+  if (id < 0) return make_float4(0.f, 0.f, 0.f, 0.f);
+  const BlockRec r = own ? unpack_rec(__ldg(q + 2), __ldg(q + 3), __ldg(q + 4))
+                         : load_rec(t.blocks + id);
+  return sample_rec(t, r, pf, fl, lut);
+}
+
+// One fetch per thread per round, grid-strided (coalesced coordinates and
+// RGBA).
 __global__ void __launch_bounds__(256)
 sparse_fetch_kernel(SparseTex t, const float *__restrict__ uvw, size_t n,
                     float4 *__restrict__ rgba, uint32_t *__restrict__ err) {
   __shared__ float lut[256];  // byte texel b -> (float)b / 255.0f
   for (int k = threadIdx.x; k < 256; k += blockDim.x) lut[k] = (float)k / 255.0f;
   __syncthreads();
-  const size_t step = (size_t)blockDim.x * kFetchILP;
-  for (size_t base = (size_t)blockIdx.x * step + threadIdx.x; base < n;
-       base += (size_t)gridDim.x * step) {
-    float pf[kFetchILP][3];
-    double p[kFetchILP][3];
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float pf[3];
 #pragma unroll
-    for (int j = 0; j < kFetchILP; j++) {
-      const size_t i = base + (size_t)j * blockDim.x;
-#pragma unroll
-      for (int k = 0; k < 3; k++) {
-        pf[j][k] = (i < n ? __ldg(&uvw[3 * i + k]) : 0.0f) * (float)t.gdim[k];
-        p[j][k] = (double)pf[j][k];
-      }
-    }
-    int id[kFetchILP];
+    for (int k = 0; k < 3; k++) pf[k] = __ldg(&uvw[3 * i + k]) * (float)t.gdim[k];
+    float4 out;
     if (t.cells) {
-      CellView cv[kFetchILP];
-#pragma unroll
-      for (int j = 0; j < kFetchILP; j++) cv[j] = load_cell(t.cells + cell_of(t, pf[j]));
-#pragma unroll
-      for (int j = 0; j < kFetchILP; j++) id[j] = locate_cell(t, cv[j], pf[j], p[j], err);
+      out = fetch_cells(t, pf, lut, err);
     } else {
+      const double p[3] = {(double)pf[0], (double)pf[1], (double)pf[2]};
+      int fl[3];
 #pragma unroll
-      for (int j = 0; j < kFetchILP; j++) id[j] = locate(t.tree, p[j], t.max_iter, err);
+      for (int k = 0; k < 3; k++) fl[k] = __float2int_rd(pf[k]);
+      const int id = locate(t.tree, p, t.max_iter, err);
+      out = id >= 0 ? sample_rec(t, load_rec(t.blocks + id), pf, fl, lut)
+                    : make_float4(0.f, 0.f, 0.f, 0.f);
     }
-    float4 out[kFetchILP];
-#pragma unroll
-    for (int j = 0; j < kFetchILP; j++)
-      out[j] = id[j] >= 0 ? sample_block(t, id[j], p[j], lut) : make_float4(0.f, 0.f, 0.f, 0.f);
-#pragma unroll
-    for (int j = 0; j < kFetchILP; j++) {
-      const size_t i = base + (size_t)j * blockDim.x;
-      if (i < n) rgba[i] = out[j];
-    }
+    rgba[i] = out;
   }
 }
 
@@ -404,7 +409,7 @@ float round_down_f(double x) {
 }
 
 void build_cell_grid(const std::vector<TopNode> &tree, const srt_volume_block *blocks,
-                     size_t nblocks, CellGrid &G) {
+                     const std::vector<BlockRec> &recs, size_t nblocks, CellGrid &G) {
   G = CellGrid();
   // leaves in depth-first order, left child first (Locate's visiting order)
   std::vector<int32_t> stk{0};
@@ -519,7 +524,10 @@ void build_cell_grid(const std::vector<TopNode> &tree, const srt_volume_block *b
         SparseCell &C = G.cells[ci];
         C = SparseCell{};
         C.owner = -1;
-        C.off = (uint32_t)G.list.size();
+        for (int k = 0; k < 3; k++) {  // an empty core until one is cut
+          C.core_lo[k] = INFINITY;
+          C.core_hi[k] = -INFINITY;
+        }
         uint32_t own = cnt[ci];
         for (uint32_t j = 0; j < cnt[ci]; j++) {
           const SparseLeaf &L = G.leaves[cand[ci * cap + j]];
@@ -531,17 +539,16 @@ void build_cell_grid(const std::vector<TopNode> &tree, const srt_volume_block *b
         }
         const bool has_owner = own < cnt[ci];
         if ((has_owner ? own : cnt[ci]) > kCellList || (!has_owner && more[ci])) {
-          C.walk = 1;
+          C.list = kWalk;
           continue;
         }
         const uint32_t n = has_owner ? own : cnt[ci];
+        C.list = (uint32_t)G.list.size() << 5 | n;
         for (uint32_t j = 0; j < n; j++) G.list.push_back(cand[ci * cap + j]);
-        C.n = n;
-        for (int k = 0; k < 3; k++) {
-          C.core_lo[k] = INFINITY;
-          C.core_hi[k] = -INFINITY;
+        if (has_owner) {
+          C.owner = G.leaves[cand[ci * cap + own]].block;
+          C.rec = recs[C.owner];
         }
-        if (has_owner) C.owner = G.leaves[cand[ci * cap + own]].block;
         // the open core: the cell cut clear of each listed leaf (those before
         // the owner; with no owner, all that reach in), on the side that keeps
         // the most of it.  A point in the core is in the owner (or in none).
@@ -686,22 +693,28 @@ SRT_API srt_status srt_texture3d_set_sparse(srt_texture3d *t, int format, int co
   }
   std::vector<TopNode> tree;
   build_top_tree(lo.data(), hi.data(), nblocks, tree);
-  CellGrid G;
-  build_cell_grid(tree, blocks, nblocks, G);
-  cudaSetDevice(t->ctx->device);
-  srt_status s = upload(t->ctx, t->data, pool, pool_bytes);
-  if (s == SRT_OK) s = upload(t->ctx, t->tree, tree.data(), tree.size() * sizeof(TopNode));
   std::vector<BlockRec> recs(nblocks);
   for (size_t i = 0; i < nblocks; i++) {
     BlockRec &r = recs[i];
     r = BlockRec{};
     r.sx = (double)blocks[i].size[0] / (double)blocks[i].extent[0];
     r.data_off = blocks[i].data_offset;
-    for (int k = 0; k < 3; k++) r.off[k] = blocks[i].offset[k];
+    r.fast = blocks[i].size[0] == blocks[i].extent[0];
+    for (int k = 0; k < 3; k++) {
+      r.off[k] = blocks[i].offset[k];
+      if (blocks[i].offset[k] < 0 ||
+          (int64_t)blocks[i].offset[k] + blocks[i].extent[k] > (int64_t)1 << 22)
+        r.fast = 0;
+    }
     r.size0 = blocks[i].size[0];
     r.size1 = blocks[i].size[1];
     r.size2 = blocks[i].size[2];
   }
+  CellGrid G;
+  build_cell_grid(tree, blocks, recs, nblocks, G);
+  cudaSetDevice(t->ctx->device);
+  srt_status s = upload(t->ctx, t->data, pool, pool_bytes);
+  if (s == SRT_OK) s = upload(t->ctx, t->tree, tree.data(), tree.size() * sizeof(TopNode));
   if (s == SRT_OK) s = upload(t->ctx, t->blocks, recs.data(), nblocks * sizeof(BlockRec));
   t->cells.release();
   if (s == SRT_OK && G.built) {

@@ -594,7 +594,7 @@ def sparse_table(offsets, extents, sizes, fmt, comps, seed):
     return b, b"".join(chunks)
 
 
-LOCATE_CASES = ("crowded", "negative", "single", "nested", "slabs")
+LOCATE_CASES = ("crowded", "negative", "single", "nested", "slabs", "unit")
 
 
 def sparse_locate_case(case, fmt, comps):
@@ -603,7 +603,7 @@ def sparse_locate_case(case, fmt, comps):
     a single block, nested blocks (one around all), long thin slabs.
     Returns (blocks, pool, global dims)."""
     rng = np.random.default_rng({"crowded": 1, "negative": 2, "single": 3, "nested": 4,
-                                 "slabs": 5}[case])
+                                 "slabs": 5, "unit": 6}[case])
     if case == "crowded":
         n = 80
         ext = rng.integers(3, 17, size=(n, 3))
@@ -626,13 +626,22 @@ def sparse_locate_case(case, fmt, comps):
         ext[0], off[0] = (40, 40, 40), (0, 0, 0)
         ext[5], off[5] = (20, 20, 20), (10, 10, 10)
         gdim = (40, 40, 40)
-    else:
+    elif case == "slabs":
         n = 24
         ext = np.where(rng.random((n, 3)) < 0.3, rng.integers(50, 200, size=(n, 3)),
                        rng.integers(1, 4, size=(n, 3)))
         off = rng.integers(0, 60, size=(n, 3))
         gdim = (128, 128, 128)
+    else:  # one voxel per unit (size == extent) around the origin, both signs
+        n = 27
+        ext = rng.integers(2, 9, size=(n, 3))
+        off = rng.integers(-12, 8, size=(n, 3))
+        off[0], ext[0] = (-4, -4, -4), (8, 8, 8)
+        gdim = (24, 24, 24)
     sizes = rng.integers(1, 9, size=(n, 3))
+    if case == "unit":
+        sizes = ext.copy()
+        sizes[1::3] = rng.integers(1, 9, size=sizes[1::3].shape)
     blocks, pool = sparse_table(off, ext, sizes, fmt, comps, seed=n + fmt)
     return blocks, pool, gdim
 
@@ -657,4 +666,8 @@ def sparse_edge_coords(blocks, gdim, n, seed, spread=(0.0, 1.0)):
             step = np.nextafter(step, to).astype(np.float32)
         u = np.where(ulps == k, step, u)
     anywhere = rng.uniform(*spread, size=(n // 4, 3)).astype(np.float32)
-    return np.concatenate([u, anywhere]).astype(np.float32)
+    # tiny coordinates of both signs around the origin
+    tiny = np.array([0.0, -0.0, 1e-30, -1e-30, 1e-12, -1e-12, 1e-7, -1e-7, 2e-38, -2e-38],
+                    np.float32)
+    special = tiny[rng.integers(0, tiny.size, size=(max(n // 16, 16), 3))]
+    return np.concatenate([u, anywhere, special]).astype(np.float32)
