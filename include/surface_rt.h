@@ -546,6 +546,36 @@ SRT_API srt_status srt_batch_config(srt_batch *b, int32_t *block,
                                     int32_t *graph_captured,
                                     uint64_t *kernels_per_call);
 
+/* ---------------------------------------------------------------- lines
+ * LineAccel (render/render_accel_line.{h,cc}): capped cylinders between the
+ * end points of line segments (Lines, render/render_prim_line.h).
+ * srt_line_build replaces LineAccel::Build (render_accel_line.cc:298): the
+ * same spatial-median tree and line order (positions: nverts xyz floats;
+ * radius: per vertex or NULL for constant_radius; segments: 2 vertex indices
+ * per line; min_leaf, max_depth and cap as LineBuildOptions, 0 for its
+ * defaults 4 and 512).  srt_line_trace replaces LineAccel::Traverse (:704):
+ * closest hit per ray (t, u, v, line index; u = distance from the axis on a
+ * cap, v = 0 / 1 on a cap or the position along the axis), normals (3 floats
+ * per ray, BuildIntersection's, may be NULL).  Inputs may be host or device
+ * memory.  srt_line_bbox replaces LineAccel::BoundingBox (:776),
+ * srt_line_dump LineAccel::Dump (:343, the same file format); srt_line_export
+ * copies the tree in the Dump record layout (40 bytes per node) and the line
+ * order. */
+typedef struct srt_line_accel srt_line_accel;
+SRT_API srt_status srt_line_create(srt_ctx *ctx, srt_line_accel **out);
+SRT_API srt_status srt_line_destroy(srt_line_accel *accel);
+SRT_API srt_status srt_line_build(srt_line_accel *accel, const float *positions,
+                                  size_t nverts, const float *radius, float constant_radius,
+                                  const uint32_t *segments, size_t nlines, int32_t min_leaf,
+                                  int32_t max_depth, int32_t cap);
+SRT_API srt_status srt_line_trace(srt_line_accel *accel, const srt_ray *rays, size_t n,
+                                  srt_hit *hits, float *normals);
+SRT_API srt_status srt_line_bbox(srt_line_accel *accel, double bmin[3], double bmax[3]);
+SRT_API srt_status srt_line_info(srt_line_accel *accel, uint64_t *nlines, uint64_t *nnodes,
+                                 int32_t *depth);
+SRT_API srt_status srt_line_export(srt_line_accel *accel, void *nodes, uint32_t *indices);
+SRT_API srt_status srt_line_dump(srt_line_accel *accel, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

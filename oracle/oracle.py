@@ -114,6 +114,15 @@ def lib():
         L.so_scene_candidates.restype = _SZ
         L.so_scene_candidates.argtypes = [_P, _P, _P, _P, _P, _SZ]
         L.so_scene_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, _P, C.c_int, C.c_int]
+        L.so_line_build.restype = _P
+        L.so_line_build.argtypes = [_P, _P, C.c_float, _P, _SZ, C.c_int, C.c_int, C.c_int]
+        L.so_line_free.argtypes = [_P]
+        L.so_line_num_nodes.restype = _SZ
+        L.so_line_num_nodes.argtypes = [_P]
+        L.so_line_depth.restype = C.c_int
+        L.so_line_depth.argtypes = [_P]
+        L.so_line_export.argtypes = [_P, _P, _P]
+        L.so_line_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int]
         _ORACLE = L
     return _ORACLE
 
@@ -172,6 +181,12 @@ def ref():
         L.ref_bvh_nodes.argtypes = [_P, _P, _P, _SZ]
         L.ref_bvh_trace.restype = _SZ
         L.ref_bvh_trace.argtypes = [_P, _P, _P, _P, _P, _SZ]
+        L.ref_line_build.restype = _P
+        L.ref_line_build.argtypes = [_P, _P, C.c_float, _P, _SZ, C.c_int, C.c_int, C.c_int]
+        L.ref_line_free.argtypes = [_P]
+        L.ref_line_dump.argtypes = [_P, C.c_char_p]
+        L.ref_line_bbox.argtypes = [_P, _P, _P]
+        L.ref_line_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
         _REF = L
     return _REF
 
@@ -821,3 +836,113 @@ def sparse_fetch(blocks, pool, fmt, comps, gdim, uvw, use_ref=False):
         finally:
             lib().so_scene_free(tree)
     return out
+
+
+# ---------------------------------------------------------------- lines
+LINE_NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("flag", "<i4"),
+                            ("axis", "<i4"), ("data", "<u4", 2)])  # LineNode, 40 bytes
+
+
+def parse_line_dump(raw):
+    """LineAccel::Dump(): (nodes LINE_NODE_DTYPE, indices uint32)."""
+    nn = int(np.frombuffer(raw[:8], np.uint64)[0])
+    nodes = np.frombuffer(raw[8:8 + 40 * nn], LINE_NODE_DTYPE).copy()
+    off = 8 + 40 * nn
+    ni = int(np.frombuffer(raw[off:off + 8], np.uint64)[0])
+    idx = np.frombuffer(raw[off + 8:off + 8 + 4 * ni], np.uint32).copy()
+    return nodes, idx
+
+
+def line_nodes_masked(nodes):
+    """Node records with the fields a leaf leaves unset (its axis) zeroed."""
+    n = nodes.copy()
+    n["axis"][n["flag"] == 1] = 0
+    return n
+
+
+class _LinesBase:
+    def _inputs(self, pos, segments, radius, const_radius):
+        self.pos = np.ascontiguousarray(pos, np.float32).reshape(-1)
+        self.seg = np.ascontiguousarray(segments, np.uint32).reshape(-1)
+        self.radius = None if radius is None else np.ascontiguousarray(radius, np.float32)
+        self.const_radius = float(const_radius)
+        self.n = self.seg.size // 2
+
+
+class OracleLines(_LinesBase):
+    """The restatement of LineAccel: Build, Traverse (hits and normals)."""
+
+    def __init__(self, pos, segments, radius=None, const_radius=0.0, min_leaf=4,
+                 max_depth=512, cap=True):
+        self._inputs(pos, segments, radius, const_radius)
+        self.h = lib().so_line_build(_ptr(self.pos), _ptr(self.radius),
+                                     C.c_float(self.const_radius), _ptr(self.seg), self.n,
+                                     min_leaf, max_depth, int(cap))
+
+    def export(self):
+        nn = lib().so_line_num_nodes(self.h)
+        nodes = np.zeros(nn, LINE_NODE_DTYPE)
+        idx = np.zeros(self.n, np.uint32)
+        lib().so_line_export(self.h, _ptr(nodes), _ptr(idx))
+        return nodes, idx
+
+    def depth(self):
+        return lib().so_line_depth(self.h)
+
+    def trace(self, rays, nthreads=0):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        nrm = np.zeros((rays.size, 3), np.float32)
+        lib().so_line_trace(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(nrm), nthreads)
+        return hits, nrm
+
+    def __del__(self):
+        try:
+            lib().so_line_free(self.h)
+        except Exception:  # noqa: BLE001
+            pass
+
+
+class RefLines(_LinesBase):
+    """The reference's own LineAccel (Build, Traverse, Dump, BoundingBox)."""
+
+    def __init__(self, pos, segments, radius=None, const_radius=0.0, min_leaf=4,
+                 max_depth=512, cap=True):
+        L = ref()
+        if L is None:
+            raise RuntimeError("reference harness not built")
+        self.L = L
+        self._inputs(pos, segments, radius, const_radius)
+        self.h = L.ref_line_build(_ptr(self.pos), _ptr(self.radius),
+                                  C.c_float(self.const_radius), _ptr(self.seg), self.n,
+                                  min_leaf, max_depth, int(cap))
+
+    def dump_bytes(self):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "lines.bin")
+            self.L.ref_line_dump(self.h, path.encode())
+            with open(path, "rb") as fp:
+                return fp.read()
+
+    def dump(self):
+        return parse_line_dump(self.dump_bytes())
+
+    def bbox(self):
+        mn = np.zeros(3)
+        mx = np.zeros(3)
+        self.L.ref_line_bbox(self.h, _ptr(mn), _ptr(mx))
+        return mn, mx
+
+    def trace(self, rays, nthreads=0, chunk=64):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        nrm = np.zeros((rays.size, 3), np.float32)
+        self.L.ref_line_trace(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(nrm),
+                              nthreads, chunk)
+        return hits, nrm
+
+    def __del__(self):
+        try:
+            self.L.ref_line_free(self.h)
+        except Exception:  # noqa: BLE001
+            pass

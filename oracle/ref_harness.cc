@@ -26,6 +26,7 @@
 #include <limits>
 #include <vector>
 
+#include "render_accel_line.h"
 #include "render_accel_particle.h"
 #include "render_accel_tetra.h"
 #include "render_accel_triangle.h"
@@ -502,5 +503,65 @@ REF_API void ref_sparse_fetch(const int32_t *blocks, size_t nblocks, const unsig
     for (int k = 0; k < 3; k++) position[k] = uvw[3 * i + k] * sv.globalDim[k];
     acc.Sample(value, position);
     for (int k = 0; k < 4; k++) rgba[4 * i + k] = value[k];
+  }
+}
+
+// ---------------------------------------------------------------- lines
+// LineAccel (render/render_accel_line.cc): spatial-median BVH over capped
+// cylinders (Build), closest hit (Traverse), its Intersection's normal.
+struct LineHandle {
+  Lines lines;
+  LineAccel accel;
+};
+
+REF_API void *ref_line_build(const float *pos, const float *radius, float const_radius,
+                             const uint32_t *segments, size_t nlines, int min_leaf,
+                             int max_depth, int cap) {
+  LineHandle *h = new LineHandle();
+  memset(&h->lines, 0, sizeof(h->lines));
+  h->lines.numLines = nlines;
+  h->lines.positions = pos;
+  h->lines.dpositions = nullptr;
+  h->lines.isDoublePrecisionPos = false;
+  h->lines.radius = radius;
+  h->lines.constantRadius = const_radius;
+  h->lines.segments = const_cast<uint32_t *>(segments);
+  LineBuildOptions opt;
+  if (min_leaf > 0) opt.minLeafPrimitives = min_leaf;
+  if (max_depth > 0) opt.maxTreeDepth = max_depth;
+  opt.cap = cap != 0;
+  {
+    QuietStdout q;
+    h->accel.Build(&h->lines, opt);
+  }
+  return h;
+}
+
+REF_API void ref_line_free(void *p) { delete static_cast<LineHandle *>(p); }
+
+REF_API int ref_line_dump(void *p, const char *path) {
+  return static_cast<LineHandle *>(p)->accel.Dump(path) ? 0 : 1;
+}
+
+REF_API void ref_line_bbox(void *p, double bmin[3], double bmax[3]) {
+  static_cast<LineHandle *>(p)->accel.BoundingBox(bmin, bmax);
+}
+
+REF_API void ref_line_trace(void *p, const RayRec *rays, size_t n, HitRec *hits,
+                            float *normals, int nthreads, int chunk) {
+  const LineAccel &acc = static_cast<LineHandle *>(p)->accel;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (chunk <= 0) chunk = 64;
+#pragma omp parallel for schedule(dynamic, chunk) num_threads(nthreads)
+  for (long long i = 0; i < (long long)n; i++) {
+    Ray ray = make_ray(rays[i], nullptr);
+    Intersection isect;
+    bool hit = acc.Traverse(isect, ray);
+    hits[i].t = hit ? isect.t : std::numeric_limits<float>::max();
+    hits[i].u = hit ? isect.u : 0.0f;
+    hits[i].v = hit ? isect.v : 0.0f;
+    hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
+    if (normals)
+      for (int k = 0; k < 3; k++) normals[3 * i + k] = hit ? isect.normal[k] : 0.0f;
   }
 }

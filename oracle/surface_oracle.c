@@ -2567,3 +2567,419 @@ SO_API void so_sparse_fetch(const so_scene *tree, const so_block *b, const void 
     for (int k = 0; k < 4; k++) rgba[4 * i + k] = (float)v[k];
   }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Lines: LineAccel (render/render_accel_line.cc), capped cylinders between  */
+/* segment end points, a spatial-median BVH built top-down and a closest-hit */
+/* walk that tests each popped branch's own box.  Float throughout, except   */
+/* where the reference's unqualified sqrt/fabs resolve to the double C       */
+/* functions (the quadratic's first root is formed and divided in double).   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  float bmin[3], bmax[3];
+  int32_t flag, axis; /* flag 1: leaf (data = count, first); 0: branch (children) */
+  uint32_t data[2];
+} so_line_node; /* 40 bytes, the reference's LineNode and Dump() record */
+
+typedef struct {
+  const float *pos, *radius;
+  float constr;
+  const uint32_t *seg;
+  size_t n;
+  int min_leaf, max_depth, cap, depth_seen;
+  so_line_node *nodes;
+  size_t nnodes, ncap;
+  uint32_t *idx;
+} so_lines;
+
+static inline float line_r(const so_lines *L, uint32_t v) {
+  return L->radius ? L->radius[v] : L->constr;
+}
+
+/* GetBoundingBoxOfLine (:83-116): both end points +-r, then widened by
+ * FLT_EPSILON * 16 of each coordinate's own magnitude. */
+static void line_box(const so_lines *L, uint32_t i, float bmin[3], float bmax[3]) {
+  const uint32_t a = L->seg[2 * i], b = L->seg[2 * i + 1];
+  const float r0 = line_r(L, a), r1 = line_r(L, b);
+  float pt[4][3];
+  for (int k = 0; k < 3; k++) {
+    pt[0][k] = L->pos[3 * a + k] - r0;
+    pt[1][k] = L->pos[3 * a + k] + r0;
+    pt[2][k] = L->pos[3 * b + k] - r1;
+    pt[3][k] = L->pos[3 * b + k] + r1;
+  }
+  for (int k = 0; k < 3; k++) bmin[k] = bmax[k] = pt[0][k];
+  for (int q = 1; q < 4; q++)
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = (bmin[k] < pt[q][k]) ? bmin[k] : pt[q][k];
+      bmax[k] = (bmax[k] > pt[q][k]) ? bmax[k] : pt[q][k];
+    }
+  const float eps = FLT_EPSILON * 16.0f;
+  for (int k = 0; k < 3; k++) {
+    bmin[k] -= bmin[k] * eps;
+    bmax[k] += bmax[k] * eps;
+  }
+}
+
+/* ComputeBoundingBox (:142-163) over idx[l, r). */
+static void line_range_box(const so_lines *L, size_t l, size_t r, float bmin[3],
+                           float bmax[3]) {
+  line_box(L, L->idx[l], bmin, bmax);
+  for (size_t i = l; i < r; i++) {
+    float c0[3], c1[3];
+    line_box(L, L->idx[i], c0, c1);
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = (bmin[k] < c0[k]) ? bmin[k] : c0[k];
+      bmax[k] = (bmax[k] > c1[k]) ? bmax[k] : c1[k];
+    }
+  }
+}
+
+/* PartPred (:118-139): the segment's midpoint (p0 + p1) * 0.5 below pos. */
+static inline int line_left(const so_lines *L, uint32_t i, int axis, float pos) {
+  const uint32_t a = L->seg[2 * i], b = L->seg[2 * i + 1];
+  const float c = (L->pos[3 * a + axis] + L->pos[3 * b + axis]) * 0.5f;
+  return c < pos;
+}
+
+/* The two-ended partition of libstdc++'s std::partition for bidirectional
+ * iterators: skip left-side items from the front and right-side items from
+ * the back, swap the two that stop the scans, repeat. */
+static size_t line_partition(so_lines *L, size_t first, size_t last, int axis, float pos) {
+  for (;;) {
+    for (;;) {
+      if (first == last) return first;
+      if (line_left(L, L->idx[first], axis, pos))
+        first++;
+      else
+        break;
+    }
+    last--;
+    for (;;) {
+      if (first == last) return first;
+      if (!line_left(L, L->idx[last], axis, pos))
+        last--;
+      else
+        break;
+    }
+    const uint32_t t = L->idx[first];
+    L->idx[first] = L->idx[last];
+    L->idx[last] = t;
+    first++;
+  }
+}
+
+static size_t line_push(so_lines *L) {
+  if (L->nnodes == L->ncap) {
+    L->ncap = L->ncap ? 2 * L->ncap : 64;
+    L->nodes = (so_line_node *)realloc(L->nodes, L->ncap * sizeof(so_line_node));
+  }
+  memset(&L->nodes[L->nnodes], 0, sizeof(so_line_node));
+  return L->nnodes++;
+}
+
+/* LineAccel::BuildTree (:167-296): a leaf below min_leaf lines or at
+ * max_depth; else the spatial median of the longest axis first (the cut
+ * position formed in double, stored as float), then the next axes, and the
+ * object median when no axis splits. */
+static size_t line_build(so_lines *L, size_t l, size_t r, int depth) {
+  const size_t off = line_push(L);
+  if (L->depth_seen < depth) L->depth_seen = depth;
+  float bmin[3], bmax[3];
+  line_range_box(L, l, r, bmin, bmax);
+  const size_t n = r - l;
+  if (n < (size_t)L->min_leaf || depth >= L->max_depth) {
+    so_line_node *nd = &L->nodes[off];
+    memcpy(nd->bmin, bmin, sizeof(bmin));
+    memcpy(nd->bmax, bmax, sizeof(bmax));
+    nd->flag = 1;
+    nd->data[0] = (uint32_t)n;
+    nd->data[1] = (uint32_t)l;
+    return off;
+  }
+  float bsize[3];
+  for (int k = 0; k < 3; k++) bsize[k] = bmax[k] - bmin[k];
+  float maxsize = bsize[0];
+  int longest = 0;
+  if (maxsize < bsize[1]) {
+    maxsize = bsize[1];
+    longest = 1;
+  }
+  if (maxsize < bsize[2]) {
+    maxsize = bsize[2];
+    longest = 2;
+  }
+  size_t mid = 0;
+  int axis = 0;
+  for (int t = 0; t < 3; t++) {
+    axis = (longest + t) % 3;
+    const float pos = (float)((double)bmin[axis] + 0.5 * (double)bsize[axis]);
+    mid = line_partition(L, l, r, axis, pos);
+    if (mid == l || mid == r)
+      mid = l + (n >> 1);
+    else
+      break;
+  }
+  L->nodes[off].axis = axis;
+  const size_t left = line_build(L, l, mid, depth + 1);
+  const size_t right = line_build(L, mid, r, depth + 1);
+  so_line_node *nd = &L->nodes[off];
+  nd->data[0] = (uint32_t)left;
+  nd->data[1] = (uint32_t)right;
+  memcpy(nd->bmin, bmin, sizeof(bmin));
+  memcpy(nd->bmax, bmax, sizeof(bmax));
+  return off;
+}
+
+SO_API so_lines *so_line_build(const float *pos, const float *radius, float const_radius,
+                               const uint32_t *seg, size_t n, int min_leaf, int max_depth,
+                               int cap) {
+  so_lines *L = (so_lines *)calloc(1, sizeof(so_lines));
+  L->pos = pos;
+  L->radius = radius;
+  L->constr = const_radius;
+  L->seg = seg;
+  L->n = n;
+  L->min_leaf = min_leaf > 0 ? min_leaf : 4;
+  L->max_depth = max_depth > 0 ? max_depth : 512;
+  L->cap = cap;
+  L->idx = (uint32_t *)malloc((n ? n : 1) * sizeof(uint32_t));
+  for (size_t i = 0; i < n; i++) L->idx[i] = (uint32_t)i;
+  if (n) line_build(L, 0, n, 0);
+  return L;
+}
+
+SO_API void so_line_free(so_lines *L) {
+  if (!L) return;
+  free(L->nodes);
+  free(L->idx);
+  free(L);
+}
+
+SO_API size_t so_line_num_nodes(const so_lines *L) { return L->nnodes; }
+SO_API int so_line_depth(const so_lines *L) { return L->depth_seen; }
+
+SO_API void so_line_export(const so_lines *L, so_line_node *nodes, uint32_t *idx) {
+  if (nodes) memcpy(nodes, L->nodes, L->nnodes * sizeof(so_line_node));
+  if (idx) memcpy(idx, L->idx, L->n * sizeof(uint32_t));
+}
+
+static inline float ldot(const float a[3], const float b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+/* vnormalize (:439-454): the length through the double sqrt, unchanged when
+ * not above FLT_EPSILON * 16. */
+static inline void lnormalize(const float a[3], float out[3]) {
+  const float len = (float)sqrt((double)ldot(a, a));
+  out[0] = a[0];
+  out[1] = a[1];
+  out[2] = a[2];
+  if (len > FLT_EPSILON * 16.0f) {
+    const float inv = (float)(1.0 / (double)len);
+    for (int k = 0; k < 3; k++) out[k] *= inv;
+  }
+}
+
+/* solve2e (:456-486); returns the smaller root in root0. */
+static int line_solve(float *root0, float A, float B, float C) {
+  if (fabsf(A) <= FLT_EPSILON) {
+    *root0 = -C / B;
+    return 1;
+  }
+  const float D = B * B - A * C;
+  if (D < 0) return 0;
+  if (D == 0) {
+    *root0 = -B / A;
+    return 1;
+  }
+  float x1 = (float)(((double)fabsf(B) + sqrt((double)D)) / (double)A);
+  if (B >= 0.0f) x1 = -x1;
+  const float x2 = C / (A * x1);
+  *root0 = x1 > x2 ? x2 : x1;
+  return 2;
+}
+
+/* CylinderIsect (:488-577): the two end planes (caps) first, then the side
+ * surface of the cylinder of radius max(r0, r1). */
+static int line_isect(float *pt, float *pu, float *pv, int *hit_cap, const float p0[3],
+                      float r0, const float p1[3], float r1, const float org[3],
+                      const float dir[3], int cap) {
+  const float tmax = *pt;
+  const float rr = r0 > r1 ? r0 : r1;
+  float d[3], m[3];
+  for (int k = 0; k < 3; k++) {
+    d[k] = p1[k] - p0[k];
+    m[k] = org[k] - p0[k];
+  }
+  const float md = ldot(m, d), nd = ldot(dir, d), dd = ldot(d, d);
+  *hit_cap = 0;
+  float capT = FLT_MAX;
+  if (cap) {
+    float dn0[3], dn1[3], rd[3], e[3];
+    for (int k = 0; k < 3; k++) e[k] = p0[k] - p1[k];
+    lnormalize(e, dn0);
+    for (int k = 0; k < 3; k++) dn1[k] = -dn0[k];
+    lnormalize(dir, rd);
+    if (fabsf(ldot(dir, dn0)) > 1.0e-6f) {
+      const float p0D = -ldot(p0, dn0), p1D = -ldot(p1, dn1);
+      const float p0T = -(ldot(org, dn0) + p0D) / ldot(rd, dn0);
+      const float p1T = -(ldot(org, dn1) + p1D) / ldot(rd, dn1);
+      float q0[3], q1[3];
+      for (int k = 0; k < 3; k++) {
+        q0[k] = org[k] + rd[k] * p0T;
+        q1[k] = org[k] + rd[k] * p1T;
+      }
+      float a0[3], a1[3];
+      for (int k = 0; k < 3; k++) {
+        a0[k] = q0[k] - p0[k];
+        a1[k] = q1[k] - p1[k];
+      }
+      const float s0 = ldot(a0, a0), s1 = ldot(a1, a1);
+      if (p0T > 0.0f && p0T < tmax && (s0 < rr * rr)) {
+        *hit_cap = 1;
+        capT = p0T;
+        *pt = capT;
+        *pu = (float)sqrt((double)s0);
+        *pv = 0.0f;
+      }
+      if (p1T > 0.0f && p1T < tmax && p1T < capT && (s1 < rr * rr)) {
+        *hit_cap = 1;
+        capT = p1T;
+        *pt = capT;
+        *pu = (float)sqrt((double)s1);
+        *pv = 1.0f;
+      }
+    }
+  }
+  if (md <= 0.0f && nd <= 0.0f) return *hit_cap;
+  if (md >= dd && nd >= 0.0f) return *hit_cap;
+  const float nn = ldot(dir, dir), mn = ldot(m, dir);
+  const float A = dd * nn - nd * nd;
+  const float kk = ldot(m, m) - rr * rr;
+  const float C = dd * kk - md * md;
+  const float B = dd * mn - nd * md;
+  float t;
+  if (line_solve(&t, A, B, C)) {
+    if (0 <= t && t <= tmax && t <= capT) {
+      float s = md + t * nd;
+      s /= dd;
+      if (0 <= s && s <= 1) {
+        *hit_cap = 0;
+        *pt = t;
+        *pu = 0.0f;
+        *pv = s;
+        return 1;
+      }
+    }
+  }
+  return *hit_cap;
+}
+
+/* IntersectRayAABB (:377-420) with the reference's selection order. */
+static inline int line_box_hit(const so_line_node *nd, const float org[3], const float inv[3],
+                               const int sign[3], float maxT) {
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; k++) {
+    lo[k] = sign[k] ? nd->bmax[k] : nd->bmin[k];
+    hi[k] = sign[k] ? nd->bmin[k] : nd->bmax[k];
+  }
+  const float tx0 = (lo[0] - org[0]) * inv[0], tx1 = (hi[0] - org[0]) * inv[0];
+  const float ty0 = (lo[1] - org[1]) * inv[1], ty1 = (hi[1] - org[1]) * inv[1];
+  float tmin = (tx0 > ty0) ? tx0 : ty0;
+  float tmax = (tx1 < ty1) ? tx1 : ty1;
+  const float tz0 = (lo[2] - org[2]) * inv[2], tz1 = (hi[2] - org[2]) * inv[2];
+  tmin = (tmin > tz0) ? tmin : tz0;
+  tmax = (tmax < tz1) ? tmax : tz1;
+  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= maxT);
+}
+
+/* LineAccel::Traverse (:704-774) and BuildIntersection (:654-701). */
+static void line_trace_one(const so_lines *L, const so_ray *ray, so_hit *hit, float *normal) {
+  float hitT = FLT_MAX, it = FLT_MAX, iu = 0.0f, iv = 0.0f;
+  int icap = 0;
+  uint32_t prim = 0xffffffffu;
+  int sign[3];
+  float inv[3];
+  for (int k = 0; k < 3; k++) {
+    sign[k] = ray->dir[k] < 0.0f ? 1 : 0;
+    inv[k] = (float)(1.0 / (double)ray->dir[k]);
+  }
+  int stack[520];
+  int sp = 0;
+  stack[0] = 0;
+  while (L->nnodes && sp >= 0) {
+    const so_line_node *nd = &L->nodes[stack[sp]];
+    sp--;
+    if (nd->flag == 0) {
+      if (line_box_hit(nd, ray->org, inv, sign, hitT)) {
+        const int nearc = sign[nd->axis];
+        stack[++sp] = (int)nd->data[1 - nearc];
+        stack[++sp] = (int)nd->data[nearc];
+      }
+    } else {
+      float t = it;
+      int any = 0;
+      for (uint32_t j = 0; j < nd->data[0]; j++) {
+        const uint32_t i = L->idx[nd->data[1] + j];
+        const uint32_t a = L->seg[2 * i], b = L->seg[2 * i + 1];
+        float u, v;
+        int hc = 0;
+        if (line_isect(&t, &u, &v, &hc, &L->pos[3 * a], line_r(L, a), &L->pos[3 * b],
+                       line_r(L, b), ray->org, ray->dir, L->cap)) {
+          it = t;
+          iu = u;
+          iv = v;
+          icap = hc;
+          prim = i;
+          any = 1;
+        }
+      }
+      if (any) hitT = it;
+    }
+  }
+  if (it < FLT_MAX) {
+    hit->t = it;
+    hit->u = iu;
+    hit->v = iv;
+    hit->prim = prim;
+    if (normal) {
+      const uint32_t a = L->seg[2 * prim], b = L->seg[2 * prim + 1];
+      const float *p0 = &L->pos[3 * a], *p1 = &L->pos[3 * b];
+      float p[3], d[3], n[3];
+      for (int k = 0; k < 3; k++) {
+        p[k] = ray->org[k] + it * ray->dir[k];
+        d[k] = p1[k] - p0[k];
+      }
+      if (icap) {
+        float c[3], pc[3];
+        for (int k = 0; k < 3; k++) c[k] = d[k] * 0.5f + p0[k];
+        lnormalize(d, n);
+        for (int k = 0; k < 3; k++) pc[k] = p[k] - c[k];
+        if (!(ldot(pc, n) > 0.0f))
+          for (int k = 0; k < 3; k++) n[k] = -n[k];
+      } else {
+        float e[3];
+        for (int k = 0; k < 3; k++) e[k] = p[k] - (p0[k] + iv * d[k]);
+        lnormalize(e, n);
+      }
+      for (int k = 0; k < 3; k++) normal[k] = n[k];
+    }
+  } else {
+    hit->t = FLT_MAX;
+    hit->u = hit->v = 0.0f;
+    hit->prim = 0xffffffffu;
+    if (normal) normal[0] = normal[1] = normal[2] = 0.0f;
+  }
+}
+
+SO_API void so_line_trace(const so_lines *L, const so_ray *rays, size_t n, so_hit *hits,
+                          float *normals, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+#endif
+  for (long long i = 0; i < (long long)n; i++)
+    line_trace_one(L, &rays[i], &hits[i], normals ? &normals[3 * i] : NULL);
+}

@@ -140,6 +140,14 @@ _SIGS = {
     "srt_texture3d_set_remap": [_P, C.c_int, _P, _SZ],
     "srt_texture3d_set_sparse": [_P, C.c_int, C.c_int, _P, _P, _SZ, _P, _SZ],
     "srt_texture3d_fetch": [_P, _P, _SZ, _P],
+    "srt_line_create": [_P, C.POINTER(_P)],
+    "srt_line_destroy": [_P],
+    "srt_line_build": [_P, _P, _SZ, _P, C.c_float, _P, _SZ, C.c_int32, C.c_int32, C.c_int32],
+    "srt_line_trace": [_P, _P, _SZ, _P, _P],
+    "srt_line_bbox": [_P, _P, _P],
+    "srt_line_info": [_P, _P, _P, _P],
+    "srt_line_export": [_P, _P, _P],
+    "srt_line_dump": [_P, C.c_char_p],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],

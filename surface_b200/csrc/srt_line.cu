@@ -1,0 +1,723 @@
+// srt_line.cu -- LineAccel (render/render_accel_line.cc) on the GPU: capped
+// cylinders between segment end points, closest hit.
+//
+// Build (LineAccel::BuildTree, :167-296) runs on the host like the
+// reference's: top-down over an index array, a leaf below min_leaf lines or
+// at max_depth, else a cut at the spatial median of the node box's longest
+// axis (the position formed in double and stored as float), then the other
+// axes in turn, with the two-ended partition of std::partition on the
+// segment midpoints, and the object median when no axis separates them.
+// Nodes are emitted in pre-order; the device copy packs each into 32 bytes.
+// The lines are gathered in leaf order into 64-byte records holding the
+// per-line terms of CylinderIsect (end points, max radius, |d|^2, the cap
+// plane normal and offsets), computed with the reference's float operations.
+//
+// Trace (LineAccel::Traverse, :704-774): one thread per ray, the stack of
+// the reference (a popped branch tests its own box against the closest hit
+// so far, then pushes far and near children by the sign of the ray's
+// direction on the branch's axis), every line of a popped leaf tested in
+// order by CylinderIsect (:488-577).  Compiled without FMA contraction; the
+// reference's unqualified sqrt and fabs are the double C functions, so the
+// quadratic's first root is formed in double, and every other sqrt and
+// reciprocal rounds as the float operation does.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "srt_internal.cuh"
+
+namespace {
+
+// The reference's LineNode (Dump record, 40 bytes).
+struct LineNodeH {
+  float bmin[3], bmax[3];
+  int32_t flag, axis;  // flag 1: leaf (data = count, first), 0: branch (children)
+  uint32_t data[2];
+};
+static_assert(sizeof(LineNodeH) == 40, "LineNode layout");
+
+// Device node: w1 bit 31 set for a leaf (w0 = first record, the low bits = count),
+// else w0 = left child, w1 = right child | axis << 29.
+struct alignas(16) LNode {
+  float bmin[3];
+  uint32_t w0;
+  float bmax[3];
+  uint32_t w1;
+};
+static_assert(sizeof(LNode) == 32, "two 16-byte loads");
+
+// One line in leaf order: the terms of CylinderIsect that do not depend on
+// the ray.  dn0 = normalize(p0 - p1); p0D = -dot(p0, dn0); p1D = -dot(p1, -dn0).
+struct alignas(16) LineRec {
+  float p0[3], rr;
+  float p1[3], dd;
+  float dn0[3], p0D;
+  float p1D;
+  uint32_t prim;
+  float pad[2];
+};
+static_assert(sizeof(LineRec) == 64, "four 16-byte loads");
+
+constexpr uint32_t kLineLeaf = 0x80000000u;
+constexpr float kCapEps = 1.0e-6f;  // the file-level kEPS of render_accel_line.cc
+
+}  // namespace
+
+struct srt_line_accel {
+  srt_ctx *ctx = nullptr;
+  bool built = false;
+  size_t nlines = 0;
+  int depth = 0, cap = 1;
+  std::vector<LineNodeH> nodes;  // reference layout (Dump, export)
+  std::vector<uint32_t> idx;
+  srt::DevBuf dnodes, drecs;
+};
+
+namespace {
+
+using srt::DevBuf;
+
+// ------------------------------------------------------------------ build
+struct LineInputs {
+  const float *pos;
+  const float *rad;  // per vertex, or null
+  float constr;
+  const uint32_t *seg;
+};
+
+inline float vrad(const LineInputs &in, uint32_t v) { return in.rad ? in.rad[v] : in.constr; }
+
+// GetBoundingBoxOfLine (:83-116).
+void line_box(const LineInputs &in, uint32_t i, float bmin[3], float bmax[3]) {
+  const uint32_t a = in.seg[2 * i], b = in.seg[2 * i + 1];
+  const float r0 = vrad(in, a), r1 = vrad(in, b);
+  float pt[4][3];
+  for (int k = 0; k < 3; k++) {
+    pt[0][k] = in.pos[3 * a + k] - r0;
+    pt[1][k] = in.pos[3 * a + k] + r0;
+    pt[2][k] = in.pos[3 * b + k] - r1;
+    pt[3][k] = in.pos[3 * b + k] + r1;
+  }
+  for (int k = 0; k < 3; k++) bmin[k] = bmax[k] = pt[0][k];
+  for (int q = 1; q < 4; q++)
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = (bmin[k] < pt[q][k]) ? bmin[k] : pt[q][k];
+      bmax[k] = (bmax[k] > pt[q][k]) ? bmax[k] : pt[q][k];
+    }
+  const float eps = FLT_EPSILON * 16.0f;
+  for (int k = 0; k < 3; k++) {
+    bmin[k] -= bmin[k] * eps;
+    bmax[k] += bmax[k] * eps;
+  }
+}
+
+struct Builder {
+  const std::vector<float> &box;  // 6 floats per line
+  const std::vector<float> &mid;  // 3 floats per line: (p0 + p1) * 0.5
+  std::vector<uint32_t> &idx;
+  std::vector<LineNodeH> &nodes;
+  int min_leaf, max_depth, depth_seen = 0;
+
+  // ComputeBoundingBox (:142-163): min/max over the lines' boxes, in order.
+  void range_box(size_t l, size_t r, float bmin[3], float bmax[3]) const {
+    const float *b0 = &box[6 * idx[l]];
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = b0[k];
+      bmax[k] = b0[3 + k];
+    }
+    for (size_t i = l; i < r; i++) {
+      const float *b = &box[6 * idx[i]];
+      for (int k = 0; k < 3; k++) {
+        bmin[k] = (bmin[k] < b[k]) ? bmin[k] : b[k];
+        bmax[k] = (bmax[k] > b[3 + k]) ? bmax[k] : b[3 + k];
+      }
+    }
+  }
+
+  // std::partition's two-ended scan: lines whose midpoint lies below pos
+  // first.
+  size_t partition(size_t first, size_t last, int axis, float pos) {
+    for (;;) {
+      while (first != last && mid[3 * idx[first] + axis] < pos) first++;
+      if (first == last) return first;
+      last--;
+      while (first != last && !(mid[3 * idx[last] + axis] < pos)) last--;
+      if (first == last) return first;
+      std::swap(idx[first], idx[last]);
+      first++;
+    }
+  }
+
+  size_t build(size_t l, size_t r, int depth) {
+    const size_t off = nodes.size();
+    nodes.push_back(LineNodeH{});
+    depth_seen = std::max(depth_seen, depth);
+    float bmin[3], bmax[3];
+    range_box(l, r, bmin, bmax);
+    const size_t n = r - l;
+    if (n < (size_t)min_leaf || depth >= max_depth) {
+      LineNodeH &nd = nodes[off];
+      std::memcpy(nd.bmin, bmin, sizeof(bmin));
+      std::memcpy(nd.bmax, bmax, sizeof(bmax));
+      nd.flag = 1;
+      nd.data[0] = (uint32_t)n;
+      nd.data[1] = (uint32_t)l;
+      return off;
+    }
+    float bsize[3];
+    for (int k = 0; k < 3; k++) bsize[k] = bmax[k] - bmin[k];
+    int longest = 0;
+    float m = bsize[0];
+    if (m < bsize[1]) {
+      m = bsize[1];
+      longest = 1;
+    }
+    if (m < bsize[2]) longest = 2;
+    size_t split = l;
+    int axis = 0;
+    for (int t = 0; t < 3; t++) {
+      axis = (longest + t) % 3;
+      const float pos = (float)((double)bmin[axis] + 0.5 * (double)bsize[axis]);
+      split = partition(l, r, axis, pos);
+      if (split != l && split != r) break;
+      split = l + (n >> 1);
+    }
+    nodes[off].axis = axis;
+    const size_t left = build(l, split, depth + 1);
+    const size_t right = build(split, r, depth + 1);
+    LineNodeH &nd = nodes[off];
+    nd.data[0] = (uint32_t)left;
+    nd.data[1] = (uint32_t)right;
+    std::memcpy(nd.bmin, bmin, sizeof(bmin));
+    std::memcpy(nd.bmax, bmax, sizeof(bmax));
+    return off;
+  }
+};
+
+// ------------------------------------------------------------------ device
+__device__ __forceinline__ float dot3(const float a[3], const float b[3]) {
+  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
+}
+
+// vnormalize (:439-454): (float)sqrt((double)x) is the float sqrt and
+// (float)(1.0 / (double)len) the float reciprocal, both correctly rounded.
+__device__ __forceinline__ void normalize3(const float a[3], float out[3]) {
+  const float len = __fsqrt_rn(dot3(a, a));
+  out[0] = a[0];
+  out[1] = a[1];
+  out[2] = a[2];
+  if (len > FLT_EPSILON * 16.0f) {
+    const float inv = __frcp_rn(len);
+    out[0] *= inv;
+    out[1] *= inv;
+    out[2] *= inv;
+  }
+}
+
+__global__ void line_rec_kernel(const float *__restrict__ pos, const float *__restrict__ rad,
+                                float constr, const uint32_t *__restrict__ seg,
+                                const uint32_t *__restrict__ order, size_t n,
+                                LineRec *__restrict__ out) {
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
+       j += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t i = order[j];
+    const uint32_t a = seg[2 * i], b = seg[2 * i + 1];
+    LineRec r;
+    float e[3], d[3], dn1[3];
+    for (int k = 0; k < 3; k++) {
+      r.p0[k] = pos[3 * a + k];
+      r.p1[k] = pos[3 * b + k];
+      e[k] = r.p0[k] - r.p1[k];
+      d[k] = r.p1[k] - r.p0[k];
+    }
+    const float r0 = rad ? rad[a] : constr, r1 = rad ? rad[b] : constr;
+    r.rr = (r0 < r1) ? r1 : r0;  // std::max<real>(r0, r1)
+    r.dd = dot3(d, d);
+    normalize3(e, r.dn0);
+    for (int k = 0; k < 3; k++) dn1[k] = -r.dn0[k];
+    r.p0D = -dot3(r.p0, r.dn0);
+    r.p1D = -dot3(r.p1, dn1);
+    r.prim = i;
+    r.pad[0] = r.pad[1] = 0.0f;
+    out[j] = r;
+  }
+}
+
+__device__ __forceinline__ LineRec load_line(const LineRec *p) {
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+  const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
+  LineRec r;
+  r.p0[0] = a.x;
+  r.p0[1] = a.y;
+  r.p0[2] = a.z;
+  r.rr = a.w;
+  r.p1[0] = b.x;
+  r.p1[1] = b.y;
+  r.p1[2] = b.z;
+  r.dd = b.w;
+  r.dn0[0] = c.x;
+  r.dn0[1] = c.y;
+  r.dn0[2] = c.z;
+  r.p0D = c.w;
+  r.p1D = d.x;
+  r.prim = __float_as_uint(d.y);
+  return r;
+}
+
+struct RayL {
+  float org[3], dir[3], rd[3], inv[3], nn;
+  int sign[3];
+};
+
+// CylinderIsect (:488-577) for one line record; *pt is the closest hit so
+// far (updated on a hit, as the reference does through its pointer).
+__device__ __forceinline__ bool cyl_isect(const LineRec &L, const RayL &R, bool cap, float *pt,
+                                          float *pu, float *pv, bool &hit_cap) {
+  const float tmax = *pt;
+  float d[3], m[3];
+  for (int k = 0; k < 3; k++) {
+    d[k] = L.p1[k] - L.p0[k];
+    m[k] = R.org[k] - L.p0[k];
+  }
+  const float md = dot3(m, d), nd = dot3(R.dir, d), dd = L.dd, rr = L.rr;
+  hit_cap = false;
+  float capT = FLT_MAX;
+  if (cap && fabsf(dot3(R.dir, L.dn0)) > kCapEps) {
+    const float dn1[3] = {-L.dn0[0], -L.dn0[1], -L.dn0[2]};
+    const float p0T = -(dot3(R.org, L.dn0) + L.p0D) / dot3(R.rd, L.dn0);
+    const float p1T = -(dot3(R.org, dn1) + L.p1D) / dot3(R.rd, dn1);
+    float a0[3], a1[3];
+    for (int k = 0; k < 3; k++) {
+      a0[k] = (R.org[k] + R.rd[k] * p0T) - L.p0[k];
+      a1[k] = (R.org[k] + R.rd[k] * p1T) - L.p1[k];
+    }
+    const float s0 = dot3(a0, a0), s1 = dot3(a1, a1);
+    if (p0T > 0.0f && p0T < tmax && s0 < rr * rr) {
+      hit_cap = true;
+      capT = p0T;
+      *pt = capT;
+      *pu = __fsqrt_rn(s0);
+      *pv = 0.0f;
+    }
+    if (p1T > 0.0f && p1T < tmax && p1T < capT && s1 < rr * rr) {
+      hit_cap = true;
+      capT = p1T;
+      *pt = capT;
+      *pu = __fsqrt_rn(s1);
+      *pv = 1.0f;
+    }
+  }
+  if (md <= 0.0f && nd <= 0.0f) return hit_cap;
+  if (md >= dd && nd >= 0.0f) return hit_cap;
+  const float mn = dot3(m, R.dir);
+  const float A = dd * R.nn - nd * nd;
+  const float kk = dot3(m, m) - rr * rr;
+  const float C = dd * kk - md * md;
+  const float B = dd * mn - nd * md;
+  // solve2e (:456-486), the smaller root
+  float t;
+  if (fabsf(A) <= FLT_EPSILON) {
+    t = -C / B;
+  } else {
+    const float D = B * B - A * C;
+    if (D < 0.0f) return hit_cap;
+    if (D == 0.0f) {
+      t = -B / A;
+    } else {
+      float x1 = (float)(((double)fabsf(B) + sqrt((double)D)) / (double)A);
+      if (B >= 0.0f) x1 = -x1;
+      const float x2 = C / (A * x1);
+      t = x1 > x2 ? x2 : x1;
+    }
+  }
+  if (0.0f <= t && t <= tmax && t <= capT) {
+    float s = md + t * nd;
+    s /= dd;
+    if (0.0f <= s && s <= 1.0f) {
+      hit_cap = false;
+      *pt = t;
+      *pu = 0.0f;
+      *pv = s;
+      return true;
+    }
+  }
+  return hit_cap;
+}
+
+// IntersectRayAABB (:377-420) with the reference's selection order.
+__device__ __forceinline__ bool box_hit(const LNode &nd, const RayL &R, float maxT) {
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; k++) {
+    lo[k] = R.sign[k] ? nd.bmax[k] : nd.bmin[k];
+    hi[k] = R.sign[k] ? nd.bmin[k] : nd.bmax[k];
+  }
+  const float tx0 = (lo[0] - R.org[0]) * R.inv[0], tx1 = (hi[0] - R.org[0]) * R.inv[0];
+  const float ty0 = (lo[1] - R.org[1]) * R.inv[1], ty1 = (hi[1] - R.org[1]) * R.inv[1];
+  float tmin = (tx0 > ty0) ? tx0 : ty0;
+  float tmax = (tx1 < ty1) ? tx1 : ty1;
+  const float tz0 = (lo[2] - R.org[2]) * R.inv[2], tz1 = (hi[2] - R.org[2]) * R.inv[2];
+  tmin = (tmin > tz0) ? tmin : tz0;
+  tmax = (tmax < tz1) ? tmax : tz1;
+  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= maxT);
+}
+
+__device__ __forceinline__ LNode load_node(const LNode *p) {
+  const float4 *q = reinterpret_cast<const float4 *>(p);
+  const float4 a = __ldg(q), b = __ldg(q + 1);
+  LNode n;
+  n.bmin[0] = a.x;
+  n.bmin[1] = a.y;
+  n.bmin[2] = a.z;
+  n.w0 = __float_as_uint(a.w);
+  n.bmax[0] = b.x;
+  n.bmax[1] = b.y;
+  n.bmax[2] = b.z;
+  n.w1 = __float_as_uint(b.w);
+  return n;
+}
+
+template <int STACK>
+__global__ void __launch_bounds__(128)
+line_trace_kernel(const LNode *__restrict__ nodes, const LineRec *__restrict__ recs, bool cap,
+                  const srt_ray *__restrict__ rays, size_t n, srt_hit *__restrict__ hits,
+                  float *__restrict__ normals) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float4 *rq = reinterpret_cast<const float4 *>(rays + i);
+    const float4 r0 = __ldg(rq), r1 = __ldg(rq + 1);
+    RayL R;
+    R.org[0] = r0.x;
+    R.org[1] = r0.y;
+    R.org[2] = r0.z;
+    R.dir[0] = r1.x;
+    R.dir[1] = r1.y;
+    R.dir[2] = r1.z;
+    for (int k = 0; k < 3; k++) {
+      R.sign[k] = R.dir[k] < 0.0f ? 1 : 0;
+      R.inv[k] = __frcp_rn(R.dir[k]);  // (float)(1.0 / dir), correctly rounded
+    }
+    normalize3(R.dir, R.rd);
+    R.nn = dot3(R.dir, R.dir);
+    float hitT = FLT_MAX, it = FLT_MAX, iu = 0.0f, iv = 0.0f;
+    bool icap = false;
+    int best = -1;
+    int stack[STACK];
+    int sp = 0;
+    stack[0] = 0;
+    while (sp >= 0) {
+      const LNode nd = load_node(nodes + stack[sp]);
+      sp--;
+      if (!(nd.w1 & kLineLeaf)) {
+        if (box_hit(nd, R, hitT)) {
+          const int axis = (int)(nd.w1 >> 29);
+          const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
+          const int nearc = R.sign[axis];
+          stack[++sp] = nearc ? left : right;  // far
+          stack[++sp] = nearc ? right : left;  // near
+        }
+      } else {
+        float t = it;
+        bool any = false;
+        const uint32_t first = nd.w0, cnt = nd.w1 & ~kLineLeaf;
+        for (uint32_t j = 0; j < cnt; j++) {
+          const LineRec L = load_line(recs + first + j);
+          float u, v;
+          bool hc;
+          if (cyl_isect(L, R, cap, &t, &u, &v, hc)) {
+            it = t;
+            iu = u;
+            iv = v;
+            icap = hc;
+            best = (int)(first + j);
+            any = true;
+          }
+        }
+        if (any) hitT = it;
+      }
+    }
+    srt_hit h;
+    if (it < FLT_MAX) {
+      const LineRec L = load_line(recs + best);
+      h.t = it;
+      h.u = iu;
+      h.v = iv;
+      h.prim = L.prim;
+      if (normals) {
+        // BuildIntersection (:654-701)
+        float p[3], d[3], nrm[3], e[3];
+        for (int k = 0; k < 3; k++) {
+          p[k] = R.org[k] + it * R.dir[k];
+          d[k] = L.p1[k] - L.p0[k];
+        }
+        if (icap) {
+          normalize3(d, nrm);
+          for (int k = 0; k < 3; k++) e[k] = p[k] - (d[k] * 0.5f + L.p0[k]);
+          if (!(dot3(e, nrm) > 0.0f))
+            for (int k = 0; k < 3; k++) nrm[k] = -nrm[k];
+        } else {
+          for (int k = 0; k < 3; k++) e[k] = p[k] - (L.p0[k] + iv * d[k]);
+          normalize3(e, nrm);
+        }
+        for (int k = 0; k < 3; k++) normals[3 * i + k] = nrm[k];
+      }
+    } else {
+      h.t = FLT_MAX;
+      h.u = h.v = 0.0f;
+      h.prim = SRT_MISS;
+      if (normals)
+        for (int k = 0; k < 3; k++) normals[3 * i + k] = 0.0f;
+    }
+    reinterpret_cast<float4 *>(hits)[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+  }
+}
+
+srt_status line_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
+                     const void **out) {
+  if (!p || srt::is_device_ptr(p)) {
+    *out = p;
+    return SRT_OK;
+  }
+  cudaError_t e = stage.ensure(bytes ? bytes : 1);
+  if (e == cudaSuccess && bytes)
+    e = cudaMemcpyAsync(stage.p, p, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return srt::cuda_status(e, "line staging");
+  *out = stage.p;
+  return SRT_OK;
+}
+
+// A host copy of an input that may live on the device.
+template <typename T>
+srt_status host_copy(const T *p, size_t count, std::vector<T> &buf, const T **out) {
+  if (!p || !srt::is_device_ptr(p)) {
+    *out = p;
+    return SRT_OK;
+  }
+  buf.resize(count ? count : 1);
+  cudaError_t e = cudaMemcpy(buf.data(), p, count * sizeof(T), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return srt::cuda_status(e, "line input copy");
+  *out = buf.data();
+  return SRT_OK;
+}
+
+}  // namespace
+
+using namespace srt;
+
+extern "C" {
+
+SRT_API srt_status srt_line_create(srt_ctx *ctx, srt_line_accel **out) {
+  if (!ctx || !out) return SRT_ERR_INVALID;
+  srt_line_accel *a = new (std::nothrow) srt_line_accel();
+  if (!a) return SRT_ERR_NO_MEMORY;
+  a->ctx = ctx;
+  *out = a;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_destroy(srt_line_accel *a) {
+  if (!a) return SRT_OK;
+  cudaSetDevice(a->ctx->device);
+  cudaStreamSynchronize(a->ctx->stream);
+  delete a;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_build(srt_line_accel *a, const float *positions, size_t nverts,
+                                  const float *radius, float constant_radius,
+                                  const uint32_t *segments, size_t nlines, int32_t min_leaf,
+                                  int32_t max_depth, int32_t cap) {
+  if (!a || !positions || !segments || nlines == 0 || nverts == 0) {
+    set_error("srt_line_build: positions, segments and at least one line");
+    return SRT_ERR_INVALID;
+  }
+  if (nlines >= (1u << 31)) {
+    set_error("srt_line_build: fewer than 2^31 lines");
+    return SRT_ERR_INVALID;
+  }
+  if (min_leaf <= 0) min_leaf = 4;    // LineBuildOptions defaults
+  if (max_depth <= 0) max_depth = 512;
+  if (max_depth > 512) {
+    set_error("srt_line_build: max_depth above 512 (the traversal stack)");
+    return SRT_ERR_INVALID;
+  }
+  srt_ctx *ctx = a->ctx;
+  cudaSetDevice(ctx->device);
+  std::vector<float> hp, hr;
+  std::vector<uint32_t> hs;
+  const float *pos, *rad;
+  const uint32_t *seg;
+  srt_status s = host_copy(positions, nverts * 3, hp, &pos);
+  if (s == SRT_OK) s = host_copy(radius, radius ? nverts : 0, hr, &rad);
+  if (s == SRT_OK) s = host_copy(segments, nlines * 2, hs, &seg);
+  if (s != SRT_OK) return s;
+  for (size_t i = 0; i < 2 * nlines; i++)
+    if (seg[i] >= nverts) {
+      set_error("srt_line_build: a segment names a vertex beyond nverts");
+      return SRT_ERR_INVALID;
+    }
+  const LineInputs in{pos, rad, constant_radius, seg};
+  std::vector<float> box(6 * nlines), mid(3 * nlines);
+  for (size_t i = 0; i < nlines; i++) {
+    line_box(in, (uint32_t)i, &box[6 * i], &box[6 * i + 3]);
+    const uint32_t p = seg[2 * i], q = seg[2 * i + 1];
+    for (int k = 0; k < 3; k++) mid[3 * i + k] = (pos[3 * p + k] + pos[3 * q + k]) * 0.5f;
+  }
+  a->built = false;
+  a->idx.resize(nlines);
+  for (size_t i = 0; i < nlines; i++) a->idx[i] = (uint32_t)i;
+  a->nodes.clear();
+  Builder B{box, mid, a->idx, a->nodes, min_leaf, max_depth};
+  B.build(0, nlines, 0);
+  if (a->nodes.size() >= (1u << 29)) {
+    set_error("srt_line_build: more than 2^29 nodes");
+    return SRT_ERR_INVALID;
+  }
+  std::vector<LNode> dn(a->nodes.size());
+  for (size_t i = 0; i < a->nodes.size(); i++) {
+    const LineNodeH &h = a->nodes[i];
+    LNode &d = dn[i];
+    for (int k = 0; k < 3; k++) {
+      d.bmin[k] = h.bmin[k];
+      d.bmax[k] = h.bmax[k];
+    }
+    if (h.flag) {
+      d.w0 = h.data[1];
+      d.w1 = kLineLeaf | h.data[0];
+    } else {
+      d.w0 = h.data[0];
+      d.w1 = h.data[1] | ((uint32_t)h.axis << 29);
+    }
+  }
+  cudaError_t e;
+  if ((e = a->dnodes.ensure(dn.size() * sizeof(LNode))) != cudaSuccess ||
+      (e = a->drecs.ensure(nlines * sizeof(LineRec))) != cudaSuccess)
+    return cuda_status(e, "line accel");
+  e = cudaMemcpyAsync(a->dnodes.p, dn.data(), dn.size() * sizeof(LNode),
+                      cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return cuda_status(e, "line nodes");
+  DevBuf sp, sr, ss, so;
+  const void *dp, *dr, *ds;
+  if ((s = line_view(ctx, positions, nverts * 12, sp, &dp)) != SRT_OK) return s;
+  if ((s = line_view(ctx, radius, radius ? nverts * 4 : 0, sr, &dr)) != SRT_OK) return s;
+  if ((s = line_view(ctx, segments, nlines * 8, ss, &ds)) != SRT_OK) return s;
+  if ((e = so.ensure(nlines * 4)) != cudaSuccess) return cuda_status(e, "line order");
+  e = cudaMemcpyAsync(so.p, a->idx.data(), nlines * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return cuda_status(e, "line order");
+  const unsigned grid = (unsigned)std::min<size_t>((nlines + 255) / 256, 4096);
+  line_rec_kernel<<<grid, 256, 0, ctx->stream>>>(
+      static_cast<const float *>(dp), static_cast<const float *>(dr), constant_radius,
+      static_cast<const uint32_t *>(ds), so.as<uint32_t>(), nlines, a->drecs.as<LineRec>());
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "line records");
+  // the staged inputs are freed on return: finish with them first
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "line build");
+  a->nlines = nlines;
+  a->depth = B.depth_seen;
+  a->cap = cap != 0;
+  a->built = true;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_trace(srt_line_accel *a, const srt_ray *rays, size_t n,
+                                  srt_hit *hits, float *normals) {
+  if (!a || (n && (!rays || !hits))) return SRT_ERR_INVALID;
+  if (!a->built) {
+    set_error("line accel not built");
+    return SRT_ERR_INVALID;
+  }
+  if (n == 0) return SRT_OK;
+  srt_ctx *ctx = a->ctx;
+  cudaSetDevice(ctx->device);
+  const void *dr;
+  srt_status s = line_view(ctx, rays, n * sizeof(srt_ray), ctx->s_stage_in, &dr);
+  if (s != SRT_OK) return s;
+  const bool hdev = is_device_ptr(hits), ndev = !normals || is_device_ptr(normals);
+  srt_hit *dh = hits;
+  float *dn = normals;
+  cudaError_t e;
+  if (!hdev) {
+    if ((e = ctx->s_stage_out.ensure(n * sizeof(srt_hit))) != cudaSuccess)
+      return cuda_status(e, "hit staging");
+    dh = ctx->s_stage_out.as<srt_hit>();
+  }
+  if (!ndev) {
+    if ((e = ctx->s_stage_norm.ensure(n * 12)) != cudaSuccess)
+      return cuda_status(e, "normal staging");
+    dn = ctx->s_stage_norm.as<float>();
+  }
+  if ((reinterpret_cast<uintptr_t>(dr) | reinterpret_cast<uintptr_t>(dh)) & 15u) {
+    set_error("ray and hit arrays must be 16-byte aligned");
+    return SRT_ERR_INVALID;
+  }
+  const unsigned grid = (unsigned)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * 32);
+  const LNode *nd = a->dnodes.as<LNode>();
+  const LineRec *rc = a->drecs.as<LineRec>();
+  const srt_ray *rr = static_cast<const srt_ray *>(dr);
+  if (a->depth + 2 <= 64)
+    line_trace_kernel<64><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, n, dh, dn);
+  else
+    line_trace_kernel<520><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, n, dh, dn);
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "line trace");
+  if (!hdev) cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, ctx->stream);
+  if (!ndev) cudaMemcpyAsync(normals, dn, n * 12, cudaMemcpyDeviceToHost, ctx->stream);
+  if (!hdev || !ndev || !is_device_ptr(rays))
+    return cuda_status(cudaStreamSynchronize(ctx->stream), "line trace");
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_bbox(srt_line_accel *a, double bmin[3], double bmax[3]) {
+  if (!a || !bmin || !bmax) return SRT_ERR_INVALID;
+  if (!a->built) {  // LineAccel::BoundingBox of an empty tree
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = DBL_MAX;
+      bmax[k] = -DBL_MAX;
+    }
+    return SRT_OK;
+  }
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = a->nodes[0].bmin[k];
+    bmax[k] = a->nodes[0].bmax[k];
+  }
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_info(srt_line_accel *a, uint64_t *nlines, uint64_t *nnodes,
+                                 int32_t *depth) {
+  if (!a) return SRT_ERR_INVALID;
+  if (nlines) *nlines = a->built ? a->nlines : 0;
+  if (nnodes) *nnodes = a->built ? a->nodes.size() : 0;
+  if (depth) *depth = a->built ? a->depth : 0;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_export(srt_line_accel *a, void *nodes, uint32_t *indices) {
+  if (!a || !a->built) return SRT_ERR_INVALID;
+  if (nodes) std::memcpy(nodes, a->nodes.data(), a->nodes.size() * sizeof(LineNodeH));
+  if (indices) std::memcpy(indices, a->idx.data(), a->idx.size() * sizeof(uint32_t));
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_line_dump(srt_line_accel *a, const char *path) {
+  if (!a || !path || !a->built) return SRT_ERR_INVALID;
+  FILE *fp = fopen(path, "wb");
+  if (!fp) {
+    set_error(std::string("cannot write ") + path);
+    return SRT_ERR_INVALID;
+  }
+  const unsigned long long nn = a->nodes.size(), ni = a->idx.size();
+  bool ok = fwrite(&nn, 8, 1, fp) == 1 &&
+            fwrite(a->nodes.data(), sizeof(LineNodeH), nn, fp) == nn &&
+            fwrite(&ni, 8, 1, fp) == 1 && fwrite(a->idx.data(), 4, ni, fp) == ni;
+  ok = (fclose(fp) == 0) && ok;
+  if (!ok) {
+    set_error(std::string("write failed: ") + path);
+    return SRT_ERR_INVALID;
+  }
+  return SRT_OK;
+}
+
+}  // extern "C"

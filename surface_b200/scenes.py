@@ -211,6 +211,15 @@ def pinhole_rays(width, height, eye, lookat, up=(0, 1, 0), fov_deg=45.0):
     return rays
 
 
+def make_rays(org, dirs):
+    """Ray records from (n, 3) origins and directions (not normalised)."""
+    rays = np.zeros(len(org), RAY_DTYPE)
+    rays["org"] = np.asarray(org, np.float32)
+    rays["dir"] = np.asarray(dirs, np.float32)
+    rays["prev_prim"] = MISS
+    return rays
+
+
 def ortho_rays(width, height, lo=(0.0, 0.0), hi=(1.0, 1.0), z=2.0):
     """Orthographic rays along -z through pixel centres of [lo,hi]^2."""
     xs = lo[0] + (np.arange(width) + 0.5) * (hi[0] - lo[0]) / width
@@ -671,3 +680,92 @@ def sparse_edge_coords(blocks, gdim, n, seed, spread=(0.0, 1.0)):
                     np.float32)
     special = tiny[rng.integers(0, tiny.size, size=(max(n // 16, 16), 3))]
     return np.concatenate([u, anywhere, special]).astype(np.float32)
+
+
+def line_strands(nstrands=2000, nseg=16, seed=123456, radius=0.004, taper=True):
+    """Seeded hair-like strands for the line (capped cylinder) accel:
+    `nstrands` polylines of `nseg` segments rooted on the unit sphere,
+    growing outward with a random bend.  Returns (positions (V, 3) float32,
+    segments (nstrands * nseg, 2) uint32 vertex pairs, per-vertex radius
+    (V,) float32)."""
+    rng = np.random.default_rng(seed)
+    root = rng.normal(size=(nstrands, 3))
+    root /= np.linalg.norm(root, axis=1, keepdims=True)
+    d = root + 0.3 * rng.normal(size=(nstrands, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    pts = np.empty((nstrands, nseg + 1, 3), np.float64)
+    pts[:, 0] = root
+    step = 0.6 / nseg
+    for j in range(1, nseg + 1):
+        d = d + 0.25 * rng.normal(size=(nstrands, 3))
+        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pts[:, j] = pts[:, j - 1] + step * d
+    pos = pts.reshape(-1, 3).astype(np.float32)
+    base = np.arange(nstrands)[:, None] * (nseg + 1) + np.arange(nseg)[None, :]
+    seg = np.stack([base, base + 1], axis=-1).reshape(-1, 2).astype(np.uint32)
+    w = (1.0 - 0.7 * np.arange(nseg + 1) / nseg) if taper else np.ones(nseg + 1)
+    rad = (radius * np.tile(w, nstrands)).astype(np.float32)
+    return pos, seg, rad
+
+
+def line_segments(n=20000, seed=7, extent=1.0, radius=(0.002, 0.02)):
+    """Seeded independent segments of random length and direction in a cube,
+    radii per vertex (different at the two ends), with a few zero-length and
+    coincident segments."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-extent, extent, size=(n, 3))
+    b = a + rng.normal(scale=0.08 * extent, size=(n, 3))
+    b[: n // 50] = a[: n // 50]  # zero length
+    a[n // 50: n // 25] = a[n // 25: n // 25 + (n // 25 - n // 50)]  # shared start points
+    pos = np.stack([a, b], axis=1).reshape(-1, 3).astype(np.float32)
+    seg = np.arange(2 * n, dtype=np.uint32).reshape(n, 2)
+    rad = rng.uniform(*radius, size=2 * n).astype(np.float32)
+    return pos, seg, rad
+
+
+def line_cases():
+    """Small line sets with the shapes that stress LineAccel: (name, positions,
+    segments, radius or None, constant radius, options dict, rays)."""
+    out = []
+    rng = np.random.default_rng(11)
+    # axis-aligned segments, rays along the axes (zero direction components),
+    # rays along a segment's own axis (through both caps), rays from inside
+    pos = np.array([[0, 0, 0], [1, 0, 0], [0, 0.5, 0], [0, 0.5, 1], [0.5, -0.5, 0.5],
+                    [0.5, 1.5, 0.5], [2, 2, 2], [2, 2, 2]], np.float32)
+    seg = np.array([[0, 1], [2, 3], [4, 5], [6, 7]], np.uint32)
+    rad = np.array([0.1, 0.2, 0.15, 0.15, 0.05, 0.3, 0.2, 0.2], np.float32)
+    o = []
+    for x in np.linspace(-0.5, 2.5, 13):
+        for y in np.linspace(-0.7, 2.3, 13):
+            o.append(((x, y, -3.0), (0.0, 0.0, 1.0)))
+            o.append(((-3.0, y, x), (1.0, 0.0, 0.0)))
+            o.append(((x, -3.0, y), (0.0, 1.0, 0.0)))
+    o += [((-2.0, 0.0, 0.0), (1.0, 0.0, 0.0)), ((3.0, 0.0, 0.0), (-1.0, 0.0, 0.0)),
+          ((0.0, 0.5, -2.0), (0.0, 0.0, 1.0)), ((0.5, 0.0, 0.0), (0.0, 0.3, 1.0)),
+          ((0.5, 0.02, 0.01), (1.0, 0.0, 0.0)), ((0.5, 0.5, 0.5), (0.0, 1.0, 0.0)),
+          ((2.0, 2.0, 0.0), (0.0, 0.0, 1.0)), ((2.0, 2.0, 2.0), (0.0, 0.0, -1.0))]
+    rays = make_rays(np.array([a for a, _ in o], np.float32), np.array([b for _, b in o], np.float32))
+    for cap in (True, False):
+        out.append((f"axes-cap{int(cap)}", pos, seg, rad, 0.0, dict(cap=cap), rays))
+    # one, two and three lines (the root is a leaf), constant radius
+    for n in (1, 2, 3):
+        out.append((f"tiny{n}", pos[:2 * n], np.arange(2 * n, dtype=np.uint32).reshape(n, 2),
+                    None, 0.12, {}, rays))
+    # a chain of lines at midpoints 2^-k: every spatial split peels one off
+    k = np.arange(90, dtype=np.float64)
+    a = np.stack([2.0 ** -k, np.zeros_like(k), np.zeros_like(k)], 1)
+    b = a + np.array([0.0, 0.0, 2.0 ** -20])
+    pos2 = np.stack([a, b], 1).reshape(-1, 3).astype(np.float32)
+    seg2 = np.arange(2 * k.size, dtype=np.uint32).reshape(-1, 2)
+    eye = rng.uniform(-0.5, 1.5, size=(2000, 3)).astype(np.float32)
+    tgt = np.stack([2.0 ** -rng.uniform(0, 40, 2000), np.zeros(2000), np.zeros(2000)], 1)
+    rays2 = make_rays(eye, (tgt - eye).astype(np.float32))
+    out.append(("chain", pos2, seg2, None, 2.0 ** -22, dict(min_leaf=1), rays2))
+    # random segments with leaf and depth limits
+    p3, s3, r3 = line_segments(3000, seed=5)
+    eye = rng.uniform(-2, 2, size=(4000, 3)).astype(np.float32)
+    d = rng.normal(size=(4000, 3)).astype(np.float32)
+    rays3 = make_rays(eye, d)
+    out.append(("limits", p3, s3, r3, 0.0, dict(min_leaf=7, max_depth=6), rays3))
+    out.append(("leaf1", p3, s3, r3, 0.0, dict(min_leaf=1), rays3))
+    return out
