@@ -113,6 +113,15 @@ def make_workload(name):
                                         "hit + RGBA8 and depth write per step",
                             "elements": len(E["elements"]),
                             "prims": int(sum(E["prims"])), "rays": 1024 * 1024})
+    if name == "lines":
+        pos, seg, rad = S.line_strands(100000, 16, seed=123456)
+        rays = S.pinhole_rays(1024, 1024, (0.3, 0.5, 3.4), (0, 0, 0), fov_deg=40)
+        return dict(kind="lines", pos=pos, seg=seg, rad=rad, rays=rays,
+                    config={"workload": "hair1.6M: 100,000 strands x 16 capped cylinders "
+                                        "(1,600,000 lines, tapered radius 0.004) on the "
+                                        "unit sphere, 1024x1024 pinhole rays; closest hit "
+                                        "+ normal per step, accel resident (built once)",
+                            "lines": int(seg.shape[0]), "rays": int(rays.size)})
     if name == "texture":
         blocks, pool, gdim = S.sparse_pages()
         uvw = S.march_coords()
@@ -463,6 +472,27 @@ def cpu_reference_texture(W, nthreads=0):
             "reference" if use_ref else "port")
 
 
+def cpu_reference_lines(W, nthreads=0, stride=4):
+    """LineAccel::Traverse of every stride-th ray on the host: the
+    reference's own code (oracle/_ref) or else the restatement, OpenMP over
+    all cores; the accel is built once outside the timing.  Returns
+    (Mrays/s, build s, trace s scaled, rays traced, kind)."""
+    from oracle import oracle as O
+    use_ref = O.have_ref() and O.ref() is not None
+    if "_cpu_lines" not in W:
+        t0 = time.perf_counter()
+        W["_cpu_lines"] = (O.RefLines if use_ref else O.OracleLines)(W["pos"], W["seg"],
+                                                                      W["rad"])
+        W["_cpu_lines_build"] = time.perf_counter() - t0
+    acc = W["_cpu_lines"]
+    sample = W["rays"][::stride]
+    t0 = time.perf_counter()
+    acc.trace(sample, nthreads=nthreads)
+    tt = (time.perf_counter() - t0) * stride
+    return (W["rays"].size / tt / 1e6, W["_cpu_lines_build"], tt, sample.size,
+            "reference" if use_ref else "port")
+
+
 def run_reference_arm(args, W):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -470,7 +500,8 @@ def run_reference_arm(args, W):
     cores = os.cpu_count() or 1
     step = {"batched": cpu_reference_batched, "sphere": cpu_reference_particles,
             "frame": cpu_reference_frame, "scene": cpu_reference_scene,
-            "texture": cpu_reference_texture}.get(W["kind"], cpu_reference_step)
+            "texture": cpu_reference_texture, "lines": cpu_reference_lines}.get(
+                W["kind"], cpu_reference_step)
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
@@ -497,6 +528,10 @@ def run_reference_arm(args, W):
                   f"4th pixel ({ns} of {nr}) scaled to all, by the CPU restatement "
                   f"(OpenMP; the reference's RenderGraph needs its GL front end); median "
                   f"of {args.steps}")
+    if W["kind"] == "lines":
+        sample = (f"every 4th ray ({ns} of {nr}) per step through the reference's own "
+                  f"LineAccel::Traverse (OpenMP, {cores} threads; accel built once), "
+                  f"scaled to all rays; median of {args.steps}")
     if W["kind"] == "texture":
         sample = (f"every fetch ({ns}) per step through the reference's own "
                   f"SparseVolumeAccel (Build + Sample) over {cores} threads; median of "
@@ -505,7 +540,7 @@ def run_reference_arm(args, W):
         "impl": "reference",
         "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART,
                    "frame": METRIC_FRAME, "scene": METRIC_SCENE,
-                   "texture": METRIC_TEX}.get(W["kind"], METRIC),
+                   "texture": METRIC_TEX, "lines": METRIC_LINES}.get(W["kind"], METRIC),
         "value": round(value, 4), "unit": unit,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
@@ -531,8 +566,10 @@ METRIC_FRAME = "Mrays/s (frame: eye rays + closest hit + framebuffer write per s
 METRIC_SCENE = ("Mrays/s (scene frame: top-level build + eye rays + closest hit over "
                 "transformed elements + framebuffer write per step)")
 METRIC_TEX = "Mfetches/s (sparse volume texture3D fetch per step)"
+METRIC_LINES = "Mrays/s (capped-cylinder line accel: closest hit + normal per step)"
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
          "texture": "u8 texels / f64 block tree",
+         "lines": "f32 (f64 quadratic root)",
          "volume": "f32", "batched": "f32", "frame": "f32",
          "scene": "f64 transforms and top-level boxes / f32 + f64 element tests"}
 
@@ -787,6 +824,136 @@ def run_texture(args, W):
         print(json.dumps(line), flush=True)
     tex.close()
     dist_teardown()
+
+
+# ---------------------------------------------------------------- lines
+def run_lines(args, W):
+    """Closest hit + normal for every ray against the resident line accel
+    (device rays, hits and normals larger than L2).  e2e: rays from pinned
+    host memory in, hits and normals back, every step.  The host build is
+    timed once and reported beside the line."""
+    import torch
+
+    from surface_b200 import _lib
+    from surface_b200.lines import LineAccel, Lines
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
+    acc = LineAccel(device=dev.index)
+    t0 = time.perf_counter()
+    acc.Build(Lines(W["pos"], W["seg"], W["rad"]))
+    build_s = time.perf_counter() - t0
+    L = _lib.load()
+    rays_np = W["rays"]
+    n = rays_np.size
+    rays = torch.from_numpy(rays_np.view(np.float32).reshape(-1, 8)).to(dev)
+    hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def step():
+        acc.ctx.use_torch_stream()
+        check_line(L, acc, rays, n, hits, nrm)
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = L.srt_ctx_launch_count(acc.ctx.h)
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        barrier()
+        launches = L.srt_ctx_launch_count(acc.ctx.h) - launches0
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
+    ms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in ev)], dev)[0]
+    value = whole_job_mrays(n, world, ms)
+    # work counters of one untimed pass: the bytes a ray touches
+    stats = torch.zeros(3, dtype=torch.int64, device=dev)
+    acc.Traverse(rays, hits, stats=stats)
+    torch.cuda.synchronize()
+    nb, nl, nt = (int(x) for x in stats.cpu())
+
+    h_rays = torch.from_numpy(rays_np.view(np.float32).reshape(-1, 8).copy()).pin_memory()
+    h_hits = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+    h_nrm = torch.empty((n, 3), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        rays.copy_(h_rays, non_blocking=True)
+        step()
+        h_hits.copy_(hits, non_blocking=True)
+        h_nrm.copy_(nrm, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e = {"value": round(whole_job_mrays(n, world, e2e_ms), 3), "unit": "Mrays/s",
+           "h2d_bytes_per_step": int(h_rays.numel() * 4),
+           "d2h_bytes_per_step": int((h_hits.numel() + h_nrm.numel()) * 4),
+           "ms_per_step": round(e2e_ms, 3)}
+    # roofline: ray (32) + hit (16) + normal (12) per ray, 32 per branch
+    # popped, 32 per leaf popped and 64 per line tested
+    hbm, src = peaks()
+    alg = n * (32 + 16 + 12) + 32 * (nb + nl) + 64 * nt
+    traffic = None
+    prof = os.path.join(PROFILES, "line_trace_kernel.hair1.6M.md")
+    if os.path.exists(prof):
+        m = re.search(r"traffic_per_launch_bytes:\s*(\d+)", open(prof).read())
+        traffic = int(m.group(1)) if m else None
+    roofline = {"bound": "hbm", "kernel": "line_trace_kernel",
+                "achieved": round(alg / (ms * 1e-3) / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(alg / (ms * 1e-3) / 1e9 / hbm, 4), "peak_source": src,
+                "traffic": traffic, "algorithmic_bytes_per_launch": int(alg),
+                "per_ray": {"branches": round(nb / n, 2), "leaves": round(nl / n, 2),
+                            "line_tests": round(nt / n, 2)},
+                "note": "node and line bytes are served mostly from L2 (tree 180 MB)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        got = hits.cpu().numpy()[:: 97]
+        want, _ = O.OracleLines(W["pos"], W["seg"], W["rad"]).trace(rays_np[:: 97])
+        if not np.array_equal(got.view(np.uint32), want.view(np.float32).reshape(-1, 4)
+                              .view(np.uint32)):
+            raise SystemExit("line hits differ from the oracle")
+        v, _, tt, ns, kind = cpu_reference_lines(W)
+        cpu = {"value": round(v, 3), "unit": "Mrays/s", "cores": os.cpu_count(),
+               "kind": kind, "sample": f"every 4th ray ({ns}), OpenMP over "
+                                       f"{os.cpu_count()} threads, scaled to all rays",
+               "seconds": round(tt, 3)}
+    line = {"metric": METRIC_LINES, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": DTYPE["lines"], "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)"),
+            "build_ms_host": round(1e3 * build_s, 1), "clocks": clk.summary(), "e2e": e2e,
+            "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    acc.close()
+    dist_teardown()
+
+
+def check_line(L, acc, rays, n, hits, nrm):
+    from surface_b200._lib import check
+    check(L.srt_line_trace(acc.h, rays.data_ptr(), n, hits.data_ptr(), nrm.data_ptr(), None))
 
 
 # ---------------------------------------------------------------- batched
@@ -1653,7 +1820,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
                     choices=["tet", "tri", "particles", "volume", "batched", "frame",
-                             "scene", "texture"])
+                             "scene", "texture", "lines"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -1679,6 +1846,8 @@ def main():
         run_scene(args, W)
     elif args.workload == "texture":
         run_texture(args, W)
+    elif args.workload == "lines":
+        run_lines(args, W)
     else:
         run_ours(args, W)
 

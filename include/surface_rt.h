@@ -556,7 +556,9 @@ SRT_API srt_status srt_batch_config(srt_batch *b, int32_t *block,
  * defaults 4 and 512).  srt_line_trace replaces LineAccel::Traverse (:704):
  * closest hit per ray (t, u, v, line index; u = distance from the axis on a
  * cap, v = 0 / 1 on a cap or the position along the axis), normals (3 floats
- * per ray, BuildIntersection's, may be NULL).  Inputs may be host or device
+ * per ray, BuildIntersection's, may be NULL); stats (device memory, NULL
+ * or 3 uint64 accumulated: branches popped, leaves popped, lines tested).
+ * Inputs may be host or device
  * memory.  srt_line_bbox replaces LineAccel::BoundingBox (:776),
  * srt_line_dump LineAccel::Dump (:343, the same file format); srt_line_export
  * copies the tree in the Dump record layout (40 bytes per node) and the line
@@ -569,7 +571,7 @@ SRT_API srt_status srt_line_build(srt_line_accel *accel, const float *positions,
                                   const uint32_t *segments, size_t nlines, int32_t min_leaf,
                                   int32_t max_depth, int32_t cap);
 SRT_API srt_status srt_line_trace(srt_line_accel *accel, const srt_ray *rays, size_t n,
-                                  srt_hit *hits, float *normals);
+                                  srt_hit *hits, float *normals, uint64_t *stats);
 SRT_API srt_status srt_line_bbox(srt_line_accel *accel, double bmin[3], double bmax[3]);
 SRT_API srt_status srt_line_info(srt_line_accel *accel, uint64_t *nlines, uint64_t *nnodes,
                                  int32_t *depth);

@@ -143,7 +143,7 @@ _SIGS = {
     "srt_line_create": [_P, C.POINTER(_P)],
     "srt_line_destroy": [_P],
     "srt_line_build": [_P, _P, _SZ, _P, C.c_float, _P, _SZ, C.c_int32, C.c_int32, C.c_int32],
-    "srt_line_trace": [_P, _P, _SZ, _P, _P],
+    "srt_line_trace": [_P, _P, _SZ, _P, _P, _P],
     "srt_line_bbox": [_P, _P, _P],
     "srt_line_info": [_P, _P, _P, _P],
     "srt_line_export": [_P, _P, _P],

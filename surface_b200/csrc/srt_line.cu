@@ -12,7 +12,8 @@
 // per-line terms of CylinderIsect (end points, max radius, |d|^2, the cap
 // plane normal and offsets), computed with the reference's float operations.
 //
-// Trace (LineAccel::Traverse, :704-774): one thread per ray, the stack of
+// Trace (LineAccel::Traverse, :704-774): one thread per ray (in a Morton
+// order of the rays for large batches), the stack of
 // the reference (a popped branch tests its own box against the closest hit
 // so far, then pushes far and near children by the sign of the ray's
 // direction on the branch's axis), every line of a popped leaf tested in
@@ -378,13 +379,19 @@ __device__ __forceinline__ LNode load_node(const LNode *p) {
   return n;
 }
 
-template <int STACK>
+// One thread per ray (grid-strided).  order (may be null): thread k traces
+// ray order[k].  STATS: count popped branches, popped leaves and line tests
+// into stats[0..2].
+template <int STACK, bool STATS>
 __global__ void __launch_bounds__(128)
 line_trace_kernel(const LNode *__restrict__ nodes, const LineRec *__restrict__ recs, bool cap,
-                  const srt_ray *__restrict__ rays, size_t n, srt_hit *__restrict__ hits,
-                  float *__restrict__ normals) {
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
+                  const srt_ray *__restrict__ rays, const uint32_t *__restrict__ order,
+                  size_t n, srt_hit *__restrict__ hits, float *__restrict__ normals,
+                  unsigned long long *__restrict__ stats) {
+  unsigned long long nb = 0, nl = 0, nt = 0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = order ? (size_t)__ldg(&order[k]) : k;
     const float4 *rq = reinterpret_cast<const float4 *>(rays + i);
     const float4 r0 = __ldg(rq), r1 = __ldg(rq + 1);
     RayL R;
@@ -410,6 +417,7 @@ line_trace_kernel(const LNode *__restrict__ nodes, const LineRec *__restrict__ r
       const LNode nd = load_node(nodes + stack[sp]);
       sp--;
       if (!(nd.w1 & kLineLeaf)) {
+        if (STATS) nb++;
         if (box_hit(nd, R, hitT)) {
           const int axis = (int)(nd.w1 >> 29);
           const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
@@ -421,6 +429,10 @@ line_trace_kernel(const LNode *__restrict__ nodes, const LineRec *__restrict__ r
         float t = it;
         bool any = false;
         const uint32_t first = nd.w0, cnt = nd.w1 & ~kLineLeaf;
+        if (STATS) {
+          nl++;
+          nt += cnt;
+        }
         for (uint32_t j = 0; j < cnt; j++) {
           const LineRec L = load_line(recs + first + j);
           float u, v;
@@ -470,6 +482,18 @@ line_trace_kernel(const LNode *__restrict__ nodes, const LineRec *__restrict__ r
         for (int k = 0; k < 3; k++) normals[3 * i + k] = 0.0f;
     }
     reinterpret_cast<float4 *>(hits)[i] = make_float4(h.t, h.u, h.v, __uint_as_float(h.prim));
+  }
+  if (STATS) {
+    for (int o = 16; o > 0; o >>= 1) {
+      nb += __shfl_xor_sync(0xffffffffu, nb, o);
+      nl += __shfl_xor_sync(0xffffffffu, nl, o);
+      nt += __shfl_xor_sync(0xffffffffu, nt, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      atomicAdd(&stats[0], nb);
+      atomicAdd(&stats[1], nl);
+      atomicAdd(&stats[2], nt);
+    }
   }
 }
 
@@ -622,8 +646,12 @@ SRT_API srt_status srt_line_build(srt_line_accel *a, const float *positions, siz
 }
 
 SRT_API srt_status srt_line_trace(srt_line_accel *a, const srt_ray *rays, size_t n,
-                                  srt_hit *hits, float *normals) {
+                                  srt_hit *hits, float *normals, uint64_t *stats) {
   if (!a || (n && (!rays || !hits))) return SRT_ERR_INVALID;
+  if (stats && !is_device_ptr(stats)) {
+    set_error("stats must be device memory");
+    return SRT_ERR_INVALID;
+  }
   if (!a->built) {
     set_error("line accel not built");
     return SRT_ERR_INVALID;
@@ -656,10 +684,24 @@ SRT_API srt_status srt_line_trace(srt_line_accel *a, const srt_ray *rays, size_t
   const LNode *nd = a->dnodes.as<LNode>();
   const LineRec *rc = a->drecs.as<LineRec>();
   const srt_ray *rr = static_cast<const srt_ray *>(dr);
-  if (a->depth + 2 <= 64)
-    line_trace_kernel<64><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, n, dh, dn);
+  unsigned long long *st = reinterpret_cast<unsigned long long *>(stats);
+  // a coherent ray order (a Morton curve over origin and direction) keeps
+  // the lanes of a warp on nearby paths; the hits do not depend on it
+  const uint32_t *ord = nullptr;
+  if (n >= 32768 && (s = ray_order(ctx, rr, n, &ord)) != SRT_OK) return s;
+  const bool shallow = a->depth + 2 <= 64;
+  if (shallow && !st)
+    line_trace_kernel<64, false><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, ord, n, dh,
+                                                                 dn, st);
+  else if (shallow)
+    line_trace_kernel<64, true><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, ord, n, dh,
+                                                                dn, st);
+  else if (!st)
+    line_trace_kernel<520, false><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, ord, n, dh,
+                                                                  dn, st);
   else
-    line_trace_kernel<520><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, n, dh, dn);
+    line_trace_kernel<520, true><<<grid, 128, 0, ctx->stream>>>(nd, rc, a->cap, rr, ord, n, dh,
+                                                                 dn, st);
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "line trace");
   if (!hdev) cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, ctx->stream);

@@ -92,8 +92,9 @@ class LineAccel:
         check(self.L.srt_line_dump(self.h, str(filename).encode()))
         return True
 
-    def Traverse(self, rays, hits=None, want_normal=False):
-        """Closest hit per ray (batched LineAccel::Traverse)."""
+    def Traverse(self, rays, hits=None, want_normal=False, stats=None):
+        """Closest hit per ray (batched LineAccel::Traverse).  stats: a CUDA
+        int64 tensor of 3 counters (branches, leaves, line tests) to add to."""
         if not self.built:
             raise SurfaceError(_lib.SRT_ERR_INVALID, "accel not built")
         if _is_cuda(rays):
@@ -114,7 +115,8 @@ class LineAccel:
             self.ctx.use_own_stream()
             rp, hp = r.ctypes.data, hits.ctypes.data
             np_ = nrm.ctypes.data if nrm is not None else None
-        check(self.L.srt_line_trace(self.h, rp, n, hp, np_))
+        check(self.L.srt_line_trace(self.h, rp, n, hp, np_,
+                                    None if stats is None else stats.data_ptr()))
         return (hits, nrm) if want_normal else hits
 
     def close(self):
