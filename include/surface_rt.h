@@ -578,6 +578,33 @@ SRT_API srt_status srt_line_info(srt_line_accel *accel, uint64_t *nlines, uint64
 SRT_API srt_status srt_line_export(srt_line_accel *accel, void *nodes, uint32_t *indices);
 SRT_API srt_status srt_line_dump(srt_line_accel *accel, const char *path);
 
+/* ---------------------------------------------------------------- solids
+ * SolidAccel (render/render_accel_solid.{h,cc}) over Solid
+ * (render/render_prim_solid.h): pyramids (verts_per_solid 5), prisms (6),
+ * hexahedra (8).  srt_solid_build replaces SolidAccel::Build32
+ * (render_accel_solid.cc:1795; the same tree and solid order, for 2 or more
+ * solids -- the reference switches to its SAH Build below 1024);
+ * srt_solid_trace replaces SolidAccel::Traverse (:2345): per ray the
+ * nearest entry or exit point (t, solid in hits[i].prim; u = v = 0, which
+ * the reference leaves unset), skipping the solid named by prev_prim, and
+ * optionally the point's normal and position (3 floats per ray each, NULL
+ * to skip).  Inputs may be host or device memory.  srt_solid_bbox replaces
+ * SolidAccel::BoundingBox, srt_solid_dump SolidAccel::Dump (:2126, the same
+ * file format); srt_solid_export copies the tree in the Dump record layout
+ * (40 bytes per node) and the solid order. */
+typedef struct srt_solid_accel srt_solid_accel;
+SRT_API srt_status srt_solid_create(srt_ctx *ctx, srt_solid_accel **out);
+SRT_API srt_status srt_solid_destroy(srt_solid_accel *accel);
+SRT_API srt_status srt_solid_build(srt_solid_accel *accel, int32_t verts_per_solid,
+                                   const float *vertices, size_t nverts,
+                                   const uint32_t *indices, size_t nsolids);
+SRT_API srt_status srt_solid_trace(srt_solid_accel *accel, const srt_ray *rays, size_t n,
+                                   srt_hit *hits, float *normals, float *positions);
+SRT_API srt_status srt_solid_bbox(srt_solid_accel *accel, double bmin[3], double bmax[3]);
+SRT_API srt_status srt_solid_info(srt_solid_accel *accel, uint64_t *nsolids, uint64_t *nnodes);
+SRT_API srt_status srt_solid_export(srt_solid_accel *accel, void *nodes, uint32_t *indices);
+SRT_API srt_status srt_solid_dump(srt_solid_accel *accel, const char *path);
+
 #ifdef __cplusplus
 }
 #endif

@@ -123,6 +123,13 @@ def lib():
         L.so_line_depth.argtypes = [_P]
         L.so_line_export.argtypes = [_P, _P, _P]
         L.so_line_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int]
+        L.so_solid_build.restype = _P
+        L.so_solid_build.argtypes = [C.c_int, _P, _P, _SZ]
+        L.so_solid_free.argtypes = [_P]
+        L.so_solid_num_nodes.restype = _SZ
+        L.so_solid_num_nodes.argtypes = [_P]
+        L.so_solid_export.argtypes = [_P, _P, _P]
+        L.so_solid_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, C.c_int]
         _ORACLE = L
     return _ORACLE
 
@@ -187,6 +194,12 @@ def ref():
         L.ref_line_dump.argtypes = [_P, C.c_char_p]
         L.ref_line_bbox.argtypes = [_P, _P, _P]
         L.ref_line_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
+        L.ref_solid_build.restype = _P
+        L.ref_solid_build.argtypes = [C.c_int, _P, _P, _SZ]
+        L.ref_solid_free.argtypes = [_P]
+        L.ref_solid_dump.argtypes = [_P, C.c_char_p]
+        L.ref_solid_bbox.argtypes = [_P, _P, _P]
+        L.ref_solid_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, C.c_int, C.c_int]
         _REF = L
     return _REF
 
@@ -946,3 +959,107 @@ class RefLines(_LinesBase):
             self.L.ref_line_free(self.h)
         except Exception:  # noqa: BLE001
             pass
+
+
+# ---------------------------------------------------------------- solids
+SOLID_NODE_DTYPE = LINE_NODE_DTYPE  # SolidNode: the same 40-byte record
+
+
+def parse_solid_dump(raw):
+    """SolidAccel::Dump(): (nodes SOLID_NODE_DTYPE, indices uint32)."""
+    return parse_line_dump(raw)
+
+
+class OracleSolids:
+    """The restatement of SolidAccel::Build32 / Traverse (nv = 5 pyramids,
+    6 prisms, 8 hexahedra)."""
+
+    def __init__(self, nv, verts, indices):
+        self.nv = int(nv)
+        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        self.n = self.ix.size // self.nv
+        self.h = lib().so_solid_build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
+
+    def export(self):
+        nn = lib().so_solid_num_nodes(self.h)
+        nodes = np.zeros(nn, SOLID_NODE_DTYPE)
+        idx = np.zeros(self.n, np.uint32)
+        lib().so_solid_export(self.h, _ptr(nodes), _ptr(idx))
+        return nodes, idx
+
+    def trace(self, rays, nthreads=0):
+        """(hits, normals, positions)."""
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        nrm = np.zeros((rays.size, 3), np.float32)
+        pos = np.zeros((rays.size, 3), np.float32)
+        lib().so_solid_trace(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(nrm), _ptr(pos),
+                             nthreads)
+        return hits, nrm, pos
+
+    def __del__(self):
+        try:
+            lib().so_solid_free(self.h)
+        except Exception:  # noqa: BLE001
+            pass
+
+
+class RefSolids:
+    """The reference's own SolidAccel (Build32, Traverse, Dump, BoundingBox)."""
+
+    def __init__(self, nv, verts, indices):
+        L = ref()
+        if L is None:
+            raise RuntimeError("reference harness not built")
+        self.L = L
+        self.nv = int(nv)
+        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        self.n = self.ix.size // self.nv
+        self.h = L.ref_solid_build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
+
+    def dump(self):
+        with tempfile.TemporaryDirectory() as td:
+            path = os.path.join(td, "solids.bin")
+            self.L.ref_solid_dump(self.h, path.encode())
+            with open(path, "rb") as fp:
+                return parse_solid_dump(fp.read())
+
+    def bbox(self):
+        mn = np.zeros(3)
+        mx = np.zeros(3)
+        self.L.ref_solid_bbox(self.h, _ptr(mn), _ptr(mx))
+        return mn, mx
+
+    def trace(self, rays, nthreads=0, chunk=64):
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        nrm = np.zeros((rays.size, 3), np.float32)
+        pos = np.zeros((rays.size, 3), np.float32)
+        self.L.ref_solid_trace(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(nrm), _ptr(pos),
+                               nthreads, chunk)
+        return hits, nrm, pos
+
+    def __del__(self):
+        try:
+            self.L.ref_solid_free(self.h)
+        except Exception:  # noqa: BLE001
+            pass
+
+
+def tree_canonical(nodes, root=0):
+    """A 40-byte-node tree (LineNode / SolidNode) as a pre-order list of its
+    nodes from the root, independent of the record order: branches (axis,
+    box) and leaves (box, count, first)."""
+    out, stack = [], [root]
+    while stack:
+        nd = nodes[stack.pop()]
+        if nd["flag"] == 1:
+            out.append(("L", nd["bmin"].tobytes(), nd["bmax"].tobytes(), int(nd["data"][0]),
+                        int(nd["data"][1])))
+        else:
+            out.append(("B", int(nd["axis"]), nd["bmin"].tobytes(), nd["bmax"].tobytes()))
+            stack.append(int(nd["data"][1]))
+            stack.append(int(nd["data"][0]))
+    return out

@@ -28,6 +28,7 @@
 
 #include "render_accel_line.h"
 #include "render_accel_particle.h"
+#include "render_accel_solid.h"
 #include "render_accel_tetra.h"
 #include "render_accel_triangle.h"
 #include "render_accel_volume.h"
@@ -563,5 +564,62 @@ REF_API void ref_line_trace(void *p, const RayRec *rays, size_t n, HitRec *hits,
     hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
     if (normals)
       for (int k = 0; k < 3; k++) normals[3 * i + k] = hit ? isect.normal[k] : 0.0f;
+  }
+}
+
+// ---------------------------------------------------------------- solids
+// SolidAccel (render/render_accel_solid.cc): Build32 (its SAH Build below
+// 1024 solids), Traverse with its Intersection's t, position and normal
+// (u and v are left unset by the reference's solid tests: reported as 0).
+struct SolidHandle {
+  Solid solids;
+  SolidAccel accel;
+};
+
+REF_API void *ref_solid_build(int nv, const float *verts, const uint32_t *indices, size_t n) {
+  SolidHandle *h = new SolidHandle();
+  memset(&h->solids, 0, sizeof(h->solids));
+  h->solids.numVertsPerSolid = nv;
+  h->solids.numSolids = n;
+  h->solids.vertices = verts;
+  h->solids.dvertices = nullptr;
+  h->solids.isDoublePrecisionPos = false;
+  h->solids.indices = const_cast<uint32_t *>(indices);
+  SolidBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build32(&h->solids, opt);
+  }
+  return h;
+}
+
+REF_API void ref_solid_free(void *p) { delete static_cast<SolidHandle *>(p); }
+
+REF_API int ref_solid_dump(void *p, const char *path) {
+  return static_cast<SolidHandle *>(p)->accel.Dump(path) ? 0 : 1;
+}
+
+REF_API void ref_solid_bbox(void *p, double bmin[3], double bmax[3]) {
+  static_cast<SolidHandle *>(p)->accel.BoundingBox(bmin, bmax);
+}
+
+REF_API void ref_solid_trace(void *p, const RayRec *rays, size_t n, HitRec *hits,
+                             float *normals, float *positions, int nthreads, int chunk) {
+  const SolidAccel &acc = static_cast<SolidHandle *>(p)->accel;
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+  if (chunk <= 0) chunk = 64;
+#pragma omp parallel for schedule(dynamic, chunk) num_threads(nthreads)
+  for (long long i = 0; i < (long long)n; i++) {
+    Ray ray = make_ray(rays[i], nullptr);
+    Intersection isect;
+    bool hit = acc.Traverse(isect, ray);
+    hits[i].t = hit ? isect.t : std::numeric_limits<float>::max();
+    hits[i].u = 0.0f;
+    hits[i].v = 0.0f;
+    hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
+    for (int k = 0; k < 3; k++) {
+      if (normals) normals[3 * i + k] = hit ? isect.normal[k] : 0.0f;
+      if (positions) positions[3 * i + k] = hit ? isect.position[k] : 0.0f;
+    }
   }
 }

@@ -2983,3 +2983,400 @@ SO_API void so_line_trace(const so_lines *L, const so_ray *rays, size_t n, so_hi
   for (long long i = 0; i < (long long)n; i++)
     line_trace_one(L, &rays[i], &hits[i], normals ? &normals[3 * i] : NULL);
 }
+
+/* ------------------------------------------------------------------------ */
+/* Solids: SolidAccel (render/render_accel_solid.cc) -- pyramids (5          */
+/* vertices), prisms (6) and hexahedra (8).  Build32 (:1795-2124): the LBVH  */
+/* of the tetrahedra with the solid's centroid (the running sum of its       */
+/* vertices times 1.0f / nv); Traverse (:2345-2435): every popped node tests */
+/* its own box, leaves test their solids in double (Intersect*D, :455-717).  */
+/* The reference's TestLeafNode returns a shadowed flag (always false), so   */
+/* the walk never lowers its distance bound: no box is culled by distance.   */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+  float bmin[3], bmax[3];
+  int32_t flag, axis;
+  uint32_t data[2];
+} so_solid_node; /* 40 bytes, the reference's SolidNode and Dump() record */
+
+typedef struct {
+  int nv;
+  const float *v;
+  const uint32_t *ix;
+  size_t n;
+  so_solid_node *nodes;
+  size_t nnodes, ncap;
+  uint32_t *sidx, *code, *child;
+  uint8_t *lt, *rt;
+} so_solids;
+
+/* Leaf box over sorted solids [l, r) (ComputeBoundingBox30, :1121-1169). */
+static void solid_box(const so_solids *S, size_t l, size_t r, float bmin[3], float bmax[3]) {
+  const float eps = FLT_EPSILON * 16;
+  const uint32_t f0 = S->ix[(size_t)S->nv * S->sidx[l]];
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = S->v[3 * (size_t)f0 + k] - eps;
+    bmax[k] = S->v[3 * (size_t)f0 + k] + eps;
+  }
+  for (size_t i = l; i < r; i++)
+    for (int j = 0; j < S->nv; j++) {
+      const uint32_t f = S->ix[(size_t)S->nv * S->sidx[i] + j];
+      for (int k = 0; k < 3; k++) {
+        const float lo = S->v[3 * (size_t)f + k] - eps, hi = S->v[3 * (size_t)f + k] + eps;
+        if (bmin[k] > lo) bmin[k] = lo;
+        if (bmax[k] < hi) bmax[k] = hi;
+      }
+    }
+}
+
+static inline int solid_axis(uint32_t code) { return (clz32(code) - 2) % 3; }
+
+static size_t solid_push(so_solids *S) {
+  if (S->nnodes == S->ncap) {
+    S->ncap = S->ncap ? 2 * S->ncap : 64;
+    S->nodes = (so_solid_node *)realloc(S->nodes, S->ncap * sizeof(so_solid_node));
+  }
+  memset(&S->nodes[S->nnodes], 0, sizeof(so_solid_node));
+  return S->nnodes++;
+}
+
+/* BuildTreeRecursive32 (:1361-1453): keys [l, r] inclusive. */
+static size_t solid_emit(so_solids *S, uint32_t root, uint32_t l, uint32_t r, int leaf,
+                         int depth, float bmin[3], float bmax[3]) {
+  if (leaf || (r - l) <= 4 || depth > 22) {
+    const size_t off = solid_push(S);
+    solid_box(S, l, (size_t)r + 1, bmin, bmax);
+    so_solid_node *nd = &S->nodes[off];
+    memcpy(nd->bmin, bmin, 12);
+    memcpy(nd->bmax, bmax, 12);
+    nd->flag = 1;
+    nd->data[0] = r + 1 - l;
+    nd->data[1] = l;
+    return off;
+  }
+  const uint32_t mid = S->child[root];
+  const size_t off = solid_push(S);
+  float lb0[3], lb1[3], rb0[3], rb1[3];
+  const size_t left = solid_emit(S, mid, l, mid, S->lt[root], depth + 1, lb0, lb1);
+  const size_t right = solid_emit(S, mid + 1, mid + 1, r, S->rt[root], depth + 1, rb0, rb1);
+  for (int k = 0; k < 3; k++) { /* MergeBoundingBox: std::min / std::max */
+    bmin[k] = (rb0[k] < lb0[k]) ? rb0[k] : lb0[k];
+    bmax[k] = (lb1[k] < rb1[k]) ? rb1[k] : lb1[k];
+  }
+  so_solid_node *nd = &S->nodes[off];
+  nd->axis = solid_axis(S->code[root]);
+  nd->data[0] = (uint32_t)left;
+  nd->data[1] = (uint32_t)right;
+  memcpy(nd->bmin, bmin, 12);
+  memcpy(nd->bmax, bmax, 12);
+  return off;
+}
+
+SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, size_t n) {
+  so_solids *S = (so_solids *)calloc(1, sizeof(so_solids));
+  S->nv = nv;
+  S->v = v;
+  S->ix = ix;
+  S->n = n;
+  S->sidx = (uint32_t *)malloc((n + 1) * 4);
+  S->code = (uint32_t *)malloc((n + 1) * 4);
+  S->child = (uint32_t *)malloc((n + 1) * 4);
+  S->lt = (uint8_t *)malloc(n + 1);
+  S->rt = (uint8_t *)malloc(n + 1);
+  if (n < 2) return S;
+  /* scene box: every vertex -+ FLT_EPSILON * 16 (ComputeBoundingBoxOMP, :1171-1262) */
+  const float eps = FLT_EPSILON * 16;
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; k++) {
+    lo[k] = v[3 * (size_t)ix[0] + k] - eps;
+    hi[k] = v[3 * (size_t)ix[0] + k] + eps;
+  }
+  for (size_t i = 0; i < n * (size_t)nv; i++)
+    for (int k = 0; k < 3; k++) {
+      lo[k] = fmin_ref(lo[k], v[3 * (size_t)ix[i] + k] - eps);
+      hi[k] = fmax_ref(hi[k], v[3 * (size_t)ix[i] + k] + eps);
+    }
+  /* CalculateMortonCodesSolidFloat30 (render/render_prefix_tree_util.cc:347-382) */
+  float inv[3];
+  morton_inv(lo, hi, inv);
+  const float invdiv = 1.0f / (float)nv;
+  for (size_t i = 0; i < n; i++) {
+    float c[3] = {0.0f, 0.0f, 0.0f};
+    for (int j = 0; j < nv; j++)
+      for (int k = 0; k < 3; k++) c[k] = c[k] + v[3 * (size_t)ix[(size_t)nv * i + j] + k];
+    for (int k = 0; k < 3; k++) c[k] *= invdiv;
+    S->code[i] = morton_of(c, lo, inv);
+    S->sidx[i] = (uint32_t)i;
+  }
+  so_sort_pairs(S->code, S->sidx, n);
+  so_karras(S->code, n, S->child, S->lt, S->rt);
+  solid_push(S); /* the root, filled below */
+  float lb0[3], lb1[3], rb0[3], rb1[3];
+  const uint32_t mid = S->child[0];
+  const size_t left = solid_emit(S, mid, 0, mid, S->lt[0], 0, lb0, lb1);
+  const size_t right = solid_emit(S, mid + 1, mid + 1, (uint32_t)n - 1, S->rt[0], 0, rb0, rb1);
+  so_solid_node *rt = &S->nodes[0];
+  for (int k = 0; k < 3; k++) {
+    rt->bmin[k] = (rb0[k] < lb0[k]) ? rb0[k] : lb0[k];
+    rt->bmax[k] = (lb1[k] < rb1[k]) ? rb1[k] : lb1[k];
+  }
+  rt->axis = solid_axis(S->code[0]);
+  rt->data[0] = (uint32_t)left;
+  rt->data[1] = (uint32_t)right;
+  return S;
+}
+
+SO_API void so_solid_free(so_solids *S) {
+  if (!S) return;
+  free(S->nodes);
+  free(S->sidx);
+  free(S->code);
+  free(S->child);
+  free(S->lt);
+  free(S->rt);
+  free(S);
+}
+
+SO_API size_t so_solid_num_nodes(const so_solids *S) { return S->nnodes; }
+
+SO_API void so_solid_export(const so_solids *S, so_solid_node *nodes, uint32_t *idx) {
+  if (nodes) memcpy(nodes, S->nodes, S->nnodes * sizeof(so_solid_node));
+  if (idx) memcpy(idx, S->sidx, S->n * 4);
+}
+
+/* --- the Pluecker tests in double ---------------------------------------- */
+typedef struct {
+  float pos[3], nrm[3];
+  float t;
+} so_sisect;
+
+static inline d3 dsub(d3 a, d3 b) { return (d3){a.x - b.x, a.y - b.y, a.z - b.z}; }
+static inline d3 dcross(d3 a, d3 b) {
+  return (d3){a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+static inline double ddot(d3 a, d3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+static inline d3 dscale(d3 a, double f) { return (d3){a.x * f, a.y * f, a.z * f}; }
+static inline d3 dadd(d3 a, d3 b) { return (d3){a.x + b.x, a.y + b.y, a.z + b.z}; }
+
+/* normalize (:85): a / |a| in double, then to float. */
+static inline void s_unit(d3 a, float out[3]) {
+  const double len = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+  out[0] = (float)(a.x / len);
+  out[1] = (float)(a.y / len);
+  out[2] = (float)(a.z / len);
+}
+
+/* SetCrossPoint_Sq (double, :438-444): the crossing point of a quad face. */
+static inline void s_quad_point(float out[3], d3 v0, d3 v1, d3 v2, double ws0, double ws1,
+                                double ws2, double ws3, d3 e2, d3 e3, d3 dir) {
+  const double w = ws2 + ws3 + ddot(dcross(e2, e3), dir);
+  const d3 p = dadd(dadd(dscale(v2, ws0), dscale(v0, ws1)), dscale(v1, w));
+  const double den = ws0 + ws1 + w;
+  out[0] = (float)(p.x / den);
+  out[1] = (float)(p.y / den);
+  out[2] = (float)(p.z / den);
+}
+
+/* The crossing point of a triangle face: toreal3(a*wa + b*wb + c*wc) / (float)(wa + wb + wc),
+ * the weighted sum in double, the division in float. */
+static inline void s_tri_point(float out[3], d3 a, double wa, d3 b, double wb, d3 c, double wc,
+                               double den) {
+  const d3 p = dadd(dadd(dscale(a, wa), dscale(b, wb)), dscale(c, wc));
+  const float f = (float)den;
+  out[0] = (float)p.x / f;
+  out[1] = (float)p.y / f;
+  out[2] = (float)p.z / f;
+}
+
+static inline void s_weights(int ne, const d3 *e, const d3 *vv, int mod, d3 dir, d3 org,
+                             double *ws, int cw[2][12]) {
+  const d3 rpc = dcross(dir, org);
+  for (int i = 0; i < ne; i++) {
+    const d3 epc = dcross(e[i], vv[i % mod]);
+    ws[i] = ddot(dir, epc) + ddot(e[i], rpc);
+    cw[0][i] = ws[i] >= 0;
+    cw[1][i] = ws[i] <= 0;
+  }
+}
+
+/* t of both points along the last axis with |dir| > 0.1 (:500-504). */
+static inline void s_params(so_sisect is[2], d3 org, d3 dir) {
+  const double o[3] = {org.x, org.y, org.z}, d[3] = {dir.x, dir.y, dir.z};
+  for (int j = 0; j < 3; j++)
+    if (d[j] > 0.1 || d[j] < -0.1) {
+      is[0].t = (float)(((double)is[0].pos[j] - o[j]) / d[j]);
+      is[1].t = (float)(((double)is[1].pos[j] - o[j]) / d[j]);
+    }
+  for (int k = 0; k < 3; k++) is[1].nrm[k] = -1.0f * is[1].nrm[k];
+}
+
+/* IntersectPyramidD (:455-505). */
+static int s_pyramid(d3 org, d3 dir, const d3 *v, so_sisect is[2]) {
+  d3 e[8] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[3], v[2]), dsub(v[0], v[3]),
+             dsub(v[4], v[0]), dsub(v[4], v[1]), dsub(v[4], v[2]), dsub(v[4], v[3])};
+  double ws[12];
+  int cw[2][12];
+  s_weights(8, e, v, 4, dir, org, ws, cw);
+  for (int i = 1, n = 0; n < 2; i--, n++) {
+    if (cw[i][0] && cw[i][1] && cw[i][2] && cw[i][3]) {
+      s_quad_point(is[n].pos, v[0], v[1], v[2], ws[0], ws[1], ws[2], ws[3], e[2], e[3], dir);
+      s_unit(dcross(e[1], e[0]), is[n].nrm);
+    } else if (cw[n][0] && cw[i][4] && cw[n][5]) {
+      s_tri_point(is[n].pos, v[4], -ws[0], v[1], ws[4], v[0], -ws[5], -ws[0] + ws[4] - ws[5]);
+      s_unit(dcross(e[4], e[0]), is[n].nrm);
+    } else if (cw[n][1] && cw[i][5] && cw[n][6]) {
+      s_tri_point(is[n].pos, v[4], -ws[1], v[2], ws[5], v[1], -ws[6], -ws[1] + ws[5] - ws[6]);
+      s_unit(dcross(e[5], e[1]), is[n].nrm);
+    } else if (cw[n][2] && cw[i][6] && cw[n][7]) {
+      s_tri_point(is[n].pos, v[4], -ws[2], v[3], ws[6], v[2], -ws[7], -ws[2] + ws[6] - ws[7]);
+      s_unit(dcross(e[6], e[2]), is[n].nrm);
+    } else if (cw[n][3] && cw[i][7] && cw[n][4]) {
+      s_tri_point(is[n].pos, v[4], -ws[3], v[0], ws[7], v[3], -ws[4], -ws[3] + ws[7] - ws[4]);
+      s_unit(dcross(e[7], e[3]), is[n].nrm);
+    } else {
+      return 0;
+    }
+  }
+  s_params(is, org, dir);
+  return 1;
+}
+
+/* IntersectPrismD (:559-611). */
+static int s_prism(d3 org, d3 dir, const d3 *v, so_sisect is[2]) {
+  d3 e[9] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[0], v[2]),
+             dsub(v[4], v[3]), dsub(v[5], v[4]), dsub(v[3], v[5]),
+             dsub(v[3], v[0]), dsub(v[4], v[1]), dsub(v[5], v[2])};
+  double ws[12];
+  int cw[2][12];
+  s_weights(9, e, v, 6, dir, org, ws, cw);
+  for (int i = 0, n = 1; i < 2; i++, n--) {
+    if (cw[n][0] && cw[n][1] && cw[n][2]) {
+      s_tri_point(is[i].pos, v[2], ws[0], v[0], ws[1], v[1], ws[2], ws[0] + ws[1] + ws[2]);
+      s_unit(dcross(e[0], e[1]), is[i].nrm);
+    } else if (cw[i][3] && cw[i][4] && cw[i][5]) {
+      s_tri_point(is[i].pos, v[5], ws[3], v[3], ws[4], v[4], ws[5], ws[3] + ws[4] + ws[5]);
+      s_unit(dcross(e[3], e[4]), is[i].nrm);
+    } else if (cw[i][2] && cw[i][6] && cw[n][5] && cw[n][8]) {
+      s_quad_point(is[i].pos, v[2], v[0], v[3], ws[2], ws[6], -ws[5], -ws[8], e[5], e[8], dir);
+      s_unit(dcross(e[2], e[6]), is[i].nrm);
+    } else if (cw[i][0] && cw[i][7] && cw[n][3] && cw[n][6]) {
+      s_quad_point(is[i].pos, v[0], v[1], v[4], ws[0], ws[7], -ws[3], -ws[6], e[3], e[6], dir);
+      s_unit(dcross(e[0], e[7]), is[i].nrm);
+    } else if (cw[i][1] && cw[i][8] && cw[n][4] && cw[n][7]) {
+      s_quad_point(is[i].pos, v[1], v[2], v[5], ws[1], ws[8], -ws[4], -ws[7], e[4], e[7], dir);
+      s_unit(dcross(e[1], e[8]), is[i].nrm);
+    } else {
+      return 0;
+    }
+  }
+  s_params(is, org, dir);
+  return 1;
+}
+
+/* IntersectHexaD (:664-716). */
+static int s_hexa(d3 org, d3 dir, const d3 *v, so_sisect is[2]) {
+  d3 e[12] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[3], v[2]), dsub(v[0], v[3]),
+              dsub(v[5], v[4]), dsub(v[6], v[5]), dsub(v[7], v[6]), dsub(v[4], v[7]),
+              dsub(v[4], v[0]), dsub(v[5], v[1]), dsub(v[6], v[2]), dsub(v[7], v[3])};
+  double ws[12];
+  int cw[2][12];
+  s_weights(12, e, v, 8, dir, org, ws, cw);
+  for (int i = 0, n = 1; i < 2; i++, n--) {
+    if (cw[n][0] && cw[n][1] && cw[n][2] && cw[n][3]) {
+      s_quad_point(is[i].pos, v[0], v[1], v[2], ws[0], ws[1], ws[2], ws[3], e[2], e[3], dir);
+      s_unit(dcross(e[0], e[1]), is[i].nrm);
+    } else if (cw[i][4] && cw[i][5] && cw[i][6] && cw[i][7]) {
+      s_quad_point(is[i].pos, v[4], v[5], v[6], ws[4], ws[5], ws[6], ws[7], e[6], e[7], dir);
+      s_unit(dcross(e[4], e[5]), is[i].nrm);
+    } else if (cw[i][0] && cw[i][9] && cw[n][4] && cw[n][8]) {
+      s_quad_point(is[i].pos, v[0], v[1], v[5], ws[0], ws[9], -ws[4], -ws[8], e[4], e[8], dir);
+      s_unit(dcross(e[0], e[9]), is[i].nrm);
+    } else if (cw[i][1] && cw[i][10] && cw[n][5] && cw[n][9]) {
+      s_quad_point(is[i].pos, v[1], v[2], v[6], ws[1], ws[10], -ws[5], -ws[9], e[5], e[9], dir);
+      s_unit(dcross(e[1], e[10]), is[i].nrm);
+    } else if (cw[i][2] && cw[i][11] && cw[n][6] && cw[n][10]) {
+      s_quad_point(is[i].pos, v[2], v[3], v[7], ws[2], ws[11], -ws[6], -ws[10], e[6], e[10], dir);
+      s_unit(dcross(e[2], e[11]), is[i].nrm);
+    } else if (cw[i][3] && cw[i][8] && cw[n][7] && cw[n][11]) {
+      s_quad_point(is[i].pos, v[3], v[0], v[4], ws[3], ws[8], -ws[7], -ws[11], e[7], e[11], dir);
+      s_unit(dcross(e[3], e[8]), is[i].nrm);
+    } else {
+      return 0;
+    }
+  }
+  s_params(is, org, dir);
+  return 1;
+}
+
+/* SolidAccel::Traverse + TestLeafNode (:2206-2334): hits (t, u = v = 0: the
+ * reference leaves them unset), the hit's normal and position. */
+static void solid_trace_one(const so_solids *S, const so_ray *ray, so_hit *hit, float *nrm,
+                            float *pos) {
+  const float big = FLT_MAX;
+  float t = big, bn[3] = {0, 0, 0}, bp[3] = {0, 0, 0};
+  uint32_t prim = 0xffffffffu;
+  int sign[3];
+  float inv[3];
+  for (int k = 0; k < 3; k++) {
+    sign[k] = ray->dir[k] < 0.0f ? 1 : 0;
+    inv[k] = (float)(1.0 / (double)ray->dir[k]);
+  }
+  const d3 org = {ray->org[0], ray->org[1], ray->org[2]};
+  const d3 dir = {ray->dir[0], ray->dir[1], ray->dir[2]};
+  int stack[520], sp = 0;
+  stack[0] = 0;
+  while (S->nnodes && sp >= 0) {
+    const so_solid_node *nd = &S->nodes[stack[sp--]];
+    const int boxhit = line_box_hit((const so_line_node *)nd, ray->org, inv, sign, big);
+    if (nd->flag == 0) {
+      if (boxhit) {
+        const int nearc = sign[nd->axis];
+        stack[++sp] = (int)nd->data[1 - nearc];
+        stack[++sp] = (int)nd->data[nearc];
+      }
+    } else if (boxhit) {
+      for (uint32_t j = 0; j < nd->data[0]; j++) {
+        const uint32_t p = S->sidx[nd->data[1] + j];
+        if (p == ray->prev_prim) continue;
+        d3 vv[8];
+        for (int q = 0; q < S->nv; q++) {
+          const float *x = &S->v[3 * (size_t)S->ix[(size_t)S->nv * p + q]];
+          vv[q] = (d3){x[0], x[1], x[2]};
+        }
+        so_sisect is[2];
+        memset(is, 0, sizeof(is));
+        int h = S->nv == 5 ? s_pyramid(org, dir, vv, is)
+                           : (S->nv == 6 ? s_prism(org, dir, vv, is) : s_hexa(org, dir, vv, is));
+        if (!h) continue;
+        for (int s = 0; s < 2; s++)
+          if (is[s].t >= 0.0f && is[s].t < t) {
+            t = is[s].t;
+            prim = p;
+            memcpy(bn, is[s].nrm, 12);
+            memcpy(bp, is[s].pos, 12);
+          }
+      }
+    }
+  }
+  hit->t = t;
+  hit->u = hit->v = 0.0f;
+  hit->prim = t < big ? prim : 0xffffffffu;
+  if (t >= big) {
+    memset(bn, 0, 12);
+    memset(bp, 0, 12);
+  }
+  if (nrm) memcpy(nrm, bn, 12);
+  if (pos) memcpy(pos, bp, 12);
+}
+
+SO_API void so_solid_trace(const so_solids *S, const so_ray *rays, size_t n, so_hit *hits,
+                           float *normals, float *positions, int nthreads) {
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 256) num_threads(nthreads)
+#endif
+  for (long long i = 0; i < (long long)n; i++)
+    solid_trace_one(S, &rays[i], &hits[i], normals ? &normals[3 * i] : NULL,
+                    positions ? &positions[3 * i] : NULL);
+}

@@ -148,6 +148,14 @@ _SIGS = {
     "srt_line_info": [_P, _P, _P, _P],
     "srt_line_export": [_P, _P, _P],
     "srt_line_dump": [_P, C.c_char_p],
+    "srt_solid_create": [_P, C.POINTER(_P)],
+    "srt_solid_destroy": [_P],
+    "srt_solid_build": [_P, C.c_int32, _P, _SZ, _P, _SZ],
+    "srt_solid_trace": [_P, _P, _SZ, _P, _P, _P],
+    "srt_solid_bbox": [_P, _P, _P],
+    "srt_solid_info": [_P, _P, _P],
+    "srt_solid_export": [_P, _P, _P],
+    "srt_solid_dump": [_P, C.c_char_p],
     "srt_batch_create": [_P, C.POINTER(_P)],
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],

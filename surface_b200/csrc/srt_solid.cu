@@ -1,0 +1,709 @@
+// srt_solid.cu -- SolidAccel (render/render_accel_solid.cc) on the GPU:
+// pyramids (5 vertices), prisms (6) and hexahedra (8), closest hit.
+//
+// Build (SolidAccel::Build32, :1795-2124): the scene box (every vertex
+// -+ FLT_EPSILON * 16) and the quantisation constants on the host; on the
+// GPU the Morton codes of the solids' centroids (the running sum of the
+// vertices times 1.0f / nv, render/render_prefix_tree_util.cc:347-382), the
+// stable 30-bit radix sort and the Karras split of every internal node
+// (ConstructBinaryRadixTree30) -- the stages the tetrahedra use; then on
+// the host the reference's top-down emission (BuildTreeRecursive32,
+// :1361-1453: a leaf for a Karras leaf, for up to 5 solids or below depth
+// 22; leaf boxes over the solids' vertices -+ FLT_EPSILON * 16, branch
+// boxes merged), in its pre-order.  A gather kernel copies each solid's
+// vertices into a record in leaf order.
+//
+// Trace (SolidAccel::Traverse, :2345-2435): one thread per ray, every
+// popped node tests its own box; a leaf whose box is hit tests its solids
+// (skipping Ray::prev_prim_id) with the Pluecker tests of Intersect*D
+// (:455-717) in double, keeping the entry or exit point nearer than the
+// current hit.  The reference's TestLeafNode returns a shadowed flag
+// (always false), so its walk never lowers the distance bound of the box
+// test: no box is culled by distance here either.  Compiled without FMA
+// contraction, so every double and float operation rounds as the
+// reference's x86-64 build does.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <vector>
+
+#include "srt_internal.cuh"
+
+namespace {
+
+// The reference's SolidNode (Dump record, 40 bytes).
+struct SolidNodeH {
+  float bmin[3], bmax[3];
+  int32_t flag, axis;  // flag 1: leaf (data = count, first), 0: branch (children)
+  uint32_t data[2];
+};
+static_assert(sizeof(SolidNodeH) == 40, "SolidNode layout");
+
+// Device node: w1 bit 31 set for a leaf (w0 = first record, low bits = count),
+// else w0 = left child, w1 = right child | axis << 29.
+struct alignas(16) SNode {
+  float bmin[3];
+  uint32_t w0;
+  float bmax[3];
+  uint32_t w1;
+};
+static_assert(sizeof(SNode) == 32, "two 16-byte loads");
+
+constexpr uint32_t kSolidLeaf = 0x80000000u;
+
+// floats per record: nv vertices (xyz) and the solid's index, padded to 16 bytes
+__host__ __device__ constexpr int rec_floats(int nv) { return ((3 * nv + 1) + 3) / 4 * 4; }
+
+}  // namespace
+
+struct srt_solid_accel {
+  srt_ctx *ctx = nullptr;
+  bool built = false;
+  int nv = 0;
+  size_t n = 0;
+  std::vector<SolidNodeH> nodes;  // reference layout (Dump, export)
+  std::vector<uint32_t> idx;
+  srt::DevBuf dnodes, drecs;
+};
+
+namespace {
+
+using srt::DevBuf;
+
+// ------------------------------------------------------------------ build
+__global__ void solid_morton_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+                                    int nv, size_t n, float lx, float ly, float lz, float ix_,
+                                    float iy, float iz, uint32_t *__restrict__ codes) {
+  const float invdiv = 1.0f / (float)nv;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    float c[3] = {0.0f, 0.0f, 0.0f};
+    for (int j = 0; j < nv; j++) {
+      const uint32_t f = ix[(size_t)nv * i + j];
+      for (int k = 0; k < 3; k++) c[k] = c[k] + v[3 * (size_t)f + k];
+    }
+    for (int k = 0; k < 3; k++) c[k] *= invdiv;
+    const uint32_t qx = srt::f2u32_x86((c[0] - lx) * ix_);
+    const uint32_t qy = srt::f2u32_x86((c[1] - ly) * iy);
+    const uint32_t qz = srt::f2u32_x86((c[2] - lz) * iz);
+    codes[i] = (srt::spread10(qx) << 2) | (srt::spread10(qy) << 1) | srt::spread10(qz);
+  }
+}
+
+__global__ void solid_gather_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+                                    const uint32_t *__restrict__ order, int nv, size_t n,
+                                    float *__restrict__ recs) {
+  const int rf = rec_floats(nv);
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
+       j += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t p = order[j];
+    float *r = recs + (size_t)rf * j;
+    for (int q = 0; q < nv; q++) {
+      const uint32_t f = ix[(size_t)nv * p + q];
+      for (int k = 0; k < 3; k++) r[3 * q + k] = v[3 * (size_t)f + k];
+    }
+    r[3 * nv] = __uint_as_float(p);
+    for (int k = 3 * nv + 1; k < rf; k++) r[k] = 0.0f;
+  }
+}
+
+struct Emitter {
+  const float *v;
+  const uint32_t *ix;
+  int nv;
+  const uint32_t *sidx, *code, *child;
+  const uint8_t *flags;  // bit 0: left child is a single key, bit 1: right
+  std::vector<SolidNodeH> &nodes;
+
+  // ComputeBoundingBox30 (:1121-1169) over sorted solids [l, r).
+  void leaf_box(size_t l, size_t r, float bmin[3], float bmax[3]) const {
+    const float eps = FLT_EPSILON * 16;
+    const uint32_t f0 = ix[(size_t)nv * sidx[l]];
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = v[3 * (size_t)f0 + k] - eps;
+      bmax[k] = v[3 * (size_t)f0 + k] + eps;
+    }
+    for (size_t i = l; i < r; i++)
+      for (int j = 0; j < nv; j++) {
+        const uint32_t f = ix[(size_t)nv * sidx[i] + j];
+        for (int k = 0; k < 3; k++) {
+          const float lo = v[3 * (size_t)f + k] - eps, hi = v[3 * (size_t)f + k] + eps;
+          if (bmin[k] > lo) bmin[k] = lo;
+          if (bmax[k] < hi) bmax[k] = hi;
+        }
+      }
+  }
+
+  static int axis_of(uint32_t c) { return ((c ? __builtin_clz(c) : 32) - 2) % 3; }
+
+  static void merge(const float a0[3], const float a1[3], const float b0[3], const float b1[3],
+                    float bmin[3], float bmax[3]) {
+    for (int k = 0; k < 3; k++) {  // MergeBoundingBox: std::min / std::max
+      bmin[k] = (b0[k] < a0[k]) ? b0[k] : a0[k];
+      bmax[k] = (a1[k] < b1[k]) ? b1[k] : a1[k];
+    }
+  }
+
+  // keys [l, r] inclusive
+  size_t emit(uint32_t root, uint32_t l, uint32_t r, bool leaf, int depth, float bmin[3],
+              float bmax[3]) {
+    const size_t off = nodes.size();
+    nodes.push_back(SolidNodeH{});
+    if (leaf || (r - l) <= 4 || depth > 22) {
+      leaf_box(l, (size_t)r + 1, bmin, bmax);
+      SolidNodeH &nd = nodes[off];
+      std::memcpy(nd.bmin, bmin, 12);
+      std::memcpy(nd.bmax, bmax, 12);
+      nd.flag = 1;
+      nd.data[0] = r + 1 - l;
+      nd.data[1] = l;
+      return off;
+    }
+    const uint32_t mid = child[root];
+    float a0[3], a1[3], b0[3], b1[3];
+    const size_t left = emit(mid, l, mid, flags[root] & 1, depth + 1, a0, a1);
+    const size_t right = emit(mid + 1, mid + 1, r, flags[root] & 2, depth + 1, b0, b1);
+    merge(a0, a1, b0, b1, bmin, bmax);
+    SolidNodeH &nd = nodes[off];
+    nd.axis = axis_of(code[root]);
+    nd.data[0] = (uint32_t)left;
+    nd.data[1] = (uint32_t)right;
+    std::memcpy(nd.bmin, bmin, 12);
+    std::memcpy(nd.bmax, bmax, 12);
+    return off;
+  }
+};
+
+// ------------------------------------------------------------------ trace
+struct D3 {
+  double x, y, z;
+};
+__device__ __forceinline__ D3 dsub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+__device__ __forceinline__ D3 dadd(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+__device__ __forceinline__ D3 dscale(D3 a, double f) { return {a.x * f, a.y * f, a.z * f}; }
+__device__ __forceinline__ D3 dcross(D3 a, D3 b) {
+  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
+}
+__device__ __forceinline__ double ddot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+
+struct SIsect {
+  float pos[3], nrm[3];
+  float t;
+};
+
+// normalize (:85), then to float
+__device__ __forceinline__ void s_unit(D3 a, float out[3]) {
+  const double len = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
+  out[0] = (float)(a.x / len);
+  out[1] = (float)(a.y / len);
+  out[2] = (float)(a.z / len);
+}
+
+// SetCrossPoint_Sq (double, :438-444): a quad face's crossing point
+__device__ __forceinline__ void s_quad(float out[3], D3 v0, D3 v1, D3 v2, double ws0, double ws1,
+                                       double ws2, double ws3, D3 e2, D3 e3, D3 dir) {
+  const double w = ws2 + ws3 + ddot(dcross(e2, e3), dir);
+  const D3 p = dadd(dadd(dscale(v2, ws0), dscale(v0, ws1)), dscale(v1, w));
+  const double den = ws0 + ws1 + w;
+  out[0] = (float)(p.x / den);
+  out[1] = (float)(p.y / den);
+  out[2] = (float)(p.z / den);
+}
+
+// a triangle face's crossing point: the weighted sum in double, then the
+// float vector divided by the float sum of the weights
+__device__ __forceinline__ void s_tri(float out[3], D3 a, double wa, D3 b, double wb, D3 c,
+                                      double wc, double den) {
+  const D3 p = dadd(dadd(dscale(a, wa), dscale(b, wb)), dscale(c, wc));
+  const float f = (float)den;
+  out[0] = (float)p.x / f;
+  out[1] = (float)p.y / f;
+  out[2] = (float)p.z / f;
+}
+
+// t of both points along the last axis with |dir| > 0.1; the exit normal flipped
+__device__ __forceinline__ void s_params(SIsect is[2], D3 org, D3 dir) {
+  const double o[3] = {org.x, org.y, org.z}, d[3] = {dir.x, dir.y, dir.z};
+  for (int j = 0; j < 3; j++)
+    if (d[j] > 0.1 || d[j] < -0.1) {
+      is[0].t = (float)(((double)is[0].pos[j] - o[j]) / d[j]);
+      is[1].t = (float)(((double)is[1].pos[j] - o[j]) / d[j]);
+    }
+  for (int k = 0; k < 3; k++) is[1].nrm[k] = -1.0f * is[1].nrm[k];
+}
+
+template <int NE, int MOD>
+__device__ __forceinline__ void s_weights(const D3 *e, const D3 *v, D3 dir, D3 org, double *ws,
+                                          bool (&c0)[NE], bool (&c1)[NE]) {
+  const D3 rpc = dcross(dir, org);
+#pragma unroll
+  for (int i = 0; i < NE; i++) {
+    ws[i] = ddot(dir, dcross(e[i], v[i % MOD])) + ddot(e[i], rpc);
+    c0[i] = ws[i] >= 0;
+    c1[i] = ws[i] <= 0;
+  }
+}
+
+// IntersectPyramidD (:455-505)
+__device__ bool s_pyramid(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
+  const D3 e[8] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[3], v[2]), dsub(v[0], v[3]),
+                   dsub(v[4], v[0]), dsub(v[4], v[1]), dsub(v[4], v[2]), dsub(v[4], v[3])};
+  double ws[8];
+  bool cw[2][8];
+  s_weights<8, 4>(e, v, dir, org, ws, cw[0], cw[1]);
+  for (int i = 1, n = 0; n < 2; i--, n++) {
+    if (cw[i][0] && cw[i][1] && cw[i][2] && cw[i][3]) {
+      s_quad(is[n].pos, v[0], v[1], v[2], ws[0], ws[1], ws[2], ws[3], e[2], e[3], dir);
+      s_unit(dcross(e[1], e[0]), is[n].nrm);
+    } else if (cw[n][0] && cw[i][4] && cw[n][5]) {
+      s_tri(is[n].pos, v[4], -ws[0], v[1], ws[4], v[0], -ws[5], -ws[0] + ws[4] - ws[5]);
+      s_unit(dcross(e[4], e[0]), is[n].nrm);
+    } else if (cw[n][1] && cw[i][5] && cw[n][6]) {
+      s_tri(is[n].pos, v[4], -ws[1], v[2], ws[5], v[1], -ws[6], -ws[1] + ws[5] - ws[6]);
+      s_unit(dcross(e[5], e[1]), is[n].nrm);
+    } else if (cw[n][2] && cw[i][6] && cw[n][7]) {
+      s_tri(is[n].pos, v[4], -ws[2], v[3], ws[6], v[2], -ws[7], -ws[2] + ws[6] - ws[7]);
+      s_unit(dcross(e[6], e[2]), is[n].nrm);
+    } else if (cw[n][3] && cw[i][7] && cw[n][4]) {
+      s_tri(is[n].pos, v[4], -ws[3], v[0], ws[7], v[3], -ws[4], -ws[3] + ws[7] - ws[4]);
+      s_unit(dcross(e[7], e[3]), is[n].nrm);
+    } else {
+      return false;
+    }
+  }
+  s_params(is, org, dir);
+  return true;
+}
+
+// IntersectPrismD (:559-611)
+__device__ bool s_prism(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
+  const D3 e[9] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[0], v[2]),
+                   dsub(v[4], v[3]), dsub(v[5], v[4]), dsub(v[3], v[5]),
+                   dsub(v[3], v[0]), dsub(v[4], v[1]), dsub(v[5], v[2])};
+  double ws[9];
+  bool cw[2][9];
+  s_weights<9, 6>(e, v, dir, org, ws, cw[0], cw[1]);
+  for (int i = 0, n = 1; i < 2; i++, n--) {
+    if (cw[n][0] && cw[n][1] && cw[n][2]) {
+      s_tri(is[i].pos, v[2], ws[0], v[0], ws[1], v[1], ws[2], ws[0] + ws[1] + ws[2]);
+      s_unit(dcross(e[0], e[1]), is[i].nrm);
+    } else if (cw[i][3] && cw[i][4] && cw[i][5]) {
+      s_tri(is[i].pos, v[5], ws[3], v[3], ws[4], v[4], ws[5], ws[3] + ws[4] + ws[5]);
+      s_unit(dcross(e[3], e[4]), is[i].nrm);
+    } else if (cw[i][2] && cw[i][6] && cw[n][5] && cw[n][8]) {
+      s_quad(is[i].pos, v[2], v[0], v[3], ws[2], ws[6], -ws[5], -ws[8], e[5], e[8], dir);
+      s_unit(dcross(e[2], e[6]), is[i].nrm);
+    } else if (cw[i][0] && cw[i][7] && cw[n][3] && cw[n][6]) {
+      s_quad(is[i].pos, v[0], v[1], v[4], ws[0], ws[7], -ws[3], -ws[6], e[3], e[6], dir);
+      s_unit(dcross(e[0], e[7]), is[i].nrm);
+    } else if (cw[i][1] && cw[i][8] && cw[n][4] && cw[n][7]) {
+      s_quad(is[i].pos, v[1], v[2], v[5], ws[1], ws[8], -ws[4], -ws[7], e[4], e[7], dir);
+      s_unit(dcross(e[1], e[8]), is[i].nrm);
+    } else {
+      return false;
+    }
+  }
+  s_params(is, org, dir);
+  return true;
+}
+
+// IntersectHexaD (:664-716)
+__device__ bool s_hexa(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
+  const D3 e[12] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[3], v[2]), dsub(v[0], v[3]),
+                    dsub(v[5], v[4]), dsub(v[6], v[5]), dsub(v[7], v[6]), dsub(v[4], v[7]),
+                    dsub(v[4], v[0]), dsub(v[5], v[1]), dsub(v[6], v[2]), dsub(v[7], v[3])};
+  double ws[12];
+  bool cw[2][12];
+  s_weights<12, 8>(e, v, dir, org, ws, cw[0], cw[1]);
+  for (int i = 0, n = 1; i < 2; i++, n--) {
+    if (cw[n][0] && cw[n][1] && cw[n][2] && cw[n][3]) {
+      s_quad(is[i].pos, v[0], v[1], v[2], ws[0], ws[1], ws[2], ws[3], e[2], e[3], dir);
+      s_unit(dcross(e[0], e[1]), is[i].nrm);
+    } else if (cw[i][4] && cw[i][5] && cw[i][6] && cw[i][7]) {
+      s_quad(is[i].pos, v[4], v[5], v[6], ws[4], ws[5], ws[6], ws[7], e[6], e[7], dir);
+      s_unit(dcross(e[4], e[5]), is[i].nrm);
+    } else if (cw[i][0] && cw[i][9] && cw[n][4] && cw[n][8]) {
+      s_quad(is[i].pos, v[0], v[1], v[5], ws[0], ws[9], -ws[4], -ws[8], e[4], e[8], dir);
+      s_unit(dcross(e[0], e[9]), is[i].nrm);
+    } else if (cw[i][1] && cw[i][10] && cw[n][5] && cw[n][9]) {
+      s_quad(is[i].pos, v[1], v[2], v[6], ws[1], ws[10], -ws[5], -ws[9], e[5], e[9], dir);
+      s_unit(dcross(e[1], e[10]), is[i].nrm);
+    } else if (cw[i][2] && cw[i][11] && cw[n][6] && cw[n][10]) {
+      s_quad(is[i].pos, v[2], v[3], v[7], ws[2], ws[11], -ws[6], -ws[10], e[6], e[10], dir);
+      s_unit(dcross(e[2], e[11]), is[i].nrm);
+    } else if (cw[i][3] && cw[i][8] && cw[n][7] && cw[n][11]) {
+      s_quad(is[i].pos, v[3], v[0], v[4], ws[3], ws[8], -ws[7], -ws[11], e[7], e[11], dir);
+      s_unit(dcross(e[3], e[8]), is[i].nrm);
+    } else {
+      return false;
+    }
+  }
+  s_params(is, org, dir);
+  return true;
+}
+
+// IntersectRayAABB (:2160-2204) with the reference's selection order.
+__device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], const float inv[3],
+                                         const int sign[3]) {
+  float lo[3], hi[3];
+  for (int k = 0; k < 3; k++) {
+    lo[k] = sign[k] ? nd.bmax[k] : nd.bmin[k];
+    hi[k] = sign[k] ? nd.bmin[k] : nd.bmax[k];
+  }
+  const float tx0 = (lo[0] - org[0]) * inv[0], tx1 = (hi[0] - org[0]) * inv[0];
+  const float ty0 = (lo[1] - org[1]) * inv[1], ty1 = (hi[1] - org[1]) * inv[1];
+  float tmin = (tx0 > ty0) ? tx0 : ty0;
+  float tmax = (tx1 < ty1) ? tx1 : ty1;
+  const float tz0 = (lo[2] - org[2]) * inv[2], tz1 = (hi[2] - org[2]) * inv[2];
+  tmin = (tmin > tz0) ? tmin : tz0;
+  tmax = (tmax < tz1) ? tmax : tz1;
+  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= FLT_MAX);
+}
+
+template <int NV>
+__global__ void __launch_bounds__(128)
+solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
+                   const srt_ray *__restrict__ rays, size_t n, srt_hit *__restrict__ hits,
+                   float *__restrict__ normals, float *__restrict__ positions) {
+  constexpr int RF = rec_floats(NV);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const float4 *rq = reinterpret_cast<const float4 *>(rays + i);
+    const float4 r0 = __ldg(rq), r1 = __ldg(rq + 1);
+    const float org[3] = {r0.x, r0.y, r0.z}, dir[3] = {r1.x, r1.y, r1.z};
+    const uint32_t prev = __float_as_uint(r0.w);
+    int sign[3];
+    float inv[3];
+    for (int k = 0; k < 3; k++) {
+      sign[k] = dir[k] < 0.0f ? 1 : 0;
+      inv[k] = __frcp_rn(dir[k]);  // (float)(1.0 / dir), correctly rounded
+    }
+    const D3 dorg = {org[0], org[1], org[2]}, ddir = {dir[0], dir[1], dir[2]};
+    float t = FLT_MAX, bn[3] = {0.f, 0.f, 0.f}, bp[3] = {0.f, 0.f, 0.f};
+    uint32_t prim = SRT_MISS;
+    int stack[64];
+    int sp = 0;
+    stack[0] = 0;
+    while (sp >= 0) {
+      const float4 *q = reinterpret_cast<const float4 *>(nodes + stack[sp]);
+      const float4 a = __ldg(q), b = __ldg(q + 1);
+      sp--;
+      const SNode nd = {{a.x, a.y, a.z}, __float_as_uint(a.w), {b.x, b.y, b.z},
+                        __float_as_uint(b.w)};
+      if (!sbox_hit(nd, org, inv, sign)) continue;
+      if (!(nd.w1 & kSolidLeaf)) {
+        const int axis = (int)(nd.w1 >> 29);
+        const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
+        const int nearc = sign[axis];
+        stack[++sp] = nearc ? left : right;  // far
+        stack[++sp] = nearc ? right : left;  // near
+        continue;
+      }
+      const uint32_t first = nd.w0, cnt = nd.w1 & ~kSolidLeaf;
+      for (uint32_t j = 0; j < cnt; j++) {
+        const float *r = recs + (size_t)RF * (first + j);
+        const uint32_t p = __float_as_uint(__ldg(r + 3 * NV));
+        if (p == prev) continue;  // Ray::prev_prim_id
+        D3 v[NV];
+#pragma unroll
+        for (int k = 0; k < NV; k++)
+          v[k] = {(double)__ldg(r + 3 * k), (double)__ldg(r + 3 * k + 1),
+                  (double)__ldg(r + 3 * k + 2)};
+        SIsect is[2];
+        for (int s = 0; s < 2; s++) is[s].t = 0.0f;
+        const bool h = NV == 5 ? s_pyramid(dorg, ddir, v, is)
+                               : (NV == 6 ? s_prism(dorg, ddir, v, is) : s_hexa(dorg, ddir, v, is));
+        if (!h) continue;
+        for (int s = 0; s < 2; s++)
+          if (is[s].t >= 0.0f && is[s].t < t) {
+            t = is[s].t;
+            prim = p;
+            for (int k = 0; k < 3; k++) {
+              bn[k] = is[s].nrm[k];
+              bp[k] = is[s].pos[k];
+            }
+          }
+      }
+    }
+    const bool got = t < FLT_MAX;
+    reinterpret_cast<float4 *>(hits)[i] =
+        make_float4(t, 0.0f, 0.0f, __uint_as_float(got ? prim : SRT_MISS));
+    for (int k = 0; k < 3; k++) {
+      if (normals) normals[3 * i + k] = got ? bn[k] : 0.0f;
+      if (positions) positions[3 * i + k] = got ? bp[k] : 0.0f;
+    }
+  }
+}
+
+srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
+                      const void **out) {
+  if (!p || srt::is_device_ptr(p)) {
+    *out = p;
+    return SRT_OK;
+  }
+  cudaError_t e = stage.ensure(bytes ? bytes : 1);
+  if (e == cudaSuccess && bytes)
+    e = cudaMemcpyAsync(stage.p, p, bytes, cudaMemcpyHostToDevice, ctx->stream);
+  if (e != cudaSuccess) return srt::cuda_status(e, "solid staging");
+  *out = stage.p;
+  return SRT_OK;
+}
+
+template <typename T>
+srt_status to_host(const T *p, size_t count, std::vector<T> &buf, const T **out) {
+  if (!srt::is_device_ptr(p)) {
+    *out = p;
+    return SRT_OK;
+  }
+  buf.resize(count ? count : 1);
+  cudaError_t e = cudaMemcpy(buf.data(), p, count * sizeof(T), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) return srt::cuda_status(e, "solid input copy");
+  *out = buf.data();
+  return SRT_OK;
+}
+
+}  // namespace
+
+using namespace srt;
+
+extern "C" {
+
+SRT_API srt_status srt_solid_create(srt_ctx *ctx, srt_solid_accel **out) {
+  if (!ctx || !out) return SRT_ERR_INVALID;
+  srt_solid_accel *a = new (std::nothrow) srt_solid_accel();
+  if (!a) return SRT_ERR_NO_MEMORY;
+  a->ctx = ctx;
+  *out = a;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_destroy(srt_solid_accel *a) {
+  if (!a) return SRT_OK;
+  cudaSetDevice(a->ctx->device);
+  cudaStreamSynchronize(a->ctx->stream);
+  delete a;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
+                                   const float *vertices, size_t nverts,
+                                   const uint32_t *indices, size_t nsolids) {
+  if (!a || !vertices || !indices) return SRT_ERR_INVALID;
+  const int nv = verts_per_solid;
+  if ((nv != 5 && nv != 6 && nv != 8) || nsolids < 2 || nsolids >= (1u << 29)) {
+    set_error("srt_solid_build: 5, 6 or 8 vertices per solid and 2 .. 2^29 solids");
+    return SRT_ERR_INVALID;
+  }
+  srt_ctx *ctx = a->ctx;
+  cudaSetDevice(ctx->device);
+  std::vector<float> hv;
+  std::vector<uint32_t> hi;
+  const float *v;
+  const uint32_t *ix;
+  srt_status s = to_host(vertices, nverts * 3, hv, &v);
+  if (s == SRT_OK) s = to_host(indices, nsolids * nv, hi, &ix);
+  if (s != SRT_OK) return s;
+  for (size_t i = 0; i < nsolids * (size_t)nv; i++)
+    if (ix[i] >= nverts) {
+      set_error("srt_solid_build: an index names a vertex beyond nverts");
+      return SRT_ERR_INVALID;
+    }
+  // scene box (ComputeBoundingBoxOMP, :1171-1262; min and max in any order)
+  const float eps = FLT_EPSILON * 16;
+  float lo[3], hi3[3];
+  for (int k = 0; k < 3; k++) lo[k] = hi3[k] = v[3 * (size_t)ix[0] + k];
+  for (int k = 0; k < 3; k++) {
+    lo[k] -= eps;
+    hi3[k] += eps;
+  }
+  for (size_t i = 0; i < nsolids * (size_t)nv; i++)
+    for (int k = 0; k < 3; k++) {
+      const float x0 = v[3 * (size_t)ix[i] + k] - eps, x1 = v[3 * (size_t)ix[i] + k] + eps;
+      lo[k] = (x0 < lo[k]) ? x0 : lo[k];
+      hi3[k] = (hi3[k] < x1) ? x1 : hi3[k];
+    }
+  float inv[3];
+  const int kdiv = 1 << 10;
+  for (int k = 0; k < 3; k++) inv[k] = kdiv / (hi3[k] - lo[k]);
+  DevBuf sv, si, codes, order, child, flags;
+  const void *dv, *di;
+  if ((s = solid_view(ctx, vertices, nverts * 12, sv, &dv)) != SRT_OK) return s;
+  if ((s = solid_view(ctx, indices, nsolids * nv * 4, si, &di)) != SRT_OK) return s;
+  cudaError_t e;
+  const size_t n = nsolids;
+  if ((e = codes.ensure(n * 4)) != cudaSuccess || (e = order.ensure(n * 4)) != cudaSuccess ||
+      (e = child.ensure(n * 4)) != cudaSuccess || (e = flags.ensure(n)) != cudaSuccess)
+    return cuda_status(e, "solid build");
+  const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
+  solid_morton_kernel<<<grid, 256, 0, ctx->stream>>>(
+      static_cast<const float *>(dv), static_cast<const uint32_t *>(di), nv, n, lo[0], lo[1],
+      lo[2], inv[0], inv[1], inv[2], codes.as<uint32_t>());
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid morton");
+  if ((s = sort_pairs(ctx, codes.as<uint32_t>(), order.as<uint32_t>(), n, true, 30)) != SRT_OK)
+    return s;
+  if ((s = stage_karras(ctx, codes.as<uint32_t>(), n, child.as<uint32_t>(),
+                        flags.as<uint8_t>())) != SRT_OK)
+    return s;
+  std::vector<uint32_t> hcode(n), hchild(n), hidx(n);
+  std::vector<uint8_t> hflags(n);
+  if ((e = cudaMemcpyAsync(hcode.data(), codes.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(hidx.data(), order.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream)) !=
+          cudaSuccess ||
+      (e = cudaMemcpyAsync(hchild.data(), child.p, (n - 1) * 4, cudaMemcpyDeviceToHost,
+                           ctx->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(hflags.data(), flags.p, n - 1, cudaMemcpyDeviceToHost, ctx->stream)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid tree");
+  // the reference's emission (root first, then the left and right subtrees)
+  a->built = false;
+  a->nodes.clear();
+  Emitter E{v, ix, nv, hidx.data(), hcode.data(), hchild.data(), hflags.data(), a->nodes};
+  a->nodes.push_back(SolidNodeH{});
+  float a0[3], a1[3], b0[3], b1[3];
+  const uint32_t mid = hchild[0];
+  const size_t left = E.emit(mid, 0, mid, hflags[0] & 1, 0, a0, a1);
+  const size_t right = E.emit(mid + 1, mid + 1, (uint32_t)n - 1, hflags[0] & 2, 0, b0, b1);
+  SolidNodeH &root = a->nodes[0];
+  Emitter::merge(a0, a1, b0, b1, root.bmin, root.bmax);
+  root.axis = Emitter::axis_of(hcode[0]);
+  root.data[0] = (uint32_t)left;
+  root.data[1] = (uint32_t)right;
+  a->idx = hidx;
+  std::vector<SNode> dn(a->nodes.size());
+  for (size_t i = 0; i < a->nodes.size(); i++) {
+    const SolidNodeH &h = a->nodes[i];
+    for (int k = 0; k < 3; k++) {
+      dn[i].bmin[k] = h.bmin[k];
+      dn[i].bmax[k] = h.bmax[k];
+    }
+    dn[i].w0 = h.flag ? h.data[1] : h.data[0];
+    dn[i].w1 = h.flag ? (kSolidLeaf | h.data[0]) : (h.data[1] | ((uint32_t)h.axis << 29));
+  }
+  if ((e = a->dnodes.ensure(dn.size() * sizeof(SNode))) != cudaSuccess ||
+      (e = a->drecs.ensure(n * rec_floats(nv) * 4)) != cudaSuccess)
+    return cuda_status(e, "solid accel");
+  if ((e = cudaMemcpyAsync(a->dnodes.p, dn.data(), dn.size() * sizeof(SNode),
+                           cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid nodes");
+  solid_gather_kernel<<<grid, 256, 0, ctx->stream>>>(
+      static_cast<const float *>(dv), static_cast<const uint32_t *>(di), order.as<uint32_t>(), nv,
+      n, a->drecs.as<float>());
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid records");
+  // staged inputs and scratch are freed on return: finish with them first
+  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(e, "solid build");
+  a->nv = nv;
+  a->n = n;
+  a->built = true;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size_t n,
+                                   srt_hit *hits, float *normals, float *positions) {
+  if (!a || (n && (!rays || !hits))) return SRT_ERR_INVALID;
+  if (!a->built) {
+    set_error("solid accel not built");
+    return SRT_ERR_INVALID;
+  }
+  if (n == 0) return SRT_OK;
+  srt_ctx *ctx = a->ctx;
+  cudaSetDevice(ctx->device);
+  const void *dr;
+  srt_status s = solid_view(ctx, rays, n * sizeof(srt_ray), ctx->s_stage_in, &dr);
+  if (s != SRT_OK) return s;
+  cudaError_t e;
+  srt_hit *dh = hits;
+  float *dn = normals, *dp = positions;
+  const bool hdev = is_device_ptr(hits), ndev = !normals || is_device_ptr(normals),
+             pdev = !positions || is_device_ptr(positions);
+  if (!hdev) {
+    if ((e = ctx->s_stage_out.ensure(n * sizeof(srt_hit))) != cudaSuccess)
+      return cuda_status(e, "hit staging");
+    dh = ctx->s_stage_out.as<srt_hit>();
+  }
+  if (!ndev) {
+    if ((e = ctx->s_stage_norm.ensure(n * 12)) != cudaSuccess) return cuda_status(e, "staging");
+    dn = ctx->s_stage_norm.as<float>();
+  }
+  if (!pdev) {
+    if ((e = ctx->s_stage_scal.ensure(n * 12)) != cudaSuccess) return cuda_status(e, "staging");
+    dp = ctx->s_stage_scal.as<float>();
+  }
+  if ((reinterpret_cast<uintptr_t>(dr) | reinterpret_cast<uintptr_t>(dh)) & 15u) {
+    set_error("ray and hit arrays must be 16-byte aligned");
+    return SRT_ERR_INVALID;
+  }
+  const unsigned grid = (unsigned)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * 32);
+  const SNode *nd = a->dnodes.as<SNode>();
+  const float *rc = a->drecs.as<float>();
+  const srt_ray *rr = static_cast<const srt_ray *>(dr);
+  if (a->nv == 5)
+    solid_trace_kernel<5><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, n, dh, dn, dp);
+  else if (a->nv == 6)
+    solid_trace_kernel<6><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, n, dh, dn, dp);
+  else
+    solid_trace_kernel<8><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, n, dh, dn, dp);
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid trace");
+  if (!hdev) cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, ctx->stream);
+  if (!ndev) cudaMemcpyAsync(normals, dn, n * 12, cudaMemcpyDeviceToHost, ctx->stream);
+  if (!pdev) cudaMemcpyAsync(positions, dp, n * 12, cudaMemcpyDeviceToHost, ctx->stream);
+  if (!hdev || !ndev || !pdev || !is_device_ptr(rays))
+    return cuda_status(cudaStreamSynchronize(ctx->stream), "solid trace");
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_bbox(srt_solid_accel *a, double bmin[3], double bmax[3]) {
+  if (!a || !bmin || !bmax) return SRT_ERR_INVALID;
+  if (!a->built) {
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = DBL_MAX;
+      bmax[k] = -DBL_MAX;
+    }
+    return SRT_OK;
+  }
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = a->nodes[0].bmin[k];
+    bmax[k] = a->nodes[0].bmax[k];
+  }
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_info(srt_solid_accel *a, uint64_t *nsolids, uint64_t *nnodes) {
+  if (!a) return SRT_ERR_INVALID;
+  if (nsolids) *nsolids = a->built ? a->n : 0;
+  if (nnodes) *nnodes = a->built ? a->nodes.size() : 0;
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_export(srt_solid_accel *a, void *nodes, uint32_t *indices) {
+  if (!a || !a->built) return SRT_ERR_INVALID;
+  if (nodes) std::memcpy(nodes, a->nodes.data(), a->nodes.size() * sizeof(SolidNodeH));
+  if (indices) std::memcpy(indices, a->idx.data(), a->idx.size() * 4);
+  return SRT_OK;
+}
+
+SRT_API srt_status srt_solid_dump(srt_solid_accel *a, const char *path) {
+  if (!a || !path || !a->built) return SRT_ERR_INVALID;
+  FILE *fp = fopen(path, "wb");
+  if (!fp) {
+    set_error(std::string("cannot write ") + path);
+    return SRT_ERR_INVALID;
+  }
+  const unsigned long long nn = a->nodes.size(), ni = a->idx.size();
+  bool ok = fwrite(&nn, 8, 1, fp) == 1 &&
+            fwrite(a->nodes.data(), sizeof(SolidNodeH), nn, fp) == nn &&
+            fwrite(&ni, 8, 1, fp) == 1 && fwrite(a->idx.data(), 4, ni, fp) == ni;
+  ok = (fclose(fp) == 0) && ok;
+  if (!ok) {
+    set_error(std::string("write failed: ") + path);
+    return SRT_ERR_INVALID;
+  }
+  return SRT_OK;
+}
+
+}  // extern "C"

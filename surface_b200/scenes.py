@@ -769,3 +769,58 @@ def line_cases():
     out.append(("limits", p3, s3, r3, 0.0, dict(min_leaf=7, max_depth=6), rays3))
     out.append(("leaf1", p3, s3, r3, 0.0, dict(min_leaf=1), rays3))
     return out
+
+
+# hexahedron corner order: 0..3 the bottom face, 4..7 above them
+_HEX_CORNERS = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                         [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]])
+# pyramid bases from the hexahedron's faces (base b0..b3, apex at the cell centre)
+_PYR_BASES = [(0, 1, 2, 3), (4, 7, 6, 5), (0, 4, 5, 1), (1, 5, 6, 2), (2, 6, 7, 3), (0, 3, 7, 4)]
+
+
+def solid_grid(nv, g, seed=3, jitter=0.2):
+    """Seeded solids filling the unit cube: g^3 cells of a jittered grid as
+    hexahedra (nv = 8), two prisms per cell (nv = 6) or six pyramids around
+    the cell centre (nv = 5).  Returns (vertices (V, 3) float32, indices
+    (N, nv) uint32)."""
+    rng = np.random.default_rng(seed)
+    ax = np.arange(g + 1, dtype=np.float64) / g
+    X, Y, Z = np.meshgrid(ax, ax, ax, indexing="ij")
+    P = np.stack([X, Y, Z], -1)
+    inner = np.zeros(P.shape[:3], bool)
+    inner[1:-1, 1:-1, 1:-1] = True
+    P[inner] += rng.uniform(-jitter, jitter, size=(inner.sum(), 3)) / g
+    verts = P.reshape(-1, 3)
+    c = np.stack(np.meshgrid(np.arange(g), np.arange(g), np.arange(g), indexing="ij"), -1)
+    c = c.reshape(-1, 3)
+    corner = c[:, None, :] + _HEX_CORNERS[None]
+    hexa = (corner[..., 0] * (g + 1) + corner[..., 1]) * (g + 1) + corner[..., 2]
+    if nv == 8:
+        return verts.astype(np.float32), hexa.astype(np.uint32)
+    if nv == 6:
+        a = hexa[:, [0, 1, 2, 4, 5, 6]]
+        b = hexa[:, [0, 2, 3, 4, 6, 7]]
+        return verts.astype(np.float32), np.concatenate([a, b]).astype(np.uint32)
+    centre = verts[hexa].mean(axis=1)
+    cid = verts.shape[0] + np.arange(hexa.shape[0])
+    pyr = [np.concatenate([hexa[:, list(b)], cid[:, None]], 1) for b in _PYR_BASES]
+    return (np.concatenate([verts, centre]).astype(np.float32),
+            np.concatenate(pyr).astype(np.uint32))
+
+
+def solid_rays(n_side=96, seed=5):
+    """Rays for the solid tests: grid-aligned orthographic rays through
+    vertex planes (ties at shared faces and edges), pinhole rays, and rays
+    starting inside the cube in random directions."""
+    o1 = ortho_rays(n_side, n_side, (-0.05, -0.05), (1.05, 1.05), z=1.5)
+    xs = (np.arange(n_side // 2) + 0.5) / (n_side // 2)
+    X, Y = np.meshgrid(xs, xs)
+    o2 = make_rays(np.stack([X.ravel(), np.full(X.size, -0.5), Y.ravel()], 1),
+                   np.tile([0.0, 1.0, 0.0], (X.size, 1)))
+    p = pinhole_rays(n_side, n_side, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)
+    rng = np.random.default_rng(seed)
+    org = rng.uniform(0.05, 0.95, size=(n_side * n_side // 2, 3))
+    d = rng.normal(size=org.shape)
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    inside = make_rays(org, d)
+    return np.concatenate([o1, o2, p, inside])

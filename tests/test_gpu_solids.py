@@ -1,0 +1,86 @@
+"""The solid accel on the GPU (srt_solid_*) against the oracle's SolidAccel
+Build32 / Traverse, bit for bit: the tree (same pre-order records) and solid
+order, per ray the hit (t, solid), its normal and position -- pyramids,
+prisms and hexahedra, grid-aligned, pinhole and interior rays, secondary
+rays that skip the solid they leave; host and device inputs; Dump() bytes,
+BoundingBox, small meshes and bad input."""
+import numpy as np
+import pytest
+import torch
+
+import surface_b200 as sb
+from oracle import oracle as O
+from surface_b200 import scenes as S
+from surface_b200.solids import Solid, SolidAccel
+
+from conftest import bits
+
+pytestmark = pytest.mark.gpu
+
+CASES = {"hexahedra": (8, 14), "prisms": (6, 11), "pyramids": (5, 8)}
+
+
+def _check(nv, v, ix, rays, device_inputs=False):
+    o = O.OracleSolids(nv, v, ix)
+    acc = SolidAccel()
+    if device_inputs:
+        acc.Build32(Solid(nv, torch.as_tensor(v).cuda(),
+                          torch.as_tensor(ix.astype(np.int32)).cuda()))
+    else:
+        acc.Build32(Solid(nv, v, ix))
+    gn, gi = acc.export()
+    on, oi = o.export()
+    assert gn.tobytes() == on.tobytes()
+    assert np.array_equal(gi, oi)
+    want, wn, wp = o.trace(rays)
+    got, gnrm, gpos = acc.Traverse(rays, want_point=True)
+    assert np.array_equal(bits(got.view(np.float32).reshape(-1, 4)),
+                          bits(want.view(np.float32).reshape(-1, 4)))
+    assert np.array_equal(bits(gnrm), bits(wn)) and np.array_equal(bits(gpos), bits(wp))
+    rt = torch.from_numpy(np.ascontiguousarray(rays).view(np.float32).reshape(-1, 8)).cuda()
+    gd = acc.Traverse(rt).cpu().numpy()
+    assert np.array_equal(bits(gd), bits(want.view(np.float32).reshape(-1, 4)))
+    return acc, want, wp
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_solids(case):
+    nv, g = CASES[case]
+    v, ix = S.solid_grid(nv, g, seed=9)
+    rays = S.solid_rays(128, seed=nv)
+    _, h, p = _check(nv, v, ix, rays, device_inputs=(nv == 6))
+    assert 0.5 < (h["prim"] != O.MISS).mean() < 0.95
+    ok = h["prim"] != O.MISS
+    rng = np.random.default_rng(nv)
+    d = rng.normal(size=(ok.sum(), 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays2 = S.make_rays(p[ok], d)
+    rays2["prev_prim"] = h["prim"][ok]
+    _, h2, _ = _check(nv, v, ix, rays2)
+    assert (h2["prim"] != rays2["prev_prim"]).all()
+
+
+@pytest.mark.parametrize("nsolids", [2, 3, 7, 40])
+def test_small_meshes(nsolids):
+    v, ix = S.solid_grid(8, 4, seed=2)
+    ix = ix[:nsolids]
+    _check(8, v, ix, S.solid_rays(32))
+
+
+def test_dump_bbox_and_errors(tmp_path):
+    v, ix = S.solid_grid(6, 6, seed=4)
+    acc = SolidAccel()
+    acc.Build32(Solid(6, v, ix))
+    acc.Dump(tmp_path / "s.bin")
+    nodes, idx = O.parse_solid_dump((tmp_path / "s.bin").read_bytes())
+    on, oi = O.OracleSolids(6, v, ix).export()
+    assert nodes.tobytes() == on.tobytes() and np.array_equal(idx, oi)
+    lo, hi = acc.BoundingBox()
+    assert np.array_equal(lo, on[0]["bmin"].astype(np.float64))
+    assert np.array_equal(hi, on[0]["bmax"].astype(np.float64))
+    bad = ix.copy()
+    bad[3, 2] = v.shape[0]
+    with pytest.raises(sb.SurfaceError):
+        SolidAccel().Build32(Solid(6, v, bad))
+    with pytest.raises(sb.SurfaceError):
+        SolidAccel().Build32(Solid(7, v, ix))  # 7 vertices per solid
