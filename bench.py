@@ -113,6 +113,14 @@ def make_workload(name):
                                         "hit + RGBA8 and depth write per step",
                             "elements": len(E["elements"]),
                             "prims": int(sum(E["prims"])), "rays": 1024 * 1024})
+    if name == "solids":
+        v, ix = S.solid_grid(8, 64, seed=123456)
+        rays = S.pinhole_rays(512, 512, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)
+        return dict(kind="solids", verts=v, prims=ix, rays=rays,
+                    config={"workload": "hex64: 262,144 hexahedra (64^3 jittered cells), "
+                                        "512x512 pinhole rays; SolidAccel Build32 + closest "
+                                        "hit with position and normal per step",
+                            "prims": int(ix.shape[0]), "rays": int(rays.size)})
     if name == "lines":
         pos, seg, rad = S.line_strands(100000, 16, seed=123456)
         rays = S.pinhole_rays(1024, 1024, (0.3, 0.5, 3.4), (0, 0, 0), fov_deg=40)
@@ -472,6 +480,24 @@ def cpu_reference_texture(W, nthreads=0):
             "reference" if use_ref else "port")
 
 
+def cpu_reference_solids(W, nthreads=0, stride=16):
+    """SolidAccel::Build32 of the mesh and Traverse of every stride-th ray on
+    the host: the reference's own code (oracle/_ref) or else the
+    restatement, OpenMP over all cores.  Returns (Mrays/s, build s, trace s
+    scaled, rays traced, kind)."""
+    from oracle import oracle as O
+    use_ref = O.have_ref() and O.ref() is not None
+    t0 = time.perf_counter()
+    acc = (O.RefSolids if use_ref else O.OracleSolids)(8, W["verts"], W["prims"])
+    tb = time.perf_counter() - t0
+    sample = W["rays"][::stride]
+    t0 = time.perf_counter()
+    acc.trace(sample, nthreads=nthreads)
+    tt = (time.perf_counter() - t0) * stride
+    return (W["rays"].size / (tb + tt) / 1e6, tb, tt, sample.size,
+            "reference" if use_ref else "port")
+
+
 def cpu_reference_lines(W, nthreads=0, stride=4):
     """LineAccel::Traverse of every stride-th ray on the host: the
     reference's own code (oracle/_ref) or else the restatement, OpenMP over
@@ -500,8 +526,8 @@ def run_reference_arm(args, W):
     cores = os.cpu_count() or 1
     step = {"batched": cpu_reference_batched, "sphere": cpu_reference_particles,
             "frame": cpu_reference_frame, "scene": cpu_reference_scene,
-            "texture": cpu_reference_texture, "lines": cpu_reference_lines}.get(
-                W["kind"], cpu_reference_step)
+            "texture": cpu_reference_texture, "lines": cpu_reference_lines,
+            "solids": cpu_reference_solids}.get(W["kind"], cpu_reference_step)
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
@@ -528,6 +554,10 @@ def run_reference_arm(args, W):
                   f"4th pixel ({ns} of {nr}) scaled to all, by the CPU restatement "
                   f"(OpenMP; the reference's RenderGraph needs its GL front end); median "
                   f"of {args.steps}")
+    if W["kind"] == "solids":
+        sample = (f"full Build32 + every 16th ray ({ns} of {nr}) per step through the "
+                  f"reference's own SolidAccel (OpenMP, {cores} threads), trace time scaled "
+                  f"to all rays; median of {args.steps}")
     if W["kind"] == "lines":
         sample = (f"every 4th ray ({ns} of {nr}) per step through the reference's own "
                   f"LineAccel::Traverse (OpenMP, {cores} threads; accel built once), "
@@ -540,7 +570,8 @@ def run_reference_arm(args, W):
         "impl": "reference",
         "metric": {"batched": METRIC_BATCH, "sphere": METRIC_PART,
                    "frame": METRIC_FRAME, "scene": METRIC_SCENE,
-                   "texture": METRIC_TEX, "lines": METRIC_LINES}.get(W["kind"], METRIC),
+                   "texture": METRIC_TEX, "lines": METRIC_LINES,
+                   "solids": METRIC_SOLIDS}.get(W["kind"], METRIC),
         "value": round(value, 4), "unit": unit,
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
@@ -567,9 +598,11 @@ METRIC_SCENE = ("Mrays/s (scene frame: top-level build + eye rays + closest hit 
                 "transformed elements + framebuffer write per step)")
 METRIC_TEX = "Mfetches/s (sparse volume texture3D fetch per step)"
 METRIC_LINES = "Mrays/s (capped-cylinder line accel: closest hit + normal per step)"
+METRIC_SOLIDS = "Mrays/s (hexahedron solid accel: Build32 + closest hit per step)"
 DTYPE = {"tet": "f32 boxes / f64 Pluecker", "tri": "f32", "sphere": "f32 (f64 discriminant)",
          "texture": "u8 texels / f64 block tree",
          "lines": "f32 (f64 quadratic root)",
+         "solids": "f32 boxes / f64 Pluecker",
          "volume": "f32", "batched": "f32", "frame": "f32",
          "scene": "f64 transforms and top-level boxes / f32 + f64 element tests"}
 
@@ -945,6 +978,133 @@ def run_lines(args, W):
             "config": dict(W["config"], l2="flushed between steps (256 MiB write)"),
             "build_ms_host": round(1e3 * build_s, 1), "clocks": clk.summary(), "e2e": e2e,
             "gpu_launches": int(launches), "roofline": roofline, "cpu_baseline": cpu}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    acc.close()
+    dist_teardown()
+
+
+# ---------------------------------------------------------------- solids
+def run_solids(args, W):
+    """Build32 of the resident mesh + closest hit (position and normal) of
+    every ray per step.  e2e: mesh and rays from pinned host memory in, hits
+    back, every step."""
+    import torch
+
+    from surface_b200 import _lib
+    from surface_b200.solids import Solid, SolidAccel
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(dev)
+    torch.cuda.set_stream(stream)
+    world, rank = dist_setup(dev)
+    L = _lib.load()
+    acc = SolidAccel(device=dev.index)
+    v = torch.as_tensor(W["verts"], device=dev)
+    ix = torch.as_tensor(W["prims"].astype(np.int32), device=dev)
+    rays_np = W["rays"]
+    n = rays_np.size
+    rays = torch.from_numpy(rays_np.view(np.float32).reshape(-1, 8)).to(dev)
+    hits = torch.empty((n, 4), dtype=torch.float32, device=dev)
+    nrm = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    pos = torch.empty((n, 3), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    from surface_b200._lib import check
+
+    def step():
+        acc.Build32(Solid(8, v, ix))
+        acc.ctx.use_torch_stream()
+        check(L.srt_solid_trace(acc.h, rays.data_ptr(), n, hits.data_ptr(), nrm.data_ptr(),
+                                pos.data_ptr()))
+
+    for _ in range(max(args.warmup, 3)):
+        step()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+          for _ in range(args.steps)]
+    tev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+           for _ in range(args.steps)]
+    with ClockSampler(dev.index) as clk:
+        clk.keep_busy(step, torch.cuda.synchronize)
+        barrier()
+        torch.cuda.synchronize()
+        launches0 = L.srt_ctx_launch_count(acc.ctx.h)
+        for k in range(args.steps):
+            flush.zero_()
+            ev[k][0].record()
+            acc.Build32(Solid(8, v, ix))
+            acc.ctx.use_torch_stream()
+            tev[k][0].record()
+            check(L.srt_solid_trace(acc.h, rays.data_ptr(), n, hits.data_ptr(),
+                                    nrm.data_ptr(), pos.data_ptr()))
+            tev[k][1].record()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        barrier()
+        launches = L.srt_ctx_launch_count(acc.ctx.h) - launches0
+        clk.keep_busy(step, torch.cuda.synchronize, extra=1)
+    ms, tms = max_over_ranks([statistics.mean(a.elapsed_time(b) for a, b in ev),
+                              statistics.mean(a.elapsed_time(b) for a, b in tev)], dev)
+    value = whole_job_mrays(n, world, ms)
+
+    h_v = torch.from_numpy(W["verts"]).pin_memory()
+    h_ix = torch.from_numpy(W["prims"].astype(np.int32)).pin_memory()
+    h_rays = torch.from_numpy(rays_np.view(np.float32).reshape(-1, 8).copy()).pin_memory()
+    h_hits = torch.empty((n, 4), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        v.copy_(h_v, non_blocking=True)
+        ix.copy_(h_ix, non_blocking=True)
+        rays.copy_(h_rays, non_blocking=True)
+        step()
+        h_hits.copy_(hits, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+
+    for _ in range(max(args.warmup, 3)):
+        e2e_step()
+    e2e_s = []
+    for _ in range(args.steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        e2e_step()
+        e2e_s.append(time.perf_counter() - t0)
+    e2e_ms = max_over_ranks([1e3 * sum(e2e_s) / len(e2e_s)], dev)[0]
+    e2e = {"value": round(whole_job_mrays(n, world, e2e_ms), 3), "unit": "Mrays/s",
+           "h2d_bytes_per_step": int((h_v.numel() + h_ix.numel() + h_rays.numel()) * 4),
+           "d2h_bytes_per_step": int(h_hits.numel() * 4), "ms_per_step": round(e2e_ms, 3)}
+    # roofline of the trace kernel: ray (32) + hit, normal, position (40) per
+    # ray and the 112-byte solid records and 32-byte nodes it reads
+    hbm, src = peaks()
+    nn = acc.info()[1]
+    alg = n * (32 + 40) + 112 * W["prims"].shape[0] + 32 * nn
+    roofline = {"bound": "hbm", "kernel": "solid_trace_kernel<8>",
+                "achieved": round(alg / (tms * 1e-3) / 1e9, 1), "peak": hbm, "unit": "GB/s",
+                "frac": round(alg / (tms * 1e-3) / 1e9 / hbm, 4), "peak_source": src,
+                "traffic": None, "algorithmic_bytes_per_launch": int(alg),
+                "note": "unique bytes; the walk is FP64 compute bound (every box on the "
+                        "ray's line is visited, as in the reference)"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        from oracle import oracle as O
+        got = hits.cpu().numpy()[:: 97]
+        want, _, _ = O.OracleSolids(8, W["verts"], W["prims"]).trace(rays_np[:: 97])
+        if not np.array_equal(got.view(np.uint32), want.view(np.float32).reshape(-1, 4)
+                              .view(np.uint32)):
+            raise SystemExit("solid hits differ from the oracle")
+        cv, tb, tt, ns, kind = cpu_reference_solids(W)
+        cpu = {"value": round(cv, 3), "unit": "Mrays/s", "cores": os.cpu_count(),
+               "kind": kind, "sample": f"full Build32 + every 16th ray ({ns}), OpenMP over "
+                                       f"{os.cpu_count()} threads, trace scaled to all rays",
+               "build_s": round(tb, 3), "trace_s": round(tt, 3)}
+    line = {"metric": METRIC_SOLIDS, "value": round(value, 3), "unit": "Mrays/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms, 4), "trace_ms": round(tms, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": DTYPE["solids"], "data": "synthetic",
+            "config": dict(W["config"], l2="flushed between steps (256 MiB write)"),
+            "clocks": clk.summary(), "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roofline, "cpu_baseline": cpu}
     if rank == 0:
         print(json.dumps(line), flush=True)
     acc.close()
@@ -1820,7 +1980,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
                     choices=["tet", "tri", "particles", "volume", "batched", "frame",
-                             "scene", "texture", "lines"])
+                             "scene", "texture", "lines", "solids"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
@@ -1848,6 +2008,8 @@ def main():
         run_texture(args, W)
     elif args.workload == "lines":
         run_lines(args, W)
+    elif args.workload == "solids":
+        run_solids(args, W)
     else:
         run_ours(args, W)
 

@@ -233,41 +233,94 @@ __device__ __forceinline__ void s_params(SIsect is[2], D3 org, D3 dir) {
   for (int k = 0; k < 3; k++) is[1].nrm[k] = -1.0f * is[1].nrm[k];
 }
 
-template <int NE, int MOD>
-__device__ __forceinline__ void s_weights(const D3 *e, const D3 *v, D3 dir, D3 org, double *ws,
-                                          bool (&c0)[NE], bool (&c1)[NE]) {
+// Edges of each solid (GetEdges, :119-154): edge i = vertex hi[i] - vertex
+// lo[i]; the Pluecker moment of edge i uses vertex i % MOD (:470).
+template <int NV>
+struct SolidTab;
+template <>
+struct SolidTab<5> {
+  static constexpr int NE = 8, MOD = 4;
+  __device__ static int hi(int i) {
+    constexpr int t[8] = {1, 2, 3, 0, 4, 4, 4, 4};
+    return t[i];
+  }
+  __device__ static int lo(int i) {
+    constexpr int t[8] = {0, 1, 2, 3, 0, 1, 2, 3};
+    return t[i];
+  }
+};
+template <>
+struct SolidTab<6> {
+  static constexpr int NE = 9, MOD = 6;
+  __device__ static int hi(int i) {
+    constexpr int t[9] = {1, 2, 0, 4, 5, 3, 3, 4, 5};
+    return t[i];
+  }
+  __device__ static int lo(int i) {
+    constexpr int t[9] = {0, 1, 2, 3, 4, 5, 0, 1, 2};
+    return t[i];
+  }
+};
+template <>
+struct SolidTab<8> {
+  static constexpr int NE = 12, MOD = 8;
+  __device__ static int hi(int i) {
+    constexpr int t[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
+    return t[i];
+  }
+  __device__ static int lo(int i) {
+    constexpr int t[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
+    return t[i];
+  }
+};
+
+// One solid's vertices (floats, exactly as stored) read as doubles on use;
+// edges are recomputed from them (the same double subtraction each time).
+template <int NV>
+struct SolidV {
+  float x[NV][3];
+  __device__ __forceinline__ D3 v(int k) const {
+    return {(double)x[k][0], (double)x[k][1], (double)x[k][2]};
+  }
+  __device__ __forceinline__ D3 e(int i) const {
+    return dsub(v(SolidTab<NV>::hi(i)), v(SolidTab<NV>::lo(i)));
+  }
+};
+
+// ws[i] = dir . (e_i x v_{i % MOD}) + e_i . (dir x org) (:467-476)
+template <int NV>
+__device__ __forceinline__ void s_weights(const SolidV<NV> &S, D3 dir, D3 org,
+                                          double (&ws)[SolidTab<NV>::NE]) {
   const D3 rpc = dcross(dir, org);
 #pragma unroll
-  for (int i = 0; i < NE; i++) {
-    ws[i] = ddot(dir, dcross(e[i], v[i % MOD])) + ddot(e[i], rpc);
-    c0[i] = ws[i] >= 0;
-    c1[i] = ws[i] <= 0;
+  for (int i = 0; i < SolidTab<NV>::NE; i++) {
+    const D3 ei = S.e(i);
+    ws[i] = ddot(dir, dcross(ei, S.v(i % SolidTab<NV>::MOD))) + ddot(ei, rpc);
   }
 }
 
 // IntersectPyramidD (:455-505)
-__device__ bool s_pyramid(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
-  const D3 e[8] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[3], v[2]), dsub(v[0], v[3]),
-                   dsub(v[4], v[0]), dsub(v[4], v[1]), dsub(v[4], v[2]), dsub(v[4], v[3])};
+__device__ bool s_pyramid(D3 org, D3 dir, const SolidV<5> &S, SIsect is[2]) {
   double ws[8];
-  bool cw[2][8];
-  s_weights<8, 4>(e, v, dir, org, ws, cw[0], cw[1]);
+  s_weights<5>(S, dir, org, ws);
   for (int i = 1, n = 0; n < 2; i--, n++) {
-    if (cw[i][0] && cw[i][1] && cw[i][2] && cw[i][3]) {
-      s_quad(is[n].pos, v[0], v[1], v[2], ws[0], ws[1], ws[2], ws[3], e[2], e[3], dir);
-      s_unit(dcross(e[1], e[0]), is[n].nrm);
-    } else if (cw[n][0] && cw[i][4] && cw[n][5]) {
-      s_tri(is[n].pos, v[4], -ws[0], v[1], ws[4], v[0], -ws[5], -ws[0] + ws[4] - ws[5]);
-      s_unit(dcross(e[4], e[0]), is[n].nrm);
-    } else if (cw[n][1] && cw[i][5] && cw[n][6]) {
-      s_tri(is[n].pos, v[4], -ws[1], v[2], ws[5], v[1], -ws[6], -ws[1] + ws[5] - ws[6]);
-      s_unit(dcross(e[5], e[1]), is[n].nrm);
-    } else if (cw[n][2] && cw[i][6] && cw[n][7]) {
-      s_tri(is[n].pos, v[4], -ws[2], v[3], ws[6], v[2], -ws[7], -ws[2] + ws[6] - ws[7]);
-      s_unit(dcross(e[6], e[2]), is[n].nrm);
-    } else if (cw[n][3] && cw[i][7] && cw[n][4]) {
-      s_tri(is[n].pos, v[4], -ws[3], v[0], ws[7], v[3], -ws[4], -ws[3] + ws[7] - ws[4]);
-      s_unit(dcross(e[7], e[3]), is[n].nrm);
+    // cw[0][k]: ws[k] >= 0, cw[1][k]: ws[k] <= 0
+    auto cw = [&](int side, int k) { return side == 0 ? ws[k] >= 0 : ws[k] <= 0; };
+    if (cw(i, 0) && cw(i, 1) && cw(i, 2) && cw(i, 3)) {
+      s_quad(is[n].pos, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3), dir);
+      s_unit(dcross(S.e(1), S.e(0)), is[n].nrm);
+    } else if (cw(n, 0) && cw(i, 4) && cw(n, 5)) {
+      s_tri(is[n].pos, S.v(4), -ws[0], S.v(1), ws[4], S.v(0), -ws[5], -ws[0] + ws[4] - ws[5]);
+      s_unit(dcross(S.e(4), S.e(0)), is[n].nrm);
+    } else if (cw(n, 1) && cw(i, 5) && cw(n, 6)) {
+      s_tri(is[n].pos, S.v(4), -ws[1], S.v(2), ws[5], S.v(1), -ws[6], -ws[1] + ws[5] - ws[6]);
+      s_unit(dcross(S.e(5), S.e(1)), is[n].nrm);
+    } else if (cw(n, 2) && cw(i, 6) && cw(n, 7)) {
+      s_tri(is[n].pos, S.v(4), -ws[2], S.v(3), ws[6], S.v(2), -ws[7], -ws[2] + ws[6] - ws[7]);
+      s_unit(dcross(S.e(6), S.e(2)), is[n].nrm);
+    } else if (cw(n, 3) && cw(i, 7) && cw(n, 4)) {
+      s_tri(is[n].pos, S.v(4), -ws[3], S.v(0), ws[7], S.v(3), -ws[4], -ws[3] + ws[7] - ws[4]);
+      s_unit(dcross(S.e(7), S.e(3)), is[n].nrm);
     } else {
       return false;
     }
@@ -277,29 +330,26 @@ __device__ bool s_pyramid(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
 }
 
 // IntersectPrismD (:559-611)
-__device__ bool s_prism(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
-  const D3 e[9] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[0], v[2]),
-                   dsub(v[4], v[3]), dsub(v[5], v[4]), dsub(v[3], v[5]),
-                   dsub(v[3], v[0]), dsub(v[4], v[1]), dsub(v[5], v[2])};
+__device__ bool s_prism(D3 org, D3 dir, const SolidV<6> &S, SIsect is[2]) {
   double ws[9];
-  bool cw[2][9];
-  s_weights<9, 6>(e, v, dir, org, ws, cw[0], cw[1]);
+  s_weights<6>(S, dir, org, ws);
   for (int i = 0, n = 1; i < 2; i++, n--) {
-    if (cw[n][0] && cw[n][1] && cw[n][2]) {
-      s_tri(is[i].pos, v[2], ws[0], v[0], ws[1], v[1], ws[2], ws[0] + ws[1] + ws[2]);
-      s_unit(dcross(e[0], e[1]), is[i].nrm);
-    } else if (cw[i][3] && cw[i][4] && cw[i][5]) {
-      s_tri(is[i].pos, v[5], ws[3], v[3], ws[4], v[4], ws[5], ws[3] + ws[4] + ws[5]);
-      s_unit(dcross(e[3], e[4]), is[i].nrm);
-    } else if (cw[i][2] && cw[i][6] && cw[n][5] && cw[n][8]) {
-      s_quad(is[i].pos, v[2], v[0], v[3], ws[2], ws[6], -ws[5], -ws[8], e[5], e[8], dir);
-      s_unit(dcross(e[2], e[6]), is[i].nrm);
-    } else if (cw[i][0] && cw[i][7] && cw[n][3] && cw[n][6]) {
-      s_quad(is[i].pos, v[0], v[1], v[4], ws[0], ws[7], -ws[3], -ws[6], e[3], e[6], dir);
-      s_unit(dcross(e[0], e[7]), is[i].nrm);
-    } else if (cw[i][1] && cw[i][8] && cw[n][4] && cw[n][7]) {
-      s_quad(is[i].pos, v[1], v[2], v[5], ws[1], ws[8], -ws[4], -ws[7], e[4], e[7], dir);
-      s_unit(dcross(e[1], e[8]), is[i].nrm);
+    auto cw = [&](int side, int k) { return side == 0 ? ws[k] >= 0 : ws[k] <= 0; };
+    if (cw(n, 0) && cw(n, 1) && cw(n, 2)) {
+      s_tri(is[i].pos, S.v(2), ws[0], S.v(0), ws[1], S.v(1), ws[2], ws[0] + ws[1] + ws[2]);
+      s_unit(dcross(S.e(0), S.e(1)), is[i].nrm);
+    } else if (cw(i, 3) && cw(i, 4) && cw(i, 5)) {
+      s_tri(is[i].pos, S.v(5), ws[3], S.v(3), ws[4], S.v(4), ws[5], ws[3] + ws[4] + ws[5]);
+      s_unit(dcross(S.e(3), S.e(4)), is[i].nrm);
+    } else if (cw(i, 2) && cw(i, 6) && cw(n, 5) && cw(n, 8)) {
+      s_quad(is[i].pos, S.v(2), S.v(0), S.v(3), ws[2], ws[6], -ws[5], -ws[8], S.e(5), S.e(8), dir);
+      s_unit(dcross(S.e(2), S.e(6)), is[i].nrm);
+    } else if (cw(i, 0) && cw(i, 7) && cw(n, 3) && cw(n, 6)) {
+      s_quad(is[i].pos, S.v(0), S.v(1), S.v(4), ws[0], ws[7], -ws[3], -ws[6], S.e(3), S.e(6), dir);
+      s_unit(dcross(S.e(0), S.e(7)), is[i].nrm);
+    } else if (cw(i, 1) && cw(i, 8) && cw(n, 4) && cw(n, 7)) {
+      s_quad(is[i].pos, S.v(1), S.v(2), S.v(5), ws[1], ws[8], -ws[4], -ws[7], S.e(4), S.e(7), dir);
+      s_unit(dcross(S.e(1), S.e(8)), is[i].nrm);
     } else {
       return false;
     }
@@ -309,38 +359,48 @@ __device__ bool s_prism(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
 }
 
 // IntersectHexaD (:664-716)
-__device__ bool s_hexa(D3 org, D3 dir, const D3 *v, SIsect is[2]) {
-  const D3 e[12] = {dsub(v[1], v[0]), dsub(v[2], v[1]), dsub(v[3], v[2]), dsub(v[0], v[3]),
-                    dsub(v[5], v[4]), dsub(v[6], v[5]), dsub(v[7], v[6]), dsub(v[4], v[7]),
-                    dsub(v[4], v[0]), dsub(v[5], v[1]), dsub(v[6], v[2]), dsub(v[7], v[3])};
+__device__ bool s_hexa(D3 org, D3 dir, const SolidV<8> &S, SIsect is[2]) {
   double ws[12];
-  bool cw[2][12];
-  s_weights<12, 8>(e, v, dir, org, ws, cw[0], cw[1]);
+  s_weights<8>(S, dir, org, ws);
   for (int i = 0, n = 1; i < 2; i++, n--) {
-    if (cw[n][0] && cw[n][1] && cw[n][2] && cw[n][3]) {
-      s_quad(is[i].pos, v[0], v[1], v[2], ws[0], ws[1], ws[2], ws[3], e[2], e[3], dir);
-      s_unit(dcross(e[0], e[1]), is[i].nrm);
-    } else if (cw[i][4] && cw[i][5] && cw[i][6] && cw[i][7]) {
-      s_quad(is[i].pos, v[4], v[5], v[6], ws[4], ws[5], ws[6], ws[7], e[6], e[7], dir);
-      s_unit(dcross(e[4], e[5]), is[i].nrm);
-    } else if (cw[i][0] && cw[i][9] && cw[n][4] && cw[n][8]) {
-      s_quad(is[i].pos, v[0], v[1], v[5], ws[0], ws[9], -ws[4], -ws[8], e[4], e[8], dir);
-      s_unit(dcross(e[0], e[9]), is[i].nrm);
-    } else if (cw[i][1] && cw[i][10] && cw[n][5] && cw[n][9]) {
-      s_quad(is[i].pos, v[1], v[2], v[6], ws[1], ws[10], -ws[5], -ws[9], e[5], e[9], dir);
-      s_unit(dcross(e[1], e[10]), is[i].nrm);
-    } else if (cw[i][2] && cw[i][11] && cw[n][6] && cw[n][10]) {
-      s_quad(is[i].pos, v[2], v[3], v[7], ws[2], ws[11], -ws[6], -ws[10], e[6], e[10], dir);
-      s_unit(dcross(e[2], e[11]), is[i].nrm);
-    } else if (cw[i][3] && cw[i][8] && cw[n][7] && cw[n][11]) {
-      s_quad(is[i].pos, v[3], v[0], v[4], ws[3], ws[8], -ws[7], -ws[11], e[7], e[11], dir);
-      s_unit(dcross(e[3], e[8]), is[i].nrm);
+    auto cw = [&](int side, int k) { return side == 0 ? ws[k] >= 0 : ws[k] <= 0; };
+    if (cw(n, 0) && cw(n, 1) && cw(n, 2) && cw(n, 3)) {
+      s_quad(is[i].pos, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3), dir);
+      s_unit(dcross(S.e(0), S.e(1)), is[i].nrm);
+    } else if (cw(i, 4) && cw(i, 5) && cw(i, 6) && cw(i, 7)) {
+      s_quad(is[i].pos, S.v(4), S.v(5), S.v(6), ws[4], ws[5], ws[6], ws[7], S.e(6), S.e(7), dir);
+      s_unit(dcross(S.e(4), S.e(5)), is[i].nrm);
+    } else if (cw(i, 0) && cw(i, 9) && cw(n, 4) && cw(n, 8)) {
+      s_quad(is[i].pos, S.v(0), S.v(1), S.v(5), ws[0], ws[9], -ws[4], -ws[8], S.e(4), S.e(8), dir);
+      s_unit(dcross(S.e(0), S.e(9)), is[i].nrm);
+    } else if (cw(i, 1) && cw(i, 10) && cw(n, 5) && cw(n, 9)) {
+      s_quad(is[i].pos, S.v(1), S.v(2), S.v(6), ws[1], ws[10], -ws[5], -ws[9], S.e(5), S.e(9),
+             dir);
+      s_unit(dcross(S.e(1), S.e(10)), is[i].nrm);
+    } else if (cw(i, 2) && cw(i, 11) && cw(n, 6) && cw(n, 10)) {
+      s_quad(is[i].pos, S.v(2), S.v(3), S.v(7), ws[2], ws[11], -ws[6], -ws[10], S.e(6), S.e(10),
+             dir);
+      s_unit(dcross(S.e(2), S.e(11)), is[i].nrm);
+    } else if (cw(i, 3) && cw(i, 8) && cw(n, 7) && cw(n, 11)) {
+      s_quad(is[i].pos, S.v(3), S.v(0), S.v(4), ws[3], ws[8], -ws[7], -ws[11], S.e(7), S.e(11),
+             dir);
+      s_unit(dcross(S.e(3), S.e(8)), is[i].nrm);
     } else {
       return false;
     }
   }
   s_params(is, org, dir);
   return true;
+}
+
+__device__ __forceinline__ bool s_isect(D3 org, D3 dir, const SolidV<5> &S, SIsect is[2]) {
+  return s_pyramid(org, dir, S, is);
+}
+__device__ __forceinline__ bool s_isect(D3 org, D3 dir, const SolidV<6> &S, SIsect is[2]) {
+  return s_prism(org, dir, S, is);
+}
+__device__ __forceinline__ bool s_isect(D3 org, D3 dir, const SolidV<8> &S, SIsect is[2]) {
+  return s_hexa(org, dir, S, is);
 }
 
 // IntersectRayAABB (:2160-2204) with the reference's selection order.
@@ -361,8 +421,11 @@ __device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], co
   return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= FLT_MAX);
 }
 
+#ifndef SRT_SOLID_MIN_BLOCKS
+#define SRT_SOLID_MIN_BLOCKS 1
+#endif
 template <int NV>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, SRT_SOLID_MIN_BLOCKS)
 solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
                    const srt_ray *__restrict__ rays, size_t n, srt_hit *__restrict__ hits,
                    float *__restrict__ normals, float *__restrict__ positions) {
@@ -405,15 +468,13 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
         const float *r = recs + (size_t)RF * (first + j);
         const uint32_t p = __float_as_uint(__ldg(r + 3 * NV));
         if (p == prev) continue;  // Ray::prev_prim_id
-        D3 v[NV];
+        SolidV<NV> S;
 #pragma unroll
         for (int k = 0; k < NV; k++)
-          v[k] = {(double)__ldg(r + 3 * k), (double)__ldg(r + 3 * k + 1),
-                  (double)__ldg(r + 3 * k + 2)};
+          for (int c = 0; c < 3; c++) S.x[k][c] = __ldg(r + 3 * k + c);
         SIsect is[2];
         for (int s = 0; s < 2; s++) is[s].t = 0.0f;
-        const bool h = NV == 5 ? s_pyramid(dorg, ddir, v, is)
-                               : (NV == 6 ? s_prism(dorg, ddir, v, is) : s_hexa(dorg, ddir, v, is));
+        const bool h = s_isect(dorg, ddir, S, is);
         if (!h) continue;
         for (int s = 0; s < 2; s++)
           if (is[s].t >= 0.0f && is[s].t < t) {
