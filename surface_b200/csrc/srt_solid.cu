@@ -1,17 +1,18 @@
 // srt_solid.cu -- SolidAccel (render/render_accel_solid.cc) on the GPU:
 // pyramids (5 vertices), prisms (6) and hexahedra (8), closest hit.
 //
-// Build (SolidAccel::Build32, :1795-2124): the scene box (every vertex
-// -+ FLT_EPSILON * 16) and the quantisation constants on the host; on the
-// GPU the Morton codes of the solids' centroids (the running sum of the
-// vertices times 1.0f / nv, render/render_prefix_tree_util.cc:347-382), the
-// stable 30-bit radix sort and the Karras split of every internal node
-// (ConstructBinaryRadixTree30) -- the stages the tetrahedra use; then on
-// the host the reference's top-down emission (BuildTreeRecursive32,
-// :1361-1453: a leaf for a Karras leaf, for up to 5 solids or below depth
-// 22; leaf boxes over the solids' vertices -+ FLT_EPSILON * 16, branch
-// boxes merged), in its pre-order.  A gather kernel copies each solid's
-// vertices into a record in leaf order.
+// Build (SolidAccel::Build32, :1795-2124) on the GPU: the scene box (every
+// vertex -+ FLT_EPSILON * 16, an order-free min / max), the Morton codes of
+// the solids' centroids (the running sum of the vertices times 1.0f / nv,
+// render/render_prefix_tree_util.cc:347-382), the stable 30-bit radix sort
+// and the Karras split of every internal node (ConstructBinaryRadixTree30)
+// -- the stages the tetrahedra use; the reference's top-down emission
+// order (BuildTreeRecursive32, :1361-1453: a leaf for a Karras leaf, for up
+// to 5 solids or below depth 22) is laid out on the host from the split
+// table alone, then the GPU fills the boxes: leaf boxes over the solids'
+// vertices -+ FLT_EPSILON * 16, branch boxes merged left then right, one
+// depth level at a time from the deepest.  A gather kernel copies each
+// solid's vertices into a record in leaf order.
 //
 // Trace (SolidAccel::Traverse, :2345-2435): one thread per ray, every
 // popped node tests its own box; a leaf whose box is hit tests its solids
@@ -23,6 +24,7 @@
 // contraction, so every double and float operation rounds as the
 // reference's x86-64 build does.
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -108,69 +110,120 @@ __global__ void solid_gather_kernel(const float *__restrict__ v, const uint32_t 
   }
 }
 
-struct Emitter {
-  const float *v;
-  const uint32_t *ix;
-  int nv;
-  const uint32_t *sidx, *code, *child;
-  const uint8_t *flags;  // bit 0: left child is a single key, bit 1: right
-  std::vector<SolidNodeH> &nodes;
+// order-preserving float -> int (for atomic min / max of non-NaN floats)
+__device__ __forceinline__ int f2o(float f) {
+  const int i = __float_as_int(f);
+  return i >= 0 ? i : i ^ 0x7fffffff;
+}
 
-  // ComputeBoundingBox30 (:1121-1169) over sorted solids [l, r).
-  void leaf_box(size_t l, size_t r, float bmin[3], float bmax[3]) const {
-    const float eps = FLT_EPSILON * 16;
-    const uint32_t f0 = ix[(size_t)nv * sidx[l]];
-    for (int k = 0; k < 3; k++) {
-      bmin[k] = v[3 * (size_t)f0 + k] - eps;
-      bmax[k] = v[3 * (size_t)f0 + k] + eps;
+// Scene box: min / max of every referenced vertex -+ FLT_EPSILON * 16
+// (ComputeBoundingBoxOMP; min and max do not depend on the order), and a
+// flag for an index at or beyond nverts.  box: 3 mins then 3 maxes as
+// ordered ints, initialised to INT_MAX / INT_MIN.
+__global__ void solid_box_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+                                 size_t refs, size_t nverts, int *__restrict__ box,
+                                 uint32_t *__restrict__ bad) {
+  const float eps = FLT_EPSILON * 16;
+  int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
+  bool oob = false;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < refs;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t f = ix[i];
+    if (f >= nverts) {
+      oob = true;
+      continue;
     }
-    for (size_t i = l; i < r; i++)
-      for (int j = 0; j < nv; j++) {
-        const uint32_t f = ix[(size_t)nv * sidx[i] + j];
+    for (int k = 0; k < 3; k++) {
+      const float x = v[3 * (size_t)f + k];
+      lo[k] = min(lo[k], f2o(x - eps));
+      hi[k] = max(hi[k], f2o(x + eps));
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1)
+    for (int k = 0; k < 3; k++) {
+      lo[k] = min(lo[k], __shfl_xor_sync(0xffffffffu, lo[k], o));
+      hi[k] = max(hi[k], __shfl_xor_sync(0xffffffffu, hi[k], o));
+    }
+  if (__any_sync(0xffffffffu, oob) && (threadIdx.x & 31) == 0) atomicOr(bad, 1u);
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 3; k++) {
+      atomicMin(&box[k], lo[k]);
+      atomicMax(&box[3 + k], hi[k]);
+    }
+}
+
+// Leaf boxes (ComputeBoundingBox30, :1121-1169): node ids of the leaves in
+// leaves[], each over its sorted solids.
+__global__ void solid_leafbox_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+                                     const uint32_t *__restrict__ order, int nv,
+                                     const uint32_t *__restrict__ leaves, size_t nleaves,
+                                     SNode *__restrict__ nodes) {
+  const float eps = FLT_EPSILON * 16;
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < nleaves;
+       j += (size_t)gridDim.x * blockDim.x) {
+    SNode &nd = nodes[leaves[j]];
+    const uint32_t first = nd.w0, cnt = nd.w1 & ~kSolidLeaf;
+    const uint32_t f0 = ix[(size_t)nv * order[first]];
+    float lo[3], hi[3];
+    for (int k = 0; k < 3; k++) {
+      lo[k] = v[3 * (size_t)f0 + k] - eps;
+      hi[k] = v[3 * (size_t)f0 + k] + eps;
+    }
+    for (uint32_t i = first; i < first + cnt; i++)
+      for (int q = 0; q < nv; q++) {
+        const uint32_t f = ix[(size_t)nv * order[i] + q];
         for (int k = 0; k < 3; k++) {
-          const float lo = v[3 * (size_t)f + k] - eps, hi = v[3 * (size_t)f + k] + eps;
-          if (bmin[k] > lo) bmin[k] = lo;
-          if (bmax[k] < hi) bmax[k] = hi;
+          const float a = v[3 * (size_t)f + k] - eps, b = v[3 * (size_t)f + k] + eps;
+          if (lo[k] > a) lo[k] = a;
+          if (hi[k] < b) hi[k] = b;
         }
       }
+    for (int k = 0; k < 3; k++) {
+      nd.bmin[k] = lo[k];
+      nd.bmax[k] = hi[k];
+    }
   }
+}
+
+// Branch boxes of one depth level (MergeBoundingBox: std::min / std::max of
+// the left then the right child), deepest level first.
+__global__ void solid_merge_kernel(const uint32_t *__restrict__ ids, size_t n,
+                                   SNode *__restrict__ nodes) {
+  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
+       j += (size_t)gridDim.x * blockDim.x) {
+    SNode &nd = nodes[ids[j]];
+    const SNode &l = nodes[nd.w0], &r = nodes[nd.w1 & 0x1fffffffu];
+    for (int k = 0; k < 3; k++) {
+      nd.bmin[k] = (r.bmin[k] < l.bmin[k]) ? r.bmin[k] : l.bmin[k];
+      nd.bmax[k] = (l.bmax[k] < r.bmax[k]) ? r.bmax[k] : l.bmax[k];
+    }
+  }
+}
+
+// The reference's emission order (BuildTreeRecursive32, :1361-1453) on the
+// host, topology only: device nodes in pre-order, each node's depth.
+struct Topology {
+  const uint32_t *code, *child;
+  const uint8_t *flags;  // bit 0: left child is a single key, bit 1: right
+  std::vector<SNode> &nodes;
+  std::vector<int> &depth;
 
   static int axis_of(uint32_t c) { return ((c ? __builtin_clz(c) : 32) - 2) % 3; }
 
-  static void merge(const float a0[3], const float a1[3], const float b0[3], const float b1[3],
-                    float bmin[3], float bmax[3]) {
-    for (int k = 0; k < 3; k++) {  // MergeBoundingBox: std::min / std::max
-      bmin[k] = (b0[k] < a0[k]) ? b0[k] : a0[k];
-      bmax[k] = (a1[k] < b1[k]) ? b1[k] : a1[k];
-    }
-  }
-
-  // keys [l, r] inclusive
-  size_t emit(uint32_t root, uint32_t l, uint32_t r, bool leaf, int depth, float bmin[3],
-              float bmax[3]) {
+  size_t emit(uint32_t root, uint32_t l, uint32_t r, bool leaf, int d) {
     const size_t off = nodes.size();
-    nodes.push_back(SolidNodeH{});
-    if (leaf || (r - l) <= 4 || depth > 22) {
-      leaf_box(l, (size_t)r + 1, bmin, bmax);
-      SolidNodeH &nd = nodes[off];
-      std::memcpy(nd.bmin, bmin, 12);
-      std::memcpy(nd.bmax, bmax, 12);
-      nd.flag = 1;
-      nd.data[0] = r + 1 - l;
-      nd.data[1] = l;
+    nodes.push_back(SNode{});
+    depth.push_back(d);
+    if (leaf || (r - l) <= 4 || d > 22) {
+      nodes[off].w0 = l;
+      nodes[off].w1 = kSolidLeaf | (r + 1 - l);
       return off;
     }
     const uint32_t mid = child[root];
-    float a0[3], a1[3], b0[3], b1[3];
-    const size_t left = emit(mid, l, mid, flags[root] & 1, depth + 1, a0, a1);
-    const size_t right = emit(mid + 1, mid + 1, r, flags[root] & 2, depth + 1, b0, b1);
-    merge(a0, a1, b0, b1, bmin, bmax);
-    SolidNodeH &nd = nodes[off];
-    nd.axis = axis_of(code[root]);
-    nd.data[0] = (uint32_t)left;
-    nd.data[1] = (uint32_t)right;
-    std::memcpy(nd.bmin, bmin, 12);
-    std::memcpy(nd.bmax, bmax, 12);
+    const size_t left = emit(mid, l, mid, flags[root] & 1, d + 1);
+    const size_t right = emit(mid + 1, mid + 1, r, flags[root] & 2, d + 1);
+    nodes[off].w0 = (uint32_t)left;
+    nodes[off].w1 = (uint32_t)right | ((uint32_t)axis_of(code[root]) << 29);
     return off;
   }
 };
@@ -511,19 +564,6 @@ srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
   return SRT_OK;
 }
 
-template <typename T>
-srt_status to_host(const T *p, size_t count, std::vector<T> &buf, const T **out) {
-  if (!srt::is_device_ptr(p)) {
-    *out = p;
-    return SRT_OK;
-  }
-  buf.resize(count ? count : 1);
-  cudaError_t e = cudaMemcpy(buf.data(), p, count * sizeof(T), cudaMemcpyDeviceToHost);
-  if (e != cudaSuccess) return srt::cuda_status(e, "solid input copy");
-  *out = buf.data();
-  return SRT_OK;
-}
-
 }  // namespace
 
 using namespace srt;
@@ -558,48 +598,52 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
   }
   srt_ctx *ctx = a->ctx;
   cudaSetDevice(ctx->device);
-  std::vector<float> hv;
-  std::vector<uint32_t> hi;
-  const float *v;
-  const uint32_t *ix;
-  srt_status s = to_host(vertices, nverts * 3, hv, &v);
-  if (s == SRT_OK) s = to_host(indices, nsolids * nv, hi, &ix);
-  if (s != SRT_OK) return s;
-  for (size_t i = 0; i < nsolids * (size_t)nv; i++)
-    if (ix[i] >= nverts) {
-      set_error("srt_solid_build: an index names a vertex beyond nverts");
-      return SRT_ERR_INVALID;
-    }
-  // scene box (ComputeBoundingBoxOMP, :1171-1262; min and max in any order)
-  const float eps = FLT_EPSILON * 16;
-  float lo[3], hi3[3];
-  for (int k = 0; k < 3; k++) lo[k] = hi3[k] = v[3 * (size_t)ix[0] + k];
-  for (int k = 0; k < 3; k++) {
-    lo[k] -= eps;
-    hi3[k] += eps;
-  }
-  for (size_t i = 0; i < nsolids * (size_t)nv; i++)
-    for (int k = 0; k < 3; k++) {
-      const float x0 = v[3 * (size_t)ix[i] + k] - eps, x1 = v[3 * (size_t)ix[i] + k] + eps;
-      lo[k] = (x0 < lo[k]) ? x0 : lo[k];
-      hi3[k] = (hi3[k] < x1) ? x1 : hi3[k];
-    }
-  float inv[3];
-  const int kdiv = 1 << 10;
-  for (int k = 0; k < 3; k++) inv[k] = kdiv / (hi3[k] - lo[k]);
-  DevBuf sv, si, codes, order, child, flags;
+  const size_t n = nsolids, refs = nsolids * (size_t)nv;
+  DevBuf sv, si, codes, order, child, flags, boxbuf, dleaves, dlevel;
   const void *dv, *di;
+  srt_status s;
   if ((s = solid_view(ctx, vertices, nverts * 12, sv, &dv)) != SRT_OK) return s;
-  if ((s = solid_view(ctx, indices, nsolids * nv * 4, si, &di)) != SRT_OK) return s;
+  if ((s = solid_view(ctx, indices, refs * 4, si, &di)) != SRT_OK) return s;
+  const float *d_v = static_cast<const float *>(dv);
+  const uint32_t *d_ix = static_cast<const uint32_t *>(di);
   cudaError_t e;
-  const size_t n = nsolids;
+  // scene box and index check on the GPU
+  int hbox[8] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN, 0, 0};
+  if ((e = boxbuf.ensure(sizeof(hbox))) != cudaSuccess ||
+      (e = cudaMemcpyAsync(boxbuf.p, hbox, sizeof(hbox), cudaMemcpyHostToDevice, ctx->stream)) !=
+          cudaSuccess)
+    return cuda_status(e, "solid box");
+  const unsigned gbox = (unsigned)std::min<size_t>((refs + 255) / 256, (size_t)ctx->num_sms * 8);
+  solid_box_kernel<<<gbox, 256, 0, ctx->stream>>>(d_v, d_ix, refs, nverts, boxbuf.as<int>(),
+                                                   reinterpret_cast<uint32_t *>(boxbuf.as<int>() + 6));
+  ctx->launches++;
+  if ((e = cudaMemcpyAsync(hbox, boxbuf.p, sizeof(hbox), cudaMemcpyDeviceToHost, ctx->stream)) !=
+          cudaSuccess ||
+      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid box");
+  if (hbox[6]) {
+    set_error("srt_solid_build: an index names a vertex beyond nverts");
+    return SRT_ERR_INVALID;
+  }
+  float lo[3], hi3[3], inv[3];
+  auto o2f_h = [](int i) {
+    const int b = i >= 0 ? i : i ^ 0x7fffffff;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+  };
+  const int kdiv = 1 << 10;
+  for (int k = 0; k < 3; k++) {
+    lo[k] = o2f_h(hbox[k]);
+    hi3[k] = o2f_h(hbox[3 + k]);
+    inv[k] = kdiv / (hi3[k] - lo[k]);
+  }
   if ((e = codes.ensure(n * 4)) != cudaSuccess || (e = order.ensure(n * 4)) != cudaSuccess ||
       (e = child.ensure(n * 4)) != cudaSuccess || (e = flags.ensure(n)) != cudaSuccess)
     return cuda_status(e, "solid build");
   const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
-  solid_morton_kernel<<<grid, 256, 0, ctx->stream>>>(
-      static_cast<const float *>(dv), static_cast<const uint32_t *>(di), nv, n, lo[0], lo[1],
-      lo[2], inv[0], inv[1], inv[2], codes.as<uint32_t>());
+  solid_morton_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, nv, n, lo[0], lo[1], lo[2],
+                                                      inv[0], inv[1], inv[2], codes.as<uint32_t>());
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid morton");
   if ((s = sort_pairs(ctx, codes.as<uint32_t>(), order.as<uint32_t>(), n, true, 30)) != SRT_OK)
@@ -619,44 +663,91 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
           cudaSuccess ||
       (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
     return cuda_status(e, "solid tree");
-  // the reference's emission (root first, then the left and right subtrees)
+  // topology on the host, in the reference's pre-order (root, left, right)
   a->built = false;
-  a->nodes.clear();
-  Emitter E{v, ix, nv, hidx.data(), hcode.data(), hchild.data(), hflags.data(), a->nodes};
-  a->nodes.push_back(SolidNodeH{});
-  float a0[3], a1[3], b0[3], b1[3];
+  std::vector<SNode> dn;
+  std::vector<int> depth;
+  dn.reserve(n);
+  depth.reserve(n);
+  Topology T{hcode.data(), hchild.data(), hflags.data(), dn, depth};
+  dn.push_back(SNode{});
+  depth.push_back(-1);
   const uint32_t mid = hchild[0];
-  const size_t left = E.emit(mid, 0, mid, hflags[0] & 1, 0, a0, a1);
-  const size_t right = E.emit(mid + 1, mid + 1, (uint32_t)n - 1, hflags[0] & 2, 0, b0, b1);
-  SolidNodeH &root = a->nodes[0];
-  Emitter::merge(a0, a1, b0, b1, root.bmin, root.bmax);
-  root.axis = Emitter::axis_of(hcode[0]);
-  root.data[0] = (uint32_t)left;
-  root.data[1] = (uint32_t)right;
-  a->idx = hidx;
-  std::vector<SNode> dn(a->nodes.size());
-  for (size_t i = 0; i < a->nodes.size(); i++) {
-    const SolidNodeH &h = a->nodes[i];
-    for (int k = 0; k < 3; k++) {
-      dn[i].bmin[k] = h.bmin[k];
-      dn[i].bmax[k] = h.bmax[k];
-    }
-    dn[i].w0 = h.flag ? h.data[1] : h.data[0];
-    dn[i].w1 = h.flag ? (kSolidLeaf | h.data[0]) : (h.data[1] | ((uint32_t)h.axis << 29));
+  const size_t left = T.emit(mid, 0, mid, hflags[0] & 1, 0);
+  const size_t right = T.emit(mid + 1, mid + 1, (uint32_t)n - 1, hflags[0] & 2, 0);
+  dn[0].w0 = (uint32_t)left;
+  dn[0].w1 = (uint32_t)right | ((uint32_t)Topology::axis_of(hcode[0]) << 29);
+  // leaves, then branches grouped by depth (deepest first) for the refit
+  int maxd = 0;
+  for (int d : depth) maxd = std::max(maxd, d);
+  std::vector<uint32_t> leaves, byd;
+  std::vector<size_t> start(maxd + 3, 0);
+  for (size_t i = 0; i < dn.size(); i++)
+    if (dn[i].w1 & kSolidLeaf)
+      leaves.push_back((uint32_t)i);
+    else
+      start[depth[i] + 2]++;
+  for (int d = 1; d < maxd + 3; d++) start[d] += start[d - 1];
+  byd.resize(start[maxd + 2]);
+  {
+    std::vector<size_t> fill(start.begin(), start.end());
+    for (size_t i = 0; i < dn.size(); i++)
+      if (!(dn[i].w1 & kSolidLeaf)) byd[fill[depth[i] + 1]++] = (uint32_t)i;
   }
   if ((e = a->dnodes.ensure(dn.size() * sizeof(SNode))) != cudaSuccess ||
-      (e = a->drecs.ensure(n * rec_floats(nv) * 4)) != cudaSuccess)
+      (e = a->drecs.ensure(n * rec_floats(nv) * 4)) != cudaSuccess ||
+      (e = dleaves.ensure(leaves.size() * 4)) != cudaSuccess ||
+      (e = dlevel.ensure(std::max<size_t>(byd.size(), 1) * 4)) != cudaSuccess)
     return cuda_status(e, "solid accel");
   if ((e = cudaMemcpyAsync(a->dnodes.p, dn.data(), dn.size() * sizeof(SNode),
-                           cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess)
+                           cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
+      (e = cudaMemcpyAsync(dleaves.p, leaves.data(), leaves.size() * 4, cudaMemcpyHostToDevice,
+                           ctx->stream)) != cudaSuccess ||
+      (byd.size() && (e = cudaMemcpyAsync(dlevel.p, byd.data(), byd.size() * 4,
+                                          cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess))
     return cuda_status(e, "solid nodes");
-  solid_gather_kernel<<<grid, 256, 0, ctx->stream>>>(
-      static_cast<const float *>(dv), static_cast<const uint32_t *>(di), order.as<uint32_t>(), nv,
-      n, a->drecs.as<float>());
+  SNode *d_nodes = a->dnodes.as<SNode>();
+  solid_leafbox_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order.as<uint32_t>(), nv,
+                                                       dleaves.as<uint32_t>(), leaves.size(),
+                                                       d_nodes);
+  ctx->launches++;
+  for (int d = maxd; d >= -1; d--) {  // depth -1 is the root
+    const size_t b0 = start[d + 1], b1 = start[d + 2];
+    if (b1 == b0) continue;
+    const unsigned gm = (unsigned)std::min<size_t>((b1 - b0 + 255) / 256, 1024);
+    solid_merge_kernel<<<gm, 256, 0, ctx->stream>>>(dlevel.as<uint32_t>() + b0, b1 - b0, d_nodes);
+    ctx->launches++;
+  }
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid refit");
+  solid_gather_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order.as<uint32_t>(), nv, n,
+                                                      a->drecs.as<float>());
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid records");
+  // the reference-layout copy (Dump, export, BoundingBox)
+  if ((e = cudaMemcpyAsync(dn.data(), d_nodes, dn.size() * sizeof(SNode), cudaMemcpyDeviceToHost,
+                           ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid nodes");
   // staged inputs and scratch are freed on return: finish with them first
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(e, "solid build");
+  a->nodes.resize(dn.size());
+  for (size_t i = 0; i < dn.size(); i++) {
+    SolidNodeH &h = a->nodes[i];
+    h = SolidNodeH{};
+    for (int k = 0; k < 3; k++) {
+      h.bmin[k] = dn[i].bmin[k];
+      h.bmax[k] = dn[i].bmax[k];
+    }
+    if (dn[i].w1 & kSolidLeaf) {
+      h.flag = 1;
+      h.data[0] = dn[i].w1 & ~kSolidLeaf;
+      h.data[1] = dn[i].w0;
+    } else {
+      h.axis = (int)(dn[i].w1 >> 29);
+      h.data[0] = dn[i].w0;
+      h.data[1] = dn[i].w1 & 0x1fffffffu;
+    }
+  }
+  a->idx = std::move(hidx);
   a->nv = nv;
   a->n = n;
   a->built = true;
