@@ -499,6 +499,22 @@ SRT_API srt_status srt_cache_build_spheres(srt_cache *cache, const srt_cache_key
                                            const float *radius, float constant_radius,
                                            size_t n, srt_accel **out);
 SRT_API srt_status srt_cache_invalidate(srt_cache *cache, uint64_t buffer);
+/* AccelBuilder::BuildLineAccel (gles/gles_accel_builder.cc:188-256) and
+ * BuildSolidAccel (:328-397): the same cache for line and solid accels
+ * (srt_line_build with LineBuildOptions' defaults and the given cap;
+ * srt_solid_build). */
+typedef struct srt_line_accel srt_line_accel;
+typedef struct srt_solid_accel srt_solid_accel;
+SRT_API srt_status srt_cache_build_lines(srt_cache *cache, const srt_cache_key *key,
+                                         int is_static, const float *positions, size_t nverts,
+                                         const float *radius, float constant_radius,
+                                         const uint32_t *segments, size_t nlines, int32_t cap,
+                                         srt_line_accel **out);
+SRT_API srt_status srt_cache_build_solids(srt_cache *cache, const srt_cache_key *key,
+                                          int is_static, int32_t verts_per_solid,
+                                          const float *vertices, size_t nverts,
+                                          const uint32_t *indices, size_t nsolids,
+                                          srt_solid_accel **out);
 SRT_API srt_status srt_cache_end_frame(srt_cache *cache);
 SRT_API srt_status srt_cache_info_get(srt_cache *cache, srt_cache_info *info);
 
@@ -563,7 +579,6 @@ SRT_API srt_status srt_batch_config(srt_batch *b, int32_t *block,
  * srt_line_dump LineAccel::Dump (:343, the same file format); srt_line_export
  * copies the tree in the Dump record layout (40 bytes per node) and the line
  * order. */
-typedef struct srt_line_accel srt_line_accel;
 SRT_API srt_status srt_line_create(srt_ctx *ctx, srt_line_accel **out);
 SRT_API srt_status srt_line_destroy(srt_line_accel *accel);
 SRT_API srt_status srt_line_build(srt_line_accel *accel, const float *positions,
@@ -592,7 +607,6 @@ SRT_API srt_status srt_line_dump(srt_line_accel *accel, const char *path);
  * SolidAccel::BoundingBox, srt_solid_dump SolidAccel::Dump (:2126, the same
  * file format); srt_solid_export copies the tree in the Dump record layout
  * (40 bytes per node) and the solid order. */
-typedef struct srt_solid_accel srt_solid_accel;
 SRT_API srt_status srt_solid_create(srt_ctx *ctx, srt_solid_accel **out);
 SRT_API srt_status srt_solid_destroy(srt_solid_accel *accel);
 SRT_API srt_status srt_solid_build(srt_solid_accel *accel, int32_t verts_per_solid,

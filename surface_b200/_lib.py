@@ -148,6 +148,9 @@ _SIGS = {
     "srt_line_info": [_P, _P, _P, _P],
     "srt_line_export": [_P, _P, _P],
     "srt_line_dump": [_P, C.c_char_p],
+    "srt_cache_build_lines": [_P, _P, C.c_int, _P, _SZ, _P, C.c_float, _P, _SZ, C.c_int32,
+                              C.POINTER(_P)],
+    "srt_cache_build_solids": [_P, _P, C.c_int, C.c_int32, _P, _SZ, _P, _SZ, C.POINTER(_P)],
     "srt_solid_create": [_P, C.POINTER(_P)],
     "srt_solid_destroy": [_P],
     "srt_solid_build": [_P, C.c_int32, _P, _SZ, _P, _SZ],

@@ -21,6 +21,8 @@ from . import _lib
 from ._lib import SRT_SPHERES, SRT_TETRAHEDRA, SRT_TRIANGLES, check
 from .accel import (Context, Mesh, ParticleAccel, Particles, TetraAccel, Tetrahedron,
                     TriangleAccel, _View, torch)
+from .lines import LineAccel, Lines
+from .solids import Solid, SolidAccel
 
 # Each Build* returns an accel object over the cached handle.
 
@@ -37,9 +39,12 @@ def _owned_by_cache(base):
     return Cached
 
 
+_LINES, _SOLIDS = 3, 4  # the cache's kinds beyond srt_kind
 _CACHED = {SRT_TRIANGLES: _owned_by_cache(TriangleAccel),
            SRT_TETRAHEDRA: _owned_by_cache(TetraAccel),
-           SRT_SPHERES: _owned_by_cache(ParticleAccel)}
+           SRT_SPHERES: _owned_by_cache(ParticleAccel),
+           _LINES: _owned_by_cache(LineAccel),
+           _SOLIDS: _owned_by_cache(SolidAccel)}
 
 
 class AccelBuilder:
@@ -101,6 +106,41 @@ class AccelBuilder:
                                              C.c_float(particles.constantRadius),
                                              p.nbytes // 12, C.byref(out)))
         return self._finish(SRT_SPHERES, out, (p, r), b0)
+
+    def BuildLineAccel(self, lines: Lines, elembuf, arraybuf, count, offset=0,
+                       position_offset=0, static=True, cap=True):
+        """AccelBuilder::BuildLineAccel (gles/gles_accel_builder.cc:188)."""
+        key = self._key(elembuf, arraybuf, position_offset, count, offset)
+        p = _View(lines.positions, np.float32, torch.float32)
+        s = _View(lines.segments, np.uint32, torch.int32)
+        r = _View(lines.radius, np.float32, torch.float32)
+        out = C.c_void_p()
+        b0 = self.info().builds
+        if p.device or s.device or (r.obj is not None and r.device):
+            torch.cuda.current_stream().synchronize()
+        self.ctx.use_own_stream()
+        check(self.L.srt_cache_build_lines(self.h, C.byref(key), int(static), p.ptr,
+                                           p.nbytes // 12, r.ptr,
+                                           C.c_float(lines.constantRadius), s.ptr,
+                                           s.nbytes // 8, int(cap), C.byref(out)))
+        return self._finish(_LINES, out, (p, s, r), b0)
+
+    def BuildSolidAccel(self, solids: Solid, elembuf, arraybuf, count, offset=0,
+                        position_offset=0, static=True):
+        """AccelBuilder::BuildSolidAccel (gles/gles_accel_builder.cc:328)."""
+        key = self._key(elembuf, arraybuf, position_offset, count, offset)
+        nv = int(solids.numVertsPerSolid)
+        v = _View(solids.vertices, np.float32, torch.float32)
+        ix = _View(solids.indices, np.uint32, torch.int32)
+        out = C.c_void_p()
+        b0 = self.info().builds
+        if v.device or ix.device:
+            torch.cuda.current_stream().synchronize()
+        self.ctx.use_own_stream()
+        check(self.L.srt_cache_build_solids(self.h, C.byref(key), int(static), nv, v.ptr,
+                                            v.nbytes // 12, ix.ptr, ix.nbytes // (4 * nv),
+                                            C.byref(out)))
+        return self._finish(_SOLIDS, out, (v, ix), b0)
 
     def Invalidate(self, buffer):
         check(self.L.srt_cache_invalidate(self.h, buffer))

@@ -269,10 +269,12 @@ srt_status load_common(srt_accel *a, srt_kind kind, const char *path, const floa
 struct srt_cache {
   srt_ctx *ctx = nullptr;
   uint64_t max_bytes = 0, used = 0, hits = 0, builds = 0;
+  // kind: an srt_kind, or kLines / kSolids; obj: srt_accel, srt_line_accel
+  // or srt_solid_accel
   struct Entry {
     srt_cache_key key;
-    srt_kind kind;
-    srt_accel *accel;
+    int kind;
+    void *obj;
     uint64_t bytes, hit_count;
   };
   std::vector<Entry> static_list, dynamic_list;
@@ -291,15 +293,34 @@ uint64_t accel_bytes(const srt_accel *a) {
          a->in_verts.cap + a->in_faces.cap + a->in_radius.cap;
 }
 
-void drop(srt_cache *c, srt_cache::Entry &e) {
-  c->used -= e.bytes;
-  srt_accel_destroy(e.accel);
-  e.accel = nullptr;
+constexpr int kLines = 3, kSolids = 4;  // cache kinds beyond srt_kind
+
+void destroy_obj(int kind, void *obj) {
+  if (kind == kLines)
+    srt_line_destroy(static_cast<srt_line_accel *>(obj));
+  else if (kind == kSolids)
+    srt_solid_destroy(static_cast<srt_solid_accel *>(obj));
+  else
+    srt_accel_destroy(static_cast<srt_accel *>(obj));
 }
 
-template <typename Build>
-srt_status cache_get(srt_cache *c, srt_kind kind, const srt_cache_key *key, int is_static,
-                     srt_accel **out, Build build) {
+uint64_t obj_bytes(int kind, void *obj) {
+  if (kind == kLines) return line_accel_bytes(static_cast<srt_line_accel *>(obj));
+  if (kind == kSolids) return solid_accel_bytes(static_cast<srt_solid_accel *>(obj));
+  return accel_bytes(static_cast<srt_accel *>(obj));
+}
+
+void drop(srt_cache *c, srt_cache::Entry &e) {
+  c->used -= e.bytes;
+  destroy_obj(e.kind, e.obj);
+  e.obj = nullptr;
+}
+
+// AccelBuilder's Build*Accel: Locate a static entry (the key and kind), else
+// create (create(&obj)), build (build(obj)) and keep a new one.
+template <typename T, typename Create, typename Build>
+srt_status cache_get(srt_cache *c, int kind, const srt_cache_key *key, int is_static, T **out,
+                     Create create, Build build) {
   if (!c || !key || !out) return fail(SRT_ERR_INVALID, "NULL argument");
   *out = nullptr;
   // Locate: the static entries only (a dynamic entry lives one frame)
@@ -307,23 +328,31 @@ srt_status cache_get(srt_cache *c, srt_kind kind, const srt_cache_key *key, int 
     if (e.kind == kind && same_key(e.key, *key)) {
       e.hit_count++;
       c->hits++;
-      *out = e.accel;
+      *out = static_cast<T *>(e.obj);
       return SRT_OK;
     }
-  srt_accel *a = nullptr;
-  srt_status s = srt_accel_create(c->ctx, kind, &a);
+  T *a = nullptr;
+  srt_status s = create(&a);
   if (s != SRT_OK) return s;
   s = build(a);
   if (s != SRT_OK) {
-    srt_accel_destroy(a);
+    destroy_obj(kind, a);
     return s;
   }
-  srt_cache::Entry e{*key, kind, a, accel_bytes(a), 1};
+  srt_cache::Entry e{*key, kind, a, obj_bytes(kind, a), 1};
   c->used += e.bytes;
   c->builds++;
   (is_static ? c->static_list : c->dynamic_list).push_back(e);
   *out = a;
   return SRT_OK;
+}
+
+template <typename Build>
+srt_status cache_get_accel(srt_cache *c, srt_kind kind, const srt_cache_key *key, int is_static,
+                           srt_accel **out, Build build) {
+  return cache_get<srt_accel>(
+      c, kind, key, is_static, out,
+      [&](srt_accel **a) { return srt_accel_create(c->ctx, kind, a); }, build);
 }
 
 }  // namespace
@@ -371,7 +400,7 @@ SRT_API srt_status srt_cache_build_triangles(srt_cache *c, const srt_cache_key *
                                              int is_static, const float *vertices,
                                              size_t nvertices, const uint32_t *faces,
                                              size_t nfaces, srt_accel **out) {
-  return cache_get(c, SRT_TRIANGLES, key, is_static, out, [&](srt_accel *a) {
+  return cache_get_accel(c, SRT_TRIANGLES, key, is_static, out, [&](srt_accel *a) {
     return srt_accel_build_triangles(a, vertices, nvertices, faces, nfaces);
   });
 }
@@ -380,7 +409,7 @@ SRT_API srt_status srt_cache_build_tetrahedra(srt_cache *c, const srt_cache_key 
                                               int is_static, const float *vertices,
                                               size_t nvertices, const uint32_t *tets,
                                               size_t ntets, srt_accel **out) {
-  return cache_get(c, SRT_TETRAHEDRA, key, is_static, out, [&](srt_accel *a) {
+  return cache_get_accel(c, SRT_TETRAHEDRA, key, is_static, out, [&](srt_accel *a) {
     return srt_accel_build_tetrahedra(a, vertices, nvertices, tets, ntets);
   });
 }
@@ -389,9 +418,35 @@ SRT_API srt_status srt_cache_build_spheres(srt_cache *c, const srt_cache_key *ke
                                            int is_static, const float *centers,
                                            const float *radius, float constant_radius,
                                            size_t n, srt_accel **out) {
-  return cache_get(c, SRT_SPHERES, key, is_static, out, [&](srt_accel *a) {
+  return cache_get_accel(c, SRT_SPHERES, key, is_static, out, [&](srt_accel *a) {
     return srt_accel_build_spheres(a, centers, radius, constant_radius, n);
   });
+}
+
+SRT_API srt_status srt_cache_build_lines(srt_cache *c, const srt_cache_key *key, int is_static,
+                                        const float *positions, size_t nverts,
+                                        const float *radius, float constant_radius,
+                                        const uint32_t *segments, size_t nlines, int32_t cap,
+                                        srt_line_accel **out) {
+  return cache_get<srt_line_accel>(
+      c, kLines, key, is_static, out,
+      [&](srt_line_accel **a) { return srt_line_create(c->ctx, a); },
+      [&](srt_line_accel *a) {
+        return srt_line_build(a, positions, nverts, radius, constant_radius, segments, nlines,
+                              0, 0, cap);
+      });
+}
+
+SRT_API srt_status srt_cache_build_solids(srt_cache *c, const srt_cache_key *key, int is_static,
+                                         int32_t verts_per_solid, const float *vertices,
+                                         size_t nverts, const uint32_t *indices, size_t nsolids,
+                                         srt_solid_accel **out) {
+  return cache_get<srt_solid_accel>(
+      c, kSolids, key, is_static, out,
+      [&](srt_solid_accel **a) { return srt_solid_create(c->ctx, a); },
+      [&](srt_solid_accel *a) {
+        return srt_solid_build(a, verts_per_solid, vertices, nverts, indices, nsolids);
+      });
 }
 
 SRT_API srt_status srt_cache_invalidate(srt_cache *c, uint64_t buffer) {

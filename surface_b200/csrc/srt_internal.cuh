@@ -284,6 +284,9 @@ srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uin
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
 // array in context scratch, valid until the context's next sort.
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);
+// Device bytes held by a line or solid accel (srt_line.cu, srt_solid.cu).
+uint64_t line_accel_bytes(const srt_line_accel *a);
+uint64_t solid_accel_bytes(const srt_solid_accel *a);
 // Exclusive prefix sum of n uint32 on the context's stream (out may alias in).
 srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n);
 // Stable sort of (key, value) pairs by key; key_bits: how many low bits of

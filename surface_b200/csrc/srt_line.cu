@@ -527,6 +527,10 @@ srt_status host_copy(const T *p, size_t count, std::vector<T> &buf, const T **ou
 
 }  // namespace
 
+namespace srt {
+uint64_t line_accel_bytes(const srt_line_accel *a) { return a->dnodes.cap + a->drecs.cap; }
+}  // namespace srt
+
 using namespace srt;
 
 extern "C" {

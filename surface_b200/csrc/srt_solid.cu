@@ -566,6 +566,10 @@ srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
 
 }  // namespace
 
+namespace srt {
+uint64_t solid_accel_bytes(const srt_solid_accel *a) { return a->dnodes.cap + a->drecs.cap; }
+}  // namespace srt
+
 using namespace srt;
 
 extern "C" {

@@ -184,3 +184,42 @@ def test_cache_static_dynamic_invalidate():
     torch.cuda.synchronize()
     assert np.array_equal(_hits(a4, rays), _hits(a3, rays))
     cache.close()
+
+
+def test_cache_lines_and_solids():
+    """AccelBuilder::BuildLineAccel / BuildSolidAccel: the same cache rules
+    for the line and solid accels (a static hit returns the same accel, a
+    different kind with the same key is another entry, EndFrame frees the
+    dynamic ones, Invalidate the buffer's), and cached accels trace like
+    direct builds."""
+    from surface_b200.lines import LineAccel, Lines
+    from surface_b200.solids import Solid, SolidAccel
+    pos, seg, rad = S.line_strands(2000, 8, seed=2)
+    v, ix = S.solid_grid(8, 11, seed=2)
+    cache = AccelBuilder()
+    l1 = cache.BuildLineAccel(Lines(pos, seg, rad), elembuf=1, arraybuf=2, count=seg.size)
+    l2 = cache.BuildLineAccel(Lines(pos, seg, rad), elembuf=1, arraybuf=2, count=seg.size)
+    s1 = cache.BuildSolidAccel(Solid(8, v, ix), elembuf=1, arraybuf=2, count=seg.size)
+    info = cache.info()
+    assert l1.h.value == l2.h.value and s1.h.value != l1.h.value
+    assert info.builds == 2 and info.hits == 1 and info.static_entries == 2
+    d = cache.BuildSolidAccel(Solid(8, v, ix), elembuf=5, arraybuf=6, count=ix.size,
+                              static=False)
+    assert cache.info().dynamic_entries == 1
+    rays = S.pinhole_rays(96, 96, (0.2, 0.4, 3.1), (0, 0, 0))
+    direct = LineAccel()
+    direct.Build(Lines(pos, seg, rad))
+    assert np.array_equal(bits(l1.Traverse(rays).view(np.float32).reshape(-1, 4)),
+                          bits(direct.Traverse(rays).view(np.float32).reshape(-1, 4)))
+    srays = S.solid_rays(48)
+    ds = SolidAccel()
+    ds.Build32(Solid(8, v, ix))
+    want = bits(ds.Traverse(srays).view(np.float32).reshape(-1, 4))
+    assert np.array_equal(bits(s1.Traverse(srays).view(np.float32).reshape(-1, 4)), want)
+    assert np.array_equal(bits(d.Traverse(srays).view(np.float32).reshape(-1, 4)), want)
+    used = cache.info().bytes_used
+    cache.EndFrame()
+    assert cache.info().dynamic_entries == 0 and cache.info().bytes_used < used
+    cache.Invalidate(2)
+    assert cache.info().static_entries == 0 and cache.info().bytes_used == 0
+    cache.close()
