@@ -474,11 +474,8 @@ __device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], co
   return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= FLT_MAX);
 }
 
-#ifndef SRT_SOLID_MIN_BLOCKS
-#define SRT_SOLID_MIN_BLOCKS 1
-#endif
 template <int NV>
-__global__ void __launch_bounds__(128, SRT_SOLID_MIN_BLOCKS)
+__global__ void __launch_bounds__(128)
 solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
                    const srt_ray *__restrict__ rays, size_t n, srt_hit *__restrict__ hits,
                    float *__restrict__ normals, float *__restrict__ positions) {
