@@ -25,6 +25,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <thread>
 #include <vector>
 
 #include "srt_internal.cuh"
@@ -151,6 +152,28 @@ struct Builder {
     }
   }
 
+  // The cut of [l, r) (idx partitioned in place): the split and its axis.
+  size_t cut(size_t l, size_t r, const float bmin[3], const float bmax[3], int &axis) {
+    float bsize[3];
+    for (int k = 0; k < 3; k++) bsize[k] = bmax[k] - bmin[k];
+    int longest = 0;
+    float m = bsize[0];
+    if (m < bsize[1]) {
+      m = bsize[1];
+      longest = 1;
+    }
+    if (m < bsize[2]) longest = 2;
+    size_t split = l;
+    for (int t = 0; t < 3; t++) {
+      axis = (longest + t) % 3;
+      const float pos = (float)((double)bmin[axis] + 0.5 * (double)bsize[axis]);
+      split = partition(l, r, axis, pos);
+      if (split != l && split != r) break;
+      split = l + ((r - l) >> 1);
+    }
+    return split;
+  }
+
   size_t build(size_t l, size_t r, int depth) {
     const size_t off = nodes.size();
     nodes.push_back(LineNodeH{});
@@ -167,24 +190,8 @@ struct Builder {
       nd.data[1] = (uint32_t)l;
       return off;
     }
-    float bsize[3];
-    for (int k = 0; k < 3; k++) bsize[k] = bmax[k] - bmin[k];
-    int longest = 0;
-    float m = bsize[0];
-    if (m < bsize[1]) {
-      m = bsize[1];
-      longest = 1;
-    }
-    if (m < bsize[2]) longest = 2;
-    size_t split = l;
     int axis = 0;
-    for (int t = 0; t < 3; t++) {
-      axis = (longest + t) % 3;
-      const float pos = (float)((double)bmin[axis] + 0.5 * (double)bsize[axis]);
-      split = partition(l, r, axis, pos);
-      if (split != l && split != r) break;
-      split = l + (n >> 1);
-    }
+    const size_t split = cut(l, r, bmin, bmax, axis);
     nodes[off].axis = axis;
     const size_t left = build(l, split, depth + 1);
     const size_t right = build(split, r, depth + 1);
@@ -196,6 +203,54 @@ struct Builder {
     return off;
   }
 };
+
+// The same tree with the top `par` levels' subtrees built on their own
+// threads (their idx ranges are disjoint) into local arrays, then laid out
+// in pre-order: the node, its left subtree, its right subtree, child indices
+// moved by the subtrees' offsets.
+void build_par(const std::vector<float> &box, const std::vector<float> &mid,
+               std::vector<uint32_t> &idx, int min_leaf, int max_depth, size_t l, size_t r,
+               int depth, int par, std::vector<LineNodeH> &out, int &depth_seen) {
+  Builder B{box, mid, idx, out, min_leaf, max_depth};
+  const size_t n = r - l;
+  if (par <= 0 || n < (size_t)min_leaf || depth >= max_depth || n < 4096) {
+    B.depth_seen = depth;
+    B.build(l, r, depth);
+    depth_seen = std::max(depth_seen, B.depth_seen);
+    return;
+  }
+  out.push_back(LineNodeH{});
+  depth_seen = std::max(depth_seen, depth);
+  float bmin[3], bmax[3];
+  B.range_box(l, r, bmin, bmax);
+  int axis = 0;
+  const size_t split = B.cut(l, r, bmin, bmax, axis);
+  std::vector<LineNodeH> L, R;
+  int dl = 0, dr = 0;
+  std::thread t([&] {
+    build_par(box, mid, idx, min_leaf, max_depth, l, split, depth + 1, par - 1, L, dl);
+  });
+  build_par(box, mid, idx, min_leaf, max_depth, split, r, depth + 1, par - 1, R, dr);
+  t.join();
+  depth_seen = std::max(depth_seen, std::max(dl, dr));
+  LineNodeH &root = out[0];
+  std::memcpy(root.bmin, bmin, sizeof(bmin));
+  std::memcpy(root.bmax, bmax, sizeof(bmax));
+  root.axis = axis;
+  root.data[0] = 1;
+  root.data[1] = (uint32_t)(1 + L.size());
+  out.reserve(1 + L.size() + R.size());
+  for (const auto *sub : {&L, &R}) {
+    const uint32_t shift = (uint32_t)out.size();
+    for (LineNodeH nd : *sub) {
+      if (!nd.flag) {
+        nd.data[0] += shift;
+        nd.data[1] += shift;
+      }
+      out.push_back(nd);
+    }
+  }
+}
 
 // ------------------------------------------------------------------ device
 __device__ __forceinline__ float dot3(const float a[3], const float b[3]) {
@@ -596,8 +651,11 @@ SRT_API srt_status srt_line_build(srt_line_accel *a, const float *positions, siz
   a->idx.resize(nlines);
   for (size_t i = 0; i < nlines; i++) a->idx[i] = (uint32_t)i;
   a->nodes.clear();
-  Builder B{box, mid, a->idx, a->nodes, min_leaf, max_depth};
-  B.build(0, nlines, 0);
+  int depth_seen = 0;
+  const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+  int par = 0;
+  while ((1u << (par + 1)) <= std::min(hw, 16u)) par++;
+  build_par(box, mid, a->idx, min_leaf, max_depth, 0, nlines, 0, par, a->nodes, depth_seen);
   if (a->nodes.size() >= (1u << 29)) {
     set_error("srt_line_build: more than 2^29 nodes");
     return SRT_ERR_INVALID;
@@ -643,7 +701,7 @@ SRT_API srt_status srt_line_build(srt_line_accel *a, const float *positions, siz
   if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
     return cuda_status(e, "line build");
   a->nlines = nlines;
-  a->depth = B.depth_seen;
+  a->depth = depth_seen;
   a->cap = cap != 0;
   a->built = true;
   return SRT_OK;
