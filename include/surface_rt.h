@@ -419,7 +419,9 @@ SRT_API size_t srt_scene_top_nodes(srt_scene *scene, double *boxes,
  * FLOAT / DOUBLE); texels x fastest, components interleaved (1..4 dense).
  * Data are copied to the device (the call synchronises the context stream).
  * srt_texture3d_fetch: uvw (3 floats per sample) and rgba (4 floats per
- * sample, 16-byte aligned) are device arrays; asynchronous. */
+ * sample; 16-byte aligned when on the device): device arrays are used in
+ * place and the call is asynchronous; host arrays are staged and the call
+ * returns with the result written. */
 typedef struct srt_texture3d srt_texture3d;
 typedef struct srt_volume_block {      /* VolumeBlock, render/render_prim_volume.h:18-26 */
   int32_t offset[3], extent[3], size[3], level;

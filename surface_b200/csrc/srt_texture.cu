@@ -755,9 +755,24 @@ SRT_API srt_status srt_texture3d_fetch(srt_texture3d *t, const float *uvw, size_
   if (n == 0) return SRT_OK;
   srt_ctx *ctx = t->ctx;
   cudaSetDevice(ctx->device);
-  if (!is_device_ptr(uvw) || !is_device_ptr(rgba) ||
-      (reinterpret_cast<uintptr_t>(rgba) & 15u)) {
-    set_error("srt_texture3d_fetch: device arrays, rgba 16-byte aligned");
+  // host arrays are staged through the context's scratch
+  const bool uhost = !is_device_ptr(uvw), ohost = !is_device_ptr(rgba);
+  cudaError_t se;
+  if (uhost) {
+    if ((se = ctx->s_stage_in.ensure(n * 12)) != cudaSuccess ||
+        (se = cudaMemcpyAsync(ctx->s_stage_in.p, uvw, n * 12, cudaMemcpyHostToDevice,
+                              ctx->stream)) != cudaSuccess)
+      return cuda_status(se, "texture coordinates");
+    uvw = ctx->s_stage_in.as<float>();
+  }
+  float *const user_rgba = rgba;
+  if (ohost) {
+    if ((se = ctx->s_stage_out.ensure(n * 16)) != cudaSuccess)
+      return cuda_status(se, "texture output");
+    rgba = ctx->s_stage_out.as<float>();
+  }
+  if (reinterpret_cast<uintptr_t>(rgba) & 15u) {
+    set_error("srt_texture3d_fetch: device rgba must be 16-byte aligned");
     return SRT_ERR_INVALID;
   }
   const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
@@ -801,7 +816,13 @@ SRT_API srt_status srt_texture3d_fetch(srt_texture3d *t, const float *uvw, size_
       dense_fetch_kernel<2><<<grid, 256, 0, ctx->stream>>>(dt, uvw, n, out);
   }
   ctx->launches++;
-  return cuda_status(cudaGetLastError(), "texture fetch");
+  if ((se = cudaGetLastError()) != cudaSuccess) return cuda_status(se, "texture fetch");
+  if (ohost &&
+      (se = cudaMemcpyAsync(user_rgba, rgba, n * 16, cudaMemcpyDeviceToHost, ctx->stream)) !=
+          cudaSuccess)
+    return cuda_status(se, "texture output");
+  if (uhost || ohost) return cuda_status(cudaStreamSynchronize(ctx->stream), "texture fetch");
+  return SRT_OK;
 }
 
 }  // extern "C"

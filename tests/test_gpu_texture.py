@@ -114,3 +114,19 @@ def test_sparse_locate_edge_cases(case):
         uvw = S.sparse_edge_coords(blocks, gdim, 30000, fmt, spread=(-1.5, 1.5))
         want = _check_sparse(blocks, pool, fmt, comps, gdim, uvw)
         assert (want[:, 3] != 0).mean() > 0.2
+
+
+def test_fetch_host_arrays_through_the_c_abi():
+    """srt_texture3d_fetch with host coordinate and output arrays (staged by
+    the library) gives the device path's result."""
+    blocks, pool, gdim = S.sparse_pages(ndiv=4, page=8, seed=5)
+    t = Texture3D()
+    t.set_sparse(blocks, pool, 0, 1, gdim)
+    uvw = S.sparse_edge_coords(blocks, gdim, 5000, 3)
+    dev = t.Fetch(torch.from_numpy(uvw).cuda()).cpu().numpy()
+    host = np.zeros((uvw.shape[0], 4), np.float32)
+    u = np.ascontiguousarray(uvw)
+    from surface_b200._lib import check
+    check(t.L.srt_texture3d_fetch(t.h, u.ctypes.data, u.shape[0], host.ctypes.data))
+    assert same(host, dev)
+    assert same(host, O.sparse_fetch(blocks, pool, 0, 1, gdim, uvw))
