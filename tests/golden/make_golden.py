@@ -151,13 +151,50 @@ def dump_fixtures():
     return out
 
 
+def lines_solids_fixtures():
+    """The reference's LineAccel and SolidAccel (Build32) on small scenes:
+    their Dump() files and, per ray, the hit (t, u, v, prim) and normal (and
+    for solids the position), plus a sparse volume's fetches with edge
+    coordinates through the reference's SparseVolumeAccel."""
+    out = {}
+    pos, seg, rad = S.line_strands(300, 8, seed=81)
+    lrays = S.pinhole_rays(48, 48, (0.2, 0.4, 3.1), (0, 0, 0), fov_deg=45)
+    name, cp, cs, cr, cc, copts, crays = next(c for c in S.line_cases() if c[0] == "axes-cap1")
+    out.update(line_pos=pos, line_seg=seg, line_rad=rad, line_rays=lrays,
+               edge_pos=cp, edge_seg=cs, edge_rad=cr, edge_rays=crays)
+    for tag, (p_, s_, r_, rays) in {"line": (pos, seg, rad, lrays),
+                                   "edge": (cp, cs, cr, crays)}.items():
+        acc = O.RefLines(p_, s_, r_)
+        h, n = acc.trace(rays)
+        out[f"{tag}_dump"] = np.frombuffer(acc.dump_bytes(), np.uint8).copy()
+        out[f"{tag}_hits"] = h.view(np.float32).reshape(-1, 4).copy()
+        out[f"{tag}_normals"] = n
+    for nv, g in ((8, 11), (6, 8), (5, 6)):
+        v, ix = S.solid_grid(nv, g, seed=83)
+        rays = S.solid_rays(24, seed=nv)
+        acc = O.RefSolids(nv, v, ix)
+        h, n, q = acc.trace(rays)
+        nodes, idx = acc.dump()
+        out.update({f"solid{nv}_verts": v, f"solid{nv}_ix": ix, f"solid{nv}_rays": rays,
+                    f"solid{nv}_nodes": nodes.view(np.uint8).copy(), f"solid{nv}_idx": idx,
+                    f"solid{nv}_hits": h.view(np.float32).reshape(-1, 4).copy(),
+                    f"solid{nv}_normals": n, f"solid{nv}_positions": q})
+    blocks, pool, gdim = S.sparse_pages(ndiv=4, page=8, seed=5)
+    uvw = S.sparse_edge_coords(blocks, gdim, 2000, 1)
+    out.update(sp_blocks=blocks.view(np.uint8).copy(), sp_pool=np.frombuffer(pool, np.uint8).copy(),
+               sp_gdim=np.array(gdim, np.int32), sp_uvw=uvw,
+               sp_rgba=O.sparse_fetch(blocks, pool, 0, 1, gdim, uvw, use_ref=True))
+    return out
+
+
 def main():
     L = O.ref()
     if L is None:
         raise SystemExit("reference harness missing: run `make -C oracle` with the reference tree")
     only = sys.argv[1:]  # names of fixtures to write (default: all)
     jobs = {"prefix_tree": lambda: prefix_tree(L), "scenes_small": scene_fixtures,
-            "texture3d": lambda: tex_fixture(L), "dumps_small": dump_fixtures}
+            "texture3d": lambda: tex_fixture(L), "dumps_small": dump_fixtures,
+            "lines_solids": lines_solids_fixtures}
     for name, make in jobs.items():
         if not only or name in only:
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **make())

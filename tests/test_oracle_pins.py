@@ -249,3 +249,32 @@ def test_reference_dump_fixtures_match_oracle(golden):
         o = acc()
         assert np.array_equal(idx, o.indices)
         assert np.array_equal(O.canonicalize(nodes, 0), o.canonical())
+
+
+def test_lines_solids_sparse_fixtures(golden):
+    """The oracle's LineAccel, SolidAccel (Build32) and sparse-volume fetch
+    against the reference's own outputs stored in lines_solids.npz (made by
+    tests/golden/make_golden.py): trees, hits, normals, positions, texels."""
+    g = golden("lines_solids.npz")
+    for tag in ("line", "edge"):
+        o = O.OracleLines(g[f"{tag}_pos"], g[f"{tag}_seg"], g[f"{tag}_rad"])
+        nodes, idx = O.parse_line_dump(g[f"{tag}_dump"].tobytes())
+        on, oi = o.export()
+        assert O.line_nodes_masked(on).tobytes() == O.line_nodes_masked(nodes).tobytes()
+        assert np.array_equal(oi, idx)
+        h, n = o.trace(g[f"{tag}_rays"])
+        assert np.array_equal(bits(h.view(np.float32).reshape(-1, 4)), bits(g[f"{tag}_hits"]))
+        assert np.array_equal(bits(n), bits(g[f"{tag}_normals"]))
+    for nv in (8, 6, 5):
+        o = O.OracleSolids(nv, g[f"solid{nv}_verts"], g[f"solid{nv}_ix"])
+        on, oi = o.export()
+        ref_nodes = g[f"solid{nv}_nodes"].view(O.SOLID_NODE_DTYPE)
+        assert O.tree_canonical(on) == O.tree_canonical(ref_nodes)
+        assert np.array_equal(oi, g[f"solid{nv}_idx"])
+        h, n, q = o.trace(g[f"solid{nv}_rays"])
+        assert np.array_equal(bits(h.view(np.float32).reshape(-1, 4)), bits(g[f"solid{nv}_hits"]))
+        assert np.array_equal(bits(n), bits(g[f"solid{nv}_normals"]))
+        assert np.array_equal(bits(q), bits(g[f"solid{nv}_positions"]))
+    blocks = g["sp_blocks"].view(O.BLOCK_DTYPE)
+    got = O.sparse_fetch(blocks, g["sp_pool"].tobytes(), 0, 1, tuple(g["sp_gdim"]), g["sp_uvw"])
+    assert np.array_equal(bits(got), bits(g["sp_rgba"]))
