@@ -1,7 +1,7 @@
 """Benchmark: LBVH build + closest-hit throughput on B200 (one JSON line).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload tet|tri|particles|volume|batched|frame|scene|texture]
+                    [--workload tet|tri|particles|volume|volume_nu|batched|frame|scene|texture|lines|solids]
 
 Default workload (``tet``): the tetrahedral-mesh configuration -- 64^3 cells in
 the unit cube, five tetrahedra per cell (1,310,720 tets), interior vertices
@@ -91,6 +91,15 @@ def make_workload(name):
                                         "step 0.5 voxel, emission-absorption forward + "
                                         "adjoint of an L2 loss",
                             "rays": 512 * 512})
+    if name == "volume_nu":
+        W = make_workload("volume")
+        W["nonuniform"] = True
+        W["config"] = {"workload": "volume256-nu: the volume256 march with the y axis "
+                                   "remapped through a 257-entry exponential coordinate "
+                                   "table and GL's repeat wrap (the reference's non-uniform "
+                                   "volume example), forward + adjoint",
+                       "rays": 512 * 512}
+        return W
     if name == "frame":
         v, f = S.displaced_octasphere(7)
         return dict(kind="frame", verts=v, prims=f, rays=np.zeros(512 * 512, np.uint8),
@@ -639,15 +648,20 @@ def run_volume(args, W):
     p = V.camera(512, 512, res=256)
     dens = torch.as_tensor(W["dens"], device=dev)
     tf = torch.as_tensor(W["tf"], device=dev)
-    target = V.march(torch.as_tensor(W["target_dens"], device=dev), tf, p)[0]
+    smp = None
+    if W.get("nonuniform"):
+        from surface_b200 import scenes as S
+        smp = V.Sampling(remap=(None, S.exp_coord_map(257), None), clamp=(False,) * 3,
+                         device=dev.index)
+    target = V.march(torch.as_tensor(W["target_dens"], device=dev), tf, p, sampling=smp)[0]
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     def fwd():
-        return V.march(dens, tf, p)
+        return V.march(dens, tf, p, sampling=smp)
 
     def fwd_bwd():
-        img, tr = V.march(dens, tf, p)
-        return V.march_backward(dens, tf, p, tr, 2 * (img - target))
+        img, tr = V.march(dens, tf, p, sampling=smp)
+        return V.march_backward(dens, tf, p, tr, 2 * (img - target), sampling=smp)
 
     from surface_b200 import _lib
     from surface_b200.accel import Context
@@ -729,7 +743,12 @@ def run_volume(args, W):
         q = np.zeros(1, O.VOL_DTYPE)
         q[...] = p.view(O.VOL_DTYPE)
         t0 = time.perf_counter()
-        O.volume_fwd_f32(q, W["dens"], (256, 256, 256), W["tf"])
+        if W.get("nonuniform"):
+            from surface_b200 import scenes as S
+            O.volume_fwd_f32(q, W["dens"], (256, 256, 256), W["tf"],
+                             remap=(None, S.exp_coord_map(257), None), clamp=(0, 0, 0))
+        else:
+            O.volume_fwd_f32(q, W["dens"], (256, 256, 256), W["tf"])
         tc = time.perf_counter() - t0
         cpu = {"value": round(nr / tc / 1e6, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
                "kind": "port", "sample": "FP32 forward march restatement over all 512^2 "
@@ -1980,18 +1999,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tet",
                     choices=["tet", "tri", "particles", "volume", "batched", "frame",
-                             "scene", "texture", "lines", "solids"])
+                             "scene", "texture", "lines", "solids", "volume_nu"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     args = ap.parse_args()
     if args.impl == "reference" and int(os.environ.get("RANK", "0")) != 0:
         return  # the CPU reference runs on rank 0 alone; other ranks exit 0
-    if args.impl == "reference" and args.workload == "volume":
+    if args.impl == "reference" and args.workload in ("volume", "volume_nu"):
         print(json.dumps({"impl": "reference", "unavailable":
                           "the reference's march is GLSL shader code that needs its closed "
                           "prebuilt compiler; no reference CPU march exists"}), flush=True)
         return
     W = make_workload(args.workload)
-    if args.workload == "volume":
+    if args.workload in ("volume", "volume_nu"):
         run_volume(args, W)
         return
     if args.impl == "reference":

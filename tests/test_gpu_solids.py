@@ -84,3 +84,27 @@ def test_dump_bbox_and_errors(tmp_path):
         SolidAccel().Build32(Solid(6, v, bad))
     with pytest.raises(sb.SurfaceError):
         SolidAccel().Build32(Solid(7, v, ix))  # 7 vertices per solid
+
+
+def test_against_reference_fixtures(golden):
+    """The CUDA line and solid accels against the reference's own outputs
+    (tests/golden/lines_solids.npz), bit for bit."""
+    from surface_b200.lines import LineAccel, Lines
+    g = golden("lines_solids.npz")
+    for tag in ("line", "edge"):
+        acc = LineAccel()
+        acc.Build(Lines(g[f"{tag}_pos"], g[f"{tag}_seg"], g[f"{tag}_rad"]))
+        h, n = acc.Traverse(g[f"{tag}_rays"], want_normal=True)
+        assert np.array_equal(bits(h.view(np.float32).reshape(-1, 4)), bits(g[f"{tag}_hits"]))
+        assert np.array_equal(bits(n), bits(g[f"{tag}_normals"]))
+    for nv in (8, 6, 5):
+        acc = SolidAccel()
+        acc.Build32(Solid(nv, g[f"solid{nv}_verts"], g[f"solid{nv}_ix"]))
+        nodes, idx = acc.export()
+        assert O.tree_canonical(nodes) == O.tree_canonical(
+            g[f"solid{nv}_nodes"].view(O.SOLID_NODE_DTYPE))
+        assert np.array_equal(idx, g[f"solid{nv}_idx"])
+        h, n, q = acc.Traverse(g[f"solid{nv}_rays"], want_point=True)
+        assert np.array_equal(bits(h.view(np.float32).reshape(-1, 4)), bits(g[f"solid{nv}_hits"]))
+        assert np.array_equal(bits(n), bits(g[f"solid{nv}_normals"]))
+        assert np.array_equal(bits(q), bits(g[f"solid{nv}_positions"]))
