@@ -14,7 +14,8 @@
 // depth level at a time from the deepest.  A gather kernel copies each
 // solid's vertices into a record in leaf order.
 //
-// Trace (SolidAccel::Traverse, :2345-2435): one thread per ray, every
+// Trace (SolidAccel::Traverse, :2345-2435): one thread per ray (in a Morton
+// order of the rays for large batches), every
 // popped node tests its own box; a leaf whose box is hit tests its solids
 // (skipping Ray::prev_prim_id) with the Pluecker tests of Intersect*D
 // (:455-717) in double, keeping the entry or exit point nearer than the
@@ -477,11 +478,13 @@ __device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], co
 template <int NV>
 __global__ void __launch_bounds__(128)
 solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
-                   const srt_ray *__restrict__ rays, size_t n, srt_hit *__restrict__ hits,
-                   float *__restrict__ normals, float *__restrict__ positions) {
+                   const srt_ray *__restrict__ rays, const uint32_t *__restrict__ order,
+                   size_t n, srt_hit *__restrict__ hits, float *__restrict__ normals,
+                   float *__restrict__ positions) {
   constexpr int RF = rec_floats(NV);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
+       k += (size_t)gridDim.x * blockDim.x) {
+    const size_t i = order ? (size_t)__ldg(&order[k]) : k;
     const float4 *rq = reinterpret_cast<const float4 *>(rays + i);
     const float4 r0 = __ldg(rq), r1 = __ldg(rq + 1);
     const float org[3] = {r0.x, r0.y, r0.z}, dir[3] = {r1.x, r1.y, r1.z};
@@ -794,12 +797,16 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
   const SNode *nd = a->dnodes.as<SNode>();
   const float *rc = a->drecs.as<float>();
   const srt_ray *rr = static_cast<const srt_ray *>(dr);
+  // a coherent ray order (a Morton curve over origin and direction) for
+  // large batches; the hits do not depend on it
+  const uint32_t *ord = nullptr;
+  if (n >= 32768 && (s = ray_order(ctx, rr, n, &ord)) != SRT_OK) return s;
   if (a->nv == 5)
-    solid_trace_kernel<5><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, n, dh, dn, dp);
+    solid_trace_kernel<5><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
   else if (a->nv == 6)
-    solid_trace_kernel<6><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, n, dh, dn, dp);
+    solid_trace_kernel<6><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
   else
-    solid_trace_kernel<8><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, n, dh, dn, dp);
+    solid_trace_kernel<8><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid trace");
   if (!hdev) cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, ctx->stream);
