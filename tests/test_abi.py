@@ -71,6 +71,18 @@ def test_null_arguments_are_rejected():
     assert L.srt_ctx_synchronize(None) == _lib.SRT_ERR_INVALID
     assert L.srt_accel_destroy(None) == _lib.SRT_OK
     assert L.srt_ctx_launch_count(None) == 0
+    # line, solid, texture and cache entry points
+    assert L.srt_line_create(None, None) == _lib.SRT_ERR_INVALID
+    assert L.srt_line_destroy(None) == _lib.SRT_OK
+    assert L.srt_line_trace(None, None, 0, None, None, None) == _lib.SRT_ERR_INVALID
+    assert L.srt_solid_create(None, None) == _lib.SRT_ERR_INVALID
+    assert L.srt_solid_destroy(None) == _lib.SRT_OK
+    assert L.srt_solid_trace(None, None, 0, None, None, None) == _lib.SRT_ERR_INVALID
+    assert L.srt_texture3d_fetch(None, None, 0, None) == _lib.SRT_ERR_INVALID
+    assert L.srt_cache_build_lines(None, None, 1, None, 0, None, 0.0, None, 0, 1,
+                                   None) == _lib.SRT_ERR_INVALID
+    assert L.srt_cache_build_solids(None, None, 1, 8, None, 0, None, 0, None) == \
+        _lib.SRT_ERR_INVALID
 
 
 def test_volume_camera_matches_oracle():

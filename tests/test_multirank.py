@@ -71,3 +71,18 @@ def test_single_rank_helpers_without_a_group():
     assert bench.dist_setup(torch.device("cpu")) == (1, 0) or os.environ.get("WORLD_SIZE")
     assert bench.max_over_ranks([3.0, 4.0], torch.device("cpu")) == [3.0, 4.0]
     assert bench.whole_job_mrays(262144, 1, 1.0) == pytest.approx(262.144)
+
+
+@pytest.mark.parametrize("workload", ["texture", "lines", "solids"])
+def test_reference_arm_of_the_newer_workloads(workload):
+    """bench.py --impl reference for the texture, line and solid workloads:
+    one JSON line with the contract's keys from the reference's own CPU code."""
+    out = subprocess.run([sys.executable, os.path.join(ROOT, "bench.py"), "--impl", "reference",
+                          "--workload", workload, "--steps", "1", "--warmup", "0"],
+                         capture_output=True, text=True, timeout=600, cwd=ROOT)
+    assert out.returncode == 0, out.stderr[-2000:]
+    import json
+    line = json.loads(out.stdout.strip().splitlines()[-1])
+    assert line["impl"] == "reference" and line["value"] > 0
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["e2e"]["h2d_bytes_per_step"] == 0
