@@ -3,15 +3,16 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload tet|tri|particles|volume|volume_nu|batched|frame|scene|texture|lines|solids]
 
-Default workload (``tet``): the tetrahedral-mesh configuration -- 64^3 cells in
-the unit cube, five tetrahedra per cell (1,310,720 tets), interior vertices
-jittered by +-0.2 cell, per-vertex scalar; 1024x1024 orthographic rays.  One
-step = LBVH build from the resident mesh + closest hit (FP64 Pluecker test)
-with barycentric scalar interpolation for every ray.  ``value`` = rays per
-second of the whole step (build included), in Mrays/s.  ``tri`` is the
-131,072-triangle / 512^2 pinhole configuration; ``particles`` one frame of the
-16,777,216-sphere configuration (rebuild + 2048^2 primaries); ``texture``
-16,777,216 texture3D fetches of a 512^3 sparse byte volume, in Mfetches/s.
+Default workload (``tri``): the plain triangle configuration -- an octasphere
+of 131,072 FP32 triangles displaced radially by seeded value noise, 512x512
+pinhole rays from distance 3 (45 deg).  One step = LBVH build from the
+resident mesh + closest hit (prim, t, u, v) for every ray.  ``value`` = rays
+per second of the whole step (build included), in Mrays/s.  ``tet`` is the
+tetrahedral-mesh configuration (64^3 cells x 5 = 1,310,720 tets, FP64
+Pluecker test, 1024^2 orthographic rays, barycentric scalar); ``particles``
+one frame of the 16,777,216-sphere configuration (rebuild + 2048^2
+primaries); ``texture`` 16,777,216 texture3D fetches of a 512^3 sparse byte
+volume, in Mfetches/s.
 
 Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
 on the launching stream; the L2 is flushed (256 MiB write) between steps,
@@ -21,7 +22,8 @@ outside the events.  Multi-GPU (torchrun): every rank runs the same workload
 rays copied in, hits and scalars copied out every step).
 
 ``--impl reference`` times the reference's own CPU code (Build32 + OpenMP
-Traverse, compiled from its sources into oracle/_ref) on the host cores.
+Traverse, compiled from its sources into oracle/_ref) on the host cores, for
+every ray of the step (nothing sampled or scaled).
 """
 from __future__ import annotations
 
@@ -315,9 +317,10 @@ def dist_teardown():
 
 
 # ---------------------------------------------------------------- CPU side
-def cpu_reference_step(W, nthreads=0, stride=4):
-    """Reference Build32 + OpenMP Traverse on a strided ray sample.
-    Returns (Mrays/s scaled to the full ray set, build s, trace s, sample rays)."""
+def cpu_reference_step(W, nthreads=0, stride=1):
+    """Reference Build32 + OpenMP Traverse of every ray (every stride-th ray
+    when stride > 1, the trace time then scaled to all rays).
+    Returns (Mrays/s, build s, trace s, rays traced, kind)."""
     from oracle import oracle as O
     kind = {"tet": O.TET, "tri": O.TRI, "sphere": O.SPHERE}[W["kind"]]
     use_ref = O.have_ref() and O.ref() is not None
@@ -339,10 +342,10 @@ def cpu_reference_step(W, nthreads=0, stride=4):
     return value, tb, tt, sample.size, ("reference" if use_ref else "port")
 
 
-def cpu_reference_batched(W, nthreads=0, stride=16):
+def cpu_reference_batched(W, nthreads=0, stride=1):
     """Reference loop over the scenes: Build32 of every scene + OpenMP
-    Traverse of every 16th ray of each.  Returns (Mrays/s scaled to all rays,
-    build s, trace s, sample rays, kind)."""
+    Traverse of every ray of each (every stride-th ray when stride > 1,
+    scaled).  Returns (Mrays/s, build s, trace s, rays traced, kind)."""
     from oracle import oracle as O
     B = W["B"]
     use_ref = O.have_ref() and O.ref() is not None
@@ -368,12 +371,12 @@ def cpu_reference_batched(W, nthreads=0, stride=16):
     return value, tb, tt, ns, ("reference" if use_ref else "port")
 
 
-def cpu_reference_particles(W, nthreads=0, stride=4):
-    """Reference Build32 of the frame-0 cloud + OpenMP Traverse of every 4th
-    primary and every 4th secondary (the secondaries spawned from the
-    reference's own primary hits by the workload's bounce rule, outside the
-    timed calls).  Returns (Mrays/s scaled to all rays, build s, trace s,
-    sample rays, kind)."""
+def cpu_reference_particles(W, nthreads=0, stride=1):
+    """Reference Build32 of the frame-0 cloud + OpenMP Traverse of every
+    primary and every secondary (every stride-th when stride > 1, scaled);
+    the secondaries are spawned from the reference's own primary hits by the
+    workload's bounce rule, outside the timed calls.  Returns (Mrays/s, build
+    s, trace s, rays traced, kind)."""
     from oracle import oracle as O
     from surface_b200 import scenes as S
     use_ref = O.have_ref() and O.ref() is not None
@@ -439,9 +442,9 @@ def _oracle_scene(W):
     return W["_cpu_accs"]
 
 
-def cpu_reference_scene(W, nthreads=0, stride=4):
+def cpu_reference_scene(W, nthreads=0, stride=1):
     """The CPU restatement of one scene frame (RenderGraph::Build, the eye
-    rays, RenderGraph::Trace with OpenMP over every stride-th pixel, the
+    rays, RenderGraph::Trace with OpenMP over every pixel, the
     framebuffer write); element accels built once outside the timing.
     Returns (Mrays/s, build+rays+write s, trace s scaled, rays traced, kind)."""
     from oracle import oracle as O
@@ -489,7 +492,7 @@ def cpu_reference_texture(W, nthreads=0):
             "reference" if use_ref else "port")
 
 
-def cpu_reference_solids(W, nthreads=0, stride=16):
+def cpu_reference_solids(W, nthreads=0, stride=1):
     """SolidAccel::Build32 of the mesh and Traverse of every stride-th ray on
     the host: the reference's own code (oracle/_ref) or else the
     restatement, OpenMP over all cores.  Returns (Mrays/s, build s, trace s
@@ -507,7 +510,7 @@ def cpu_reference_solids(W, nthreads=0, stride=16):
             "reference" if use_ref else "port")
 
 
-def cpu_reference_lines(W, nthreads=0, stride=4):
+def cpu_reference_lines(W, nthreads=0, stride=1):
     """LineAccel::Traverse of every stride-th ray on the host: the
     reference's own code (oracle/_ref) or else the restatement, OpenMP over
     all cores; the accel is built once outside the timing.  Returns
@@ -540,37 +543,43 @@ def run_reference_arm(args, W):
     for _ in range(args.warmup):
         step(W)
     vals, tbs, tts = [], [], []
+    flush = np.zeros(256 * 1024 * 1024 // 8, np.float64)
     for _ in range(args.steps):
+        flush[:] = 1.0  # 256 MiB written between steps: host caches hold no step state
         v, tb, tt, ns, kind = step(W)
         vals.append(v)
         tbs.append(tb)
         tts.append(tt)
     value = statistics.median(vals)
-    nr = W["rays"].size
-    if W["kind"] == "sphere":
-        nr = int(ns * 4)  # primaries + secondaries of one frame
-    ms = 1e3 * nr / (value * 1e6)
+    # every ray is traced (no scaling): the median step's measured time
+    ms = 1e3 * ns / (value * 1e6)
     unit = "Mfetches/s" if W["kind"] == "texture" else "Mrays/s"
-    stride = 16 if W["kind"] == "batched" else 4
-    sample = (f"full Build32 + every {stride}th ray ({ns} of {nr}) per step, trace time "
-              f"scaled to all rays; median of {args.steps}")
+    sample = (f"the full step: Build32 + Traverse of every ray ({ns}) through the "
+              f"reference's own code (OpenMP, {cores} threads); median of {args.steps}")
+    if W["kind"] == "batched":
+        sample = (f"the full step: Build32 + Traverse of every ray of all 64 scenes ({ns}) "
+                  f"through the reference's own code (OpenMP, {cores} threads); median of "
+                  f"{args.steps}")
+    if W["kind"] == "sphere":
+        sample = (f"the full frame: Build32 + Traverse of every primary and every "
+                  f"secondary ({ns} rays) through the reference's own code (OpenMP, "
+                  f"{cores} threads); median of {args.steps}")
     if W["kind"] == "frame":
         sample = (f"every pixel ({ns} rays): eye rays and framebuffer write of the CPU "
                   f"restatement, Traverse of the reference (accel built once); median of "
                   f"{args.steps}")
     if W["kind"] == "scene":
-        sample = (f"top-level build, eye rays and write of every pixel, scene trace of every "
-                  f"4th pixel ({ns} of {nr}) scaled to all, by the CPU restatement "
-                  f"(OpenMP; the reference's RenderGraph needs its GL front end); median "
-                  f"of {args.steps}")
+        sample = (f"top-level build, eye rays, scene trace and write of every pixel ({ns}) "
+                  f"by the CPU restatement (OpenMP; the reference's RenderGraph needs its "
+                  f"GL front end); median of {args.steps}")
     if W["kind"] == "solids":
-        sample = (f"full Build32 + every 16th ray ({ns} of {nr}) per step through the "
-                  f"reference's own SolidAccel (OpenMP, {cores} threads), trace time scaled "
-                  f"to all rays; median of {args.steps}")
+        sample = (f"full Build32 + Traverse of every ray ({ns}) per step through the "
+                  f"reference's own SolidAccel (OpenMP, {cores} threads); median of "
+                  f"{args.steps}")
     if W["kind"] == "lines":
-        sample = (f"every 4th ray ({ns} of {nr}) per step through the reference's own "
-                  f"LineAccel::Traverse (OpenMP, {cores} threads; accel built once), "
-                  f"scaled to all rays; median of {args.steps}")
+        sample = (f"every ray ({ns}) per step through the reference's own "
+                  f"LineAccel::Traverse (OpenMP, {cores} threads; accel built once); "
+                  f"median of {args.steps}")
     if W["kind"] == "texture":
         sample = (f"every fetch ({ns}) per step through the reference's own "
                   f"SparseVolumeAccel (Build + Sample) over {cores} threads; median of "
@@ -585,7 +594,8 @@ def run_reference_arm(args, W):
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(ms, 3), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": DTYPE[W["kind"]], "data": "synthetic",
-        "config": W["config"],
+        "config": dict(W["config"], l2="flushed between steps (256 MiB write)",
+                       parallelism=f"replicas x{args.gpus}"),
         ("rays_write_ms" if W["kind"] in ("frame", "scene") else "build_ms"):
             round(1e3 * statistics.median(tbs), 3),
         "cpu_baseline": {"value": round(value, 4), "unit": unit, "cores": cores,
@@ -987,8 +997,8 @@ def run_lines(args, W):
             raise SystemExit("line hits differ from the oracle")
         v, _, tt, ns, kind = cpu_reference_lines(W)
         cpu = {"value": round(v, 3), "unit": "Mrays/s", "cores": os.cpu_count(),
-               "kind": kind, "sample": f"every 4th ray ({ns}), OpenMP over "
-                                       f"{os.cpu_count()} threads, scaled to all rays",
+               "kind": kind, "sample": f"every ray ({ns}), OpenMP over "
+                                       f"{os.cpu_count()} threads",
                "seconds": round(tt, 3)}
     line = {"metric": METRIC_LINES, "value": round(value, 3), "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1113,8 +1123,8 @@ def run_solids(args, W):
             raise SystemExit("solid hits differ from the oracle")
         cv, tb, tt, ns, kind = cpu_reference_solids(W)
         cpu = {"value": round(cv, 3), "unit": "Mrays/s", "cores": os.cpu_count(),
-               "kind": kind, "sample": f"full Build32 + every 16th ray ({ns}), OpenMP over "
-                                       f"{os.cpu_count()} threads, trace scaled to all rays",
+               "kind": kind, "sample": f"full Build32 + every ray ({ns}), OpenMP over "
+                                       f"{os.cpu_count()} threads",
                "build_s": round(tb, 3), "trace_s": round(tt, 3)}
     line = {"metric": METRIC_SOLIDS, "value": round(value, 3), "unit": "Mrays/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -1287,8 +1297,8 @@ def run_batched(args, W):
         cv, ctb, ctt, cns, ck = cpu_reference_batched(W)
         cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
                "kind": ck, "build_s": round(ctb, 3), "trace_s": round(ctt, 3),
-               "sample": f"Build32 of all 64 scenes + every 16th ray of each ({cns} of "
-                         f"{nr}), trace time scaled to all rays"}
+               "sample": f"Build32 of all 64 scenes + every ray of each ({cns} of "
+                         f"{nr})"}
     for a in accs:
         L.srt_accel_destroy(a)
     if rank == 0:
@@ -1468,8 +1478,8 @@ def run_particles(args, W):
         cv, ctb, ctt, cns, ck = cpu_reference_particles(W)
         cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
                "kind": ck, "build_s": round(ctb, 3), "trace_s": round(ctt, 3),
-               "sample": f"Build32 of frame 0 + every 4th primary and the secondaries of "
-                         f"those hits ({cns} rays), trace time scaled to the frame"}
+               "sample": f"Build32 of frame 0 + every primary and the secondaries of "
+                         f"its hits ({cns} rays)"}
     L.srt_accel_destroy(acc)
     if rank == 0:
         line = {
@@ -1780,9 +1790,8 @@ def run_scene(args, W):
         cv, ctr, ctt, cns, ck = sorted(vals)[1]
         cpu = {"value": round(cv, 4), "unit": "Mrays/s", "cores": os.cpu_count(), "kind": ck,
                "build_rays_write_s": round(ctr, 4), "trace_s": round(ctt, 4),
-               "sample": f"top-level build, eye rays and write of every pixel; scene trace "
-                         f"of every 4th pixel ({cns} rays, OpenMP) scaled to all; median "
-                         f"of 3, CPU restatement"}
+               "sample": f"top-level build, eye rays, scene trace and write of every "
+                         f"pixel ({cns} rays, OpenMP); median of 3, CPU restatement"}
     L.srt_scene_destroy(sc)
     for h in accs:
         L.srt_accel_destroy(h)
@@ -1965,8 +1974,8 @@ def run_ours(args, W):
         v, tb, tt, ns, ck = cpu_reference_step(W)
         cpu = {"value": round(v, 4), "unit": "Mrays/s", "cores": os.cpu_count(),
                "kind": ck, "build_s": round(tb, 4), "trace_s": round(tt, 4),
-               "sample": f"full Build32 + every 4th ray ({ns} of {nr}), trace time "
-                         f"scaled to all rays"}
+               "sample": f"the full step: Build32 + every ray ({ns} of {nr}), OpenMP "
+                         f"over {os.cpu_count()} threads"}
 
     if rank == 0:
         line = {
@@ -1997,7 +2006,7 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="tet",
+    ap.add_argument("--workload", default="tri",
                     choices=["tet", "tri", "particles", "volume", "batched", "frame",
                              "scene", "texture", "lines", "solids", "volume_nu"])
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
