@@ -85,6 +85,34 @@ typedef struct srt_hit {
   uint32_t prim;
 } srt_hit;
 
+/* Shading record of a hit (80 bytes): the Intersection fields that the
+ * reference's Traverse fills through BuildIntersection besides t/u/v/prim_id
+ * and subface_id (render/render_intersection.h:18-62), i.e. what the GLSL
+ * fragment stage interpolates varyings from (gles/gles_common.cc:1007-1141).
+ *   triangles (render/render_accel_triangle.cc:2439-2507): position =
+ *     org + t * dir, normal = normalised (p1 - p0) x (p2 - p0), f0..f2 = the
+ *     face's vertex ids; tangent, binormal, f3 and d are 0.
+ *   tetrahedra (render/render_accel_tetra.cc:2124-2196): position, normal of
+ *     the entering face (face_table of subface_id), f0..f3 = the tet's vertex
+ *     ids, d[0..3] = InterpolateTetra's weights (:148-241).
+ *   spheres (render/render_accel_particle.cc:2966-3049): position, normal =
+ *     vnormalize(position - centre), tangent and binormal of the spherical
+ *     parameterisation, f0 = f1 = f2 = prim id; the spherical (u, v) go to
+ *     srt_hit.u / .v (as in every sphere trace).
+ * Intersection::geometric equals normal for all three.  A miss writes an
+ * all-zero record (the reference leaves the fields unset). */
+typedef struct srt_isect {
+  float position[3];
+  uint32_t f0;
+  float normal[3];
+  uint32_t f1;
+  float tangent[3];
+  uint32_t f2;
+  float binormal[3];
+  uint32_t f3;
+  float d[4];
+} srt_isect;
+
 /* Optional per-call inputs/outputs of srt_trace_closest.  Any field may be
  * NULL / 0. */
 typedef struct srt_trace_opts {
@@ -107,7 +135,16 @@ typedef struct srt_trace_opts {
   unsigned long long *stats;
   /* SRT_TRACE_* bits */
   uint32_t flags;
-  uint32_t reserved;
+  /* cap on the steps (nodes popped) of one ray's walk; 0 = the default,
+   * 8 * primitives + 64, which a walk over a valid tree never reaches.  A
+   * ray that reaches the cap stops with whatever it found so far and the
+   * call (or srt_ctx_synchronize) reports SRT_ERR_LIMIT, like the
+   * reference's stack-depth assert (render/render_accel_triangle.cc:2661);
+   * the context stays usable. */
+  uint32_t max_iter;
+  /* per-ray shading record (srt_isect), written after the closest hit is
+   * known: the reference's BuildIntersection */
+  srt_isect *isect;
 } srt_trace_opts;
 
 /* srt_trace_opts.flags: walk the tree once in the reference's own order
@@ -234,7 +271,10 @@ SRT_API srt_status srt_trace_closest(srt_accel *accel, const srt_ray *rays,
  *     overlap in time (different streams, unordered threads) race on it.
  *     Order them on one stream or synchronise between them.
  *   - Nothing needs to be zeroed by the caller: each call clears the array's
- *     deferred-ray count on the stream before its first kernel. */
+ *     deferred-ray count on the stream before its first kernel.
+ *   - The array's address is kept per device number for the life of the
+ *     process: a cudaDeviceReset, or a caller that runs the library in a
+ *     non-primary driver context, is not supported with this call. */
 SRT_API srt_status srt_trace_closest_noalloc(srt_accel *accel,
                                              const srt_ray *rays, size_t n,
                                              srt_hit *hits);
@@ -421,7 +461,9 @@ SRT_API size_t srt_scene_top_nodes(srt_scene *scene, double *boxes,
  * srt_texture3d_fetch: uvw (3 floats per sample) and rgba (4 floats per
  * sample; 16-byte aligned when on the device): device arrays are used in
  * place and the call is asynchronous; host arrays are staged and the call
- * returns with the result written. */
+ * returns with the result written.  A sparse fetch whose block-tree walk
+ * reaches its step cap returns SRT_ERR_LIMIT: from the call itself when it
+ * staged host arrays, else from the next srt_ctx_synchronize. */
 typedef struct srt_texture3d srt_texture3d;
 typedef struct srt_volume_block {      /* VolumeBlock, render/render_prim_volume.h:18-26 */
   int32_t offset[3], extent[3], size[3], level;
@@ -504,7 +546,9 @@ SRT_API srt_status srt_cache_invalidate(srt_cache *cache, uint64_t buffer);
 /* AccelBuilder::BuildLineAccel (gles/gles_accel_builder.cc:188-256) and
  * BuildSolidAccel (:328-397): the same cache for line and solid accels
  * (srt_line_build with LineBuildOptions' defaults and the given cap;
- * srt_solid_build). */
+ * srt_solid_build).  As in AccelBuilder::Locate, the line cap flag is not
+ * part of the key: a static line accel built with one cap value is returned
+ * for a later call with the other. */
 typedef struct srt_line_accel srt_line_accel;
 typedef struct srt_solid_accel srt_solid_accel;
 SRT_API srt_status srt_cache_build_lines(srt_cache *cache, const srt_cache_key *key,

@@ -32,6 +32,10 @@ MISS = 0xFFFFFFFF
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
                       ("prev_t", "<f4")])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4")])
+# shading record of a hit (BuildIntersection's fields; srt_isect in the C ABI)
+ISECT_DTYPE = np.dtype([("position", "<f4", 3), ("f0", "<u4"), ("normal", "<f4", 3),
+                        ("f1", "<u4"), ("tangent", "<f4", 3), ("f2", "<u4"),
+                        ("binormal", "<f4", 3), ("f3", "<u4"), ("d", "<f4", 4)])
 # generic node (own box, leaf flag, axis, d0, d1): so_node in surface_oracle.c
 NODE_DTYPE = np.dtype([("bmin", "<f4", 3), ("bmax", "<f4", 3), ("leaf", "<i4"),
                        ("axis", "<i4"), ("d0", "<u4"), ("d1", "<u4")])
@@ -74,6 +78,7 @@ def lib():
         L.so_canonicalize.argtypes = [_P, _SZ, _SZ, _P, _SZ]
         L.so_trace.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, _P, _P, C.c_int]
         L.so_trace2.argtypes = [_P, _P, _SZ, _P, _P, _P, _P, C.c_int]
+        L.so_isect_records.argtypes = [_P, _P, _SZ, _P, _P, _P, C.c_int]
         L.so_morton_bits.restype = C.c_uint32
         L.so_morton_bits.argtypes = [C.c_uint32] * 3
         for n in ("so_morton_tris", "so_morton_tets"):
@@ -163,6 +168,9 @@ def ref():
         L.ref_tri_trace.argtypes = [_P, _P, _SZ, _P, C.c_int, C.c_int]
         L.ref_tet_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
         L.ref_sphere_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
+        L.ref_tri_trace_isect.argtypes = [_P, _P, _SZ, _P, _P, C.c_int]
+        L.ref_tet_trace_isect.argtypes = [_P, _P, _SZ, _P, _P, _P, C.c_int]
+        L.ref_sphere_trace_isect.argtypes = [_P, _P, _SZ, _P, _P, _P, C.c_int]
         L.ref_node_sizes.argtypes = [_P]
         L.ref_morton_points.argtypes = [_P, _SZ, _P, _P, _P, C.c_int]
         L.ref_morton_tris.argtypes = [_P, _P, _SZ, _P, _P, _P]
@@ -291,6 +299,16 @@ class OracleAccel:
         if want_stats:
             out.append(st)
         return out[0] if len(out) == 1 else tuple(out)
+
+    def isect(self, rays, hits, subface=None, nthreads=0):
+        """BuildIntersection's shading records (ISECT_DTYPE) of traced rays."""
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.ascontiguousarray(hits, HIT_DTYPE)
+        sub = None if subface is None else np.ascontiguousarray(subface, np.uint32)
+        rec = np.zeros(rays.size, ISECT_DTYPE)
+        lib().so_isect_records(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(sub),
+                               _ptr(rec), nthreads)
+        return rec
 
     def __del__(self):
         try:
@@ -499,6 +517,27 @@ class RefAccel:
         self.L.ref_sphere_trace(self.h, _ptr(rays), rays.size, _ptr(pn), _ptr(hits),
                                 nthreads, chunk)
         return hits
+
+    def trace_isect(self, rays, prev_normals=None, nthreads=0):
+        """Every Intersection field the reference's Traverse fills: (hits,
+        subface (tetrahedra, else None), ISECT_DTYPE records)."""
+        rays = np.ascontiguousarray(rays, RAY_DTYPE)
+        hits = np.zeros(rays.size, HIT_DTYPE)
+        rec = np.zeros(rays.size, ISECT_DTYPE)
+        sub = None
+        if self.kind == TRI:
+            self.L.ref_tri_trace_isect(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(rec),
+                                       nthreads)
+        elif self.kind == TET:
+            sub = np.zeros(rays.size, np.uint32)
+            self.L.ref_tet_trace_isect(self.h, _ptr(rays), rays.size, _ptr(hits), _ptr(sub),
+                                       _ptr(rec), nthreads)
+        else:
+            pn = None if prev_normals is None else np.ascontiguousarray(prev_normals,
+                                                                        np.float32)
+            self.L.ref_sphere_trace_isect(self.h, _ptr(rays), rays.size, _ptr(pn), _ptr(hits),
+                                          _ptr(rec), nthreads)
+        return hits, sub, rec
 
     def __del__(self):
         try:

@@ -253,10 +253,87 @@ REF_API void ref_sphere_trace(void *p, const RayRec *rays, size_t n,
     Intersection isect;
     bool hit = acc.Traverse(isect, ray);
     hits[i].t = isect.t;
-    hits[i].u = 0.0f;  // spherical uv is shading-only
-    hits[i].v = 0.0f;
+    hits[i].u = hit ? isect.u : 0.0f;  // BuildIntersection's spherical (u, v)
+    hits[i].v = hit ? isect.v : 0.0f;
     hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
   }
+}
+
+// ---------------------------------------------------------------- shading
+// Every Intersection field the reference's Traverse fills (through
+// BuildIntersection) for each ray: t/u/v/prim in hits, subface_id, and the
+// 80-byte record {position, f0, normal, f1, tangent, f2, binormal, f3,
+// d0..d3} (the product's srt_isect; zero on a miss).  Geometric and shading
+// normals are equal in all three accels; normal here is Intersection::normal.
+struct IsectRec {
+  float position[3];
+  uint32_t f0;
+  float normal[3];
+  uint32_t f1;
+  float tangent[3];
+  uint32_t f2;
+  float binormal[3];
+  uint32_t f3;
+  float d[4];
+};
+
+namespace {
+template <typename Accel>
+void trace_isect(const Accel &acc, int kind, const RayRec *rays, size_t n,
+                 const float *prev_normals, HitRec *hits, uint32_t *subface,
+                 IsectRec *rec, int nthreads) {
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic, 64) num_threads(nthreads)
+  for (long long i = 0; i < (long long)n; i++) {
+    Ray ray = make_ray(rays[i], prev_normals ? &prev_normals[3 * i] : nullptr);
+    Intersection isect;
+    memset(&isect, 0, sizeof(isect));
+    bool hit = acc.Traverse(isect, ray);
+    hits[i].t = hit ? isect.t : std::numeric_limits<float>::max();
+    hits[i].u = hit ? isect.u : 0.0f;
+    hits[i].v = hit ? isect.v : 0.0f;
+    hits[i].prim = hit ? isect.prim_id : 0xffffffffu;
+    if (subface) subface[i] = hit ? isect.subface_id : 0u;
+    IsectRec &r = rec[i];
+    memset(&r, 0, sizeof(r));
+    if (!hit) continue;
+    for (int k = 0; k < 3; k++) {
+      r.position[k] = isect.position[k];
+      r.normal[k] = isect.normal[k];
+      if (kind == 2) {
+        r.tangent[k] = isect.tangent[k];
+        r.binormal[k] = isect.binormal[k];
+      }
+    }
+    r.f0 = isect.f0;
+    r.f1 = isect.f1;
+    r.f2 = isect.f2;
+    if (kind == 1) {
+      r.f3 = isect.f3;
+      r.d[0] = isect.d0;
+      r.d[1] = isect.d1;
+      r.d[2] = isect.d2;
+      r.d[3] = isect.d3;
+    }
+  }
+}
+}  // namespace
+
+REF_API void ref_tri_trace_isect(void *p, const RayRec *rays, size_t n, HitRec *hits,
+                                 IsectRec *rec, int nthreads) {
+  trace_isect(static_cast<TriHandle *>(p)->accel, 0, rays, n, nullptr, hits, nullptr, rec,
+              nthreads);
+}
+REF_API void ref_tet_trace_isect(void *p, const RayRec *rays, size_t n, HitRec *hits,
+                                 uint32_t *subface, IsectRec *rec, int nthreads) {
+  trace_isect(static_cast<TetHandle *>(p)->accel, 1, rays, n, nullptr, hits, subface, rec,
+              nthreads);
+}
+REF_API void ref_sphere_trace_isect(void *p, const RayRec *rays, size_t n,
+                                    const float *prev_normals, HitRec *hits, IsectRec *rec,
+                                    int nthreads) {
+  trace_isect(static_cast<SphereHandle *>(p)->accel, 2, rays, n, prev_normals, hits, nullptr,
+              rec, nthreads);
 }
 
 // Node record sizes of the reference's Dump() format.

@@ -21,6 +21,9 @@
  *   - closest-hit traversal    render/render_accel_triangle.cc:1815-1938,1994-2437,2511-2669
  *                              render/render_accel_tetra.cc:89-567,1934-2122,2200-2289
  *                              render/render_accel_particle.cc:1990-2035,2423-2834,3053-3218
+ *   - shading records          render/render_accel_triangle.cc:2439-2507,
+ *     (BuildIntersection)      render/render_accel_tetra.cc:148-241,2124-2196,
+ *                              render/render_accel_particle.cc:2966-3049
  *   - trilinear 3D fetch       render/render_texture.cc:97-121,946-1058
  *   - volume march             examples/nonuniform_volume_render/input.frag:16-141
  *                              (camera, slab test, texel mapping); the
@@ -1332,6 +1335,209 @@ static void trace2_one(const so_accel *a, const so_ray *ray, const float *prevN,
   }
 }
 
+/* ---- BuildIntersection: the shading record of a hit ----------------------
+ * The fields the reference's Traverse fills after the closest hit is known
+ * and the GLSL stage reads (gles/gles_common.cc:1007-1141).  Record layout
+ * (80 bytes, the product's srt_isect): position, f0, normal, f1, tangent, f2,
+ * binormal, f3, d[4]; a miss is all zero.  Float arithmetic in the
+ * reference's order; the spheres' angles from the C library's double atan2
+ * and acos, which is what the reference's unqualified atan2 / acos calls on
+ * floats resolve to in its build (checked against its outputs). */
+typedef struct {
+  float position[3];
+  uint32_t f0;
+  float normal[3];
+  uint32_t f1;
+  float tangent[3];
+  uint32_t f2;
+  float binormal[3];
+  uint32_t f3;
+  float d[4];
+} so_isect;
+
+static inline void sub3f(const float a[3], const float b[3], float c[3]) {
+  c[0] = a[0] - b[0];
+  c[1] = a[1] - b[1];
+  c[2] = a[2] - b[2];
+}
+/* real3::length (render/render_common.h) */
+static inline float len3f(const float a[3]) {
+  return (float)sqrt((double)(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]));
+}
+/* real3::normalize (render/render_common.h): scale by 1/sqrt in double */
+static inline void normalize_real3(float n[3]) {
+  double l2 = n[0] * n[0] + n[1] * n[1] + n[2] * n[2];
+  double len = 0.0;
+  if (fabs(l2) > 1.0e-30) len = 1.0 / sqrt(l2);
+  for (int k = 0; k < 3; k++) n[k] = (float)(n[k] * len);
+}
+/* vnormalize (render/render_accel_particle.cc:2041-2056) */
+static inline void vnormalize_p(float n[3]) {
+  const float kEPS = FLT_EPSILON * 16.0;
+  float len = (float)sqrt((double)dot3f(n, n));
+  if (len > kEPS) {
+    float inv = (float)(1.0 / len);
+    n[0] *= inv;
+    n[1] *= inv;
+    n[2] *= inv;
+  }
+}
+/* Spherical (u, v) of a unit normal (render/render_accel_particle.cc:3013-3014) */
+static inline void sphere_uv_ref(const float n[3], float *u, float *v) {
+  *u = (float)((atan2((double)n[0], (double)n[2]) + M_PI) * 0.5 * (1.0 / M_PI));
+  *v = (float)(acos((double)n[1]) / M_PI);
+}
+
+/* InterpolateTetra (render/render_accel_tetra.cc:148-241), mode 0. */
+static void interpolate_tetra(const float pt[3], const float V[4][3], float dout[4]) {
+  static const int fl[4][3] = {{0, 2, 1}, {1, 2, 3}, {0, 3, 2}, {0, 1, 3}};
+  const float kEPS = 0.001;
+  float E[6][3];
+  sub3f(V[1], V[0], E[0]);
+  sub3f(V[2], V[1], E[1]);
+  sub3f(V[0], V[2], E[2]);
+  sub3f(V[3], V[0], E[3]);
+  sub3f(V[3], V[1], E[4]);
+  sub3f(V[3], V[2], E[5]);
+  for (int v = 0; v < 4; v++) {
+    const float *ro = V[v];
+    float rd[3], pc[3], tmp[3];
+    sub3f(pt, ro, rd);
+    cross3f(rd, ro, pc);
+    sub3f(pt, ro, tmp);
+    float d = len3f(tmp);
+    float ws[6];
+    int cw0[6], cw1[6];
+    for (int i = 0; i < 6; i++) {
+      float cv[3];
+      cross3f(E[i], V[i % 3], cv);
+      ws[i] = dot3f(rd, cv) + dot3f(E[i], pc);
+      cw0[i] = ws[i] >= -kEPS;
+      cw1[i] = ws[i] <= kEPS;
+    }
+    int in[4];
+    for (int f = 0; f < 4; f++) in[f] = fl[f][0] == v || fl[f][1] == v || fl[f][2] == v;
+    float cp[3] = {1e16f, 1e16f, 1e16f};
+    if (cw0[0] && cw0[1] && cw0[2] && !in[0]) {
+      float s = ws[0] + ws[1] + ws[2];
+      for (int k = 0; k < 3; k++) cp[k] = (V[2][k] * ws[0] + V[0][k] * ws[1] + V[1][k] * ws[2]) / s;
+    } else if (cw1[1] && cw0[4] && cw1[5] && !in[1]) {
+      float s = ws[5] + ws[1] - ws[4];
+      for (int k = 0; k < 3; k++) cp[k] = (V[3][k] * ws[1] + V[1][k] * ws[5] - V[2][k] * ws[4]) / s;
+    } else if (cw1[2] && cw1[3] && cw0[5] && !in[2]) {
+      float s = ws[2] + ws[3] - ws[5];
+      for (int k = 0; k < 3; k++) cp[k] = (V[3][k] * ws[2] + V[2][k] * ws[3] - V[0][k] * ws[5]) / s;
+    } else if (cw1[0] && cw0[3] && cw1[4] && !in[3]) {
+      float s = ws[0] + ws[4] - ws[3];
+      for (int k = 0; k < 3; k++) cp[k] = (V[3][k] * ws[0] + V[0][k] * ws[4] - V[1][k] * ws[3]) / s;
+    }
+    float cr[3];
+    sub3f(cp, ro, cr);
+    dout[v] = d / len3f(cr);
+    if (dout[v] < 0) {
+      dout[v] = 0;
+    } else if (!(dout[v] < 1) && !(dout[v] > 0)) {
+      dout[v] = 1;
+    }
+    dout[v] = 1 - dout[v];
+  }
+  float ds = 0, dd[4], w = 0;
+  for (int i = 0; i < 4; i++) {
+    float r[3];
+    sub3f(pt, V[i], r);
+    ds += len3f(r);
+  }
+  for (int i = 0; i < 4; i++) {
+    float r[3];
+    sub3f(pt, V[i], r);
+    dd[i] = ds / len3f(r);
+  }
+  for (int i = 0; i < 4; i++) {
+    dout[i] *= dd[i];
+    w += dout[i];
+  }
+  for (int i = 0; i < 4; i++) dout[i] = dout[i] / w;
+}
+
+static void build_isect(const so_accel *a, const so_ray *ray, const so_hit *h, uint32_t sub,
+                        so_isect *o) {
+  memset(o, 0, sizeof(*o));
+  if (h->prim == 0xffffffffu) return;
+  const uint32_t prim = h->prim;
+  for (int k = 0; k < 3; k++) o->position[k] = ray->org[k] + h->t * ray->dir[k];
+  if (a->kind == SO_TRI) {
+    const uint32_t *fv = &a->faces[3 * (size_t)prim];
+    o->f0 = fv[0];
+    o->f1 = fv[1];
+    o->f2 = fv[2];
+    const float *p0 = &a->verts[3 * (size_t)fv[0]], *p1 = &a->verts[3 * (size_t)fv[1]],
+                *p2 = &a->verts[3 * (size_t)fv[2]];
+    float e1[3], e2[3];
+    sub3f(p1, p0, e1);
+    sub3f(p2, p0, e2);
+    cross3f(e1, e2, o->normal);
+    normalize_real3(o->normal);
+  } else if (a->kind == SO_TET) {
+    static const int ft[4][3] = {{0, 1, 3}, {1, 2, 3}, {2, 0, 3}, {0, 1, 2}};
+    const uint32_t *fv = &a->faces[4 * (size_t)prim];
+    o->f0 = fv[0];
+    o->f1 = fv[1];
+    o->f2 = fv[2];
+    o->f3 = fv[3];
+    float p[4][3];
+    for (int j = 0; j < 4; j++)
+      for (int k = 0; k < 3; k++) p[j][k] = a->verts[3 * (size_t)fv[j] + k];
+    float e1[3], e2[3];
+    sub3f(p[ft[sub & 3][1]], p[ft[sub & 3][0]], e1);
+    sub3f(p[ft[sub & 3][2]], p[ft[sub & 3][0]], e2);
+    cross3f(e1, e2, o->normal);
+    normalize_real3(o->normal);
+    interpolate_tetra(o->position, (const float(*)[3])p, o->d);
+  } else {
+    o->f0 = o->f1 = o->f2 = prim;
+    const float *c = &a->verts[3 * (size_t)prim];
+    float *n = o->normal;
+    sub3f(o->position, c, n);
+    vnormalize_p(n);
+    float xz2 = n[0] * n[0] + n[2] * n[2];
+    if (xz2 > 0.0) {
+      float xz = sqrtf(xz2);
+      float inv = (float)(1.0 / xz);
+      o->tangent[0] = (float)(-2.0 * M_PI * n[0]);
+      o->tangent[1] = (float)(2.0 * M_PI * n[2]);
+      o->tangent[2] = 0.0f;
+      o->binormal[0] = (float)(-M_PI * n[2] * inv * n[1]);
+      o->binormal[1] = (float)(-M_PI * n[0] * inv * n[1]);
+      o->binormal[2] = (float)(M_PI * xz);
+    } else {
+      o->tangent[2] = 1.0f;
+      o->binormal[0] = n[1] > 0.0 ? 1.0f : -1.0f;
+    }
+  }
+}
+
+/* The sphere hit's (u, v) as the reference's Traverse returns them: the
+ * spherical coordinates BuildIntersection computes from its normal. */
+static void sphere_finish(const so_accel *a, const so_ray *ray, so_hit *h) {
+  if (a->kind != SO_SPHERE || h->prim == 0xffffffffu) return;
+  so_isect r;
+  build_isect(a, ray, h, 0, &r);
+  sphere_uv_ref(r.normal, &h->u, &h->v);
+}
+
+/* Shading records of n traced rays (hits and, for tetrahedra, entering
+ * faces from so_trace / so_trace2). */
+SO_API void so_isect_records(const so_accel *a, const so_ray *rays, size_t n,
+                             const so_hit *hits, const uint32_t *subface, so_isect *out,
+                             int nthreads) {
+#ifdef _OPENMP
+  if (nthreads <= 0) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(static) num_threads(nthreads)
+#endif
+  for (long long i = 0; i < (long long)n; i++)
+    build_isect(a, &rays[i], &hits[i], subface ? subface[i] : 0u, &out[i]);
+}
+
 /* stats (optional): 4 x uint64 (branch visits, leaf visits, primitive
  * tests, rays that fell back to the reference's walk). */
 SO_API void so_trace2(const so_accel *a, const so_ray *rays, size_t n,
@@ -1347,6 +1553,7 @@ SO_API void so_trace2(const so_accel *a, const so_ray *rays, size_t n,
     int fall = 0;
     trace2_one(a, &rays[i], prev_normals ? &prev_normals[3 * i] : NULL, &hits[i],
                subface ? &subface[i] : NULL, NULL, NULL, &st, &fall);
+    sphere_finish(a, &rays[i], &hits[i]);
     bv += st.branch_visits;
     lv += st.leaf_visits;
     pt += st.prim_tests;
@@ -1378,6 +1585,7 @@ SO_API void so_trace(const so_accel *a, const so_ray *rays, size_t n,
     trace_one(a, &rays[i], prev_normals ? &prev_normals[3 * i] : NULL, &hits[i],
               subface ? &subface[i] : NULL, vscalar,
               scalar_out ? &scalar_out[i] : NULL, &st);
+    sphere_finish(a, &rays[i], &hits[i]);
     bv += st.branch_visits;
     lv += st.leaf_visits;
     pt += st.prim_tests;
@@ -2310,6 +2518,7 @@ SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
       }
       nvis += st.branch_visits + st.prim_tests;
       if (h.prim == 0xffffffffu || !(h.t < FLT_MAX)) continue;
+      sphere_finish(s->acc[e], &lr, &h); /* the element's Traverse, local ray */
       double lp[3], wp[3];
       for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)h.t * ld[k]);
       scene_multv(&s->T[16 * e], lp, wp);

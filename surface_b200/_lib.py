@@ -50,6 +50,10 @@ class CacheInfo(C.Structure):
 RAY_DTYPE = np.dtype([("org", "<f4", 3), ("prev_prim", "<u4"), ("dir", "<f4", 3),
                       ("prev_t", "<f4")])
 HIT_DTYPE = np.dtype([("t", "<f4"), ("u", "<f4"), ("v", "<f4"), ("prim", "<u4")])
+# srt_isect: BuildIntersection's shading record of a hit (80 bytes)
+ISECT_DTYPE = np.dtype([("position", "<f4", 3), ("f0", "<u4"), ("normal", "<f4", 3),
+                        ("f1", "<u4"), ("tangent", "<f4", 3), ("f2", "<u4"),
+                        ("binormal", "<f4", 3), ("f3", "<u4"), ("d", "<f4", 4)])
 VOL_DTYPE = np.dtype([("width", "<i4"), ("height", "<i4"), ("max_steps", "<i4"),
                       ("reserved", "<i4"), ("eye", "<f4", 3), ("corner", "<f4", 3),
                       ("du", "<f4", 3), ("dv", "<f4", 3), ("step", "<f4"),
@@ -66,7 +70,7 @@ class TraceOpts(C.Structure):
     _fields_ = [("prev_normals", C.c_void_p), ("subface", C.c_void_p),
                 ("vertex_scalar", C.c_void_p), ("scalar_out", C.c_void_p),
                 ("normal_out", C.c_void_p), ("stats", C.c_void_p),
-                ("flags", C.c_uint32), ("reserved", C.c_uint32)]
+                ("flags", C.c_uint32), ("max_iter", C.c_uint32), ("isect", C.c_void_p)]
 
 
 class AccelInfo(C.Structure):

@@ -24,7 +24,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (HIT_DTYPE, MISS, RAY_DTYPE, SRT_SPHERES, SRT_TETRAHEDRA,
+from ._lib import (HIT_DTYPE, ISECT_DTYPE, MISS, RAY_DTYPE, SRT_SPHERES, SRT_TETRAHEDRA,
                    SRT_TRIANGLES, AccelInfo, SurfaceError, TraceOpts, check)
 
 try:  # torch is optional for the host API (numpy works alone)
@@ -162,6 +162,7 @@ class TraceResult:
     subface: object = None
     scalar: object = None
     normal: object = None
+    isect: object = None  # BuildIntersection's records (ISECT_DTYPE, or (n, 20) float32 CUDA)
     extra: dict = field(default_factory=dict)
 
 
@@ -220,12 +221,16 @@ class _Accel:
     # -- traversal --------------------------------------------------------
     def Traverse(self, rays, hits=None, prev_normals=None, want_subface=False,
                  vertex_scalar=None, want_scalar=False, want_normal=False,
-                 single_pass=False, sort_rays=False):
+                 single_pass=False, sort_rays=False, want_isect=False, max_iter=0):
         """Closest hit for every ray (batched XxxAccel::Traverse).
 
         single_pass=True walks the tree once in the reference's own order;
         the default two-pass walk returns the same hits with less work.
-        sort_rays=True traverses in a coherent ray order (same hits)."""
+        sort_rays=True traverses in a coherent ray order (same hits).
+        want_isect=True also returns BuildIntersection's shading record per
+        ray (position, normal, tangent, binormal, f0..f3, d0..d3).
+        max_iter > 0 caps the steps of each ray's walk (SRT_ERR_LIMIT when a
+        ray reaches it)."""
         if not self.built:
             raise SurfaceError(_lib.SRT_ERR_INVALID, "accel not built")
         cuda = _is_cuda(rays)
@@ -244,6 +249,7 @@ class _Accel:
             sub = out((n,), torch.int32) if want_subface else None
             sca = out((n,)) if want_scalar else None
             nrm = out((n, 3)) if want_normal else None
+            isx = out((n, 20)) if want_isect else None
             self.ctx.use_torch_stream()
         else:
             r = np.ascontiguousarray(rays, RAY_DTYPE)
@@ -255,6 +261,7 @@ class _Accel:
             sub = np.zeros(n, np.uint32) if want_subface else None
             sca = np.zeros(n, np.float32) if want_scalar else None
             nrm = np.zeros((n, 3), np.float32) if want_normal else None
+            isx = np.zeros(n, ISECT_DTYPE) if want_isect else None
             self.ctx.use_own_stream()
         pn = _View(prev_normals, np.float32, torch.float32 if torch is not None else None)
         vs = _View(vertex_scalar, np.float32, torch.float32 if torch is not None else None)
@@ -264,11 +271,13 @@ class _Accel:
                       vs.ptr, _View(sca, np.float32).ptr if sca is not None else None,
                       _View(nrm, np.float32).ptr if nrm is not None else None, None,
                       (_lib.SRT_TRACE_SINGLE_PASS if single_pass else 0)
-                      | (_lib.SRT_TRACE_SORT_RAYS if sort_rays else 0), 0)
+                      | (_lib.SRT_TRACE_SORT_RAYS if sort_rays else 0), int(max_iter),
+                      _View(isx, ISECT_DTYPE if not cuda else None).ptr
+                      if isx is not None else None)
         check(self.L.srt_trace_closest(self.h, rv.ptr, n, hv.ptr, C.byref(o)))
-        if not (want_subface or want_scalar or want_normal):
+        if not (want_subface or want_scalar or want_normal or want_isect):
             return hits
-        return TraceResult(hits, sub, sca, nrm)
+        return TraceResult(hits, sub, sca, nrm, isx)
 
     def close(self):
         if getattr(self, "h", None):
@@ -433,4 +442,4 @@ __all__ = ["Context", "Mesh", "Tetrahedron", "Particles", "TriangleAccel", "Tetr
            "ParticleAccel", "TriangleBuildOptions", "TetraBuildOptions",
            "ParticleBuildOptions", "stage_morton", "stage_sort_pairs", "stage_karras",
            "spawn_secondary",
-           "RAY_DTYPE", "HIT_DTYPE", "MISS", "SurfaceError"]
+           "RAY_DTYPE", "HIT_DTYPE", "ISECT_DTYPE", "MISS", "SurfaceError"]

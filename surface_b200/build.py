@@ -24,7 +24,7 @@ LIB = os.path.join(PKG, "libsurface_rt.so")
 
 SOURCES = ["srt_build.cu", "srt_trace.cu", "srt_raysort.cu", "srt_volume.cu", "srt_batch.cu",
            "srt_spawn.cu", "srt_camera.cu", "srt_scene.cu", "srt_cache.cu", "srt_texture.cu",
-           "srt_line.cu", "srt_solid.cu", "srt_capi.cu"]
+           "srt_line.cu", "srt_solid.cu", "srt_isect.cu", "srt_capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "-I" + INCLUDE]

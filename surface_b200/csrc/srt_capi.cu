@@ -75,7 +75,9 @@ static srt_status device_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf 
   return SRT_OK;
 }
 
-static srt_status check_device_errors(srt_ctx *ctx) {
+// Waits for the context stream and reports (then clears) the kernels' limit
+// flags.
+srt_status check_device_errors(srt_ctx *ctx) {
   cudaError_t e = cudaMemcpyAsync(ctx->h_err, ctx->d_err, 4, cudaMemcpyDeviceToHost,
                                   ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -599,17 +601,30 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
       bool ok = true;
       void *pn = direct_view(o.prev_normals, ok), *sub = direct_view(o.subface, ok);
       void *scal = direct_view(o.scalar_out, ok), *norm = direct_view(o.normal_out, ok);
+      void *isx = direct_view(o.isect, ok);
       if (ok) {
         if ((reinterpret_cast<uintptr_t>(mr) | reinterpret_cast<uintptr_t>(mh)) & 15u) {
           set_error("ray and hit arrays must be 16-byte aligned");
           return SRT_ERR_INVALID;
         }
+        if (isx && !sub && a->kind == SRT_TETRAHEDRA) {
+          // the shading pass needs each ray's entering face
+          cudaError_t e = ctx->s_isect_sub.ensure(n * 4);
+          if (e != cudaSuccess) return cuda_status(e, "entering faces");
+          sub = ctx->s_isect_sub.p;
+        }
         srt_status s = launch_trace(
             a, static_cast<const srt_ray *>(mr), n, static_cast<srt_hit *>(mh),
             static_cast<const float *>(pn), static_cast<uint32_t *>(sub),
             a->kind == SRT_TETRAHEDRA ? o.vertex_scalar : nullptr, static_cast<float *>(scal),
-            static_cast<float *>(norm), o.stats, o.flags);
+            static_cast<float *>(norm), o.stats, o.flags, o.max_iter);
         if (s != SRT_OK) return s;
+        if (isx) {
+          s = launch_isect(a, static_cast<const srt_ray *>(mr), n,
+                           static_cast<const srt_hit *>(mh), static_cast<uint32_t *>(sub),
+                           static_cast<srt_isect *>(isx));
+          if (s != SRT_OK) return s;
+        }
         return check_device_errors(ctx);
       }
     }
@@ -641,9 +656,21 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
   }
   uint32_t *dsub = o.subface;
   float *dscal = o.scalar_out, *dnorm = o.normal_out;
+  srt_isect *disx = o.isect;
   if (dsub && !is_device_ptr(dsub)) {
     if ((e = ctx->s_stage_sub.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
     dsub = ctx->s_stage_sub.as<uint32_t>();
+  }
+  uint32_t *isub = dsub;  // entering faces for the shading pass
+  if (disx && !isub && a->kind == SRT_TETRAHEDRA) {
+    if ((e = ctx->s_isect_sub.ensure(n * 4)) != cudaSuccess)
+      return cuda_status(e, "entering faces");
+    isub = ctx->s_isect_sub.as<uint32_t>();
+  }
+  if (disx && !is_device_ptr(disx)) {
+    if ((e = ctx->s_stage_isect.ensure(n * sizeof(srt_isect))) != cudaSuccess)
+      return cuda_status(e, "staging");
+    disx = ctx->s_stage_isect.as<srt_isect>();
   }
   if (dscal && !is_device_ptr(dscal)) {
     if ((e = ctx->s_stage_scal.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
@@ -662,12 +689,18 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
     return SRT_ERR_INVALID;
   }
   s = launch_trace(a, static_cast<const srt_ray *>(drays), n, dh,
-                   static_cast<const float *>(dpn), dsub, static_cast<const float *>(dvs),
-                   dscal, dnorm, o.stats, o.flags);
+                   static_cast<const float *>(dpn), isub, static_cast<const float *>(dvs),
+                   dscal, dnorm, o.stats, o.flags, o.max_iter);
   if (s != SRT_OK) return s;
+  if (disx) {
+    s = launch_isect(a, static_cast<const srt_ray *>(drays), n, dh, isub, disx);
+    if (s != SRT_OK) return s;
+  }
   cudaStream_t st = ctx->stream;
   bool any_host = !hits_dev || (dsub != o.subface) || (dscal != o.scalar_out) ||
-                  (dnorm != o.normal_out);
+                  (dnorm != o.normal_out) || (disx != o.isect);
+  if (disx != o.isect)
+    cudaMemcpyAsync(o.isect, disx, n * sizeof(srt_isect), cudaMemcpyDeviceToHost, st);
   if (!hits_dev)
     cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, st);
   if (dsub != o.subface) cudaMemcpyAsync(o.subface, dsub, n * 4, cudaMemcpyDeviceToHost, st);

@@ -124,6 +124,20 @@ __device__ __forceinline__ int split_axis(uint32_t code) {
   return (__clz(code) - 2) % 3;  // __clz(0) = 32
 }
 
+// Spherical (u, v) of a sphere hit's unit normal n, the values ParticleAccel's
+// BuildIntersection stores in Intersection::u / v
+// (render/render_accel_particle.cc:3013-3014): u = (atan2(n.x, n.z) + pi) *
+// 0.5 * (1 / pi), v = acos(n.y) / pi, all in double and rounded to float at
+// the end.  The reference's build evaluates the angles with the C library's
+// double atan2 / acos; CUDA's double atan2 / acos may differ from those in the
+// last bit or two of the double, which changes the float result only when it
+// lies within a few double ulps of a float rounding boundary.
+constexpr double kPi = 3.14159265358979323846;
+__device__ __forceinline__ void sphere_uv(const float n[3], float &u, float &v) {
+  u = (float)((atan2((double)n[0], (double)n[2]) + kPi) * 0.5 * (1.0 / kPi));
+  v = (float)(acos((double)n[1]) / kPi);
+}
+
 // ---------------------------------------------------------------- host side
 // Bumped whenever any DevBuf frees memory; a captured CUDA graph that holds
 // scratch pointers is valid only while the epoch it was captured at holds.
@@ -158,7 +172,7 @@ struct srt_ctx {
   srt::DevBuf s_keys2, s_vals2, s_hist, s_scan, s_kchild, s_kflags, s_krange,
       s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
       s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm,
-      s_defer, s_spawn, s_rkey, s_rorder;
+      s_defer, s_spawn, s_rkey, s_rorder, s_isect_sub, s_stage_isect;
 };
 
 struct srt_accel {
@@ -179,6 +193,10 @@ struct srt_accel {
 };
 
 namespace srt {
+// Synchronises the context stream and reports kernel limit flags
+// (SRT_ERR_LIMIT) raised since the last report (srt_capi.cu).
+srt_status check_device_errors(srt_ctx *ctx);
+
 // Many triangle scenes built as one forest (srt_batch).
 struct BatchTree {
   DevBuf nodes, indices, codes, prims, scenes, roots, acc, foff, ioff, roff;
@@ -301,10 +319,16 @@ srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
                               srt_hit *hits, int block, int rays_per_thread,
                               unsigned long long *stats);
 
-// traversal (srt_trace.cu)
+// traversal (srt_trace.cu); max_iter 0 = the default walk cap
 srt_status launch_trace(srt_accel *a, const srt_ray *d_rays, size_t n,
                         srt_hit *d_hits, const float *d_prev_normals,
                         uint32_t *d_subface, const float *d_vertex_scalar,
                         float *d_scalar_out, float *d_normal_out,
-                        unsigned long long *d_stats, uint32_t flags);
+                        unsigned long long *d_stats, uint32_t flags,
+                        uint32_t max_iter = 0);
+// shading records of n traced rays (srt_isect.cu): BuildIntersection per hit;
+// d_subface is required for tetrahedra
+srt_status launch_isect(srt_accel *a, const srt_ray *d_rays, size_t n,
+                        const srt_hit *d_hits, const uint32_t *d_subface,
+                        srt_isect *d_isect);
 }  // namespace srt

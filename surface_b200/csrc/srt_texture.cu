@@ -821,7 +821,8 @@ SRT_API srt_status srt_texture3d_fetch(srt_texture3d *t, const float *uvw, size_
       (se = cudaMemcpyAsync(user_rgba, rgba, n * 16, cudaMemcpyDeviceToHost, ctx->stream)) !=
           cudaSuccess)
     return cuda_status(se, "texture output");
-  if (uhost || ohost) return cuda_status(cudaStreamSynchronize(ctx->stream), "texture fetch");
+  // a host-staged call waits anyway: report the sparse walk's cap flag here
+  if (uhost || ohost) return check_device_errors(ctx);
   return SRT_OK;
 }
 

@@ -551,17 +551,42 @@ __device__ void window_walk2(const Node2 *__restrict__ nodes,
 // main kernels keeps their register and stack footprint small.
 
 
+// BuildIntersection's (u, v) of a sphere hit (render/render_accel_particle.cc:
+// 2968-3047): position = org + t * dir, n = vnormalize(position - centre),
+// then the spherical coordinates of n.  Also returns n.
+__device__ __forceinline__ void sphere_hit_uv(const RayF &r, const float4 *__restrict__ prims,
+                                              Best &b, float nn[3]) {
+  const float4 s = prims[b.j];
+  const float c3[3] = {s.x, s.y, s.z};
+#pragma unroll
+  for (int k = 0; k < 3; k++) nn[k] = (r.o[k] + b.t * r.d[k]) - c3[k];
+  const float len = sqrtf(dot3(nn, nn));
+  if (len > FLT_EPSILON * 16) {
+    const float il = __frcp_rn(len);
+#pragma unroll
+    for (int k = 0; k < 3; k++) nn[k] *= il;
+  }
+  sphere_uv(nn, b.u, b.v);
+}
+
 template <int KIND>
 __device__ __forceinline__ void store_node2(size_t i, const Best &b, const Ctx2 &c,
                                             const float4 *__restrict__ prims,
                                             srt_hit *__restrict__ hits,
                                             float *__restrict__ normal_out) {
   const bool any = b.t < FLT_MAX && b.prim != kNone;
-  reinterpret_cast<float4 *>(hits)[i] =
-      make_float4(any ? b.t : FLT_MAX, any ? b.u : 0.0f, any ? b.v : 0.0f,
-                  __uint_as_float(any ? b.prim : kNone));
-  if (!normal_out) return;
   float nn[3] = {0.0f, 0.0f, 0.0f};
+  float hu = any ? b.u : 0.0f, hv = any ? b.v : 0.0f;
+  if (KIND == SRT_SPHERES && any) {
+    // the spherical (u, v) replace the hit's u, v, as in the reference
+    Best bs = b;
+    sphere_hit_uv(c.r, prims, bs, nn);
+    hu = bs.u;
+    hv = bs.v;
+  }
+  reinterpret_cast<float4 *>(hits)[i] =
+      make_float4(any ? b.t : FLT_MAX, hu, hv, __uint_as_float(any ? b.prim : kNone));
+  if (!normal_out) return;
   if (any) {
     if (KIND == SRT_TRIANGLES) {
       const float4 q0 = prims[3 * (size_t)b.j];
@@ -571,18 +596,6 @@ __device__ __forceinline__ void store_node2(size_t i, const Best &b, const Ctx2 
       const float e2[3] = {q2.x - q0.x, q2.y - q0.y, q2.z - q0.z};
       cross3(e1, e2, nn);
       normalize_ref(nn);
-    } else {
-      // position = org + t * dir; vnormalize(position - centre)
-      const float4 s = prims[b.j];
-      const float c3[3] = {s.x, s.y, s.z};
-#pragma unroll
-      for (int k = 0; k < 3; k++) nn[k] = (c.r.o[k] + b.t * c.r.d[k]) - c3[k];
-      const float len = sqrtf(dot3(nn, nn));
-      if (len > FLT_EPSILON * 16) {
-        const float il = __frcp_rn(len);
-#pragma unroll
-        for (int k = 0; k < 3; k++) nn[k] *= il;
-      }
     }
   }
   normal_out[3 * i] = nn[0];
@@ -1156,7 +1169,7 @@ resolve_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__
 srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hits,
                         const float *prev_normals, uint32_t *subface,
                         const float *vscalar, float *scalar_out, float *normal_out,
-                        unsigned long long *stats, uint32_t flags) {
+                        unsigned long long *stats, uint32_t flags, uint32_t max_iter_cap) {
   if (n == 0) return SRT_OK;
   if (n > 0xffffffffull) {
     set_error("at most 2^32-1 rays per call");
@@ -1166,8 +1179,10 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
   const int block = 128;
   const unsigned grid = (unsigned)((n + block - 1) / block);
   const unsigned rgrid = (unsigned)ctx->num_sms * 8;
-  // every node and leaf is visited at most once per walk
-  const uint32_t max_iter = (uint32_t)std::min<size_t>(8 * a->n + 64, 0xfffffff0u);
+  // every node and leaf is visited at most once per walk; a caller's cap
+  // may only lower that
+  uint32_t max_iter = (uint32_t)std::min<size_t>(8 * a->n + 64, 0xfffffff0u);
+  if (max_iter_cap) max_iter = std::min(max_iter, max_iter_cap);
   const SceneInfo *scene = a->scene.as<SceneInfo>();
   const bool single = (flags & SRT_TRACE_SINGLE_PASS) != 0;
   cudaStream_t st = ctx->stream;
@@ -1599,6 +1614,15 @@ __global__ void scene_range_kernel(SceneWork W, int phase) {
   W.bounds[4 * phase + t] = (uint32_t)lo;
 }
 
+// A sphere element's hit takes the spherical (u, v) that the element
+// accel's Traverse returns, from the local ray and local distance.
+template <typename Ctx>
+__device__ __forceinline__ void elem_sphere_uv(const Ctx &c, const SceneElem &e, Best &b) {
+  if (!(b.t < FLT_MAX) || b.prim == kNone) return;
+  float nn[3];
+  sphere_hit_uv(c.r, e.prims, b, nn);
+}
+
 // An element walk's result: phase 0 (each ray's first candidate) makes it
 // the ray's running best; phase 1 (later candidates that the early cull
 // keeps after phase 0) stores it per (ray, slot) for the selection.
@@ -1663,6 +1687,7 @@ scene_walk_kernel(SceneWork W, int phase) {
       c[3] += w.prim;
       if (w.fail) atomicOr(W.err, kErrIter);
       if (done) {
+        if constexpr (KIND == SRT_SPHERES) elem_sphere_uv(ctx, e, b);
         finish_item(W, phase, ray, cs, e_id, e, lo3, ld3, r0.o, b);
       } else {
         W.dlist[lo + atomicAdd(dcount, 1u)] = Deferred{item, full ? 1u : 0u, m};
@@ -1699,6 +1724,7 @@ scene_resolve_kernel(SceneWork W, int phase) {
     c[2] += w.leaf;
     c[3] += w.prim;
     if (w.fail) atomicOr(W.err, kErrIter);
+    if constexpr (KIND == SRT_SPHERES) elem_sphere_uv(ctx, e, b);
     finish_item(W, phase, ray, cs, e_id, e, lo3, ld3, r0.o, b);
   }
   if (W.stats) add_counts(W.stats, 1, c, 4);
@@ -1716,6 +1742,7 @@ __device__ __forceinline__ bool elem_hit(const SceneWork &W, uint32_t i, uint32_
   bool full;
   if (!elem_pass1<KIND>(e, ctx, b, w, W.max_iter, m, full)) elem_replay<KIND>(e, ctx, b, w, W.max_iter, m, full);
   if (w.fail) atomicOr(W.err, kErrIter);
+  if constexpr (KIND == SRT_SPHERES) elem_sphere_uv(ctx, e, b);
   return b.t < FLT_MAX && b.prim != kNone;
 }
 

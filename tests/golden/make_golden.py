@@ -118,6 +118,28 @@ def scene_fixtures():
     return out
 
 
+def isect_fixtures():
+    """Every Intersection field the reference's Traverse fills (t/u/v/prim,
+    subface_id and BuildIntersection's position, normal, tangent, binormal,
+    f0..f3, d0..d3) for small scenes of the three kinds, with oblique rays."""
+    out = {}
+    v, f = S.displaced_octasphere(4, seed=7)
+    rays = S.pinhole_rays(40, 40, (0.4, 0.3, 2.8), (0, 0, 0), fov_deg=50)
+    h, _, rec = O.RefAccel(O.TRI, v, f).trace_isect(rays)
+    out.update(tri_verts=v, tri_faces=f, tri_rays=rays, tri_hits=h, tri_isect=rec)
+    vt, ft, _ = S.tet_grid(8, seed=11)
+    rays = S.pinhole_rays(40, 40, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)
+    h, sub, rec = O.RefAccel(O.TET, vt, ft).trace_isect(rays)
+    out.update(tet_verts=vt, tet_faces=ft, tet_rays=rays, tet_hits=h, tet_subface=sub,
+               tet_isect=rec)
+    pos, rad = S.particles(4096, seed=13)
+    rad = (rad * 30.0).astype(np.float32)  # most rays hit a sphere
+    rays = S.pinhole_rays(40, 40, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    h, _, rec = O.RefAccel(O.SPHERE, pos, None, rad).trace_isect(rays)
+    out.update(sph_pos=pos, sph_rad=rad, sph_rays=rays, sph_hits=h, sph_isect=rec)
+    return out
+
+
 def tex_fixture(L):
     rng = np.random.default_rng(5)
     w, h, d = 9, 7, 5
@@ -194,7 +216,7 @@ def main():
     only = sys.argv[1:]  # names of fixtures to write (default: all)
     jobs = {"prefix_tree": lambda: prefix_tree(L), "scenes_small": scene_fixtures,
             "texture3d": lambda: tex_fixture(L), "dumps_small": dump_fixtures,
-            "lines_solids": lines_solids_fixtures}
+            "lines_solids": lines_solids_fixtures, "isect_small": isect_fixtures}
     for name, make in jobs.items():
         if not only or name in only:
             np.savez_compressed(os.path.join(HERE, name + ".npz"), **make())

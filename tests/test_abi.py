@@ -42,11 +42,85 @@ def test_library_exports_every_declared_symbol():
 def test_record_layouts_match_header():
     assert _lib.RAY_DTYPE.itemsize == 32
     assert _lib.HIT_DTYPE.itemsize == 16
-    assert C.sizeof(_lib.TraceOpts) == 6 * 8 + 8
+    assert C.sizeof(_lib.TraceOpts) == 6 * 8 + 8 + 8
+    assert _lib.ISECT_DTYPE.itemsize == 80
     assert _lib.VOL_DTYPE.itemsize == 4 * 4 + 12 * 4 + 3 * 4
     from oracle import oracle as O
     assert O.RAY_DTYPE == _lib.RAY_DTYPE and O.HIT_DTYPE == _lib.HIT_DTYPE
+    assert O.ISECT_DTYPE == _lib.ISECT_DTYPE
     assert O.VOL_DTYPE == _lib.VOL_DTYPE
+
+
+def test_header_layouts_compile():
+    """sizeof/offsetof of the header's records as a C compiler lays them out."""
+    src = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "surface_rt.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu\n", sizeof(srt_ray), sizeof(srt_hit), sizeof(srt_isect),
+         sizeof(srt_trace_opts), offsetof(srt_trace_opts, isect), offsetof(srt_isect, d));
+  return 0;
+}
+"""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        c = os.path.join(td, "l.c")
+        open(c, "w").write(src)
+        exe = os.path.join(td, "l")
+        subprocess.run(["gcc", "-I" + os.path.join(ROOT, "include"), c, "-o", exe], check=True)
+        out = subprocess.run([exe], capture_output=True, text=True, check=True).stdout.split()
+    assert [int(x) for x in out] == [32, 16, 80, 64, 56, 64]
+
+
+REF_RENDER = os.path.join(os.environ.get("SURFACE_REF", os.path.join(ROOT, "..", "reference")),
+                          "render")
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF_RENDER, "render_accel_triangle.h")),
+                    reason="reference tree absent")
+def test_dropin_header_compiles_against_reference_headers():
+    """include/surface_rt_accel.hpp (GpuTriangleAccel, GpuTetraAccel,
+    GpuParticleAccel) compiles inside the reference's render/ headers, the way
+    a SURFACE maintainer would include it, and its members have the reference
+    accels' signatures."""
+    src = r"""
+#include "surface_rt_accel.hpp"
+using namespace lsgl::render;
+template <typename T, typename P, typename O> void sig() {
+  bool (T::*b)(const P *, const O &) = &T::Build32;
+  bool (T::*t)(Intersection &, Ray &) const = &T::Traverse;
+  void (T::*x)(double *, double *) const = &T::BoundingBox;
+  bool (T::*d)(const char *) = &T::Dump;
+  (void)b; (void)t; (void)x; (void)d;
+}
+int main() {
+  sig<GpuTriangleAccel, Mesh, TriangleBuildOptions>();
+  sig<GpuTetraAccel, Tetrahedron, TetraBuildOptions>();
+  sig<GpuParticleAccel, Particles, ParticleBuildOptions>();
+  sig<TriangleAccel, Mesh, TriangleBuildOptions>();
+  return 0;
+}
+"""
+    import tempfile
+    with tempfile.TemporaryDirectory() as td:
+        c = os.path.join(td, "shim.cc")
+        open(c, "w").write(src)
+        subprocess.run(["g++", "-std=gnu++11", "-fsyntax-only", "-w", "-I" + REF_RENDER,
+                        "-I" + os.path.join(ROOT, "include"), c], check=True)
+
+
+def test_shim_check_library_loads():
+    """The field-by-field checker of the drop-ins (oracle/_ref/libshim_check.so)
+    loads with the product library and exports its entry points."""
+    path = os.path.join(ROOT, "oracle", "_ref", "libshim_check.so")
+    if not os.path.exists(path):
+        pytest.skip("shim checker not built (reference tree absent)")
+    L = C.CDLL(path)
+    for n in ("shim_record_bytes", "shim_check_triangles", "shim_check_tetrahedra",
+              "shim_check_spheres"):
+        getattr(L, n)
+    assert L.shim_record_bytes() == 148
 
 
 def test_no_gpu_fails_loudly():

@@ -44,6 +44,22 @@ def assert_hits_equal(h, ref, fields=("t", "u", "v", "prim")):
         assert bad.size == 0, f"{f}: {bad.size} mismatches, first at {bad[:5]}"
 
 
+# Sphere hits carry BuildIntersection's spherical (u, v): evaluated with the C
+# library's double atan2 / acos in the reference and CUDA's on the GPU, which
+# may differ in the last bits of the double; after rounding to float that is
+# at most an ulp or two.  t and prim stay bit-exact.
+SPHERE_UV_TOL = 1e-6
+
+
+def assert_sphere_hits(h, ref):
+    assert_hits_equal(h, ref, ("t", "prim"))
+    hit = ref["prim"] != O.MISS
+    for f in ("u", "v"):
+        assert np.array_equal(bits(h[f][~hit]), bits(ref[f][~hit])), f
+        d = np.abs(h[f][hit].astype(np.float64) - ref[f][hit].astype(np.float64))
+        assert d.size == 0 or d.max() <= SPHERE_UV_TOL, f"{f}: max |diff| {d.max()}"
+
+
 def trace_both(acc, rays, **kw):
     """Trace with the default two-pass walk, the single-pass walk in the
     reference's order and the default walk in sorted ray order; all must
@@ -145,9 +161,9 @@ def test_build_and_trace_match_reference_fixture(golden, tag, kind):
     elif kind == O.TRI:
         assert_hits_equal(trace_both(acc, g["tri_rays"]), g["tri_hits"])
     else:
-        assert_hits_equal(trace_both(acc, g["sph_rays"]), g["sph_hits"], ("t", "prim"))
+        assert_sphere_hits(trace_both(acc, g["sph_rays"]), g["sph_hits"])
         h2 = trace_both(acc, g["sph_sec_rays"], prev_normals=g["sph_sec_normals"])
-        assert_hits_equal(h2, g["sph_sec_hits"], ("t", "prim"))
+        assert_sphere_hits(h2, g["sph_sec_hits"])
 
 
 # ---------------------------------------------------------------- vs oracle
@@ -207,7 +223,7 @@ def test_spheres_build_trace_and_self_hit_rule():
     rays = S.pinhole_rays(128, 128, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
     res = trace_both(acc, rays, want_normal=True)
     oh = o.trace(rays)
-    assert_hits_equal(res.hits, oh, ("t", "prim"))
+    assert_sphere_hits(res.hits, oh)
     hit = oh["prim"] != O.MISS
     sec = np.zeros(int(hit.sum()), O.RAY_DTYPE)
     p = rays["org"][hit] + res.hits["t"][hit, None] * rays["dir"][hit]
@@ -216,8 +232,8 @@ def test_spheres_build_trace_and_self_hit_rule():
     sec["dir"] = S.hemisphere_dirs(nrm, seed=7)
     sec["prev_prim"] = oh["prim"][hit]
     sec["prev_t"] = oh["t"][hit]
-    assert_hits_equal(trace_both(acc, sec, prev_normals=nrm),
-                      o.trace(sec, prev_normals=nrm), ("t", "prim"))
+    assert_sphere_hits(trace_both(acc, sec, prev_normals=nrm),
+                      o.trace(sec, prev_normals=nrm))
 
 
 def test_sphere_pole_hits_take_the_reference_walk():
@@ -231,7 +247,7 @@ def test_sphere_pole_hits_take_the_reference_walk():
     from test_walk_restatement import pole_pairs
     pos, rad, rays = pole_pairs()
     o, acc = _compare_build(O.SPHERE, pos, None, rad)
-    assert_hits_equal(trace_both(acc, rays), o.trace(rays), ("t", "prim"))
+    assert_sphere_hits(trace_both(acc, rays), o.trace(rays))
     st = torch.zeros(4, dtype=torch.int64, device="cuda")
     rt = torch.as_tensor(rays.view(np.float32).reshape(-1, 8)).cuda()
     h = torch.empty((rays.size, 4), device="cuda")
@@ -251,7 +267,7 @@ def test_constant_radius_spheres():
     can, idx, _ = gpu_canonical(acc, O.SPHERE)
     assert np.array_equal(can, o.canonical())
     rays = S.pinhole_rays(64, 64, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
-    assert_hits_equal(acc.Traverse(rays), o.trace(rays), ("t", "prim"))
+    assert_sphere_hits(acc.Traverse(rays), o.trace(rays))
 
 
 def test_dump_is_reference_format():
@@ -391,7 +407,7 @@ def test_full_size_particle_frame():
     pos, rad = S.particles()
     o, acc = _compare_build(O.SPHERE, pos, None, rad)
     rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)[::37]
-    assert_hits_equal(trace_both(acc, rays), o.trace(rays), ("t", "prim"))
+    assert_sphere_hits(trace_both(acc, rays), o.trace(rays))
 
 
 # ---------------------------------------------------------------- exact ties
@@ -414,7 +430,7 @@ def test_duplicate_spheres_tie_break():
     rad2 = np.concatenate([rad, rad[::-1]])
     o, acc = _compare_build(O.SPHERE, pos2, None, rad2)
     rays = S.pinhole_rays(96, 96, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
-    assert_hits_equal(trace_both(acc, rays), o.trace(rays), ("t", "prim"))
+    assert_sphere_hits(trace_both(acc, rays), o.trace(rays))
 
 
 def test_duplicate_tetrahedra_tie_break():

@@ -118,13 +118,12 @@ def test_oracle_build_and_trace_match_reference_fixture(golden, tag, kind):
         h = acc.trace(g[f"{tag}_rays"])
     ref = g[f"{tag}_hits"]
     for f in ("t", "u", "v", "prim"):
-        if kind == O.SPHERE and f in ("u", "v"):
-            continue
         assert np.array_equal(bits(h[f]), bits(ref[f])), f
     if kind == O.SPHERE:
+        # secondaries (self-hit rule); u, v = BuildIntersection's spherical coordinates
         h2 = acc.trace(g["sph_sec_rays"], prev_normals=g["sph_sec_normals"])
-        assert np.array_equal(h2["prim"], g["sph_sec_hits"]["prim"])
-        assert np.array_equal(bits(h2["t"]), bits(g["sph_sec_hits"]["t"]))
+        for f in ("t", "u", "v", "prim"):
+            assert np.array_equal(bits(h2[f]), bits(g["sph_sec_hits"][f])), f
 
 
 def test_tex3d_matches_reference_fixture(golden):
@@ -185,8 +184,8 @@ def test_oracle_vs_reference_spheres_with_coincident_points():
     assert np.array_equal(o.indices, ridx)
     rays = S.pinhole_rays(96, 96, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
     ho, hr = o.trace(rays), r.trace(rays)
-    assert np.array_equal(ho["prim"], hr["prim"])
-    assert np.array_equal(bits(ho["t"]), bits(hr["t"]))
+    for k in ("t", "u", "v", "prim"):
+        assert np.array_equal(bits(ho[k]), bits(hr[k])), k
 
 
 @need_ref
