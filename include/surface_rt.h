@@ -157,6 +157,11 @@ typedef struct srt_trace_opts {
  * on large ray sets at the cost of the sort.  Hits are identical and are
  * written at each ray's own index. */
 #define SRT_TRACE_SORT_RAYS 2u
+/* Launch the first traversal pass as one thread per ray over a grid of all
+ * rays instead of the default persistent warps (as many blocks as the GPU
+ * holds at once, each warp taking 32 rays at a time until none are left).
+ * Same hits; the default keeps every SM busy to the end of the launch. */
+#define SRT_TRACE_GRID 4u
 
 typedef struct srt_ctx srt_ctx;
 typedef struct srt_accel srt_accel;

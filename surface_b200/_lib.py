@@ -19,6 +19,7 @@ SRT_TRIANGLES, SRT_TETRAHEDRA, SRT_SPHERES = 0, 1, 2
 MISS = 0xFFFFFFFF
 SRT_TRACE_SINGLE_PASS = 1
 SRT_TRACE_SORT_RAYS = 2
+SRT_TRACE_GRID = 4
 
 
 class Camera(C.Structure):

@@ -221,12 +221,15 @@ class _Accel:
     # -- traversal --------------------------------------------------------
     def Traverse(self, rays, hits=None, prev_normals=None, want_subface=False,
                  vertex_scalar=None, want_scalar=False, want_normal=False,
-                 single_pass=False, sort_rays=False, want_isect=False, max_iter=0):
+                 single_pass=False, sort_rays=False, want_isect=False, max_iter=0,
+                 grid_launch=False):
         """Closest hit for every ray (batched XxxAccel::Traverse).
 
         single_pass=True walks the tree once in the reference's own order;
         the default two-pass walk returns the same hits with less work.
         sort_rays=True traverses in a coherent ray order (same hits).
+        grid_launch=True runs the first pass one thread per ray over a full
+        grid instead of persistent warps (same hits).
         want_isect=True also returns BuildIntersection's shading record per
         ray (position, normal, tangent, binormal, f0..f3, d0..d3).
         max_iter > 0 caps the steps of each ray's walk (SRT_ERR_LIMIT when a
@@ -271,7 +274,8 @@ class _Accel:
                       vs.ptr, _View(sca, np.float32).ptr if sca is not None else None,
                       _View(nrm, np.float32).ptr if nrm is not None else None, None,
                       (_lib.SRT_TRACE_SINGLE_PASS if single_pass else 0)
-                      | (_lib.SRT_TRACE_SORT_RAYS if sort_rays else 0), int(max_iter),
+                      | (_lib.SRT_TRACE_SORT_RAYS if sort_rays else 0)
+                      | (_lib.SRT_TRACE_GRID if grid_launch else 0), int(max_iter),
                       _View(isx, ISECT_DTYPE if not cuda else None).ptr
                       if isx is not None else None)
         check(self.L.srt_trace_closest(self.h, rv.ptr, n, hv.ptr, C.byref(o)))

@@ -22,7 +22,7 @@ INCLUDE = os.path.join(ROOT, "include")
 OBJDIR = os.path.join(ROOT, "_build", "surface_rt")
 LIB = os.path.join(PKG, "libsurface_rt.so")
 
-SOURCES = ["srt_build.cu", "srt_trace.cu", "srt_raysort.cu", "srt_volume.cu", "srt_batch.cu",
+SOURCES = ["srt_build.cu", "srt_sort.cu", "srt_trace.cu", "srt_raysort.cu", "srt_volume.cu", "srt_batch.cu",
            "srt_spawn.cu", "srt_camera.cu", "srt_scene.cu", "srt_cache.cu", "srt_texture.cu",
            "srt_line.cu", "srt_solid.cu", "srt_isect.cu", "srt_capi.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]

@@ -6,23 +6,25 @@
 //        render/render_accel_tetra.cc:973-1030, render/render_accel_particle.cc:304-369
 //   2. Morton codes       morton_kernel
 //        render/render_prefix_tree_util.cc:151-304, render/render_prefix_tree_util.h:113-157
-//   3. stable sort        rs_hist / scan / rs_scatter: 3 x 10-bit LSD passes over
-//        the 30-bit codes (4 x 8-bit for full 32-bit keys)
+//   3. stable sort        3 x 10-bit LSD passes over the 30-bit codes:
+//        sort_codes30 (srt_sort.cu; one look-back kernel per pass) up to 2^18
+//        keys, rs_hist / scan / rs_scatter below for more keys, full 32-bit
+//        keys and segmented sorts
 //        render/render_prefix_tree_util.h:296-457 (stable; ties keep input order)
 //   4. Karras tree        karras_kernel
 //        render/render_prefix_tree_util.cc:501-649
-//   5. leaf collapse      level_kernel: a Karras node is emitted as a branch iff
-//        its range holds more than max_leaf+1 keys and its level is <= 23;
-//        both tests are monotone along root paths, so the emitted branches
-//        are exactly the top-down recursion's (BuildTreeRecursive32,
+//   5. leaf collapse      level_scan_kernel: a Karras node is emitted as a
+//        branch iff its range holds more than max_leaf+1 keys and its level
+//        is <= 23; both tests are monotone along root paths, so the emitted
+//        branches are exactly the top-down recursion's (BuildTreeRecursive32,
 //        render/render_accel_triangle.cc:896-992; tetra :1113-1243;
-//        particle :521-661)
+//        particle :521-661).  The same kernel compacts: the exclusive prefix
+//        sum of the branch flags (node slots) by tile look-back.
 //   6. primitive cache    cache_kernel: leaf-ordered primitives for traversal
 //   7. boxes              refit_kernel over the emitted tree only: leaves by
 //        ComputeBoundingBox30 order (render/render_accel_triangle.cc:661-709),
 //        branches bottom up by MergeBoundingBox, left first (:804)
-//   8. compaction         exclusive scan of the branch flags -> node slots
-//   9. emission           emit_node2_kernel / emit_tet_kernel
+//   8. emission           emit_node2_kernel / emit_tet_kernel
 #include <algorithm>
 #include <climits>
 #include <cstdio>
@@ -130,7 +132,15 @@ template <int KIND>
 __global__ void bbox_partial_kernel(const float *__restrict__ v,
                                     const uint32_t *__restrict__ f,
                                     const float *__restrict__ radius, float constr,
-                                    size_t n, Box *__restrict__ partial) {
+                                    size_t n, Box *__restrict__ partial,
+                                    uint32_t *__restrict__ hist_zero,
+                                    unsigned long long *__restrict__ tickets_zero) {
+  // block 0 clears the digit histograms the Morton kernel fills and the sort
+  // passes' tile counters
+  if (hist_zero && blockIdx.x == 0) {
+    for (int i = threadIdx.x; i < 3 * 1024; i += blockDim.x) hist_zero[i] = 0;
+    if (threadIdx.x < 3) tickets_zero[threadIdx.x] = 0ull;
+  }
   Box b;
   box_init(b);
   const float e = (KIND == SRT_TRIANGLES) ? 0.0f : FLT_EPSILON * 16;
@@ -175,6 +185,31 @@ __global__ void bbox_partial_kernel(const float *__restrict__ v,
   }
 }
 
+// Build constants of a scene box: Morton scale, leaf padding, epsScale.
+template <int KIND>
+__device__ __forceinline__ SceneInfo scene_of_box(const Box &r) {
+  SceneInfo s;
+  for (int k = 0; k < 3; k++) {
+    s.lo[k] = r.lo[k];
+    s.hi[k] = r.hi[k];
+    s.inv[k] = 1024.0f / (r.hi[k] - r.lo[k]);
+  }
+  if (KIND == SRT_TRIANGLES) {
+    // epsScale = max extent (render/render_accel_triangle.cc:1452-1463)
+    double es = (double)(r.hi[0] - r.lo[0]);
+    if (es < (double)(r.hi[1] - r.lo[1])) es = (double)(r.hi[1] - r.lo[1]);
+    if (es < (double)(r.hi[2] - r.lo[2])) es = (double)(r.hi[2] - r.lo[2]);
+    s.eps_scale = es;
+    s.keps = FLT_EPSILON * (float)es;
+  } else {
+    s.eps_scale = 16.0;
+    s.keps = FLT_EPSILON * 16;
+  }
+  s.nbranches = 0;
+  s.pad = 0;
+  return s;
+}
+
 template <int KIND>
 __global__ void bbox_final_kernel(const Box *__restrict__ partial, int np,
                                   SceneInfo *__restrict__ scene) {
@@ -206,26 +241,7 @@ __global__ void bbox_final_kernel(const Box *__restrict__ partial, int np,
     }
   }
   if (lane != 0) return;
-  SceneInfo s;
-  for (int k = 0; k < 3; k++) {
-    s.lo[k] = r.lo[k];
-    s.hi[k] = r.hi[k];
-    s.inv[k] = 1024.0f / (r.hi[k] - r.lo[k]);
-  }
-  if (KIND == SRT_TRIANGLES) {
-    // epsScale = max extent (render/render_accel_triangle.cc:1452-1463)
-    double es = (double)(r.hi[0] - r.lo[0]);
-    if (es < (double)(r.hi[1] - r.lo[1])) es = (double)(r.hi[1] - r.lo[1]);
-    if (es < (double)(r.hi[2] - r.lo[2])) es = (double)(r.hi[2] - r.lo[2]);
-    s.eps_scale = es;
-    s.keps = FLT_EPSILON * (float)es;
-  } else {
-    s.eps_scale = 16.0;
-    s.keps = FLT_EPSILON * 16;
-  }
-  s.nbranches = 0;
-  s.pad = 0;
-  *scene = s;
+  *scene = scene_of_box<KIND>(r);
 }
 
 // ------------------------------------------------------------------ 2. Morton
@@ -262,6 +278,88 @@ __global__ void morton_kernel(const float *__restrict__ v,
     uint32_t qz = f2u32_x86((cz - lz) * iz);
     codes[i] = (spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz);
     if (index) index[i] = (uint32_t)i;
+  }
+}
+
+// The same codes with the scene box reduced from the partial boxes in every
+// block (block 0 stores the SceneInfo) and, into `hist`, the digit counts of
+// the sort's three 10-bit passes (shared histograms, warp-aggregated) -- so
+// neither a final-box kernel nor a histogram pass over the codes is needed.
+template <int KIND>
+__global__ void __launch_bounds__(kBlock)
+morton_hist_kernel(const float *__restrict__ v, const uint32_t *__restrict__ f, size_t n,
+                   const Box *__restrict__ partial, int np, SceneInfo *__restrict__ scene,
+                   uint32_t *__restrict__ codes, uint32_t *__restrict__ hist) {
+  __shared__ uint32_t h[3][1024];
+  __shared__ Box sh[kBlock / 32];
+  __shared__ SceneInfo ss;
+  for (int i = threadIdx.x; i < 3 * 1024; i += kBlock) (&h[0][0])[i] = 0;
+  // scene box: any merge order gives the same values (min / max are exact;
+  // the reference's OpenMP merge leaves only the sign of zero unspecified)
+  Box b;
+  box_init(b);
+  for (int i = threadIdx.x; i < np; i += kBlock) b = box_merge(b, partial[i]);
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      b.lo[k] = fmin_ref(b.lo[k], __shfl_down_sync(0xffffffffu, b.lo[k], o));
+      b.hi[k] = fmax_ref(b.hi[k], __shfl_down_sync(0xffffffffu, b.hi[k], o));
+    }
+  }
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (lane == 0) sh[w] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Box r = sh[0];
+    for (int i = 1; i < kBlock / 32; i++) r = box_merge(r, sh[i]);
+    ss = scene_of_box<KIND>(r);
+    if (blockIdx.x == 0) *scene = ss;
+  }
+  __syncthreads();
+  const float lx = ss.lo[0], ly = ss.lo[1], lz = ss.lo[2];
+  const float ix = ss.inv[0], iy = ss.inv[1], iz = ss.inv[2];
+  const size_t stride = (size_t)gridDim.x * kBlock;
+  for (size_t base = (size_t)blockIdx.x * kBlock; base < n; base += stride) {
+    const size_t i = base + threadIdx.x;
+    const bool ok = i < n;
+    uint32_t code = 0;
+    if (ok) {
+      float cx, cy, cz;
+      if (KIND == SRT_SPHERES) {
+        cx = v[3 * i];
+        cy = v[3 * i + 1];
+        cz = v[3 * i + 2];
+      } else if (KIND == SRT_TRIANGLES) {
+        const float third = 1.0f / 3.0f;
+        size_t a = f[3 * i], b2 = f[3 * i + 1], c = f[3 * i + 2];
+        cx = third * ((v[3 * a] + v[3 * b2]) + v[3 * c]);
+        cy = third * ((v[3 * a + 1] + v[3 * b2 + 1]) + v[3 * c + 1]);
+        cz = third * ((v[3 * a + 2] + v[3 * b2 + 2]) + v[3 * c + 2]);
+      } else {
+        const float fourth = 1.0f / 4.0f;
+        size_t a = f[4 * i], b2 = f[4 * i + 1], c = f[4 * i + 2], d = f[4 * i + 3];
+        cx = fourth * (((v[3 * a] + v[3 * b2]) + v[3 * c]) + v[3 * d]);
+        cy = fourth * (((v[3 * a + 1] + v[3 * b2 + 1]) + v[3 * c + 1]) + v[3 * d + 1]);
+        cz = fourth * (((v[3 * a + 2] + v[3 * b2 + 2]) + v[3 * c + 2]) + v[3 * d + 2]);
+      }
+      const uint32_t qx = f2u32_x86((cx - lx) * ix);
+      const uint32_t qy = f2u32_x86((cy - ly) * iy);
+      const uint32_t qz = f2u32_x86((cz - lz) * iz);
+      code = (spread10(qx) << 2) | (spread10(qy) << 1) | spread10(qz);
+      codes[i] = code;
+    }
+    const unsigned act = __ballot_sync(0xffffffffu, ok);
+#pragma unroll
+    for (int p = 0; p < 3; p++) {
+      const uint32_t d = (code >> (10 * p)) & 1023u;
+      const unsigned peers = __match_any_sync(0xffffffffu, d) & act;
+      if (ok && lane == __ffs(peers) - 1) atomicAdd(&h[p][d], (uint32_t)__popc(peers));
+    }
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < 3 * 1024; i += kBlock) {
+    const uint32_t c = (&h[0][0])[i];
+    if (c) atomicAdd(&hist[i], c);
   }
 }
 
@@ -597,7 +695,10 @@ __device__ __forceinline__ int kdelta(const uint32_t *__restrict__ c, int i, int
 __global__ void karras_kernel(const uint32_t *__restrict__ codes, int n,
                               uint32_t *__restrict__ kchild, uint8_t *__restrict__ kflags,
                               uint2 *__restrict__ krange, uint32_t *__restrict__ kparent,
-                              uint32_t *__restrict__ lparent) {
+                              uint32_t *__restrict__ lparent,
+                              unsigned long long *__restrict__ ticket = nullptr) {
+  // the tile counter of level_scan_kernel, which follows on the stream
+  if (ticket && blockIdx.x == 0 && threadIdx.x == 0) *ticket = 0ull;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
        i += gridDim.x * blockDim.x) {
     int d = (kdelta(codes, i, i + 1, n) - kdelta(codes, i, i - 1, n)) >= 0 ? 1 : -1;
@@ -673,102 +774,250 @@ __global__ void cache_kernel(const float *__restrict__ v, const uint32_t *__rest
 template <int KIND>
 __device__ __forceinline__ Box range_box(const float4 *__restrict__ prims, uint32_t lo,
                                          uint32_t hi, float keps) {
+  // groups of four primitives: their loads are issued together
+  constexpr int kGroup = 4;
   Box b = cache_box<KIND>(prims, lo, keps);
-  for (uint32_t j = lo + 1; j <= hi; j++) b = box_merge(b, cache_box<KIND>(prims, j, keps));
+  for (uint32_t j = lo + 1; j <= hi; j += kGroup) {
+    Box bx[kGroup];
+#pragma unroll
+    for (int q = 0; q < kGroup; q++)
+      if (j + q <= hi) bx[q] = cache_box<KIND>(prims, j + q, keps);
+#pragma unroll
+    for (int q = 0; q < kGroup; q++)
+      if (j + q <= hi) b = box_merge(b, bx[q]);
+  }
   return b;
 }
 
-// Box of child `c` (kleaf: Karras leaf = one sorted primitive; else Karras
-// internal node whose box is in ibox).
-template <int KIND>
-__device__ __forceinline__ Box child_box(const float4 *__restrict__ prims,
-                                         const Box *__restrict__ ibox, uint32_t c, bool kleaf,
-                                         float keps) {
-  if (kleaf) return cache_box<KIND>(prims, c, keps);
-  Box b;
-  const float *src = reinterpret_cast<const float *>(&ibox[c]);
-  b.lo[0] = __ldcg(src + 0); b.lo[1] = __ldcg(src + 1); b.lo[2] = __ldcg(src + 2);
-  b.hi[0] = __ldcg(src + 3); b.hi[1] = __ldcg(src + 4); b.hi[2] = __ldcg(src + 5);
-  return b;
+// Internal-node boxes of the build: 32 bytes each, two 16-byte words
+// (lo.x, lo.y, lo.z, hi.x), (hi.y, hi.z, -, -).
+struct __align__(16) BoxP {
+  float4 a, b;
+};
+__device__ __forceinline__ BoxP box_pack(const Box &x) {
+  BoxP p;
+  p.a = make_float4(x.lo[0], x.lo[1], x.lo[2], x.hi[0]);
+  p.b = make_float4(x.hi[1], x.hi[2], 0.0f, 0.0f);
+  return p;
+}
+__device__ __forceinline__ Box box_unpack(const float4 a, const float4 b) {
+  Box x;
+  x.lo[0] = a.x; x.lo[1] = a.y; x.lo[2] = a.z;
+  x.hi[0] = a.w; x.hi[1] = b.x; x.hi[2] = b.y;
+  return x;
+}
+// A box written by another thread of the running kernel (after the acquire
+// of the arrival counter): read through L2.
+__device__ __forceinline__ Box ibox_load(const BoxP *__restrict__ ibox, uint32_t c) {
+  const float4 *q = reinterpret_cast<const float4 *>(ibox + c);
+  return box_unpack(__ldcg(q), __ldcg(q + 1));
+}
+__device__ __forceinline__ void ibox_store(BoxP *__restrict__ ibox, uint32_t c, const Box &x) {
+  const BoxP p = box_pack(x);
+  float4 *q = reinterpret_cast<float4 *>(ibox + c);
+  __stcg(q, p.a);
+  __stcg(q + 1, p.b);
+}
+// Arrival at a node's two-child counter: release this thread's box stores,
+// acquire the other child's; returns the count before this arrival.
+__device__ __forceinline__ uint32_t arrive(uint32_t *counter) {
+  uint32_t old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;"
+               : "=r"(old) : "l"(counter) : "memory");
+  return old;
 }
 
-// Boxes of the emitted tree only.  Thread per Karras internal node i that is
-// emitted as a branch (flag[i]): children that become leaves of the emitted
+// Boxes of the emitted tree only.  Thread per emitted branch (Karras internal
+// node i = kidx[slot]): children that become leaves of the emitted
 // tree get their box here -- a Karras leaf from the cache, a collapsed
 // subtree c by range_box into ibox[c] -- and branch boxes are merged bottom
-// up, left first, by the second of the two children to finish (atomic
-// counter per node).  Ancestors of an emitted branch are emitted branches.
+// up, left first, by the second of the two children to finish (arrival
+// counter per node), each climb carrying its own box and reading only the
+// sibling's.  Ancestors of an emitted branch are emitted branches.
 template <int KIND>
-__global__ void refit_kernel(const uint32_t *__restrict__ kchild,
-                             const uint8_t *__restrict__ kflags,
-                             const uint2 *__restrict__ krange,
-                             const uint32_t *__restrict__ kparent,
-                             const uint32_t *__restrict__ flag, int n,
-                             const SceneInfo *__restrict__ scene,
-                             const float4 *__restrict__ prims, uint32_t *__restrict__ counter,
-                             Box *__restrict__ ibox, uint32_t *__restrict__ err) {
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n - 1 || !flag[i]) return;
+__global__ void __launch_bounds__(256)
+refit_kernel(const uint32_t *__restrict__ kchild, const uint8_t *__restrict__ kflags,
+             const uint2 *__restrict__ krange, const uint32_t *__restrict__ kparent,
+             const uint32_t *__restrict__ flag, const uint32_t *__restrict__ kidx, int n,
+             const SceneInfo *__restrict__ scene, const float4 *__restrict__ prims,
+             uint32_t *__restrict__ counter, BoxP *__restrict__ ibox,
+             uint32_t *__restrict__ err) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= scene->nbranches) return;
+  const uint32_t i = __ldg(&kidx[t]);  // the emitted branches are dense in slot order
   const float keps = scene->keps;
-  const uint32_t g = kchild[i];
-  const uint8_t fl = kflags[i];
+  const uint32_t g = __ldg(&kchild[i]);
+  const uint8_t fl = __ldg(&kflags[i]);
   bool leafside[2];
+  Box lb[2];
 #pragma unroll
   for (int side = 0; side < 2; side++) {
     const uint32_t c = g + side;
     const bool kleaf = fl & (1 << side);
-    leafside[side] = kleaf || !flag[c];
-    if (!kleaf && !flag[c]) {  // collapsed subtree: one emitted leaf
-      const uint2 r = krange[c];
-      ibox[c] = range_box<KIND>(prims, r.x, r.y, keps);
+    leafside[side] = kleaf || !__ldg(&flag[c]);
+    if (kleaf) {
+      lb[side] = cache_box<KIND>(prims, c, keps);
+    } else if (leafside[side]) {  // collapsed subtree: one emitted leaf
+      const uint2 r = __ldg(&krange[c]);
+      lb[side] = range_box<KIND>(prims, r.x, r.y, keps);
+      ibox_store(ibox, c, lb[side]);  // for the emission, and a sibling's climb
     }
   }
-  uint32_t node = (uint32_t)i;
-  if (!(leafside[0] && leafside[1])) {
-    if (!leafside[0] && !leafside[1]) return;  // two branch children climb here
-    __threadfence();
-    if (atomicAdd(&counter[node], 1u) == 0) return;  // the branch child merges
-    __threadfence();
+  if (!leafside[0] && !leafside[1]) return;  // two branch children climb here
+  Box mine;
+  if (leafside[0] && leafside[1]) {
+    mine = box_merge(lb[0], lb[1]);
+  } else {
+    // one leaf child (a collapsed subtree's box is in its own slot already; a
+    // Karras leaf's is read from the cache by whoever merges): meet the
+    // branch child's climb
+    const int ls = leafside[0] ? 0 : 1;
+    const Box lbox = ls == 0 ? lb[0] : lb[1];
+    if (arrive(&counter[i]) == 0) return;
+    const Box bb = ibox_load(ibox, g + (1 - ls));
+    mine = ls == 0 ? box_merge(lbox, bb) : box_merge(bb, lbox);
   }
-  // this thread completes `node` (both children's boxes are written) and
-  // climbs while it is the second arrival
+  // climb: per level one arrival and one sibling-box read; the parent's
+  // parent and split are loaded ahead, alongside the arrival
+  uint32_t node = i;
+  uint32_t q = node == 0 ? kNone : __ldg(&kparent[node]);
   for (int guard = 0; guard < 64; guard++) {
-    const uint32_t gl = __ldcg(&kchild[node]);
-    const uint8_t f2 = __ldcg(&kflags[node]);
-    const Box bl = child_box<KIND>(prims, ibox, gl, f2 & 1, keps);
-    const Box br = child_box<KIND>(prims, ibox, gl + 1, f2 & 2, keps);
-    ibox[node] = box_merge(bl, br);
-    if (node == 0) return;
-    node = __ldcg(&kparent[node]);
-    if (node == kNone) return;
-    __threadfence();
-    if (atomicAdd(&counter[node], 1u) == 0) return;
-    __threadfence();
+    ibox_store(ibox, node, mine);
+    if (node == 0 || q == kNone) return;
+    const uint32_t gq = __ldg(&kchild[q]);
+    const uint8_t fq = __ldg(&kflags[q]);
+    const uint32_t qnext = q == 0 ? kNone : __ldg(&kparent[q]);
+    if (arrive(&counter[q]) == 0) return;
+    const bool left = (gq == node) && !(fq & 1);
+    const uint32_t sib = left ? gq + 1 : gq;
+    const bool sib_kleaf = left ? (fq & 2) : (fq & 1);
+    const Box sb = sib_kleaf ? cache_box<KIND>(prims, sib, keps) : ibox_load(ibox, sib);
+    mine = left ? box_merge(mine, sb) : box_merge(sb, mine);
+    node = q;
+    q = qnext;
   }
   atomicOr(err, kErrTree);
 }
 
 // ------------------------------------------------------------------ 6. levels
-// flag[i] = 1 iff Karras internal node i is emitted as a branch.
-__global__ void level_kernel(const uint2 *__restrict__ krange,
-                             const uint32_t *__restrict__ kparent, int n, int max_leaf,
-                             uint32_t *__restrict__ flag) {
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
-       i += gridDim.x * blockDim.x) {
-    uint2 r = krange[i];
-    uint32_t f = 0;
+// flag[i] = 1 iff Karras internal node i is emitted as a branch: its range
+// holds more than max_leaf + 1 keys and it lies at level <= 23 (the root is
+// always split).
+// The same flags, their exclusive prefix sum (the emitted branches' node slots, in Karras index
+// order), the inverse map kidx (slot -> Karras node) and the branch count,
+// in one pass: tiles of
+// 1024 nodes in ticket order, each adding the flagged counts of earlier tiles
+// by look-back (64-bit words: epoch, flag bits 30-31, count).  Also zeroes
+// the refit's arrival counters.  Waits are bounded (kErrSortWait).
+constexpr int kLsThreads = 256;
+constexpr int kLsItems = 4;
+constexpr int kLsTile = kLsThreads * kLsItems;
+
+__global__ void __launch_bounds__(kLsThreads)
+level_scan_kernel(const uint2 *__restrict__ krange, const uint32_t *__restrict__ kparent,
+                  int n, int max_leaf, uint32_t *__restrict__ flag,
+                  uint32_t *__restrict__ slot, uint32_t *__restrict__ kidx,
+                  uint32_t *__restrict__ counter,
+                  unsigned long long *__restrict__ status, unsigned long long *__restrict__ ticket,
+                  uint32_t epoch, SceneInfo *__restrict__ scene, uint32_t *__restrict__ err) {
+  __shared__ uint32_t s_tile, s_prefix, s_warp[kLsThreads / 32];
+  if (threadIdx.x == 0) s_tile = (uint32_t)atomicAdd(ticket, 1ull);
+  __syncthreads();
+  const uint32_t tile = s_tile;
+  if (tile >= gridDim.x) {  // a counter left over from a failed launch
+    if (threadIdx.x == 0) atomicOr(err, kErrSortWait);
+    return;
+  }
+  const uint32_t m = (uint32_t)n - 1u;
+  const uint32_t base = tile * (uint32_t)kLsTile + threadIdx.x * (uint32_t)kLsItems;
+  uint32_t f[kLsItems];
+#pragma unroll
+  for (int q = 0; q < kLsItems; q++) {
+    const uint32_t i = base + q;
+    f[q] = 0;
+    if (i >= m) continue;
+    counter[i] = 0;
+    const uint2 r = __ldg(&krange[i]);
     if (i == 0) {
-      f = 1;  // Build32 always splits the root
+      f[q] = 1;  // Build32 always splits the root
     } else if (r.y - r.x > (uint32_t)max_leaf) {
       int lvl = 0;
-      uint32_t x = (uint32_t)i;
+      uint32_t x = i;
       while (x != 0 && lvl <= kMaxLevel) {
-        x = kparent[x];
+        x = __ldg(&kparent[x]);
         lvl++;
       }
-      f = (lvl <= kMaxLevel) ? 1u : 0u;
+      f[q] = (lvl <= kMaxLevel) ? 1u : 0u;
     }
-    flag[i] = f;
+  }
+  // exclusive scan within the tile
+  uint32_t x[kLsItems], sum = 0;
+#pragma unroll
+  for (int q = 0; q < kLsItems; q++) {
+    x[q] = sum;
+    sum += f[q];
+  }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t inc = sum;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const uint32_t y = __shfl_up_sync(0xffffffffu, inc, o);
+    if (lane >= o) inc += y;
+  }
+  if (lane == 31) s_warp[w] = inc;
+  __syncthreads();
+  uint32_t wbase = 0, total = 0;
+#pragma unroll
+  for (int k = 0; k < kLsThreads / 32; k++) {
+    const uint32_t v = s_warp[k];
+    if (k < w) wbase += v;
+    total += v;
+  }
+  if (threadIdx.x == 0) {
+    const unsigned long long ep = (unsigned long long)epoch << 32;
+    constexpr uint32_t kAgg = 1u << 30, kInc = 2u << 30, kCnt = (1u << 30) - 1u;
+    unsigned long long *mine = status + tile;
+    uint32_t prefix = 0;
+    if (tile == 0) {
+      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(mine), "l"(ep | kInc | total)
+                   : "memory");
+    } else {
+      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(mine), "l"(ep | kAgg | total)
+                   : "memory");
+      int j = (int)tile - 1;
+      uint32_t spins = 0;
+      while (j >= 0) {
+        unsigned long long v;
+        asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(status + j)
+                     : "memory");
+        if ((uint32_t)(v >> 32) != epoch) {
+          if (++spins > (1u << 22)) {
+            atomicOr(err, kErrSortWait);
+            break;
+          }
+          __nanosleep(64);
+          continue;
+        }
+        prefix += (uint32_t)v & kCnt;
+        if ((uint32_t)v & kInc) break;
+        j--;
+      }
+      asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(mine),
+                   "l"(ep | kInc | ((prefix + total) & kCnt)) : "memory");
+    }
+    s_prefix = prefix;
+    if (tile == gridDim.x - 1) scene->nbranches = prefix + total;
+  }
+  __syncthreads();
+  const uint32_t off = s_prefix + wbase + inc - sum;
+#pragma unroll
+  for (int q = 0; q < kLsItems; q++) {
+    const uint32_t i = base + q;
+    if (i < m) {
+      flag[i] = f[q];
+      slot[i] = off + x[q];
+      if (f[q]) kidx[off + x[q]] = i;  // emitted branches in slot order
+    }
   }
 }
 
@@ -778,7 +1027,7 @@ __device__ __forceinline__ void child_info(uint32_t c, bool kleaf,
                                            const uint2 *__restrict__ krange,
                                            const uint32_t *__restrict__ flag,
                                            const uint32_t *__restrict__ slot,
-                                           const Box *__restrict__ ibox,
+                                           const BoxP *__restrict__ ibox,
                                            const float4 *__restrict__ prims, float keps,
                                            Box &box, bool &is_branch, uint32_t &ref,
                                            uint32_t &count) {
@@ -789,7 +1038,7 @@ __device__ __forceinline__ void child_info(uint32_t c, bool kleaf,
     count = 1;
     return;
   }
-  box = ibox[c];
+  box = box_unpack(__ldg(&ibox[c].a), __ldg(&ibox[c].b));
   if (flag[c]) {
     is_branch = true;
     ref = slot[c];
@@ -809,14 +1058,16 @@ __global__ void emit_node2_kernel(const uint32_t *__restrict__ codes,
                                   const uint2 *__restrict__ krange,
                                   const uint32_t *__restrict__ flag,
                                   const uint32_t *__restrict__ slot,
-                                  const Box *__restrict__ ibox,
+                                  const BoxP *__restrict__ ibox,
                                   const float4 *__restrict__ prims,
-                                  const SceneInfo *__restrict__ scene, int n,
+                                  const SceneInfo *__restrict__ scene,
+                                  const uint32_t *__restrict__ kidx,
                                   Node2 *__restrict__ nodes, uint32_t *__restrict__ err) {
   const float keps = scene->keps;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
-       i += gridDim.x * blockDim.x) {
-    if (!flag[i]) continue;
+  const uint32_t nb = scene->nbranches;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += gridDim.x * blockDim.x) {
+    const uint32_t i = __ldg(&kidx[t]);
     uint32_t g = kchild[i];
     uint8_t fl = kflags[i];
     Box b0, b1;
@@ -831,7 +1082,7 @@ __global__ void emit_node2_kernel(const uint32_t *__restrict__ codes,
     nd.b = make_float4(b0.hi[1], b0.hi[2], b1.lo[0], b1.lo[1]);
     nd.c = make_float4(b1.lo[2], b1.hi[0], b1.hi[1], b1.hi[2]);
     nd.d = make_uint4(r0, r1, (c0 & kCountMask) | (axis << 30), c1 & kCountMask);
-    nodes[slot[i]] = nd;
+    nodes[t] = nd;  // slot[i] == t
   }
 }
 
@@ -848,16 +1099,20 @@ __global__ void emit_tet_kernel(const uint32_t *__restrict__ codes,
                                 const uint2 *__restrict__ krange,
                                 const uint32_t *__restrict__ flag,
                                 const uint32_t *__restrict__ slot,
-                                const Box *__restrict__ ibox,
+                                const BoxP *__restrict__ ibox,
                                 const float4 *__restrict__ prims,
-                                const SceneInfo *__restrict__ scene, int n,
+                                const SceneInfo *__restrict__ scene,
+                                const uint32_t *__restrict__ kidx,
                                 NodeT *__restrict__ nodes, uint32_t *__restrict__ err) {
   const float keps = scene->keps;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
-       i += gridDim.x * blockDim.x) {
-    if (!flag[i]) continue;
-    uint32_t s = slot[i];
-    if (i == 0) nodes[0] = make_tet_node(ibox[0], (uint32_t)split_axis(codes[0]), 1u);
+  const uint32_t nb = scene->nbranches;
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < nb;
+       t += gridDim.x * blockDim.x) {
+    const uint32_t i = __ldg(&kidx[t]);
+    const uint32_t s = t;  // slot[i]
+    if (i == 0)
+      nodes[0] = make_tet_node(box_unpack(__ldg(&ibox[0].a), __ldg(&ibox[0].b)),
+                               (uint32_t)split_axis(codes[0]), 1u);
     uint32_t g = kchild[i];
     uint8_t fl = kflags[i];
 #pragma unroll
@@ -882,23 +1137,29 @@ __global__ void emit_tet_kernel(const uint32_t *__restrict__ codes,
   }
 }
 
-__global__ void finish_kernel(const uint32_t *__restrict__ flag,
-                              const uint32_t *__restrict__ slot, int n,
-                              SceneInfo *__restrict__ scene) {
-  scene->nbranches = slot[n - 2] + flag[n - 2];
-}
 
+// Scene box and Morton codes.  With `hist` (3 x 1024 words) and `tickets`,
+// also the digit histograms of sort_codes30's passes (hist_ready).
 template <int KIND>
 srt_status launch_bbox_morton(srt_ctx *ctx, const float *v, const uint32_t *f,
                               const float *radius, float constr, size_t n,
-                              SceneInfo *scene, uint32_t *codes, uint32_t *index) {
+                              SceneInfo *scene, uint32_t *codes, uint32_t *index,
+                              uint32_t *hist = nullptr,
+                              unsigned long long *tickets = nullptr) {
   cudaStream_t st = ctx->stream;
-  int gb = grid_for(n, kBlock, ctx->num_sms * 4);
+  int gb = grid_for(n, kBlock, ctx->num_sms * (n > (4u << 20) ? 4 : 1));
   cudaError_t e = ctx->s_partial.ensure((size_t)gb * sizeof(Box));
   if (e != cudaSuccess) return cuda_status(e, "bbox scratch");
   Box *partial = ctx->s_partial.as<Box>();
-  bbox_partial_kernel<KIND><<<gb, kBlock, 0, st>>>(v, f, radius, constr, n, partial);
+  bbox_partial_kernel<KIND><<<gb, kBlock, 0, st>>>(v, f, radius, constr, n, partial, hist,
+                                                   tickets);
   ctx->launches++;
+  if (hist) {
+    const int gm = grid_for(n, kBlock, ctx->num_sms * 8);
+    morton_hist_kernel<KIND><<<gm, kBlock, 0, st>>>(v, f, n, partial, gb, scene, codes, hist);
+    ctx->launches++;
+    return cuda_status(cudaGetLastError(), "bbox/morton");
+  }
   bbox_final_kernel<KIND><<<1, 32, 0, st>>>(partial, gb, scene);
   ctx->launches++;
   int gm = grid_for(n, kBlock, ctx->num_sms * 16);
@@ -906,6 +1167,8 @@ srt_status launch_bbox_morton(srt_ctx *ctx, const float *v, const uint32_t *f,
   ctx->launches++;
   return cuda_status(cudaGetLastError(), "bbox/morton");
 }
+
+constexpr size_t kOneSweepMax = (size_t)1 << 18;
 
 template <int KIND>
 srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
@@ -926,61 +1189,94 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
   ENSURE(a->scene, sizeof(SceneInfo));
   size_t max_nodes = (KIND == SRT_TETRAHEDRA) ? (2 * m + 1) : m;
   ENSURE(a->nodes, max_nodes * (KIND == SRT_TETRAHEDRA ? sizeof(NodeT) : sizeof(Node2)));
+
   ENSURE(ctx->s_kchild, m * 4);
   ENSURE(ctx->s_kflags, m);
   ENSURE(ctx->s_krange, m * sizeof(uint2));
   ENSURE(ctx->s_kparent, m * 4);
   ENSURE(ctx->s_counter, m * 4);
-  ENSURE(ctx->s_ibox, m * sizeof(Box));
+  ENSURE(ctx->s_ibox, (m + 1) * sizeof(BoxP));
+  ENSURE(ctx->s_kidx, m * 4);
   ENSURE(ctx->s_flag, m * 4);
   ENSURE(ctx->s_slot, m * 4);
 #undef ENSURE
+#define ENSURE2(buf, bytes)                                  \
+  do {                                                       \
+    if ((e = (buf).ensure(bytes)) != cudaSuccess)            \
+      return cuda_status(e, "build allocation " #buf);       \
+  } while (0)
   SceneInfo *scene = a->scene.as<SceneInfo>();
   uint32_t *codes = a->codes.as<uint32_t>();
   uint32_t *idx = a->indices.as<uint32_t>();
-  srt_status s = launch_bbox_morton<KIND>(ctx, v, f, radius, constr, n, scene, codes, nullptr);
-  if (s != SRT_OK) return s;
-  s = sort_pairs(ctx, codes, idx, n, true, 30);  // 30-bit Morton codes
+  // Morton codes, then their stable sort: up to kOneSweepMax keys with one
+  // look-back kernel per digit pass (the Morton kernel fills its digit
+  // histograms), larger arrays with the histogram / scan / scatter passes,
+  // which keep more of the GPU busy per pass at those sizes (measured)
+  srt_status s;
+  if (n <= kOneSweepMax) {
+    uint32_t *hist = nullptr;
+    unsigned long long *tickets = nullptr;
+    s = sort_codes30_scratch(ctx, n, &hist, &tickets);
+    if (s != SRT_OK) return s;
+    s = launch_bbox_morton<KIND>(ctx, v, f, radius, constr, n, scene, codes, nullptr, hist,
+                                 tickets);
+    if (s != SRT_OK) return s;
+    s = sort_codes30(ctx, codes, idx, n, true, true);
+  } else {
+    s = launch_bbox_morton<KIND>(ctx, v, f, radius, constr, n, scene, codes, nullptr);
+    if (s != SRT_OK) return s;
+    s = sort_pairs(ctx, codes, idx, n, true, 30);
+  }
   if (s != SRT_OK) return s;
   uint32_t *kchild = ctx->s_kchild.as<uint32_t>();
   uint8_t *kflags = ctx->s_kflags.as<uint8_t>();
   uint2 *krange = ctx->s_krange.as<uint2>();
   uint32_t *kparent = ctx->s_kparent.as<uint32_t>();
   uint32_t *counter = ctx->s_counter.as<uint32_t>();
-  Box *ibox = ctx->s_ibox.as<Box>();
+  BoxP *ibox = ctx->s_ibox.as<BoxP>();
+  uint32_t *kidx = ctx->s_kidx.as<uint32_t>();
   uint32_t *flag = ctx->s_flag.as<uint32_t>();
   uint32_t *slot = ctx->s_slot.as<uint32_t>();
+  // level-scan look-back words (ticket + one per tile; zero when allocated)
+  const uint32_t ltiles = (uint32_t)((m + kLsTile - 1) / kLsTile);
+  const size_t lbytes = 256 + (size_t)ltiles * 8;
+  if (lbytes > ctx->s_lscan.cap || !ctx->s_lscan.p) {
+    ENSURE2(ctx->s_lscan, lbytes);
+    if ((e = cudaMemsetAsync(ctx->s_lscan.p, 0, ctx->s_lscan.cap, st)) != cudaSuccess)
+      return cuda_status(e, "level scan");
+  }
+  unsigned long long *lticket = ctx->s_lscan.as<unsigned long long>();
+  unsigned long long *lstatus =
+      reinterpret_cast<unsigned long long *>(ctx->s_lscan.as<char>() + 256);
   int gk = grid_for(m, kBlock, ctx->num_sms * 16);
-  karras_kernel<<<gk, kBlock, 0, st>>>(codes, in, kchild, kflags, krange, kparent, nullptr);
-  ctx->launches++;
-  if ((e = cudaMemsetAsync(counter, 0, m * 4, st)) != cudaSuccess)
-    return cuda_status(e, "refit counters");
-  level_kernel<<<gk, kBlock, 0, st>>>(krange, kparent, in, PrimTraits<KIND>::kMaxLeaf,
-                                      flag);
+  karras_kernel<<<gk, kBlock, 0, st>>>(codes, in, kchild, kflags, krange, kparent, nullptr,
+                                       lticket);
+  const uint32_t lepoch = ++ctx->os_epoch == 0 ? ++ctx->os_epoch : ctx->os_epoch;
+  level_scan_kernel<<<ltiles, kLsThreads, 0, st>>>(krange, kparent, in,
+                                                   PrimTraits<KIND>::kMaxLeaf, flag, slot,
+                                                   kidx, counter, lstatus, lticket, lepoch,
+                                                   scene, ctx->d_err);
   cache_kernel<KIND><<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, st>>>(
       v, f, radius, constr, idx, in, a->prims.as<float4>());
   refit_kernel<KIND><<<(unsigned)((m + kBlock - 1) / kBlock), kBlock, 0, st>>>(
-      kchild, kflags, krange, kparent, flag, in, scene, a->prims.as<float4>(), counter, ibox,
-      ctx->d_err);
-  ctx->launches += 3;
+      kchild, kflags, krange, kparent, flag, kidx, in, scene, a->prims.as<float4>(), counter,
+      ibox, ctx->d_err);
+  ctx->launches += 4;
   s = cuda_status(cudaGetLastError(), "karras/level/cache/refit");
-  if (s != SRT_OK) return s;
-  s = exclusive_scan(ctx, flag, slot, m);
   if (s != SRT_OK) return s;
   if (KIND == SRT_TETRAHEDRA) {
     emit_tet_kernel<<<gk, kBlock, 0, st>>>(codes, kchild, kflags, krange, flag, slot, ibox,
-                                           a->prims.as<float4>(), scene, in,
+                                           a->prims.as<float4>(), scene, kidx,
                                            a->nodes.as<NodeT>(), ctx->d_err);
     ctx->launches++;
   } else {
     emit_node2_kernel<KIND><<<gk, kBlock, 0, st>>>(codes, kchild, kflags, krange, flag,
                                                    slot, ibox, a->prims.as<float4>(),
-                                                   scene, in, a->nodes.as<Node2>(),
+                                                   scene, kidx, a->nodes.as<Node2>(),
                                                    ctx->d_err);
     ctx->launches++;
   }
-  finish_kernel<<<1, 1, 0, st>>>(flag, slot, in, scene);
-  ctx->launches++;
+#undef ENSURE2
   return cuda_status(cudaGetLastError(), "emit");
 }
 

@@ -90,6 +90,7 @@ srt_status check_device_errors(srt_ctx *ctx) {
     if (flags & kErrStack) m += " traversal stack overflow;";
     if (flags & kErrIter) m += " traversal iteration cap;";
     if (flags & kErrTree) m += " malformed tree / leaf too large;";
+    if (flags & kErrSortWait) m += " sort pass gave up waiting on an earlier tile;";
     set_error(m);
     return SRT_ERR_LIMIT;
   }
@@ -208,8 +209,13 @@ SRT_API srt_status srt_ctx_destroy(srt_ctx *c) {
                     &c->s_counter, &c->s_ibox, &c->s_flag, &c->s_slot, &c->s_partial,
                     &c->s_stage_in, &c->s_stage_out, &c->s_stage_aux, &c->s_stage_sub,
                     &c->s_stage_scal, &c->s_stage_norm, &c->s_defer, &c->s_spawn, &c->s_rkey,
-                    &c->s_rorder};
+                    &c->s_rorder, &c->s_isect_sub, &c->s_stage_isect, &c->s_keys3,
+                    &c->s_vals3, &c->s_status, &c->s_lscan, &c->s_rays_in, &c->s_kidx};
+  if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   for (DevBuf *b : bufs) b->release();
+  if (c->ev_copy) cudaEventDestroy(c->ev_copy);
+  if (c->ev_free) cudaEventDestroy(c->ev_free);
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->d_err) cudaFree(c->d_err);
   if (c->h_err) cudaFreeHost(c->h_err);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -555,6 +561,44 @@ static void *mapped_host(const void *p) {
   return at.devicePointer;
 }
 
+// A large page-locked host ray array is copied to the device on the
+// context's side stream, which starts at once: the copy overlaps whatever
+// the context stream is still running (typically the build that precedes a
+// trace), and the context stream waits for it before the trace.  Small
+// arrays are read in place over the host link (*out unchanged).
+#ifndef SRT_PRESTAGE_MIN_BYTES
+#define SRT_PRESTAGE_MIN_BYTES ((size_t)1 << 20)
+#endif
+static srt_status prestage_rays(srt_ctx *ctx, const srt_ray *rays, size_t n,
+                                const srt_ray **out) {
+  const size_t bytes = n * sizeof(srt_ray);
+  if (bytes < SRT_PRESTAGE_MIN_BYTES) return SRT_OK;
+  cudaError_t e;
+  if (!ctx->copy_stream) {
+    if ((e = cudaStreamCreateWithFlags(&ctx->copy_stream, cudaStreamNonBlocking)) !=
+            cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_copy, cudaEventDisableTiming)) != cudaSuccess ||
+        (e = cudaEventCreateWithFlags(&ctx->ev_free, cudaEventDisableTiming)) != cudaSuccess)
+      return cuda_status(e, "ray staging stream");
+  }
+  if (bytes > ctx->s_rays_in.cap) {
+    // a reallocation: nothing of the old buffer may still be read
+    if (ctx->ev_free_recorded && (e = cudaEventSynchronize(ctx->ev_free)) != cudaSuccess)
+      return cuda_status(e, "ray staging");
+    if ((e = ctx->s_rays_in.ensure(bytes)) != cudaSuccess) return cuda_status(e, "ray staging");
+  }
+  if (ctx->ev_free_recorded &&
+      (e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free, 0)) != cudaSuccess)
+    return cuda_status(e, "ray staging");
+  if ((e = cudaMemcpyAsync(ctx->s_rays_in.p, rays, bytes, cudaMemcpyHostToDevice,
+                           ctx->copy_stream)) != cudaSuccess ||
+      (e = cudaEventRecord(ctx->ev_copy, ctx->copy_stream)) != cudaSuccess ||
+      (e = cudaStreamWaitEvent(ctx->stream, ctx->ev_copy, 0)) != cudaSuccess)
+    return cuda_status(e, "ray staging");
+  *out = ctx->s_rays_in.as<srt_ray>();
+  return SRT_OK;
+}
+
 // An optional array that the kernels can address directly: NULL, device
 // memory, or page-locked host memory.  Sets ok = false for pageable memory.
 static void *direct_view(const void *p, bool &ok) {
@@ -592,9 +636,11 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
     return SRT_ERR_INVALID;
   }
   {
-    // Page-locked host rays and hits: the kernels read the rays and write the
-    // hits over the host link while they traverse, so the transfers overlap
-    // the traversal instead of preceding and following it.
+    // Page-locked host rays and hits: the kernels write the hits over the
+    // host link while they traverse, and read small ray arrays the same way;
+    // a large ray array is copied on the side stream as soon as the call is
+    // made (prestage_rays), overlapping a build still running.  Either way
+    // the transfers overlap GPU work instead of preceding and following it.
     // (a sorted trace reads the rays three times: those are staged instead)
     void *mr = mapped_host(rays), *mh = mapped_host(hits);
     if (mr && mh && !(o.flags & SRT_TRACE_SORT_RAYS)) {
@@ -613,17 +659,24 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
           if (e != cudaSuccess) return cuda_status(e, "entering faces");
           sub = ctx->s_isect_sub.p;
         }
-        srt_status s = launch_trace(
-            a, static_cast<const srt_ray *>(mr), n, static_cast<srt_hit *>(mh),
+        const srt_ray *trays = static_cast<const srt_ray *>(mr);
+        srt_status s = prestage_rays(ctx, rays, n, &trays);
+        if (s != SRT_OK) return s;
+        s = launch_trace(
+            a, trays, n, static_cast<srt_hit *>(mh),
             static_cast<const float *>(pn), static_cast<uint32_t *>(sub),
             a->kind == SRT_TETRAHEDRA ? o.vertex_scalar : nullptr, static_cast<float *>(scal),
             static_cast<float *>(norm), o.stats, o.flags, o.max_iter);
         if (s != SRT_OK) return s;
         if (isx) {
-          s = launch_isect(a, static_cast<const srt_ray *>(mr), n,
-                           static_cast<const srt_hit *>(mh), static_cast<uint32_t *>(sub),
-                           static_cast<srt_isect *>(isx));
+          s = launch_isect(a, trays, n, static_cast<const srt_hit *>(mh),
+                           static_cast<uint32_t *>(sub), static_cast<srt_isect *>(isx));
           if (s != SRT_OK) return s;
+        }
+        if (trays != mr) {
+          cudaError_t e = cudaEventRecord(ctx->ev_free, ctx->stream);
+          if (e != cudaSuccess) return cuda_status(e, "ray staging event");
+          ctx->ev_free_recorded = true;
         }
         return check_device_errors(ctx);
       }

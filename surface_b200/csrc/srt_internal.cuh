@@ -31,6 +31,7 @@ constexpr uint32_t kNone = 0xffffffffu;
 constexpr uint32_t kErrStack = 1u;
 constexpr uint32_t kErrIter = 2u;
 constexpr uint32_t kErrTree = 4u;
+constexpr uint32_t kErrSortWait = 8u;  // a sort pass gave up waiting on a tile
 
 // ---------------------------------------------------------------- layouts
 // Two-child node (triangles, spheres): 64 bytes, the reference's
@@ -172,7 +173,15 @@ struct srt_ctx {
   srt::DevBuf s_keys2, s_vals2, s_hist, s_scan, s_kchild, s_kflags, s_krange,
       s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
       s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm,
-      s_defer, s_spawn, s_rkey, s_rorder, s_isect_sub, s_stage_isect;
+      s_defer, s_spawn, s_rkey, s_rorder, s_isect_sub, s_stage_isect, s_keys3, s_vals3,
+      s_status, s_lscan, s_rays_in, s_kidx;
+  uint32_t os_epoch = 0;  // look-back epoch of the last sort pass (srt_sort.cu)
+  // side stream that copies a page-locked host ray array to the device while
+  // earlier work (a build) still runs on the context stream; ev_copy: copy
+  // done, ev_free: the last trace that read s_rays_in is done
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_copy = nullptr, ev_free = nullptr;
+  bool ev_free_recorded = false;
 };
 
 struct srt_accel {
@@ -311,6 +320,14 @@ srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_
 // the keys can be non-zero (30 for Morton codes).
 srt_status sort_pairs(srt_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals,
                       size_t n, bool identity_vals, int key_bits = 32);
+// The same order for 30-bit keys (Morton codes) with one kernel per 10-bit
+// pass (srt_sort.cu); n < 2^30.
+srt_status sort_codes30(srt_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals, size_t n,
+                        bool identity_vals, bool hist_ready = false);
+// Its scratch for n keys: the digit histograms (3 x 1024 words, to be filled
+// before a hist_ready sort) and the three passes' tile counters (zeroed).
+srt_status sort_codes30_scratch(srt_ctx *ctx, size_t n, uint32_t **hist,
+                                unsigned long long **tickets);
 srt_status stage_karras(srt_ctx *ctx, const uint32_t *d_codes, size_t n,
                         uint32_t *d_child, uint8_t *d_flags);
 srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32_t *f,

@@ -710,6 +710,29 @@ __device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
   viol_out = viol;
 }
 
+// Rays of a first-pass kernel: with `next` (a zeroed counter), persistent
+// warps take 32 consecutive rays at a time until all n are done, so every SM
+// stays busy to the end whatever the rays cost; without it, one thread per
+// ray over the grid.
+template <typename Body>
+__device__ __forceinline__ void for_each_ray(size_t n, uint32_t *__restrict__ next,
+                                             const Body &body) {
+  if (!next) {
+    const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    if (k < n) body(k);
+    return;
+  }
+  const int lane = threadIdx.x & 31;
+  while (true) {
+    uint32_t b0 = 0;
+    if (lane == 0) b0 = atomicAdd(next, 32u);
+    b0 = __shfl_sync(0xffffffffu, b0, 0);
+    if ((size_t)b0 >= n) break;
+    const size_t k = (size_t)b0 + (size_t)lane;
+    if (k < n) body(k);
+  }
+}
+
 // Two-child kinds (triangles, spheres).  SINGLE: the reference's walk for
 // every ray.
 template <int KIND, bool SINGLE>
@@ -721,30 +744,31 @@ trace_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
                    const float *__restrict__ prev_normals, float *__restrict__ normal_out,
                    unsigned long long *__restrict__ stats, Deferred *__restrict__ dlist,
                    uint32_t *__restrict__ dcount, uint32_t max_iter,
-                   uint32_t *__restrict__ err, const uint32_t *__restrict__ order) {
-  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
-  const Ctx2 c = make_ctx2<KIND>(rays, i, scene, prev_normals);
-  Work w;
-  Best b;
-  if (SINGLE) {
-    ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
-  } else {
-    float m;
-    uint32_t at_m;
-    bool viol;
-    pass1_node2<KIND>(nodes, prims, sidx, c, 0u, b, w, max_iter, m, at_m, viol);
-    if (!w.fail && (viol || at_m > 1)) {
-      const uint32_t k = atomicAdd(dcount, 1u);
-      dlist[k] = Deferred{(uint32_t)i, viol ? 1u : 0u, (double)m};
-      add_stats(stats, w, 0);
-      return;
+                   uint32_t *__restrict__ err, const uint32_t *__restrict__ order,
+                   uint32_t *__restrict__ next = nullptr) {
+  for_each_ray(n, next, [&](size_t k) {
+    const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
+    const Ctx2 c = make_ctx2<KIND>(rays, i, scene, prev_normals);
+    Work w;
+    Best b;
+    if (SINGLE) {
+      ref_walk2<KIND>(nodes, prims, sidx, c, b, w, max_iter);
+    } else {
+      float m;
+      uint32_t at_m;
+      bool viol;
+      pass1_node2<KIND>(nodes, prims, sidx, c, 0u, b, w, max_iter, m, at_m, viol);
+      if (!w.fail && (viol || at_m > 1)) {
+        const uint32_t q = atomicAdd(dcount, 1u);
+        dlist[q] = Deferred{(uint32_t)i, viol ? 1u : 0u, (double)m};
+        add_stats(stats, w, 0);
+        return;
+      }
     }
-  }
-  if (w.fail) atomicOr(err, kErrIter);
-  add_stats(stats, w, 0);
-  store_node2<KIND>(i, b, c, prims, hits, normal_out);
+    if (w.fail) atomicOr(err, kErrIter);
+    add_stats(stats, w, 0);
+    store_node2<KIND>(i, b, c, prims, hits, normal_out);
+  });
 }
 
 template <int KIND>
@@ -1029,29 +1053,29 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
                  float *__restrict__ scalar_out, unsigned long long *__restrict__ stats,
                  Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
                  uint32_t max_iter, uint32_t *__restrict__ err,
-                 const uint32_t *__restrict__ order) {
-  const size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
-  if (k >= n) return;
-  const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
-  const CtxT c = make_ctxT(rays, i);
-  Work w;
-  Best b;
-  if (SINGLE) {
-    walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
-  } else {
-    double m;
-    bool defer, full;
-    pass1_tet(nodes, prims, sidx, c, b, w, max_iter, m, defer, full);
-    if (!w.fail && defer) {
-      const uint32_t k = atomicAdd(dcount, 1u);
-      dlist[k] = Deferred{(uint32_t)i, full ? 1u : 0u, m};
-      add_stats(stats, w, 0);
-      return;
+                 const uint32_t *__restrict__ order, uint32_t *__restrict__ next = nullptr) {
+  for_each_ray(n, next, [&](size_t k) {
+    const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
+    const CtxT c = make_ctxT(rays, i);
+    Work w;
+    Best b;
+    if (SINGLE) {
+      walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+    } else {
+      double m;
+      bool defer, full;
+      pass1_tet(nodes, prims, sidx, c, b, w, max_iter, m, defer, full);
+      if (!w.fail && defer) {
+        const uint32_t q = atomicAdd(dcount, 1u);
+        dlist[q] = Deferred{(uint32_t)i, full ? 1u : 0u, m};
+        add_stats(stats, w, 0);
+        return;
+      }
     }
-  }
-  if (w.fail) atomicOr(err, kErrIter);
-  add_stats(stats, w, 0);
-  store_tet(i, b, hits, subface, faces, vscalar, scalar_out);
+    if (w.fail) atomicOr(err, kErrIter);
+    add_stats(stats, w, 0);
+    store_tet(i, b, hits, subface, faces, vscalar, scalar_out);
+  });
 }
 
 __global__ void __launch_bounds__(128)
@@ -1166,6 +1190,23 @@ resolve_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__
 
 }  // namespace
 
+// Blocks of `block` threads of kernel fn that one SM holds at once (the same
+// on every device of this architecture; looked up once per kernel).
+int resident_blocks(const void *fn, int block) {
+  static std::mutex mu;
+  static std::vector<std::pair<const void *, int>> known;
+  std::lock_guard<std::mutex> lock(mu);
+  for (auto &k : known)
+    if (k.first == fn) return k.second;
+  int nb = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, block, 0) != cudaSuccess || nb < 1) {
+    cudaGetLastError();
+    nb = 1;
+  }
+  known.emplace_back(fn, nb);
+  return nb;
+}
+
 srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hits,
                         const float *prev_normals, uint32_t *subface,
                         const float *vscalar, float *scalar_out, float *normal_out,
@@ -1186,17 +1227,27 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
   const SceneInfo *scene = a->scene.as<SceneInfo>();
   const bool single = (flags & SRT_TRACE_SINGLE_PASS) != 0;
   cudaStream_t st = ctx->stream;
+  // scratch header: [0] deferred-ray count, [1] persistent warps' ray counter
   Deferred *dlist = nullptr;
-  uint32_t *dcount = nullptr;
-  if (!single) {
-    cudaError_t e = ctx->s_defer.ensure(n * sizeof(Deferred) + 256);
+  uint32_t *dcount = nullptr, *next = nullptr;
+  {
+    cudaError_t e = ctx->s_defer.ensure((single ? 0 : n * sizeof(Deferred)) + 256);
     if (e != cudaSuccess) return cuda_status(e, "deferred list");
     dcount = ctx->s_defer.as<uint32_t>();
     dlist = reinterpret_cast<Deferred *>(ctx->s_defer.as<char>() + 256);
-    if ((e = cudaMemsetAsync(dcount, 0, 4, st)) != cudaSuccess)
+    if ((e = cudaMemsetAsync(dcount, 0, 8, st)) != cudaSuccess)
       return cuda_status(e, "deferred count");
+    if (single) dcount = nullptr, dlist = nullptr;
+    if (!(flags & SRT_TRACE_GRID)) next = ctx->s_defer.as<uint32_t>() + 1;
   }
   const float *pn = a->kind == SRT_SPHERES ? prev_normals : nullptr;
+  // first-pass grid: the whole ray set, or (persistent warps) as many blocks
+  // as the SMs hold at once, never more than the rays need
+  auto fgrid = [&](const void *fn) -> unsigned {
+    if (!next) return grid;
+    const unsigned p = (unsigned)(ctx->num_sms * resident_blocks(fn, block));
+    return std::max(1u, std::min(grid, p));
+  };
   const uint32_t *order = nullptr;
   if (flags & SRT_TRACE_SORT_RAYS) {
     srt_status s = ray_order(ctx, rays, n, &order);
@@ -1208,34 +1259,20 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
       const Node2 *nd = a->nodes.as<Node2>();
       const float4 *pr = a->prims.as<float4>();
       const uint32_t *ix = a->indices.as<uint32_t>();
-      if (a->kind == SRT_TRIANGLES) {
-        if (single)
-          trace_node2_kernel<SRT_TRIANGLES, true><<<grid, block, 0, st>>>(
-              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, nullptr, nullptr,
-              max_iter, ctx->d_err, order);
-        else {
-          trace_node2_kernel<SRT_TRIANGLES, false><<<grid, block, 0, st>>>(
-              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount,
-              max_iter, ctx->d_err, order);
-          resolve_node2_kernel<SRT_TRIANGLES><<<rgrid, block, 0, st>>>(
-              nd, pr, ix, rays, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
-              ctx->d_err);
-          ctx->launches++;
-        }
-      } else {
-        if (single)
-          trace_node2_kernel<SRT_SPHERES, true><<<grid, block, 0, st>>>(
-              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, nullptr, nullptr,
-              max_iter, ctx->d_err, order);
-        else {
-          trace_node2_kernel<SRT_SPHERES, false><<<grid, block, 0, st>>>(
-              nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount,
-              max_iter, ctx->d_err, order);
-          resolve_node2_kernel<SRT_SPHERES><<<rgrid, block, 0, st>>>(
-              nd, pr, ix, rays, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
-              ctx->d_err);
-          ctx->launches++;
-        }
+      const bool tri = a->kind == SRT_TRIANGLES;
+      const auto kern = tri ? (single ? trace_node2_kernel<SRT_TRIANGLES, true>
+                                      : trace_node2_kernel<SRT_TRIANGLES, false>)
+                            : (single ? trace_node2_kernel<SRT_SPHERES, true>
+                                      : trace_node2_kernel<SRT_SPHERES, false>);
+      kern<<<fgrid((const void *)kern), block, 0, st>>>(
+          nd, pr, ix, rays, n, hits, scene, pn, normal_out, stats, dlist, dcount, max_iter,
+          ctx->d_err, order, next);
+      if (!single) {
+        const auto res = tri ? resolve_node2_kernel<SRT_TRIANGLES>
+                             : resolve_node2_kernel<SRT_SPHERES>;
+        res<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, scene, pn, normal_out, stats,
+                                     dlist, dcount, max_iter, ctx->d_err);
+        ctx->launches++;
       }
       break;
     }
@@ -1243,16 +1280,12 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
       const NodeT *nd = a->nodes.as<NodeT>();
       const float4 *pr = a->prims.as<float4>();
       const uint32_t *ix = a->indices.as<uint32_t>();
-      if (single)
-        trace_tet_kernel<true><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
-                                                       a->src_faces, vscalar, scalar_out,
-                                                       stats, nullptr, nullptr, max_iter,
-                                                       ctx->d_err, order);
-      else {
-        trace_tet_kernel<false><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
+      const auto kern = single ? trace_tet_kernel<true> : trace_tet_kernel<false>;
+      kern<<<fgrid((const void *)kern), block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
                                                         a->src_faces, vscalar, scalar_out,
                                                         stats, dlist, dcount, max_iter,
-                                                        ctx->d_err, order);
+                                                        ctx->d_err, order, next);
+      if (!single) {
         resolve_tet_kernel<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, subface,
                                                     a->src_faces, vscalar, scalar_out,
                                                     stats, dlist, dcount, max_iter,

@@ -62,11 +62,14 @@ def assert_sphere_hits(h, ref):
 
 def trace_both(acc, rays, **kw):
     """Trace with the default two-pass walk, the single-pass walk in the
-    reference's order and the default walk in sorted ray order; all must
-    agree bit for bit.  Returns the first."""
+    reference's order, the default walk in sorted ray order and both walks
+    launched over a full grid instead of persistent warps; all must agree bit
+    for bit.  Returns the first."""
     a = acc.Traverse(rays, **kw)
     for other in (acc.Traverse(rays, single_pass=True, **kw),
-                  acc.Traverse(rays, sort_rays=True, **kw)):
+                  acc.Traverse(rays, sort_rays=True, **kw),
+                  acc.Traverse(rays, grid_launch=True, **kw),
+                  acc.Traverse(rays, single_pass=True, grid_launch=True, **kw)):
         ha = a.hits if hasattr(a, "hits") else a
         hb = other.hits if hasattr(other, "hits") else other
         assert_hits_equal(ha, hb)
