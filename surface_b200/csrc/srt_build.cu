@@ -696,7 +696,8 @@ __global__ void karras_kernel(const uint32_t *__restrict__ codes, int n,
                               uint32_t *__restrict__ kchild, uint8_t *__restrict__ kflags,
                               uint2 *__restrict__ krange, uint32_t *__restrict__ kparent,
                               uint32_t *__restrict__ lparent,
-                              unsigned long long *__restrict__ ticket = nullptr) {
+                              unsigned long long *__restrict__ ticket = nullptr,
+                              uint8_t *__restrict__ kprefix = nullptr) {
   // the tile counter of level_scan_kernel, which follows on the stream
   if (ticket && blockIdx.x == 0 && threadIdx.x == 0) *ticket = 0ull;
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n - 1;
@@ -722,6 +723,7 @@ __global__ void karras_kernel(const uint32_t *__restrict__ codes, int n,
     bool lleaf = (lo == g), rleaf = (hi == g + 1);
     if (kchild) kchild[i] = (uint32_t)g;
     kflags[i] = (uint8_t)((lleaf ? 1 : 0) | (rleaf ? 2 : 0));
+    if (kprefix) kprefix[i] = (uint8_t)dnode;  // <= 64
     if (krange) krange[i] = make_uint2((uint32_t)lo, (uint32_t)hi);
     if (kparent) {
       if (!lleaf) kparent[g] = (uint32_t)i;
@@ -915,7 +917,8 @@ constexpr int kLsTile = kLsThreads * kLsItems;
 
 __global__ void __launch_bounds__(kLsThreads)
 level_scan_kernel(const uint2 *__restrict__ krange, const uint32_t *__restrict__ kparent,
-                  int n, int max_leaf, uint32_t *__restrict__ flag,
+                  const uint8_t *__restrict__ kprefix, int n, int max_leaf,
+                  uint32_t *__restrict__ flag,
                   uint32_t *__restrict__ slot, uint32_t *__restrict__ kidx,
                   uint32_t *__restrict__ counter,
                   unsigned long long *__restrict__ status, unsigned long long *__restrict__ ticket,
@@ -930,6 +933,11 @@ level_scan_kernel(const uint2 *__restrict__ krange, const uint32_t *__restrict__
   }
   const uint32_t m = (uint32_t)n - 1u;
   const uint32_t base = tile * (uint32_t)kLsTile + threadIdx.x * (uint32_t)kLsItems;
+  // Each level down a root path lengthens the common prefix of the range's
+  // (code, index) keys by at least one bit, so a node's depth is at most its
+  // prefix length minus the root's: within the level cap there, no parent
+  // walk is needed.
+  const int root_prefix = __ldg(&kprefix[0]);
   uint32_t f[kLsItems];
 #pragma unroll
   for (int q = 0; q < kLsItems; q++) {
@@ -941,13 +949,17 @@ level_scan_kernel(const uint2 *__restrict__ krange, const uint32_t *__restrict__
     if (i == 0) {
       f[q] = 1;  // Build32 always splits the root
     } else if (r.y - r.x > (uint32_t)max_leaf) {
-      int lvl = 0;
-      uint32_t x = i;
-      while (x != 0 && lvl <= kMaxLevel) {
-        x = __ldg(&kparent[x]);
-        lvl++;
+      if ((int)__ldg(&kprefix[i]) - root_prefix <= kMaxLevel) {
+        f[q] = 1u;
+      } else {
+        int lvl = 0;
+        uint32_t x = i;
+        while (x != 0 && lvl <= kMaxLevel) {
+          x = __ldg(&kparent[x]);
+          lvl++;
+        }
+        f[q] = (lvl <= kMaxLevel) ? 1u : 0u;
       }
-      f[q] = (lvl <= kMaxLevel) ? 1u : 0u;
     }
   }
   // exclusive scan within the tile
@@ -1197,6 +1209,7 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
   ENSURE(ctx->s_counter, m * 4);
   ENSURE(ctx->s_ibox, (m + 1) * sizeof(BoxP));
   ENSURE(ctx->s_kidx, m * 4);
+  ENSURE(ctx->s_kprefix, m);
   ENSURE(ctx->s_flag, m * 4);
   ENSURE(ctx->s_slot, m * 4);
 #undef ENSURE
@@ -1249,10 +1262,11 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
   unsigned long long *lstatus =
       reinterpret_cast<unsigned long long *>(ctx->s_lscan.as<char>() + 256);
   int gk = grid_for(m, kBlock, ctx->num_sms * 16);
+  uint8_t *kprefix = ctx->s_kprefix.as<uint8_t>();
   karras_kernel<<<gk, kBlock, 0, st>>>(codes, in, kchild, kflags, krange, kparent, nullptr,
-                                       lticket);
+                                       lticket, kprefix);
   const uint32_t lepoch = ++ctx->os_epoch == 0 ? ++ctx->os_epoch : ctx->os_epoch;
-  level_scan_kernel<<<ltiles, kLsThreads, 0, st>>>(krange, kparent, in,
+  level_scan_kernel<<<ltiles, kLsThreads, 0, st>>>(krange, kparent, kprefix, in,
                                                    PrimTraits<KIND>::kMaxLeaf, flag, slot,
                                                    kidx, counter, lstatus, lticket, lepoch,
                                                    scene, ctx->d_err);

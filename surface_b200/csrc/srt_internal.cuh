@@ -174,7 +174,7 @@ struct srt_ctx {
       s_kparent, s_lparent, s_counter, s_ibox, s_flag, s_slot, s_partial,
       s_stage_in, s_stage_out, s_stage_aux, s_stage_sub, s_stage_scal, s_stage_norm,
       s_defer, s_spawn, s_rkey, s_rorder, s_isect_sub, s_stage_isect, s_keys3, s_vals3,
-      s_status, s_lscan, s_rays_in, s_kidx;
+      s_status, s_lscan, s_rays_in, s_kidx, s_kprefix;
   uint32_t os_epoch = 0;  // look-back epoch of the last sort pass (srt_sort.cu)
   // side stream that copies a page-locked host ray array to the device while
   // earlier work (a build) still runs on the context stream; ev_copy: copy

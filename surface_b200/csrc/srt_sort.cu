@@ -1,10 +1,9 @@
-// srt_sort.cu -- stable sort of (Morton code, index) pairs in one kernel per
-// digit pass.
+// srt_sort.cu -- stable sort of (Morton code, index) pairs.
 //
 // The order is the reference's: ascending 30-bit code, ties in input order
 // (RadixSort30OMP, render/render_prefix_tree_util.h:296-402, is a stable LSD
-// sort whose keys start as index = i).  Here: three 10-bit LSD passes with
-// decoupled look-back.
+// sort whose keys start as index = i).  Here: three 10-bit LSD passes, one
+// decoupled look-back kernel per pass:
 //
 //   os_hist_kernel   one read of the codes: the global count of every digit
 //                    of the three passes (shared-memory histograms, warp-

@@ -121,6 +121,18 @@ def test_sort_stage_is_stable_and_exact(n):
     assert np.array_equal(i, ri)
 
 
+@pytest.mark.parametrize("n", [131_071, 131_072, 131_073, 200_000, 262_144, 262_145])
+def test_build_sort_paths_by_size(n):
+    """The build sorts up to 2^18 codes with one look-back kernel per pass,
+    more with the histogram / scan / scatter passes: sorted codes, order,
+    tree and boxes exact on either side of the switch and at tile sizes."""
+    v, f = S.octasphere_for_count(n, seed=n)
+    f = f[:n]
+    o, acc = _compare_build(O.TRI, v, f)
+    rays = S.pinhole_rays(64, 64, (0, 0, 3), (0, 0, 0))
+    assert_hits_equal(acc.Traverse(rays), o.trace(rays))
+
+
 def test_karras_stage_matches_reference_fixture(golden):
     g = golden("prefix_tree.npz")
     for n in [8, 15, 31, 1023, 1000, 3211]:
