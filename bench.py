@@ -1212,6 +1212,7 @@ def run_batched(args, W):
     _lib.check(L.srt_ctx_synchronize(ctx.h))
     same = torch.equal(hits.view(torch.int32), hits_loop.view(torch.int32))
     block, rpt, captured, kpc = tb.config()
+    tuned = tb.tuning()
 
     # traversal work counters of every scene (one untimed pass) for the roofline
     st = torch.zeros(4, dtype=torch.int64, device=dev)
@@ -1313,6 +1314,7 @@ def run_batched(args, W):
             "speedup_vs_per_scene_loop": round(loop_ms / ms_per_step, 3),
             "batch_launch_shape": {"block": block, "rays_per_grab": rpt,
                                    "graph_captured": captured, "kernels_per_call": kpc},
+            "autotuned": tuned,
             "loop_kernels_per_step": int(loop_launches // args.steps),
             "hits_identical_to_loop": bool(same),
             "clocks": clk.summary(),

@@ -612,6 +612,20 @@ SRT_API srt_status srt_batch_config(srt_batch *b, int32_t *block,
                                     int32_t *rays_per_thread,
                                     int32_t *graph_captured,
                                     uint64_t *kernels_per_call);
+/* The traversal point the autotuner picked on the batch's first call: block
+ * size, grabs of 32 rays per warp, traversal stack depth (24, 32 or 48
+ * entries) and ray order (0: array order; 12 or 22: sorted within each
+ * scene by that many top bits of a Morton code over origin and direction). */
+SRT_API srt_status srt_batch_tuning(srt_batch *b, int32_t *block,
+                                    int32_t *rays_per_grab, int32_t *stack_depth,
+                                    int32_t *sort_bits);
+/* Pin the traversal point instead of autotuning it (block 64, 128 or 256;
+ * 1..8 grabs; depth 24, 32 or 48; sort bits 0, 12 or 22).  Drops a captured
+ * graph.  Hits do not depend on the point, except that a depth the trees
+ * overflow ends the call with SRT_ERR_LIMIT. */
+SRT_API srt_status srt_batch_set_tuning(srt_batch *b, int32_t block,
+                                        int32_t rays_per_grab, int32_t stack_depth,
+                                        int32_t sort_bits);
 
 /* ---------------------------------------------------------------- lines
  * LineAccel (render/render_accel_line.{h,cc}): capped cylinders between the

@@ -100,6 +100,8 @@ def lib():
         L.so_volume_fwd_f32_ex.argtypes = [_P, _P, _P, _P, _P, _P, C.c_int]
         L.so_volume_f64_ex.restype = C.c_double
         L.so_volume_f64_ex.argtypes = [_P, _P, _P, _P, _P, _P, _P, _P, _P]
+        L.so_volume_f64_pixels.restype = C.c_double
+        L.so_volume_f64_pixels.argtypes = [_P, _P, _P, _P, _P, _P, _SZ]
         L.so_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int, _P]
         L.so_camera_rays.restype = _SZ
         L.so_camera_rays.argtypes = [_P, _P, _P, _P]
@@ -673,6 +675,40 @@ def volume_f64(params, dens, dims, tf, target=None, want_grad=False, want_img=Fa
                                   _ptr(dens), _ptr(np.asarray(dims, np.int32)), _ptr(tf),
                                   _ptr(tg), _ptr(img), _ptr(gd), _ptr(gt))
     return loss, img, gd, gt
+
+
+def volume_f64_pixels(params, dens, dims, tf, target, pixels):
+    """The FP64 loss over the listed pixels (py * width + px) only."""
+    dens = np.ascontiguousarray(dens, np.float64)
+    tf = np.ascontiguousarray(tf, np.float64)
+    tg = np.ascontiguousarray(target, np.float32)
+    px = np.ascontiguousarray(pixels, np.uint32)
+    return lib().so_volume_f64_pixels(_ptr(params), _ptr(dens),
+                                      _ptr(np.asarray(dims, np.int32)), _ptr(tf), _ptr(tg),
+                                      _ptr(px), px.size)
+
+
+def volume_pixels_near(params, dims, center, radius):
+    """Pixels whose rays pass within `radius` texels (max norm) of texel
+    `center` (x, y, z) of a uniform volume: the only ones a change of that
+    texel can affect (a conservative superset, from the rays' slab entry and
+    exit in float64)."""
+    W, H = int(params["width"][0]), int(params["height"][0])
+    px, py = np.meshgrid(np.arange(W) + 0.5, np.arange(H) + 0.5)
+    v = (params["corner"][0][None, None, :] + px[..., None] * params["du"][0]
+         + py[..., None] * params["dv"][0] - params["eye"][0])
+    d = v / np.linalg.norm(v, axis=-1, keepdims=True)
+    o = params["eye"][0].astype(np.float64)
+    # texel i of n spans world [2 i/(n-1) - 1 +- 2 r/(n-1)] (texel-corner map u = 0.5 p + 0.5)
+    lo = np.array([2.0 * (center[k] - radius) / (dims[k] - 1) - 1.0 for k in range(3)])
+    hi = np.array([2.0 * (center[k] + radius) / (dims[k] - 1) - 1.0 for k in range(3)])
+    with np.errstate(divide="ignore", invalid="ignore"):
+        ta = (lo - o) / d
+        tb = (hi - o) / d
+    tmin = np.nanmax(np.minimum(ta, tb), axis=-1)
+    tmax = np.nanmin(np.maximum(ta, tb), axis=-1)
+    hit = tmin <= tmax
+    return np.nonzero(hit.reshape(-1))[0].astype(np.uint32)
 
 
 # ---------------------------------------------------------------- eye rays

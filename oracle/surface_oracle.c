@@ -1868,35 +1868,52 @@ static double tex3d_f64(const double *img, const int dim[3], const double q[3],
  * adjoint).  img (optional): width*height*4 output. */
 static double vol_f64(const so_vol_params *P, const so_sampling *S, const double *dens,
                       const int dim[3], const double *tf, const float *target, double *img,
-                      double *grad_dens, double *grad_tf);
+                      double *grad_dens, double *grad_tf, const uint32_t *pixels,
+                      size_t npix);
 
 SO_API double so_volume_f64(const so_vol_params *P, const double *dens,
                             const int dim[3], const double *tf,
                             const float *target, double *img, double *grad_dens,
                             double *grad_tf) {
-  return vol_f64(P, NULL, dens, dim, tf, target, img, grad_dens, grad_tf);
+  return vol_f64(P, NULL, dens, dim, tf, target, img, grad_dens, grad_tf, NULL, 0);
+}
+
+/* The loss over a subset of pixels (indices py * W + px) -- for finite
+ * differences of a local perturbation, which changes only the pixels whose
+ * rays pass near it. */
+SO_API double so_volume_f64_pixels(const so_vol_params *P, const double *dens,
+                                   const int dim[3], const double *tf, const float *target,
+                                   const uint32_t *pixels, size_t npix) {
+  return vol_f64(P, NULL, dens, dim, tf, target, NULL, NULL, NULL, pixels, npix);
 }
 
 SO_API double so_volume_f64_ex(const so_vol_params *P, const so_sampling *S,
                                const double *dens, const int dim[3], const double *tf,
                                const float *target, double *img, double *grad_dens,
                                double *grad_tf) {
-  return vol_f64(P, S, dens, dim, tf, target, img, grad_dens, grad_tf);
+  return vol_f64(P, S, dens, dim, tf, target, img, grad_dens, grad_tf, NULL, 0);
 }
 
+/* pixels: NULL for every pixel of the image, else the npix pixel indices
+ * (py * W + px) whose loss (and gradient) is taken.  Pixels run in parallel;
+ * gradients are accumulated with atomic adds (the order of the double sums
+ * then varies from run to run, within rounding). */
 static double vol_f64(const so_vol_params *P, const so_sampling *S, const double *dens,
                       const int dim[3], const double *tf, const float *target, double *img,
-                      double *grad_dens, double *grad_tf) {
+                      double *grad_dens, double *grad_tf, const uint32_t *pixels,
+                      size_t npix) {
   int W = P->width, H = P->height;
   double loss = 0.0;
-  const int par = !grad_dens && !grad_tf; /* loss/image only: pixels in parallel */
   const double step = P->step;
   const int maxs = P->max_steps;
+  const long long count = pixels ? (long long)npix : (long long)W * H;
 #ifdef _OPENMP
-#pragma omp parallel for schedule(dynamic, 4) reduction(+ : loss) if (par)
+#pragma omp parallel for schedule(dynamic, 64) reduction(+ : loss)
 #endif
-  for (int py = 0; py < H; py++) {
-    for (int px = 0; px < W; px++) {
+  for (long long item = 0; item < count; item++) {
+    {
+      const long long pix = pixels ? (long long)pixels[item] : item;
+      const int py = (int)(pix / W), px = (int)(pix % W);
       double o[3], d[3];
       vol_ray_f64(P, px, py, o, d);
       /* slab test in double mirroring the FP32 one */
@@ -1987,15 +2004,28 @@ static double vol_f64(const so_vol_params *P, const so_sampling *S, const double
         gc[3] = clamped ? 0.0 : ga * P->sigma_scale * step * e;
         if (grad_tf) {
           for (int k = 0; k < 4; k++) {
-            grad_tf[4 * i0 + k] += (1 - f) * gc[k];
-            grad_tf[4 * i1 + k] += f * gc[k];
+            const double g0 = (1 - f) * gc[k], g1 = f * gc[k];
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+            grad_tf[4 * i0 + k] += g0;
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+            grad_tf[4 * i1 + k] += g1;
           }
         }
         if (grad_dens && inr) {
           double drho = 0.0;
           for (int k = 0; k < 4; k++) drho += gc[k] * (tf[4 * i1 + k] - tf[4 * i0 + k]);
           drho *= 255.0;
-          for (int cc = 0; cc < 8; cc++) grad_dens[cx[cc]] += w[cc] * drho;
+          for (int cc = 0; cc < 8; cc++) {
+            const double g = w[cc] * drho;
+#ifdef _OPENMP
+#pragma omp atomic
+#endif
+            grad_dens[cx[cc]] += g;
+          }
         }
         for (int k = 0; k < 3; k++) Cb[k] += Tk * al * c[k];
         Tn = Tk;

@@ -168,6 +168,8 @@ _SIGS = {
     "srt_batch_destroy": [_P],
     "srt_batch_build_trace": [_P, C.c_int32, _P, _P, _P, _P, _P, _P],
     "srt_batch_config": [_P, _P, _P, _P, _P],
+    "srt_batch_tuning": [_P, _P, _P, _P, _P],
+    "srt_batch_set_tuning": [_P, C.c_int32, C.c_int32, C.c_int32, C.c_int32],
 }
 _RESTYPES = {"srt_last_error": C.c_char_p, "srt_ctx_get_stream": _P,
              "srt_scene_top_nodes": _SZ, "srt_matrix_inverse": None,

@@ -69,6 +69,19 @@ class TriangleBatch:
                                       C.byref(k)))
         return blk.value, r.value, bool(g.value), k.value
 
+    def tuning(self):
+        """The autotuned traversal point: {"block", "rays_per_grab",
+        "stack_depth", "sort_bits"} (sort_bits 0: rays in array order)."""
+        v = [C.c_int32() for _ in range(4)]
+        check(self.L.srt_batch_tuning(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("block", "rays_per_grab", "stack_depth", "sort_bits"),
+                        (x.value for x in v)))
+
+    def set_tuning(self, block=128, rays_per_grab=1, stack_depth=32, sort_bits=0):
+        """Pin the traversal point instead of autotuning it."""
+        check(self.L.srt_batch_set_tuning(self.h, int(block), int(rays_per_grab),
+                                          int(stack_depth), int(sort_bits)))
+
     def launches(self):
         return self.L.srt_ctx_launch_count(self.ctx.h)
 

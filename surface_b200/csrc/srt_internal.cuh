@@ -311,6 +311,11 @@ srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uin
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
 // array in context scratch, valid until the context's next sort.
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);
+// The same for the rays of a batch (ray offsets roff over nseg scenes, on
+// the device), kept grouped by scene, ordered within a scene by the top
+// mbits of their Morton code: keys (n + 16 words of scratch) and order (n).
+srt_status batch_ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t *roff,
+                           int nseg, int mbits, uint32_t *keys, uint32_t *order);
 // Device bytes held by a line or solid accel (srt_line.cu, srt_solid.cu).
 uint64_t line_accel_bytes(const srt_line_accel *a);
 uint64_t solid_accel_bytes(const srt_solid_accel *a);
@@ -332,9 +337,11 @@ srt_status stage_karras(srt_ctx *ctx, const uint32_t *d_codes, size_t n,
                         uint32_t *d_child, uint8_t *d_flags);
 srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32_t *f,
                        const uint32_t *h_foff, int nseg);
+// stack_depth: 24, 32 or 48 entries; order: NULL or a batch_ray_order.
 srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
                               srt_hit *hits, int block, int rays_per_thread,
-                              unsigned long long *stats);
+                              unsigned long long *stats, int stack_depth = 32,
+                              const uint32_t *order = nullptr);
 
 // traversal (srt_trace.cu); max_iter 0 = the default walk cap
 srt_status launch_trace(srt_accel *a, const srt_ray *d_rays, size_t n,

@@ -61,21 +61,25 @@ __global__ void ray_box_kernel(const srt_ray *__restrict__ rays, size_t n, int *
   }
 }
 
-__global__ void ray_key_kernel(const srt_ray *__restrict__ rays, size_t n,
-                               const int *__restrict__ box, uint32_t *__restrict__ keys) {
+// The rays' quantization: per coordinate its low end and scale, the
+// coordinates that vary (dims[0..nd)) and the bits each gets (30 / nd).
+struct RayQuant {
   float lo[6], scale[6];
-  int dims[6], nd = 0;
+  int dims[6], nd, bits;
+  __device__ __forceinline__ explicit RayQuant(const int *__restrict__ box) {
+    nd = 0;
 #pragma unroll
-  for (int k = 0; k < 6; k++) {
-    lo[k] = ord_i(box[k]);
-    const float ext = ord_i(box[6 + k]) - lo[k];
-    scale[k] = ext > 0.0f ? 1.0f / ext : 0.0f;
-    if (ext > 0.0f) dims[nd++] = k;
+    for (int k = 0; k < 6; k++) {
+      lo[k] = ord_i(box[k]);
+      const float ext = ord_i(box[6 + k]) - lo[k];
+      scale[k] = ext > 0.0f ? 1.0f / ext : 0.0f;
+      if (ext > 0.0f) dims[nd++] = k;
+    }
+    bits = nd ? 30 / nd : 0;  // bits per varying coordinate (<= 30 total)
   }
-  const int bits = nd ? 30 / nd : 0;  // bits per varying coordinate (<= 30 total)
-  const float qmax = (float)((1u << bits) - 1u);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
+  // Morton code (up to 30 bits) of ray i
+  __device__ __forceinline__ uint32_t key(const srt_ray *__restrict__ rays, size_t i) const {
+    const float qmax = (float)((1u << bits) - 1u);
     const float4 *r4 = reinterpret_cast<const float4 *>(rays + i);
     const float4 a = __ldg(r4), b = __ldg(r4 + 1);
     const float x[6] = {a.x, a.y, a.z, b.x, b.y, b.z};
@@ -89,11 +93,55 @@ __global__ void ray_key_kernel(const srt_ray *__restrict__ rays, size_t n,
     uint32_t key = 0;
     for (int bit = bits - 1; bit >= 0; bit--)
       for (int c = 0; c < nd; c++) key = (key << 1) | ((q[c] >> bit) & 1u);
-    keys[i] = key;
+    return key;
+  }
+};
+
+__global__ void ray_key_kernel(const srt_ray *__restrict__ rays, size_t n,
+                               const int *__restrict__ box, uint32_t *__restrict__ keys) {
+  const RayQuant Q(box);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    keys[i] = Q.key(rays, i);
+}
+
+// Batch keys: the ray's scene above the top mbits of its Morton code, so
+// that the order keeps every scene's rays together.
+__global__ void batch_ray_key_kernel(const srt_ray *__restrict__ rays, size_t n,
+                                     const int *__restrict__ box,
+                                     const uint32_t *__restrict__ roff, int nseg, int mbits,
+                                     uint32_t *__restrict__ keys) {
+  const RayQuant Q(box);
+  const int used = Q.nd * Q.bits;  // significant bits of a Morton code
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const uint32_t m = Q.key(rays, i);
+    const uint32_t top = used > mbits ? m >> (used - mbits) : m << (mbits - used);
+    keys[i] = ((uint32_t)seg_of(roff, nseg, (uint32_t)i) << mbits) | top;
   }
 }
 
 }  // namespace
+
+srt_status batch_ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t *roff,
+                           int nseg, int mbits, uint32_t *keys, uint32_t *order) {
+  int segbits = 0;
+  while ((1 << segbits) < nseg) segbits++;
+  if (mbits < 1 || segbits + mbits > 30) {
+    set_error("ray order: scene and Morton bits exceed 30");
+    return SRT_ERR_INVALID;
+  }
+  int *box = reinterpret_cast<int *>(keys + n);  // 12 ints after the keys
+  cudaStream_t st = ctx->stream;
+  const int grid = ctx->num_sms * 4;
+  ray_box_init_kernel<<<1, 32, 0, st>>>(box);
+  ray_box_kernel<<<grid, 256, 0, st>>>(rays, n, box);
+  batch_ray_key_kernel<<<grid, 256, 0, st>>>(rays, n, box, roff, nseg, mbits, keys);
+  ctx->launches += 3;
+  srt_status s = cuda_status(cudaGetLastError(), "batch ray keys");
+  if (s != SRT_OK) return s;
+  return sort_pairs(ctx, keys, order, n, true, segbits + mbits);
+}
 
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order) {
   cudaError_t e;

@@ -475,77 +475,130 @@ __device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], co
   return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= FLT_MAX);
 }
 
+// The reference's walk (render/render_accel_solid.cc:2345): near child first,
+// every solid whose leaf box the ray enters tested (no culling by distance:
+// a quad face's crossing point is an affine combination of its corners that
+// can fall outside the solid's box, so a box entered beyond the running
+// distance may still hold a nearer hit), the first of the smallest t kept.
+constexpr int kSolidQ = 32;  // solids a lane queues before the warp tests them
+
 template <int NV>
 __global__ void __launch_bounds__(128)
 solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
                    const srt_ray *__restrict__ rays, const uint32_t *__restrict__ order,
                    size_t n, srt_hit *__restrict__ hits, float *__restrict__ normals,
                    float *__restrict__ positions) {
+  // Each lane walks its ray and queues the solids of the leaves it enters
+  // (in the walk's order) until kSolidQ are queued or the walk ends; then
+  // the lanes test their queues side by side, so the costly solid tests run
+  // on full warps instead of on the few lanes that reached a leaf.  A lane
+  // whose walk and queue are done writes its hit and takes the next ray.
   constexpr int RF = rec_floats(NV);
-  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < n;
-       k += (size_t)gridDim.x * blockDim.x) {
-    const size_t i = order ? (size_t)__ldg(&order[k]) : k;
+  __shared__ uint32_t queue[kSolidQ][128];
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  size_t i = 0;
+  float org[3], dir[3], inv[3];
+  int sign[3];
+  uint32_t prev = 0;
+  float t = FLT_MAX, bn[3], bp[3];
+  uint32_t prim = SRT_MISS;
+  int stack[64];
+  int sp = -1;
+  uint32_t leaf_next = 0, leaf_left = 0;
+  auto start = [&]() {
+    i = order ? (size_t)__ldg(&order[k]) : k;
     const float4 *rq = reinterpret_cast<const float4 *>(rays + i);
     const float4 r0 = __ldg(rq), r1 = __ldg(rq + 1);
-    const float org[3] = {r0.x, r0.y, r0.z}, dir[3] = {r1.x, r1.y, r1.z};
-    const uint32_t prev = __float_as_uint(r0.w);
-    int sign[3];
-    float inv[3];
-    for (int k = 0; k < 3; k++) {
-      sign[k] = dir[k] < 0.0f ? 1 : 0;
-      inv[k] = __frcp_rn(dir[k]);  // (float)(1.0 / dir), correctly rounded
+    org[0] = r0.x; org[1] = r0.y; org[2] = r0.z;
+    dir[0] = r1.x; dir[1] = r1.y; dir[2] = r1.z;
+    prev = __float_as_uint(r0.w);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+      sign[c] = dir[c] < 0.0f ? 1 : 0;
+      inv[c] = __frcp_rn(dir[c]);  // (float)(1.0 / dir), correctly rounded
+      bn[c] = bp[c] = 0.0f;
+    }
+    t = FLT_MAX;
+    prim = SRT_MISS;
+    stack[0] = 0;
+    sp = 0;
+    leaf_left = 0;
+  };
+  bool live = k < n;
+  if (live) start();
+  while (__any_sync(0xffffffffu, live)) {
+    int len = 0;
+    if (live) {
+      while (len < kSolidQ) {
+        if (leaf_left) {
+          queue[len++][threadIdx.x] = leaf_next++;
+          leaf_left--;
+          continue;
+        }
+        if (sp < 0) break;
+        const float4 *q = reinterpret_cast<const float4 *>(nodes + stack[sp]);
+        const float4 a = __ldg(q), b = __ldg(q + 1);
+        sp--;
+        const SNode nd = {{a.x, a.y, a.z}, __float_as_uint(a.w), {b.x, b.y, b.z},
+                          __float_as_uint(b.w)};
+        if (!sbox_hit(nd, org, inv, sign)) continue;
+        if (!(nd.w1 & kSolidLeaf)) {
+          const int axis = (int)(nd.w1 >> 29);
+          const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
+          const int nearc = sign[axis];
+          stack[++sp] = nearc ? left : right;  // far
+          stack[++sp] = nearc ? right : left;  // near
+          continue;
+        }
+        leaf_next = nd.w0;
+        leaf_left = nd.w1 & ~kSolidLeaf;
+      }
     }
     const D3 dorg = {org[0], org[1], org[2]}, ddir = {dir[0], dir[1], dir[2]};
-    float t = FLT_MAX, bn[3] = {0.f, 0.f, 0.f}, bp[3] = {0.f, 0.f, 0.f};
-    uint32_t prim = SRT_MISS;
-    int stack[64];
-    int sp = 0;
-    stack[0] = 0;
-    while (sp >= 0) {
-      const float4 *q = reinterpret_cast<const float4 *>(nodes + stack[sp]);
-      const float4 a = __ldg(q), b = __ldg(q + 1);
-      sp--;
-      const SNode nd = {{a.x, a.y, a.z}, __float_as_uint(a.w), {b.x, b.y, b.z},
-                        __float_as_uint(b.w)};
-      if (!sbox_hit(nd, org, inv, sign)) continue;
-      if (!(nd.w1 & kSolidLeaf)) {
-        const int axis = (int)(nd.w1 >> 29);
-        const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
-        const int nearc = sign[axis];
-        stack[++sp] = nearc ? left : right;  // far
-        stack[++sp] = nearc ? right : left;  // near
-        continue;
-      }
-      const uint32_t first = nd.w0, cnt = nd.w1 & ~kSolidLeaf;
-      for (uint32_t j = 0; j < cnt; j++) {
-        const float *r = recs + (size_t)RF * (first + j);
-        const uint32_t p = __float_as_uint(__ldg(r + 3 * NV));
-        if (p == prev) continue;  // Ray::prev_prim_id
-        SolidV<NV> S;
+    for (int qi = 0; qi < len; qi++) {
+      const uint32_t j = queue[qi][threadIdx.x];
+      const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)RF * j);
+      float rv[RF];
 #pragma unroll
-        for (int k = 0; k < NV; k++)
-          for (int c = 0; c < 3; c++) S.x[k][c] = __ldg(r + 3 * k + c);
-        SIsect is[2];
-        for (int s = 0; s < 2; s++) is[s].t = 0.0f;
-        const bool h = s_isect(dorg, ddir, S, is);
-        if (!h) continue;
-        for (int s = 0; s < 2; s++)
-          if (is[s].t >= 0.0f && is[s].t < t) {
-            t = is[s].t;
-            prim = p;
-            for (int k = 0; k < 3; k++) {
-              bn[k] = is[s].nrm[k];
-              bp[k] = is[s].pos[k];
-            }
-          }
+      for (int q4 = 0; q4 < RF / 4; q4++) {
+        const float4 v4 = __ldg(r4 + q4);
+        rv[4 * q4] = v4.x;
+        rv[4 * q4 + 1] = v4.y;
+        rv[4 * q4 + 2] = v4.z;
+        rv[4 * q4 + 3] = v4.w;
       }
+      const uint32_t p = __float_as_uint(rv[3 * NV]);
+      if (p == prev) continue;  // Ray::prev_prim_id
+      SolidV<NV> S;
+#pragma unroll
+      for (int c = 0; c < NV; c++)
+#pragma unroll
+        for (int e = 0; e < 3; e++) S.x[c][e] = rv[3 * c + e];
+      SIsect is[2];
+      for (int h = 0; h < 2; h++) is[h].t = 0.0f;
+      if (!s_isect(dorg, ddir, S, is)) continue;
+      for (int h = 0; h < 2; h++)
+        if (is[h].t >= 0.0f && is[h].t < t) {
+          t = is[h].t;
+          prim = p;
+          for (int c = 0; c < 3; c++) {
+            bn[c] = is[h].nrm[c];
+            bp[c] = is[h].pos[c];
+          }
+        }
     }
-    const bool got = t < FLT_MAX;
-    reinterpret_cast<float4 *>(hits)[i] =
-        make_float4(t, 0.0f, 0.0f, __uint_as_float(got ? prim : SRT_MISS));
-    for (int k = 0; k < 3; k++) {
-      if (normals) normals[3 * i + k] = got ? bn[k] : 0.0f;
-      if (positions) positions[3 * i + k] = got ? bp[k] : 0.0f;
+    if (live && sp < 0 && leaf_left == 0) {
+      const bool got = t < FLT_MAX;
+      reinterpret_cast<float4 *>(hits)[i] =
+          make_float4(t, 0.0f, 0.0f, __uint_as_float(got ? prim : SRT_MISS));
+      for (int c = 0; c < 3; c++) {
+        if (normals) normals[3 * i + c] = got ? bn[c] : 0.0f;
+        if (positions) positions[3 * i + c] = got ? bp[c] : 0.0f;
+      }
+      k += stride;
+      live = k < n;
+      if (live) start();
     }
   }
 }
@@ -793,7 +846,19 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
     set_error("ray and hit arrays must be 16-byte aligned");
     return SRT_ERR_INVALID;
   }
-  const unsigned grid = (unsigned)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * 32);
+  // as many blocks as the SMs hold at once: lanes take their next ray as
+  // soon as they finish one
+  const void *kfn = a->nv == 5   ? (const void *)solid_trace_kernel<5>
+                    : a->nv == 6 ? (const void *)solid_trace_kernel<6>
+                                 : (const void *)solid_trace_kernel<8>;
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 128, 0) != cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const unsigned grid =
+      (unsigned)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * per_sm);
   const SNode *nd = a->dnodes.as<SNode>();
   const float *rc = a->drecs.as<float>();
   const srt_ray *rr = static_cast<const srt_ray *>(dr);

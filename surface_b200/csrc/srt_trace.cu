@@ -29,6 +29,7 @@
 // a hit leaf is pushed as a (first primitive, count) entry, which visits
 // leaves in exactly the reference's order.
 #include <mutex>
+#include <type_traits>
 
 #include "srt_internal.cuh"
 
@@ -131,7 +132,6 @@ struct D3 {
 };
 __device__ __forceinline__ D3 dsub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
 __device__ __forceinline__ D3 dadd(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ D3 dscale(double f, D3 v) { return {v.x * f, v.y * f, v.z * f}; }
 __device__ __forceinline__ D3 dcross(D3 a, D3 b) {
   return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
 }
@@ -146,123 +146,123 @@ __device__ __forceinline__ Plk plk(D3 v0, D3 v1) { return {dsub(v1, v0), dcross(
 __device__ __forceinline__ double pdot(const Plk &a, const Plk &b) {
   return ddot(a.d, b.c) + ddot(b.d, a.c);
 }
-__device__ __forceinline__ D3 bary(double a, double b, D3 A, D3 B, D3 C) {
-  return dadd(dadd(dscale(1 - a - b, A), dscale(a, B)), dscale(b, C));
+// The ray's side of the Pluecker tests, formed once per ray: its Pluecker
+// coordinates (through orig and orig + dir) and, for ComputeParametricDist,
+// the first axis with a nonzero direction, the origin's coordinate on it and
+// the direction's reciprocal there.
+struct TetRay {
+  Plk ray;
+  double oa, iva;
+  float sel[3];  // one-hot selector of that axis
+};
+
+__device__ __forceinline__ TetRay tet_ray(D3 orig, D3 dir) {
+  TetRay t;
+  t.ray = plk(orig, dadd(orig, dir));
+  const int ax = dir.x != 0.0 ? 0 : (dir.y != 0.0 ? 1 : 2);
+  const double da = ax == 0 ? dir.x : (ax == 1 ? dir.y : dir.z);
+  t.oa = ax == 0 ? orig.x : (ax == 1 ? orig.y : orig.z);
+  t.iva = 1.0 / da;
+  t.sel[0] = ax == 0 ? 1.0f : 0.0f;
+  t.sel[1] = ax == 1 ? 1.0f : 0.0f;
+  t.sel[2] = ax == 2 ? 1.0f : 0.0f;
+  return t;
 }
-__device__ __forceinline__ double param_enter(D3 o, D3 d, D3 pe) {
-  if (d.x != 0.0) {
-    double iv = 1.0 / d.x;
-    return (pe.x - o.x) * iv;
-  } else if (d.y != 0.0) {
-    double iv = 1.0 / d.y;
-    return (pe.y - o.y) * iv;
+
+// A tetrahedron's vertices as stored (float), widened at use.
+struct TetV {
+  float v[12];
+  __device__ __forceinline__ D3 operator[](int k) const {
+    return {(double)v[3 * k], (double)v[3 * k + 1], (double)v[3 * k + 2]};
   }
-  double iv = 1.0 / d.z;
-  return (pe.z - o.z) * iv;
-}
+  // coordinate of vertex k on the axis selected one-hot by sel (exact: the
+  // other two terms are zeros)
+  __device__ __forceinline__ double axis(int k, const float (&sel)[3]) const {
+    return (double)((v[3 * k] * sel[0] + v[3 * k + 1] * sel[1]) + v[3 * k + 2] * sel[2]);
+  }
+};
 
 // Entering face, its barycentrics (ue1, ue2), the leaving face's first
-// barycentric ul1 and tEnter.  Same branch structure as RayTetraPluecker;
-// only the entering point is needed for tEnter (ComputeParametricDist).
-__device__ bool ray_tet(D3 orig, D3 dir, const D3 V[4], int &ef, double &ue1,
-                        double &ue2, double &ul1, double &te) {
-  double uAB, uAC, uDB = 0, uDC = 0, uBC = 0, uAD = 0;
-  int sAB, sAC, sDB = -2, sDC = -2, sBC = -2, sAD = -2;
-  double eu1 = 0, eu2 = 0, lu1 = 0;
-  D3 ep = {0, 0, 0};
-  int enterF = -1;
-  const D3 dest = dadd(orig, dir);
-  const Plk ray = plk(orig, dest);
-  int next = 0;
-#define ENTER(F, A1, A2, P0, P1, P2) \
-  do { enterF = F; eu1 = A1; eu2 = A2; ep = bary(eu1, eu2, P0, P1, P2); } while (0)
-#define LEAVE(F, A1, A2) \
-  do { lu1 = A1; (void)(A2); } while (0)
-#define DONE() \
-  do { te = param_enter(orig, dir, ep); ef = enterF; ue1 = eu1; ue2 = eu2; ul1 = lu1; return true; } while (0)
-
-  uAB = pdot(ray, plk(V[0], V[1])); sAB = dsign(uAB);
-  uAC = pdot(ray, plk(V[0], V[2])); sAC = dsign(uAC);
+// barycentric ul1 and tEnter, as RayTetraPluecker decides them
+// (render/render_accel_tetra.cc:243-567), written without divergent
+// arithmetic: all six edge products are formed up front (the reference forms
+// those its branches reach; each is the same value whenever formed), the
+// branch structure runs on their signs alone to pick the entering and
+// leaving faces, and then each face's barycentrics come from its own
+// expression -- face f: inv = 1 / ((P + Q) - R), (a1, a2) = (X * inv, Y * inv):
+//   f = 3: P, Q, R = uAB, uBC, uAC   X, Y = -uAC,  uAB   points (A, B, C)
+//   f = 2:           uAD, uDB, uAB         uDB, -uAB          (B, A, D)
+//   f = 1:           uAC, -uDC, uAD        uAC, -uDC          (C, D, A)
+//   f = 0:           uDC, -uBC, uDB       -uDB,  uDC          (D, C, B)
+// Only the entering point's coordinate on the ray's first nonzero axis is
+// formed, (pe - o) * (1 / d) there as ComputeParametricDist does, the point
+// being the reference's ((1 - a - b) * P0 + a * P1) + b * P2.
+__device__ __forceinline__ bool ray_tet(const TetRay &R, const TetV &V, int &ef, double &ue1,
+                                        double &ue2, double &ul1, double &te) {
+  const Plk &ray = R.ray;
+  const double uAB = pdot(ray, plk(V[0], V[1])), uAC = pdot(ray, plk(V[0], V[2]));
+  const double uAD = pdot(ray, plk(V[0], V[3])), uBC = pdot(ray, plk(V[1], V[2]));
+  const double uDB = pdot(ray, plk(V[3], V[1])), uDC = pdot(ray, plk(V[3], V[2]));
+  const int sAB = dsign(uAB), sAC = dsign(uAC), sAD = dsign(uAD), sBC = dsign(uBC),
+            sDB = dsign(uDB), sDC = dsign(uDC);
+  int enter = -1, leave = -1;
   if ((sAC == -sAB) || (sAC == 0) || (sAB == 0)) {
-    uBC = pdot(ray, plk(V[1], V[2])); sBC = dsign(uBC);
     int sABC = sAB;
     if (sABC == 0) { sABC = -sAC; if (sABC == 0) sABC = sBC; }
     if ((sABC != 0) && ((sBC == sABC) || (sBC == 0))) {
-      double inv = 1.0 / (uAB + uBC - uAC);
-      if (sABC == 1) { ENTER(3, -uAC * inv, uAB * inv, V[0], V[1], V[2]); next = -1; }
-      else { LEAVE(3, -uAC * inv, uAB * inv); next = 1; }
-      uAD = pdot(ray, plk(V[0], V[3])); sAD = dsign(uAD);
-      if ((sAD == next) || (sAD == 0)) {
-        uDB = pdot(ray, plk(V[3], V[1])); sDB = dsign(uDB);
-        if ((sDB == next) || ((sDB == 0) && ((sAD != 0) || (sAB != 0)))) {
-          double iv = 1.0 / (uAD + uDB - uAB);
-          if (next == 1) ENTER(2, uDB * iv, -uAB * iv, V[1], V[0], V[3]);
-          else LEAVE(2, uDB * iv, -uAB * iv);
-          DONE();
-        }
-      }
-      uDC = pdot(ray, plk(V[3], V[2])); sDC = dsign(uDC);
-      if ((sDC == -next) || ((sDC == 0) && ((sAD != 0) || (sAC != 0)))) {
-        double iv = 1.0 / (uAC - uDC - uAD);
-        if (next == 1) ENTER(1, uAC * iv, -uDC * iv, V[2], V[3], V[0]);
-        else LEAVE(1, uAC * iv, -uDC * iv);
-        DONE();
-      } else {
-        if (sDB == -2) uDB = pdot(ray, plk(V[3], V[1]));
-        double iv = 1.0 / (uDC - uBC - uDB);
-        if (next == 1) ENTER(0, -uDB * iv, uDC * iv, V[3], V[2], V[1]);
-        else LEAVE(0, -uDB * iv, uDC * iv);
-        DONE();
-      }
+      const int next = sABC == 1 ? -1 : 1;
+      int f2;
+      if (((sAD == next) || (sAD == 0)) &&
+          ((sDB == next) || ((sDB == 0) && ((sAD != 0) || (sAB != 0)))))
+        f2 = 2;
+      else if ((sDC == -next) || ((sDC == 0) && ((sAD != 0) || (sAC != 0))))
+        f2 = 1;
+      else
+        f2 = 0;
+      enter = next == 1 ? f2 : 3;
+      leave = next == 1 ? 3 : f2;
     }
   }
-  uAD = pdot(ray, plk(V[0], V[3])); sAD = dsign(uAD);
-  if ((sAD == -sAB) || (sAB == 0) || (sAD == 0)) {
-    uDB = pdot(ray, plk(V[3], V[1])); sDB = dsign(uDB);
+  if (enter < 0 && ((sAD == -sAB) || (sAB == 0) || (sAD == 0))) {
     int sBAD = -sAB;
     if (sBAD == 0) { sBAD = sAD; if (sBAD == 0) sBAD = sDB; }
     if ((sBAD != 0) && ((sDB == sBAD) || (sDB == 0))) {
-      double inv = 1.0 / (uAD + uDB - uAB);
-      if (sBAD == 1) { ENTER(2, uDB * inv, -uAB * inv, V[1], V[0], V[3]); next = -1; }
-      else { LEAVE(2, uDB * inv, -uAB * inv); next = 1; }
-      uDC = pdot(ray, plk(V[3], V[2])); sDC = dsign(uDC);
-      if ((sDC == -next) || ((sDC == 0) && ((sAD != 0) || (sAC != 0)))) {
-        double iv = 1.0 / (uAC - uDC - uAD);
-        if (next == 1) ENTER(1, uAC * iv, -uDC * iv, V[2], V[3], V[0]);
-        else LEAVE(1, uAC * iv, -uDC * iv);
-        DONE();
-      } else {
-        if (sBC == -2) uBC = pdot(ray, plk(V[1], V[2]));
-        double iv = 1.0 / (uDC - uBC - uDB);
-        if (next == 1) ENTER(0, -uDB * iv, uDC * iv, V[3], V[2], V[1]);
-        else LEAVE(0, -uDB * iv, uDC * iv);
-        DONE();
-      }
+      const int next = sBAD == 1 ? -1 : 1;
+      const int f2 = ((sDC == -next) || ((sDC == 0) && ((sAD != 0) || (sAC != 0)))) ? 1 : 0;
+      enter = next == 1 ? f2 : 2;
+      leave = next == 1 ? 2 : f2;
     }
   }
-  if ((-sAD == sAC) || (sAC == 0) || (sAD == 0)) {
-    uDC = pdot(ray, plk(V[3], V[2])); sDC = dsign(uDC);
+  if (enter < 0 && ((-sAD == sAC) || (sAC == 0) || (sAD == 0))) {
     int sCDA = sAC;
     if (sCDA == 0) { sCDA = -sAD; if (sCDA == 0) sCDA = -sDC; }
     if ((sCDA != 0) && ((-sDC == sCDA) || (sDC == 0))) {
-      double ivCDA = 1.0 / (uAC - uDC - uAD);
-      if (sBC == -2) uBC = pdot(ray, plk(V[1], V[2]));
-      if (sDB == -2) uDB = pdot(ray, plk(V[3], V[1]));
-      double ivDCB = 1.0 / (uDC - uBC - uDB);
-      if (sCDA == 1) {
-        ENTER(1, uAC * ivCDA, -uDC * ivCDA, V[2], V[3], V[0]);
-        LEAVE(0, -uDB * ivDCB, uDC * ivDCB);
-      } else {
-        LEAVE(1, uAC * ivCDA, -uDC * ivCDA);
-        ENTER(0, -uDB * ivDCB, uDC * ivDCB, V[3], V[2], V[1]);
-      }
-      DONE();
+      enter = sCDA == 1 ? 1 : 0;
+      leave = sCDA == 1 ? 0 : 1;
     }
   }
-#undef ENTER
-#undef LEAVE
-#undef DONE
-  return false;
+  if (enter < 0) return false;
+  // face terms, selected by face id
+  auto P = [&](int f) { return f == 3 ? uAB : f == 2 ? uAD : f == 1 ? uAC : uDC; };
+  auto Q = [&](int f) { return f == 3 ? uBC : f == 2 ? uDB : f == 1 ? -uDC : -uBC; };
+  auto Rr = [&](int f) { return f == 3 ? uAC : f == 2 ? uAB : f == 1 ? uAD : uDB; };
+  auto X = [&](int f) { return f == 3 ? -uAC : f == 2 ? uDB : f == 1 ? uAC : -uDB; };
+  auto Y = [&](int f) { return f == 3 ? uAB : f == 2 ? -uAB : f == 1 ? -uDC : uDC; };
+  const double inv_e = 1.0 / ((P(enter) + Q(enter)) - Rr(enter));
+  const double inv_l = 1.0 / ((P(leave) + Q(leave)) - Rr(leave));
+  const double a = X(enter) * inv_e, b = Y(enter) * inv_e;
+  // entering point's vertices (3 - f, f ^ 2, f ^ 1), coordinates on the axis
+  const double c0 = V.axis(0, R.sel), c1 = V.axis(1, R.sel), c2 = V.axis(2, R.sel),
+               c3 = V.axis(3, R.sel);
+  auto C = [&](int k) { return k == 0 ? c0 : k == 1 ? c1 : k == 2 ? c2 : c3; };
+  const double p0 = C(3 - enter), p1 = C(enter ^ 2), p2 = C(enter ^ 1);
+  const double epa = (p0 * (1 - a - b) + p1 * a) + p2 * b;
+  te = (epa - R.oa) * R.iva;
+  ef = enter;
+  ue1 = a;
+  ue2 = b;
+  ul1 = X(leave) * inv_l;
+  return true;
 }
 
 // --------------------------------------------------------------- sphere
@@ -397,30 +397,53 @@ struct Ctx2 {
   float keps;
 };
 
+// One primitive of a two-child kind as loaded from the primitive cache
+// (a triangle's three corners with its id, or a sphere and its id), so that
+// a leaf walk can load the next primitive while it tests this one.
+template <int KIND>
+struct Prim2 {
+  float4 q0, q1, q2;
+  uint32_t f;
+  __device__ __forceinline__ void load(const float4 *__restrict__ prims,
+                                       const uint32_t *__restrict__ sidx, uint32_t j) {
+    if (KIND == SRT_TRIANGLES) {
+      q0 = __ldg(&prims[3 * (size_t)j]);
+      q1 = __ldg(&prims[3 * (size_t)j + 1]);
+      q2 = __ldg(&prims[3 * (size_t)j + 2]);
+      f = __float_as_uint(q0.w);
+    } else {
+      q0 = __ldg(&prims[j]);
+      f = __ldg(&sidx[j]);
+    }
+  }
+  // Hit distance below tio (t, u, v), false on a miss.
+  __device__ __forceinline__ bool test(const Ctx2 &c, float tio, float &t, float &u,
+                                       float &v) const {
+    if (KIND == SRT_TRIANGLES) {
+      if (f == c.prev_prim) return false;
+      const float p0[3] = {q0.x, q0.y, q0.z}, p1[3] = {q1.x, q1.y, q1.z},
+                  p2[3] = {q2.x, q2.y, q2.z};
+      t = tio;
+      return tri_isect(t, u, v, p0, p1, p2, c.r, c.keps);
+    } else {
+      const float c3[3] = {q0.x, q0.y, q0.z};
+      t = tio;
+      u = v = 0.0f;
+      return sphere_isect(t, c3, q0.w, c.r, c.prev_t, c.pn, c.prev_prim == f);
+    }
+  }
+};
+
 // Hit distance of sorted primitive j (two-child kinds), FLT_MAX on a miss.
 template <int KIND>
 __device__ __forceinline__ bool cand2(const float4 *__restrict__ prims,
                                       const uint32_t *__restrict__ sidx, uint32_t j,
                                       const Ctx2 &c, float tio, float &t, float &u, float &v,
                                       uint32_t &f) {
-  if (KIND == SRT_TRIANGLES) {
-    const float4 q0 = __ldg(&prims[3 * (size_t)j]);
-    f = __float_as_uint(q0.w);
-    if (f == c.prev_prim) return false;
-    const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
-    const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
-    const float p0[3] = {q0.x, q0.y, q0.z}, p1[3] = {q1.x, q1.y, q1.z},
-                p2[3] = {q2.x, q2.y, q2.z};
-    t = tio;
-    return tri_isect(t, u, v, p0, p1, p2, c.r, c.keps);
-  } else {
-    const float4 s = __ldg(&prims[j]);
-    f = __ldg(&sidx[j]);
-    const float c3[3] = {s.x, s.y, s.z};
-    t = tio;
-    u = v = 0.0f;
-    return sphere_isect(t, c3, s.w, c.r, c.prev_t, c.pn, c.prev_prim == f);
-  }
+  Prim2<KIND> P;
+  P.load(prims, sidx, j);
+  f = P.f;
+  return P.test(c, tio, t, u, v);
 }
 
 // The reference's Traverse, step for step (render/render_accel_triangle.cc:2511,
@@ -628,33 +651,91 @@ __device__ __forceinline__ Ctx2 make_ctx2(const srt_ray *__restrict__ rays, size
   return c;
 }
 
+// Stacks of the front-to-back walks, entries (child entry, box entry
+// distance).  LocalStack: a per-thread array.  SharedStack: the first
+// kShDepth entries of each thread in shared memory, entry k of thread t at
+// [k][t] so that the lanes of a warp fall on 32 different banks whatever
+// their depths, deeper entries in a per-thread array (a front-to-back walk
+// holds at most one entry per tree level; the trees of the scenes here are
+// 19 to 21 levels deep, so the array is seldom touched).
+constexpr int kShDepth = 16;
+
+template <int D>
+struct LocalStackN {
+  static constexpr int kDepth = D;
+  uint2 e[D];
+  float t[D];
+  __device__ __forceinline__ void put(int k, uint2 v, float d) {
+    e[k] = v;
+    t[k] = d;
+  }
+  __device__ __forceinline__ uint2 get(int k, float &d) const {
+    d = t[k];
+    return e[k];
+  }
+};
+
+using LocalStack = LocalStackN<kStack>;
+
+template <int NT>
+struct SharedStack {
+  static constexpr int kDepth = kStack;
+  uint2 (*se)[NT];
+  float (*st)[NT];
+  uint2 e[kStack - kShDepth];
+  float t[kStack - kShDepth];
+  __device__ __forceinline__ SharedStack(uint2 (*se_)[NT], float (*st_)[NT])
+      : se(se_), st(st_) {}
+  __device__ __forceinline__ void put(int k, uint2 v, float d) {
+    if (k < kShDepth) {
+      se[k][threadIdx.x] = v;
+      st[k][threadIdx.x] = d;
+    } else {
+      e[k - kShDepth] = v;
+      t[k - kShDepth] = d;
+    }
+  }
+  __device__ __forceinline__ uint2 get(int k, float &d) const {
+    if (k < kShDepth) {
+      d = st[k][threadIdx.x];
+      return se[k][threadIdx.x];
+    }
+    d = t[k - kShDepth];
+    return e[k - kShDepth];
+  }
+};
+
+// Shared-memory columns of a block of NT threads' stacks.
+#define SRT_SHARED_STACK(NAME, NT)                         \
+  __shared__ uint2 NAME##_e[kShDepth][NT];                 \
+  __shared__ float NAME##_t[kShDepth][NT];                 \
+  SharedStack<NT> NAME(NAME##_e, NAME##_t)
+
 // Pass 1 of the default walk for the two-child kinds: front to back from
 // `root`; returns m (smallest hit distance), how many primitives hit at m,
 // the one found first (in b), and whether one of those at m was reported
 // before its own leaf box's entry.
-template <int KIND>
+template <int KIND, class Stk = LocalStack>
 __device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
                                             const float4 *__restrict__ prims,
                                             const uint32_t *__restrict__ sidx,
                                             const Ctx2 &c, uint32_t root, Best &b, Work &w,
                                             uint32_t max_iter, float &m_out,
-                                            uint32_t &at_m_out, bool &viol_out) {
+                                            uint32_t &at_m_out, bool &viol_out,
+                                            Stk &&stk = Stk()) {
   float m = FLT_MAX, m2 = FLT_MAX;  // smallest and second smallest distance
   float e_best = 0.0f;              // leaf box entry of the candidate at m
   uint32_t at_m = 0;
   bool viol = false;
-  uint2 stk[kStack];
-  float stt[kStack];
   int sp = 0;
-  stk[0] = make_uint2(root, 0u);
-  stt[0] = -FLT_MAX;
+  stk.put(0, make_uint2(root, 0u), -FLT_MAX);
   while (true) {
     uint2 leaf = make_uint2(0u, 0u);
     float lt = 0.0f;
     while (sp >= 0) {
       if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
-      const uint2 e = stk[sp];
-      const float et = stt[sp];
+      float et;
+      const uint2 e = stk.get(sp, et);
       sp--;
       const float bnd = bound_rel(m, kRelTri);
       if (et > bnd) continue;
@@ -668,31 +749,35 @@ __device__ __forceinline__ void pass1_node2(const Node2 *__restrict__ nodes,
       const bool h1 = ray_aabb_t<true>(bnd, bb.z, bb.w, cc.x, cc.y, cc.z, cc.w, c.r, t1);
       const uint2 e0 = make_uint2(d.x, d.z & kCountMask),
                   e1 = make_uint2(d.y, d.w & kCountMask);
-      if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
+      if (sp + 2 >= std::remove_reference_t<Stk>::kDepth) { w.fail = true; sp = -1; break; }
       if (h0 && h1) {
         const bool first1 = t1 < t0;
-        stk[++sp] = first1 ? e0 : e1; stt[sp] = first1 ? t0 : t1;
-        stk[++sp] = first1 ? e1 : e0; stt[sp] = first1 ? t1 : t0;
+        stk.put(++sp, first1 ? e0 : e1, first1 ? t0 : t1);
+        stk.put(++sp, first1 ? e1 : e0, first1 ? t1 : t0);
       } else if (h0) {
-        stk[++sp] = e0; stt[sp] = t0;
+        stk.put(++sp, e0, t0);
       } else if (h1) {
-        stk[++sp] = e1; stt[sp] = t1;
+        stk.put(++sp, e1, t1);
       }
     }
     if (leaf.y == 0) break;
     w.leaf++;
     w.prim += leaf.y;
+    // primitive j + 1 is loaded while j is tested
+    Prim2<KIND> nx;
+    nx.load(prims, sidx, leaf.x);
     for (uint32_t j = leaf.x; j < leaf.x + leaf.y; j++) {
+      const Prim2<KIND> P = nx;
+      if (j + 1 < leaf.x + leaf.y) nx.load(prims, sidx, j + 1);
       float t, u, v;
-      uint32_t f;
-      if (!cand2<KIND>(prims, sidx, j, c, FLT_MAX, t, u, v, f)) continue;
+      if (!P.test(c, FLT_MAX, t, u, v)) continue;
       if (t < m) {
         m2 = m;
         m = t;
         at_m = 1;
         viol = below_entry(t, lt);
         e_best = lt;
-        b.t = t; b.u = u; b.v = v; b.prim = f; b.j = j;
+        b.t = t; b.u = u; b.v = v; b.prim = P.f; b.j = j;
       } else {
         if (t < m2) m2 = t;
         if (t == m) {
@@ -805,7 +890,7 @@ resolve_node2_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__
 // ---- tetrahedra (own-box nodes, FP64 entry distance)
 struct CtxT {
   RayF r;
-  D3 o, d;
+  TetRay tr;
   uint32_t prev_prim;
 };
 
@@ -818,9 +903,8 @@ __device__ __forceinline__ bool candT(const float4 *__restrict__ prims,
   const float4 q0 = __ldg(&prims[3 * (size_t)j]);
   const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
   const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
-  const D3 V[4] = {{q0.x, q0.y, q0.z}, {q0.w, q1.x, q1.y}, {q1.z, q1.w, q2.x},
-                   {q2.y, q2.z, q2.w}};
-  return ray_tet(c.o, c.d, V, ef, e1, e2, ul1, te) && te >= 0.0;
+  const TetV V = {{q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
+  return ray_tet(c.tr, V, ef, e1, e2, ul1, te) && te >= 0.0;
 }
 
 __device__ __forceinline__ void take_tet(Best &b, double te, double e1, double e2,
@@ -915,10 +999,10 @@ __device__ __forceinline__ void store_tet(size_t i, const Best &b,
     if (any && faces && vscalar) {
       // entering face vertex order (A, B, C) per face id, as the Pluecker
       // test forms its barycentric point
-      const int fA[4] = {3, 2, 1, 0}, fB[4] = {2, 3, 0, 1}, fC[4] = {1, 0, 3, 2};
+      // (A, B, C) = (3 - f, f ^ 2, f ^ 1): faces 0..3 -> (3,2,1), (2,3,0), (1,0,3), (0,1,2)
       const uint32_t *tv = faces + 4 * (size_t)b.prim;
-      const double sa = vscalar[tv[fA[b.sub]]], sb = vscalar[tv[fB[b.sub]]],
-                   sc = vscalar[tv[fC[b.sub]]];
+      const double sa = vscalar[tv[3 - b.sub]], sb = vscalar[tv[b.sub ^ 2u]],
+                   sc = vscalar[tv[b.sub ^ 1u]];
       s = (float)((1.0 - b.e1 - b.e2) * sa + b.e1 * sb + b.e2 * sc);
     }
     scalar_out[i] = s;
@@ -929,77 +1013,36 @@ __device__ __forceinline__ CtxT make_ctxT(const srt_ray *__restrict__ rays, size
   CtxT c;
   float prev_t;
   c.r = load_ray(rays, i, c.prev_prim, prev_t);
-  c.o = {c.r.o[0], c.r.o[1], c.r.o[2]};
-  c.d = {c.r.d[0], c.r.d[1], c.r.d[2]};
+  c.tr = tet_ray({c.r.o[0], c.r.o[1], c.r.o[2]}, {c.r.d[0], c.r.d[1], c.r.d[2]});
   return c;
 }
 
-// Pass 1 of the default tetrahedron walk: front to back; nwin counts entry
-// distances within 8 float steps of the running minimum m (the list is kept
-// to recount when m drops).  defer: the ray needs the reference-order walk,
-// over the whole tree (full: a candidate in that window reported before its
-// own leaf box's entry) or through the window at m (several candidates near
-// m).
-__device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
-                                          const float4 *__restrict__ prims,
-                                          const uint32_t *__restrict__ sidx, const CtxT &c,
-                                          Best &b, Work &w, uint32_t max_iter, double &m_out,
-                                          bool &defer_out, bool &full_out) {
-  double m = DBL_MAX, m2 = DBL_MAX;  // smallest and second smallest distance
-  float e_best = 0.0f;               // leaf box entry of the candidate at m
-  double wl[4];
-  uint32_t wviol = 0;  // bit k: wl[k] lies below its own leaf box's entry
-  int nwin = 0;
+// Per-ray state of a tetrahedron first pass: the smallest and second
+// smallest hit distances m, m2 and the window of up to four entry distances
+// within 8 float steps of m (kept to recount when m drops), each rounded up
+// to float -- exact for the comparisons against the float window bound.
+// defer: the ray needs the reference-order walk, over the whole tree (full:
+// a candidate in that window reported before its own leaf box's entry) or
+// through the window at m (several candidates near m).  The outcome does not
+// depend on the order the leaves are visited in: every tetrahedron whose leaf
+// box is entered below the final pruning bound is tested in any order.
+struct TetPass1 {
+  double m = DBL_MAX, m2 = DBL_MAX;
+  float e_best = 0.0f;  // leaf box entry of the candidate at m
+  float wl[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  uint32_t wset = 0;   // bit k: window slot k holds an entry
+  uint32_t wviol = 0;  // bit k: slot k's entry lies below its own leaf box's entry
   bool overflow = false, viol_lost = false;
-  uint32_t stk[kStack];
-  float stt[kStack];
-  int sp = -1;
-  {
-    const float4 *np = reinterpret_cast<const float4 *>(nodes);
-    const float4 a = __ldg(np), bb = __ldg(np + 1);
-    float t0;
-    if (ray_aabb_t<false>(FLT_MAX, a.x, a.y, a.z, bb.x, bb.y, bb.z, c.r, t0)) {
-      stk[0] = 0u;
-      stt[0] = t0;
-      sp = 0;
-    }
+
+  __device__ __forceinline__ float bound() const {
+    return (m < DBL_MAX) ? bound_rel((float)m, kRelTet) : FLT_MAX;
   }
-  while (true) {
-    uint32_t lref = 0, lcnt = 0;
-    float lt = 0.0f;
-    while (sp >= 0) {
-      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
-      const uint32_t ni = stk[sp];
-      const float et = stt[sp];
-      sp--;
-      const float bnd = (m < DBL_MAX) ? bound_rel((float)m, kRelTet) : FLT_MAX;
-      if (et > bnd) continue;
-      const float4 *np = reinterpret_cast<const float4 *>(nodes + ni);
-      const uint32_t meta = __float_as_uint(__ldg(&np[0].w));
-      const uint32_t ref = __float_as_uint(__ldg(&np[1].w));
-      if (meta & kLeafBit) { lref = ref; lcnt = meta & kCountMask; lt = et; break; }
-      w.branch++;
-      // the two children are adjacent: test their own boxes here
-      const float4 *cp = reinterpret_cast<const float4 *>(nodes + ref);
-      const float4 a0 = __ldg(cp), b0 = __ldg(cp + 1), a1 = __ldg(cp + 2), b1 = __ldg(cp + 3);
-      float t0, t1;
-      const bool h0 = ray_aabb_t<false>(bnd, a0.x, a0.y, a0.z, b0.x, b0.y, b0.z, c.r, t0);
-      const bool h1 = ray_aabb_t<false>(bnd, a1.x, a1.y, a1.z, b1.x, b1.y, b1.z, c.r, t1);
-      if (sp + 2 >= kStack) { w.fail = true; sp = -1; break; }
-      if (h0 && h1) {
-        const bool first1 = t1 < t0;
-        stk[++sp] = first1 ? ref : ref + 1; stt[sp] = first1 ? t0 : t1;
-        stk[++sp] = first1 ? ref + 1 : ref; stt[sp] = first1 ? t1 : t0;
-      } else if (h0) {
-        stk[++sp] = ref; stt[sp] = t0;
-      } else if (h1) {
-        stk[++sp] = ref + 1; stt[sp] = t1;
-      }
-    }
-    if (lcnt == 0) break;
-    w.leaf++;
-    w.prim += lcnt;
-    for (uint32_t j = lref; j < lref + lcnt; j++) {
+
+  // Tests the `cnt` tetrahedra of a leaf at sorted slot `ref`, entered at lt.
+  __device__ __forceinline__ void leaf(const float4 *__restrict__ prims,
+                                       const uint32_t *__restrict__ sidx, const CtxT &c,
+                                       uint32_t ref, uint32_t cnt, float lt, Best &b) {
+    for (uint32_t j = ref; j < ref + cnt; j++) {
       uint32_t f;
       int ef;
       double e1, e2, ul1, te;
@@ -1010,23 +1053,23 @@ __device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
         m = te;
         e_best = lt;
         take_tet(b, te, e1, e2, ul1, f, ef);
-        const double whi = window_hi(m);
-        int k2 = 0;
-        uint32_t v2 = 0;
-        for (int k = 0; k < nwin; k++)
-          if (wl[k] <= whi) {
-            v2 |= ((wviol >> k) & 1u) << k2;
-            wl[k2++] = wl[k];
-          }
-        nwin = k2;
-        wviol = v2;
+        const float whi = (float)window_hi(m);
+#pragma unroll
+        for (int k = 0; k < 4; k++)
+          if (!(wl[k] <= whi)) wset &= ~(1u << k);
+        wviol &= wset;
       } else if (te < m2) {
         m2 = te;
       }
       if (te <= window_hi(m)) {
-        if (nwin < 4) {
-          wviol |= (below ? 1u : 0u) << nwin;
-          wl[nwin++] = te;
+        if (wset != 0xfu) {
+          const int k = __ffs(~wset) - 1;  // first free slot
+          const float r = __double2float_ru(te);
+#pragma unroll
+          for (int q = 0; q < 4; q++)
+            if (q == k) wl[q] = r;
+          wset |= 1u << k;
+          wviol |= (below ? 1u : 0u) << k;
         } else {
           overflow = true;
           viol_lost = viol_lost || below;
@@ -1034,14 +1077,84 @@ __device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
       }
     }
   }
-  bool viol = viol_lost || wviol != 0;
-  // a single candidate below its box's entry e is hidden only by another
-  // primitive nearer than e (all tested: e lies below the pruning bound)
-  if (viol && nwin == 1 && !overflow)
-    viol = !(m2 >= (double)e_best) || !(e_best < bound_rel((float)m, kRelTet));
-  m_out = m;
-  defer_out = viol || nwin > 1 || overflow;
-  full_out = viol;
+
+  __device__ __forceinline__ void finish(double &m_out, bool &defer_out,
+                                         bool &full_out) const {
+    const int nwin = __popc(wset);
+    bool viol = viol_lost || wviol != 0;
+    // a single candidate below its box's entry e is hidden only by another
+    // primitive nearer than e (all tested: e lies below the pruning bound)
+    if (viol && nwin == 1 && !overflow)
+      viol = !(m2 >= (double)e_best) || !(e_best < bound_rel((float)m, kRelTet));
+    m_out = m;
+    defer_out = viol || nwin > 1 || overflow;
+    full_out = viol;
+  }
+};
+
+// A child's stack entry, read with its box at the parent: (ref, leaf count),
+// count 0 for a branch (whose children sit at ref, ref + 1).
+__device__ __forceinline__ uint2 tet_entry(float4 lo, float4 hi) {
+  const uint32_t meta = __float_as_uint(lo.w);
+  return make_uint2(__float_as_uint(hi.w), (meta & kLeafBit) ? meta & kCountMask : 0u);
+}
+
+// Pass 1 of the default tetrahedron walk for one ray: front to back, stack
+// entries from tet_entry so that a popped branch loads only its children's
+// boxes.
+template <class Stk = LocalStack>
+__device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
+                                          const float4 *__restrict__ prims,
+                                          const uint32_t *__restrict__ sidx, const CtxT &c,
+                                          Best &b, Work &w, uint32_t max_iter, double &m_out,
+                                          bool &defer_out, bool &full_out, Stk &&stk = Stk()) {
+  TetPass1 P;
+  int sp = -1;
+  {
+    const float4 *np = reinterpret_cast<const float4 *>(nodes);
+    const float4 a = __ldg(np), bb = __ldg(np + 1);
+    float t0;
+    if (ray_aabb_t<false>(FLT_MAX, a.x, a.y, a.z, bb.x, bb.y, bb.z, c.r, t0)) {
+      stk.put(0, tet_entry(a, bb), t0);
+      sp = 0;
+    }
+  }
+  while (true) {
+    uint2 leaf = make_uint2(0u, 0u);
+    float lt = 0.0f;
+    while (sp >= 0) {
+      if (++w.it > max_iter) { w.fail = true; sp = -1; break; }
+      float et;
+      const uint2 e = stk.get(sp, et);
+      sp--;
+      const float bnd = P.bound();
+      if (et > bnd) continue;
+      if (e.y != 0) { leaf = e; lt = et; break; }
+      w.branch++;
+      // the two children are adjacent: test their own boxes here
+      const float4 *cp = reinterpret_cast<const float4 *>(nodes + e.x);
+      const float4 a0 = __ldg(cp), b0 = __ldg(cp + 1), a1 = __ldg(cp + 2), b1 = __ldg(cp + 3);
+      float t0, t1;
+      const bool h0 = ray_aabb_t<false>(bnd, a0.x, a0.y, a0.z, b0.x, b0.y, b0.z, c.r, t0);
+      const bool h1 = ray_aabb_t<false>(bnd, a1.x, a1.y, a1.z, b1.x, b1.y, b1.z, c.r, t1);
+      const uint2 e0 = tet_entry(a0, b0), e1 = tet_entry(a1, b1);
+      if (sp + 2 >= std::remove_reference_t<Stk>::kDepth) { w.fail = true; sp = -1; break; }
+      if (h0 && h1) {
+        const bool first1 = t1 < t0;
+        stk.put(++sp, first1 ? e0 : e1, first1 ? t0 : t1);
+        stk.put(++sp, first1 ? e1 : e0, first1 ? t1 : t0);
+      } else if (h0) {
+        stk.put(++sp, e0, t0);
+      } else if (h1) {
+        stk.put(++sp, e1, t1);
+      }
+    }
+    if (leaf.y == 0) break;
+    w.leaf++;
+    w.prim += leaf.y;
+    P.leaf(prims, sidx, c, leaf.x, leaf.y, lt, b);
+  }
+  P.finish(m_out, defer_out, full_out);
 }
 
 template <bool SINGLE>
@@ -1054,6 +1167,7 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
                  Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
                  uint32_t max_iter, uint32_t *__restrict__ err,
                  const uint32_t *__restrict__ order, uint32_t *__restrict__ next = nullptr) {
+  SRT_SHARED_STACK(sstk, 128);
   for_each_ray(n, next, [&](size_t k) {
     const size_t i = order ? (size_t)__ldg(&order[k]) : k;  // ray of this thread
     const CtxT c = make_ctxT(rays, i);
@@ -1064,7 +1178,7 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
     } else {
       double m;
       bool defer, full;
-      pass1_tet(nodes, prims, sidx, c, b, w, max_iter, m, defer, full);
+      pass1_tet(nodes, prims, sidx, c, b, w, max_iter, m, defer, full, sstk);
       if (!w.fail && defer) {
         const uint32_t q = atomicAdd(dcount, 1u);
         dlist[q] = Deferred{(uint32_t)i, full ? 1u : 0u, m};
@@ -1110,7 +1224,10 @@ resolve_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ p
 // All rays of many triangle scenes in one persistent launch: each warp
 // takes the next 32 * R rays from a global counter (scenes of very
 // different cost balance across the GPU), finds the ray's scene from the
-// ray offsets and walks that scene's tree from its root.
+// ray offsets and walks that scene's tree from its root, with a stack of
+// DEPTH entries (a walk that would need more stops with the limit error).
+// order (or NULL): the rays in a coherent order, grouped by scene.
+template <int DEPTH>
 __global__ void __launch_bounds__(256)
 trace_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ prims,
                    const srt_ray *__restrict__ rays, srt_hit *__restrict__ hits,
@@ -1118,7 +1235,8 @@ trace_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
                    const uint32_t *__restrict__ roff, int nseg, uint32_t total,
                    uint32_t *__restrict__ work, int R, unsigned long long *__restrict__ stats,
                    Deferred *__restrict__ dlist, uint32_t *__restrict__ dcount,
-                   uint32_t max_iter, uint32_t *__restrict__ err) {
+                   uint32_t max_iter, uint32_t *__restrict__ err,
+                   const uint32_t *__restrict__ order) {
   // each warp takes 32 * R rays at a time (no block-wide barrier: a warp
   // whose rays finish early takes more work at once)
   const uint32_t lane = threadIdx.x & 31u;
@@ -1128,8 +1246,9 @@ trace_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
     base = __shfl_sync(0xffffffffu, base, 0);
     if (base >= total) break;
     for (int r = 0; r < R; r++) {
-      const uint32_t i = base + (uint32_t)r * 32u + lane;
-      if (i >= total) break;
+      const uint32_t k = base + (uint32_t)r * 32u + lane;
+      if (k >= total) break;
+      const uint32_t i = order ? __ldg(&order[k]) : k;
       const int sg = seg_of(roff, nseg, i);
       Ctx2 c;
       c.r = load_ray(rays, i, c.prev_prim, c.prev_t);
@@ -1141,10 +1260,10 @@ trace_batch_kernel(const Node2 *__restrict__ nodes, const float4 *__restrict__ p
       uint32_t at_m;
       bool viol;
       pass1_node2<SRT_TRIANGLES>(nodes, prims, nullptr, c, __ldg(&roots[sg]), b, w, max_iter,
-                                 m, at_m, viol);
+                                 m, at_m, viol, LocalStackN<DEPTH>());
       if (!w.fail && (viol || at_m > 1)) {
-        const uint32_t k = atomicAdd(dcount, 1u);
-        dlist[k] = Deferred{i, viol ? 1u : 0u, (double)m};
+        const uint32_t q = atomicAdd(dcount, 1u);
+        dlist[q] = Deferred{i, viol ? 1u : 0u, (double)m};
       } else {
         if (w.fail) atomicOr(err, kErrIter);
         store_node2<SRT_TRIANGLES>(i, b, c, prims, hits, nullptr);
@@ -1301,7 +1420,8 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
 
 srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
                               srt_hit *hits, int block, int R,
-                              unsigned long long *stats) {
+                              unsigned long long *stats, int depth,
+                              const uint32_t *order) {
   const uint32_t total = (uint32_t)bt.nrays;
   if (total == 0) return SRT_OK;
   cudaStream_t st = ctx->stream;
@@ -1311,14 +1431,16 @@ srt_status launch_trace_batch(srt_ctx *ctx, BatchTree &bt, const srt_ray *rays,
   Deferred *dlist = reinterpret_cast<Deferred *>(ctx->s_defer.as<char>() + 256);
   if ((e = cudaMemsetAsync(dcount, 0, 8, st)) != cudaSuccess)
     return cuda_status(e, "batch counters");
+  const auto kern = depth <= 24 ? trace_batch_kernel<24>
+                    : depth <= 32 ? trace_batch_kernel<32> : trace_batch_kernel<48>;
   int per_sm = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, trace_batch_kernel, block, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, block, 0);
   if (per_sm < 1) per_sm = 1;
   const uint32_t max_iter = (uint32_t)std::min<size_t>(8 * bt.nprims + 64, 0xfffffff0u);
-  trace_batch_kernel<<<ctx->num_sms * per_sm, block, 0, st>>>(
+  kern<<<ctx->num_sms * per_sm, block, 0, st>>>(
       bt.nodes.as<Node2>(), bt.prims.as<float4>(), rays, hits, bt.scenes.as<SceneInfo>(),
       bt.roots.as<uint32_t>(), bt.roff.as<uint32_t>(), bt.nseg, total, dcount + 1, R, stats,
-      dlist, dcount, max_iter, ctx->d_err);
+      dlist, dcount, max_iter, ctx->d_err, order);
   resolve_batch_kernel<<<ctx->num_sms * 8, 128, 0, st>>>(
       bt.nodes.as<Node2>(), bt.prims.as<float4>(), rays, hits, bt.scenes.as<SceneInfo>(),
       bt.roots.as<uint32_t>(), bt.roff.as<uint32_t>(), bt.nseg, stats, dlist, dcount,
@@ -1511,8 +1633,7 @@ elem_ctx(const SceneWork &W, uint32_t i, uint32_t e_id, const SceneElem &e, cons
   if constexpr (KIND == SRT_TETRAHEDRA) {
     CtxT c;
     c.r = lr;
-    c.o = {lr.o[0], lr.o[1], lr.o[2]};
-    c.d = {lr.d[0], lr.d[1], lr.d[2]};
+    c.tr = tet_ray({lr.o[0], lr.o[1], lr.o[2]}, {lr.d[0], lr.d[1], lr.d[2]});
     c.prev_prim = same ? prev_prim : kNone;
     return c;
   } else {

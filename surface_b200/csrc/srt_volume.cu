@@ -105,28 +105,30 @@ __device__ __forceinline__ bool inside(const float p[3]) {
          p[2] < 1.0f;
 }
 
-// FilterTexture3DFloat, clamp-to-edge, one component.
+// FilterTexture3DFloat, clamp-to-edge, one component.  Voxel indices are
+// 32-bit: make_const rejects volumes of 2^31 voxels or more.
 __device__ __forceinline__ float fetch(const float *__restrict__ img, const int dim[3],
                                        float u, float v, float r, Cell *cell) {
   const float vox0 = u * (dim[0] - 1.0f);
   const float vox1 = v * (dim[1] - 1.0f);
   const float vox2 = r * (dim[2] - 1.0f);
-  int vx = min(max((int)vox0, 0), dim[0] - 1);
-  int vy = min(max((int)vox1, 0), dim[1] - 1);
-  int vz = min(max((int)vox2, 0), dim[2] - 1);
-  const int vx1 = min(vx + 1, dim[0] - 1), vy1 = min(vy + 1, dim[1] - 1),
-            vz1 = min(vz + 1, dim[2] - 1);
+  const int vx = min(max((int)vox0, 0), dim[0] - 1);
+  const int vy = min(max((int)vox1, 0), dim[1] - 1);
+  const int vz = min(max((int)vox2, 0), dim[2] - 1);
+  const int sy = dim[0], sz = dim[0] * dim[1];
+  const int ox = vx + 1 < dim[0] ? 1 : 0;
+  const int oy = vy + 1 < dim[1] ? sy : 0;
+  const int oz = vz + 1 < dim[2] ? sz : 0;
   const float dx = vox0 - vx, dy = vox1 - vy, dz = vox2 - vz;
-  const size_t sx = 1, sy = (size_t)dim[0], sz = (size_t)dim[0] * dim[1];
-  const size_t i000 = vz * sz + vy * sy + vx * sx;
-  const float D000 = __ldg(&img[i000]);
-  const float D100 = __ldg(&img[vz * sz + vy * sy + vx1]);
-  const float D010 = __ldg(&img[vz * sz + vy1 * sy + vx]);
-  const float D110 = __ldg(&img[vz * sz + vy1 * sy + vx1]);
-  const float D001 = __ldg(&img[vz1 * sz + vy * sy + vx]);
-  const float D101 = __ldg(&img[vz1 * sz + vy * sy + vx1]);
-  const float D011 = __ldg(&img[vz1 * sz + vy1 * sy + vx]);
-  const float D111 = __ldg(&img[vz1 * sz + vy1 * sy + vx1]);
+  const float *q = img + (vz * sz + vy * sy + vx);
+  const float D000 = __ldg(q);
+  const float D100 = __ldg(q + ox);
+  const float D010 = __ldg(q + oy);
+  const float D110 = __ldg(q + oy + ox);
+  const float D001 = __ldg(q + oz);
+  const float D101 = __ldg(q + oz + ox);
+  const float D011 = __ldg(q + oz + oy);
+  const float D111 = __ldg(q + oz + oy + ox);
   const float d00 = lerpf(dx, D000, D100);
   const float d10 = lerpf(dx, D010, D110);
   const float d01 = lerpf(dx, D001, D101);
@@ -210,38 +212,34 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
   if (trans) trans[pix] = T;
 }
 
-constexpr int kTfCopies = 8;  // copies of the block-local TF gradient
+constexpr int kTfCopies = 4;  // copies of the block-local TF gradient
 
-__device__ __forceinline__ void flush_entry(float *g, int i, float (&a)[4]) {
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    if (a[k] != 0.0f) atomicAdd(&g[4 * i + k], a[k]);
-    a[k] = 0.0f;
+// Transfer-function gradient of one table entry added to the block's
+// shared copy: the colour part is the ray's image gradient g (constant along
+// the ray) times the run's summed weight a.x, the opacity part a.y.
+__device__ __forceinline__ void flush_entry(float *g, int i, float2 &a, const float4 &gi) {
+  if (a.x != 0.0f) {
+    if (gi.x != 0.0f) atomicAdd(&g[4 * i], a.x * gi.x);
+    if (gi.y != 0.0f) atomicAdd(&g[4 * i + 1], a.x * gi.y);
+    if (gi.z != 0.0f) atomicAdd(&g[4 * i + 2], a.x * gi.z);
   }
-}
-
-__device__ __forceinline__ void flush_tf(float *g, int i0, int i1, float (&a0)[4],
-                                         float (&a1)[4]) {
-#pragma unroll
-  for (int k = 0; k < 4; k++) {
-    if (a0[k] != 0.0f) atomicAdd(&g[4 * i0 + k], a0[k]);
-    if (a1[k] != 0.0f) atomicAdd(&g[4 * i1 + k], a1[k]);
-    a0[k] = 0.0f;
-    a1[k] = 0.0f;
-  }
+  if (a.y != 0.0f) atomicAdd(&g[4 * i + 3], a.y);
+  a = make_float2(0.0f, 0.0f);
 }
 
 // Add the eight corner sums of one texel cell (lower corner vx, vy, vz;
 // upper corners clamped like the fetch) to the density gradient.
 __device__ __forceinline__ void flush_dens(float *__restrict__ g, const int dim[3], int vx,
                                            int vy, int vz, float (&a)[8]) {
-  const size_t sy = (size_t)dim[0], sz = (size_t)dim[0] * dim[1];
-  const int xs[2] = {vx, min(vx + 1, dim[0] - 1)};
-  const int ys[2] = {vy, min(vy + 1, dim[1] - 1)};
-  const int zs[2] = {vz, min(vz + 1, dim[2] - 1)};
+  const int sy = dim[0], sz = dim[0] * dim[1];
+  const int ox = vx + 1 < dim[0] ? 1 : 0;
+  const int oy = vy + 1 < dim[1] ? sy : 0;
+  const int oz = vz + 1 < dim[2] ? sz : 0;
+  float *q = g + (vz * sz + vy * sy + vx);
 #pragma unroll
   for (int k = 0; k < 8; k++) {
-    if (a[k] != 0.0f) atomicAdd(&g[zs[k >> 2] * sz + ys[(k >> 1) & 1] * sy + xs[k & 1]], a[k]);
+    const int off = ((k & 1) ? ox : 0) + ((k & 2) ? oy : 0) + ((k & 4) ? oz : 0);
+    if (a[k] != 0.0f) atomicAdd(q + off, a[k]);
     a[k] = 0.0f;
   }
 }
@@ -271,15 +269,19 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
       if (ns > K.p.max_steps) ns = K.p.max_steps;
       const float4 g = gimg[pix];
       const float Tfin = trans[pix];
+      const float gwT = g.w * Tfin;
       float Tn = Tfin;
-      float Cb0 = 0.f, Cb1 = 0.f, Cb2 = 0.f;
+      float gCb = 0.0f;  // g . (colour composited behind the sample)
       const float top = (float)(K.tfn - 1);
+      const float sstep = K.p.sigma_scale * K.p.step;
       // Run-length accumulators: consecutive samples often share the
       // transfer-function bin (always in empty space) and the voxel cell
       // (the step is half a voxel); contributions are summed in registers
-      // and flushed when the bin / cell changes.
+      // and flushed when the bin / cell changes.  A table entry's colour
+      // gradient is g times a scalar weight sum, so a run keeps per entry
+      // (colour weight, opacity gradient).
       int run_i0 = -1;
-      float ta0[4] = {0.f, 0.f, 0.f, 0.f}, ta1[4] = {0.f, 0.f, 0.f, 0.f};
+      float2 ta0 = make_float2(0.f, 0.f), ta1 = make_float2(0.f, 0.f);
       int run_cell = -1, rvx = 0, rvy = 0, rvz = 0;
       float da[8];
 #pragma unroll
@@ -297,17 +299,17 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         float f;
         bool inr;
         tf_lookup_ab(tf, K.tfn, rho, c, i0, i1, f, inr, ta, tb);
-        const float sig = K.p.sigma_scale * c.w;
-        const float e = expf(-sig * K.p.step);
+        const float e = expf(-(K.p.sigma_scale * c.w) * K.p.step);
         float al = 1.0f - e;
         const bool clamped = al > K.p.alpha_max;
         if (clamped) al = K.p.alpha_max;
-        const float iom = 1.0f / (1.0f - al);
+        const float iom = __frcp_rn(1.0f - al);
         const float Tk = Tn * iom;  // transmittance in front of sample s
-        const float gc0 = g.x * Tk * al, gc1 = g.y * Tk * al, gc2 = g.z * Tk * al;
-        float ga = g.x * (Tk * c.x - Cb0 * iom) + g.y * (Tk * c.y - Cb1 * iom) +
-                   g.z * (Tk * c.z - Cb2 * iom) + g.w * (Tfin * iom);
-        const float gc3 = clamped ? 0.0f : ga * K.p.sigma_scale * K.p.step * e;
+        const float w = Tk * al;    // the sample's weight in the image
+        const float gcol = g.x * c.x + g.y * c.y + g.z * c.z;
+        // d loss / d alpha: Tk g.c - (g.Cb - g.w Tfin) / (1 - al)
+        const float ga = Tk * gcol - iom * (gCb - gwT);
+        const float gc3 = clamped ? 0.0f : ga * sstep * e;
         // transfer-function gradient: i1 = i0 + 1 except at the top entry
         if (i0 != run_i0) {
           // The run's two table entries are run_i0 (ta0) and run_i0 + 1 (ta1).
@@ -315,25 +317,30 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
           // flushes only the entry that leaves.
           if (run_i0 >= 0) {
             if (i0 == run_i0 + 1) {
-              flush_entry(my_gtf, run_i0, ta0);
-#pragma unroll
-              for (int k = 0; k < 4; k++) { ta0[k] = ta1[k]; ta1[k] = 0.0f; }
+              flush_entry(my_gtf, run_i0, ta0, g);
+              ta0 = ta1;
+              ta1 = make_float2(0.0f, 0.0f);
             } else if (i0 == run_i0 - 1) {
-              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1);
-#pragma unroll
-              for (int k = 0; k < 4; k++) { ta1[k] = ta0[k]; ta0[k] = 0.0f; }
+              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
+              ta1 = ta0;
+              ta0 = make_float2(0.0f, 0.0f);
             } else {
-              flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
+              flush_entry(my_gtf, run_i0, ta0, g);
+              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
             }
           }
           run_i0 = i0;
         }
-        const float wf0 = 1.0f - f, wf1 = f;
-        ta0[0] += wf0 * gc0; ta0[1] += wf0 * gc1; ta0[2] += wf0 * gc2; ta0[3] += wf0 * gc3;
-        ta1[0] += wf1 * gc0; ta1[1] += wf1 * gc1; ta1[2] += wf1 * gc2; ta1[3] += wf1 * gc3;
-        if (inr) {
-          const float drho = (gc0 * (tb.x - ta.x) + gc1 * (tb.y - ta.y) +
-                              gc2 * (tb.z - ta.z) + gc3 * (tb.w - ta.w)) * top;
+        const float wf0 = 1.0f - f;
+        ta0.x += wf0 * w;
+        ta0.y += wf0 * gc3;
+        ta1.x += f * w;
+        ta1.y += f * gc3;
+        const float drho = inr ? (w * (g.x * (tb.x - ta.x) + g.y * (tb.y - ta.y) +
+                                       g.z * (tb.z - ta.z)) +
+                                  gc3 * (tb.w - ta.w)) * top
+                               : 0.0f;
+        if (drho != 0.0f) {
           const int key = (cl.vz * K.dim[1] + cl.vy) * K.dim[0] + cl.vx;
           if (key != run_cell) {
             if (run_cell >= 0) flush_dens(gdens, K.dim, rvx, rvy, rvz, da);
@@ -355,12 +362,13 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
           da[6] += x0 * y1z1;
           da[7] += x1 * y1z1;
         }
-        Cb0 += Tk * al * c.x;
-        Cb1 += Tk * al * c.y;
-        Cb2 += Tk * al * c.z;
+        gCb += w * gcol;
         Tn = Tk;
       }
-      if (run_i0 >= 0) flush_tf(my_gtf, run_i0, min(run_i0 + 1, K.tfn - 1), ta0, ta1);
+      if (run_i0 >= 0) {
+        flush_entry(my_gtf, run_i0, ta0, g);
+        flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
+      }
       if (run_cell >= 0) flush_dens(gdens, K.dim, rvx, rvy, rvz, da);
     }
   }
@@ -553,7 +561,7 @@ SRT_API srt_status srt_volume_march_bwd_ex(srt_ctx *ctx, const srt_volume_params
     return s;
   if ((s = vol_view(ctx, transmittance, npix * 4, s_tr, &dtr, st)) != SRT_OK) return s;
   if ((s = vol_view(ctx, grad_image, npix * 16, s_g, &dg, st)) != SRT_OK) return s;
-  size_t shmem = (size_t)kTfCopies * (4 * tf_entries + 1) * sizeof(float);
+  const size_t shmem = (size_t)kTfCopies * (4 * tf_entries + 1) * sizeof(float);
   if (shmem > 48 * 1024) {
     cudaError_t ea = cudaFuncSetAttribute(vol_bwd_kernel,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,

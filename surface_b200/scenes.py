@@ -247,7 +247,10 @@ def hemisphere_dirs(normals, seed):
 
 # ---------------------------------------------------------------- volume
 def volume_blobs(res=256, nblobs=32, seed=123456, shift_voxels=0.0):
-    """Density grid (res,res,res) float32 (z slowest, x fastest) in [0,1]."""
+    """Density grid (res,res,res) float32 (z slowest, x fastest) in [0,1]:
+    the blob sum scaled down, when it exceeds 0.95, to peak at 0.95 -- no
+    plateau of texels on the transfer function's upper clamp, where the
+    density gradient has a kink (one-sided derivatives differ)."""
     rng = np.random.default_rng(seed)
     cen = rng.uniform(0.2, 0.8, size=(nblobs, 3))
     cen = cen + shift_voxels / (res - 1)
@@ -260,7 +263,10 @@ def volume_blobs(res=256, nblobs=32, seed=123456, shift_voxels=0.0):
         gy = np.exp(-0.5 * ((x - cen[b, 1]) / sig[b, 1]) ** 2)
         gz = np.exp(-0.5 * ((x - cen[b, 2]) / sig[b, 2]) ** 2)
         out += (amp[b] * gz[:, None, None] * gy[None, :, None] * gx[None, None, :]).astype(np.float32)
-    return np.clip(out, 0.0, 1.0).astype(np.float32)
+    peak = float(out.max())
+    if peak > 0.95:
+        out *= np.float32(0.95 / peak)
+    return out.astype(np.float32)
 
 
 def transfer_function(entries=256, seed=123456):

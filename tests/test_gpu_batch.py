@@ -83,6 +83,39 @@ def test_graph_capture_and_replay_are_identical():
     assert tb.config()[3] == kpc
 
 
+@pytest.mark.parametrize("depth", [24, 32, 48])
+@pytest.mark.parametrize("sort_bits", [0, 12, 22])
+def test_every_tuning_point_gives_the_same_hits(depth, sort_bits):
+    """The autotuner's axes -- stack depth and ray order -- pinned one point at
+    a time: the same hits as the per-scene path, through capture and replay."""
+    B = small_batch(seed=5, n=10)
+    v, f, r = to_dev(B)
+    want = per_scene(B, v, f, r)
+    tb = TriangleBatch()
+    tb.set_tuning(block=64 if sort_bits else 256, rays_per_grab=2, stack_depth=depth,
+                  sort_bits=sort_bits)
+    hits = torch.empty((r.shape[0], 4), device="cuda")
+    for _ in range(3):
+        hits.fill_(float("nan"))
+        assert_same(hits_np(tb.build_trace(v, f, B["face_offsets"], r, B["ray_offsets"],
+                                           hits=hits)), want)
+    assert tb.config()[2]
+    assert tb.tuning() == {"block": 64 if sort_bits else 256, "rays_per_grab": 2,
+                           "stack_depth": depth, "sort_bits": sort_bits}
+
+
+def test_autotuned_point_is_reported():
+    B = small_batch(seed=8, n=8)
+    v, f, r = to_dev(B)
+    tb = TriangleBatch()
+    tb.build_trace(v, f, B["face_offsets"], r, B["ray_offsets"])
+    t = tb.tuning()
+    assert t["block"] in (64, 128, 256) and t["rays_per_grab"] in (1, 2, 4)
+    assert t["stack_depth"] in (24, 32, 48) and t["sort_bits"] in (0, 12, 22)
+    with pytest.raises(sb.SurfaceError):
+        tb.set_tuning(stack_depth=40)
+
+
 def test_replay_sees_new_input_values():
     """A replay reads the buffers again: moved vertices give new hits."""
     B = small_batch(seed=3, n=6)
@@ -131,7 +164,8 @@ def test_invalid_batches_are_rejected():
 
 
 def test_full_size_batch_matches_per_scene():
-    """64 scenes, 1e3-1e6 faces, images 128^2..1024^2."""
+    """64 scenes, 1e3-1e6 faces, images 128^2..1024^2: the batch against the
+    per-scene GPU loop and every scene against the oracle."""
     B = S.batched_scenes()
     v, f, r = to_dev(B)
     tb = TriangleBatch()
@@ -142,3 +176,10 @@ def test_full_size_batch_matches_per_scene():
         tb.build_trace(v, f, B["face_offsets"], r, B["ray_offsets"], hits=tb._keep[3])
     assert tb.config()[2]
     assert_same(hits_np(tb._keep[3]), h)
+    # every scene against the oracle (its own build and trace of the scene)
+    fo, ro = B["face_offsets"], B["ray_offsets"]
+    for s_ in range(fo.size - 1):
+        faces = B["faces"][int(fo[s_]):int(fo[s_ + 1])]
+        o = O.OracleAccel(O.TRI, B["vertices"], faces)
+        want = o.trace(B["rays"][int(ro[s_]):int(ro[s_ + 1])])
+        assert_same(h[int(ro[s_]):int(ro[s_ + 1])], want)

@@ -418,11 +418,65 @@ def test_full_size_tetra_workload():
 
 
 def test_full_size_particle_frame():
-    """16,777,216 spheres: build and a strided subset of 2048^2 primaries."""
-    pos, rad = S.particles()
+    """The particle configuration's frame 3 (16,777,216 spheres advected three
+    times): the build, all 2048^2 primaries and the hemisphere secondary of
+    every hit (self-hit rule) against the oracle."""
+    import torch
+    pos0, rad = S.particles()
+    pos = S.particle_frames(pos0, 4, device="cuda")[3].cpu().numpy()
+    del pos0
     o, acc = _compare_build(O.SPHERE, pos, None, rad)
-    rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)[::37]
-    assert_sphere_hits(trace_both(acc, rays), o.trace(rays))
+    rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    rt = torch.as_tensor(rays.view(np.float32).reshape(-1, 8)).cuda()
+    res = acc.Traverse(rt, want_normal=True)
+    hits = res.hits.cpu().numpy().reshape(-1).view(O.HIT_DTYPE)
+    assert_sphere_hits(hits, o.trace(rays))
+    sec, sn = sb.spawn_secondary(rt, res.hits, res.normal, seed=3)
+    h2 = acc.Traverse(sec, prev_normals=sn)
+    torch.cuda.synchronize()
+    sr = sec.cpu().numpy().reshape(-1).view(O.RAY_DTYPE)
+    assert sr.size == int((hits["prim"] != O.MISS).sum()) > 1_000_000
+    want = o.trace(sr, prev_normals=sn.cpu().numpy())
+    assert_sphere_hits(h2.cpu().numpy().reshape(-1).view(O.HIT_DTYPE), want)
+    assert (want["prim"] != O.MISS).any()
+
+
+# The oracle against the reference's own build and trace (oracle/_ref) at the
+# three full configurations.  No GPU is used; they run with the GPU suite for
+# the box's host cores (minutes of CPU time on a small host).
+need_ref = pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+
+
+@need_ref
+def test_oracle_vs_reference_full_triangles():
+    v, f = S.displaced_octasphere(7)
+    o, r = O.OracleAccel(O.TRI, v, f), O.RefAccel(O.TRI, v, f)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc) and np.array_equal(o.indices, ridx)
+    rays = S.pinhole_rays(512, 512, (0, 0, 3), (0, 0, 0))
+    assert_hits_equal(o.trace(rays), r.trace(rays))
+
+
+@need_ref
+def test_oracle_vs_reference_full_tetrahedra():
+    v, f, _ = S.tet_grid(64)
+    o, r = O.OracleAccel(O.TET, v, f), O.RefAccel(O.TET, v, f)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc) and np.array_equal(o.indices, ridx)
+    rays = S.ortho_rays(1024, 1024)
+    (ho, so), (hr, sr) = o.trace(rays, want_subface=True), r.trace(rays)
+    assert_hits_equal(ho, hr)
+    assert np.array_equal(so, sr)
+
+
+@need_ref
+def test_oracle_vs_reference_full_particles():
+    pos, rad = S.particles()
+    o, r = O.OracleAccel(O.SPHERE, pos, None, rad), O.RefAccel(O.SPHERE, pos, None, rad)
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc) and np.array_equal(o.indices, ridx)
+    rays = S.pinhole_rays(2048, 2048, (0.5, 0.5, 2.2), (0.5, 0.5, 0.5), fov_deg=30)
+    assert_hits_equal(o.trace(rays), r.trace(rays))
 
 
 # ---------------------------------------------------------------- exact ties

@@ -99,6 +99,55 @@ def test_adjoint_matches_fp64_reference_and_fd():
     assert worst <= TOL_GRAD, worst
 
 
+def test_adjoint_full_config():
+    """The differentiable-volume configuration: 256^3 density of 32 blobs,
+    256-entry transfer function, 512^2 rays, step 0.5 voxel, L2 loss against
+    the image of the blobs shifted by 2 voxels.  The CUDA adjoint against the
+    FP64 oracle gradient (whole arrays) and FP64 central finite differences on
+    64 voxels (loss over the pixels whose rays pass near the voxel: the only
+    ones a change there can reach) and 16 transfer-function entries (whole
+    image); relative error <= 1e-3."""
+    dens = S.volume_blobs(256, nblobs=32)
+    tgt = S.volume_blobs(256, nblobs=32, shift_voxels=2.0)
+    tf = S.transfer_function(256)
+    p = V.camera(512, 512, eye=(0.0, 0.0, 3.0), res=256)
+    q = oracle_params(p)
+    dims = (256, 256, 256)
+    target = O.volume_fwd_f32(q, tgt, dims, tf)
+    loss, gd, gt = _gpu_grad(p, dens, tf, target)
+    rloss, _, rgd, rgt = O.volume_f64(q, dens, dims, tf, target=target, want_grad=True)
+    assert abs(loss - rloss) <= 1e-4 * rloss
+    assert np.linalg.norm(gd - rgd) <= TOL_GRAD * np.linalg.norm(rgd)
+    assert np.linalg.norm(gt - rgt) <= TOL_GRAD * np.linalg.norm(rgt)
+    rng = np.random.default_rng(5)
+    flat = rgd.reshape(-1)
+    sig = np.nonzero(np.abs(flat) > 1e-2 * np.abs(flat).max())[0]
+    vox = rng.choice(sig, size=64, replace=False)
+    h = 1e-6
+    d64 = dens.astype(np.float64).reshape(-1)
+    worst = 0.0
+    for v in vox:
+        z, rem = divmod(int(v), 256 * 256)
+        y, x = divmod(rem, 256)
+        pix = O.volume_pixels_near(q, dims, (x, y, z), 1.5)
+        assert pix.size > 0
+        dp, dm = d64.copy(), d64.copy()
+        dp[v] += h
+        dm[v] -= h
+        fd = (O.volume_f64_pixels(q, dp.reshape(dens.shape), dims, tf, target, pix)
+              - O.volume_f64_pixels(q, dm.reshape(dens.shape), dims, tf, target, pix)) / (2 * h)
+        worst = max(worst, abs(gd.reshape(-1)[v] - fd) / abs(fd))
+    t64 = tf.astype(np.float64).reshape(-1)
+    for e in np.argsort(-np.abs(rgt.reshape(-1)))[:16]:
+        tp, tm = t64.copy(), t64.copy()
+        tp[e] += h
+        tm[e] -= h
+        fd = (O.volume_f64(q, dens, dims, tp.reshape(tf.shape), target=target)[0]
+              - O.volume_f64(q, dens, dims, tm.reshape(tf.shape), target=target)[0]) / (2 * h)
+        worst = max(worst, abs(gt.reshape(-1)[e] - fd) / abs(fd))
+    assert worst <= TOL_GRAD, worst
+
+
 def test_autograd_function_matches_direct_adjoint():
     p, dens, tgt, tf = case(32, 40)
     d = torch.as_tensor(dens).cuda()
