@@ -403,6 +403,44 @@ SRT_API srt_status srt_framebuffer_write(srt_ctx *ctx, const srt_camera *cam,
                                          int32_t format, void *color,
                                          float *depth);
 
+/* Several samples per pixel and the stereo environment camera, as OnData
+ * does them with sampleCoverage and lsglSetStereoEnvCamera
+ * (gles/gles_raytrace_engine.cc:549-553, 747-800, 826-877;
+ * render/render_camera.cc:65-118). */
+typedef struct srt_camera_samples {
+  int32_t subsamples;      /* per axis (sampleCoverageValue), 1..16 */
+  int32_t stereo_env;      /* 1: Camera::generateStereoEnvRay rays */
+  float zero_parallax;     /* stereo camera's focal distance */
+  float eye_separation;    /* stereo camera's eye separation */
+  /* The sample jitter: subsample (vv, uu) lies at ((uu + ju) / S, (vv + jv)
+   * / S) in its pixel, ju (uu != 0) then jv (vv != 0) drawn from the serial
+   * renderer's random stream -- TinyMT64 with the parameters of
+   * gles_common.cc's initialize_random, seeded jitter_seed (1234 there),
+   * draws as (float) of its doubles -- in pixel order (rows, then x) over
+   * the kept pixels, after jitter_offset draws (those of earlier frames). */
+  uint64_t jitter_seed;
+  uint64_t jitter_offset;
+} srt_camera_samples;
+
+/* srt_camera_rays with samples: per kept loop pixel (rows, then x) its
+ * subsamples^2 rays, (vv, uu) row-major; pixel (optional) gets each ray's
+ * loop pixel; rays/pixel need room for subsamples^2 rays per loop pixel.
+ * *draws receives the jitter draws the frame consumed (the next frame's
+ * jitter_offset is this one's plus it).  With stereo_env the camera's
+ * fov and ortho are not used.  Device arrays; asynchronous. */
+SRT_API srt_status srt_camera_rays_ex(srt_ctx *ctx, const srt_camera *cam,
+                                      const srt_camera_samples *smp, srt_ray *rays,
+                                      uint32_t *pixel, uint32_t *count,
+                                      uint64_t *draws);
+/* The write of n rays made by srt_camera_rays_ex: per loop pixel the sum of
+ * its hits' colours and depths times 1 / subsamples^2 fills its block, for
+ * pixels with at least one hit (other arguments as srt_framebuffer_write). */
+SRT_API srt_status srt_framebuffer_write_ex(srt_ctx *ctx, const srt_camera *cam,
+                                            const srt_camera_samples *smp,
+                                            const srt_hit *hits, const uint32_t *pixel,
+                                            const float *rgba, uint32_t n,
+                                            int32_t format, void *color, float *depth);
+
 /* ---- scenes: several accels with transforms ----------------------------- */
 /* RenderGraph (gles/gles_render_graph.cc:104-314) on the GPU: built accels
  * placed in the world by 4x4 transforms, a top-level tree over their world

@@ -107,6 +107,12 @@ def lib():
         L.so_camera_rays.argtypes = [_P, _P, _P, _P]
         L.so_framebuffer_write.argtypes = [C.c_int, C.c_int, C.c_int, _P, _P, _P, _SZ,
                                            C.c_int, _P, _P]
+        L.so_stereo_env_ray.argtypes = [_P, _P, _P, C.c_float, C.c_float, C.c_float, C.c_float,
+                                        C.c_int, C.c_int, _P, _P]
+        L.so_camera_rays_ex.restype = _SZ
+        L.so_camera_rays_ex.argtypes = [_P, _P, _P, _P, C.c_uint64, C.c_uint64, _P, _P]
+        L.so_framebuffer_write_ex.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, _P, _P, _P,
+                                              _SZ, C.c_int, _P, _P]
         L.so_tex_fetch.argtypes = [C.c_int, _P, _P, C.c_int, _P, _P, _P, _P, _SZ, _P]
         L.so_sparse_tree.restype = _P
         L.so_sparse_tree.argtypes = [_P, _SZ]
@@ -187,6 +193,8 @@ def ref():
                                            C.c_uint64, _SZ, _P]
         L.ref_camera_frame.argtypes = [_P, _P, _P, C.c_float, C.c_int, C.c_int, C.c_int,
                                        _P]
+        L.ref_stereo_env_ray.argtypes = [_P, _P, _P, C.c_float, C.c_float, C.c_float,
+                                         C.c_float, C.c_int, C.c_int, _P]
         L.ref_tex_fetch.argtypes = [C.c_int, _P, C.c_int, C.c_int, C.c_int, C.c_int, _P,
                                     _P, C.c_int, _P, C.c_int, _P, C.c_int, _P, _SZ, _P]
         L.ref_sparse_fetch.argtypes = [_P, _SZ, _P, C.c_int, C.c_int, _P, _P, _SZ, _P]
@@ -738,6 +746,64 @@ def camera_rays(cam):
     pix = np.zeros(cap, np.uint32)
     n = lib().so_camera_rays(_ptr(f), _ptr(ints), _ptr(rays), _ptr(pix))
     return rays[:n], pix[:n]
+
+
+def stereo_env_ray(eye, lookat, up, zero_parallax, eye_separation, image_u, image_v, width,
+                   height, use_ref=False):
+    """Camera::generateStereoEnvRay -- the restatement, or with use_ref the
+    reference's own (render/render_camera.cc:65-118).  Returns (org, dir)."""
+    e, la, u = (np.ascontiguousarray(x, np.float32) for x in (eye, lookat, up))
+    if use_ref:
+        out = np.zeros(6, np.float32)
+        ref().ref_stereo_env_ray(_ptr(e), _ptr(la), _ptr(u), C.c_float(zero_parallax),
+                                 C.c_float(eye_separation), C.c_float(image_u),
+                                 C.c_float(image_v), int(width), int(height), _ptr(out))
+        return out[:3], out[3:]
+    o = np.zeros(3, np.float32)
+    d = np.zeros(3, np.float32)
+    lib().so_stereo_env_ray(_ptr(e), _ptr(la), _ptr(u), C.c_float(zero_parallax),
+                            C.c_float(eye_separation), C.c_float(image_u), C.c_float(image_v),
+                            int(width), int(height), _ptr(o), _ptr(d))
+    return o, d
+
+
+def camera_rays_ex(cam, subsamples=1, stereo=None, seed=1234, offset=0):
+    """OnData's eye rays with subsamples x subsamples rays per pixel (the
+    serial renderer's jitter stream: TinyMT64 seeded `seed`, `offset` draws
+    consumed before the frame) and, with stereo = (zero_parallax,
+    eye_separation), the stereo environment camera.  Returns (rays, pixel),
+    subsamples^2 consecutive rays per kept loop pixel."""
+    f = np.zeros(10, np.float32)
+    f[0:3], f[3:6], f[6:9], f[9] = cam["eye"], cam["lookat"], cam["up"], cam["fov"]
+    ints = np.array([cam["ortho"], cam["width"], cam["height"], *cam["viewport"],
+                     *cam["region"], cam["step"]], np.int32)
+    si = np.array([subsamples, 1 if stereo else 0], np.int32)
+    sf = np.array(stereo if stereo else (0.0, 0.0), np.float32)
+    x0, y0, x1, y1 = cam["region"]
+    cap = max(1, len(range(x0, x1, cam["step"])) * len(range(y0, y1, cam["step"])))
+    cap *= subsamples * subsamples
+    rays = np.zeros(cap, RAY_DTYPE)
+    pix = np.zeros(cap, np.uint32)
+    n = lib().so_camera_rays_ex(_ptr(f), _ptr(ints), _ptr(si), _ptr(sf), C.c_uint64(seed),
+                                C.c_uint64(offset), _ptr(rays), _ptr(pix))
+    return rays[:n], pix[:n]
+
+
+def framebuffer_write_ex(cam, subsamples, hits, pixel, rgba=None, fmt=0, color=None,
+                         depth=None):
+    """The write of camera_rays_ex's rays: each pixel's hits averaged."""
+    W, H = cam["width"], cam["height"]
+    if color is None:
+        color = np.zeros((H, W, 4), np.uint8 if fmt == 0 else np.float32)
+    if depth is None:
+        depth = np.zeros((H, W), np.float32)
+    hits = np.ascontiguousarray(hits, HIT_DTYPE)
+    pixel = np.ascontiguousarray(pixel, np.uint32)
+    rg = None if rgba is None else np.ascontiguousarray(rgba, np.float32)
+    lib().so_framebuffer_write_ex(W, H, cam["step"], int(subsamples), _ptr(hits), _ptr(pixel),
+                                  None if rg is None else _ptr(rg), hits.size, fmt,
+                                  _ptr(color), _ptr(depth))
+    return color, depth
 
 
 def framebuffer_write(cam, hits, pixel, rgba=None, fmt=0, color=None, depth=None):

@@ -444,6 +444,21 @@ REF_API void ref_camera_frame(const float eye[3], const float lookat[3], const f
   }
 }
 
+// Camera::generateStereoEnvRay (render/render_camera.cc:65-118) of the
+// stereo camera (render/render_camera.h:44-60): out = org[3], dir[3].
+REF_API void ref_stereo_env_ray(const float eye[3], const float lookat[3], const float up[3],
+                                float zero_parallax, float eye_separation, float image_u,
+                                float image_v, int width, int height, float out[6]) {
+  Camera cam(real3(eye[0], eye[1], eye[2]), real3(lookat[0], lookat[1], lookat[2]),
+             real3(up[0], up[1], up[2]), zero_parallax, eye_separation);
+  real3 org, dir;
+  cam.generateStereoEnvRay(org, dir, image_u, image_v, width, height);
+  for (int k = 0; k < 3; k++) {
+    out[k] = org[k];
+    out[3 + k] = dir[k];
+  }
+}
+
 // BVHTree (render/render_bvh_tree.cc), the top-level tree of RenderGraph.
 REF_API void *ref_bvh_build(const double *bmin, const double *bmax, const uint32_t *ids,
                             size_t n) {

@@ -2222,6 +2222,172 @@ SO_API void so_framebuffer_write(int width, int height, int step, const so_hit *
   }
 }
 
+/* ---- several samples per pixel and the stereo environment camera
+ * OnData with sampleCoverage (gles/gles_raytrace_engine.cc:549-553,
+ * 747-800): per loop pixel subSamples^2 rays, (vv, uu) row-major, at
+ * u = (uu + ju) / S, v = (vv + jv) / S where ju (uu != 0) and then jv
+ * (vv != 0) are draws of randomreal: (float) of TinyMT64's double, the
+ * serial renderer's single stream seeded 1234 with gles_common.cc's
+ * parameters (initialize_random, :260-280), consumed in pixel order (rows,
+ * then x) over the kept pixels -- `offset` draws already consumed.  The
+ * write averages each pixel's hits: colour sum * (1 / S^2), depth sum *
+ * (1 / S^2), for pixels with at least one hit (:826-877). */
+
+/* Camera::generateStereoEnvRay (render/render_camera.cc:65-118) for the
+ * stereo camera of render/render_camera.h:44-60 (m_uvw = (normalize(up x
+ * look), normalize(look x u), normalize(look))). */
+SO_API void so_stereo_env_ray(const float eye[3], const float lookat[3], const float up[3],
+                              float zero_parallax, float eye_sep, float image_u, float image_v,
+                              int width, int height, float org[3], float dir[3]) {
+  float look[3], u[3], v[3];
+  for (int k = 0; k < 3; k++) look[k] = lookat[k] - eye[k];
+  cam_cross(up, look, u);
+  cam_norm(u);
+  cam_cross(look, u, v);
+  cam_norm(v);
+  cam_norm(look);
+  const int is_left = image_v < (float)(height / 2);
+  const float focal = zero_parallax, r = eye_sep;
+  const float theta = (float)(M_PI * fmod(2.0 * image_v / height, 1.0));
+  const float phi = (float)(2.0 * M_PI * (image_u / (float)width));
+  float dir_o[3];
+  dir_o[0] = sinf(theta) * cosf(phi);
+  dir_o[1] = cosf(theta);
+  dir_o[2] = sinf(theta) * sinf(phi);
+  float par[3];
+  if (is_left) {
+    par[0] = -dir_o[2];
+    par[1] = 0.0f;
+    par[2] = dir_o[0];
+  } else {
+    par[0] = dir_o[2];
+    par[1] = 0.0f;
+    par[2] = -dir_o[0];
+  }
+  cam_norm(par);
+  for (int k = 0; k < 3; k++) par[k] = par[k] * r;
+  for (int k = 0; k < 3; k++) org[k] = eye[k] + par[k];
+  float psi = (float)atan2((double)r, (double)focal);
+  if (is_left) psi = -psi;
+  float d[3];
+  d[0] = (float)(dir_o[0] * cos((double)psi) - dir_o[2] * sin((double)psi));
+  d[1] = dir_o[1];
+  d[2] = (float)(dir_o[0] * sin((double)psi) + dir_o[2] * cos((double)psi));
+  for (int k = 0; k < 3; k++) dir[k] = u[k] * d[0] + v[k] * d[1] + look[k] * d[2];
+}
+
+/* cam, ints as so_camera_rays; smp_i: subsamples, stereo; smp_f: zero
+ * parallax, eye separation.  Rays: per kept loop pixel (rows, then x) its
+ * S^2 rays; pixel: each ray's loop pixel.  Returns the ray count. */
+SO_API size_t so_camera_rays_ex(const float cam[10], const int ints[12], const int smp_i[2],
+                                const float smp_f[2], uint64_t seed, uint64_t offset,
+                                so_ray *rays, uint32_t *pixel) {
+  const int ortho = ints[0], W = ints[1], H = ints[2], vx = ints[3], vy = ints[4],
+            vw = ints[5], vh = ints[6], x0 = ints[7], y0 = ints[8], x1 = ints[9],
+            y1 = ints[10], step = ints[11];
+  const int S = smp_i[0], stereo = smp_i[1];
+  float fr[9];
+  so_camera_frame(cam, cam + 3, cam + 6, cam[9], ortho, W, H, fr);
+  const float *corner = fr, *ud = fr + 3, *vd = fr + 6;
+  float look[3];
+  cam_cross(ud, vd, look);
+  cam_norm(look);
+  so_tinymt64 rng;
+  rng.mat1 = 0xfa051f40u;
+  rng.mat2 = 0xffd0fff4u;
+  rng.tmat = UINT64_C(0x58d02ffeffbfffbc);
+  tmt_seed(&rng, seed);
+  for (uint64_t i = 0; i < offset; i++) tmt_step(&rng);
+  size_t n = 0;
+  for (int y = y0; y < y1; y += step) {
+    const int py = cam_viewport(y, 1, H, vy, vh);
+    if (py < 0 || py >= H) continue;
+    for (int x = x0; x < x1; x += step) {
+      const int px = cam_viewport(x, 0, W, vx, vw);
+      if (px < 0 || px >= W) continue;
+      for (int vv = 0; vv < S; vv++)
+        for (int uu = 0; uu < S; uu++) {
+          float ju = 0.0f, jv = 0.0f;
+          if (uu != 0) {
+            tmt_step(&rng);
+            ju = (float)((double)tmt_out(&rng) * (1.0 / 18446744073709551616.0));
+          }
+          if (vv != 0) {
+            tmt_step(&rng);
+            jv = (float)((double)tmt_out(&rng) * (1.0 / 18446744073709551616.0));
+          }
+          const float su = ((float)uu + ju) / (float)S, sv = ((float)vv + jv) / (float)S;
+          const float a = ((float)px + su) + (float)step / 2.0f;
+          const float b = (((float)py + sv) - (float)step / 2.0f) + 1.0f;
+          float o[3], d[3];
+          if (stereo) {
+            so_stereo_env_ray(cam, cam + 3, cam + 6, smp_f[0], smp_f[1], a, b, W, H, o, d);
+          } else {
+            for (int k = 0; k < 3; k++) {
+              const float p = (corner[k] + ud[k] * a) + vd[k] * b;
+              if (ortho) {
+                o[k] = p;
+                d[k] = look[k];
+              } else {
+                o[k] = cam[k];
+                d[k] = p - cam[k];
+              }
+            }
+          }
+          cam_norm(d);
+          so_ray *r = &rays[n];
+          for (int k = 0; k < 3; k++) {
+            r->org[k] = o[k];
+            r->dir[k] = d[k];
+          }
+          r->prev_prim = 0xffffffffu;
+          r->prev_t = 0.0f;
+          pixel[n] = ((uint32_t)y << 16) | (uint32_t)x;
+          n++;
+        }
+    }
+  }
+  return n;
+}
+
+/* The write of n rays made S^2 per loop pixel by so_camera_rays_ex. */
+SO_API void so_framebuffer_write_ex(int width, int height, int step, int S, const so_hit *hits,
+                                    const uint32_t *pixel, const float *rgba, size_t n,
+                                    int format, void *color, float *depth) {
+  const size_t per = (size_t)S * S;
+  const float inv_n = 1.0f / (float)(S * S);
+  for (size_t g = 0; g + per <= n; g += per) {
+    float fc[4] = {0.0f, 0.0f, 0.0f, 0.0f}, dv = 0.0f;
+    int frag = 0;
+    for (size_t q = g; q < g + per; q++) {
+      if (hits[q].prim == 0xffffffffu) continue;
+      for (int k = 0; k < 4; k++) fc[k] += rgba ? rgba[4 * q + k] : 1.0f;
+      dv += hits[q].t;
+      frag = 1;
+    }
+    if (!frag) continue;
+    dv *= inv_n;
+    const int x = (int)(pixel[g] & 0xffffu), y = (int)(pixel[g] >> 16);
+    for (int vv = 0; vv < step; vv++) {
+      const int row = height - y - 1 + vv;
+      if (row > height - 1 || row < 0) continue;
+      for (int uu = 0; uu < step; uu++) {
+        const int col = x + uu;
+        if (col > width - 1) continue;
+        const size_t p = (size_t)row * width + col;
+        if (color && format == 0) {
+          unsigned char *o = (unsigned char *)color + 4 * p;
+          for (int k = 0; k < 4; k++) o[k] = fb_clamp(fc[k] * inv_n);
+        } else if (color) {
+          float *o = (float *)color + 4 * p;
+          for (int k = 0; k < 4; k++) o[k] = fc[k] * inv_n;
+        }
+        if (depth) depth[p] = dv;
+      }
+    }
+  }
+}
+
 /* ======================================================== scenes
  * RenderGraph::Build / Trace (gles/gles_render_graph.cc:104-314) over
  * elements = (accel, T, invT, invT33, world box), restated:

@@ -29,6 +29,14 @@ class Camera(C.Structure):
                 ("height", C.c_int32), ("viewport", C.c_int32 * 4),
                 ("region", C.c_int32 * 4), ("step", C.c_int32)]
 
+
+class CameraSamples(C.Structure):
+    """srt_camera_samples (include/surface_rt.h)."""
+    _fields_ = [("subsamples", C.c_int32), ("stereo_env", C.c_int32),
+                ("zero_parallax", C.c_float), ("eye_separation", C.c_float),
+                ("jitter_seed", C.c_uint64), ("jitter_offset", C.c_uint64)]
+
+
 class VolumeSampling(C.Structure):
     """srt_volume_sampling (include/surface_rt.h)."""
     _fields_ = [("remap", C.c_void_p * 3), ("remap_n", C.c_uint32 * 3),
@@ -127,6 +135,8 @@ _SIGS = {
     "srt_scene_trace": [_P, _P, _SZ, _P, _P, _P, _P, _P],
     "srt_scene_top_nodes": [_P, _P, _P, _SZ],
     "srt_framebuffer_write": [_P, _P, _P, _P, _P, C.c_uint32, C.c_int32, _P, _P],
+    "srt_camera_rays_ex": [_P, _P, _P, _P, _P, _P, _P],
+    "srt_framebuffer_write_ex": [_P, _P, _P, _P, _P, _P, C.c_uint32, C.c_int32, _P, _P],
     "srt_accel_load_triangles": [_P, C.c_char_p, _P, _SZ, _P, _SZ],
     "srt_accel_load_tetrahedra": [_P, C.c_char_p, _P, _SZ, _P, _SZ],
     "srt_accel_load_spheres": [_P, C.c_char_p, _P, _P, C.c_float, _SZ],

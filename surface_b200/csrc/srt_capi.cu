@@ -210,7 +210,8 @@ SRT_API srt_status srt_ctx_destroy(srt_ctx *c) {
                     &c->s_stage_in, &c->s_stage_out, &c->s_stage_aux, &c->s_stage_sub,
                     &c->s_stage_scal, &c->s_stage_norm, &c->s_defer, &c->s_spawn, &c->s_rkey,
                     &c->s_rorder, &c->s_isect_sub, &c->s_stage_isect, &c->s_keys3,
-                    &c->s_vals3, &c->s_status, &c->s_lscan, &c->s_rays_in, &c->s_kidx, &c->s_kprefix};
+                    &c->s_vals3, &c->s_status, &c->s_lscan, &c->s_rays_in,
+                    &c->s_kidx, &c->s_kprefix};
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   for (DevBuf *b : bufs) b->release();
   if (c->ev_copy) cudaEventDestroy(c->ev_copy);

@@ -241,11 +241,6 @@ __device__ __forceinline__ D3 dcross(D3 a, D3 b) {
 }
 __device__ __forceinline__ double ddot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 
-struct SIsect {
-  float pos[3], nrm[3];
-  float t;
-};
-
 // normalize (:85), then to float
 __device__ __forceinline__ void s_unit(D3 a, float out[3]) {
   const double len = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
@@ -254,37 +249,42 @@ __device__ __forceinline__ void s_unit(D3 a, float out[3]) {
   out[2] = (float)(a.z / len);
 }
 
-// SetCrossPoint_Sq (double, :438-444): a quad face's crossing point
-__device__ __forceinline__ void s_quad(float out[3], D3 v0, D3 v1, D3 v2, double ws0, double ws1,
-                                       double ws2, double ws3, D3 e2, D3 e3, D3 dir) {
+__device__ __forceinline__ double comp(D3 a, int j) { return j == 0 ? a.x : (j == 1 ? a.y : a.z); }
+
+// The crossing point of a face, every coordinate (FULL) or coordinate j
+// only (out[j]; the one a hit's t is measured along).
+// SetCrossPoint_Sq (double, :438-444): a quad face.
+template <bool FULL>
+__device__ __forceinline__ void s_quad(float out[3], int j, D3 v0, D3 v1, D3 v2, double ws0,
+                                       double ws1, double ws2, double ws3, D3 e2, D3 e3,
+                                       D3 dir) {
   const double w = ws2 + ws3 + ddot(dcross(e2, e3), dir);
-  const D3 p = dadd(dadd(dscale(v2, ws0), dscale(v0, ws1)), dscale(v1, w));
   const double den = ws0 + ws1 + w;
-  out[0] = (float)(p.x / den);
-  out[1] = (float)(p.y / den);
-  out[2] = (float)(p.z / den);
+  if (FULL) {
+    const D3 p = dadd(dadd(dscale(v2, ws0), dscale(v0, ws1)), dscale(v1, w));
+    out[0] = (float)(p.x / den);
+    out[1] = (float)(p.y / den);
+    out[2] = (float)(p.z / den);
+  } else {
+    const double pj = (comp(v2, j) * ws0 + comp(v0, j) * ws1) + comp(v1, j) * w;
+    out[j] = (float)(pj / den);
+  }
 }
 
-// a triangle face's crossing point: the weighted sum in double, then the
-// float vector divided by the float sum of the weights
-__device__ __forceinline__ void s_tri(float out[3], D3 a, double wa, D3 b, double wb, D3 c,
-                                      double wc, double den) {
-  const D3 p = dadd(dadd(dscale(a, wa), dscale(b, wb)), dscale(c, wc));
+// A triangle face: the weighted sum in double, then the float vector
+// divided by the float sum of the weights.
+template <bool FULL>
+__device__ __forceinline__ void s_tri(float out[3], int j, D3 a, double wa, D3 b, double wb,
+                                      D3 c, double wc, double den) {
   const float f = (float)den;
-  out[0] = (float)p.x / f;
-  out[1] = (float)p.y / f;
-  out[2] = (float)p.z / f;
-}
-
-// t of both points along the last axis with |dir| > 0.1; the exit normal flipped
-__device__ __forceinline__ void s_params(SIsect is[2], D3 org, D3 dir) {
-  const double o[3] = {org.x, org.y, org.z}, d[3] = {dir.x, dir.y, dir.z};
-  for (int j = 0; j < 3; j++)
-    if (d[j] > 0.1 || d[j] < -0.1) {
-      is[0].t = (float)(((double)is[0].pos[j] - o[j]) / d[j]);
-      is[1].t = (float)(((double)is[1].pos[j] - o[j]) / d[j]);
-    }
-  for (int k = 0; k < 3; k++) is[1].nrm[k] = -1.0f * is[1].nrm[k];
+  if (FULL) {
+    const D3 p = dadd(dadd(dscale(a, wa), dscale(b, wb)), dscale(c, wc));
+    out[0] = (float)p.x / f;
+    out[1] = (float)p.y / f;
+    out[2] = (float)p.z / f;
+  } else {
+    out[j] = (float)((comp(a, j) * wa + comp(b, j) * wb) + comp(c, j) * wc) / f;
+  }
 }
 
 // Edges of each solid (GetEdges, :119-154): edge i = vertex hi[i] - vertex
@@ -353,108 +353,166 @@ __device__ __forceinline__ void s_weights(const SolidV<NV> &S, D3 dir, D3 org,
   }
 }
 
-// IntersectPyramidD (:455-505)
-__device__ bool s_pyramid(D3 org, D3 dir, const SolidV<5> &S, SIsect is[2]) {
-  double ws[8];
-  s_weights<5>(S, dir, org, ws);
-  for (int i = 1, n = 0; n < 2; i--, n++) {
-    // cw[0][k]: ws[k] >= 0, cw[1][k]: ws[k] <= 0
-    auto cw = [&](int side, int k) { return side == 0 ? ws[k] >= 0 : ws[k] <= 0; };
-    if (cw(i, 0) && cw(i, 1) && cw(i, 2) && cw(i, 3)) {
-      s_quad(is[n].pos, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3), dir);
-      s_unit(dcross(S.e(1), S.e(0)), is[n].nrm);
-    } else if (cw(n, 0) && cw(i, 4) && cw(n, 5)) {
-      s_tri(is[n].pos, S.v(4), -ws[0], S.v(1), ws[4], S.v(0), -ws[5], -ws[0] + ws[4] - ws[5]);
-      s_unit(dcross(S.e(4), S.e(0)), is[n].nrm);
-    } else if (cw(n, 1) && cw(i, 5) && cw(n, 6)) {
-      s_tri(is[n].pos, S.v(4), -ws[1], S.v(2), ws[5], S.v(1), -ws[6], -ws[1] + ws[5] - ws[6]);
-      s_unit(dcross(S.e(5), S.e(1)), is[n].nrm);
-    } else if (cw(n, 2) && cw(i, 6) && cw(n, 7)) {
-      s_tri(is[n].pos, S.v(4), -ws[2], S.v(3), ws[6], S.v(2), -ws[7], -ws[2] + ws[6] - ws[7]);
-      s_unit(dcross(S.e(6), S.e(2)), is[n].nrm);
-    } else if (cw(n, 3) && cw(i, 7) && cw(n, 4)) {
-      s_tri(is[n].pos, S.v(4), -ws[3], S.v(0), ws[7], S.v(3), -ws[4], -ws[3] + ws[7] - ws[4]);
-      s_unit(dcross(S.e(7), S.e(3)), is[n].nrm);
-    } else {
-      return false;
-    }
-  }
-  s_params(is, org, dir);
-  return true;
+// The reference's Intersect{Pyramid,Prism,Hexa}D (:455-505, :559-611,
+// :664-716) split in two.  face(ws, slot): the face its sign tests pick for
+// crossing point `slot` (0 the first point, 1 the second; -1: the solid is
+// missed).  point<FULL>(S, ws, face, ...): that face's crossing point (all
+// of it and the face normal when FULL, else only coordinate j) by the same
+// expressions.  A ray tests every solid's two points for t and forms the
+// full point and normal only for a point that becomes its closest hit.
+__device__ __forceinline__ bool s_cw(const double *ws, int side, int k) {
+  return side == 0 ? ws[k] >= 0 : ws[k] <= 0;
 }
 
-// IntersectPrismD (:559-611)
-__device__ bool s_prism(D3 org, D3 dir, const SolidV<6> &S, SIsect is[2]) {
-  double ws[9];
-  s_weights<6>(S, dir, org, ws);
-  for (int i = 0, n = 1; i < 2; i++, n--) {
-    auto cw = [&](int side, int k) { return side == 0 ? ws[k] >= 0 : ws[k] <= 0; };
-    if (cw(n, 0) && cw(n, 1) && cw(n, 2)) {
-      s_tri(is[i].pos, S.v(2), ws[0], S.v(0), ws[1], S.v(1), ws[2], ws[0] + ws[1] + ws[2]);
-      s_unit(dcross(S.e(0), S.e(1)), is[i].nrm);
-    } else if (cw(i, 3) && cw(i, 4) && cw(i, 5)) {
-      s_tri(is[i].pos, S.v(5), ws[3], S.v(3), ws[4], S.v(4), ws[5], ws[3] + ws[4] + ws[5]);
-      s_unit(dcross(S.e(3), S.e(4)), is[i].nrm);
-    } else if (cw(i, 2) && cw(i, 6) && cw(n, 5) && cw(n, 8)) {
-      s_quad(is[i].pos, S.v(2), S.v(0), S.v(3), ws[2], ws[6], -ws[5], -ws[8], S.e(5), S.e(8), dir);
-      s_unit(dcross(S.e(2), S.e(6)), is[i].nrm);
-    } else if (cw(i, 0) && cw(i, 7) && cw(n, 3) && cw(n, 6)) {
-      s_quad(is[i].pos, S.v(0), S.v(1), S.v(4), ws[0], ws[7], -ws[3], -ws[6], S.e(3), S.e(6), dir);
-      s_unit(dcross(S.e(0), S.e(7)), is[i].nrm);
-    } else if (cw(i, 1) && cw(i, 8) && cw(n, 4) && cw(n, 7)) {
-      s_quad(is[i].pos, S.v(1), S.v(2), S.v(5), ws[1], ws[8], -ws[4], -ws[7], S.e(4), S.e(7), dir);
-      s_unit(dcross(S.e(1), S.e(8)), is[i].nrm);
-    } else {
-      return false;
+template <int NV>
+struct SolidFaces;
+
+template <>
+struct SolidFaces<5> {  // IntersectPyramidD: point n uses i = 1 - n
+  __device__ static int face(const double (&ws)[8], int slot) {
+    const int n = slot, i = 1 - slot;
+    if (s_cw(ws, i, 0) && s_cw(ws, i, 1) && s_cw(ws, i, 2) && s_cw(ws, i, 3)) return 0;
+    if (s_cw(ws, n, 0) && s_cw(ws, i, 4) && s_cw(ws, n, 5)) return 1;
+    if (s_cw(ws, n, 1) && s_cw(ws, i, 5) && s_cw(ws, n, 6)) return 2;
+    if (s_cw(ws, n, 2) && s_cw(ws, i, 6) && s_cw(ws, n, 7)) return 3;
+    if (s_cw(ws, n, 3) && s_cw(ws, i, 7) && s_cw(ws, n, 4)) return 4;
+    return -1;
+  }
+  template <bool FULL>
+  __device__ static void point(const SolidV<5> &S, const double (&ws)[8], int f, D3 dir, int j,
+                               float pos[3], float nrm[3]) {
+    switch (f) {
+      case 0:
+        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3),
+                     dir);
+        if (FULL) s_unit(dcross(S.e(1), S.e(0)), nrm);
+        break;
+      case 1:
+        s_tri<FULL>(pos, j, S.v(4), -ws[0], S.v(1), ws[4], S.v(0), -ws[5], -ws[0] + ws[4] - ws[5]);
+        if (FULL) s_unit(dcross(S.e(4), S.e(0)), nrm);
+        break;
+      case 2:
+        s_tri<FULL>(pos, j, S.v(4), -ws[1], S.v(2), ws[5], S.v(1), -ws[6], -ws[1] + ws[5] - ws[6]);
+        if (FULL) s_unit(dcross(S.e(5), S.e(1)), nrm);
+        break;
+      case 3:
+        s_tri<FULL>(pos, j, S.v(4), -ws[2], S.v(3), ws[6], S.v(2), -ws[7], -ws[2] + ws[6] - ws[7]);
+        if (FULL) s_unit(dcross(S.e(6), S.e(2)), nrm);
+        break;
+      default:
+        s_tri<FULL>(pos, j, S.v(4), -ws[3], S.v(0), ws[7], S.v(3), -ws[4], -ws[3] + ws[7] - ws[4]);
+        if (FULL) s_unit(dcross(S.e(7), S.e(3)), nrm);
+        break;
     }
   }
-  s_params(is, org, dir);
-  return true;
-}
+};
 
-// IntersectHexaD (:664-716)
-__device__ bool s_hexa(D3 org, D3 dir, const SolidV<8> &S, SIsect is[2]) {
-  double ws[12];
-  s_weights<8>(S, dir, org, ws);
-  for (int i = 0, n = 1; i < 2; i++, n--) {
-    auto cw = [&](int side, int k) { return side == 0 ? ws[k] >= 0 : ws[k] <= 0; };
-    if (cw(n, 0) && cw(n, 1) && cw(n, 2) && cw(n, 3)) {
-      s_quad(is[i].pos, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3), dir);
-      s_unit(dcross(S.e(0), S.e(1)), is[i].nrm);
-    } else if (cw(i, 4) && cw(i, 5) && cw(i, 6) && cw(i, 7)) {
-      s_quad(is[i].pos, S.v(4), S.v(5), S.v(6), ws[4], ws[5], ws[6], ws[7], S.e(6), S.e(7), dir);
-      s_unit(dcross(S.e(4), S.e(5)), is[i].nrm);
-    } else if (cw(i, 0) && cw(i, 9) && cw(n, 4) && cw(n, 8)) {
-      s_quad(is[i].pos, S.v(0), S.v(1), S.v(5), ws[0], ws[9], -ws[4], -ws[8], S.e(4), S.e(8), dir);
-      s_unit(dcross(S.e(0), S.e(9)), is[i].nrm);
-    } else if (cw(i, 1) && cw(i, 10) && cw(n, 5) && cw(n, 9)) {
-      s_quad(is[i].pos, S.v(1), S.v(2), S.v(6), ws[1], ws[10], -ws[5], -ws[9], S.e(5), S.e(9),
-             dir);
-      s_unit(dcross(S.e(1), S.e(10)), is[i].nrm);
-    } else if (cw(i, 2) && cw(i, 11) && cw(n, 6) && cw(n, 10)) {
-      s_quad(is[i].pos, S.v(2), S.v(3), S.v(7), ws[2], ws[11], -ws[6], -ws[10], S.e(6), S.e(10),
-             dir);
-      s_unit(dcross(S.e(2), S.e(11)), is[i].nrm);
-    } else if (cw(i, 3) && cw(i, 8) && cw(n, 7) && cw(n, 11)) {
-      s_quad(is[i].pos, S.v(3), S.v(0), S.v(4), ws[3], ws[8], -ws[7], -ws[11], S.e(7), S.e(11),
-             dir);
-      s_unit(dcross(S.e(3), S.e(8)), is[i].nrm);
-    } else {
-      return false;
+template <>
+struct SolidFaces<6> {  // IntersectPrismD: point i uses n = 1 - i
+  __device__ static int face(const double (&ws)[9], int slot) {
+    const int i = slot, n = 1 - slot;
+    if (s_cw(ws, n, 0) && s_cw(ws, n, 1) && s_cw(ws, n, 2)) return 0;
+    if (s_cw(ws, i, 3) && s_cw(ws, i, 4) && s_cw(ws, i, 5)) return 1;
+    if (s_cw(ws, i, 2) && s_cw(ws, i, 6) && s_cw(ws, n, 5) && s_cw(ws, n, 8)) return 2;
+    if (s_cw(ws, i, 0) && s_cw(ws, i, 7) && s_cw(ws, n, 3) && s_cw(ws, n, 6)) return 3;
+    if (s_cw(ws, i, 1) && s_cw(ws, i, 8) && s_cw(ws, n, 4) && s_cw(ws, n, 7)) return 4;
+    return -1;
+  }
+  template <bool FULL>
+  __device__ static void point(const SolidV<6> &S, const double (&ws)[9], int f, D3 dir, int j,
+                               float pos[3], float nrm[3]) {
+    switch (f) {
+      case 0:
+        s_tri<FULL>(pos, j, S.v(2), ws[0], S.v(0), ws[1], S.v(1), ws[2], ws[0] + ws[1] + ws[2]);
+        if (FULL) s_unit(dcross(S.e(0), S.e(1)), nrm);
+        break;
+      case 1:
+        s_tri<FULL>(pos, j, S.v(5), ws[3], S.v(3), ws[4], S.v(4), ws[5], ws[3] + ws[4] + ws[5]);
+        if (FULL) s_unit(dcross(S.e(3), S.e(4)), nrm);
+        break;
+      case 2:
+        s_quad<FULL>(pos, j, S.v(2), S.v(0), S.v(3), ws[2], ws[6], -ws[5], -ws[8], S.e(5),
+                     S.e(8), dir);
+        if (FULL) s_unit(dcross(S.e(2), S.e(6)), nrm);
+        break;
+      case 3:
+        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(4), ws[0], ws[7], -ws[3], -ws[6], S.e(3),
+                     S.e(6), dir);
+        if (FULL) s_unit(dcross(S.e(0), S.e(7)), nrm);
+        break;
+      default:
+        s_quad<FULL>(pos, j, S.v(1), S.v(2), S.v(5), ws[1], ws[8], -ws[4], -ws[7], S.e(4),
+                     S.e(7), dir);
+        if (FULL) s_unit(dcross(S.e(1), S.e(8)), nrm);
+        break;
     }
   }
-  s_params(is, org, dir);
-  return true;
+};
+
+template <>
+struct SolidFaces<8> {  // IntersectHexaD: point i uses n = 1 - i
+  __device__ static int face(const double (&ws)[12], int slot) {
+    const int i = slot, n = 1 - slot;
+    if (s_cw(ws, n, 0) && s_cw(ws, n, 1) && s_cw(ws, n, 2) && s_cw(ws, n, 3)) return 0;
+    if (s_cw(ws, i, 4) && s_cw(ws, i, 5) && s_cw(ws, i, 6) && s_cw(ws, i, 7)) return 1;
+    if (s_cw(ws, i, 0) && s_cw(ws, i, 9) && s_cw(ws, n, 4) && s_cw(ws, n, 8)) return 2;
+    if (s_cw(ws, i, 1) && s_cw(ws, i, 10) && s_cw(ws, n, 5) && s_cw(ws, n, 9)) return 3;
+    if (s_cw(ws, i, 2) && s_cw(ws, i, 11) && s_cw(ws, n, 6) && s_cw(ws, n, 10)) return 4;
+    if (s_cw(ws, i, 3) && s_cw(ws, i, 8) && s_cw(ws, n, 7) && s_cw(ws, n, 11)) return 5;
+    return -1;
+  }
+  template <bool FULL>
+  __device__ static void point(const SolidV<8> &S, const double (&ws)[12], int f, D3 dir, int j,
+                               float pos[3], float nrm[3]) {
+    switch (f) {
+      case 0:
+        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3),
+                     dir);
+        if (FULL) s_unit(dcross(S.e(0), S.e(1)), nrm);
+        break;
+      case 1:
+        s_quad<FULL>(pos, j, S.v(4), S.v(5), S.v(6), ws[4], ws[5], ws[6], ws[7], S.e(6), S.e(7),
+                     dir);
+        if (FULL) s_unit(dcross(S.e(4), S.e(5)), nrm);
+        break;
+      case 2:
+        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(5), ws[0], ws[9], -ws[4], -ws[8], S.e(4),
+                     S.e(8), dir);
+        if (FULL) s_unit(dcross(S.e(0), S.e(9)), nrm);
+        break;
+      case 3:
+        s_quad<FULL>(pos, j, S.v(1), S.v(2), S.v(6), ws[1], ws[10], -ws[5], -ws[9], S.e(5),
+                     S.e(9), dir);
+        if (FULL) s_unit(dcross(S.e(1), S.e(10)), nrm);
+        break;
+      case 4:
+        s_quad<FULL>(pos, j, S.v(2), S.v(3), S.v(7), ws[2], ws[11], -ws[6], -ws[10], S.e(6),
+                     S.e(10), dir);
+        if (FULL) s_unit(dcross(S.e(2), S.e(11)), nrm);
+        break;
+      default:
+        s_quad<FULL>(pos, j, S.v(3), S.v(0), S.v(4), ws[3], ws[8], -ws[7], -ws[11], S.e(7),
+                     S.e(11), dir);
+        if (FULL) s_unit(dcross(S.e(3), S.e(8)), nrm);
+        break;
+    }
+  }
+};
+
+// The full crossing point and normal of a hit that becomes a ray's closest
+// (seldom: kept out of line so the test loop keeps its registers).
+template <int NV>
+__device__ __noinline__ void s_full_point(const SolidV<NV> &S,
+                                          const double (&ws)[SolidTab<NV>::NE], int f, D3 dir,
+                                          float pos[3], float nrm[3]) {
+  SolidFaces<NV>::template point<true>(S, ws, f, dir, 0, pos, nrm);
 }
 
-__device__ __forceinline__ bool s_isect(D3 org, D3 dir, const SolidV<5> &S, SIsect is[2]) {
-  return s_pyramid(org, dir, S, is);
-}
-__device__ __forceinline__ bool s_isect(D3 org, D3 dir, const SolidV<6> &S, SIsect is[2]) {
-  return s_prism(org, dir, S, is);
-}
-__device__ __forceinline__ bool s_isect(D3 org, D3 dir, const SolidV<8> &S, SIsect is[2]) {
-  return s_hexa(org, dir, S, is);
+// t of a crossing point along axis j (the last with |dir| > 0.1; none: 0),
+// as the reference's parameter step computes it (:2280-2290).
+__device__ __forceinline__ float s_t(float pj, int j, D3 org, D3 dir) {
+  if (j < 0) return 0.0f;
+  return (float)(((double)pj - comp(org, j)) / comp(dir, j));
 }
 
 // IntersectRayAABB (:2160-2204) with the reference's selection order.
@@ -483,7 +541,7 @@ __device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], co
 constexpr int kSolidQ = 32;  // solids a lane queues before the warp tests them
 
 template <int NV>
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 3)  // 3 blocks per SM: 168 registers
 solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
                    const srt_ray *__restrict__ rays, const uint32_t *__restrict__ order,
                    size_t n, srt_hit *__restrict__ hits, float *__restrict__ normals,
@@ -556,6 +614,10 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
       }
     }
     const D3 dorg = {org[0], org[1], org[2]}, ddir = {dir[0], dir[1], dir[2]};
+    int jax = -1;  // the last axis with |dir| > 0.1
+#pragma unroll
+    for (int c = 0; c < 3; c++)
+      if (dir[c] > 0.1 || dir[c] < -0.1) jax = c;
     for (int qi = 0; qi < len; qi++) {
       const uint32_t j = queue[qi][threadIdx.x];
       const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)RF * j);
@@ -575,16 +637,27 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
       for (int c = 0; c < NV; c++)
 #pragma unroll
         for (int e = 0; e < 3; e++) S.x[c][e] = rv[3 * c + e];
-      SIsect is[2];
-      for (int h = 0; h < 2; h++) is[h].t = 0.0f;
-      if (!s_isect(dorg, ddir, S, is)) continue;
+      double ws[SolidTab<NV>::NE];
+      s_weights<NV>(S, ddir, dorg, ws);
+      const int f0 = SolidFaces<NV>::face(ws, 0);
+      const int f1 = f0 < 0 ? -1 : SolidFaces<NV>::face(ws, 1);
+      if (f1 < 0) continue;
+      float pt[3] = {0.0f, 0.0f, 0.0f}, nd3[3];
+      float th[2];
+#pragma unroll
+      for (int h = 0; h < 2; h++) {
+        if (jax >= 0) SolidFaces<NV>::template point<false>(S, ws, h ? f1 : f0, ddir, jax, pt, nd3);
+        th[h] = s_t(jax >= 0 ? pt[jax] : 0.0f, jax, dorg, ddir);
+      }
+#pragma unroll
       for (int h = 0; h < 2; h++)
-        if (is[h].t >= 0.0f && is[h].t < t) {
-          t = is[h].t;
+        if (th[h] >= 0.0f && th[h] < t) {
+          t = th[h];
           prim = p;
-          for (int c = 0; c < 3; c++) {
-            bn[c] = is[h].nrm[c];
-            bp[c] = is[h].pos[c];
+          s_full_point<NV>(S, ws, h ? f1 : f0, ddir, bp, bn);
+          if (h) {  // the second point's normal is flipped
+#pragma unroll
+            for (int c = 0; c < 3; c++) bn[c] = -1.0f * bn[c];
           }
         }
     }

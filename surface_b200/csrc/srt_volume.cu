@@ -149,6 +149,8 @@ __device__ __forceinline__ float fetch(const float *__restrict__ img, const int 
 
 // Transfer-function lookup: returns rgba, sets i0/i1/f and whether rho was
 // inside the table's range (clamped samples have no density gradient).
+// (SHARED: the table is a shared-memory copy, else global memory.)
+template <bool SHARED = false>
 __device__ __forceinline__ void tf_lookup_ab(const float4 *__restrict__ tf, int tfn,
                                              float rho, float4 &c, int &i0, int &i1,
                                              float &f, bool &inrange, float4 &a, float4 &b) {
@@ -159,8 +161,8 @@ __device__ __forceinline__ void tf_lookup_ab(const float4 *__restrict__ tf, int 
   i0 = (int)x;
   i1 = min(i0 + 1, tfn - 1);
   f = x - (float)i0;
-  a = __ldg(&tf[i0]);
-  b = __ldg(&tf[i1]);
+  a = SHARED ? tf[i0] : __ldg(&tf[i0]);
+  b = SHARED ? tf[i1] : __ldg(&tf[i1]);
   c = make_float4(lerpf(f, a.x, b.x), lerpf(f, a.y, b.y), lerpf(f, a.z, b.z),
                   lerpf(f, a.w, b.w));
 }
@@ -227,25 +229,26 @@ __device__ __forceinline__ void flush_entry(float *g, int i, float2 &a, const fl
   a = make_float2(0.0f, 0.0f);
 }
 
-// Add the eight corner sums of one texel cell (lower corner vx, vy, vz;
-// upper corners clamped like the fetch) to the density gradient.
-__device__ __forceinline__ void flush_dens(float *__restrict__ g, const int dim[3], int vx,
-                                           int vy, int vz, float (&a)[8]) {
-  const int sy = dim[0], sz = dim[0] * dim[1];
-  const int ox = vx + 1 < dim[0] ? 1 : 0;
-  const int oy = vy + 1 < dim[1] ? sy : 0;
-  const int oz = vz + 1 < dim[2] ? sz : 0;
-  float *q = g + (vz * sz + vy * sy + vx);
+// Add the eight corner sums of one texel cell to the density gradient: its
+// lower corner's index `key` and, in `edge`, whether the cell sits on the
+// last texel of x (bit 0), y (bit 1), z (bit 2), where the fetch clamps the
+// upper corner onto the lower one.
+__device__ __forceinline__ void flush_dens(float *__restrict__ g, const int dim[3], int key,
+                                           int edge, float (&a)[8]) {
+  const int ox = (edge & 1) ? 0 : 1;
+  const int oy = (edge & 2) ? 0 : dim[0];
+  const int oz = (edge & 4) ? 0 : dim[0] * dim[1];
+  float *q = g + key;
 #pragma unroll
   for (int k = 0; k < 8; k++) {
     const int off = ((k & 1) ? ox : 0) + ((k & 2) ? oy : 0) + ((k & 4) ? oz : 0);
-    if (a[k] != 0.0f) atomicAdd(q + off, a[k]);
+    atomicAdd(q + off, a[k]);
     a[k] = 0.0f;
   }
 }
 constexpr int kTfMax = 1024;  // kTfCopies * (4 * kTfMax + 1) floats of shared memory
 
-__global__ void __launch_bounds__(128)
+__global__ void __launch_bounds__(128, 8)
 vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
                const float4 *__restrict__ tf, const float *__restrict__ trans,
                const float4 *__restrict__ gimg, float *__restrict__ gdens,
@@ -256,6 +259,9 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
   extern __shared__ float s_gtf[];
   const int tstride = 4 * K.tfn + 1;
   for (int i = threadIdx.x; i < kTfCopies * tstride; i += blockDim.x) s_gtf[i] = 0.0f;
+  // the transfer function itself, after the copies (16-byte aligned)
+  float4 *s_tf = reinterpret_cast<float4 *>(s_gtf + ((kTfCopies * tstride + 3) & ~3));
+  for (int i = threadIdx.x; i < K.tfn; i += blockDim.x) s_tf[i] = __ldg(&tf[i]);
   __syncthreads();
   float *my_gtf = s_gtf + (threadIdx.x & (kTfCopies - 1)) * tstride;
   const int W = K.p.width, H = K.p.height;
@@ -282,7 +288,7 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
       // (colour weight, opacity gradient).
       int run_i0 = -1;
       float2 ta0 = make_float2(0.f, 0.f), ta1 = make_float2(0.f, 0.f);
-      int run_cell = -1, rvx = 0, rvy = 0, rvz = 0;
+      int run_cell = -1, run_edge = 0;
       float da[8];
 #pragma unroll
       for (int cc = 0; cc < 8; cc++) da[cc] = 0.0f;
@@ -298,12 +304,12 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         int i0, i1;
         float f;
         bool inr;
-        tf_lookup_ab(tf, K.tfn, rho, c, i0, i1, f, inr, ta, tb);
-        const float e = expf(-(K.p.sigma_scale * c.w) * K.p.step);
+        tf_lookup_ab<true>(s_tf, K.tfn, rho, c, i0, i1, f, inr, ta, tb);
+        const float e = __expf(-(K.p.sigma_scale * c.w) * K.p.step);
         float al = 1.0f - e;
         const bool clamped = al > K.p.alpha_max;
         if (clamped) al = K.p.alpha_max;
-        const float iom = __frcp_rn(1.0f - al);
+        const float iom = __fdividef(1.0f, 1.0f - al);
         const float Tk = Tn * iom;  // transmittance in front of sample s
         const float w = Tk * al;    // the sample's weight in the image
         const float gcol = g.x * c.x + g.y * c.y + g.z * c.z;
@@ -343,11 +349,10 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         if (drho != 0.0f) {
           const int key = (cl.vz * K.dim[1] + cl.vy) * K.dim[0] + cl.vx;
           if (key != run_cell) {
-            if (run_cell >= 0) flush_dens(gdens, K.dim, rvx, rvy, rvz, da);
+            if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
             run_cell = key;
-            rvx = cl.vx;
-            rvy = cl.vy;
-            rvz = cl.vz;
+            run_edge = (cl.vx + 1 < K.dim[0] ? 0 : 1) | (cl.vy + 1 < K.dim[1] ? 0 : 2) |
+                       (cl.vz + 1 < K.dim[2] ? 0 : 4);
           }
           // corner c = x + 2y + 4z gets drho * wx * wy * wz
           const float x0 = drho * (1.0f - cl.dx), x1 = drho * cl.dx;
@@ -369,7 +374,7 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         flush_entry(my_gtf, run_i0, ta0, g);
         flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
       }
-      if (run_cell >= 0) flush_dens(gdens, K.dim, rvx, rvy, rvz, da);
+      if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
     }
   }
   __syncthreads();
@@ -561,7 +566,8 @@ SRT_API srt_status srt_volume_march_bwd_ex(srt_ctx *ctx, const srt_volume_params
     return s;
   if ((s = vol_view(ctx, transmittance, npix * 4, s_tr, &dtr, st)) != SRT_OK) return s;
   if ((s = vol_view(ctx, grad_image, npix * 16, s_g, &dg, st)) != SRT_OK) return s;
-  const size_t shmem = (size_t)kTfCopies * (4 * tf_entries + 1) * sizeof(float);
+  const size_t shmem =
+      (size_t)(((kTfCopies * (4 * tf_entries + 1) + 3) & ~3) + 4 * tf_entries) * sizeof(float);
   if (shmem > 48 * 1024) {
     cudaError_t ea = cudaFuncSetAttribute(vol_bwd_kernel,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -84,3 +84,81 @@ def test_camera_arguments_are_checked():
     rays, pix = K.camera_rays(cam)
     with pytest.raises(sb.SurfaceError):
         K.framebuffer_write(cam, rays.cpu()[:, :4].contiguous(), pix.cpu(), fmt=0)
+
+
+# ------------------------------------------------- subsamples, stereo camera
+SAMPLE_CASES = [
+    (dict(width=160, height=120, eye=(0, 0, 3), lookat=(0, 0, 0), fov=45.0), 2, None, 0),
+    (dict(width=97, height=61, eye=(0.3, 0.2, 3), lookat=(0, 0.1, 0), fov=30.0, step=2), 3,
+     None, 12345),
+    (dict(width=120, height=80, eye=(1, 2, 3), lookat=(0, 0, 0), up=(0, 0, 1), ortho=True,
+          viewport=(8, -4, 110, 90), region=(4, 2, 116, 78)), 4, None, 7),
+    (dict(width=256, height=128, eye=(0.1, 0.0, 0.2), lookat=(0, 0, -1), fov=45.0), 2,
+     (1.5, 0.065), 0),
+]
+STEREO_TOL = 2e-6  # C library vs CUDA trigonometry, relative
+
+
+@pytest.mark.parametrize("case,S,stereo,offset", SAMPLE_CASES)
+def test_subsample_rays_match_oracle(case, S, stereo, offset):
+    """subsamples^2 rays per pixel with the serial renderer's jitter stream
+    (jumped to `offset` draws on the host, drawn per row on the GPU) and the
+    stereo environment camera, against the restated OnData loop."""
+    cam = K.make_camera(**case)
+    smp = K.make_samples(S, stereo=stereo, jitter_offset=offset)
+    rays, pix = K.camera_rays(cam, samples=smp)
+    torch.cuda.synchronize()
+    ref, rpix = O.camera_rays_ex(K.camera_dict(cam), S, stereo=stereo, offset=offset)
+    got = rays.cpu().numpy().reshape(-1).view(O.RAY_DTYPE)
+    assert got.size == ref.size > 0
+    assert rays.draws == got.size // (S * S) * 2 * S * (S - 1)
+    assert np.array_equal(pix.cpu().numpy().view(np.uint32), rpix)
+    for f in ("prev_prim", "prev_t"):
+        assert np.array_equal(bits(got[f]), bits(ref[f])), f
+    if stereo is None:
+        for f in ("org", "dir"):
+            assert np.array_equal(bits(got[f]), bits(ref[f])), f
+    else:
+        for f in ("org", "dir"):
+            d = np.abs(got[f].astype(np.float64) - ref[f].astype(np.float64))
+            assert d.max() <= STEREO_TOL * max(1.0, np.abs(ref[f]).max()), (f, d.max())
+        # nearly all bit-equal: the C library's float sine and cosine are
+        # correctly rounded in all but rare cases
+        same = np.all(bits(got["dir"]) == bits(ref["dir"]), axis=1).mean()
+        assert same > 0.9, same
+
+
+def test_jitter_offsets_continue_the_stream():
+    """Two frames drawn one after the other equal one frame drawn from the
+    draw count of the first (the stream's state carried across frames)."""
+    cam = K.make_camera(64, 48, eye=(0, 0, 3), lookat=(0, 0, 0), fov=40.0)
+    a, _ = K.camera_rays(cam, samples=K.make_samples(3))
+    b, _ = K.camera_rays(cam, samples=K.make_samples(3, jitter_offset=a.draws))
+    ref_b, _ = O.camera_rays_ex(K.camera_dict(cam), 3, offset=a.draws)
+    got = b.cpu().numpy().reshape(-1).view(O.RAY_DTYPE)
+    assert np.array_equal(bits(got["dir"]), bits(ref_b["dir"]))
+    assert not np.array_equal(bits(a.cpu().numpy()), bits(b.cpu().numpy()))
+
+
+@pytest.mark.parametrize("S", [2, 3])
+def test_subsample_framebuffer_matches_oracle(S):
+    """Per pixel the average of its subsamples' hits (colour and depth)."""
+    acc = _scene()
+    cam = K.make_camera(180, 140, eye=(0.2, 0.1, 2.6), lookat=(0, 0, 0), fov=45.0, step=2)
+    smp = K.make_samples(S)
+    rays, pix = K.camera_rays(cam, samples=smp)
+    hits = acc.Traverse(rays)
+    gen = torch.Generator(device="cuda").manual_seed(5)
+    rgba = torch.rand((rays.shape[0], 4), device="cuda", generator=gen) * 1.2 - 0.1
+    torch.cuda.synchronize()
+    h = hits.cpu().numpy().reshape(-1).view(O.HIT_DTYPE)
+    p = pix.cpu().numpy().view(np.uint32)
+    d = K.camera_dict(cam)
+    for fmt in (0, 1):
+        col, dep = K.framebuffer_write(cam, hits, pix, rgba, fmt=fmt, samples=smp)
+        rc, rd = O.framebuffer_write_ex(d, S, h, p, rgba.cpu().numpy(), fmt=fmt)
+        assert col.cpu().numpy().tobytes() == rc.tobytes()
+        assert np.array_equal(bits(dep.cpu().numpy()), bits(rd))
+    # partial coverage: some pixels averaged over fewer hits than samples
+    per = h["prim"].reshape(-1, S * S) != O.MISS
+    assert ((per.sum(1) > 0) & (per.sum(1) < S * S)).any()

@@ -217,6 +217,59 @@ def test_camera_frame_matches_reference(cam):
         assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
 
 
+@pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+def test_stereo_env_ray_matches_reference():
+    """The restated Camera::generateStereoEnvRay equals the reference's, bit
+    for bit, over both eye halves of the image and random cameras."""
+    rng = np.random.default_rng(11)
+    for _ in range(400):
+        eye = rng.uniform(-3, 3, 3).astype(np.float32)
+        la = rng.uniform(-1, 1, 3).astype(np.float32)
+        up = np.float32([0, 1, 0]) if rng.random() < 0.7 else rng.normal(size=3).astype(np.float32)
+        W, H = int(rng.integers(8, 400)), int(rng.integers(8, 400))
+        u, v = np.float32(rng.uniform(0, W)), np.float32(rng.uniform(0, H))
+        zp, es = np.float32(rng.uniform(0.5, 5)), np.float32(rng.uniform(0.01, 0.2))
+        a = O.stereo_env_ray(eye, la, up, zp, es, u, v, W, H)
+        b = O.stereo_env_ray(eye, la, up, zp, es, u, v, W, H, use_ref=True)
+        for x, y in zip(a, b):
+            assert np.array_equal(x.view(np.uint32), y.view(np.uint32))
+
+
+@pytest.mark.skipif(not O.have_ref(), reason="reference build absent")
+def test_subsample_jitter_is_the_serial_stream():
+    """The restated loop's jitter: pixel by pixel, subsample (vv, uu) lies at
+    ((uu + ju) / S, (vv + jv) / S) with ju (uu != 0) then jv (vv != 0) taken
+    in order from the reference's TinyMT64 stream (seed 1234,
+    initialize_random's parameters) as floats.  Orthographic rays give the
+    sample positions back exactly enough to read the jitter off them."""
+    cam = {"eye": (0, 0, 3), "lookat": (0, 0, 0), "up": (0, 1, 0), "fov": 0.0,
+           "ortho": 1, "width": 8, "height": 4, "viewport": (0, 0, 8, 4),
+           "region": (0, 0, 8, 4), "step": 1}
+    S = 3
+    rays, pix = O.camera_rays_ex(cam, S, offset=5)
+    D = 2 * S * (S - 1)
+    draws = O.tinymt64_doubles(5 + 32 * D, seed=1234, use_ref=True)[5:].astype(np.float32)
+    rays0, _ = O.camera_rays_ex(cam, 1)
+    corner, u, v = O.camera_frame(*[cam[k] for k in ("eye", "lookat", "up", "fov", "ortho",
+                                                     "width", "height")])
+    k = 0
+    for q in range(32):
+        for vv in range(S):
+            for uu in range(S):
+                ju = draws[k] if uu else np.float32(0)
+                k += 1 if uu else 0
+                jv = draws[k] if vv else np.float32(0)
+                k += 1 if vv else 0
+                r = rays[q * S * S + vv * S + uu]
+                su = np.float32(np.float32(uu) + ju) / np.float32(S)
+                sv = np.float32(np.float32(vv) + jv) / np.float32(S)
+                # offset from the pixel's first sample, along u and v
+                off = r["org"].astype(np.float64) - rays[q * S * S]["org"].astype(np.float64)
+                assert abs(off @ u / (u @ u) - su) < 1e-3
+                assert abs(off @ v / (v @ v) - sv) < 1e-3
+    assert k == 32 * D
+
+
 def test_camera_rays_restatement_properties():
     """Eye rays of the restated OnData loop: unit directions, the pinhole
     rays pass through the eye, the viewport offset shifts pixels."""
