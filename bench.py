@@ -197,6 +197,18 @@ def algorithmic_bytes_per_ray(kind, stats, nrays):
 
 
 # ---------------------------------------------------------------- clocks
+def e2e_warmup(step, args, min_steps=10, min_s=0.25):
+    """Untimed end-to-end steps before the timed ones: at least the bench's
+    warm-up count, `min_steps` and `min_s` seconds -- the first host-driven
+    steps after the device-timed loop run well above the steady state (host
+    allocations and the clock sampler's exit just before them)."""
+    t_end = time.perf_counter() + min_s
+    k = 0
+    while k < max(args.warmup, 3, min_steps) or time.perf_counter() < t_end:
+        step()
+        k += 1
+
+
 class ClockSampler:
     def __init__(self, device):
         self.proc = None
@@ -718,8 +730,7 @@ def run_volume(args, W):
         h_gt.copy_(gt, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()
@@ -839,8 +850,7 @@ def run_texture(args, W):
         h_out.copy_(out, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         torch.cuda.synchronize()
@@ -957,8 +967,7 @@ def run_lines(args, W):
         h_nrm.copy_(nrm, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()
@@ -1089,8 +1098,7 @@ def run_solids(args, W):
         h_hits.copy_(hits, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()
@@ -1266,8 +1274,7 @@ def run_batched(args, W):
         h_h.copy_(hits, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()
@@ -1451,8 +1458,7 @@ def run_particles(args, W):
         torch.cuda.current_stream().synchronize()
         return c
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s, e2e_c = [], []
     for _ in range(args.steps):
         flush.zero_()
@@ -1597,8 +1603,7 @@ def run_frame(args, W):
         h_depth.copy_(depth, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()
@@ -1759,8 +1764,7 @@ def run_scene(args, W):
         h_depth.copy_(depth, non_blocking=True)
         torch.cuda.current_stream().synchronize()
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()
@@ -1941,8 +1945,7 @@ def run_ours(args, W):
         _lib.check(L.srt_trace_closest(e2e_acc, h_rays.data_ptr(), nr, h_hits.data_ptr(),
                                        C.byref(o)))
 
-    for _ in range(max(args.warmup, 3)):
-        e2e_step()
+    e2e_warmup(e2e_step, args)
     e2e_s = []
     for _ in range(args.steps):
         flush.zero_()

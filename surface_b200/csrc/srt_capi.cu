@@ -146,6 +146,15 @@ static srt_status build_common(srt_accel *a, const float *verts, size_t nverts,
     s = device_view(ctx, radius, nprims * sizeof(float), a->in_radius, &dr);
     if (s != SRT_OK) return s;
   }
+  if (dv != verts || (df && df != prims) || (dr && dr != radius)) {
+    // host inputs were copied: a ray array staged next (prestage_rays) waits
+    // for these copies, so the build's inputs cross the host link first
+    cudaError_t e = cudaSuccess;
+    if (!ctx->ev_inputs) e = cudaEventCreateWithFlags(&ctx->ev_inputs, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_inputs, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e, "input copy event");
+    ctx->inputs_pending = true;
+  }
   a->n = nprims;
   a->src_verts = static_cast<const float *>(dv);
   a->src_faces = static_cast<const uint32_t *>(df);
@@ -215,6 +224,7 @@ SRT_API srt_status srt_ctx_destroy(srt_ctx *c) {
   if (c->copy_stream) cudaStreamSynchronize(c->copy_stream);
   for (DevBuf *b : bufs) b->release();
   if (c->ev_copy) cudaEventDestroy(c->ev_copy);
+  if (c->ev_inputs) cudaEventDestroy(c->ev_inputs);
   if (c->ev_free) cudaEventDestroy(c->ev_free);
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   if (c->d_err) cudaFree(c->d_err);
@@ -591,6 +601,11 @@ static srt_status prestage_rays(srt_ctx *ctx, const srt_ray *rays, size_t n,
   if (ctx->ev_free_recorded &&
       (e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_free, 0)) != cudaSuccess)
     return cuda_status(e, "ray staging");
+  if (ctx->inputs_pending) {
+    if ((e = cudaStreamWaitEvent(ctx->copy_stream, ctx->ev_inputs, 0)) != cudaSuccess)
+      return cuda_status(e, "ray staging");
+    ctx->inputs_pending = false;
+  }
   if ((e = cudaMemcpyAsync(ctx->s_rays_in.p, rays, bytes, cudaMemcpyHostToDevice,
                            ctx->copy_stream)) != cudaSuccess ||
       (e = cudaEventRecord(ctx->ev_copy, ctx->copy_stream)) != cudaSuccess ||

@@ -176,6 +176,10 @@ struct srt_ctx {
       s_defer, s_spawn, s_rkey, s_rorder, s_isect_sub, s_stage_isect, s_keys3, s_vals3,
       s_status, s_lscan, s_rays_in, s_kidx, s_kprefix;
   uint32_t os_epoch = 0;  // look-back epoch of the last sort pass (srt_sort.cu)
+  // recorded after a build's host inputs were copied; the next staged ray
+  // array waits for it (inputs_pending)
+  cudaEvent_t ev_inputs = nullptr;
+  bool inputs_pending = false;
   // side stream that copies a page-locked host ray array to the device while
   // earlier work (a build) still runs on the context stream; ev_copy: copy
   // done, ev_free: the last trace that read s_rays_in is done

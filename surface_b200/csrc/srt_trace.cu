@@ -197,8 +197,11 @@ struct TetV {
 // Only the entering point's coordinate on the ray's first nonzero axis is
 // formed, (pe - o) * (1 / d) there as ComputeParametricDist does, the point
 // being the reference's ((1 - a - b) * P0 + a * P1) + b * P2.
-__device__ __forceinline__ bool ray_tet(const TetRay &R, const TetV &V, int &ef, double &ue1,
-                                        double &ue2, double &ul1, double &te) {
+// ul1 (the leaving face's barycentric, only a kept hit reports it) is formed
+// only when te < take_below.
+__device__ __forceinline__ bool ray_tet(const TetRay &R, const TetV &V, double take_below,
+                                        int &ef, double &ue1, double &ue2, double &ul1,
+                                        double &te) {
   const Plk &ray = R.ray;
   const double uAB = pdot(ray, plk(V[0], V[1])), uAC = pdot(ray, plk(V[0], V[2]));
   const double uAD = pdot(ray, plk(V[0], V[3])), uBC = pdot(ray, plk(V[1], V[2]));
@@ -249,7 +252,6 @@ __device__ __forceinline__ bool ray_tet(const TetRay &R, const TetV &V, int &ef,
   auto X = [&](int f) { return f == 3 ? -uAC : f == 2 ? uDB : f == 1 ? uAC : -uDB; };
   auto Y = [&](int f) { return f == 3 ? uAB : f == 2 ? -uAB : f == 1 ? -uDC : uDC; };
   const double inv_e = 1.0 / ((P(enter) + Q(enter)) - Rr(enter));
-  const double inv_l = 1.0 / ((P(leave) + Q(leave)) - Rr(leave));
   const double a = X(enter) * inv_e, b = Y(enter) * inv_e;
   // entering point's vertices (3 - f, f ^ 2, f ^ 1), coordinates on the axis
   const double c0 = V.axis(0, R.sel), c1 = V.axis(1, R.sel), c2 = V.axis(2, R.sel),
@@ -261,7 +263,8 @@ __device__ __forceinline__ bool ray_tet(const TetRay &R, const TetV &V, int &ef,
   ef = enter;
   ue1 = a;
   ue2 = b;
-  ul1 = X(leave) * inv_l;
+  ul1 = 0.0;
+  if (te < take_below) ul1 = X(leave) * (1.0 / ((P(leave) + Q(leave)) - Rr(leave)));
   return true;
 }
 
@@ -894,17 +897,18 @@ struct CtxT {
   uint32_t prev_prim;
 };
 
+// (ul1 is formed only for te < take_below: the candidates a caller keeps)
 __device__ __forceinline__ bool candT(const float4 *__restrict__ prims,
                                       const uint32_t *__restrict__ sidx, uint32_t j,
-                                      const CtxT &c, uint32_t &f, int &ef, double &e1,
-                                      double &e2, double &ul1, double &te) {
+                                      const CtxT &c, double take_below, uint32_t &f, int &ef,
+                                      double &e1, double &e2, double &ul1, double &te) {
   f = __ldg(&sidx[j]);
   if (f == c.prev_prim) return false;
   const float4 q0 = __ldg(&prims[3 * (size_t)j]);
   const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
   const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
   const TetV V = {{q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
-  return ray_tet(c.tr, V, ef, e1, e2, ul1, te) && te >= 0.0;
+  return ray_tet(c.tr, V, take_below, ef, e1, e2, ul1, te) && te >= 0.0;
 }
 
 __device__ __forceinline__ void take_tet(Best &b, double te, double e1, double e2,
@@ -954,7 +958,7 @@ __device__ void walkT(const NodeT *__restrict__ nodes, const float4 *__restrict_
       uint32_t f;
       int ef;
       double e1, e2, ul1, te;
-      if (!candT(prims, sidx, j, c, f, ef, e1, e2, ul1, te)) continue;
+      if (!candT(prims, sidx, j, c, (double)t, f, ef, e1, e2, ul1, te)) continue;
       if (WINDOW && !(te <= whi)) continue;
       if (te < (double)t) {
         take_tet(b, te, e1, e2, ul1, f, ef);
@@ -1046,7 +1050,7 @@ struct TetPass1 {
       uint32_t f;
       int ef;
       double e1, e2, ul1, te;
-      if (!candT(prims, sidx, j, c, f, ef, e1, e2, ul1, te)) continue;
+      if (!candT(prims, sidx, j, c, m, f, ef, e1, e2, ul1, te)) continue;
       const bool below = below_entry(te, lt);
       if (te < m) {
         m2 = m;
