@@ -722,6 +722,18 @@ SRT_API srt_status srt_solid_info(srt_solid_accel *accel, uint64_t *nsolids, uin
 SRT_API srt_status srt_solid_export(srt_solid_accel *accel, void *nodes, uint32_t *indices);
 SRT_API srt_status srt_solid_dump(srt_solid_accel *accel, const char *path);
 
+/* Line and solid accels as scene elements: RenderGraph::Trace's
+ * PRIMITIVE_LINES and PRIMITIVE_PYRAMIDS / PRISMS / HEXAHEDRONS cases
+ * (gles/gles_render_graph.cc:239-260), added as srt_scene_add_element adds
+ * an srt_accel (local box = srt_line_bbox / srt_solid_bbox, RenderElement's
+ * world box and inverse matrices).  A hit on a line element carries the
+ * line's (u, v); on a solid element u = v = 0, and the previous solid is
+ * skipped inside the element the ray left (prev_element). */
+SRT_API srt_status srt_scene_add_lines(srt_scene *scene, srt_line_accel *accel,
+                                       const double T[16], uint32_t *id);
+SRT_API srt_status srt_scene_add_solids(srt_scene *scene, srt_solid_accel *accel,
+                                        const double T[16], uint32_t *id);
+
 #ifdef __cplusplus
 }
 #endif

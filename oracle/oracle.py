@@ -122,6 +122,8 @@ def lib():
         L.so_scene_build.restype = _P
         L.so_scene_build.argtypes = [_P, _P, _P, _P, _P, _P, _SZ]
         L.so_scene_free.argtypes = [_P]
+        L.so_scene_set_kind.restype = None
+        L.so_scene_set_kind.argtypes = [_P, _SZ, C.c_int]
         L.so_scene_top_nodes.restype = _SZ
         L.so_scene_top_nodes.argtypes = [_P, _P, _P, _SZ]
         L.so_scene_candidates.restype = _SZ
@@ -887,8 +889,8 @@ class RefTopTree:
 
 class OracleScene:
     """RenderGraph::Build / Trace restated (so_scene_*): elements are
-    OracleAccel objects with their transforms (4x4 row-major doubles as
-    Matrixd's m[row][col]) and world boxes."""
+    OracleAccel, OracleLines or OracleSolids objects with their transforms
+    (4x4 row-major doubles as Matrixd's m[row][col]) and world boxes."""
 
     def __init__(self, accels, T, invT, invT33, bmin, bmax):
         self.accels = list(accels)  # None entries: top-level tree only
@@ -901,6 +903,9 @@ class OracleScene:
         hs = (C.c_void_p * n)(*[None if a is None else a.h for a in self.accels])
         self.h = lib().so_scene_build(hs, _ptr(self._T), _ptr(self._iT), _ptr(self._iT33),
                                       _ptr(self._bmin), _ptr(self._bmax), n)
+        for e, a in enumerate(self.accels):
+            if isinstance(a, (OracleLines, OracleSolids)):
+                lib().so_scene_set_kind(self.h, e, 3 if isinstance(a, OracleLines) else 4)
         self.cap = 2 * n + 2
 
     def nodes(self):

@@ -2421,10 +2421,16 @@ typedef struct {
 
 typedef struct {
   size_t n, nn, cap;
-  const so_accel **acc;
+  const so_accel **acc; /* per element: so_accel, or so_lines / so_solids (kind) */
+  int *kind;            /* 0: so_accel; 3: so_lines; 4: so_solids */
   double *T, *invT, *invT33;
   so_top *nodes;
 } so_scene;
+
+/* The closest hit of a local ray in a line (kind 3) or solid (kind 4)
+ * element: LineAccel::Traverse / SolidAccel::Traverse, defined with them
+ * below. */
+static void scene_other_trace(int kind, const void *obj, const so_ray *lr, so_hit *h);
 
 static size_t top_partition(so_topdata *d, size_t l, size_t r, double pos, int axis) {
   so_topdata leftmost = d[l];
@@ -2542,6 +2548,7 @@ SO_API so_scene *so_scene_build(const so_accel *const *acc, const double *T,
   s->T = (double *)malloc(n * 16 * sizeof(double));
   s->invT = (double *)malloc(n * 16 * sizeof(double));
   s->invT33 = (double *)malloc(n * 16 * sizeof(double));
+  s->kind = (int *)calloc(n ? n : 1, sizeof(int));
   memcpy(s->acc, acc, n * sizeof(*s->acc));
   memcpy(s->T, T, n * 16 * sizeof(double));
   memcpy(s->invT, invT, n * 16 * sizeof(double));
@@ -2562,8 +2569,16 @@ SO_API so_scene *so_scene_build(const so_accel *const *acc, const double *T,
   return s;
 }
 
+/* Element e is a line (3) or solid (4) accel: acc[e] holds an so_lines /
+ * so_solids (RenderGraph::Trace's PRIMITIVE_LINES and solid cases,
+ * gles/gles_render_graph.cc:239-260). */
+SO_API void so_scene_set_kind(so_scene *s, size_t e, int kind) {
+  if (s && e < s->n) s->kind[e] = kind;
+}
+
 SO_API void so_scene_free(so_scene *s) {
   if (!s) return;
+  free(s->kind);
   free(s->acc);
   free(s->T);
   free(s->invT);
@@ -2706,7 +2721,9 @@ SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
       const float *pn = (same && prev_normals) ? &prev_normals[3 * i] : zero3;
       so_hit h;
       so_stats st = {0, 0, 0};
-      if (walk2) {
+      if (s->kind[e] != 0) {
+        scene_other_trace(s->kind[e], s->acc[e], &lr, &h);
+      } else if (walk2) {
         int fall = 0;
         trace2_one(s->acc[e], &lr, pn, &h, NULL, NULL, NULL, &st, &fall);
       } else {
@@ -2714,7 +2731,7 @@ SO_API void so_scene_trace(const so_scene *s, const so_ray *rays, size_t n,
       }
       nvis += st.branch_visits + st.prim_tests;
       if (h.prim == 0xffffffffu || !(h.t < FLT_MAX)) continue;
-      sphere_finish(s->acc[e], &lr, &h); /* the element's Traverse, local ray */
+      if (s->kind[e] == 0) sphere_finish(s->acc[e], &lr, &h); /* the element's Traverse */
       double lp[3], wp[3];
       for (int k = 0; k < 3; k++) lp[k] = (double)(float)(lo[k] + (double)h.t * ld[k]);
       scene_multv(&s->T[16 * e], lp, wp);
@@ -3784,4 +3801,11 @@ SO_API void so_solid_trace(const so_solids *S, const so_ray *rays, size_t n, so_
   for (long long i = 0; i < (long long)n; i++)
     solid_trace_one(S, &rays[i], &hits[i], normals ? &normals[3 * i] : NULL,
                     positions ? &positions[3 * i] : NULL);
+}
+
+static void scene_other_trace(int kind, const void *obj, const so_ray *lr, so_hit *h) {
+  if (kind == 3)
+    line_trace_one((const so_lines *)obj, lr, h, NULL);
+  else
+    solid_trace_one((const so_solids *)obj, lr, h, NULL, NULL);
 }

@@ -8,3 +8,5 @@ from .accel import (HIT_DTYPE, MISS, RAY_DTYPE, Context, Mesh, ParticleAccel,  #
                     ParticleBuildOptions, Particles, SurfaceError, Tetrahedron,
                     TetraAccel, TetraBuildOptions, TriangleAccel, TriangleBuildOptions,
                     spawn_secondary, stage_karras, stage_morton, stage_sort_pairs)
+from .lines import LineAccel, LineBuildOptions, Lines  # noqa: F401
+from .solids import Solid, SolidAccel  # noqa: F401

@@ -130,6 +130,8 @@ _SIGS = {
     "srt_scene_destroy": [_P],
     "srt_scene_add": [_P, _P, _P, _P, _P, _P, _P, _P],
     "srt_scene_add_element": [_P, _P, _P, _P],
+    "srt_scene_add_lines": [_P, _P, _P, _P],
+    "srt_scene_add_solids": [_P, _P, _P, _P],
     "srt_matrix_inverse": [_P],
     "srt_scene_build": [_P],
     "srt_scene_trace": [_P, _P, _SZ, _P, _P, _P, _P, _P],

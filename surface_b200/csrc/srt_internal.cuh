@@ -244,11 +244,16 @@ struct TopNode {
   uint32_t id;       // element of a leaf
   uint32_t pad;
 };
+// Scene element kinds beyond srt_kind: line and solid accels.
+constexpr int32_t kSceneLines = 3, kSceneSolids = 4;
 // One element of a scene: a built accel and its transforms, 4x4 doubles in
-// the reference's Matrixd layout (m[row][col], p' = p m + m[3]).
+// the reference's Matrixd layout (m[row][col], p' = p m + m[3]).  Line and
+// solid elements keep their device nodes in nodes and records in prims;
+// aux: the line accel's cap flag, the solid accel's vertices per solid.
 struct SceneElem {
   int32_t kind;
   uint32_t nprims;
+  int32_t aux;
   const void *nodes;
   const float4 *prims;
   const uint32_t *sidx;
@@ -277,7 +282,7 @@ struct SceneWork {
   const SceneElem *elems;
   const uint32_t *elem_rank;  // element id -> rank in kind order
   uint32_t nelem;
-  uint32_t rank_start[4];     // first rank of triangles, tetrahedra, spheres; nelem
+  uint32_t rank_start[4];     // first rank of triangles, tetrahedra, spheres, loop-only kinds
   const srt_ray *rays;
   const uint32_t *prev_element;
   const float *prev_normals;
@@ -309,9 +314,10 @@ struct SceneStreams {
 // the root, TopNode.id of a leaf is its box's index.
 void build_top_tree(const double *bmin, const double *bmax, size_t n,
                     std::vector<TopNode> &out);
-// kinds: bit k set when the scene holds elements of kind k.
+// kinds: bit k set when the scene holds elements of kind k; deep_lines: a
+// line element's tree is deeper than 62 levels.
 srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds,
-                              const SceneStreams &ss);
+                              bool deep_lines, const SceneStreams &ss);
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
 // array in context scratch, valid until the context's next sort.
 srt_status ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const uint32_t **order);
@@ -323,6 +329,11 @@ srt_status batch_ray_order(srt_ctx *ctx, const srt_ray *rays, size_t n, const ui
 // Device bytes held by a line or solid accel (srt_line.cu, srt_solid.cu).
 uint64_t line_accel_bytes(const srt_line_accel *a);
 uint64_t solid_accel_bytes(const srt_solid_accel *a);
+// A built line or solid accel as a scene element: its context, device
+// nodes and records, element count, aux (cap flag / vertices per solid)
+// and tree depth (lines).  False when the accel is not built.
+bool line_scene_view(const srt_line_accel *a, srt_ctx **ctx, SceneElem &e, int &depth);
+bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e);
 // Exclusive prefix sum of n uint32 on the context's stream (out may alias in).
 srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n);
 // Stable sort of (key, value) pairs by key; key_bits: how many low bits of

@@ -29,8 +29,11 @@
 #include <vector>
 
 #include "srt_internal.cuh"
+#include "srt_walks.cuh"
 
 namespace {
+
+using namespace srt_line_walk;
 
 // The reference's LineNode (Dump record, 40 bytes).
 struct LineNodeH {
@@ -39,31 +42,6 @@ struct LineNodeH {
   uint32_t data[2];
 };
 static_assert(sizeof(LineNodeH) == 40, "LineNode layout");
-
-// Device node: w1 bit 31 set for a leaf (w0 = first record, the low bits = count),
-// else w0 = left child, w1 = right child | axis << 29.
-struct alignas(16) LNode {
-  float bmin[3];
-  uint32_t w0;
-  float bmax[3];
-  uint32_t w1;
-};
-static_assert(sizeof(LNode) == 32, "two 16-byte loads");
-
-// One line in leaf order: the terms of CylinderIsect that do not depend on
-// the ray.  dn0 = normalize(p0 - p1); p0D = -dot(p0, dn0); p1D = -dot(p1, -dn0).
-struct alignas(16) LineRec {
-  float p0[3], rr;
-  float p1[3], dd;
-  float dn0[3], p0D;
-  float p1D;
-  uint32_t prim;
-  float pad[2];
-};
-static_assert(sizeof(LineRec) == 64, "four 16-byte loads");
-
-constexpr uint32_t kLineLeaf = 0x80000000u;
-constexpr float kCapEps = 1.0e-6f;  // the file-level kEPS of render_accel_line.cc
 
 }  // namespace
 
@@ -253,25 +231,6 @@ void build_par(const std::vector<float> &box, const std::vector<float> &mid,
 }
 
 // ------------------------------------------------------------------ device
-__device__ __forceinline__ float dot3(const float a[3], const float b[3]) {
-  return a[0] * b[0] + a[1] * b[1] + a[2] * b[2];
-}
-
-// vnormalize (:439-454): (float)sqrt((double)x) is the float sqrt and
-// (float)(1.0 / (double)len) the float reciprocal, both correctly rounded.
-__device__ __forceinline__ void normalize3(const float a[3], float out[3]) {
-  const float len = __fsqrt_rn(dot3(a, a));
-  out[0] = a[0];
-  out[1] = a[1];
-  out[2] = a[2];
-  if (len > FLT_EPSILON * 16.0f) {
-    const float inv = __frcp_rn(len);
-    out[0] *= inv;
-    out[1] *= inv;
-    out[2] *= inv;
-  }
-}
-
 __global__ void line_rec_kernel(const float *__restrict__ pos, const float *__restrict__ rad,
                                 float constr, const uint32_t *__restrict__ seg,
                                 const uint32_t *__restrict__ order, size_t n,
@@ -301,139 +260,6 @@ __global__ void line_rec_kernel(const float *__restrict__ pos, const float *__re
   }
 }
 
-__device__ __forceinline__ LineRec load_line(const LineRec *p) {
-  const float4 *q = reinterpret_cast<const float4 *>(p);
-  const float4 a = __ldg(q), b = __ldg(q + 1), c = __ldg(q + 2), d = __ldg(q + 3);
-  LineRec r;
-  r.p0[0] = a.x;
-  r.p0[1] = a.y;
-  r.p0[2] = a.z;
-  r.rr = a.w;
-  r.p1[0] = b.x;
-  r.p1[1] = b.y;
-  r.p1[2] = b.z;
-  r.dd = b.w;
-  r.dn0[0] = c.x;
-  r.dn0[1] = c.y;
-  r.dn0[2] = c.z;
-  r.p0D = c.w;
-  r.p1D = d.x;
-  r.prim = __float_as_uint(d.y);
-  return r;
-}
-
-struct RayL {
-  float org[3], dir[3], rd[3], inv[3], nn;
-  int sign[3];
-};
-
-// CylinderIsect (:488-577) for one line record; *pt is the closest hit so
-// far (updated on a hit, as the reference does through its pointer).
-__device__ __forceinline__ bool cyl_isect(const LineRec &L, const RayL &R, bool cap, float *pt,
-                                          float *pu, float *pv, bool &hit_cap) {
-  const float tmax = *pt;
-  float d[3], m[3];
-  for (int k = 0; k < 3; k++) {
-    d[k] = L.p1[k] - L.p0[k];
-    m[k] = R.org[k] - L.p0[k];
-  }
-  const float md = dot3(m, d), nd = dot3(R.dir, d), dd = L.dd, rr = L.rr;
-  hit_cap = false;
-  float capT = FLT_MAX;
-  if (cap && fabsf(dot3(R.dir, L.dn0)) > kCapEps) {
-    const float dn1[3] = {-L.dn0[0], -L.dn0[1], -L.dn0[2]};
-    const float p0T = -(dot3(R.org, L.dn0) + L.p0D) / dot3(R.rd, L.dn0);
-    const float p1T = -(dot3(R.org, dn1) + L.p1D) / dot3(R.rd, dn1);
-    float a0[3], a1[3];
-    for (int k = 0; k < 3; k++) {
-      a0[k] = (R.org[k] + R.rd[k] * p0T) - L.p0[k];
-      a1[k] = (R.org[k] + R.rd[k] * p1T) - L.p1[k];
-    }
-    const float s0 = dot3(a0, a0), s1 = dot3(a1, a1);
-    if (p0T > 0.0f && p0T < tmax && s0 < rr * rr) {
-      hit_cap = true;
-      capT = p0T;
-      *pt = capT;
-      *pu = __fsqrt_rn(s0);
-      *pv = 0.0f;
-    }
-    if (p1T > 0.0f && p1T < tmax && p1T < capT && s1 < rr * rr) {
-      hit_cap = true;
-      capT = p1T;
-      *pt = capT;
-      *pu = __fsqrt_rn(s1);
-      *pv = 1.0f;
-    }
-  }
-  if (md <= 0.0f && nd <= 0.0f) return hit_cap;
-  if (md >= dd && nd >= 0.0f) return hit_cap;
-  const float mn = dot3(m, R.dir);
-  const float A = dd * R.nn - nd * nd;
-  const float kk = dot3(m, m) - rr * rr;
-  const float C = dd * kk - md * md;
-  const float B = dd * mn - nd * md;
-  // solve2e (:456-486), the smaller root
-  float t;
-  if (fabsf(A) <= FLT_EPSILON) {
-    t = -C / B;
-  } else {
-    const float D = B * B - A * C;
-    if (D < 0.0f) return hit_cap;
-    if (D == 0.0f) {
-      t = -B / A;
-    } else {
-      float x1 = (float)(((double)fabsf(B) + sqrt((double)D)) / (double)A);
-      if (B >= 0.0f) x1 = -x1;
-      const float x2 = C / (A * x1);
-      t = x1 > x2 ? x2 : x1;
-    }
-  }
-  if (0.0f <= t && t <= tmax && t <= capT) {
-    float s = md + t * nd;
-    s /= dd;
-    if (0.0f <= s && s <= 1.0f) {
-      hit_cap = false;
-      *pt = t;
-      *pu = 0.0f;
-      *pv = s;
-      return true;
-    }
-  }
-  return hit_cap;
-}
-
-// IntersectRayAABB (:377-420) with the reference's selection order.
-__device__ __forceinline__ bool box_hit(const LNode &nd, const RayL &R, float maxT) {
-  float lo[3], hi[3];
-  for (int k = 0; k < 3; k++) {
-    lo[k] = R.sign[k] ? nd.bmax[k] : nd.bmin[k];
-    hi[k] = R.sign[k] ? nd.bmin[k] : nd.bmax[k];
-  }
-  const float tx0 = (lo[0] - R.org[0]) * R.inv[0], tx1 = (hi[0] - R.org[0]) * R.inv[0];
-  const float ty0 = (lo[1] - R.org[1]) * R.inv[1], ty1 = (hi[1] - R.org[1]) * R.inv[1];
-  float tmin = (tx0 > ty0) ? tx0 : ty0;
-  float tmax = (tx1 < ty1) ? tx1 : ty1;
-  const float tz0 = (lo[2] - R.org[2]) * R.inv[2], tz1 = (hi[2] - R.org[2]) * R.inv[2];
-  tmin = (tmin > tz0) ? tmin : tz0;
-  tmax = (tmax < tz1) ? tmax : tz1;
-  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= maxT);
-}
-
-__device__ __forceinline__ LNode load_node(const LNode *p) {
-  const float4 *q = reinterpret_cast<const float4 *>(p);
-  const float4 a = __ldg(q), b = __ldg(q + 1);
-  LNode n;
-  n.bmin[0] = a.x;
-  n.bmin[1] = a.y;
-  n.bmin[2] = a.z;
-  n.w0 = __float_as_uint(a.w);
-  n.bmax[0] = b.x;
-  n.bmax[1] = b.y;
-  n.bmax[2] = b.z;
-  n.w1 = __float_as_uint(b.w);
-  return n;
-}
-
 // One thread per ray (grid-strided).  order (may be null): thread k traces
 // ray order[k].  STATS: count popped branches, popped leaves and line tests
 // into stats[0..2].
@@ -449,61 +275,12 @@ line_trace_kernel(const LNode *__restrict__ nodes, const LineRec *__restrict__ r
     const size_t i = order ? (size_t)__ldg(&order[k]) : k;
     const float4 *rq = reinterpret_cast<const float4 *>(rays + i);
     const float4 r0 = __ldg(rq), r1 = __ldg(rq + 1);
-    RayL R;
-    R.org[0] = r0.x;
-    R.org[1] = r0.y;
-    R.org[2] = r0.z;
-    R.dir[0] = r1.x;
-    R.dir[1] = r1.y;
-    R.dir[2] = r1.z;
-    for (int k = 0; k < 3; k++) {
-      R.sign[k] = R.dir[k] < 0.0f ? 1 : 0;
-      R.inv[k] = __frcp_rn(R.dir[k]);  // (float)(1.0 / dir), correctly rounded
-    }
-    normalize3(R.dir, R.rd);
-    R.nn = dot3(R.dir, R.dir);
-    float hitT = FLT_MAX, it = FLT_MAX, iu = 0.0f, iv = 0.0f;
-    bool icap = false;
-    int best = -1;
-    int stack[STACK];
-    int sp = 0;
-    stack[0] = 0;
-    while (sp >= 0) {
-      const LNode nd = load_node(nodes + stack[sp]);
-      sp--;
-      if (!(nd.w1 & kLineLeaf)) {
-        if (STATS) nb++;
-        if (box_hit(nd, R, hitT)) {
-          const int axis = (int)(nd.w1 >> 29);
-          const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
-          const int nearc = R.sign[axis];
-          stack[++sp] = nearc ? left : right;  // far
-          stack[++sp] = nearc ? right : left;  // near
-        }
-      } else {
-        float t = it;
-        bool any = false;
-        const uint32_t first = nd.w0, cnt = nd.w1 & ~kLineLeaf;
-        if (STATS) {
-          nl++;
-          nt += cnt;
-        }
-        for (uint32_t j = 0; j < cnt; j++) {
-          const LineRec L = load_line(recs + first + j);
-          float u, v;
-          bool hc;
-          if (cyl_isect(L, R, cap, &t, &u, &v, hc)) {
-            it = t;
-            iu = u;
-            iv = v;
-            icap = hc;
-            best = (int)(first + j);
-            any = true;
-          }
-        }
-        if (any) hitT = it;
-      }
-    }
+    const float ro[3] = {r0.x, r0.y, r0.z}, rdir[3] = {r1.x, r1.y, r1.z};
+    const RayL R = make_ray(ro, rdir);
+    const LineHit H = line_walk<STACK, STATS>(nodes, recs, cap, R, nb, nl, nt);
+    const float it = H.t, iu = H.u, iv = H.v;
+    const bool icap = H.cap;
+    const int best = H.rec;
     srt_hit h;
     if (it < FLT_MAX) {
       const LineRec L = load_line(recs + best);
@@ -584,6 +361,19 @@ srt_status host_copy(const T *p, size_t count, std::vector<T> &buf, const T **ou
 
 namespace srt {
 uint64_t line_accel_bytes(const srt_line_accel *a) { return a->dnodes.cap + a->drecs.cap; }
+bool line_scene_view(const srt_line_accel *a, srt_ctx **ctx, SceneElem &e, int &depth) {
+  if (!a || !a->built) return false;
+  *ctx = a->ctx;
+  e.kind = kSceneLines;
+  e.nprims = (uint32_t)a->nlines;
+  e.aux = a->cap;
+  e.nodes = a->dnodes.p;
+  e.prims = a->drecs.as<float4>();
+  e.sidx = nullptr;
+  e.scene = nullptr;
+  depth = a->depth;
+  return true;
+}
 }  // namespace srt
 
 using namespace srt;

@@ -20,7 +20,9 @@ using namespace srt;
 struct srt_scene {
   srt_ctx *ctx = nullptr;
   struct Elem {
-    srt_accel *acc;
+    srt_accel *acc = nullptr;  // or one of:
+    srt_line_accel *lines = nullptr;
+    srt_solid_accel *solids = nullptr;
     double T[16], invT[16], invT33[16], bmin[3], bmax[3];
   };
   std::vector<Elem> elems;
@@ -29,7 +31,8 @@ struct srt_scene {
   bool built = false;
   uint32_t max_iter = 64;
   uint32_t kinds = 0;          // bit k: the scene holds elements of kind k
-  uint32_t rank_start[4] = {};  // first rank of each kind (kind order), count
+  uint32_t rank_start[4] = {};  // first rank of triangles, tetrahedra, spheres, lines + solids
+  bool deep_lines = false;      // a line element deeper than the loop's short stack
   SceneStreams ss;
   ~srt_scene() {
     for (cudaStream_t &q : ss.side)
@@ -290,20 +293,15 @@ SRT_API srt_status srt_scene_destroy(srt_scene *s) {
   return SRT_OK;
 }
 
-SRT_API srt_status srt_scene_add(srt_scene *s, srt_accel *acc, const double T[16],
-                                 const double invT[16], const double invT33[16],
-                                 const double world_bmin[3], const double world_bmax[3],
-                                 uint32_t *id) {
-  if (!s || !acc || !T || !invT || !invT33 || !world_bmin || !world_bmax) {
-    set_error("NULL argument");
-    return SRT_ERR_INVALID;
-  }
-  if (!acc->built || acc->ctx != s->ctx) {
-    set_error("scene elements must be built accels of the scene's context");
-    return SRT_ERR_INVALID;
-  }
-  srt_scene::Elem e;
-  e.acc = acc;
+}  // extern "C"
+
+namespace {
+
+// Appends element e (its accel pointer set) with the caller's matrices and
+// world box.
+srt_status scene_push(srt_scene *s, srt_scene::Elem e, const double T[16], const double invT[16],
+                      const double invT33[16], const double world_bmin[3],
+                      const double world_bmax[3], uint32_t *id) {
   for (int k = 0; k < 16; k++) {
     e.T[k] = T[k];
     e.invT[k] = invT[k];
@@ -319,18 +317,92 @@ SRT_API srt_status srt_scene_add(srt_scene *s, srt_accel *acc, const double T[16
   return SRT_OK;
 }
 
+// RenderElement's constructor for an element with local box lbmin / lbmax.
+srt_status scene_push_update(srt_scene *s, const srt_scene::Elem &e, const double T[16],
+                             const double lbmin[3], const double lbmax[3], uint32_t *id) {
+  double invT[16], invT33[16], wbmin[3], wbmax[3];
+  element_update(T, lbmin, lbmax, invT, invT33, wbmin, wbmax);
+  return scene_push(s, e, T, invT, invT33, wbmin, wbmax, id);
+}
+
+}  // namespace
+
+extern "C" {
+
+SRT_API srt_status srt_scene_add(srt_scene *s, srt_accel *acc, const double T[16],
+                                 const double invT[16], const double invT33[16],
+                                 const double world_bmin[3], const double world_bmax[3],
+                                 uint32_t *id) {
+  if (!s || !acc || !T || !invT || !invT33 || !world_bmin || !world_bmax) {
+    set_error("NULL argument");
+    return SRT_ERR_INVALID;
+  }
+  if (!acc->built || acc->ctx != s->ctx) {
+    set_error("scene elements must be built accels of the scene's context");
+    return SRT_ERR_INVALID;
+  }
+  srt_scene::Elem e;
+  e.acc = acc;
+  return scene_push(s, e, T, invT, invT33, world_bmin, world_bmax, id);
+}
+
 SRT_API srt_status srt_scene_add_element(srt_scene *s, srt_accel *acc, const double T[16],
                                          uint32_t *id) {
   if (!s || !acc || !T) {
     set_error("NULL argument");
     return SRT_ERR_INVALID;
   }
+  if (!acc->built || acc->ctx != s->ctx) {
+    set_error("scene elements must be built accels of the scene's context");
+    return SRT_ERR_INVALID;
+  }
   double lbmin[3], lbmax[3];
   srt_status st = srt_accel_bbox(acc, lbmin, lbmax);
   if (st != SRT_OK) return st;
-  double invT[16], invT33[16], wbmin[3], wbmax[3];
-  element_update(T, lbmin, lbmax, invT, invT33, wbmin, wbmax);
-  return srt_scene_add(s, acc, T, invT, invT33, wbmin, wbmax, id);
+  srt_scene::Elem e;
+  e.acc = acc;
+  return scene_push_update(s, e, T, lbmin, lbmax, id);
+}
+
+SRT_API srt_status srt_scene_add_lines(srt_scene *s, srt_line_accel *acc, const double T[16],
+                                       uint32_t *id) {
+  if (!s || !acc || !T) {
+    set_error("NULL argument");
+    return SRT_ERR_INVALID;
+  }
+  srt_ctx *c = nullptr;
+  SceneElem v{};
+  int depth = 0;
+  if (!line_scene_view(acc, &c, v, depth) || c != s->ctx) {
+    set_error("scene elements must be built accels of the scene's context");
+    return SRT_ERR_INVALID;
+  }
+  double lbmin[3], lbmax[3];
+  srt_status st = srt_line_bbox(acc, lbmin, lbmax);
+  if (st != SRT_OK) return st;
+  srt_scene::Elem e;
+  e.lines = acc;
+  return scene_push_update(s, e, T, lbmin, lbmax, id);
+}
+
+SRT_API srt_status srt_scene_add_solids(srt_scene *s, srt_solid_accel *acc, const double T[16],
+                                        uint32_t *id) {
+  if (!s || !acc || !T) {
+    set_error("NULL argument");
+    return SRT_ERR_INVALID;
+  }
+  srt_ctx *c = nullptr;
+  SceneElem v{};
+  if (!solid_scene_view(acc, &c, v) || c != s->ctx) {
+    set_error("scene elements must be built accels of the scene's context");
+    return SRT_ERR_INVALID;
+  }
+  double lbmin[3], lbmax[3];
+  srt_status st = srt_solid_bbox(acc, lbmin, lbmax);
+  if (st != SRT_OK) return st;
+  srt_scene::Elem e;
+  e.solids = acc;
+  return scene_push_update(s, e, T, lbmin, lbmax, id);
 }
 
 SRT_API srt_status srt_scene_build(srt_scene *s) {
@@ -349,39 +421,53 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
   std::vector<SceneElem> el(s->elems.size());
   size_t total = 0;
   uint32_t kinds = 0;
+  bool deep = false;
   for (size_t i = 0; i < el.size(); i++) {
-    const srt_accel *a = s->elems[i].acc;
-    if (!a->built) {
+    const srt_scene::Elem &se = s->elems[i];
+    srt_ctx *c = nullptr;
+    bool ok;
+    if (se.lines) {
+      int depth = 0;
+      ok = line_scene_view(se.lines, &c, el[i], depth);
+      deep = deep || depth + 2 > 64;
+    } else if (se.solids) {
+      ok = solid_scene_view(se.solids, &c, el[i]);
+    } else {
+      const srt_accel *a = se.acc;
+      ok = a->built;
+      el[i].kind = a->kind;
+      el[i].nprims = (uint32_t)a->n;
+      el[i].aux = 0;
+      el[i].nodes = a->nodes.p;
+      el[i].prims = a->prims.as<float4>();
+      el[i].sidx = a->indices.as<uint32_t>();
+      el[i].scene = a->scene.as<SceneInfo>();
+    }
+    if (!ok) {
       set_error("scene element not built");
       return SRT_ERR_INVALID;
     }
-    el[i].kind = a->kind;
-    el[i].nprims = (uint32_t)a->n;
-    el[i].nodes = a->nodes.p;
-    el[i].prims = a->prims.as<float4>();
-    el[i].sidx = a->indices.as<uint32_t>();
-    el[i].scene = a->scene.as<SceneInfo>();
     for (int k = 0; k < 16; k++) {
       el[i].T[k] = s->elems[i].T[k];
       el[i].invT[k] = s->elems[i].invT[k];
       el[i].invT33[k] = s->elems[i].invT33[k];
     }
-    total += a->n;
-    kinds |= 1u << a->kind;
+    total += el[i].nprims;
+    kinds |= 1u << el[i].kind;
   }
   cudaSetDevice(s->ctx->device);
   cudaError_t e;
-  // element ranks: ids grouped by kind (triangles, tetrahedra, spheres),
-  // each group in id order -- the trace sorts its items by rank, so each
-  // kind's items form one range
+  // element ranks: ids grouped by kind (triangles, tetrahedra, spheres,
+  // then lines and solids), each group in id order -- the trace sorts its
+  // items by rank, so each kind's items form one range; lines and solids
+  // (ranks from rank_start[3] on) are walked by the per-ray loop only
   std::vector<uint32_t> rank(el.size());
   uint32_t r = 0;
-  for (int k = 0; k < 3; k++) {
-    s->rank_start[k] = r;
+  for (int k = 0; k < 5; k++) {
+    if (k < 4) s->rank_start[k] = r;
     for (size_t i = 0; i < el.size(); i++)
       if (el[i].kind == k) rank[i] = r++;
   }
-  s->rank_start[3] = r;
   if (r != el.size()) {
     set_error("scene element of unknown kind");
     return SRT_ERR_INVALID;
@@ -403,6 +489,7 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
   if (e != cudaSuccess) return cuda_status(e, "scene upload");
   s->max_iter = (uint32_t)std::min<size_t>(8 * total + 64 + 8 * s->top.size(), 0xfffffff0u);
   s->kinds = kinds;
+  s->deep_lines = deep;
   s->built = true;
   return SRT_OK;
 }
@@ -503,7 +590,7 @@ SRT_API srt_status srt_scene_trace(srt_scene *s, const srt_ray *rays, size_t n,
   W.max_iter = s->max_iter;
   W.stats = reinterpret_cast<unsigned long long *>(stats);
   W.err = ctx->d_err;
-  return launch_scene_trace(ctx, s->d_top.as<TopNode>(), W, s->kinds, s->ss);
+  return launch_scene_trace(ctx, s->d_top.as<TopNode>(), W, s->kinds, s->deep_lines, s->ss);
 }
 
 }  // extern "C"

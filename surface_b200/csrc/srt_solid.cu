@@ -32,8 +32,11 @@
 #include <vector>
 
 #include "srt_internal.cuh"
+#include "srt_walks.cuh"
 
 namespace {
+
+using namespace srt_solid_walk;
 
 // The reference's SolidNode (Dump record, 40 bytes).
 struct SolidNodeH {
@@ -42,21 +45,6 @@ struct SolidNodeH {
   uint32_t data[2];
 };
 static_assert(sizeof(SolidNodeH) == 40, "SolidNode layout");
-
-// Device node: w1 bit 31 set for a leaf (w0 = first record, low bits = count),
-// else w0 = left child, w1 = right child | axis << 29.
-struct alignas(16) SNode {
-  float bmin[3];
-  uint32_t w0;
-  float bmax[3];
-  uint32_t w1;
-};
-static_assert(sizeof(SNode) == 32, "two 16-byte loads");
-
-constexpr uint32_t kSolidLeaf = 0x80000000u;
-
-// floats per record: nv vertices (xyz) and the solid's index, padded to 16 bytes
-__host__ __device__ constexpr int rec_floats(int nv) { return ((3 * nv + 1) + 3) / 4 * 4; }
 
 }  // namespace
 
@@ -230,314 +218,6 @@ struct Topology {
 };
 
 // ------------------------------------------------------------------ trace
-struct D3 {
-  double x, y, z;
-};
-__device__ __forceinline__ D3 dsub(D3 a, D3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
-__device__ __forceinline__ D3 dadd(D3 a, D3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
-__device__ __forceinline__ D3 dscale(D3 a, double f) { return {a.x * f, a.y * f, a.z * f}; }
-__device__ __forceinline__ D3 dcross(D3 a, D3 b) {
-  return {a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x};
-}
-__device__ __forceinline__ double ddot(D3 a, D3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-
-// normalize (:85), then to float
-__device__ __forceinline__ void s_unit(D3 a, float out[3]) {
-  const double len = sqrt(a.x * a.x + a.y * a.y + a.z * a.z);
-  out[0] = (float)(a.x / len);
-  out[1] = (float)(a.y / len);
-  out[2] = (float)(a.z / len);
-}
-
-__device__ __forceinline__ double comp(D3 a, int j) { return j == 0 ? a.x : (j == 1 ? a.y : a.z); }
-
-// The crossing point of a face, every coordinate (FULL) or coordinate j
-// only (out[j]; the one a hit's t is measured along).
-// SetCrossPoint_Sq (double, :438-444): a quad face.
-template <bool FULL>
-__device__ __forceinline__ void s_quad(float out[3], int j, D3 v0, D3 v1, D3 v2, double ws0,
-                                       double ws1, double ws2, double ws3, D3 e2, D3 e3,
-                                       D3 dir) {
-  const double w = ws2 + ws3 + ddot(dcross(e2, e3), dir);
-  const double den = ws0 + ws1 + w;
-  if (FULL) {
-    const D3 p = dadd(dadd(dscale(v2, ws0), dscale(v0, ws1)), dscale(v1, w));
-    out[0] = (float)(p.x / den);
-    out[1] = (float)(p.y / den);
-    out[2] = (float)(p.z / den);
-  } else {
-    const double pj = (comp(v2, j) * ws0 + comp(v0, j) * ws1) + comp(v1, j) * w;
-    out[j] = (float)(pj / den);
-  }
-}
-
-// A triangle face: the weighted sum in double, then the float vector
-// divided by the float sum of the weights.
-template <bool FULL>
-__device__ __forceinline__ void s_tri(float out[3], int j, D3 a, double wa, D3 b, double wb,
-                                      D3 c, double wc, double den) {
-  const float f = (float)den;
-  if (FULL) {
-    const D3 p = dadd(dadd(dscale(a, wa), dscale(b, wb)), dscale(c, wc));
-    out[0] = (float)p.x / f;
-    out[1] = (float)p.y / f;
-    out[2] = (float)p.z / f;
-  } else {
-    out[j] = (float)((comp(a, j) * wa + comp(b, j) * wb) + comp(c, j) * wc) / f;
-  }
-}
-
-// Edges of each solid (GetEdges, :119-154): edge i = vertex hi[i] - vertex
-// lo[i]; the Pluecker moment of edge i uses vertex i % MOD (:470).
-template <int NV>
-struct SolidTab;
-template <>
-struct SolidTab<5> {
-  static constexpr int NE = 8, MOD = 4;
-  __device__ static int hi(int i) {
-    constexpr int t[8] = {1, 2, 3, 0, 4, 4, 4, 4};
-    return t[i];
-  }
-  __device__ static int lo(int i) {
-    constexpr int t[8] = {0, 1, 2, 3, 0, 1, 2, 3};
-    return t[i];
-  }
-};
-template <>
-struct SolidTab<6> {
-  static constexpr int NE = 9, MOD = 6;
-  __device__ static int hi(int i) {
-    constexpr int t[9] = {1, 2, 0, 4, 5, 3, 3, 4, 5};
-    return t[i];
-  }
-  __device__ static int lo(int i) {
-    constexpr int t[9] = {0, 1, 2, 3, 4, 5, 0, 1, 2};
-    return t[i];
-  }
-};
-template <>
-struct SolidTab<8> {
-  static constexpr int NE = 12, MOD = 8;
-  __device__ static int hi(int i) {
-    constexpr int t[12] = {1, 2, 3, 0, 5, 6, 7, 4, 4, 5, 6, 7};
-    return t[i];
-  }
-  __device__ static int lo(int i) {
-    constexpr int t[12] = {0, 1, 2, 3, 4, 5, 6, 7, 0, 1, 2, 3};
-    return t[i];
-  }
-};
-
-// One solid's vertices (floats, exactly as stored) read as doubles on use;
-// edges are recomputed from them (the same double subtraction each time).
-template <int NV>
-struct SolidV {
-  float x[NV][3];
-  __device__ __forceinline__ D3 v(int k) const {
-    return {(double)x[k][0], (double)x[k][1], (double)x[k][2]};
-  }
-  __device__ __forceinline__ D3 e(int i) const {
-    return dsub(v(SolidTab<NV>::hi(i)), v(SolidTab<NV>::lo(i)));
-  }
-};
-
-// ws[i] = dir . (e_i x v_{i % MOD}) + e_i . (dir x org) (:467-476)
-template <int NV>
-__device__ __forceinline__ void s_weights(const SolidV<NV> &S, D3 dir, D3 org,
-                                          double (&ws)[SolidTab<NV>::NE]) {
-  const D3 rpc = dcross(dir, org);
-#pragma unroll
-  for (int i = 0; i < SolidTab<NV>::NE; i++) {
-    const D3 ei = S.e(i);
-    ws[i] = ddot(dir, dcross(ei, S.v(i % SolidTab<NV>::MOD))) + ddot(ei, rpc);
-  }
-}
-
-// The reference's Intersect{Pyramid,Prism,Hexa}D (:455-505, :559-611,
-// :664-716) split in two.  face(ws, slot): the face its sign tests pick for
-// crossing point `slot` (0 the first point, 1 the second; -1: the solid is
-// missed).  point<FULL>(S, ws, face, ...): that face's crossing point (all
-// of it and the face normal when FULL, else only coordinate j) by the same
-// expressions.  A ray tests every solid's two points for t and forms the
-// full point and normal only for a point that becomes its closest hit.
-__device__ __forceinline__ bool s_cw(const double *ws, int side, int k) {
-  return side == 0 ? ws[k] >= 0 : ws[k] <= 0;
-}
-
-template <int NV>
-struct SolidFaces;
-
-template <>
-struct SolidFaces<5> {  // IntersectPyramidD: point n uses i = 1 - n
-  __device__ static int face(const double (&ws)[8], int slot) {
-    const int n = slot, i = 1 - slot;
-    if (s_cw(ws, i, 0) && s_cw(ws, i, 1) && s_cw(ws, i, 2) && s_cw(ws, i, 3)) return 0;
-    if (s_cw(ws, n, 0) && s_cw(ws, i, 4) && s_cw(ws, n, 5)) return 1;
-    if (s_cw(ws, n, 1) && s_cw(ws, i, 5) && s_cw(ws, n, 6)) return 2;
-    if (s_cw(ws, n, 2) && s_cw(ws, i, 6) && s_cw(ws, n, 7)) return 3;
-    if (s_cw(ws, n, 3) && s_cw(ws, i, 7) && s_cw(ws, n, 4)) return 4;
-    return -1;
-  }
-  template <bool FULL>
-  __device__ static void point(const SolidV<5> &S, const double (&ws)[8], int f, D3 dir, int j,
-                               float pos[3], float nrm[3]) {
-    switch (f) {
-      case 0:
-        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3),
-                     dir);
-        if (FULL) s_unit(dcross(S.e(1), S.e(0)), nrm);
-        break;
-      case 1:
-        s_tri<FULL>(pos, j, S.v(4), -ws[0], S.v(1), ws[4], S.v(0), -ws[5], -ws[0] + ws[4] - ws[5]);
-        if (FULL) s_unit(dcross(S.e(4), S.e(0)), nrm);
-        break;
-      case 2:
-        s_tri<FULL>(pos, j, S.v(4), -ws[1], S.v(2), ws[5], S.v(1), -ws[6], -ws[1] + ws[5] - ws[6]);
-        if (FULL) s_unit(dcross(S.e(5), S.e(1)), nrm);
-        break;
-      case 3:
-        s_tri<FULL>(pos, j, S.v(4), -ws[2], S.v(3), ws[6], S.v(2), -ws[7], -ws[2] + ws[6] - ws[7]);
-        if (FULL) s_unit(dcross(S.e(6), S.e(2)), nrm);
-        break;
-      default:
-        s_tri<FULL>(pos, j, S.v(4), -ws[3], S.v(0), ws[7], S.v(3), -ws[4], -ws[3] + ws[7] - ws[4]);
-        if (FULL) s_unit(dcross(S.e(7), S.e(3)), nrm);
-        break;
-    }
-  }
-};
-
-template <>
-struct SolidFaces<6> {  // IntersectPrismD: point i uses n = 1 - i
-  __device__ static int face(const double (&ws)[9], int slot) {
-    const int i = slot, n = 1 - slot;
-    if (s_cw(ws, n, 0) && s_cw(ws, n, 1) && s_cw(ws, n, 2)) return 0;
-    if (s_cw(ws, i, 3) && s_cw(ws, i, 4) && s_cw(ws, i, 5)) return 1;
-    if (s_cw(ws, i, 2) && s_cw(ws, i, 6) && s_cw(ws, n, 5) && s_cw(ws, n, 8)) return 2;
-    if (s_cw(ws, i, 0) && s_cw(ws, i, 7) && s_cw(ws, n, 3) && s_cw(ws, n, 6)) return 3;
-    if (s_cw(ws, i, 1) && s_cw(ws, i, 8) && s_cw(ws, n, 4) && s_cw(ws, n, 7)) return 4;
-    return -1;
-  }
-  template <bool FULL>
-  __device__ static void point(const SolidV<6> &S, const double (&ws)[9], int f, D3 dir, int j,
-                               float pos[3], float nrm[3]) {
-    switch (f) {
-      case 0:
-        s_tri<FULL>(pos, j, S.v(2), ws[0], S.v(0), ws[1], S.v(1), ws[2], ws[0] + ws[1] + ws[2]);
-        if (FULL) s_unit(dcross(S.e(0), S.e(1)), nrm);
-        break;
-      case 1:
-        s_tri<FULL>(pos, j, S.v(5), ws[3], S.v(3), ws[4], S.v(4), ws[5], ws[3] + ws[4] + ws[5]);
-        if (FULL) s_unit(dcross(S.e(3), S.e(4)), nrm);
-        break;
-      case 2:
-        s_quad<FULL>(pos, j, S.v(2), S.v(0), S.v(3), ws[2], ws[6], -ws[5], -ws[8], S.e(5),
-                     S.e(8), dir);
-        if (FULL) s_unit(dcross(S.e(2), S.e(6)), nrm);
-        break;
-      case 3:
-        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(4), ws[0], ws[7], -ws[3], -ws[6], S.e(3),
-                     S.e(6), dir);
-        if (FULL) s_unit(dcross(S.e(0), S.e(7)), nrm);
-        break;
-      default:
-        s_quad<FULL>(pos, j, S.v(1), S.v(2), S.v(5), ws[1], ws[8], -ws[4], -ws[7], S.e(4),
-                     S.e(7), dir);
-        if (FULL) s_unit(dcross(S.e(1), S.e(8)), nrm);
-        break;
-    }
-  }
-};
-
-template <>
-struct SolidFaces<8> {  // IntersectHexaD: point i uses n = 1 - i
-  __device__ static int face(const double (&ws)[12], int slot) {
-    const int i = slot, n = 1 - slot;
-    if (s_cw(ws, n, 0) && s_cw(ws, n, 1) && s_cw(ws, n, 2) && s_cw(ws, n, 3)) return 0;
-    if (s_cw(ws, i, 4) && s_cw(ws, i, 5) && s_cw(ws, i, 6) && s_cw(ws, i, 7)) return 1;
-    if (s_cw(ws, i, 0) && s_cw(ws, i, 9) && s_cw(ws, n, 4) && s_cw(ws, n, 8)) return 2;
-    if (s_cw(ws, i, 1) && s_cw(ws, i, 10) && s_cw(ws, n, 5) && s_cw(ws, n, 9)) return 3;
-    if (s_cw(ws, i, 2) && s_cw(ws, i, 11) && s_cw(ws, n, 6) && s_cw(ws, n, 10)) return 4;
-    if (s_cw(ws, i, 3) && s_cw(ws, i, 8) && s_cw(ws, n, 7) && s_cw(ws, n, 11)) return 5;
-    return -1;
-  }
-  template <bool FULL>
-  __device__ static void point(const SolidV<8> &S, const double (&ws)[12], int f, D3 dir, int j,
-                               float pos[3], float nrm[3]) {
-    switch (f) {
-      case 0:
-        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(2), ws[0], ws[1], ws[2], ws[3], S.e(2), S.e(3),
-                     dir);
-        if (FULL) s_unit(dcross(S.e(0), S.e(1)), nrm);
-        break;
-      case 1:
-        s_quad<FULL>(pos, j, S.v(4), S.v(5), S.v(6), ws[4], ws[5], ws[6], ws[7], S.e(6), S.e(7),
-                     dir);
-        if (FULL) s_unit(dcross(S.e(4), S.e(5)), nrm);
-        break;
-      case 2:
-        s_quad<FULL>(pos, j, S.v(0), S.v(1), S.v(5), ws[0], ws[9], -ws[4], -ws[8], S.e(4),
-                     S.e(8), dir);
-        if (FULL) s_unit(dcross(S.e(0), S.e(9)), nrm);
-        break;
-      case 3:
-        s_quad<FULL>(pos, j, S.v(1), S.v(2), S.v(6), ws[1], ws[10], -ws[5], -ws[9], S.e(5),
-                     S.e(9), dir);
-        if (FULL) s_unit(dcross(S.e(1), S.e(10)), nrm);
-        break;
-      case 4:
-        s_quad<FULL>(pos, j, S.v(2), S.v(3), S.v(7), ws[2], ws[11], -ws[6], -ws[10], S.e(6),
-                     S.e(10), dir);
-        if (FULL) s_unit(dcross(S.e(2), S.e(11)), nrm);
-        break;
-      default:
-        s_quad<FULL>(pos, j, S.v(3), S.v(0), S.v(4), ws[3], ws[8], -ws[7], -ws[11], S.e(7),
-                     S.e(11), dir);
-        if (FULL) s_unit(dcross(S.e(3), S.e(8)), nrm);
-        break;
-    }
-  }
-};
-
-// The full crossing point and normal of a hit that becomes a ray's closest
-// (seldom: kept out of line so the test loop keeps its registers).
-template <int NV>
-__device__ __noinline__ void s_full_point(const SolidV<NV> &S,
-                                          const double (&ws)[SolidTab<NV>::NE], int f, D3 dir,
-                                          float pos[3], float nrm[3]) {
-  SolidFaces<NV>::template point<true>(S, ws, f, dir, 0, pos, nrm);
-}
-
-// t of a crossing point along axis j (the last with |dir| > 0.1; none: 0),
-// as the reference's parameter step computes it (:2280-2290).
-__device__ __forceinline__ float s_t(float pj, int j, D3 org, D3 dir) {
-  if (j < 0) return 0.0f;
-  return (float)(((double)pj - comp(org, j)) / comp(dir, j));
-}
-
-// IntersectRayAABB (:2160-2204) with the reference's selection order.
-__device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], const float inv[3],
-                                         const int sign[3]) {
-  float lo[3], hi[3];
-  for (int k = 0; k < 3; k++) {
-    lo[k] = sign[k] ? nd.bmax[k] : nd.bmin[k];
-    hi[k] = sign[k] ? nd.bmin[k] : nd.bmax[k];
-  }
-  const float tx0 = (lo[0] - org[0]) * inv[0], tx1 = (hi[0] - org[0]) * inv[0];
-  const float ty0 = (lo[1] - org[1]) * inv[1], ty1 = (hi[1] - org[1]) * inv[1];
-  float tmin = (tx0 > ty0) ? tx0 : ty0;
-  float tmax = (tx1 < ty1) ? tx1 : ty1;
-  const float tz0 = (lo[2] - org[2]) * inv[2], tz1 = (hi[2] - org[2]) * inv[2];
-  tmin = (tmin > tz0) ? tmin : tz0;
-  tmax = (tmax < tz1) ? tmax : tz1;
-  return (tmax > 0.0f) && (tmin <= tmax) && (tmin <= FLT_MAX);
-}
-
-// The reference's walk (render/render_accel_solid.cc:2345): near child first,
-// every solid whose leaf box the ray enters tested (no culling by distance:
-// a quad face's crossing point is an affine combination of its corners that
-// can fall outside the solid's box, so a box entered beyond the running
-// distance may still hold a nearer hit), the first of the smallest t kept.
 constexpr int kSolidQ = 32;  // solids a lane queues before the warp tests them
 
 template <int NV>
@@ -551,7 +231,6 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
   // the lanes test their queues side by side, so the costly solid tests run
   // on full warps instead of on the few lanes that reached a leaf.  A lane
   // whose walk and queue are done writes its hit and takes the next ray.
-  constexpr int RF = rec_floats(NV);
   __shared__ uint32_t queue[kSolidQ][128];
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
@@ -618,49 +297,8 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
 #pragma unroll
     for (int c = 0; c < 3; c++)
       if (dir[c] > 0.1 || dir[c] < -0.1) jax = c;
-    for (int qi = 0; qi < len; qi++) {
-      const uint32_t j = queue[qi][threadIdx.x];
-      const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)RF * j);
-      float rv[RF];
-#pragma unroll
-      for (int q4 = 0; q4 < RF / 4; q4++) {
-        const float4 v4 = __ldg(r4 + q4);
-        rv[4 * q4] = v4.x;
-        rv[4 * q4 + 1] = v4.y;
-        rv[4 * q4 + 2] = v4.z;
-        rv[4 * q4 + 3] = v4.w;
-      }
-      const uint32_t p = __float_as_uint(rv[3 * NV]);
-      if (p == prev) continue;  // Ray::prev_prim_id
-      SolidV<NV> S;
-#pragma unroll
-      for (int c = 0; c < NV; c++)
-#pragma unroll
-        for (int e = 0; e < 3; e++) S.x[c][e] = rv[3 * c + e];
-      double ws[SolidTab<NV>::NE];
-      s_weights<NV>(S, ddir, dorg, ws);
-      const int f0 = SolidFaces<NV>::face(ws, 0);
-      const int f1 = f0 < 0 ? -1 : SolidFaces<NV>::face(ws, 1);
-      if (f1 < 0) continue;
-      float pt[3] = {0.0f, 0.0f, 0.0f}, nd3[3];
-      float th[2];
-#pragma unroll
-      for (int h = 0; h < 2; h++) {
-        if (jax >= 0) SolidFaces<NV>::template point<false>(S, ws, h ? f1 : f0, ddir, jax, pt, nd3);
-        th[h] = s_t(jax >= 0 ? pt[jax] : 0.0f, jax, dorg, ddir);
-      }
-#pragma unroll
-      for (int h = 0; h < 2; h++)
-        if (th[h] >= 0.0f && th[h] < t) {
-          t = th[h];
-          prim = p;
-          s_full_point<NV>(S, ws, h ? f1 : f0, ddir, bp, bn);
-          if (h) {  // the second point's normal is flipped
-#pragma unroll
-            for (int c = 0; c < 3; c++) bn[c] = -1.0f * bn[c];
-          }
-        }
-    }
+    for (int qi = 0; qi < len; qi++)
+      solid_test<NV>(recs, queue[qi][threadIdx.x], prev, dorg, ddir, jax, t, prim, bp, bn);
     if (live && sp < 0 && leaf_left == 0) {
       const bool got = t < FLT_MAX;
       reinterpret_cast<float4 *>(hits)[i] =
@@ -694,6 +332,18 @@ srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
 
 namespace srt {
 uint64_t solid_accel_bytes(const srt_solid_accel *a) { return a->dnodes.cap + a->drecs.cap; }
+bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e) {
+  if (!a || !a->built) return false;
+  *ctx = a->ctx;
+  e.kind = kSceneSolids;
+  e.nprims = (uint32_t)a->n;
+  e.aux = a->nv;
+  e.nodes = a->dnodes.p;
+  e.prims = a->drecs.as<float4>();
+  e.sidx = nullptr;
+  e.scene = nullptr;
+  return true;
+}
 }  // namespace srt
 
 using namespace srt;

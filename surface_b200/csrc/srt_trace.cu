@@ -32,6 +32,7 @@
 #include <type_traits>
 
 #include "srt_internal.cuh"
+#include "srt_walks.cuh"
 
 namespace srt {
 namespace {
@@ -1740,7 +1741,11 @@ scene_top_kernel(const TopNode *__restrict__ top, SceneWork W) {
   if (W.element) W.element[i] = kNone;
   W.tnear[i] = inf_f();
   uint32_t key = W.nelem;  // no first candidate for the rounds
-  if (nc > kRoundCand) {
+  bool loop_only = nc > kRoundCand;
+  if (W.rank_start[3] < W.nelem)  // line and solid elements: the per-ray loop walks them
+    for (int c = 0; c < nc && !loop_only; c++)
+      loop_only = __ldg(&W.elem_rank[cid[c]]) >= W.rank_start[3];
+  if (loop_only) {
     W.ncand[i] = 0;
     W.ovf[atomicAdd(&W.counters[2], 1u)] = (uint32_t)i;
   } else {
@@ -1956,8 +1961,54 @@ scene_select_kernel(SceneWork W) {
   }
 }
 
+// Closest hit of a local ray in a line element (LineAccel::Traverse; the
+// reference's line walk has no self-hit rule).  LSTACK: the walk's stack.
+template <int LSTACK>
+__device__ __forceinline__ bool elem_hit_lines(const SceneElem &e, const RayF &lr, Best &b,
+                                               uint32_t c[4]) {
+  using namespace srt_line_walk;
+  const RayL R = make_ray(lr.o, lr.d);
+  unsigned long long nb = 0, nl = 0, nt = 0;
+  const LineHit H = line_walk<LSTACK, true>(static_cast<const LNode *>(e.nodes),
+                                            reinterpret_cast<const LineRec *>(e.prims),
+                                            e.aux != 0, R, nb, nl, nt);
+  c[1] += (uint32_t)nb;
+  c[2] += (uint32_t)nl;
+  c[3] += (uint32_t)nt;
+  if (H.rec < 0) return false;
+  b.t = H.t;
+  b.u = H.u;
+  b.v = H.v;
+  b.prim = __ldg(&reinterpret_cast<const LineRec *>(e.prims)[H.rec].prim);
+  return true;
+}
+
+// Closest hit of a local ray in a solid element (SolidAccel::Traverse, the
+// previous solid skipped inside the element the ray left): u = v = 0.
+__device__ __forceinline__ bool elem_hit_solids(const SceneElem &e, const RayF &lr,
+                                                uint32_t prev, Best &b) {
+  using namespace srt_solid_walk;
+  const SNode *nodes = static_cast<const SNode *>(e.nodes);
+  const float *recs = reinterpret_cast<const float *>(e.prims);
+  float t, bp[3], bn[3];
+  uint32_t prim;
+  if (e.aux == 5)
+    solid_walk<5>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+  else if (e.aux == 6)
+    solid_walk<6>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+  else
+    solid_walk<8>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+  if (!(t < FLT_MAX)) return false;
+  b.t = t;
+  b.u = b.v = 0.0f;
+  b.prim = prim;
+  return true;
+}
+
 // The whole loop in one thread, for the rays with more candidates than
-// the per-ray slots hold.
+// the per-ray slots hold and the rays that meet a line or solid element.
+// LSTACK: the line walks' stack (the deepest line tree + 2 at least).
+template <int LSTACK>
 __global__ void __launch_bounds__(128)
 scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
   const uint32_t cnt = *(volatile uint32_t *)&W.counters[2];
@@ -1983,7 +2034,13 @@ scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
       Best b;
       Work w;
       bool hit;
-      if (e.kind == SRT_TETRAHEDRA)
+      if (e.kind >= kSceneLines) {
+        const double ro3[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd3[3] = {r0.d[0], r0.d[1], r0.d[2]};
+        const RayF lr = local_ray(e, ro3, rd3, lo, ld);
+        const bool same = W.prev_element && __ldg(&W.prev_element[i]) == cid[q];
+        hit = e.kind == kSceneLines ? elem_hit_lines<LSTACK>(e, lr, b, c)
+                                    : elem_hit_solids(e, lr, same ? prev_prim : kNone, b);
+      } else if (e.kind == SRT_TETRAHEDRA)
         hit = elem_hit<SRT_TETRAHEDRA>(W, i, cid[q], e, r0, prev_prim, prev_t, lo, ld, b, w);
       else if (e.kind == SRT_TRIANGLES)
         hit = elem_hit<SRT_TRIANGLES>(W, i, cid[q], e, r0, prev_prim, prev_t, lo, ld, b, w);
@@ -2011,16 +2068,18 @@ scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
 }
 
 // Resident blocks per SM of the persistent kernels (the same on every device
-// of one architecture): walks of the three kinds, loop.
-int g_per_sm[4] = {1, 1, 1, 1};
+// of one architecture): walks of the three kinds, loop (short and long line
+// stack).
+int g_per_sm[5] = {1, 1, 1, 1, 1};
 std::once_flag g_per_sm_once;
 
 void scene_occupancy() {
-  const void *fn[4] = {(const void *)scene_walk_kernel<SRT_TRIANGLES>,
+  const void *fn[5] = {(const void *)scene_walk_kernel<SRT_TRIANGLES>,
                        (const void *)scene_walk_kernel<SRT_TETRAHEDRA>,
                        (const void *)scene_walk_kernel<SRT_SPHERES>,
-                       (const void *)scene_loop_kernel};
-  for (int k = 0; k < 4; k++) {
+                       (const void *)scene_loop_kernel<64>,
+                       (const void *)scene_loop_kernel<520>};
+  for (int k = 0; k < 5; k++) {
     int per_sm = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn[k], 128, 0);
     g_per_sm[k] = per_sm > 0 ? per_sm : 1;
@@ -2037,7 +2096,7 @@ static void launch_kind(srt_ctx *ctx, const SceneWork &W, int phase, cudaStream_
 }
 
 srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds,
-                              const SceneStreams &ss) {
+                              bool deep_lines, const SceneStreams &ss) {
   if (W.n == 0) return SRT_OK;
   cudaStream_t st = ctx->stream;
   cudaError_t e = cudaMemsetAsync(W.counters, 0, kSceneCounters * sizeof(uint32_t), st);
@@ -2051,7 +2110,10 @@ srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uin
   // the rays with more candidates than slots run their loop alongside
   cudaEventRecord(ss.fork[0], st);
   cudaStreamWaitEvent(ss.side[3], ss.fork[0], 0);
-  scene_loop_kernel<<<(unsigned)(ctx->num_sms * g_per_sm[3]), 128, 0, ss.side[3]>>>(top, W);
+  if (deep_lines)
+    scene_loop_kernel<520><<<(unsigned)(ctx->num_sms * g_per_sm[4]), 128, 0, ss.side[3]>>>(top, W);
+  else
+    scene_loop_kernel<64><<<(unsigned)(ctx->num_sms * g_per_sm[3]), 128, 0, ss.side[3]>>>(top, W);
   ctx->launches++;
   cudaEventRecord(ss.join[3], ss.side[3]);
   for (int phase = 0; phase < 2; phase++) {

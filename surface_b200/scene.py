@@ -4,6 +4,7 @@
     scene = RenderGraph()
     scene.AddRenderElement(mesh_accel, T)        # T: 4x4, Matrixd layout
     scene.AddRenderElement(particle_accel, T2)
+    scene.AddRenderElement(line_accel, T3)      # LineAccel / SolidAccel too
     scene.Build()
     hits, element = scene.Trace(rays)          # CUDA tensors in, CUDA out
 
@@ -24,6 +25,8 @@ import torch
 from . import _lib
 from ._lib import HIT_DTYPE, MISS, RAY_DTYPE, SurfaceError, check
 from .accel import Context, _Accel
+from .lines import LineAccel
+from .solids import SolidAccel
 
 
 def _mat(m):
@@ -49,14 +52,21 @@ class RenderGraph:
         self.h = h
         self.elements = []
 
-    def AddRenderElement(self, accel: _Accel, T=None) -> int:
-        """Add a built accel under transform T (identity when None); returns
-        its element id."""
+    def AddRenderElement(self, accel, T=None) -> int:
+        """Add a built accel (triangles, tetrahedra, particles, LineAccel or
+        SolidAccel) under transform T (identity when None); returns its
+        element id."""
         if accel.ctx is not self.ctx and accel.ctx.h.value != self.ctx.h.value:
             raise SurfaceError(_lib.SRT_ERR_INVALID, "accel of another context")
         t = _mat(np.eye(4) if T is None else T)
         eid = C.c_uint32()
-        check(self.L.srt_scene_add_element(self.h, accel.h, t.ctypes.data, C.byref(eid)))
+        if isinstance(accel, LineAccel):
+            add = self.L.srt_scene_add_lines
+        elif isinstance(accel, SolidAccel):
+            add = self.L.srt_scene_add_solids
+        else:
+            add = self.L.srt_scene_add_element
+        check(add(self.h, accel.h, t.ctypes.data, C.byref(eid)))
         self.elements.append(accel)
         return eid.value
 

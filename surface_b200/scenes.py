@@ -399,14 +399,17 @@ def affine(rotation_axis=(0.0, 0.0, 1.0), angle_deg=0.0, scale=(1.0, 1.0, 1.0),
     return m
 
 
-def scene_elements(seed=31, ntri=3, nsph=2, ntet=1, spread=4.0):
-    """A mixed scene: ntri displaced octaspheres, nsph particle clouds and
-    ntet tetrahedral grids, each under a seeded rotation, (non-uniform)
-    scale and translation inside [-spread, spread]^3.  Returns a list of
-    dicts with kind (0 tri, 1 tet, 2 sphere), verts, faces or radius, T."""
+def scene_elements(seed=31, ntri=3, nsph=2, ntet=1, spread=4.0, nline=0, nsolid=0):
+    """A mixed scene: ntri displaced octaspheres, nsph particle clouds, ntet
+    tetrahedral grids, nline hair-strand line sets and nsolid solid grids
+    (hexahedra, prisms, pyramids in turn), each under a seeded rotation,
+    (non-uniform) scale and translation inside [-spread, spread]^3.  Returns
+    a list of dicts with kind (0 tri, 1 tet, 2 sphere, 3 lines, 4 solids),
+    verts, faces (tri, tet), radius (sphere, lines), segments (lines), nv
+    (solids) and T."""
     rng = np.random.default_rng(seed)
     out = []
-    kinds = [0] * ntri + [2] * nsph + [1] * ntet
+    kinds = [0] * ntri + [2] * nsph + [1] * ntet + [3] * nline + [4] * nsolid
     for j, k in enumerate(kinds):
         T = affine(rng.normal(size=3), rng.uniform(0, 360),
                    rng.uniform(0.5, 1.5, size=3), rng.uniform(-spread, spread, size=3))
@@ -416,6 +419,13 @@ def scene_elements(seed=31, ntri=3, nsph=2, ntet=1, spread=4.0):
         elif k == 2:
             p, r = particles(2000 + 500 * j, seed=seed + j, median_radius=0.02)
             out.append(dict(kind=2, verts=p, radius=r, T=T))
+        elif k == 3:
+            p, sg, r = line_strands(150 + 50 * (j % 3), 8, seed=seed + j, radius=0.03)
+            out.append(dict(kind=3, verts=p, segments=sg, radius=r, T=T))
+        elif k == 4:  # 1024 solids or more: the reference's Build32 range
+            nv = (8, 6, 5)[j % 3]
+            v, ix = solid_grid(nv, {8: 11, 6: 8, 5: 6}[nv], seed=seed + j)
+            out.append(dict(kind=4, verts=v - np.float32(0.5), faces=ix, nv=nv, T=T))
         else:
             v, f, _ = tet_grid(4 + j % 3, seed=seed + j)
             out.append(dict(kind=1, verts=v, faces=f, T=T))

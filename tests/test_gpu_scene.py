@@ -1,6 +1,7 @@
 """Scenes of transformed accels (srt_scene_*, RenderGraph) on the GPU against
 the oracle, bit for bit: the top-level tree, primary rays and secondary
-rays that leave a hit element (self-hit rule inside prev_element only)."""
+rays that leave a hit element (self-hit rule inside prev_element only), for
+triangle, tetrahedron, particle, line and solid elements."""
 import numpy as np
 import pytest
 import torch
@@ -18,6 +19,14 @@ KIND = {0: (O.TRI, sb.TriangleAccel), 1: (O.TET, sb.TetraAccel), 2: (O.SPHERE, s
 
 
 def gpu_accel(e):
+    if e["kind"] == 3:
+        acc = sb.LineAccel()
+        acc.Build(sb.Lines(e["verts"], e["segments"], e["radius"]))
+        return acc
+    if e["kind"] == 4:
+        acc = sb.SolidAccel()
+        acc.Build32(sb.Solid(e["nv"], e["verts"], e["faces"]))
+        return acc
     cls = KIND[e["kind"]][1]
     acc = cls()
     if e["kind"] == 0:
@@ -30,6 +39,10 @@ def gpu_accel(e):
 
 
 def oracle_accel(e):
+    if e["kind"] == 3:
+        return O.OracleLines(e["verts"], e["segments"], e["radius"])
+    if e["kind"] == 4:
+        return O.OracleSolids(e["nv"], e["verts"], e["faces"])
     k = KIND[e["kind"]][0]
     if e["kind"] == 2:
         return O.OracleAccel(k, e["verts"], None, e["radius"])
@@ -130,6 +143,45 @@ def test_secondary_rays_match_oracle(mixed):
     hits, el = g.Trace(st, torch.from_numpy(pe.view(np.int32)).cuda(), torch.from_numpy(pn).cuda())
     torch.cuda.synchronize()
     assert_same(hits, el, w2, we2, sphere_mask(gacc))
+
+
+@pytest.fixture(scope="module")
+def with_lines_solids():
+    elems = S.scene_elements(seed=43, ntri=1, nsph=1, ntet=1, nline=2, nsolid=3)
+    return (elems,) + make_pair(elems)
+
+
+def test_line_and_solid_elements_match_oracle(with_lines_solids):
+    """Line and solid elements (walked by the per-ray loop) beside the
+    accels of the rounds: primary rays, then secondary rays leaving the hit
+    element (a solid skips the solid it leaves)."""
+    elems, g, o, gacc, wlo, whi = with_lines_solids
+    sph = sphere_mask(gacc)
+    gb, gi = g.top_nodes()
+    ob, oi = o.nodes()
+    assert np.array_equal(gi, oi) and np.array_equal(bits(gb), bits(ob))
+    rays = S.scene_rays(60_000, wlo.min(0), whi.max(0), seed=9, boxes=(wlo, whi))
+    want, wel = o.trace(rays)
+    kinds = np.array([e["kind"] for e in elems])
+    got_kinds = set(kinds[wel[wel != S.MISS]].tolist())
+    assert got_kinds == {0, 1, 2, 3, 4}
+    hits, el = g.Trace(torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda())
+    torch.cuda.synchronize()
+    assert_same(hits, el, want, wel, sph)
+    hit = np.nonzero(wel != S.MISS)[0]
+    rng = np.random.default_rng(5)
+    sec = np.zeros(hit.size, O.RAY_DTYPE)
+    sec["org"] = rays["org"][hit] + want["t"][hit, None] * rays["dir"][hit]
+    sec["dir"] = S._normalize(rng.normal(size=(hit.size, 3))).astype(np.float32)
+    sec["prev_prim"] = want["prim"][hit]
+    sec["prev_t"] = want["t"][hit]
+    pe = wel[hit]
+    pn = S._normalize(rng.normal(size=(hit.size, 3))).astype(np.float32)
+    w2, we2 = o.trace(sec, pe, pn)
+    h2, e2 = g.Trace(torch.from_numpy(sec.view(np.float32).reshape(-1, 8)).cuda(),
+                     torch.from_numpy(pe.view(np.int32)).cuda(), torch.from_numpy(pn).cuda())
+    torch.cuda.synchronize()
+    assert_same(h2, e2, w2, we2, sph)
 
 
 def test_many_instances_of_one_accel():

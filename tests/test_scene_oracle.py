@@ -7,8 +7,9 @@
   reference's BVHTree build and Trace.
 * RenderGraph::Trace: the oracle's scene trace against a composition of the
   reference's own pieces -- its BVHTree candidates, its accels' Traverse on
-  the local rays, and the world-distance rule of gles/gles_render_graph.cc:
-  170-306 written out in numpy."""
+  the local rays (triangles, tetrahedra, particles, lines, solids), and the
+  world-distance rule of gles/gles_render_graph.cc:170-306 written out in
+  numpy."""
 import numpy as np
 import pytest
 
@@ -130,6 +131,10 @@ def _multv(m, v):
 
 
 def _ref_accel(e):
+    if e["kind"] == 3:
+        return O.RefLines(e["verts"], e["segments"], e["radius"])
+    if e["kind"] == 4:
+        return O.RefSolids(e["nv"], e["verts"], e["faces"])
     if e["kind"] == 0:
         return O.RefAccel(O.TRI, e["verts"], e["faces"])
     if e["kind"] == 1:
@@ -138,6 +143,10 @@ def _ref_accel(e):
 
 
 def _oracle_accel(e):
+    if e["kind"] == 3:
+        return O.OracleLines(e["verts"], e["segments"], e["radius"])
+    if e["kind"] == 4:
+        return O.OracleSolids(e["nv"], e["verts"], e["faces"])
     if e["kind"] == 0:
         return O.OracleAccel(O.TRI, e["verts"], e["faces"])
     if e["kind"] == 1:
@@ -163,7 +172,10 @@ def composed_reference_trace(refs, mats, tree, rays, prev_element=None, prev_nor
         pn = np.zeros((n, 3), np.float32)
         if prev_normals is not None:
             pn[same] = prev_normals[same]
-        h = acc.trace(lr, pn)
+        if isinstance(acc, (O.RefLines, O.RefSolids)):  # no self-hit normal
+            h = acc.trace(lr)[0]
+        else:
+            h = acc.trace(lr, pn)
         if isinstance(h, tuple):  # tetrahedra also return the sub-face
             h = h[0]
         with np.errstate(over="ignore", invalid="ignore"):  # misses carry FLT_MAX
@@ -205,8 +217,10 @@ def build_scene_pair(elems, bboxes):
 
 
 @needs_ref
-def test_scene_trace_matches_composed_reference():
-    elems = S.scene_elements(seed=31)
+@pytest.mark.parametrize("mix", ["accels", "lines_solids"])
+def test_scene_trace_matches_composed_reference(mix):
+    elems = (S.scene_elements(seed=31) if mix == "accels" else
+             S.scene_elements(seed=43, ntri=1, nsph=1, ntet=1, nline=2, nsolid=3))
     refs = [_ref_accel(e) for e in elems]
     orcs = [_oracle_accel(e) for e in elems]
     mats, wlo, whi = build_scene_pair(elems, [r.bbox() for r in refs])
