@@ -216,14 +216,40 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
 
 constexpr int kTfCopies = 4;  // copies of the block-local TF gradient
 
+// Scale of the block's fixed-point colour accumulators.  An entry's colour
+// gradient is the sum over the block's rays of g.c times the ray's weight
+// on the entry; a ray's weights are compositing weights, which sum to at
+// most 1 - T <= 1, so every partial sum is bounded by bound = the sum over
+// the rays of max_c |g.c|.  The scale 2^29 / bound (a power of two: scaling
+// and the final division are exact) leaves 2x headroom for the rounding of
+// the reconstructed weights and the per-term rounding below 2^31; the
+// resolution is bound * 2^-29.  Shared-memory integer adds are native, float
+// adds are not, and the block's sums in integers are exact.
+__device__ __forceinline__ float colour_scale(float bound) {
+  int e;
+  frexpf(bound, &e);  // bound in [2^(e-1), 2^e)
+  return ldexpf(1.0f, 29 - max(e, -90));
+}
+
 // Transfer-function gradient of one table entry added to the block's
 // shared copy: the colour part is the ray's image gradient g (constant along
-// the ray) times the run's summed weight a.x, the opacity part a.y.
-__device__ __forceinline__ void flush_entry(float *g, int i, float2 &a, const float4 &gi) {
+// the ray) times the run's summed weight a.x, in fixed point at scale
+// cscale (float adds when cscale is 0: a block with a non-finite gradient);
+// the opacity part a.y as a float.
+__device__ __forceinline__ void flush_entry(float *g, int i, float2 &a, const float4 &gi,
+                                            float cscale) {
   if (a.x != 0.0f) {
-    if (gi.x != 0.0f) atomicAdd(&g[4 * i], a.x * gi.x);
-    if (gi.y != 0.0f) atomicAdd(&g[4 * i + 1], a.x * gi.y);
-    if (gi.z != 0.0f) atomicAdd(&g[4 * i + 2], a.x * gi.z);
+    if (cscale != 0.0f) {
+      int *q = reinterpret_cast<int *>(g) + 4 * i;
+      const float w = a.x * cscale;
+      if (gi.x != 0.0f) atomicAdd(q, __float2int_rn(w * gi.x));
+      if (gi.y != 0.0f) atomicAdd(q + 1, __float2int_rn(w * gi.y));
+      if (gi.z != 0.0f) atomicAdd(q + 2, __float2int_rn(w * gi.z));
+    } else {
+      if (gi.x != 0.0f) atomicAdd(&g[4 * i], a.x * gi.x);
+      if (gi.y != 0.0f) atomicAdd(&g[4 * i + 1], a.x * gi.y);
+      if (gi.z != 0.0f) atomicAdd(&g[4 * i + 2], a.x * gi.z);
+    }
   }
   if (a.y != 0.0f) atomicAdd(&g[4 * i + 3], a.y);
   a = make_float2(0.0f, 0.0f);
@@ -257,23 +283,35 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
   // so that lanes accumulating into the same entry hit different copies;
   // copies are padded by one word to fall on different banks.
   extern __shared__ float s_gtf[];
+  __shared__ float s_bound[4];
   const int tstride = 4 * K.tfn + 1;
   for (int i = threadIdx.x; i < kTfCopies * tstride; i += blockDim.x) s_gtf[i] = 0.0f;
   // the transfer function itself, after the copies (16-byte aligned)
   float4 *s_tf = reinterpret_cast<float4 *>(s_gtf + ((kTfCopies * tstride + 3) & ~3));
   for (int i = threadIdx.x; i < K.tfn; i += blockDim.x) s_tf[i] = __ldg(&tf[i]);
-  __syncthreads();
   float *my_gtf = s_gtf + (threadIdx.x & (kTfCopies - 1)) * tstride;
   const int W = K.p.width, H = K.p.height;
   int px, py;
-  if (tile_pixel(blockIdx.x * blockDim.x + threadIdx.x, W, H, px, py)) {
-    const int pix = py * W + px;
+  const bool pixel = tile_pixel(blockIdx.x * blockDim.x + threadIdx.x, W, H, px, py);
+  const int pix = pixel ? py * W + px : 0;
+  const float4 g = pixel ? gimg[pix] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  // the block's colour bound: sum over its rays of max_c |g.c|
+  float gb = fmaxf(fabsf(g.x), fmaxf(fabsf(g.y), fabsf(g.z)));
+  if (!(gb <= FLT_MAX)) gb = __int_as_float(0x7f800000);  // NaN counts as infinite
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) gb += __shfl_xor_sync(0xffffffffu, gb, o);
+  if ((threadIdx.x & 31) == 0) s_bound[threadIdx.x >> 5] = gb;
+  __syncthreads();
+  float bound = 0.0f;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) bound += s_bound[w];
+  // 0: float adds (a block whose gradient is not finite, or all zero)
+  const float cscale = (bound > 0.0f && bound <= FLT_MAX) ? colour_scale(bound) : 0.0f;
+  if (pixel) {
     float o[3], d[3], t0, t1;
     pixel_ray(K.p, px, py, o, d);
     if (slab(o, d, t0, t1)) {
       int ns = (int)((t1 - t0) / K.p.step);
       if (ns > K.p.max_steps) ns = K.p.max_steps;
-      const float4 g = gimg[pix];
       const float Tfin = trans[pix];
       const float gwT = g.w * Tfin;
       float Tn = Tfin;
@@ -323,16 +361,16 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
           // flushes only the entry that leaves.
           if (run_i0 >= 0) {
             if (i0 == run_i0 + 1) {
-              flush_entry(my_gtf, run_i0, ta0, g);
+              flush_entry(my_gtf, run_i0, ta0, g, cscale);
               ta0 = ta1;
               ta1 = make_float2(0.0f, 0.0f);
             } else if (i0 == run_i0 - 1) {
-              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
+              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale);
               ta1 = ta0;
               ta0 = make_float2(0.0f, 0.0f);
             } else {
-              flush_entry(my_gtf, run_i0, ta0, g);
-              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
+              flush_entry(my_gtf, run_i0, ta0, g, cscale);
+              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale);
             }
           }
           run_i0 = i0;
@@ -371,8 +409,8 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
         Tn = Tk;
       }
       if (run_i0 >= 0) {
-        flush_entry(my_gtf, run_i0, ta0, g);
-        flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g);
+        flush_entry(my_gtf, run_i0, ta0, g, cscale);
+        flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale);
       }
       if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
     }
@@ -380,8 +418,15 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
   __syncthreads();
   for (int i = threadIdx.x; i < 4 * K.tfn; i += blockDim.x) {
     float v = 0.0f;
+    if ((i & 3) != 3 && cscale != 0.0f) {  // colour: the copies' integer sum, unscaled
+      long long q = 0;
 #pragma unroll
-    for (int c = 0; c < kTfCopies; c++) v += s_gtf[c * tstride + i];
+      for (int c = 0; c < kTfCopies; c++) q += __float_as_int(s_gtf[c * tstride + i]);
+      v = (float)((double)q / (double)cscale);
+    } else {
+#pragma unroll
+      for (int c = 0; c < kTfCopies; c++) v += s_gtf[c * tstride + i];
+    }
     if (v != 0.0f) atomicAdd(&gtf[i], v);
   }
 }
