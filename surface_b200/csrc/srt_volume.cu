@@ -216,7 +216,7 @@ vol_fwd_kernel(const VolConst K, const float *__restrict__ dens,
 
 constexpr int kTfCopies = 4;  // copies of the block-local TF gradient
 
-// Scale of the block's fixed-point colour accumulators.  An entry's colour
+// Scale of the block's fixed-point accumulators.  An entry's colour
 // gradient is the sum over the block's rays of g.c times the ray's weight
 // on the entry; a ray's weights are compositing weights, which sum to at
 // most 1 - T <= 1, so every partial sum is bounded by bound = the sum over
@@ -231,13 +231,28 @@ __device__ __forceinline__ float colour_scale(float bound) {
   return ldexpf(1.0f, 29 - max(e, -90));
 }
 
+// The opacity part of an entry's gradient sums the samples' gc3 = ga * sstep
+// * e (0 where alpha is clamped) times their interpolation weights.  With
+// G = sum_c |g.c|, cm the table's largest |colour| component and
+// iom * e = 1 (e = 1 - alpha unclamped), |ga| <= Tk G cm + iom (G cm + |g.w|)
+// gives |gc3| <= sstep (2 G cm + |g.w|) per sample (Tk e <= 1), so the
+// ray's sum is bounded by ns sstep (2 G cm + |g.w|) and the block's by the
+// sum of that over its rays: the opacity accumulators' bound, scaled as the
+// colour ones.
+
+// |x|, or infinity when x is not finite (NaN included).
+__device__ __forceinline__ float abs_or_inf(float x) {
+  const float a = fabsf(x);
+  return a <= FLT_MAX ? a : __int_as_float(0x7f800000);
+}
+
 // Transfer-function gradient of one table entry added to the block's
 // shared copy: the colour part is the ray's image gradient g (constant along
 // the ray) times the run's summed weight a.x, in fixed point at scale
-// cscale (float adds when cscale is 0: a block with a non-finite gradient);
-// the opacity part a.y as a float.
+// cscale, the opacity part a.y in fixed point at scale oscale (float adds
+// where a scale is 0: a block whose bound is not finite, or zero).
 __device__ __forceinline__ void flush_entry(float *g, int i, float2 &a, const float4 &gi,
-                                            float cscale) {
+                                            float cscale, float oscale) {
   if (a.x != 0.0f) {
     if (cscale != 0.0f) {
       int *q = reinterpret_cast<int *>(g) + 4 * i;
@@ -251,7 +266,12 @@ __device__ __forceinline__ void flush_entry(float *g, int i, float2 &a, const fl
       if (gi.z != 0.0f) atomicAdd(&g[4 * i + 2], a.x * gi.z);
     }
   }
-  if (a.y != 0.0f) atomicAdd(&g[4 * i + 3], a.y);
+  if (a.y != 0.0f) {
+    if (oscale != 0.0f)
+      atomicAdd(reinterpret_cast<int *>(g) + 4 * i + 3, __float2int_rn(a.y * oscale));
+    else
+      atomicAdd(&g[4 * i + 3], a.y);
+  }
   a = make_float2(0.0f, 0.0f);
 }
 
@@ -283,146 +303,170 @@ vol_bwd_kernel(const VolConst K, const float *__restrict__ dens,
   // so that lanes accumulating into the same entry hit different copies;
   // copies are padded by one word to fall on different banks.
   extern __shared__ float s_gtf[];
-  __shared__ float s_bound[4];
+  __shared__ float s_bound[4][4];
   const int tstride = 4 * K.tfn + 1;
   for (int i = threadIdx.x; i < kTfCopies * tstride; i += blockDim.x) s_gtf[i] = 0.0f;
-  // the transfer function itself, after the copies (16-byte aligned)
+  // the transfer function itself, after the copies (16-byte aligned), and
+  // its largest |colour| component
   float4 *s_tf = reinterpret_cast<float4 *>(s_gtf + ((kTfCopies * tstride + 3) & ~3));
-  for (int i = threadIdx.x; i < K.tfn; i += blockDim.x) s_tf[i] = __ldg(&tf[i]);
+  float cm = 0.0f;
+  for (int i = threadIdx.x; i < K.tfn; i += blockDim.x) {
+    const float4 v = __ldg(&tf[i]);
+    s_tf[i] = v;
+    cm = fmaxf(cm, fmaxf(abs_or_inf(v.x), fmaxf(abs_or_inf(v.y), abs_or_inf(v.z))));
+  }
   float *my_gtf = s_gtf + (threadIdx.x & (kTfCopies - 1)) * tstride;
   const int W = K.p.width, H = K.p.height;
   int px, py;
   const bool pixel = tile_pixel(blockIdx.x * blockDim.x + threadIdx.x, W, H, px, py);
   const int pix = pixel ? py * W + px : 0;
   const float4 g = pixel ? gimg[pix] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  // the block's colour bound: sum over its rays of max_c |g.c|
-  float gb = fmaxf(fabsf(g.x), fmaxf(fabsf(g.y), fabsf(g.z)));
-  if (!(gb <= FLT_MAX)) gb = __int_as_float(0x7f800000);  // NaN counts as infinite
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) gb += __shfl_xor_sync(0xffffffffu, gb, o);
-  if ((threadIdx.x & 31) == 0) s_bound[threadIdx.x >> 5] = gb;
-  __syncthreads();
-  float bound = 0.0f;
-  for (int w = 0; w < (int)(blockDim.x >> 5); w++) bound += s_bound[w];
-  // 0: float adds (a block whose gradient is not finite, or all zero)
-  const float cscale = (bound > 0.0f && bound <= FLT_MAX) ? colour_scale(bound) : 0.0f;
+  float o[3], d[3], t0 = 0.0f, t1 = 0.0f;
+  int ns = 0;
   if (pixel) {
-    float o[3], d[3], t0, t1;
     pixel_ray(K.p, px, py, o, d);
     if (slab(o, d, t0, t1)) {
-      int ns = (int)((t1 - t0) / K.p.step);
+      ns = (int)((t1 - t0) / K.p.step);
       if (ns > K.p.max_steps) ns = K.p.max_steps;
-      const float Tfin = trans[pix];
-      const float gwT = g.w * Tfin;
-      float Tn = Tfin;
-      float gCb = 0.0f;  // g . (colour composited behind the sample)
-      const float top = (float)(K.tfn - 1);
-      const float sstep = K.p.sigma_scale * K.p.step;
-      // Run-length accumulators: consecutive samples often share the
-      // transfer-function bin (always in empty space) and the voxel cell
-      // (the step is half a voxel); contributions are summed in registers
-      // and flushed when the bin / cell changes.  A table entry's colour
-      // gradient is g times a scalar weight sum, so a run keeps per entry
-      // (colour weight, opacity gradient).
-      int run_i0 = -1;
-      float2 ta0 = make_float2(0.f, 0.f), ta1 = make_float2(0.f, 0.f);
-      int run_cell = -1, run_edge = 0;
-      float da[8];
-#pragma unroll
-      for (int cc = 0; cc < 8; cc++) da[cc] = 0.0f;
-      for (int s = ns - 1; s >= 0; s--) {
-        const float t = t0 + ((float)s + 0.5f) * K.p.step;
-        const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
-        if (!inside(p)) continue;
-        Cell cl;
-        const float rho = fetch(dens, K.dim, tex_coord(K, 0, 0.5f * p[0] + 0.5f),
-                                tex_coord(K, 1, 0.5f * p[1] + 0.5f),
-                                tex_coord(K, 2, 0.5f * p[2] + 0.5f), &cl);
-        float4 c, ta, tb;
-        int i0, i1;
-        float f;
-        bool inr;
-        tf_lookup_ab<true>(s_tf, K.tfn, rho, c, i0, i1, f, inr, ta, tb);
-        const float e = __expf(-(K.p.sigma_scale * c.w) * K.p.step);
-        float al = 1.0f - e;
-        const bool clamped = al > K.p.alpha_max;
-        if (clamped) al = K.p.alpha_max;
-        const float iom = __fdividef(1.0f, 1.0f - al);
-        const float Tk = Tn * iom;  // transmittance in front of sample s
-        const float w = Tk * al;    // the sample's weight in the image
-        const float gcol = g.x * c.x + g.y * c.y + g.z * c.z;
-        // d loss / d alpha: Tk g.c - (g.Cb - g.w Tfin) / (1 - al)
-        const float ga = Tk * gcol - iom * (gCb - gwT);
-        const float gc3 = clamped ? 0.0f : ga * sstep * e;
-        // transfer-function gradient: i1 = i0 + 1 except at the top entry
-        if (i0 != run_i0) {
-          // The run's two table entries are run_i0 (ta0) and run_i0 + 1 (ta1).
-          // A step of one bin keeps the shared entry in registers and
-          // flushes only the entry that leaves.
-          if (run_i0 >= 0) {
-            if (i0 == run_i0 + 1) {
-              flush_entry(my_gtf, run_i0, ta0, g, cscale);
-              ta0 = ta1;
-              ta1 = make_float2(0.0f, 0.0f);
-            } else if (i0 == run_i0 - 1) {
-              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale);
-              ta1 = ta0;
-              ta0 = make_float2(0.0f, 0.0f);
-            } else {
-              flush_entry(my_gtf, run_i0, ta0, g, cscale);
-              flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale);
-            }
-          }
-          run_i0 = i0;
-        }
-        const float wf0 = 1.0f - f;
-        ta0.x += wf0 * w;
-        ta0.y += wf0 * gc3;
-        ta1.x += f * w;
-        ta1.y += f * gc3;
-        const float drho = inr ? (w * (g.x * (tb.x - ta.x) + g.y * (tb.y - ta.y) +
-                                       g.z * (tb.z - ta.z)) +
-                                  gc3 * (tb.w - ta.w)) * top
-                               : 0.0f;
-        if (drho != 0.0f) {
-          const int key = (cl.vz * K.dim[1] + cl.vy) * K.dim[0] + cl.vx;
-          if (key != run_cell) {
-            if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
-            run_cell = key;
-            run_edge = (cl.vx + 1 < K.dim[0] ? 0 : 1) | (cl.vy + 1 < K.dim[1] ? 0 : 2) |
-                       (cl.vz + 1 < K.dim[2] ? 0 : 4);
-          }
-          // corner c = x + 2y + 4z gets drho * wx * wy * wz
-          const float x0 = drho * (1.0f - cl.dx), x1 = drho * cl.dx;
-          const float y0z0 = (1.0f - cl.dy) * (1.0f - cl.dz), y1z0 = cl.dy * (1.0f - cl.dz);
-          const float y0z1 = (1.0f - cl.dy) * cl.dz, y1z1 = cl.dy * cl.dz;
-          da[0] += x0 * y0z0;
-          da[1] += x1 * y0z0;
-          da[2] += x0 * y1z0;
-          da[3] += x1 * y1z0;
-          da[4] += x0 * y0z1;
-          da[5] += x1 * y0z1;
-          da[6] += x0 * y1z1;
-          da[7] += x1 * y1z1;
-        }
-        gCb += w * gcol;
-        Tn = Tk;
-      }
-      if (run_i0 >= 0) {
-        flush_entry(my_gtf, run_i0, ta0, g, cscale);
-        flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale);
-      }
-      if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
     }
+  }
+  const float sstep = K.p.sigma_scale * K.p.step;
+  // the block's bounds: colour = sum of max_c |g.c|; opacity = sstep
+  // (cm * sum of 2 ns G + sum of ns |g.w|)
+  const float ax = abs_or_inf(g.x), ay = abs_or_inf(g.y), az = abs_or_inf(g.z);
+  float b[4] = {fmaxf(ax, fmaxf(ay, az)), 2.0f * (float)ns * (ax + ay + az),
+                (float)ns * abs_or_inf(g.w), cm};
+#pragma unroll
+  for (int sh = 16; sh > 0; sh >>= 1) {
+#pragma unroll
+    for (int k = 0; k < 3; k++) b[k] += __shfl_xor_sync(0xffffffffu, b[k], sh);
+    b[3] = fmaxf(b[3], __shfl_xor_sync(0xffffffffu, b[3], sh));
+  }
+  if ((threadIdx.x & 31) == 0)
+    for (int k = 0; k < 4; k++) s_bound[threadIdx.x >> 5][k] = b[k];
+  __syncthreads();
+  float bc = 0.0f, b1 = 0.0f, b2 = 0.0f, bm = 0.0f;
+  for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+    bc += s_bound[w][0];
+    b1 += s_bound[w][1];
+    b2 += s_bound[w][2];
+    bm = fmaxf(bm, s_bound[w][3]);
+  }
+  const float bo = fabsf(sstep) * (b1 * bm + b2);
+  // 0: float adds (a block whose bound is not finite, or zero)
+  const float cscale = (bc > 0.0f && bc <= FLT_MAX) ? colour_scale(bc) : 0.0f;
+  const float oscale = (bo > 0.0f && bo <= FLT_MAX) ? colour_scale(bo) : 0.0f;
+  if (ns > 0) {
+    const float Tfin = trans[pix];
+    const float gwT = g.w * Tfin;
+    float Tn = Tfin;
+    float gCb = 0.0f;  // g . (colour composited behind the sample)
+    const float top = (float)(K.tfn - 1);
+    // Run-length accumulators: consecutive samples often share the
+    // transfer-function bin (always in empty space) and the voxel cell
+    // (the step is half a voxel); contributions are summed in registers
+    // and flushed when the bin / cell changes.  A table entry's colour
+    // gradient is g times a scalar weight sum, so a run keeps per entry
+    // (colour weight, opacity gradient).
+    int run_i0 = -1;
+    float2 ta0 = make_float2(0.f, 0.f), ta1 = make_float2(0.f, 0.f);
+    int run_cell = -1, run_edge = 0;
+    float da[8];
+#pragma unroll
+    for (int cc = 0; cc < 8; cc++) da[cc] = 0.0f;
+    for (int s = ns - 1; s >= 0; s--) {
+      const float t = t0 + ((float)s + 0.5f) * K.p.step;
+      const float p[3] = {o[0] + t * d[0], o[1] + t * d[1], o[2] + t * d[2]};
+      if (!inside(p)) continue;
+      Cell cl;
+      const float rho = fetch(dens, K.dim, tex_coord(K, 0, 0.5f * p[0] + 0.5f),
+                              tex_coord(K, 1, 0.5f * p[1] + 0.5f),
+                              tex_coord(K, 2, 0.5f * p[2] + 0.5f), &cl);
+      float4 c, ta, tb;
+      int i0, i1;
+      float f;
+      bool inr;
+      tf_lookup_ab<true>(s_tf, K.tfn, rho, c, i0, i1, f, inr, ta, tb);
+      const float e = __expf(-(K.p.sigma_scale * c.w) * K.p.step);
+      float al = 1.0f - e;
+      const bool clamped = al > K.p.alpha_max;
+      if (clamped) al = K.p.alpha_max;
+      const float iom = __fdividef(1.0f, 1.0f - al);
+      const float Tk = Tn * iom;  // transmittance in front of sample s
+      const float w = Tk * al;    // the sample's weight in the image
+      const float gcol = g.x * c.x + g.y * c.y + g.z * c.z;
+      // d loss / d alpha: Tk g.c - (g.Cb - g.w Tfin) / (1 - al)
+      const float ga = Tk * gcol - iom * (gCb - gwT);
+      const float gc3 = clamped ? 0.0f : ga * sstep * e;
+      // transfer-function gradient: i1 = i0 + 1 except at the top entry
+      if (i0 != run_i0) {
+        // The run's two table entries are run_i0 (ta0) and run_i0 + 1 (ta1).
+        // A step of one bin keeps the shared entry in registers and
+        // flushes only the entry that leaves.
+        if (run_i0 >= 0) {
+          if (i0 == run_i0 + 1) {
+            flush_entry(my_gtf, run_i0, ta0, g, cscale, oscale);
+            ta0 = ta1;
+            ta1 = make_float2(0.0f, 0.0f);
+          } else if (i0 == run_i0 - 1) {
+            flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale, oscale);
+            ta1 = ta0;
+            ta0 = make_float2(0.0f, 0.0f);
+          } else {
+            flush_entry(my_gtf, run_i0, ta0, g, cscale, oscale);
+            flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale, oscale);
+          }
+        }
+        run_i0 = i0;
+      }
+      const float wf0 = 1.0f - f;
+      ta0.x += wf0 * w;
+      ta0.y += wf0 * gc3;
+      ta1.x += f * w;
+      ta1.y += f * gc3;
+      const float drho = inr ? (w * (g.x * (tb.x - ta.x) + g.y * (tb.y - ta.y) +
+                                     g.z * (tb.z - ta.z)) +
+                                gc3 * (tb.w - ta.w)) * top
+                             : 0.0f;
+      if (drho != 0.0f) {
+        const int key = (cl.vz * K.dim[1] + cl.vy) * K.dim[0] + cl.vx;
+        if (key != run_cell) {
+          if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
+          run_cell = key;
+          run_edge = (cl.vx + 1 < K.dim[0] ? 0 : 1) | (cl.vy + 1 < K.dim[1] ? 0 : 2) |
+                     (cl.vz + 1 < K.dim[2] ? 0 : 4);
+        }
+        // corner c = x + 2y + 4z gets drho * wx * wy * wz
+        const float x0 = drho * (1.0f - cl.dx), x1 = drho * cl.dx;
+        const float y0z0 = (1.0f - cl.dy) * (1.0f - cl.dz), y1z0 = cl.dy * (1.0f - cl.dz);
+        const float y0z1 = (1.0f - cl.dy) * cl.dz, y1z1 = cl.dy * cl.dz;
+        da[0] += x0 * y0z0;
+        da[1] += x1 * y0z0;
+        da[2] += x0 * y1z0;
+        da[3] += x1 * y1z0;
+        da[4] += x0 * y0z1;
+        da[5] += x1 * y0z1;
+        da[6] += x0 * y1z1;
+        da[7] += x1 * y1z1;
+      }
+      gCb += w * gcol;
+      Tn = Tk;
+    }
+    if (run_i0 >= 0) {
+      flush_entry(my_gtf, run_i0, ta0, g, cscale, oscale);
+      flush_entry(my_gtf, min(run_i0 + 1, K.tfn - 1), ta1, g, cscale, oscale);
+    }
+    if (run_cell >= 0) flush_dens(gdens, K.dim, run_cell, run_edge, da);
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 4 * K.tfn; i += blockDim.x) {
     float v = 0.0f;
-    if ((i & 3) != 3 && cscale != 0.0f) {  // colour: the copies' integer sum, unscaled
+    const float sc = (i & 3) == 3 ? oscale : cscale;
+    if (sc != 0.0f) {  // fixed point: the copies' integer sum, unscaled
       long long q = 0;
 #pragma unroll
       for (int c = 0; c < kTfCopies; c++) q += __float_as_int(s_gtf[c * tstride + i]);
-      v = (float)((double)q / (double)cscale);
+      v = (float)((double)q / (double)sc);
     } else {
 #pragma unroll
       for (int c = 0; c < kTfCopies; c++) v += s_gtf[c * tstride + i];

@@ -232,3 +232,28 @@ def test_nonuniform_adjoint_matches_fp64_reference_and_fd():
                              clamp=clamp)[0]) / (2 * h)
         worst = max(worst, abs(gd.reshape(-1)[v] - fd) / abs(fd))
     assert worst <= TOL_GRAD, worst
+
+
+def test_adjoint_gradient_scale_and_non_finite():
+    """The transfer-function gradient is summed per block in fixed point at
+    a power-of-two scale taken from the block's image gradient: scaling the
+    image gradient by 2^+-100 scales both gradients by the same factor, and
+    a non-finite image gradient reaches the result (float path) instead of
+    being rounded away."""
+    p, dens, tgt, tf = case(32, 48)
+    d = torch.as_tensor(dens).cuda()
+    t = torch.as_tensor(tf).cuda()
+    target = V.march(torch.as_tensor(tgt).cuda(), t, p)[0]
+    img, trans = V.march(d, t, p)
+    g = 2 * (img - target)
+    gd, gt = V.march_backward(d, t, p, trans, g)
+    assert gt.abs().max() > 0 and gd.abs().max() > 0
+    for e in (-100, 100):
+        f = 2.0 ** e
+        gd2, gt2 = V.march_backward(d, t, p, trans, g * f)
+        assert torch.allclose(gt2 / f, gt, rtol=1e-5, atol=1e-7 * float(gt.abs().max()))
+        assert torch.allclose(gd2 / f, gd, rtol=1e-5, atol=1e-7 * float(gd.abs().max()))
+    g_nan = g.clone()
+    g_nan[24, 24, 0] = float("nan")
+    _, gt3 = V.march_backward(d, t, p, trans, g_nan)
+    assert torch.isnan(gt3).any()
