@@ -1810,6 +1810,54 @@ srt_status stage_morton(srt_ctx *ctx, srt_kind kind, const float *v, const uint3
   return SRT_ERR_INVALID;
 }
 
+srt_status stage_topology(srt_ctx *ctx, const uint32_t *codes, size_t n, int max_leaf,
+                          SceneInfo *info, Topology &t) {
+  if (n < 2) return SRT_ERR_INVALID;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const size_t m = n - 1;
+  if ((e = ctx->s_kchild.ensure(m * 4)) != cudaSuccess ||
+      (e = ctx->s_kflags.ensure(m)) != cudaSuccess ||
+      (e = ctx->s_krange.ensure(m * sizeof(uint2))) != cudaSuccess ||
+      (e = ctx->s_kparent.ensure(m * 4)) != cudaSuccess ||
+      (e = ctx->s_counter.ensure(m * 4)) != cudaSuccess ||
+      (e = ctx->s_kidx.ensure(m * 4)) != cudaSuccess ||
+      (e = ctx->s_kprefix.ensure(m)) != cudaSuccess ||
+      (e = ctx->s_flag.ensure(m * 4)) != cudaSuccess ||
+      (e = ctx->s_slot.ensure(m * 4)) != cudaSuccess)
+    return cuda_status(e, "topology scratch");
+  const uint32_t ltiles = (uint32_t)((m + kLsTile - 1) / kLsTile);
+  const size_t lbytes = 256 + (size_t)ltiles * 8;
+  if (lbytes > ctx->s_lscan.cap || !ctx->s_lscan.p) {
+    if ((e = ctx->s_lscan.ensure(lbytes)) != cudaSuccess ||
+        (e = cudaMemsetAsync(ctx->s_lscan.p, 0, ctx->s_lscan.cap, st)) != cudaSuccess)
+      return cuda_status(e, "level scan");
+  }
+  unsigned long long *lticket = ctx->s_lscan.as<unsigned long long>();
+  unsigned long long *lstatus =
+      reinterpret_cast<unsigned long long *>(ctx->s_lscan.as<char>() + 256);
+  t.kchild = ctx->s_kchild.as<uint32_t>();
+  t.kflags = ctx->s_kflags.as<uint8_t>();
+  t.krange = ctx->s_krange.as<uint2>();
+  t.kparent = ctx->s_kparent.as<uint32_t>();
+  t.counter = ctx->s_counter.as<uint32_t>();
+  t.kidx = ctx->s_kidx.as<uint32_t>();
+  t.flag = ctx->s_flag.as<uint32_t>();
+  t.slot = ctx->s_slot.as<uint32_t>();
+  uint8_t *kprefix = ctx->s_kprefix.as<uint8_t>();
+  const int gk = grid_for(m, kBlock, ctx->num_sms * 16);
+  karras_kernel<<<gk, kBlock, 0, st>>>(codes, (int)n, ctx->s_kchild.as<uint32_t>(),
+                                       ctx->s_kflags.as<uint8_t>(), ctx->s_krange.as<uint2>(),
+                                       ctx->s_kparent.as<uint32_t>(), nullptr, lticket, kprefix);
+  const uint32_t lepoch = ++ctx->os_epoch == 0 ? ++ctx->os_epoch : ctx->os_epoch;
+  level_scan_kernel<<<ltiles, kLsThreads, 0, st>>>(
+      ctx->s_krange.as<uint2>(), ctx->s_kparent.as<uint32_t>(), kprefix, (int)n, max_leaf,
+      ctx->s_flag.as<uint32_t>(), ctx->s_slot.as<uint32_t>(), ctx->s_kidx.as<uint32_t>(),
+      ctx->s_counter.as<uint32_t>(), lstatus, lticket, lepoch, info, ctx->d_err);
+  ctx->launches += 2;
+  return cuda_status(cudaGetLastError(), "topology");
+}
+
 srt_status stage_karras(srt_ctx *ctx, const uint32_t *codes, size_t n, uint32_t *child,
                         uint8_t *flags) {
   int gk = grid_for(n - 1, kBlock, ctx->num_sms * 16);

@@ -348,6 +348,25 @@ srt_status sort_codes30(srt_ctx *ctx, uint32_t *d_keys, uint32_t *d_vals, size_t
 // before a hist_ready sort) and the three passes' tile counters (zeroed).
 srt_status sort_codes30_scratch(srt_ctx *ctx, size_t n, uint32_t **hist,
                                 unsigned long long **tickets);
+// The Karras tree of n >= 2 sorted codes and its emitted branches
+// (srt_build.cu): an internal node is a branch iff it is the root, or its
+// range holds more than max_leaf + 1 keys and it lies at level <= kMaxLevel
+// (BuildTreeRecursive32's leaf rule).  Device arrays in the context's
+// scratch, valid until the context's next build: per internal node i its
+// split kchild[i] (children kchild[i] and kchild[i] + 1), kflags[i] (bit s:
+// child s is a single key), krange[i] (first and last key), kparent[i]
+// (internal parent; none for the root), flag[i] (branch), slot[i] (the
+// branch's index among the branches in node order) and a zeroed arrival
+// counter; kidx[slot] inverts slot.  info->nbranches receives the branch
+// count.
+struct Topology {
+  const uint32_t *kchild, *kparent, *flag, *slot, *kidx;
+  const uint8_t *kflags;
+  const uint2 *krange;
+  uint32_t *counter;
+};
+srt_status stage_topology(srt_ctx *ctx, const uint32_t *codes, size_t n, int max_leaf,
+                          SceneInfo *info, Topology &t);
 srt_status stage_karras(srt_ctx *ctx, const uint32_t *d_codes, size_t n,
                         uint32_t *d_child, uint8_t *d_flags);
 srt_status build_batch(srt_ctx *ctx, BatchTree &bt, const float *v, const uint32_t *f,

@@ -6,16 +6,19 @@
 // the solids' centroids (the running sum of the vertices times 1.0f / nv,
 // render/render_prefix_tree_util.cc:347-382), the stable 30-bit radix sort
 // and the Karras split of every internal node (ConstructBinaryRadixTree30)
-// -- the stages the tetrahedra use; the reference's top-down emission
-// order (BuildTreeRecursive32, :1361-1453: a leaf for a Karras leaf, for up
-// to 5 solids or below depth 22) is laid out on the host from the split
-// table alone, then the GPU fills the boxes: leaf boxes over the solids'
-// vertices -+ FLT_EPSILON * 16, branch boxes merged left then right, one
-// depth level at a time from the deepest.  A gather kernel copies each
-// solid's vertices into a record in leaf order.
+// -- the stages the tetrahedra use, with the same emitted-branch flags
+// (BuildTreeRecursive32, :1361-1453: a leaf for a Karras leaf, for up to 5
+// solids or below depth 22).  A gather kernel copies each solid's vertices
+// into a record in leaf order; one kernel then writes every emitted node
+// (branches by their slot, leaves by their first solid) and its box: leaf
+// boxes over the solids' vertices -+ FLT_EPSILON * 16, branch boxes merged
+// left then right as both children arrive.  The build stays on the GPU
+// after one host read of the scene box; the reference's node order
+// (pre-order, for Dump and export) is laid out on the host from the device
+// tree only when asked for.
 //
-// Trace (SolidAccel::Traverse, :2345-2435): one thread per ray (in a Morton
-// order of the rays for large batches), every
+// Trace (SolidAccel::Traverse, :2345-2435): one lane per ray (in a Morton
+// order of the rays for large batches) walking near child first; every
 // popped node tests its own box; a leaf whose box is hit tests its solids
 // (skipping Ray::prev_prim_id) with the Pluecker tests of Intersect*D
 // (:455-717) in double, keeping the entry or exit point nearer than the
@@ -53,9 +56,19 @@ struct srt_solid_accel {
   bool built = false;
   int nv = 0;
   size_t n = 0;
-  std::vector<SolidNodeH> nodes;  // reference layout (Dump, export)
+  // device tree: branch b at node b, the leaf over sorted solids from r at
+  // node n - 1 + r; records in sorted order; the sorted order itself; the
+  // branch count (SceneInfo.nbranches)
+  srt::DevBuf dnodes, drecs, dorder, dcodes, dinfo, dbox;
+  // ordering across streams: the latest build's end (waited for by traces
+  // and host reads) and the latest trace's launch (waited for by the next
+  // build before it overwrites the tree)
+  cudaEvent_t ev_built = nullptr, ev_used = nullptr;
+  bool used = false;
+  // the reference layout (Dump, export), made from the device tree on first use
+  bool host_ready = false;
+  std::vector<SolidNodeH> nodes;
   std::vector<uint32_t> idx;
-  srt::DevBuf dnodes, drecs;
 };
 
 namespace {
@@ -141,81 +154,155 @@ __global__ void solid_box_kernel(const float *__restrict__ v, const uint32_t *__
     }
 }
 
-// Leaf boxes (ComputeBoundingBox30, :1121-1169): node ids of the leaves in
-// leaves[], each over its sorted solids.
-__global__ void solid_leafbox_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
-                                     const uint32_t *__restrict__ order, int nv,
-                                     const uint32_t *__restrict__ leaves, size_t nleaves,
-                                     SNode *__restrict__ nodes) {
+// Leaf box (ComputeBoundingBox30, :1121-1169) over the records of sorted
+// solids first..last: every vertex -+ FLT_EPSILON * 16, the first vertex
+// first, then strict comparisons.
+template <int NV>
+__device__ __forceinline__ void leaf_box(const float *__restrict__ recs, uint32_t first,
+                                         uint32_t last, float lo[3], float hi[3]) {
+  constexpr int RF = rec_floats(NV);
   const float eps = FLT_EPSILON * 16;
-  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < nleaves;
-       j += (size_t)gridDim.x * blockDim.x) {
-    SNode &nd = nodes[leaves[j]];
-    const uint32_t first = nd.w0, cnt = nd.w1 & ~kSolidLeaf;
-    const uint32_t f0 = ix[(size_t)nv * order[first]];
-    float lo[3], hi[3];
-    for (int k = 0; k < 3; k++) {
-      lo[k] = v[3 * (size_t)f0 + k] - eps;
-      hi[k] = v[3 * (size_t)f0 + k] + eps;
-    }
-    for (uint32_t i = first; i < first + cnt; i++)
-      for (int q = 0; q < nv; q++) {
-        const uint32_t f = ix[(size_t)nv * order[i] + q];
-        for (int k = 0; k < 3; k++) {
-          const float a = v[3 * (size_t)f + k] - eps, b = v[3 * (size_t)f + k] + eps;
-          if (lo[k] > a) lo[k] = a;
-          if (hi[k] < b) hi[k] = b;
-        }
+  const float *r0 = recs + (size_t)RF * first;
+  for (int k = 0; k < 3; k++) {
+    lo[k] = r0[k] - eps;
+    hi[k] = r0[k] + eps;
+  }
+  for (uint32_t i = first; i <= last; i++) {
+    const float *r = recs + (size_t)RF * i;
+#pragma unroll
+    for (int q = 0; q < NV; q++)
+#pragma unroll
+      for (int k = 0; k < 3; k++) {
+        const float x = r[3 * q + k];
+        const float a = x - eps, b = x + eps;
+        if (lo[k] > a) lo[k] = a;
+        if (hi[k] < b) hi[k] = b;
       }
-    for (int k = 0; k < 3; k++) {
-      nd.bmin[k] = lo[k];
-      nd.bmax[k] = hi[k];
-    }
   }
 }
 
-// Branch boxes of one depth level (MergeBoundingBox: std::min / std::max of
-// the left then the right child), deepest level first.
-__global__ void solid_merge_kernel(const uint32_t *__restrict__ ids, size_t n,
-                                   SNode *__restrict__ nodes) {
-  for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
-       j += (size_t)gridDim.x * blockDim.x) {
-    SNode &nd = nodes[ids[j]];
-    const SNode &l = nodes[nd.w0], &r = nodes[nd.w1 & 0x1fffffffu];
-    for (int k = 0; k < 3; k++) {
-      nd.bmin[k] = (r.bmin[k] < l.bmin[k]) ? r.bmin[k] : l.bmin[k];
-      nd.bmax[k] = (l.bmax[k] < r.bmax[k]) ? r.bmax[k] : l.bmax[k];
-    }
+__device__ __forceinline__ void node_box_store(SNode *nd, const float lo[3], const float hi[3]) {
+  for (int k = 0; k < 3; k++) {
+    __stcg(&nd->bmin[k], lo[k]);
+    __stcg(&nd->bmax[k], hi[k]);
   }
 }
-
-// The reference's emission order (BuildTreeRecursive32, :1361-1453) on the
-// host, topology only: device nodes in pre-order, each node's depth.
-struct Topology {
-  const uint32_t *code, *child;
-  const uint8_t *flags;  // bit 0: left child is a single key, bit 1: right
-  std::vector<SNode> &nodes;
-  std::vector<int> &depth;
-
-  static int axis_of(uint32_t c) { return ((c ? __builtin_clz(c) : 32) - 2) % 3; }
-
-  size_t emit(uint32_t root, uint32_t l, uint32_t r, bool leaf, int d) {
-    const size_t off = nodes.size();
-    nodes.push_back(SNode{});
-    depth.push_back(d);
-    if (leaf || (r - l) <= 4 || d > 22) {
-      nodes[off].w0 = l;
-      nodes[off].w1 = kSolidLeaf | (r + 1 - l);
-      return off;
-    }
-    const uint32_t mid = child[root];
-    const size_t left = emit(mid, l, mid, flags[root] & 1, d + 1);
-    const size_t right = emit(mid + 1, mid + 1, r, flags[root] & 2, d + 1);
-    nodes[off].w0 = (uint32_t)left;
-    nodes[off].w1 = (uint32_t)right | ((uint32_t)axis_of(code[root]) << 29);
-    return off;
+__device__ __forceinline__ void node_box_load(const SNode *nd, float lo[3], float hi[3]) {
+  for (int k = 0; k < 3; k++) {
+    lo[k] = __ldcg(&nd->bmin[k]);
+    hi[k] = __ldcg(&nd->bmax[k]);
   }
-};
+}
+// MergeBoundingBox: the right box's bound only where strictly beyond the left's.
+__device__ __forceinline__ void merge_lr(const float llo[3], const float lhi[3],
+                                         const float rlo[3], const float rhi[3], float lo[3],
+                                         float hi[3]) {
+  for (int k = 0; k < 3; k++) {
+    lo[k] = (rlo[k] < llo[k]) ? rlo[k] : llo[k];
+    hi[k] = (lhi[k] < rhi[k]) ? rhi[k] : lhi[k];
+  }
+}
+// Arrival at a node's two-child counter: release this thread's box stores,
+// acquire the other child's; returns the count before this arrival.
+__device__ __forceinline__ uint32_t arrive_at(uint32_t *counter) {
+  uint32_t old;
+  asm volatile("atom.add.acq_rel.gpu.global.u32 %0, [%1], 1;" : "=r"(old) : "l"(counter)
+               : "memory");
+  return old;
+}
+
+// The emitted tree (BuildTreeRecursive32, :1361-1453: a leaf for a Karras
+// leaf, for up to 5 solids or below depth 22) as device nodes, and its
+// boxes, in one pass.  Thread per branch: branch b is node b (its slot; the
+// root is slot 0), the leaf over sorted solids r.x..r.y is node m + r.x (m
+// internal nodes; emitted leaves cover disjoint ranges).  A branch's thread
+// writes its children links, axis ((clz(code) - 2) % 3 of its split code)
+// and leaf children; boxes then climb to the root, the second child to
+// arrive at a branch merging both (left then right).
+template <int NV>
+__global__ void __launch_bounds__(256)
+solid_tree_kernel(const uint32_t *__restrict__ codes, srt::Topology T,
+                  const srt::SceneInfo *__restrict__ info, uint32_t m,
+                  const float *__restrict__ recs, SNode *__restrict__ nodes,
+                  uint32_t *__restrict__ err) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= info->nbranches) return;
+  const uint32_t i = __ldg(&T.kidx[t]);
+  const uint32_t g = __ldg(&T.kchild[i]);
+  const uint8_t fl = __ldg(&T.kflags[i]);
+  uint32_t id[2];
+  bool leaf[2];
+  float clo[2][3], chi[2][3];
+#pragma unroll
+  for (int side = 0; side < 2; side++) {
+    const uint32_t c = g + side;
+    const bool kleaf = fl & (1 << side);
+    leaf[side] = kleaf || !__ldg(&T.flag[c]);
+    if (leaf[side]) {
+      const uint2 r = kleaf ? make_uint2(c, c) : __ldg(&T.krange[c]);
+      id[side] = m + r.x;
+      leaf_box<NV>(recs, r.x, r.y, clo[side], chi[side]);
+      SNode *ln = nodes + id[side];
+      node_box_store(ln, clo[side], chi[side]);
+      __stcg(&ln->w0, r.x);
+      __stcg(&ln->w1, kSolidLeaf | (r.y - r.x + 1));
+    } else {
+      id[side] = __ldg(&T.slot[c]);
+    }
+  }
+  const uint32_t code = __ldg(&codes[i]);
+  const uint32_t axis = (uint32_t)(((code ? __clz(code) : 32) - 2) % 3);
+  __stcg(&nodes[t].w0, id[0]);
+  __stcg(&nodes[t].w1, id[1] | (axis << 29));
+  if (!leaf[0] && !leaf[1]) return;  // both children climb here
+  float lo[3], hi[3];
+  if (leaf[0] && leaf[1]) {
+    merge_lr(clo[0], chi[0], clo[1], chi[1], lo, hi);
+  } else {
+    // one leaf child: meet the branch child's climb
+    if (arrive_at(&T.counter[i]) == 0) return;
+    const int bs = leaf[0] ? 1 : 0;  // the branch side
+    float blo[3], bhi[3];
+    node_box_load(nodes + id[bs], blo, bhi);
+    if (bs == 1)
+      merge_lr(clo[0], chi[0], blo, bhi, lo, hi);
+    else
+      merge_lr(blo, bhi, clo[1], chi[1], lo, hi);
+  }
+  uint32_t node = i;
+  for (int guard = 0; guard < 64; guard++) {
+    const uint32_t ns = node == i ? t : __ldg(&T.slot[node]);
+    node_box_store(nodes + ns, lo, hi);
+    if (node == 0) return;
+    const uint32_t q = __ldg(&T.kparent[node]);
+    if (arrive_at(&T.counter[q]) == 0) return;
+    const uint32_t gq = __ldg(&T.kchild[q]);
+    const uint8_t fq = __ldg(&T.kflags[q]);
+    const bool left = (gq == node) && !(fq & 1);
+    const uint32_t sib = left ? gq + 1 : gq;
+    const bool sib_kleaf = left ? (fq & 2) : (fq & 1);
+    uint32_t sid;
+    if (sib_kleaf)
+      sid = m + sib;
+    else if (__ldg(&T.flag[sib]))
+      sid = __ldg(&T.slot[sib]);
+    else
+      sid = m + __ldg(&T.krange[sib]).x;
+    float slo[3], shi[3];
+    node_box_load(nodes + sid, slo, shi);
+    float nlo[3], nhi[3];
+    if (left)
+      merge_lr(lo, hi, slo, shi, nlo, nhi);
+    else
+      merge_lr(slo, shi, lo, hi, nlo, nhi);
+    for (int k = 0; k < 3; k++) {
+      lo[k] = nlo[k];
+      hi[k] = nhi[k];
+    }
+    node = q;
+  }
+  atomicOr(err, srt::kErrTree);
+}
 
 // ------------------------------------------------------------------ trace
 constexpr int kSolidQ = 32;  // solids a lane queues before the warp tests them
@@ -334,6 +421,7 @@ namespace srt {
 uint64_t solid_accel_bytes(const srt_solid_accel *a) { return a->dnodes.cap + a->drecs.cap; }
 bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e) {
   if (!a || !a->built) return false;
+  cudaEventSynchronize(a->ev_built);  // the build may have run on another stream
   *ctx = a->ctx;
   e.kind = kSceneSolids;
   e.nprims = (uint32_t)a->n;
@@ -348,6 +436,69 @@ bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e) {
 
 using namespace srt;
 
+namespace {
+
+// The device tree's root node (its box is the accel's BoundingBox).
+srt_status solid_root(srt_solid_accel *a, SNode &root) {
+  cudaSetDevice(a->ctx->device);
+  cudaError_t e = cudaStreamWaitEvent(a->ctx->stream, a->ev_built, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&root, a->dnodes.p, sizeof(SNode), cudaMemcpyDeviceToHost,
+                        a->ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(a->ctx->stream);
+  return cuda_status(e, "solid root");
+}
+
+// Pre-order (root, left, right) copy of the device subtree at node id in
+// the reference's node layout; returns its index.
+uint32_t solid_preorder(const std::vector<SNode> &dn, uint32_t id, std::vector<SolidNodeH> &out) {
+  const SNode &d = dn[id];
+  const uint32_t me = (uint32_t)out.size();
+  out.push_back(SolidNodeH{});
+  SolidNodeH h{};
+  for (int k = 0; k < 3; k++) {
+    h.bmin[k] = d.bmin[k];
+    h.bmax[k] = d.bmax[k];
+  }
+  if (d.w1 & kSolidLeaf) {
+    h.flag = 1;
+    h.data[0] = d.w1 & ~kSolidLeaf;
+    h.data[1] = d.w0;
+  } else {
+    h.axis = (int)(d.w1 >> 29);
+    h.data[0] = solid_preorder(dn, d.w0, out);
+    h.data[1] = solid_preorder(dn, d.w1 & 0x1fffffffu, out);
+  }
+  out[me] = h;
+  return me;
+}
+
+// The reference layout of the tree (BuildTreeRecursive32's node order:
+// pre-order) and the solid order, from the device tree, once per build.
+srt_status solid_host_layout(srt_solid_accel *a) {
+  if (a->host_ready) return SRT_OK;
+  srt_ctx *ctx = a->ctx;
+  cudaSetDevice(ctx->device);
+  const size_t n = a->n, m = n - 1;
+  std::vector<SNode> dn(m + n);
+  a->idx.resize(n);
+  cudaError_t e = cudaStreamWaitEvent(ctx->stream, a->ev_built, 0);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dn.data(), a->dnodes.p, dn.size() * sizeof(SNode),
+                        cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->idx.data(), a->dorder.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_status(e, "solid layout");
+  a->nodes.clear();
+  a->nodes.reserve(2 * n);
+  solid_preorder(dn, 0, a->nodes);
+  a->host_ready = true;
+  return SRT_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 SRT_API srt_status srt_solid_create(srt_ctx *ctx, srt_solid_accel **out) {
@@ -355,6 +506,14 @@ SRT_API srt_status srt_solid_create(srt_ctx *ctx, srt_solid_accel **out) {
   srt_solid_accel *a = new (std::nothrow) srt_solid_accel();
   if (!a) return SRT_ERR_NO_MEMORY;
   a->ctx = ctx;
+  cudaSetDevice(ctx->device);
+  cudaError_t e = cudaEventCreateWithFlags(&a->ev_built, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&a->ev_used, cudaEventDisableTiming);
+  if (e != cudaSuccess) {
+    if (a->ev_built) cudaEventDestroy(a->ev_built);
+    delete a;
+    return cuda_status(e, "solid accel events");
+  }
   *out = a;
   return SRT_OK;
 }
@@ -363,6 +522,10 @@ SRT_API srt_status srt_solid_destroy(srt_solid_accel *a) {
   if (!a) return SRT_OK;
   cudaSetDevice(a->ctx->device);
   cudaStreamSynchronize(a->ctx->stream);
+  cudaEventSynchronize(a->ev_built);
+  cudaEventSynchronize(a->ev_used);
+  cudaEventDestroy(a->ev_built);
+  cudaEventDestroy(a->ev_used);
   delete a;
   return SRT_OK;
 }
@@ -372,14 +535,14 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
                                    const uint32_t *indices, size_t nsolids) {
   if (!a || !vertices || !indices) return SRT_ERR_INVALID;
   const int nv = verts_per_solid;
-  if ((nv != 5 && nv != 6 && nv != 8) || nsolids < 2 || nsolids >= (1u << 29)) {
-    set_error("srt_solid_build: 5, 6 or 8 vertices per solid and 2 .. 2^29 solids");
+  if ((nv != 5 && nv != 6 && nv != 8) || nsolids < 2 || nsolids >= (1u << 28)) {
+    set_error("srt_solid_build: 5, 6 or 8 vertices per solid and 2 .. 2^28 - 1 solids");
     return SRT_ERR_INVALID;
   }
   srt_ctx *ctx = a->ctx;
   cudaSetDevice(ctx->device);
-  const size_t n = nsolids, refs = nsolids * (size_t)nv;
-  DevBuf sv, si, codes, order, child, flags, boxbuf, dleaves, dlevel;
+  const size_t n = nsolids, refs = nsolids * (size_t)nv, m = n - 1;
+  DevBuf sv, si;  // staging of host inputs
   const void *dv, *di;
   srt_status s;
   if ((s = solid_view(ctx, vertices, nverts * 12, sv, &dv)) != SRT_OK) return s;
@@ -387,18 +550,29 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
   const float *d_v = static_cast<const float *>(dv);
   const uint32_t *d_ix = static_cast<const uint32_t *>(di);
   cudaError_t e;
-  // scene box and index check on the GPU
+  a->built = false;
+  a->host_ready = false;
+  // the latest trace (on any stream) reads the tree this build overwrites
+  if (a->used && (e = cudaStreamWaitEvent(ctx->stream, a->ev_used, 0)) != cudaSuccess)
+    return cuda_status(e, "solid build");
+  if ((e = a->dbox.ensure(64)) != cudaSuccess || (e = a->dcodes.ensure(n * 4)) != cudaSuccess ||
+      (e = a->dorder.ensure(n * 4)) != cudaSuccess ||
+      (e = a->dinfo.ensure(sizeof(srt::SceneInfo))) != cudaSuccess ||
+      (e = a->dnodes.ensure((m + n) * sizeof(SNode))) != cudaSuccess ||
+      (e = a->drecs.ensure(n * rec_floats(nv) * 4)) != cudaSuccess)
+    return cuda_status(e, "solid accel");
+  // scene box and index check on the GPU: the one host round trip (an index
+  // beyond nverts must fail before any kernel reads through it)
   int hbox[8] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN, 0, 0};
-  if ((e = boxbuf.ensure(sizeof(hbox))) != cudaSuccess ||
-      (e = cudaMemcpyAsync(boxbuf.p, hbox, sizeof(hbox), cudaMemcpyHostToDevice, ctx->stream)) !=
-          cudaSuccess)
+  if ((e = cudaMemcpyAsync(a->dbox.p, hbox, sizeof(hbox), cudaMemcpyHostToDevice,
+                           ctx->stream)) != cudaSuccess)
     return cuda_status(e, "solid box");
   const unsigned gbox = (unsigned)std::min<size_t>((refs + 255) / 256, (size_t)ctx->num_sms * 8);
-  solid_box_kernel<<<gbox, 256, 0, ctx->stream>>>(d_v, d_ix, refs, nverts, boxbuf.as<int>(),
-                                                   reinterpret_cast<uint32_t *>(boxbuf.as<int>() + 6));
+  solid_box_kernel<<<gbox, 256, 0, ctx->stream>>>(d_v, d_ix, refs, nverts, a->dbox.as<int>(),
+                                                   reinterpret_cast<uint32_t *>(a->dbox.as<int>() + 6));
   ctx->launches++;
-  if ((e = cudaMemcpyAsync(hbox, boxbuf.p, sizeof(hbox), cudaMemcpyDeviceToHost, ctx->stream)) !=
-          cudaSuccess ||
+  if ((e = cudaMemcpyAsync(hbox, a->dbox.p, sizeof(hbox), cudaMemcpyDeviceToHost,
+                           ctx->stream)) != cudaSuccess ||
       (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
     return cuda_status(e, "solid box");
   if (hbox[6]) {
@@ -418,116 +592,37 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
     hi3[k] = o2f_h(hbox[3 + k]);
     inv[k] = kdiv / (hi3[k] - lo[k]);
   }
-  if ((e = codes.ensure(n * 4)) != cudaSuccess || (e = order.ensure(n * 4)) != cudaSuccess ||
-      (e = child.ensure(n * 4)) != cudaSuccess || (e = flags.ensure(n)) != cudaSuccess)
-    return cuda_status(e, "solid build");
+  uint32_t *codes = a->dcodes.as<uint32_t>(), *order = a->dorder.as<uint32_t>();
   const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
   solid_morton_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, nv, n, lo[0], lo[1], lo[2],
-                                                      inv[0], inv[1], inv[2], codes.as<uint32_t>());
+                                                      inv[0], inv[1], inv[2], codes);
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid morton");
-  if ((s = sort_pairs(ctx, codes.as<uint32_t>(), order.as<uint32_t>(), n, true, 30)) != SRT_OK)
-    return s;
-  if ((s = stage_karras(ctx, codes.as<uint32_t>(), n, child.as<uint32_t>(),
-                        flags.as<uint8_t>())) != SRT_OK)
-    return s;
-  std::vector<uint32_t> hcode(n), hchild(n), hidx(n);
-  std::vector<uint8_t> hflags(n);
-  if ((e = cudaMemcpyAsync(hcode.data(), codes.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(hidx.data(), order.p, n * 4, cudaMemcpyDeviceToHost, ctx->stream)) !=
-          cudaSuccess ||
-      (e = cudaMemcpyAsync(hchild.data(), child.p, (n - 1) * 4, cudaMemcpyDeviceToHost,
-                           ctx->stream)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(hflags.data(), flags.p, n - 1, cudaMemcpyDeviceToHost, ctx->stream)) !=
-          cudaSuccess ||
-      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
-    return cuda_status(e, "solid tree");
-  // topology on the host, in the reference's pre-order (root, left, right)
-  a->built = false;
-  std::vector<SNode> dn;
-  std::vector<int> depth;
-  dn.reserve(n);
-  depth.reserve(n);
-  Topology T{hcode.data(), hchild.data(), hflags.data(), dn, depth};
-  dn.push_back(SNode{});
-  depth.push_back(-1);
-  const uint32_t mid = hchild[0];
-  const size_t left = T.emit(mid, 0, mid, hflags[0] & 1, 0);
-  const size_t right = T.emit(mid + 1, mid + 1, (uint32_t)n - 1, hflags[0] & 2, 0);
-  dn[0].w0 = (uint32_t)left;
-  dn[0].w1 = (uint32_t)right | ((uint32_t)Topology::axis_of(hcode[0]) << 29);
-  // leaves, then branches grouped by depth (deepest first) for the refit
-  int maxd = 0;
-  for (int d : depth) maxd = std::max(maxd, d);
-  std::vector<uint32_t> leaves, byd;
-  std::vector<size_t> start(maxd + 3, 0);
-  for (size_t i = 0; i < dn.size(); i++)
-    if (dn[i].w1 & kSolidLeaf)
-      leaves.push_back((uint32_t)i);
-    else
-      start[depth[i] + 2]++;
-  for (int d = 1; d < maxd + 3; d++) start[d] += start[d - 1];
-  byd.resize(start[maxd + 2]);
-  {
-    std::vector<size_t> fill(start.begin(), start.end());
-    for (size_t i = 0; i < dn.size(); i++)
-      if (!(dn[i].w1 & kSolidLeaf)) byd[fill[depth[i] + 1]++] = (uint32_t)i;
-  }
-  if ((e = a->dnodes.ensure(dn.size() * sizeof(SNode))) != cudaSuccess ||
-      (e = a->drecs.ensure(n * rec_floats(nv) * 4)) != cudaSuccess ||
-      (e = dleaves.ensure(leaves.size() * 4)) != cudaSuccess ||
-      (e = dlevel.ensure(std::max<size_t>(byd.size(), 1) * 4)) != cudaSuccess)
-    return cuda_status(e, "solid accel");
-  if ((e = cudaMemcpyAsync(a->dnodes.p, dn.data(), dn.size() * sizeof(SNode),
-                           cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess ||
-      (e = cudaMemcpyAsync(dleaves.p, leaves.data(), leaves.size() * 4, cudaMemcpyHostToDevice,
-                           ctx->stream)) != cudaSuccess ||
-      (byd.size() && (e = cudaMemcpyAsync(dlevel.p, byd.data(), byd.size() * 4,
-                                          cudaMemcpyHostToDevice, ctx->stream)) != cudaSuccess))
-    return cuda_status(e, "solid nodes");
-  SNode *d_nodes = a->dnodes.as<SNode>();
-  solid_leafbox_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order.as<uint32_t>(), nv,
-                                                       dleaves.as<uint32_t>(), leaves.size(),
-                                                       d_nodes);
-  ctx->launches++;
-  for (int d = maxd; d >= -1; d--) {  // depth -1 is the root
-    const size_t b0 = start[d + 1], b1 = start[d + 2];
-    if (b1 == b0) continue;
-    const unsigned gm = (unsigned)std::min<size_t>((b1 - b0 + 255) / 256, 1024);
-    solid_merge_kernel<<<gm, 256, 0, ctx->stream>>>(dlevel.as<uint32_t>() + b0, b1 - b0, d_nodes);
-    ctx->launches++;
-  }
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid refit");
-  solid_gather_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order.as<uint32_t>(), nv, n,
+  if ((s = sort_pairs(ctx, codes, order, n, true, 30)) != SRT_OK) return s;
+  srt::Topology T;
+  srt::SceneInfo *info = a->dinfo.as<srt::SceneInfo>();
+  if ((s = srt::stage_topology(ctx, codes, n, 4, info, T)) != SRT_OK) return s;
+  solid_gather_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order, nv, n,
                                                       a->drecs.as<float>());
-  ctx->launches++;
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid records");
-  // the reference-layout copy (Dump, export, BoundingBox)
-  if ((e = cudaMemcpyAsync(dn.data(), d_nodes, dn.size() * sizeof(SNode), cudaMemcpyDeviceToHost,
-                           ctx->stream)) != cudaSuccess)
-    return cuda_status(e, "solid nodes");
-  // staged inputs and scratch are freed on return: finish with them first
-  if ((e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) return cuda_status(e, "solid build");
-  a->nodes.resize(dn.size());
-  for (size_t i = 0; i < dn.size(); i++) {
-    SolidNodeH &h = a->nodes[i];
-    h = SolidNodeH{};
-    for (int k = 0; k < 3; k++) {
-      h.bmin[k] = dn[i].bmin[k];
-      h.bmax[k] = dn[i].bmax[k];
-    }
-    if (dn[i].w1 & kSolidLeaf) {
-      h.flag = 1;
-      h.data[0] = dn[i].w1 & ~kSolidLeaf;
-      h.data[1] = dn[i].w0;
-    } else {
-      h.axis = (int)(dn[i].w1 >> 29);
-      h.data[0] = dn[i].w0;
-      h.data[1] = dn[i].w1 & 0x1fffffffu;
-    }
-  }
-  a->idx = std::move(hidx);
+  const unsigned gt = (unsigned)((m + 255) / 256);
+  SNode *d_nodes = a->dnodes.as<SNode>();
+  const float *recs = a->drecs.as<float>();
+  if (nv == 5)
+    solid_tree_kernel<5><<<gt, 256, 0, ctx->stream>>>(codes, T, info, (uint32_t)m, recs, d_nodes,
+                                                      ctx->d_err);
+  else if (nv == 6)
+    solid_tree_kernel<6><<<gt, 256, 0, ctx->stream>>>(codes, T, info, (uint32_t)m, recs, d_nodes,
+                                                      ctx->d_err);
+  else
+    solid_tree_kernel<8><<<gt, 256, 0, ctx->stream>>>(codes, T, info, (uint32_t)m, recs, d_nodes,
+                                                      ctx->d_err);
+  ctx->launches += 2;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid tree");
+  if ((e = cudaEventRecord(a->ev_built, ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid build");
+  // staged host inputs are freed on return: finish with them first
+  if ((sv.p || si.p) && (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid build");
   a->nv = nv;
   a->n = n;
   a->built = true;
@@ -589,6 +684,9 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
   // large batches; the hits do not depend on it
   const uint32_t *ord = nullptr;
   if (n >= 32768 && (s = ray_order(ctx, rr, n, &ord)) != SRT_OK) return s;
+  // the build may have run on another stream
+  if ((e = cudaStreamWaitEvent(ctx->stream, a->ev_built, 0)) != cudaSuccess)
+    return cuda_status(e, "solid trace");
   if (a->nv == 5)
     solid_trace_kernel<5><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
   else if (a->nv == 6)
@@ -597,6 +695,9 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
     solid_trace_kernel<8><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid trace");
+  if ((e = cudaEventRecord(a->ev_used, ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid trace");
+  a->used = true;
   if (!hdev) cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, ctx->stream);
   if (!ndev) cudaMemcpyAsync(normals, dn, n * 12, cudaMemcpyDeviceToHost, ctx->stream);
   if (!pdev) cudaMemcpyAsync(positions, dp, n * 12, cudaMemcpyDeviceToHost, ctx->stream);
@@ -614,9 +715,12 @@ SRT_API srt_status srt_solid_bbox(srt_solid_accel *a, double bmin[3], double bma
     }
     return SRT_OK;
   }
+  SNode root;
+  srt_status s = solid_root(a, root);
+  if (s != SRT_OK) return s;
   for (int k = 0; k < 3; k++) {
-    bmin[k] = a->nodes[0].bmin[k];
-    bmax[k] = a->nodes[0].bmax[k];
+    bmin[k] = root.bmin[k];
+    bmax[k] = root.bmax[k];
   }
   return SRT_OK;
 }
@@ -624,12 +728,21 @@ SRT_API srt_status srt_solid_bbox(srt_solid_accel *a, double bmin[3], double bma
 SRT_API srt_status srt_solid_info(srt_solid_accel *a, uint64_t *nsolids, uint64_t *nnodes) {
   if (!a) return SRT_ERR_INVALID;
   if (nsolids) *nsolids = a->built ? a->n : 0;
-  if (nnodes) *nnodes = a->built ? a->nodes.size() : 0;
+  if (nnodes) {
+    *nnodes = 0;
+    if (a->built) {
+      srt_status s = solid_host_layout(a);
+      if (s != SRT_OK) return s;
+      *nnodes = a->nodes.size();
+    }
+  }
   return SRT_OK;
 }
 
 SRT_API srt_status srt_solid_export(srt_solid_accel *a, void *nodes, uint32_t *indices) {
   if (!a || !a->built) return SRT_ERR_INVALID;
+  srt_status s = solid_host_layout(a);
+  if (s != SRT_OK) return s;
   if (nodes) std::memcpy(nodes, a->nodes.data(), a->nodes.size() * sizeof(SolidNodeH));
   if (indices) std::memcpy(indices, a->idx.data(), a->idx.size() * 4);
   return SRT_OK;
@@ -637,6 +750,8 @@ SRT_API srt_status srt_solid_export(srt_solid_accel *a, void *nodes, uint32_t *i
 
 SRT_API srt_status srt_solid_dump(srt_solid_accel *a, const char *path) {
   if (!a || !path || !a->built) return SRT_ERR_INVALID;
+  srt_status s = solid_host_layout(a);
+  if (s != SRT_OK) return s;
   FILE *fp = fopen(path, "wb");
   if (!fp) {
     set_error(std::string("cannot write ") + path);

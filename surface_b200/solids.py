@@ -46,9 +46,11 @@ class SolidAccel:
         v = _View(solids.vertices, np.float32, torch.float32)
         ix = _View(solids.indices, np.uint32, torch.int32)
         nv = int(solids.numVertsPerSolid)
+        # device inputs: in torch's stream order; host inputs: the context's stream
         if v.device or ix.device:
-            torch.cuda.current_stream().synchronize()
-        self.ctx.use_own_stream()
+            self.ctx.use_torch_stream()
+        else:
+            self.ctx.use_own_stream()
         check(self.L.srt_solid_build(self.h, nv, v.ptr, v.nbytes // 12, ix.ptr,
                                      ix.nbytes // (4 * nv)))
         self.built = True

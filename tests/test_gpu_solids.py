@@ -108,3 +108,30 @@ def test_against_reference_fixtures(golden):
         assert np.array_equal(bits(h.view(np.float32).reshape(-1, 4)), bits(g[f"solid{nv}_hits"]))
         assert np.array_equal(bits(n), bits(g[f"solid{nv}_normals"]))
         assert np.array_equal(bits(q), bits(g[f"solid{nv}_positions"]))
+
+
+def test_rebuild_and_trace_across_streams():
+    """Builds from device arrays run in torch's stream order and the trace
+    waits for the accel's latest build even when it is issued on another
+    stream; the next build waits for the latest trace.  Every step's hits
+    equal the oracle's."""
+    v, ix = S.solid_grid(8, 24, seed=11)
+    rays = S.pinhole_rays(192, 192, (1.7, 1.3, 2.1), (0.5, 0.5, 0.5), fov_deg=50)
+    want, _, _ = O.OracleSolids(8, v, ix).trace(rays)
+    acc = SolidAccel()
+    dv = torch.as_tensor(v).cuda()
+    dix = torch.as_tensor(ix.view(np.int32)).cuda()
+    rt = torch.from_numpy(rays.view(np.float32).reshape(-1, 8)).cuda()
+    s_build, s_trace = torch.cuda.Stream(), torch.cuda.Stream()
+    torch.cuda.synchronize()  # the inputs' copies ran on the default stream
+    outs = []
+    for k in range(4):
+        with torch.cuda.stream(s_build):
+            acc.Build32(Solid(8, dv, dix))
+        with torch.cuda.stream(s_trace):
+            outs.append(acc.Traverse(rt))
+    torch.cuda.synchronize()
+    for h in outs:
+        assert np.array_equal(bits(h.cpu().numpy()), bits(want.view(np.float32).reshape(-1, 4)))
+    n, nn = acc.info()
+    assert n == ix.shape[0] and nn > 1
