@@ -700,8 +700,10 @@ SRT_API srt_status srt_line_dump(srt_line_accel *accel, const char *path);
  * SolidAccel (render/render_accel_solid.{h,cc}) over Solid
  * (render/render_prim_solid.h): pyramids (verts_per_solid 5), prisms (6),
  * hexahedra (8).  srt_solid_build replaces SolidAccel::Build32
- * (render_accel_solid.cc:1795; the same tree and solid order, for 2 or more
- * solids -- the reference switches to its SAH Build below 1024);
+ * (render_accel_solid.cc:1795; the same tree and solid order for 2 to
+ * 2^28 - 1 solids: the LBVH on the GPU from 1024 solids on, and below 1024,
+ * as the reference does, its binned-SAH SolidAccel::Build (:1612-1793) on
+ * the host);
  * srt_solid_trace replaces SolidAccel::Traverse (:2345): per ray the
  * nearest entry or exit point (t, solid in hits[i].prim; u = v = 0, which
  * the reference leaves unset), skipping the solid named by prev_prim, and

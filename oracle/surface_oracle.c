@@ -3495,6 +3495,163 @@ static size_t solid_emit(so_solids *S, uint32_t root, uint32_t l, uint32_t r, in
   return off;
 }
 
+/* SolidAccel::Build (:1612-1793, binned SAH on 64 bins, costTaabb 0.2,
+ * minLeafPrimitives 4, maxTreeDepth 256), which Build32 runs below 1024
+ * solids (:1806-1809).  Float arithmetic in the reference's order. */
+static const float *sah_vert(const so_solids *S, uint32_t solid, int j) {
+  return &S->v[3 * (size_t)S->ix[(size_t)S->nv * solid + j]];
+}
+
+/* CalculateSurfaceArea (:791-799) */
+static float sah_area(const float lo[3], const float hi[3]) {
+  const float b0 = hi[0] - lo[0], b1 = hi[1] - lo[1], b2 = hi[2] - lo[2];
+  const float sum = (b0 * b1 + b1 * b2) + b2 * b0;
+  return (float)(2.0 * (double)sum);
+}
+
+/* SAHPred (:1034-1053) */
+static int sah_left(const so_solids *S, uint32_t solid, int axis, float pos) {
+  float c = 0.0f;
+  for (int j = 0; j < S->nv; j++) c += sah_vert(S, solid, j)[axis];
+  return c < pos * (float)S->nv;
+}
+
+/* std::partition of libstdc++ on bidirectional iterators (both ends) */
+static uint32_t sah_partition(so_solids *S, uint32_t first, uint32_t last, int axis, float pos) {
+  for (;;) {
+    for (;;) {
+      if (first == last) return first;
+      if (sah_left(S, S->sidx[first], axis, pos)) first++;
+      else break;
+    }
+    last--;
+    for (;;) {
+      if (first == last) return first;
+      if (!sah_left(S, S->sidx[last], axis, pos)) last--;
+      else break;
+    }
+    const uint32_t t = S->sidx[first];
+    S->sidx[first] = S->sidx[last];
+    S->sidx[last] = t;
+    first++;
+  }
+}
+
+static size_t sah_build(so_solids *S, uint32_t l, uint32_t r, int depth) {
+  const float eps = FLT_EPSILON * 16;
+  enum { BINS = 64 };
+  /* ComputeBoundingBox (:1076-1118) */
+  float bmin[3], bmax[3];
+  const float *p0 = sah_vert(S, S->sidx[l], 0);
+  for (int k = 0; k < 3; k++) {
+    bmin[k] = p0[k] - eps;
+    bmax[k] = p0[k] + eps;
+  }
+  for (uint32_t i = l; i < r; i++)
+    for (int j = 0; j < S->nv; j++) {
+      const float *p = sah_vert(S, S->sidx[i], j);
+      for (int k = 0; k < 3; k++) {
+        const float mn = p[k] - eps, mx = p[k] + eps;
+        if (bmin[k] > mn) bmin[k] = mn;
+        if (bmax[k] < mx) bmax[k] = mx;
+      }
+    }
+  const size_t me = solid_push(S);
+  so_solid_node *nd = &S->nodes[me];
+  for (int k = 0; k < 3; k++) {
+    nd->bmin[k] = bmin[k];
+    nd->bmax[k] = bmax[k];
+  }
+  const uint32_t n = r - l;
+  if (n < 4 || depth >= 256) {
+    nd->flag = 1;
+    nd->data[0] = n;
+    nd->data[1] = l;
+    return me;
+  }
+  /* ContributeBinBuffer (:833-887) */
+  static _Thread_local size_t bins[2][3][BINS];
+  memset(bins, 0, sizeof(bins));
+  float inv[3];
+  for (int k = 0; k < 3; k++) {
+    const float size = bmax[k] - bmin[k];
+    inv[k] = size > eps ? (float)BINS / size : 0.0f;
+  }
+  for (uint32_t i = l; i < r; i++) {
+    float slo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, shi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+    for (int j = 0; j < S->nv; j++) { /* GetBoundingBoxOfSolid: std::min / std::max */
+      const float *p = sah_vert(S, S->sidx[i], j);
+      for (int k = 0; k < 3; k++) {
+        if (p[k] < slo[k]) slo[k] = p[k];
+        if (shi[k] < p[k]) shi[k] = p[k];
+      }
+    }
+    for (int k = 0; k < 3; k++) {
+      size_t a = (size_t)(unsigned int)floorf((slo[k] - bmin[k]) * inv[k]);
+      size_t b = (size_t)(unsigned int)floorf((shi[k] - bmin[k]) * inv[k]);
+      if (a >= BINS) a = BINS - 1;
+      if (b >= BINS) b = BINS - 1;
+      bins[0][k][a]++;
+      bins[1][k][b]++;
+    }
+  }
+  /* FindCutFromBinBuffer (:916-988) and SAH (:890-899) */
+  const float taabb = 0.2f, ttri = (float)(1.0 - (double)taabb);
+  float bstep[3], cut[3], best[3];
+  for (int k = 0; k < 3; k++) bstep[k] = (bmax[k] - bmin[k]) * (float)(1.0 / BINS);
+  const float sa = sah_area(bmin, bmax);
+  const float inv_sa = sa > eps ? (float)(1.0 / (double)sa) : 0.0f;
+  for (int k = 0; k < 3; k++) {
+    float best_pos = bmin[k] + 0.5f * bstep[k];
+    best[k] = FLT_MAX;
+    size_t left = 0, right = n;
+    float llo[3], lhi[3], rlo[3], rhi[3];
+    for (int q = 0; q < 3; q++) {
+      llo[q] = rlo[q] = bmin[q];
+      lhi[q] = rhi[q] = bmax[q];
+    }
+    for (int i = 0; i < BINS - 1; i++) {
+      left += bins[0][k][i];
+      right -= bins[1][k][i];
+      const float pos = bmin[k] + ((float)i + 0.5f) * bstep[k];
+      lhi[k] = pos;
+      rlo[k] = pos;
+      const float sl = sah_area(llo, lhi), sr = sah_area(rlo, rhi);
+      const float t1 = ((sl * inv_sa) * (float)left) * ttri;
+      const float t2 = ((sr * inv_sa) * (float)right) * ttri;
+      const float cost = (2.0f * taabb + t1) + t2;
+      if (cost < best[k]) {
+        best[k] = cost;
+        best_pos = pos;
+      }
+    }
+    cut[k] = best_pos;
+  }
+  int ax = 0;
+  float c = best[0];
+  if (c > best[1]) {
+    ax = 1;
+    c = best[1];
+  }
+  if (c > best[2]) ax = 2;
+  uint32_t mid = l;
+  int axis = ax;
+  for (int t = 0; t < 3; t++) {
+    axis = (ax + t) % 3;
+    mid = sah_partition(S, l, r, axis, cut[axis]);
+    if (mid == l || mid == r) mid = l + (n >> 1);
+    else break;
+  }
+  const size_t lc = sah_build(S, l, mid, depth + 1);
+  const size_t rc = sah_build(S, mid, r, depth + 1);
+  nd = &S->nodes[me]; /* the node array may have moved */
+  nd->flag = 0;
+  nd->axis = axis;
+  nd->data[0] = (uint32_t)lc;
+  nd->data[1] = (uint32_t)rc;
+  return me;
+}
+
 SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, size_t n) {
   so_solids *S = (so_solids *)calloc(1, sizeof(so_solids));
   S->nv = nv;
@@ -3506,7 +3663,11 @@ SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, siz
   S->child = (uint32_t *)malloc((n + 1) * 4);
   S->lt = (uint8_t *)malloc(n + 1);
   S->rt = (uint8_t *)malloc(n + 1);
-  if (n < 2) return S;
+  if (n < 1024) { /* Build32 runs Build below 1024 solids */
+    for (size_t i = 0; i < n; i++) S->sidx[i] = (uint32_t)i;
+    if (n > 0) sah_build(S, 0, (uint32_t)n, 0);
+    return S;
+  }
   /* scene box: every vertex -+ FLT_EPSILON * 16 (ComputeBoundingBoxOMP, :1171-1262) */
   const float eps = FLT_EPSILON * 16;
   float lo[3], hi[3];

@@ -315,7 +315,7 @@ struct SceneStreams {
 void build_top_tree(const double *bmin, const double *bmax, size_t n,
                     std::vector<TopNode> &out);
 // kinds: bit k set when the scene holds elements of kind k; deep_lines: a
-// line element's tree is deeper than 62 levels.
+// line or solid element's tree is deeper than 62 levels.
 srt_status launch_scene_trace(srt_ctx *ctx, const TopNode *top, SceneWork W, uint32_t kinds,
                               bool deep_lines, const SceneStreams &ss);
 // Coherent traversal order of n rays (srt_raysort.cu): *order is a device
@@ -331,9 +331,10 @@ uint64_t line_accel_bytes(const srt_line_accel *a);
 uint64_t solid_accel_bytes(const srt_solid_accel *a);
 // A built line or solid accel as a scene element: its context, device
 // nodes and records, element count, aux (cap flag / vertices per solid)
-// and tree depth (lines).  False when the accel is not built.
+// and tree depth (lines) or whether the tree is deeper than 62 levels
+// (solids).  False when the accel is not built.
 bool line_scene_view(const srt_line_accel *a, srt_ctx **ctx, SceneElem &e, int &depth);
-bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e);
+bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e, bool &deep);
 // Exclusive prefix sum of n uint32 on the context's stream (out may alias in).
 srt_status scan_exclusive(srt_ctx *ctx, const uint32_t *in, uint32_t *out, size_t n);
 // Stable sort of (key, value) pairs by key; key_bits: how many low bits of

@@ -393,7 +393,8 @@ SRT_API srt_status srt_scene_add_solids(srt_scene *s, srt_solid_accel *acc, cons
   }
   srt_ctx *c = nullptr;
   SceneElem v{};
-  if (!solid_scene_view(acc, &c, v) || c != s->ctx) {
+  bool deep = false;
+  if (!solid_scene_view(acc, &c, v, deep) || c != s->ctx) {
     set_error("scene elements must be built accels of the scene's context");
     return SRT_ERR_INVALID;
   }
@@ -431,7 +432,9 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
       ok = line_scene_view(se.lines, &c, el[i], depth);
       deep = deep || depth + 2 > 64;
     } else if (se.solids) {
-      ok = solid_scene_view(se.solids, &c, el[i]);
+      bool sdeep = false;
+      ok = solid_scene_view(se.solids, &c, el[i], sdeep);
+      deep = deep || sdeep;
     } else {
       const srt_accel *a = se.acc;
       ok = a->built;

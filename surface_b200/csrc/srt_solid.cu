@@ -65,6 +65,7 @@ struct srt_solid_accel {
   // build before it overwrites the tree)
   cudaEvent_t ev_built = nullptr, ev_used = nullptr;
   bool used = false;
+  bool deep = false;  // tree deeper than the short walk stack (SAH builds)
   // the reference layout (Dump, export), made from the device tree on first use
   bool host_ready = false;
   std::vector<SolidNodeH> nodes;
@@ -304,15 +305,195 @@ solid_tree_kernel(const uint32_t *__restrict__ codes, srt::Topology T,
   atomicOr(err, srt::kErrTree);
 }
 
+// ------------------------------------------------------------------ SAH build
+// SolidAccel::Build (:1612-1793), which Build32 runs for fewer than 1024
+// solids: a top-down binned-SAH build on the host (the inputs are small),
+// float arithmetic in the reference's operation order, the tree in the
+// reference's node order.  Options are the defaults of SolidBuildOptions
+// (render_accel_solid.h:46-56): costTaabb 0.2, minLeafPrimitives 4,
+// maxTreeDepth 256, binSize 64.
+struct SahBuilder {
+  const float *v;
+  const uint32_t *ix;
+  int nv;
+  std::vector<uint32_t> &idx;
+  std::vector<SolidNodeH> &nodes;
+  int max_depth = 0;
+  static constexpr int kBins = 64, kMinLeaf = 4, kMaxDepth = 256;
+  static constexpr float kTaabb = 0.2f;
+
+  const float *vert(uint32_t solid, int j) const { return v + 3 * (size_t)ix[(size_t)nv * solid + j]; }
+
+  // ComputeBoundingBox (:1076-1118): every vertex -+ FLT_EPSILON * 16
+  void range_box(uint32_t l, uint32_t r, float lo[3], float hi[3]) const {
+    const float eps = FLT_EPSILON * 16;
+    const float *p0 = vert(idx[l], 0);
+    for (int k = 0; k < 3; k++) {
+      lo[k] = p0[k] - eps;
+      hi[k] = p0[k] + eps;
+    }
+    for (uint32_t i = l; i < r; i++)
+      for (int j = 0; j < nv; j++) {
+        const float *p = vert(idx[i], j);
+        for (int k = 0; k < 3; k++) {
+          const float a = p[k] - eps, b = p[k] + eps;
+          if (lo[k] > a) lo[k] = a;
+          if (hi[k] < b) hi[k] = b;
+        }
+      }
+  }
+  // CalculateSurfaceArea (:791-799): float products and sums, doubled
+  static float area(const float lo[3], const float hi[3]) {
+    const float b0 = hi[0] - lo[0], b1 = hi[1] - lo[1], b2 = hi[2] - lo[2];
+    return (float)(2.0 * (double)((b0 * b1 + b1 * b2) + b2 * b0));
+  }
+  // SAHPred (:1034-1053): the summed vertex coordinate against pos * nv
+  bool left_of(uint32_t solid, int axis, float pos) const {
+    float c = 0.0f;
+    for (int j = 0; j < nv; j++) c += vert(solid, j)[axis];
+    return c < pos * (float)nv;
+  }
+  // std::partition as libstdc++ runs it on bidirectional iterators: from
+  // both ends, swapping a misplaced pair at a time
+  uint32_t split(uint32_t l, uint32_t r, int axis, float pos) {
+    uint32_t first = l, last = r;
+    while (true) {
+      while (true) {
+        if (first == last) return first;
+        if (left_of(idx[first], axis, pos)) first++;
+        else break;
+      }
+      last--;
+      while (true) {
+        if (first == last) return first;
+        if (!left_of(idx[last], axis, pos)) last--;
+        else break;
+      }
+      std::swap(idx[first], idx[last]);
+      first++;
+    }
+  }
+  // ContributeBinBuffer + FindCutFromBinBuffer (:833-988): per axis the
+  // cheapest bin boundary; returns the cheapest axis, cut[] per axis
+  int find_cut(uint32_t l, uint32_t r, const float bmin[3], const float bmax[3], float cut[3]) const {
+    const float eps = FLT_EPSILON * 16;
+    std::vector<size_t> bins(2 * 3 * kBins, 0);
+    float inv[3];
+    for (int k = 0; k < 3; k++) {
+      const float size = bmax[k] - bmin[k];
+      inv[k] = size > eps ? (float)kBins / size : 0.0f;
+    }
+    for (uint32_t i = l; i < r; i++) {
+      float slo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, shi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
+      for (int j = 0; j < nv; j++) {  // GetBoundingBoxOfSolid: std::min / std::max
+        const float *p = vert(idx[i], j);
+        for (int k = 0; k < 3; k++) {
+          slo[k] = (p[k] < slo[k]) ? p[k] : slo[k];
+          shi[k] = (shi[k] < p[k]) ? p[k] : shi[k];
+        }
+      }
+      for (int k = 0; k < 3; k++) {
+        size_t a = (size_t)(unsigned int)std::floor((slo[k] - bmin[k]) * inv[k]);
+        size_t b = (size_t)(unsigned int)std::floor((shi[k] - bmin[k]) * inv[k]);
+        if (a >= (size_t)kBins) a = kBins - 1;
+        if (b >= (size_t)kBins) b = kBins - 1;
+        bins[0 * 3 * kBins + k * kBins + a]++;
+        bins[1 * 3 * kBins + k * kBins + b]++;
+      }
+    }
+    const size_t n = r - l;
+    const float ttri = (float)(1.0 - (double)kTaabb);
+    float bstep[3];
+    for (int k = 0; k < 3; k++) bstep[k] = (bmax[k] - bmin[k]) * (float)(1.0 / kBins);
+    const float sa = area(bmin, bmax);
+    const float inv_sa = sa > eps ? (float)(1.0 / (double)sa) : 0.0f;
+    float best[3];
+    for (int k = 0; k < 3; k++) {
+      float best_pos = bmin[k] + 0.5f * bstep[k];
+      best[k] = FLT_MAX;
+      size_t left = 0, right = n;
+      float llo[3], lhi[3], rlo[3], rhi[3];
+      for (int q = 0; q < 3; q++) {
+        llo[q] = rlo[q] = bmin[q];
+        lhi[q] = rhi[q] = bmax[q];
+      }
+      for (int i = 0; i < kBins - 1; i++) {
+        left += bins[0 * 3 * kBins + k * kBins + i];
+        right -= bins[1 * 3 * kBins + k * kBins + i];
+        const float pos = bmin[k] + ((float)i + 0.5f) * bstep[k];
+        lhi[k] = pos;
+        rlo[k] = pos;
+        const float sl = area(llo, lhi), sr = area(rlo, rhi);
+        // SAH (:890-899), left to right
+        const float cost = (2.0f * kTaabb + ((sl * inv_sa) * (float)left) * ttri) +
+                           ((sr * inv_sa) * (float)right) * ttri;
+        if (cost < best[k]) {
+          best[k] = cost;
+          best_pos = pos;
+        }
+      }
+      cut[k] = best_pos;
+    }
+    int axis = 0;
+    float c = best[0];
+    if (c > best[1]) {
+      axis = 1;
+      c = best[1];
+    }
+    if (c > best[2]) axis = 2;
+    return axis;
+  }
+  // BuildTree (:1612-1752); returns the node's index
+  uint32_t build(uint32_t l, uint32_t r, int depth) {
+    const uint32_t me = (uint32_t)nodes.size();
+    max_depth = std::max(max_depth, depth);
+    float bmin[3], bmax[3];
+    range_box(l, r, bmin, bmax);
+    nodes.push_back(SolidNodeH{});
+    const uint32_t n = r - l;
+    SolidNodeH h{};
+    for (int k = 0; k < 3; k++) {
+      h.bmin[k] = bmin[k];
+      h.bmax[k] = bmax[k];
+    }
+    if ((int)n < kMinLeaf || depth >= kMaxDepth) {
+      h.flag = 1;
+      h.data[0] = n;
+      h.data[1] = l;
+      nodes[me] = h;
+      return me;
+    }
+    float cut[3];
+    const int best = find_cut(l, r, bmin, bmax, cut);
+    uint32_t mid = l;
+    int axis = best;
+    for (int t = 0; t < 3; t++) {  // the cheapest axis first, then the others
+      axis = (best + t) % 3;
+      mid = split(l, r, axis, cut[axis]);
+      if (mid == l || mid == r) mid = l + (n >> 1);  // object median unless another axis cuts
+      else break;
+    }
+    h.flag = 0;
+    h.axis = axis;
+    h.data[0] = build(l, mid, depth + 1);
+    h.data[1] = build(mid, r, depth + 1);
+    nodes[me] = h;
+    return me;
+  }
+};
+
 // ------------------------------------------------------------------ trace
 constexpr int kSolidQ = 32;  // solids a lane queues before the warp tests them
+// walk stack entries: Build32 trees have at most 24 levels, SAH trees (Build,
+// below 1024 solids) up to 257
+constexpr int kSolidStackShort = 64, kSolidStackDeep = 264;
 
-template <int NV>
+template <int NV, int STACK>
 __global__ void __launch_bounds__(128, 3)  // 3 blocks per SM: 168 registers
 solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
                    const srt_ray *__restrict__ rays, const uint32_t *__restrict__ order,
                    size_t n, srt_hit *__restrict__ hits, float *__restrict__ normals,
-                   float *__restrict__ positions) {
+                   float *__restrict__ positions, uint32_t *__restrict__ err) {
   // Each lane walks its ray and queues the solids of the leaves it enters
   // (in the walk's order) until kSolidQ are queued or the walk ends; then
   // the lanes test their queues side by side, so the costly solid tests run
@@ -327,7 +508,7 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
   uint32_t prev = 0;
   float t = FLT_MAX, bn[3], bp[3];
   uint32_t prim = SRT_MISS;
-  int stack[64];
+  int stack[STACK];
   int sp = -1;
   uint32_t leaf_next = 0, leaf_left = 0;
   auto start = [&]() {
@@ -371,6 +552,11 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
           const int axis = (int)(nd.w1 >> 29);
           const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
           const int nearc = sign[axis];
+          if (sp + 2 >= STACK) {  // deeper than the build's trees: stop the ray
+            atomicOr(err, srt::kErrStack);
+            sp = -1;
+            continue;
+          }
           stack[++sp] = nearc ? left : right;  // far
           stack[++sp] = nearc ? right : left;  // near
           continue;
@@ -419,7 +605,7 @@ srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
 
 namespace srt {
 uint64_t solid_accel_bytes(const srt_solid_accel *a) { return a->dnodes.cap + a->drecs.cap; }
-bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e) {
+bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e, bool &deep) {
   if (!a || !a->built) return false;
   cudaEventSynchronize(a->ev_built);  // the build may have run on another stream
   *ctx = a->ctx;
@@ -430,6 +616,7 @@ bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e) {
   e.prims = a->drecs.as<float4>();
   e.sidx = nullptr;
   e.scene = nullptr;
+  deep = a->deep;
   return true;
 }
 }  // namespace srt
@@ -497,6 +684,82 @@ srt_status solid_host_layout(srt_solid_accel *a) {
   return SRT_OK;
 }
 
+// Build32 below kSahMax solids: SolidAccel::Build on the host (SahBuilder),
+// then the tree and the records in leaf order are uploaded.  v / ix may be
+// host or device memory (device copies are read after the context's
+// stream).
+constexpr size_t kSahMax = 1024;
+
+srt_status solid_build_sah(srt_solid_accel *a, int nv, const float *v, size_t nverts,
+                           const uint32_t *ix, size_t n) {
+  srt_ctx *ctx = a->ctx;
+  const size_t refs = n * (size_t)nv;
+  std::vector<float> hv(3 * nverts);
+  std::vector<uint32_t> hix(refs);
+  cudaError_t e = cudaMemcpyAsync(hv.data(), v, hv.size() * 4, cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(hix.data(), ix, refs * 4, cudaMemcpyDefault, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_status(e, "solid inputs");
+  for (size_t i = 0; i < refs; i++)
+    if (hix[i] >= nverts) {
+      set_error("srt_solid_build: an index names a vertex beyond nverts");
+      return SRT_ERR_INVALID;
+    }
+  a->nodes.clear();
+  a->idx.resize(n);
+  for (size_t i = 0; i < n; i++) a->idx[i] = (uint32_t)i;
+  SahBuilder B{hv.data(), hix.data(), nv, a->idx, a->nodes};
+  B.build(0, (uint32_t)n, 0);
+  // device layout: node k is reference node k; records in leaf order
+  std::vector<SNode> dn(a->nodes.size());
+  for (size_t k = 0; k < dn.size(); k++) {
+    const SolidNodeH &h = a->nodes[k];
+    for (int c = 0; c < 3; c++) {
+      dn[k].bmin[c] = h.bmin[c];
+      dn[k].bmax[c] = h.bmax[c];
+    }
+    if (h.flag) {
+      dn[k].w0 = h.data[1];
+      dn[k].w1 = kSolidLeaf | h.data[0];
+    } else {
+      dn[k].w0 = h.data[0];
+      dn[k].w1 = h.data[1] | ((uint32_t)h.axis << 29);
+    }
+  }
+  const int rf = rec_floats(nv);
+  std::vector<float> recs((size_t)rf * n, 0.0f);
+  for (size_t j = 0; j < n; j++) {
+    const uint32_t p = a->idx[j];
+    float *r = recs.data() + (size_t)rf * j;
+    for (int q = 0; q < nv; q++)
+      for (int k = 0; k < 3; k++) r[3 * q + k] = hv[3 * (size_t)hix[(size_t)nv * p + q] + k];
+    uint32_t pid = p;
+    std::memcpy(&r[3 * nv], &pid, 4);
+  }
+  if ((e = a->dnodes.ensure(dn.size() * sizeof(SNode))) != cudaSuccess ||
+      (e = a->drecs.ensure(recs.size() * 4)) != cudaSuccess ||
+      (e = a->dorder.ensure(n * 4)) != cudaSuccess)
+    return cuda_status(e, "solid accel");
+  e = cudaMemcpyAsync(a->dnodes.p, dn.data(), dn.size() * sizeof(SNode), cudaMemcpyHostToDevice,
+                      ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->drecs.p, recs.data(), recs.size() * 4, cudaMemcpyHostToDevice,
+                        ctx->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(a->dorder.p, a->idx.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream);
+  if (e == cudaSuccess) e = cudaEventRecord(a->ev_built, ctx->stream);
+  // the host vectors go out of scope: the copies must be done
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess) return cuda_status(e, "solid upload");
+  a->deep = B.max_depth + 2 > kSolidStackShort;
+  a->host_ready = true;
+  a->nv = nv;
+  a->n = n;
+  a->built = true;
+  return SRT_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -555,6 +818,8 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
   // the latest trace (on any stream) reads the tree this build overwrites
   if (a->used && (e = cudaStreamWaitEvent(ctx->stream, a->ev_used, 0)) != cudaSuccess)
     return cuda_status(e, "solid build");
+  if (n < kSahMax) return solid_build_sah(a, nv, d_v, nverts, d_ix, n);
+  a->deep = false;
   if ((e = a->dbox.ensure(64)) != cudaSuccess || (e = a->dcodes.ensure(n * 4)) != cudaSuccess ||
       (e = a->dorder.ensure(n * 4)) != cudaSuccess ||
       (e = a->dinfo.ensure(sizeof(srt::SceneInfo))) != cudaSuccess ||
@@ -666,9 +931,13 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
   }
   // as many blocks as the SMs hold at once: lanes take their next ray as
   // soon as they finish one
-  const void *kfn = a->nv == 5   ? (const void *)solid_trace_kernel<5>
-                    : a->nv == 6 ? (const void *)solid_trace_kernel<6>
-                                 : (const void *)solid_trace_kernel<8>;
+  const void *kfn =
+      a->deep ? (a->nv == 5   ? (const void *)solid_trace_kernel<5, kSolidStackDeep>
+                 : a->nv == 6 ? (const void *)solid_trace_kernel<6, kSolidStackDeep>
+                              : (const void *)solid_trace_kernel<8, kSolidStackDeep>)
+              : (a->nv == 5   ? (const void *)solid_trace_kernel<5, kSolidStackShort>
+                 : a->nv == 6 ? (const void *)solid_trace_kernel<6, kSolidStackShort>
+                              : (const void *)solid_trace_kernel<8, kSolidStackShort>);
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 128, 0) != cudaSuccess ||
       per_sm < 1) {
@@ -687,12 +956,10 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
   // the build may have run on another stream
   if ((e = cudaStreamWaitEvent(ctx->stream, a->ev_built, 0)) != cudaSuccess)
     return cuda_status(e, "solid trace");
-  if (a->nv == 5)
-    solid_trace_kernel<5><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
-  else if (a->nv == 6)
-    solid_trace_kernel<6><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
-  else
-    solid_trace_kernel<8><<<grid, 128, 0, ctx->stream>>>(nd, rc, rr, ord, n, dh, dn, dp);
+  void *args[] = {(void *)&nd, (void *)&rc, (void *)&rr, (void *)&ord, (void *)&n,
+                  (void *)&dh, (void *)&dn, (void *)&dp, (void *)&ctx->d_err};
+  if ((e = cudaLaunchKernel(kfn, dim3(grid), dim3(128), args, 0, ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid trace");
   ctx->launches++;
   if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid trace");
   if ((e = cudaEventRecord(a->ev_used, ctx->stream)) != cudaSuccess)

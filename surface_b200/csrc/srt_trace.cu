@@ -1985,19 +1985,23 @@ __device__ __forceinline__ bool elem_hit_lines(const SceneElem &e, const RayF &l
 
 // Closest hit of a local ray in a solid element (SolidAccel::Traverse, the
 // previous solid skipped inside the element the ray left): u = v = 0.
+// STACK: the walk's stack.
+template <int STACK>
 __device__ __forceinline__ bool elem_hit_solids(const SceneElem &e, const RayF &lr,
-                                                uint32_t prev, Best &b) {
+                                                uint32_t prev, Best &b, uint32_t *err) {
   using namespace srt_solid_walk;
   const SNode *nodes = static_cast<const SNode *>(e.nodes);
   const float *recs = reinterpret_cast<const float *>(e.prims);
   float t, bp[3], bn[3];
   uint32_t prim;
+  bool ok;
   if (e.aux == 5)
-    solid_walk<5>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+    ok = solid_walk<5, STACK>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
   else if (e.aux == 6)
-    solid_walk<6>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+    ok = solid_walk<6, STACK>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
   else
-    solid_walk<8>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+    ok = solid_walk<8, STACK>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+  if (!ok) atomicOr(err, kErrStack);
   if (!(t < FLT_MAX)) return false;
   b.t = t;
   b.u = b.v = 0.0f;
@@ -2007,7 +2011,8 @@ __device__ __forceinline__ bool elem_hit_solids(const SceneElem &e, const RayF &
 
 // The whole loop in one thread, for the rays with more candidates than
 // the per-ray slots hold and the rays that meet a line or solid element.
-// LSTACK: the line walks' stack (the deepest line tree + 2 at least).
+// LSTACK: the line and solid walks' stack (the deepest such tree + 2 at
+// least).
 template <int LSTACK>
 __global__ void __launch_bounds__(128)
 scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
@@ -2038,8 +2043,9 @@ scene_loop_kernel(const TopNode *__restrict__ top, SceneWork W) {
         const double ro3[3] = {r0.o[0], r0.o[1], r0.o[2]}, rd3[3] = {r0.d[0], r0.d[1], r0.d[2]};
         const RayF lr = local_ray(e, ro3, rd3, lo, ld);
         const bool same = W.prev_element && __ldg(&W.prev_element[i]) == cid[q];
-        hit = e.kind == kSceneLines ? elem_hit_lines<LSTACK>(e, lr, b, c)
-                                    : elem_hit_solids(e, lr, same ? prev_prim : kNone, b);
+        hit = e.kind == kSceneLines
+                  ? elem_hit_lines<LSTACK>(e, lr, b, c)
+                  : elem_hit_solids<LSTACK>(e, lr, same ? prev_prim : kNone, b, W.err);
       } else if (e.kind == SRT_TETRAHEDRA)
         hit = elem_hit<SRT_TETRAHEDRA>(W, i, cid[q], e, r0, prev_prim, prev_t, lo, ld, b, w);
       else if (e.kind == SRT_TRIANGLES)

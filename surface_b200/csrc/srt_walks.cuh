@@ -644,9 +644,11 @@ __device__ __forceinline__ void solid_test(const float *__restrict__ recs, uint3
 
 // SolidAccel::Traverse for one ray, one thread: the reference's walk (near
 // child first, every solid of every entered leaf tested, no distance
-// culling).  prim = 0xFFFFFFFF and t = FLT_MAX when nothing is hit.
-template <int NV>
-__device__ __forceinline__ void solid_walk(const SNode *__restrict__ nodes,
+// culling).  prim = 0xFFFFFFFF and t = FLT_MAX when nothing is hit.  STACK:
+// the walk's stack (the tree's depth + 2 at least); returns false (the walk
+// stopped) for a deeper tree.
+template <int NV, int STACK>
+__device__ __forceinline__ bool solid_walk(const SNode *__restrict__ nodes,
                                            const float *__restrict__ recs,
                                            const float org[3], const float dir[3],
                                            uint32_t prev, float &t, uint32_t &prim,
@@ -664,7 +666,7 @@ __device__ __forceinline__ void solid_walk(const SNode *__restrict__ nodes,
   const D3 dorg = {org[0], org[1], org[2]}, ddir = {dir[0], dir[1], dir[2]};
   t = FLT_MAX;
   prim = 0xffffffffu;
-  int stack[64];
+  int stack[STACK];
   int sp = 0;
   stack[0] = 0;
   while (sp >= 0) {
@@ -678,6 +680,7 @@ __device__ __forceinline__ void solid_walk(const SNode *__restrict__ nodes,
       const int axis = (int)(nd.w1 >> 29);
       const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
       const int nearc = sign[axis];
+      if (sp + 2 >= STACK) return false;
       stack[++sp] = nearc ? left : right;  // far
       stack[++sp] = nearc ? right : left;  // near
       continue;
@@ -686,6 +689,7 @@ __device__ __forceinline__ void solid_walk(const SNode *__restrict__ nodes,
     for (uint32_t j = first; j < first + cnt; j++)
       solid_test<NV>(recs, j, prev, dorg, ddir, jax, t, prim, bp, bn);
   }
+  return true;
 }
 
 }  // namespace srt_solid_walk

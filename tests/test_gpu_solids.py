@@ -17,7 +17,7 @@ from conftest import bits
 
 pytestmark = pytest.mark.gpu
 
-CASES = {"hexahedra": (8, 14), "prisms": (6, 11), "pyramids": (5, 8)}
+CASES = {"hexahedra": (8, 14), "prisms": (6, 11), "pyramids": (5, 8)}  # >= 1024 solids
 
 
 def _check(nv, v, ix, rays, device_inputs=False):
@@ -65,6 +65,18 @@ def test_small_meshes(nsolids):
     v, ix = S.solid_grid(8, 4, seed=2)
     ix = ix[:nsolids]
     _check(8, v, ix, S.solid_rays(32))
+
+
+@pytest.mark.parametrize("nv,g,m", [(8, 9, 500), (6, 7, 686), (5, 5, 750), (8, 11, 1023)])
+def test_sah_build_below_1024(nv, g, m):
+    """Fewer than 1024 solids: the reference's binned-SAH Build (host build,
+    uploaded tree): tree, order, hits, normals and positions equal the
+    oracle's, from host and device inputs."""
+    v, ix = S.solid_grid(nv, g, seed=3)
+    ix = ix[:m]
+    rays = S.solid_rays(64, seed=nv)
+    _check(nv, v, ix, rays)
+    _check(nv, v, ix, rays, device_inputs=True)
 
 
 def test_dump_bbox_and_errors(tmp_path):

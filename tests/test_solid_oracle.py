@@ -57,3 +57,52 @@ def test_solids_match_reference(case):
     assert np.array_equal(bits(oh2.view(np.float32).reshape(-1, 4)),
                           bits(rh2.view(np.float32).reshape(-1, 4)))
     assert (rh2["prim"] != rays2["prev_prim"]).all()
+
+
+def _raw(nodes):
+    """Node bytes with the leaves' axis cleared (the reference leaves it unset)."""
+    x = nodes.copy()
+    x["axis"][x["flag"] == 1] = 0
+    return x.tobytes()
+
+
+def _sah_cases():
+    out = []
+    for nv, g in ((8, 9), (6, 7), (5, 5)):
+        v, ix = S.solid_grid(nv, g, seed=3)
+        for m in (2, 3, 4, 5, 17, 100, 500, ix.shape[0]):
+            if m < 1024:
+                out.append((f"nv{nv}-{m}", nv, v, ix[:m]))
+    v, ix = S.solid_grid(8, 6, seed=5)
+    out.append(("duplicates", 8, v, np.concatenate([ix[:50]] * 4)))
+    flat = v.copy()
+    flat[:, 2] = 0.5
+    out.append(("flat", 8, flat, ix[:300]))
+    return out
+
+
+@needs_ref
+@pytest.mark.parametrize("name,nv,v,ix", _sah_cases(), ids=[c[0] for c in _sah_cases()])
+def test_sah_build_below_1024_matches_reference(name, nv, v, ix):
+    """Below 1024 solids Build32 runs SolidAccel::Build (binned SAH,
+    render/render_accel_solid.cc:1612-1793): the oracle's tree (node for
+    node, in the reference's order), solid order and hits equal the
+    reference's."""
+    o = O.OracleSolids(nv, v, ix)
+    r = O.RefSolids(nv, v, ix)
+    on, oi = o.export()
+    rn, ri = r.dump()
+    assert _raw(on) == _raw(rn)
+    assert np.array_equal(oi, ri)
+    rays = S.solid_rays(48, seed=nv)
+    oh, onr, op = o.trace(rays)
+    rh, rnr, rp = r.trace(rays)
+    assert np.array_equal(bits(oh.view(np.float32).reshape(-1, 4)),
+                          bits(rh.view(np.float32).reshape(-1, 4)))
+    assert np.array_equal(bits(onr), bits(rnr)) and np.array_equal(bits(op), bits(rp))
+    rays2 = secondary(rays, rh, rp, nv)
+    if rays2.size:
+        oh2, _, _ = o.trace(rays2)
+        rh2, _, _ = r.trace(rays2)
+        assert np.array_equal(bits(oh2.view(np.float32).reshape(-1, 4)),
+                              bits(rh2.view(np.float32).reshape(-1, 4)))
