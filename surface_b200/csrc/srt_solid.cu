@@ -531,6 +531,8 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
     leaf_left = 0;
   };
   bool live = k < n;
+  bool overflow = false;  // reported once, after the loop (an atomic inside it
+                          // made the kernel several times slower)
   if (live) start();
   while (__any_sync(0xffffffffu, live)) {
     int len = 0;
@@ -553,7 +555,7 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
           const int right = (int)(nd.w1 & 0x1fffffffu), left = (int)nd.w0;
           const int nearc = sign[axis];
           if (sp + 2 >= STACK) {  // deeper than the build's trees: stop the ray
-            atomicOr(err, srt::kErrStack);
+            overflow = true;
             sp = -1;
             continue;
           }
@@ -585,6 +587,7 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
       if (live) start();
     }
   }
+  if (overflow) atomicOr(err, srt::kErrStack);
 }
 
 srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
