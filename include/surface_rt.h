@@ -717,6 +717,15 @@ SRT_API srt_status srt_solid_destroy(srt_solid_accel *accel);
 SRT_API srt_status srt_solid_build(srt_solid_accel *accel, int32_t verts_per_solid,
                                    const float *vertices, size_t nverts,
                                    const uint32_t *indices, size_t nsolids);
+/* The same with double-precision positions: Solid::dvertices with
+ * isDoublePrecisionPos (render/render_prim_solid.h).  As the reference does,
+ * the scene box and node boxes pad each double coordinate in double and
+ * round to float, the Morton codes and SAH bins use the positions rounded
+ * to float, SAHPredD sums in double, and the Pluecker tests take the
+ * doubles (render_accel_solid.cc:1628-1640, 1836-1880, 2243-2250). */
+SRT_API srt_status srt_solid_build_double(srt_solid_accel *accel, int32_t verts_per_solid,
+                                          const double *vertices, size_t nverts,
+                                          const uint32_t *indices, size_t nsolids);
 SRT_API srt_status srt_solid_trace(srt_solid_accel *accel, const srt_ray *rays, size_t n,
                                    srt_hit *hits, float *normals, float *positions);
 SRT_API srt_status srt_solid_bbox(srt_solid_accel *accel, double bmin[3], double bmax[3]);

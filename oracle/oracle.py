@@ -140,6 +140,8 @@ def lib():
         L.so_line_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int]
         L.so_solid_build.restype = _P
         L.so_solid_build.argtypes = [C.c_int, _P, _P, _SZ]
+        L.so_solid_build_d.restype = _P
+        L.so_solid_build_d.argtypes = [C.c_int, _P, _P, _SZ]
         L.so_solid_free.argtypes = [_P]
         L.so_solid_num_nodes.restype = _SZ
         L.so_solid_num_nodes.argtypes = [_P]
@@ -216,6 +218,8 @@ def ref():
         L.ref_line_trace.argtypes = [_P, _P, _SZ, _P, _P, C.c_int, C.c_int]
         L.ref_solid_build.restype = _P
         L.ref_solid_build.argtypes = [C.c_int, _P, _P, _SZ]
+        L.ref_solid_build_d.restype = _P
+        L.ref_solid_build_d.argtypes = [C.c_int, _P, _P, _SZ]
         L.ref_solid_free.argtypes = [_P]
         L.ref_solid_dump.argtypes = [_P, C.c_char_p]
         L.ref_solid_bbox.argtypes = [_P, _P, _P]
@@ -1116,16 +1120,25 @@ def parse_solid_dump(raw):
     return parse_line_dump(raw)
 
 
+def _solid_verts(verts):
+    """float64 vertices keep double precision (Solid::dvertices); any other
+    dtype is taken as float32."""
+    v = np.asarray(verts)
+    dt = np.float64 if v.dtype == np.float64 else np.float32
+    return np.ascontiguousarray(v, dt).reshape(-1)
+
+
 class OracleSolids:
     """The restatement of SolidAccel::Build32 / Traverse (nv = 5 pyramids,
-    6 prisms, 8 hexahedra)."""
+    6 prisms, 8 hexahedra); float64 vertices are double-precision positions."""
 
     def __init__(self, nv, verts, indices):
         self.nv = int(nv)
-        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.verts = _solid_verts(verts)
         self.ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
         self.n = self.ix.size // self.nv
-        self.h = lib().so_solid_build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
+        build = lib().so_solid_build_d if self.verts.dtype == np.float64 else lib().so_solid_build
+        self.h = build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
 
     def export(self):
         nn = lib().so_solid_num_nodes(self.h)
@@ -1160,10 +1173,11 @@ class RefSolids:
             raise RuntimeError("reference harness not built")
         self.L = L
         self.nv = int(nv)
-        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        self.verts = _solid_verts(verts)
         self.ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
         self.n = self.ix.size // self.nv
-        self.h = L.ref_solid_build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
+        build = L.ref_solid_build_d if self.verts.dtype == np.float64 else L.ref_solid_build
+        self.h = build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
 
     def dump(self):
         with tempfile.TemporaryDirectory() as td:

@@ -685,6 +685,24 @@ REF_API void *ref_solid_build(int nv, const float *verts, const uint32_t *indice
   return h;
 }
 
+// The same with double-precision positions (Solid::dvertices).
+REF_API void *ref_solid_build_d(int nv, const double *dverts, const uint32_t *indices, size_t n) {
+  SolidHandle *h = new SolidHandle();
+  memset(&h->solids, 0, sizeof(h->solids));
+  h->solids.numVertsPerSolid = nv;
+  h->solids.numSolids = n;
+  h->solids.vertices = nullptr;
+  h->solids.dvertices = dverts;
+  h->solids.isDoublePrecisionPos = true;
+  h->solids.indices = const_cast<uint32_t *>(indices);
+  SolidBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build32(&h->solids, opt);
+  }
+  return h;
+}
+
 REF_API void ref_solid_free(void *p) { delete static_cast<SolidHandle *>(p); }
 
 REF_API int ref_solid_dump(void *p, const char *path) {

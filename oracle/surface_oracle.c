@@ -3431,21 +3431,39 @@ typedef struct {
   size_t nnodes, ncap;
   uint32_t *sidx, *code, *child;
   uint8_t *lt, *rt;
+  const double *dv; /* double-precision positions (isDoublePrecisionPos), else NULL */
 } so_solids;
+
+/* Vertex coordinates: as float, as double, and padded by FLT_EPSILON * 16
+ * (ComputeBoundingBox*: float positions in float; double positions in
+ * double, then rounded to float). */
+static inline float s_f(const so_solids *S, size_t f, int k) {
+  return S->dv ? (float)S->dv[3 * f + k] : S->v[3 * f + k];
+}
+static inline double s_d(const so_solids *S, size_t f, int k) {
+  return S->dv ? S->dv[3 * f + k] : (double)S->v[3 * f + k];
+}
+static inline float s_lo(const so_solids *S, size_t f, int k) {
+  const float eps = FLT_EPSILON * 16;
+  return S->dv ? (float)(S->dv[3 * f + k] - (double)eps) : S->v[3 * f + k] - eps;
+}
+static inline float s_hi(const so_solids *S, size_t f, int k) {
+  const float eps = FLT_EPSILON * 16;
+  return S->dv ? (float)(S->dv[3 * f + k] + (double)eps) : S->v[3 * f + k] + eps;
+}
 
 /* Leaf box over sorted solids [l, r) (ComputeBoundingBox30, :1121-1169). */
 static void solid_box(const so_solids *S, size_t l, size_t r, float bmin[3], float bmax[3]) {
-  const float eps = FLT_EPSILON * 16;
   const uint32_t f0 = S->ix[(size_t)S->nv * S->sidx[l]];
   for (int k = 0; k < 3; k++) {
-    bmin[k] = S->v[3 * (size_t)f0 + k] - eps;
-    bmax[k] = S->v[3 * (size_t)f0 + k] + eps;
+    bmin[k] = s_lo(S, f0, k);
+    bmax[k] = s_hi(S, f0, k);
   }
   for (size_t i = l; i < r; i++)
     for (int j = 0; j < S->nv; j++) {
       const uint32_t f = S->ix[(size_t)S->nv * S->sidx[i] + j];
       for (int k = 0; k < 3; k++) {
-        const float lo = S->v[3 * (size_t)f + k] - eps, hi = S->v[3 * (size_t)f + k] + eps;
+        const float lo = s_lo(S, f, k), hi = s_hi(S, f, k);
         if (bmin[k] > lo) bmin[k] = lo;
         if (bmax[k] < hi) bmax[k] = hi;
       }
@@ -3498,8 +3516,8 @@ static size_t solid_emit(so_solids *S, uint32_t root, uint32_t l, uint32_t r, in
 /* SolidAccel::Build (:1612-1793, binned SAH on 64 bins, costTaabb 0.2,
  * minLeafPrimitives 4, maxTreeDepth 256), which Build32 runs below 1024
  * solids (:1806-1809).  Float arithmetic in the reference's order. */
-static const float *sah_vert(const so_solids *S, uint32_t solid, int j) {
-  return &S->v[3 * (size_t)S->ix[(size_t)S->nv * solid + j]];
+static size_t sah_vert(const so_solids *S, uint32_t solid, int j) {
+  return S->ix[(size_t)S->nv * solid + j];
 }
 
 /* CalculateSurfaceArea (:791-799) */
@@ -3509,10 +3527,15 @@ static float sah_area(const float lo[3], const float hi[3]) {
   return (float)(2.0 * (double)sum);
 }
 
-/* SAHPred (:1034-1053) */
+/* SAHPred / SAHPredD (:1034-1074): a float sum (double addends added in
+ * double) against pos * nv (float; double for double positions) */
 static int sah_left(const so_solids *S, uint32_t solid, int axis, float pos) {
   float c = 0.0f;
-  for (int j = 0; j < S->nv; j++) c += sah_vert(S, solid, j)[axis];
+  if (S->dv) {
+    for (int j = 0; j < S->nv; j++) c = (float)((double)c + s_d(S, sah_vert(S, solid, j), axis));
+    return (double)c < (double)pos * (double)(float)S->nv;
+  }
+  for (int j = 0; j < S->nv; j++) c += s_f(S, sah_vert(S, solid, j), axis);
   return c < pos * (float)S->nv;
 }
 
@@ -3542,16 +3565,16 @@ static size_t sah_build(so_solids *S, uint32_t l, uint32_t r, int depth) {
   enum { BINS = 64 };
   /* ComputeBoundingBox (:1076-1118) */
   float bmin[3], bmax[3];
-  const float *p0 = sah_vert(S, S->sidx[l], 0);
+  const size_t p0 = sah_vert(S, S->sidx[l], 0);
   for (int k = 0; k < 3; k++) {
-    bmin[k] = p0[k] - eps;
-    bmax[k] = p0[k] + eps;
+    bmin[k] = s_lo(S, p0, k);
+    bmax[k] = s_hi(S, p0, k);
   }
   for (uint32_t i = l; i < r; i++)
     for (int j = 0; j < S->nv; j++) {
-      const float *p = sah_vert(S, S->sidx[i], j);
+      const size_t pj = sah_vert(S, S->sidx[i], j);
       for (int k = 0; k < 3; k++) {
-        const float mn = p[k] - eps, mx = p[k] + eps;
+        const float mn = s_lo(S, pj, k), mx = s_hi(S, pj, k);
         if (bmin[k] > mn) bmin[k] = mn;
         if (bmax[k] < mx) bmax[k] = mx;
       }
@@ -3580,10 +3603,11 @@ static size_t sah_build(so_solids *S, uint32_t l, uint32_t r, int depth) {
   for (uint32_t i = l; i < r; i++) {
     float slo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, shi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
     for (int j = 0; j < S->nv; j++) { /* GetBoundingBoxOfSolid: std::min / std::max */
-      const float *p = sah_vert(S, S->sidx[i], j);
+      const size_t pj = sah_vert(S, S->sidx[i], j);
       for (int k = 0; k < 3; k++) {
-        if (p[k] < slo[k]) slo[k] = p[k];
-        if (shi[k] < p[k]) shi[k] = p[k];
+        const float x = s_f(S, pj, k);
+        if (x < slo[k]) slo[k] = x;
+        if (shi[k] < x) shi[k] = x;
       }
     }
     for (int k = 0; k < 3; k++) {
@@ -3652,10 +3676,12 @@ static size_t sah_build(so_solids *S, uint32_t l, uint32_t r, int depth) {
   return me;
 }
 
-SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, size_t n) {
+static so_solids *solid_build(int nv, const float *v, const double *dv, const uint32_t *ix,
+                              size_t n) {
   so_solids *S = (so_solids *)calloc(1, sizeof(so_solids));
   S->nv = nv;
   S->v = v;
+  S->dv = dv;
   S->ix = ix;
   S->n = n;
   S->sidx = (uint32_t *)malloc((n + 1) * 4);
@@ -3669,16 +3695,15 @@ SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, siz
     return S;
   }
   /* scene box: every vertex -+ FLT_EPSILON * 16 (ComputeBoundingBoxOMP, :1171-1262) */
-  const float eps = FLT_EPSILON * 16;
   float lo[3], hi[3];
   for (int k = 0; k < 3; k++) {
-    lo[k] = v[3 * (size_t)ix[0] + k] - eps;
-    hi[k] = v[3 * (size_t)ix[0] + k] + eps;
+    lo[k] = s_lo(S, ix[0], k);
+    hi[k] = s_hi(S, ix[0], k);
   }
   for (size_t i = 0; i < n * (size_t)nv; i++)
     for (int k = 0; k < 3; k++) {
-      lo[k] = fmin_ref(lo[k], v[3 * (size_t)ix[i] + k] - eps);
-      hi[k] = fmax_ref(hi[k], v[3 * (size_t)ix[i] + k] + eps);
+      lo[k] = fmin_ref(lo[k], s_lo(S, ix[i], k));
+      hi[k] = fmax_ref(hi[k], s_hi(S, ix[i], k));
     }
   /* CalculateMortonCodesSolidFloat30 (render/render_prefix_tree_util.cc:347-382) */
   float inv[3];
@@ -3687,7 +3712,7 @@ SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, siz
   for (size_t i = 0; i < n; i++) {
     float c[3] = {0.0f, 0.0f, 0.0f};
     for (int j = 0; j < nv; j++)
-      for (int k = 0; k < 3; k++) c[k] = c[k] + v[3 * (size_t)ix[(size_t)nv * i + j] + k];
+      for (int k = 0; k < 3; k++) c[k] = c[k] + s_f(S, ix[(size_t)nv * i + j], k);
     for (int k = 0; k < 3; k++) c[k] *= invdiv;
     S->code[i] = morton_of(c, lo, inv);
     S->sidx[i] = (uint32_t)i;
@@ -3708,6 +3733,15 @@ SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, siz
   rt->data[0] = (uint32_t)left;
   rt->data[1] = (uint32_t)right;
   return S;
+}
+
+SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, size_t n) {
+  return solid_build(nv, v, NULL, ix, n);
+}
+
+/* Double-precision positions (Solid::dvertices, isDoublePrecisionPos). */
+SO_API so_solids *so_solid_build_d(int nv, const double *dv, const uint32_t *ix, size_t n) {
+  return solid_build(nv, NULL, dv, ix, n);
 }
 
 SO_API void so_solid_free(so_solids *S) {
@@ -3924,8 +3958,8 @@ static void solid_trace_one(const so_solids *S, const so_ray *ray, so_hit *hit, 
         if (p == ray->prev_prim) continue;
         d3 vv[8];
         for (int q = 0; q < S->nv; q++) {
-          const float *x = &S->v[3 * (size_t)S->ix[(size_t)S->nv * p + q]];
-          vv[q] = (d3){x[0], x[1], x[2]};
+          const size_t f = S->ix[(size_t)S->nv * p + q];
+          vv[q] = (d3){s_d(S, f, 0), s_d(S, f, 1), s_d(S, f, 2)};
         }
         so_sisect is[2];
         memset(is, 0, sizeof(is));

@@ -246,10 +246,13 @@ struct TopNode {
 };
 // Scene element kinds beyond srt_kind: line and solid accels.
 constexpr int32_t kSceneLines = 3, kSceneSolids = 4;
+// SceneElem.aux bit of a solid element with double-precision positions.
+constexpr int32_t kSolidAuxDouble = 256;
 // One element of a scene: a built accel and its transforms, 4x4 doubles in
 // the reference's Matrixd layout (m[row][col], p' = p m + m[3]).  Line and
 // solid elements keep their device nodes in nodes and records in prims;
-// aux: the line accel's cap flag, the solid accel's vertices per solid.
+// aux: the line accel's cap flag, the solid accel's vertices per solid (|
+// kSolidAuxDouble for double-precision positions).
 struct SceneElem {
   int32_t kind;
   uint32_t nprims;

@@ -66,6 +66,7 @@ struct srt_solid_accel {
   cudaEvent_t ev_built = nullptr, ev_used = nullptr;
   bool used = false;
   bool deep = false;  // tree deeper than the short walk stack (SAH builds)
+  bool dbl = false;   // double-precision positions (records of doubles)
   // the reference layout (Dump, export), made from the device tree on first use
   bool host_ready = false;
   std::vector<SolidNodeH> nodes;
@@ -77,7 +78,22 @@ namespace {
 using srt::DevBuf;
 
 // ------------------------------------------------------------------ build
-__global__ void solid_morton_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+// A vertex coordinate padded by FLT_EPSILON * 16 (ComputeBoundingBox*'s
+// `real v = vertices[i] -+ kEPS`): float positions in float, double
+// positions in double, then rounded to float.
+__host__ __device__ __forceinline__ float pad_lo(float x) { return x - FLT_EPSILON * 16; }
+__host__ __device__ __forceinline__ float pad_hi(float x) { return x + FLT_EPSILON * 16; }
+__host__ __device__ __forceinline__ float pad_lo(double x) {
+  return (float)(x - (double)(FLT_EPSILON * 16));
+}
+__host__ __device__ __forceinline__ float pad_hi(double x) {
+  return (float)(x + (double)(FLT_EPSILON * 16));
+}
+
+// CalculateMortonCodesSolid{Float,Double}30: the centroid of the vertices
+// rounded to float.
+template <typename T>
+__global__ void solid_morton_kernel(const T *__restrict__ v, const uint32_t *__restrict__ ix,
                                     int nv, size_t n, float lx, float ly, float lz, float ix_,
                                     float iy, float iz, uint32_t *__restrict__ codes) {
   const float invdiv = 1.0f / (float)nv;
@@ -86,7 +102,7 @@ __global__ void solid_morton_kernel(const float *__restrict__ v, const uint32_t 
     float c[3] = {0.0f, 0.0f, 0.0f};
     for (int j = 0; j < nv; j++) {
       const uint32_t f = ix[(size_t)nv * i + j];
-      for (int k = 0; k < 3; k++) c[k] = c[k] + v[3 * (size_t)f + k];
+      for (int k = 0; k < 3; k++) c[k] = c[k] + (float)v[3 * (size_t)f + k];
     }
     for (int k = 0; k < 3; k++) c[k] *= invdiv;
     const uint32_t qx = srt::f2u32_x86((c[0] - lx) * ix_);
@@ -96,20 +112,31 @@ __global__ void solid_morton_kernel(const float *__restrict__ v, const uint32_t 
   }
 }
 
-__global__ void solid_gather_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+// The solid's index in a record's word after the vertices.
+__host__ __device__ __forceinline__ void rec_id(float *r, uint32_t p) {
+  std::memcpy(r, &p, 4);
+}
+__host__ __device__ __forceinline__ void rec_id(double *r, uint32_t p) {
+  const unsigned long long w = p;
+  std::memcpy(r, &w, 8);
+}
+
+// Records in leaf order: the solid's vertices as given (T), its index.
+template <typename T>
+__global__ void solid_gather_kernel(const T *__restrict__ v, const uint32_t *__restrict__ ix,
                                     const uint32_t *__restrict__ order, int nv, size_t n,
-                                    float *__restrict__ recs) {
-  const int rf = rec_floats(nv);
+                                    T *__restrict__ recs) {
+  const int rw = rec_bytes<T>(nv) / (int)sizeof(T);
   for (size_t j = blockIdx.x * (size_t)blockDim.x + threadIdx.x; j < n;
        j += (size_t)gridDim.x * blockDim.x) {
     const uint32_t p = order[j];
-    float *r = recs + (size_t)rf * j;
+    T *r = recs + (size_t)rw * j;
     for (int q = 0; q < nv; q++) {
       const uint32_t f = ix[(size_t)nv * p + q];
       for (int k = 0; k < 3; k++) r[3 * q + k] = v[3 * (size_t)f + k];
     }
-    r[3 * nv] = __uint_as_float(p);
-    for (int k = 3 * nv + 1; k < rf; k++) r[k] = 0.0f;
+    rec_id(r + 3 * nv, p);
+    for (int k = 3 * nv + 1; k < rw; k++) r[k] = (T)0;
   }
 }
 
@@ -123,10 +150,10 @@ __device__ __forceinline__ int f2o(float f) {
 // (ComputeBoundingBoxOMP; min and max do not depend on the order), and a
 // flag for an index at or beyond nverts.  box: 3 mins then 3 maxes as
 // ordered ints, initialised to INT_MAX / INT_MIN.
-__global__ void solid_box_kernel(const float *__restrict__ v, const uint32_t *__restrict__ ix,
+template <typename T>
+__global__ void solid_box_kernel(const T *__restrict__ v, const uint32_t *__restrict__ ix,
                                  size_t refs, size_t nverts, int *__restrict__ box,
                                  uint32_t *__restrict__ bad) {
-  const float eps = FLT_EPSILON * 16;
   int lo[3] = {INT_MAX, INT_MAX, INT_MAX}, hi[3] = {INT_MIN, INT_MIN, INT_MIN};
   bool oob = false;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < refs;
@@ -137,9 +164,9 @@ __global__ void solid_box_kernel(const float *__restrict__ v, const uint32_t *__
       continue;
     }
     for (int k = 0; k < 3; k++) {
-      const float x = v[3 * (size_t)f + k];
-      lo[k] = min(lo[k], f2o(x - eps));
-      hi[k] = max(hi[k], f2o(x + eps));
+      const T x = v[3 * (size_t)f + k];
+      lo[k] = min(lo[k], f2o(pad_lo(x)));
+      hi[k] = max(hi[k], f2o(pad_hi(x)));
     }
   }
   for (int o = 16; o > 0; o >>= 1)
@@ -158,24 +185,23 @@ __global__ void solid_box_kernel(const float *__restrict__ v, const uint32_t *__
 // Leaf box (ComputeBoundingBox30, :1121-1169) over the records of sorted
 // solids first..last: every vertex -+ FLT_EPSILON * 16, the first vertex
 // first, then strict comparisons.
-template <int NV>
-__device__ __forceinline__ void leaf_box(const float *__restrict__ recs, uint32_t first,
+template <int NV, typename T>
+__device__ __forceinline__ void leaf_box(const T *__restrict__ recs, uint32_t first,
                                          uint32_t last, float lo[3], float hi[3]) {
-  constexpr int RF = rec_floats(NV);
-  const float eps = FLT_EPSILON * 16;
-  const float *r0 = recs + (size_t)RF * first;
+  constexpr int RW = rec_bytes<T>(NV) / (int)sizeof(T);
+  const T *r0 = recs + (size_t)RW * first;
   for (int k = 0; k < 3; k++) {
-    lo[k] = r0[k] - eps;
-    hi[k] = r0[k] + eps;
+    lo[k] = pad_lo(r0[k]);
+    hi[k] = pad_hi(r0[k]);
   }
   for (uint32_t i = first; i <= last; i++) {
-    const float *r = recs + (size_t)RF * i;
+    const T *r = recs + (size_t)RW * i;
 #pragma unroll
     for (int q = 0; q < NV; q++)
 #pragma unroll
       for (int k = 0; k < 3; k++) {
-        const float x = r[3 * q + k];
-        const float a = x - eps, b = x + eps;
+        const T x = r[3 * q + k];
+        const float a = pad_lo(x), b = pad_hi(x);
         if (lo[k] > a) lo[k] = a;
         if (hi[k] < b) hi[k] = b;
       }
@@ -220,11 +246,11 @@ __device__ __forceinline__ uint32_t arrive_at(uint32_t *counter) {
 // writes its children links, axis ((clz(code) - 2) % 3 of its split code)
 // and leaf children; boxes then climb to the root, the second child to
 // arrive at a branch merging both (left then right).
-template <int NV>
+template <int NV, typename V>
 __global__ void __launch_bounds__(256)
 solid_tree_kernel(const uint32_t *__restrict__ codes, srt::Topology T,
                   const srt::SceneInfo *__restrict__ info, uint32_t m,
-                  const float *__restrict__ recs, SNode *__restrict__ nodes,
+                  const V *__restrict__ recs, SNode *__restrict__ nodes,
                   uint32_t *__restrict__ err) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= info->nbranches) return;
@@ -242,7 +268,7 @@ solid_tree_kernel(const uint32_t *__restrict__ codes, srt::Topology T,
     if (leaf[side]) {
       const uint2 r = kleaf ? make_uint2(c, c) : __ldg(&T.krange[c]);
       id[side] = m + r.x;
-      leaf_box<NV>(recs, r.x, r.y, clo[side], chi[side]);
+      leaf_box<NV, V>(recs, r.x, r.y, clo[side], chi[side]);
       SNode *ln = nodes + id[side];
       node_box_store(ln, clo[side], chi[side]);
       __stcg(&ln->w0, r.x);
@@ -311,9 +337,12 @@ solid_tree_kernel(const uint32_t *__restrict__ codes, srt::Topology T,
 // float arithmetic in the reference's operation order, the tree in the
 // reference's node order.  Options are the defaults of SolidBuildOptions
 // (render_accel_solid.h:46-56): costTaabb 0.2, minLeafPrimitives 4,
-// maxTreeDepth 256, binSize 64.
+// maxTreeDepth 256, binSize 64.  T: float or double positions (the
+// reference's vertices / dvertices: boxes of double positions padded in
+// double, bins over their float roundings, SAHPredD's double sum).
+template <typename T>
 struct SahBuilder {
-  const float *v;
+  const T *v;
   const uint32_t *ix;
   int nv;
   std::vector<uint32_t> &idx;
@@ -322,21 +351,20 @@ struct SahBuilder {
   static constexpr int kBins = 64, kMinLeaf = 4, kMaxDepth = 256;
   static constexpr float kTaabb = 0.2f;
 
-  const float *vert(uint32_t solid, int j) const { return v + 3 * (size_t)ix[(size_t)nv * solid + j]; }
+  const T *vert(uint32_t solid, int j) const { return v + 3 * (size_t)ix[(size_t)nv * solid + j]; }
 
   // ComputeBoundingBox (:1076-1118): every vertex -+ FLT_EPSILON * 16
   void range_box(uint32_t l, uint32_t r, float lo[3], float hi[3]) const {
-    const float eps = FLT_EPSILON * 16;
-    const float *p0 = vert(idx[l], 0);
+    const T *p0 = vert(idx[l], 0);
     for (int k = 0; k < 3; k++) {
-      lo[k] = p0[k] - eps;
-      hi[k] = p0[k] + eps;
+      lo[k] = pad_lo(p0[k]);
+      hi[k] = pad_hi(p0[k]);
     }
     for (uint32_t i = l; i < r; i++)
       for (int j = 0; j < nv; j++) {
-        const float *p = vert(idx[i], j);
+        const T *p = vert(idx[i], j);
         for (int k = 0; k < 3; k++) {
-          const float a = p[k] - eps, b = p[k] + eps;
+          const float a = pad_lo(p[k]), b = pad_hi(p[k]);
           if (lo[k] > a) lo[k] = a;
           if (hi[k] < b) hi[k] = b;
         }
@@ -347,10 +375,13 @@ struct SahBuilder {
     const float b0 = hi[0] - lo[0], b1 = hi[1] - lo[1], b2 = hi[2] - lo[2];
     return (float)(2.0 * (double)((b0 * b1 + b1 * b2) + b2 * b0));
   }
-  // SAHPred (:1034-1053): the summed vertex coordinate against pos * nv
+  // SAHPred / SAHPredD (:1034-1074): the summed vertex coordinate (a
+  // float sum; double addends are added in double and rounded) against
+  // pos * nv (float, or double for double positions)
   bool left_of(uint32_t solid, int axis, float pos) const {
     float c = 0.0f;
-    for (int j = 0; j < nv; j++) c += vert(solid, j)[axis];
+    for (int j = 0; j < nv; j++) c = (float)(c + vert(solid, j)[axis]);
+    if (sizeof(T) == 8) return (double)c < (double)pos * (double)(float)nv;
     return c < pos * (float)nv;
   }
   // std::partition as libstdc++ runs it on bidirectional iterators: from
@@ -386,7 +417,8 @@ struct SahBuilder {
     for (uint32_t i = l; i < r; i++) {
       float slo[3] = {FLT_MAX, FLT_MAX, FLT_MAX}, shi[3] = {-FLT_MAX, -FLT_MAX, -FLT_MAX};
       for (int j = 0; j < nv; j++) {  // GetBoundingBoxOfSolid: std::min / std::max
-        const float *p = vert(idx[i], j);
+        const T *pv = vert(idx[i], j);
+        const float p[3] = {(float)pv[0], (float)pv[1], (float)pv[2]};
         for (int k = 0; k < 3; k++) {
           slo[k] = (p[k] < slo[k]) ? p[k] : slo[k];
           shi[k] = (shi[k] < p[k]) ? p[k] : shi[k];
@@ -488,9 +520,9 @@ constexpr int kSolidQ = 32;  // solids a lane queues before the warp tests them
 // below 1024 solids) up to 257
 constexpr int kSolidStackShort = 64, kSolidStackDeep = 264;
 
-template <int NV, int STACK>
+template <int NV, int STACK, typename T>
 __global__ void __launch_bounds__(128, 3)  // 3 blocks per SM: 168 registers
-solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ recs,
+solid_trace_kernel(const SNode *__restrict__ nodes, const void *__restrict__ recs,
                    const srt_ray *__restrict__ rays, const uint32_t *__restrict__ order,
                    size_t n, srt_hit *__restrict__ hits, float *__restrict__ normals,
                    float *__restrict__ positions, uint32_t *__restrict__ err) {
@@ -573,7 +605,7 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
     for (int c = 0; c < 3; c++)
       if (dir[c] > 0.1 || dir[c] < -0.1) jax = c;
     for (int qi = 0; qi < len; qi++)
-      solid_test<NV>(recs, queue[qi][threadIdx.x], prev, dorg, ddir, jax, t, prim, bp, bn);
+      solid_test<NV, T>(recs, queue[qi][threadIdx.x], prev, dorg, ddir, jax, t, prim, bp, bn);
     if (live && sp < 0 && leaf_left == 0) {
       const bool got = t < FLT_MAX;
       reinterpret_cast<float4 *>(hits)[i] =
@@ -588,6 +620,22 @@ solid_trace_kernel(const SNode *__restrict__ nodes, const float *__restrict__ re
     }
   }
   if (overflow) atomicOr(err, srt::kErrStack);
+}
+
+// The trace kernel for nv vertices per solid, a deep tree (SAH builds), and
+// double-precision positions.
+template <typename T>
+const void *solid_kernel_t(int nv, bool deep) {
+  if (deep)
+    return nv == 5   ? (const void *)solid_trace_kernel<5, kSolidStackDeep, T>
+           : nv == 6 ? (const void *)solid_trace_kernel<6, kSolidStackDeep, T>
+                     : (const void *)solid_trace_kernel<8, kSolidStackDeep, T>;
+  return nv == 5   ? (const void *)solid_trace_kernel<5, kSolidStackShort, T>
+         : nv == 6 ? (const void *)solid_trace_kernel<6, kSolidStackShort, T>
+                   : (const void *)solid_trace_kernel<8, kSolidStackShort, T>;
+}
+const void *solid_kernel(int nv, bool deep, bool dbl) {
+  return dbl ? solid_kernel_t<double>(nv, deep) : solid_kernel_t<float>(nv, deep);
 }
 
 srt_status solid_view(srt_ctx *ctx, const void *p, size_t bytes, DevBuf &stage,
@@ -614,7 +662,7 @@ bool solid_scene_view(const srt_solid_accel *a, srt_ctx **ctx, SceneElem &e, boo
   *ctx = a->ctx;
   e.kind = kSceneSolids;
   e.nprims = (uint32_t)a->n;
-  e.aux = a->nv;
+  e.aux = a->nv | (a->dbl ? kSolidAuxDouble : 0);
   e.nodes = a->dnodes.p;
   e.prims = a->drecs.as<float4>();
   e.sidx = nullptr;
@@ -693,13 +741,15 @@ srt_status solid_host_layout(srt_solid_accel *a) {
 // stream).
 constexpr size_t kSahMax = 1024;
 
-srt_status solid_build_sah(srt_solid_accel *a, int nv, const float *v, size_t nverts,
+template <typename T>
+srt_status solid_build_sah(srt_solid_accel *a, int nv, const T *v, size_t nverts,
                            const uint32_t *ix, size_t n) {
   srt_ctx *ctx = a->ctx;
   const size_t refs = n * (size_t)nv;
-  std::vector<float> hv(3 * nverts);
+  std::vector<T> hv(3 * nverts);
   std::vector<uint32_t> hix(refs);
-  cudaError_t e = cudaMemcpyAsync(hv.data(), v, hv.size() * 4, cudaMemcpyDefault, ctx->stream);
+  cudaError_t e =
+      cudaMemcpyAsync(hv.data(), v, hv.size() * sizeof(T), cudaMemcpyDefault, ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(hix.data(), ix, refs * 4, cudaMemcpyDefault, ctx->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
@@ -712,7 +762,7 @@ srt_status solid_build_sah(srt_solid_accel *a, int nv, const float *v, size_t nv
   a->nodes.clear();
   a->idx.resize(n);
   for (size_t i = 0; i < n; i++) a->idx[i] = (uint32_t)i;
-  SahBuilder B{hv.data(), hix.data(), nv, a->idx, a->nodes};
+  SahBuilder<T> B{hv.data(), hix.data(), nv, a->idx, a->nodes};
   B.build(0, (uint32_t)n, 0);
   // device layout: node k is reference node k; records in leaf order
   std::vector<SNode> dn(a->nodes.size());
@@ -730,24 +780,23 @@ srt_status solid_build_sah(srt_solid_accel *a, int nv, const float *v, size_t nv
       dn[k].w1 = h.data[1] | ((uint32_t)h.axis << 29);
     }
   }
-  const int rf = rec_floats(nv);
-  std::vector<float> recs((size_t)rf * n, 0.0f);
+  const int rw = rec_bytes<T>(nv) / (int)sizeof(T);
+  std::vector<T> recs((size_t)rw * n, (T)0);
   for (size_t j = 0; j < n; j++) {
     const uint32_t p = a->idx[j];
-    float *r = recs.data() + (size_t)rf * j;
+    T *r = recs.data() + (size_t)rw * j;
     for (int q = 0; q < nv; q++)
       for (int k = 0; k < 3; k++) r[3 * q + k] = hv[3 * (size_t)hix[(size_t)nv * p + q] + k];
-    uint32_t pid = p;
-    std::memcpy(&r[3 * nv], &pid, 4);
+    rec_id(r + 3 * nv, p);
   }
   if ((e = a->dnodes.ensure(dn.size() * sizeof(SNode))) != cudaSuccess ||
-      (e = a->drecs.ensure(recs.size() * 4)) != cudaSuccess ||
+      (e = a->drecs.ensure(recs.size() * sizeof(T))) != cudaSuccess ||
       (e = a->dorder.ensure(n * 4)) != cudaSuccess)
     return cuda_status(e, "solid accel");
   e = cudaMemcpyAsync(a->dnodes.p, dn.data(), dn.size() * sizeof(SNode), cudaMemcpyHostToDevice,
                       ctx->stream);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(a->drecs.p, recs.data(), recs.size() * 4, cudaMemcpyHostToDevice,
+    e = cudaMemcpyAsync(a->drecs.p, recs.data(), recs.size() * sizeof(T), cudaMemcpyHostToDevice,
                         ctx->stream);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(a->dorder.p, a->idx.data(), n * 4, cudaMemcpyHostToDevice, ctx->stream);
@@ -756,7 +805,110 @@ srt_status solid_build_sah(srt_solid_accel *a, int nv, const float *v, size_t nv
   if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) return cuda_status(e, "solid upload");
   a->deep = B.max_depth + 2 > kSolidStackShort;
+  a->dbl = sizeof(T) == 8;
   a->host_ready = true;
+  a->nv = nv;
+  a->n = n;
+  a->built = true;
+  return SRT_OK;
+}
+
+template <typename T>
+srt_status solid_build_t(srt_solid_accel *a, int32_t verts_per_solid, const T *vertices,
+                         size_t nverts, const uint32_t *indices, size_t nsolids) {
+  if (!a || !vertices || !indices) return SRT_ERR_INVALID;
+  const int nv = verts_per_solid;
+  if ((nv != 5 && nv != 6 && nv != 8) || nsolids < 2 || nsolids >= (1u << 28)) {
+    set_error("srt_solid_build: 5, 6 or 8 vertices per solid and 2 .. 2^28 - 1 solids");
+    return SRT_ERR_INVALID;
+  }
+  srt_ctx *ctx = a->ctx;
+  cudaSetDevice(ctx->device);
+  const size_t n = nsolids, refs = nsolids * (size_t)nv, m = n - 1;
+  DevBuf sv, si;  // staging of host inputs
+  const void *dv, *di;
+  srt_status s;
+  if ((s = solid_view(ctx, vertices, nverts * 3 * sizeof(T), sv, &dv)) != SRT_OK) return s;
+  if ((s = solid_view(ctx, indices, refs * 4, si, &di)) != SRT_OK) return s;
+  const T *d_v = static_cast<const T *>(dv);
+  const uint32_t *d_ix = static_cast<const uint32_t *>(di);
+  cudaError_t e;
+  a->built = false;
+  a->host_ready = false;
+  // the latest trace (on any stream) reads the tree this build overwrites
+  if (a->used && (e = cudaStreamWaitEvent(ctx->stream, a->ev_used, 0)) != cudaSuccess)
+    return cuda_status(e, "solid build");
+  if (n < kSahMax) return solid_build_sah<T>(a, nv, d_v, nverts, d_ix, n);
+  a->deep = false;
+  a->dbl = sizeof(T) == 8;
+  if ((e = a->dbox.ensure(64)) != cudaSuccess || (e = a->dcodes.ensure(n * 4)) != cudaSuccess ||
+      (e = a->dorder.ensure(n * 4)) != cudaSuccess ||
+      (e = a->dinfo.ensure(sizeof(srt::SceneInfo))) != cudaSuccess ||
+      (e = a->dnodes.ensure((m + n) * sizeof(SNode))) != cudaSuccess ||
+      (e = a->drecs.ensure(n * (size_t)rec_bytes<T>(nv))) != cudaSuccess)
+    return cuda_status(e, "solid accel");
+  // scene box and index check on the GPU: the one host round trip (an index
+  // beyond nverts must fail before any kernel reads through it)
+  int hbox[8] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN, 0, 0};
+  if ((e = cudaMemcpyAsync(a->dbox.p, hbox, sizeof(hbox), cudaMemcpyHostToDevice,
+                           ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid box");
+  const unsigned gbox = (unsigned)std::min<size_t>((refs + 255) / 256, (size_t)ctx->num_sms * 8);
+  solid_box_kernel<<<gbox, 256, 0, ctx->stream>>>(d_v, d_ix, refs, nverts, a->dbox.as<int>(),
+                                                   reinterpret_cast<uint32_t *>(a->dbox.as<int>() + 6));
+  ctx->launches++;
+  if ((e = cudaMemcpyAsync(hbox, a->dbox.p, sizeof(hbox), cudaMemcpyDeviceToHost,
+                           ctx->stream)) != cudaSuccess ||
+      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid box");
+  if (hbox[6]) {
+    set_error("srt_solid_build: an index names a vertex beyond nverts");
+    return SRT_ERR_INVALID;
+  }
+  float lo[3], hi3[3], inv[3];
+  auto o2f_h = [](int i) {
+    const int b = i >= 0 ? i : i ^ 0x7fffffff;
+    float f;
+    std::memcpy(&f, &b, 4);
+    return f;
+  };
+  const int kdiv = 1 << 10;
+  for (int k = 0; k < 3; k++) {
+    lo[k] = o2f_h(hbox[k]);
+    hi3[k] = o2f_h(hbox[3 + k]);
+    inv[k] = kdiv / (hi3[k] - lo[k]);
+  }
+  uint32_t *codes = a->dcodes.as<uint32_t>(), *order = a->dorder.as<uint32_t>();
+  const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
+  solid_morton_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, nv, n, lo[0], lo[1], lo[2],
+                                                      inv[0], inv[1], inv[2], codes);
+  ctx->launches++;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid morton");
+  if ((s = sort_pairs(ctx, codes, order, n, true, 30)) != SRT_OK) return s;
+  srt::Topology topo;
+  srt::SceneInfo *info = a->dinfo.as<srt::SceneInfo>();
+  if ((s = srt::stage_topology(ctx, codes, n, 4, info, topo)) != SRT_OK) return s;
+  solid_gather_kernel<T><<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order, nv, n,
+                                                         a->drecs.as<T>());
+  const unsigned gt = (unsigned)((m + 255) / 256);
+  SNode *d_nodes = a->dnodes.as<SNode>();
+  const T *recs = a->drecs.as<T>();
+  if (nv == 5)
+    solid_tree_kernel<5, T><<<gt, 256, 0, ctx->stream>>>(codes, topo, info, (uint32_t)m, recs, d_nodes,
+                                                      ctx->d_err);
+  else if (nv == 6)
+    solid_tree_kernel<6, T><<<gt, 256, 0, ctx->stream>>>(codes, topo, info, (uint32_t)m, recs, d_nodes,
+                                                      ctx->d_err);
+  else
+    solid_tree_kernel<8, T><<<gt, 256, 0, ctx->stream>>>(codes, topo, info, (uint32_t)m, recs, d_nodes,
+                                                      ctx->d_err);
+  ctx->launches += 2;
+  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid tree");
+  if ((e = cudaEventRecord(a->ev_built, ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid build");
+  // staged host inputs are freed on return: finish with them first
+  if ((sv.p || si.p) && (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
+    return cuda_status(e, "solid build");
   a->nv = nv;
   a->n = n;
   a->built = true;
@@ -799,102 +951,13 @@ SRT_API srt_status srt_solid_destroy(srt_solid_accel *a) {
 SRT_API srt_status srt_solid_build(srt_solid_accel *a, int32_t verts_per_solid,
                                    const float *vertices, size_t nverts,
                                    const uint32_t *indices, size_t nsolids) {
-  if (!a || !vertices || !indices) return SRT_ERR_INVALID;
-  const int nv = verts_per_solid;
-  if ((nv != 5 && nv != 6 && nv != 8) || nsolids < 2 || nsolids >= (1u << 28)) {
-    set_error("srt_solid_build: 5, 6 or 8 vertices per solid and 2 .. 2^28 - 1 solids");
-    return SRT_ERR_INVALID;
-  }
-  srt_ctx *ctx = a->ctx;
-  cudaSetDevice(ctx->device);
-  const size_t n = nsolids, refs = nsolids * (size_t)nv, m = n - 1;
-  DevBuf sv, si;  // staging of host inputs
-  const void *dv, *di;
-  srt_status s;
-  if ((s = solid_view(ctx, vertices, nverts * 12, sv, &dv)) != SRT_OK) return s;
-  if ((s = solid_view(ctx, indices, refs * 4, si, &di)) != SRT_OK) return s;
-  const float *d_v = static_cast<const float *>(dv);
-  const uint32_t *d_ix = static_cast<const uint32_t *>(di);
-  cudaError_t e;
-  a->built = false;
-  a->host_ready = false;
-  // the latest trace (on any stream) reads the tree this build overwrites
-  if (a->used && (e = cudaStreamWaitEvent(ctx->stream, a->ev_used, 0)) != cudaSuccess)
-    return cuda_status(e, "solid build");
-  if (n < kSahMax) return solid_build_sah(a, nv, d_v, nverts, d_ix, n);
-  a->deep = false;
-  if ((e = a->dbox.ensure(64)) != cudaSuccess || (e = a->dcodes.ensure(n * 4)) != cudaSuccess ||
-      (e = a->dorder.ensure(n * 4)) != cudaSuccess ||
-      (e = a->dinfo.ensure(sizeof(srt::SceneInfo))) != cudaSuccess ||
-      (e = a->dnodes.ensure((m + n) * sizeof(SNode))) != cudaSuccess ||
-      (e = a->drecs.ensure(n * rec_floats(nv) * 4)) != cudaSuccess)
-    return cuda_status(e, "solid accel");
-  // scene box and index check on the GPU: the one host round trip (an index
-  // beyond nverts must fail before any kernel reads through it)
-  int hbox[8] = {INT_MAX, INT_MAX, INT_MAX, INT_MIN, INT_MIN, INT_MIN, 0, 0};
-  if ((e = cudaMemcpyAsync(a->dbox.p, hbox, sizeof(hbox), cudaMemcpyHostToDevice,
-                           ctx->stream)) != cudaSuccess)
-    return cuda_status(e, "solid box");
-  const unsigned gbox = (unsigned)std::min<size_t>((refs + 255) / 256, (size_t)ctx->num_sms * 8);
-  solid_box_kernel<<<gbox, 256, 0, ctx->stream>>>(d_v, d_ix, refs, nverts, a->dbox.as<int>(),
-                                                   reinterpret_cast<uint32_t *>(a->dbox.as<int>() + 6));
-  ctx->launches++;
-  if ((e = cudaMemcpyAsync(hbox, a->dbox.p, sizeof(hbox), cudaMemcpyDeviceToHost,
-                           ctx->stream)) != cudaSuccess ||
-      (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
-    return cuda_status(e, "solid box");
-  if (hbox[6]) {
-    set_error("srt_solid_build: an index names a vertex beyond nverts");
-    return SRT_ERR_INVALID;
-  }
-  float lo[3], hi3[3], inv[3];
-  auto o2f_h = [](int i) {
-    const int b = i >= 0 ? i : i ^ 0x7fffffff;
-    float f;
-    std::memcpy(&f, &b, 4);
-    return f;
-  };
-  const int kdiv = 1 << 10;
-  for (int k = 0; k < 3; k++) {
-    lo[k] = o2f_h(hbox[k]);
-    hi3[k] = o2f_h(hbox[3 + k]);
-    inv[k] = kdiv / (hi3[k] - lo[k]);
-  }
-  uint32_t *codes = a->dcodes.as<uint32_t>(), *order = a->dorder.as<uint32_t>();
-  const unsigned grid = (unsigned)std::min<size_t>((n + 255) / 256, (size_t)ctx->num_sms * 16);
-  solid_morton_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, nv, n, lo[0], lo[1], lo[2],
-                                                      inv[0], inv[1], inv[2], codes);
-  ctx->launches++;
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid morton");
-  if ((s = sort_pairs(ctx, codes, order, n, true, 30)) != SRT_OK) return s;
-  srt::Topology T;
-  srt::SceneInfo *info = a->dinfo.as<srt::SceneInfo>();
-  if ((s = srt::stage_topology(ctx, codes, n, 4, info, T)) != SRT_OK) return s;
-  solid_gather_kernel<<<grid, 256, 0, ctx->stream>>>(d_v, d_ix, order, nv, n,
-                                                      a->drecs.as<float>());
-  const unsigned gt = (unsigned)((m + 255) / 256);
-  SNode *d_nodes = a->dnodes.as<SNode>();
-  const float *recs = a->drecs.as<float>();
-  if (nv == 5)
-    solid_tree_kernel<5><<<gt, 256, 0, ctx->stream>>>(codes, T, info, (uint32_t)m, recs, d_nodes,
-                                                      ctx->d_err);
-  else if (nv == 6)
-    solid_tree_kernel<6><<<gt, 256, 0, ctx->stream>>>(codes, T, info, (uint32_t)m, recs, d_nodes,
-                                                      ctx->d_err);
-  else
-    solid_tree_kernel<8><<<gt, 256, 0, ctx->stream>>>(codes, T, info, (uint32_t)m, recs, d_nodes,
-                                                      ctx->d_err);
-  ctx->launches += 2;
-  if ((e = cudaGetLastError()) != cudaSuccess) return cuda_status(e, "solid tree");
-  if ((e = cudaEventRecord(a->ev_built, ctx->stream)) != cudaSuccess)
-    return cuda_status(e, "solid build");
-  // staged host inputs are freed on return: finish with them first
-  if ((sv.p || si.p) && (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess)
-    return cuda_status(e, "solid build");
-  a->nv = nv;
-  a->n = n;
-  a->built = true;
-  return SRT_OK;
+  return solid_build_t<float>(a, verts_per_solid, vertices, nverts, indices, nsolids);
+}
+
+SRT_API srt_status srt_solid_build_double(srt_solid_accel *a, int32_t verts_per_solid,
+                                          const double *vertices, size_t nverts,
+                                          const uint32_t *indices, size_t nsolids) {
+  return solid_build_t<double>(a, verts_per_solid, vertices, nverts, indices, nsolids);
 }
 
 SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size_t n,
@@ -934,13 +997,7 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
   }
   // as many blocks as the SMs hold at once: lanes take their next ray as
   // soon as they finish one
-  const void *kfn =
-      a->deep ? (a->nv == 5   ? (const void *)solid_trace_kernel<5, kSolidStackDeep>
-                 : a->nv == 6 ? (const void *)solid_trace_kernel<6, kSolidStackDeep>
-                              : (const void *)solid_trace_kernel<8, kSolidStackDeep>)
-              : (a->nv == 5   ? (const void *)solid_trace_kernel<5, kSolidStackShort>
-                 : a->nv == 6 ? (const void *)solid_trace_kernel<6, kSolidStackShort>
-                              : (const void *)solid_trace_kernel<8, kSolidStackShort>);
+  const void *kfn = solid_kernel(a->nv, a->deep, a->dbl);
   int per_sm = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, 128, 0) != cudaSuccess ||
       per_sm < 1) {
@@ -950,7 +1007,7 @@ SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size
   const unsigned grid =
       (unsigned)std::min<size_t>((n + 127) / 128, (size_t)ctx->num_sms * per_sm);
   const SNode *nd = a->dnodes.as<SNode>();
-  const float *rc = a->drecs.as<float>();
+  const void *rc = a->drecs.p;
   const srt_ray *rr = static_cast<const srt_ray *>(dr);
   // a coherent ray order (a Morton curve over origin and direction) for
   // large batches; the hits do not depend on it

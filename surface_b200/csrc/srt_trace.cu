@@ -1991,16 +1991,25 @@ __device__ __forceinline__ bool elem_hit_solids(const SceneElem &e, const RayF &
                                                 uint32_t prev, Best &b, uint32_t *err) {
   using namespace srt_solid_walk;
   const SNode *nodes = static_cast<const SNode *>(e.nodes);
-  const float *recs = reinterpret_cast<const float *>(e.prims);
+  const void *recs = e.prims;
   float t, bp[3], bn[3];
   uint32_t prim;
   bool ok;
-  if (e.aux == 5)
+  const int nv = e.aux & 255;
+  if (e.aux & kSolidAuxDouble) {
+    if (nv == 5)
+      ok = solid_walk<5, STACK, double>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+    else if (nv == 6)
+      ok = solid_walk<6, STACK, double>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+    else
+      ok = solid_walk<8, STACK, double>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+  } else if (nv == 5) {
     ok = solid_walk<5, STACK>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
-  else if (e.aux == 6)
+  } else if (nv == 6) {
     ok = solid_walk<6, STACK>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
-  else
+  } else {
     ok = solid_walk<8, STACK>(nodes, recs, lr.o, lr.d, prev, t, prim, bp, bn);
+  }
   if (!ok) atomicOr(err, kErrStack);
   if (!(t < FLT_MAX)) return false;
   b.t = t;

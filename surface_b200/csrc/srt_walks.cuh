@@ -281,6 +281,15 @@ constexpr uint32_t kSolidLeaf = 0x80000000u;
 
 // floats per record: nv vertices (xyz) and the solid's index, padded to 16 bytes
 __host__ __device__ constexpr int rec_floats(int nv) { return ((3 * nv + 1) + 3) / 4 * 4; }
+// The same for double-precision positions: doubles per record (nv vertices,
+// then the solid's index in the low word of one more double), padded to 16
+// bytes.
+__host__ __device__ constexpr int rec_doubles(int nv) { return ((3 * nv + 1) + 1) / 2 * 2; }
+// Bytes of one record of scalar type T.
+template <typename T>
+__host__ __device__ constexpr int rec_bytes(int nv) {
+  return sizeof(T) == 8 ? 8 * rec_doubles(nv) : 4 * rec_floats(nv);
+}
 
 // ------------------------------------------------------------------ trace
 struct D3 {
@@ -381,11 +390,12 @@ struct SolidTab<8> {
   }
 };
 
-// One solid's vertices (floats, exactly as stored) read as doubles on use;
-// edges are recomputed from them (the same double subtraction each time).
-template <int NV>
+// One solid's vertices (floats or doubles, exactly as stored: T) read as
+// doubles on use; edges are recomputed from them (the same double
+// subtraction each time).
+template <int NV, typename T = float>
 struct SolidV {
-  float x[NV][3];
+  T x[NV][3];
   __device__ __forceinline__ D3 v(int k) const {
     return {(double)x[k][0], (double)x[k][1], (double)x[k][2]};
   }
@@ -395,8 +405,8 @@ struct SolidV {
 };
 
 // ws[i] = dir . (e_i x v_{i % MOD}) + e_i . (dir x org) (:467-476)
-template <int NV>
-__device__ __forceinline__ void s_weights(const SolidV<NV> &S, D3 dir, D3 org,
+template <int NV, typename T>
+__device__ __forceinline__ void s_weights(const SolidV<NV, T> &S, D3 dir, D3 org,
                                           double (&ws)[SolidTab<NV>::NE]) {
   const D3 rpc = dcross(dir, org);
 #pragma unroll
@@ -431,8 +441,8 @@ struct SolidFaces<5> {  // IntersectPyramidD: point n uses i = 1 - n
     if (s_cw(ws, n, 3) && s_cw(ws, i, 7) && s_cw(ws, n, 4)) return 4;
     return -1;
   }
-  template <bool FULL>
-  __device__ static void point(const SolidV<5> &S, const double (&ws)[8], int f, D3 dir, int j,
+  template <bool FULL, typename T>
+  __device__ static void point(const SolidV<5, T> &S, const double (&ws)[8], int f, D3 dir, int j,
                                float pos[3], float nrm[3]) {
     switch (f) {
       case 0:
@@ -471,8 +481,8 @@ struct SolidFaces<6> {  // IntersectPrismD: point i uses n = 1 - i
     if (s_cw(ws, i, 1) && s_cw(ws, i, 8) && s_cw(ws, n, 4) && s_cw(ws, n, 7)) return 4;
     return -1;
   }
-  template <bool FULL>
-  __device__ static void point(const SolidV<6> &S, const double (&ws)[9], int f, D3 dir, int j,
+  template <bool FULL, typename T>
+  __device__ static void point(const SolidV<6, T> &S, const double (&ws)[9], int f, D3 dir, int j,
                                float pos[3], float nrm[3]) {
     switch (f) {
       case 0:
@@ -514,8 +524,8 @@ struct SolidFaces<8> {  // IntersectHexaD: point i uses n = 1 - i
     if (s_cw(ws, i, 3) && s_cw(ws, i, 8) && s_cw(ws, n, 7) && s_cw(ws, n, 11)) return 5;
     return -1;
   }
-  template <bool FULL>
-  __device__ static void point(const SolidV<8> &S, const double (&ws)[12], int f, D3 dir, int j,
+  template <bool FULL, typename T>
+  __device__ static void point(const SolidV<8, T> &S, const double (&ws)[12], int f, D3 dir, int j,
                                float pos[3], float nrm[3]) {
     switch (f) {
       case 0:
@@ -554,11 +564,11 @@ struct SolidFaces<8> {  // IntersectHexaD: point i uses n = 1 - i
 
 // The full crossing point and normal of a hit that becomes a ray's closest
 // (seldom: kept out of line so the test loop keeps its registers).
-template <int NV>
-__device__ __noinline__ void s_full_point(const SolidV<NV> &S,
+template <int NV, typename T>
+__device__ __noinline__ void s_full_point(const SolidV<NV, T> &S,
                                           const double (&ws)[SolidTab<NV>::NE], int f, D3 dir,
                                           float pos[3], float nrm[3]) {
-  SolidFaces<NV>::template point<true>(S, ws, f, dir, 0, pos, nrm);
+  SolidFaces<NV>::template point<true, T>(S, ws, f, dir, 0, pos, nrm);
 }
 
 // t of a crossing point along axis j (the last with |dir| > 0.1; none: 0),
@@ -595,30 +605,50 @@ __device__ __forceinline__ bool sbox_hit(const SNode &nd, const float org[3], co
 // the reference keeps (entry, then exit), its solid id, position and
 // normal; a record whose id is the ray's previous primitive is skipped.
 // jax: the last axis with |dir| > 0.1 (-1: none).
-template <int NV>
-__device__ __forceinline__ void solid_test(const float *__restrict__ recs, uint32_t j,
+// recs: records of scalar type T (rec_floats / rec_doubles per solid).
+template <int NV, typename T = float>
+__device__ __forceinline__ void solid_test(const void *__restrict__ recs, uint32_t j,
                                            uint32_t prev, D3 dorg, D3 ddir, int jax, float &t,
                                            uint32_t &prim, float bp[3], float bn[3]) {
-  constexpr int RF = rec_floats(NV);
-  const float4 *r4 = reinterpret_cast<const float4 *>(recs + (size_t)RF * j);
-  float rv[RF];
+  SolidV<NV, T> S;
+  uint32_t p;
+  if constexpr (sizeof(T) == 8) {
+    constexpr int RD = rec_doubles(NV);
+    const double2 *r2 = reinterpret_cast<const double2 *>(recs) + (size_t)(RD / 2) * j;
+    double rv[RD];
 #pragma unroll
-  for (int q4 = 0; q4 < RF / 4; q4++) {
-    const float4 v4 = __ldg(r4 + q4);
-    rv[4 * q4] = v4.x;
-    rv[4 * q4 + 1] = v4.y;
-    rv[4 * q4 + 2] = v4.z;
-    rv[4 * q4 + 3] = v4.w;
+    for (int q = 0; q < RD / 2; q++) {
+      const double2 v2 = __ldg(r2 + q);
+      rv[2 * q] = v2.x;
+      rv[2 * q + 1] = v2.y;
+    }
+    p = (uint32_t)__double_as_longlong(rv[3 * NV]);
+    if (p == prev) return;  // Ray::prev_prim_id
+#pragma unroll
+    for (int c = 0; c < NV; c++)
+#pragma unroll
+      for (int e = 0; e < 3; e++) S.x[c][e] = rv[3 * c + e];
+  } else {
+    constexpr int RF = rec_floats(NV);
+    const float4 *r4 = reinterpret_cast<const float4 *>(recs) + (size_t)(RF / 4) * j;
+    float rv[RF];
+#pragma unroll
+    for (int q4 = 0; q4 < RF / 4; q4++) {
+      const float4 v4 = __ldg(r4 + q4);
+      rv[4 * q4] = v4.x;
+      rv[4 * q4 + 1] = v4.y;
+      rv[4 * q4 + 2] = v4.z;
+      rv[4 * q4 + 3] = v4.w;
+    }
+    p = __float_as_uint(rv[3 * NV]);
+    if (p == prev) return;  // Ray::prev_prim_id
+#pragma unroll
+    for (int c = 0; c < NV; c++)
+#pragma unroll
+      for (int e = 0; e < 3; e++) S.x[c][e] = rv[3 * c + e];
   }
-  const uint32_t p = __float_as_uint(rv[3 * NV]);
-  if (p == prev) return;  // Ray::prev_prim_id
-  SolidV<NV> S;
-#pragma unroll
-  for (int c = 0; c < NV; c++)
-#pragma unroll
-    for (int e = 0; e < 3; e++) S.x[c][e] = rv[3 * c + e];
   double ws[SolidTab<NV>::NE];
-  s_weights<NV>(S, ddir, dorg, ws);
+  s_weights<NV, T>(S, ddir, dorg, ws);
   const int f0 = SolidFaces<NV>::face(ws, 0);
   const int f1 = f0 < 0 ? -1 : SolidFaces<NV>::face(ws, 1);
   if (f1 < 0) return;
@@ -626,7 +656,8 @@ __device__ __forceinline__ void solid_test(const float *__restrict__ recs, uint3
   float th[2];
 #pragma unroll
   for (int h = 0; h < 2; h++) {
-    if (jax >= 0) SolidFaces<NV>::template point<false>(S, ws, h ? f1 : f0, ddir, jax, pt, nd3);
+    if (jax >= 0)
+      SolidFaces<NV>::template point<false, T>(S, ws, h ? f1 : f0, ddir, jax, pt, nd3);
     th[h] = s_t(jax >= 0 ? pt[jax] : 0.0f, jax, dorg, ddir);
   }
 #pragma unroll
@@ -634,7 +665,7 @@ __device__ __forceinline__ void solid_test(const float *__restrict__ recs, uint3
     if (th[h] >= 0.0f && th[h] < t) {
       t = th[h];
       prim = p;
-      s_full_point<NV>(S, ws, h ? f1 : f0, ddir, bp, bn);
+      s_full_point<NV, T>(S, ws, h ? f1 : f0, ddir, bp, bn);
       if (h) {  // the second point's normal is flipped
 #pragma unroll
         for (int c = 0; c < 3; c++) bn[c] = -1.0f * bn[c];
@@ -647,9 +678,9 @@ __device__ __forceinline__ void solid_test(const float *__restrict__ recs, uint3
 // culling).  prim = 0xFFFFFFFF and t = FLT_MAX when nothing is hit.  STACK:
 // the walk's stack (the tree's depth + 2 at least); returns false (the walk
 // stopped) for a deeper tree.
-template <int NV, int STACK>
+template <int NV, int STACK, typename T = float>
 __device__ __forceinline__ bool solid_walk(const SNode *__restrict__ nodes,
-                                           const float *__restrict__ recs,
+                                           const void *__restrict__ recs,
                                            const float org[3], const float dir[3],
                                            uint32_t prev, float &t, uint32_t &prim,
                                            float bp[3], float bn[3]) {
@@ -687,7 +718,7 @@ __device__ __forceinline__ bool solid_walk(const SNode *__restrict__ nodes,
     }
     const uint32_t first = nd.w0, cnt = nd.w1 & ~kSolidLeaf;
     for (uint32_t j = first; j < first + cnt; j++)
-      solid_test<NV>(recs, j, prev, dorg, ddir, jax, t, prim, bp, bn);
+      solid_test<NV, T>(recs, j, prev, dorg, ddir, jax, t, prim, bp, bn);
   }
   return true;
 }

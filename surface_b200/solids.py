@@ -26,7 +26,8 @@ SOLID_NODE_DTYPE = LINE_NODE_DTYPE  # SolidNode: the same 40-byte record
 @dataclass
 class Solid:
     """render/render_prim_solid.h: numVertsPerSolid (5, 6 or 8), vertices
-    (V, 3) float32, indices (N, numVertsPerSolid) uint32."""
+    (V, 3) float32, or float64 for double-precision positions (dvertices,
+    isDoublePrecisionPos), indices (N, numVertsPerSolid) uint32."""
     numVertsPerSolid: int
     vertices: object
     indices: object
@@ -43,7 +44,9 @@ class SolidAccel:
 
     def Build32(self, solids: Solid, options=None) -> bool:
         """SolidAccel::Build32 (render/render_accel_solid.cc:1795)."""
-        v = _View(solids.vertices, np.float32, torch.float32)
+        dbl = getattr(solids.vertices, "dtype", None) in (np.float64, torch.float64)
+        v = (_View(solids.vertices, np.float64, torch.float64) if dbl
+             else _View(solids.vertices, np.float32, torch.float32))
         ix = _View(solids.indices, np.uint32, torch.int32)
         nv = int(solids.numVertsPerSolid)
         # device inputs: in torch's stream order; host inputs: the context's stream
@@ -51,8 +54,9 @@ class SolidAccel:
             self.ctx.use_torch_stream()
         else:
             self.ctx.use_own_stream()
-        check(self.L.srt_solid_build(self.h, nv, v.ptr, v.nbytes // 12, ix.ptr,
-                                     ix.nbytes // (4 * nv)))
+        build = self.L.srt_solid_build_double if dbl else self.L.srt_solid_build
+        check(build(self.h, nv, v.ptr, v.nbytes // (24 if dbl else 12), ix.ptr,
+                    ix.nbytes // (4 * nv)))
         self.built = True
         return True
 

@@ -147,3 +147,56 @@ def test_rebuild_and_trace_across_streams():
         assert np.array_equal(bits(h.cpu().numpy()), bits(want.view(np.float32).reshape(-1, 4)))
     n, nn = acc.info()
     assert n == ix.shape[0] and nn > 1
+
+
+@pytest.mark.parametrize("nv,g,m,shift", [(8, 11, None, 0.0), (6, 8, None, 100.0),
+                                          (5, 6, None, 0.0), (8, 9, 400, 0.0)])
+def test_double_positions(nv, g, m, shift):
+    """Double-precision positions (float64 vertices: Solid::dvertices): the
+    GPU Build32 (and the SAH Build below 1024 solids) and trace equal the
+    oracle's, which equals the reference's, from host and device inputs."""
+    v, ix = S.solid_grid(nv, g, seed=nv)
+    rng = np.random.default_rng(nv + 100)
+    v64 = v.astype(np.float64) + shift + rng.uniform(-1e-9, 1e-9, size=v.shape)
+    if m is not None:
+        ix = ix[:m]
+    rays = S.solid_rays(64, seed=nv)
+    rays["org"] += np.float32(shift)
+    _check(nv, v64, ix, rays)
+    _check(nv, v64, ix, rays, device_inputs=True)
+
+
+def test_double_position_solids_in_a_scene():
+    """A double-precision solid element beside a triangle element: the scene
+    trace's per-ray loop walks it with the double records."""
+    from surface_b200.scene import RenderGraph
+    v, ix = S.solid_grid(8, 11, seed=4)
+    v64 = v.astype(np.float64) - 0.5 + np.random.default_rng(3).uniform(-1e-9, 1e-9, v.shape)
+    tv, tf = S.displaced_octasphere(3, seed=5)
+    Ts = [S.affine((0, 0, 1), 30, (1.0, 1.2, 0.8), (-1.0, 0, 0)), S.affine(scale=(0.6,) * 3,
+                                                                             translate=(1.2, 0, 0))]
+    solid = SolidAccel()
+    solid.Build32(Solid(8, v64, ix))
+    tri = sb.TriangleAccel()
+    tri.Build32(sb.Mesh(tv, tf))
+    g = RenderGraph()
+    g.AddRenderElement(solid, Ts[0])
+    g.AddRenderElement(tri, Ts[1])
+    g.Build()
+    oacc = [O.OracleSolids(8, v64, ix), O.OracleAccel(O.TRI, tv, tf)]
+    mats, wlo, whi = [], [], []
+    for a, T in zip((solid, tri), Ts):
+        lo, hi = a.BoundingBox()
+        i1, i2, b0, b1 = O.element_update(T, lo, hi)
+        mats.append((np.asarray(T).reshape(16), i1.reshape(16), i2.reshape(16)))
+        wlo.append(b0)
+        whi.append(b1)
+    o = O.OracleScene(oacc, [m[0] for m in mats], [m[1] for m in mats], [m[2] for m in mats],
+                      wlo, whi)
+    wlo, whi = np.array(wlo), np.array(whi)
+    rays = S.scene_rays(40_000, wlo.min(0), whi.max(0), seed=6, boxes=(wlo, whi))
+    want, wel = o.trace(rays)
+    assert set(wel[wel != S.MISS].tolist()) == {0, 1}
+    got, gel = g.Trace(rays)
+    assert np.array_equal(gel, wel)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))

@@ -106,3 +106,48 @@ def test_sah_build_below_1024_matches_reference(name, nv, v, ix):
         rh2, _, _ = r.trace(rays2)
         assert np.array_equal(bits(oh2.view(np.float32).reshape(-1, 4)),
                               bits(rh2.view(np.float32).reshape(-1, 4)))
+
+
+def _double_grid(nv, g, seed, shift=0.0):
+    """A solid grid with double-precision positions that float does not
+    hold: the float grid's vertices plus a seeded sub-ulp jitter, shifted."""
+    v, ix = S.solid_grid(nv, g, seed=seed)
+    rng = np.random.default_rng(seed + 100)
+    v64 = v.astype(np.float64) + shift + rng.uniform(-1e-9, 1e-9, size=v.shape)
+    return v64, ix
+
+
+@needs_ref
+@pytest.mark.parametrize("nv,g,m,shift", [(8, 11, None, 0.0), (6, 8, None, 100.0),
+                                          (5, 6, None, 0.0), (8, 9, 400, 0.0),
+                                          (6, 7, 600, 37.5)])
+def test_double_positions_match_reference(nv, g, m, shift):
+    """isDoublePrecisionPos: the oracle's Build32 (and SAH Build below 1024
+    solids) and Traverse over double positions equal the reference's, node
+    for node and hit for hit."""
+    v64, ix = _double_grid(nv, g, seed=nv, shift=shift)
+    if m is not None:
+        ix = ix[:m]
+    o = O.OracleSolids(nv, v64, ix)
+    r = O.RefSolids(nv, v64, ix)
+    assert o.verts.dtype == np.float64 and r.verts.dtype == np.float64
+    on, oi = o.export()
+    rn, ri = r.dump()
+    if ix.shape[0] < 1024:
+        assert _raw(on) == _raw(rn)
+    else:
+        assert O.tree_canonical(on) == O.tree_canonical(rn)
+    assert np.array_equal(oi, ri)
+    rays = S.solid_rays(48, seed=nv)
+    rays["org"] += np.float32(shift)
+    oh, onr, op = o.trace(rays)
+    rh, rnr, rp = r.trace(rays)
+    assert np.array_equal(bits(oh.view(np.float32).reshape(-1, 4)),
+                          bits(rh.view(np.float32).reshape(-1, 4)))
+    assert np.array_equal(bits(onr), bits(rnr)) and np.array_equal(bits(op), bits(rp))
+    assert (rh["prim"] != O.MISS).mean() > 0.3
+    # the double positions matter: the float build differs somewhere
+    f = O.OracleSolids(nv, v64.astype(np.float32), ix)
+    fh, _, fp = f.trace(rays)
+    assert not (np.array_equal(fh.view(np.uint32), oh.view(np.uint32))
+                and np.array_equal(fp.view(np.uint32), op.view(np.uint32)))
