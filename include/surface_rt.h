@@ -726,6 +726,16 @@ SRT_API srt_status srt_solid_build(srt_solid_accel *accel, int32_t verts_per_sol
 SRT_API srt_status srt_solid_build_double(srt_solid_accel *accel, int32_t verts_per_solid,
                                           const double *vertices, size_t nverts,
                                           const uint32_t *indices, size_t nsolids);
+/* SolidAccel::Build, the binned-SAH build (render_accel_solid.cc:1754), at
+ * every size: the build the reference's GLES accel builder runs
+ * (gles/gles_accel_builder.cc:967; srt_cache_build_solids uses it).  A host
+ * build uploaded to the GPU; traversal as above. */
+SRT_API srt_status srt_solid_build_sah(srt_solid_accel *accel, int32_t verts_per_solid,
+                                       const float *vertices, size_t nverts,
+                                       const uint32_t *indices, size_t nsolids);
+SRT_API srt_status srt_solid_build_sah_double(srt_solid_accel *accel, int32_t verts_per_solid,
+                                              const double *vertices, size_t nverts,
+                                              const uint32_t *indices, size_t nsolids);
 SRT_API srt_status srt_solid_trace(srt_solid_accel *accel, const srt_ray *rays, size_t n,
                                    srt_hit *hits, float *normals, float *positions);
 SRT_API srt_status srt_solid_bbox(srt_solid_accel *accel, double bmin[3], double bmax[3]);

@@ -142,6 +142,8 @@ def lib():
         L.so_solid_build.argtypes = [C.c_int, _P, _P, _SZ]
         L.so_solid_build_d.restype = _P
         L.so_solid_build_d.argtypes = [C.c_int, _P, _P, _SZ]
+        L.so_solid_build_sah.restype = _P
+        L.so_solid_build_sah.argtypes = [C.c_int, _P, _P, _P, _SZ]
         L.so_solid_free.argtypes = [_P]
         L.so_solid_num_nodes.restype = _SZ
         L.so_solid_num_nodes.argtypes = [_P]
@@ -220,6 +222,8 @@ def ref():
         L.ref_solid_build.argtypes = [C.c_int, _P, _P, _SZ]
         L.ref_solid_build_d.restype = _P
         L.ref_solid_build_d.argtypes = [C.c_int, _P, _P, _SZ]
+        L.ref_solid_build_sah.restype = _P
+        L.ref_solid_build_sah.argtypes = [C.c_int, _P, _P, _P, _SZ]
         L.ref_solid_free.argtypes = [_P]
         L.ref_solid_dump.argtypes = [_P, C.c_char_p]
         L.ref_solid_bbox.argtypes = [_P, _P, _P]
@@ -1132,13 +1136,20 @@ class OracleSolids:
     """The restatement of SolidAccel::Build32 / Traverse (nv = 5 pyramids,
     6 prisms, 8 hexahedra); float64 vertices are double-precision positions."""
 
-    def __init__(self, nv, verts, indices):
+    def __init__(self, nv, verts, indices, sah=False):
+        """sah: SolidAccel::Build (binned SAH) at every size."""
         self.nv = int(nv)
         self.verts = _solid_verts(verts)
         self.ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
         self.n = self.ix.size // self.nv
-        build = lib().so_solid_build_d if self.verts.dtype == np.float64 else lib().so_solid_build
-        self.h = build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
+        dbl = self.verts.dtype == np.float64
+        if sah:
+            self.h = lib().so_solid_build_sah(self.nv, None if dbl else _ptr(self.verts),
+                                              _ptr(self.verts) if dbl else None, _ptr(self.ix),
+                                              self.n)
+        else:
+            build = lib().so_solid_build_d if dbl else lib().so_solid_build
+            self.h = build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
 
     def export(self):
         nn = lib().so_solid_num_nodes(self.h)
@@ -1167,7 +1178,8 @@ class OracleSolids:
 class RefSolids:
     """The reference's own SolidAccel (Build32, Traverse, Dump, BoundingBox)."""
 
-    def __init__(self, nv, verts, indices):
+    def __init__(self, nv, verts, indices, sah=False):
+        """sah: SolidAccel::Build (binned SAH) at every size."""
         L = ref()
         if L is None:
             raise RuntimeError("reference harness not built")
@@ -1176,8 +1188,14 @@ class RefSolids:
         self.verts = _solid_verts(verts)
         self.ix = np.ascontiguousarray(indices, np.uint32).reshape(-1)
         self.n = self.ix.size // self.nv
-        build = L.ref_solid_build_d if self.verts.dtype == np.float64 else L.ref_solid_build
-        self.h = build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
+        dbl = self.verts.dtype == np.float64
+        if sah:
+            self.h = L.ref_solid_build_sah(self.nv, None if dbl else _ptr(self.verts),
+                                           _ptr(self.verts) if dbl else None, _ptr(self.ix),
+                                           self.n)
+        else:
+            build = L.ref_solid_build_d if dbl else L.ref_solid_build
+            self.h = build(self.nv, _ptr(self.verts), _ptr(self.ix), self.n)
 
     def dump(self):
         with tempfile.TemporaryDirectory() as td:

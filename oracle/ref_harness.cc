@@ -685,6 +685,26 @@ REF_API void *ref_solid_build(int nv, const float *verts, const uint32_t *indice
   return h;
 }
 
+// SolidAccel::Build (binned SAH) at every size; dverts non-null: double
+// positions.
+REF_API void *ref_solid_build_sah(int nv, const float *verts, const double *dverts,
+                                  const uint32_t *indices, size_t n) {
+  SolidHandle *h = new SolidHandle();
+  memset(&h->solids, 0, sizeof(h->solids));
+  h->solids.numVertsPerSolid = nv;
+  h->solids.numSolids = n;
+  h->solids.vertices = verts;
+  h->solids.dvertices = dverts;
+  h->solids.isDoublePrecisionPos = dverts != nullptr;
+  h->solids.indices = const_cast<uint32_t *>(indices);
+  SolidBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build(&h->solids, opt);
+  }
+  return h;
+}
+
 // The same with double-precision positions (Solid::dvertices).
 REF_API void *ref_solid_build_d(int nv, const double *dverts, const uint32_t *indices, size_t n) {
   SolidHandle *h = new SolidHandle();

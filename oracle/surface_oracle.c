@@ -3677,7 +3677,7 @@ static size_t sah_build(so_solids *S, uint32_t l, uint32_t r, int depth) {
 }
 
 static so_solids *solid_build(int nv, const float *v, const double *dv, const uint32_t *ix,
-                              size_t n) {
+                              size_t n, int sah) {
   so_solids *S = (so_solids *)calloc(1, sizeof(so_solids));
   S->nv = nv;
   S->v = v;
@@ -3689,7 +3689,7 @@ static so_solids *solid_build(int nv, const float *v, const double *dv, const ui
   S->child = (uint32_t *)malloc((n + 1) * 4);
   S->lt = (uint8_t *)malloc(n + 1);
   S->rt = (uint8_t *)malloc(n + 1);
-  if (n < 1024) { /* Build32 runs Build below 1024 solids */
+  if (sah || n < 1024) { /* Build; Build32 runs it below 1024 solids */
     for (size_t i = 0; i < n; i++) S->sidx[i] = (uint32_t)i;
     if (n > 0) sah_build(S, 0, (uint32_t)n, 0);
     return S;
@@ -3736,12 +3736,18 @@ static so_solids *solid_build(int nv, const float *v, const double *dv, const ui
 }
 
 SO_API so_solids *so_solid_build(int nv, const float *v, const uint32_t *ix, size_t n) {
-  return solid_build(nv, v, NULL, ix, n);
+  return solid_build(nv, v, NULL, ix, n, 0);
 }
 
 /* Double-precision positions (Solid::dvertices, isDoublePrecisionPos). */
 SO_API so_solids *so_solid_build_d(int nv, const double *dv, const uint32_t *ix, size_t n) {
-  return solid_build(nv, NULL, dv, ix, n);
+  return solid_build(nv, NULL, dv, ix, n, 0);
+}
+
+/* SolidAccel::Build (binned SAH) at every size, float or double positions. */
+SO_API so_solids *so_solid_build_sah(int nv, const float *v, const double *dv,
+                                     const uint32_t *ix, size_t n) {
+  return solid_build(nv, v, dv, ix, n, 1);
 }
 
 SO_API void so_solid_free(so_solids *S) {

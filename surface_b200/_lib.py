@@ -171,6 +171,8 @@ _SIGS = {
     "srt_solid_create": [_P, C.POINTER(_P)],
     "srt_solid_destroy": [_P],
     "srt_solid_build": [_P, C.c_int32, _P, _SZ, _P, _SZ],
+    "srt_solid_build_sah": [_P, C.c_int32, _P, _SZ, _P, _SZ],
+    "srt_solid_build_sah_double": [_P, C.c_int32, _P, _SZ, _P, _SZ],
     "srt_solid_build_double": [_P, C.c_int32, _P, _SZ, _P, _SZ],
     "srt_solid_trace": [_P, _P, _SZ, _P, _P, _P],
     "srt_solid_bbox": [_P, _P, _P],

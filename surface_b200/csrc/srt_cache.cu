@@ -445,7 +445,9 @@ SRT_API srt_status srt_cache_build_solids(srt_cache *c, const srt_cache_key *key
       c, kSolids, key, is_static, out,
       [&](srt_solid_accel **a) { return srt_solid_create(c->ctx, a); },
       [&](srt_solid_accel *a) {
-        return srt_solid_build(a, verts_per_solid, vertices, nverts, indices, nsolids);
+        // AccelBuilder::BuildSolidAccel builds with SolidAccel::Build, the
+        // binned-SAH build, at every size (gles/gles_accel_builder.cc:967)
+        return srt_solid_build_sah(a, verts_per_solid, vertices, nverts, indices, nsolids);
       });
 }
 

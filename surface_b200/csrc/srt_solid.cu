@@ -813,9 +813,12 @@ srt_status solid_build_sah(srt_solid_accel *a, int nv, const T *v, size_t nverts
   return SRT_OK;
 }
 
+// sah: SolidAccel::Build (the binned-SAH build) for every size, as the
+// GLES accel builder calls it; else Build32 (SAH below kSahMax, LBVH above).
 template <typename T>
 srt_status solid_build_t(srt_solid_accel *a, int32_t verts_per_solid, const T *vertices,
-                         size_t nverts, const uint32_t *indices, size_t nsolids) {
+                         size_t nverts, const uint32_t *indices, size_t nsolids,
+                         bool sah = false) {
   if (!a || !vertices || !indices) return SRT_ERR_INVALID;
   const int nv = verts_per_solid;
   if ((nv != 5 && nv != 6 && nv != 8) || nsolids < 2 || nsolids >= (1u << 28)) {
@@ -838,7 +841,7 @@ srt_status solid_build_t(srt_solid_accel *a, int32_t verts_per_solid, const T *v
   // the latest trace (on any stream) reads the tree this build overwrites
   if (a->used && (e = cudaStreamWaitEvent(ctx->stream, a->ev_used, 0)) != cudaSuccess)
     return cuda_status(e, "solid build");
-  if (n < kSahMax) return solid_build_sah<T>(a, nv, d_v, nverts, d_ix, n);
+  if (sah || n < kSahMax) return solid_build_sah<T>(a, nv, d_v, nverts, d_ix, n);
   a->deep = false;
   a->dbl = sizeof(T) == 8;
   if ((e = a->dbox.ensure(64)) != cudaSuccess || (e = a->dcodes.ensure(n * 4)) != cudaSuccess ||
@@ -958,6 +961,18 @@ SRT_API srt_status srt_solid_build_double(srt_solid_accel *a, int32_t verts_per_
                                           const double *vertices, size_t nverts,
                                           const uint32_t *indices, size_t nsolids) {
   return solid_build_t<double>(a, verts_per_solid, vertices, nverts, indices, nsolids);
+}
+
+SRT_API srt_status srt_solid_build_sah(srt_solid_accel *a, int32_t verts_per_solid,
+                                       const float *vertices, size_t nverts,
+                                       const uint32_t *indices, size_t nsolids) {
+  return solid_build_t<float>(a, verts_per_solid, vertices, nverts, indices, nsolids, true);
+}
+
+SRT_API srt_status srt_solid_build_sah_double(srt_solid_accel *a, int32_t verts_per_solid,
+                                              const double *vertices, size_t nverts,
+                                              const uint32_t *indices, size_t nsolids) {
+  return solid_build_t<double>(a, verts_per_solid, vertices, nverts, indices, nsolids, true);
 }
 
 SRT_API srt_status srt_solid_trace(srt_solid_accel *a, const srt_ray *rays, size_t n,

@@ -42,8 +42,16 @@ class SolidAccel:
         self.h = h
         self.built = False
 
+    def Build(self, solids: Solid, options=None) -> bool:
+        """SolidAccel::Build (render/render_accel_solid.cc:1754): the binned-SAH
+        build at every size, as the GLES accel builder runs it."""
+        return self._build(solids, sah=True)
+
     def Build32(self, solids: Solid, options=None) -> bool:
         """SolidAccel::Build32 (render/render_accel_solid.cc:1795)."""
+        return self._build(solids, sah=False)
+
+    def _build(self, solids: Solid, sah: bool) -> bool:
         dbl = getattr(solids.vertices, "dtype", None) in (np.float64, torch.float64)
         v = (_View(solids.vertices, np.float64, torch.float64) if dbl
              else _View(solids.vertices, np.float32, torch.float32))
@@ -54,7 +62,10 @@ class SolidAccel:
             self.ctx.use_torch_stream()
         else:
             self.ctx.use_own_stream()
-        build = self.L.srt_solid_build_double if dbl else self.L.srt_solid_build
+        if sah:
+            build = self.L.srt_solid_build_sah_double if dbl else self.L.srt_solid_build_sah
+        else:
+            build = self.L.srt_solid_build_double if dbl else self.L.srt_solid_build
         check(build(self.h, nv, v.ptr, v.nbytes // (24 if dbl else 12), ix.ptr,
                     ix.nbytes // (4 * nv)))
         self.built = True

@@ -213,7 +213,8 @@ def test_cache_lines_and_solids():
                           bits(direct.Traverse(rays).view(np.float32).reshape(-1, 4)))
     srays = S.solid_rays(48)
     ds = SolidAccel()
-    ds.Build32(Solid(8, v, ix))
+    ds.Build(Solid(8, v, ix))  # BuildSolidAccel runs SolidAccel::Build at every size
+    assert s1.export()[0].tobytes() == O.OracleSolids(8, v, ix, sah=True).export()[0].tobytes()
     want = bits(ds.Traverse(srays).view(np.float32).reshape(-1, 4))
     assert np.array_equal(bits(s1.Traverse(srays).view(np.float32).reshape(-1, 4)), want)
     assert np.array_equal(bits(d.Traverse(srays).view(np.float32).reshape(-1, 4)), want)

@@ -200,3 +200,24 @@ def test_double_position_solids_in_a_scene():
     got, gel = g.Trace(rays)
     assert np.array_equal(gel, wel)
     assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
+
+
+@pytest.mark.parametrize("nv,g,dbl", [(8, 14, False), (6, 11, True)])
+def test_sah_build_at_every_size(nv, g, dbl):
+    """SolidAccel::Build (binned SAH at every size, the GLES builder's
+    choice): the uploaded tree, order and hits equal the oracle's."""
+    v, ix = S.solid_grid(nv, g, seed=nv)
+    if dbl:
+        v = v.astype(np.float64) + np.random.default_rng(1).uniform(-1e-9, 1e-9, v.shape)
+    o = O.OracleSolids(nv, v, ix, sah=True)
+    acc = SolidAccel()
+    acc.Build(Solid(nv, v, ix))
+    gn, gi = acc.export()
+    on, oi = o.export()
+    assert gn.tobytes() == on.tobytes() and np.array_equal(gi, oi)
+    rays = S.solid_rays(64, seed=nv)
+    want, wn, wp = o.trace(rays)
+    got, gnrm, gpos = acc.Traverse(rays, want_point=True)
+    assert np.array_equal(bits(got.view(np.float32).reshape(-1, 4)),
+                          bits(want.view(np.float32).reshape(-1, 4)))
+    assert np.array_equal(bits(gnrm), bits(wn)) and np.array_equal(bits(gpos), bits(wp))

@@ -151,3 +151,28 @@ def test_double_positions_match_reference(nv, g, m, shift):
     fh, _, fp = f.trace(rays)
     assert not (np.array_equal(fh.view(np.uint32), oh.view(np.uint32))
                 and np.array_equal(fp.view(np.uint32), op.view(np.uint32)))
+
+
+@needs_ref
+@pytest.mark.parametrize("nv,g,dbl", [(8, 14, False), (6, 11, False), (5, 8, True)])
+def test_sah_build_at_every_size_matches_reference(nv, g, dbl):
+    """SolidAccel::Build, which the reference's GLES accel builder runs at
+    every size (gles/gles_accel_builder.cc:967): the oracle's SAH tree over
+    1024 solids or more equals the reference's node for node, float and
+    double positions."""
+    if dbl:
+        v, ix = _double_grid(nv, g, seed=nv)
+    else:
+        v, ix = S.solid_grid(nv, g, seed=nv)
+    o = O.OracleSolids(nv, v, ix, sah=True)
+    r = O.RefSolids(nv, v, ix, sah=True)
+    on, oi = o.export()
+    rn, ri = r.dump()
+    assert len(on) < 2 * ix.shape[0] and _raw(on) == _raw(rn)
+    assert np.array_equal(oi, ri)
+    rays = S.solid_rays(48, seed=nv)
+    oh, _, op = o.trace(rays)
+    rh, _, rp = r.trace(rays)
+    assert np.array_equal(bits(oh.view(np.float32).reshape(-1, 4)),
+                          bits(rh.view(np.float32).reshape(-1, 4)))
+    assert np.array_equal(bits(op), bits(rp))
