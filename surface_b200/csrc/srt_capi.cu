@@ -5,6 +5,8 @@
 #include <string>
 #include <vector>
 
+#include <type_traits>
+
 #include "srt_internal.cuh"
 
 namespace srt {
@@ -54,6 +56,19 @@ bool is_device_ptr(const void *p) {
     return false;
   }
   return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// A page-locked host array that the device reaches through unified
+// addressing (cudaHostAlloc / cudaHostRegister memory is mapped): the device
+// address to write it directly, else null (pageable memory).
+static void *mapped_ptr(void *p) {
+  if (!p) return nullptr;
+  cudaPointerAttributes at;
+  if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+    cudaGetLastError();
+    return nullptr;
+  }
+  return at.type == cudaMemoryTypeHost ? at.devicePointer : nullptr;
 }
 
 // Device view of a caller array: the pointer itself, or a copy into `stage`.
@@ -714,41 +729,49 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
     }
     dvs = o.vertex_scalar;
   }
-  // outputs: device pointers are written in place, host ones via staging
+  // outputs: device pointers are written in place; page-locked host arrays
+  // too, through their mapped addresses (the kernels' stores cross PCIe
+  // while they run, instead of a copy after them); pageable ones via staging
   const bool hits_dev = is_device_ptr(hits);
+  bool any_host = !hits_dev;
   srt_hit *dh = hits;
   cudaError_t e;
   if (!hits_dev) {
-    if ((e = ctx->s_stage_out.ensure(n * sizeof(srt_hit))) != cudaSuccess)
-      return cuda_status(e, "hit staging");
-    dh = ctx->s_stage_out.as<srt_hit>();
+    dh = static_cast<srt_hit *>(mapped_ptr(hits));
+    if (!dh) {
+      if ((e = ctx->s_stage_out.ensure(n * sizeof(srt_hit))) != cudaSuccess)
+        return cuda_status(e, "hit staging");
+      dh = ctx->s_stage_out.as<srt_hit>();
+    }
   }
   uint32_t *dsub = o.subface;
   float *dscal = o.scalar_out, *dnorm = o.normal_out;
   srt_isect *disx = o.isect;
-  if (dsub && !is_device_ptr(dsub)) {
-    if ((e = ctx->s_stage_sub.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
-    dsub = ctx->s_stage_sub.as<uint32_t>();
-  }
+  // a host output: its mapped address, else the staging buffer
+  auto host_out = [&](auto *&d, DevBuf &stage, size_t bytes) -> cudaError_t {
+    using P = std::remove_reference_t<decltype(d)>;
+    if (!d || is_device_ptr(d)) return cudaSuccess;
+    any_host = true;
+    if (void *m = mapped_ptr(d)) {
+      d = static_cast<P>(m);
+      return cudaSuccess;
+    }
+    cudaError_t err = stage.ensure(bytes);
+    if (err == cudaSuccess) d = stage.as<std::remove_pointer_t<P>>();
+    return err;
+  };
+  if ((e = host_out(dsub, ctx->s_stage_sub, n * 4)) != cudaSuccess)
+    return cuda_status(e, "staging");
   uint32_t *isub = dsub;  // entering faces for the shading pass
   if (disx && !isub && a->kind == SRT_TETRAHEDRA) {
     if ((e = ctx->s_isect_sub.ensure(n * 4)) != cudaSuccess)
       return cuda_status(e, "entering faces");
     isub = ctx->s_isect_sub.as<uint32_t>();
   }
-  if (disx && !is_device_ptr(disx)) {
-    if ((e = ctx->s_stage_isect.ensure(n * sizeof(srt_isect))) != cudaSuccess)
-      return cuda_status(e, "staging");
-    disx = ctx->s_stage_isect.as<srt_isect>();
-  }
-  if (dscal && !is_device_ptr(dscal)) {
-    if ((e = ctx->s_stage_scal.ensure(n * 4)) != cudaSuccess) return cuda_status(e, "staging");
-    dscal = ctx->s_stage_scal.as<float>();
-  }
-  if (dnorm && !is_device_ptr(dnorm)) {
-    if ((e = ctx->s_stage_norm.ensure(n * 12)) != cudaSuccess) return cuda_status(e, "staging");
-    dnorm = ctx->s_stage_norm.as<float>();
-  }
+  if ((e = host_out(disx, ctx->s_stage_isect, n * sizeof(srt_isect))) != cudaSuccess ||
+      (e = host_out(dscal, ctx->s_stage_scal, n * 4)) != cudaSuccess ||
+      (e = host_out(dnorm, ctx->s_stage_norm, n * 12)) != cudaSuccess)
+    return cuda_status(e, "staging");
   if ((reinterpret_cast<uintptr_t>(drays) | reinterpret_cast<uintptr_t>(dh)) & 15u) {
     set_error("ray and hit arrays must be 16-byte aligned");
     return SRT_ERR_INVALID;
@@ -766,16 +789,16 @@ SRT_API srt_status srt_trace_closest(srt_accel *a, const srt_ray *rays, size_t n
     if (s != SRT_OK) return s;
   }
   cudaStream_t st = ctx->stream;
-  bool any_host = !hits_dev || (dsub != o.subface) || (dscal != o.scalar_out) ||
-                  (dnorm != o.normal_out) || (disx != o.isect);
-  if (disx != o.isect)
+  // staged outputs come back by copies (mapped ones were written in place)
+  if (disx != o.isect && disx == ctx->s_stage_isect.as<srt_isect>())
     cudaMemcpyAsync(o.isect, disx, n * sizeof(srt_isect), cudaMemcpyDeviceToHost, st);
-  if (!hits_dev)
+  if (dh == ctx->s_stage_out.as<srt_hit>() && dh != hits)
     cudaMemcpyAsync(hits, dh, n * sizeof(srt_hit), cudaMemcpyDeviceToHost, st);
-  if (dsub != o.subface) cudaMemcpyAsync(o.subface, dsub, n * 4, cudaMemcpyDeviceToHost, st);
-  if (dscal != o.scalar_out)
+  if (dsub != o.subface && dsub == ctx->s_stage_sub.as<uint32_t>())
+    cudaMemcpyAsync(o.subface, dsub, n * 4, cudaMemcpyDeviceToHost, st);
+  if (dscal != o.scalar_out && dscal == ctx->s_stage_scal.as<float>())
     cudaMemcpyAsync(o.scalar_out, dscal, n * 4, cudaMemcpyDeviceToHost, st);
-  if (dnorm != o.normal_out)
+  if (dnorm != o.normal_out && dnorm == ctx->s_stage_norm.as<float>())
     cudaMemcpyAsync(o.normal_out, dnorm, n * 12, cudaMemcpyDeviceToHost, st);
   if (any_host || !is_device_ptr(rays)) return check_device_errors(ctx);
   return cuda_status(cudaGetLastError(), "trace");
