@@ -212,6 +212,19 @@ SRT_API srt_status srt_accel_build_tetrahedra(srt_accel *accel,
                                               size_t nvertices,
                                               const uint32_t *tets,
                                               size_t ntets);
+/* The same with double-precision positions (Tetrahedron::dvertices,
+ * isDoublePrecisionPos; render/render_prim_tetra.h): as the reference's
+ * Build32 does, the scene and node boxes pad each double coordinate in
+ * double and round to float, the Morton codes use the positions rounded to
+ * float, and the Pluecker tests take the doubles
+ * (render/render_accel_tetra.cc:1621-1660, 2009-2060).  The shading records
+ * (srt_trace_opts.isect) use the positions rounded to float, as
+ * BuildIntersection's real3 does (:2135-2150). */
+SRT_API srt_status srt_accel_build_tetrahedra_double(srt_accel *accel,
+                                                     const double *vertices,
+                                                     size_t nvertices,
+                                                     const uint32_t *tets,
+                                                     size_t ntets);
 /* n spheres: xyz centres; radius per sphere, or NULL for constant_radius
  * (Particles::radius / constantRadius, render/render_prim_particle.h:19-27). */
 SRT_API srt_status srt_accel_build_spheres(srt_accel *accel,

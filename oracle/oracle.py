@@ -69,6 +69,8 @@ def lib():
         L = C.CDLL(ORACLE_SO)
         L.so_build.restype = _P
         L.so_build.argtypes = [C.c_int, _P, _P, _P, C.c_float, _SZ]
+        L.so_build_tet_d.restype = _P
+        L.so_build_tet_d.argtypes = [_P, _SZ, _P, _SZ]
         L.so_free.argtypes = [_P]
         L.so_num_nodes.restype = _SZ
         L.so_num_nodes.argtypes = [_P]
@@ -177,6 +179,8 @@ def ref():
         L.ref_tri_build.argtypes = [_P, _SZ, _P, _SZ]
         L.ref_tet_build.restype = _P
         L.ref_tet_build.argtypes = [_P, _P, _SZ]
+        L.ref_tet_build_d.restype = _P
+        L.ref_tet_build_d.argtypes = [_P, _P, _SZ]
         L.ref_sphere_build.restype = _P
         L.ref_sphere_build.argtypes = [_P, _P, C.c_float, _SZ]
         L.ref_tri_trace.argtypes = [_P, _P, _SZ, _P, C.c_int, C.c_int]
@@ -240,8 +244,11 @@ class OracleAccel:
     emission order (depth-first, left first)."""
 
     def __init__(self, kind, verts, faces=None, radius=None, const_radius=0.0):
+        """Tetrahedra with float64 vertices keep double precision
+        (isDoublePrecisionPos)."""
         self.kind = kind
-        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        dbl = kind == TET and np.asarray(verts).dtype == np.float64
+        self.verts = np.ascontiguousarray(verts, np.float64 if dbl else np.float32).reshape(-1)
         self.faces = None if faces is None else np.ascontiguousarray(faces, np.uint32).reshape(-1)
         self.radius = None if radius is None else np.ascontiguousarray(radius, np.float32)
         n = {TRI: None, TET: None, SPHERE: None}[kind]
@@ -252,8 +259,12 @@ class OracleAccel:
         else:
             n = self.verts.size // 3
         self.n = n
-        self.h = lib().so_build(kind, _ptr(self.verts), _ptr(self.faces),
-                                _ptr(self.radius), C.c_float(const_radius), n)
+        if dbl:
+            self.h = lib().so_build_tet_d(_ptr(self.verts), self.verts.size // 3,
+                                          _ptr(self.faces), n)
+        else:
+            self.h = lib().so_build(kind, _ptr(self.verts), _ptr(self.faces),
+                                    _ptr(self.radius), C.c_float(const_radius), n)
         if not self.h:
             raise ValueError("oracle build needs at least 2 primitives")
         nn = lib().so_num_nodes(self.h)
@@ -486,7 +497,8 @@ class RefAccel:
             raise RuntimeError("reference harness not built")
         self.L = L
         self.kind = kind
-        self.verts = np.ascontiguousarray(verts, np.float32).reshape(-1)
+        dbl = kind == TET and np.asarray(verts).dtype == np.float64
+        self.verts = np.ascontiguousarray(verts, np.float64 if dbl else np.float32).reshape(-1)
         self.faces = None if faces is None else np.ascontiguousarray(faces, np.uint32).reshape(-1)
         self.radius = None if radius is None else np.ascontiguousarray(radius, np.float32)
         if kind == TRI:
@@ -496,7 +508,8 @@ class RefAccel:
             self.tag = "tri"
         elif kind == TET:
             self.n = self.faces.size // 4
-            self.h = L.ref_tet_build(_ptr(self.verts), _ptr(self.faces), self.n)
+            build = L.ref_tet_build_d if dbl else L.ref_tet_build
+            self.h = build(_ptr(self.verts), _ptr(self.faces), self.n)
             self.tag = "tet"
         else:
             self.n = self.verts.size // 3

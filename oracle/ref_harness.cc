@@ -182,6 +182,23 @@ REF_API void *ref_tet_build(const float *verts, const uint32_t *faces,
   return h;
 }
 
+// The same with double-precision positions (Tetrahedron::dvertices).
+REF_API void *ref_tet_build_d(const double *dverts, const uint32_t *faces, size_t ntets) {
+  TetHandle *h = new TetHandle();
+  memset(&h->tets, 0, sizeof(h->tets));
+  h->tets.numTetrahedrons = ntets;
+  h->tets.vertices = nullptr;
+  h->tets.dvertices = dverts;
+  h->tets.isDoublePrecisionPos = true;
+  h->tets.faces = const_cast<uint32_t *>(faces);
+  TetraBuildOptions opt;
+  {
+    QuietStdout q;
+    h->accel.Build32(&h->tets, opt);
+  }
+  return h;
+}
+
 REF_API void ref_tet_free(void *p) { delete static_cast<TetHandle *>(p); }
 
 REF_API int ref_tet_dump(void *p, const char *path) {

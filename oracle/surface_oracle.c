@@ -361,6 +361,10 @@ typedef struct {
   const uint32_t *faces;
   const float *radius;
   float constr;
+  /* tetrahedra with double-precision positions (isDoublePrecisionPos):
+   * dverts is borrowed, verts then holds them rounded to float (owned) */
+  const double *dverts;
+  float *own_verts;
 } so_accel;
 
 static size_t push_node(so_accel *a) {
@@ -394,10 +398,12 @@ static void leaf_box(const so_accel *a, uint32_t lo, uint32_t hi, float bmin[3],
     } else {
       int nv = a->kind == SO_TRI ? 3 : 4;
       for (int j = 0; j < nv; j++) {
-        const float *q = &a->verts[3 * (size_t)a->faces[(size_t)nv * p + j]];
+        const size_t vi = a->faces[(size_t)nv * p + j];
+        const float *q = &a->verts[3 * vi];
         for (int k = 0; k < 3; k++) {
-          float mn = q[k] - e;
-          float mx = q[k] + e;
+          /* double positions: padded in double, then rounded */
+          float mn = a->dverts ? (float)(a->dverts[3 * vi + k] - (double)e) : q[k] - e;
+          float mx = a->dverts ? (float)(a->dverts[3 * vi + k] + (double)e) : q[k] + e;
           if (bmin[k] > mn) bmin[k] = mn;
           if (bmax[k] < mx) bmax[k] = mx;
         }
@@ -442,12 +448,19 @@ static size_t emit(so_accel *a, uint32_t root, uint32_t lo, uint32_t hi,
 /* Build32 for the three primitive kinds (render/render_accel_triangle.cc:1389,
  * render/render_accel_tetra.cc:1579, render/render_accel_particle.cc:1560).
  * Requires n >= 2 (the reference switches to its SAH builder below 1024). */
-SO_API so_accel *so_build(int kind, const float *verts, const uint32_t *faces,
-                          const float *radius, float constr, size_t n) {
+static so_accel *build_impl(int kind, const float *verts, const double *dverts,
+                            size_t nverts, const uint32_t *faces, const float *radius,
+                            float constr, size_t n) {
   if (n < 2) return NULL;
   so_accel *a = (so_accel *)calloc(1, sizeof(so_accel));
   a->kind = kind;
   a->nprims = n;
+  if (dverts) { /* positions rounded to float: Morton codes, shading records */
+    a->own_verts = (float *)malloc(3 * nverts * sizeof(float));
+    for (size_t i = 0; i < 3 * nverts; i++) a->own_verts[i] = (float)dverts[i];
+    verts = a->own_verts;
+    a->dverts = dverts;
+  }
   a->verts = verts;
   a->faces = faces;
   a->radius = radius;
@@ -464,6 +477,22 @@ SO_API so_accel *so_build(int kind, const float *verts, const uint32_t *faces,
     a->keps = FLT_EPSILON * (float)es;
     a->max_leaf = 16;
     so_morton_tris(verts, faces, n, bmin, bmax, a->codes);
+  } else if (kind == SO_TET && dverts) {
+    /* ComputeBoundingBoxOMP over dvertices: padded in double, rounded */
+    const double e = (double)(FLT_EPSILON * 16);
+    for (int k = 0; k < 3; k++) {
+      bmin[k] = FLT_MAX;
+      bmax[k] = -FLT_MAX;
+    }
+    for (size_t i = 0; i < 4 * n; i++)
+      for (int k = 0; k < 3; k++) {
+        bmin[k] = fmin_ref(bmin[k], (float)(dverts[3 * (size_t)faces[i] + k] - e));
+        bmax[k] = fmax_ref(bmax[k], (float)(dverts[3 * (size_t)faces[i] + k] + e));
+      }
+    a->eps_scale = 16.0;
+    a->keps = FLT_EPSILON * 16;
+    a->max_leaf = 4;
+    so_morton_tets(verts, faces, n, bmin, bmax, a->codes);
   } else if (kind == SO_TET) {
     so_bbox_tets(verts, faces, n, bmin, bmax);
     a->eps_scale = 16.0;
@@ -503,8 +532,20 @@ SO_API so_accel *so_build(int kind, const float *verts, const uint32_t *faces,
   return a;
 }
 
+SO_API so_accel *so_build(int kind, const float *verts, const uint32_t *faces,
+                          const float *radius, float constr, size_t n) {
+  return build_impl(kind, verts, NULL, 0, faces, radius, constr, n);
+}
+
+/* Tetrahedra with double-precision positions (Tetrahedron::dvertices). */
+SO_API so_accel *so_build_tet_d(const double *dverts, size_t nverts, const uint32_t *faces,
+                                size_t n) {
+  return build_impl(SO_TET, NULL, dverts, nverts, faces, NULL, 0.0f, n);
+}
+
 SO_API void so_free(so_accel *a) {
   if (!a) return;
+  free(a->own_verts);
   free(a->nodes);
   free(a->indices);
   free(a->codes);
@@ -727,6 +768,20 @@ static inline void param_dist(d3 o, d3 d, d3 pe, d3 pl, double *te, double *tl) 
 
 /* Output: enter face, enter barycentrics (ue1, ue2), leave barycentric ul1,
  * enter distance.  Mirrors RayTetraPluecker's face order and sign logic. */
+/* Corner vi of a tetrahedron as the Pluecker test takes it: the float
+ * position, or the double one (TestLeafNode's dvertices branch). */
+static inline void tet_corner(const so_accel *a, size_t vi, d3 *out) {
+  if (a->dverts) {
+    out->x = a->dverts[3 * vi];
+    out->y = a->dverts[3 * vi + 1];
+    out->z = a->dverts[3 * vi + 2];
+  } else {
+    out->x = a->verts[3 * vi];
+    out->y = a->verts[3 * vi + 1];
+    out->z = a->verts[3 * vi + 2];
+  }
+}
+
 static int ray_tet(d3 orig, d3 dir, const d3 V[4], int *ef, double *ue1,
                    double *ue2, double *ul1, double *te) {
   int enterF = -1, leaveF = -1;
@@ -917,10 +972,7 @@ static int trace_from(const so_accel *a, const so_ray *ray, const float *prevN,
           if (f == ray->prev_prim) continue;
           st->prim_tests++;
           d3 V[4];
-          for (int j = 0; j < 4; j++) {
-            const float *p = &a->verts[3 * (size_t)a->faces[4 * (size_t)f + j]];
-            V[j].x = p[0]; V[j].y = p[1]; V[j].z = p[2];
-          }
+          for (int j = 0; j < 4; j++) tet_corner(a, a->faces[4 * (size_t)f + j], &V[j]);
           int ef;
           double ue1, ue2, ul1, te;
           if (ray_tet(o, d, V, &ef, &ue1, &ue2, &ul1, &te)) {
@@ -1094,10 +1146,7 @@ static inline int prim_candidate(const so_accel *a, uint32_t f, const so_ray *ra
   }
   if (f == ray->prev_prim) return 0;
   d3 V[4];
-  for (int j = 0; j < 4; j++) {
-    const float *p = &a->verts[3 * (size_t)a->faces[4 * (size_t)f + j]];
-    V[j].x = p[0]; V[j].y = p[1]; V[j].z = p[2];
-  }
+  for (int j = 0; j < 4; j++) tet_corner(a, a->faces[4 * (size_t)f + j], &V[j]);
   double te;
   if (!ray_tet(o, d, V, ef, e1, e2, ul1, &te) || !(te >= 0.0)) return 0;
   *tc = te;

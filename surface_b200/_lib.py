@@ -106,6 +106,7 @@ _SIGS = {
     "srt_accel_destroy": [_P],
     "srt_accel_build_triangles": [_P, _P, _SZ, _P, _SZ],
     "srt_accel_build_tetrahedra": [_P, _P, _SZ, _P, _SZ],
+    "srt_accel_build_tetrahedra_double": [_P, _P, _SZ, _P, _SZ],
     "srt_accel_build_spheres": [_P, _P, _P, C.c_float, _SZ],
     "srt_build_triangles": [_P, _P, _SZ, _P, _SZ, C.POINTER(_P)],
     "srt_build_tetrahedra": [_P, _P, _SZ, _P, _SZ, C.POINTER(_P)],

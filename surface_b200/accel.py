@@ -124,7 +124,7 @@ class Mesh:
 @dataclass
 class Tetrahedron:
     """render/render_prim_tetra.h:30-37."""
-    vertices: object  # (V,3) float32
+    vertices: object  # (V,3) float32, or float64 for double positions (dvertices)
     faces: object     # (N,4) uint32
 
 
@@ -327,12 +327,17 @@ class TetraAccel(_Accel):
     KIND = SRT_TETRAHEDRA
 
     def Build32(self, tetras: Tetrahedron, options: TetraBuildOptions | None = None) -> bool:
-        """LBVH build (render/render_accel_tetra.cc:1579-1850)."""
-        v = _View(tetras.vertices, np.float32, torch.float32 if torch is not None else None)
+        """LBVH build (render/render_accel_tetra.cc:1579-1850); float64
+        vertices keep double precision (isDoublePrecisionPos)."""
+        dbl = str(getattr(tetras.vertices, "dtype", "")) in ("float64", "torch.float64")
+        if dbl:
+            v = _View(tetras.vertices, np.float64, torch.float64 if torch is not None else None)
+        else:
+            v = _View(tetras.vertices, np.float32, torch.float32 if torch is not None else None)
         f = _View(tetras.faces, np.uint32, torch.int32 if torch is not None else None)
         self._sync_stream(tetras.vertices, tetras.faces)
-        check(self.L.srt_accel_build_tetrahedra(self.h, v.ptr, v.nbytes // 12, f.ptr,
-                                                f.nbytes // 16))
+        build = self.L.srt_accel_build_tetrahedra_double if dbl else self.L.srt_accel_build_tetrahedra
+        check(build(self.h, v.ptr, v.nbytes // (24 if dbl else 12), f.ptr, f.nbytes // 16))
         self._keep = (v, f)
         self.built = True
         return True

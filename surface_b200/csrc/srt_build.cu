@@ -127,6 +127,98 @@ __device__ __forceinline__ Box cache_box(const float4 *__restrict__ prims, uint3
   return b;
 }
 
+// A tetrahedron of double-precision positions in the primitive cache: 12
+// doubles (six double2) per tetrahedron, its four corners.  Its box pads
+// each coordinate in double and rounds to float (ComputeBoundingBox30 over
+// dvertices: `real v = dvertices[i] -+ kEPS`).
+__device__ __forceinline__ void box_add_d(Box &b, double x, double y, double z, float e) {
+  const double de = (double)e;
+  float m;
+  m = (float)(x - de); if (b.lo[0] > m) b.lo[0] = m;
+  m = (float)(y - de); if (b.lo[1] > m) b.lo[1] = m;
+  m = (float)(z - de); if (b.lo[2] > m) b.lo[2] = m;
+  m = (float)(x + de); if (b.hi[0] < m) b.hi[0] = m;
+  m = (float)(y + de); if (b.hi[1] < m) b.hi[1] = m;
+  m = (float)(z + de); if (b.hi[2] < m) b.hi[2] = m;
+}
+template <int KIND>
+__device__ __forceinline__ Box cache_box(const double2 *__restrict__ prims, uint32_t j,
+                                         float keps) {
+  static_assert(KIND == SRT_TETRAHEDRA, "double-precision cache: tetrahedra only");
+  Box b;
+  box_init(b);
+  double x[12];
+#pragma unroll
+  for (int q = 0; q < 6; q++) {
+    const double2 d = __ldcg(&prims[6 * (size_t)j + q]);
+    x[2 * q] = d.x;
+    x[2 * q + 1] = d.y;
+  }
+#pragma unroll
+  for (int c = 0; c < 4; c++) box_add_d(b, x[3 * c], x[3 * c + 1], x[3 * c + 2], keps);
+  return b;
+}
+
+// Double-precision tetrahedra: the positions rounded to float (the Morton
+// codes' and the shading records' vertices, as real3 takes them), the
+// scene box's partial boxes padded in double, and the double cache.
+__global__ void round_vertices_kernel(const double *__restrict__ dv, size_t n3,
+                                      float *__restrict__ vf) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n3;
+       i += (size_t)gridDim.x * blockDim.x)
+    vf[i] = (float)dv[i];
+}
+
+__global__ void bbox_partial_tet_d_kernel(const double *__restrict__ dv,
+                                          const uint32_t *__restrict__ f, size_t n,
+                                          Box *__restrict__ partial) {
+  Box b;
+  box_init(b);
+  const float e = FLT_EPSILON * 16;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const size_t vi = f[4 * i + c];
+      box_add_d(b, dv[3 * vi], dv[3 * vi + 1], dv[3 * vi + 2], e);
+    }
+  }
+  __shared__ Box sh[kBlock / 32];
+#pragma unroll
+  for (int k = 0; k < 3; k++) {
+    for (int o = 16; o > 0; o >>= 1) {
+      b.lo[k] = fmin_ref(b.lo[k], __shfl_down_sync(0xffffffffu, b.lo[k], o));
+      b.hi[k] = fmax_ref(b.hi[k], __shfl_down_sync(0xffffffffu, b.hi[k], o));
+    }
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  if (l == 0) sh[w] = b;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    Box r = sh[0];
+    for (int i = 1; i < (int)(blockDim.x >> 5); i++) r = box_merge(r, sh[i]);
+    partial[blockIdx.x] = r;
+  }
+}
+
+__global__ void cache_tet_d_kernel(const double *__restrict__ dv, const uint32_t *__restrict__ f,
+                                   const uint32_t *__restrict__ sidx, int n,
+                                   double2 *__restrict__ prims) {
+  for (int j = blockIdx.x * blockDim.x + threadIdx.x; j < n; j += gridDim.x * blockDim.x) {
+    const uint32_t p = sidx[j];
+    double x[12];
+#pragma unroll
+    for (int c = 0; c < 4; c++) {
+      const size_t q = f[4 * (size_t)p + c];
+      x[3 * c] = dv[3 * q];
+      x[3 * c + 1] = dv[3 * q + 1];
+      x[3 * c + 2] = dv[3 * q + 2];
+    }
+#pragma unroll
+    for (int q = 0; q < 6; q++) prims[6 * (size_t)j + q] = make_double2(x[2 * q], x[2 * q + 1]);
+  }
+}
+
 // ------------------------------------------------------------------ 1. scene box
 template <int KIND>
 __global__ void bbox_partial_kernel(const float *__restrict__ v,
@@ -773,8 +865,8 @@ __global__ void cache_kernel(const float *__restrict__ v, const uint32_t *__rest
 // Box of the sorted primitive range [lo, hi] in order -- ComputeBoundingBox30
 // (render/render_accel_triangle.cc:661-709): the first value seen wins ties,
 // as the left-first merges of MergeBoundingBox do.
-template <int KIND>
-__device__ __forceinline__ Box range_box(const float4 *__restrict__ prims, uint32_t lo,
+template <int KIND, typename P = float4>
+__device__ __forceinline__ Box range_box(const P *__restrict__ prims, uint32_t lo,
                                          uint32_t hi, float keps) {
   // groups of four primitives: their loads are issued together
   constexpr int kGroup = 4;
@@ -836,12 +928,12 @@ __device__ __forceinline__ uint32_t arrive(uint32_t *counter) {
 // up, left first, by the second of the two children to finish (arrival
 // counter per node), each climb carrying its own box and reading only the
 // sibling's.  Ancestors of an emitted branch are emitted branches.
-template <int KIND>
+template <int KIND, typename P = float4>
 __global__ void __launch_bounds__(256)
 refit_kernel(const uint32_t *__restrict__ kchild, const uint8_t *__restrict__ kflags,
              const uint2 *__restrict__ krange, const uint32_t *__restrict__ kparent,
              const uint32_t *__restrict__ flag, const uint32_t *__restrict__ kidx, int n,
-             const SceneInfo *__restrict__ scene, const float4 *__restrict__ prims,
+             const SceneInfo *__restrict__ scene, const P *__restrict__ prims,
              uint32_t *__restrict__ counter, BoxP *__restrict__ ibox,
              uint32_t *__restrict__ err) {
   const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -861,7 +953,7 @@ refit_kernel(const uint32_t *__restrict__ kchild, const uint8_t *__restrict__ kf
       lb[side] = cache_box<KIND>(prims, c, keps);
     } else if (leafside[side]) {  // collapsed subtree: one emitted leaf
       const uint2 r = __ldg(&krange[c]);
-      lb[side] = range_box<KIND>(prims, r.x, r.y, keps);
+      lb[side] = range_box<KIND, P>(prims, r.x, r.y, keps);
       ibox_store(ibox, c, lb[side]);  // for the emission, and a sibling's climb
     }
   }
@@ -1034,13 +1126,13 @@ level_scan_kernel(const uint2 *__restrict__ krange, const uint32_t *__restrict__
 }
 
 // ------------------------------------------------------------------ 7. emission
-template <int KIND>
+template <int KIND, typename P = float4>
 __device__ __forceinline__ void child_info(uint32_t c, bool kleaf,
                                            const uint2 *__restrict__ krange,
                                            const uint32_t *__restrict__ flag,
                                            const uint32_t *__restrict__ slot,
                                            const BoxP *__restrict__ ibox,
-                                           const float4 *__restrict__ prims, float keps,
+                                           const P *__restrict__ prims, float keps,
                                            Box &box, bool &is_branch, uint32_t &ref,
                                            uint32_t &count) {
   if (kleaf) {
@@ -1105,6 +1197,7 @@ __device__ __forceinline__ NodeT make_tet_node(const Box &b, uint32_t meta, uint
   return t;
 }
 
+template <typename P = float4>
 __global__ void emit_tet_kernel(const uint32_t *__restrict__ codes,
                                 const uint32_t *__restrict__ kchild,
                                 const uint8_t *__restrict__ kflags,
@@ -1112,7 +1205,7 @@ __global__ void emit_tet_kernel(const uint32_t *__restrict__ codes,
                                 const uint32_t *__restrict__ flag,
                                 const uint32_t *__restrict__ slot,
                                 const BoxP *__restrict__ ibox,
-                                const float4 *__restrict__ prims,
+                                const P *__restrict__ prims,
                                 const SceneInfo *__restrict__ scene,
                                 const uint32_t *__restrict__ kidx,
                                 NodeT *__restrict__ nodes, uint32_t *__restrict__ err) {
@@ -1133,7 +1226,7 @@ __global__ void emit_tet_kernel(const uint32_t *__restrict__ codes,
       Box b;
       bool br;
       uint32_t ref, cnt;
-      child_info<SRT_TETRAHEDRA>(c, fl & (1 << side), krange, flag, slot, ibox, prims,
+      child_info<SRT_TETRAHEDRA, P>(c, fl & (1 << side), krange, flag, slot, ibox, prims,
                                  keps, b, br, ref, cnt);
       uint32_t meta, r;
       if (br) {
@@ -1293,6 +1386,64 @@ srt_status build_kind(srt_accel *a, const float *v, const uint32_t *f,
 #undef ENSURE2
   return cuda_status(cudaGetLastError(), "emit");
 }
+
+}  // namespace
+
+// Build32 of tetrahedra with double-precision positions (the reference's
+// isDoublePrecisionPos, render/render_accel_tetra.cc:1621-1660): the scene
+// box pads each double coordinate in double and rounds to float, the Morton
+// codes take the positions rounded to float (CalculateMortonCodesTetraDouble30
+// builds real3 from them), leaf boxes pad the doubles again, and the
+// primitive cache keeps the doubles for the Pluecker tests.  vf (3 * nverts
+// floats) receives the rounded positions.
+srt_status build_tet_double(srt_accel *a, const double *dv, size_t nverts, const uint32_t *f,
+                            size_t n, float *vf) {
+  srt_ctx *ctx = a->ctx;
+  cudaStream_t st = ctx->stream;
+  cudaError_t e;
+  const size_t m = n - 1;
+  if ((e = a->codes.ensure(n * 4)) != cudaSuccess || (e = a->indices.ensure(n * 4)) != cudaSuccess ||
+      (e = a->prims.ensure(n * 6 * sizeof(double2))) != cudaSuccess ||
+      (e = a->scene.ensure(sizeof(SceneInfo))) != cudaSuccess ||
+      (e = a->nodes.ensure((2 * m + 1) * sizeof(NodeT))) != cudaSuccess ||
+      (e = ctx->s_ibox.ensure((m + 1) * sizeof(BoxP))) != cudaSuccess)
+    return cuda_status(e, "build allocation");
+  SceneInfo *scene = a->scene.as<SceneInfo>();
+  uint32_t *codes = a->codes.as<uint32_t>(), *idx = a->indices.as<uint32_t>();
+  round_vertices_kernel<<<grid_for(3 * nverts, kBlock, ctx->num_sms * 16), kBlock, 0, st>>>(
+      dv, 3 * nverts, vf);
+  const int gb = grid_for(n, kBlock, ctx->num_sms * (n > (4u << 20) ? 4 : 1));
+  if ((e = ctx->s_partial.ensure((size_t)gb * sizeof(Box))) != cudaSuccess)
+    return cuda_status(e, "bbox scratch");
+  Box *partial = ctx->s_partial.as<Box>();
+  bbox_partial_tet_d_kernel<<<gb, kBlock, 0, st>>>(dv, f, n, partial);
+  bbox_final_kernel<SRT_TETRAHEDRA><<<1, 32, 0, st>>>(partial, gb, scene);
+  morton_kernel<SRT_TETRAHEDRA><<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, st>>>(
+      vf, f, n, scene, codes, nullptr);
+  ctx->launches += 4;
+  srt_status s = cuda_status(cudaGetLastError(), "bbox/morton");
+  if (s != SRT_OK) return s;
+  if ((s = sort_pairs(ctx, codes, idx, n, true, 30)) != SRT_OK) return s;
+  Topology T;
+  if ((s = stage_topology(ctx, codes, n, PrimTraits<SRT_TETRAHEDRA>::kMaxLeaf, scene, T)) !=
+      SRT_OK)
+    return s;
+  double2 *prims = a->prims.as<double2>();
+  BoxP *ibox = ctx->s_ibox.as<BoxP>();
+  cache_tet_d_kernel<<<grid_for(n, kBlock, ctx->num_sms * 16), kBlock, 0, st>>>(dv, f, idx,
+                                                                               (int)n, prims);
+  refit_kernel<SRT_TETRAHEDRA, double2><<<(unsigned)((m + kBlock - 1) / kBlock), kBlock, 0, st>>>(
+      T.kchild, T.kflags, T.krange, T.kparent, T.flag, T.kidx, (int)n, scene, prims, T.counter,
+      ibox, ctx->d_err);
+  const int gk = grid_for(m, kBlock, ctx->num_sms * 16);
+  emit_tet_kernel<double2><<<gk, kBlock, 0, st>>>(codes, T.kchild, T.kflags, T.krange, T.flag,
+                                                  T.slot, ibox, prims, scene, T.kidx,
+                                                  a->nodes.as<NodeT>(), ctx->d_err);
+  ctx->launches += 3;
+  return cuda_status(cudaGetLastError(), "tetrahedra (double)");
+}
+
+namespace {
 
 }  // namespace
 

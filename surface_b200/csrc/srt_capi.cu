@@ -171,10 +171,53 @@ static srt_status build_common(srt_accel *a, const float *verts, size_t nverts,
     ctx->inputs_pending = true;
   }
   a->n = nprims;
+  a->dbl = false;
   a->src_verts = static_cast<const float *>(dv);
   a->src_faces = static_cast<const uint32_t *>(df);
   s = build_accel(a, static_cast<const float *>(dv), static_cast<const uint32_t *>(df),
                   static_cast<const float *>(dr), constr, nprims);
+  a->built = (s == SRT_OK);
+  return s;
+}
+
+// Tetrahedra with double-precision positions.
+static srt_status build_tet_d(srt_accel *a, const double *verts, size_t nverts,
+                              const uint32_t *tets, size_t ntets) {
+  if (!a || !verts || !tets || nverts == 0) {
+    set_error("NULL argument");
+    return SRT_ERR_INVALID;
+  }
+  if (a->kind != SRT_TETRAHEDRA) {
+    set_error("accel kind is not tetrahedra");
+    return SRT_ERR_INVALID;
+  }
+  if (ntets < 2 || ntets >= (1u << 30)) {
+    set_error("primitive count must be in [2, 2^30)");
+    return SRT_ERR_INVALID;
+  }
+  srt_ctx *ctx = a->ctx;
+  if (cudaSetDevice(ctx->device) != cudaSuccess) return cuda_status(cudaGetLastError(), "device");
+  const void *dv = nullptr, *df = nullptr;
+  srt_status s = device_view(ctx, verts, nverts * 3 * sizeof(double), a->in_dverts, &dv);
+  if (s != SRT_OK) return s;
+  if ((s = device_view(ctx, tets, ntets * 4 * sizeof(uint32_t), a->in_faces, &df)) != SRT_OK)
+    return s;
+  if (dv != verts || df != tets) {  // as build_common: staged rays wait for these copies
+    cudaError_t e = cudaSuccess;
+    if (!ctx->ev_inputs) e = cudaEventCreateWithFlags(&ctx->ev_inputs, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev_inputs, ctx->stream);
+    if (e != cudaSuccess) return cuda_status(e, "input copy event");
+    ctx->inputs_pending = true;
+  }
+  cudaError_t e = a->in_verts.ensure(nverts * 3 * sizeof(float));
+  if (e != cudaSuccess) return cuda_status(e, "rounded positions");
+  a->n = ntets;
+  a->dbl = true;
+  a->host_scene_valid = false;
+  a->src_verts = a->in_verts.as<float>();
+  a->src_faces = static_cast<const uint32_t *>(df);
+  s = build_tet_double(a, static_cast<const double *>(dv), nverts,
+                       static_cast<const uint32_t *>(df), ntets, a->in_verts.as<float>());
   a->built = (s == SRT_OK);
   return s;
 }
@@ -307,6 +350,12 @@ SRT_API srt_status srt_accel_build_tetrahedra(srt_accel *a, const float *vertice
     return SRT_ERR_INVALID;
   }
   return build_common(a, vertices, nvertices, tets, ntets, 4, nullptr, 0.0f);
+}
+
+SRT_API srt_status srt_accel_build_tetrahedra_double(srt_accel *a, const double *vertices,
+                                                     size_t nvertices, const uint32_t *tets,
+                                                     size_t ntets) {
+  return build_tet_d(a, vertices, nvertices, tets, ntets);
 }
 
 SRT_API srt_status srt_accel_build_spheres(srt_accel *a, const float *centers,

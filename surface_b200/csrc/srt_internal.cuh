@@ -200,6 +200,11 @@ struct srt_accel {
   // or the caller's device arrays, borrowed like the reference's mesh_)
   const float *src_verts = nullptr;
   const uint32_t *src_faces = nullptr;
+  // tetrahedra with double-precision positions: the primitive cache holds
+  // doubles (six double2 per tetrahedron); src_verts the positions rounded
+  // to float; in_dverts a device copy of host positions
+  bool dbl = false;
+  srt::DevBuf in_dverts;
   // host-side cache of the device SceneInfo (valid after a sync)
   srt::SceneInfo host_scene;
   bool host_scene_valid = false;
@@ -223,6 +228,10 @@ srt_status cuda_status(cudaError_t e, const char *what);
 bool is_device_ptr(const void *p);
 
 // build pipeline pieces (srt_build.cu)
+// Build32 of tetrahedra with double-precision positions (srt_build.cu);
+// vf receives the positions rounded to float.
+srt_status build_tet_double(srt_accel *a, const double *dv, size_t nverts, const uint32_t *f,
+                            size_t n, float *vf);
 srt_status build_accel(srt_accel *a, const float *d_verts, const uint32_t *d_faces,
                        const float *d_radius, float const_radius, size_t n);
 // An accel from a tree read from a file (srt_cache.cu): host nodes in the
@@ -246,8 +255,10 @@ struct TopNode {
 };
 // Scene element kinds beyond srt_kind: line and solid accels.
 constexpr int32_t kSceneLines = 3, kSceneSolids = 4;
-// SceneElem.aux bit of a solid element with double-precision positions.
+// SceneElem.aux bit of a solid element with double-precision positions,
+// and of a tetrahedron element with them.
 constexpr int32_t kSolidAuxDouble = 256;
+constexpr int32_t kTetAuxDouble = 512;
 // One element of a scene: a built accel and its transforms, 4x4 doubles in
 // the reference's Matrixd layout (m[row][col], p' = p m + m[3]).  Line and
 // solid elements keep their device nodes in nodes and records in prims;

@@ -440,7 +440,7 @@ SRT_API srt_status srt_scene_build(srt_scene *s) {
       ok = a->built;
       el[i].kind = a->kind;
       el[i].nprims = (uint32_t)a->n;
-      el[i].aux = 0;
+      el[i].aux = a->dbl ? kTetAuxDouble : 0;
       el[i].nodes = a->nodes.p;
       el[i].prims = a->prims.as<float4>();
       el[i].sidx = a->indices.as<uint32_t>();

@@ -171,6 +171,16 @@ __device__ __forceinline__ TetRay tet_ray(D3 orig, D3 dir) {
 }
 
 // A tetrahedron's vertices as stored (float), widened at use.
+// The corners of a tetrahedron of double-precision positions (the same
+// interface; the one-hot axis product of doubles is exact as well).
+struct TetVD {
+  double v[12];
+  __device__ __forceinline__ D3 operator[](int k) const { return {v[3 * k], v[3 * k + 1], v[3 * k + 2]}; }
+  __device__ __forceinline__ double axis(int k, const float (&sel)[3]) const {
+    return (v[3 * k] * (double)sel[0] + v[3 * k + 1] * (double)sel[1]) + v[3 * k + 2] * (double)sel[2];
+  }
+};
+
 struct TetV {
   float v[12];
   __device__ __forceinline__ D3 operator[](int k) const {
@@ -200,7 +210,8 @@ struct TetV {
 // being the reference's ((1 - a - b) * P0 + a * P1) + b * P2.
 // ul1 (the leaving face's barycentric, only a kept hit reports it) is formed
 // only when te < take_below.
-__device__ __forceinline__ bool ray_tet(const TetRay &R, const TetV &V, double take_below,
+template <class TV>
+__device__ __forceinline__ bool ray_tet(const TetRay &R, const TV &V, double take_below,
                                         int &ef, double &ue1, double &ue2, double &ul1,
                                         double &te) {
   const Plk &ray = R.ray;
@@ -899,17 +910,31 @@ struct CtxT {
 };
 
 // (ul1 is formed only for te < take_below: the candidates a caller keeps)
-__device__ __forceinline__ bool candT(const float4 *__restrict__ prims,
+// P: float4 (a float cache, three per tetrahedron) or double2 (a cache of
+// double-precision positions, six per tetrahedron).
+template <typename P>
+__device__ __forceinline__ bool candT(const P *__restrict__ prims,
                                       const uint32_t *__restrict__ sidx, uint32_t j,
                                       const CtxT &c, double take_below, uint32_t &f, int &ef,
                                       double &e1, double &e2, double &ul1, double &te) {
   f = __ldg(&sidx[j]);
   if (f == c.prev_prim) return false;
-  const float4 q0 = __ldg(&prims[3 * (size_t)j]);
-  const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
-  const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
-  const TetV V = {{q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
-  return ray_tet(c.tr, V, take_below, ef, e1, e2, ul1, te) && te >= 0.0;
+  if constexpr (std::is_same<P, double2>::value) {
+    TetVD V;
+#pragma unroll
+    for (int q = 0; q < 6; q++) {
+      const double2 d = __ldg(&prims[6 * (size_t)j + q]);
+      V.v[2 * q] = d.x;
+      V.v[2 * q + 1] = d.y;
+    }
+    return ray_tet(c.tr, V, take_below, ef, e1, e2, ul1, te) && te >= 0.0;
+  } else {
+    const float4 q0 = __ldg(&prims[3 * (size_t)j]);
+    const float4 q1 = __ldg(&prims[3 * (size_t)j + 1]);
+    const float4 q2 = __ldg(&prims[3 * (size_t)j + 2]);
+    const TetV V = {{q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w, q2.x, q2.y, q2.z, q2.w}};
+    return ray_tet(c.tr, V, take_below, ef, e1, e2, ul1, te) && te >= 0.0;
+  }
 }
 
 __device__ __forceinline__ void take_tet(Best &b, double te, double e1, double e2,
@@ -927,8 +952,8 @@ __device__ __forceinline__ void take_tet(Best &b, double te, double e1, double e
 // running distance starting at t0 or, with WINDOW, the reference order
 // through boxes entered before `bnd` keeping only candidates at most `whi`
 // away.
-template <bool WINDOW>
-__device__ void walkT(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
+template <bool WINDOW, typename P = float4>
+__device__ void walkT(const NodeT *__restrict__ nodes, const P *__restrict__ prims,
                       const uint32_t *__restrict__ sidx, const CtxT &c, float bnd,
                       double whi, Best &b, Work &w, uint32_t max_iter, float t0 = FLT_MAX) {
   b = Best();
@@ -978,14 +1003,15 @@ __device__ __forceinline__ double window_hi(double m) {
 
 // The tetrahedron fallback: the reference's walk from pass 1's pruning
 // bound, the full walk if nothing is accepted below it (see ref_walk2_from).
+template <typename P>
 __device__ __forceinline__ void walkT_from(const NodeT *__restrict__ nodes,
-                                           const float4 *__restrict__ prims,
+                                           const P *__restrict__ prims,
                                            const uint32_t *__restrict__ sidx, const CtxT &c,
                                            Best &b, Work &w, uint32_t max_iter, double m) {
-  walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter, bound_rel((float)m, kRelTet));
+  walkT<false, P>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter, bound_rel((float)m, kRelTet));
   if (b.prim != kNone || w.fail) return;
   w.it = 0;
-  walkT<false>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
+  walkT<false, P>(nodes, prims, sidx, c, 0.0f, 0.0, b, w, max_iter);
 }
 
 __device__ __forceinline__ void store_tet(size_t i, const Best &b,
@@ -1044,7 +1070,8 @@ struct TetPass1 {
   }
 
   // Tests the `cnt` tetrahedra of a leaf at sorted slot `ref`, entered at lt.
-  __device__ __forceinline__ void leaf(const float4 *__restrict__ prims,
+  template <typename P>
+  __device__ __forceinline__ void leaf(const P *__restrict__ prims,
                                        const uint32_t *__restrict__ sidx, const CtxT &c,
                                        uint32_t ref, uint32_t cnt, float lt, Best &b) {
     for (uint32_t j = ref; j < ref + cnt; j++) {
@@ -1107,9 +1134,9 @@ __device__ __forceinline__ uint2 tet_entry(float4 lo, float4 hi) {
 // Pass 1 of the default tetrahedron walk for one ray: front to back, stack
 // entries from tet_entry so that a popped branch loads only its children's
 // boxes.
-template <class Stk = LocalStack>
+template <class Stk = LocalStack, typename PT = float4>
 __device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
-                                          const float4 *__restrict__ prims,
+                                          const PT *__restrict__ prims,
                                           const uint32_t *__restrict__ sidx, const CtxT &c,
                                           Best &b, Work &w, uint32_t max_iter, double &m_out,
                                           bool &defer_out, bool &full_out, Stk &&stk = Stk()) {
@@ -1162,9 +1189,9 @@ __device__ __forceinline__ void pass1_tet(const NodeT *__restrict__ nodes,
   P.finish(m_out, defer_out, full_out);
 }
 
-template <bool SINGLE>
+template <bool SINGLE, typename P = float4>
 __global__ void __launch_bounds__(128)
-trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
+trace_tet_kernel(const NodeT *__restrict__ nodes, const P *__restrict__ prims,
                  const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
                  size_t n, srt_hit *__restrict__ hits, uint32_t *__restrict__ subface,
                  const uint32_t *__restrict__ faces, const float *__restrict__ vscalar,
@@ -1197,8 +1224,9 @@ trace_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ pri
   });
 }
 
+template <typename P = float4>
 __global__ void __launch_bounds__(128)
-resolve_tet_kernel(const NodeT *__restrict__ nodes, const float4 *__restrict__ prims,
+resolve_tet_kernel(const NodeT *__restrict__ nodes, const P *__restrict__ prims,
                    const uint32_t *__restrict__ sidx, const srt_ray *__restrict__ rays,
                    srt_hit *__restrict__ hits, uint32_t *__restrict__ subface,
                    const uint32_t *__restrict__ faces, const float *__restrict__ vscalar,
@@ -1402,20 +1430,28 @@ srt_status launch_trace(srt_accel *a, const srt_ray *rays, size_t n, srt_hit *hi
     }
     case SRT_TETRAHEDRA: {
       const NodeT *nd = a->nodes.as<NodeT>();
-      const float4 *pr = a->prims.as<float4>();
       const uint32_t *ix = a->indices.as<uint32_t>();
-      const auto kern = single ? trace_tet_kernel<true> : trace_tet_kernel<false>;
-      kern<<<fgrid((const void *)kern), block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
-                                                        a->src_faces, vscalar, scalar_out,
-                                                        stats, dlist, dcount, max_iter,
-                                                        ctx->d_err, order, next);
-      if (!single) {
-        resolve_tet_kernel<<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, subface,
-                                                    a->src_faces, vscalar, scalar_out,
-                                                    stats, dlist, dcount, max_iter,
-                                                    ctx->d_err);
-        ctx->launches++;
-      }
+      // the primitive cache holds floats, or the doubles of double-precision
+      // positions
+      auto run = [&](auto *pr) {
+        using P = std::remove_cv_t<std::remove_pointer_t<decltype(pr)>>;
+        const auto kern = single ? trace_tet_kernel<true, P> : trace_tet_kernel<false, P>;
+        kern<<<fgrid((const void *)kern), block, 0, st>>>(nd, pr, ix, rays, n, hits, subface,
+                                                          a->src_faces, vscalar, scalar_out,
+                                                          stats, dlist, dcount, max_iter,
+                                                          ctx->d_err, order, next);
+        if (!single) {
+          resolve_tet_kernel<P><<<rgrid, block, 0, st>>>(nd, pr, ix, rays, hits, subface,
+                                                         a->src_faces, vscalar, scalar_out,
+                                                         stats, dlist, dcount, max_iter,
+                                                         ctx->d_err);
+          ctx->launches++;
+        }
+      };
+      if (a->dbl)
+        run(a->prims.as<const double2>());
+      else
+        run(a->prims.as<const float4>());
       break;
     }
   }
@@ -1662,8 +1698,12 @@ __device__ __forceinline__ bool elem_pass1(const SceneElem &e, const typename Ki
                                            bool &full) {
   if constexpr (KIND == SRT_TETRAHEDRA) {
     bool defer;
-    pass1_tet(static_cast<const NodeT *>(e.nodes), e.prims, e.sidx, c, b, w, max_iter, m, defer,
-              full);
+    const NodeT *nodes = static_cast<const NodeT *>(e.nodes);
+    if (e.aux & kTetAuxDouble)
+      pass1_tet(nodes, reinterpret_cast<const double2 *>(e.prims), e.sidx, c, b, w, max_iter, m,
+                defer, full);
+    else
+      pass1_tet(nodes, e.prims, e.sidx, c, b, w, max_iter, m, defer, full);
     return w.fail || !defer;
   } else {
     float mf;
@@ -1686,13 +1726,19 @@ __device__ __forceinline__ void elem_replay(const SceneElem &e,
   w.it = 0;
   if constexpr (KIND == SRT_TETRAHEDRA) {
     const NodeT *nodes = static_cast<const NodeT *>(e.nodes);
-    if (full) {
-      walkT_from(nodes, e.prims, e.sidx, c, b, w, max_iter, m);
-    } else {
-      const double whi = window_hi(m);
-      walkT<true>(nodes, e.prims, e.sidx, c, bound_rel((float)whi, kRelTet), whi, b, w,
-                  max_iter);
-    }
+    auto replay = [&](auto *prims) {
+      if (full) {
+        walkT_from(nodes, prims, e.sidx, c, b, w, max_iter, m);
+      } else {
+        const double whi = window_hi(m);
+        walkT<true>(nodes, prims, e.sidx, c, bound_rel((float)whi, kRelTet), whi, b, w,
+                    max_iter);
+      }
+    };
+    if (e.aux & kTetAuxDouble)
+      replay(reinterpret_cast<const double2 *>(e.prims));
+    else
+      replay(e.prims);
   } else {
     const Node2 *nodes = static_cast<const Node2 *>(e.nodes);
     const float mf = (float)m;
@@ -2281,6 +2327,10 @@ extern "C" SRT_API srt_status srt_trace_closest_noalloc(srt_accel *a, const srt_
       break;
     }
     case SRT_TETRAHEDRA: {
+      if (a->dbl) {
+        set_error("srt_trace_closest_noalloc: double-precision tetrahedra take srt_trace_closest");
+        return SRT_ERR_UNSUPPORTED;
+      }
       const NodeT *nd = a->nodes.as<NodeT>();
       trace_tet_kernel<false><<<grid, block, 0, st>>>(nd, pr, ix, rays, n, hits, nullptr,
                                                       a->src_faces, nullptr, nullptr, nullptr,

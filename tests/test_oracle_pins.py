@@ -174,6 +174,38 @@ def test_oracle_vs_reference_tetra():
 
 
 @need_ref
+@pytest.mark.parametrize("shift", [0.0, 100.0])
+def test_oracle_vs_reference_tetra_double_positions(shift):
+    """isDoublePrecisionPos: tetrahedra over float64 positions that float
+    does not hold (sub-ulp jitter, shifted away from the origin): the
+    oracle's Build32 (double-padded boxes, Morton codes of the rounded
+    positions) and Pluecker tests over the doubles equal the reference's,
+    which differ from a build over the rounded positions."""
+    v, f, _ = S.tet_grid(12, seed=3)
+    rng = np.random.default_rng(9)
+    v64 = v.astype(np.float64) + shift + rng.uniform(-1e-9, 1e-9, size=v.shape)
+    o = O.OracleAccel(O.TET, v64, f)
+    r = O.RefAccel(O.TET, v64, f)
+    assert o.verts.dtype == np.float64 and r.verts.dtype == np.float64
+    rc, ridx = r.canonical()
+    assert np.array_equal(o.canonical(), rc)
+    assert np.array_equal(o.indices, ridx)
+    rays = S.ortho_rays(96, 96)
+    rays["org"] += np.float32(shift)
+    obl = S.pinhole_rays(64, 64, (1.7 + shift, 1.3 + shift, 2.1 + shift),
+                         (0.5 + shift, 0.5 + shift, 0.5 + shift), fov_deg=50)
+    for rr in (rays, obl):
+        (ho, so), (hr, sr) = o.trace(rr, want_subface=True), r.trace(rr)
+        assert np.array_equal(so, sr)
+        for k in ("t", "u", "v", "prim"):
+            assert np.array_equal(bits(ho[k]), bits(hr[k]))
+        assert (hr["prim"] != O.MISS).mean() > 0.3
+    f32 = O.OracleAccel(O.TET, v64.astype(np.float32), f)
+    hf = f32.trace(obl)
+    assert not all(np.array_equal(bits(hf[k]), bits(ho[k])) for k in ("t", "u", "v"))
+
+
+@need_ref
 def test_oracle_vs_reference_spheres_with_coincident_points():
     pos, rad = S.particles(20000, seed=4)
     pos[100:400] = pos[100]  # coincident centres (same Morton key)
