@@ -190,15 +190,20 @@ class GpuTetraAccel : public srt_shim::Base {
  public:
   GpuTetraAccel() : Base(SRT_TETRAHEDRA) {}
   bool Build32(const Tetrahedron *tets, const TetraBuildOptions &) {
-    if (!acc_ || !tets || tets->isDoublePrecisionPos) return false;
+    if (!acc_ || !tets) return false;
     // the vertex count is not stored in Tetrahedron: one past the largest id
     size_t nv = 0;
     for (size_t i = 0; i < 4 * (size_t)tets->numTetrahedrons; i++)
       if (tets->faces[i] + 1 > nv) nv = tets->faces[i] + 1;
     tets_ = tets;
-    return srt_accel_build_tetrahedra(acc_, tets->vertices, nv, tets->faces,
-                                      tets->numTetrahedrons) == SRT_OK &&
-           srt_ctx_synchronize(srt_shim::context()) == SRT_OK;
+    // double-precision positions (dvertices) keep their precision
+    const srt_status s =
+        tets->isDoublePrecisionPos
+            ? srt_accel_build_tetrahedra_double(acc_, tets->dvertices, nv, tets->faces,
+                                                tets->numTetrahedrons)
+            : srt_accel_build_tetrahedra(acc_, tets->vertices, nv, tets->faces,
+                                         tets->numTetrahedrons);
+    return s == SRT_OK && srt_ctx_synchronize(srt_shim::context()) == SRT_OK;
   }
 
  private:
