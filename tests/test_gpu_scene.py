@@ -228,3 +228,36 @@ def test_explicit_matrices_and_errors(mixed):
         RenderGraph().Build()  # empty scene
     with pytest.raises(sb.SurfaceError):
         RenderGraph().AddRenderElement(sb.TriangleAccel(), np.eye(4))  # not built
+
+
+def test_deep_line_element_in_a_scene():
+    """A line element whose tree is 90 levels deep (a chain of segments at
+    midpoints 2^-k, every split peels one off) beside a triangle element:
+    the per-ray loop runs with the long walk stack and equals the oracle."""
+    name, pos, seg, rad, constr, opts, rays = [c for c in S.line_cases() if c[0] == "chain"][0]
+    lines = sb.LineAccel()
+    lines.Build(sb.Lines(pos, seg, rad, constr), sb.LineBuildOptions(minLeafPrimitives=1))
+    assert lines.info()[2] > 62
+    tv, tf = S.displaced_octasphere(2, seed=8)
+    tri = sb.TriangleAccel()
+    tri.Build32(sb.Mesh(tv, tf))
+    Ts = [np.eye(4), S.affine(scale=(0.3,) * 3, translate=(0.5, 0.8, 0.0))]
+    g = RenderGraph()
+    g.AddRenderElement(lines, Ts[0])
+    g.AddRenderElement(tri, Ts[1])
+    g.Build()
+    oacc = [O.OracleLines(pos, seg, None, constr, min_leaf=1), O.OracleAccel(O.TRI, tv, tf)]
+    mats, wlo, whi = [], [], []
+    for a, T in zip((lines, tri), Ts):
+        lo, hi = a.BoundingBox()
+        i1, i2, b0, b1 = O.element_update(T, lo, hi)
+        mats.append((np.asarray(T, np.float64).reshape(16), i1.reshape(16), i2.reshape(16)))
+        wlo.append(b0)
+        whi.append(b1)
+    o = O.OracleScene(oacc, [m[0] for m in mats], [m[1] for m in mats], [m[2] for m in mats],
+                      wlo, whi)
+    want, wel = o.trace(rays)
+    assert (wel == 0).sum() > 10
+    got, gel = g.Trace(rays)
+    assert np.array_equal(gel, wel)
+    assert np.array_equal(got.view(np.uint32), want.view(np.uint32))
