@@ -685,7 +685,9 @@ SRT_API srt_status srt_batch_set_tuning(srt_batch *b, int32_t block,
  * same spatial-median tree and line order (positions: nverts xyz floats;
  * radius: per vertex or NULL for constant_radius; segments: 2 vertex indices
  * per line; min_leaf, max_depth and cap as LineBuildOptions, 0 for its
- * defaults 4 and 512).  srt_line_trace replaces LineAccel::Traverse (:704):
+ * defaults 4 and 512), built on the GPU level by level; a segment naming a
+ * vertex beyond nverts, or a NaN position or radius, is SRT_ERR_INVALID.
+ * srt_line_trace replaces LineAccel::Traverse (:704):
  * closest hit per ray (t, u, v, line index; u = distance from the axis on a
  * cap, v = 0 / 1 on a cap or the position along the axis), normals (3 floats
  * per ray, BuildIntersection's, may be NULL); stats (device memory, NULL
