@@ -641,13 +641,19 @@ __device__ __forceinline__ void store_node2(size_t i, const Best &b, const Ctx2 
   normal_out[3 * i + 2] = nn[2];
 }
 
+// Work counters of the rays the active lanes finished, merged per warp
+// before the atomics (per-ray atomics on four addresses serialise in L2).
 __device__ __forceinline__ void add_stats(unsigned long long *stats, const Work &w,
                                           uint32_t full) {
   if (!stats) return;
-  atomicAdd(&stats[0], (unsigned long long)w.branch);
-  atomicAdd(&stats[1], (unsigned long long)w.leaf);
-  atomicAdd(&stats[2], (unsigned long long)w.prim);
-  if (full) atomicAdd(&stats[3], 1ull);
+  const unsigned m = __activemask();
+  const int leader = __ffs(m) - 1;
+  const uint32_t c[4] = {w.branch, w.leaf, w.prim, full ? 1u : 0u};
+#pragma unroll
+  for (int k = 0; k < 4; k++) {
+    const uint32_t s = __reduce_add_sync(m, c[k]);
+    if ((int)(threadIdx.x & 31u) == leader && s) atomicAdd(&stats[k], (unsigned long long)s);
+  }
 }
 
 template <int KIND>
