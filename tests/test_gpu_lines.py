@@ -86,3 +86,25 @@ def test_dump_and_bbox(tmp_path):
     bad[5, 1] = pos.shape[0]  # a vertex past the end
     with pytest.raises(sb.SurfaceError):
         LineAccel().Build(Lines(pos, bad, rad))
+
+
+def test_bad_inputs_rejected():
+    """A NaN position and a segment naming a vertex beyond nverts end the
+    GPU build with SRT_ERR_INVALID (the build kernel flags them and reads
+    no vertex out of range); the accel then builds and traces normally."""
+    from surface_b200 import SurfaceError
+    pos, seg, rad = S.line_strands(300, 4, seed=2)
+    acc = LineAccel()
+    bad = pos.copy()
+    bad[7, 1] = np.nan
+    with pytest.raises(SurfaceError):
+        acc.Build(Lines(bad, seg, rad))
+    seg2 = seg.copy()
+    seg2[5, 1] = pos.shape[0] + 3
+    with pytest.raises(SurfaceError):
+        acc.Build(Lines(pos, seg2, rad))
+    acc.Build(Lines(pos, seg, rad))
+    gn, gi = acc.export()
+    on, oi = O.OracleLines(pos, seg, rad).export()
+    assert np.array_equal(O.line_nodes_masked(on).tobytes(), O.line_nodes_masked(gn).tobytes())
+    assert np.array_equal(gi, oi)
